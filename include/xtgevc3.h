@@ -1,0 +1,97 @@
+/*
+ * xtgevc3 -- C ABI of the B200 (sm_100a) implementation of the blocked generalized
+ * eigenvector routines xTGEVC3.
+ *
+ * Given an upper quasi-triangular S and upper triangular P (real), or upper triangular S
+ * and P (complex), as produced by a generalized Schur factorisation (xGGES), compute some
+ * or all right eigenvectors x (beta*S*x = alpha*P*x) and/or left eigenvectors y
+ * (y^H*(beta*S - alpha*P) = 0), optionally multiplied by the Schur vectors Z / Q.
+ *
+ * Argument meaning, INFO codes and the LWORK=-1 workspace query are those of the upstream
+ * library (include/tgevc3.h:9-12 of vlovero/xTGEVC3):
+ *   side    'R', 'L' or 'B' (any other value computes nothing and returns INFO = 0)
+ *   howmny  'A' all, 'B' all and back-transformed by VR = Z / VL = Q given on entry,
+ *           'S' the eigenvalues flagged in select (a complex pair counts when either of its
+ *           two flags is set; select may be NULL, which selects nothing)
+ *   mm      columns available in VL/VR;  *m (may be NULL) receives the columns used
+ *   work/lwork  lwork = -1 returns the upstream workspace size in work[0]; the GPU path
+ *           does not use the workspace but keeps the size rule and its error code
+ *   info    0 success, -2 bad howmny, -16 mm too small, -19 lwork too small,
+ *           1 a CUDA call failed (text in xtgevc3_last_error()); positive codes are new:
+ *           the upstream code never returns them.
+ * Real pencils return a complex pair (k, k+1) as two columns (Re x, Im x) of the
+ * eigenvector for alphar[k] + i*alphai[k] (alphai[k] > 0); columns are in ascending
+ * eigenvalue order.  Complex arrays are interleaved (re, im) pairs, the layout of
+ * std::complex / C99 _Complex.  Matrices are column-major.
+ *
+ * Output scale: unless XTGEVC3_NORMALIZE is set the eigenvectors carry the scale of the
+ * upstream algorithm (x_k = 1 on the eigenvalue's own row); when the overflow guards fire,
+ * this implementation scales single columns where the upstream code scales a 32-column
+ * panel, so those columns differ from the upstream output by a positive factor.
+ */
+#ifndef XTGEVC3_H
+#define XTGEVC3_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Option flags. */
+#define XTGEVC3_NORMALIZE 1u /* scale every eigenvector (a real pair jointly) to max_i |re|+|im| = 1 */
+#define XTGEVC3_SIMT 2u      /* use the SIMT GEMM kernels instead of the FP64 tensor-core kernel */
+
+/* Process-wide flags used by the drop-in entry points below (default 0). */
+void xtgevc3_set_flags(unsigned flags);
+unsigned xtgevc3_get_flags(void);
+
+/* Text of the last CUDA failure seen by the calling thread ("" if none). */
+const char *xtgevc3_last_error(void);
+
+/* ---- host-pointer entry points (drop-in) -------------------------------------------
+ * C-linkage twins of dtgevc3/stgevc3/ztgevc3/ctgevc3 (include/tgevc3.h).  Inputs are
+ * copied to the current CUDA device, results copied back before return.             */
+
+/* replaces upstream dtgevc3, src/dtgevc3.cpp:1150 */
+void xtgevc3_dtgevc3(char side, char howmny, const int *select, int n, const double *S, int lds, const double *P,
+                     int ldp, const double *alphar, const double *alphai, const double *beta, double *VL, int ldvl,
+                     double *VR, int ldvr, int mm, int *m, double *work, int lwork, int *info);
+/* replaces upstream stgevc3, src/stgevc3.cpp:1122 */
+void xtgevc3_stgevc3(char side, char howmny, const int *select, int n, const float *S, int lds, const float *P,
+                     int ldp, const float *alphar, const float *alphai, const float *beta, float *VL, int ldvl,
+                     float *VR, int ldvr, int mm, int *m, float *work, int lwork, int *info);
+/* replaces upstream ztgevc3, src/ztgevc3.cpp:435 (complex arrays interleaved) */
+void xtgevc3_ztgevc3(char side, char howmny, const int *select, int n, const double *S, int lds, const double *P,
+                     int ldp, const double *alpha, const double *beta, double *VL, int ldvl, double *VR, int ldvr,
+                     int mm, int *m, double *work, int lwork, int *info);
+/* replaces upstream ctgevc3, src/ctgevc3.cpp:435 (complex arrays interleaved) */
+void xtgevc3_ctgevc3(char side, char howmny, const int *select, int n, const float *S, int lds, const float *P,
+                     int ldp, const float *alpha, const float *beta, float *VL, int ldvl, float *VR, int ldvr, int mm,
+                     int *m, float *work, int lwork, int *info);
+
+/* ---- device-pointer entry points ----------------------------------------------------
+ * Same computation on matrices already resident on the current CUDA device: S, P, VL, VR
+ * are device pointers; the alpha, alphai, beta and select arrays are HOST arrays of
+ * length n.  Work is queued on
+ * `stream` (a cudaStream_t, NULL = legacy default stream) and complete on return.
+ * Scratch memory comes from the device's stream-ordered pool.  INFO as above (no
+ * workspace argument, so no -19).  Returns 0, or 1 if a CUDA call failed.
+ * These have no upstream counterpart (the upstream library is CPU-only).              */
+int xtgevc3_dtgevc3_dev(unsigned flags, void *stream, char side, char howmny, const int *select, int n,
+                        const double *S, int lds, const double *P, int ldp, const double *alphar,
+                        const double *alphai, const double *beta, double *VL, int ldvl, double *VR, int ldvr, int mm,
+                        int *m, int *info);
+int xtgevc3_stgevc3_dev(unsigned flags, void *stream, char side, char howmny, const int *select, int n,
+                        const float *S, int lds, const float *P, int ldp, const float *alphar, const float *alphai,
+                        const float *beta, float *VL, int ldvl, float *VR, int ldvr, int mm, int *m, int *info);
+int xtgevc3_ztgevc3_dev(unsigned flags, void *stream, char side, char howmny, const int *select, int n,
+                        const double *S, int lds, const double *P, int ldp, const double *alpha, const double *beta,
+                        double *VL, int ldvl, double *VR, int ldvr, int mm, int *m, int *info);
+int xtgevc3_ctgevc3_dev(unsigned flags, void *stream, char side, char howmny, const int *select, int n,
+                        const float *S, int lds, const float *P, int ldp, const float *alpha, const float *beta,
+                        float *VL, int ldvl, float *VR, int ldvr, int mm, int *m, int *info);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XTGEVC3_H */

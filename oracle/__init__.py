@@ -1,0 +1,283 @@
+"""CPU oracle for the xTGEVC3 path -- TEST INFRASTRUCTURE ONLY.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU legs of ``bench.py`` import
+this package, and only as the checker / CPU baseline.  The product
+(``xtgevc3_b200``) never imports it.
+
+Contents
+  * ctypes bindings of two CPU implementations with the upstream argument list:
+      - ``oracle`` : this repository's C restatement (oracle/tgevc3_oracle.c),
+      - ``ref``    : the upstream sources compiled as they are (oracle/_ref, built by
+                     ``make -C oracle ref`` where the upstream tree is present);
+  * residual checks and the comparison normalisation (the seeded pencil generators live
+    in ``xtgevc3_b200.pencils`` and are re-exported here for the tests).
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "liboracle_tgevc3.so")
+REF_SO = os.path.join(HERE, "_ref", "libref_tgevc3.so")
+
+_libs: dict = {}
+
+
+def build(ref: bool = False) -> None:
+    """Compile the C restatement (and, with ``ref``, the upstream sources)."""
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    if ref:
+        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+
+
+def _load(path: str, prefix: str):
+    lib = ct.CDLL(path)
+    P = ct.c_void_p
+    I = ct.c_int
+    Ch = ct.c_char
+    for p in "ds":
+        f = getattr(lib, f"{prefix}{p}tgevc3")
+        f.argtypes = [Ch, Ch, P, I, P, I, P, I, P, P, P, P, I, P, I, I, P, P, I, P]
+        f.restype = None
+    for p in "zc":
+        f = getattr(lib, f"{prefix}{p}tgevc3")
+        f.argtypes = [Ch, Ch, P, I, P, I, P, I, P, P, P, I, P, I, I, P, P, I, P]
+        f.restype = None
+    return lib
+
+
+def oracle_lib():
+    if "oracle" not in _libs:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        _libs["oracle"] = _load(ORACLE_SO, "oracle_")
+    return _libs["oracle"]
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    if "ref" not in _libs:
+        if not ref_available():
+            raise FileNotFoundError(REF_SO)
+        lib = _load(REF_SO, "ref_")
+        lib.ref_set_num_threads.argtypes = [ct.c_int]
+        _libs["ref"] = lib
+    return _libs["ref"]
+
+
+def set_ref_threads(n: int) -> None:
+    ref_lib().ref_set_num_threads(int(n))
+
+
+_PREFIX = {np.float64: "d", np.float32: "s", np.complex128: "z", np.complex64: "c"}
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ct.c_void_p)
+
+
+def tgevc3(side, howmny, S, P, alpha, beta, alphai=None, VL=None, VR=None, select=None,
+           impl="oracle", lwork=None, mm=None):
+    """Call ``<impl>_{d,s,z,c}tgevc3`` with the upstream argument list.
+
+    Real pencils pass ``alpha`` = alphar and ``alphai``; complex pencils pass complex
+    ``alpha``.  S, P, VL, VR are Fortran-ordered; VL/VR are updated in place (they hold
+    Q/Z on entry for HOWMNY='B') and also returned.  Returns (VL, VR, m, info).
+    """
+    lib = oracle_lib() if impl == "oracle" else ref_lib()
+    dt = S.dtype.type
+    pfx = _PREFIX[dt]
+    n = S.shape[0]
+    fn = getattr(lib, f"{'oracle_' if impl == 'oracle' else 'ref_'}{pfx}tgevc3")
+    S = np.asfortranarray(S)
+    P = np.asfortranarray(P)
+    sel = None if select is None else np.ascontiguousarray(select, dtype=np.int32)
+    mm = n if mm is None else mm
+    if VL is None:
+        VL = np.zeros((n, max(mm, 1)), dtype=dt, order="F")
+    if VR is None:
+        VR = np.zeros((n, max(mm, 1)), dtype=dt, order="F")
+    m = ct.c_int(0)
+    info = ct.c_int(0)
+    q = np.zeros(2, dtype=dt)
+    ld = max(n, 1)
+    rdt = np.float64 if pfx in "dz" else np.float32
+    args_head = [side.encode(), howmny.encode(), _ptr(sel), n, _ptr(S), ld, _ptr(P), ld]
+    if pfx in "ds":
+        al = np.ascontiguousarray(alpha, dtype=rdt)
+        ai = np.ascontiguousarray(alphai, dtype=rdt)
+        be = np.ascontiguousarray(beta, dtype=rdt)
+        eig = [_ptr(al), _ptr(ai), _ptr(be)]
+    else:
+        al = np.ascontiguousarray(alpha, dtype=dt)
+        be = np.ascontiguousarray(beta, dtype=dt)
+        eig = [_ptr(al), _ptr(be)]
+    tail = [_ptr(VL), ld, _ptr(VR), ld, mm, ct.byref(m)]
+    if lwork is None:
+        fn(*args_head, *eig, *tail, _ptr(q), -1, ct.byref(info))
+        if info.value != 0:
+            return VL, VR, m.value, info.value
+        lwork = int(np.real(q[0]))
+    work = np.zeros(max(lwork, 1), dtype=dt)
+    fn(*args_head, *eig, *tail, _ptr(work), lwork, ct.byref(info))
+    return VL, VR, m.value, info.value
+
+
+from xtgevc3_b200.pencils import (gen_quasi_triangular, gen_upper_triangular_complex,  # noqa: E402,F401
+                                  gen_gges, gen_schur_like)
+
+
+def _openblas():
+    if "openblas" not in _libs:
+        import glob
+        import scipy
+        d = os.path.join(os.path.dirname(scipy.__file__), "..", "scipy.libs")
+        _libs["openblas"] = ct.CDLL(sorted(glob.glob(os.path.join(d, "libscipy_openblas*.so")))[0])
+    return _libs["openblas"]
+
+
+def lapack_tgevc(S, P):
+    """Second oracle: LAPACK xTGEVC (SIDE='B', HOWMNY='A') from SciPy's bundled OpenBLAS,
+    called through its Fortran interface.  Returns (VL, VR); LAPACK normalises each
+    eigenvector so that max |re| + |im| = 1."""
+    dt = S.dtype.type
+    pfx = _PREFIX[dt]
+    n = S.shape[0]
+    f = getattr(_openblas(), f"scipy_{pfx}tgevc_")
+    S = np.asfortranarray(S)
+    P = np.asfortranarray(P)
+    VL = np.zeros((n, n), dtype=dt, order="F")
+    VR = np.zeros((n, n), dtype=dt, order="F")
+    cplx = pfx in "zc"
+    rdt = np.float64 if pfx in "dz" else np.float32
+    work = np.zeros(6 * n if not cplx else 2 * n, dtype=dt)
+    rwork = np.zeros(2 * n, dtype=rdt)
+    iv = lambda v: ct.byref(ct.c_int(v))  # noqa: E731
+    m = ct.c_int(0)
+    info = ct.c_int(0)
+    args = [ct.c_char_p(b"B"), ct.c_char_p(b"A"), None, iv(n), _ptr(S), iv(n), _ptr(P), iv(n), _ptr(VL), iv(n),
+            _ptr(VR), iv(n), iv(n), ct.byref(m), _ptr(work)]
+    if cplx:
+        args.append(_ptr(rwork))
+    args += [ct.byref(info), ct.c_size_t(1), ct.c_size_t(1)]
+    f(*args)
+    if info.value != 0:
+        raise RuntimeError(f"{pfx}tgevc info={info.value}")
+    return VL, VR
+
+
+# --------------------------------------------------------------------------------------
+# residuals and normalisation
+# --------------------------------------------------------------------------------------
+
+def eig_columns(alphai, n_cols=None):
+    """Yield (col, is_pair) for real eigenvector storage: a pair occupies (Re, Im) columns."""
+    k = 0
+    n = len(alphai) if n_cols is None else n_cols
+    while k < n:
+        pair = alphai[k] != 0 and k + 1 < len(alphai)
+        yield k, pair
+        k += 2 if pair else 1
+
+
+def selected_items(n, howmny, select=None, alphai=None):
+    """(k, is_pair) of every computed eigenvector in output order (upstream selection rule,
+    src/dtgevc3.cpp:1193-1207: a pair counts when either flag is set)."""
+    items = []
+    k = 0
+    while k < n:
+        pair = alphai is not None and alphai[k] != 0 and k + 1 < n
+        sel = howmny in ("A", "B")
+        if howmny == "S" and select is not None:
+            sel = bool(select[k]) or (pair and bool(select[k + 1]))
+        if sel:
+            items.append((k, pair))
+        k += 2 if pair else 1
+    return items
+
+
+def to_complex_real_storage(V, alphai, howmny="A", select=None):
+    """Real (Re, Im)-pair storage -> complex matrix with one column per eigenvalue
+    (a pair's second column becomes the conjugate eigenvector)."""
+    n, m = V.shape
+    W = V.astype(np.complex128)
+    c = 0
+    for k, pair in selected_items(len(alphai), howmny, select, alphai):
+        if c >= m:
+            break
+        if pair:
+            W[:, c] = V[:, c] + 1j * V[:, c + 1]
+            W[:, c + 1] = V[:, c] - 1j * V[:, c + 1]
+            c += 2
+        else:
+            c += 1
+    return W
+
+
+def column_eigenvalues(alpha, beta, howmny="A", select=None, alphai=None):
+    """(alpha, beta) of each output column, complex alpha for real pencils."""
+    n = len(beta)
+    a = np.asarray(alpha) + (1j * np.asarray(alphai) if alphai is not None else 0)
+    idx = []
+    for k, pair in selected_items(n, howmny, select, alphai):
+        idx += [k, k + 1] if pair else [k]
+    idx = np.array(idx, dtype=int)
+    return a[idx], np.asarray(beta)[idx]
+
+
+def residual_ratio(S, P, V, alpha, beta, left=False):
+    """Per column: ||beta*S*v - alpha*P*v||_1 / ((|beta|*||S||_1 + |alpha|*||P||_1) * ||v||_1) / eps,
+    the DGET52-style measure of tests/test_lapack_d.cpp:38-168 (complex V, complex alpha)."""
+    eps = np.finfo(np.float64 if V.real.dtype == np.float64 else np.float32).eps
+    S = S.astype(np.complex128)
+    P = P.astype(np.complex128)
+    V = V.astype(np.complex128)
+    # the ratio is invariant under (S, alpha) -> (S, alpha)/s and (P, beta) -> (P, beta)/p;
+    # working with unit-norm S, P keeps pencils scaled near overflow finite here
+    nS0 = max(np.abs(S).sum(0).max(), 1e-300)
+    nP0 = max(np.abs(P).sum(0).max(), 1e-300)
+    S, alpha = S / nS0, np.asarray(alpha) / nS0
+    P, beta = P / nP0, np.asarray(beta) / nP0
+    V = V / np.maximum(np.abs(V).max(0), 1e-300)[None, :]
+    nS = nP = 1.0
+    if left:
+        R = (S.conj().T @ V) * np.conj(beta)[None, :] - (P.conj().T @ V) * np.conj(alpha)[None, :]
+    else:
+        R = (S @ V) * beta[None, :] - (P @ V) * alpha[None, :]
+    nv = np.abs(V).sum(0)
+    nv[nv == 0] = 1.0
+    den = (np.abs(beta) * nS + np.abs(alpha) * nP) * nv
+    den = np.maximum(den, np.finfo(np.float64).tiny)
+    return np.abs(R).sum(0) / den / eps
+
+
+def normalize_like(V, Vref):
+    """Scale each complex column of V and Vref by their value at the row where |Vref| is
+    largest, so both carry the same (scale, phase) convention.  Returns (V', Vref')."""
+    idx = np.argmax(np.abs(Vref), axis=0)
+    cols = np.arange(V.shape[1])
+    a = V[idx, cols]
+    b = Vref[idx, cols]
+    a = np.where(a == 0, 1, a)
+    b = np.where(b == 0, 1, b)
+    return V / a[None, :], Vref / b[None, :]
+
+
+def max_rel_diff(V, Vref):
+    """Max over columns of max|v - vref| / max|vref| after ``normalize_like``; also
+    returns the per-column array.  Non-finite reference columns are reported as nan."""
+    Vn, Rn = normalize_like(V, Vref)
+    num = np.abs(Vn - Rn).max(0)
+    den = np.abs(Rn).max(0)
+    den[den == 0] = 1.0
+    err = num / den
+    bad = ~np.isfinite(Vref).all(0)
+    err[bad] = np.nan
+    return (np.nanmax(err) if np.isfinite(err).any() else 0.0), err

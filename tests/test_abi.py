@@ -1,0 +1,114 @@
+"""The C-ABI library: it loads, exports every symbol the headers declare, and implements
+the upstream argument checks (INFO, M, LWORK query) -- all without touching a GPU."""
+import ctypes as ct
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import xtgevc3_b200 as X
+from conftest import ROOT
+
+HEADERS = [os.path.join(ROOT, "include", h) for h in ("xtgevc3.h", "tgevc3.h")]
+
+
+def declared_c_functions():
+    src = open(HEADERS[0]).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(xtgevc3_\w+)\s*\(", src)))
+
+
+def exported():
+    out = subprocess.run(["nm", "-D", "--defined-only", X.lib()._name], capture_output=True, text=True).stdout
+    return {line.split()[-1] for line in out.splitlines() if line.strip()}
+
+
+def test_exports_c_abi():
+    syms = exported()
+    decl = declared_c_functions()
+    assert len(decl) >= 11
+    missing = [f for f in decl if f not in syms]
+    assert not missing, missing
+
+
+def test_exports_cpp_dropin_symbols():
+    """include/tgevc3.h keeps C++ linkage, like the upstream header: the mangled names of
+    the four upstream functions must be defined by libxtgevc3.so."""
+    syms = exported()
+    demangled = subprocess.run(["c++filt"], input="\n".join(sorted(syms)), capture_output=True,
+                               text=True).stdout.splitlines()
+    for p, t in (("d", "double"), ("s", "float"), ("z", "std::complex<double>"), ("c", "std::complex<float>")):
+        want = f"{p}tgevc3(char, char, int const*, int, {t} const*, int, {t} const*, int"
+        assert any(d.startswith(want) for d in demangled), p
+
+
+@pytest.mark.parametrize("pfx", ["d", "s", "z", "c"])
+def test_lwork_query_and_info_codes(pfx):
+    from xtgevc3_b200 import pencils
+    n = 17
+    if pfx in "ds":
+        dt = np.float64 if pfx == "d" else np.float32
+        S, P, ar, ai, be = pencils.gen_quasi_triangular(n, 3, dtype=dt)
+        kw = dict(alphai=ai)
+        al = ar
+    else:
+        dt = np.complex128 if pfx == "z" else np.complex64
+        S, P, al, be = pencils.gen_upper_triangular_complex(n, 3, dtype=dt)
+        kw = {}
+    # LWORK = -1 query: upstream formula 2n(b+1) + 4(b+1)^2 + 2(b+1), b = 32
+    lib = X.lib()
+    m = ct.c_int(-1)
+    info = ct.c_int(-99)
+    q = np.zeros(2, dtype=dt)
+    rdt = np.float64 if pfx in "dz" else np.float32
+    head = [b"B", b"A", None, n, S.ctypes.data_as(ct.c_void_p), n, P.ctypes.data_as(ct.c_void_p), n]
+    VL = np.zeros((n, n), dtype=dt, order="F")
+    VR = np.zeros((n, n), dtype=dt, order="F")
+    if pfx in "ds":
+        eig = [np.ascontiguousarray(a, dtype=rdt) for a in (al, kw["alphai"], be)]
+    else:
+        eig = [np.ascontiguousarray(a, dtype=dt) for a in (al, be)]
+    eigp = [e.ctypes.data_as(ct.c_void_p) for e in eig]
+    f = getattr(lib, f"xtgevc3_{pfx}tgevc3")
+    f(*head, *eigp, VL.ctypes.data_as(ct.c_void_p), n, VR.ctypes.data_as(ct.c_void_p), n, n, ct.byref(m),
+      q.ctypes.data_as(ct.c_void_p), -1, ct.byref(info))
+    assert info.value == 0 and m.value == n
+    assert int(np.real(q[0])) == X.lwork_query(pfx, n) == 2 * n * 33 + 4 * 33 * 33 + 66
+    # bad HOWMNY -> -2 (SIDE is not validated upstream)
+    _, _, _, inf = X.tgevc3("B", "Q", S, P, al, be, **kw)
+    assert inf == -2
+    # MM < M -> -16, and M is still reported
+    _, _, mm, inf = X.tgevc3("B", "A", S, P, al, be, mm=3, **kw)
+    assert inf == -16 and mm == n
+    # LWORK too small for every block size -> -19
+    _, _, mm, inf = X.tgevc3("B", "A", S, P, al, be, lwork=5, **kw)
+    assert inf == -19
+    # n = 0 -> info 0, m = 0
+    e = np.zeros((0, 0), dtype=dt, order="F")
+    _, _, mm, inf = X.tgevc3("B", "A", e, e, np.zeros(0, dt), np.zeros(0, dt),
+                             **({"alphai": np.zeros(0, dt)} if pfx in "ds" else {}), mm=0)
+    assert inf == 0 and mm == 0
+    # HOWMNY='S' with no selection: nothing computed, info 0
+    _, _, mm, inf = X.tgevc3("B", "S", S, P, al, be, select=np.zeros(n, np.int32), **kw)
+    assert inf == 0 and mm == 0
+
+
+def test_selection_count_pairs():
+    """A pair counts (2 columns) when either flag is set; a pair flag on the last row is real."""
+    from xtgevc3_b200 import pencils
+    S, P, ar, ai, be = pencils.gen_quasi_triangular(30, 9, pair_frac=0.6)
+    pairs = [k for k in range(29) if ai[k] > 0]
+    k = pairs[0]
+    sel = np.zeros(30, np.int32)
+    sel[k + 1] = 1  # only the second flag of the pair
+    _, _, m, info = X.tgevc3("R", "S", S, P, ar, be, alphai=ai, select=sel, mm=0)
+    assert info == -16 and m == 2
+
+
+def test_flags_roundtrip():
+    old = X.get_flags()
+    X.set_flags(X.NORMALIZE | X.SIMT)
+    assert X.get_flags() == 3
+    X.set_flags(old)

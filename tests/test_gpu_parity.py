@@ -1,0 +1,201 @@
+"""CUDA path (libxtgevc3.so through its C ABI) against the upstream outputs and the oracle.
+
+Tolerances (stated per test): after both sides are scaled by the reference's value at the
+reference's largest component (``oracle.normalize_like``), the elementwise difference
+relative to the column max must be below TOL; the DGET52-style residual of
+tests/test_lapack_d.cpp:38-168 (in units of eps) must be below 100, the upstream warning
+level.  Eigenvectors of the random triangular pencils of the upstream self-tests are
+ill-conditioned (components spread over many orders of magnitude), so those cases get a
+looser elementwise bound than the xGGES pencils.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import xtgevc3_b200 as X
+from conftest import golden_files, load_golden
+from xtgevc3_b200 import pencils
+
+pytestmark = pytest.mark.gpu
+
+TOL_WELL = {np.float64: 1e-11, np.complex128: 1e-11, np.float32: 2e-4, np.complex64: 2e-4}
+TOL_ILL = {np.float64: 1e-8, np.complex128: 1e-8, np.float32: 5e-3, np.complex64: 5e-3}
+
+
+def as_complex(V, d):
+    if d.get("alphai") is not None and np.isrealobj(V):
+        return oracle.to_complex_real_storage(V, d["alphai"], d["howmny"], d.get("select"))
+    return V.astype(np.complex128)
+
+
+def compare(d, VL, VR, m, VLr, VRr, tol, check_resid=True):
+    howmny = d["howmny"]
+    for side, V, Vr in (("L", VL, VLr), ("R", VR, VRr)):
+        if d["side"] not in (side, "B"):
+            continue
+        V, Vr = V[:, :m], Vr[:, :m]
+        a, b = as_complex(V, d), as_complex(Vr, d)
+        err, cols = oracle.max_rel_diff(a, b)
+        assert err <= tol, (side, err, int(np.nanargmax(cols)))
+        if check_resid and howmny in ("A", "S"):
+            al, be = oracle.column_eigenvalues(d["alpha"], d["beta"], howmny, d.get("select"), d.get("alphai"))
+            r = oracle.residual_ratio(d["S"], d["P"], a, al, be, left=(side == "L"))
+            assert r.max() < 100, (side, r.max())
+
+
+def run_gpu(d, **kw):
+    return X.tgevc3(d["side"], d["howmny"], d["S"], d["P"], d["alpha"], d["beta"], alphai=d.get("alphai"),
+                    VL=d["VL_in"].copy(order="F"), VR=d["VR_in"].copy(order="F"), select=d.get("select"), **kw)
+
+
+@pytest.mark.parametrize("path", golden_files(), ids=lambda p: p.split("/")[-1][:-4])
+def test_golden(cuda_ok, path):
+    d = load_golden(path)
+    VL, VR, m, info = run_gpu(d)
+    assert (m, info) == (d["m"], d["info"])
+    ill = "quasi" in d["name"] or "tri" in d["name"] or "edge" in d["name"]
+    tol = (TOL_ILL if ill else TOL_WELL)[d["S"].dtype.type]
+    compare(d, VL, VR, m, d["VL_out"], d["VR_out"], tol)
+
+
+def _pencil(kind, n, seed, dt):
+    if kind == "gges":
+        out = pencils.gen_gges(n, seed, dtype=dt)
+        if np.issubdtype(dt, np.complexfloating):
+            S, P, a, b, Q, Z = out
+            return dict(S=S, P=P, alpha=a, beta=b, alphai=None, Q=Q, Z=Z)
+        S, P, ar, ai, be, Q, Z = out
+        return dict(S=S, P=P, alpha=ar, alphai=ai, beta=be, Q=Q, Z=Z)
+    if kind == "graded":
+        S, P, a, b, Q, Z = pencils.gen_gges(n, seed, dtype=dt, graded=True)
+        return dict(S=S, P=P, alpha=a, beta=b, alphai=None, Q=Q, Z=Z)
+    if kind == "schur":
+        S, P, ar, ai, be = pencils.gen_schur_like(n, seed, dtype=dt)
+        I = np.eye(n, dtype=dt, order="F")
+        return dict(S=S, P=P, alpha=ar, alphai=ai, beta=be, Q=I, Z=I.copy(order="F"))
+    raise ValueError(kind)
+
+
+CASES = [
+    # (kind, n, seed, dtype, side, howmny)
+    ("gges", 128, 21, np.float64, "B", "B"),
+    ("gges", 257, 22, np.float64, "B", "A"),
+    ("gges", 200, 23, np.float64, "R", "B"),
+    ("gges", 190, 24, np.float64, "L", "B"),
+    ("schur", 700, 25, np.float64, "B", "A"),
+    ("gges", 160, 26, np.float32, "B", "B"),
+    ("gges", 150, 27, np.complex128, "B", "B"),
+    ("gges", 131, 28, np.complex128, "R", "A"),
+    ("gges", 120, 29, np.complex64, "B", "B"),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c[0]}-{c[1]}-{np.dtype(c[3]).name}-{c[4]}{c[5]}")
+def test_against_oracle(cuda_ok, case):
+    kind, n, seed, dt, side, howmny = case
+    p = _pencil(kind, n, seed, dt)
+    d = dict(side=side, howmny=howmny, S=p["S"], P=p["P"], alpha=p["alpha"], beta=p["beta"], alphai=p["alphai"],
+             VL_in=p["Q"], VR_in=p["Z"], name=kind)
+    ref = oracle.tgevc3(side, howmny, d["S"], d["P"], d["alpha"], d["beta"], alphai=d["alphai"],
+                        VL=p["Q"].copy(order="F"), VR=p["Z"].copy(order="F"))
+    VL, VR, m, info = run_gpu(d)
+    assert (m, info) == (ref[2], ref[3])
+    tol = (TOL_ILL if kind == "schur" else TOL_WELL)[np.dtype(dt).type]
+    compare(d, VL, VR, m, ref[0], ref[1], tol)
+
+
+def test_graded_complex_scale_guards(cuda_ok):
+    """zgges pencil of A, D*B with log10 d_i ~ U(-8, 8): eigenvalues over many orders of
+    magnitude.  Columns where the oracle itself is non-finite (repeated infinite
+    eigenvalues make its triangular solves singular) are excluded from the comparison; the
+    CUDA path must stay finite everywhere and satisfy the residual bound."""
+    p = _pencil("graded", 160, 31, np.complex128)
+    I = np.eye(160, dtype=np.complex128, order="F")
+    d = dict(side="R", howmny="A", S=p["S"], P=p["P"], alpha=p["alpha"], beta=p["beta"], alphai=None,
+             VL_in=I, VR_in=I.copy(order="F"), name="graded")
+    ref = oracle.tgevc3("R", "A", d["S"], d["P"], d["alpha"], d["beta"])
+    VL, VR, m, info = run_gpu(d)
+    assert info == 0 and np.isfinite(VR).all()
+    err, cols = oracle.max_rel_diff(VR[:, :m], ref[1][:, :m])
+    assert err < 1e-9, err
+    r = oracle.residual_ratio(d["S"], d["P"], VR[:, :m], d["alpha"], d["beta"])
+    assert r.max() < 100
+
+
+def test_selection_and_one_sided(cuda_ok):
+    p = _pencil("gges", 150, 41, np.float64)
+    rng = np.random.default_rng(0)
+    sel = (rng.random(150) < 0.3).astype(np.int32)
+    for side in ("R", "L", "B"):
+        d = dict(side=side, howmny="S", S=p["S"], P=p["P"], alpha=p["alpha"], beta=p["beta"], alphai=p["alphai"],
+                 VL_in=np.zeros((150, 150), order="F"), VR_in=np.zeros((150, 150), order="F"), select=sel,
+                 name="sel")
+        ref = oracle.tgevc3(side, "S", d["S"], d["P"], d["alpha"], d["beta"], alphai=d["alphai"], select=sel)
+        VL, VR, m, info = run_gpu(d)
+        assert (m, info) == (ref[2], ref[3])
+        compare(d, VL, VR, m, ref[0], ref[1], TOL_WELL[np.float64])
+
+
+def test_normalize_flag(cuda_ok):
+    p = _pencil("gges", 140, 42, np.float64)
+    d = dict(side="B", howmny="B", S=p["S"], P=p["P"], alpha=p["alpha"], beta=p["beta"], alphai=p["alphai"],
+             VL_in=p["Q"], VR_in=p["Z"], name="norm")
+    VL0, VR0, m, _ = run_gpu(d)
+    X.set_flags(X.NORMALIZE)
+    try:
+        VL1, VR1, m1, _ = run_gpu(d)
+    finally:
+        X.set_flags(0)
+    for V0, V1 in ((VL0, VL1), (VR0, VR1)):
+        c1 = as_complex(V1, d)
+        mx = (np.abs(c1.real) + np.abs(c1.imag)).max(0)
+        np.testing.assert_allclose(mx, 1.0, rtol=1e-13)
+        err, _ = oracle.max_rel_diff(c1, as_complex(V0, d))
+        assert err < 1e-13
+
+
+def test_simt_and_tensor_core_paths_agree(cuda_ok):
+    p = _pencil("gges", 300, 43, np.float64)
+    d = dict(side="B", howmny="B", S=p["S"], P=p["P"], alpha=p["alpha"], beta=p["beta"], alphai=p["alphai"],
+             VL_in=p["Q"], VR_in=p["Z"], name="simt")
+    VL0, VR0, m, _ = run_gpu(d)
+    X.set_flags(X.SIMT)
+    try:
+        VL1, VR1, _, _ = run_gpu(d)
+    finally:
+        X.set_flags(0)
+    for A, B in ((VL0, VL1), (VR0, VR1)):
+        den = np.abs(B).max(0)
+        assert (np.abs(A - B).max(0) / den).max() < 1e-12
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 63, 64, 65, 129])
+def test_small_and_boundary_sizes(cuda_ok, n):
+    S, P, ar, ai, be = pencils.gen_quasi_triangular(n, 100 + n, pair_frac=0.5)
+    I = np.eye(n, order="F")
+    d = dict(side="B", howmny="A", S=S, P=P, alpha=ar, beta=be, alphai=ai, VL_in=I, VR_in=I.copy(order="F"),
+             name="quasi")
+    ref = oracle.tgevc3("B", "A", S, P, ar, be, alphai=ai)
+    VL, VR, m, info = run_gpu(d)
+    assert (m, info) == (ref[2], ref[3])
+    compare(d, VL, VR, m, ref[0], ref[1], TOL_ILL[np.float64], check_resid=False)
+
+
+def test_device_api_matches_host_api(cuda_ok):
+    import torch
+    p = _pencil("gges", 180, 44, np.float64)
+    n = 180
+    d = dict(side="B", howmny="B", S=p["S"], P=p["P"], alpha=p["alpha"], beta=p["beta"], alphai=p["alphai"],
+             VL_in=p["Q"], VR_in=p["Z"], name="dev")
+    VLh, VRh, m, info = run_gpu(d)
+
+    def dev(a):  # column-major device tensor
+        return torch.from_numpy(np.ascontiguousarray(a.T)).cuda().t()
+
+    S, P, VL, VR = dev(p["S"]), dev(p["P"]), dev(p["Q"]), dev(p["Z"])
+    m2, info2 = X.tgevc3_dev("B", "B", S, P, p["alpha"], p["beta"], alphai=p["alphai"], VL=VL, VR=VR)
+    torch.cuda.synchronize()
+    assert (m2, info2) == (m, info)
+    np.testing.assert_array_equal(VL.t().cpu().numpy().T, VLh[:, :m])
+    np.testing.assert_array_equal(VR.t().cpu().numpy().T, VRh[:, :m])
+    assert n == m

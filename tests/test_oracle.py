@@ -1,0 +1,82 @@
+"""The CPU oracle (oracle/tgevc3_oracle.c) against the upstream library's own outputs.
+
+The fixtures in tests/golden/ were produced by the upstream src/*.cpp (see
+tests/golden/make_golden.py).  The oracle follows the same algorithm (same 32-column
+panels, same whole-panel overflow guards), so its raw outputs must agree column by
+column up to rounding: BLAS summation order is the only difference.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden_files, load_golden
+
+# per-column max |oracle - upstream| / max |upstream|, raw (no normalisation)
+TOL = {np.float64: 1e-11, np.complex128: 1e-11, np.float32: 5e-5, np.complex64: 5e-5}
+
+
+@pytest.mark.parametrize("path", golden_files(), ids=lambda p: p.split("/")[-1][:-4])
+def test_oracle_matches_upstream(path):
+    d = load_golden(path)
+    VL, VR, m, info = oracle.tgevc3(d["side"], d["howmny"], d["S"], d["P"], d["alpha"], d["beta"],
+                                    alphai=d.get("alphai"), VL=d["VL_in"].copy(order="F"),
+                                    VR=d["VR_in"].copy(order="F"), select=d.get("select"), impl="oracle")
+    assert (m, info) == (d["m"], d["info"])
+    tol = TOL[d["S"].dtype.type]
+    for side, V, Vr in (("L", VL, d["VL_out"]), ("R", VR, d["VR_out"])):
+        if side not in d["side"] and d["side"] != "B":
+            continue
+        V, Vr = V[:, :m], Vr[:, :m]
+        assert np.isfinite(Vr).all()
+        den = np.abs(Vr).max(0)
+        den[den == 0] = 1
+        err = np.abs(V - Vr).max(0) / den
+        assert err.max() <= tol, (side, err.max())
+
+
+def _real_pencil_residuals(d, VL, VR, m):
+    ai = d["alphai"]
+    alpha = d["alpha"] + 1j * ai
+    out = []
+    for left, V in ((True, VL), (False, VR)):
+        Vc = oracle.to_complex_real_storage(V[:, :m], ai)
+        out.append(oracle.residual_ratio(d["S"], d["P"], Vc, alpha, d["beta"], left=left).max())
+    return out
+
+
+def test_oracle_residual_bound_gges():
+    """DGET52-style residual (tests/test_lapack_d.cpp:38-168) below the upstream warning level."""
+    from xtgevc3_b200 import pencils
+    S, P, ar, ai, be, Q, Z = pencils.gen_gges(96, 11)
+    VL, VR, m, info = oracle.tgevc3("B", "A", S, P, ar, be, alphai=ai)
+    assert info == 0 and m == 96
+    d = dict(S=S, P=P, alpha=ar, alphai=ai, beta=be)
+    rl, rr = _real_pencil_residuals(d, VL, VR, m)
+    assert rl < 100 and rr < 100
+
+
+def test_oracle_matches_lapack_tgevc():
+    """Second oracle: LAPACK xTGEVC on the same pencil, compared after normalisation."""
+    from xtgevc3_b200 import pencils
+    S, P, ar, ai, be, Q, Z = pencils.gen_gges(80, 12)
+    VL, VR, m, info = oracle.tgevc3("B", "A", S, P, ar, be, alphai=ai)
+    vl_lap, vr_lap = oracle.lapack_tgevc(S, P)
+    for V, W in ((VL, vl_lap), (VR, vr_lap)):
+        a = oracle.to_complex_real_storage(V, ai)
+        b = oracle.to_complex_real_storage(W, ai)
+        err, _ = oracle.max_rel_diff(a, b)
+        assert err < 1e-10
+
+
+def test_oracle_lwork_and_info():
+    from xtgevc3_b200 import pencils
+    S, P, ar, ai, be = pencils.gen_quasi_triangular(20, 0)
+    # bad HOWMNY
+    _, _, m, info = oracle.tgevc3("B", "X", S, P, ar, be, alphai=ai)
+    assert info == -2
+    # MM too small
+    _, _, m, info = oracle.tgevc3("B", "A", S, P, ar, be, alphai=ai, mm=5)
+    assert info == -16 and m == 20
+    # LWORK too small even for block size 1
+    _, _, m, info = oracle.tgevc3("B", "A", S, P, ar, be, alphai=ai, lwork=10)
+    assert info == -19

@@ -1,0 +1,182 @@
+"""xtgevc3_b200 -- generalized eigenvectors of a (quasi-)triangular pencil on NVIDIA B200.
+
+Python view of the C ABI in include/xtgevc3.h (libxtgevc3.so, built by
+``python -m xtgevc3_b200.build``).  Two call forms:
+
+``tgevc3(side, howmny, S, P, alpha, beta, alphai=..., VL=..., VR=..., select=...)``
+    The upstream argument list (include/tgevc3.h:9-12 of vlovero/xTGEVC3) on host
+    (numpy, Fortran-ordered) arrays; calls the drop-in entry point
+    ``xtgevc3_{d,s,z,c}tgevc3``.  Returns (VL, VR, m, info).
+
+``tgevc3_dev(side, howmny, S, P, alpha, beta, alphai=..., VL=..., VR=..., select=..., flags=0)``
+    Matrices are CUDA tensors in column-major layout (``stride(0) == 1``, e.g.
+    ``torch.empty(n, n, device='cuda').t()``); eigenvalue arrays / select stay on the host.
+    Calls ``xtgevc3_{d,s,z,c}tgevc3_dev`` on torch's current stream.  Returns (m, info).
+
+There is no CPU fallback: importing the package loads the CUDA library and raises if it
+cannot be loaded or built.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+import numpy as np
+
+from . import build as _build
+
+NORMALIZE = 1
+SIMT = 2
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_lib = None
+
+_P = ct.c_void_p
+_I = ct.c_int
+_C = ct.c_char
+_U = ct.c_uint
+
+
+def lib():
+    """The loaded libxtgevc3.so (built on first use if it is missing)."""
+    global _lib
+    if _lib is None:
+        path = _build.LIB
+        if not os.path.exists(path):
+            _build.build()
+        L = ct.CDLL(path)
+        for p in "ds":
+            f = getattr(L, f"xtgevc3_{p}tgevc3")
+            f.argtypes = [_C, _C, _P, _I, _P, _I, _P, _I, _P, _P, _P, _P, _I, _P, _I, _I, _P, _P, _I, _P]
+            f.restype = None
+            f = getattr(L, f"xtgevc3_{p}tgevc3_dev")
+            f.argtypes = [_U, _P, _C, _C, _P, _I, _P, _I, _P, _I, _P, _P, _P, _P, _I, _P, _I, _I, _P, _P]
+            f.restype = _I
+        for p in "zc":
+            f = getattr(L, f"xtgevc3_{p}tgevc3")
+            f.argtypes = [_C, _C, _P, _I, _P, _I, _P, _I, _P, _P, _P, _I, _P, _I, _I, _P, _P, _I, _P]
+            f.restype = None
+            f = getattr(L, f"xtgevc3_{p}tgevc3_dev")
+            f.argtypes = [_U, _P, _C, _C, _P, _I, _P, _I, _P, _I, _P, _P, _P, _I, _P, _I, _I, _P, _P]
+            f.restype = _I
+        L.xtgevc3_set_flags.argtypes = [_U]
+        L.xtgevc3_set_flags.restype = None
+        L.xtgevc3_get_flags.restype = _U
+        L.xtgevc3_last_error.restype = ct.c_char_p
+        _lib = L
+    return _lib
+
+
+def set_flags(flags: int) -> None:
+    """Flags used by the host-pointer (drop-in) entry points (NORMALIZE, SIMT)."""
+    lib().xtgevc3_set_flags(int(flags))
+
+
+def get_flags() -> int:
+    return int(lib().xtgevc3_get_flags())
+
+
+def last_error() -> str:
+    return lib().xtgevc3_last_error().decode()
+
+
+_PFX = {np.float64: "d", np.float32: "s", np.complex128: "z", np.complex64: "c"}
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+def lwork_query(prefix: str, n: int) -> int:
+    """The upstream LWORK=-1 answer for order n (2n(b+1) + 4(b+1)^2 + 2(b+1), b = 32)."""
+    b = 32
+    return 2 * n * (b + 1) + 4 * (b + 1) ** 2 + 2 * (b + 1)
+
+
+def tgevc3(side, howmny, S, P, alpha, beta, alphai=None, VL=None, VR=None, select=None, mm=None, lwork=None):
+    """Host-array form of s/d/c/ztgevc3 (see module docstring).  VL/VR are updated in place."""
+    L = lib()
+    dt = S.dtype.type
+    pfx = _PFX[dt]
+    n = S.shape[0]
+    S = np.asfortranarray(S)
+    P = np.asfortranarray(P)
+    sel = None if select is None else np.ascontiguousarray(select, dtype=np.int32)
+    mm = n if mm is None else mm
+    if VL is None:
+        VL = np.zeros((n, max(mm, 1)), dtype=dt, order="F")
+    if VR is None:
+        VR = np.zeros((n, max(mm, 1)), dtype=dt, order="F")
+    assert VL.flags.f_contiguous and VR.flags.f_contiguous
+    m = ct.c_int(0)
+    info = ct.c_int(0)
+    ld = max(n, 1)
+    rdt = np.float64 if pfx in "dz" else np.float32
+    head = [side.encode(), howmny.encode(), _ptr(sel), n, _ptr(S), ld, _ptr(P), ld]
+    if pfx in "ds":
+        al = np.ascontiguousarray(alpha, dtype=rdt)
+        ai = np.ascontiguousarray(alphai, dtype=rdt)
+        be = np.ascontiguousarray(beta, dtype=rdt)
+        eig = [_ptr(al), _ptr(ai), _ptr(be)]
+    else:
+        al = np.ascontiguousarray(alpha, dtype=dt)
+        be = np.ascontiguousarray(beta, dtype=dt)
+        eig = [_ptr(al), _ptr(be)]
+    tail = [_ptr(VL), ld, _ptr(VR), ld, mm, ct.byref(m)]
+    fn = getattr(L, f"xtgevc3_{pfx}tgevc3")
+    if lwork is None:
+        q = np.zeros(2, dtype=dt)
+        fn(*head, *eig, *tail, _ptr(q), -1, ct.byref(info))
+        if info.value != 0:
+            return VL, VR, m.value, info.value
+        lwork = int(np.real(q[0]))
+    work = np.zeros(max(min(lwork, 4), 1), dtype=dt)  # the GPU path never touches WORK beyond the query
+    fn(*head, *eig, *tail, _ptr(work), lwork, ct.byref(info))
+    if info.value > 0:
+        raise RuntimeError(f"xtgevc3_{pfx}tgevc3 failed: {last_error()}")
+    return VL, VR, m.value, info.value
+
+
+def _colmajor(t):
+    """(pointer, leading dimension) of a column-major 2-D CUDA tensor."""
+    if t is None:
+        return None, 1
+    if t.dim() != 2 or t.stride(0) != 1:
+        raise ValueError("matrices must be column-major (stride(0) == 1), e.g. torch.empty(n, n).t()")
+    return ct.c_void_p(t.data_ptr()), max(t.stride(1), t.shape[0], 1)
+
+
+def tgevc3_dev(side, howmny, S, P, alpha, beta, alphai=None, VL=None, VR=None, select=None, flags=0,
+               stream=None):
+    """Device form (see module docstring).  Raises on CUDA failure; returns (m, info)."""
+    import torch
+    L = lib()
+    tdt = S.dtype
+    pfx = {torch.float64: "d", torch.float32: "s", torch.complex128: "z", torch.complex64: "c"}[tdt]
+    n = S.shape[0]
+    sp, lds = _colmajor(S)
+    pp, ldp = _colmajor(P)
+    vlp, ldvl = _colmajor(VL)
+    vrp, ldvr = _colmajor(VR)
+    mm = max(VL.shape[1] if VL is not None else 0, VR.shape[1] if VR is not None else 0)
+    sel = None if select is None else np.ascontiguousarray(select, dtype=np.int32)
+    rdt = np.float64 if pfx in "dz" else np.float32
+    cdt = np.complex128 if pfx == "z" else np.complex64
+    if stream is None:
+        stream = torch.cuda.current_stream().cuda_stream
+    m = ct.c_int(0)
+    info = ct.c_int(0)
+    head = [int(flags), ct.c_void_p(stream), side.encode(), howmny.encode(), _ptr(sel), n, sp, lds, pp, ldp]
+    if pfx in "ds":
+        al = np.ascontiguousarray(alpha, dtype=rdt)
+        ai = np.ascontiguousarray(alphai, dtype=rdt)
+        be = np.ascontiguousarray(beta, dtype=rdt)
+        eig = [_ptr(al), _ptr(ai), _ptr(be)]
+    else:
+        al = np.ascontiguousarray(alpha, dtype=cdt)
+        be = np.ascontiguousarray(beta, dtype=cdt)
+        eig = [_ptr(al), _ptr(be)]
+    rc = getattr(L, f"xtgevc3_{pfx}tgevc3_dev")(*head, *eig, vlp, ldvl, vrp, ldvr, mm, ct.byref(m), ct.byref(info))
+    if rc != 0:
+        raise RuntimeError(f"xtgevc3_{pfx}tgevc3_dev failed: {last_error()}")
+    return m.value, info.value

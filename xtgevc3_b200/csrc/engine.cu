@@ -1,0 +1,424 @@
+// Device algorithm of the blocked generalized-eigenvector back-substitution (xTGEVC3).
+//
+// Right eigenvectors of the upper quasi-triangular pencil (S, P) are computed for all
+// selected eigenvalues at once with a right-looking blocked substitution over row blocks
+// of kBlock rows, bottom to top:
+//     for each row block I = [r0, r1):
+//         diag_solve:  X[I, c] = (ac_c S_II - b_c P_II)^-1 X[I, c]  for active columns c
+//         update:      X[0:r0, c] += S[0:r0, I] (-ac_c X[I, c]) + P[0:r0, I] (b_c X[I, c])
+// (the upstream driver does the same per 32-column panel, src/dtgevc3.cpp:1281-1470;
+// panels are independent, so all of them advance together here and every update is one
+// large GEMM instead of nb_sel <= 33 columns at a time).
+//
+// Left eigenvectors y (y^H (b S - a P) = 0) are the right eigenvectors of the reversed
+// (conjugate-)transposed pencil (F S^H F, F P^H F), F the reversal permutation, with the
+// columns and rows of the result reversed back; the same code therefore serves both sides
+// (upstream: src/dtgevc3.cpp:1476-1663).
+//
+// HOWMNY = 'B' multiplies by Z (Q) with a triangular-aware GEMM; otherwise the triangle is
+// written back with zeros elsewhere.
+#include "engine.cuh"
+#include "kernels_diag.cuh"
+#include "kernels_gemm.cuh"
+#include "kernels_misc.cuh"
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <type_traits>
+#include <vector>
+
+namespace xtg {
+
+static thread_local std::string g_err;
+const char *last_error() { return g_err.c_str(); }
+void set_last_error(const std::string &s) { g_err = s; }
+
+#define XTG_CK(call)                                                                              \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) {                                                                  \
+            set_last_error(std::string(#call) + ": " + cudaGetErrorString(e_));                   \
+            return 1;                                                                             \
+        }                                                                                         \
+    } while (0)
+
+static inline int round_up(int v, int q) { return (v + q - 1) / q * q; }
+
+// Stream-ordered scratch; the device's default pool keeps freed memory for reuse.
+struct Scratch {
+    cudaStream_t st;
+    std::vector<void *> ptrs;
+    cudaError_t err = cudaSuccess;
+    explicit Scratch(cudaStream_t s) : st(s) {}
+    template <class T>
+    T *get(size_t count)
+    {
+        void *p = nullptr;
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMallocAsync(&p, count * sizeof(T), st);
+        if (e != cudaSuccess) {
+            err = e;
+            return nullptr;
+        }
+        ptrs.push_back(p);
+        return static_cast<T *>(p);
+    }
+    ~Scratch()
+    {
+        for (void *p : ptrs) cudaFreeAsync(p, st);
+    }
+};
+
+static std::once_flag g_pool_once[64];
+static void configure_device(int dev)
+{
+    if (dev < 0 || dev >= 64) return;
+    std::call_once(g_pool_once[dev], [dev]() {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t thr = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+        cudaFuncSetAttribute(diag_solve_real<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             2 * kBlock * kSmLd * (int)sizeof(double));
+        cudaFuncSetAttribute(diag_solve_real<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             2 * kBlock * kSmLd * (int)sizeof(float));
+        cudaFuncSetAttribute(diag_solve_cplx<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             2 * kBlock * kSmLd * (int)sizeof(cplx<double>));
+        cudaFuncSetAttribute(diag_solve_cplx<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             2 * kBlock * kSmLd * (int)sizeof(cplx<float>));
+        cudaFuncSetAttribute(gemm_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::SMEM_BYTES);
+    });
+}
+
+// Selected eigenvalues in ascending order; a complex-conjugate pair (real arithmetic) is
+// one item of two columns.  Selection rule of src/dtgevc3.cpp:1193-1207 / 1295-1324.
+struct Item {
+    int k;
+    bool pair;
+    int out;  // first output column
+};
+
+// Per-column description of one side's computation (problem orientation).
+struct ColList {
+    int m = 0;
+    std::vector<int> colk, src, kext, outcol;
+    std::vector<uint8_t> kind;
+};
+
+template <class E>
+static void launch_gemm(const GemmArgs<E> &g, bool simt, cudaStream_t st)
+{
+    if (g.M <= 0 || g.N <= 0 || g.K <= 0) return;
+    if constexpr (std::is_same<E, double>::value) {
+        // the cp.async path copies 16-byte pairs of rows: even leading dimensions and
+        // 16-byte aligned bases only (caller-given ld may be odd on the device API)
+        auto al = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+        bool ok = (g.lda0 % 2 == 0) && (g.lda1 % 2 == 0) && (g.ldb % 2 == 0) && al(g.A0) && al(g.A1) && al(g.B);
+        if (!simt && ok) {
+            dim3 grid((g.M + dmma::BM - 1) / dmma::BM, (g.N + dmma::BN - 1) / dmma::BN);
+            gemm_dmma<<<grid, 256, dmma::SMEM_BYTES, st>>>(g);
+            return;
+        }
+    }
+    dim3 grid((g.M + 63) / 64, (g.N + 63) / 64);
+    gemm_simt<E><<<grid, 256, 0, st>>>(g);
+}
+
+template <class R, bool CPLX>
+int solve_device(char side, char howmny, const int *select, int n, const void *S_, int lds, const void *P_,
+                 int ldp, const void *alpha_, const void *alphai_, const void *beta_, void *VL_, int ldvl,
+                 void *VR_, int ldvr, int m_total, const Options &opt, cudaStream_t st)
+{
+    using E = typename std::conditional<CPLX, cplx<R>, R>::type;
+    const E *S = static_cast<const E *>(S_);
+    const E *P = static_cast<const E *>(P_);
+    E *VL = static_cast<E *>(VL_);
+    E *VR = static_cast<E *>(VR_);
+    const bool want_r = (side == 'R' || side == 'B') && VR;
+    const bool want_l = (side == 'L' || side == 'B') && VL;
+    const bool do_back = howmny == 'B';
+    const bool do_all = howmny == 'A' || howmny == 'B';
+    if (n <= 0 || m_total <= 0 || (!want_r && !want_l)) return 0;
+
+    int dev = 0;
+    XTG_CK(cudaGetDevice(&dev));
+    configure_device(dev);
+    XTG_CK(cudaGetLastError());
+
+    // ---- host-side structure: selection items, 2x2 blocks --------------------------------
+    const R *alphai = static_cast<const R *>(alphai_);
+    std::vector<Item> items;
+    std::vector<char> pairstart(n + 1, 0);
+    {
+        int out = 0;
+        for (int k = 0; k < n;) {
+            bool pair = !CPLX && alphai[k] != R(0) && k + 1 < n;
+            bool sel = do_all;
+            if (!do_all && select) {
+                sel = select[k] != 0;
+                if (pair) sel = sel || select[k + 1] != 0;
+            }
+            if (pair) pairstart[k] = 1;
+            if (sel) {
+                items.push_back({k, pair, out});
+                out += pair ? 2 : 1;
+            }
+            k += pair ? 2 : 1;
+        }
+        if (out != m_total) {
+            set_last_error("internal: selection count mismatch");
+            return 1;
+        }
+    }
+    std::vector<char> sub(n, 0);  // sub[k] = S[k+1, k] != 0
+    if constexpr (!CPLX) {
+        if (n > 1) {
+            std::vector<E> d(n - 1);
+            XTG_CK(cudaMemcpy2DAsync(d.data(), sizeof(E), S + 1, (size_t)(lds + 1) * sizeof(E), sizeof(E), n - 1,
+                                     cudaMemcpyDeviceToHost, st));
+            XTG_CK(cudaStreamSynchronize(st));
+            for (int k = 0; k + 1 < n; k++) sub[k] = d[k] != E(0);
+        }
+    }
+
+    Scratch scr(st);
+    // eigenvalue data on the device (for the coefficient kernels)
+    const int ncoef = CPLX ? 6 : 4;
+    R *d_eig = scr.get<R>(CPLX ? 4 * (size_t)n : 3 * (size_t)n);
+    R *d_sums = scr.get<R>(2 * (size_t)n);
+    R *d_norms = scr.get<R>(2);
+    if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
+    if (CPLX) {
+        XTG_CK(cudaMemcpyAsync(d_eig, alpha_, 2 * n * sizeof(R), cudaMemcpyHostToDevice, st));
+        XTG_CK(cudaMemcpyAsync(d_eig + 2 * n, beta_, 2 * n * sizeof(R), cudaMemcpyHostToDevice, st));
+    } else {
+        XTG_CK(cudaMemcpyAsync(d_eig, alpha_, n * sizeof(R), cudaMemcpyHostToDevice, st));
+        XTG_CK(cudaMemcpyAsync(d_eig + n, alphai_, n * sizeof(R), cudaMemcpyHostToDevice, st));
+        XTG_CK(cudaMemcpyAsync(d_eig + 2 * n, beta_, n * sizeof(R), cudaMemcpyHostToDevice, st));
+    }
+    // anorm / bnorm (src/dtgevc3.cpp:1254-1270; complex: rows <= col only)
+    colsum_kernel<E, R><<<(n + 7) / 8, 256, 0, st>>>(S, lds, P, ldp, n, CPLX ? 0 : 1, d_sums);
+    colmax_kernel<R><<<1, 1024, 0, st>>>(d_sums, n, d_norms);
+    XTG_CK(cudaGetLastError());
+
+    const R safemin = limits<R>::safemin, eps = limits<R>::eps;
+    const R bignum = R(1) / (safemin / eps);
+    const int ld_n = round_up(n, 32);
+
+    auto run_side = [&](bool left) -> int {
+        // ---- column list in problem orientation ---------------------------------------
+        ColList L;
+        L.m = m_total;
+        L.colk.resize(m_total);
+        L.src.resize(m_total);
+        L.kext.resize(m_total);
+        L.outcol.resize(m_total);
+        L.kind.resize(m_total);
+        {
+            int c = 0;
+            auto emit = [&](const Item &it) {
+                int kk = left ? (it.pair ? n - 2 - it.k : n - 1 - it.k) : it.k;
+                int w = it.pair ? 2 : 1;
+                for (int q = 0; q < w; q++) {
+                    L.colk[c] = kk;
+                    L.src[c] = it.k;
+                    L.kext[c] = kk + w;
+                    L.outcol[c] = it.out + q;
+                    L.kind[c] = it.pair ? (q == 0 ? kPairRe : kPairIm) : kReal;
+                    c++;
+                }
+            };
+            if (!left) for (const Item &it : items) emit(it);
+            else for (auto it = items.rbegin(); it != items.rend(); ++it) emit(*it);
+        }
+        // row blocks (problem orientation), bottom to top; a 2x2 block is never split
+        auto split = [&](int j) -> bool {  // rows j-1, j form a 2x2 diagonal block
+            if (CPLX || j <= 0 || j >= n) return false;
+            int kq = left ? n - 1 - j : j - 1;  // original index of the block's first row
+            return sub[kq] || pairstart[kq];
+        };
+        std::vector<std::pair<int, int>> blocks;
+        for (int cur = n; cur > 0;) {
+            int j = std::max(0, cur - kBlock);
+            if (j > 0 && split(j)) j += 1;
+            blocks.push_back({j, cur});
+            cur = j;
+        }
+
+        // ---- device buffers -------------------------------------------------------------
+        const int m = m_total;
+        const E *Sp = S, *Pp = P;
+        int lsp = lds, lpp = ldp;
+        if (left) {
+            E *St = scr.get<E>((size_t)ld_n * n);
+            E *Pt = scr.get<E>((size_t)ld_n * n);
+            if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
+            dim3 g((n + 31) / 32, (n + 31) / 32), b(32, 8);
+            rev_transpose_kernel<E><<<g, b, 0, st>>>(S, lds, St, ld_n, n, 1);
+            rev_transpose_kernel<E><<<g, b, 0, st>>>(P, ldp, Pt, ld_n, n, 1);
+            Sp = St;
+            Pp = Pt;
+            lsp = lpp = ld_n;
+        }
+        const int ldx = ld_n, ldy = 2 * kBlock;
+        E *X = scr.get<E>((size_t)ldx * m);
+        E *Y = scr.get<E>((size_t)ldy * m);
+        R *coef = scr.get<R>((size_t)ncoef * m);
+        int *d_ints = scr.get<int>(4 * (size_t)m);
+        uint8_t *d_kind = scr.get<uint8_t>((size_t)m);
+        if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
+        std::vector<int> ints(4 * (size_t)m);
+        std::copy(L.colk.begin(), L.colk.end(), ints.begin());
+        std::copy(L.src.begin(), L.src.end(), ints.begin() + m);
+        std::copy(L.kext.begin(), L.kext.end(), ints.begin() + 2 * m);
+        std::copy(L.outcol.begin(), L.outcol.end(), ints.begin() + 3 * m);
+        XTG_CK(cudaMemcpyAsync(d_ints, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        XTG_CK(cudaMemcpyAsync(d_kind, L.kind.data(), m, cudaMemcpyHostToDevice, st));
+        const int *d_colk = d_ints, *d_src = d_ints + m, *d_kext = d_ints + 2 * m, *d_outcol = d_ints + 3 * m;
+        XTG_CK(cudaMemsetAsync(X, 0, (size_t)ldx * m * sizeof(E), st));
+
+        if constexpr (CPLX) {
+            coef_cplx_kernel<R><<<(m + 127) / 128, 128, 0, st>>>(reinterpret_cast<const cplx<R> *>(d_eig),
+                                                                 reinterpret_cast<const cplx<R> *>(d_eig + 2 * n),
+                                                                 d_src, m, left ? 1 : 0, d_norms, coef);
+        } else {
+            coef_real_kernel<R><<<(m + 127) / 128, 128, 0, st>>>(d_eig, d_eig + n, d_eig + 2 * n, d_src, d_kind, m,
+                                                                 left ? 1 : 0, d_norms, coef);
+        }
+        XTG_CK(cudaGetLastError());
+
+        // ---- blocked substitution ----------------------------------------------------------
+        const size_t diag_smem = 2 * kBlock * kSmLd * sizeof(E);
+        for (const auto &bk : blocks) {
+            const int r0 = bk.first, r1 = bk.second, jnb = r1 - r0;
+            const int c0 = int(std::lower_bound(L.colk.begin(), L.colk.end(), r0) - L.colk.begin());
+            if (c0 >= m) continue;
+            const int bpad = round_up(jnb, kKPad);
+            DiagArgs<R> da;
+            da.S = reinterpret_cast<const R *>(Sp);
+            da.P = reinterpret_cast<const R *>(Pp);
+            da.lds = lsp;
+            da.ldp = lpp;
+            da.n = n;
+            da.r0 = r0;
+            da.r1 = r1;
+            da.bpad = bpad;
+            da.c0 = c0;
+            da.m = m;
+            da.colk = d_colk;
+            da.kind = d_kind;
+            da.coef = coef;
+            da.X = reinterpret_cast<R *>(X);
+            da.ldx = ldx;
+            da.Y = reinterpret_cast<R *>(Y);
+            da.ldy = ldy;
+            da.thr_rhs = bignum / R(10);
+            da.thr_upd = bignum / R(std::max(1, jnb));
+            da.left_seed = left ? 1 : 0;
+            const int ncols = m - c0;
+            const int grid = std::max(1, std::min((ncols + 7) / 8, 2 * 148));
+            if constexpr (CPLX) diag_solve_cplx<R><<<grid, 256, diag_smem, st>>>(da);
+            else diag_solve_real<R><<<grid, 256, diag_smem, st>>>(da);
+            if (r0 > 0) {
+                GemmArgs<E> g;
+                g.M = r0;
+                g.N = ncols;
+                g.K = 2 * bpad;
+                g.A0 = Sp + (size_t)r0 * lsp;
+                g.A1 = Pp + (size_t)r0 * lpp;
+                g.lda0 = lsp;
+                g.lda1 = lpp;
+                g.ksplit = bpad;
+                g.acols0 = n - r0;
+                g.acols1 = n - r0;
+                g.B = Y + (size_t)c0 * ldy;
+                g.ldb = ldy;
+                g.brows = 2 * bpad;
+                g.C = X + (size_t)c0 * ldx;
+                g.ldc = ldx;
+                g.ccol = nullptr;
+                g.kext = nullptr;
+                g.accumulate = 1;
+                launch_gemm<E>(g, opt.simt != 0, st);
+            }
+            XTG_CK(cudaGetLastError());
+        }
+
+        // ---- write-back / back-transform -----------------------------------------------------
+        E *V = left ? VL : VR;
+        const int ldv = left ? ldvl : ldvr;
+        if (do_back) {
+            // copy of Z (right) or column-reversed Q (left), so V can be overwritten
+            E *Zc = scr.get<E>((size_t)ld_n * n);
+            if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
+            if (left) {
+                dim3 g((n + 255) / 256, n);
+                rev_columns_kernel<E><<<g, 256, 0, st>>>(V, ldv, Zc, ld_n, n, n);
+            } else {
+                XTG_CK(cudaMemcpy2DAsync(Zc, (size_t)ld_n * sizeof(E), V, (size_t)ldv * sizeof(E), n * sizeof(E), n,
+                                         cudaMemcpyDeviceToDevice, st));
+            }
+            GemmArgs<E> g;
+            g.M = n;
+            g.N = m;
+            g.K = n;
+            g.A0 = Zc;
+            g.A1 = Zc;
+            g.lda0 = g.lda1 = ld_n;
+            g.ksplit = n;
+            g.acols0 = n;
+            g.acols1 = 0;
+            g.B = X;
+            g.ldb = ldx;
+            g.brows = n;
+            g.C = V;
+            g.ldc = ldv;
+            g.ccol = d_outcol;
+            g.kext = d_kext;
+            g.accumulate = 0;
+            launch_gemm<E>(g, opt.simt != 0, st);
+        } else {
+            dim3 g(std::max(1, std::min((n + 255) / 256, 64)), m);
+            writeback_kernel<E><<<g, 256, 0, st>>>(X, ldx, V, ldv, n, m, d_outcol, d_kext, left ? 1 : 0);
+        }
+        XTG_CK(cudaGetLastError());
+
+        if (opt.normalize) {
+            if constexpr (CPLX) {
+                normalize_cplx_kernel<R><<<m, 256, 0, st>>>(reinterpret_cast<cplx<R> *>(V), ldv, n, m);
+            } else {
+                std::vector<uint8_t> ok(m, kReal);
+                for (int c = 0; c < m; c++) ok[L.outcol[c]] = L.kind[c];
+                uint8_t *d_ok = scr.get<uint8_t>(m);
+                if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
+                XTG_CK(cudaMemcpyAsync(d_ok, ok.data(), m, cudaMemcpyHostToDevice, st));
+                normalize_real_kernel<R><<<m, 256, 0, st>>>(V, ldv, n, d_ok, m);
+            }
+            XTG_CK(cudaGetLastError());
+        }
+        return 0;
+    };
+
+    if (want_r && run_side(false)) return 1;
+    if (want_l && run_side(true)) return 1;
+    XTG_CK(cudaStreamSynchronize(st));
+    return 0;
+}
+
+template int solve_device<double, false>(char, char, const int *, int, const void *, int, const void *, int,
+                                         const void *, const void *, const void *, void *, int, void *, int, int,
+                                         const Options &, cudaStream_t);
+template int solve_device<float, false>(char, char, const int *, int, const void *, int, const void *, int,
+                                        const void *, const void *, const void *, void *, int, void *, int, int,
+                                        const Options &, cudaStream_t);
+template int solve_device<double, true>(char, char, const int *, int, const void *, int, const void *, int,
+                                        const void *, const void *, const void *, void *, int, void *, int, int,
+                                        const Options &, cudaStream_t);
+template int solve_device<float, true>(char, char, const int *, int, const void *, int, const void *, int,
+                                       const void *, const void *, const void *, void *, int, void *, int, int,
+                                       const Options &, cudaStream_t);
+
+}  // namespace xtg

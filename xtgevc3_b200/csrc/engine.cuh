@@ -1,0 +1,30 @@
+// Host-side driver of the device algorithm (declarations shared by engine.cu and api.cpp).
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+
+namespace xtg {
+
+// Options of one call (see XTGEVC3_* flags in include/xtgevc3.h).
+struct Options {
+    int normalize = 0;  // scale every eigenvector to max |re| + |im| = 1 (LAPACK convention)
+    int simt = 0;       // force the SIMT GEMM kernels instead of the tensor-core kernel
+};
+
+// One call on device-resident matrices.
+//   S, P, VL, VR : device pointers, leading dimensions in elements of the scalar type
+//                  (a complex number counts as one element).  VR (VL) holds Z (Q) on entry
+//                  when howmny == 'B'.
+//   alpha, alphai, beta, select : HOST pointers of length n.  Real: alpha = alphar (R*),
+//                  alphai (R*), beta (R*).  Complex: alpha, beta interleaved, alphai unused.
+//   m_total      : number of eigenvector columns (as counted by the argument check).
+// Returns 0, or 1 when a CUDA call failed (message in last_error()).
+template <class R, bool CPLX>
+int solve_device(char side, char howmny, const int *select, int n, const void *S, int lds, const void *P,
+                 int ldp, const void *alpha, const void *alphai, const void *beta, void *VL, int ldvl, void *VR,
+                 int ldvr, int m_total, const Options &opt, cudaStream_t st);
+
+const char *last_error();
+void set_last_error(const std::string &s);
+
+}  // namespace xtg

@@ -1,0 +1,250 @@
+// GEMM kernels of the substitution: the trailing update of the accumulated right-hand
+// sides and the back-transform by Z (or Q).
+//
+//   C[0:M, j] (+)= sum_kk A(m, kk) * B(kk, j)
+//
+// A is column-major and may be stacked from two sources along K (A0 for kk < ksplit,
+// A1 after), which lets one launch apply both halves of the update
+//   X[0:r0, c] += S[0:r0, I] * (-ac x) + P[0:r0, I] * (b x)
+// (upstream: the two dgemm_ calls at src/dtgevc3.cpp:1432-1433).  For the back-transform
+// (src/dtgevc3.cpp:1446, 1638) A is Z (or Q with reversed columns), B is the upper
+// triangular X, and `kext` gives per column the number of leading rows of B that can be
+// nonzero so that a column tile only runs K up to its last nonzero row.  The optional
+// column map scatters result columns into their output positions.
+#pragma once
+#include "common.cuh"
+
+namespace xtg {
+
+template <class E>
+struct GemmArgs {
+    int M, N, K;
+    const E *A0, *A1;
+    int lda0, lda1, ksplit;
+    int acols0, acols1;  // columns of A0 / A1 that exist in memory (beyond: read as zero)
+    const E *B;
+    int ldb, brows;      // rows of B that exist in memory
+    E *C;
+    int ldc;
+    const int *ccol;     // output column of result column j (nullptr: j)
+    const int *kext;     // nonzero leading rows of B per column (nullptr: K)
+    int accumulate;
+};
+
+template <class R> __device__ __forceinline__ R zero_of() { return R(0); }
+
+template <class E>
+__device__ __forceinline__ E load_a(const GemmArgs<E> &g, int m, int kk)
+{
+    if (m >= g.M) return E(0);
+    if (kk < g.ksplit) {
+        if (kk >= g.acols0) return E(0);
+        return g.A0[(size_t)m + (size_t)kk * g.lda0];
+    }
+    int k2 = kk - g.ksplit;
+    if (k2 >= g.acols1) return E(0);
+    return g.A1[(size_t)m + (size_t)k2 * g.lda1];
+}
+
+template <class E>
+__device__ __forceinline__ int tile_kmax(const GemmArgs<E> &g, int n0, int BN)
+{
+    int kmax = g.K;
+    if (g.kext) {
+        int last = min(n0 + BN, g.N) - 1;
+        kmax = min(kmax, g.kext[last]);
+    }
+    return kmax;
+}
+
+// ------------------------------------------------------------------------------------
+// SIMT kernel (any element type): 64 x 64 tile, 256 threads, 4 x 4 outputs per thread.
+// ------------------------------------------------------------------------------------
+template <class E>
+__global__ void __launch_bounds__(256) gemm_simt(GemmArgs<E> g)
+{
+    constexpr int BM = 64, BN = 64, BK = 16;
+    __shared__ E As[BK][BM + 1];
+    __shared__ E Bs[BK][BN + 1];
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int kmax = tile_kmax(g, n0, BN);
+    E acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = E(0);
+
+    for (int k0 = 0; k0 < kmax; k0 += BK) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            int e = tid + 256 * q;
+            int m = e % BM, kk = e / BM;
+            As[kk][m] = (k0 + kk < kmax) ? load_a(g, m0 + m, k0 + kk) : E(0);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            int e = tid + 256 * q;
+            int kk = e % BK, n = e / BK;
+            int kr = k0 + kk, col = n0 + n;
+            Bs[kk][n] = (kr < kmax && kr < g.brows && col < g.N) ? g.B[(size_t)kr + (size_t)col * g.ldb] : E(0);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BK; kk++) {
+            E a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) a[i] = As[kk][tx + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; j++) b[j] = Bs[kk][ty + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] = acc[i][j] + a[i] * b[j];
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        int col = n0 + ty + 16 * j;
+        if (col >= g.N) continue;
+        int oc = g.ccol ? g.ccol[col] : col;
+        E *cp = g.C + (size_t)oc * g.ldc;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            int row = m0 + tx + 16 * i;
+            if (row < g.M) cp[row] = g.accumulate ? cp[row] + acc[i][j] : acc[i][j];
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// FP64 tensor-core kernel (DMMA, mma.sync m8n8k4 f64).
+// CTA tile 128 x 64, K step 16, 8 warps as 4 (M) x 2 (N) with 32 x 32 warp tiles,
+// 3-stage cp.async pipeline into padded shared memory (conflict-free fragment loads).
+// ------------------------------------------------------------------------------------
+namespace dmma {
+constexpr int BM = 128, BN = 64, BK = 16, STAGES = 3;
+constexpr int ALD = BM + 8;   // A tile stored [k][m]
+constexpr int BLD = BK + 4;   // B tile stored [n][k]
+constexpr int A_STAGE = BK * ALD;
+constexpr int B_STAGE = BN * BLD;
+constexpr int SMEM_BYTES = STAGES * (A_STAGE + B_STAGE) * 8;
+}  // namespace dmma
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes)
+{
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void dmma884(double &d0, double &d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(256) gemm_dmma(GemmArgs<double> g)
+{
+    using namespace dmma;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    double *As = reinterpret_cast<double *>(smem_raw);
+    double *Bs = As + STAGES * A_STAGE;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp & 3, wn = warp >> 2;
+    const int gq = lane >> 2, tq = lane & 3;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int kmax = tile_kmax(g, n0, BN);
+    const int ktiles = (kmax + BK - 1) / BK;
+
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            acc[i][j][0] = 0.0;
+            acc[i][j][1] = 0.0;
+        }
+
+    auto load_stage = [&](int kt, int st) {
+        const int k0 = kt * BK;
+        double *as = As + st * A_STAGE;
+        double *bs = Bs + st * B_STAGE;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {  // A: 16 columns x 64 chunks
+            int e = tid + 256 * q;
+            int kk = e >> 6, ch = e & 63;
+            int row = m0 + 2 * ch, kg = k0 + kk;
+            const double *src = g.A0;
+            int col = kg, ok = kg < kmax, lda = g.lda0;
+            if (kg >= g.ksplit) { src = g.A1; col = kg - g.ksplit; ok = ok && col < g.acols1; lda = g.lda1; }
+            else ok = ok && col < g.acols0;
+            int bytes = 0;
+            if (ok) bytes = row + 1 < g.M ? 16 : (row < g.M ? 8 : 0);
+            const double *gp = bytes ? src + (size_t)row + (size_t)col * lda : g.A0;
+            cp_async16(as + kk * ALD + 2 * ch, gp, bytes);
+        }
+#pragma unroll
+        for (int q = 0; q < 2; q++) {  // B: 64 columns x 8 chunks
+            int e = tid + 256 * q;
+            int nn = e >> 3, ch = e & 7;
+            int kr = k0 + 2 * ch, col = n0 + nn;
+            int lim = min(kmax, g.brows);
+            int bytes = 0;
+            if (col < g.N) bytes = kr + 1 < lim ? 16 : (kr < lim ? 8 : 0);
+            const double *gp = bytes ? g.B + (size_t)kr + (size_t)col * g.ldb : g.B;
+            cp_async16(bs + nn * BLD + 2 * ch, gp, bytes);
+        }
+    };
+
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; s++) {
+        if (s < ktiles) load_stage(s, s);
+        cp_async_commit();
+    }
+    for (int kt = 0; kt < ktiles; kt++) {
+        cp_async_wait<STAGES - 2>();
+        __syncthreads();
+        int nk = kt + STAGES - 1;
+        if (nk < ktiles) load_stage(nk, nk % STAGES);
+        cp_async_commit();
+        const double *as = As + (kt % STAGES) * A_STAGE;
+        const double *bs = Bs + (kt % STAGES) * B_STAGE;
+#pragma unroll
+        for (int kk = 0; kk < BK; kk += 4) {
+            double a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) a[i] = as[(kk + tq) * ALD + wm * 32 + i * 8 + gq];
+#pragma unroll
+            for (int j = 0; j < 4; j++) b[j] = bs[(wn * 32 + j * 8 + gq) * BLD + kk + tq];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) dmma884(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+        }
+    }
+    cp_async_wait<0>();
+
+    // epilogue: fragment (row gq, cols 2tq, 2tq+1) of each 8x8 tile
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            int col = n0 + wn * 32 + j * 8 + 2 * tq + h;
+            if (col >= g.N) continue;
+            int oc = g.ccol ? g.ccol[col] : col;
+            double *cp = g.C + (size_t)oc * g.ldc;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                int row = m0 + wm * 32 + i * 8 + gq;
+                if (row < g.M) cp[row] = g.accumulate ? cp[row] + acc[i][j][h] : acc[i][j][h];
+            }
+        }
+    }
+}
+
+}  // namespace xtg

@@ -1,0 +1,247 @@
+// Auxiliary kernels of the xTGEVC3 path: pencil norms and shift coefficients, the
+// reversal/transposition that turns the left problem into a right problem, the
+// write-back of untransformed eigenvectors, and the final column normalisation.
+#pragma once
+#include "common.cuh"
+
+namespace xtg {
+
+template <class R> __device__ __forceinline__ R absval(R v) { return fabs(v); }
+template <class R> __device__ __forceinline__ R absval(cplx<R> v) { return hypot(v.x, v.y); }
+
+// Column sums of |S| and |P| over rows <= min(col + extra, n - 1): the 1-norms behind
+// ascale/bscale (src/dtgevc3.cpp:1254-1270 with extra = 1; src/ztgevc3.cpp:528-542
+// with extra = 0).  One warp per column.
+template <class E, class R>
+__global__ void colsum_kernel(const E *S, int lds, const E *P, int ldp, int n, int extra, R *sums)
+{
+    int col = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (col >= n) return;
+    int last = min(col + extra, n - 1);
+    R ss = 0, sp = 0;
+    for (int r = lane; r <= last; r += 32) {
+        ss += absval(S[(size_t)r + (size_t)col * lds]);
+        sp += absval(P[(size_t)r + (size_t)col * ldp]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ss += __shfl_xor_sync(0xffffffffu, ss, o);
+        sp += __shfl_xor_sync(0xffffffffu, sp, o);
+    }
+    if (lane == 0) {
+        sums[col] = ss;
+        sums[n + col] = sp;
+    }
+}
+
+// norms[0] = anorm, norms[1] = bnorm (single block).
+template <class R>
+__global__ void colmax_kernel(const R *sums, int n, R *norms)
+{
+    __shared__ R sa[32], sb[32];
+    R a = 0, b = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        a = fmax(a, sums[i]);
+        b = fmax(b, sums[n + i]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+        b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sa[threadIdx.x >> 5] = a;
+        sb[threadIdx.x >> 5] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) {
+            a = fmax(a, sa[w]);
+            b = fmax(b, sb[w]);
+        }
+        norms[0] = a;
+        norms[1] = b;
+    }
+}
+
+// Shift coefficients of every computed column (src/dtgevc3.cpp:716-725, 1372-1381):
+//   t = 1 / max(|ar| ascale + |ai| ascale, |b| bscale, safemin)
+//   ac = (t b bscale) ascale,  b_re = (t ar ascale) bscale,  b_im = (t ai ascale) bscale,
+// with (ac, b) = (0, 1) for an infinite eigenvalue.  `neg_im` flips ai (the left problem
+// solves for the conjugate eigenvalue).  smin is the pivot floor of the shifted solves:
+// max(eps * (|ac| anorm + |b| bnorm), safemin).
+template <class R>
+__global__ void coef_real_kernel(const R *alphar, const R *alphai, const R *beta, const int *src,
+                                 const uint8_t *kind, int m, int neg_im, const R *norms, R *coef)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m) return;
+    const R safemin = limits<R>::safemin, eps = limits<R>::eps;
+    R anorm = norms[0], bnorm = norms[1];
+    R ascale = R(1) / fmax(anorm, safemin), bscale = R(1) / fmax(bnorm, safemin);
+    int k = src[c];
+    R ar = alphar[k], ai = kind[c] == kReal ? R(0) : alphai[k], b = beta[k];
+    if (neg_im) ai = -ai;
+    R den = fmax(fmax(fabs(ar) * ascale + fabs(ai) * ascale, fabs(b) * bscale), safemin);
+    R t = R(1) / den;
+    R ac = (t * b * bscale) * ascale;
+    R br = (t * ar * ascale) * bscale;
+    R bi = (t * ai * ascale) * bscale;
+    if (fabs(b) <= safemin && (fabs(ar) + fabs(ai)) > safemin) {
+        ac = R(0);
+        br = R(1);
+        bi = R(0);
+    }
+    coef[4 * c + 0] = ac;
+    coef[4 * c + 1] = br;
+    coef[4 * c + 2] = bi;
+    coef[4 * c + 3] = fmax(eps * (fabs(ac) * anorm + (fabs(br) + fabs(bi)) * bnorm), safemin);
+}
+
+// Complex form (src/ztgevc3.cpp:148-156): t = 1 / max(|a| ascale, |b| bscale, safemin),
+// ac = (t ascale) b bscale, bc = (t bscale) a ascale; `conj_ab` conjugates a and b (left).
+template <class R>
+__global__ void coef_cplx_kernel(const cplx<R> *alpha, const cplx<R> *beta, const int *src, int m,
+                                 int conj_ab, const R *norms, R *coef)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m) return;
+    const R safemin = limits<R>::safemin, eps = limits<R>::eps;
+    R anorm = norms[0], bnorm = norms[1];
+    R ascale = R(1) / fmax(anorm, safemin), bscale = R(1) / fmax(bnorm, safemin);
+    int k = src[c];
+    cplx<R> a = alpha[k], b = beta[k];
+    if (conj_ab) {
+        a = conjg(a);
+        b = conjg(b);
+    }
+    R na = hypot(a.x, a.y), nb = hypot(b.x, b.y);
+    R t = R(1) / fmax(fmax(na * ascale, nb * bscale), safemin);
+    cplx<R> ac = (cplx<R>(t * ascale, R(0)) * b) * cplx<R>(bscale, R(0));
+    cplx<R> bc = (cplx<R>(t * bscale, R(0)) * a) * cplx<R>(ascale, R(0));
+    if (nb <= safemin && na > safemin) {
+        ac = cplx<R>(0, 0);
+        bc = cplx<R>(1, 0);
+    }
+    coef[6 * c + 0] = ac.x;
+    coef[6 * c + 1] = ac.y;
+    coef[6 * c + 2] = bc.x;
+    coef[6 * c + 3] = bc.y;
+    coef[6 * c + 4] = fmax(eps * (l1abs(ac) * anorm + l1abs(bc) * bnorm), safemin);
+    coef[6 * c + 5] = R(0);
+}
+
+template <class E> __device__ __forceinline__ E maybe_conj(E v, int) { return v; }
+template <class R> __device__ __forceinline__ cplx<R> maybe_conj(cplx<R> v, int c) { return c ? conjg(v) : v; }
+
+// out(i, j) = f(in(n-1-j, n-1-i)), f = conj when `cj`: the left problem
+// y^H (b S - a P) = 0 becomes the right problem of (F S^H F, F P^H F), F the reversal.
+// 32 x 32 tiles through shared memory.
+template <class E>
+__global__ void rev_transpose_kernel(const E *in, int ldi, E *out, int ldo, int n, int cj)
+{
+    __shared__ E tile[32][33];
+    int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+    // read in(n-1-j, n-1-i) for j in [j0, j0+32) (rows of in), i in [i0, i0+32) (cols of in)
+    int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+    for (int q = ty; q < 32; q += 8) {
+        int j = j0 + tx, i = i0 + q;
+        if (i < n && j < n) tile[q][tx] = in[(size_t)(n - 1 - j) + (size_t)(n - 1 - i) * ldi];
+    }
+    __syncthreads();
+    for (int q = ty; q < 32; q += 8) {
+        int i = i0 + tx, j = j0 + q;
+        if (i < n && j < n) out[(size_t)i + (size_t)j * ldo] = maybe_conj(tile[tx][q], cj);
+    }
+}
+
+// out[:, j] = in[:, n-1-j] for j < n (rows 0..rows-1).
+template <class E>
+__global__ void rev_columns_kernel(const E *in, int ldi, E *out, int ldo, int rows, int n)
+{
+    int j = blockIdx.y;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
+        out[(size_t)r + (size_t)j * ldo] = in[(size_t)r + (size_t)(n - 1 - j) * ldi];
+}
+
+// V[r, ccol[c]] = X[r, c] for r < kext[c], 0 otherwise (upstream write-back,
+// src/dtgevc3.cpp:1455-1465).  With `rev` the row order is reversed (left problem):
+// V[r, ccol[c]] = X[n-1-r, c].
+template <class E>
+__global__ void writeback_kernel(const E *X, int ldx, E *V, int ldv, int n, int m, const int *ccol,
+                                 const int *kext, int rev)
+{
+    int c = blockIdx.y;
+    if (c >= m) return;
+    int ke = kext[c];
+    E *out = V + (size_t)ccol[c] * ldv;
+    const E *in = X + (size_t)c * ldx;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        int src = rev ? n - 1 - r : r;
+        out[r] = src < ke ? in[src] : E(0);
+    }
+}
+
+// Final normalisation (not done by the upstream code; LAPACK xTGEVC convention): every
+// eigenvector is scaled so that max_i (|re_i| + |im_i|) = 1, a real pair (Re, Im) jointly.
+// One CTA per eigenvector; the column (pair) is read twice, the second time from L2.
+template <class R>
+__global__ void normalize_real_kernel(R *V, int ldv, int n, const uint8_t *outkind, int m)
+{
+    int c = blockIdx.x;
+    if (c >= m) return;
+    uint8_t kd = outkind[c];
+    if (kd == kPairIm) return;
+    R *v0 = V + (size_t)c * ldv;
+    R *v1 = kd == kPairRe ? v0 + ldv : nullptr;
+    R mx = 0;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) mx = fmax(mx, fabs(v0[r]) + (v1 ? fabs(v1[r]) : R(0)));
+    __shared__ R red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        R v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : R(0);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (threadIdx.x == 0) red[0] = v;
+    }
+    __syncthreads();
+    mx = red[0];
+    if (!(mx > R(0))) return;
+    R s = R(1) / mx;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        v0[r] *= s;
+        if (v1) v1[r] *= s;
+    }
+}
+
+template <class R>
+__global__ void normalize_cplx_kernel(cplx<R> *V, int ldv, int n, int m)
+{
+    int c = blockIdx.x;
+    if (c >= m) return;
+    cplx<R> *v = V + (size_t)c * ldv;
+    R mx = 0;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) mx = fmax(mx, l1abs(v[r]));
+    __shared__ R red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        R w = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : R(0);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) w = fmax(w, __shfl_xor_sync(0xffffffffu, w, o));
+        if (threadIdx.x == 0) red[0] = w;
+    }
+    __syncthreads();
+    mx = red[0];
+    if (!(mx > R(0))) return;
+    R s = R(1) / mx;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) v[r] = s * v[r];
+}
+
+}  // namespace xtg
