@@ -1,0 +1,453 @@
+#!/usr/bin/env python
+"""Benchmark: dtgevc3 SIDE='B' HOWMNY='B' (left and right eigenvectors, back-transformed
+by Q and Z) on an n = 8192 real pencil in generalized Schur form, on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 8192]
+
+One "step" = one full dtgevc3 call (all 2n eigenvectors) on one pencil.  With N > 1
+(torchrun, one process per GPU) every rank solves its own pencil: the units (pencils)
+are independent, there is no data-path collective, scaling is weak.
+
+Prints one JSON line (rank 0).  value = eigenvectors/s of the whole job with inputs
+resident in HBM; e2e = the same through the host-pointer C ABI (xtgevc3_dtgevc3) from
+pinned host buffers, copies included.  roofline = the dominant kernel class from the
+library's CUDA-event trace against the FP64 GEMM peak measured in this run (cuBLAS
+DGEMM, MEASURED_PEAKS.json has no FP64 figure).  cpu_baseline = the upstream CPU library
+(oracle/_ref, OpenBLAS on all host cores) on a bounded window of the same pencil.
+--impl reference times that CPU library alone (rank 0), one window sample per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "dtgevc3 n=8192 eigvecs/s vs plain FP64 GPU at resid<=1e-12; batched pencils/s"
+UNIT = "eigvecs/s"
+DATA = ("synthetic: seeded real generalized-Schur-form pencil with the statistics of xGGES output "
+        "of N(0,1) A,B (stand-in: xGGES at n=8192 takes ~1.5 h); random orthogonal Q, Z")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=8192)
+    ap.add_argument("--seed", type=int, default=8192)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--cpu-window", type=int, default=1024, help="eigenvalues per side in the CPU sample")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------------------
+# clocks during the timed region
+# ----------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.idx)], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.2)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                rows.append((float(p[1]), float(p[2]), float(p[3]) if p[3] not in ("[N/A]", "N/A") else 0.0, p[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        maxmhz = max(r[1] for r in rows)
+        load = [r for r in rows if r[2] > 200.0] or rows
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[i] for r in load for i, v in enumerate(r[3]) if v.lower() == "active"})
+        return {"sm_mhz": float(np.median([r[0] for r in load])), "sm_max_mhz": maxmhz, "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(r[2] for r in rows)}
+
+
+# ----------------------------------------------------------------------------------------
+# inputs
+# ----------------------------------------------------------------------------------------
+def host_pencil(n, seed):
+    from xtgevc3_b200 import pencils
+    return pencils.gen_schur_like(n, seed)
+
+
+def colmajor_cuda(a, torch):
+    """numpy Fortran matrix -> column-major CUDA tensor (stride(0) == 1)."""
+    return torch.from_numpy(np.ascontiguousarray(a.T)).cuda().t()
+
+
+def orthogonal(n, seed, torch):
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    A = torch.randn(n, n, device="cuda", dtype=torch.float64, generator=g)
+    Q, _ = torch.linalg.qr(A)
+    return Q.t().contiguous().t()  # column-major copy
+
+
+def dgemm_peak(torch):
+    """cuBLAS DGEMM 8192^3, best of 5 (burst), TFLOP/s: the FP64 denominator."""
+    n = 8192
+    a = torch.randn(n, n, device="cuda", dtype=torch.float64)
+    b = torch.randn_like(a)
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    best = 1e30
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(5):
+        e0.record()
+        a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def residual_max(torch, S, P, ar, ai, be, Q, Z, VL, VR):
+    """max over eigenvectors of ||beta S x - alpha P x||_1 / ((|beta| ||S||_1 + |alpha| ||P||_1) ||x||_1)
+    in Schur coordinates (x = Z^T v, y = Q^T u; Q, Z orthogonal)."""
+    dev = S.device
+    ar_t = torch.as_tensor(ar, device=dev)
+    ai_t = torch.as_tensor(ai, device=dev)
+    be_t = torch.as_tensor(be, device=dev)
+    nS = S.abs().sum(0).max()
+    nP = P.abs().sum(0).max()
+    out = []
+    for left, V, B in ((False, VR, Z), (True, VL, Q)):
+        W = B.t() @ V
+        Sm, Pm = (S.t(), P.t()) if left else (S, P)
+        SW = Sm @ W
+        PW = Pm @ W
+        n = W.shape[1]
+        re_c = torch.zeros(n, dtype=torch.bool, device=dev)
+        k = 0
+        pairs = []
+        ai_h = ai
+        while k < n:
+            if ai_h[k] != 0 and k + 1 < n:
+                pairs.append(k)
+                k += 2
+            else:
+                k += 1
+        idx = torch.as_tensor(pairs, device=dev, dtype=torch.long)
+        R = SW * be_t[None, :] - PW * ar_t[None, :]
+        num = R.abs().sum(0)
+        if len(pairs):
+            sg = 1.0 if not left else -1.0
+            xr, xi = idx, idx + 1
+            b = be_t[xr][None, :]
+            a_r, a_i = ar_t[xr][None, :], ai_t[xr][None, :]
+            rr = SW[:, xr] * b - PW[:, xr] * a_r + sg * a_i * PW[:, xi]
+            ri = SW[:, xi] * b - PW[:, xi] * a_r - sg * a_i * PW[:, xr]
+            pn = rr.abs().sum(0) + ri.abs().sum(0)
+            num[xr] = pn
+            num[xi] = pn
+            re_c[xr] = True
+        vn = W.abs().sum(0)
+        if len(pairs):
+            vv = vn[idx] + vn[idx + 1]
+            vn[idx] = vv
+            vn[idx + 1] = vv
+        amag = ar_t.abs() + ai_t.abs()
+        den = (be_t.abs() * nS + amag * nP) * vn
+        out.append(float((num / den).max()))
+    return max(out)
+
+
+# ----------------------------------------------------------------------------------------
+# CPU: the upstream library on a bounded window of the same pencil
+# ----------------------------------------------------------------------------------------
+def cpu_windows(n, w):
+    """Right window centred on n/sqrt(3), left on n - n/sqrt(3): the right eigenvector of
+    eigenvalue k costs ~k^2 and the left one ~(n-k)^2, whose means sit at those points.
+    Windows are aligned to the upstream 32-column panels."""
+    c = n / math.sqrt(3.0)
+    a_r = n - 32 * int(round((n - (c - w / 2)) / 32))
+    a_r = max(0, min(a_r, n - w))
+    c_l = n - c
+    a_l = 32 * int(round((c_l - w / 2) / 32))
+    a_l = max(0, min(a_l, n - w))
+    return (a_r, a_r + w), (a_l, a_l + w)
+
+
+def cpu_sample(S, P, ar, ai, be, w, threads):
+    """One sample: upstream dtgevc3 SIDE='R' and SIDE='L', HOWMNY='S' on the two windows.
+    Returns (eigenvectors, seconds, kind)."""
+    import oracle
+    n = S.shape[0]
+    (r0, r1), (l0, l1) = cpu_windows(n, w)
+    impl = "ref" if oracle.ref_available() else "oracle"
+    if impl == "ref":
+        oracle.set_ref_threads(threads)
+    tot_m, tot_t = 0, 0.0
+    for side, (a, b) in (("R", (r0, r1)), ("L", (l0, l1))):
+        sel = np.zeros(n, dtype=np.int32)
+        sel[a:b] = 1
+        mm = w + 2
+        V = np.zeros((n, mm), order="F")
+        t0 = time.perf_counter()
+        if side == "R":
+            _, _, m, info = oracle.tgevc3("R", "S", S, P, ar, be, alphai=ai, VR=V, VL=None, select=sel, mm=mm,
+                                          impl=impl)
+        else:
+            _, _, m, info = oracle.tgevc3("L", "S", S, P, ar, be, alphai=ai, VL=V, VR=None, select=sel, mm=mm,
+                                          impl=impl)
+        tot_t += time.perf_counter() - t0
+        assert info == 0
+        tot_m += m
+    return tot_m, tot_t, ("reference" if impl == "ref" else "port")
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    n = args.n
+    S, P, ar, ai, be = host_pencil(n, args.seed)
+    thr = host_threads()
+    w = 256
+    for _ in range(args.warmup):
+        cpu_sample(S, P, ar, ai, be, w, thr)
+    ms_tot, t_tot = 0, 0.0
+    kind = "reference"
+    for _ in range(args.steps):
+        m, t, kind = cpu_sample(S, P, ar, ai, be, w, thr)
+        ms_tot += m
+        t_tot += t
+    v = ms_tot / t_tot
+    sample = (f"upstream dtgevc3 HOWMNY='S' on one window of {w} eigenvalues per side (right window "
+              f"centred at n/sqrt(3), left at n-n/sqrt(3)) of the n={n} pencil per step; excludes the "
+              f"back-transform GEMM, so it overstates the CPU rate of HOWMNY='B'")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_tot / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
+            "config": {"workload": f"dtgevc3 SIDE=B HOWMNY=B n={n}", "n": n, "side": "B", "howmny": "B",
+                       "form": "upstream CPU (OpenBLAS)"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": thr, "kind": kind, "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------------------
+# GPU arm
+# ----------------------------------------------------------------------------------------
+def load_traffic():
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary, as bytes
+    per algorithmic flop (scaled to a launch of the bench by its flops)."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(p):
+        return None
+    try:
+        return json.load(open(p))
+    except (OSError, ValueError):
+        return None
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    import torch
+    import xtgevc3_b200 as X
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    n = args.n
+    # inputs: one pencil per rank
+    S_h, P_h, ar, ai, be = host_pencil(n, args.seed + rank)
+    S = colmajor_cuda(S_h, torch)
+    P = colmajor_cuda(P_h, torch)
+    Q = orthogonal(n, 2 * args.seed + 1 + 7 * rank, torch)
+    Z = orthogonal(n, 2 * args.seed + 2 + 7 * rank, torch)
+    VL = torch.empty_like(Q)
+    VR = torch.empty_like(Z)
+    peak_fp64 = dgemm_peak(torch)
+
+    def step():
+        VL.copy_(Q)
+        VR.copy_(Z)
+        X.tgevc3_dev("B", "B", S, P, ar, be, alphai=ai, VL=VL, VR=VR)
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = X.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    launches = X.launch_count() - l0
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        if dist:
+            dist.barrier()
+    value = world * 2 * n / (ms * 1e-3)
+
+    # accuracy of the timed result (outside the timed region)
+    resid = residual_max(torch, S, P, ar, ai, be, Q, Z, VL, VR)
+
+    # kernel trace (separate pass, same steps)
+    X.trace_reset()
+    X.trace_enable(True)
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize()
+    X.trace_enable(False)
+    tr = X.trace()
+    kernels = {k: dict(v, ms_per_step=v["ms"] / args.steps) for k, v in tr.items() if v["launches"]}
+    dom = max(kernels, key=lambda k: kernels[k]["ms"])
+    kd = kernels[dom]
+    if kd["flops"] > 0:
+        achieved = kd["flops"] / (kd["ms"] * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak_fp64, "unit": "TFLOP/s",
+                "frac": achieved / peak_fp64, "kernel": dom,
+                "peak_source": "cuBLAS DGEMM 8192^3 burst measured in this run (FP64; MEASURED_PEAKS.json "
+                               "has no FP64 figure)"}
+    else:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+            os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0}
+        achieved = kd["bytes"] / (kd["ms"] * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "kernel": dom, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
+    tinfo = load_traffic()
+    traffic = None
+    if tinfo and dom in tinfo.get("bytes_per_flop", {}) and kd["flops"] > 0:
+        traffic = tinfo["bytes_per_flop"][dom] * kd["flops"] / kd["launches"]
+        roof["traffic_note"] = tinfo.get("note", "")
+    roof["traffic"] = traffic
+    roof["algorithmic_per_launch"] = (kd["flops"] if kd["flops"] > 0 else kd["bytes"]) / kd["launches"]
+    for k in kernels.values():
+        if k["flops"] > 0:
+            k["tflops"] = k["flops"] / (k["ms"] * 1e-3) / 1e12
+        k["gbs"] = k["bytes"] / (k["ms"] * 1e-3) / 1e9 if k["ms"] > 0 else None
+
+    # end-to-end through the host-pointer C ABI (pinned host buffers, copies timed)
+    def pinned(shape):
+        t = torch.empty((shape[1], shape[0]), dtype=torch.float64, pin_memory=True)
+        return t.numpy().T  # Fortran-ordered view
+
+    hS, hP, hQ, hZ, hVL, hVR = (pinned((n, n)) for _ in range(6))
+    hS[...] = S_h
+    hP[...] = P_h
+    hQ[...] = Q.t().cpu().numpy().T
+    hZ[...] = Z.t().cpu().numpy().T
+    e2e_t = []
+    for it in range(args.warmup + args.steps):
+        np.copyto(hVL, hQ)
+        np.copyto(hVR, hZ)
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        _, _, m_, info_ = X.tgevc3("B", "B", hS, hP, ar, be, alphai=ai, VL=hVL, VR=hVR)
+        t1 = time.perf_counter()
+        assert info_ == 0
+        if it >= args.warmup:
+            e2e_t.append(t1 - t0)
+    e2e_s = float(np.mean(e2e_t))
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * 2 * n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 4 * n * n * 8,
+           "d2h_bytes_per_step": 2 * n * n * 8, "ms_per_step": 1e3 * e2e_s,
+           "path": "xtgevc3_dtgevc3 (host pointers, pinned), H2D/D2H inside the call"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        thr = host_threads()
+        m, t, kind = cpu_sample(S_h, P_h, ar, ai, be, args.cpu_window, thr)
+        cpu = {"value": m / t, "unit": UNIT, "cores": thr, "kind": kind, "seconds": t,
+               "sample": (f"upstream dtgevc3 HOWMNY='S' on one window of {args.cpu_window} eigenvalues per "
+                          f"side (right centred at n/sqrt(3), left at n-n/sqrt(3), where the per-vector cost "
+                          f"equals the mean) of the same n={n} pencil; excludes the back-transform, so it "
+                          f"overstates the CPU rate of HOWMNY='B'")}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": DATA,
+                "config": {"workload": f"dtgevc3 SIDE=B HOWMNY=B n={n}, plain FP64 form", "n": n, "side": "B",
+                           "howmny": "B", "form": "plain-fp64", "pencils_per_gpu": 1,
+                           "l2": "inputs larger than L2 (S,P,Q,Z = 2 GiB); no flush",
+                           "parallelism": f"independent pencil per GPU x{world}",
+                           "resid_max": resid, "resid_bound": 1e-12},
+                "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roof, "kernels": kernels,
+                "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -47,6 +47,19 @@ unsigned xtgevc3_get_flags(void);
 /* Text of the last CUDA failure seen by the calling thread ("" if none). */
 const char *xtgevc3_last_error(void);
 
+/* ---- kernel trace (no upstream counterpart) -------------------------------------------
+ * When enabled, every kernel the library launches is bracketed by CUDA events on its
+ * stream; per kernel class the launch count, summed device time (ms) and algorithmic
+ * flops / bytes (operation counts of the math, not hardware counters) accumulate until
+ * reset.  Classes: 0 prep, 1 diag_solve, 2 gemm_update, 3 gemm_backtransform,
+ * 4 writeback, 5 normalize.  xtgevc3_trace_get returns -1 for an unknown class.
+ * xtgevc3_launch_count counts every kernel launched by the library (traced or not). */
+void xtgevc3_trace_enable(int on);
+void xtgevc3_trace_reset(void);
+int xtgevc3_trace_get(int cls, long long *launches, double *ms, double *flops, double *bytes);
+const char *xtgevc3_trace_name(int cls);
+long long xtgevc3_launch_count(void);
+
 /* ---- host-pointer entry points (drop-in) -------------------------------------------
  * C-linkage twins of dtgevc3/stgevc3/ztgevc3/ctgevc3 (include/tgevc3.h).  Inputs are
  * copied to the current CUDA device, results copied back before return.             */

@@ -106,20 +106,28 @@ def test_against_oracle(cuda_ok, case):
 
 def test_graded_complex_scale_guards(cuda_ok):
     """zgges pencil of A, D*B with log10 d_i ~ U(-8, 8): eigenvalues over many orders of
-    magnitude.  Columns where the oracle itself is non-finite (repeated infinite
-    eigenvalues make its triangular solves singular) are excluded from the comparison; the
-    CUDA path must stay finite everywhere and satisfy the residual bound."""
+    magnitude and several exactly infinite ones (beta = 0).
+
+    The upstream code divides by the zero pivots of the repeated infinite eigenvalues
+    (non-finite columns), and its panel-wide overflow guard then scales the whole
+    32-column panel by (bignum/10)/inf = 0, so the other columns of that panel come back
+    as zero vectors.  Those degenerate oracle columns are excluded from the elementwise
+    comparison and checked by residual instead; the CUDA path (exact zero pivots raised
+    to smin, per-column guards) must be finite everywhere."""
     p = _pencil("graded", 160, 31, np.complex128)
     I = np.eye(160, dtype=np.complex128, order="F")
     d = dict(side="R", howmny="A", S=p["S"], P=p["P"], alpha=p["alpha"], beta=p["beta"], alphai=None,
              VL_in=I, VR_in=I.copy(order="F"), name="graded")
-    ref = oracle.tgevc3("R", "A", d["S"], d["P"], d["alpha"], d["beta"])
+    ref = oracle.tgevc3("R", "A", d["S"], d["P"], d["alpha"], d["beta"])[1]
     VL, VR, m, info = run_gpu(d)
     assert info == 0 and np.isfinite(VR).all()
-    err, cols = oracle.max_rel_diff(VR[:, :m], ref[1][:, :m])
+    good = np.isfinite(ref).all(0) & (np.abs(ref).max(0) > 0)
+    assert good.sum() >= 100
+    err, cols = oracle.max_rel_diff(VR[:, good], ref[:, good])
     assert err < 1e-9, err
+    finite_eig = np.abs(d["beta"]) > 0
     r = oracle.residual_ratio(d["S"], d["P"], VR[:, :m], d["alpha"], d["beta"])
-    assert r.max() < 100
+    assert r[finite_eig].max() < 100, r[finite_eig].max()
 
 
 def test_selection_and_one_sided(cuda_ok):

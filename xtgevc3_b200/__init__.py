@@ -63,8 +63,46 @@ def lib():
         L.xtgevc3_set_flags.restype = None
         L.xtgevc3_get_flags.restype = _U
         L.xtgevc3_last_error.restype = ct.c_char_p
+        L.xtgevc3_trace_enable.argtypes = [_I]
+        L.xtgevc3_trace_enable.restype = None
+        L.xtgevc3_trace_reset.restype = None
+        L.xtgevc3_trace_get.argtypes = [_I, _P, _P, _P, _P]
+        L.xtgevc3_trace_get.restype = _I
+        L.xtgevc3_trace_name.argtypes = [_I]
+        L.xtgevc3_trace_name.restype = ct.c_char_p
+        L.xtgevc3_launch_count.restype = ct.c_longlong
         _lib = L
     return _lib
+
+
+def trace_enable(on: bool = True) -> None:
+    """Time every library kernel with CUDA events (per kernel class; see trace())."""
+    lib().xtgevc3_trace_enable(1 if on else 0)
+
+
+def trace_reset() -> None:
+    lib().xtgevc3_trace_reset()
+
+
+def trace() -> dict:
+    """{class name: {launches, ms, flops, bytes}} accumulated since trace_reset()."""
+    out = {}
+    L = lib()
+    for cls in range(16):
+        n = ct.c_longlong(0)
+        ms = ct.c_double(0)
+        fl = ct.c_double(0)
+        by = ct.c_double(0)
+        if L.xtgevc3_trace_get(cls, ct.byref(n), ct.byref(ms), ct.byref(fl), ct.byref(by)) != 0:
+            break
+        out[L.xtgevc3_trace_name(cls).decode()] = dict(launches=n.value, ms=ms.value, flops=fl.value,
+                                                        bytes=by.value)
+    return out
+
+
+def launch_count() -> int:
+    """Kernels launched by the library so far in this process."""
+    return int(lib().xtgevc3_launch_count())
 
 
 def set_flags(flags: int) -> None:

@@ -204,6 +204,15 @@ void xtgevc3_set_flags(unsigned flags) { g_flags.store(flags); }
 unsigned xtgevc3_get_flags(void) { return g_flags.load(); }
 const char *xtgevc3_last_error(void) { return xtg::last_error(); }
 
+void xtgevc3_trace_enable(int on) { xtg::trace_enable(on); }
+void xtgevc3_trace_reset(void) { xtg::trace_reset(); }
+int xtgevc3_trace_get(int cls, long long *launches, double *ms, double *flops, double *bytes)
+{
+    return xtg::trace_get(cls, launches, ms, flops, bytes);
+}
+const char *xtgevc3_trace_name(int cls) { return xtg::trace_name(cls); }
+long long xtgevc3_launch_count(void) { return xtg::launch_count(); }
+
 void xtgevc3_dtgevc3(char side, char howmny, const int *select, int n, const double *S, int lds, const double *P,
                      int ldp, const double *alphar, const double *alphai, const double *beta, double *VL, int ldvl,
                      double *VR, int ldvr, int mm, int *m, double *work, int lwork, int *info)

@@ -23,6 +23,7 @@
 #include "kernels_misc.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <mutex>
@@ -45,6 +46,91 @@ void set_last_error(const std::string &s) { g_err = s; }
     } while (0)
 
 static inline int round_up(int v, int q) { return (v + q - 1) / q * q; }
+
+// ---- kernel trace ----------------------------------------------------------------------
+namespace {
+struct TraceTotals {
+    long long launches = 0;
+    double ms = 0, flops = 0, bytes = 0;
+};
+std::atomic<long long> g_launches{0};
+std::atomic<int> g_trace_on{0};
+std::mutex g_trace_mu;
+TraceTotals g_tot[kTCount];
+const char *g_trace_names[kTCount] = {"prep", "diag_solve", "gemm_update", "gemm_backtransform", "writeback",
+                                      "normalize"};
+
+// Brackets each kernel launch of one call with events when tracing is on; totals are
+// folded in after the call's stream synchronisation.
+struct Tracer {
+    struct Ev {
+        int cat;
+        cudaEvent_t a, b;
+        double flops, bytes;
+    };
+    std::vector<Ev> pend;
+    bool on = g_trace_on.load() != 0;
+    template <class F>
+    void run(int cat, double flops, double bytes, cudaStream_t st, F &&launch)
+    {
+        g_launches.fetch_add(1);
+        if (!on) {
+            launch();
+            return;
+        }
+        Ev e{cat, nullptr, nullptr, flops, bytes};
+        cudaEventCreate(&e.a);
+        cudaEventCreate(&e.b);
+        cudaEventRecord(e.a, st);
+        launch();
+        cudaEventRecord(e.b, st);
+        pend.push_back(e);
+    }
+    void flush()
+    {
+        std::lock_guard<std::mutex> lk(g_trace_mu);
+        for (Ev &e : pend) {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, e.a, e.b) == cudaSuccess) {
+                TraceTotals &t = g_tot[e.cat];
+                t.launches += 1;
+                t.ms += ms;
+                t.flops += e.flops;
+                t.bytes += e.bytes;
+            }
+            cudaEventDestroy(e.a);
+            cudaEventDestroy(e.b);
+        }
+        pend.clear();
+    }
+    ~Tracer()
+    {
+        for (Ev &e : pend) {
+            cudaEventDestroy(e.a);
+            cudaEventDestroy(e.b);
+        }
+    }
+};
+}  // namespace
+
+const char *trace_name(int cat) { return (cat >= 0 && cat < kTCount) ? g_trace_names[cat] : ""; }
+void trace_enable(int on) { g_trace_on.store(on ? 1 : 0); }
+void trace_reset()
+{
+    std::lock_guard<std::mutex> lk(g_trace_mu);
+    for (auto &t : g_tot) t = TraceTotals{};
+}
+int trace_get(int cat, long long *launches, double *ms, double *flops, double *bytes)
+{
+    if (cat < 0 || cat >= kTCount) return -1;
+    std::lock_guard<std::mutex> lk(g_trace_mu);
+    if (launches) *launches = g_tot[cat].launches;
+    if (ms) *ms = g_tot[cat].ms;
+    if (flops) *flops = g_tot[cat].flops;
+    if (bytes) *bytes = g_tot[cat].bytes;
+    return 0;
+}
+long long launch_count() { return g_launches.load(); }
 
 // Stream-ordered scratch; the device's default pool keeps freed memory for reuse.
 struct Scratch {
@@ -89,7 +175,8 @@ static void configure_device(int dev)
                              2 * kBlock * kSmLd * (int)sizeof(cplx<double>));
         cudaFuncSetAttribute(diag_solve_cplx<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              2 * kBlock * kSmLd * (int)sizeof(cplx<float>));
-        cudaFuncSetAttribute(gemm_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::SMEM_BYTES);
+        cudaFuncSetAttribute(gemm_dmma<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::SMEM_BYTES);
+        cudaFuncSetAttribute(gemm_dmma<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::SMEM_BYTES);
     });
 }
 
@@ -111,15 +198,16 @@ struct ColList {
 template <class E>
 static void launch_gemm(const GemmArgs<E> &g, bool simt, cudaStream_t st)
 {
-    if (g.M <= 0 || g.N <= 0 || g.K <= 0) return;
     if constexpr (std::is_same<E, double>::value) {
         // the cp.async path copies 16-byte pairs of rows: even leading dimensions and
         // 16-byte aligned bases only (caller-given ld may be odd on the device API)
         auto al = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
-        bool ok = (g.lda0 % 2 == 0) && (g.lda1 % 2 == 0) && (g.ldb % 2 == 0) && al(g.A0) && al(g.A1) && al(g.B);
+        bool ok = (g.ldb % 2 == 0) && al(g.B) && (g.C != nullptr);
+        for (int s = 0; s < g.nseg; s++) ok = ok && (g.seg[s].lda % 2 == 0) && al(g.seg[s].A) && (g.seg[s].boff % 2 == 0);
         if (!simt && ok) {
             dim3 grid((g.M + dmma::BM - 1) / dmma::BM, (g.N + dmma::BN - 1) / dmma::BN);
-            gemm_dmma<<<grid, 256, dmma::SMEM_BYTES, st>>>(g);
+            if (g.accumulate) gemm_dmma<1><<<grid, 256, dmma::SMEM_BYTES, st>>>(g);
+            else gemm_dmma<0><<<grid, 256, dmma::SMEM_BYTES, st>>>(g);
             return;
         }
     }
@@ -185,6 +273,8 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
     }
 
     Scratch scr(st);
+    Tracer tr;
+    const double esz = sizeof(E), cfl = CPLX ? 4.0 : 1.0;
     // eigenvalue data on the device (for the coefficient kernels)
     const int ncoef = CPLX ? 6 : 4;
     R *d_eig = scr.get<R>(CPLX ? 4 * (size_t)n : 3 * (size_t)n);
@@ -200,15 +290,18 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         XTG_CK(cudaMemcpyAsync(d_eig + 2 * n, beta_, n * sizeof(R), cudaMemcpyHostToDevice, st));
     }
     // anorm / bnorm (src/dtgevc3.cpp:1254-1270; complex: rows <= col only)
-    colsum_kernel<E, R><<<(n + 7) / 8, 256, 0, st>>>(S, lds, P, ldp, n, CPLX ? 0 : 1, d_sums);
-    colmax_kernel<R><<<1, 1024, 0, st>>>(d_sums, n, d_norms);
+    tr.run(kTPrep, 0, (double)n * (n + 1) * esz, st, [&] {
+        colsum_kernel<E, R><<<(n + 7) / 8, 256, 0, st>>>(S, lds, P, ldp, n, CPLX ? 0 : 1, d_sums);
+    });
+    tr.run(kTPrep, 0, 2.0 * n * sizeof(R), st, [&] { colmax_kernel<R><<<1, 1024, 0, st>>>(d_sums, n, d_norms); });
     XTG_CK(cudaGetLastError());
 
     const R safemin = limits<R>::safemin, eps = limits<R>::eps;
     const R bignum = R(1) / (safemin / eps);
     const int ld_n = round_up(n, 32);
 
-    auto run_side = [&](bool left) -> int {
+    // One side on stream `st` with scratch from `scr` (both shadow the call's own).
+    auto run_side = [&](bool left, cudaStream_t st, Scratch &scr) -> int {
         // ---- column list in problem orientation ---------------------------------------
         ColList L;
         L.m = m_total;
@@ -257,45 +350,99 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             E *Pt = scr.get<E>((size_t)ld_n * n);
             if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
             dim3 g((n + 31) / 32, (n + 31) / 32), b(32, 8);
-            rev_transpose_kernel<E><<<g, b, 0, st>>>(S, lds, St, ld_n, n, 1);
-            rev_transpose_kernel<E><<<g, b, 0, st>>>(P, ldp, Pt, ld_n, n, 1);
+            tr.run(kTPrep, 0, 2.0 * n * n * esz, st,
+                   [&] { rev_transpose_kernel<E><<<g, b, 0, st>>>(S, lds, St, ld_n, n, 1); });
+            tr.run(kTPrep, 0, 2.0 * n * n * esz, st,
+                   [&] { rev_transpose_kernel<E><<<g, b, 0, st>>>(P, ldp, Pt, ld_n, n, 1); });
             Sp = St;
             Pp = Pt;
             lsp = lpp = ld_n;
         }
-        const int ldx = ld_n, ldy = 2 * kBlock;
+        const int ldx = ld_n, ldy = 4 * kBlock;  // two halves of two padded row blocks
+        // work items of the diagonal solves: every column that starts an eigenvector
+        std::vector<int> items;
+        items.reserve(m);
+        for (int c = 0; c < m; c++)
+            if (L.kind[c] != kPairIm) items.push_back(c);
+        const int nitems = (int)items.size();
         E *X = scr.get<E>((size_t)ldx * m);
         E *Y = scr.get<E>((size_t)ldy * m);
         R *coef = scr.get<R>((size_t)ncoef * m);
-        int *d_ints = scr.get<int>(4 * (size_t)m);
+        int *d_ints = scr.get<int>(5 * (size_t)m);
         uint8_t *d_kind = scr.get<uint8_t>((size_t)m);
         if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
-        std::vector<int> ints(4 * (size_t)m);
+        std::vector<int> ints(5 * (size_t)m, 0);
         std::copy(L.colk.begin(), L.colk.end(), ints.begin());
         std::copy(L.src.begin(), L.src.end(), ints.begin() + m);
         std::copy(L.kext.begin(), L.kext.end(), ints.begin() + 2 * m);
         std::copy(L.outcol.begin(), L.outcol.end(), ints.begin() + 3 * m);
+        std::copy(items.begin(), items.end(), ints.begin() + 4 * m);
         XTG_CK(cudaMemcpyAsync(d_ints, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice, st));
         XTG_CK(cudaMemcpyAsync(d_kind, L.kind.data(), m, cudaMemcpyHostToDevice, st));
         const int *d_colk = d_ints, *d_src = d_ints + m, *d_kext = d_ints + 2 * m, *d_outcol = d_ints + 3 * m;
+        const int *d_items = d_ints + 4 * m;
         XTG_CK(cudaMemsetAsync(X, 0, (size_t)ldx * m * sizeof(E), st));
 
-        if constexpr (CPLX) {
-            coef_cplx_kernel<R><<<(m + 127) / 128, 128, 0, st>>>(reinterpret_cast<const cplx<R> *>(d_eig),
-                                                                 reinterpret_cast<const cplx<R> *>(d_eig + 2 * n),
-                                                                 d_src, m, left ? 1 : 0, d_norms, coef);
-        } else {
-            coef_real_kernel<R><<<(m + 127) / 128, 128, 0, st>>>(d_eig, d_eig + n, d_eig + 2 * n, d_src, d_kind, m,
-                                                                 left ? 1 : 0, d_norms, coef);
-        }
+        tr.run(kTPrep, 0, (double)m * ncoef * sizeof(R), st, [&] {
+            if constexpr (CPLX) {
+                coef_cplx_kernel<R><<<(m + 127) / 128, 128, 0, st>>>(
+                    reinterpret_cast<const cplx<R> *>(d_eig), reinterpret_cast<const cplx<R> *>(d_eig + 2 * n), d_src,
+                    m, left ? 1 : 0, d_norms, coef);
+            } else {
+                coef_real_kernel<R><<<(m + 127) / 128, 128, 0, st>>>(d_eig, d_eig + n, d_eig + 2 * n, d_src, d_kind,
+                                                                     m, left ? 1 : 0, d_norms, coef);
+            }
+        });
         XTG_CK(cudaGetLastError());
 
         // ---- blocked substitution ----------------------------------------------------------
+        // Row blocks are taken in pairs (a lower block L and the upper block U above it):
+        //   solve L; update the rows of U with L's solution (small GEMM); solve U;
+        //   update every row above U with both blocks at once (K = 4 strips).
+        // so the large trailing GEMMs see K = 2 * (|U| + |L|) ~ 256.  The update operand Y
+        // of a pair holds [-ac x_U; -ac x_L | b x_U; b x_L], each block padded to kKPad.
         const size_t diag_smem = 2 * kBlock * kSmLd * sizeof(E);
-        for (const auto &bk : blocks) {
-            const int r0 = bk.first, r1 = bk.second, jnb = r1 - r0;
-            const int c0 = int(std::lower_bound(L.colk.begin(), L.colk.end(), r0) - L.colk.begin());
-            if (c0 >= m) continue;
+        auto first_col = [&](int r) {
+            return int(std::lower_bound(L.colk.begin(), L.colk.end(), r) - L.colk.begin());
+        };
+        auto strip = [&](const E *A, int lda, int w0, int col, int jnb, int boff) {
+            GemmSeg<E> sg;
+            sg.A = A + (size_t)w0 + (size_t)col * lda;
+            sg.lda = lda;
+            sg.acols = jnb;
+            sg.K = round_up(jnb, kKPad);
+            sg.boff = boff;
+            return sg;
+        };
+        // X[w0 + mlo : w0 + M, c0:m] += sum over segments
+        auto update = [&](int w0, int mlo, int M, int c0, int nseg, const GemmSeg<E> *segs, double kflops) {
+            GemmArgs<E> g;
+            g.M = M;
+            g.N = m - c0;
+            g.mlo = mlo;
+            g.nseg = nseg;
+            g.K = 0;
+            for (int s = 0; s < nseg; s++) {
+                g.seg[s] = segs[s];
+                g.K += segs[s].K;
+            }
+            g.B = Y + (size_t)c0 * ldy;
+            g.ldb = ldy;
+            g.brows = ldy;
+            g.C = X + (size_t)w0 + (size_t)c0 * ldx;
+            g.ldc = ldx;
+            g.ccol = nullptr;
+            g.kext = nullptr;
+            g.accumulate = 1;
+            const double rows = M - mlo;
+            const double uf = 2.0 * rows * g.N * kflops * cfl;
+            const double ub = (2.0 * rows * g.N + rows * kflops + kflops * g.N) * esz;
+            tr.run(kTUpdate, uf, ub, st, [&] { launch_gemm<E>(g, opt.simt != 0, st); });
+        };
+        auto diag_solve = [&](int r0, int r1, int ys_off, int yhalf, int zl_off, int zl_len) {
+            const int jnb = r1 - r0;
+            const int c0 = first_col(r0);
+            if (c0 >= m) return;
             const int bpad = round_up(jnb, kKPad);
             DiagArgs<R> da;
             da.S = reinterpret_cast<const R *>(Sp);
@@ -305,9 +452,14 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             da.n = n;
             da.r0 = r0;
             da.r1 = r1;
-            da.bpad = bpad;
-            da.c0 = c0;
-            da.m = m;
+            da.ys_off = ys_off;
+            da.yhalf = yhalf;
+            da.ypad = bpad;
+            da.zl_off = zl_off;
+            da.zl_len = zl_len;
+            da.items = d_items;
+            da.it0 = int(std::lower_bound(items.begin(), items.end(), c0) - items.begin());
+            da.nitems = nitems;
             da.colk = d_colk;
             da.kind = d_kind;
             da.coef = coef;
@@ -318,33 +470,55 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             da.thr_rhs = bignum / R(10);
             da.thr_upd = bignum / R(std::max(1, jnb));
             da.left_seed = left ? 1 : 0;
-            const int ncols = m - c0;
-            const int grid = std::max(1, std::min((ncols + 7) / 8, 2 * 148));
-            if constexpr (CPLX) diag_solve_cplx<R><<<grid, 256, diag_smem, st>>>(da);
-            else diag_solve_real<R><<<grid, 256, diag_smem, st>>>(da);
-            if (r0 > 0) {
-                GemmArgs<E> g;
-                g.M = r0;
-                g.N = ncols;
-                g.K = 2 * bpad;
-                g.A0 = Sp + (size_t)r0 * lsp;
-                g.A1 = Pp + (size_t)r0 * lpp;
-                g.lda0 = lsp;
-                g.lda1 = lpp;
-                g.ksplit = bpad;
-                g.acols0 = n - r0;
-                g.acols1 = n - r0;
-                g.B = Y + (size_t)c0 * ldy;
-                g.ldb = ldy;
-                g.brows = 2 * bpad;
-                g.C = X + (size_t)c0 * ldx;
-                g.ldc = ldx;
-                g.ccol = nullptr;
-                g.kext = nullptr;
-                g.accumulate = 1;
-                launch_gemm<E>(g, opt.simt != 0, st);
+            const int grid = std::max(1, std::min((nitems - da.it0 + 7) / 8, 2 * 148));
+            // algorithmic work of the shifted solves: ~2 nrows^2 real flops per real column,
+            // 4x that per complex column or (Re, Im) pair; bytes: rhs in, solution and
+            // update operand out, the S/P block once
+            double dfl = 0, dby = 2.0 * jnb * jnb * esz;
+            for (int c = c0; c < m; c++) {
+                if (L.kind[c] == kPairIm) continue;
+                const int nr = L.colk[c] < r1 ? L.colk[c] - r0 : jnb;
+                const double w = (CPLX || L.kind[c] == kPairRe) ? 4.0 : 1.0;
+                const double cols = L.kind[c] == kPairRe ? 2.0 : 1.0;
+                dfl += 2.0 * nr * nr * w;
+                dby += cols * (double(nr < jnb ? 0 : jnb) + jnb + 2.0 * bpad) * esz;
+            }
+            tr.run(kTDiag, dfl, dby, st, [&] {
+                if constexpr (CPLX) diag_solve_cplx<R><<<grid, 256, diag_smem, st>>>(da);
+                else diag_solve_real<R><<<grid, 256, diag_smem, st>>>(da);
+            });
+        };
+        const int nbk = (int)blocks.size();
+        for (int bi = 0; bi < nbk;) {
+            const int l0 = blocks[bi].first, l1 = blocks[bi].second, jl = l1 - l0, bl = round_up(jl, kKPad);
+            if (bi + 1 == nbk) {  // unpaired top block
+                diag_solve(l0, l1, 0, bl, 0, 0);
+                const int c0 = first_col(l0);
+                if (l0 > 0 && c0 < m) {
+                    GemmSeg<E> sg[2] = {strip(Sp, lsp, 0, l0, jl, 0), strip(Pp, lpp, 0, l0, jl, bl)};
+                    update(0, 0, l0, c0, 2, sg, 2.0 * jl);
+                }
+                XTG_CK(cudaGetLastError());
+                bi += 1;
+                continue;
+            }
+            const int u0 = blocks[bi + 1].first, ju = l0 - u0, bu = round_up(ju, kKPad), bh = bu + bl;
+            diag_solve(l0, l1, bu, bh, 0, 0);
+            const int c0l = first_col(l0);
+            if (c0l < m) {  // rows of U (window from an even row) += L's contribution
+                const int w0 = u0 & ~1, mlo = u0 & 1;
+                GemmSeg<E> sg[2] = {strip(Sp, lsp, w0, l0, jl, bu), strip(Pp, lpp, w0, l0, jl, bh + bu)};
+                update(w0, mlo, mlo + ju, c0l, 2, sg, 2.0 * jl);
+            }
+            diag_solve(u0, l0, 0, bh, bu, bl);
+            const int c0u = first_col(u0);
+            if (u0 > 0 && c0u < m) {
+                GemmSeg<E> sg[4] = {strip(Sp, lsp, 0, u0, ju, 0), strip(Sp, lsp, 0, l0, jl, bu),
+                                    strip(Pp, lpp, 0, u0, ju, bh), strip(Pp, lpp, 0, l0, jl, bh + bu)};
+                update(0, 0, u0, c0u, 4, sg, 2.0 * (ju + jl));
             }
             XTG_CK(cudaGetLastError());
+            bi += 2;
         }
 
         // ---- write-back / back-transform -----------------------------------------------------
@@ -356,7 +530,8 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
             if (left) {
                 dim3 g((n + 255) / 256, n);
-                rev_columns_kernel<E><<<g, 256, 0, st>>>(V, ldv, Zc, ld_n, n, n);
+                tr.run(kTPrep, 0, 2.0 * n * n * esz, st,
+                       [&] { rev_columns_kernel<E><<<g, 256, 0, st>>>(V, ldv, Zc, ld_n, n, n); });
             } else {
                 XTG_CK(cudaMemcpy2DAsync(Zc, (size_t)ld_n * sizeof(E), V, (size_t)ldv * sizeof(E), n * sizeof(E), n,
                                          cudaMemcpyDeviceToDevice, st));
@@ -364,13 +539,10 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             GemmArgs<E> g;
             g.M = n;
             g.N = m;
-            g.K = n;
-            g.A0 = Zc;
-            g.A1 = Zc;
-            g.lda0 = g.lda1 = ld_n;
-            g.ksplit = n;
-            g.acols0 = n;
-            g.acols1 = 0;
+            g.mlo = 0;
+            g.nseg = 1;
+            g.seg[0] = strip(Zc, ld_n, 0, 0, n, 0);
+            g.K = g.seg[0].K;
             g.B = X;
             g.ldb = ldx;
             g.brows = n;
@@ -379,32 +551,75 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             g.ccol = d_outcol;
             g.kext = d_kext;
             g.accumulate = 0;
-            launch_gemm<E>(g, opt.simt != 0, st);
+            double bf = 0, bk = 0;
+            for (int c = 0; c < m; c++) bk += L.kext[c];
+            bf = 2.0 * n * bk * cfl;
+            const double bb = ((double)n * L.kext[m - 1] + bk + (double)n * m) * esz;
+            tr.run(kTBack, bf, bb, st, [&] { launch_gemm<E>(g, opt.simt != 0, st); });
         } else {
             dim3 g(std::max(1, std::min((n + 255) / 256, 64)), m);
-            writeback_kernel<E><<<g, 256, 0, st>>>(X, ldx, V, ldv, n, m, d_outcol, d_kext, left ? 1 : 0);
+            tr.run(kTWriteback, 0, 2.0 * n * m * esz, st, [&] {
+                writeback_kernel<E><<<g, 256, 0, st>>>(X, ldx, V, ldv, n, m, d_outcol, d_kext, left ? 1 : 0);
+            });
         }
         XTG_CK(cudaGetLastError());
 
         if (opt.normalize) {
             if constexpr (CPLX) {
-                normalize_cplx_kernel<R><<<m, 256, 0, st>>>(reinterpret_cast<cplx<R> *>(V), ldv, n, m);
+                tr.run(kTNormalize, 0, 2.0 * n * m * esz, st, [&] {
+                    normalize_cplx_kernel<R><<<m, 256, 0, st>>>(reinterpret_cast<cplx<R> *>(V), ldv, n, m);
+                });
             } else {
                 std::vector<uint8_t> ok(m, kReal);
                 for (int c = 0; c < m; c++) ok[L.outcol[c]] = L.kind[c];
                 uint8_t *d_ok = scr.get<uint8_t>(m);
                 if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
                 XTG_CK(cudaMemcpyAsync(d_ok, ok.data(), m, cudaMemcpyHostToDevice, st));
-                normalize_real_kernel<R><<<m, 256, 0, st>>>(V, ldv, n, d_ok, m);
+                tr.run(kTNormalize, 0, 2.0 * n * m * esz, st,
+                       [&] { normalize_real_kernel<R><<<m, 256, 0, st>>>(V, ldv, n, d_ok, m); });
             }
             XTG_CK(cudaGetLastError());
         }
         return 0;
     };
 
-    if (want_r && run_side(false)) return 1;
-    if (want_l && run_side(true)) return 1;
+    // The two sides are independent problems: with both requested they run concurrently,
+    // the left one on a second stream (serially while tracing, so that kernel times are
+    // not inflated by overlap).
+    if (want_r && want_l && !tr.on) {
+        struct Fork {
+            cudaStream_t s = nullptr;
+            cudaEvent_t fork = nullptr, join = nullptr;
+            ~Fork()
+            {
+                if (fork) cudaEventDestroy(fork);
+                if (join) cudaEventDestroy(join);
+                if (s) cudaStreamDestroy(s);
+            }
+        } fk;
+        XTG_CK(cudaStreamCreateWithFlags(&fk.s, cudaStreamNonBlocking));
+        XTG_CK(cudaEventCreateWithFlags(&fk.fork, cudaEventDisableTiming));
+        XTG_CK(cudaEventCreateWithFlags(&fk.join, cudaEventDisableTiming));
+        XTG_CK(cudaEventRecord(fk.fork, st));
+        XTG_CK(cudaStreamWaitEvent(fk.s, fk.fork, 0));
+        int rc = 0;
+        {
+            Scratch scr2(fk.s);
+            rc |= run_side(false, st, scr);
+            rc |= run_side(true, fk.s, scr2);
+            XTG_CK(cudaEventRecord(fk.join, fk.s));
+            XTG_CK(cudaStreamWaitEvent(st, fk.join, 0));
+        }
+        if (rc) {
+            cudaStreamSynchronize(fk.s);
+            return 1;
+        }
+    } else {
+        if (want_r && run_side(false, st, scr)) return 1;
+        if (want_l && run_side(true, st, scr)) return 1;
+    }
     XTG_CK(cudaStreamSynchronize(st));
+    tr.flush();
     return 0;
 }
 

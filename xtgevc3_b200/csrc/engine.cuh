@@ -27,4 +27,13 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
 const char *last_error();
 void set_last_error(const std::string &s);
 
+// Kernel trace: per kernel class, launches, CUDA-event time on the launching stream and
+// algorithmic flops / bytes (the operation counts of the math, not hardware counters).
+enum TraceCat { kTPrep = 0, kTDiag, kTUpdate, kTBack, kTWriteback, kTNormalize, kTCount };
+const char *trace_name(int cat);
+void trace_enable(int on);
+void trace_reset();
+int trace_get(int cat, long long *launches, double *ms, double *flops, double *bytes);
+long long launch_count();
+
 }  // namespace xtg

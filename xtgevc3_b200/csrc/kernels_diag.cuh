@@ -12,9 +12,14 @@
 //
 // Layout: one warp owns one eigenvector (a real column, a (Re, Im) column pair, or a
 // complex column); lane l holds rows l and l + 32 of the block.  S[I,I], P[I,I] live in
-// shared memory.  The solve is column-oriented block back substitution: after x_j is
-// known it is broadcast by shuffle and every lane updates its rows.  2x2 diagonal blocks
-// of S (S[j, j-1] != 0) are solved as 2x2 systems with partial pivoting.
+// shared memory.  Per eigenvector the lanes first factor, in parallel, every diagonal
+// block of W = ac S - b P: the reciprocal of each 1x1 pivot and the partially pivoted LU
+// of each 2x2 block (S[j, j-1] != 0; rows paired greedily from the bottom of the block).
+// The solve is then column-oriented block back substitution: the lane owning a block's
+// rows computes its solution, broadcasts it by shuffle, and every lane updates its rows.
+// An exactly zero (or subnormal) pivot is replaced by the column's smin =
+// max(eps (|ac| anorm + |b| bnorm), safemin), LAPACK xTGEVC's perturbation, so repeated
+// infinite eigenvalues give finite vectors; the upstream code divides by zero there.
 //
 // Overflow guards, per column (the upstream code rescales a whole 32-column panel):
 //   * before the solve: if max|rhs| > bignum/10, scale the column by (bignum/10)/max
@@ -36,6 +41,11 @@ constexpr int kSmLd = kBlock + 1;  // shared-memory leading dimension of the S/P
 
 template <class T>
 __device__ __forceinline__ T shfl(T v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+template <class R>
+__device__ __forceinline__ cplx<R> shfl(cplx<R> v, int src)
+{
+    return cplx<R>(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
 
 template <class R>
 __device__ __forceinline__ R warp_max(R v)
@@ -58,24 +68,43 @@ __device__ __forceinline__ void set_row(T (&r)[2], int row, int lane, T v)
     }
 }
 
+__device__ __forceinline__ double rcp(double v) { return __drcp_rn(v); }
+__device__ __forceinline__ float rcp(float v) { return __frcp_rn(v); }
+template <class R>
+__device__ __forceinline__ cplx<R> rcp(cplx<R> v) { return cdiv(cplx<R>(R(1), R(0)), v); }
+
+template <class R>
+__device__ __forceinline__ R mag(R v) { return fabs(v); }
+template <class R>
+__device__ __forceinline__ R mag(cplx<R> v) { return l1abs(v); }
+
+// A pivot that is zero (or subnormal) is replaced by smin; every other pivot is used as
+// is, like the upstream solves, which divide by whatever pivot they meet.  Graded pencils
+// legitimately have pivots far below eps * ||W||, so only exact singularity is perturbed.
 template <class R>
 __device__ __forceinline__ R floor_pivot(R w, R smin)
 {
-    return fabs(w) < smin ? (w < R(0) ? -smin : smin) : w;
+    return fabs(w) < limits<R>::safemin ? (w < R(0) ? -smin : smin) : w;
 }
 
 template <class R>
 __device__ __forceinline__ cplx<R> floor_pivot(cplx<R> w, R smin)
 {
-    return l1abs(w) < smin ? cplx<R>(smin, R(0)) : w;
+    return l1abs(w) < limits<R>::safemin ? cplx<R>(smin, R(0)) : w;
 }
 
 template <class R>
 struct DiagArgs {
     const R *S, *P;  // pencil in the orientation being solved (right problem)
     int lds, ldp, n;
-    int r0, r1, bpad;
-    int c0, m;
+    int r0, r1;
+    // update operand layout: this block's -ac x rows start at Y row ys_off, its b x rows at
+    // ys_off + yhalf; ypad (>= r1 - r0) rows are written, zeros past the block.  For a
+    // column whose eigenvalue lies in this block, rows [zl_off, zl_off + zl_len) of both
+    // halves (a lower block of the same update, where such a column is zero) are zeroed.
+    int ys_off, yhalf, ypad, zl_off, zl_len;
+    const int *items;        // columns that start an eigenvector (a pair's Re column), ascending
+    int it0, nitems;         // items [it0, nitems) are active in this block
     const int *colk;         // eigenvalue index (first member of a pair) per column
     const uint8_t *kind;     // kReal / kPairRe / kPairIm (real arithmetic only)
     const R *coef;           // 4 per column: ac, b_re, b_im, smin  (complex: 6: ac, b, smin, 0)
@@ -84,15 +113,146 @@ struct DiagArgs {
     R *Y;                    // 2*bpad x m update operand
     int ldy;
     R thr_rhs, thr_upd;
-    int left_seed;           // 2x2 seed of the left problem (see seed_pair)
+    int left_seed;           // 2x2 seed of the left problem (see the pair branch)
 };
 
 // Multiply rows [a, b) of one column by s (warp-cooperative).  Used on the rows of a
 // column outside the current block when an overflow guard fires.
-template <class R>
-__device__ __forceinline__ void scale_rows(R *col, int a, int b, R s, int lane)
+template <class E, class R>
+__device__ __forceinline__ void scale_rows(E *col, int a, int b, R s, int lane)
 {
-    for (int i = a + lane; i < b; i += 32) col[i] *= s;
+    for (int i = a + lane; i < b; i += 32) col[i] = s * col[i];
+}
+
+// Write this block's rows of one update-operand column: ys = -ac x, yp = b x for rows
+// i < jnb, zeros up to ypad, and the lower-block zeros of a diagonal-case column.
+template <class E, class R>
+__device__ __forceinline__ void write_y(const DiagArgs<R> &a, E *ycol, int jnb, bool diag, int lane, const E (&ys)[2],
+                                       const E (&yp)[2])
+{
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+        const int i = lane + 32 * s;
+        if (i < a.ypad) {
+            const bool in = i < jnb;
+            ycol[a.ys_off + i] = in ? ys[s] : E(0);
+            ycol[a.ys_off + a.yhalf + i] = in ? yp[s] : E(0);
+        }
+    }
+    if (diag)
+        for (int i = lane; i < a.zl_len; i += 32) {
+            ycol[a.zl_off + i] = E(0);
+            ycol[a.zl_off + a.yhalf + i] = E(0);
+        }
+}
+
+template <class E>
+__device__ __forceinline__ void load_block(const E *S, int lds, const E *P, int ldp, int r0, int jnb, int sub,
+                                           E *Ss, E *Ps)
+{
+    for (int t = threadIdx.x; t < jnb * jnb; t += blockDim.x) {
+        int i = t % jnb, j = t / jnb;
+        bool keep = i <= j + sub;  // upper triangle (plus the subdiagonal for real S)
+        Ss[i + j * kSmLd] = keep ? S[(size_t)(r0 + i) + (size_t)(r0 + j) * lds] : E(0);
+        Ps[i + j * kSmLd] = keep ? P[(size_t)(r0 + i) + (size_t)(r0 + j) * ldp] : E(0);
+    }
+}
+
+// Factors of the diagonal blocks of W for the rows a lane owns: inv1 = 1 / w_ii for every
+// row; for the second row i of a 2x2 block (i-1, i): the LU with partial pivoting on
+// column i-1:  swap rows if |w_i,i-1| > |w_i-1,i-1|, then (a b; c d) -> a^-1, b, m = c/a,
+// (d - m b)^-1.
+template <class E>
+struct Factors {
+    E inv1[2], fa[2], fb[2], fm[2], fu[2];
+    bool sw[2];
+};
+
+template <class E, class R, class WF>
+__device__ __forceinline__ void factor_rows(Factors<E> &F, uint64_t sec, int nrows, int lane, R smin, WF W)
+{
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+        const int i = lane + 32 * s;
+        F.inv1[s] = E(0);
+        F.fa[s] = F.fb[s] = F.fm[s] = F.fu[s] = E(0);
+        F.sw[s] = false;
+        if (i < nrows) {
+            F.inv1[s] = rcp(floor_pivot(W(i, i), smin));
+            if (i >= 1 && ((sec >> i) & 1ull)) {
+                E w11 = W(i - 1, i - 1), w12 = W(i - 1, i), w21 = W(i, i - 1), w22 = W(i, i);
+                const bool sw = mag(w21) > mag(w11);
+                E pa = sw ? w21 : w11, pb = sw ? w22 : w12, pc = sw ? w11 : w21, pd = sw ? w12 : w22;
+                E ia = rcp(floor_pivot(pa, smin));
+                E m = pc * ia;
+                F.fa[s] = ia;
+                F.fb[s] = pb;
+                F.fm[s] = m;
+                F.fu[s] = rcp(floor_pivot(pd - m * pb, smin));
+                F.sw[s] = sw;
+            }
+        }
+    }
+}
+
+// Block back substitution of one eigenvector held in r (rows [0, nrows)); on return r
+// holds the solution.  W(i, j) gives the shifted operator entry.
+template <class E, class WF>
+__device__ __forceinline__ void back_substitute(E (&r)[2], const Factors<E> &F, uint64_t sec, int nrows, int lane,
+                                                WF W)
+{
+    int j = nrows - 1;
+    while (j >= 0) {
+        if (j >= 1 && ((sec >> j) & 1ull)) {
+            const int p = j - 1, q = j;
+            const int sq = q >> 5;
+            const E rp = shfl(row_of(r, p), p & 31);
+            const E rq = row_of(r, q);  // valid on the owner of q, which does the solve
+            const bool sw = sq ? F.sw[1] : F.sw[0];
+            const E ia = sq ? F.fa[1] : F.fa[0], b = sq ? F.fb[1] : F.fb[0];
+            const E m = sq ? F.fm[1] : F.fm[0], iu = sq ? F.fu[1] : F.fu[0];
+            const E r1 = sw ? rq : rp, r2 = sw ? rp : rq;
+            E xq = (r2 - m * r1) * iu;
+            E xp = (r1 - b * xq) * ia;
+            xq = shfl(xq, q & 31);
+            xp = shfl(xp, q & 31);
+            set_row(r, p, lane, xp);
+            set_row(r, q, lane, xq);
+            if (lane < p) r[0] = r[0] - (W(lane, p) * xp + W(lane, q) * xq);
+            if (p > 32 && lane + 32 < p) r[1] = r[1] - (W(lane + 32, p) * xp + W(lane + 32, q) * xq);
+            j -= 2;
+        } else {
+            const E x = shfl((j >> 5) ? r[1] * F.inv1[1] : r[0] * F.inv1[0], j & 31);
+            set_row(r, j, lane, x);
+            if (lane < j) r[0] = r[0] - W(lane, j) * x;
+            if (j > 32 && lane + 32 < j) r[1] = r[1] - W(lane + 32, j) * x;
+            j -= 1;
+        }
+    }
+}
+
+// bit j set: rows (j-1, j) of the block form a 2x2 block, pairing greedily from the bottom
+template <class R>
+__device__ __forceinline__ void pair_mask(const R *Ss, int jnb, uint64_t *out)
+{
+    if (threadIdx.x < 32) {
+        const int l = threadIdx.x;
+        const bool b0 = l >= 1 && l < jnb && Ss[l + (l - 1) * kSmLd] != R(0);
+        const bool b1 = l + 32 < jnb && Ss[(l + 32) + (l + 31) * kSmLd] != R(0);
+        const uint64_t sub = (uint64_t)__ballot_sync(0xffffffffu, b0) | ((uint64_t)__ballot_sync(0xffffffffu, b1) << 32);
+        if (l == 0) {
+            uint64_t sec = 0;
+            for (int j = jnb - 1; j >= 1;) {
+                if ((sub >> j) & 1ull) {
+                    sec |= 1ull << j;
+                    j -= 2;
+                } else {
+                    j -= 1;
+                }
+            }
+            *out = sec;
+        }
+    }
 }
 
 // ------------------------------------------------------------------------------------
@@ -102,24 +262,21 @@ template <class R>
 __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ uint64_t s_sec;
     R *Ss = reinterpret_cast<R *>(smem_raw);
     R *Ps = Ss + kSmLd * kBlock;
     const int jnb = a.r1 - a.r0;
-    for (int t = threadIdx.x; t < jnb * jnb; t += blockDim.x) {
-        int i = t % jnb, j = t / jnb;
-        bool keep = i <= j + 1;  // upper triangle plus the subdiagonal
-        size_t gs = (size_t)(a.r0 + i) + (size_t)(a.r0 + j) * a.lds;
-        size_t gp = (size_t)(a.r0 + i) + (size_t)(a.r0 + j) * a.ldp;
-        Ss[i + j * kSmLd] = keep ? a.S[gs] : R(0);
-        Ps[i + j * kSmLd] = keep ? a.P[gp] : R(0);
-    }
+    load_block(a.S, a.lds, a.P, a.ldp, a.r0, jnb, 1, Ss, Ps);
     __syncthreads();
+    pair_mask(Ss, jnb, &s_sec);
+    __syncthreads();
+    const uint64_t sec = s_sec;
 
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int c = a.c0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); c < a.m; c += warps) {
+    for (int it = a.it0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); it < a.nitems; it += warps) {
+        const int c = a.items[it];
         const uint8_t kd = a.kind[c];
-        if (kd == kPairIm) continue;
         const int k = a.colk[c];
         const int kl = k - a.r0;
         const bool diag = k < a.r1;
@@ -128,14 +285,14 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
         const int nrows = diag ? kl : jnb;
         if (kd == kReal) {
             const int top = k;
+            auto W = [&](int i, int j) -> R { return ac * Ss[i + j * kSmLd] - br * Ps[i + j * kSmLd]; };
             R r[2];
             R seed = diag ? R(1) : R(0);
 #pragma unroll
             for (int s = 0; s < 2; s++) {
                 int i = lane + 32 * s;
                 R v = R(0);
-                if (i < nrows)
-                    v = diag ? -(ac * Ss[i + kl * kSmLd] - br * Ps[i + kl * kSmLd]) : colr[a.r0 + i];
+                if (i < nrows) v = diag ? -W(i, kl) : colr[a.r0 + i];
                 r[s] = v;
             }
             if (nrows > 0) {
@@ -146,51 +303,9 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
                     if (!diag) { scale_rows(colr, 0, a.r0, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane); }
                 }
             }
-            // block back substitution
-            int j = nrows - 1;
-            while (j >= 0) {
-                const bool two = j >= 1 && Ss[j + (j - 1) * kSmLd] != R(0);
-                if (!two) {
-                    R w = floor_pivot(ac * Ss[j + j * kSmLd] - br * Ps[j + j * kSmLd], smin);
-                    R rj = shfl(row_of(r, j), j & 31);
-                    R xj = rj / w;
-                    set_row(r, j, lane, xj);
-#pragma unroll
-                    for (int s = 0; s < 2; s++) {
-                        int i = lane + 32 * s;
-                        if (i < j) r[s] -= (ac * Ss[i + j * kSmLd] - br * Ps[i + j * kSmLd]) * xj;
-                    }
-                    j -= 1;
-                } else {
-                    const int p = j - 1, q = j;
-                    R w11 = ac * Ss[p + p * kSmLd] - br * Ps[p + p * kSmLd];
-                    R w12 = ac * Ss[p + q * kSmLd] - br * Ps[p + q * kSmLd];
-                    R w21 = ac * Ss[q + p * kSmLd] - br * Ps[q + p * kSmLd];
-                    R w22 = ac * Ss[q + q * kSmLd] - br * Ps[q + q * kSmLd];
-                    R rp = shfl(row_of(r, p), p & 31), rq = shfl(row_of(r, q), q & 31);
-                    if (fabs(w21) > fabs(w11)) {  // row interchange (partial pivoting on column p)
-                        R t;
-                        t = w11; w11 = w21; w21 = t;
-                        t = w12; w12 = w22; w22 = t;
-                        t = rp; rp = rq; rq = t;
-                    }
-                    w11 = floor_pivot(w11, smin);
-                    R mult = w21 / w11;
-                    R u22 = floor_pivot(w22 - mult * w12, smin);
-                    R xq = (rq - mult * rp) / u22;
-                    R xp = (rp - w12 * xq) / w11;
-                    set_row(r, p, lane, xp);
-                    set_row(r, q, lane, xq);
-#pragma unroll
-                    for (int s = 0; s < 2; s++) {
-                        int i = lane + 32 * s;
-                        if (i < p)
-                            r[s] -= (ac * Ss[i + p * kSmLd] - br * Ps[i + p * kSmLd]) * xp +
-                                    (ac * Ss[i + q * kSmLd] - br * Ps[i + q * kSmLd]) * xq;
-                    }
-                    j -= 2;
-                }
-            }
+            Factors<R> F;
+            factor_rows(F, sec, nrows, lane, smin, W);
+            back_substitute(r, F, sec, nrows, lane, W);
             // assemble the block column (solution rows, seed, zeros below the seed)
             R x[2];
 #pragma unroll
@@ -204,17 +319,15 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
                 x[0] *= sc; x[1] *= sc;
                 if (!diag) { scale_rows(colr, 0, a.r0, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane); }
             }
-            R *ycol = a.Y + (size_t)c * a.ldy;
+            R ys[2], yp[2];
 #pragma unroll
             for (int s = 0; s < 2; s++) {
                 int i = lane + 32 * s;
                 if (i < jnb) colr[a.r0 + i] = x[s];
-                if (i < a.bpad) {
-                    bool in = i < jnb;
-                    ycol[i] = in ? -ac * x[s] : R(0);
-                    ycol[a.bpad + i] = in ? br * x[s] : R(0);
-                }
+                ys[s] = -ac * x[s];
+                yp[s] = br * x[s];
             }
+            write_y(a, a.Y + (size_t)c * a.ldy, jnb, diag, lane, ys, yp);
         } else {
             // complex pair stored as (Re, Im) in columns (c, c+1); shift b = br + i*bi
             using C = cplx<R>;
@@ -257,48 +370,9 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
                     }
                 }
             }
-            int j = nrows - 1;
-            while (j >= 0) {
-                const bool two = j >= 1 && Ss[j + (j - 1) * kSmLd] != R(0);
-                if (!two) {
-                    C w = floor_pivot(W(j, j), smin);
-                    C rs = row_of(r, j);
-                    C rj(shfl(rs.x, j & 31), shfl(rs.y, j & 31));
-                    C xj = cdiv(rj, w);
-                    set_row(r, j, lane, xj);
-#pragma unroll
-                    for (int s = 0; s < 2; s++) {
-                        int i = lane + 32 * s;
-                        if (i < j) r[s] = r[s] - W(i, j) * xj;
-                    }
-                    j -= 1;
-                } else {
-                    const int p = j - 1, q = j;
-                    C w11 = W(p, p), w12 = W(p, q), w21 = W(q, p), w22 = W(q, q);
-                    C sp_ = row_of(r, p), sq_ = row_of(r, q);
-                    C rp(shfl(sp_.x, p & 31), shfl(sp_.y, p & 31));
-                    C rq(shfl(sq_.x, q & 31), shfl(sq_.y, q & 31));
-                    if (l1abs(w21) > l1abs(w11)) {
-                        C t;
-                        t = w11; w11 = w21; w21 = t;
-                        t = w12; w12 = w22; w22 = t;
-                        t = rp; rp = rq; rq = t;
-                    }
-                    w11 = floor_pivot(w11, smin);
-                    C mult = cdiv(w21, w11);
-                    C u22 = floor_pivot(w22 - mult * w12, smin);
-                    C xq = cdiv(rq - mult * rp, u22);
-                    C xp = cdiv(rp - w12 * xq, w11);
-                    set_row(r, p, lane, xp);
-                    set_row(r, q, lane, xq);
-#pragma unroll
-                    for (int s = 0; s < 2; s++) {
-                        int i = lane + 32 * s;
-                        if (i < p) r[s] = r[s] - (W(i, p) * xp + W(i, q) * xq);
-                    }
-                    j -= 2;
-                }
-            }
+            Factors<C> F;
+            factor_rows(F, sec, nrows, lane, smin, W);
+            back_substitute(r, F, sec, nrows, lane, W);
             C x[2];
 #pragma unroll
             for (int s = 0; s < 2; s++) {
@@ -320,20 +394,20 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
                     scale_rows(coli, 0, a.r0, sc, lane); scale_rows(coli, a.r1, top + 1, sc, lane);
                 }
             }
-            R *yre = a.Y + (size_t)c * a.ldy, *yim = yre + a.ldy;
+            R ysr[2], ysi[2], ypr[2], ypi[2];
 #pragma unroll
             for (int s = 0; s < 2; s++) {
                 int i = lane + 32 * s;
                 if (i < jnb) { colr[a.r0 + i] = x[s].x; coli[a.r0 + i] = x[s].y; }
-                if (i < a.bpad) {
-                    bool in = i < jnb;
-                    C yp = b * x[s];
-                    yre[i] = in ? -ac * x[s].x : R(0);
-                    yim[i] = in ? -ac * x[s].y : R(0);
-                    yre[a.bpad + i] = in ? yp.x : R(0);
-                    yim[a.bpad + i] = in ? yp.y : R(0);
-                }
+                C yp = b * x[s];
+                ysr[s] = -ac * x[s].x;
+                ysi[s] = -ac * x[s].y;
+                ypr[s] = yp.x;
+                ypi[s] = yp.y;
             }
+            R *yre = a.Y + (size_t)c * a.ldy;
+            write_y(a, yre, jnb, diag, lane, ysr, ypr);
+            write_y(a, yre + a.ldy, jnb, diag, lane, ysi, ypi);
         }
     }
 }
@@ -348,24 +422,17 @@ __global__ void __launch_bounds__(256) diag_solve_cplx(DiagArgs<R> a)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *Ss = reinterpret_cast<C *>(smem_raw);
     C *Ps = Ss + kSmLd * kBlock;
-    const C *S = reinterpret_cast<const C *>(a.S);
-    const C *P = reinterpret_cast<const C *>(a.P);
     const int jnb = a.r1 - a.r0;
-    for (int t = threadIdx.x; t < jnb * jnb; t += blockDim.x) {
-        int i = t % jnb, j = t / jnb;
-        bool keep = i <= j;
-        size_t gs = (size_t)(a.r0 + i) + (size_t)(a.r0 + j) * a.lds;
-        size_t gp = (size_t)(a.r0 + i) + (size_t)(a.r0 + j) * a.ldp;
-        Ss[i + j * kSmLd] = keep ? S[gs] : C(0, 0);
-        Ps[i + j * kSmLd] = keep ? P[gp] : C(0, 0);
-    }
+    load_block(reinterpret_cast<const C *>(a.S), a.lds, reinterpret_cast<const C *>(a.P), a.ldp, a.r0, jnb, 0, Ss,
+               Ps);
     __syncthreads();
 
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
     C *X = reinterpret_cast<C *>(a.X);
     C *Y = reinterpret_cast<C *>(a.Y);
-    for (int c = a.c0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); c < a.m; c += warps) {
+    for (int it = a.it0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); it < a.nitems; it += warps) {
+        const int c = a.items[it];
         const int k = a.colk[c];
         const int kl = k - a.r0;
         const bool diag = k < a.r1;
@@ -390,24 +457,12 @@ __global__ void __launch_bounds__(256) diag_solve_cplx(DiagArgs<R> a)
             if (mx > a.thr_rhs) {
                 R sc = a.thr_rhs / mx;
                 r[0] = sc * r[0]; r[1] = sc * r[1]; seed = sc * seed;
-                if (!diag) {
-                    for (int i = lane; i < a.r0; i += 32) col[i] = sc * col[i];
-                    for (int i = a.r1 + lane; i <= top; i += 32) col[i] = sc * col[i];
-                }
+                if (!diag) { scale_rows(col, 0, a.r0, sc, lane); scale_rows(col, a.r1, top + 1, sc, lane); }
             }
         }
-        for (int j = nrows - 1; j >= 0; j--) {
-            C w = floor_pivot(W(j, j), smin);
-            C rs = row_of(r, j);
-            C rj(shfl(rs.x, j & 31), shfl(rs.y, j & 31));
-            C xj = cdiv(rj, w);
-            set_row(r, j, lane, xj);
-#pragma unroll
-            for (int s = 0; s < 2; s++) {
-                int i = lane + 32 * s;
-                if (i < j) r[s] = r[s] - W(i, j) * xj;
-            }
-        }
+        Factors<C> F;
+        factor_rows(F, 0ull, nrows, lane, smin, W);
+        back_substitute(r, F, 0ull, nrows, lane, W);
         C x[2];
 #pragma unroll
         for (int s = 0; s < 2; s++) {
@@ -421,22 +476,17 @@ __global__ void __launch_bounds__(256) diag_solve_cplx(DiagArgs<R> a)
         if (mx > a.thr_upd) {
             R sc = a.thr_upd / mx;
             x[0] = sc * x[0]; x[1] = sc * x[1];
-            if (!diag) {
-                for (int i = lane; i < a.r0; i += 32) col[i] = sc * col[i];
-                for (int i = a.r1 + lane; i <= top; i += 32) col[i] = sc * col[i];
-            }
+            if (!diag) { scale_rows(col, 0, a.r0, sc, lane); scale_rows(col, a.r1, top + 1, sc, lane); }
         }
-        C *ycol = Y + (size_t)c * a.ldy;
+        C ys[2], yp[2];
 #pragma unroll
         for (int s = 0; s < 2; s++) {
             int i = lane + 32 * s;
             if (i < jnb) col[a.r0 + i] = x[s];
-            if (i < a.bpad) {
-                bool in = i < jnb;
-                ycol[i] = in ? -(ac * x[s]) : C(0, 0);
-                ycol[a.bpad + i] = in ? bc * x[s] : C(0, 0);
-            }
+            ys[s] = -(ac * x[s]);
+            yp[s] = bc * x[s];
         }
+        write_y(a, Y + (size_t)c * a.ldy, jnb, diag, lane, ys, yp);
     }
 }
 

@@ -1,27 +1,36 @@
 // GEMM kernels of the substitution: the trailing update of the accumulated right-hand
 // sides and the back-transform by Z (or Q).
 //
-//   C[0:M, j] (+)= sum_kk A(m, kk) * B(kk, j)
+//   C[mlo:M, j] (+)= sum_kk A(m, kk) * B(kk, j)
 //
-// A is column-major and may be stacked from two sources along K (A0 for kk < ksplit,
-// A1 after), which lets one launch apply both halves of the update
+// A is column-major and stacked from up to four segments along K (each a strip of S or P
+// or of Z), which lets one launch apply every half of an update
 //   X[0:r0, c] += S[0:r0, I] * (-ac x) + P[0:r0, I] * (b x)
-// (upstream: the two dgemm_ calls at src/dtgevc3.cpp:1432-1433).  For the back-transform
-// (src/dtgevc3.cpp:1446, 1638) A is Z (or Q with reversed columns), B is the upper
-// triangular X, and `kext` gives per column the number of leading rows of B that can be
-// nonzero so that a column tile only runs K up to its last nonzero row.  The optional
-// column map scatters result columns into their output positions.
+// (upstream: the two dgemm_ calls at src/dtgevc3.cpp:1432-1433), also for two row blocks
+// at once (K = 4 strips).  Segment s covers K rows [kb_s, kb_s + K_s) (K_s a multiple of
+// 16), reads A_s columns [0, acols_s) (beyond them: zero) and B rows boff_s + (kk - kb_s).
+// Rows [0, mlo) of the row window are computed but neither read nor written in C (they
+// let a window start on an even row).  For the back-transform (src/dtgevc3.cpp:1446, 1638)
+// A is Z (or Q with reversed columns), B is the upper triangular X, and `kext` gives per
+// column the number of leading rows of B that can be nonzero so that a column tile only
+// runs K up to its last nonzero row.  The optional column map scatters result columns
+// into their output positions.
 #pragma once
 #include "common.cuh"
 
 namespace xtg {
 
 template <class E>
+struct GemmSeg {
+    const E *A;  // row 0 of the window, first column of the strip
+    int lda, acols, K, boff;
+};
+
+template <class E>
 struct GemmArgs {
-    int M, N, K;
-    const E *A0, *A1;
-    int lda0, lda1, ksplit;
-    int acols0, acols1;  // columns of A0 / A1 that exist in memory (beyond: read as zero)
+    int M, N, K, mlo;
+    int nseg;
+    GemmSeg<E> seg[4];
     const E *B;
     int ldb, brows;      // rows of B that exist in memory
     E *C;
@@ -31,19 +40,21 @@ struct GemmArgs {
     int accumulate;
 };
 
-template <class R> __device__ __forceinline__ R zero_of() { return R(0); }
-
+// Segment holding K row kk (segments are contiguous and cover [0, K)); kb = its first row.
 template <class E>
-__device__ __forceinline__ E load_a(const GemmArgs<E> &g, int m, int kk)
+__device__ __forceinline__ int find_seg(const GemmArgs<E> &g, int kk, int &kb)
 {
-    if (m >= g.M) return E(0);
-    if (kk < g.ksplit) {
-        if (kk >= g.acols0) return E(0);
-        return g.A0[(size_t)m + (size_t)kk * g.lda0];
+    int base = 0;
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+        if (s < g.nseg && kk < base + g.seg[s].K) {
+            kb = base;
+            return s;
+        }
+        if (s < g.nseg) base += g.seg[s].K;
     }
-    int k2 = kk - g.ksplit;
-    if (k2 >= g.acols1) return E(0);
-    return g.A1[(size_t)m + (size_t)k2 * g.lda1];
+    kb = base;
+    return -1;
 }
 
 template <class E>
@@ -76,18 +87,25 @@ __global__ void __launch_bounds__(256) gemm_simt(GemmArgs<E> g)
         for (int j = 0; j < 4; j++) acc[i][j] = E(0);
 
     for (int k0 = 0; k0 < kmax; k0 += BK) {
+        int kb = 0;
+        const int s = find_seg(g, k0, kb);
+        const GemmSeg<E> sg = g.seg[s < 0 ? 0 : s];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             int e = tid + 256 * q;
             int m = e % BM, kk = e / BM;
-            As[kk][m] = (k0 + kk < kmax) ? load_a(g, m0 + m, k0 + kk) : E(0);
+            int col = k0 - kb + kk, row = m0 + m;
+            As[kk][m] = (s >= 0 && k0 + kk < kmax && col < sg.acols && row < g.M)
+                            ? sg.A[(size_t)row + (size_t)col * sg.lda]
+                            : E(0);
         }
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             int e = tid + 256 * q;
             int kk = e % BK, n = e / BK;
-            int kr = k0 + kk, col = n0 + n;
-            Bs[kk][n] = (kr < kmax && kr < g.brows && col < g.N) ? g.B[(size_t)kr + (size_t)col * g.ldb] : E(0);
+            int kr = sg.boff + k0 - kb + kk, col = n0 + n;
+            Bs[kk][n] = (s >= 0 && k0 + kk < kmax && kr < g.brows && col < g.N) ? g.B[(size_t)kr + (size_t)col * g.ldb]
+                                                                              : E(0);
         }
         __syncthreads();
 #pragma unroll
@@ -113,7 +131,7 @@ __global__ void __launch_bounds__(256) gemm_simt(GemmArgs<E> g)
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             int row = m0 + tx + 16 * i;
-            if (row < g.M) cp[row] = g.accumulate ? cp[row] + acc[i][j] : acc[i][j];
+            if (row >= g.mlo && row < g.M) cp[row] = g.accumulate ? cp[row] + acc[i][j] : acc[i][j];
         }
     }
 }
@@ -122,6 +140,8 @@ __global__ void __launch_bounds__(256) gemm_simt(GemmArgs<E> g)
 // FP64 tensor-core kernel (DMMA, mma.sync m8n8k4 f64).
 // CTA tile 128 x 64, K step 16, 8 warps as 4 (M) x 2 (N) with 32 x 32 warp tiles,
 // 3-stage cp.async pipeline into padded shared memory (conflict-free fragment loads).
+// Requires 16-byte aligned segment bases and B, and even leading dimensions (checked by
+// the launcher, which uses the SIMT kernel otherwise).
 // ------------------------------------------------------------------------------------
 namespace dmma {
 constexpr int BM = 128, BN = 64, BK = 16, STAGES = 3;
@@ -148,6 +168,8 @@ __device__ __forceinline__ void dmma884(double &d0, double &d1, double a, double
                  : "d"(a), "d"(b));
 }
 
+// ACC = 1: trailing update (C += A B); ACC = 0: back-transform (C = A B, triangular B).
+template <int ACC>
 __global__ void __launch_bounds__(256) gemm_dmma(GemmArgs<double> g)
 {
     using namespace dmma;
@@ -172,30 +194,29 @@ __global__ void __launch_bounds__(256) gemm_dmma(GemmArgs<double> g)
 
     auto load_stage = [&](int kt, int st) {
         const int k0 = kt * BK;
+        int kb = 0;
+        const int s = find_seg(g, k0, kb);
+        const GemmSeg<double> sg = g.seg[s < 0 ? 0 : s];
         double *as = As + st * A_STAGE;
         double *bs = Bs + st * B_STAGE;
 #pragma unroll
         for (int q = 0; q < 4; q++) {  // A: 16 columns x 64 chunks
             int e = tid + 256 * q;
             int kk = e >> 6, ch = e & 63;
-            int row = m0 + 2 * ch, kg = k0 + kk;
-            const double *src = g.A0;
-            int col = kg, ok = kg < kmax, lda = g.lda0;
-            if (kg >= g.ksplit) { src = g.A1; col = kg - g.ksplit; ok = ok && col < g.acols1; lda = g.lda1; }
-            else ok = ok && col < g.acols0;
+            int row = m0 + 2 * ch, col = k0 - kb + kk;
             int bytes = 0;
-            if (ok) bytes = row + 1 < g.M ? 16 : (row < g.M ? 8 : 0);
-            const double *gp = bytes ? src + (size_t)row + (size_t)col * lda : g.A0;
+            if (s >= 0 && k0 + kk < kmax && col < sg.acols) bytes = row + 1 < g.M ? 16 : (row < g.M ? 8 : 0);
+            const double *gp = bytes ? sg.A + (size_t)row + (size_t)col * sg.lda : g.B;
             cp_async16(as + kk * ALD + 2 * ch, gp, bytes);
         }
 #pragma unroll
         for (int q = 0; q < 2; q++) {  // B: 64 columns x 8 chunks
             int e = tid + 256 * q;
             int nn = e >> 3, ch = e & 7;
-            int kr = k0 + 2 * ch, col = n0 + nn;
-            int lim = min(kmax, g.brows);
+            int kr = sg.boff + k0 - kb + 2 * ch, col = n0 + nn;
+            int lim = min(sg.boff + kmax - kb, g.brows);
             int bytes = 0;
-            if (col < g.N) bytes = kr + 1 < lim ? 16 : (kr < lim ? 8 : 0);
+            if (s >= 0 && col < g.N) bytes = kr + 1 < lim ? 16 : (kr < lim ? 8 : 0);
             const double *gp = bytes ? g.B + (size_t)kr + (size_t)col * g.ldb : g.B;
             cp_async16(bs + nn * BLD + 2 * ch, gp, bytes);
         }
@@ -205,6 +226,24 @@ __global__ void __launch_bounds__(256) gemm_dmma(GemmArgs<double> g)
     for (int s = 0; s < STAGES - 1; s++) {
         if (s < ktiles) load_stage(s, s);
         cp_async_commit();
+    }
+    // Accumulating launches start from C: its loads are issued here, behind the first
+    // pipeline stages, so their latency overlaps the prologue instead of the epilogue.
+    if (ACC) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int col = n0 + wn * 32 + j * 8 + 2 * tq + h;
+                if (col >= g.N) continue;
+                const double *cp = g.C + (size_t)(g.ccol ? g.ccol[col] : col) * g.ldc;
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const int row = m0 + wm * 32 + i * 8 + gq;
+                    if (row >= g.mlo && row < g.M) acc[i][j][h] = cp[row];
+                }
+            }
+        }
     }
     for (int kt = 0; kt < ktiles; kt++) {
         cp_async_wait<STAGES - 2>();
@@ -241,7 +280,7 @@ __global__ void __launch_bounds__(256) gemm_dmma(GemmArgs<double> g)
 #pragma unroll
             for (int i = 0; i < 4; i++) {
                 int row = m0 + wm * 32 + i * 8 + gq;
-                if (row < g.M) cp[row] = g.accumulate ? cp[row] + acc[i][j][h] : acc[i][j][h];
+                if (row >= g.mlo && row < g.M) cp[row] = acc[i][j][h];
             }
         }
     }
