@@ -103,6 +103,23 @@ int xtgevc3_ctgevc3_dev(unsigned flags, void *stream, char side, char howmny, co
                         const float *S, int lds, const float *P, int ldp, const float *alpha, const float *beta,
                         float *VL, int ldvl, float *VR, int ldvr, int mm, int *m, int *info);
 
+/* ---- allocation-free device entry point (no counterpart in the upstream library) -----
+ * Same computation and arguments as xtgevc3_dtgevc3_dev (without flags), for callers that
+ * cannot allocate device memory at this point: e.g. a framework that has reserved the
+ * device memory for its own pool, or a latency-critical loop where a device allocation is
+ * not acceptable.  It calls no cudaMalloc/cudaFree or other allocating routine: its scratch
+ * is one 8 MiB block of device memory inside the library, held on every GPU that loads
+ * the library until exit, so problems are limited to what fits (SIDE='B', HOWMNY='B':
+ * n <= 448); larger ones return 2 with a message in xtgevc3_last_error(), without device
+ * work.  The first call on a device looks up the block's device address (make it before
+ * any stream capture).  All calls share the block: calls whose work overlaps on the GPU
+ * race and must be ordered by the caller (e.g. one stream).
+ * Returns 0, 1 (CUDA failure, *info = 1) or 2 (too large).                              */
+int xtgevc3_dtgevc3_dev_noalloc(void *stream, char side, char howmny, const int *select, int n, const double *S,
+                                int lds, const double *P, int ldp, const double *alphar, const double *alphai,
+                                const double *beta, double *VL, int ldvl, double *VR, int ldvr, int mm, int *m,
+                                int *info);
+
 #ifdef __cplusplus
 }
 #endif

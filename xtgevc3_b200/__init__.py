@@ -71,6 +71,9 @@ def lib():
         L.xtgevc3_trace_name.argtypes = [_I]
         L.xtgevc3_trace_name.restype = ct.c_char_p
         L.xtgevc3_launch_count.restype = ct.c_longlong
+        L.xtgevc3_dtgevc3_dev_noalloc.argtypes = [_P, _C, _C, _P, _I, _P, _I, _P, _I, _P, _P, _P, _P, _I, _P, _I,
+                                                  _I, _P, _P]
+        L.xtgevc3_dtgevc3_dev_noalloc.restype = _I
         _lib = L
     return _lib
 

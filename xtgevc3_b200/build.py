@@ -26,7 +26,7 @@ def sources():
 
 def deps():
     return sources() + sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + sorted(
-        glob.glob(os.path.join(HERE, "..", "include", "*.h")))
+        glob.glob(os.path.join(CSRC, "*.h"))) + sorted(glob.glob(os.path.join(HERE, "..", "include", "*.h")))
 
 
 def up_to_date() -> bool:

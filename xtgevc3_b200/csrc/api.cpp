@@ -3,6 +3,7 @@
 // src/ztgevc3.cpp:457-517), then host<->device staging and the device algorithm.
 #include "../../include/tgevc3.h"
 #include "../../include/xtgevc3.h"
+#include "args.h"
 #include "engine.cuh"
 
 #include <atomic>
@@ -24,43 +25,7 @@ xtg::Options make_opts(unsigned flags)
 
 int req_work(int n, int bs) { return 2 * n * (bs + 1) + 4 * (bs + 1) * (bs + 1) + 2 * (bs + 1); }
 
-// Upstream argument checks.  Returns true when the caller should stop (info set).
-// `count` is the number of eigenvector columns.
-template <class R>
-bool check_args(bool cplx, char howmny, const int *select, int n, const R *alphai, int mm, int *m, int *info,
-                int *count)
-{
-    const bool do_all = howmny == 'A' || howmny == 'B';
-    const bool do_sel = howmny == 'S';
-    if (!do_all && !do_sel) {
-        *info = -2;
-        return true;
-    }
-    if (n == 0) {
-        *info = 0;
-        if (m) *m = 0;
-        return true;
-    }
-    int num = 0;
-    for (int k = 0; k < n;) {
-        bool pair = !cplx && alphai[k] != R(0) && k + 1 < n;
-        bool sel = do_all;
-        if (do_sel && select) {
-            sel = select[k] != 0;
-            if (pair) sel = sel || select[k + 1] != 0;
-        }
-        if (do_sel && !select) sel = false;
-        if (sel) num += pair ? 2 : 1;
-        k += pair ? 2 : 1;
-    }
-    if (m) *m = num;
-    if (mm < num) {
-        *info = -16;
-        return true;
-    }
-    *count = num;
-    return false;
-}
+using xtg::check_args;
 
 // LWORK rule of the upstream driver (block size 32 shrunk until the workspace fits).
 template <class W>

@@ -132,18 +132,34 @@ int trace_get(int cat, long long *launches, double *ms, double *flops, double *b
 }
 long long launch_count() { return g_launches.load(); }
 
-// Stream-ordered scratch; the device's default pool keeps freed memory for reuse.
+// Scratch of one call.  Default: stream-ordered allocations from the device's pool (which
+// keeps freed memory for reuse).  Arena mode: 256-byte aligned slices of a caller-owned
+// device buffer, nothing allocated or freed; `used` can be rewound to reuse a region once
+// the work using it is ordered before the next user on the same stream.
 struct Scratch {
     cudaStream_t st;
     std::vector<void *> ptrs;
     cudaError_t err = cudaSuccess;
+    unsigned char *arena = nullptr;
+    size_t cap = 0, used = 0;
     explicit Scratch(cudaStream_t s) : st(s) {}
+    Scratch(cudaStream_t s, void *a, size_t c) : st(s), arena(static_cast<unsigned char *>(a)), cap(c) {}
     template <class T>
     T *get(size_t count)
     {
-        void *p = nullptr;
         if (count == 0) count = 1;
-        cudaError_t e = cudaMallocAsync(&p, count * sizeof(T), st);
+        const size_t bytes = count * sizeof(T);
+        if (arena) {
+            const size_t off = (used + 255) & ~size_t(255);
+            if (off + bytes > cap) {
+                err = cudaErrorMemoryAllocation;
+                return nullptr;
+            }
+            used = off + bytes;
+            return reinterpret_cast<T *>(arena + off);
+        }
+        void *p = nullptr;
+        cudaError_t e = cudaMallocAsync(&p, bytes, st);
         if (e != cudaSuccess) {
             err = e;
             return nullptr;
@@ -156,6 +172,27 @@ struct Scratch {
         for (void *p : ptrs) cudaFreeAsync(p, st);
     }
 };
+
+size_t arena_bytes_needed(int n, int m, bool right, bool left, bool back, bool normalize, bool cplx, size_t rsz)
+{
+    auto r256 = [](size_t b) { return (std::max<size_t>(b, 1) + 255) & ~size_t(255); };
+    const size_t esz = cplx ? 2 * rsz : rsz, ld = (size_t)round_up(n, 32);
+    const size_t nn = (size_t)n, mm = (size_t)m;
+    const size_t shared = r256(rsz * (cplx ? 4 : 3) * nn) + r256(rsz * 2 * nn) + r256(rsz * 2);
+    auto side = [&](bool lft) {
+        size_t b = 0;
+        if (lft) b += 2 * r256(esz * ld * nn);
+        b += r256(esz * ld * mm) + r256(esz * 4 * kBlock * mm) + r256(rsz * (cplx ? 6 : 4) * mm) +
+             r256(sizeof(int) * 5 * mm) + r256(mm);
+        if (back) b += r256(esz * ld * nn);
+        if (normalize && !cplx) b += r256(mm);
+        return b;
+    };
+    size_t s = 0;
+    if (right) s = side(false);
+    if (left) s = std::max(s, side(true));
+    return shared + s;
+}
 
 static std::once_flag g_pool_once[64];
 static void configure_device(int dev)
@@ -272,7 +309,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         }
     }
 
-    Scratch scr(st);
+    Scratch scr = opt.arena ? Scratch(st, opt.arena, opt.arena_bytes) : Scratch(st);
     Tracer tr;
     const double esz = sizeof(E), cfl = CPLX ? 4.0 : 1.0;
     // eigenvalue data on the device (for the coefficient kernels)
@@ -586,7 +623,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
     // The two sides are independent problems: with both requested they run concurrently,
     // the left one on a second stream (serially while tracing, so that kernel times are
     // not inflated by overlap).
-    if (want_r && want_l && !tr.on) {
+    if (want_r && want_l && !tr.on && !opt.arena) {
         struct Fork {
             cudaStream_t s = nullptr;
             cudaEvent_t fork = nullptr, join = nullptr;
@@ -615,7 +652,11 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             return 1;
         }
     } else {
+        const size_t mark = scr.used;
         if (want_r && run_side(false, st, scr)) return 1;
+        // arena: the right side's slices are reused; its kernels precede the left side's
+        // on the same stream
+        if (opt.arena) scr.used = mark;
         if (want_l && run_side(true, st, scr)) return 1;
     }
     XTG_CK(cudaStreamSynchronize(st));

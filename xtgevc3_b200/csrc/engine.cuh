@@ -9,7 +9,15 @@ namespace xtg {
 struct Options {
     int normalize = 0;  // scale every eigenvector to max |re| + |im| = 1 (LAPACK convention)
     int simt = 0;       // force the SIMT GEMM kernels instead of the tensor-core kernel
+    // When set, all device scratch of the call is carved from this buffer (nothing is
+    // allocated) and the two sides run one after the other on the caller's stream.
+    void *arena = nullptr;
+    size_t arena_bytes = 0;
 };
+
+// Device scratch (bytes) a call needs in arena mode: shared eigenvalue data plus the larger
+// side (the sides reuse one region).  Counts each slice rounded up to 256 bytes.
+size_t arena_bytes_needed(int n, int m, bool right, bool left, bool back, bool normalize, bool cplx, size_t real_size);
 
 // One call on device-resident matrices.
 //   S, P, VL, VR : device pointers, leading dimensions in elements of the scalar type

@@ -1,0 +1,100 @@
+// Allocation-free device entry point: xtgevc3_dtgevc3_dev_noalloc.
+//
+// Who needs it: code that must not call cudaMalloc (or any allocating routine) at the
+// point where it computes eigenvectors -- for example an application whose framework
+// has already reserved the device memory for its own pool, a real-time loop where a
+// device allocation (which may synchronise the device) is not acceptable, or a library
+// invoked from inside another allocator's bookkeeping.  The regular device entry point
+// takes its scratch from the CUDA stream-ordered pool; this one takes it from a fixed
+// block of device memory that is part of the library image.
+//
+// The block: g_noalloc_scratch below, kNoAllocBytes = 8 MiB, declared at file scope.
+// Every GPU on which the library is loaded holds these 8 MiB until the process exits.
+// That bounds the problem size: a call is accepted when the scratch it needs fits
+// (arena_bytes_needed); for SIDE='B', HOWMNY='B' that is n <= 448.  Larger calls are
+// rejected before any device work with return code 2 and a message in
+// xtgevc3_last_error().
+//
+// Host code cannot use the symbol's name as a device address (it names a host-side
+// shadow), so the address is looked up with cudaGetSymbolAddress once per device, with
+// that device current, on the first call made on it; make that first call before any
+// stream capture begins.
+//
+// All calls share the one block, and it keeps whatever the previous call left in it: the
+// computation zeroes what must start at zero itself.  Two calls whose work overlaps on the
+// GPU (different streams without ordering, several host threads) race on the block; the
+// caller must order them, e.g. issue them on one stream.
+#include "../../include/xtgevc3.h"
+#include "args.h"
+#include "engine.cuh"
+
+#include <cstdio>
+#include <mutex>
+#include <string>
+
+namespace {
+
+constexpr size_t kNoAllocBytes = size_t(8) << 20;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kMaxDevices = 64;
+std::once_flag g_once[kMaxDevices];
+void *g_addr[kMaxDevices];
+cudaError_t g_addr_err[kMaxDevices];
+
+}  // namespace
+
+extern "C" int xtgevc3_dtgevc3_dev_noalloc(void *stream, char side, char howmny, const int *select, int n,
+                                           const double *S, int lds, const double *P, int ldp, const double *alphar,
+                                           const double *alphai, const double *beta, double *VL, int ldvl,
+                                           double *VR, int ldvr, int mm, int *m, int *info)
+{
+    int dummy = 0;
+    if (!info) info = &dummy;
+    int count = 0;
+    if (xtg::check_args<double>(false, howmny, select, n, alphai, mm, m, info, &count)) return 0;
+    *info = 0;
+    xtg::set_last_error("");
+    if (count == 0) return 0;
+
+    const bool right = (side == 'R' || side == 'B') && VR;
+    const bool left = (side == 'L' || side == 'B') && VL;
+    if (!right && !left) return 0;
+    const size_t need = xtg::arena_bytes_needed(n, count, right, left, howmny == 'B', false, false, sizeof(double));
+    if (need > kNoAllocBytes) {
+        char msg[256];
+        std::snprintf(msg, sizeof msg,
+                      "xtgevc3_dtgevc3_dev_noalloc: n=%d with %d eigenvector columns needs %zu bytes of scratch; "
+                      "the static scratch holds %zu bytes (SIDE='B', HOWMNY='B': n <= 448)",
+                      n, count, need, kNoAllocBytes);
+        xtg::set_last_error(msg);
+        return 2;
+    }
+
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        xtg::set_last_error(std::string("xtgevc3_dtgevc3_dev_noalloc: cudaGetDevice: ") + cudaGetErrorString(e));
+        *info = 1;
+        return 1;
+    }
+    std::call_once(g_once[dev], [dev]() {
+        g_addr_err[dev] = cudaGetSymbolAddress(&g_addr[dev], g_noalloc_scratch);
+    });
+    if (g_addr_err[dev] != cudaSuccess || !g_addr[dev]) {
+        xtg::set_last_error(std::string("xtgevc3_dtgevc3_dev_noalloc: cudaGetSymbolAddress: ") +
+                            cudaGetErrorString(g_addr_err[dev]));
+        *info = 1;
+        return 1;
+    }
+
+    xtg::Options opt;
+    opt.arena = g_addr[dev];
+    opt.arena_bytes = kNoAllocBytes;
+    const int rc = xtg::solve_device<double, false>(side, howmny, select, n, S, lds, P, ldp, alphar, alphai, beta,
+                                                    left ? VL : nullptr, ldvl, right ? VR : nullptr, ldvr, count, opt,
+                                                    static_cast<cudaStream_t>(stream));
+    if (rc) *info = 1;
+    return rc;
+}
