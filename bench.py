@@ -48,6 +48,10 @@ def parse():
     ap.add_argument("--seed", type=int, default=8192)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-window", type=int, default=1024, help="eigenvalues per side in the CPU sample")
+    ap.add_argument("--form", default="both", choices=["plain", "split", "both"],
+                    help="plain FP64, split precision (BF16 slices), or both (the faster one meeting the "
+                         "residual bound is the headline)")
+    ap.add_argument("--slices", type=int, default=6, help="BF16 slices of the split form")
     return ap.parse_args()
 
 
@@ -293,6 +297,53 @@ def load_traffic():
         return None
 
 
+
+
+def measure_form(name, flags, args, X, torch, data, dist, local, world):
+    """Time K steps of one form (device-resident inputs), check the residual of the result,
+    then trace K more steps for the per-kernel breakdown."""
+    S, P, ar, ai, be, Q, Z, VL, VR = data
+    n = S.shape[0]
+
+    def step():
+        VL.copy_(Q)
+        VR.copy_(Z)
+        X.tgevc3_dev("B", "B", S, P, ar, be, alphai=ai, VL=VL, VR=VR, flags=flags)
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = X.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    launches = X.launch_count() - l0
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    resid = residual_max(torch, S, P, ar, ai, be, Q, Z, VL, VR)
+    X.trace_reset()
+    X.trace_enable(True)
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize()
+    X.trace_enable(False)
+    kernels = {k: dict(v, ms_per_step=v["ms"] / args.steps) for k, v in X.trace().items() if v["launches"]}
+    return {"name": name, "flags": flags, "ms": ms, "value": world * 2 * n / (ms * 1e-3), "resid": resid,
+            "clocks": clk, "launches": launches, "kernels": kernels}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -319,75 +370,56 @@ def main():
     Z = orthogonal(n, 2 * args.seed + 2 + 7 * rank, torch)
     VL = torch.empty_like(Q)
     VR = torch.empty_like(Z)
+    data = (S, P, ar, ai, be, Q, Z, VL, VR)
     peak_fp64 = dgemm_peak(torch)
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    peak_bf16 = peaks.get("bf16_tflops", 1590.0)
+    peak_hbm = peaks.get("hbm_gbs", 6650.0)
 
-    def step():
-        VL.copy_(Q)
-        VR.copy_(Z)
-        X.tgevc3_dev("B", "B", S, P, ar, be, alphai=ai, VL=VL, VR=VR)
+    s = max(1, min(6, args.slices))
+    forms = {"plain": 0, "split": X.SPLIT | X.slices(s)}
+    names = ["plain", "split"] if args.form == "both" else [args.form]
+    res = {nm: measure_form(nm, forms[nm], args, X, torch, data, dist, local, world) for nm in names}
+    ok = [nm for nm in names if res[nm]["resid"] <= 1e-12]
+    head = min(ok or names, key=lambda nm: res[nm]["ms"])
+    h = res[head]
+    kernels = h["kernels"]
 
-    for _ in range(max(args.warmup, 1)):
-        step()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
-    l0 = X.launch_count()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.steps):
-        step()
-    e1.record()
-    torch.cuda.synchronize()
-    launches = X.launch_count() - l0
-    clk = clocks.stop()
-    ms = e0.elapsed_time(e1) / args.steps
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        if dist:
-            dist.barrier()
-    value = world * 2 * n / (ms * 1e-3)
-
-    # accuracy of the timed result (outside the timed region)
-    resid = residual_max(torch, S, P, ar, ai, be, Q, Z, VL, VR)
-
-    # kernel trace (separate pass, same steps)
-    X.trace_reset()
-    X.trace_enable(True)
-    for _ in range(args.steps):
-        step()
-    torch.cuda.synchronize()
-    X.trace_enable(False)
-    tr = X.trace()
-    kernels = {k: dict(v, ms_per_step=v["ms"] / args.steps) for k, v in tr.items() if v["launches"]}
+    # roofline of the dominant kernel class of the headline form
     dom = max(kernels, key=lambda k: kernels[k]["ms"])
     kd = kernels[dom]
-    if kd["flops"] > 0:
+    pairs = s * (s + 1) // 2
+    if kd["flops"] > 0 and head == "split" and dom.startswith("gemm"):
+        # BF16 slice products actually executed: pairs x the FP64-equivalent flops
+        achieved = pairs * kd["flops"] / (kd["ms"] * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak_bf16, "unit": "TFLOP/s",
+                "frac": achieved / peak_bf16, "kernel": dom,
+                "fp64_equivalent_tflops": kd["flops"] / (kd["ms"] * 1e-3) / 1e12,
+                "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst), BF16 slice products counted"}
+    elif kd["flops"] > 0:
         achieved = kd["flops"] / (kd["ms"] * 1e-3) / 1e12
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak_fp64, "unit": "TFLOP/s",
                 "frac": achieved / peak_fp64, "kernel": dom,
                 "peak_source": "cuBLAS DGEMM 8192^3 burst measured in this run (FP64; MEASURED_PEAKS.json "
                                "has no FP64 figure)"}
     else:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-            os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0}
         achieved = kd["bytes"] / (kd["ms"] * 1e-3) / 1e9
-        roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"], "kernel": dom, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak_hbm, "unit": "GB/s",
+                "frac": achieved / peak_hbm, "kernel": dom, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
     tinfo = load_traffic()
     traffic = None
-    if tinfo and dom in tinfo.get("bytes_per_flop", {}) and kd["flops"] > 0:
-        traffic = tinfo["bytes_per_flop"][dom] * kd["flops"] / kd["launches"]
+    key = f"{head}:{dom}"
+    if tinfo and key in tinfo.get("bytes_per_flop", {}) and kd["flops"] > 0:
+        traffic = tinfo["bytes_per_flop"][key] * kd["flops"] / kd["launches"]
         roof["traffic_note"] = tinfo.get("note", "")
     roof["traffic"] = traffic
     roof["algorithmic_per_launch"] = (kd["flops"] if kd["flops"] > 0 else kd["bytes"]) / kd["launches"]
     for k in kernels.values():
         if k["flops"] > 0:
-            k["tflops"] = k["flops"] / (k["ms"] * 1e-3) / 1e12
+            k["tflops_fp64_equivalent"] = k["flops"] / (k["ms"] * 1e-3) / 1e12
         k["gbs"] = k["bytes"] / (k["ms"] * 1e-3) / 1e9 if k["ms"] > 0 else None
 
     # end-to-end through the host-pointer C ABI (pinned host buffers, copies timed)
@@ -400,18 +432,22 @@ def main():
     hP[...] = P_h
     hQ[...] = Q.t().cpu().numpy().T
     hZ[...] = Z.t().cpu().numpy().T
+    X.set_flags(h["flags"])
     e2e_t = []
-    for it in range(args.warmup + args.steps):
-        np.copyto(hVL, hQ)
-        np.copyto(hVR, hZ)
-        if dist:
-            dist.barrier()
-        t0 = time.perf_counter()
-        _, _, m_, info_ = X.tgevc3("B", "B", hS, hP, ar, be, alphai=ai, VL=hVL, VR=hVR)
-        t1 = time.perf_counter()
-        assert info_ == 0
-        if it >= args.warmup:
-            e2e_t.append(t1 - t0)
+    try:
+        for it in range(args.warmup + args.steps):
+            np.copyto(hVL, hQ)
+            np.copyto(hVR, hZ)
+            if dist:
+                dist.barrier()
+            t0 = time.perf_counter()
+            _, _, m_, info_ = X.tgevc3("B", "B", hS, hP, ar, be, alphai=ai, VL=hVL, VR=hVR)
+            t1 = time.perf_counter()
+            assert info_ == 0
+            if it >= args.warmup:
+                e2e_t.append(t1 - t0)
+    finally:
+        X.set_flags(0)
     e2e_s = float(np.mean(e2e_t))
     if dist:
         t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
@@ -419,7 +455,7 @@ def main():
         e2e_s = float(t.item())
     e2e = {"value": world * 2 * n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 4 * n * n * 8,
            "d2h_bytes_per_step": 2 * n * n * 8, "ms_per_step": 1e3 * e2e_s,
-           "path": "xtgevc3_dtgevc3 (host pointers, pinned), H2D/D2H inside the call"}
+           "path": f"xtgevc3_dtgevc3 (host pointers, pinned), {head} form, H2D/D2H inside the call"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -432,16 +468,24 @@ def main():
                           f"overstates the CPU rate of HOWMNY='B'")}
 
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        form_desc = {"plain": "plain FP64 (DMMA)", "split": f"split precision, {s} BF16 slices (tcgen05)"}
+        forms_out = {nm: {"value": r["value"], "ms_per_step": r["ms"], "resid_max": r["resid"],
+                          "meets_resid_bound": r["resid"] <= 1e-12,
+                          "kernels_ms_per_step": {k: v["ms_per_step"] for k, v in r["kernels"].items()}}
+                     for nm, r in res.items()}
+        if "plain" in res:
+            for nm in forms_out:
+                forms_out[nm]["speedup_vs_plain"] = res["plain"]["ms"] / res[nm]["ms"]
+        line = {"metric": METRIC, "value": h["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": h["ms"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": DATA,
-                "config": {"workload": f"dtgevc3 SIDE=B HOWMNY=B n={n}, plain FP64 form", "n": n, "side": "B",
-                           "howmny": "B", "form": "plain-fp64", "pencils_per_gpu": 1,
+                "config": {"workload": f"dtgevc3 SIDE=B HOWMNY=B n={n}", "n": n, "side": "B", "howmny": "B",
+                           "form": form_desc[head], "pencils_per_gpu": 1,
                            "l2": "inputs larger than L2 (S,P,Q,Z = 2 GiB); no flush",
                            "parallelism": f"independent pencil per GPU x{world}",
-                           "resid_max": resid, "resid_bound": 1e-12},
-                "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roof, "kernels": kernels,
-                "cpu_baseline": cpu}
+                           "resid_max": h["resid"], "resid_bound": 1e-12},
+                "forms": forms_out, "clocks": h["clocks"], "e2e": e2e, "gpu_launches": h["launches"],
+                "roofline": roof, "kernels": kernels, "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -39,6 +39,13 @@ extern "C" {
 /* Option flags. */
 #define XTGEVC3_NORMALIZE 1u /* scale every eigenvector (a real pair jointly) to max_i |re|+|im| = 1 */
 #define XTGEVC3_SIMT 2u      /* use the SIMT GEMM kernels instead of the FP64 tensor-core kernel */
+/* Split-precision form (dtgevc3 only): the trailing updates and the back-transform run as
+ * products of BF16 slices of the FP64 operands on the BF16 tensor cores, with exact FP32
+ * accumulation per 128-deep K chunk and FP64 summation; the diagonal solves, scale factors
+ * and 2x2 solves stay FP64.  XTGEVC3_SLICES(s) picks the slice count s in [1, 6] (default 6,
+ * ~48 bits per operand). */
+#define XTGEVC3_SPLIT 4u
+#define XTGEVC3_SLICES(s) ((unsigned)(s) << 8)
 
 /* Process-wide flags used by the drop-in entry points below (default 0). */
 void xtgevc3_set_flags(unsigned flags);

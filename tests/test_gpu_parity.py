@@ -207,3 +207,33 @@ def test_device_api_matches_host_api(cuda_ok):
     np.testing.assert_array_equal(VL.t().cpu().numpy().T, VLh[:, :m])
     np.testing.assert_array_equal(VR.t().cpu().numpy().T, VRh[:, :m])
     assert n == m
+
+
+SPLIT_CASES = [
+    # (kind, n, seed, side, howmny, slices, elementwise tolerance vs the FP64 oracle)
+    ("gges", 257, 71, "B", "B", 6, 1e-10),
+    ("gges", 300, 72, "B", "A", 6, 1e-10),
+    ("schur", 700, 73, "B", "B", 6, 1e-6),
+]
+
+
+@pytest.mark.parametrize("case", SPLIT_CASES, ids=lambda c: f"{c[0]}-{c[1]}-{c[3]}{c[4]}-s{c[5]}")
+def test_split_precision_form(cuda_ok, case):
+    """XTGEVC3_SPLIT: updates and back-transform as BF16-slice products on the tensor cores
+    (FP32 accumulation exact per 128-deep chunk, FP64 summation); solves stay FP64.  With 6
+    slices (~48 bits per operand) the result must match the FP64 oracle elementwise within
+    the stated tolerance (looser on the ill-conditioned stand-in pencil) and its residual
+    must meet the DGET52 bound used for the plain form."""
+    kind, n, seed, side, howmny, s, tol = case
+    p = _pencil(kind, n, seed, np.float64)
+    d = dict(side=side, howmny=howmny, S=p["S"], P=p["P"], alpha=p["alpha"], beta=p["beta"], alphai=p["alphai"],
+             VL_in=p["Q"], VR_in=p["Z"], name=kind)
+    ref = oracle.tgevc3(side, howmny, d["S"], d["P"], d["alpha"], d["beta"], alphai=d["alphai"],
+                        VL=p["Q"].copy(order="F"), VR=p["Z"].copy(order="F"))
+    X.set_flags(X.SPLIT | X.slices(s))
+    try:
+        VL, VR, m, info = run_gpu(d)
+    finally:
+        X.set_flags(0)
+    assert (m, info) == (ref[2], ref[3])
+    compare(d, VL, VR, m, ref[0], ref[1], tol, check_resid=(howmny == "A"))

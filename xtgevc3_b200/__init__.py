@@ -27,6 +27,12 @@ from . import build as _build
 
 NORMALIZE = 1
 SIMT = 2
+SPLIT = 4
+
+
+def slices(s: int) -> int:
+    """Flag bits selecting s BF16 slices for the SPLIT form (1..6)."""
+    return int(s) << 8
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _lib = None

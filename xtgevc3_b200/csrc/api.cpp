@@ -20,6 +20,10 @@ xtg::Options make_opts(unsigned flags)
     xtg::Options o;
     o.normalize = (flags & XTGEVC3_NORMALIZE) ? 1 : 0;
     o.simt = (flags & XTGEVC3_SIMT) ? 1 : 0;
+    if (flags & XTGEVC3_SPLIT) {
+        const int s = (int)((flags >> 8) & 15u);
+        o.split = s > 0 ? s : 6;
+    }
     return o;
 }
 

@@ -11,7 +11,7 @@ namespace xtg {
 template <class R>
 struct alignas(2 * sizeof(R)) cplx {
     R x, y;
-    __host__ __device__ cplx() = default;
+    cplx() = default;
     __host__ __device__ constexpr cplx(R r, R i = R(0)) : x(r), y(i) {}
 };
 

@@ -21,6 +21,9 @@
 #include "kernels_diag.cuh"
 #include "kernels_gemm.cuh"
 #include "kernels_misc.cuh"
+#include "kernels_split.cuh"
+
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <atomic>
@@ -214,6 +217,8 @@ static void configure_device(int dev)
                              2 * kBlock * kSmLd * (int)sizeof(cplx<float>));
         cudaFuncSetAttribute(gemm_dmma<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::SMEM_BYTES);
         cudaFuncSetAttribute(gemm_dmma<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::SMEM_BYTES);
+        cudaFuncSetAttribute(split::gemm_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             split::SMEM_BYTES);
     });
 }
 
@@ -231,6 +236,81 @@ struct ColList {
     std::vector<int> colk, src, kext, outcol;
     std::vector<uint8_t> kind;
 };
+
+// ---- split-precision GEMM launcher ---------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, []() {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// 2-D BF16 tensor map over a row-major [rows][cols] buffer, 64-byte swizzled boxes of
+// 32 columns (64 B, the swizzle span) by box_rows rows.
+static bool bf16_tensor_map(CUtensorMap *m, const void *base, int cols, int rows, int box_rows)
+{
+    auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+    cuuint32_t box[2] = {(cuuint32_t)split::BK, (cuuint32_t)box_rows};
+    cuuint32_t es[2] = {1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Reusable slice buffers of one side (grown on demand from the call's scratch).
+struct SplitBufs {
+    __nv_bfloat16 *A = nullptr, *B = nullptr;
+    int *ea = nullptr, *eb = nullptr;
+    size_t acap = 0, bcap = 0, ecap_a = 0, ecap_b = 0;
+};
+
+// C (+)= A B for a GemmArgs<double> launch, through BF16 slices and tcgen05 (see
+// kernels_split.cuh).  Returns a CUDA error code (cudaSuccess on success).
+static cudaError_t launch_split(const GemmArgs<double> &g, int s, SplitBufs &sb, Scratch &scr, int *d_err,
+                                cudaStream_t st)
+{
+    using namespace split;
+    const int Kp = round_up(g.K, BK), Mp = round_up(g.M, BM), Np = round_up(g.N, BN);
+    const size_t an = (size_t)s * Mp * Kp, bn = (size_t)s * Np * Kp;
+    if (an > sb.acap) { sb.A = scr.get<__nv_bfloat16>(an); sb.acap = an; }
+    if (bn > sb.bcap) { sb.B = scr.get<__nv_bfloat16>(bn); sb.bcap = bn; }
+    if ((size_t)Mp > sb.ecap_a) { sb.ea = scr.get<int>(Mp); sb.ecap_a = Mp; }
+    if ((size_t)Np > sb.ecap_b) { sb.eb = scr.get<int>(Np); sb.ecap_b = Np; }
+    if (scr.err) return scr.err;
+    slice_rows_kernel<<<Mp / 32, 256, 0, st>>>(g, Kp, Mp, s, sb.A, sb.ea);
+    slice_cols_kernel<<<Np / 8, 256, 0, st>>>(g, Kp, Np, s, sb.B, sb.eb);
+    CUtensorMap tmA, tmB;
+    if (!bf16_tensor_map(&tmA, sb.A, Kp, s * Mp, BM) || !bf16_tensor_map(&tmB, sb.B, Kp, s * Np, BN))
+        return cudaErrorInvalidValue;
+    Params p;
+    p.M = g.M;
+    p.N = g.N;
+    p.Kp = Kp;
+    p.s = s;
+    p.Mp = Mp;
+    p.Np = Np;
+    p.mlo = g.mlo;
+    p.accumulate = g.accumulate;
+    p.ea = sb.ea;
+    p.eb = sb.eb;
+    p.kext = g.kext;
+    p.C = g.C;
+    p.ldc = g.ldc;
+    p.ccol = g.ccol;
+    p.err = d_err;
+    gemm_split_kernel<<<dim3(Mp / BM, Np / BN), THREADS, SMEM_BYTES, st>>>(tmA, tmB, p);
+    return cudaGetLastError();
+}
 
 template <class E>
 static void launch_gemm(const GemmArgs<E> &g, bool simt, cudaStream_t st)
@@ -317,7 +397,13 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
     R *d_eig = scr.get<R>(CPLX ? 4 * (size_t)n : 3 * (size_t)n);
     R *d_sums = scr.get<R>(2 * (size_t)n);
     R *d_norms = scr.get<R>(2);
+    // split-precision GEMMs: real double only; their bounded waits report through d_err
+    const int nsplit = (!CPLX && std::is_same<R, double>::value && opt.split > 0)
+                           ? std::min(opt.split, (int)split::MAXS)
+                           : 0;
+    int *d_err = nsplit ? scr.get<int>(1) : nullptr;
     if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
+    if (d_err) XTG_CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
     if (CPLX) {
         XTG_CK(cudaMemcpyAsync(d_eig, alpha_, 2 * n * sizeof(R), cudaMemcpyHostToDevice, st));
         XTG_CK(cudaMemcpyAsync(d_eig + 2 * n, beta_, 2 * n * sizeof(R), cudaMemcpyHostToDevice, st));
@@ -339,6 +425,21 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
 
     // One side on stream `st` with scratch from `scr` (both shadow the call's own).
     auto run_side = [&](bool left, cudaStream_t st, Scratch &scr) -> int {
+        SplitBufs sbuf;
+        cudaError_t split_err = cudaSuccess;
+        // C (+)= A B of one update or back-transform launch, FP64 DMMA/SIMT or BF16 slices
+        auto gemm = [&](const GemmArgs<E> &g) {
+            if constexpr (std::is_same<E, double>::value) {
+                // launches with few output rows (the update of the upper block of a pair) do
+                // too little work per tile to amortise slicing and the tensor-core pipeline
+                if (nsplit && g.M - g.mlo >= 512) {
+                    cudaError_t e = launch_split(g, nsplit, sbuf, scr, d_err, st);
+                    if (e != cudaSuccess) split_err = e;
+                    return;
+                }
+            }
+            launch_gemm<E>(g, opt.simt != 0, st);
+        };
         // ---- column list in problem orientation ---------------------------------------
         ColList L;
         L.m = m_total;
@@ -474,7 +575,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             const double rows = M - mlo;
             const double uf = 2.0 * rows * g.N * kflops * cfl;
             const double ub = (2.0 * rows * g.N + rows * kflops + kflops * g.N) * esz;
-            tr.run(kTUpdate, uf, ub, st, [&] { launch_gemm<E>(g, opt.simt != 0, st); });
+            tr.run(kTUpdate, uf, ub, st, [&] { gemm(g); });
         };
         auto diag_solve = [&](int r0, int r1, int ys_off, int yhalf, int zl_off, int zl_len) {
             const int jnb = r1 - r0;
@@ -592,7 +693,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             for (int c = 0; c < m; c++) bk += L.kext[c];
             bf = 2.0 * n * bk * cfl;
             const double bb = ((double)n * L.kext[m - 1] + bk + (double)n * m) * esz;
-            tr.run(kTBack, bf, bb, st, [&] { launch_gemm<E>(g, opt.simt != 0, st); });
+            tr.run(kTBack, bf, bb, st, [&] { gemm(g); });
         } else {
             dim3 g(std::max(1, std::min((n + 255) / 256, 64)), m);
             tr.run(kTWriteback, 0, 2.0 * n * m * esz, st, [&] {
@@ -616,6 +717,10 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
                        [&] { normalize_real_kernel<R><<<m, 256, 0, st>>>(V, ldv, n, d_ok, m); });
             }
             XTG_CK(cudaGetLastError());
+        }
+        if (split_err != cudaSuccess) {
+            set_last_error(std::string("split-precision GEMM launch: ") + cudaGetErrorString(split_err));
+            return 1;
         }
         return 0;
     };
@@ -661,6 +766,14 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
     }
     XTG_CK(cudaStreamSynchronize(st));
     tr.flush();
+    if (d_err) {
+        int h_err = 0;
+        XTG_CK(cudaMemcpy(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (h_err) {
+            set_last_error("split-precision GEMM: a bounded wait in the tensor-core pipeline expired");
+            return 1;
+        }
+    }
     return 0;
 }
 

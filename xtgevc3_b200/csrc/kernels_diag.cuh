@@ -29,9 +29,9 @@
 // Scaling a column means scaling every stored row of it: the accumulated rows above the
 // block, the rows solved in earlier blocks and the current block.
 //
-// Output: X[I, c] (solution), and the stacked update operand
-//   Y[0:bpad, c] = -ac * x,  Y[bpad:2*bpad, c] = b * x   (zero padded)
-// consumed by the update GEMM  X[0:r0, c] += S[0:r0, I] Y[0:bpad] + P[0:r0, I] Y[bpad:].
+// Output: X[I, c] (solution), and this block's rows of the stacked update operand
+//   Y[ys_off + i, c] = -ac * x_i,  Y[ys_off + yhalf + i, c] = b * x_i   (zero padded)
+// consumed by the update GEMMs  X[rows above, c] += S[rows above, I] (-ac x) + P[..] (b x).
 #pragma once
 #include "common.cuh"
 
@@ -261,9 +261,9 @@ __device__ __forceinline__ void pair_mask(const R *Ss, int jnb, uint64_t *out)
 template <class R>
 __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(16) unsigned char smem_diag[];
     __shared__ uint64_t s_sec;
-    R *Ss = reinterpret_cast<R *>(smem_raw);
+    R *Ss = reinterpret_cast<R *>(smem_diag);
     R *Ps = Ss + kSmLd * kBlock;
     const int jnb = a.r1 - a.r0;
     load_block(a.S, a.lds, a.P, a.ldp, a.r0, jnb, 1, Ss, Ps);
@@ -419,8 +419,8 @@ template <class R>
 __global__ void __launch_bounds__(256) diag_solve_cplx(DiagArgs<R> a)
 {
     using C = cplx<R>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    C *Ss = reinterpret_cast<C *>(smem_raw);
+    extern __shared__ __align__(16) unsigned char smem_diag[];
+    C *Ss = reinterpret_cast<C *>(smem_diag);
     C *Ps = Ss + kSmLd * kBlock;
     const int jnb = a.r1 - a.r0;
     load_block(reinterpret_cast<const C *>(a.S), a.lds, reinterpret_cast<const C *>(a.P), a.ldp, a.r0, jnb, 0, Ss,

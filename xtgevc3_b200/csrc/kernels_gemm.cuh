@@ -173,8 +173,8 @@ template <int ACC>
 __global__ void __launch_bounds__(256) gemm_dmma(GemmArgs<double> g)
 {
     using namespace dmma;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    double *As = reinterpret_cast<double *>(smem_raw);
+    extern __shared__ __align__(16) unsigned char smem_gemm[];
+    double *As = reinterpret_cast<double *>(smem_gemm);
     double *Bs = As + STAGES * A_STAGE;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = warp & 3, wn = warp >> 2;
