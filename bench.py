@@ -52,6 +52,9 @@ def parse():
                     help="plain FP64, split precision (BF16 slices), or both (the faster one meeting the "
                          "residual bound is the headline)")
     ap.add_argument("--slices", type=int, default=6, help="BF16 slices of the split form")
+    ap.add_argument("--batch-count", type=int, default=2048,
+                    help="pencils of the batched workload (0 skips it)")
+    ap.add_argument("--batch-seed", type=int, default=2048)
     return ap.parse_args()
 
 
@@ -344,6 +347,154 @@ def measure_form(name, flags, args, X, torch, data, dist, local, world):
             "clocks": clk, "launches": launches, "kernels": kernels}
 
 
+def batched_inputs(count, seed, torch):
+    """The batched workload on the device: `count` pencils of orders n ~ U{16..512}
+    (seeded), each in generalized Schur form with the block statistics of the single-pencil
+    workload (strictly upper parts N(0,1) drawn on the device), Householder Q and Z; the
+    FP32 batch is the same pencils rounded to FP32.  Returns (sizes, batches) with batches
+    = {"d": [...], "s": [...]}, each pencil a dict of device tensors plus host eigenvalues."""
+    from xtgevc3_b200 import pencils as gen
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(16, 513, size=count).astype(np.int64)
+    offs = np.concatenate([[0], np.cumsum(sizes ** 2)])
+    tot = int(offs[-1])
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    out = {}
+    for prec, tdt in (("d", torch.float64), ("s", torch.float32)):
+        out[prec] = {k: torch.empty(tot, device="cuda", dtype=tdt) for k in ("S", "P", "Q", "Z", "VL", "VR")}
+    bd, bs = out["d"], out["s"]
+    plist = {"d": [], "s": []}
+    for i, n in enumerate(sizes):
+        n = int(n)
+        o = int(offs[i])
+
+        def view(buf):
+            return buf[o:o + n * n].view(n, n).t()  # column-major n x n
+
+        S, P, Q, Z = view(bd["S"]), view(bd["P"]), view(bd["Q"]), view(bd["Z"])
+        S.copy_(torch.triu(torch.randn(n, n, generator=g, device="cuda", dtype=torch.float64), 1))
+        P.copy_(torch.triu(torch.randn(n, n, generator=g, device="cuda", dtype=torch.float64), 1))
+        k1, s1, p1, k2, s2, p2, ar, ai, be = gen.schur_blocks(n, rng)
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+        k1t, k2t = t(k1), t(k2)
+        S[k1t, k1t] = t(s1)
+        P[k1t, k1t] = t(p1)
+        if k2.size:
+            S[k2t, k2t], S[k2t, k2t + 1] = t(s2[:, 0]), t(s2[:, 1])
+            S[k2t + 1, k2t], S[k2t + 1, k2t + 1] = t(s2[:, 2]), t(s2[:, 3])
+            P[k2t, k2t], P[k2t + 1, k2t + 1], P[k2t, k2t + 1] = t(p2[:, 0]), t(p2[:, 1]), 0.0
+        for M in (Q, Z):
+            v = torch.randn(n, 1, generator=g, device="cuda", dtype=torch.float64)
+            M.copy_(torch.eye(n, device="cuda", dtype=torch.float64) - (2.0 / (v.t() @ v)) * (v @ v.t()))
+        for prec, b in (("d", bd), ("s", bs)):
+            dt = np.float64 if prec == "d" else np.float32
+            ph = dict(n=n, ar=ar.astype(dt), ai=ai.astype(dt), be=be.astype(dt))
+            pd = dict(S=view(b["S"]), P=view(b["P"]), Q=view(b["Q"]), Z=view(b["Z"]), VL=view(b["VL"]),
+                      VR=view(b["VR"]))
+            for key in ("alphar", "alphai", "beta"):
+                pd[key] = torch.from_numpy(ph[{"alphar": "ar", "alphai": "ai", "beta": "be"}[key]]).cuda()
+            pd["host"] = ph
+            plist[prec].append(pd)
+    for k in ("S", "P", "Q", "Z"):
+        bs[k].copy_(bd[k])
+    return sizes, plist, out
+
+
+def measure_batched(args, X, torch, dist, world):
+    """The batched form (one persistent kernel in a CUDA graph per precision, tile
+    configuration from the project's tuner) against a loop of per-pencil plain launches
+    (xtgevc3_{d,s}tgevc3_dev) over the same pencils; both on device-resident inputs."""
+    rank = int(os.environ.get("RANK", "0"))
+    sizes, plist, bufs = batched_inputs(args.batch_count, args.batch_seed + 7919 * rank, torch)
+    count = len(sizes)
+    flops = float(np.sum(10.0 / 3.0 * sizes.astype(np.float64) ** 3))
+    res = {}
+    for prec in ("d", "s"):
+        pens = [{k: v for k, v in p.items() if k != "host"} for p in plist[prec]]
+        cfg, tune_ms = X.batched_tune("B", "B", pens, reps=2)
+        plan = X.Batch("B", "B", pens)
+        for _ in range(max(args.warmup, 1)):
+            plan.run()
+        plan.wait()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        l0 = X.launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            plan.run()
+        e1.record()
+        plan.wait()
+        ms = e0.elapsed_time(e1) / args.steps
+        launches = X.launch_count() - l0
+        if dist:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        info = plan.info()
+        # loop of plain per-pencil launches (in place, so VL/VR start as Q/Z each call)
+        VLl = torch.empty_like(bufs[prec]["VL"])
+        VRl = torch.empty_like(bufs[prec]["VR"])
+        offs = np.concatenate([[0], np.cumsum(sizes ** 2)])
+
+        def loop(idx):
+            for i in idx:
+                p, h = plist[prec][i], plist[prec][i]["host"]
+                n, o = h["n"], int(offs[i])
+                vl = VLl[o:o + n * n].view(n, n).t()
+                vr = VRl[o:o + n * n].view(n, n).t()
+                vl.copy_(p["Q"])
+                vr.copy_(p["Z"])
+                X.tgevc3_dev("B", "B", p["S"], p["P"], h["ar"], h["be"], alphai=h["ai"], VL=vl, VR=vr)
+
+        loop(range(min(16, count)))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        loop(range(count))
+        f1.record()
+        torch.cuda.synchronize()
+        loop_ms = f0.elapsed_time(f1)
+        loop_wall = time.perf_counter() - t0
+        # agreement of the two on every pencil (elementwise, relative to the column max)
+        worst = 0.0
+        for V, W in ((bufs[prec]["VL"], VLl), (bufs[prec]["VR"], VRl)):
+            for i in range(count):
+                n, o = int(sizes[i]), int(offs[i])
+                a, b = V[o:o + n * n].view(n, n), W[o:o + n * n].view(n, n)  # rows = columns of V
+                den = b.abs().amax(1).clamp_min(1e-300)
+                worst = max(worst, float(((a - b).abs().amax(1) / den).max()))
+        big = np.argsort(-sizes)[:2]
+        resid = []
+        for i in big:
+            p, h = plist[prec][i], plist[prec][i]["host"]
+            S64, P64, Q64, Z64, VL64, VR64 = (p[k].double() for k in ("S", "P", "Q", "Z", "VL", "VR"))
+            resid.append(residual_max(torch, S64, P64, h["ar"].astype(np.float64), h["ai"].astype(np.float64),
+                                      h["be"].astype(np.float64), Q64, Z64, VL64, VR64))
+        res[prec] = {"ms": ms, "pencils_per_s": count / (ms * 1e-3), "tflops": flops / (ms * 1e-3) / 1e12,
+                     "config": {"nt": info["nt"], "h": info["h"], "grid_ctas": info["grid"],
+                                "units": info["units"], "tuner_ms": tune_ms},
+                     "graph_launches": launches,
+                     "loop_ms": loop_ms, "loop_wall_s": loop_wall, "loop_pencils_per_s": count / (loop_ms * 1e-3),
+                     "speedup_vs_loop": loop_ms / ms, "max_rel_diff_vs_loop": worst,
+                     "resid_max_two_largest": max(resid)}
+        plan.close()
+        del VLl, VRl
+    tot_ms = res["d"]["ms"] + res["s"]["ms"]
+    tot_loop = res["d"]["loop_ms"] + res["s"]["loop_ms"]
+    return {"value": world * 2 * count / (tot_ms * 1e-3), "unit": "pencils/s",
+            "workload": (f"{count} pencils per GPU, n ~ U{{16..512}} (seed {args.batch_seed}), dtgevc3 and "
+                         f"stgevc3 SIDE=B HOWMNY=B, each pencil in both precisions"),
+            "sum_n3_flops_per_precision": flops, "ms_per_step_both_precisions": tot_ms,
+            "loop_ms_both_precisions": tot_loop, "speedup_vs_loop": tot_loop / tot_ms,
+            "d": res["d"], "s": res["s"],
+            "data": "synthetic Schur-form pencils (device-drawn strictly upper parts, seeded diagonal blocks), "
+                    "Householder Q, Z; inputs larger than L2 (no flush)"}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -457,6 +608,8 @@ def main():
            "d2h_bytes_per_step": 2 * n * n * 8, "ms_per_step": 1e3 * e2e_s,
            "path": f"xtgevc3_dtgevc3 (host pointers, pinned), {head} form, H2D/D2H inside the call"}
 
+    batched = measure_batched(args, X, torch, dist, world) if args.batch_count > 0 else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         thr = host_threads()
@@ -485,7 +638,7 @@ def main():
                            "parallelism": f"independent pencil per GPU x{world}",
                            "resid_max": h["resid"], "resid_bound": 1e-12},
                 "forms": forms_out, "clocks": h["clocks"], "e2e": e2e, "gpu_launches": h["launches"],
-                "roofline": roof, "kernels": kernels, "cpu_baseline": cpu}
+                "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "batched": batched}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -127,6 +127,65 @@ int xtgevc3_dtgevc3_dev_noalloc(void *stream, char side, char howmny, const int 
                                 const double *beta, double *VL, int ldvl, double *VR, int ldvr, int mm, int *m,
                                 int *info);
 
+/* ---- batched form (no counterpart in the upstream library) ---------------------------
+ * Eigenvectors of many independent real pencils of different orders in one persistent
+ * kernel launch, captured once in a CUDA graph.  One pencil: every pointer is a device
+ * pointer on the current device, matrices column-major with the given leading dimensions
+ * (>= n); alphar/alphai/beta are device arrays of length n.  Q and Z (HOWMNY='B') are
+ * read only and the eigenvectors go to VL / VR, which must not overlap Q / Z (unlike
+ * the in-place upstream interface).  Computes all eigenvectors (HOWMNY 'A' or 'B'; 'S'
+ * is not offered): n columns of VL and/or VR per pencil, as the single-pencil entry
+ * points would return them.  Unused pointers may be NULL. */
+typedef struct xtgevc3_dpencil {
+    int n, lds, ldp, ldq, ldz, ldvl, ldvr;
+    const double *S, *P;
+    const double *alphar, *alphai, *beta;
+    const double *Q, *Z;
+    double *VL, *VR;
+} xtgevc3_dpencil;
+typedef struct xtgevc3_spencil {
+    int n, lds, ldp, ldq, ldz, ldvl, ldvr;
+    const float *S, *P;
+    const float *alphar, *alphai, *beta;
+    const float *Q, *Z;
+    float *VL, *VR;
+} xtgevc3_spencil;
+
+/* A plan binds one batch: the descriptor array (copied), the tile configuration, the
+ * device workspace and the captured graph.  xtgevc3_batched_run launches the graph on
+ * `stream`; run it again after writing new data into the same device buffers.  The
+ * result is complete when the stream reaches the end of the launch;
+ * xtgevc3_batched_wait synchronises the stream and reports the kernel's status word.
+ * config: XTGEVC3_BATCH_CONFIG(nt, h) = NT columns per tile (16 or 32) and row blocks of
+ * H rows (32 or 64); 0 takes the process default (set by the tuner, by
+ * xtgevc3_batched_set_default, or by the environment variable XTGEVC3_BATCH_CONFIG,
+ * e.g. "d:16x64,s:32x64").  The largest order a configuration accepts follows from the
+ * shared memory per block (n <= 512 with every configuration on B200; larger orders are
+ * refused with a message).  Returns 0, -1 (bad argument: message in
+ * xtgevc3_last_error()) or 1 (CUDA failure). */
+typedef struct xtgevc3_batch xtgevc3_batch;
+#define XTGEVC3_BATCH_CONFIG(nt, h) (((unsigned)(nt) << 8) | (unsigned)(h))
+int xtgevc3_dtgevc3_batched_create(char side, char howmny, int count, const xtgevc3_dpencil *pencils,
+                                   unsigned config, xtgevc3_batch **plan);
+int xtgevc3_stgevc3_batched_create(char side, char howmny, int count, const xtgevc3_spencil *pencils,
+                                   unsigned config, xtgevc3_batch **plan);
+int xtgevc3_batched_run(xtgevc3_batch *plan, void *stream);
+/* 0 ok, 1 CUDA failure, 3 a bounded wait of the kernel's work queue expired */
+int xtgevc3_batched_wait(xtgevc3_batch *plan, void *stream);
+void xtgevc3_batched_destroy(xtgevc3_batch *plan);
+/* the plan's tile configuration, grid size (CTAs) and units of work */
+int xtgevc3_batched_info(const xtgevc3_batch *plan, unsigned *config, int *grid, int *units);
+/* Tuner: times every tile configuration that fits on this batch (reps launches each, after
+ * one warm-up) and returns the fastest in *best (and its time in ms in *best_ms); it
+ * becomes the process default for that precision.  Returns as _create. */
+int xtgevc3_dtgevc3_batched_tune(char side, char howmny, int count, const xtgevc3_dpencil *pencils, int reps,
+                                 unsigned *best, float *best_ms);
+int xtgevc3_stgevc3_batched_tune(char side, char howmny, int count, const xtgevc3_spencil *pencils, int reps,
+                                 unsigned *best, float *best_ms);
+/* prec 'd' or 's'; config 0 restores the built-in default */
+void xtgevc3_batched_set_default(char prec, unsigned config);
+unsigned xtgevc3_batched_get_default(char prec);
+
 #ifdef __cplusplus
 }
 #endif

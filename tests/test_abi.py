@@ -112,3 +112,49 @@ def test_flags_roundtrip():
     X.set_flags(X.NORMALIZE | X.SIMT)
     assert X.get_flags() == 3
     X.set_flags(old)
+
+
+def _fake_desc(n=8, **over):
+    """A descriptor with distinct non-NULL (never dereferenced) addresses."""
+    d = X.PencilDesc()
+    d.n = n
+    for i, key in enumerate(("S", "P", "alphar", "alphai", "beta", "Q", "Z", "VL", "VR")):
+        setattr(d, key, ct.c_void_p(0x100000 * (i + 1)))
+    for ld in ("lds", "ldp", "ldq", "ldz", "ldvl", "ldvr"):
+        setattr(d, ld, n)
+    for k, v in over.items():
+        setattr(d, k, v)
+    return d
+
+
+@pytest.mark.parametrize("case,msg", [
+    (dict(side=b"X"), "side"),
+    (dict(howmny=b"S"), "howmny"),
+    (dict(n=-1), "n < 0"),
+    (dict(S=None), "NULL input"),
+    (dict(lds=4), "lds/ldp"),
+    (dict(VR=ct.c_void_p(0x100000 * 7 + 8)), "in place"),
+    (dict(config=X.batch_config(8, 16)), "unknown tile configuration"),
+])
+def test_batched_create_argument_checks(case, msg):
+    """Bad batched arguments are refused with -1 and a message before any CUDA call."""
+    case = dict(case)
+    side = case.pop("side", b"B")
+    howmny = case.pop("howmny", b"B")
+    config = case.pop("config", 0)
+    arr = (X.PencilDesc * 2)(_fake_desc(8), _fake_desc(**{"n": 8, **case}))
+    plan = ct.c_void_p()
+    L = X.lib()
+    for pfx in "ds":
+        rc = getattr(L, f"xtgevc3_{pfx}tgevc3_batched_create")(side, howmny, 2, ct.cast(arr, ct.c_void_p), config,
+                                                                ct.byref(plan))
+        assert rc == -1 and not plan.value
+        assert msg in X.last_error(), X.last_error()
+
+
+def test_batched_default_config_roundtrip():
+    old = X.batched_get_default("d")
+    X.batched_set_default("d", X.batch_config(32, 32))
+    assert X.batched_get_default("d") == X.batch_config(32, 32)
+    X.batched_set_default("d", 0)
+    assert X.batched_get_default("d") == old

@@ -80,6 +80,25 @@ def lib():
         L.xtgevc3_dtgevc3_dev_noalloc.argtypes = [_P, _C, _C, _P, _I, _P, _I, _P, _I, _P, _P, _P, _P, _I, _P, _I,
                                                   _I, _P, _P]
         L.xtgevc3_dtgevc3_dev_noalloc.restype = _I
+        for p in "ds":
+            f = getattr(L, f"xtgevc3_{p}tgevc3_batched_create")
+            f.argtypes = [_C, _C, _I, _P, _U, _P]
+            f.restype = _I
+            f = getattr(L, f"xtgevc3_{p}tgevc3_batched_tune")
+            f.argtypes = [_C, _C, _I, _P, _I, _P, _P]
+            f.restype = _I
+        L.xtgevc3_batched_run.argtypes = [_P, _P]
+        L.xtgevc3_batched_run.restype = _I
+        L.xtgevc3_batched_wait.argtypes = [_P, _P]
+        L.xtgevc3_batched_wait.restype = _I
+        L.xtgevc3_batched_destroy.argtypes = [_P]
+        L.xtgevc3_batched_destroy.restype = None
+        L.xtgevc3_batched_info.argtypes = [_P, _P, _P, _P]
+        L.xtgevc3_batched_info.restype = _I
+        L.xtgevc3_batched_set_default.argtypes = [_C, _U]
+        L.xtgevc3_batched_set_default.restype = None
+        L.xtgevc3_batched_get_default.argtypes = [_C]
+        L.xtgevc3_batched_get_default.restype = _U
         _lib = L
     return _lib
 
@@ -227,3 +246,111 @@ def tgevc3_dev(side, howmny, S, P, alpha, beta, alphai=None, VL=None, VR=None, s
     if rc != 0:
         raise RuntimeError(f"xtgevc3_{pfx}tgevc3_dev failed: {last_error()}")
     return m.value, info.value
+
+
+# ---- batched form ------------------------------------------------------------------------
+class PencilDesc(ct.Structure):
+    """xtgevc3_dpencil / xtgevc3_spencil (include/xtgevc3.h): device pointers of one pencil."""
+    _fields_ = [("n", _I), ("lds", _I), ("ldp", _I), ("ldq", _I), ("ldz", _I), ("ldvl", _I), ("ldvr", _I),
+                ("S", _P), ("P", _P), ("alphar", _P), ("alphai", _P), ("beta", _P), ("Q", _P), ("Z", _P),
+                ("VL", _P), ("VR", _P)]
+
+
+def batch_config(nt: int, h: int) -> int:
+    """XTGEVC3_BATCH_CONFIG(nt, h): NT eigenvector columns per tile, row blocks of H rows."""
+    return (int(nt) << 8) | int(h)
+
+
+def _descs(pencils):
+    """ctypes array of descriptors for a list of dicts of CUDA tensors (matrices column-major:
+    S, P, and as needed Q, Z, VL, VR; vectors alphar, alphai, beta)."""
+    import torch
+    arr = (PencilDesc * len(pencils))()
+    prec = None
+    for i, p in enumerate(pencils):
+        S = p["S"]
+        prec = prec or {torch.float64: "d", torch.float32: "s"}[S.dtype]
+        d = arr[i]
+        d.n = S.shape[0]
+        for key, ld in (("S", "lds"), ("P", "ldp"), ("Q", "ldq"), ("Z", "ldz"), ("VL", "ldvl"), ("VR", "ldvr")):
+            t = p.get(key)
+            ptr, l = _colmajor(t)
+            setattr(d, key, ptr)
+            setattr(d, ld, l if t is not None else max(d.n, 1))
+        for key in ("alphar", "alphai", "beta"):
+            t = p[key]
+            if not t.is_contiguous():
+                raise ValueError(f"{key} must be contiguous")
+            setattr(d, key, ct.c_void_p(t.data_ptr()))
+    return arr, prec or "d"
+
+
+class Batch:
+    """Plan of the batched form (xtgevc3_{d,s}tgevc3_batched_create) over CUDA tensors.
+
+    ``pencils``: list of dicts with S, P, alphar, alphai, beta and, as the side and howmny
+    need them, Q, Z (read only) and VL, VR (outputs, not overlapping Q / Z).  The plan keeps
+    the tensors alive; ``run()`` launches the captured graph on torch's current stream
+    (or ``stream``), ``wait()`` synchronises and raises if the kernel reported a failure.
+    """
+
+    def __init__(self, side, howmny, pencils, config=0):
+        L = lib()
+        self._keep = pencils
+        self._arr, self.prec = _descs(pencils)
+        self._plan = ct.c_void_p()
+        rc = getattr(L, f"xtgevc3_{self.prec}tgevc3_batched_create")(
+            side.encode(), howmny.encode(), len(pencils), ct.cast(self._arr, _P), int(config), ct.byref(self._plan))
+        if rc != 0:
+            raise RuntimeError(f"batched create failed ({rc}): {last_error()}")
+
+    @staticmethod
+    def _stream(stream):
+        import torch
+        return ct.c_void_p(torch.cuda.current_stream().cuda_stream if stream is None else stream)
+
+    def run(self, stream=None):
+        if lib().xtgevc3_batched_run(self._plan, self._stream(stream)) != 0:
+            raise RuntimeError(f"batched run failed: {last_error()}")
+
+    def wait(self, stream=None):
+        rc = lib().xtgevc3_batched_wait(self._plan, self._stream(stream))
+        if rc != 0:
+            raise RuntimeError(f"batched wait ({rc}): {last_error()}")
+
+    def info(self):
+        c, g, u = ct.c_uint(0), ct.c_int(0), ct.c_int(0)
+        lib().xtgevc3_batched_info(self._plan, ct.byref(c), ct.byref(g), ct.byref(u))
+        return dict(nt=c.value >> 8, h=c.value & 255, grid=g.value, units=u.value)
+
+    def close(self):
+        if self._plan:
+            lib().xtgevc3_batched_destroy(self._plan)
+            self._plan = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batched_tune(side, howmny, pencils, reps=3):
+    """Time every tile configuration on this batch; the fastest becomes the process default
+    for the precision.  Returns (config, ms)."""
+    arr, prec = _descs(pencils)
+    best, ms = ct.c_uint(0), ct.c_float(0)
+    rc = getattr(lib(), f"xtgevc3_{prec}tgevc3_batched_tune")(side.encode(), howmny.encode(), len(pencils),
+                                                               ct.cast(arr, _P), int(reps), ct.byref(best),
+                                                               ct.byref(ms))
+    if rc != 0:
+        raise RuntimeError(f"batched tune failed ({rc}): {last_error()}")
+    return best.value, ms.value
+
+
+def batched_set_default(prec: str, config: int) -> None:
+    lib().xtgevc3_batched_set_default(prec.encode(), int(config))
+
+
+def batched_get_default(prec: str) -> int:
+    return int(lib().xtgevc3_batched_get_default(prec.encode()))

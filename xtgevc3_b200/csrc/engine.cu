@@ -134,6 +134,7 @@ int trace_get(int cat, long long *launches, double *ms, double *flops, double *b
     return 0;
 }
 long long launch_count() { return g_launches.load(); }
+void count_launches(long long k) { g_launches.fetch_add(k); }
 
 // Scratch of one call.  Default: stream-ordered allocations from the device's pool (which
 // keeps freed memory for reuse).  Arena mode: 256-byte aligned slices of a caller-owned

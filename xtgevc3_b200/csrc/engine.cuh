@@ -44,5 +44,7 @@ void trace_enable(int on);
 void trace_reset();
 int trace_get(int cat, long long *launches, double *ms, double *flops, double *bytes);
 long long launch_count();
+// Adds launches made outside solve_device (the batched form's graph launches).
+void count_launches(long long k);
 
 }  // namespace xtg

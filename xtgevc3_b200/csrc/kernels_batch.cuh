@@ -1,0 +1,760 @@
+// Batched form: many independent pencils of uneven order in one persistent launch.
+//
+// Work is split into units taken from a global queue (one atomic counter) by a grid of
+// resident CTAs:
+//   * a prep unit per pencil: the norms behind the shift coefficients
+//     (src/dtgevc3.cpp:1254-1270), the complex-pair structure of the eigenvalues
+//     (src/dtgevc3.cpp:1193-1207), the per-column shift coefficients of both problem
+//     orientations (src/dtgevc3.cpp:716-725) and a partition of the columns into tiles
+//     that never separate the two columns of a complex pair.  It ends by setting the
+//     pencil's ready flag;
+//   * a compute unit per (pencil, side, column tile): the whole right-looking blocked
+//     substitution of the tile's eigenvectors (at most NT columns) with the tile X[0:c_hi,
+//     tile] resident in shared memory, followed by the back-transform V = Z X (right) or
+//     V = Q F X (left, F the row reversal) or the plain write-back.  A compute unit waits
+//     (bounded) for its pencil's ready flag.
+// The queue holds every pencil's prep unit before any compute unit, so a unit only ever
+// waits for work that a running CTA has already taken: no deadlock is possible.  A wait
+// that runs past its limit sets kErrWaitTimeout in the status word and the unit is
+// skipped; the host turns the status into an error return.
+//
+// The per-tile algorithm is the one of the single-pencil path (left problem = right
+// problem of (F S^T F, F P^T F); per-column overflow guards; seeds of the 1x1 and 2x2
+// diagonal blocks), restricted to the tile's columns:
+//     for each row block I = [r0, r1) of at most H rows, bottom to top from c_hi:
+//         solve   (ac_c S_II - b_c P_II) x = X[I, c]     (one warp per eigenvector)
+//         update  X[0:r0, tile] += [S[0:r0, I] | P[0:r0, I]] [-ac x ; b x]
+// The update and the back-transform are CTA-wide GEMMs: 256 threads, each owning up to
+// 4 rows (64 apart) x NT/4 columns of the output, the A operand (strips of S and P, or of
+// Z / Q) staged through shared memory in chunks of KC columns by cp.async, double
+// buffered; the B operand (the solved block, or X itself) is read from shared memory by
+// broadcast.  The left problem's strips are rows of S and P: the stager reads them along
+// the row (contiguous in memory) and transposes on the way into shared memory.
+#pragma once
+#include "common.cuh"
+#include "kernels_diag.cuh"
+#include "../../include/xtgevc3.h"
+
+namespace xtg {
+namespace batch {
+
+constexpr int THREADS = 256;
+constexpr int WARPS = THREADS / 32;
+constexpr int KC = 16;          // A-operand columns per staged chunk
+constexpr int PASS = 256;       // output rows per GEMM pass: 64 row lanes x 4 row slots
+constexpr int ALD = PASS + 1;   // leading dimension of a staged chunk
+
+template <class T> struct PencilOf;
+template <> struct PencilOf<double> { using type = xtgevc3_dpencil; };
+template <> struct PencilOf<float> { using type = xtgevc3_spencil; };
+
+// Row strides of the shared X tile and of the solved-block operand: 16-byte aligned rows,
+// shifted by 16 bytes from one row to the next (conflict-free 16-byte accesses).
+template <class T, int NT> struct Lds {
+    static constexpr int X = NT + 16 / (int)sizeof(T);
+    static constexpr int Y = NT + 16 / (int)sizeof(T);
+};
+
+__host__ __device__ inline int max_tiles(int n, int nt) { return (n + nt - 2) / (nt - 1); }
+
+// Per-pencil workspace, written by the prep unit.
+template <class T>
+struct Work {
+    T *coef;          // [2][n][4]: ac, b_re, b_im, smin per column (side 0 right, 1 left)
+    T *norms;         // [2]: anorm, bnorm
+    int *tiles;       // [2][maxt + 1]: first column of each tile, then n
+    int *ntiles;      // [2]
+    uint8_t *kind;    // [2][n]: kReal / kPairRe / kPairIm in problem orientation
+    uint8_t *splitf;  // [2][n + 1]: rows j-1, j form a 2x2 diagonal block (orientation)
+};
+
+__host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+template <class T>
+__host__ __device__ inline size_t work_layout(unsigned char *base, int n, int nt, Work<T> *w)
+{
+    const int maxt = max_tiles(n, nt);
+    size_t off = 0;
+    auto take = [&](size_t bytes, size_t al) {
+        off = align_up(off, al);
+        size_t o = off;
+        off += bytes;
+        return o;
+    };
+    const size_t o_coef = take(sizeof(T) * 8 * (size_t)n, 16);
+    const size_t o_norm = take(sizeof(T) * 2, 16);
+    const size_t o_tiles = take(sizeof(int) * 2 * (size_t)(maxt + 1), 16);
+    const size_t o_nt = take(sizeof(int) * 2, 16);
+    const size_t o_kind = take(2 * (size_t)n, 16);
+    const size_t o_split = take(2 * (size_t)(n + 1), 16);
+    if (w) {
+        w->coef = reinterpret_cast<T *>(base + o_coef);
+        w->norms = reinterpret_cast<T *>(base + o_norm);
+        w->tiles = reinterpret_cast<int *>(base + o_tiles);
+        w->ntiles = reinterpret_cast<int *>(base + o_nt);
+        w->kind = base + o_kind;
+        w->splitf = base + o_split;
+    }
+    return align_up(off, 256);
+}
+
+template <class T>
+struct Args {
+    const typename PencilOf<T>::type *pencils;
+    const int4 *units;       // {0: prep | 1: compute, pencil, side, tile}
+    int nunits;
+    unsigned char *ws;       // per-pencil workspaces
+    const long long *woff;   // byte offset of each pencil's workspace
+    int *ctrl;               // [0] queue counter, [1] status word, [2 + p] ready flag of pencil p
+    int back;                // HOWMNY = 'B'
+    int xrows;               // rows of the shared X tile (>= every n)
+    long long spin_limit;    // polls of a ready flag before giving up
+};
+
+template <class T, int NT, int H>
+__host__ __device__ constexpr size_t smem_union_bytes()
+{
+    return (2 * (size_t)KC * ALD > 2 * (size_t)H * (H + 1) ? 2 * (size_t)KC * ALD : 2 * (size_t)H * (H + 1)) *
+           sizeof(T);
+}
+
+template <class T, int NT, int H>
+__host__ __device__ inline size_t smem_bytes(int xrows)
+{
+    return (size_t)xrows * Lds<T, NT>::X * sizeof(T) + 2 * (size_t)H * Lds<T, NT>::Y * sizeof(T) +
+           smem_union_bytes<T, NT, H>();
+}
+
+// ---- small helpers -------------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ void cp_async_elem(T *smem, const T *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    if constexpr (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// CPT consecutive elements from 16-byte aligned shared memory.
+template <int CPT>
+__device__ __forceinline__ void load_vec(double (&v)[CPT], const double *p)
+{
+#pragma unroll
+    for (int j = 0; j < CPT; j += 2) {
+        const double2 t = *reinterpret_cast<const double2 *>(p + j);
+        v[j] = t.x;
+        v[j + 1] = t.y;
+    }
+}
+template <int CPT>
+__device__ __forceinline__ void load_vec(float (&v)[CPT], const float *p)
+{
+#pragma unroll
+    for (int j = 0; j < CPT; j += 4) {
+        const float4 t = *reinterpret_cast<const float4 *>(p + j);
+        v[j] = t.x;
+        v[j + 1] = t.y;
+        v[j + 2] = t.z;
+        v[j + 3] = t.w;
+    }
+}
+template <int CPT>
+__device__ __forceinline__ void store_vec(double *p, const double (&v)[CPT])
+{
+#pragma unroll
+    for (int j = 0; j < CPT; j += 2) *reinterpret_cast<double2 *>(p + j) = make_double2(v[j], v[j + 1]);
+}
+template <int CPT>
+__device__ __forceinline__ void store_vec(float *p, const float (&v)[CPT])
+{
+#pragma unroll
+    for (int j = 0; j < CPT; j += 4)
+        *reinterpret_cast<float4 *>(p + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+}
+
+// Output rows [p0 + rl + 64 q] x columns [cg * CPT, +CPT) of acc += A B over K, where the A
+// chunks (KC columns of the pass's rows, as As[k * ALD + row]) are staged by `issue` and
+// B is row-major in shared memory (row k at Bs + k * bld).
+template <class T, int CPT, int QN, class Issue>
+__device__ __forceinline__ void gemm_pass(T *As, const T *Bs, int bld, int K, Issue &&issue, T (&acc)[QN][CPT],
+                                          int rl, int cg)
+{
+    const int nch = (K + KC - 1) / KC;
+    issue(As, 0);
+    cp_commit();
+    for (int c = 0; c < nch; c++) {
+        if (c + 1 < nch) issue(As + ((c + 1) & 1) * KC * ALD, (c + 1) * KC);
+        cp_commit();
+        cp_wait<1>();
+        __syncthreads();
+        const T *a = As + (c & 1) * KC * ALD + rl;
+        const T *b = Bs + (size_t)c * KC * bld + cg * CPT;
+        const int kn = min(KC, K - c * KC);
+#pragma unroll 4
+        for (int kk = 0; kk < kn; kk++) {
+            T av[QN], bv[CPT];
+#pragma unroll
+            for (int q = 0; q < QN; q++) av[q] = a[kk * ALD + 64 * q];
+            load_vec<CPT>(bv, b + kk * bld);
+#pragma unroll
+            for (int q = 0; q < QN; q++)
+#pragma unroll
+                for (int j = 0; j < CPT; j++) acc[q][j] = fma(av[q], bv[j], acc[q][j]);
+        }
+        __syncthreads();
+    }
+}
+
+// Shared per-column description of the current tile.
+template <class T, int NT>
+struct TileCols {
+    T coef[NT][4];
+    int colk[NT];
+    int out[NT];
+    uint8_t kind[NT];
+};
+
+template <class T>
+__device__ __forceinline__ void scale_col(T *col, int ld, int a, int b, T s, int lane)
+{
+    for (int i = a + lane; i < b; i += 32) col[(size_t)i * ld] *= s;
+}
+
+// ---- prep unit -------------------------------------------------------------------------
+template <class T, int NT>
+__device__ void prep_unit(const Args<T> &a, int p, unsigned char *smem)
+{
+    const auto &d = a.pencils[p];
+    const int n = d.n;
+    Work<T> w;
+    work_layout<T>(a.ws + a.woff[p], n, NT, &w);
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    T *red = reinterpret_cast<T *>(smem);                  // [2][WARPS]
+    T *ai = red + 2 * WARPS;                                // [n] alphai
+    uint8_t *start = reinterpret_cast<uint8_t *>(ai + n);   // [n] complex pair starts here
+    uint8_t *sub = start + n;                               // [n] S[k+1, k] != 0
+    uint8_t *kinds = sub + n;                               // [2][n]
+    for (int k = tid; k < n; k += THREADS) ai[k] = d.alphai[k];
+    // 1-norm of the quasi-triangle of S and of P: column sums over rows <= col + 1
+    T ma = T(0), mb = T(0);
+    for (int col = wid; col < n; col += WARPS) {
+        const int last = min(col + 1, n - 1);
+        T ss = T(0), sp = T(0);
+        for (int r = lane; r <= last; r += 32) {
+            ss += fabs(d.S[(size_t)r + (size_t)col * d.lds]);
+            sp += fabs(d.P[(size_t)r + (size_t)col * d.ldp]);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            ss += __shfl_xor_sync(0xffffffffu, ss, o);
+            sp += __shfl_xor_sync(0xffffffffu, sp, o);
+        }
+        ma = fmax(ma, ss);
+        mb = fmax(mb, sp);
+    }
+    if (lane == 0) {
+        red[wid] = ma;
+        red[WARPS + wid] = mb;
+    }
+    __syncthreads();
+    // pair starts: k starts a pair iff alphai[k] != 0, k + 1 < n, and the run of nonzero
+    // alphai ending just above k has even length (the upstream scan pairs greedily from 0)
+    for (int k = tid; k < n; k += THREADS) {
+        int run = 0;
+        while (k - run - 1 >= 0 && ai[k - run - 1] != T(0)) run++;
+        start[k] = (ai[k] != T(0) && k + 1 < n && (run & 1) == 0) ? 1 : 0;
+        sub[k] = (k + 1 < n) && d.S[(size_t)(k + 1) + (size_t)k * d.lds] != T(0);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        T x = red[0], y = red[WARPS];
+        for (int q = 1; q < WARPS; q++) {
+            x = fmax(x, red[q]);
+            y = fmax(y, red[WARPS + q]);
+        }
+        red[0] = x;
+        red[WARPS] = y;
+        w.norms[0] = x;
+        w.norms[1] = y;
+    }
+    // kinds and block-split flags of both orientations
+    for (int c = tid; c < n; c += THREADS) {
+        const uint8_t kr = start[c] ? kPairRe : (c > 0 && start[c - 1] ? kPairIm : kReal);
+        const uint8_t kl = (c <= n - 2 && start[n - 2 - c]) ? kPairRe : (start[n - 1 - c] ? kPairIm : kReal);
+        kinds[c] = kr;
+        kinds[n + c] = kl;
+        w.kind[c] = kr;
+        w.kind[n + c] = kl;
+    }
+    for (int j = tid; j <= n; j += THREADS) {
+        uint8_t fr = 0, fl = 0;
+        if (j >= 1 && j < n) {
+            fr = sub[j - 1] || start[j - 1];
+            const int kq = n - 1 - j;
+            fl = sub[kq] || start[kq];
+        }
+        w.splitf[j] = fr;
+        w.splitf[(n + 1) + j] = fl;
+    }
+    __syncthreads();
+    // shift coefficients (the single-pencil path's coef_real_kernel, both orientations)
+    {
+        const T safemin = limits<T>::safemin, eps = limits<T>::eps;
+        const T anorm = red[0], bnorm = red[WARPS];
+        const T ascale = T(1) / fmax(anorm, safemin), bscale = T(1) / fmax(bnorm, safemin);
+        for (int q = tid; q < 2 * n; q += THREADS) {
+            const int side = q / n, c = q % n;
+            const uint8_t kd = kinds[q];
+            int src;
+            if (side == 0) src = kd == kPairIm ? c - 1 : c;
+            else src = kd == kReal ? n - 1 - c : (kd == kPairRe ? n - 2 - c : n - 1 - c);
+            T ar = d.alphar[src], ai = kd == kReal ? T(0) : d.alphai[src], b = d.beta[src];
+            if (side == 1) ai = -ai;
+            const T den = fmax(fmax(fabs(ar) * ascale + fabs(ai) * ascale, fabs(b) * bscale), safemin);
+            const T t = T(1) / den;
+            T ac = (t * b * bscale) * ascale;
+            T br = (t * ar * ascale) * bscale;
+            T bi = (t * ai * ascale) * bscale;
+            if (fabs(b) <= safemin && (fabs(ar) + fabs(ai)) > safemin) {
+                ac = T(0);
+                br = T(1);
+                bi = T(0);
+            }
+            T *cf = w.coef + 4 * (size_t)q;
+            cf[0] = ac;
+            cf[1] = br;
+            cf[2] = bi;
+            cf[3] = fmax(eps * (fabs(ac) * anorm + (fabs(br) + fabs(bi)) * bnorm), safemin);
+        }
+    }
+    // column tiles: NT columns, one fewer when the last would be the Re column of a pair
+    if (tid < 2) {
+        const int side = tid, maxt = max_tiles(n, NT);
+        int *tl = w.tiles + side * (maxt + 1);
+        int c = 0, t = 0;
+        while (c < n) {
+            tl[t++] = c;
+            int e = min(c + NT, n);
+            if (e < n && kinds[side * n + e - 1] == kPairRe) e -= 1;
+            c = e;
+        }
+        tl[t] = n;
+        w.ntiles[side] = t;
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) atomicExch(a.ctrl + 2 + p, 1);
+}
+
+// ---- one eigenvector item of a row block -------------------------------------------------
+// The solve of diag_solve_real (kernels_diag.cuh) on a shared-memory tile column: X rows are
+// Xc[i * XLD], the block's update operand goes to Ys rows i (-ac x) and jnb + i (b x).
+template <class T, int NT, int H>
+__device__ void solve_item(const TileCols<T, NT> &tc, int j, int r0, int r1, const T *Sd, const T *Pd,
+                           uint64_t sec, T *Xs, T *Ys, bool left, T thr_rhs, T thr_upd, int lane)
+{
+    constexpr int XLD = Lds<T, NT>::X, YLD = Lds<T, NT>::Y, DLD = H + 1;
+    const uint8_t kd = tc.kind[j];
+    const int k = tc.colk[j];
+    const int kl = k - r0;
+    const bool diag = k < r1;
+    const int jnb = r1 - r0;
+    const T ac = tc.coef[j][0], br = tc.coef[j][1], bi = tc.coef[j][2], smin = tc.coef[j][3];
+    T *colr = Xs + j;
+    const int nrows = diag ? kl : jnb;
+    if (kd == kReal) {
+        const int top = k;
+        auto W = [&](int i, int c) -> T { return ac * Sd[i + c * DLD] - br * Pd[i + c * DLD]; };
+        T r[2];
+        T seed = diag ? T(1) : T(0);
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+            const int i = lane + 32 * s;
+            T v = T(0);
+            if (i < nrows) v = diag ? -W(i, kl) : colr[(size_t)(r0 + i) * XLD];
+            r[s] = v;
+        }
+        if (nrows > 0) {
+            const T mx = warp_max(fmax(fabs(r[0]), fabs(r[1])));
+            if (mx > thr_rhs) {
+                const T sc = thr_rhs / mx;
+                r[0] *= sc; r[1] *= sc; seed *= sc;
+                if (!diag) { scale_col(colr, XLD, 0, r0, sc, lane); scale_col(colr, XLD, r1, top + 1, sc, lane); }
+            }
+        }
+        Factors<T> F;
+        factor_rows(F, sec, nrows, lane, smin, W);
+        back_substitute(r, F, sec, nrows, lane, W);
+        T x[2];
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+            const int i = lane + 32 * s;
+            x[s] = i < nrows ? r[s] : (diag && i == kl ? seed : T(0));
+        }
+        const T mx = warp_max(fmax(fmax(fabs(ac * x[0]), fabs(br * x[0])), fmax(fabs(ac * x[1]), fabs(br * x[1]))));
+        if (mx > thr_upd) {
+            const T sc = thr_upd / mx;
+            x[0] *= sc; x[1] *= sc;
+            if (!diag) { scale_col(colr, XLD, 0, r0, sc, lane); scale_col(colr, XLD, r1, top + 1, sc, lane); }
+        }
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+            const int i = lane + 32 * s;
+            if (i < jnb) {
+                colr[(size_t)(r0 + i) * XLD] = x[s];
+                Ys[i * YLD + j] = -ac * x[s];
+                Ys[(jnb + i) * YLD + j] = br * x[s];
+            }
+        }
+    } else {
+        using C = cplx<T>;
+        T *coli = colr + 1;
+        const int top = k + 1;
+        const C b(br, bi);
+        auto W = [&](int i, int c) -> C {
+            const T s = Sd[i + c * DLD], p = Pd[i + c * DLD];
+            return C(ac * s - br * p, -bi * p);
+        };
+        C seed0(0, 0), seed1(0, 0);
+        if (diag) {
+            if (!left) {  // (x_k, x_k+1) = (-w12, w11), src/dtgevc3.cpp:727-740
+                seed0 = -W(kl, kl + 1);
+                seed1 = W(kl, kl);
+            } else {      // the left problem's seed, mirrored: (w22, -w21)
+                seed0 = W(kl + 1, kl + 1);
+                seed1 = -W(kl + 1, kl);
+            }
+        }
+        C r[2];
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+            const int i = lane + 32 * s;
+            C v(0, 0);
+            if (i < nrows) {
+                if (diag) v = -(W(i, kl) * seed0 + W(i, kl + 1) * seed1);
+                else v = C(colr[(size_t)(r0 + i) * XLD], coli[(size_t)(r0 + i) * XLD]);
+            }
+            r[s] = v;
+        }
+        if (nrows > 0) {
+            const T mx = warp_max(fmax(fmax(fabs(r[0].x), fabs(r[0].y)), fmax(fabs(r[1].x), fabs(r[1].y))));
+            if (mx > thr_rhs) {
+                const T sc = thr_rhs / mx;
+                r[0] = sc * r[0]; r[1] = sc * r[1]; seed0 = sc * seed0; seed1 = sc * seed1;
+                if (!diag) {
+                    scale_col(colr, XLD, 0, r0, sc, lane); scale_col(colr, XLD, r1, top + 1, sc, lane);
+                    scale_col(coli, XLD, 0, r0, sc, lane); scale_col(coli, XLD, r1, top + 1, sc, lane);
+                }
+            }
+        }
+        Factors<C> F;
+        factor_rows(F, sec, nrows, lane, smin, W);
+        back_substitute(r, F, sec, nrows, lane, W);
+        C x[2];
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+            const int i = lane + 32 * s;
+            x[s] = i < nrows ? r[s] : (diag && i == kl ? seed0 : (diag && i == kl + 1 ? seed1 : C(0, 0)));
+        }
+        T mx = T(0);
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+            const C ys = ac * x[s], yp = b * x[s];
+            mx = fmax(mx, fmax(fmax(fabs(ys.x), fabs(ys.y)), fmax(fabs(yp.x), fabs(yp.y))));
+        }
+        mx = warp_max(mx);
+        if (mx > thr_upd) {
+            const T sc = thr_upd / mx;
+            x[0] = sc * x[0]; x[1] = sc * x[1];
+            if (!diag) {
+                scale_col(colr, XLD, 0, r0, sc, lane); scale_col(colr, XLD, r1, top + 1, sc, lane);
+                scale_col(coli, XLD, 0, r0, sc, lane); scale_col(coli, XLD, r1, top + 1, sc, lane);
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+            const int i = lane + 32 * s;
+            if (i < jnb) {
+                colr[(size_t)(r0 + i) * XLD] = x[s].x;
+                coli[(size_t)(r0 + i) * XLD] = x[s].y;
+                const C yp = b * x[s];
+                Ys[i * YLD + j] = -ac * x[s].x;
+                Ys[i * YLD + j + 1] = -ac * x[s].y;
+                Ys[(jnb + i) * YLD + j] = yp.x;
+                Ys[(jnb + i) * YLD + j + 1] = yp.y;
+            }
+        }
+    }
+}
+
+// ---- compute unit ------------------------------------------------------------------------
+template <class T, int NT, int H, int QN>
+__device__ __forceinline__ void update_pass(const typename PencilOf<T>::type &d, bool left, int r0, int jnb, int p0,
+                                            int rows, T *Xs, const T *Ys, T *As)
+{
+    constexpr int XLD = Lds<T, NT>::X, YLD = Lds<T, NT>::Y, CPT = NT / 4;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int rl = (wid >> 2) * 32 + lane, cg = wid & 3;
+    const int n = d.n, K = 2 * jnb;
+    T acc[QN][CPT];
+#pragma unroll
+    for (int q = 0; q < QN; q++) {
+        const int i = rl + 64 * q;
+        if (i < rows) load_vec<CPT>(acc[q], Xs + (size_t)(p0 + i) * XLD + cg * CPT);
+        else
+#pragma unroll
+            for (int j = 0; j < CPT; j++) acc[q][j] = T(0);
+    }
+    auto issue = [&](T *dst, int k0) {
+        if (!left) {
+            if (tid < rows) {
+                const int row = p0 + tid;
+#pragma unroll 4
+                for (int kk = 0; kk < KC; kk++) {
+                    const int k = k0 + kk;
+                    if (k < K) {
+                        const T *src = k < jnb ? d.S + (size_t)row + (size_t)(r0 + k) * d.lds
+                                               : d.P + (size_t)row + (size_t)(r0 + k - jnb) * d.ldp;
+                        cp_async_elem(dst + kk * ALD + tid, src);
+                    }
+                }
+            }
+        } else {
+            const int kk = tid % KC, k = k0 + kk;
+            if (k < K) {
+                const int rs = k < jnb ? n - 1 - (r0 + k) : n - 1 - (r0 + k - jnb);
+                const T *base = k < jnb ? d.S + rs : d.P + rs;
+                const size_t ld = k < jnb ? (size_t)d.lds : (size_t)d.ldp;
+                for (int r = tid / KC; r < rows; r += THREADS / KC)
+                    cp_async_elem(dst + kk * ALD + r, base + (size_t)(n - 1 - (p0 + r)) * ld);
+            }
+        }
+    };
+    gemm_pass<T, CPT, QN>(As, Ys, YLD, K, issue, acc, rl, cg);
+#pragma unroll
+    for (int q = 0; q < QN; q++) {
+        const int i = rl + 64 * q;
+        if (i < rows) store_vec<CPT>(Xs + (size_t)(p0 + i) * XLD + cg * CPT, acc[q]);
+    }
+}
+
+template <class T, int NT, int H, int QN>
+__device__ __forceinline__ void back_pass(const typename PencilOf<T>::type &d, bool left, int khi, int p0, int rows,
+                                          const T *Xs, T *As, const TileCols<T, NT> &tc, int ntc)
+{
+    constexpr int XLD = Lds<T, NT>::X, CPT = NT / 4;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int rl = (wid >> 2) * 32 + lane, cg = wid & 3;
+    const int n = d.n;
+    T acc[QN][CPT];
+#pragma unroll
+    for (int q = 0; q < QN; q++)
+#pragma unroll
+        for (int j = 0; j < CPT; j++) acc[q][j] = T(0);
+    const T *Zb = left ? d.Q : d.Z;
+    const size_t ldz = left ? (size_t)d.ldq : (size_t)d.ldz;
+    auto issue = [&](T *dst, int k0) {
+        if (tid < rows) {
+            const int row = p0 + tid;
+#pragma unroll 4
+            for (int kk = 0; kk < KC; kk++) {
+                const int k = k0 + kk;
+                if (k < khi) {
+                    const int zc = left ? n - 1 - k : k;
+                    cp_async_elem(dst + kk * ALD + tid, Zb + (size_t)row + (size_t)zc * ldz);
+                }
+            }
+        }
+    };
+    gemm_pass<T, CPT, QN>(As, Xs, XLD, khi, issue, acc, rl, cg);
+    T *V = left ? d.VL : d.VR;
+    const size_t ldv = left ? (size_t)d.ldvl : (size_t)d.ldvr;
+#pragma unroll
+    for (int q = 0; q < QN; q++) {
+        const int i = rl + 64 * q;
+        if (i < rows)
+#pragma unroll
+            for (int j = 0; j < CPT; j++) {
+                const int c = cg * CPT + j;
+                if (c < ntc) V[(size_t)(p0 + i) + (size_t)tc.out[c] * ldv] = acc[q][j];
+            }
+    }
+}
+
+template <class T, int NT, int H>
+__device__ void compute_unit(const Args<T> &a, int p, int side, int t, unsigned char *smem, TileCols<T, NT> &tc,
+                             uint64_t &s_sec)
+{
+    constexpr int XLD = Lds<T, NT>::X, YLD = Lds<T, NT>::Y, DLD = H + 1;
+    const auto &d = a.pencils[p];
+    const int n = d.n;
+    const bool left = side == 1;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    Work<T> w;
+    work_layout<T>(a.ws + a.woff[p], n, NT, &w);
+    const int maxt = max_tiles(n, NT);
+    const int ntiles = __ldcg(w.ntiles + side);
+    if (t >= ntiles) return;
+    const int c_lo = __ldcg(w.tiles + side * (maxt + 1) + t), c_hi = __ldcg(w.tiles + side * (maxt + 1) + t + 1);
+    const int ntc = c_hi - c_lo;
+
+    T *Xs = reinterpret_cast<T *>(smem);
+    T *Ys = Xs + (size_t)a.xrows * XLD;
+    T *U = Ys + 2 * H * YLD;  // staged A chunks, or the diagonal blocks of S and P
+    T *Sd = U, *Pd = U + H * DLD;
+
+    if (tid < NT) {
+        const int c = c_lo + tid;
+        if (tid < ntc) {
+            const uint8_t kd = __ldcg(w.kind + side * n + c);
+            tc.kind[tid] = kd;
+            tc.colk[tid] = kd == kPairIm ? c - 1 : c;
+#pragma unroll
+            for (int q = 0; q < 4; q++) tc.coef[tid][q] = __ldcg(w.coef + 4 * ((size_t)side * n + c) + q);
+            tc.out[tid] = !left ? c : (kd == kReal ? n - 1 - c : (kd == kPairRe ? n - 2 - c : n - c));
+        } else {
+            tc.kind[tid] = kPairIm;  // never a solve item
+            tc.colk[tid] = -1;
+            tc.out[tid] = 0;
+        }
+    }
+    for (int idx = tid; idx < c_hi * NT; idx += THREADS) Xs[(size_t)(idx / NT) * XLD + idx % NT] = T(0);
+    __syncthreads();
+
+    const T safemin = limits<T>::safemin, eps = limits<T>::eps;
+    const T bignum = T(1) / (safemin / eps);
+    const uint8_t *splitf = w.splitf + side * (n + 1);
+    for (int cur = c_hi; cur > 0;) {
+        const int r1 = cur;
+        int r0 = max(0, cur - H);
+        if (r0 > 0 && __ldcg(splitf + r0)) r0 += 1;
+        const int jnb = r1 - r0;
+        // diagonal blocks (problem orientation) and a zeroed update operand
+        for (int idx = tid; idx < jnb * jnb; idx += THREADS) {
+            int i, j;
+            T sv = T(0), pv = T(0);
+            if (!left) {
+                i = idx % jnb;
+                j = idx / jnb;
+                if (i <= j + 1) {
+                    sv = d.S[(size_t)(r0 + i) + (size_t)(r0 + j) * d.lds];
+                    pv = d.P[(size_t)(r0 + i) + (size_t)(r0 + j) * d.ldp];
+                }
+            } else {
+                i = idx / jnb;
+                j = idx % jnb;
+                if (i <= j + 1) {
+                    sv = d.S[(size_t)(n - 1 - (r0 + j)) + (size_t)(n - 1 - (r0 + i)) * d.lds];
+                    pv = d.P[(size_t)(n - 1 - (r0 + j)) + (size_t)(n - 1 - (r0 + i)) * d.ldp];
+                }
+            }
+            Sd[i + j * DLD] = sv;
+            Pd[i + j * DLD] = pv;
+        }
+        for (int idx = tid; idx < 2 * jnb * NT; idx += THREADS) Ys[(idx / NT) * YLD + idx % NT] = T(0);
+        __syncthreads();
+        if (tid < 32) {  // 2x2 diagonal blocks, paired greedily from the bottom
+            const bool b0 = lane >= 1 && lane < jnb && Sd[lane + (lane - 1) * DLD] != T(0);
+            const bool b1 = lane + 32 < jnb && Sd[(lane + 32) + (lane + 31) * DLD] != T(0);
+            const uint64_t sub =
+                (uint64_t)__ballot_sync(0xffffffffu, b0) | ((uint64_t)__ballot_sync(0xffffffffu, b1) << 32);
+            if (lane == 0) {
+                uint64_t sec = 0;
+                for (int j = jnb - 1; j >= 1;) {
+                    if ((sub >> j) & 1ull) {
+                        sec |= 1ull << j;
+                        j -= 2;
+                    } else {
+                        j -= 1;
+                    }
+                }
+                s_sec = sec;
+            }
+        }
+        __syncthreads();
+        const uint64_t sec = s_sec;
+        for (int j = wid; j < ntc; j += WARPS) {
+            if (tc.kind[j] == kPairIm || tc.colk[j] < r0) continue;
+            solve_item<T, NT, H>(tc, j, r0, r1, Sd, Pd, sec, Xs, Ys, left, bignum / T(10),
+                                 bignum / T(max(1, jnb)), lane);
+        }
+        __syncthreads();
+        for (int p0 = 0; p0 < r0; p0 += PASS) {
+            const int rows = min(PASS, r0 - p0);
+            switch ((rows + 63) / 64) {
+            case 1: update_pass<T, NT, H, 1>(d, left, r0, jnb, p0, rows, Xs, Ys, U); break;
+            case 2: update_pass<T, NT, H, 2>(d, left, r0, jnb, p0, rows, Xs, Ys, U); break;
+            case 3: update_pass<T, NT, H, 3>(d, left, r0, jnb, p0, rows, Xs, Ys, U); break;
+            default: update_pass<T, NT, H, 4>(d, left, r0, jnb, p0, rows, Xs, Ys, U); break;
+            }
+        }
+        __syncthreads();
+        cur = r0;
+    }
+
+    if (a.back) {
+        for (int p0 = 0; p0 < n; p0 += PASS) {
+            const int rows = min(PASS, n - p0);
+            switch ((rows + 63) / 64) {
+            case 1: back_pass<T, NT, H, 1>(d, left, c_hi, p0, rows, Xs, U, tc, ntc); break;
+            case 2: back_pass<T, NT, H, 2>(d, left, c_hi, p0, rows, Xs, U, tc, ntc); break;
+            case 3: back_pass<T, NT, H, 3>(d, left, c_hi, p0, rows, Xs, U, tc, ntc); break;
+            default: back_pass<T, NT, H, 4>(d, left, c_hi, p0, rows, Xs, U, tc, ntc); break;
+            }
+        }
+    } else {
+        T *V = left ? d.VL : d.VR;
+        const size_t ldv = left ? (size_t)d.ldvl : (size_t)d.ldvr;
+        for (int idx = tid; idx < n * ntc; idx += THREADS) {
+            const int i = idx % n, j = idx / n;
+            const int src = left ? n - 1 - i : i;
+            V[(size_t)i + (size_t)tc.out[j] * ldv] = src < c_hi ? Xs[(size_t)src * XLD + j] : T(0);
+        }
+    }
+}
+
+// ---- the persistent kernel ---------------------------------------------------------------
+template <class T, int NT, int H>
+__global__ void __launch_bounds__(THREADS, 1) batch_kernel(Args<T> a)
+{
+    extern __shared__ __align__(16) unsigned char smem_batch[];
+    __shared__ TileCols<T, NT> tc;
+    __shared__ uint64_t s_sec;
+    __shared__ int s_unit, s_ok;
+    for (;;) {
+        if (threadIdx.x == 0) s_unit = atomicAdd(a.ctrl, 1);
+        __syncthreads();
+        const int u = s_unit;
+        if (u >= a.nunits) break;
+        const int4 wu = a.units[u];
+        if (wu.x == 0) {
+            prep_unit<T, NT>(a, wu.y, smem_batch);
+        } else {
+            if (threadIdx.x == 0) {
+                int ok = 1;
+                const volatile int *flag = a.ctrl + 2 + wu.y;
+                long long it = 0;
+                while (*flag == 0) {
+                    if (++it > a.spin_limit) {
+                        atomicOr(a.ctrl + 1, kErrWaitTimeout);
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(128);
+                }
+                __threadfence();
+                s_ok = ok;
+            }
+            __syncthreads();
+            if (s_ok) compute_unit<T, NT, H>(a, wu.y, wu.z, wu.w, smem_batch, tc, s_sec);
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace batch
+}  // namespace xtg

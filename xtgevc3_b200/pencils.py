@@ -157,3 +157,59 @@ def gen_schur_like(n, seed=0, dtype=np.float64, with_qz=False):
         Z, _ = np.linalg.qr(rng.standard_normal((n, n)))
         out = out + (np.asfortranarray(Q.astype(dtype)), np.asfortranarray(Z.astype(dtype)))
     return out
+
+
+
+def schur_blocks(n, rng):
+    """Diagonal blocks of a gen_schur_like pencil of order n (same statistics), drawn with
+    vectorised calls: returns (k1, s1, p1, k2, s2, p2, alphar, alphai, beta) where k1 are
+    the rows of the 1x1 blocks with S[k,k] = s1, P[k,k] = p1, and k2 the first rows of the
+    2x2 blocks with S[k:k+2, k:k+2] = s2[:, 2x2] (row-major 4-vectors) and P = diag(p2)
+    (P[k, k+1] = 0)."""
+    n_real = int(round(np.sqrt(2.0 * n / np.pi)))
+    if (n - n_real) % 2:
+        n_real += 1
+    n_real = min(n_real, n)
+    n_pairs = (n - n_real) // 2
+    kinds = np.array([1] * n_real + [2] * n_pairs, dtype=np.int64)
+    rng.shuffle(kinds)
+    starts = np.concatenate([[0], np.cumsum(kinds)[:-1]]).astype(np.int64) if n else np.zeros(0, np.int64)
+    scale = 0.67 * np.sqrt(n)
+    ar, ai, be = np.zeros(n), np.zeros(n), np.zeros(n)
+    k1 = starts[kinds == 1]
+    p1 = scale * rng.uniform(0.2, 1.5, k1.size) * rng.choice([-1.0, 1.0], k1.size)
+    lam = rng.standard_normal(k1.size) / rng.standard_normal(k1.size)
+    s1 = lam * p1
+    ar[k1], be[k1] = s1, p1
+    k2 = starts[kinds == 2]
+    m = k2.size
+    g = (rng.standard_normal(m) + 1j * rng.standard_normal(m)) / (rng.standard_normal(m) +
+                                                                  1j * rng.standard_normal(m))
+    x, y = g.real, np.abs(g.imag) + 1e-3
+    q1, q2 = scale * rng.uniform(0.2, 1.5, m), scale * rng.uniform(0.2, 1.5, m)
+    c = y * np.exp(0.5 * rng.standard_normal(m)) * rng.choice([-1.0, 1.0], m)
+    s2 = np.stack([q1 * x, q1 * c, q2 * (-y * y / c), q2 * x], axis=1)
+    p2 = np.stack([q1, q2], axis=1)
+    b = np.sqrt(q1 * q2)
+    ar[k2] = ar[k2 + 1] = x * b
+    ai[k2], ai[k2 + 1] = y * b, -y * b
+    be[k2] = be[k2 + 1] = b
+    return k1, s1, p1, k2, s2, p2, ar, ai, be
+
+
+def gen_schur_batch(sizes, seed=0, dtype=np.float64):
+    """Many pencils with the statistics of gen_schur_like (diagonal blocks from
+    schur_blocks, strictly upper parts N(0,1)).  Returns a list of (S, P, alphar, alphai,
+    beta), Fortran-ordered."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for n in sizes:
+        n = int(n)
+        S = np.asfortranarray(np.triu(rng.standard_normal((n, n)), 1).astype(dtype))
+        P = np.asfortranarray(np.triu(rng.standard_normal((n, n)), 1).astype(dtype))
+        k1, s1, p1, k2, s2, p2, ar, ai, be = schur_blocks(n, rng)
+        S[k1, k1], P[k1, k1] = s1, p1
+        S[k2, k2], S[k2, k2 + 1], S[k2 + 1, k2], S[k2 + 1, k2 + 1] = s2[:, 0], s2[:, 1], s2[:, 2], s2[:, 3]
+        P[k2, k2], P[k2 + 1, k2 + 1], P[k2, k2 + 1] = p2[:, 0], p2[:, 1], 0.0
+        out.append((S, P, ar.astype(dtype), ai.astype(dtype), be.astype(dtype)))
+    return out
