@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--batch-count", type=int, default=2048,
                     help="pencils of the batched workload (0 skips it)")
     ap.add_argument("--batch-seed", type=int, default=2048)
+    ap.add_argument("--adjoint-n", type=int, default=2048, help="order of the dtgevc3 adjoint case (0 skips)")
+    ap.add_argument("--adjoint-c-count", type=int, default=256, help="complex64 pencils of the ctgevc3 adjoint case")
+    ap.add_argument("--adjoint-c-n", type=int, default=128)
     return ap.parse_args()
 
 
@@ -495,6 +498,58 @@ def measure_batched(args, X, torch, dist, world):
                     "Householder Q, Z; inputs larger than L2 (no flush)"}
 
 
+def measure_adjoint(args, X, torch):
+    """xtgevc3_adjoint: dL/dS, dL/dP of the right eigenvectors (SIDE='R', HOWMNY='A') for a
+    seeded upstream gradient dL/dX ~ N(0,1); d at order --adjoint-n, and c on
+    --adjoint-c-count complex64 pencils of order --adjoint-c-n (one call per pencil).  The
+    forward runs once, outside the timed region."""
+    from xtgevc3_b200 import pencils as gen
+    out = {}
+    n = args.adjoint_n
+    S_h, P_h, ar, ai, be = gen.gen_schur_like(n, args.seed + 11)
+    S, P = colmajor_cuda(S_h, torch), colmajor_cuda(P_h, torch)
+    VR = torch.zeros(n, n, device="cuda", dtype=torch.float64).t()
+    X.tgevc3_dev("R", "A", S, P, ar, be, alphai=ai, VR=VR)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(args.seed + 12)
+    G = torch.randn(n, n, device="cuda", dtype=torch.float64, generator=g).t()
+    for _ in range(max(args.warmup, 1)):
+        X.adjoint(S, P, ar, be, VR, G, alphai=ai)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        dS, dP = X.adjoint(S, P, ar, be, VR, G, alphai=ai)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    # masked gradient GEMMs (2 x 2 n^3) plus the transposed solves (~ n^3 / 3 x 2)
+    fl = 2 * 2.0 * n ** 3 + 2.0 * n ** 3 / 3.0
+    out["d"] = {"n": n, "ms": ms, "gradients_per_s": 1e3 / ms, "tflops_nominal": fl / (ms * 1e-3) / 1e12,
+                "finite": bool(torch.isfinite(dS).all() and torch.isfinite(dP).all())}
+    cnt, nc = args.adjoint_c_count, args.adjoint_c_n
+    cases = []
+    for i in range(cnt):
+        Sc, Pc, al, bc = gen.gen_upper_triangular_complex(nc, args.seed + 100 + i, dtype=np.complex64)
+        Sd, Pd = colmajor_cuda(Sc, torch), colmajor_cuda(Pc, torch)
+        V = torch.zeros(nc, nc, device="cuda", dtype=torch.complex64).t()
+        X.tgevc3_dev("R", "A", Sd, Pd, al, bc, VR=V)
+        Gc = torch.randn(nc, nc, device="cuda", dtype=torch.complex64, generator=g).t()
+        cases.append((Sd, Pd, al, bc, V, Gc))
+    for c in cases[:4]:
+        X.adjoint(c[0], c[1], c[2], c[3], c[4], c[5])
+    torch.cuda.synchronize()
+    e0.record()
+    for c in cases:
+        X.adjoint(c[0], c[1], c[2], c[3], c[4], c[5])
+    e1.record()
+    torch.cuda.synchronize()
+    msc = e0.elapsed_time(e1)
+    out["c"] = {"pencils": cnt, "n": nc, "ms_all": msc, "gradients_per_s": cnt / (msc * 1e-3),
+                "path": "one xtgevc3_adjoint call per pencil"}
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -609,6 +664,7 @@ def main():
            "path": f"xtgevc3_dtgevc3 (host pointers, pinned), {head} form, H2D/D2H inside the call"}
 
     batched = measure_batched(args, X, torch, dist, world) if args.batch_count > 0 else None
+    adjoint = measure_adjoint(args, X, torch) if args.adjoint_n > 0 and rank == 0 else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -638,7 +694,8 @@ def main():
                            "parallelism": f"independent pencil per GPU x{world}",
                            "resid_max": h["resid"], "resid_bound": 1e-12},
                 "forms": forms_out, "clocks": h["clocks"], "e2e": e2e, "gpu_launches": h["launches"],
-                "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "batched": batched}
+                "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "batched": batched,
+                "adjoint": adjoint}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

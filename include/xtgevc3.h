@@ -127,6 +127,25 @@ int xtgevc3_dtgevc3_dev_noalloc(void *stream, char side, char howmny, const int 
                                 const double *beta, double *VL, int ldvl, double *VR, int ldvr, int mm, int *m,
                                 int *info);
 
+/* ---- adjoint of the right eigenvectors (no counterpart in the upstream library) -------
+ * Reverse-mode derivative of X = the right eigenvectors computed with SIDE='R',
+ * HOWMNY='A' (in the Schur basis; for HOWMNY='B', V = Z X, pass G = Z^T dL/dV) with
+ * respect to S and P, the eigenvalues held fixed:  given G = dL/dX, returns dS = dL/dS and
+ * dP = dL/dP.  prec 'd', 's' (real arrays; a complex pair's two columns carry dL/dRe x and
+ * dL/dIm x) or 'z', 'c' (interleaved complex; gradients are dL/dRe + i dL/dIm).  S, P, X,
+ * G, dS, dP are device pointers on the current device (column-major, leading dimensions
+ * >= n); alpha (alphar), alphai and beta are HOST arrays as for the device entry points
+ * (alphai NULL for 'z'/'c').  X must be the forward's output for these S, P, alpha, beta:
+ * its per-column scale (the overflow guards of the forward) is read back from it.  The
+ * derivative includes the dependence of a complex pair's scale on the pencil norms (the
+ * upstream coefficient scaling) and of its 2x2 seed on S and P.  The forward reads the
+ * upper Hessenberg band (i <= j + 1) of a real S, subdiagonal zeros included, and the
+ * upper triangle of P and of complex pencils; every other entry gets 0.  Work is queued on `stream` and complete on return.
+ * Returns 0, -1 (bad argument) or 1 (CUDA failure); message in xtgevc3_last_error(). */
+int xtgevc3_adjoint(char prec, void *stream, int n, const void *S, int lds, const void *P, int ldp,
+                    const void *alpha, const void *alphai, const void *beta, const void *X, int ldx, const void *G,
+                    int ldg, void *dS, int ldds, void *dP, int lddp);
+
 /* ---- batched form (no counterpart in the upstream library) ---------------------------
  * Eigenvectors of many independent real pencils of different orders in one persistent
  * kernel launch, captured once in a CUDA graph.  One pencil: every pointer is a device

@@ -158,3 +158,21 @@ def test_batched_default_config_roundtrip():
     assert X.batched_get_default("d") == X.batch_config(32, 32)
     X.batched_set_default("d", 0)
     assert X.batched_get_default("d") == old
+
+
+@pytest.mark.parametrize("prec,n,ld,null,msg", [
+    (b"q", 4, 4, False, "prec"),
+    (b"d", -1, 4, False, "n < 0"),
+    (b"d", 4, 4, True, "NULL"),
+    (b"z", 8, 4, False, "leading dimension"),
+])
+def test_adjoint_argument_checks(prec, n, ld, null, msg):
+    """xtgevc3_adjoint refuses bad arguments with -1 and a message, before any CUDA call."""
+    L = X.lib()
+    L.xtgevc3_adjoint.argtypes = [ct.c_char] + [ct.c_void_p] + [ct.c_int] + [ct.c_void_p, ct.c_int] * 2 + \
+        [ct.c_void_p] * 3 + [ct.c_void_p, ct.c_int] * 4
+    L.xtgevc3_adjoint.restype = ct.c_int
+    p = None if null else ct.c_void_p(0x1000)
+    rc = L.xtgevc3_adjoint(prec, None, n, p, ld, p, ld, p, p, p, p, ld, p, ld, p, ld, p, ld)
+    assert rc == -1
+    assert msg in X.last_error(), X.last_error()

@@ -354,3 +354,43 @@ def batched_set_default(prec: str, config: int) -> None:
 
 def batched_get_default(prec: str) -> int:
     return int(lib().xtgevc3_batched_get_default(prec.encode()))
+
+
+# ---- adjoint -------------------------------------------------------------------------------
+def adjoint(S, P, alpha, beta, X, G, alphai=None, stream=None):
+    """dL/dS, dL/dP for the right eigenvectors X (SIDE='R', HOWMNY='A') given G = dL/dX
+    (xtgevc3_adjoint).  S, P, X, G: column-major CUDA tensors; alpha/alphai/beta: host
+    arrays.  Returns (dS, dP) as new column-major CUDA tensors."""
+    import torch
+    L = lib()
+    L.xtgevc3_adjoint.argtypes = [_C, _P, _I, _P, _I, _P, _I, _P, _P, _P, _P, _I, _P, _I, _P, _I, _P, _I]
+    L.xtgevc3_adjoint.restype = _I
+    tdt = S.dtype
+    pfx = {torch.float64: "d", torch.float32: "s", torch.complex128: "z", torch.complex64: "c"}[tdt]
+    n = S.shape[0]
+    dS = torch.zeros(n, n, dtype=tdt, device=S.device).t()
+    dP = torch.zeros(n, n, dtype=tdt, device=S.device).t()
+    rdt = np.float64 if pfx in "dz" else np.float32
+    cdt = np.complex128 if pfx == "z" else np.complex64
+    if pfx in "ds":
+        al = np.ascontiguousarray(alpha, dtype=rdt)
+        ai = np.ascontiguousarray(alphai, dtype=rdt)
+        be = np.ascontiguousarray(beta, dtype=rdt)
+    else:
+        al = np.ascontiguousarray(alpha, dtype=cdt)
+        ai = None
+        be = np.ascontiguousarray(beta, dtype=cdt)
+    if stream is None:
+        stream = torch.cuda.current_stream().cuda_stream
+    args = [pfx.encode(), ct.c_void_p(stream), n]
+    for t in (S, P):
+        p, ld = _colmajor(t)
+        args += [p, ld]
+    args += [_ptr(al), _ptr(ai), _ptr(be)]
+    for t in (X, G, dS, dP):
+        p, ld = _colmajor(t)
+        args += [p, ld]
+    rc = L.xtgevc3_adjoint(*args)
+    if rc != 0:
+        raise RuntimeError(f"xtgevc3_adjoint failed ({rc}): {last_error()}")
+    return dS, dP

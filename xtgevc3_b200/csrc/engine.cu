@@ -22,6 +22,7 @@
 #include "kernels_gemm.cuh"
 #include "kernels_misc.cuh"
 #include "kernels_split.cuh"
+#include "host_common.cuh"
 
 #include <cudaTypedefs.h>
 
@@ -39,16 +40,6 @@ static thread_local std::string g_err;
 const char *last_error() { return g_err.c_str(); }
 void set_last_error(const std::string &s) { g_err = s; }
 
-#define XTG_CK(call)                                                                              \
-    do {                                                                                          \
-        cudaError_t e_ = (call);                                                                  \
-        if (e_ != cudaSuccess) {                                                                  \
-            set_last_error(std::string(#call) + ": " + cudaGetErrorString(e_));                   \
-            return 1;                                                                             \
-        }                                                                                         \
-    } while (0)
-
-static inline int round_up(int v, int q) { return (v + q - 1) / q * q; }
 
 // ---- kernel trace ----------------------------------------------------------------------
 namespace {
@@ -136,47 +127,6 @@ int trace_get(int cat, long long *launches, double *ms, double *flops, double *b
 long long launch_count() { return g_launches.load(); }
 void count_launches(long long k) { g_launches.fetch_add(k); }
 
-// Scratch of one call.  Default: stream-ordered allocations from the device's pool (which
-// keeps freed memory for reuse).  Arena mode: 256-byte aligned slices of a caller-owned
-// device buffer, nothing allocated or freed; `used` can be rewound to reuse a region once
-// the work using it is ordered before the next user on the same stream.
-struct Scratch {
-    cudaStream_t st;
-    std::vector<void *> ptrs;
-    cudaError_t err = cudaSuccess;
-    unsigned char *arena = nullptr;
-    size_t cap = 0, used = 0;
-    explicit Scratch(cudaStream_t s) : st(s) {}
-    Scratch(cudaStream_t s, void *a, size_t c) : st(s), arena(static_cast<unsigned char *>(a)), cap(c) {}
-    template <class T>
-    T *get(size_t count)
-    {
-        if (count == 0) count = 1;
-        const size_t bytes = count * sizeof(T);
-        if (arena) {
-            const size_t off = (used + 255) & ~size_t(255);
-            if (off + bytes > cap) {
-                err = cudaErrorMemoryAllocation;
-                return nullptr;
-            }
-            used = off + bytes;
-            return reinterpret_cast<T *>(arena + off);
-        }
-        void *p = nullptr;
-        cudaError_t e = cudaMallocAsync(&p, bytes, st);
-        if (e != cudaSuccess) {
-            err = e;
-            return nullptr;
-        }
-        ptrs.push_back(p);
-        return static_cast<T *>(p);
-    }
-    ~Scratch()
-    {
-        for (void *p : ptrs) cudaFreeAsync(p, st);
-    }
-};
-
 size_t arena_bytes_needed(int n, int m, bool right, bool left, bool back, bool normalize, bool cplx, size_t rsz)
 {
     auto r256 = [](size_t b) { return (std::max<size_t>(b, 1) + 255) & ~size_t(255); };
@@ -199,7 +149,7 @@ size_t arena_bytes_needed(int n, int m, bool right, bool left, bool back, bool n
 }
 
 static std::once_flag g_pool_once[64];
-static void configure_device(int dev)
+void configure_device(int dev)
 {
     if (dev < 0 || dev >= 64) return;
     std::call_once(g_pool_once[dev], [dev]() {
@@ -311,26 +261,6 @@ static cudaError_t launch_split(const GemmArgs<double> &g, int s, SplitBufs &sb,
     p.err = d_err;
     gemm_split_kernel<<<dim3(Mp / BM, Np / BN), THREADS, SMEM_BYTES, st>>>(tmA, tmB, p);
     return cudaGetLastError();
-}
-
-template <class E>
-static void launch_gemm(const GemmArgs<E> &g, bool simt, cudaStream_t st)
-{
-    if constexpr (std::is_same<E, double>::value) {
-        // the cp.async path copies 16-byte pairs of rows: even leading dimensions and
-        // 16-byte aligned bases only (caller-given ld may be odd on the device API)
-        auto al = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
-        bool ok = (g.ldb % 2 == 0) && al(g.B) && (g.C != nullptr);
-        for (int s = 0; s < g.nseg; s++) ok = ok && (g.seg[s].lda % 2 == 0) && al(g.seg[s].A) && (g.seg[s].boff % 2 == 0);
-        if (!simt && ok) {
-            dim3 grid((g.M + dmma::BM - 1) / dmma::BM, (g.N + dmma::BN - 1) / dmma::BN);
-            if (g.accumulate) gemm_dmma<1><<<grid, 256, dmma::SMEM_BYTES, st>>>(g);
-            else gemm_dmma<0><<<grid, 256, dmma::SMEM_BYTES, st>>>(g);
-            return;
-        }
-    }
-    dim3 grid((g.M + 63) / 64, (g.N + 63) / 64);
-    gemm_simt<E><<<grid, 256, 0, st>>>(g);
 }
 
 template <class R, bool CPLX>

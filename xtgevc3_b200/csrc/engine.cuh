@@ -33,6 +33,9 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
                  int ldp, const void *alpha, const void *alphai, const void *beta, void *VL, int ldvl, void *VR,
                  int ldvr, int m_total, const Options &opt, cudaStream_t st);
 
+// Once per device: memory-pool release threshold and the kernels' shared-memory limits.
+void configure_device(int dev);
+
 const char *last_error();
 void set_last_error(const std::string &s);
 

@@ -195,14 +195,15 @@ __device__ __forceinline__ void factor_rows(Factors<E> &F, uint64_t sec, int nro
     }
 }
 
-// Block back substitution of one eigenvector held in r (rows [0, nrows)); on return r
-// holds the solution.  W(i, j) gives the shifted operator entry.
+// Block back substitution of one eigenvector held in r (rows [jlo, nrows)); on return r
+// holds the solution in those rows (rows below jlo receive updates that mean nothing).
+// W(i, j) gives the shifted operator entry.  jlo must not split a 2x2 block.
 template <class E, class WF>
 __device__ __forceinline__ void back_substitute(E (&r)[2], const Factors<E> &F, uint64_t sec, int nrows, int lane,
-                                                WF W)
+                                                WF W, int jlo = 0)
 {
     int j = nrows - 1;
-    while (j >= 0) {
+    while (j >= jlo) {
         if (j >= 1 && ((sec >> j) & 1ull)) {
             const int p = j - 1, q = j;
             const int sq = q >> 5;
