@@ -48,10 +48,11 @@ def parse():
     ap.add_argument("--seed", type=int, default=8192)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-window", type=int, default=1024, help="eigenvalues per side in the CPU sample")
-    ap.add_argument("--form", default="both", choices=["plain", "split", "both"],
-                    help="plain FP64, split precision (BF16 slices), or both (the faster one meeting the "
-                         "residual bound is the headline)")
+    ap.add_argument("--form", default="all", choices=["plain", "split", "split_i8", "all"],
+                    help="plain FP64, split precision with BF16 or INT8 slices, or all (the fastest one "
+                         "meeting the residual bound is the headline)")
     ap.add_argument("--slices", type=int, default=6, help="BF16 slices of the split form")
+    ap.add_argument("--slices-i8", type=int, default=7, help="INT8 slices of the split_i8 form")
     ap.add_argument("--batch-count", type=int, default=2048,
                     help="pencils of the batched workload (0 skips it)")
     ap.add_argument("--batch-seed", type=int, default=2048)
@@ -586,8 +587,9 @@ def main():
     peak_hbm = peaks.get("hbm_gbs", 6650.0)
 
     s = max(1, min(6, args.slices))
-    forms = {"plain": 0, "split": X.SPLIT | X.slices(s)}
-    names = ["plain", "split"] if args.form == "both" else [args.form]
+    s8 = max(1, min(7, args.slices_i8))
+    forms = {"plain": 0, "split": X.SPLIT | X.slices(s), "split_i8": X.SPLIT | X.SPLIT_INT8 | X.slices(s8)}
+    names = ["plain", "split", "split_i8"] if args.form == "all" else [args.form]
     res = {nm: measure_form(nm, forms[nm], args, X, torch, data, dist, local, world) for nm in names}
     ok = [nm for nm in names if res[nm]["resid"] <= 1e-12]
     head = min(ok or names, key=lambda nm: res[nm]["ms"])
@@ -597,14 +599,24 @@ def main():
     # roofline of the dominant kernel class of the headline form
     dom = max(kernels, key=lambda k: kernels[k]["ms"])
     kd = kernels[dom]
-    pairs = s * (s + 1) // 2
     if kd["flops"] > 0 and head == "split" and dom.startswith("gemm"):
         # BF16 slice products actually executed: pairs x the FP64-equivalent flops
+        pairs = s * (s + 1) // 2
         achieved = pairs * kd["flops"] / (kd["ms"] * 1e-3) / 1e12
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak_bf16, "unit": "TFLOP/s",
                 "frac": achieved / peak_bf16, "kernel": dom,
                 "fp64_equivalent_tflops": kd["flops"] / (kd["ms"] * 1e-3) / 1e12,
                 "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst), BF16 slice products counted"}
+    elif kd["flops"] > 0 and head == "split_i8" and dom.startswith("gemm"):
+        # INT8 slice products executed; the dense INT8 rate is twice the BF16 one on B200
+        pairs = s8 * (s8 + 1) // 2
+        achieved = pairs * kd["flops"] / (kd["ms"] * 1e-3) / 1e12
+        peak_i8 = 2.0 * peak_bf16
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak_i8, "unit": "TOP/s",
+                "frac": achieved / peak_i8, "kernel": dom,
+                "fp64_equivalent_tflops": kd["flops"] / (kd["ms"] * 1e-3) / 1e12,
+                "peak_source": "2 x MEASURED_PEAKS.json bf16_tflops (burst): INT8 dense rate, not measured; "
+                               "INT8 slice products counted"}
     elif kd["flops"] > 0:
         achieved = kd["flops"] / (kd["ms"] * 1e-3) / 1e12
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak_fp64, "unit": "TFLOP/s",
@@ -677,7 +689,8 @@ def main():
                           f"overstates the CPU rate of HOWMNY='B'")}
 
     if rank == 0:
-        form_desc = {"plain": "plain FP64 (DMMA)", "split": f"split precision, {s} BF16 slices (tcgen05)"}
+        form_desc = {"plain": "plain FP64 (DMMA)", "split": f"split precision, {s} BF16 slices (tcgen05)",
+                     "split_i8": f"split precision, {s8} INT8 slices (tcgen05 kind::i8)"}
         forms_out = {nm: {"value": r["value"], "ms_per_step": r["ms"], "resid_max": r["resid"],
                           "meets_resid_bound": r["resid"] <= 1e-12,
                           "kernels_ms_per_step": {k: v["ms_per_step"] for k, v in r["kernels"].items()}}

@@ -46,6 +46,9 @@ extern "C" {
  * ~48 bits per operand). */
 #define XTGEVC3_SPLIT 4u
 #define XTGEVC3_SLICES(s) ((unsigned)(s) << 8)
+/* With XTGEVC3_SPLIT: INT8 slices (7-bit digits, s in [1, 7], default 7, ~49 bits per
+ * operand) on the INT8 tensor cores with exact INT32 accumulation over the whole K. */
+#define XTGEVC3_SPLIT_INT8 8u
 
 /* Process-wide flags used by the drop-in entry points below (default 0). */
 void xtgevc3_set_flags(unsigned flags);

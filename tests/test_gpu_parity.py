@@ -210,27 +210,31 @@ def test_device_api_matches_host_api(cuda_ok):
 
 
 SPLIT_CASES = [
-    # (kind, n, seed, side, howmny, slices, elementwise tolerance vs the FP64 oracle)
-    ("gges", 257, 71, "B", "B", 6, 1e-10),
-    ("gges", 300, 72, "B", "A", 6, 1e-10),
-    ("schur", 700, 73, "B", "B", 6, 1e-6),
+    # (kind, n, seed, side, howmny, slices, elementwise tolerance vs the FP64 oracle, slice kind)
+    ("gges", 257, 71, "B", "B", 6, 1e-10, "bf16"),
+    ("gges", 300, 72, "B", "A", 6, 1e-10, "bf16"),
+    ("schur", 700, 73, "B", "B", 6, 1e-6, "bf16"),
+    ("gges", 257, 71, "B", "B", 7, 1e-10, "int8"),
+    ("gges", 300, 72, "B", "A", 7, 1e-10, "int8"),
+    ("schur", 700, 73, "B", "B", 7, 1e-6, "int8"),
 ]
 
 
-@pytest.mark.parametrize("case", SPLIT_CASES, ids=lambda c: f"{c[0]}-{c[1]}-{c[3]}{c[4]}-s{c[5]}")
+@pytest.mark.parametrize("case", SPLIT_CASES, ids=lambda c: f"{c[0]}-{c[1]}-{c[3]}{c[4]}-{c[7]}-s{c[5]}")
 def test_split_precision_form(cuda_ok, case):
-    """XTGEVC3_SPLIT: updates and back-transform as BF16-slice products on the tensor cores
-    (FP32 accumulation exact per 128-deep chunk, FP64 summation); solves stay FP64.  With 6
-    slices (~48 bits per operand) the result must match the FP64 oracle elementwise within
-    the stated tolerance (looser on the ill-conditioned stand-in pencil) and its residual
-    must meet the DGET52 bound used for the plain form."""
-    kind, n, seed, side, howmny, s, tol = case
+    """XTGEVC3_SPLIT: updates and back-transform as slice products on the tensor cores;
+    solves stay FP64.  BF16 slices: FP32 accumulation exact per 128-deep chunk, FP64
+    summation, 6 slices ~48 bits per operand.  INT8 slices (XTGEVC3_SPLIT_INT8): INT32
+    accumulation exact over the whole K, 7 slices ~49 bits.  The result must match the FP64
+    oracle elementwise within the stated tolerance (looser on the ill-conditioned stand-in
+    pencil) and its residual must meet the DGET52 bound used for the plain form."""
+    kind, n, seed, side, howmny, s, tol, sk = case
     p = _pencil(kind, n, seed, np.float64)
     d = dict(side=side, howmny=howmny, S=p["S"], P=p["P"], alpha=p["alpha"], beta=p["beta"], alphai=p["alphai"],
              VL_in=p["Q"], VR_in=p["Z"], name=kind)
     ref = oracle.tgevc3(side, howmny, d["S"], d["P"], d["alpha"], d["beta"], alphai=d["alphai"],
                         VL=p["Q"].copy(order="F"), VR=p["Z"].copy(order="F"))
-    X.set_flags(X.SPLIT | X.slices(s))
+    X.set_flags(X.SPLIT | X.slices(s) | (X.SPLIT_INT8 if sk == "int8" else 0))
     try:
         VL, VR, m, info = run_gpu(d)
     finally:

@@ -28,10 +28,11 @@ from . import build as _build
 NORMALIZE = 1
 SIMT = 2
 SPLIT = 4
+SPLIT_INT8 = 8
 
 
 def slices(s: int) -> int:
-    """Flag bits selecting s BF16 slices for the SPLIT form (1..6)."""
+    """Flag bits selecting s slices for the SPLIT form (BF16: 1..6, INT8: 1..7)."""
     return int(s) << 8
 
 _HERE = os.path.dirname(os.path.abspath(__file__))

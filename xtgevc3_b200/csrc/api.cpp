@@ -22,7 +22,8 @@ xtg::Options make_opts(unsigned flags)
     o.simt = (flags & XTGEVC3_SIMT) ? 1 : 0;
     if (flags & XTGEVC3_SPLIT) {
         const int s = (int)((flags >> 8) & 15u);
-        o.split = s > 0 ? s : 6;
+        o.split_kind = (flags & XTGEVC3_SPLIT_INT8) ? 1 : 0;
+        o.split = s > 0 ? s : (o.split_kind ? 7 : 6);
     }
     return o;
 }

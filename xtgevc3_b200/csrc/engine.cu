@@ -168,8 +168,10 @@ void configure_device(int dev)
                              2 * kBlock * kSmLd * (int)sizeof(cplx<float>));
         cudaFuncSetAttribute(gemm_dmma<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::SMEM_BYTES);
         cudaFuncSetAttribute(gemm_dmma<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::SMEM_BYTES);
-        cudaFuncSetAttribute(split::gemm_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             split::SMEM_BYTES);
+        cudaFuncSetAttribute(split::gemm_split_kernel<split::kBF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             split::Layout<split::kBF16>::SMEM_BYTES);
+        cudaFuncSetAttribute(split::gemm_split_kernel<split::kI8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             split::Layout<split::kI8>::SMEM_BYTES);
     });
 }
 
@@ -203,45 +205,50 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
     return fn;
 }
 
-// 2-D BF16 tensor map over a row-major [rows][cols] buffer, 64-byte swizzled boxes of
-// 32 columns (64 B, the swizzle span) by box_rows rows.
-static bool bf16_tensor_map(CUtensorMap *m, const void *base, int cols, int rows, int box_rows)
+// 2-D tensor map over a row-major [rows][cols] slice buffer: 64-byte swizzled boxes of one
+// 64-byte K row (32 BF16 or 64 INT8 elements) by box_rows rows.
+static bool slice_tensor_map(CUtensorMap *m, const void *base, int kind, int cols, int rows, int box_rows)
 {
     auto enc = tensor_map_encoder();
     if (!enc) return false;
+    const int esz = kind == split::kI8 ? 1 : 2;
     cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
-    cuuint32_t box[2] = {(cuuint32_t)split::BK, (cuuint32_t)box_rows};
+    cuuint64_t strides[1] = {(cuuint64_t)cols * esz};
+    cuuint32_t box[2] = {(cuuint32_t)(64 / esz), (cuuint32_t)box_rows};
     cuuint32_t es[2] = {1, 1};
-    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, es,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+    return enc(m, kind == split::kI8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+               const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // Reusable slice buffers of one side (grown on demand from the call's scratch).
 struct SplitBufs {
-    __nv_bfloat16 *A = nullptr, *B = nullptr;
+    unsigned char *A = nullptr, *B = nullptr;
     int *ea = nullptr, *eb = nullptr;
     size_t acap = 0, bcap = 0, ecap_a = 0, ecap_b = 0;
 };
 
-// C (+)= A B for a GemmArgs<double> launch, through BF16 slices and tcgen05 (see
-// kernels_split.cuh).  Returns a CUDA error code (cudaSuccess on success).
+// C (+)= A B for a GemmArgs<double> launch, through s slices of kind KIND on the tensor
+// cores (see kernels_split.cuh).  Returns a CUDA error code (cudaSuccess on success).
+template <int KIND>
 static cudaError_t launch_split(const GemmArgs<double> &g, int s, SplitBufs &sb, Scratch &scr, int *d_err,
                                 cudaStream_t st)
 {
     using namespace split;
-    const int Kp = round_up(g.K, BK), Mp = round_up(g.M, BM), Np = round_up(g.N, BN);
-    const size_t an = (size_t)s * Mp * Kp, bn = (size_t)s * Np * Kp;
-    if (an > sb.acap) { sb.A = scr.get<__nv_bfloat16>(an); sb.acap = an; }
-    if (bn > sb.bcap) { sb.B = scr.get<__nv_bfloat16>(bn); sb.bcap = bn; }
+    using Elem = typename Cfg<KIND>::Elem;
+    constexpr int KBK = Cfg<KIND>::BK, KBN = Cfg<KIND>::BN;
+    const int Kp = round_up(g.K, KBK), Mp = round_up(g.M, BM), Np = round_up(g.N, KBN);
+    const size_t an = (size_t)s * Mp * Kp * sizeof(Elem), bn = (size_t)s * Np * Kp * sizeof(Elem);
+    if (an > sb.acap) { sb.A = scr.get<unsigned char>(an); sb.acap = an; }
+    if (bn > sb.bcap) { sb.B = scr.get<unsigned char>(bn); sb.bcap = bn; }
     if ((size_t)Mp > sb.ecap_a) { sb.ea = scr.get<int>(Mp); sb.ecap_a = Mp; }
     if ((size_t)Np > sb.ecap_b) { sb.eb = scr.get<int>(Np); sb.ecap_b = Np; }
     if (scr.err) return scr.err;
-    slice_rows_kernel<<<Mp / 32, 256, 0, st>>>(g, Kp, Mp, s, sb.A, sb.ea);
-    slice_cols_kernel<<<Np / 8, 256, 0, st>>>(g, Kp, Np, s, sb.B, sb.eb);
+    slice_rows_kernel<KIND><<<Mp / 32, 256, 0, st>>>(g, Kp, Mp, s, reinterpret_cast<Elem *>(sb.A), sb.ea);
+    slice_cols_kernel<KIND><<<Np / 8, 256, 0, st>>>(g, Kp, Np, s, reinterpret_cast<Elem *>(sb.B), sb.eb);
     CUtensorMap tmA, tmB;
-    if (!bf16_tensor_map(&tmA, sb.A, Kp, s * Mp, BM) || !bf16_tensor_map(&tmB, sb.B, Kp, s * Np, BN))
+    if (!slice_tensor_map(&tmA, sb.A, KIND, Kp, s * Mp, BM) || !slice_tensor_map(&tmB, sb.B, KIND, Kp, s * Np, KBN))
         return cudaErrorInvalidValue;
     Params p;
     p.M = g.M;
@@ -259,7 +266,7 @@ static cudaError_t launch_split(const GemmArgs<double> &g, int s, SplitBufs &sb,
     p.ldc = g.ldc;
     p.ccol = g.ccol;
     p.err = d_err;
-    gemm_split_kernel<<<dim3(Mp / BM, Np / BN), THREADS, SMEM_BYTES, st>>>(tmA, tmB, p);
+    gemm_split_kernel<KIND><<<dim3(Mp / BM, Np / KBN), THREADS, Layout<KIND>::SMEM_BYTES, st>>>(tmA, tmB, p);
     return cudaGetLastError();
 }
 
@@ -329,9 +336,9 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
     R *d_sums = scr.get<R>(2 * (size_t)n);
     R *d_norms = scr.get<R>(2);
     // split-precision GEMMs: real double only; their bounded waits report through d_err
-    const int nsplit = (!CPLX && std::is_same<R, double>::value && opt.split > 0)
-                           ? std::min(opt.split, (int)split::MAXS)
-                           : 0;
+    const int split_max = opt.split_kind == split::kI8 ? split::Cfg<split::kI8>::MAXS : split::Cfg<split::kBF16>::MAXS;
+    const int nsplit = (!CPLX && std::is_same<R, double>::value && opt.split > 0) ? std::min(opt.split, split_max)
+                                                                                 : 0;
     int *d_err = nsplit ? scr.get<int>(1) : nullptr;
     if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
     if (d_err) XTG_CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
@@ -364,7 +371,9 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
                 // launches with few output rows (the update of the upper block of a pair) do
                 // too little work per tile to amortise slicing and the tensor-core pipeline
                 if (nsplit && g.M - g.mlo >= 512) {
-                    cudaError_t e = launch_split(g, nsplit, sbuf, scr, d_err, st);
+                    cudaError_t e = opt.split_kind == split::kI8
+                                        ? launch_split<split::kI8>(g, nsplit, sbuf, scr, d_err, st)
+                                        : launch_split<split::kBF16>(g, nsplit, sbuf, scr, d_err, st);
                     if (e != cudaSuccess) split_err = e;
                     return;
                 }

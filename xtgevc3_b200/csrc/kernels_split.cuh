@@ -46,23 +46,47 @@
 namespace xtg {
 namespace split {
 
-constexpr int BM = 128, BN = 96, BK = 32;    // output tile, K step of one TMA box
-constexpr int CHUNK = 128;                    // K per exact FP32 accumulation
-constexpr int MAXS = 6;                       // slices supported
-constexpr int NACC = 5;                       // TMEM accumulators (diagonals 0, 1, 2, 3, >= 4)
-constexpr int ASTAGES = 8;
-constexpr int A_TILE = BM * BK * 2;           // bytes per A slice tile (8 KiB)
-constexpr int B_TILE = BN * BK * 2;           // bytes per B slice tile (6 KiB, a multiple of the 512-B atom)
+constexpr int BM = 128;                      // output rows per CTA (one TMEM lane each)
 constexpr int THREADS = 320;
 constexpr int EPI_WARPS = 8;
-constexpr int EPI_COLS = BN / 2;              // columns per epilogue thread
 constexpr long long kSpinLimit = 1ll << 22;  // bounded mbarrier polls (legitimate waits are microseconds)
-static_assert(NACC * BN <= 512, "accumulators exceed TMEM");
 
-// dynamic shared memory: [B buffers: 2 x MAXS tiles][A ring: ASTAGES tiles], 1024-aligned
-constexpr int SMEM_B = 2 * MAXS * B_TILE;
-constexpr int SMEM_A = ASTAGES * A_TILE;
-constexpr int SMEM_BYTES = SMEM_B + SMEM_A + 1024;  // + alignment slack
+// Slice kinds.  Both move 64-byte K rows (one 64-byte swizzle span) per TMA box and issue
+// two 32-byte-deep MMAs per K step.
+//   kBF16: BF16 slices (8-bit digits) on kind::f16 with FP32 accumulators; diagonals
+//          0..3 exact per 128-deep K chunk, diagonals >= 4 shared (see above).
+//   kI8:   INT8 slices (7-bit digits) on kind::i8 with INT32 accumulators, one per
+//          diagonal, exact over any K up to 2^15 (|digit| <= 64, at most 7 products per
+//          diagonal: 7 * 2^12 * 2^15 < 2^31), so K is never chunked.
+enum SliceKind : int { kBF16 = 0, kI8 = 1 };
+
+template <int KIND> struct Cfg;
+template <> struct Cfg<kBF16> {
+    using Elem = __nv_bfloat16;
+    static constexpr int BN = 96, BK = 32, CHUNK = 128, MAXS = 6, NACC = 5, ASTAGES = 8;
+    // BF16 x BF16 -> FP32, K-major A and B, M = BM, N = BN
+    static constexpr uint32_t IDESC =
+        (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+};
+template <> struct Cfg<kI8> {
+    using Elem = int8_t;
+    static constexpr int BN = 64, BK = 64, CHUNK = 32768, MAXS = 7, NACC = 7, ASTAGES = 12;
+    // S8 x S8 -> S32, K-major A and B, M = BM, N = BN
+    static constexpr uint32_t IDESC =
+        (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+};
+
+template <int KIND> struct Layout {
+    using C = Cfg<KIND>;
+    static constexpr int A_TILE = BM * 64;        // bytes per A slice tile (64-byte K rows)
+    static constexpr int B_TILE = C::BN * 64;     // bytes per B slice tile (a multiple of the 512-B atom)
+    static constexpr int EPI_COLS = C::BN / 2;    // columns per epilogue thread
+    // dynamic shared memory: [B buffers: 2 x MAXS tiles][A ring: ASTAGES tiles], 1024-aligned
+    static constexpr int SMEM_B = 2 * C::MAXS * B_TILE;
+    static constexpr int SMEM_A = C::ASTAGES * A_TILE;
+    static constexpr int SMEM_BYTES = SMEM_B + SMEM_A + 1024;  // + alignment slack
+    static_assert(C::NACC * C::BN <= 512, "accumulators exceed TMEM");
+};
 
 struct Params {
     int M, N, Kp, s;          // Kp: padded K (multiple of BK) of the slice buffers
@@ -142,41 +166,50 @@ __device__ __forceinline__ uint64_t smem_desc(const void *tile, int kbyte_off)
     return d;
 }
 
-// kind::f16 instruction descriptor: BF16 x BF16 -> FP32, K-major A and B, M = BM, N = BN
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
-
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate)
+template <int KIND>
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate)
 {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+    if constexpr (KIND == kBF16)
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+            ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(Cfg<KIND>::IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0),
+            "r"(0));
+    else
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+            ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(Cfg<KIND>::IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0),
+            "r"(0));
 }
 __device__ __forceinline__ void umma_commit(uint64_t *bar)
 {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
 }
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
 {
-    uint32_t r[16];
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
-#pragma unroll
-    for (int q = 0; q < 16; q++) v[q] = __uint_as_float(r[q]);
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
 // ---- the MMA kernel ---------------------------------------------------------------------
+template <int KIND>
 __global__ void __launch_bounds__(THREADS, 1)
 gemm_split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Params p)
 {
+    using C = Cfg<KIND>;
+    using L = Layout<KIND>;
+    constexpr int BN = C::BN, BK = C::BK, CHUNK = C::CHUNK, MAXS = C::MAXS, NACC = C::NACC, ASTAGES = C::ASTAGES;
+    constexpr int A_TILE = L::A_TILE, B_TILE = L::B_TILE, EPI_COLS = L::EPI_COLS, SMEM_B = L::SMEM_B;
     extern __shared__ __align__(16) unsigned char smem_split[];
     // tiles need 512-byte alignment (64-byte swizzle atoms); SMEM_BYTES includes the slack
     unsigned char *base = reinterpret_cast<unsigned char *>(((uintptr_t)smem_split + 1023) & ~(uintptr_t)1023);
@@ -301,9 +334,9 @@ gemm_split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                             // the first product into each accumulator of a chunk overwrites it
                             const bool first = tt == 0 && i == 0 && j <= NACC - 1;
 #pragma unroll
-                            for (int kk = 0; kk < BK / 16; kk++)
-                                umma_bf16(dcol, smem_desc(at, kk * 32), smem_desc(bt, kk * 32),
-                                          (first && kk == 0) ? 0u : 1u);
+                            for (int kk = 0; kk < 2; kk++)  // two 32-byte-deep MMAs per 64-byte K step
+                                umma<KIND>(dcol, smem_desc(at, kk * 32), smem_desc(bt, kk * 32),
+                                           (first && kk == 0) ? 0u : 1u);
                         }
                         umma_commit(&a_empty[astage]);
                         astage = (astage + 1) % ASTAGES;
@@ -330,13 +363,18 @@ gemm_split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
             fph ^= 1;
             tc_fence_after();
             for (int g = 0; g < nacc; g++) {
+                // BF16 slices carry their scale 256^-i; INT8 digits are integers: 2^-7g here
+                const double w = KIND == kI8 ? ldexp(1.0, -7 * g) : 1.0;
 #pragma unroll
                 for (int h = 0; h < EPI_COLS / 16; h++) {
-                    float v[16];
+                    uint32_t v[16];
                     tmem_ld16(tbase + (uint32_t)(g * BN + h * 16), v);
                     tmem_wait_ld();
 #pragma unroll
-                    for (int q = 0; q < 16; q++) acc[h * 16 + q] += (double)v[q];
+                    for (int q = 0; q < 16; q++) {
+                        if constexpr (KIND == kI8) acc[h * 16 + q] += w * (double)(int)v[q];
+                        else acc[h * 16 + q] += (double)__uint_as_float(v[q]);
+                    }
                 }
             }
             tc_fence_before();
@@ -344,7 +382,7 @@ gemm_split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
             if (lane == 0) mbar_arrive(&acc_empty);
         }
         if (!abort_flag && row >= p.mlo && row < p.M) {
-            const int er = p.ea[row] - 16;
+            const int er = p.ea[row] - (KIND == kI8 ? 12 : 16);
 #pragma unroll
             for (int q = 0; q < EPI_COLS; q++) {
                 const int col = n0 + half * EPI_COLS + q;
@@ -369,21 +407,34 @@ gemm_split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
 // exponent e with 2^-e max in [0.5, 1) (0 for a zero vector)
 __device__ __forceinline__ int scale_exp(double mx) { return mx > 0.0 ? ilogb(mx) + 1 : 0; }
 
-// v in (-1, 1) -> s pre-scaled slices a_i 256^-i (see the header comment)
-__device__ __forceinline__ void slice_value(double v, int s, __nv_bfloat16 *out, size_t stride)
+// v in (-1, 1) -> s slices.  BF16: pre-scaled a_i 256^-i with t_0 = 256 v (see the header
+// comment).  INT8: integer digits a_i with t_0 = 64 v, t_(i+1) = 128 (t_i - a_i), so that
+// v = sum_i a_i 2^(-6-7i) + O(2^(-7s)) and |a_i| <= 64.
+template <int KIND>
+__device__ __forceinline__ void slice_value(double v, int s, typename Cfg<KIND>::Elem *out, size_t stride)
 {
-    double t = v * 256.0;
-    for (int i = 0; i < s; i++) {
-        const double a = rint(t);
-        t = (t - a) * 256.0;
-        out[(size_t)i * stride] = __double2bfloat16(ldexp(a, -8 * i));
+    if constexpr (KIND == kBF16) {
+        double t = v * 256.0;
+        for (int i = 0; i < s; i++) {
+            const double a = rint(t);
+            t = (t - a) * 256.0;
+            out[(size_t)i * stride] = __double2bfloat16(ldexp(a, -8 * i));
+        }
+    } else {
+        double t = v * 64.0;
+        for (int i = 0; i < s; i++) {
+            const double a = rint(t);
+            t = (t - a) * 128.0;
+            out[(size_t)i * stride] = (int8_t)(int)a;
+        }
     }
 }
 
 // Rows of A (through the segment description of a GEMM launch) -> slices
 // out[i][row][k] (row pitch Kp, i-th block of Mp rows), ea[row].  One CTA = 32 rows.
+template <int KIND>
 __global__ void __launch_bounds__(256) slice_rows_kernel(GemmArgs<double> g, int Kp, int Mp, int s,
-                                                         __nv_bfloat16 *out, int *ea)
+                                                         typename Cfg<KIND>::Elem *out, int *ea)
 {
     __shared__ double tile[64][33];
     __shared__ double rmax[8][32];
@@ -431,7 +482,7 @@ __global__ void __launch_bounds__(256) slice_rows_kernel(GemmArgs<double> g, int
             for (int h = 0; h < 2; h++) {
                 const int kk = tx + 32 * h;
                 if (k0 + kk >= Kp) continue;
-                slice_value(tile[kk][rr], s, out + (size_t)gr * Kp + k0 + kk, (size_t)Mp * Kp);
+                slice_value<KIND>(tile[kk][rr], s, out + (size_t)gr * Kp + k0 + kk, (size_t)Mp * Kp);
             }
         }
         __syncthreads();
@@ -440,8 +491,9 @@ __global__ void __launch_bounds__(256) slice_rows_kernel(GemmArgs<double> g, int
 
 // Columns of B (rows through the segment offsets) -> slices out[j][col][k], eb[col].
 // One warp per column, lanes along K.
+template <int KIND>
 __global__ void __launch_bounds__(256) slice_cols_kernel(GemmArgs<double> g, int Kp, int Np, int s,
-                                                         __nv_bfloat16 *out, int *eb)
+                                                         typename Cfg<KIND>::Elem *out, int *eb)
 {
     const int col = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -462,7 +514,7 @@ __global__ void __launch_bounds__(256) slice_cols_kernel(GemmArgs<double> g, int
     const int e = scale_exp(mx);
     if (lane == 0) eb[col] = e;
     for (int k = lane; k < Kp; k += 32)
-        slice_value(ldexp(bval(k), -e), s, out + (size_t)col * Kp + k, (size_t)Np * Kp);
+        slice_value<KIND>(ldexp(bval(k), -e), s, out + (size_t)col * Kp + k, (size_t)Np * Kp);
 }
 
 }  // namespace split
