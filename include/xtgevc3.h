@@ -49,6 +49,11 @@ extern "C" {
 /* With XTGEVC3_SPLIT: INT8 slices (7-bit digits, s in [1, 7], default 7, ~49 bits per
  * operand) on the INT8 tensor cores with exact INT32 accumulation over the whole K. */
 #define XTGEVC3_SPLIT_INT8 8u
+/* Look-ahead schedule: the trailing update of each pair of row blocks runs on a second
+ * stream while the next pair's diagonal solves run (guard rescaling of the rows that
+ * update writes is deferred until it has finished).  Same results bit for bit; on B200
+ * it measured no faster (the update fills the GPU), so it is off by default. */
+#define XTGEVC3_LOOKAHEAD 16u
 
 /* Process-wide flags used by the drop-in entry points below (default 0). */
 void xtgevc3_set_flags(unsigned flags);

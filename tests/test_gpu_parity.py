@@ -241,3 +241,51 @@ def test_split_precision_form(cuda_ok, case):
         X.set_flags(0)
     assert (m, info) == (ref[2], ref[3])
     compare(d, VL, VR, m, ref[0], ref[1], tol, check_resid=(howmny == "A"))
+
+
+def _overflow_pencil(n, seed, jump, left):
+    """Real triangular pencil whose eigenvectors grow by ~jump once per 64-row block: the
+    strictly upper part of one row per block (right eigenvectors) or of one column per
+    block (left eigenvectors) is scaled by jump.  Over a column the growth passes the
+    overflow threshold many times over, so the overflow guards rescale many columns, while
+    within one row block it stays representable."""
+    rng = np.random.default_rng(seed)
+    S = np.triu(rng.standard_normal((n, n)), 1)
+    if left:
+        S[:, np.arange(31, n, 64)] *= jump
+    else:
+        S[np.arange(n - 32, 0, -64), :] *= jump
+    S = np.triu(S, 1)
+    S[np.diag_indices(n)] = np.arange(1, n + 1) * (1 + 0.1 * rng.random(n))
+    P = np.triu(rng.standard_normal((n, n)), 1) * 1e-3
+    P[np.diag_indices(n)] = 1.0 + rng.random(n)
+    S, P = np.asfortranarray(S), np.asfortranarray(P)
+    return S, P, np.diag(S).copy(), np.zeros(n), np.diag(P).copy()
+
+
+@pytest.mark.parametrize("side", ["R", "L"])
+def test_lookahead_matches_serial_path_with_guards(cuda_ok, side):
+    """The look-ahead schedule (XTGEVC3_LOOKAHEAD: trailing updates on a second stream,
+    guard scaling of the rows they write deferred to a later kernel) must give
+    bit-identical numbers to the default serial schedule, also when the overflow guards
+    rescale many columns, and must match the oracle column by column after normalisation
+    (the oracle rescales whole 32-column panels where this implementation rescales single
+    columns)."""
+    n = 1536
+    S, P, ar, ai, be = _overflow_pencil(n, 91, 1e16, side == "L")
+    I = np.eye(n, order="F")
+    d = dict(side=side, howmny="A", S=S, P=P, alpha=ar, beta=be, alphai=ai, VL_in=I, VR_in=I.copy(order="F"),
+             name="overflow")
+    X.set_flags(X.LOOKAHEAD)
+    try:
+        VL0, VR0, m, info = run_gpu(d)
+    finally:
+        X.set_flags(0)
+    V0 = VL0 if side == "L" else VR0
+    assert info == 0 and np.isfinite(V0).all()
+    # the guards fired: columns come back with their seed entry x_k scaled below 1
+    assert (np.abs(np.diag(V0[:, :n])) < 1).sum() >= 8
+    VL1, VR1, _, _ = run_gpu(d)  # the default, serial schedule
+    np.testing.assert_array_equal(V0, VL1 if side == "L" else VR1)
+    ref = oracle.tgevc3(side, "A", S, P, ar, be, alphai=ai)
+    compare(d, VL0, VR0, m, ref[0], ref[1], TOL_ILL[np.float64], check_resid=False)

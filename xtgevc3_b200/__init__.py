@@ -29,6 +29,7 @@ NORMALIZE = 1
 SIMT = 2
 SPLIT = 4
 SPLIT_INT8 = 8
+LOOKAHEAD = 16
 
 
 def slices(s: int) -> int:

@@ -209,6 +209,8 @@ int adjoint_device(int n, const void *S_, int lds, const void *P_, int ldp, cons
         da.ldy = ldy;
         da.thr_rhs = da.thr_upd = R(0);
         da.left_seed = 0;
+        da.pending = nullptr;
+        da.safe_lo = 0;
         const int grid = std::max(1, std::min((da.nitems - da.it0 + 7) / 8, 2 * 148));
         if constexpr (CPLX) diag_adjoint_cplx<R><<<grid, 256, diag_smem, st>>>(da);
         else diag_adjoint_real<R><<<grid, 256, diag_smem, st>>>(da);

@@ -20,6 +20,7 @@ xtg::Options make_opts(unsigned flags)
     xtg::Options o;
     o.normalize = (flags & XTGEVC3_NORMALIZE) ? 1 : 0;
     o.simt = (flags & XTGEVC3_SIMT) ? 1 : 0;
+    o.lookahead = (flags & XTGEVC3_LOOKAHEAD) ? 1 : 0;
     if (flags & XTGEVC3_SPLIT) {
         const int s = (int)((flags >> 8) & 15u);
         o.split_kind = (flags & XTGEVC3_SPLIT_INT8) ? 1 : 0;

@@ -29,6 +29,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <type_traits>
@@ -366,19 +367,20 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         SplitBufs sbuf;
         cudaError_t split_err = cudaSuccess;
         // C (+)= A B of one update or back-transform launch, FP64 DMMA/SIMT or BF16 slices
-        auto gemm = [&](const GemmArgs<E> &g) {
+        auto gemm = [&](const GemmArgs<E> &g, cudaStream_t gs) {
             if constexpr (std::is_same<E, double>::value) {
                 // launches with few output rows (the update of the upper block of a pair) do
-                // too little work per tile to amortise slicing and the tensor-core pipeline
+                // too little work per tile to amortise slicing and the tensor-core pipeline;
+                // they never use the slice buffers, so the buffers have one user stream
                 if (nsplit && g.M - g.mlo >= 512) {
                     cudaError_t e = opt.split_kind == split::kI8
-                                        ? launch_split<split::kI8>(g, nsplit, sbuf, scr, d_err, st)
-                                        : launch_split<split::kBF16>(g, nsplit, sbuf, scr, d_err, st);
+                                        ? launch_split<split::kI8>(g, nsplit, sbuf, scr, d_err, gs)
+                                        : launch_split<split::kBF16>(g, nsplit, sbuf, scr, d_err, gs);
                     if (e != cudaSuccess) split_err = e;
                     return;
                 }
             }
-            launch_gemm<E>(g, opt.simt != 0, st);
+            launch_gemm<E>(g, opt.simt != 0, gs);
         };
         // ---- column list in problem orientation ---------------------------------------
         ColList L;
@@ -443,8 +445,16 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         for (int c = 0; c < m; c++)
             if (L.kind[c] != kPairIm) items.push_back(c);
         const int nitems = (int)items.size();
+        // look-ahead (XTGEVC3_LOOKAHEAD): the trailing update of a block pair runs on a second
+        // stream while the next pair is solved (see the loop below); off while tracing
+        // (clean per-kernel times) and in arena mode (fixed scratch)
+        const bool ahead = opt.lookahead && !tr.on && !opt.arena && blocks.size() >= 3;
         E *X = scr.get<E>((size_t)ldx * m);
-        E *Y = scr.get<E>((size_t)ldy * m);
+        E *Ybuf[2];
+        Ybuf[0] = scr.get<E>((size_t)ldy * m);
+        Ybuf[1] = ahead ? scr.get<E>((size_t)ldy * m) : Ybuf[0];
+        E *Y = Ybuf[0];
+        R *pending = ahead ? scr.get<R>((size_t)m) : nullptr;
         R *coef = scr.get<R>((size_t)ncoef * m);
         int *d_ints = scr.get<int>(5 * (size_t)m);
         uint8_t *d_kind = scr.get<uint8_t>((size_t)m);
@@ -460,6 +470,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         const int *d_colk = d_ints, *d_src = d_ints + m, *d_kext = d_ints + 2 * m, *d_outcol = d_ints + 3 * m;
         const int *d_items = d_ints + 4 * m;
         XTG_CK(cudaMemsetAsync(X, 0, (size_t)ldx * m * sizeof(E), st));
+        if (pending) fill_one_kernel<R><<<(m + 255) / 256, 256, 0, st>>>(pending, m);
 
         tr.run(kTPrep, 0, (double)m * ncoef * sizeof(R), st, [&] {
             if constexpr (CPLX) {
@@ -493,7 +504,8 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             return sg;
         };
         // X[w0 + mlo : w0 + M, c0:m] += sum over segments
-        auto update = [&](int w0, int mlo, int M, int c0, int nseg, const GemmSeg<E> *segs, double kflops) {
+        auto update = [&](int w0, int mlo, int M, int c0, int nseg, const GemmSeg<E> *segs, double kflops,
+                          cudaStream_t us) {
             GemmArgs<E> g;
             g.M = M;
             g.N = m - c0;
@@ -515,9 +527,10 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             const double rows = M - mlo;
             const double uf = 2.0 * rows * g.N * kflops * cfl;
             const double ub = (2.0 * rows * g.N + rows * kflops + kflops * g.N) * esz;
-            tr.run(kTUpdate, uf, ub, st, [&] { gemm(g); });
+            tr.run(kTUpdate, uf, ub, us, [&] { gemm(g, us); });
         };
-        auto diag_solve = [&](int r0, int r1, int ys_off, int yhalf, int zl_off, int zl_len) {
+        // safe_lo >= 0: deferred guard scaling of the rows above safe_lo (look-ahead)
+        auto diag_solve = [&](int r0, int r1, int ys_off, int yhalf, int zl_off, int zl_len, int safe_lo) {
             const int jnb = r1 - r0;
             const int c0 = first_col(r0);
             if (c0 >= m) return;
@@ -548,6 +561,8 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             da.thr_rhs = bignum / R(10);
             da.thr_upd = bignum / R(std::max(1, jnb));
             da.left_seed = left ? 1 : 0;
+            da.pending = safe_lo >= 0 ? pending : nullptr;
+            da.safe_lo = safe_lo;
             const int grid = std::max(1, std::min((nitems - da.it0 + 7) / 8, 2 * 148));
             // algorithmic work of the shifted solves: ~2 nrows^2 real flops per real column,
             // 4x that per complex column or (Re, Im) pair; bytes: rhs in, solution and
@@ -567,37 +582,119 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             });
         };
         const int nbk = (int)blocks.size();
+        // Look-ahead (ahead == true).  Pair p owns rows [u0_p, l1_p); the next pair's rows are
+        // [a0, u0_p).  On the main stream: solve L_p, small update of U_p, solve U_p; wait for
+        // the trailing update of pair p-1 (it writes rows [0, u0_p)); apply deferred guard
+        // factors to rows [0, u0_p); update the next pair's rows [a0, u0_p) (small GEMM).  On
+        // the second stream: the trailing update of rows [0, a0), which overlaps the solves of
+        // pair p+1.  Pairs alternate between two update operands Y; a solve defers guard
+        // scaling of rows [0, u0_p), the only rows the concurrent update writes.
+        cudaStream_t st2 = nullptr;
+        cudaEvent_t ev_main = nullptr, ev_tr = nullptr;
+        struct Guard {
+            cudaStream_t &s;
+            cudaEvent_t &a, &b;
+            ~Guard()
+            {
+                if (a) cudaEventDestroy(a);
+                if (b) cudaEventDestroy(b);
+                if (s) cudaStreamDestroy(s);
+            }
+        } guard{st2, ev_main, ev_tr};
+        if (ahead) {
+            // slice buffers of the trailing updates are sized here, on the main stream: growing
+            // them inside a launch on the second stream would not be ordered with its use
+            if constexpr (std::is_same<E, double>::value) {
+                if (nsplit) {
+                    const int kmax = 4 * kBlock;
+                    auto reserve = [&](int bk, int bn, size_t esz_) {
+                        const size_t an = (size_t)nsplit * round_up(n, split::BM) * round_up(kmax, bk) * esz_;
+                        const size_t bn_ = (size_t)nsplit * round_up(m, bn) * round_up(kmax, bk) * esz_;
+                        if (an > sbuf.acap) { sbuf.A = scr.get<unsigned char>(an); sbuf.acap = an; }
+                        if (bn_ > sbuf.bcap) { sbuf.B = scr.get<unsigned char>(bn_); sbuf.bcap = bn_; }
+                        const size_t mp = round_up(n, split::BM), np = round_up(m, bn);
+                        if (mp > sbuf.ecap_a) { sbuf.ea = scr.get<int>(mp); sbuf.ecap_a = mp; }
+                        if (np > sbuf.ecap_b) { sbuf.eb = scr.get<int>(np); sbuf.ecap_b = np; }
+                    };
+                    if (opt.split_kind == split::kI8)
+                        reserve(split::Cfg<split::kI8>::BK, split::Cfg<split::kI8>::BN, 1);
+                    else
+                        reserve(split::Cfg<split::kBF16>::BK, split::Cfg<split::kBF16>::BN, 2);
+                    if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
+                }
+            }
+            XTG_CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+            XTG_CK(cudaEventCreateWithFlags(&ev_main, cudaEventDisableTiming));
+            XTG_CK(cudaEventCreateWithFlags(&ev_tr, cudaEventDisableTiming));
+        }
+        bool tr_pending = false;  // a trailing update is queued on st2 and not yet waited for
+        int pidx = 0;
         for (int bi = 0; bi < nbk;) {
             const int l0 = blocks[bi].first, l1 = blocks[bi].second, jl = l1 - l0, bl = round_up(jl, kKPad);
+            Y = Ybuf[pidx & 1];
             if (bi + 1 == nbk) {  // unpaired top block
-                diag_solve(l0, l1, 0, bl, 0, 0);
+                if (tr_pending) {
+                    XTG_CK(cudaStreamWaitEvent(st, ev_tr, 0));
+                    tr_pending = false;
+                    apply_pending_kernel<E, R><<<(m * 32 + 255) / 256, 256, 0, st>>>(X, ldx, pending, m, l1);
+                }
+                diag_solve(l0, l1, 0, bl, 0, 0, -1);
                 const int c0 = first_col(l0);
                 if (l0 > 0 && c0 < m) {
                     GemmSeg<E> sg[2] = {strip(Sp, lsp, 0, l0, jl, 0), strip(Pp, lpp, 0, l0, jl, bl)};
-                    update(0, 0, l0, c0, 2, sg, 2.0 * jl);
+                    update(0, 0, l0, c0, 2, sg, 2.0 * jl, st);
                 }
                 XTG_CK(cudaGetLastError());
                 bi += 1;
                 continue;
             }
             const int u0 = blocks[bi + 1].first, ju = l0 - u0, bu = round_up(ju, kKPad), bh = bu + bl;
-            diag_solve(l0, l1, bu, bh, 0, 0);
+            const int safe = ahead ? u0 : -1;
+            diag_solve(l0, l1, bu, bh, 0, 0, safe);
             const int c0l = first_col(l0);
             if (c0l < m) {  // rows of U (window from an even row) += L's contribution
                 const int w0 = u0 & ~1, mlo = u0 & 1;
                 GemmSeg<E> sg[2] = {strip(Sp, lsp, w0, l0, jl, bu), strip(Pp, lpp, w0, l0, jl, bh + bu)};
-                update(w0, mlo, mlo + ju, c0l, 2, sg, 2.0 * jl);
+                update(w0, mlo, mlo + ju, c0l, 2, sg, 2.0 * jl, st);
             }
-            diag_solve(u0, l0, 0, bh, bu, bl);
+            diag_solve(u0, l0, 0, bh, bu, bl, safe);
             const int c0u = first_col(u0);
-            if (u0 > 0 && c0u < m) {
-                GemmSeg<E> sg[4] = {strip(Sp, lsp, 0, u0, ju, 0), strip(Sp, lsp, 0, l0, jl, bu),
-                                    strip(Pp, lpp, 0, u0, ju, bh), strip(Pp, lpp, 0, l0, jl, bh + bu)};
-                update(0, 0, u0, c0u, 4, sg, 2.0 * (ju + jl));
+            if (!ahead) {
+                if (u0 > 0 && c0u < m) {
+                    GemmSeg<E> sg[4] = {strip(Sp, lsp, 0, u0, ju, 0), strip(Sp, lsp, 0, l0, jl, bu),
+                                        strip(Pp, lpp, 0, u0, ju, bh), strip(Pp, lpp, 0, l0, jl, bh + bu)};
+                    update(0, 0, u0, c0u, 4, sg, 2.0 * (ju + jl), st);
+                }
+            } else {
+                if (tr_pending) {
+                    XTG_CK(cudaStreamWaitEvent(st, ev_tr, 0));
+                    tr_pending = false;
+                }
+                if (u0 > 0) apply_pending_kernel<E, R><<<(m * 32 + 255) / 256, 256, 0, st>>>(X, ldx, pending, m, u0);
+                if (u0 > 0 && c0u < m) {
+                    // the next pair's rows [a0, u0): its U block's start, or the top block's
+                    const int a0 = bi + 3 < nbk ? blocks[bi + 3].first : blocks[bi + 2].first;
+                    const int w0 = a0 & ~1, mlo = a0 & 1;
+                    GemmSeg<E> sa[4] = {strip(Sp, lsp, w0, u0, ju, 0), strip(Sp, lsp, w0, l0, jl, bu),
+                                        strip(Pp, lpp, w0, u0, ju, bh), strip(Pp, lpp, w0, l0, jl, bh + bu)};
+                    update(w0, mlo, mlo + (u0 - a0), c0u, 4, sa, 2.0 * (ju + jl), st);
+                    if (a0 > 0) {
+                        XTG_CK(cudaEventRecord(ev_main, st));
+                        XTG_CK(cudaStreamWaitEvent(st2, ev_main, 0));
+                        GemmSeg<E> sg[4] = {strip(Sp, lsp, 0, u0, ju, 0), strip(Sp, lsp, 0, l0, jl, bu),
+                                            strip(Pp, lpp, 0, u0, ju, bh), strip(Pp, lpp, 0, l0, jl, bh + bu)};
+                        update(0, 0, a0, c0u, 4, sg, 2.0 * (ju + jl), st2);
+                        XTG_CK(cudaEventRecord(ev_tr, st2));
+                        tr_pending = true;
+                    }
+                }
             }
             XTG_CK(cudaGetLastError());
             bi += 2;
+            pidx += 1;
         }
+        // every deferred factor was applied within its own pair (the top block scales at once)
+        if (tr_pending) XTG_CK(cudaStreamWaitEvent(st, ev_tr, 0));
 
         // ---- write-back / back-transform -----------------------------------------------------
         E *V = left ? VL : VR;
@@ -633,7 +730,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             for (int c = 0; c < m; c++) bk += L.kext[c];
             bf = 2.0 * n * bk * cfl;
             const double bb = ((double)n * L.kext[m - 1] + bk + (double)n * m) * esz;
-            tr.run(kTBack, bf, bb, st, [&] { gemm(g); });
+            tr.run(kTBack, bf, bb, st, [&] { gemm(g, st); });
         } else {
             dim3 g(std::max(1, std::min((n + 255) / 256, 64)), m);
             tr.run(kTWriteback, 0, 2.0 * n * m * esz, st, [&] {

@@ -11,6 +11,7 @@ struct Options {
     int simt = 0;       // force the SIMT GEMM kernels instead of the tensor-core kernel
     int split = 0;      // > 0: FP64 GEMMs (real double) as slice products with this many slices
     int split_kind = 0; // 0: BF16 slices (kind::f16), 1: INT8 slices (kind::i8)
+    int lookahead = 0;  // trailing updates on a second stream, overlapping the next solves
     // When set, all device scratch of the call is carved from this buffer (nothing is
     // allocated) and the two sides run one after the other on the caller's stream.
     void *arena = nullptr;

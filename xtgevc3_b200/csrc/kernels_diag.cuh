@@ -114,6 +114,11 @@ struct DiagArgs {
     int ldy;
     R thr_rhs, thr_upd;
     int left_seed;           // 2x2 seed of the left problem (see the pair branch)
+    // Deferred guard scaling (nullable).  When set, a guard rescales the rows of a column
+    // above the block only down to row safe_lo and multiplies pending[c] by the factor; the
+    // caller applies pending to rows [0, safe_lo) once no other kernel writes them.
+    R *pending;
+    int safe_lo;
 };
 
 // Multiply rows [a, b) of one column by s (warp-cooperative).  Used on the rows of a
@@ -122,6 +127,19 @@ template <class E, class R>
 __device__ __forceinline__ void scale_rows(E *col, int a, int b, R s, int lane)
 {
     for (int i = a + lane; i < b; i += 32) col[i] = s * col[i];
+}
+
+// Guard rescaling of the rows above the block [0, r0) of column c: all of them at once,
+// or (deferred mode) rows [safe_lo, r0) now and the rest through pending[c].
+template <class E, class R>
+__device__ __forceinline__ void scale_above(const DiagArgs<R> &a, E *col, int c, R s, int lane)
+{
+    if (!a.pending) {
+        scale_rows(col, 0, a.r0, s, lane);
+        return;
+    }
+    scale_rows(col, a.safe_lo < a.r0 ? a.safe_lo : a.r0, a.r0, s, lane);
+    if (lane == 0) a.pending[c] *= s;
 }
 
 // Write this block's rows of one update-operand column: ys = -ac x, yp = b x for rows
@@ -301,7 +319,7 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
                 if (mx > a.thr_rhs) {
                     R sc = a.thr_rhs / mx;
                     r[0] *= sc; r[1] *= sc; seed *= sc;
-                    if (!diag) { scale_rows(colr, 0, a.r0, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane); }
+                    if (!diag) { scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane); }
                 }
             }
             Factors<R> F;
@@ -318,7 +336,7 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
             if (mx > a.thr_upd) {
                 R sc = a.thr_upd / mx;
                 x[0] *= sc; x[1] *= sc;
-                if (!diag) { scale_rows(colr, 0, a.r0, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane); }
+                if (!diag) { scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane); }
             }
             R ys[2], yp[2];
 #pragma unroll
@@ -366,8 +384,8 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
                     R sc = a.thr_rhs / mx;
                     r[0] = sc * r[0]; r[1] = sc * r[1]; seed0 = sc * seed0; seed1 = sc * seed1;
                     if (!diag) {
-                        scale_rows(colr, 0, a.r0, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane);
-                        scale_rows(coli, 0, a.r0, sc, lane); scale_rows(coli, a.r1, top + 1, sc, lane);
+                        scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane);
+                        scale_above(a, coli, c + 1, sc, lane); scale_rows(coli, a.r1, top + 1, sc, lane);
                     }
                 }
             }
@@ -391,8 +409,8 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
                 R sc = a.thr_upd / mx;
                 x[0] = sc * x[0]; x[1] = sc * x[1];
                 if (!diag) {
-                    scale_rows(colr, 0, a.r0, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane);
-                    scale_rows(coli, 0, a.r0, sc, lane); scale_rows(coli, a.r1, top + 1, sc, lane);
+                    scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane);
+                    scale_above(a, coli, c + 1, sc, lane); scale_rows(coli, a.r1, top + 1, sc, lane);
                 }
             }
             R ysr[2], ysi[2], ypr[2], ypi[2];
@@ -458,7 +476,7 @@ __global__ void __launch_bounds__(256) diag_solve_cplx(DiagArgs<R> a)
             if (mx > a.thr_rhs) {
                 R sc = a.thr_rhs / mx;
                 r[0] = sc * r[0]; r[1] = sc * r[1]; seed = sc * seed;
-                if (!diag) { scale_rows(col, 0, a.r0, sc, lane); scale_rows(col, a.r1, top + 1, sc, lane); }
+                if (!diag) { scale_above(a, col, c, sc, lane); scale_rows(col, a.r1, top + 1, sc, lane); }
             }
         }
         Factors<C> F;
@@ -477,7 +495,7 @@ __global__ void __launch_bounds__(256) diag_solve_cplx(DiagArgs<R> a)
         if (mx > a.thr_upd) {
             R sc = a.thr_upd / mx;
             x[0] = sc * x[0]; x[1] = sc * x[1];
-            if (!diag) { scale_rows(col, 0, a.r0, sc, lane); scale_rows(col, a.r1, top + 1, sc, lane); }
+            if (!diag) { scale_above(a, col, c, sc, lane); scale_rows(col, a.r1, top + 1, sc, lane); }
         }
         C ys[2], yp[2];
 #pragma unroll

@@ -244,4 +244,28 @@ __global__ void normalize_cplx_kernel(cplx<R> *V, int ldv, int n, int m)
     for (int r = threadIdx.x; r < n; r += blockDim.x) v[r] = s * v[r];
 }
 
+// Deferred guard scaling (see DiagArgs::pending): rows [0, rows) of every column with a
+// pending factor are multiplied by it, and the factor is reset to 1.  One warp per column.
+template <class E, class R>
+__global__ void apply_pending_kernel(E *X, int ldx, R *pending, int m, int rows)
+{
+    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (c >= m) return;
+    const R f = pending[c];
+    if (f == R(1)) return;
+    E *col = X + (size_t)c * ldx;
+    for (int i = lane; i < rows; i += 32) col[i] = f * col[i];
+    __syncwarp();
+    if (lane == 0) pending[c] = R(1);
+}
+
+// pending[c] = 1 for every column.
+template <class R>
+__global__ void fill_one_kernel(R *p, int m)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) p[i] = R(1);
+}
+
 }  // namespace xtg
