@@ -33,7 +33,10 @@
 #pragma once
 #include "common.cuh"
 #include "kernels_diag.cuh"
+#include "kernels_gemm.cuh"
 #include "../../include/xtgevc3.h"
+
+#include <type_traits>
 
 namespace xtg {
 namespace batch {
@@ -111,11 +114,15 @@ struct Args {
     long long spin_limit;    // polls of a ready flag before giving up
 };
 
+// FP64 runs its GEMMs on the DMMA path with A fragments from global memory (no staging),
+// so its union region only holds the diagonal blocks.
 template <class T, int NT, int H>
 __host__ __device__ constexpr size_t smem_union_bytes()
 {
-    return (2 * (size_t)KC * ALD > 2 * (size_t)H * (H + 1) ? 2 * (size_t)KC * ALD : 2 * (size_t)H * (H + 1)) *
-           sizeof(T);
+    return std::is_same<T, double>::value
+               ? 2 * (size_t)H * (H + 1) * sizeof(T)
+               : (2 * (size_t)KC * ALD > 2 * (size_t)H * (H + 1) ? 2 * (size_t)KC * ALD : 2 * (size_t)H * (H + 1)) *
+                     sizeof(T);
 }
 
 template <class T, int NT, int H>
@@ -585,6 +592,133 @@ __device__ __forceinline__ void back_pass(const typename PencilOf<T>::type &d, b
     }
 }
 
+// ---- FP64 passes on the DMMA tensor path ---------------------------------------------------
+// One warp per 32-row tile of the output (four m8 tiles) by NT columns (NT/8 n8 tiles) of
+// mma.m8n8k4.f64.  The A fragments (lane (g, t): row g, K index t) are loaded from global
+// memory: eight consecutive rows of one column (right problem) or four consecutive rows
+// of eight columns (left problem, A = rows of S and P) -- 256 B in eight full sectors
+// either way -- one 16-deep K chunk ahead of the MMAs.  B fragments come from shared
+// memory.  Warps work on disjoint rows, so a pass needs no CTA-wide synchronisation.
+template <int NT, class LoadA>
+__device__ __forceinline__ void dmma_tile(LoadA &&loadA, const double *Bs, int bld, int K,
+                                          double (&acc)[4][NT / 8][2], int lane)
+{
+    constexpr int NJ = NT / 8;
+    const int g = lane >> 2, t = lane & 3;
+    double cur[4][4], nxt[4][4];
+    auto fetch = [&](double (&dst)[4][4], int kc) {
+#pragma unroll
+        for (int s = 0; s < 4; s++) {
+            const int k = kc + 4 * s + t;
+#pragma unroll
+            for (int i = 0; i < 4; i++) dst[s][i] = k < K ? loadA(k, i) : 0.0;
+        }
+    };
+    fetch(cur, 0);
+    for (int kc = 0; kc < K; kc += 16) {
+        if (kc + 16 < K) fetch(nxt, kc + 16);
+#pragma unroll
+        for (int s = 0; s < 4; s++) {
+            const int k = kc + 4 * s + t;
+            double b[NJ];
+#pragma unroll
+            for (int j = 0; j < NJ; j++) b[j] = k < K ? Bs[(size_t)k * bld + 8 * j + g] : 0.0;
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < NJ; j++) dmma884(acc[i][j][0], acc[i][j][1], cur[s][i], b[j]);
+        }
+#pragma unroll
+        for (int s = 0; s < 4; s++)
+#pragma unroll
+            for (int i = 0; i < 4; i++) cur[s][i] = nxt[s][i];
+    }
+}
+
+// Xs[0:r0, tile] += [S | P][0:r0, I] Ys  (I = [r0, r0 + jnb), problem orientation)
+template <int NT>
+__device__ void update_dmma(const xtgevc3_dpencil &d, bool left, int r0, int jnb, double *Xs, const double *Ys)
+{
+    constexpr int XLD = Lds<double, NT>::X, YLD = Lds<double, NT>::Y, NJ = NT / 8;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+    const int n = d.n, K = 2 * jnb;
+    for (int q = wid; q < (r0 + 31) / 32; q += WARPS) {
+        const int rb = 32 * q;
+        int rowc[4];
+        double acc[4][NJ][2];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int row = rb + 8 * i + g;
+            rowc[i] = min(row, r0 - 1);
+#pragma unroll
+            for (int j = 0; j < NJ; j++)
+#pragma unroll
+                for (int h = 0; h < 2; h++)
+                    acc[i][j][h] = row < r0 ? Xs[(size_t)row * XLD + 8 * j + 2 * t + h] : 0.0;
+        }
+        auto loadA = [&](int k, int i) -> double {
+            const bool sp = k < jnb;
+            const int kk = sp ? k : k - jnb;
+            const double *M = sp ? d.S : d.P;
+            const size_t ld = sp ? (size_t)d.lds : (size_t)d.ldp;
+            if (!left) return __ldg(M + (size_t)rowc[i] + (size_t)(r0 + kk) * ld);
+            return __ldg(M + (size_t)(n - 1 - (r0 + kk)) + (size_t)(n - 1 - rowc[i]) * ld);
+        };
+        dmma_tile<NT>(loadA, Ys, YLD, K, acc, lane);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int row = rb + 8 * i + g;
+            if (row < r0)
+#pragma unroll
+                for (int j = 0; j < NJ; j++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++) Xs[(size_t)row * XLD + 8 * j + 2 * t + h] = acc[i][j][h];
+        }
+    }
+}
+
+// V[:, out(tile)] = Z[:, 0:khi] Xs[0:khi, tile]  (left: Q with reversed columns)
+template <int NT>
+__device__ void back_dmma(const xtgevc3_dpencil &d, bool left, int khi, const double *Xs,
+                          const TileCols<double, NT> &tc, int ntc)
+{
+    constexpr int XLD = Lds<double, NT>::X, NJ = NT / 8;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+    const int n = d.n;
+    const double *Zb = left ? d.Q : d.Z;
+    const size_t ldz = left ? (size_t)d.ldq : (size_t)d.ldz;
+    double *V = left ? d.VL : d.VR;
+    const size_t ldv = left ? (size_t)d.ldvl : (size_t)d.ldvr;
+    for (int q = wid; q < (n + 31) / 32; q += WARPS) {
+        const int rb = 32 * q;
+        int rowc[4];
+        double acc[4][NJ][2];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            rowc[i] = min(rb + 8 * i + g, n - 1);
+#pragma unroll
+            for (int j = 0; j < NJ; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+        }
+        auto loadA = [&](int k, int i) -> double {
+            const int zc = left ? n - 1 - k : k;
+            return __ldg(Zb + (size_t)rowc[i] + (size_t)zc * ldz);
+        };
+        dmma_tile<NT>(loadA, Xs, XLD, khi, acc, lane);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int row = rb + 8 * i + g;
+            if (row < n)
+#pragma unroll
+                for (int j = 0; j < NJ; j++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const int c = 8 * j + 2 * t + h;
+                        if (c < ntc) V[(size_t)row + (size_t)tc.out[c] * ldv] = acc[i][j][h];
+                    }
+        }
+    }
+}
+
 template <class T, int NT, int H>
 __device__ void compute_unit(const Args<T> &a, int p, int side, int t, unsigned char *smem, TileCols<T, NT> &tc,
                              uint64_t &s_sec)
@@ -683,20 +817,26 @@ __device__ void compute_unit(const Args<T> &a, int p, int side, int t, unsigned 
                                  bignum / T(max(1, jnb)), lane);
         }
         __syncthreads();
-        for (int p0 = 0; p0 < r0; p0 += PASS) {
-            const int rows = min(PASS, r0 - p0);
-            switch ((rows + 63) / 64) {
-            case 1: update_pass<T, NT, H, 1>(d, left, r0, jnb, p0, rows, Xs, Ys, U); break;
-            case 2: update_pass<T, NT, H, 2>(d, left, r0, jnb, p0, rows, Xs, Ys, U); break;
-            case 3: update_pass<T, NT, H, 3>(d, left, r0, jnb, p0, rows, Xs, Ys, U); break;
-            default: update_pass<T, NT, H, 4>(d, left, r0, jnb, p0, rows, Xs, Ys, U); break;
+        if constexpr (std::is_same<T, double>::value) {
+            if (r0 > 0) update_dmma<NT>(d, left, r0, jnb, Xs, Ys);
+        } else {
+            for (int p0 = 0; p0 < r0; p0 += PASS) {
+                const int rows = min(PASS, r0 - p0);
+                switch ((rows + 63) / 64) {
+                case 1: update_pass<T, NT, H, 1>(d, left, r0, jnb, p0, rows, Xs, Ys, U); break;
+                case 2: update_pass<T, NT, H, 2>(d, left, r0, jnb, p0, rows, Xs, Ys, U); break;
+                case 3: update_pass<T, NT, H, 3>(d, left, r0, jnb, p0, rows, Xs, Ys, U); break;
+                default: update_pass<T, NT, H, 4>(d, left, r0, jnb, p0, rows, Xs, Ys, U); break;
+                }
             }
         }
         __syncthreads();
         cur = r0;
     }
 
-    if (a.back) {
+    if (a.back && std::is_same<T, double>::value) {
+        if constexpr (std::is_same<T, double>::value) back_dmma<NT>(d, left, c_hi, Xs, tc, ntc);
+    } else if (a.back) {
         for (int p0 = 0; p0 < n; p0 += PASS) {
             const int rows = min(PASS, n - p0);
             switch ((rows + 63) / 64) {
