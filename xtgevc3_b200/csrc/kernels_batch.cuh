@@ -216,13 +216,16 @@ __device__ __forceinline__ void gemm_pass(T *As, const T *Bs, int bld, int K, Is
     }
 }
 
-// Shared per-column description of the current tile.
+// Shared per-column description of the current tile, and the columns that start an
+// eigenvector and are active in the current row block (real ones, complex pairs).
 template <class T, int NT>
 struct TileCols {
     T coef[NT][4];
     int colk[NT];
     int out[NT];
     uint8_t kind[NT];
+    int lreal[NT], lpair[NT];
+    int nreal, npair;
 };
 
 template <class T>
@@ -493,6 +496,247 @@ __device__ void solve_item(const TileCols<T, NT> &tc, int j, int r0, int r1, con
                 Ys[i * YLD + j + 1] = -ac * x[s].y;
                 Ys[(jnb + i) * YLD + j] = yp.x;
                 Ys[(jnb + i) * YLD + j + 1] = yp.y;
+            }
+        }
+    }
+}
+
+// ---- grouped solves: 32/G eigenvectors per warp ------------------------------------------
+// The block solve of solve_item, with one eigenvector per group of G = H/4 lanes instead of
+// per warp: lane gl of a group owns rows gl + G s (s < 4).  All groups of a warp step
+// through the block's rows together (one shuffle latency per row serves 32/G
+// eigenvectors); a group whose eigenvector has fewer rows in this block idles through the
+// extra steps.  One pass handles real eigenvectors, another complex pairs, so the groups
+// of a warp never take different arithmetic paths.
+template <class E, int R>
+__device__ __forceinline__ E sel_slot(const E (&v)[R], int s)
+{
+    E x = v[0];
+#pragma unroll
+    for (int q = 1; q < R; q++) x = (s == q) ? v[q] : x;
+    return x;
+}
+template <class E, int R>
+__device__ __forceinline__ void put_slot(E (&v)[R], int s, E x)
+{
+#pragma unroll
+    for (int q = 0; q < R; q++)
+        if (q == s) v[q] = x;
+}
+template <int G, class T>
+__device__ __forceinline__ T group_max(T v)
+{
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+template <class T> __device__ __forceinline__ T cmag(T v) { return fabs(v); }
+template <class T> __device__ __forceinline__ T cmag(cplx<T> v) { return fmax(fabs(v.x), fabs(v.y)); }
+
+template <class E, int R>
+struct FactorsR {
+    E inv1[R], fa[R], fb[R], fm[R], fu[R];
+    bool sw[R];
+};
+
+template <class T, int NT, int H, bool PAIR>
+__device__ void solve_group(const TileCols<T, NT> &tc, const int *list, int cnt, int r0, int r1, const T *Sd,
+                            const T *Pd, uint64_t sec, T *Xs, T *Ys, bool left, T thr_rhs, T thr_upd)
+{
+    constexpr int XLD = Lds<T, NT>::X, YLD = Lds<T, NT>::Y, DLD = H + 1;
+    constexpr int G = H / 4, R = 4, PER = 32 / G;
+    using E = typename std::conditional<PAIR, cplx<T>, T>::type;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int gl = lane & (G - 1), gbase = lane & ~(G - 1), sg = lane / G;
+    const int jnb = r1 - r0;
+    for (int base = wid * PER; base < cnt; base += WARPS * PER) {
+        const int it = base + sg;
+        const bool has = it < cnt;  // groups past the list redo the first item and discard it
+        const int j = list[has ? it : base];
+        const int k = tc.colk[j], kl = k - r0;
+        const bool diag = k < r1;
+        const T ac = tc.coef[j][0], br = tc.coef[j][1], bi = tc.coef[j][2], smin = tc.coef[j][3];
+        const int nrows = diag ? kl : jnb;
+        int maxn = nrows;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) maxn = max(maxn, __shfl_xor_sync(0xffffffffu, maxn, o));
+        T *colr = Xs + j;
+        T *coli = colr + 1;
+        const int top = PAIR ? k + 1 : k;
+        auto W = [&](int i, int c) -> E {
+            const T sv = Sd[i + c * DLD], pv = Pd[i + c * DLD];
+            if constexpr (PAIR) return E(ac * sv - br * pv, -bi * pv);
+            else return ac * sv - br * pv;
+        };
+        auto scale_outside = [&](T sc) {  // rows of the column outside the block
+            if (diag || !has) return;
+            for (int i = gl; i < r0; i += G) {
+                colr[(size_t)i * XLD] *= sc;
+                if (PAIR) coli[(size_t)i * XLD] *= sc;
+            }
+            for (int i = r1 + gl; i <= top; i += G) {
+                colr[(size_t)i * XLD] *= sc;
+                if (PAIR) coli[(size_t)i * XLD] *= sc;
+            }
+        };
+        E seed0 = E(0), seed1 = E(0);
+        if constexpr (PAIR) {
+            if (diag) {
+                if (!left) {  // (x_k, x_k+1) = (-w12, w11), src/dtgevc3.cpp:727-740
+                    seed0 = -W(kl, kl + 1);
+                    seed1 = W(kl, kl);
+                } else {      // the left problem's seed, mirrored: (w22, -w21)
+                    seed0 = W(kl + 1, kl + 1);
+                    seed1 = -W(kl + 1, kl);
+                }
+            }
+        } else {
+            seed0 = diag ? T(1) : T(0);
+        }
+        E r[R];
+#pragma unroll
+        for (int q = 0; q < R; q++) {
+            const int i = gl + G * q;
+            E v = E(0);
+            if (i < nrows) {
+                if (diag) {
+                    if constexpr (PAIR) v = -(W(i, kl) * seed0 + W(i, kl + 1) * seed1);
+                    else v = -W(i, kl);
+                } else {
+                    if constexpr (PAIR) v = E(colr[(size_t)(r0 + i) * XLD], coli[(size_t)(r0 + i) * XLD]);
+                    else v = colr[(size_t)(r0 + i) * XLD];
+                }
+            }
+            r[q] = v;
+        }
+        {  // guard before the solve (bignum/10)
+            T mx = T(0);
+#pragma unroll
+            for (int q = 0; q < R; q++) mx = fmax(mx, cmag(r[q]));
+            mx = group_max<G>(mx);
+            if (nrows > 0 && mx > thr_rhs) {
+                const T sc = thr_rhs / mx;
+#pragma unroll
+                for (int q = 0; q < R; q++) r[q] = sc * r[q];
+                seed0 = sc * seed0;
+                seed1 = sc * seed1;
+                scale_outside(sc);
+            }
+        }
+        // factors of the owned rows: 1 / w_ii, and the pivoted LU of each 2x2 block
+        FactorsR<E, R> F;
+#pragma unroll
+        for (int q = 0; q < R; q++) {
+            const int i = gl + G * q;
+            F.inv1[q] = E(0);
+            F.fa[q] = F.fb[q] = F.fm[q] = F.fu[q] = E(0);
+            F.sw[q] = false;
+            if (i < nrows) {
+                F.inv1[q] = rcp(floor_pivot(W(i, i), smin));
+                if (i >= 1 && ((sec >> i) & 1ull)) {
+                    const E w11 = W(i - 1, i - 1), w12 = W(i - 1, i), w21 = W(i, i - 1), w22 = W(i, i);
+                    const bool swp = mag(w21) > mag(w11);
+                    const E pa = swp ? w21 : w11, pb = swp ? w22 : w12, pc = swp ? w11 : w21, pd = swp ? w12 : w22;
+                    const E ia = rcp(floor_pivot(pa, smin));
+                    const E m = pc * ia;
+                    F.fa[q] = ia;
+                    F.fb[q] = pb;
+                    F.fm[q] = m;
+                    F.fu[q] = rcp(floor_pivot(pd - m * pb, smin));
+                    F.sw[q] = swp;
+                }
+            }
+        }
+        // back substitution, warp-uniform row loop
+        for (int jr = maxn - 1; jr >= 0;) {
+            const bool act = jr < nrows;
+            if (jr >= 1 && ((sec >> jr) & 1ull)) {
+                const int pr = jr - 1, qr = jr;
+                const int sp = pr / G, sq = qr / G, op = gbase + (pr & (G - 1)), oq = gbase + (qr & (G - 1));
+                const E rp = shfl(sel_slot(r, sp), op);
+                const E rq = sel_slot(r, sq);
+                bool swp = F.sw[0];
+                E ia = F.fa[0], b = F.fb[0], m = F.fm[0], iu = F.fu[0];
+#pragma unroll
+                for (int q = 1; q < R; q++)
+                    if (q == sq) {
+                        swp = F.sw[q];
+                        ia = F.fa[q];
+                        b = F.fb[q];
+                        m = F.fm[q];
+                        iu = F.fu[q];
+                    }
+                const E e1 = swp ? rq : rp, e2 = swp ? rp : rq;
+                E xq = (e2 - m * e1) * iu;
+                E xp = (e1 - b * xq) * ia;
+                xq = shfl(xq, oq);
+                xp = shfl(xp, oq);
+                if (act) {
+                    if (gl == (pr & (G - 1))) put_slot(r, sp, xp);
+                    if (gl == (qr & (G - 1))) put_slot(r, sq, xq);
+#pragma unroll
+                    for (int q = 0; q < R; q++) {
+                        const int i = gl + G * q;
+                        if (i < pr) r[q] = r[q] - (W(i, pr) * xp + W(i, qr) * xq);
+                    }
+                }
+                jr -= 2;
+            } else {
+                const int sj = jr / G, oj = gbase + (jr & (G - 1));
+                const E x = shfl(sel_slot(r, sj) * sel_slot(F.inv1, sj), oj);
+                if (act) {
+                    if (gl == (jr & (G - 1))) put_slot(r, sj, x);
+#pragma unroll
+                    for (int q = 0; q < R; q++) {
+                        const int i = gl + G * q;
+                        if (i < jr) r[q] = r[q] - W(i, jr) * x;
+                    }
+                }
+                jr -= 1;
+            }
+        }
+        // the block column: solution rows, seed, zeros below it
+        E x[R];
+#pragma unroll
+        for (int q = 0; q < R; q++) {
+            const int i = gl + G * q;
+            x[q] = i < nrows ? r[q] : (diag && i == kl ? seed0 : (PAIR && diag && i == kl + 1 ? seed1 : E(0)));
+        }
+        const E bc = [&] {
+            if constexpr (PAIR) return E(br, bi);
+            else return br;
+        }();
+        {  // guard before the update (bignum / block height)
+            T mx = T(0);
+#pragma unroll
+            for (int q = 0; q < R; q++) mx = fmax(mx, fmax(cmag(ac * x[q]), cmag(bc * x[q])));
+            mx = group_max<G>(mx);
+            if (mx > thr_upd) {
+                const T sc = thr_upd / mx;
+#pragma unroll
+                for (int q = 0; q < R; q++) x[q] = sc * x[q];
+                scale_outside(sc);
+            }
+        }
+        if (has) {
+#pragma unroll
+            for (int q = 0; q < R; q++) {
+                const int i = gl + G * q;
+                if (i < jnb) {
+                    const E ys = -(ac * x[q]), yp = bc * x[q];
+                    if constexpr (PAIR) {
+                        colr[(size_t)(r0 + i) * XLD] = x[q].x;
+                        coli[(size_t)(r0 + i) * XLD] = x[q].y;
+                        Ys[i * YLD + j] = ys.x;
+                        Ys[i * YLD + j + 1] = ys.y;
+                        Ys[(jnb + i) * YLD + j] = yp.x;
+                        Ys[(jnb + i) * YLD + j + 1] = yp.y;
+                    } else {
+                        colr[(size_t)(r0 + i) * XLD] = x[q];
+                        Ys[i * YLD + j] = ys;
+                        Ys[(jnb + i) * YLD + j] = yp;
+                    }
+                }
             }
         }
     }
@@ -791,6 +1035,16 @@ __device__ void compute_unit(const Args<T> &a, int p, int side, int t, unsigned 
         }
         for (int idx = tid; idx < 2 * jnb * NT; idx += THREADS) Ys[(idx / NT) * YLD + idx % NT] = T(0);
         __syncthreads();
+        if (tid == 32) {  // this block's active eigenvectors, real ones and complex pairs
+            int nr = 0, np = 0;
+            for (int j = 0; j < ntc; j++) {
+                if (tc.kind[j] == kPairIm || tc.colk[j] < r0) continue;
+                if (tc.kind[j] == kReal) tc.lreal[nr++] = j;
+                else tc.lpair[np++] = j;
+            }
+            tc.nreal = nr;
+            tc.npair = np;
+        }
         if (tid < 32) {  // 2x2 diagonal blocks, paired greedily from the bottom
             const bool b0 = lane >= 1 && lane < jnb && Sd[lane + (lane - 1) * DLD] != T(0);
             const bool b1 = lane + 32 < jnb && Sd[(lane + 32) + (lane + 31) * DLD] != T(0);
@@ -811,10 +1065,19 @@ __device__ void compute_unit(const Args<T> &a, int p, int side, int t, unsigned 
         }
         __syncthreads();
         const uint64_t sec = s_sec;
-        for (int j = wid; j < ntc; j += WARPS) {
-            if (tc.kind[j] == kPairIm || tc.colk[j] < r0) continue;
-            solve_item<T, NT, H>(tc, j, r0, r1, Sd, Pd, sec, Xs, Ys, left, bignum / T(10),
-                                 bignum / T(max(1, jnb)), lane);
+        if constexpr (std::is_same<T, double>::value) {
+            // FP64: several eigenvectors per warp (measured faster); FP32 keeps one per warp,
+            // which keeps its register count low enough for two CTAs per SM
+            solve_group<T, NT, H, false>(tc, tc.lreal, tc.nreal, r0, r1, Sd, Pd, sec, Xs, Ys, left,
+                                         bignum / T(10), bignum / T(max(1, jnb)));
+            solve_group<T, NT, H, true>(tc, tc.lpair, tc.npair, r0, r1, Sd, Pd, sec, Xs, Ys, left,
+                                        bignum / T(10), bignum / T(max(1, jnb)));
+        } else {
+            for (int j = wid; j < ntc; j += WARPS) {
+                if (tc.kind[j] == kPairIm || tc.colk[j] < r0) continue;
+                solve_item<T, NT, H>(tc, j, r0, r1, Sd, Pd, sec, Xs, Ys, left, bignum / T(10),
+                                     bignum / T(max(1, jnb)), lane);
+            }
         }
         __syncthreads();
         if constexpr (std::is_same<T, double>::value) {
