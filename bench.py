@@ -59,6 +59,10 @@ def parse():
     ap.add_argument("--adjoint-n", type=int, default=2048, help="order of the dtgevc3 adjoint case (0 skips)")
     ap.add_argument("--adjoint-c-count", type=int, default=256, help="complex64 pencils of the ctgevc3 adjoint case")
     ap.add_argument("--adjoint-c-n", type=int, default=128)
+    ap.add_argument("--profile-case", default=None,
+                    help="run one small case for an ncu capture and exit (no JSON line): plain:N (two dtgevc3 "
+                         "B/B calls, FP64), split_i8:N (the same, INT8 split form), batch:COUNT (two launches "
+                         "of the batched dtgevc3 B/B kernel, tiles 32x32)")
     return ap.parse_args()
 
 
@@ -551,8 +555,46 @@ def measure_adjoint(args, X, torch):
     return out
 
 
+def profile_case(args):
+    """Small, fixed workloads for ncu captures (profiles/*.md name the exact command)."""
+    import torch
+    import xtgevc3_b200 as X
+    kind, _, size = args.profile_case.partition(":")
+    size = int(size)
+    if kind in ("plain", "split_i8"):
+        flags = 0 if kind == "plain" else X.SPLIT | X.SPLIT_INT8 | X.slices(7)
+        S_h, P_h, ar, ai, be = host_pencil(size, 3)
+        S, P = colmajor_cuda(S_h, torch), colmajor_cuda(P_h, torch)
+        Q, Z = orthogonal(size, 4, torch), orthogonal(size, 5, torch)
+        VL, VR = torch.empty_like(Q), torch.empty_like(Z)
+        for _ in range(2):
+            VL.copy_(Q)
+            VR.copy_(Z)
+            X.tgevc3_dev("B", "B", S, P, ar, be, alphai=ai, VL=VL, VR=VR, flags=flags)
+        torch.cuda.synchronize()
+        kext, k = [], 0
+        while k < size:
+            w = 2 if (ai[k] != 0 and k + 1 < size) else 1
+            kext += [k + w] * w
+            k += w
+        print(json.dumps({"case": args.profile_case, "back_flops_per_side": 2.0 * size * sum(kext)}))
+    elif kind == "batch":
+        sizes, plist, _ = batched_inputs(size, 5, torch)
+        pens = [{k: v for k, v in p.items() if k != "host"} for p in plist["d"]]
+        b = X.Batch("B", "B", pens, config=X.batch_config(32, 32))
+        for _ in range(2):
+            b.run()
+        b.wait()
+        print(json.dumps({"case": args.profile_case, "flops": float(np.sum(10.0 / 3.0 * sizes.astype(float) ** 3))}))
+    else:
+        raise SystemExit(f"unknown profile case {args.profile_case}")
+    return 0
+
+
 def main():
     args = parse()
+    if args.profile_case:
+        return profile_case(args)
     if args.impl == "reference":
         return reference_arm(args)
     import torch
