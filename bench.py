@@ -713,9 +713,13 @@ def main():
         t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e = {"value": world * 2 * n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 4 * n * n * 8,
+    # bytes the host path moves: S and P as their upper trapezoid in 512-column panels (rows
+    # <= last column + 1), Q and Z whole in; VL and VR whole out
+    trap = sum(min(n, j0 + 512 + 1) * (min(n, j0 + 512) - j0) for j0 in range(0, n, 512))
+    e2e = {"value": world * 2 * n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": (2 * trap + 2 * n * n) * 8,
            "d2h_bytes_per_step": 2 * n * n * 8, "ms_per_step": 1e3 * e2e_s,
-           "path": f"xtgevc3_dtgevc3 (host pointers, pinned), {head} form, H2D/D2H inside the call"}
+           "path": f"xtgevc3_dtgevc3 (host pointers, pinned), {head} form, H2D/D2H inside the call (S, P "
+                   f"before the solve; Q, Z and the result columns overlapped with it)"}
 
     batched = measure_batched(args, X, torch, dist, world) if args.batch_count > 0 else None
     adjoint = measure_adjoint(args, X, torch) if args.adjoint_n > 0 and rank == 0 else None

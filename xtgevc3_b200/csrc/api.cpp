@@ -61,6 +61,11 @@ bool check_work(int n, W *work, int lwork, int *info)
 inline int round_up(int v, int q) { return (v + q - 1) / q * q; }
 
 // Host pointers: stage S, P (and Q/Z for HOWMNY='B') on the device, run, copy back.
+// S and P travel as their upper trapezoid only (every kernel reads rows <= col + 1), in
+// column panels; the device copies are zeroed first so the rest holds no garbage.  Q and Z
+// upload on a second stream while the substitution runs (each side's back-transform waits
+// for its matrix), and each side's result downloads on a third stream as soon as that
+// side's kernels are queued, behind the other side's work.
 template <class R, bool CPLX>
 int run_host(char side, char howmny, const int *select, int n, const void *S, int lds, const void *P, int ldp,
              const void *alpha, const void *alphai, const void *beta, void *VL, int ldvl, void *VR, int ldvr,
@@ -71,63 +76,113 @@ int run_host(char side, char howmny, const int *select, int n, const void *S, in
     const bool want_l = (side == 'L' || side == 'B') && VL;
     if (!want_r && !want_l) return 0;
     const bool back = howmny == 'B';
-    cudaStream_t st = cudaStreamPerThread;
     const int ld = round_up(n, 32);
     const size_t mat = (size_t)ld * n * sizeof(E);
     const size_t vcols = (size_t)std::max(count, back ? n : 0);
-    void *dS = nullptr, *dP = nullptr, *dVL = nullptr, *dVR = nullptr;
+    struct Res {
+        cudaStream_t st = nullptr, sin = nullptr, sout = nullptr;
+        cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // Z ready, Q ready, right done, left done
+        void *dS = nullptr, *dP = nullptr, *dVL = nullptr, *dVR = nullptr;
+        ~Res()
+        {
+            // every stream is synchronised before its buffers go
+            for (cudaStream_t q : {st, sin, sout})
+                if (q) cudaStreamSynchronize(q);
+            for (void *p : {dS, dP, dVL, dVR})
+                if (p) cudaFree(p);
+            for (cudaEvent_t e : ev)
+                if (e) cudaEventDestroy(e);
+            for (cudaStream_t q : {st, sin, sout})
+                if (q) cudaStreamDestroy(q);
+        }
+    } r;
     auto fail = [&](cudaError_t e, const char *what) {
         xtg::set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
-        if (dS) cudaFreeAsync(dS, st);
-        if (dP) cudaFreeAsync(dP, st);
-        if (dVL) cudaFreeAsync(dVL, st);
-        if (dVR) cudaFreeAsync(dVR, st);
-        cudaStreamSynchronize(st);
         return 1;
     };
     cudaError_t e;
-    if ((e = cudaMallocAsync(&dS, mat, st)) != cudaSuccess) return fail(e, "cudaMallocAsync");
-    if ((e = cudaMallocAsync(&dP, mat, st)) != cudaSuccess) return fail(e, "cudaMallocAsync");
-    if (want_l && (e = cudaMallocAsync(&dVL, (size_t)ld * vcols * sizeof(E), st)) != cudaSuccess)
+    for (cudaStream_t *q : {&r.st, &r.sin, &r.sout})
+        if ((e = cudaStreamCreateWithFlags(q, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
+    for (cudaEvent_t &ev : r.ev)
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+    if ((e = cudaMallocAsync(&r.dS, mat, r.st)) != cudaSuccess) return fail(e, "cudaMallocAsync");
+    if ((e = cudaMallocAsync(&r.dP, mat, r.st)) != cudaSuccess) return fail(e, "cudaMallocAsync");
+    if (want_l && (e = cudaMallocAsync(&r.dVL, (size_t)ld * vcols * sizeof(E), r.st)) != cudaSuccess)
         return fail(e, "cudaMallocAsync");
-    if (want_r && (e = cudaMallocAsync(&dVR, (size_t)ld * vcols * sizeof(E), st)) != cudaSuccess)
+    if (want_r && (e = cudaMallocAsync(&r.dVR, (size_t)ld * vcols * sizeof(E), r.st)) != cudaSuccess)
         return fail(e, "cudaMallocAsync");
+    // the output buffers are written by the second stream (Q, Z) and the copies out
+    if ((e = cudaEventRecord(r.ev[0], r.st)) != cudaSuccess) return fail(e, "event");
+    if ((e = cudaStreamWaitEvent(r.sin, r.ev[0], 0)) != cudaSuccess) return fail(e, "event");
     const size_t w = (size_t)n * sizeof(E);
-    if ((e = cudaMemcpy2DAsync(dS, ld * sizeof(E), S, (size_t)lds * sizeof(E), w, n, cudaMemcpyHostToDevice, st)))
-        return fail(e, "H2D S");
-    if ((e = cudaMemcpy2DAsync(dP, ld * sizeof(E), P, (size_t)ldp * sizeof(E), w, n, cudaMemcpyHostToDevice, st)))
-        return fail(e, "H2D P");
+    const int panel = 512;
+    for (int which = 0; which < 2; which++) {
+        void *dst = which ? r.dP : r.dS;
+        const void *src = which ? P : S;
+        const int lsrc = which ? ldp : lds;
+        if ((e = cudaMemsetAsync(dst, 0, mat, r.st)) != cudaSuccess) return fail(e, "cudaMemsetAsync");
+        for (int j0 = 0; j0 < n; j0 += panel) {
+            const int j1 = std::min(n, j0 + panel), rows = std::min(n, j1 + 1);
+            e = cudaMemcpy2DAsync(static_cast<E *>(dst) + (size_t)j0 * ld, ld * sizeof(E),
+                                  static_cast<const E *>(src) + (size_t)j0 * lsrc, (size_t)lsrc * sizeof(E),
+                                  (size_t)rows * sizeof(E), j1 - j0, cudaMemcpyHostToDevice, r.st);
+            if (e != cudaSuccess) return fail(e, which ? "H2D P" : "H2D S");
+        }
+    }
+    (void)w;
+    xtg::Options opt = make_opts(flags);
     if (back) {
-        if (want_l && (e = cudaMemcpy2DAsync(dVL, ld * sizeof(E), VL, (size_t)ldvl * sizeof(E), w, n,
-                                             cudaMemcpyHostToDevice, st)))
-            return fail(e, "H2D Q");
-        if (want_r && (e = cudaMemcpy2DAsync(dVR, ld * sizeof(E), VR, (size_t)ldvr * sizeof(E), w, n,
-                                             cudaMemcpyHostToDevice, st)))
-            return fail(e, "H2D Z");
+        if (want_r) {
+            if ((e = cudaMemcpy2DAsync(r.dVR, ld * sizeof(E), VR, (size_t)ldvr * sizeof(E), (size_t)n * sizeof(E),
+                                       n, cudaMemcpyHostToDevice, r.sin)))
+                return fail(e, "H2D Z");
+            if ((e = cudaEventRecord(r.ev[0], r.sin)) != cudaSuccess) return fail(e, "event");
+            opt.back_ready[0] = r.ev[0];
+        }
+        if (want_l) {
+            if ((e = cudaMemcpy2DAsync(r.dVL, ld * sizeof(E), VL, (size_t)ldvl * sizeof(E), (size_t)n * sizeof(E),
+                                       n, cudaMemcpyHostToDevice, r.sin)))
+                return fail(e, "H2D Q");
+            if ((e = cudaEventRecord(r.ev[1], r.sin)) != cudaSuccess) return fail(e, "event");
+            opt.back_ready[1] = r.ev[1];
+        }
     }
-    int rc = xtg::solve_device<R, CPLX>(side, howmny, select, n, dS, ld, dP, ld, alpha, alphai, beta,
-                                        want_l ? dVL : nullptr, ld, want_r ? dVR : nullptr, ld, count,
-                                        make_opts(flags), st);
-    if (rc) {
-        std::string msg = xtg::last_error();
-        fail(cudaSuccess, "device");
-        xtg::set_last_error(msg);
-        return 1;
-    }
-    if (want_l && (e = cudaMemcpy2DAsync(VL, (size_t)ldvl * sizeof(E), dVL, ld * sizeof(E), w, count,
-                                         cudaMemcpyDeviceToHost, st)))
-        return fail(e, "D2H VL");
-    if (want_r && (e = cudaMemcpy2DAsync(VR, (size_t)ldvr * sizeof(E), dVR, ld * sizeof(E), w, count,
-                                         cudaMemcpyDeviceToHost, st)))
-        return fail(e, "D2H VR");
-    cudaFreeAsync(dS, st);
-    cudaFreeAsync(dP, st);
-    if (dVL) cudaFreeAsync(dVL, st);
-    if (dVR) cudaFreeAsync(dVR, st);
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) {
-        xtg::set_last_error(std::string("cudaStreamSynchronize: ") + cudaGetErrorString(e));
-        return 1;
-    }
+    cudaError_t out_err = cudaSuccess;
+    // download output columns [o0, o1) of one side once its stream reaches this point
+    std::vector<std::pair<bool, int>> chunked;  // sides whose columns went out in chunks
+    auto download = [&](bool left, cudaStream_t sst, int o0, int o1) {
+        cudaEvent_t ev = r.ev[left ? 3 : 2];
+        E *hv = static_cast<E *>(left ? VL : VR);
+        const int ldh = left ? ldvl : ldvr;
+        const E *dv = static_cast<const E *>(left ? r.dVL : r.dVR);
+        cudaError_t x = cudaEventRecord(ev, sst);
+        if (x == cudaSuccess) x = cudaStreamWaitEvent(r.sout, ev, 0);
+        if (x == cudaSuccess && o1 > o0)
+            x = cudaMemcpy2DAsync(hv + (size_t)o0 * ldh, (size_t)ldh * sizeof(E), dv + (size_t)o0 * ld,
+                                  ld * sizeof(E), (size_t)n * sizeof(E), o1 - o0, cudaMemcpyDeviceToHost, r.sout);
+        if (x != cudaSuccess) out_err = x;
+    };
+    if (back) opt.cols_done = [&](bool left, cudaStream_t sst, int o0, int o1) {
+        download(left, sst, o0, o1);
+        chunked.push_back({left, o1 - o0});
+    };
+    opt.side_done = [&](bool left, cudaStream_t sst) {
+        int done = 0;
+        for (auto &c : chunked)
+            if (c.first == left) done += c.second;
+        if (done < count) download(left, sst, 0, count);
+    };
+    int rc = xtg::solve_device<R, CPLX>(side, howmny, select, n, r.dS, ld, r.dP, ld, alpha, alphai, beta,
+                                        want_l ? r.dVL : nullptr, ld, want_r ? r.dVR : nullptr, ld, count, opt, r.st);
+    if (rc) return 1;
+    if (out_err != cudaSuccess) return fail(out_err, "D2H");
+    if ((e = cudaStreamSynchronize(r.sout)) != cudaSuccess) return fail(e, "cudaStreamSynchronize");
+    cudaFreeAsync(r.dS, r.st);
+    cudaFreeAsync(r.dP, r.st);
+    if (r.dVL) cudaFreeAsync(r.dVL, r.st);
+    if (r.dVR) cudaFreeAsync(r.dVR, r.st);
+    r.dS = r.dP = r.dVL = r.dVR = nullptr;
+    if ((e = cudaStreamSynchronize(r.st)) != cudaSuccess) return fail(e, "cudaStreamSynchronize");
     return 0;
 }
 

@@ -700,6 +700,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         E *V = left ? VL : VR;
         const int ldv = left ? ldvl : ldvr;
         if (do_back) {
+            if (opt.back_ready[left ? 1 : 0]) XTG_CK(cudaStreamWaitEvent(st, opt.back_ready[left ? 1 : 0], 0));
             // copy of Z (right) or column-reversed Q (left), so V can be overwritten
             E *Zc = scr.get<E>((size_t)ld_n * n);
             if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
@@ -711,26 +712,53 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
                 XTG_CK(cudaMemcpy2DAsync(Zc, (size_t)ld_n * sizeof(E), V, (size_t)ldv * sizeof(E), n * sizeof(E), n,
                                          cudaMemcpyDeviceToDevice, st));
             }
-            GemmArgs<E> g;
-            g.M = n;
-            g.N = m;
-            g.mlo = 0;
-            g.nseg = 1;
-            g.seg[0] = strip(Zc, ld_n, 0, 0, n, 0);
-            g.K = g.seg[0].K;
-            g.B = X;
-            g.ldb = ldx;
-            g.brows = n;
-            g.C = V;
-            g.ldc = ldv;
-            g.ccol = d_outcol;
-            g.kext = d_kext;
-            g.accumulate = 0;
-            double bf = 0, bk = 0;
-            for (int c = 0; c < m; c++) bk += L.kext[c];
-            bf = 2.0 * n * bk * cfl;
-            const double bb = ((double)n * L.kext[m - 1] + bk + (double)n * m) * esz;
-            tr.run(kTBack, bf, bb, st, [&] { gemm(g, st); });
+            // column chunks of equal work (sum of kext), never splitting a complex pair, so
+            // that a caller can download each chunk's output columns while the next runs
+            std::vector<int> cuts = {0};
+            if (opt.cols_done && !opt.normalize) {
+                double tot = 0;
+                for (int c = 0; c < m; c++) tot += L.kext[c];
+                const int nch = std::min(4, m);
+                double acc = 0;
+                for (int c = 0; c < m; c++) {
+                    acc += L.kext[c];
+                    const int nxt = c + 1;
+                    if ((int)cuts.size() < nch && nxt < m && acc >= tot * cuts.size() / nch && L.kind[nxt] != kPairIm)
+                        cuts.push_back(nxt);
+                }
+            }
+            cuts.push_back(m);
+            for (size_t q = 0; q + 1 < cuts.size(); q++) {
+                const int c0 = cuts[q], c1 = cuts[q + 1];
+                GemmArgs<E> g;
+                g.M = n;
+                g.N = c1 - c0;
+                g.mlo = 0;
+                g.nseg = 1;
+                g.seg[0] = strip(Zc, ld_n, 0, 0, n, 0);
+                g.K = g.seg[0].K;
+                g.B = X + (size_t)c0 * ldx;
+                g.ldb = ldx;
+                g.brows = n;
+                g.C = V;
+                g.ldc = ldv;
+                g.ccol = d_outcol + c0;
+                g.kext = d_kext + c0;
+                g.accumulate = 0;
+                double bk = 0;
+                for (int c = c0; c < c1; c++) bk += L.kext[c];
+                const double bf = 2.0 * n * bk * cfl;
+                const double bb = ((double)n * L.kext[c1 - 1] + bk + (double)n * (c1 - c0)) * esz;
+                tr.run(kTBack, bf, bb, st, [&] { gemm(g, st); });
+                if (opt.cols_done && !opt.normalize) {
+                    int o0 = m, o1 = 0;
+                    for (int c = c0; c < c1; c++) {
+                        o0 = std::min(o0, L.outcol[c]);
+                        o1 = std::max(o1, L.outcol[c] + 1);
+                    }
+                    if (o1 - o0 == c1 - c0) opt.cols_done(left, st, o0, o1);  // a contiguous block of outputs
+                }
+            }
         } else {
             dim3 g(std::max(1, std::min((n + 255) / 256, 64)), m);
             tr.run(kTWriteback, 0, 2.0 * n * m * esz, st, [&] {
@@ -759,6 +787,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             set_last_error(std::string("split-precision GEMM launch: ") + cudaGetErrorString(split_err));
             return 1;
         }
+        if (opt.side_done) opt.side_done(left, st);
         return 0;
     };
 

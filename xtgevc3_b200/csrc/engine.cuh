@@ -1,6 +1,7 @@
 // Host-side driver of the device algorithm (declarations shared by engine.cu and api.cpp).
 #pragma once
 #include <cuda_runtime.h>
+#include <functional>
 #include <string>
 
 namespace xtg {
@@ -16,6 +17,14 @@ struct Options {
     // allocated) and the two sides run one after the other on the caller's stream.
     void *arena = nullptr;
     size_t arena_bytes = 0;
+    // Host-pointer path: the back-transform of a side waits for this event (the upload of
+    // Z / Q on another stream), and side_done is called once a side's last kernel is
+    // queued, with that side's stream (the result can be downloaded behind the other side).
+    cudaEvent_t back_ready[2] = {nullptr, nullptr};  // right, left
+    std::function<void(bool left, cudaStream_t st)> side_done;
+    // HOWMNY='B' without normalisation: the back-transform runs in column chunks and this
+    // is called after each with the output columns [o0, o1) it completed.
+    std::function<void(bool left, cudaStream_t st, int o0, int o1)> cols_done;
 };
 
 // Device scratch (bytes) a call needs in arena mode: shared eigenvalue data plus the larger
