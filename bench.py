@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--adjoint-n", type=int, default=2048, help="order of the dtgevc3 adjoint case (0 skips)")
     ap.add_argument("--adjoint-c-count", type=int, default=256, help="complex64 pencils of the ctgevc3 adjoint case")
     ap.add_argument("--adjoint-c-n", type=int, default=128)
+    ap.add_argument("--z-n", type=int, default=4096, help="order of the ztgevc3 SIDE=R HOWMNY=A leg (0 skips)")
     ap.add_argument("--profile-case", default=None,
                     help="run one small case for an ncu capture and exit (no JSON line): plain:N (two dtgevc3 "
                          "B/B calls, FP64), split_i8:N (the same, INT8 split form), batch:COUNT (two launches "
@@ -555,6 +556,48 @@ def measure_adjoint(args, X, torch):
     return out
 
 
+def measure_ztgevc3(args, X, torch):
+    """ztgevc3 SIDE='R', HOWMNY='A' on a complex upper-triangular pencil of order --z-n
+    (the structure of the upstream complex test generator), plus a graded variant whose
+    rows of P are scaled by 10^U(-8, 8) so that eigenvalues span many orders of magnitude
+    and the overflow guards rescale columns.  Device-resident inputs, CUDA-event timing."""
+    from xtgevc3_b200 import pencils as gen
+    n = args.z_n
+    out = {}
+    for name in ("standard", "graded"):
+        S_h, P_h, al, be = gen.gen_upper_triangular_complex(n, args.seed + 21)
+        if name == "graded":
+            rng = np.random.default_rng(args.seed + 22)
+            P_h = np.asfortranarray((10.0 ** rng.uniform(-8, 8, n))[:, None] * P_h)
+            be = np.diag(P_h).copy()
+        S, P = colmajor_cuda(S_h, torch), colmajor_cuda(P_h, torch)
+        VR = torch.zeros(n, n, dtype=torch.complex128, device="cuda").t()
+        for _ in range(max(args.warmup, 1)):
+            X.tgevc3_dev("R", "A", S, P, al, be, VR=VR)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            X.tgevc3_dev("R", "A", S, P, al, be, VR=VR)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        # residual max_c ||beta S x - alpha P x||_1 / ((|beta| ||S||_1 + |alpha| ||P||_1) ||x||_1)
+        a_t = torch.as_tensor(al, device="cuda")
+        b_t = torch.as_tensor(be, device="cuda")
+        R = (S @ VR) * b_t[None, :] - (P @ VR) * a_t[None, :]
+        den = (b_t.abs() * S.abs().sum(0).max() + a_t.abs() * P.abs().sum(0).max()) * VR.abs().sum(0)
+        resid = float((R.abs().sum(0) / den).max())
+        guarded = int((torch.diagonal(VR).abs() < 1).sum())
+        out[name] = {"ms": ms, "eigvecs_per_s": n / (ms * 1e-3), "tflops": 8.0 / 3.0 * n ** 3 / (ms * 1e-3) / 1e12,
+                     "resid_max": resid, "columns_rescaled_by_guards": guarded,
+                     "finite": bool(torch.isfinite(torch.view_as_real(VR)).all())}
+        del S, P, VR, R
+    return {"n": n, "side": "R", "howmny": "A",
+            "data": "complex upper-triangular stand-in pencils (U(-1,1) parts, |P_kk| kept away from 0); "
+                    "graded: rows of P scaled by 10^U(-8,8)", **out}
+
+
 def profile_case(args):
     """Small, fixed workloads for ncu captures (profiles/*.md name the exact command)."""
     import torch
@@ -723,6 +766,7 @@ def main():
 
     batched = measure_batched(args, X, torch, dist, world) if args.batch_count > 0 else None
     adjoint = measure_adjoint(args, X, torch) if args.adjoint_n > 0 and rank == 0 else None
+    zleg = measure_ztgevc3(args, X, torch) if args.z_n > 0 and rank == 0 else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -754,7 +798,7 @@ def main():
                            "resid_max": h["resid"], "resid_bound": 1e-12},
                 "forms": forms_out, "clocks": h["clocks"], "e2e": e2e, "gpu_launches": h["launches"],
                 "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "batched": batched,
-                "adjoint": adjoint}
+                "adjoint": adjoint, "ztgevc3": zleg}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -169,6 +169,8 @@ void configure_device(int dev)
                              2 * kBlock * kSmLd * (int)sizeof(cplx<float>));
         cudaFuncSetAttribute(gemm_dmma<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::SMEM_BYTES);
         cudaFuncSetAttribute(gemm_dmma<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::SMEM_BYTES);
+        cudaFuncSetAttribute(gemm_dmma_cplx<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, zmma::SMEM_BYTES);
+        cudaFuncSetAttribute(gemm_dmma_cplx<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, zmma::SMEM_BYTES);
         cudaFuncSetAttribute(split::gemm_split_kernel<split::kBF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              split::Layout<split::kBF16>::SMEM_BYTES);
         cudaFuncSetAttribute(split::gemm_split_kernel<split::kI8>, cudaFuncAttributeMaxDynamicSharedMemorySize,

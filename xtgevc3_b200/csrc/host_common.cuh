@@ -78,6 +78,18 @@ inline void launch_gemm(const GemmArgs<E> &g, bool simt, cudaStream_t st)
             return;
         }
     }
+    if constexpr (std::is_same<E, cplx<double>>::value) {
+        // cp.async of 16-byte complex elements: 16-byte aligned operands only
+        auto al = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+        bool ok = al(g.B) && (g.C != nullptr) && al(g.C);
+        for (int s = 0; s < g.nseg; s++) ok = ok && al(g.seg[s].A);
+        if (!simt && ok) {
+            dim3 grid((g.M + zmma::BM - 1) / zmma::BM, (g.N + zmma::BN - 1) / zmma::BN);
+            if (g.accumulate) gemm_dmma_cplx<1><<<grid, 256, zmma::SMEM_BYTES, st>>>(g);
+            else gemm_dmma_cplx<0><<<grid, 256, zmma::SMEM_BYTES, st>>>(g);
+            return;
+        }
+    }
     dim3 grid((g.M + 63) / 64, (g.N + 63) / 64);
     gemm_simt<E><<<grid, 256, 0, st>>>(g);
 }

@@ -286,4 +286,147 @@ __global__ void __launch_bounds__(256) gemm_dmma(GemmArgs<double> g)
     }
 }
 
+// ------------------------------------------------------------------------------------
+// Complex FP64 on the DMMA path (z): every complex product is four real m8n8k4 MMAs,
+//   Cr += Ar Br - Ai Bi,   Ci += Ar Bi + Ai Br.
+// CTA tile 64 x 64 complex, K step 8, 8 warps as 2 (M) x 4 (N) with 32 x 16 warp tiles,
+// 3-stage cp.async pipeline of 16-byte complex elements (shared memory keeps the
+// interleaved layout; fragments pick the real or imaginary half).  Segment, K-limit and
+// column-map conventions as gemm_simt.  Needs 16-byte aligned operands (the launcher checks).
+// ------------------------------------------------------------------------------------
+namespace zmma {
+constexpr int BM = 64, BN = 64, BK = 8, STAGES = 3;
+constexpr int ALD = BM + 4;  // A tile [k][m], complex
+constexpr int BLD = BK + 1;  // B tile [n][k], complex
+constexpr int A_STAGE = BK * ALD;
+constexpr int B_STAGE = BN * BLD;
+constexpr int SMEM_BYTES = STAGES * (A_STAGE + B_STAGE) * 16;
+}  // namespace zmma
+
+template <int ACC>
+__global__ void __launch_bounds__(256) gemm_dmma_cplx(GemmArgs<cplx<double>> g)
+{
+    using namespace zmma;
+    using Z = cplx<double>;
+    extern __shared__ __align__(16) unsigned char smem_gemm_z[];
+    Z *As = reinterpret_cast<Z *>(smem_gemm_z);
+    Z *Bs = As + STAGES * A_STAGE;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp & 1, wn = warp >> 1;
+    const int gq = lane >> 2, tq = lane & 3;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int kmax = tile_kmax(g, n0, BN);
+    const int ktiles = (kmax + BK - 1) / BK;
+
+    double cr[4][2][2], ci[4][2][2];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) cr[i][j][h] = ci[i][j][h] = 0.0;
+
+    auto load_stage = [&](int kt, int st) {
+        const int k0 = kt * BK;
+        int kb = 0;
+        const int s = find_seg(g, k0, kb);
+        const GemmSeg<Z> sg = g.seg[s < 0 ? 0 : s];
+        Z *as = As + st * A_STAGE;
+        Z *bs = Bs + st * B_STAGE;
+#pragma unroll
+        for (int q = 0; q < 2; q++) {  // A: 8 columns x 64 rows
+            const int e = tid + 256 * q;
+            const int kk = e >> 6, m = e & 63;
+            const int row = m0 + m, col = k0 - kb + kk;
+            const bool ok = s >= 0 && k0 + kk < kmax && col < sg.acols && row < g.M;
+            const Z *gp = ok ? sg.A + (size_t)row + (size_t)col * sg.lda : reinterpret_cast<const Z *>(g.B);
+            cp_async16(as + kk * ALD + m, gp, ok ? 16 : 0);
+        }
+        const int lim = min(sg.boff + kmax - kb, g.brows);
+#pragma unroll
+        for (int q = 0; q < 2; q++) {  // B: 64 columns x 8 rows
+            const int e = tid + 256 * q;
+            const int kk = e & 7, nn = e >> 3;
+            const int kr = sg.boff + k0 - kb + kk, col = n0 + nn;
+            const bool ok = s >= 0 && col < g.N && kr < lim;
+            const Z *gp = ok ? g.B + (size_t)kr + (size_t)col * g.ldb : g.B;
+            cp_async16(bs + nn * BLD + kk, gp, ok ? 16 : 0);
+        }
+    };
+
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; s++) {
+        if (s < ktiles) load_stage(s, s);
+        cp_async_commit();
+    }
+    if (ACC) {
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int col = n0 + wn * 16 + j * 8 + 2 * tq + h;
+                if (col >= g.N) continue;
+                const Z *cp = g.C + (size_t)(g.ccol ? g.ccol[col] : col) * g.ldc;
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const int row = m0 + wm * 32 + i * 8 + gq;
+                    if (row >= g.mlo && row < g.M) {
+                        const Z v = cp[row];
+                        cr[i][j][h] = v.x;
+                        ci[i][j][h] = v.y;
+                    }
+                }
+            }
+    }
+    for (int kt = 0; kt < ktiles; kt++) {
+        cp_async_wait<STAGES - 2>();
+        __syncthreads();
+        const int nk = kt + STAGES - 1;
+        if (nk < ktiles) load_stage(nk, nk % STAGES);
+        cp_async_commit();
+        const Z *as = As + (kt % STAGES) * A_STAGE;
+        const Z *bs = Bs + (kt % STAGES) * B_STAGE;
+#pragma unroll
+        for (int kk = 0; kk < BK; kk += 4) {
+            double ar[4], ai[4], br[2], bi[2], nbi[2];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const Z a = as[(kk + tq) * ALD + wm * 32 + i * 8 + gq];
+                ar[i] = a.x;
+                ai[i] = a.y;
+            }
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                const Z b = bs[(wn * 16 + j * 8 + gq) * BLD + kk + tq];
+                br[j] = b.x;
+                bi[j] = b.y;
+                nbi[j] = -b.y;
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    dmma884(cr[i][j][0], cr[i][j][1], ar[i], br[j]);
+                    dmma884(cr[i][j][0], cr[i][j][1], ai[i], nbi[j]);
+                    dmma884(ci[i][j][0], ci[i][j][1], ar[i], bi[j]);
+                    dmma884(ci[i][j][0], ci[i][j][1], ai[i], br[j]);
+                }
+        }
+    }
+    cp_async_wait<0>();
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int col = n0 + wn * 16 + j * 8 + 2 * tq + h;
+            if (col >= g.N) continue;
+            Z *cp = g.C + (size_t)(g.ccol ? g.ccol[col] : col) * g.ldc;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int row = m0 + wm * 32 + i * 8 + gq;
+                if (row >= g.mlo && row < g.M) cp[row] = Z(cr[i][j][h], ci[i][j][h]);
+            }
+        }
+}
+
 }  // namespace xtg
