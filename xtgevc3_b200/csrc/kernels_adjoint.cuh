@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(256) diag_adjoint_real(DiagArgs<R> a)
             }
             Factors<R> F;
             factor_rows(F, sec, jnb, lane, smin, W);
-            back_substitute(r, F, sec, jnb, lane, W, tl);
+            back_substitute_loop(r, F, sec, jnb, lane, W, tl);
             R ys[2], yp[2];
 #pragma unroll
             for (int s = 0; s < 2; s++) {
@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(256) diag_adjoint_real(DiagArgs<R> a)
             }
             Factors<C> F;
             factor_rows(F, sec, jnb, lane, smin, W);
-            back_substitute(r, F, sec, jnb, lane, W, tl);
+            back_substitute_loop(r, F, sec, jnb, lane, W, tl);
             R ysr[2], ysi[2], ypr[2], ypi[2];
 #pragma unroll
             for (int s = 0; s < 2; s++) {

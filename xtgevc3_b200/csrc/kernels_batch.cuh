@@ -398,7 +398,7 @@ __device__ void solve_item(const TileCols<T, NT> &tc, int j, int r0, int r1, con
         }
         Factors<T> F;
         factor_rows(F, sec, nrows, lane, smin, W);
-        back_substitute(r, F, sec, nrows, lane, W);
+        back_substitute_loop(r, F, sec, nrows, lane, W);
         T x[2];
 #pragma unroll
         for (int s = 0; s < 2; s++) {
@@ -463,7 +463,7 @@ __device__ void solve_item(const TileCols<T, NT> &tc, int j, int r0, int r1, con
         }
         Factors<C> F;
         factor_rows(F, sec, nrows, lane, smin, W);
-        back_substitute(r, F, sec, nrows, lane, W);
+        back_substitute_loop(r, F, sec, nrows, lane, W);
         C x[2];
 #pragma unroll
         for (int s = 0; s < 2; s++) {

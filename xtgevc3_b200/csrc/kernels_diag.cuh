@@ -215,10 +215,55 @@ __device__ __forceinline__ void factor_rows(Factors<E> &F, uint64_t sec, int nro
 
 // Block back substitution of one eigenvector held in r (rows [jlo, nrows)); on return r
 // holds the solution in those rows (rows below jlo receive updates that mean nothing).
-// W(i, j) gives the shifted operator entry.  jlo must not split a 2x2 block.
+// W(i, j) gives the shifted operator entry.  jlo must not split a 2x2 block.  The row loop
+// is unrolled over the block's 64 rows, so every row index, register slot and lane test is
+// a constant; rows at or past nrows (uniform across the warp) are skipped.
 template <class E, class WF>
 __device__ __forceinline__ void back_substitute(E (&r)[2], const Factors<E> &F, uint64_t sec, int nrows, int lane,
                                                 WF W, int jlo = 0)
+{
+    bool skip = false;  // the row was consumed by the 2x2 block above it
+#pragma unroll
+    for (int j = kBlock - 1; j >= 0; j--) {
+        if (j >= nrows || j < jlo) continue;
+        if (skip) {
+            skip = false;
+            continue;
+        }
+        if (j >= 1 && ((sec >> j) & 1ull)) {
+            const int p = j - 1, q = j;
+            const E rp = shfl(r[p >> 5], p & 31);
+            const E rq = r[q >> 5];  // valid on the owner of q, which does the solve
+            const bool sw = F.sw[q >> 5];
+            const E ia = F.fa[q >> 5], b = F.fb[q >> 5], m = F.fm[q >> 5], iu = F.fu[q >> 5];
+            const E r1 = sw ? rq : rp, r2 = sw ? rp : rq;
+            E xq = (r2 - m * r1) * iu;
+            E xp = (r1 - b * xq) * ia;
+            xq = shfl(xq, q & 31);
+            xp = shfl(xp, q & 31);
+            if (lane == (p & 31)) r[p >> 5] = xp;
+            if (lane == (q & 31)) r[q >> 5] = xq;
+            if (p > 0) {
+                if (p >= 32 || lane < p) r[0] = r[0] - (W(lane, p) * xp + W(lane, q) * xq);
+                if (p > 32 && lane + 32 < p) r[1] = r[1] - (W(lane + 32, p) * xp + W(lane + 32, q) * xq);
+            }
+            skip = true;
+        } else {
+            const E x = shfl(r[j >> 5] * F.inv1[j >> 5], j & 31);
+            if (lane == (j & 31)) r[j >> 5] = x;
+            if (j > 0) {
+                if (j >= 32 || lane < j) r[0] = r[0] - W(lane, j) * x;
+                if (j > 32 && lane + 32 < j) r[1] = r[1] - W(lane + 32, j) * x;
+            }
+        }
+    }
+}
+
+// The same substitution as a runtime row loop (fewer registers: one code path per row
+// instead of 64): used where register pressure matters more than instructions per row.
+template <class E, class WF>
+__device__ __forceinline__ void back_substitute_loop(E (&r)[2], const Factors<E> &F, uint64_t sec, int nrows,
+                                                     int lane, WF W, int jlo = 0)
 {
     int j = nrows - 1;
     while (j >= jlo) {
@@ -226,7 +271,7 @@ __device__ __forceinline__ void back_substitute(E (&r)[2], const Factors<E> &F, 
             const int p = j - 1, q = j;
             const int sq = q >> 5;
             const E rp = shfl(row_of(r, p), p & 31);
-            const E rq = row_of(r, q);  // valid on the owner of q, which does the solve
+            const E rq = row_of(r, q);
             const bool sw = sq ? F.sw[1] : F.sw[0];
             const E ia = sq ? F.fa[1] : F.fa[0], b = sq ? F.fb[1] : F.fb[0];
             const E m = sq ? F.fm[1] : F.fm[0], iu = sq ? F.fu[1] : F.fu[0];
@@ -324,7 +369,7 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
             }
             Factors<R> F;
             factor_rows(F, sec, nrows, lane, smin, W);
-            back_substitute(r, F, sec, nrows, lane, W);
+            back_substitute_loop(r, F, sec, nrows, lane, W);
             // assemble the block column (solution rows, seed, zeros below the seed)
             R x[2];
 #pragma unroll
@@ -391,7 +436,7 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
             }
             Factors<C> F;
             factor_rows(F, sec, nrows, lane, smin, W);
-            back_substitute(r, F, sec, nrows, lane, W);
+            back_substitute_loop(r, F, sec, nrows, lane, W);
             C x[2];
 #pragma unroll
             for (int s = 0; s < 2; s++) {
