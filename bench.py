@@ -311,6 +311,22 @@ def load_traffic():
 
 
 
+def max_over_ranks(value, dist, torch, device="cuda"):
+    """The largest of the ranks' values (a time in ms, say); every rank gets it.  With no
+    process group (one GPU) the value itself."""
+    if not dist:
+        return float(value)
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_seeds(seed, batch_seed, rank):
+    """Seeds of one rank's inputs: each rank solves its own pencils (weak scaling)."""
+    return {"pencil": seed + rank, "q": 2 * seed + 1 + 7 * rank, "z": 2 * seed + 2 + 7 * rank,
+            "batch": batch_seed + 7919 * rank}
+
+
 def measure_form(name, flags, args, X, torch, data, dist, local, world):
     """Time K steps of one form (device-resident inputs), check the residual of the result,
     then trace K more steps for the per-kernel breakdown."""
@@ -339,11 +355,7 @@ def measure_form(name, flags, args, X, torch, data, dist, local, world):
     torch.cuda.synchronize()
     launches = X.launch_count() - l0
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1) / args.steps
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, torch)
     resid = residual_max(torch, S, P, ar, ai, be, Q, Z, VL, VR)
     X.trace_reset()
     X.trace_enable(True)
@@ -415,7 +427,7 @@ def measure_batched(args, X, torch, dist, world):
     configuration from the project's tuner) against a loop of per-pencil plain launches
     (xtgevc3_{d,s}tgevc3_dev) over the same pencils; both on device-resident inputs."""
     rank = int(os.environ.get("RANK", "0"))
-    sizes, plist, bufs = batched_inputs(args.batch_count, args.batch_seed + 7919 * rank, torch)
+    sizes, plist, bufs = batched_inputs(args.batch_count, rank_seeds(args.seed, args.batch_seed, rank)["batch"], torch)
     count = len(sizes)
     flops = float(np.sum(10.0 / 3.0 * sizes.astype(np.float64) ** 3))
     res = {}
@@ -438,10 +450,7 @@ def measure_batched(args, X, torch, dist, world):
         plan.wait()
         ms = e0.elapsed_time(e1) / args.steps
         launches = X.launch_count() - l0
-        if dist:
-            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ms, dist, torch)
         info = plan.info()
         # loop of plain per-pencil launches (in place, so VL/VR start as Q/Z each call)
         VLl = torch.empty_like(bufs[prec]["VL"])
@@ -655,11 +664,12 @@ def main():
                                 device_id=torch.device("cuda", local))
     n = args.n
     # inputs: one pencil per rank
-    S_h, P_h, ar, ai, be = host_pencil(n, args.seed + rank)
+    seeds = rank_seeds(args.seed, args.batch_seed, rank)
+    S_h, P_h, ar, ai, be = host_pencil(n, seeds["pencil"])
     S = colmajor_cuda(S_h, torch)
     P = colmajor_cuda(P_h, torch)
-    Q = orthogonal(n, 2 * args.seed + 1 + 7 * rank, torch)
-    Z = orthogonal(n, 2 * args.seed + 2 + 7 * rank, torch)
+    Q = orthogonal(n, seeds["q"], torch)
+    Z = orthogonal(n, seeds["z"], torch)
     VL = torch.empty_like(Q)
     VR = torch.empty_like(Z)
     data = (S, P, ar, ai, be, Q, Z, VL, VR)
@@ -751,11 +761,7 @@ def main():
                 e2e_t.append(t1 - t0)
     finally:
         X.set_flags(0)
-    e2e_s = float(np.mean(e2e_t))
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(float(np.mean(e2e_t)), dist, torch)
     # bytes the host path moves: S and P as their upper trapezoid in 512-column panels (rows
     # <= last column + 1), Q and Z whole in; VL and VR whole out
     trap = sum(min(n, j0 + 512 + 1) * (min(n, j0 + 512) - j0) for j0 in range(0, n, 512))
