@@ -125,7 +125,7 @@ int xtgevc3_ctgevc3_dev(unsigned flags, void *stream, char side, char howmny, co
  * not acceptable.  It calls no cudaMalloc/cudaFree or other allocating routine: its scratch
  * is one 8 MiB block of device memory inside the library, held on every GPU that loads
  * the library until exit, so problems are limited to what fits (SIDE='B', HOWMNY='B':
- * n <= 448); larger ones return 2 with a message in xtgevc3_last_error(), without device
+ * n <= 478); larger ones return 2 with a message in xtgevc3_last_error(), without device
  * work.  The first call on a device looks up the block's device address (make it before
  * any stream capture).  All calls share the block: calls whose work overlaps on the GPU
  * race and must be ordered by the caller (e.g. one stream).

@@ -176,3 +176,19 @@ def test_adjoint_argument_checks(prec, n, ld, null, msg):
     rc = L.xtgevc3_adjoint(prec, None, n, p, ld, p, ld, p, p, p, p, ld, p, ld, p, ld, p, ld)
     assert rc == -1
     assert msg in X.last_error(), X.last_error()
+
+
+def test_noalloc_refuses_oversize_before_device_work():
+    """xtgevc3_dtgevc3_dev_noalloc: the 8 MiB block holds SIDE='B', HOWMNY='B' up to n = 478;
+    n = 479 needs 8,393,728 bytes and is refused with return code 2 before any CUDA call
+    (so the device pointers here, never dereferenced, may be dummies)."""
+    L = X.lib()
+    n = 479
+    z, o = np.zeros(n), np.ones(n)
+    m, info = ct.c_int(0), ct.c_int(0)
+    dev = ct.c_void_p(0x1000)
+    host = [a.ctypes.data_as(ct.c_void_p) for a in (z, z, o)]
+    rc = L.xtgevc3_dtgevc3_dev_noalloc(None, b"B", b"B", None, n, dev, n, dev, n, *host, dev, n, dev, n, n,
+                                       ct.byref(m), ct.byref(info))
+    assert rc == 2
+    assert "n=479" in X.last_error() and "8393728 bytes" in X.last_error(), X.last_error()

@@ -111,10 +111,6 @@ int run_host(char side, char howmny, const int *select, int n, const void *S, in
         return fail(e, "cudaMallocAsync");
     if (want_r && (e = cudaMallocAsync(&r.dVR, (size_t)ld * vcols * sizeof(E), r.st)) != cudaSuccess)
         return fail(e, "cudaMallocAsync");
-    // the output buffers are written by the second stream (Q, Z) and the copies out
-    if ((e = cudaEventRecord(r.ev[0], r.st)) != cudaSuccess) return fail(e, "event");
-    if ((e = cudaStreamWaitEvent(r.sin, r.ev[0], 0)) != cudaSuccess) return fail(e, "event");
-    const size_t w = (size_t)n * sizeof(E);
     const int panel = 512;
     for (int which = 0; which < 2; which++) {
         void *dst = which ? r.dP : r.dS;
@@ -129,23 +125,30 @@ int run_host(char side, char howmny, const int *select, int n, const void *S, in
             if (e != cudaSuccess) return fail(e, which ? "H2D P" : "H2D S");
         }
     }
-    (void)w;
     xtg::Options opt = make_opts(flags);
+    // Q and Z (second stream) go after every copy that the solve's first kernels need: S and
+    // P, the eigenvalues and the column lists (the solver calls `staged` once those are
+    // queued).  The back-transform needs Q or Z only at the end; queued earlier, their 2n^2
+    // elements would hold the small copies behind them on the copy engine and split the
+    // link's host-to-device bandwidth with S and P.  The wait also orders the second stream
+    // after the allocations of the output buffers it writes.
+    cudaError_t in_err = cudaSuccess;
     if (back) {
-        if (want_r) {
-            if ((e = cudaMemcpy2DAsync(r.dVR, ld * sizeof(E), VR, (size_t)ldvr * sizeof(E), (size_t)n * sizeof(E),
-                                       n, cudaMemcpyHostToDevice, r.sin)))
-                return fail(e, "H2D Z");
-            if ((e = cudaEventRecord(r.ev[0], r.sin)) != cudaSuccess) return fail(e, "event");
-            opt.back_ready[0] = r.ev[0];
-        }
-        if (want_l) {
-            if ((e = cudaMemcpy2DAsync(r.dVL, ld * sizeof(E), VL, (size_t)ldvl * sizeof(E), (size_t)n * sizeof(E),
-                                       n, cudaMemcpyHostToDevice, r.sin)))
-                return fail(e, "H2D Q");
-            if ((e = cudaEventRecord(r.ev[1], r.sin)) != cudaSuccess) return fail(e, "event");
-            opt.back_ready[1] = r.ev[1];
-        }
+        opt.back_ready[0] = want_r ? r.ev[0] : nullptr;
+        opt.back_ready[1] = want_l ? r.ev[1] : nullptr;
+        opt.staged = [&](cudaStream_t sst) {
+            cudaError_t x = cudaEventRecord(r.ev[2], sst);
+            if (x == cudaSuccess) x = cudaStreamWaitEvent(r.sin, r.ev[2], 0);
+            if (x == cudaSuccess && want_r)
+                x = cudaMemcpy2DAsync(r.dVR, ld * sizeof(E), VR, (size_t)ldvr * sizeof(E), (size_t)n * sizeof(E), n,
+                                      cudaMemcpyHostToDevice, r.sin);
+            if (x == cudaSuccess && want_r) x = cudaEventRecord(r.ev[0], r.sin);
+            if (x == cudaSuccess && want_l)
+                x = cudaMemcpy2DAsync(r.dVL, ld * sizeof(E), VL, (size_t)ldvl * sizeof(E), (size_t)n * sizeof(E), n,
+                                      cudaMemcpyHostToDevice, r.sin);
+            if (x == cudaSuccess && want_l) x = cudaEventRecord(r.ev[1], r.sin);
+            if (x != cudaSuccess) in_err = x;
+        };
     }
     cudaError_t out_err = cudaSuccess;
     // download output columns [o0, o1) of one side once its stream reaches this point
@@ -175,6 +178,7 @@ int run_host(char side, char howmny, const int *select, int n, const void *S, in
     int rc = xtg::solve_device<R, CPLX>(side, howmny, select, n, r.dS, ld, r.dP, ld, alpha, alphai, beta,
                                         want_l ? r.dVL : nullptr, ld, want_r ? r.dVR : nullptr, ld, count, opt, r.st);
     if (rc) return 1;
+    if (in_err != cudaSuccess) return fail(in_err, "H2D Q/Z");
     if (out_err != cudaSuccess) return fail(out_err, "D2H");
     if ((e = cudaStreamSynchronize(r.sout)) != cudaSuccess) return fail(e, "cudaStreamSynchronize");
     cudaFreeAsync(r.dS, r.st);

@@ -133,12 +133,15 @@ size_t arena_bytes_needed(int n, int m, bool right, bool left, bool back, bool n
     auto r256 = [](size_t b) { return (std::max<size_t>(b, 1) + 255) & ~size_t(255); };
     const size_t esz = cplx ? 2 * rsz : rsz, ld = (size_t)round_up(n, 32);
     const size_t nn = (size_t)n, mm = (size_t)m;
-    const size_t shared = r256(rsz * (cplx ? 4 : 3) * nn) + r256(rsz * 2 * nn) + r256(rsz * 2);
+    // eigenvalues, column sums, norms; then each side's column lists (uploaded before either
+    // side starts, so they stay allocated for the whole call)
+    const size_t cols = r256(sizeof(int) * 5 * mm) + r256(mm);
+    const size_t shared = r256(rsz * (cplx ? 4 : 3) * nn) + r256(rsz * 2 * nn) + r256(rsz * 2) +
+                          (right ? cols : 0) + (left ? cols : 0);
     auto side = [&](bool lft) {
         size_t b = 0;
         if (lft) b += 2 * r256(esz * ld * nn);
-        b += r256(esz * ld * mm) + r256(esz * 4 * kBlock * mm) + r256(rsz * (cplx ? 6 : 4) * mm) +
-             r256(sizeof(int) * 5 * mm) + r256(mm);
+        b += r256(esz * ld * mm) + r256(esz * 4 * kBlock * mm) + r256(rsz * (cplx ? 6 : 4) * mm);
         if (back) b += r256(esz * ld * nn);
         if (normalize && !cplx) b += r256(mm);
         return b;
@@ -364,8 +367,66 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
     const R bignum = R(1) / (safemin / eps);
     const int ld_n = round_up(n, 32);
 
+    // ---- column lists of each side (problem orientation) and their device copies ------------
+    // Both sides' lists go to the device on the call's stream before either side starts, so
+    // that every host-to-device copy of the call's own is queued before `opt.staged` runs.
+    struct SideCols {
+        ColList L;
+        std::vector<int> starts;  // columns that start an eigenvector (diagonal-solve items)
+        const int *d_ints = nullptr;  // colk, src, kext, outcol, starts: m ints each
+        const uint8_t *d_kind = nullptr;
+    };
+    auto build_cols = [&](bool left, SideCols &sc) -> int {
+        ColList &L = sc.L;
+        const int m = m_total;
+        L.m = m;
+        L.colk.resize(m);
+        L.src.resize(m);
+        L.kext.resize(m);
+        L.outcol.resize(m);
+        L.kind.resize(m);
+        int c = 0;
+        auto emit = [&](const Item &it) {
+            int kk = left ? (it.pair ? n - 2 - it.k : n - 1 - it.k) : it.k;
+            int w = it.pair ? 2 : 1;
+            for (int q = 0; q < w; q++) {
+                L.colk[c] = kk;
+                L.src[c] = it.k;
+                L.kext[c] = kk + w;
+                L.outcol[c] = it.out + q;
+                L.kind[c] = it.pair ? (q == 0 ? kPairRe : kPairIm) : kReal;
+                c++;
+            }
+        };
+        if (!left) for (const Item &it : items) emit(it);
+        else for (auto it = items.rbegin(); it != items.rend(); ++it) emit(*it);
+        sc.starts.reserve(m);
+        for (int q = 0; q < m; q++)
+            if (L.kind[q] != kPairIm) sc.starts.push_back(q);
+        int *d_ints = scr.get<int>(5 * (size_t)m);
+        uint8_t *d_kind = scr.get<uint8_t>((size_t)m);
+        if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
+        std::vector<int> ints(5 * (size_t)m, 0);
+        std::copy(L.colk.begin(), L.colk.end(), ints.begin());
+        std::copy(L.src.begin(), L.src.end(), ints.begin() + m);
+        std::copy(L.kext.begin(), L.kext.end(), ints.begin() + 2 * m);
+        std::copy(L.outcol.begin(), L.outcol.end(), ints.begin() + 3 * m);
+        std::copy(sc.starts.begin(), sc.starts.end(), ints.begin() + 4 * m);
+        XTG_CK(cudaMemcpyAsync(d_ints, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        XTG_CK(cudaMemcpyAsync(d_kind, L.kind.data(), m, cudaMemcpyHostToDevice, st));
+        sc.d_ints = d_ints;
+        sc.d_kind = d_kind;
+        return 0;
+    };
+    SideCols side_cols[2];
+    if (want_r && build_cols(false, side_cols[0])) return 1;
+    if (want_l && build_cols(true, side_cols[1])) return 1;
+    if (opt.staged) opt.staged(st);
+
     // One side on stream `st` with scratch from `scr` (both shadow the call's own).
     auto run_side = [&](bool left, cudaStream_t st, Scratch &scr) -> int {
+        const SideCols &sc = side_cols[left ? 1 : 0];
+        const ColList &L = sc.L;
         SplitBufs sbuf;
         cudaError_t split_err = cudaSuccess;
         // C (+)= A B of one update or back-transform launch, FP64 DMMA/SIMT or BF16 slices
@@ -384,31 +445,6 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             }
             launch_gemm<E>(g, opt.simt != 0, gs);
         };
-        // ---- column list in problem orientation ---------------------------------------
-        ColList L;
-        L.m = m_total;
-        L.colk.resize(m_total);
-        L.src.resize(m_total);
-        L.kext.resize(m_total);
-        L.outcol.resize(m_total);
-        L.kind.resize(m_total);
-        {
-            int c = 0;
-            auto emit = [&](const Item &it) {
-                int kk = left ? (it.pair ? n - 2 - it.k : n - 1 - it.k) : it.k;
-                int w = it.pair ? 2 : 1;
-                for (int q = 0; q < w; q++) {
-                    L.colk[c] = kk;
-                    L.src[c] = it.k;
-                    L.kext[c] = kk + w;
-                    L.outcol[c] = it.out + q;
-                    L.kind[c] = it.pair ? (q == 0 ? kPairRe : kPairIm) : kReal;
-                    c++;
-                }
-            };
-            if (!left) for (const Item &it : items) emit(it);
-            else for (auto it = items.rbegin(); it != items.rend(); ++it) emit(*it);
-        }
         // row blocks (problem orientation), bottom to top; a 2x2 block is never split
         auto split = [&](int j) -> bool {  // rows j-1, j form a 2x2 diagonal block
             if (CPLX || j <= 0 || j >= n) return false;
@@ -442,10 +478,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         }
         const int ldx = ld_n, ldy = 4 * kBlock;  // two halves of two padded row blocks
         // work items of the diagonal solves: every column that starts an eigenvector
-        std::vector<int> items;
-        items.reserve(m);
-        for (int c = 0; c < m; c++)
-            if (L.kind[c] != kPairIm) items.push_back(c);
+        const std::vector<int> &items = sc.starts;
         const int nitems = (int)items.size();
         // look-ahead (XTGEVC3_LOOKAHEAD): the trailing update of a block pair runs on a second
         // stream while the next pair is solved (see the loop below); off while tracing
@@ -458,17 +491,9 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         E *Y = Ybuf[0];
         R *pending = ahead ? scr.get<R>((size_t)m) : nullptr;
         R *coef = scr.get<R>((size_t)ncoef * m);
-        int *d_ints = scr.get<int>(5 * (size_t)m);
-        uint8_t *d_kind = scr.get<uint8_t>((size_t)m);
         if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
-        std::vector<int> ints(5 * (size_t)m, 0);
-        std::copy(L.colk.begin(), L.colk.end(), ints.begin());
-        std::copy(L.src.begin(), L.src.end(), ints.begin() + m);
-        std::copy(L.kext.begin(), L.kext.end(), ints.begin() + 2 * m);
-        std::copy(L.outcol.begin(), L.outcol.end(), ints.begin() + 3 * m);
-        std::copy(items.begin(), items.end(), ints.begin() + 4 * m);
-        XTG_CK(cudaMemcpyAsync(d_ints, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-        XTG_CK(cudaMemcpyAsync(d_kind, L.kind.data(), m, cudaMemcpyHostToDevice, st));
+        const int *d_ints = sc.d_ints;
+        const uint8_t *d_kind = sc.d_kind;
         const int *d_colk = d_ints, *d_src = d_ints + m, *d_kext = d_ints + 2 * m, *d_outcol = d_ints + 3 * m;
         const int *d_items = d_ints + 4 * m;
         XTG_CK(cudaMemsetAsync(X, 0, (size_t)ldx * m * sizeof(E), st));

@@ -21,6 +21,11 @@ struct Options {
     // Z / Q on another stream), and side_done is called once a side's last kernel is
     // queued, with that side's stream (the result can be downloaded behind the other side).
     cudaEvent_t back_ready[2] = {nullptr, nullptr};  // right, left
+    // Called once, with the call's stream, after every host-to-device copy of the call's own
+    // (eigenvalues, column lists) is queued and before any side's kernels are: uploads that
+    // only the back-transform needs start from here (an event recorded on this stream), so
+    // the copy engine does not queue the small copies that start the solve behind them.
+    std::function<void(cudaStream_t st)> staged;
     std::function<void(bool left, cudaStream_t st)> side_done;
     // HOWMNY='B' without normalisation: the back-transform runs in column chunks and this
     // is called after each with the output columns [o0, o1) it completed.

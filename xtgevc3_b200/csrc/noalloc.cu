@@ -11,7 +11,7 @@
 // The block: g_noalloc_scratch below, kNoAllocBytes = 8 MiB, declared at file scope.
 // Every GPU on which the library is loaded holds these 8 MiB until the process exits.
 // That bounds the problem size: a call is accepted when the scratch it needs fits
-// (arena_bytes_needed); for SIDE='B', HOWMNY='B' that is n <= 448.  Larger calls are
+// (arena_bytes_needed); for SIDE='B', HOWMNY='B' that is n <= 478.  Larger calls are
 // rejected before any device work with return code 2 and a message in
 // xtgevc3_last_error().
 //
