@@ -130,6 +130,33 @@ def test_graded_complex_scale_guards(cuda_ok):
     assert r[finite_eig].max() < 100, r[finite_eig].max()
 
 
+@pytest.mark.parametrize("dt", [np.float64, np.complex128], ids=["d", "z"])
+def test_growth_guards_random_triangular(cuda_ok, dt):
+    """n = 2048 random triangular pencils with the structure of the upstream test
+    generators (U(-1,1) parts, |P_kk| pushed away from 0; real: 2x2 blocks as well).  Close
+    eigenvalues make many eigenvectors grow by more than 1e300 across the matrix, so the
+    overflow guards rescale hundreds of columns, in lower and upper blocks of block pairs
+    and inside 64-row blocks.  Both sides must be finite, match the oracle column by column
+    (1e-11) and have a DGET52-style residual below 100."""
+    n, seed = 2048, 8213
+    if dt == np.float64:
+        S, P, al, ai, be = pencils.gen_quasi_triangular(n, seed)
+    else:
+        (S, P, al, be), ai = pencils.gen_upper_triangular_complex(n, seed), None
+    I = np.eye(n, dtype=dt, order="F")
+    d = dict(side="B", howmny="A", S=S, P=P, alpha=al, beta=be, alphai=ai, VL_in=I, VR_in=I.copy(order="F"),
+             name="random")
+    ref = oracle.tgevc3("B", "A", S, P, al, be, alphai=ai)
+    VL, VR, m, info = run_gpu(d)
+    assert (m, info) == (ref[2], ref[3]) == (n, 0)
+    assert np.isfinite(VL).all() and np.isfinite(VR).all()
+    # a real eigenvalue's column starts from x_k = 1: |x_k| < 1 means a guard rescaled it
+    unit_seed = np.ones(n, bool) if ai is None else (ai == 0)
+    guarded = int((np.abs(np.diag(as_complex(VR, d)))[unit_seed] < 1).sum())
+    assert guarded >= 50, guarded  # the case exercises the guards
+    compare(d, VL, VR, m, ref[0], ref[1], TOL_WELL[dt])
+
+
 def test_selection_and_one_sided(cuda_ok):
     p = _pencil("gges", 150, 41, np.float64)
     rng = np.random.default_rng(0)

@@ -80,3 +80,24 @@ def test_oracle_lwork_and_info():
     # LWORK too small even for block size 1
     _, _, m, info = oracle.tgevc3("B", "A", S, P, ar, be, alphai=ai, lwork=10)
     assert info == -19
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="upstream library not built (oracle/Makefile ref)")
+@pytest.mark.parametrize("prec", ["d", "z"])
+def test_oracle_matches_upstream_library_with_many_guards(prec):
+    """n = 2048 random triangular pencils (upstream test-generator structure) on which the
+    overflow guards rescale hundreds of columns: the oracle against the upstream library
+    built from its sources, SIDE='R'.  Guard scale factors are computed from maxima that
+    differ in rounding, so the columns are compared after normalisation (1e-11)."""
+    from xtgevc3_b200 import pencils
+    if prec == "d":
+        S, P, al, ai, be = pencils.gen_quasi_triangular(2048, 8213)
+    else:
+        (S, P, al, be), ai = pencils.gen_upper_triangular_complex(2048, 8213), None
+    o = oracle.tgevc3("R", "A", S, P, al, be, alphai=ai, impl="oracle")[1]
+    r = oracle.tgevc3("R", "A", S, P, al, be, alphai=ai, impl="ref")[1]
+    assert np.isfinite(o).all() and np.isfinite(r).all()
+    if ai is not None:
+        o, r = oracle.to_complex_real_storage(o, ai), oracle.to_complex_real_storage(r, ai)
+    err, _ = oracle.max_rel_diff(o, r)
+    assert err < 1e-11, err

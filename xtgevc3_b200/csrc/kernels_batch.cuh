@@ -398,7 +398,15 @@ __device__ void solve_item(const TileCols<T, NT> &tc, int j, int r0, int r1, con
         }
         Factors<T> F;
         factor_rows(F, sec, nrows, lane, smin, W);
-        back_substitute_loop(r, F, sec, nrows, lane, W);
+        auto mid = [&](T (&rr)[2], int jtop) {
+            const T mx = warp_max(lane <= jtop ? fabs(rr[0]) : T(0));
+            if (mx > thr_rhs) {
+                const T sc = thr_rhs / mx;
+                rr[0] *= sc; rr[1] *= sc; seed *= sc;
+                if (!diag) { scale_col(colr, XLD, 0, r0, sc, lane); scale_col(colr, XLD, r1, top + 1, sc, lane); }
+            }
+        };
+        back_substitute_loop(r, F, sec, nrows, lane, W, 0, mid);
         T x[2];
 #pragma unroll
         for (int s = 0; s < 2; s++) {
@@ -463,7 +471,18 @@ __device__ void solve_item(const TileCols<T, NT> &tc, int j, int r0, int r1, con
         }
         Factors<C> F;
         factor_rows(F, sec, nrows, lane, smin, W);
-        back_substitute_loop(r, F, sec, nrows, lane, W);
+        auto mid = [&](C (&rr)[2], int jtop) {
+            const T mx = warp_max(lane <= jtop ? fmax(fabs(rr[0].x), fabs(rr[0].y)) : T(0));
+            if (mx > thr_rhs) {
+                const T sc = thr_rhs / mx;
+                rr[0] = sc * rr[0]; rr[1] = sc * rr[1]; seed0 = sc * seed0; seed1 = sc * seed1;
+                if (!diag) {
+                    scale_col(colr, XLD, 0, r0, sc, lane); scale_col(colr, XLD, r1, top + 1, sc, lane);
+                    scale_col(coli, XLD, 0, r0, sc, lane); scale_col(coli, XLD, r1, top + 1, sc, lane);
+                }
+            }
+        };
+        back_substitute_loop(r, F, sec, nrows, lane, W, 0, mid);
         C x[2];
 #pragma unroll
         for (int s = 0; s < 2; s++) {
@@ -648,7 +667,24 @@ __device__ void solve_group(const TileCols<T, NT> &tc, const int *list, int cnt,
             }
         }
         // back substitution, warp-uniform row loop
+        bool checked = H <= kMidRow || maxn <= kMidRow;  // blocks of H <= 32 rows need no check
         for (int jr = maxn - 1; jr >= 0;) {
+            if (H > kMidRow && !checked && jr < kMidRow) {  // growth check of the block's upper rows
+                checked = true;
+                T mx = T(0);
+#pragma unroll
+                for (int q = 0; q < R; q++)
+                    if (gl + G * q <= jr) mx = fmax(mx, cmag(r[q]));
+                mx = group_max<G>(mx);
+                if (nrows > kMidRow && mx > thr_rhs) {
+                    const T sc = thr_rhs / mx;
+#pragma unroll
+                    for (int q = 0; q < R; q++) r[q] = sc * r[q];
+                    seed0 = sc * seed0;
+                    seed1 = sc * seed1;
+                    scale_outside(sc);
+                }
+            }
             const bool act = jr < nrows;
             if (jr >= 1 && ((sec >> jr) & 1ull)) {
                 const int pr = jr - 1, qr = jr;

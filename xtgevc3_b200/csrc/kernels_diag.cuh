@@ -27,7 +27,10 @@
 //   * before the update: if max(|ac x|, |b x|) > bignum/jnb, scale the column
 //     (src/dtgevc3.cpp:1404-1426, with the panel width replaced by the block height).
 // Scaling a column means scaling every stored row of it: the accumulated rows above the
-// block, the rows solved in earlier blocks and the current block.
+// block, the rows solved in earlier blocks and the current block, and (upper block of a
+// pair) the lower block's rows of the pair's update operand, not yet consumed.  A third
+// check, inside the block once its rows at and above kMidRow are solved, keeps at most 32
+// rows between checks, as upstream's 32-row local solves do.
 //
 // Output: X[I, c] (solution), and this block's rows of the stacked update operand
 //   Y[ys_off + i, c] = -ac * x_i,  Y[ys_off + yhalf + i, c] = b * x_i   (zero padded)
@@ -101,7 +104,8 @@ struct DiagArgs {
     // update operand layout: this block's -ac x rows start at Y row ys_off, its b x rows at
     // ys_off + yhalf; ypad (>= r1 - r0) rows are written, zeros past the block.  For a
     // column whose eigenvalue lies in this block, rows [zl_off, zl_off + zl_len) of both
-    // halves (a lower block of the same update, where such a column is zero) are zeroed.
+    // halves (a lower block of the same update, where such a column is zero) are zeroed;
+    // for the other columns a guard rescales them with the column (scale_lower_y).
     int ys_off, yhalf, ypad, zl_off, zl_len;
     const int *items;        // columns that start an eigenvector (a pair's Re column), ascending
     int it0, nitems;         // items [it0, nitems) are active in this block
@@ -140,6 +144,20 @@ __device__ __forceinline__ void scale_above(const DiagArgs<R> &a, E *col, int c,
     }
     scale_rows(col, a.safe_lo < a.r0 ? a.safe_lo : a.r0, a.r0, s, lane);
     if (lane == 0) a.pending[c] *= s;
+}
+
+// The upper block of a pair: the lower block's rows of the update operand (rows [zl_off,
+// zl_off + zl_len) of both halves, written by the lower block's solve) are consumed by the
+// pair's trailing update together with this block's rows.  A guard that rescales a column
+// here rescales those rows too, so that the two blocks' operands carry the same scale
+// (upstream applies each block's update before the next solve and has no such operand).
+template <class E, class R>
+__device__ __forceinline__ void scale_lower_y(const DiagArgs<R> &a, E *ycol, R s, int lane)
+{
+    for (int i = lane; i < a.zl_len; i += 32) {
+        ycol[a.zl_off + i] = s * ycol[a.zl_off + i];
+        ycol[a.zl_off + a.yhalf + i] = s * ycol[a.zl_off + a.yhalf + i];
+    }
 }
 
 // Write this block's rows of one update-operand column: ys = -ac x, yp = b x for rows
@@ -213,22 +231,42 @@ __device__ __forceinline__ void factor_rows(Factors<E> &F, uint64_t sec, int nro
     }
 }
 
+// Growth check inside a block.  Upstream checks the right-hand side before every local
+// solve of at most 32 rows (`max |rhs| > bignum/10`, src/ztgevc3.cpp:183-199, bsize = 32 at
+// :454; src/dtgevc3.cpp:688-698); a block here has up to 64 rows, so the substitution calls
+// mid(r, jtop) once every row at or above kMidRow is solved, where rows [0, jtop] hold the
+// partially updated right-hand side of the block's upper rows.  Without it, a column that
+// enters the block near bignum/10 can overflow within the block where upstream's solves stay
+// finite.  NoMid is the unguarded form.
+constexpr int kMidRow = 32;
+struct NoMid {
+    template <class E>
+    __device__ __forceinline__ void operator()(E (&)[2], int) const {}
+};
+
 // Block back substitution of one eigenvector held in r (rows [jlo, nrows)); on return r
 // holds the solution in those rows (rows below jlo receive updates that mean nothing).
 // W(i, j) gives the shifted operator entry.  jlo must not split a 2x2 block.  The row loop
 // is unrolled over the block's 64 rows, so every row index, register slot and lane test is
 // a constant; rows at or past nrows (uniform across the warp) are skipped.
-template <class E, class WF>
+template <class E, class WF, class MF = NoMid>
 __device__ __forceinline__ void back_substitute(E (&r)[2], const Factors<E> &F, uint64_t sec, int nrows, int lane,
-                                                WF W, int jlo = 0)
+                                                WF W, int jlo = 0, MF mid = MF())
 {
     bool skip = false;  // the row was consumed by the 2x2 block above it
+    bool checked = nrows <= kMidRow;
 #pragma unroll
     for (int j = kBlock - 1; j >= 0; j--) {
         if (j >= nrows || j < jlo) continue;
         if (skip) {
             skip = false;
             continue;
+        }
+        // the first unsolved row below kMidRow is kMidRow - 1, or kMidRow - 2 when a 2x2
+        // block took rows (kMidRow - 1, kMidRow): two call sites, not one per row
+        if ((j == kMidRow - 1 || j == kMidRow - 2) && !checked) {
+            checked = true;
+            mid(r, j);
         }
         if (j >= 1 && ((sec >> j) & 1ull)) {
             const int p = j - 1, q = j;
@@ -261,12 +299,12 @@ __device__ __forceinline__ void back_substitute(E (&r)[2], const Factors<E> &F, 
 
 // The same substitution as a runtime row loop (fewer registers: one code path per row
 // instead of 64): used where register pressure matters more than instructions per row.
-template <class E, class WF>
+template <class E, class WF, class MF = NoMid>
 __device__ __forceinline__ void back_substitute_loop(E (&r)[2], const Factors<E> &F, uint64_t sec, int nrows,
-                                                     int lane, WF W, int jlo = 0)
+                                                     int lane, WF W, int jlo = 0, MF mid = MF())
 {
-    int j = nrows - 1;
-    while (j >= jlo) {
+    // one row, or the 2x2 block ending at row j; returns the next unsolved row
+    auto step = [&](int j) -> int {
         if (j >= 1 && ((sec >> j) & 1ull)) {
             const int p = j - 1, q = j;
             const int sq = q >> 5;
@@ -284,15 +322,20 @@ __device__ __forceinline__ void back_substitute_loop(E (&r)[2], const Factors<E>
             set_row(r, q, lane, xq);
             if (lane < p) r[0] = r[0] - (W(lane, p) * xp + W(lane, q) * xq);
             if (p > 32 && lane + 32 < p) r[1] = r[1] - (W(lane + 32, p) * xp + W(lane + 32, q) * xq);
-            j -= 2;
-        } else {
-            const E x = shfl((j >> 5) ? r[1] * F.inv1[1] : r[0] * F.inv1[0], j & 31);
-            set_row(r, j, lane, x);
-            if (lane < j) r[0] = r[0] - W(lane, j) * x;
-            if (j > 32 && lane + 32 < j) r[1] = r[1] - W(lane + 32, j) * x;
-            j -= 1;
+            return j - 2;
         }
-    }
+        const E x = shfl((j >> 5) ? r[1] * F.inv1[1] : r[0] * F.inv1[0], j & 31);
+        set_row(r, j, lane, x);
+        if (lane < j) r[0] = r[0] - W(lane, j) * x;
+        if (j > 32 && lane + 32 < j) r[1] = r[1] - W(lane + 32, j) * x;
+        return j - 1;
+    };
+    // rows at and above kMidRow, the growth check, then the rest (no per-row test)
+    int j = nrows - 1;
+    const int jsplit = jlo > kMidRow ? jlo : kMidRow;
+    while (j >= jsplit) j = step(j);
+    if (nrows > kMidRow && j >= jlo) mid(r, j);
+    while (j >= jlo) j = step(j);
 }
 
 // bit j set: rows (j-1, j) of the block form a 2x2 block, pairing greedily from the bottom
@@ -364,12 +407,26 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
                 if (mx > a.thr_rhs) {
                     R sc = a.thr_rhs / mx;
                     r[0] *= sc; r[1] *= sc; seed *= sc;
-                    if (!diag) { scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane); }
+                    if (!diag) {
+                        scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane);
+                        scale_lower_y(a, a.Y + (size_t)c * a.ldy, sc, lane);
+                    }
                 }
             }
             Factors<R> F;
             factor_rows(F, sec, nrows, lane, smin, W);
-            back_substitute_loop(r, F, sec, nrows, lane, W);
+            auto mid = [&](R (&rr)[2], int jtop) {
+                const R mx = warp_max(lane <= jtop ? fabs(rr[0]) : R(0));
+                if (mx > a.thr_rhs) {
+                    const R sc = a.thr_rhs / mx;
+                    rr[0] *= sc; rr[1] *= sc; seed *= sc;
+                    if (!diag) {
+                        scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane);
+                        scale_lower_y(a, a.Y + (size_t)c * a.ldy, sc, lane);
+                    }
+                }
+            };
+            back_substitute_loop(r, F, sec, nrows, lane, W, 0, mid);
             // assemble the block column (solution rows, seed, zeros below the seed)
             R x[2];
 #pragma unroll
@@ -381,7 +438,10 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
             if (mx > a.thr_upd) {
                 R sc = a.thr_upd / mx;
                 x[0] *= sc; x[1] *= sc;
-                if (!diag) { scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane); }
+                if (!diag) {
+                    scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane);
+                    scale_lower_y(a, a.Y + (size_t)c * a.ldy, sc, lane);
+                }
             }
             R ys[2], yp[2];
 #pragma unroll
@@ -431,12 +491,27 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
                     if (!diag) {
                         scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane);
                         scale_above(a, coli, c + 1, sc, lane); scale_rows(coli, a.r1, top + 1, sc, lane);
+                        scale_lower_y(a, a.Y + (size_t)c * a.ldy, sc, lane);
+                        scale_lower_y(a, a.Y + (size_t)(c + 1) * a.ldy, sc, lane);
                     }
                 }
             }
             Factors<C> F;
             factor_rows(F, sec, nrows, lane, smin, W);
-            back_substitute_loop(r, F, sec, nrows, lane, W);
+            auto mid = [&](C (&rr)[2], int jtop) {
+                const R mx = warp_max(lane <= jtop ? fmax(fabs(rr[0].x), fabs(rr[0].y)) : R(0));
+                if (mx > a.thr_rhs) {
+                    const R sc = a.thr_rhs / mx;
+                    rr[0] = sc * rr[0]; rr[1] = sc * rr[1]; seed0 = sc * seed0; seed1 = sc * seed1;
+                    if (!diag) {
+                        scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane);
+                        scale_above(a, coli, c + 1, sc, lane); scale_rows(coli, a.r1, top + 1, sc, lane);
+                        scale_lower_y(a, a.Y + (size_t)c * a.ldy, sc, lane);
+                        scale_lower_y(a, a.Y + (size_t)(c + 1) * a.ldy, sc, lane);
+                    }
+                }
+            };
+            back_substitute_loop(r, F, sec, nrows, lane, W, 0, mid);
             C x[2];
 #pragma unroll
             for (int s = 0; s < 2; s++) {
@@ -456,6 +531,8 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
                 if (!diag) {
                     scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane);
                     scale_above(a, coli, c + 1, sc, lane); scale_rows(coli, a.r1, top + 1, sc, lane);
+                    scale_lower_y(a, a.Y + (size_t)c * a.ldy, sc, lane);
+                    scale_lower_y(a, a.Y + (size_t)(c + 1) * a.ldy, sc, lane);
                 }
             }
             R ysr[2], ysi[2], ypr[2], ypi[2];
@@ -521,12 +598,26 @@ __global__ void __launch_bounds__(256) diag_solve_cplx(DiagArgs<R> a)
             if (mx > a.thr_rhs) {
                 R sc = a.thr_rhs / mx;
                 r[0] = sc * r[0]; r[1] = sc * r[1]; seed = sc * seed;
-                if (!diag) { scale_above(a, col, c, sc, lane); scale_rows(col, a.r1, top + 1, sc, lane); }
+                if (!diag) {
+                    scale_above(a, col, c, sc, lane); scale_rows(col, a.r1, top + 1, sc, lane);
+                    scale_lower_y(a, Y + (size_t)c * a.ldy, sc, lane);
+                }
             }
         }
         Factors<C> F;
         factor_rows(F, 0ull, nrows, lane, smin, W);
-        back_substitute(r, F, 0ull, nrows, lane, W);
+        auto mid = [&](C (&rr)[2], int jtop) {
+            const R mx = warp_max(lane <= jtop ? l1abs(rr[0]) : R(0));
+            if (mx > a.thr_rhs) {
+                const R sc = a.thr_rhs / mx;
+                rr[0] = sc * rr[0]; rr[1] = sc * rr[1]; seed = sc * seed;
+                if (!diag) {
+                    scale_above(a, col, c, sc, lane); scale_rows(col, a.r1, top + 1, sc, lane);
+                    scale_lower_y(a, Y + (size_t)c * a.ldy, sc, lane);
+                }
+            }
+        };
+        back_substitute(r, F, 0ull, nrows, lane, W, 0, mid);
         C x[2];
 #pragma unroll
         for (int s = 0; s < 2; s++) {
@@ -540,7 +631,10 @@ __global__ void __launch_bounds__(256) diag_solve_cplx(DiagArgs<R> a)
         if (mx > a.thr_upd) {
             R sc = a.thr_upd / mx;
             x[0] = sc * x[0]; x[1] = sc * x[1];
-            if (!diag) { scale_above(a, col, c, sc, lane); scale_rows(col, a.r1, top + 1, sc, lane); }
+            if (!diag) {
+                scale_above(a, col, c, sc, lane); scale_rows(col, a.r1, top + 1, sc, lane);
+                scale_lower_y(a, Y + (size_t)c * a.ldy, sc, lane);
+            }
         }
         C ys[2], yp[2];
 #pragma unroll
