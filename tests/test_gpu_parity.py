@@ -157,6 +157,45 @@ def test_growth_guards_random_triangular(cuda_ok, dt):
     compare(d, VL, VR, m, ref[0], ref[1], TOL_WELL[dt])
 
 
+@pytest.mark.parametrize("dt", [np.float64, np.complex128], ids=["d", "z"])
+def test_growth_cap_graded_left(cuda_ok, dt):
+    """n = 4096 random triangular pencil with the rows of P scaled by 10^U(-8,8) (a 2x2
+    block's rows share one factor), left eigenvectors: consecutive rows can differ by 1e16,
+    so some columns grow past the range of the format within a few rows of one block and
+    only the per-row cap keeps them finite.  Every column must be finite with a DGET52-style
+    residual below 100; where the upstream library is built (oracle/_ref), the columns must
+    also match it (1e-11 after normalisation)."""
+    n, seed = 4096, 8213
+    if dt == np.float64:
+        S, P, al, ai, be = pencils.gen_quasi_triangular(n, seed)
+    else:
+        (S, P, al, be), ai = pencils.gen_upper_triangular_complex(n, seed), None
+    g = 10.0 ** np.random.default_rng(seed + 1).uniform(-8, 8, n)
+    k = 0
+    while ai is not None and k < n:
+        if ai[k] != 0 and k + 1 < n:
+            g[k + 1] = g[k]
+            k += 2
+        else:
+            k += 1
+    P = np.asfortranarray(g[:, None] * P)
+    be = np.diag(P).copy()
+    I = np.eye(n, dtype=dt, order="F")
+    d = dict(side="L", howmny="A", S=S, P=P, alpha=al, beta=be, alphai=ai, VL_in=I, VR_in=I.copy(order="F"),
+             name="graded")
+    VL, VR, m, info = run_gpu(d)
+    assert (m, info) == (n, 0)
+    assert np.isfinite(VL).all()
+    V = as_complex(VL, d)
+    a_c, b_c = oracle.column_eigenvalues(al, be, alphai=ai)
+    r = oracle.residual_ratio(S, P, V, a_c, b_c, left=True)
+    assert r.max() < 100, r.max()
+    if oracle.ref_available():
+        ref = oracle.tgevc3("L", "A", S, P, al, be, alphai=ai, impl="ref")[0]
+        err, _ = oracle.max_rel_diff(V, as_complex(ref, d))
+        assert err < 1e-11, err
+
+
 def test_selection_and_one_sided(cuda_ok):
     p = _pencil("gges", 150, 41, np.float64)
     rng = np.random.default_rng(0)

@@ -41,10 +41,12 @@ template <class R> struct limits;
 template <> struct limits<double> {
     static constexpr double safemin = DBL_MIN;
     static constexpr double eps = DBL_EPSILON;
+    static constexpr double big = DBL_MAX;
 };
 template <> struct limits<float> {
     static constexpr float safemin = FLT_MIN;
     static constexpr float eps = FLT_EPSILON;
+    static constexpr float big = FLT_MAX;
 };
 
 // Row-block size of the right-looking substitution (rows per diagonal block).

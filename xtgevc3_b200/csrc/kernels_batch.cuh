@@ -398,15 +398,17 @@ __device__ void solve_item(const TileCols<T, NT> &tc, int j, int r0, int r1, con
         }
         Factors<T> F;
         factor_rows(F, sec, nrows, lane, smin, W);
+        auto rescale = [&](T (&rr)[2], T sc) {  // the whole column, by sc
+            rr[0] *= sc; rr[1] *= sc; seed *= sc;
+            if (!diag) { scale_col(colr, XLD, 0, r0, sc, lane); scale_col(colr, XLD, r1, top + 1, sc, lane); }
+        };
         auto mid = [&](T (&rr)[2], int jtop) {
             const T mx = warp_max(lane <= jtop ? fabs(rr[0]) : T(0));
-            if (mx > thr_rhs) {
-                const T sc = thr_rhs / mx;
-                rr[0] *= sc; rr[1] *= sc; seed *= sc;
-                if (!diag) { scale_col(colr, XLD, 0, r0, sc, lane); scale_col(colr, XLD, r1, top + 1, sc, lane); }
-            }
+            if (mx > thr_rhs) rescale(rr, thr_rhs / mx);
         };
-        back_substitute_loop(r, F, sec, nrows, lane, W, 0, mid);
+        // block and mid-block checks, no per-row cap: with it this kernel needs more than
+        // the 128 registers that leave room for a second CTA per SM
+        back_substitute_loop(r, F, sec, nrows, lane, W, 0, make_guard<false>(limits<T>::big / T(4096), thr_rhs, mid, rescale));
         T x[2];
 #pragma unroll
         for (int s = 0; s < 2; s++) {
@@ -471,18 +473,18 @@ __device__ void solve_item(const TileCols<T, NT> &tc, int j, int r0, int r1, con
         }
         Factors<C> F;
         factor_rows(F, sec, nrows, lane, smin, W);
-        auto mid = [&](C (&rr)[2], int jtop) {
-            const T mx = warp_max(lane <= jtop ? fmax(fabs(rr[0].x), fabs(rr[0].y)) : T(0));
-            if (mx > thr_rhs) {
-                const T sc = thr_rhs / mx;
-                rr[0] = sc * rr[0]; rr[1] = sc * rr[1]; seed0 = sc * seed0; seed1 = sc * seed1;
-                if (!diag) {
-                    scale_col(colr, XLD, 0, r0, sc, lane); scale_col(colr, XLD, r1, top + 1, sc, lane);
-                    scale_col(coli, XLD, 0, r0, sc, lane); scale_col(coli, XLD, r1, top + 1, sc, lane);
-                }
+        auto rescale = [&](C (&rr)[2], T sc) {  // the whole column pair, by sc
+            rr[0] = sc * rr[0]; rr[1] = sc * rr[1]; seed0 = sc * seed0; seed1 = sc * seed1;
+            if (!diag) {
+                scale_col(colr, XLD, 0, r0, sc, lane); scale_col(colr, XLD, r1, top + 1, sc, lane);
+                scale_col(coli, XLD, 0, r0, sc, lane); scale_col(coli, XLD, r1, top + 1, sc, lane);
             }
         };
-        back_substitute_loop(r, F, sec, nrows, lane, W, 0, mid);
+        auto mid = [&](C (&rr)[2], int jtop) {
+            const T mx = warp_max(lane <= jtop ? fmax(fabs(rr[0].x), fabs(rr[0].y)) : T(0));
+            if (mx > thr_rhs) rescale(rr, thr_rhs / mx);
+        };
+        back_substitute_loop(r, F, sec, nrows, lane, W, 0, make_guard<false>(limits<T>::big / T(4096), thr_rhs, mid, rescale));
         C x[2];
 #pragma unroll
         for (int s = 0; s < 2; s++) {

@@ -231,27 +231,89 @@ __device__ __forceinline__ void factor_rows(Factors<E> &F, uint64_t sec, int nro
     }
 }
 
-// Growth check inside a block.  Upstream checks the right-hand side before every local
+// Growth checks inside a block.  Upstream checks the right-hand side before every local
 // solve of at most 32 rows (`max |rhs| > bignum/10`, src/ztgevc3.cpp:183-199, bsize = 32 at
 // :454; src/dtgevc3.cpp:688-698); a block here has up to 64 rows, so the substitution calls
-// mid(r, jtop) once every row at or above kMidRow is solved, where rows [0, jtop] hold the
+// g.mid(r, jtop) once every row at or above kMidRow is solved, where rows [0, jtop] hold the
 // partially updated right-hand side of the block's upper rows.  Without it, a column that
 // enters the block near bignum/10 can overflow within the block where upstream's solves stay
-// finite.  NoMid is the unguarded form.
+// finite.
+//
+// With the per-row cap (Guard<true, ...>), a solved component above g.cap (the largest
+// finite value / 4096: room for the updates of a block's rows, |w_ij| <= 2) makes the
+// substitution rescale the column, g.rescale(r, s), by the factor that brings that
+// component to g.target (bignum/10, the level the block checks rescale to), computed from the
+// row's right-hand side and pivot without forming the overflowing product; a 2x2 block does
+// this for its second and then its first component.
+// Upstream rescales whole 32-column panels, so a column whose own growth passes the range of
+// the format inside 32 rows (rows of a graded pencil differing by 1e16) can still come back
+// finite there, scaled down by the guards of other columns of its panel; the cap gives the
+// per-column guards the same reach for one compare per row.  NoGuard is the unguarded form.
 constexpr int kMidRow = 32;
-struct NoMid {
+struct NoGuard {
+    static constexpr bool on = false;
     template <class E>
-    __device__ __forceinline__ void operator()(E (&)[2], int) const {}
+    __device__ __forceinline__ void mid(E (&)[2], int) const {}
+    template <class E, class T>
+    __device__ __forceinline__ void rescale(E (&)[2], T) const {}
+    static constexpr double cap = 0, target = 0;
 };
+// ON: mid-block check and per-row cap; off: the mid-block check only
+template <bool ON, class R, class MF, class RF>
+struct Guard {
+    static constexpr bool on = ON;
+    MF mid_f;
+    RF rescale_f;
+    R cap, target;
+    template <class E>
+    __device__ __forceinline__ void mid(E (&r)[2], int jtop) const { mid_f(r, jtop); }
+    template <class E>
+    __device__ __forceinline__ void rescale(E (&r)[2], R s) const { rescale_f(r, s); }
+};
+template <bool ON, class R, class MF, class RF>
+__device__ __forceinline__ Guard<ON, R, MF, RF> make_guard(R cap, R target, MF mid, RF rescale)
+{
+    return Guard<ON, R, MF, RF>{mid, rescale, cap, target};
+}
+
+// Per-row cap: x = r_j / w_jj (x0 = r_j, iv = 1 / w_jj, uniform across the warp) passed
+// g.cap: rescale the column so that |x| becomes g.target, and return the recomputed x.
+template <class E, class G>
+__device__ __forceinline__ E cap_row(E (&r)[2], const G &g, E x0, E iv)
+{
+    const auto s = (g.target / mag(iv)) / mag(x0);
+    g.rescale(r, s);
+    return (s * x0) * iv;
+}
+
+// The same for a 2x2 block: xq = (r2 - m r1) iu, xp = (r1 - b xq) ia (uniform inputs).
+template <class E, class G>
+__device__ __forceinline__ void cap_pair(E (&r)[2], const G &g, E r1, E r2, E m, E iu, E b, E ia, E &xp, E &xq)
+{
+    auto s = (g.target / mag(iu)) / (mag(r2) + mag(m) * mag(r1));
+    if (s < decltype(s)(1)) {
+        g.rescale(r, s);
+        r1 = s * r1;
+        r2 = s * r2;
+    }
+    xq = (r2 - m * r1) * iu;
+    s = (g.target / mag(ia)) / (mag(r1) + mag(b) * mag(xq));
+    if (s < decltype(s)(1)) {
+        g.rescale(r, s);
+        r1 = s * r1;
+        xq = s * xq;
+    }
+    xp = (r1 - b * xq) * ia;
+}
 
 // Block back substitution of one eigenvector held in r (rows [jlo, nrows)); on return r
 // holds the solution in those rows (rows below jlo receive updates that mean nothing).
 // W(i, j) gives the shifted operator entry.  jlo must not split a 2x2 block.  The row loop
 // is unrolled over the block's 64 rows, so every row index, register slot and lane test is
 // a constant; rows at or past nrows (uniform across the warp) are skipped.
-template <class E, class WF, class MF = NoMid>
+template <class E, class WF, class G = NoGuard>
 __device__ __forceinline__ void back_substitute(E (&r)[2], const Factors<E> &F, uint64_t sec, int nrows, int lane,
-                                                WF W, int jlo = 0, MF mid = MF())
+                                                WF W, int jlo = 0, G g = G())
 {
     bool skip = false;  // the row was consumed by the 2x2 block above it
     bool checked = nrows <= kMidRow;
@@ -266,7 +328,7 @@ __device__ __forceinline__ void back_substitute(E (&r)[2], const Factors<E> &F, 
         // block took rows (kMidRow - 1, kMidRow): two call sites, not one per row
         if ((j == kMidRow - 1 || j == kMidRow - 2) && !checked) {
             checked = true;
-            mid(r, j);
+            g.mid(r, j);
         }
         if (j >= 1 && ((sec >> j) & 1ull)) {
             const int p = j - 1, q = j;
@@ -279,6 +341,12 @@ __device__ __forceinline__ void back_substitute(E (&r)[2], const Factors<E> &F, 
             E xp = (r1 - b * xq) * ia;
             xq = shfl(xq, q & 31);
             xp = shfl(xp, q & 31);
+            if constexpr (G::on) {
+                if (!(mag(xq) <= g.cap && mag(xp) <= g.cap)) {
+                    const int o = q & 31;
+                    cap_pair(r, g, shfl(r1, o), shfl(r2, o), shfl(m, o), shfl(iu, o), shfl(b, o), shfl(ia, o), xp, xq);
+                }
+            }
             if (lane == (p & 31)) r[p >> 5] = xp;
             if (lane == (q & 31)) r[q >> 5] = xq;
             if (p > 0) {
@@ -287,7 +355,10 @@ __device__ __forceinline__ void back_substitute(E (&r)[2], const Factors<E> &F, 
             }
             skip = true;
         } else {
-            const E x = shfl(r[j >> 5] * F.inv1[j >> 5], j & 31);
+            E x = shfl(r[j >> 5] * F.inv1[j >> 5], j & 31);
+            if constexpr (G::on) {
+                if (!(mag(x) <= g.cap)) x = cap_row(r, g, shfl(r[j >> 5], j & 31), shfl(F.inv1[j >> 5], j & 31));
+            }
             if (lane == (j & 31)) r[j >> 5] = x;
             if (j > 0) {
                 if (j >= 32 || lane < j) r[0] = r[0] - W(lane, j) * x;
@@ -299,9 +370,9 @@ __device__ __forceinline__ void back_substitute(E (&r)[2], const Factors<E> &F, 
 
 // The same substitution as a runtime row loop (fewer registers: one code path per row
 // instead of 64): used where register pressure matters more than instructions per row.
-template <class E, class WF, class MF = NoMid>
+template <class E, class WF, class G = NoGuard>
 __device__ __forceinline__ void back_substitute_loop(E (&r)[2], const Factors<E> &F, uint64_t sec, int nrows,
-                                                     int lane, WF W, int jlo = 0, MF mid = MF())
+                                                     int lane, WF W, int jlo = 0, G g = G())
 {
     // one row, or the 2x2 block ending at row j; returns the next unsolved row
     auto step = [&](int j) -> int {
@@ -318,23 +389,33 @@ __device__ __forceinline__ void back_substitute_loop(E (&r)[2], const Factors<E>
             E xp = (r1 - b * xq) * ia;
             xq = shfl(xq, q & 31);
             xp = shfl(xp, q & 31);
+            if constexpr (G::on) {
+                if (!(mag(xq) <= g.cap && mag(xp) <= g.cap)) {
+                    const int o = q & 31;
+                    cap_pair(r, g, shfl(r1, o), shfl(r2, o), shfl(m, o), shfl(iu, o), shfl(b, o), shfl(ia, o), xp, xq);
+                }
+            }
             set_row(r, p, lane, xp);
             set_row(r, q, lane, xq);
             if (lane < p) r[0] = r[0] - (W(lane, p) * xp + W(lane, q) * xq);
             if (p > 32 && lane + 32 < p) r[1] = r[1] - (W(lane + 32, p) * xp + W(lane + 32, q) * xq);
             return j - 2;
         }
-        const E x = shfl((j >> 5) ? r[1] * F.inv1[1] : r[0] * F.inv1[0], j & 31);
+        E x = shfl((j >> 5) ? r[1] * F.inv1[1] : r[0] * F.inv1[0], j & 31);
+        if constexpr (G::on) {
+            if (!(mag(x) <= g.cap))
+                x = cap_row(r, g, shfl(row_of(r, j), j & 31), shfl((j >> 5) ? F.inv1[1] : F.inv1[0], j & 31));
+        }
         set_row(r, j, lane, x);
         if (lane < j) r[0] = r[0] - W(lane, j) * x;
         if (j > 32 && lane + 32 < j) r[1] = r[1] - W(lane + 32, j) * x;
         return j - 1;
     };
-    // rows at and above kMidRow, the growth check, then the rest (no per-row test)
+    // rows at and above kMidRow, the mid-block check, then the rest (no per-row test)
     int j = nrows - 1;
     const int jsplit = jlo > kMidRow ? jlo : kMidRow;
     while (j >= jsplit) j = step(j);
-    if (nrows > kMidRow && j >= jlo) mid(r, j);
+    if (nrows > kMidRow && j >= jlo) g.mid(r, j);
     while (j >= jlo) j = step(j);
 }
 
@@ -415,18 +496,18 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
             }
             Factors<R> F;
             factor_rows(F, sec, nrows, lane, smin, W);
-            auto mid = [&](R (&rr)[2], int jtop) {
-                const R mx = warp_max(lane <= jtop ? fabs(rr[0]) : R(0));
-                if (mx > a.thr_rhs) {
-                    const R sc = a.thr_rhs / mx;
-                    rr[0] *= sc; rr[1] *= sc; seed *= sc;
-                    if (!diag) {
-                        scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane);
-                        scale_lower_y(a, a.Y + (size_t)c * a.ldy, sc, lane);
-                    }
+            auto rescale = [&](R (&rr)[2], R sc) {  // the whole column, by sc
+                rr[0] *= sc; rr[1] *= sc; seed *= sc;
+                if (!diag) {
+                    scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane);
+                    scale_lower_y(a, a.Y + (size_t)c * a.ldy, sc, lane);
                 }
             };
-            back_substitute_loop(r, F, sec, nrows, lane, W, 0, mid);
+            auto mid = [&](R (&rr)[2], int jtop) {
+                const R mx = warp_max(lane <= jtop ? fabs(rr[0]) : R(0));
+                if (mx > a.thr_rhs) rescale(rr, a.thr_rhs / mx);
+            };
+            back_substitute_loop(r, F, sec, nrows, lane, W, 0, make_guard<true>(limits<R>::big / R(4096), a.thr_rhs, mid, rescale));
             // assemble the block column (solution rows, seed, zeros below the seed)
             R x[2];
 #pragma unroll
@@ -498,20 +579,20 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
             }
             Factors<C> F;
             factor_rows(F, sec, nrows, lane, smin, W);
-            auto mid = [&](C (&rr)[2], int jtop) {
-                const R mx = warp_max(lane <= jtop ? fmax(fabs(rr[0].x), fabs(rr[0].y)) : R(0));
-                if (mx > a.thr_rhs) {
-                    const R sc = a.thr_rhs / mx;
-                    rr[0] = sc * rr[0]; rr[1] = sc * rr[1]; seed0 = sc * seed0; seed1 = sc * seed1;
-                    if (!diag) {
-                        scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane);
-                        scale_above(a, coli, c + 1, sc, lane); scale_rows(coli, a.r1, top + 1, sc, lane);
-                        scale_lower_y(a, a.Y + (size_t)c * a.ldy, sc, lane);
-                        scale_lower_y(a, a.Y + (size_t)(c + 1) * a.ldy, sc, lane);
-                    }
+            auto rescale = [&](C (&rr)[2], R sc) {  // the whole column pair, by sc
+                rr[0] = sc * rr[0]; rr[1] = sc * rr[1]; seed0 = sc * seed0; seed1 = sc * seed1;
+                if (!diag) {
+                    scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane);
+                    scale_above(a, coli, c + 1, sc, lane); scale_rows(coli, a.r1, top + 1, sc, lane);
+                    scale_lower_y(a, a.Y + (size_t)c * a.ldy, sc, lane);
+                    scale_lower_y(a, a.Y + (size_t)(c + 1) * a.ldy, sc, lane);
                 }
             };
-            back_substitute_loop(r, F, sec, nrows, lane, W, 0, mid);
+            auto mid = [&](C (&rr)[2], int jtop) {
+                const R mx = warp_max(lane <= jtop ? fmax(fabs(rr[0].x), fabs(rr[0].y)) : R(0));
+                if (mx > a.thr_rhs) rescale(rr, a.thr_rhs / mx);
+            };
+            back_substitute_loop(r, F, sec, nrows, lane, W, 0, make_guard<true>(limits<R>::big / R(4096), a.thr_rhs, mid, rescale));
             C x[2];
 #pragma unroll
             for (int s = 0; s < 2; s++) {
@@ -606,18 +687,30 @@ __global__ void __launch_bounds__(256) diag_solve_cplx(DiagArgs<R> a)
         }
         Factors<C> F;
         factor_rows(F, 0ull, nrows, lane, smin, W);
-        auto mid = [&](C (&rr)[2], int jtop) {
-            const R mx = warp_max(lane <= jtop ? l1abs(rr[0]) : R(0));
-            if (mx > a.thr_rhs) {
-                const R sc = a.thr_rhs / mx;
-                rr[0] = sc * rr[0]; rr[1] = sc * rr[1]; seed = sc * seed;
-                if (!diag) {
-                    scale_above(a, col, c, sc, lane); scale_rows(col, a.r1, top + 1, sc, lane);
-                    scale_lower_y(a, Y + (size_t)c * a.ldy, sc, lane);
-                }
+        // The unrolled substitution runs without the per-row cap (its compare on every row
+        // costs a quarter of this kernel); a block in which a component passed the cap, or
+        // overflowed, is solved again from its right-hand side with the cap, in loop form.
+        // Factors applied to the stored rows during the first pass (acc) carry over.
+        const C r_in[2] = {r[0], r[1]};
+        R acc = R(1);
+        auto rescale = [&](C (&rr)[2], R sc) {  // the whole column, by sc
+            rr[0] = sc * rr[0]; rr[1] = sc * rr[1]; seed = sc * seed; acc *= sc;
+            if (!diag) {
+                scale_above(a, col, c, sc, lane); scale_rows(col, a.r1, top + 1, sc, lane);
+                scale_lower_y(a, Y + (size_t)c * a.ldy, sc, lane);
             }
         };
-        back_substitute(r, F, 0ull, nrows, lane, W, 0, mid);
+        auto mid = [&](C (&rr)[2], int jtop) {  // a non-finite maximum (first pass) is left to the second
+            const R mx = warp_max(lane <= jtop ? l1abs(rr[0]) : R(0));
+            if (mx > a.thr_rhs && mx <= limits<R>::big) rescale(rr, a.thr_rhs / mx);
+        };
+        const R cap = limits<R>::big / R(4096);
+        back_substitute(r, F, 0ull, nrows, lane, W, 0, make_guard<false>(cap, a.thr_rhs, mid, rescale));
+        if (__any_sync(0xffffffffu, !(l1abs(r[0]) <= cap) || !(l1abs(r[1]) <= cap))) {
+            r[0] = acc * r_in[0];
+            r[1] = acc * r_in[1];
+            back_substitute_loop(r, F, 0ull, nrows, lane, W, 0, make_guard<true>(cap, a.thr_rhs, mid, rescale));
+        }
         C x[2];
 #pragma unroll
         for (int s = 0; s < 2; s++) {
