@@ -135,8 +135,8 @@ def test_growth_guards_random_triangular(cuda_ok, dt):
     """n = 2048 random triangular pencils with the structure of the upstream test
     generators (U(-1,1) parts, |P_kk| pushed away from 0; real: 2x2 blocks as well).  Close
     eigenvalues make many eigenvectors grow by more than 1e300 across the matrix, so the
-    overflow guards rescale hundreds of columns, in lower and upper blocks of block pairs
-    and inside 64-row blocks.  Both sides must be finite, match the oracle column by column
+    overflow guards rescale hundreds of columns, in every block of a group of blocks that
+    share one trailing update, and inside 64-row blocks.  Both sides must be finite, match the oracle column by column
     (1e-11) and have a DGET52-style residual below 100."""
     n, seed = 2048, 8213
     if dt == np.float64:
@@ -331,12 +331,13 @@ def _overflow_pencil(n, seed, jump, left):
 
 @pytest.mark.parametrize("side", ["R", "L"])
 def test_lookahead_matches_serial_path_with_guards(cuda_ok, side):
-    """The look-ahead schedule (XTGEVC3_LOOKAHEAD: trailing updates on a second stream,
-    guard scaling of the rows they write deferred to a later kernel) must give
-    bit-identical numbers to the default serial schedule, also when the overflow guards
-    rescale many columns, and must match the oracle column by column after normalisation
-    (the oracle rescales whole 32-column panels where this implementation rescales single
-    columns)."""
+    """The look-ahead schedule (XTGEVC3_LOOKAHEAD: trailing updates of block pairs on a
+    second stream, guard scaling of the rows they write deferred to a later kernel) must
+    agree with the default serial schedule, which sums the trailing updates of four blocks
+    in one GEMM, to rounding also when the overflow guards rescale many columns: the same
+    guards fire, so the raw columns agree within 1e-9 of their largest entry.  It must also
+    match the oracle column by column after normalisation (the oracle rescales whole
+    32-column panels where this implementation rescales single columns)."""
     n = 1536
     S, P, ar, ai, be = _overflow_pencil(n, 91, 1e16, side == "L")
     I = np.eye(n, order="F")
@@ -352,6 +353,10 @@ def test_lookahead_matches_serial_path_with_guards(cuda_ok, side):
     # the guards fired: columns come back with their seed entry x_k scaled below 1
     assert (np.abs(np.diag(V0[:, :n])) < 1).sum() >= 8
     VL1, VR1, _, _ = run_gpu(d)  # the default, serial schedule
-    np.testing.assert_array_equal(V0, VL1 if side == "L" else VR1)
+    V1 = VL1 if side == "L" else VR1
+    den = np.abs(V1).max(0)
+    den[den == 0] = 1
+    raw = (np.abs(V0 - V1).max(0) / den).max()
+    assert raw < 1e-9, raw
     ref = oracle.tgevc3(side, "A", S, P, ar, be, alphai=ai)
     compare(d, VL0, VR0, m, ref[0], ref[1], TOL_ILL[np.float64], check_resid=False)

@@ -51,6 +51,11 @@ template <> struct limits<float> {
 
 // Row-block size of the right-looking substitution (rows per diagonal block).
 constexpr int kBlock = 64;
+// Row blocks per group of the substitution (one trailing GEMM per group, K = 2 x its
+// rows): FP64 DMMA updates, and the split-precision updates, whose per-tile fixed costs a
+// longer K amortises.
+constexpr int kGroupBlocks = 2;
+constexpr int kGroupBlocksSplit = 8;
 // K-granule of the update GEMM; each half of the stacked update operand is padded to it.
 constexpr int kKPad = 16;
 

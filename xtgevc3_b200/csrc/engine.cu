@@ -476,7 +476,6 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             Pp = Pt;
             lsp = lpp = ld_n;
         }
-        const int ldx = ld_n, ldy = 4 * kBlock;  // two halves of two padded row blocks
         // work items of the diagonal solves: every column that starts an eigenvector
         const std::vector<int> &items = sc.starts;
         const int nitems = (int)items.size();
@@ -484,6 +483,12 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         // stream while the next pair is solved (see the loop below); off while tracing
         // (clean per-kernel times) and in arena mode (fixed scratch)
         const bool ahead = opt.lookahead && !tr.on && !opt.arena && blocks.size() >= 3;
+        // Without look-ahead, row blocks are taken in groups of `group` (one trailing GEMM
+        // with K = 2 x the group's rows); arena mode keeps groups of two, so that its fixed
+        // scratch holds the update operand.  Look-ahead takes pairs with padded blocks.
+        const int group = opt.arena ? 2 : (nsplit ? kGroupBlocksSplit : kGroupBlocks);
+        const int ldx = ld_n;
+        const int ldy = ahead ? 4 * kBlock : 2 * round_up(group * kBlock, kKPad);  // both halves
         E *X = scr.get<E>((size_t)ldx * m);
         E *Ybuf[2];
         Ybuf[0] = scr.get<E>((size_t)ldy * m);
@@ -512,11 +517,15 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         XTG_CK(cudaGetLastError());
 
         // ---- blocked substitution ----------------------------------------------------------
-        // Row blocks are taken in pairs (a lower block L and the upper block U above it):
-        //   solve L; update the rows of U with L's solution (small GEMM); solve U;
-        //   update every row above U with both blocks at once (K = 4 strips).
-        // so the large trailing GEMMs see K = 2 * (|U| + |L|) ~ 256.  The update operand Y
-        // of a pair holds [-ac x_U; -ac x_L | b x_U; b x_L], each block padded to kKPad.
+        // Row blocks are taken in groups of `group` adjacent blocks, rows [q0, q1), bottom to
+        // top: each block is solved, then the rows of the group's blocks above it are updated
+        // with its solution (small GEMM); after the top block one GEMM updates every row above
+        // the group with the whole group, K = 2 (q1 - q0) (256 rows: K = 512).  The update
+        // operand Y of a group holds the -ac x rows of its blocks in row order, rows [0, q1 -
+        // q0), zero padded to Kq = round_up(q1 - q0, kKPad), then the b x rows at Kq; the
+        // GEMMs read it as one S strip and one P strip.  A guard that fires in a block rescales
+        // the rows of Y below it (zl window of the solve), which the group's GEMMs consume
+        // together with the block's own.  (Look-ahead: pairs, each block padded to kKPad.)
         const size_t diag_smem = 2 * kBlock * kSmLd * sizeof(E);
         auto first_col = [&](int r) {
             return int(std::lower_bound(L.colk.begin(), L.colk.end(), r) - L.colk.begin());
@@ -557,11 +566,13 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             tr.run(kTUpdate, uf, ub, us, [&] { gemm(g, us); });
         };
         // safe_lo >= 0: deferred guard scaling of the rows above safe_lo (look-ahead)
-        auto diag_solve = [&](int r0, int r1, int ys_off, int yhalf, int zl_off, int zl_len, int safe_lo) {
+        // ypad < 0: the block's rows padded to kKPad
+        auto diag_solve = [&](int r0, int r1, int ys_off, int yhalf, int zl_off, int zl_len, int safe_lo,
+                              int ypad = -1) {
             const int jnb = r1 - r0;
             const int c0 = first_col(r0);
             if (c0 >= m) return;
-            const int bpad = round_up(jnb, kKPad);
+            const int bpad = ypad >= 0 ? ypad : round_up(jnb, kKPad);
             DiagArgs<R> da;
             da.S = reinterpret_cast<const R *>(Sp);
             da.P = reinterpret_cast<const R *>(Pp);
@@ -609,6 +620,28 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             });
         };
         const int nbk = (int)blocks.size();
+        for (int gi = 0; !ahead && gi < nbk; gi += group) {
+            const int ge = std::min(nbk, gi + group);  // blocks [gi, ge); blocks[gi] is the lowest
+            const int q0 = blocks[ge - 1].first, q1 = blocks[gi].second;
+            const int acols = q1 - q0, kq = round_up(acols, kKPad);
+            for (int bi = gi; bi < ge; bi++) {
+                const int r0 = blocks[bi].first, r1 = blocks[bi].second, jnb = r1 - r0, ys = r0 - q0;
+                // the lowest block also writes the zero padding of the group's operand rows
+                diag_solve(r0, r1, ys, kq, ys + jnb, kq - (ys + jnb), -1, jnb + (bi == gi ? kq - acols : 0));
+                const int c0 = first_col(r0);
+                if (bi + 1 < ge && c0 < m) {  // rows [q0, r0) (window from an even row)
+                    const int w0 = q0 & ~1, mlo = q0 & 1;
+                    GemmSeg<E> sg[2] = {strip(Sp, lsp, w0, r0, jnb, ys), strip(Pp, lpp, w0, r0, jnb, kq + ys)};
+                    update(w0, mlo, mlo + (r0 - q0), c0, 2, sg, 2.0 * jnb, st);
+                }
+            }
+            const int c0 = first_col(q0);
+            if (q0 > 0 && c0 < m) {
+                GemmSeg<E> sg[2] = {strip(Sp, lsp, 0, q0, acols, 0), strip(Pp, lpp, 0, q0, acols, kq)};
+                update(0, 0, q0, c0, 2, sg, 2.0 * acols, st);
+            }
+            XTG_CK(cudaGetLastError());
+        }
         // Look-ahead (ahead == true).  Pair p owns rows [u0_p, l1_p); the next pair's rows are
         // [a0, u0_p).  On the main stream: solve L_p, small update of U_p, solve U_p; wait for
         // the trailing update of pair p-1 (it writes rows [0, u0_p)); apply deferred guard
@@ -656,7 +689,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         }
         bool tr_pending = false;  // a trailing update is queued on st2 and not yet waited for
         int pidx = 0;
-        for (int bi = 0; bi < nbk;) {
+        for (int bi = 0; ahead && bi < nbk;) {
             const int l0 = blocks[bi].first, l1 = blocks[bi].second, jl = l1 - l0, bl = round_up(jl, kKPad);
             Y = Ybuf[pidx & 1];
             if (bi + 1 == nbk) {  // unpaired top block
@@ -676,7 +709,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
                 continue;
             }
             const int u0 = blocks[bi + 1].first, ju = l0 - u0, bu = round_up(ju, kKPad), bh = bu + bl;
-            const int safe = ahead ? u0 : -1;
+            const int safe = u0;  // rows [0, u0) belong to the concurrent trailing update
             diag_solve(l0, l1, bu, bh, 0, 0, safe);
             const int c0l = first_col(l0);
             if (c0l < m) {  // rows of U (window from an even row) += L's contribution
@@ -686,34 +719,26 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             }
             diag_solve(u0, l0, 0, bh, bu, bl, safe);
             const int c0u = first_col(u0);
-            if (!ahead) {
-                if (u0 > 0 && c0u < m) {
+            if (tr_pending) {
+                XTG_CK(cudaStreamWaitEvent(st, ev_tr, 0));
+                tr_pending = false;
+            }
+            if (u0 > 0) apply_pending_kernel<E, R><<<(m * 32 + 255) / 256, 256, 0, st>>>(X, ldx, pending, m, u0);
+            if (u0 > 0 && c0u < m) {
+                // the next pair's rows [a0, u0): its U block's start, or the top block's
+                const int a0 = bi + 3 < nbk ? blocks[bi + 3].first : blocks[bi + 2].first;
+                const int w0 = a0 & ~1, mlo = a0 & 1;
+                GemmSeg<E> sa[4] = {strip(Sp, lsp, w0, u0, ju, 0), strip(Sp, lsp, w0, l0, jl, bu),
+                                    strip(Pp, lpp, w0, u0, ju, bh), strip(Pp, lpp, w0, l0, jl, bh + bu)};
+                update(w0, mlo, mlo + (u0 - a0), c0u, 4, sa, 2.0 * (ju + jl), st);
+                if (a0 > 0) {
+                    XTG_CK(cudaEventRecord(ev_main, st));
+                    XTG_CK(cudaStreamWaitEvent(st2, ev_main, 0));
                     GemmSeg<E> sg[4] = {strip(Sp, lsp, 0, u0, ju, 0), strip(Sp, lsp, 0, l0, jl, bu),
                                         strip(Pp, lpp, 0, u0, ju, bh), strip(Pp, lpp, 0, l0, jl, bh + bu)};
-                    update(0, 0, u0, c0u, 4, sg, 2.0 * (ju + jl), st);
-                }
-            } else {
-                if (tr_pending) {
-                    XTG_CK(cudaStreamWaitEvent(st, ev_tr, 0));
-                    tr_pending = false;
-                }
-                if (u0 > 0) apply_pending_kernel<E, R><<<(m * 32 + 255) / 256, 256, 0, st>>>(X, ldx, pending, m, u0);
-                if (u0 > 0 && c0u < m) {
-                    // the next pair's rows [a0, u0): its U block's start, or the top block's
-                    const int a0 = bi + 3 < nbk ? blocks[bi + 3].first : blocks[bi + 2].first;
-                    const int w0 = a0 & ~1, mlo = a0 & 1;
-                    GemmSeg<E> sa[4] = {strip(Sp, lsp, w0, u0, ju, 0), strip(Sp, lsp, w0, l0, jl, bu),
-                                        strip(Pp, lpp, w0, u0, ju, bh), strip(Pp, lpp, w0, l0, jl, bh + bu)};
-                    update(w0, mlo, mlo + (u0 - a0), c0u, 4, sa, 2.0 * (ju + jl), st);
-                    if (a0 > 0) {
-                        XTG_CK(cudaEventRecord(ev_main, st));
-                        XTG_CK(cudaStreamWaitEvent(st2, ev_main, 0));
-                        GemmSeg<E> sg[4] = {strip(Sp, lsp, 0, u0, ju, 0), strip(Sp, lsp, 0, l0, jl, bu),
-                                            strip(Pp, lpp, 0, u0, ju, bh), strip(Pp, lpp, 0, l0, jl, bh + bu)};
-                        update(0, 0, a0, c0u, 4, sg, 2.0 * (ju + jl), st2);
-                        XTG_CK(cudaEventRecord(ev_tr, st2));
-                        tr_pending = true;
-                    }
+                    update(0, 0, a0, c0u, 4, sg, 2.0 * (ju + jl), st2);
+                    XTG_CK(cudaEventRecord(ev_tr, st2));
+                    tr_pending = true;
                 }
             }
             XTG_CK(cudaGetLastError());

@@ -27,8 +27,9 @@
 //   * before the update: if max(|ac x|, |b x|) > bignum/jnb, scale the column
 //     (src/dtgevc3.cpp:1404-1426, with the panel width replaced by the block height).
 // Scaling a column means scaling every stored row of it: the accumulated rows above the
-// block, the rows solved in earlier blocks and the current block, and (upper block of a
-// pair) the lower block's rows of the pair's update operand, not yet consumed.  A third
+// block, the rows solved in earlier blocks and the current block, and the update-operand
+// rows of the lower blocks of the same group (or pair), which the group's trailing GEMM has
+// not consumed yet.  A third
 // check, inside the block once its rows at and above kMidRow are solved, keeps at most 32
 // rows between checks, as upstream's 32-row local solves do.
 //
@@ -114,7 +115,7 @@ struct DiagArgs {
     const R *coef;           // 4 per column: ac, b_re, b_im, smin  (complex: 6: ac, b, smin, 0)
     R *X;                    // n x m computed eigenvectors (complex: interleaved)
     int ldx;
-    R *Y;                    // 2*bpad x m update operand
+    R *Y;                    // 2 yhalf x m update operand (-ac x rows, then b x rows)
     int ldy;
     R thr_rhs, thr_upd;
     int left_seed;           // 2x2 seed of the left problem (see the pair branch)
@@ -146,10 +147,10 @@ __device__ __forceinline__ void scale_above(const DiagArgs<R> &a, E *col, int c,
     if (lane == 0) a.pending[c] *= s;
 }
 
-// The upper block of a pair: the lower block's rows of the update operand (rows [zl_off,
-// zl_off + zl_len) of both halves, written by the lower block's solve) are consumed by the
-// pair's trailing update together with this block's rows.  A guard that rescales a column
-// here rescales those rows too, so that the two blocks' operands carry the same scale
+// A block above others in a group (or pair): the lower blocks' rows of the update operand
+// (rows [zl_off, zl_off + zl_len) of both halves, written by their solves) are consumed by
+// the group's trailing update together with this block's rows.  A guard that rescales a
+// column here rescales those rows too, so that all the blocks' operands carry the same scale
 // (upstream applies each block's update before the next solve and has no such operand).
 template <class E, class R>
 __device__ __forceinline__ void scale_lower_y(const DiagArgs<R> &a, E *ycol, R s, int lane)
@@ -174,6 +175,10 @@ __device__ __forceinline__ void write_y(const DiagArgs<R> &a, E *ycol, int jnb, 
             ycol[a.ys_off + i] = in ? ys[s] : E(0);
             ycol[a.ys_off + a.yhalf + i] = in ? yp[s] : E(0);
         }
+    }
+    for (int i = 64 + lane; i < a.ypad; i += 32) {  // padding past a full block (jnb <= 64)
+        ycol[a.ys_off + i] = E(0);
+        ycol[a.ys_off + a.yhalf + i] = E(0);
     }
     if (diag)
         for (int i = lane; i < a.zl_len; i += 32) {
