@@ -20,7 +20,7 @@
 // accumulators are added into FP64 registers; FP64 summation across chunks.
 //
 // Kernel (one CTA per 128 x 96 output tile, 10 warps, one CTA per SM):
-//   warp 0: TMA producer.  Per 32-deep K step: the s slices of the B tile (double-
+//   warp 0: TMA producer.  Per 32-deep K step: the s slices of the B tile (BSTAGES
 //           buffered), then the s slices of the A tile through an 8-stage ring.
 //   warp 1: TMEM allocation (512 columns; 5 accumulators x 96) and MMA issue (one
 //           thread): for A slice i, MMAs with B slices i' <= s-1-i into accumulator
@@ -63,14 +63,14 @@ enum SliceKind : int { kBF16 = 0, kI8 = 1 };
 template <int KIND> struct Cfg;
 template <> struct Cfg<kBF16> {
     using Elem = __nv_bfloat16;
-    static constexpr int BN = 96, BK = 32, CHUNK = 128, MAXS = 6, NACC = 5, ASTAGES = 8;
+    static constexpr int BN = 96, BK = 32, CHUNK = 128, MAXS = 6, NACC = 5, ASTAGES = 8, BSTAGES = 2;
     // BF16 x BF16 -> FP32, K-major A and B, M = BM, N = BN
     static constexpr uint32_t IDESC =
         (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
 };
 template <> struct Cfg<kI8> {
     using Elem = int8_t;
-    static constexpr int BN = 64, BK = 64, CHUNK = 32768, MAXS = 7, NACC = 7, ASTAGES = 12;
+    static constexpr int BN = 64, BK = 64, CHUNK = 32768, MAXS = 7, NACC = 7, ASTAGES = 12, BSTAGES = 2;
     // S8 x S8 -> S32, K-major A and B, M = BM, N = BN
     static constexpr uint32_t IDESC =
         (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
@@ -81,8 +81,8 @@ template <int KIND> struct Layout {
     static constexpr int A_TILE = BM * 64;        // bytes per A slice tile (64-byte K rows)
     static constexpr int B_TILE = C::BN * 64;     // bytes per B slice tile (a multiple of the 512-B atom)
     static constexpr int EPI_COLS = C::BN / 2;    // columns per epilogue thread
-    // dynamic shared memory: [B buffers: 2 x MAXS tiles][A ring: ASTAGES tiles], 1024-aligned
-    static constexpr int SMEM_B = 2 * C::MAXS * B_TILE;
+    // dynamic shared memory: [B buffers: BSTAGES x MAXS tiles][A ring: ASTAGES tiles], 1024-aligned
+    static constexpr int SMEM_B = C::BSTAGES * C::MAXS * B_TILE;
     static constexpr int SMEM_A = C::ASTAGES * A_TILE;
     static constexpr int SMEM_BYTES = SMEM_B + SMEM_A + 1024;  // + alignment slack
     static_assert(C::NACC * C::BN <= 512, "accumulators exceed TMEM");
@@ -209,13 +209,14 @@ gemm_split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
     using C = Cfg<KIND>;
     using L = Layout<KIND>;
     constexpr int BN = C::BN, BK = C::BK, CHUNK = C::CHUNK, MAXS = C::MAXS, NACC = C::NACC, ASTAGES = C::ASTAGES;
+    constexpr int BSTAGES = C::BSTAGES;
     constexpr int A_TILE = L::A_TILE, B_TILE = L::B_TILE, EPI_COLS = L::EPI_COLS, SMEM_B = L::SMEM_B;
     extern __shared__ __align__(16) unsigned char smem_split[];
     // tiles need 512-byte alignment (64-byte swizzle atoms); SMEM_BYTES includes the slack
     unsigned char *base = reinterpret_cast<unsigned char *>(((uintptr_t)smem_split + 1023) & ~(uintptr_t)1023);
-    unsigned char *sB = base;               // [2][MAXS][B_TILE]
+    unsigned char *sB = base;               // [BSTAGES][MAXS][B_TILE]
     unsigned char *sA = base + SMEM_B;      // [ASTAGES][A_TILE]
-    __shared__ __align__(8) uint64_t a_full[ASTAGES], a_empty[ASTAGES], b_full[2], b_empty[2], acc_full, acc_empty,
+    __shared__ __align__(8) uint64_t a_full[ASTAGES], a_empty[ASTAGES], b_full[BSTAGES], b_empty[BSTAGES], acc_full, acc_empty,
         mma_done;
     __shared__ uint32_t tmem_base;
     __shared__ volatile int abort_flag;
@@ -239,7 +240,7 @@ gemm_split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
             mbar_init(&a_full[q], 1);
             mbar_init(&a_empty[q], 1);
         }
-        for (int q = 0; q < 2; q++) {
+        for (int q = 0; q < BSTAGES; q++) {
             mbar_init(&b_full[q], 1);
             mbar_init(&b_empty[q], 1);
         }
@@ -263,12 +264,12 @@ gemm_split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
         if (lane == 0) {
             int astage = 0, ause = 0;
             uint32_t aph = 0;      // phase bits of the A stages, one bit per stage
-            uint32_t bph = 0;      // phase bits of the two B buffers
+            uint32_t bph = 0;      // phase bits of the B buffers, one bit per buffer
             uint32_t afill = 0;    // stages holding a load not yet observed complete (for the drain)
-            int bfills[2] = {0, 0};
+            int bfills[BSTAGES] = {};
             for (int t = 0; t < ksteps && !abort_flag; t++) {
-                const int bb = t & 1;
-                if (t >= 2) {
+                const int bb = t % BSTAGES;
+                if (t >= BSTAGES) {
                     if (!mbar_wait(&b_empty[bb], (bph >> bb) & 1u, &abort_flag, p.err)) break;
                     bph ^= 1u << bb;
                 }
@@ -299,7 +300,7 @@ gemm_split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                     const int uses = ause / ASTAGES + (q < ause % ASTAGES ? 1 : 0);
                     if (uses) mbar_drain(&a_full[q], (uint32_t)((uses - 1) & 1));
                 }
-                for (int q = 0; q < 2; q++)
+                for (int q = 0; q < BSTAGES; q++)
                     if (bfills[q]) mbar_drain(&b_full[q], (uint32_t)((bfills[q] - 1) & 1));
             }
         }
@@ -318,7 +319,7 @@ gemm_split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                 for (int tt = 0; tt < kPerChunk && ok; tt++) {
                     const int t = c * kPerChunk + tt;
                     if (t >= ksteps) break;
-                    const int bb = t & 1;
+                    const int bb = t % BSTAGES;
                     if (!mbar_wait(&b_full[bb], (bph >> bb) & 1u, &abort_flag, p.err)) { ok = false; break; }
                     bph ^= 1u << bb;
                     tc_fence_after();
