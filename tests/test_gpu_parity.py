@@ -360,3 +360,27 @@ def test_lookahead_matches_serial_path_with_guards(cuda_ok, side):
     assert raw < 1e-9, raw
     ref = oracle.tgevc3(side, "A", S, P, ar, be, alphai=ai)
     compare(d, VL0, VR0, m, ref[0], ref[1], TOL_ILL[np.float64], check_resid=False)
+
+
+@pytest.mark.parametrize("sk,side", [("int8", "R"), ("int8", "L"), ("bf16", "R")])
+def test_split_form_guards_across_groups(cuda_ok, sk, side):
+    """Split-precision form on the n = 1536 pencil whose eigenvectors grow by 1e16 per row
+    block: its trailing updates (groups of eight row blocks, K = 2 x 512, at least 512 rows)
+    run as slice products, and guards that fire in a group's upper blocks rescale the
+    operand rows of up to seven blocks below them.  Must be finite, show the guards firing
+    and match the oracle after normalisation (1e-8, as the plain form on this pencil)."""
+    n = 1536
+    S, P, ar, ai, be = _overflow_pencil(n, 91, 1e16, side == "L")
+    I = np.eye(n, order="F")
+    d = dict(side=side, howmny="A", S=S, P=P, alpha=ar, beta=be, alphai=ai, VL_in=I, VR_in=I.copy(order="F"),
+             name="overflow")
+    X.set_flags(X.SPLIT | X.slices(7 if sk == "int8" else 6) | (X.SPLIT_INT8 if sk == "int8" else 0))
+    try:
+        VL, VR, m, info = run_gpu(d)
+    finally:
+        X.set_flags(0)
+    V = VL if side == "L" else VR
+    assert info == 0 and np.isfinite(V).all()
+    assert (np.abs(np.diag(V[:, :n])) < 1).sum() >= 8
+    ref = oracle.tgevc3(side, "A", S, P, ar, be, alphai=ai)
+    compare(d, VL, VR, m, ref[0], ref[1], TOL_ILL[np.float64], check_resid=False)
