@@ -78,7 +78,9 @@ __global__ void __launch_bounds__(256) gemm_simt(GemmArgs<E> g)
     __shared__ E As[BK][BM + 1];
     __shared__ E Bs[BK][BN + 1];
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    // with a per-column K extent (back-transform: triangular B, extent growing with the
+    // column) the column tiles run last-first, so the longest tiles start first
+    const int m0 = blockIdx.x * BM, n0 = (g.kext ? gridDim.y - 1 - blockIdx.y : blockIdx.y) * BN;
     const int kmax = tile_kmax(g, n0, BN);
     E acc[4][4];
 #pragma unroll
@@ -144,7 +146,7 @@ __global__ void __launch_bounds__(256) gemm_simt(GemmArgs<E> g)
 // the launcher, which uses the SIMT kernel otherwise).
 // ------------------------------------------------------------------------------------
 namespace dmma {
-constexpr int BM = 128, BN = 64, BK = 16, STAGES = 3;
+constexpr int BM = 128, BN = 64, BK = 16, STAGES = 3;  // BK divides kKPad (segment K)
 constexpr int ALD = BM + 8;   // A tile stored [k][m]
 constexpr int BLD = BK + 4;   // B tile stored [n][k]
 constexpr int A_STAGE = BK * ALD;
@@ -179,7 +181,9 @@ __global__ void __launch_bounds__(256) gemm_dmma(GemmArgs<double> g)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = warp & 3, wn = warp >> 2;
     const int gq = lane >> 2, tq = lane & 3;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    // with a per-column K extent (back-transform: triangular B, extent growing with the
+    // column) the column tiles run last-first, so the longest tiles start first
+    const int m0 = blockIdx.x * BM, n0 = (g.kext ? gridDim.y - 1 - blockIdx.y : blockIdx.y) * BN;
     const int kmax = tile_kmax(g, n0, BN);
     const int ktiles = (kmax + BK - 1) / BK;
 
@@ -200,9 +204,9 @@ __global__ void __launch_bounds__(256) gemm_dmma(GemmArgs<double> g)
         double *as = As + st * A_STAGE;
         double *bs = Bs + st * B_STAGE;
 #pragma unroll
-        for (int q = 0; q < 4; q++) {  // A: 16 columns x 64 chunks
+        for (int q = 0; q < BK * BM / 512; q++) {  // A: BK columns x BM/2 chunks of 16 bytes
             int e = tid + 256 * q;
-            int kk = e >> 6, ch = e & 63;
+            int kk = e / (BM / 2), ch = e % (BM / 2);
             int row = m0 + 2 * ch, col = k0 - kb + kk;
             int bytes = 0;
             if (s >= 0 && k0 + kk < kmax && col < sg.acols) bytes = row + 1 < g.M ? 16 : (row < g.M ? 8 : 0);
@@ -210,9 +214,9 @@ __global__ void __launch_bounds__(256) gemm_dmma(GemmArgs<double> g)
             cp_async16(as + kk * ALD + 2 * ch, gp, bytes);
         }
 #pragma unroll
-        for (int q = 0; q < 2; q++) {  // B: 64 columns x 8 chunks
+        for (int q = 0; q < BN * BK / 512; q++) {  // B: BN columns x BK/2 chunks
             int e = tid + 256 * q;
-            int nn = e >> 3, ch = e & 7;
+            int nn = e / (BK / 2), ch = e % (BK / 2);
             int kr = sg.boff + k0 - kb + 2 * ch, col = n0 + nn;
             int lim = min(sg.boff + kmax - kb, g.brows);
             int bytes = 0;
@@ -314,7 +318,9 @@ __global__ void __launch_bounds__(256) gemm_dmma_cplx(GemmArgs<cplx<double>> g)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = warp & 1, wn = warp >> 1;
     const int gq = lane >> 2, tq = lane & 3;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    // with a per-column K extent (back-transform: triangular B, extent growing with the
+    // column) the column tiles run last-first, so the longest tiles start first
+    const int m0 = blockIdx.x * BM, n0 = (g.kext ? gridDim.y - 1 - blockIdx.y : blockIdx.y) * BN;
     const int kmax = tile_kmax(g, n0, BN);
     const int ktiles = (kmax + BK - 1) / BK;
 

@@ -222,7 +222,9 @@ gemm_split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
     __shared__ volatile int abort_flag;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    // with a per-column K extent (back-transform) the column tiles run last-first, so the
+    // longest tiles start first
+    const int m0 = blockIdx.x * BM, n0 = (p.kext ? gridDim.y - 1 - blockIdx.y : blockIdx.y) * BN;
     const int s = p.s;
     const int nacc = s < NACC ? s : NACC;
     int kmax = p.Kp;
