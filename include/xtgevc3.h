@@ -118,6 +118,41 @@ int xtgevc3_ctgevc3_dev(unsigned flags, void *stream, char side, char howmny, co
                         const float *S, int lds, const float *P, int ldp, const float *alpha, const float *beta,
                         float *VL, int ldvl, float *VR, int ldvr, int mm, int *m, int *info);
 
+/* ---- standard eigenproblem: xTREVC3 (no counterpart in the upstream library) ----------
+ * Right and/or left eigenvectors of an upper quasi-triangular Schur factor T (from LAPACK
+ * xHSEQR / xGEES: real T with standardised 2x2 blocks; complex T upper triangular), with
+ * the argument meaning, INFO codes and results of LAPACK xTREVC3 (the upstream benchmarks
+ * time LAPACK's dtrevc3 beside dtgevc3, benchmarks/bench_dtgevc3.cpp:127-149): HOWMNY 'A',
+ * 'B' (VL/VR hold Q on entry) or 'S'; every eigenvector scaled so that its largest
+ * component has |re| + |im| = 1; a real pair stored as (Re, Im) columns with LAPACK's
+ * phase.  Eigenvalues are read from T's diagonal blocks.  Computed by the generalized
+ * solver with P = I (built on the device; its zero strips are skipped).  Differences from
+ * LAPACK: SELECT is read-only (LAPACK rewrites a pair's flags), WORK is not used (a query,
+ * LWORK = -1, answers the minimum max(1, 3n), complex max(1, 2n) and LRWORK max(1, n)).
+ * INFO: -1 SIDE, -2 HOWMNY, -4 N, -6 LDT, -8 LDVL, -10 LDVR, -11 MM < M, -14 LWORK,
+ * -16 LRWORK (complex), 1 a CUDA failure.  Complex arrays interleaved.                  */
+void xtgevc3_dtrevc3(char side, char howmny, const int *select, int n, const double *T, int ldt, double *VL,
+                     int ldvl, double *VR, int ldvr, int mm, int *m, double *work, int lwork, int *info);
+void xtgevc3_strevc3(char side, char howmny, const int *select, int n, const float *T, int ldt, float *VL, int ldvl,
+                     float *VR, int ldvr, int mm, int *m, float *work, int lwork, int *info);
+void xtgevc3_ztrevc3(char side, char howmny, const int *select, int n, const double *T, int ldt, double *VL,
+                     int ldvl, double *VR, int ldvr, int mm, int *m, double *work, int lwork, double *rwork,
+                     int lrwork, int *info);
+void xtgevc3_ctrevc3(char side, char howmny, const int *select, int n, const float *T, int ldt, float *VL, int ldvl,
+                     float *VR, int ldvr, int mm, int *m, float *work, int lwork, float *rwork, int lrwork, int *info);
+/* device forms: T, VL, VR device pointers, select a host array; flags as the _dev forms
+ * above (XTGEVC3_NORMALIZE is implied); returns 0, or 1 if a CUDA call failed           */
+int xtgevc3_dtrevc3_dev(unsigned flags, void *stream, char side, char howmny, const int *select, int n,
+                        const double *T, int ldt, double *VL, int ldvl, double *VR, int ldvr, int mm, int *m,
+                        int *info);
+int xtgevc3_strevc3_dev(unsigned flags, void *stream, char side, char howmny, const int *select, int n,
+                        const float *T, int ldt, float *VL, int ldvl, float *VR, int ldvr, int mm, int *m, int *info);
+int xtgevc3_ztrevc3_dev(unsigned flags, void *stream, char side, char howmny, const int *select, int n,
+                        const double *T, int ldt, double *VL, int ldvl, double *VR, int ldvr, int mm, int *m,
+                        int *info);
+int xtgevc3_ctrevc3_dev(unsigned flags, void *stream, char side, char howmny, const int *select, int n,
+                        const float *T, int ldt, float *VL, int ldvl, float *VR, int ldvr, int mm, int *m, int *info);
+
 /* ---- allocation-free device entry point (no counterpart in the upstream library) -----
  * Same computation and arguments as xtgevc3_dtgevc3_dev (without flags), for callers that
  * cannot allocate device memory at this point: e.g. a framework that has reserved the

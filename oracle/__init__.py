@@ -173,6 +173,62 @@ def lapack_tgevc(S, P):
     return VL, VR
 
 
+def lapack_trevc3(side, howmny, T, VL=None, VR=None, select=None, mm=None):
+    """Oracle of the xTREVC3 entry points: LAPACK xTREVC3 from SciPy's bundled OpenBLAS,
+    called through its Fortran interface with the workspace its query asks for.  VL/VR hold
+    Q on entry for HOWMNY='B'.  SELECT is copied (LAPACK rewrites a pair's flags).  Returns
+    (VL, VR, m, info)."""
+    dt = T.dtype.type
+    pfx = _PREFIX[dt]
+    n = T.shape[0]
+    f = getattr(_openblas(), f"scipy_{pfx}trevc3_")
+    T = np.asfortranarray(T)
+    mm = n if mm is None else mm
+    VL = np.zeros((n, max(mm, 1)), dtype=dt, order="F") if VL is None else np.asfortranarray(VL).copy(order="F")
+    VR = np.zeros((n, max(mm, 1)), dtype=dt, order="F") if VR is None else np.asfortranarray(VR).copy(order="F")
+    sel = np.zeros(max(n, 1), dtype=np.int32) if select is None else np.ascontiguousarray(select, dtype=np.int32).copy()
+    cplx = pfx in "zc"
+    rdt = np.float64 if pfx in "dz" else np.float32
+    iv = lambda v: ct.byref(ct.c_int(v))  # noqa: E731
+    m = ct.c_int(0)
+    info = ct.c_int(0)
+
+    def call(work, lwork, rwork, lrwork):
+        args = [ct.c_char_p(side.encode()), ct.c_char_p(howmny.encode()), _ptr(sel), iv(n), _ptr(T), iv(max(n, 1)),
+                _ptr(VL), iv(max(n, 1)), _ptr(VR), iv(max(n, 1)), iv(mm), ct.byref(m), _ptr(work), iv(lwork)]
+        if cplx:
+            args += [_ptr(rwork), iv(lrwork)]
+        args += [ct.byref(info), ct.c_size_t(1), ct.c_size_t(1)]
+        f(*args)
+
+    q, rq = np.zeros(2, dtype=dt), np.zeros(2, dtype=rdt)
+    call(q, -1, rq, -1)
+    if info.value != 0:
+        return VL, VR, m.value, info.value
+    lwork = max(int(np.real(q[0])), 1)
+    lrwork = max(int(rq[0]), n, 1)
+    call(np.zeros(lwork, dtype=dt), lwork, np.zeros(lrwork, dtype=rdt), lrwork)
+    return VL, VR, m.value, info.value
+
+
+def schur_real(n, seed, dtype=np.float64):
+    """Real Schur form of an iid N(0,1) matrix (LAPACK xGEES through SciPy: T quasi-upper
+    triangular with standardised 2x2 blocks, Q orthogonal)."""
+    import scipy.linalg
+    A = np.random.default_rng(seed).standard_normal((n, n))
+    T, Q = scipy.linalg.schur(A.astype(dtype), output="real")
+    return np.asfortranarray(T), np.asfortranarray(Q)
+
+
+def schur_complex(n, seed, dtype=np.complex128):
+    """Complex Schur form of an iid complex N(0,1) matrix (LAPACK xGEES through SciPy)."""
+    import scipy.linalg
+    rng = np.random.default_rng(seed)
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    T, Q = scipy.linalg.schur(A.astype(dtype), output="complex")
+    return np.asfortranarray(T), np.asfortranarray(Q)
+
+
 # --------------------------------------------------------------------------------------
 # residuals and normalisation
 # --------------------------------------------------------------------------------------

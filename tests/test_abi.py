@@ -192,3 +192,46 @@ def test_noalloc_refuses_oversize_before_device_work():
                                        ct.byref(m), ct.byref(info))
     assert rc == 2
     assert "n=479" in X.last_error() and "8393728 bytes" in X.last_error(), X.last_error()
+
+
+@pytest.mark.parametrize("pfx", ["d", "z"])
+def test_trevc3_info_codes_and_query(pfx):
+    """xtgevc3_{d,z}trevc3: LAPACK xTREVC3's INFO codes in its order, answered before any
+    CUDA call (-1 SIDE, -2 HOWMNY, -4 N, -6 LDT, -8 LDVL, -10 LDVR, -11 MM < M, -14 LWORK,
+    -16 LRWORK), and the workspace query (minimum max(1, 3n) real, max(1, 2n) complex)."""
+    n = 6
+    dt = np.float64 if pfx == "d" else np.complex128
+    T = np.asfortranarray(np.triu(np.arange(1, n * n + 1, dtype=np.float64).reshape(n, n)).astype(dt))
+    V = np.zeros((n, n), dtype=dt, order="F")
+
+    def call(side=b"B", howmny=b"A", nn=n, ldt=n, ldvl=n, ldvr=n, mm=n, lwork=None, lrwork=n, sel=None):
+        m, info = ct.c_int(-7), ct.c_int(0)
+        work = np.zeros(4 * n, dtype=dt)
+        lw = (3 if pfx == "d" else 2) * n if lwork is None else lwork
+        if pfx == "d":
+            X.lib().xtgevc3_dtrevc3(side, howmny, sel, nn, T.ctypes.data, ldt, V.ctypes.data, ldvl, V.ctypes.data,
+                                   ldvr, mm, ct.byref(m), work.ctypes.data, lw, ct.byref(info))
+        else:
+            rwork = np.zeros(n)
+            X.lib().xtgevc3_ztrevc3(side, howmny, sel, nn, T.ctypes.data, ldt, V.ctypes.data, ldvl, V.ctypes.data,
+                                   ldvr, mm, ct.byref(m), work.ctypes.data, lw, rwork.ctypes.data, lrwork,
+                                   ct.byref(info))
+        return info.value, m.value, work
+    assert call(side=b"X")[0] == -1
+    assert call(howmny=b"Q")[0] == -2
+    assert call(nn=-1)[0] == -4
+    assert call(ldt=n - 1)[0] == -6
+    assert call(ldvl=n - 1)[0] == -8
+    assert call(side=b"R", ldvl=1)[0] != -8  # VL not referenced for SIDE='R'
+    assert call(ldvr=n - 1)[0] == -10
+    info, m, _ = call(mm=n - 1)
+    assert (info, m) == (-11, n)
+    assert call(lwork=1)[0] == -14
+    if pfx == "z":
+        assert call(lrwork=0)[0] == -16
+    info, m, work = call(lwork=-1)
+    assert info == 0 and int(np.real(work[0])) == (3 if pfx == "d" else 2) * n
+    sel = np.zeros(n, dtype=np.int32)
+    sel[[1, 4]] = 1
+    info, m, _ = call(howmny=b"S", sel=sel.ctypes.data, lwork=-1)
+    assert (info, m) == (0, 2)

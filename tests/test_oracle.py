@@ -101,3 +101,40 @@ def test_oracle_matches_upstream_library_with_many_guards(prec):
         o, r = oracle.to_complex_real_storage(o, ai), oracle.to_complex_real_storage(r, ai)
     err, _ = oracle.max_rel_diff(o, r)
     assert err < 1e-11, err
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.complex128])
+def test_lapack_trevc3_oracle_residual(dt):
+    """The xTREVC3 oracle (LAPACK through SciPy's OpenBLAS) on a Schur form A = Q T Q^H:
+    the back-transformed eigenvectors satisfy A v = w v to a few eps (w from T's diagonal
+    blocks), and every column is normalised to max |re| + |im| = 1."""
+    n = 80
+    T, Q = (oracle.schur_real if dt == np.float64 else oracle.schur_complex)(n, 3, dt)
+    VL, VR, m, info = oracle.lapack_trevc3("B", "B", T, VL=Q, VR=Q)
+    assert (m, info) == (n, 0)
+    A = Q @ T @ Q.conj().T
+    w = np.diag(T).astype(np.complex128)
+    ai = np.zeros(n)
+    if dt == np.float64:
+        k = 0
+        while k < n:
+            if k + 1 < n and T[k + 1, k] != 0:
+                wi = np.sqrt(abs(T[k, k + 1])) * np.sqrt(abs(T[k + 1, k]))
+                w[k], w[k + 1] = T[k, k] + 1j * wi, T[k, k] - 1j * wi
+                ai[k], ai[k + 1] = wi, -wi
+                k += 2
+            else:
+                k += 1
+        V = oracle.to_complex_real_storage(VR, ai)
+        U = oracle.to_complex_real_storage(VL, ai)
+    else:
+        V, U = VR, VL
+    eps = np.finfo(np.float64).eps
+    nA = np.abs(A).sum(0).max()
+    r = np.abs(A @ V - V * w[None, :]).sum(0) / (nA * np.abs(V).sum(0)) / eps
+    assert r.max() < 100, r.max()
+    rl = np.abs(A.conj().T @ U - U * np.conj(w)[None, :]).sum(0) / (nA * np.abs(U).sum(0)) / eps
+    assert rl.max() < 100, rl.max()
+    mags = np.abs(VR.real) + np.abs(VR.imag) if dt == np.complex128 else None
+    if mags is not None:
+        assert np.allclose(mags.max(0), 1.0)

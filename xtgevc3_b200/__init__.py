@@ -67,6 +67,18 @@ def lib():
             f = getattr(L, f"xtgevc3_{p}tgevc3_dev")
             f.argtypes = [_U, _P, _C, _C, _P, _I, _P, _I, _P, _I, _P, _P, _P, _I, _P, _I, _I, _P, _P]
             f.restype = _I
+        for p in "ds":  # xTREVC3
+            f = getattr(L, f"xtgevc3_{p}trevc3")
+            f.argtypes = [_C, _C, _P, _I, _P, _I, _P, _I, _P, _I, _I, _P, _P, _I, _P]
+            f.restype = None
+        for p in "zc":
+            f = getattr(L, f"xtgevc3_{p}trevc3")
+            f.argtypes = [_C, _C, _P, _I, _P, _I, _P, _I, _P, _I, _I, _P, _P, _I, _P, _I, _P]
+            f.restype = None
+        for p in "dszc":
+            f = getattr(L, f"xtgevc3_{p}trevc3_dev")
+            f.argtypes = [_U, _P, _C, _C, _P, _I, _P, _I, _P, _I, _P, _I, _I, _P, _P]
+            f.restype = _I
         L.xtgevc3_set_flags.argtypes = [_U]
         L.xtgevc3_set_flags.restype = None
         L.xtgevc3_get_flags.restype = _U
@@ -247,6 +259,68 @@ def tgevc3_dev(side, howmny, S, P, alpha, beta, alphai=None, VL=None, VR=None, s
     rc = getattr(L, f"xtgevc3_{pfx}tgevc3_dev")(*head, *eig, vlp, ldvl, vrp, ldvr, mm, ct.byref(m), ct.byref(info))
     if rc != 0:
         raise RuntimeError(f"xtgevc3_{pfx}tgevc3_dev failed: {last_error()}")
+    return m.value, info.value
+
+
+# ---- standard problem (xTREVC3) ------------------------------------------------------------
+def trevc3(side, howmny, T, VL=None, VR=None, select=None, mm=None, lwork=None):
+    """Host-array form of s/d/c/ztrevc3: eigenvectors of the quasi-triangular Schur factor T
+    with LAPACK xTREVC3's conventions (include/xtgevc3.h).  VL/VR (Q on entry for
+    HOWMNY='B') are updated in place.  Returns (VL, VR, m, info)."""
+    L = lib()
+    dt = T.dtype.type
+    pfx = _PFX[dt]
+    n = T.shape[0]
+    T = np.asfortranarray(T)
+    sel = None if select is None else np.ascontiguousarray(select, dtype=np.int32)
+    mm = n if mm is None else mm
+    if VL is None:
+        VL = np.zeros((n, max(mm, 1)), dtype=dt, order="F")
+    if VR is None:
+        VR = np.zeros((n, max(mm, 1)), dtype=dt, order="F")
+    assert VL.flags.f_contiguous and VR.flags.f_contiguous
+    m, info = ct.c_int(0), ct.c_int(0)
+    ld = max(n, 1)
+    fn = getattr(L, f"xtgevc3_{pfx}trevc3")
+    head = [side.encode(), howmny.encode(), _ptr(sel), n, _ptr(T), ld, _ptr(VL), ld, _ptr(VR), ld, mm, ct.byref(m)]
+    rdt = np.float64 if pfx in "dz" else np.float32
+    q, rq = np.zeros(2, dtype=dt), np.zeros(2, dtype=rdt)
+    if lwork is None:
+        extra = [_ptr(rq), -1] if pfx in "zc" else []
+        fn(*head, _ptr(q), -1, *extra, ct.byref(info))
+        if info.value != 0:
+            return VL, VR, m.value, info.value
+        lwork = int(np.real(q[0]))
+    lrwork = max(n, 1)
+    work = np.zeros(max(min(lwork, 4), 1), dtype=dt)  # the GPU path never touches WORK beyond the query
+    rwork = np.zeros(1, dtype=rdt)
+    extra = [_ptr(rwork), lrwork] if pfx in "zc" else []
+    fn(*head, _ptr(work), lwork, *extra, ct.byref(info))
+    if info.value > 0:
+        raise RuntimeError(f"xtgevc3_{pfx}trevc3 failed: {last_error()}")
+    return VL, VR, m.value, info.value
+
+
+def trevc3_dev(side, howmny, T, VL=None, VR=None, select=None, flags=0, stream=None):
+    """Device form of xTREVC3 on column-major CUDA tensors.  Raises on CUDA failure;
+    returns (m, info)."""
+    import torch
+    L = lib()
+    pfx = {torch.float64: "d", torch.float32: "s", torch.complex128: "z", torch.complex64: "c"}[T.dtype]
+    n = T.shape[0]
+    tp, ldt = _colmajor(T)
+    vlp, ldvl = _colmajor(VL)
+    vrp, ldvr = _colmajor(VR)
+    mm = max(VL.shape[1] if VL is not None else 0, VR.shape[1] if VR is not None else 0)
+    sel = None if select is None else np.ascontiguousarray(select, dtype=np.int32)
+    if stream is None:
+        stream = torch.cuda.current_stream().cuda_stream
+    m, info = ct.c_int(0), ct.c_int(0)
+    rc = getattr(L, f"xtgevc3_{pfx}trevc3_dev")(int(flags), ct.c_void_p(stream), side.encode(), howmny.encode(),
+                                                 _ptr(sel), n, tp, ldt, vlp, ldvl, vrp, ldvr, mm, ct.byref(m),
+                                                 ct.byref(info))
+    if rc != 0:
+        raise RuntimeError(f"xtgevc3_{pfx}trevc3_dev failed: {last_error()}")
     return m.value, info.value
 
 

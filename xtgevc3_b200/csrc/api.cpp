@@ -6,7 +6,10 @@
 #include "args.h"
 #include "engine.cuh"
 
+#include <algorithm>
 #include <atomic>
+#include <cctype>
+#include <cmath>
 #include <complex>
 #include <cstring>
 #include <vector>
@@ -106,13 +109,14 @@ int run_host(char side, char howmny, const int *select, int n, const void *S, in
     for (cudaEvent_t &ev : r.ev)
         if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
     if ((e = cudaMallocAsync(&r.dS, mat, r.st)) != cudaSuccess) return fail(e, "cudaMallocAsync");
-    if ((e = cudaMallocAsync(&r.dP, mat, r.st)) != cudaSuccess) return fail(e, "cudaMallocAsync");
+    // P = nullptr: the standard problem (P = I, built by the solver)
+    if (P && (e = cudaMallocAsync(&r.dP, mat, r.st)) != cudaSuccess) return fail(e, "cudaMallocAsync");
     if (want_l && (e = cudaMallocAsync(&r.dVL, (size_t)ld * vcols * sizeof(E), r.st)) != cudaSuccess)
         return fail(e, "cudaMallocAsync");
     if (want_r && (e = cudaMallocAsync(&r.dVR, (size_t)ld * vcols * sizeof(E), r.st)) != cudaSuccess)
         return fail(e, "cudaMallocAsync");
     const int panel = 512;
-    for (int which = 0; which < 2; which++) {
+    for (int which = 0; which < (P ? 2 : 1); which++) {
         void *dst = which ? r.dP : r.dS;
         const void *src = which ? P : S;
         const int lsrc = which ? ldp : lds;
@@ -126,6 +130,11 @@ int run_host(char side, char howmny, const int *select, int n, const void *S, in
         }
     }
     xtg::Options opt = make_opts(flags);
+    if (!P) {  // xTREVC3 conventions
+        opt.p_identity = 1;
+        opt.lapack_pairs = 1;
+        opt.normalize = 1;
+    }
     // Q and Z (second stream) go after every copy that the solve's first kernels need: S and
     // P, the eigenvalues and the column lists (the solver calls `staged` once those are
     // queued).  The back-transform needs Q or Z only at the end; queued earlier, their 2n^2
@@ -223,6 +232,175 @@ int device_form(unsigned flags, void *stream, char side, char howmny, const int 
     return rc;
 }
 
+// ---- standard problem: xTREVC3 ------------------------------------------------------------
+// Eigenvectors of an upper quasi-triangular Schur factor T (T = Q^H A Q from LAPACK xHSEQR /
+// xGEES) with LAPACK xTREVC3's argument meaning, INFO codes and output: the generalized
+// solver with P = I and beta = 1 (P built on the device, its zero strips skipped), every
+// eigenvector normalised to max |re| + |im| = 1, real pairs with LAPACK's phase.
+
+// Eigenvalues from T's diagonal blocks.  A 2x2 block (k, k+1) is LAPACK-standardised
+// (T(k,k) = T(k+1,k+1)): alpha = T(k,k) +- i sqrt|T(k,k+1)| sqrt|T(k+1,k)|, as xTREVC3 takes
+// them.  d: the diagonal (complex: interleaved); sub, sup: sub- and superdiagonal (real).
+template <class R, bool CPLX>
+void trevc3_eigs(int n, const std::vector<R> &d, const std::vector<R> &sub, const std::vector<R> &sup,
+                 std::vector<R> &alpha, std::vector<R> &alphai, std::vector<R> &beta)
+{
+    if constexpr (CPLX) {
+        alpha = d;
+        beta.assign(2 * (size_t)n, R(0));
+        for (int k = 0; k < n; k++) beta[2 * (size_t)k] = R(1);
+        alphai.clear();
+    } else {
+        alpha.assign(n, R(0));
+        alphai.assign(n, R(0));
+        beta.assign(n, R(1));
+        for (int k = 0; k < n;) {
+            alpha[k] = d[k];
+            if (k + 1 < n && sub[k] != R(0)) {
+                const R wi = std::sqrt(std::abs(sup[k])) * std::sqrt(std::abs(sub[k]));
+                alpha[k + 1] = d[k];
+                alphai[k] = wi;
+                alphai[k + 1] = -wi;
+                k += 2;
+            } else {
+                k += 1;
+            }
+        }
+    }
+}
+
+// LAPACK xTREVC3's checks that need no eigenvalues, in its order (-1 SIDE, -2 HOWMNY, -4 N,
+// -6 LDT, -8 LDVL, -10 LDVR); -11 (MM < M) follows once M is known.
+inline int trevc3_pre(char side, char howmny, int n, int ldt, int ldvl, int ldvr)
+{
+    const bool rightv = side == 'R' || side == 'B', leftv = side == 'L' || side == 'B';
+    if (!rightv && !leftv) return -1;
+    if (howmny != 'A' && howmny != 'B' && howmny != 'S') return -2;
+    if (n < 0) return -4;
+    if (ldt < std::max(1, n)) return -6;
+    if (ldvl < 1 || (leftv && ldvl < n)) return -8;
+    if (ldvr < 1 || (rightv && ldvr < n)) return -10;
+    return 0;
+}
+
+// M: selected eigenvectors (a pair counts twice when either of its flags is set)
+template <class R, bool CPLX>
+int trevc3_count(char howmny, const int *select, int n, const std::vector<R> &alphai)
+{
+    int num = 0;
+    for (int k = 0; k < n;) {
+        const bool pair = !CPLX && alphai[k] != R(0) && k + 1 < n;
+        bool sel = howmny != 'S';
+        if (!sel) sel = select && (select[k] != 0 || (pair && select[k + 1] != 0));
+        if (sel) num += pair ? 2 : 1;
+        k += pair ? 2 : 1;
+    }
+    return num;
+}
+
+// diagonal, sub- and superdiagonal of T (host or device memory)
+template <class R, bool CPLX>
+int trevc3_diagonals(const void *T, int ldt, int n, bool on_device, cudaStream_t st, std::vector<R> &d,
+                     std::vector<R> &sub, std::vector<R> &sup)
+{
+    const int w = CPLX ? 2 : 1;  // reals per element
+    d.assign((size_t)w * n, R(0));
+    sub.assign(std::max(0, n - 1), R(0));
+    sup.assign(std::max(0, n - 1), R(0));
+    const R *t = static_cast<const R *>(T);
+    const size_t step = (size_t)w * (ldt + 1);
+    if (!on_device) {
+        for (int k = 0; k < n; k++)
+            for (int q = 0; q < w; q++) d[(size_t)w * k + q] = t[step * k + q];
+        if constexpr (!CPLX)
+            for (int k = 0; k + 1 < n; k++) {
+                sub[k] = t[step * k + 1];
+                sup[k] = t[step * k + ldt];
+            }
+        return 0;
+    }
+    cudaError_t e = cudaMemcpy2DAsync(d.data(), w * sizeof(R), t, step * sizeof(R), w * sizeof(R), n,
+                                      cudaMemcpyDeviceToHost, st);
+    if (!CPLX && n > 1 && e == cudaSuccess)
+        e = cudaMemcpy2DAsync(sub.data(), sizeof(R), t + 1, step * sizeof(R), sizeof(R), n - 1, cudaMemcpyDeviceToHost,
+                              st);
+    if (!CPLX && n > 1 && e == cudaSuccess)
+        e = cudaMemcpy2DAsync(sup.data(), sizeof(R), t + ldt, step * sizeof(R), sizeof(R), n - 1,
+                              cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        xtg::set_last_error(std::string("xTREVC3 diagonal of T: ") + cudaGetErrorString(e));
+        return 1;
+    }
+    return 0;
+}
+
+// Host form (LWORK >= max(1, 3n) real / max(1, 2n) complex, LRWORK >= max(1, n) complex;
+// work is not used, and a query answers those minima).
+template <class R, bool CPLX, class W>
+void trevc3_host(char side, char howmny, const int *select, int n, const void *T, int ldt, void *VL, int ldvl,
+                 void *VR, int ldvr, int mm, int *m, W *work, int lwork, R *rwork, int lrwork, int *info)
+{
+    side = (char)std::toupper((unsigned char)side);
+    howmny = (char)std::toupper((unsigned char)howmny);
+    const int minw = std::max(1, (CPLX ? 2 : 3) * n), minrw = std::max(1, n);
+    const bool lquery = lwork == -1 || (CPLX && lrwork == -1);
+    if (work) work[0] = W(minw);
+    if (CPLX && rwork) rwork[0] = R(minrw);
+    xtg::set_last_error("");
+    *info = trevc3_pre(side, howmny, n, ldt, ldvl, ldvr);
+    if (*info) return;
+    std::vector<R> d, sub, sup, alpha, alphai, beta;
+    trevc3_diagonals<R, CPLX>(T, ldt, n, false, nullptr, d, sub, sup);
+    trevc3_eigs<R, CPLX>(n, d, sub, sup, alpha, alphai, beta);
+    const int count = trevc3_count<R, CPLX>(howmny, select, n, alphai);
+    if (m) *m = count;
+    if (mm < count) *info = -11;
+    else if (lwork < minw && !lquery) *info = -14;
+    else if (CPLX && lrwork < minrw && !lquery) *info = -16;
+    if (*info || lquery || count == 0) return;
+    if (run_host<R, CPLX>(side, howmny, select, n, T, ldt, nullptr, 0, alpha.data(), CPLX ? nullptr : alphai.data(),
+                          beta.data(), VL, ldvl, VR, ldvr, count, g_flags.load()))
+        *info = 1;
+}
+
+// Device form: T, VL, VR on the current device, select on the host.
+template <class R, bool CPLX>
+int trevc3_device(unsigned flags, void *stream, char side, char howmny, const int *select, int n, const void *T,
+                  int ldt, void *VL, int ldvl, void *VR, int ldvr, int mm, int *m, int *info)
+{
+    int dummy = 0;
+    if (!info) info = &dummy;
+    side = (char)std::toupper((unsigned char)side);
+    howmny = (char)std::toupper((unsigned char)howmny);
+    xtg::set_last_error("");
+    *info = trevc3_pre(side, howmny, n, ldt, ldvl, ldvr);
+    if (*info) return 0;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::vector<R> d, sub, sup, alpha, alphai, beta;
+    if (n > 0 && trevc3_diagonals<R, CPLX>(T, ldt, n, true, st, d, sub, sup)) {
+        *info = 1;
+        return 1;
+    }
+    trevc3_eigs<R, CPLX>(n, d, sub, sup, alpha, alphai, beta);
+    const int count = trevc3_count<R, CPLX>(howmny, select, n, alphai);
+    if (m) *m = count;
+    if (mm < count) {
+        *info = -11;
+        return 0;
+    }
+    if (count == 0) return 0;
+    xtg::Options opt = make_opts(flags);
+    opt.p_identity = 1;
+    opt.lapack_pairs = 1;
+    opt.normalize = 1;
+    const int rc = xtg::solve_device<R, CPLX>(side, howmny, select, n, T, ldt, nullptr, 0, alpha.data(),
+                                              CPLX ? nullptr : alphai.data(), beta.data(), VL, ldvl, VR, ldvr, count,
+                                              opt, st);
+    if (rc) *info = 1;
+    return rc;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------------------
@@ -308,6 +486,65 @@ int xtgevc3_ctgevc3_dev(unsigned flags, void *stream, char side, char howmny, co
 {
     return device_form<float, true>(flags, stream, side, howmny, select, n, S, lds, P, ldp, alpha, nullptr, beta,
                                     VL, ldvl, VR, ldvr, mm, m, info);
+}
+
+void xtgevc3_dtrevc3(char side, char howmny, const int *select, int n, const double *T, int ldt, double *VL,
+                     int ldvl, double *VR, int ldvr, int mm, int *m, double *work, int lwork, int *info)
+{
+    trevc3_host<double, false, double>(side, howmny, select, n, T, ldt, VL, ldvl, VR, ldvr, mm, m, work, lwork,
+                                       nullptr, 0, info);
+}
+
+void xtgevc3_strevc3(char side, char howmny, const int *select, int n, const float *T, int ldt, float *VL, int ldvl,
+                     float *VR, int ldvr, int mm, int *m, float *work, int lwork, int *info)
+{
+    trevc3_host<float, false, float>(side, howmny, select, n, T, ldt, VL, ldvl, VR, ldvr, mm, m, work, lwork, nullptr,
+                                     0, info);
+}
+
+void xtgevc3_ztrevc3(char side, char howmny, const int *select, int n, const double *T, int ldt, double *VL,
+                     int ldvl, double *VR, int ldvr, int mm, int *m, double *work, int lwork, double *rwork,
+                     int lrwork, int *info)
+{
+    trevc3_host<double, true, std::complex<double>>(side, howmny, select, n, T, ldt, VL, ldvl, VR, ldvr, mm, m,
+                                                    reinterpret_cast<std::complex<double> *>(work), lwork, rwork,
+                                                    lrwork, info);
+}
+
+void xtgevc3_ctrevc3(char side, char howmny, const int *select, int n, const float *T, int ldt, float *VL, int ldvl,
+                     float *VR, int ldvr, int mm, int *m, float *work, int lwork, float *rwork, int lrwork, int *info)
+{
+    trevc3_host<float, true, std::complex<float>>(side, howmny, select, n, T, ldt, VL, ldvl, VR, ldvr, mm, m,
+                                                  reinterpret_cast<std::complex<float> *>(work), lwork, rwork, lrwork,
+                                                  info);
+}
+
+int xtgevc3_dtrevc3_dev(unsigned flags, void *stream, char side, char howmny, const int *select, int n,
+                        const double *T, int ldt, double *VL, int ldvl, double *VR, int ldvr, int mm, int *m, int *info)
+{
+    return trevc3_device<double, false>(flags, stream, side, howmny, select, n, T, ldt, VL, ldvl, VR, ldvr, mm, m,
+                                        info);
+}
+
+int xtgevc3_strevc3_dev(unsigned flags, void *stream, char side, char howmny, const int *select, int n,
+                        const float *T, int ldt, float *VL, int ldvl, float *VR, int ldvr, int mm, int *m, int *info)
+{
+    return trevc3_device<float, false>(flags, stream, side, howmny, select, n, T, ldt, VL, ldvl, VR, ldvr, mm, m,
+                                       info);
+}
+
+int xtgevc3_ztrevc3_dev(unsigned flags, void *stream, char side, char howmny, const int *select, int n,
+                        const double *T, int ldt, double *VL, int ldvl, double *VR, int ldvr, int mm, int *m, int *info)
+{
+    return trevc3_device<double, true>(flags, stream, side, howmny, select, n, T, ldt, VL, ldvl, VR, ldvr, mm, m,
+                                       info);
+}
+
+int xtgevc3_ctrevc3_dev(unsigned flags, void *stream, char side, char howmny, const int *select, int n,
+                        const float *T, int ldt, float *VL, int ldvl, float *VR, int ldvr, int mm, int *m, int *info)
+{
+    return trevc3_device<float, true>(flags, stream, side, howmny, select, n, T, ldt, VL, ldvl, VR, ldvr, mm, m,
+                                      info);
 }
 
 }  // extern "C"

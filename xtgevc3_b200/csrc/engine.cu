@@ -348,6 +348,17 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
     int *d_err = nsplit ? scr.get<int>(1) : nullptr;
     if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
     if (d_err) XTG_CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    // standard problem (xTREVC3): P = I, built here; the solves and the norms read it
+    if (opt.p_identity) {
+        const int ldi = round_up(n, 32);
+        E *Pid = scr.get<E>((size_t)ldi * n);
+        if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
+        XTG_CK(cudaMemsetAsync(Pid, 0, (size_t)ldi * n * sizeof(E), st));
+        identity_diag_kernel<E><<<(n + 255) / 256, 256, 0, st>>>(Pid, ldi, n);
+        XTG_CK(cudaGetLastError());
+        P = Pid;
+        ldp = ldi;
+    }
     if (CPLX) {
         XTG_CK(cudaMemcpyAsync(d_eig, alpha_, 2 * n * sizeof(R), cudaMemcpyHostToDevice, st));
         XTG_CK(cudaMemcpyAsync(d_eig + 2 * n, beta_, 2 * n * sizeof(R), cudaMemcpyHostToDevice, st));
@@ -465,16 +476,19 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         int lsp = lds, lpp = ldp;
         if (left) {
             E *St = scr.get<E>((size_t)ld_n * n);
-            E *Pt = scr.get<E>((size_t)ld_n * n);
+            E *Pt = opt.p_identity ? nullptr : scr.get<E>((size_t)ld_n * n);  // F I^H F = I
             if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
             dim3 g((n + 31) / 32, (n + 31) / 32), b(32, 8);
             tr.run(kTPrep, 0, 2.0 * n * n * esz, st,
                    [&] { rev_transpose_kernel<E><<<g, b, 0, st>>>(S, lds, St, ld_n, n, 1); });
-            tr.run(kTPrep, 0, 2.0 * n * n * esz, st,
-                   [&] { rev_transpose_kernel<E><<<g, b, 0, st>>>(P, ldp, Pt, ld_n, n, 1); });
+            if (Pt) {
+                tr.run(kTPrep, 0, 2.0 * n * n * esz, st,
+                       [&] { rev_transpose_kernel<E><<<g, b, 0, st>>>(P, ldp, Pt, ld_n, n, 1); });
+                Pp = Pt;
+                lpp = ld_n;
+            }
             Sp = St;
-            Pp = Pt;
-            lsp = lpp = ld_n;
+            lsp = ld_n;
         }
         // work items of the diagonal solves: every column that starts an eigenvector
         const std::vector<int> &items = sc.starts;
@@ -482,7 +496,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         // look-ahead (XTGEVC3_LOOKAHEAD): the trailing update of a block pair runs on a second
         // stream while the next pair is solved (see the loop below); off while tracing
         // (clean per-kernel times) and in arena mode (fixed scratch)
-        const bool ahead = opt.lookahead && !tr.on && !opt.arena && blocks.size() >= 3;
+        const bool ahead = opt.lookahead && !tr.on && !opt.arena && !opt.p_identity && blocks.size() >= 3;
         // Without look-ahead, row blocks are taken in groups of `group` (one trailing GEMM
         // with K = 2 x the group's rows); arena mode keeps groups of two, so that its fixed
         // scratch holds the update operand.  Look-ahead takes pairs with padded blocks.
@@ -620,6 +634,8 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             });
         };
         const int nbk = (int)blocks.size();
+        // the P strips of the identity are zero: the standard problem updates with S only
+        const int nstrips = opt.p_identity ? 1 : 2;
         for (int gi = 0; !ahead && gi < nbk; gi += group) {
             const int ge = std::min(nbk, gi + group);  // blocks [gi, ge); blocks[gi] is the lowest
             const int q0 = blocks[ge - 1].first, q1 = blocks[gi].second;
@@ -632,13 +648,13 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
                 if (bi + 1 < ge && c0 < m) {  // rows [q0, r0) (window from an even row)
                     const int w0 = q0 & ~1, mlo = q0 & 1;
                     GemmSeg<E> sg[2] = {strip(Sp, lsp, w0, r0, jnb, ys), strip(Pp, lpp, w0, r0, jnb, kq + ys)};
-                    update(w0, mlo, mlo + (r0 - q0), c0, 2, sg, 2.0 * jnb, st);
+                    update(w0, mlo, mlo + (r0 - q0), c0, nstrips, sg, nstrips * double(jnb), st);
                 }
             }
             const int c0 = first_col(q0);
             if (q0 > 0 && c0 < m) {
                 GemmSeg<E> sg[2] = {strip(Sp, lsp, 0, q0, acols, 0), strip(Pp, lpp, 0, q0, acols, kq)};
-                update(0, 0, q0, c0, 2, sg, 2.0 * acols, st);
+                update(0, 0, q0, c0, nstrips, sg, nstrips * double(acols), st);
             }
             XTG_CK(cudaGetLastError());
         }
@@ -747,6 +763,16 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         }
         // every deferred factor was applied within its own pair (the top block scales at once)
         if (tr_pending) XTG_CK(cudaStreamWaitEvent(st, ev_tr, 0));
+
+        // LAPACK xTREVC3's phase for real 2x2 pairs (before the back-transform, which is linear)
+        if constexpr (!CPLX) {
+            if (opt.lapack_pairs) {
+                lapack_pair_phase_kernel<R><<<(m * 32 + 255) / 256, 256, 0, st>>>(
+                    reinterpret_cast<R *>(X), ldx, m, d_colk, d_kext, d_kind, reinterpret_cast<const R *>(Sp), lsp,
+                    left ? 1 : 0);
+                XTG_CK(cudaGetLastError());
+            }
+        }
 
         // ---- write-back / back-transform -----------------------------------------------------
         E *V = left ? VL : VR;

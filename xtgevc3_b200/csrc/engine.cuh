@@ -13,6 +13,14 @@ struct Options {
     int split = 0;      // > 0: FP64 GEMMs (real double) as slice products with this many slices
     int split_kind = 0; // 0: BF16 slices (kind::f16), 1: INT8 slices (kind::i8)
     int lookahead = 0;  // trailing updates on a second stream, overlapping the next solves
+    // Standard problem (xTREVC3): P is the identity and the caller passes P = nullptr.  The
+    // solver builds it from scratch for the diagonal-block solves and the norms; the update
+    // GEMMs skip its strips (identically zero off the diagonal).
+    int p_identity = 0;
+    // Real 2x2 pairs get LAPACK xTREVC3's phase: the pair's eigenvector is multiplied by the
+    // unit complex number that makes its seed entry real with LAPACK's sign and ratio (one
+    // entry of the 2x2 seed real, the other imaginary), before the back-transform.
+    int lapack_pairs = 0;
     // When set, all device scratch of the call is carved from this buffer (nothing is
     // allocated) and the two sides run one after the other on the caller's stream.
     void *arena = nullptr;

@@ -268,4 +268,60 @@ __global__ void fill_one_kernel(R *p, int m)
     if (i < m) p[i] = R(1);
 }
 
+// Diagonal of the identity (the rest zeroed by the caller): P of the standard problem.
+template <class E>
+__global__ void identity_diag_kernel(E *A, int lda, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) A[(size_t)i * lda + i] = E(1);
+}
+
+// LAPACK xTREVC3's phase of a real 2x2 pair's eigenvector.  LAPACK seeds the pair (rows k,
+// k+1 of T, standardised block, wi = sqrt|T(k,k+1)| sqrt|T(k+1,k)|) with one real and one
+// imaginary entry (reference LAPACK dtrevc3.f, complex right / left eigenvector):
+//   right: x(k) = 1, x(k+1) = i wi/T(k,k+1)   if |T(k,k+1)| >= |T(k+1,k)|,
+//          x(k) = -wi/T(k+1,k), x(k+1) = i     otherwise;
+//   left:  y(k) = wi/T(k,k+1), y(k+1) = i      if |T(k,k+1)| >= |T(k+1,k)|,
+//          y(k) = 1, y(k+1) = -i wi/T(k+1,k)   otherwise,
+// and only ever scales by positive reals after that.  One warp per pair (Re column c, Im
+// column c + 1 of X in problem orientation, rows colk[c], colk[c] + 1; the left problem is
+// reversed, so original row k is problem row colk[c] + 1 there) multiplies the pair by the
+// unit complex number that gives its entry at the real seed row LAPACK's sign (the other
+// seed row when that entry underflowed; a pair with neither is left alone).  Sp: S in
+// problem orientation, where Sp(kk, kk+1) = T(k, k+1) and Sp(kk+1, kk) = T(k+1, k) for
+// both sides.
+template <class R>
+__global__ void lapack_pair_phase_kernel(R *X, int ldx, int m, const int *colk, const int *kext,
+                                         const uint8_t *kind, const R *Sp, int lds, int left)
+{
+    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (c >= m || kind[c] != kPairRe) return;  // uniform per warp
+    const int kk = colk[c];
+    R *xr = X + (size_t)c * ldx, *xi = xr + ldx;
+    const R a = Sp[kk + (size_t)(kk + 1) * lds], b = Sp[kk + 1 + (size_t)kk * lds];
+    const bool up = fabs(a) >= fabs(b);
+    const R wi = sqrt(fabs(a)) * sqrt(fabs(b));
+    const int rr = left ? kk + 1 : kk, ri = left ? kk : kk + 1;       // real / imaginary seed rows
+    const R tr = left ? (up ? wi / a : R(1)) : (up ? R(1) : -wi / b);  // x(real row) = tr
+    const R ti = left ? (up ? R(1) : -wi / b) : (up ? wi / a : R(1));  // x(imaginary row) = i ti
+    R cr, ci;  // unit factor: sign(t) conj(x) / |x| at the real row, sign(t) i conj(x) / |x| at the other
+    const R x0r = xr[rr], x0i = xi[rr], x0 = hypot(x0r, x0i);
+    if (x0 > R(0)) {
+        const R sg = tr < R(0) ? R(-1) : R(1);
+        cr = sg * x0r / x0;
+        ci = -sg * x0i / x0;
+    } else {
+        const R x1r = xr[ri], x1i = xi[ri], x1 = hypot(x1r, x1i);
+        if (!(x1 > R(0))) return;
+        const R sg = ti < R(0) ? R(-1) : R(1);
+        cr = sg * x1i / x1;
+        ci = sg * x1r / x1;
+    }
+    for (int i = lane; i < kext[c]; i += 32) {
+        const R u = xr[i], v = xi[i];
+        xr[i] = cr * u - ci * v;
+        xi[i] = cr * v + ci * u;
+    }
+}
+
 }  // namespace xtg
