@@ -60,6 +60,7 @@ def parse():
     ap.add_argument("--adjoint-c-count", type=int, default=256, help="complex64 pencils of the ctgevc3 adjoint case")
     ap.add_argument("--adjoint-c-n", type=int, default=128)
     ap.add_argument("--z-n", type=int, default=4096, help="order of the ztgevc3 SIDE=R HOWMNY=A leg (0 skips)")
+    ap.add_argument("--trevc3-n", type=int, default=8192, help="order of the dtrevc3 SIDE=B HOWMNY=B leg (0 skips)")
     ap.add_argument("--profile-case", default=None,
                     help="run one small case for an ncu capture and exit (no JSON line): plain:N (two dtgevc3 "
                          "B/B calls, FP64), split_i8:N (the same, INT8 split form), batch:COUNT (two launches "
@@ -607,6 +608,115 @@ def measure_ztgevc3(args, X, torch):
                     "graded: rows of P scaled by 10^U(-8,8)", **out}
 
 
+def schur_stand_in(n, seed):
+    """Stand-in for the real Schur factor T of an n x n iid N(0,1) matrix (host, Fortran):
+    strictly upper part N(0,1); about sqrt(2n/pi) real eigenvalues, uniform on [-sqrt(n),
+    sqrt(n)], and the rest complex pairs uniform in the disk of radius sqrt(n) (the circular
+    law), in random order; each pair a LAPACK-standardised block [[a, b], [c, a]] with
+    b c = -w^2 and |b| / |c| = exp(2 N(0,1)), so both of LAPACK xTREVC3's seed branches occur.
+    xGEES of an 8192 matrix takes minutes on the host, hence the stand-in.  Returns (T,
+    eigenvalue real parts, imaginary parts)."""
+    rng = np.random.default_rng(seed)
+    T = np.triu(rng.standard_normal((n, n)), 1)
+    nreal = int(round(np.sqrt(2 * n / np.pi)))
+    nreal += (n - nreal) % 2
+    kinds = np.array([0] * nreal + [1] * ((n - nreal) // 2))
+    rng.shuffle(kinds)
+    wr, wi = np.zeros(n), np.zeros(n)
+    r, k = np.sqrt(n), 0
+    for kd in kinds:
+        if kd == 0:
+            wr[k] = rng.uniform(-r, r)
+            T[k, k] = wr[k]
+            k += 1
+        else:
+            rad, th = r * np.sqrt(rng.random()), rng.uniform(0, np.pi)
+            a, w = rad * np.cos(th), rad * np.sin(th)
+            t = np.exp(rng.standard_normal())
+            T[k, k] = T[k + 1, k + 1] = a
+            T[k, k + 1], T[k + 1, k] = w * t, -w / t
+            wr[k] = wr[k + 1] = a
+            wi[k], wi[k + 1] = w, -w
+            k += 2
+    return np.asfortranarray(T), wr, wi
+
+
+def measure_trevc3(args, X, torch):
+    """dtrevc3 (the standard problem, P = I) SIDE='B', HOWMNY='B' at n = --trevc3-n on the
+    Schur-factor stand-in, device-resident, CUDA-event timing; residuals of both sides
+    against A = Q T Q^T on the device; LAPACK dtrevc3 (SciPy's OpenBLAS, all host threads)
+    on the same kind of input at n = 2048, beside this library at that size."""
+    n = args.trevc3_n
+    out = {"n": n, "side": "B", "howmny": "B"}
+
+    def run(nn, seed, steps, warm):
+        T_h, wr, wi = schur_stand_in(nn, seed)
+        T = colmajor_cuda(T_h, torch)
+        Q = orthogonal(nn, seed + 1, torch)
+        VL, VR = torch.empty_like(Q), torch.empty_like(Q)
+        ts = []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for it in range(warm + steps):
+            VL.copy_(Q)
+            VR.copy_(Q)
+            torch.cuda.synchronize()
+            e0.record()
+            X.trevc3_dev("B", "B", T, VL=VL, VR=VR)
+            e1.record()
+            torch.cuda.synchronize()
+            if it >= warm:
+                ts.append(e0.elapsed_time(e1))
+        return T_h, wr, wi, T, Q, VL, VR, float(np.mean(ts))
+
+    T_h, wr, wi, T, Q, VL, VR, ms = run(n, args.seed + 31, args.steps, max(args.warmup, 1))
+    A = Q @ T @ Q.t()
+    # columns of a pair (a +- i w): Re col j, Im col j+1; partner index and coupling per column
+    part = np.arange(n)
+    cpl = np.zeros(n)
+    k = 0
+    while k < n:
+        if wi[k] != 0:
+            part[k], part[k + 1] = k + 1, k
+            cpl[k], cpl[k + 1] = wi[k], -wi[k]
+            k += 2
+        else:
+            k += 1
+    a_t = torch.as_tensor(wr, device="cuda")
+    c_t = torch.as_tensor(cpl, device="cuda")
+    p_t = torch.as_tensor(part, device="cuda")
+    nA = A.abs().sum(0).max()
+    resid = {}
+    for side, V, M, sg in (("R", VR, A, 1.0), ("L", VL, A.t(), -1.0)):
+        R = M @ V - V * a_t[None, :] + sg * V[:, p_t] * c_t[None, :]
+        den = nA * (V.abs().sum(0) + (c_t != 0) * V[:, p_t].abs().sum(0))
+        resid[side] = float((R.abs().sum(0) / den).max())
+        del R
+    out.update({"ms": ms, "eigvecs_per_s": 2 * n / (ms * 1e-3),
+                "algorithmic_flops": 2 * (n ** 3 / 3 + n ** 3), "tflops": 2 * (n ** 3 / 3 + n ** 3) / (ms * 1e-3) / 1e12,
+                "resid_max_right": resid["R"], "resid_max_left": resid["L"],
+                "finite": bool(torch.isfinite(VL).all() and torch.isfinite(VR).all()),
+                "data": "stand-in real Schur factor (circular-law eigenvalues, N(0,1) strictly upper part, "
+                        "LAPACK-standardised 2x2 blocks), Q from the QR of a Gaussian matrix",
+                "resid": "max_c ||A v - lambda v||_1 / (||A||_1 ||v||_1), A = Q T Q^T (left: A^T, conj lambda)"})
+    del A, T, Q, VL, VR
+    if not args.no_cpu:
+        import oracle
+        nc = 2048
+        T_h, _, _, _, Qc, _, _, msg = run(nc, args.seed + 32, 3, 1)
+        Qh = Qc.cpu().numpy()
+        thr = host_threads()
+        if oracle.ref_available():
+            oracle.set_ref_threads(thr)  # the same OpenBLAS instance as the LAPACK oracle
+        t0 = time.perf_counter()
+        _, _, mc, info = oracle.lapack_trevc3("B", "B", T_h, VL=Qh, VR=Qh)
+        tc = time.perf_counter() - t0
+        out["cpu_lapack_n2048"] = {"value": 2 * nc / tc, "unit": "eigvecs/s", "seconds": tc, "cores": thr,
+                                   "info": info, "gpu_ms_same_n": msg,
+                                   "gpu_eigvecs_per_s_same_n": 2 * nc / (msg * 1e-3),
+                                   "kind": "LAPACK dtrevc3 (SciPy OpenBLAS), one call"}
+    return out
+
+
 def profile_case(args):
     """Small, fixed workloads for ncu captures (profiles/*.md name the exact command)."""
     import torch
@@ -773,6 +883,7 @@ def main():
     batched = measure_batched(args, X, torch, dist, world) if args.batch_count > 0 else None
     adjoint = measure_adjoint(args, X, torch) if args.adjoint_n > 0 and rank == 0 else None
     zleg = measure_ztgevc3(args, X, torch) if args.z_n > 0 and rank == 0 else None
+    trleg = measure_trevc3(args, X, torch) if args.trevc3_n > 0 and rank == 0 else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -804,7 +915,7 @@ def main():
                            "resid_max": h["resid"], "resid_bound": 1e-12},
                 "forms": forms_out, "clocks": h["clocks"], "e2e": e2e, "gpu_launches": h["launches"],
                 "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "batched": batched,
-                "adjoint": adjoint, "ztgevc3": zleg}
+                "adjoint": adjoint, "ztgevc3": zleg, "dtrevc3": trleg}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
