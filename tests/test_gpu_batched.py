@@ -172,3 +172,44 @@ def test_batched_tuner_sets_default(cuda_ok):
             check(h, d, "B", "B")
     finally:
         X.batched_set_default("d", old)
+
+
+def test_batched_fp32_graded_pencils_stay_finite(cuda_ok):
+    """FP32 batch of random quasi-triangular pencils of order 401-512 with the rows of P
+    graded by 10^U(-8,8) (a 2x2 block's rows share one factor): consecutive rows can differ
+    by 1e16, beyond what float's range allows between two overflow checks, so blocks whose
+    substitution passes the per-row cap are solved again with it.  Every column must be
+    finite with a DGET52-style residual below 100 (in single-precision eps)."""
+    import torch
+    dt = np.float32
+    hp, db = [], []
+    for i, n in enumerate((512, 475, 438, 401)):
+        S, P, ar, ai, be = pencils.gen_quasi_triangular(n, 900 + i, dtype=dt)
+        g = 10.0 ** np.random.default_rng(901 + i).uniform(-8, 8, n)
+        k = 0
+        while k < n:
+            if ai[k] != 0 and k + 1 < n:
+                g[k + 1] = g[k]
+                k += 2
+            else:
+                k += 1
+        P = np.asfortranarray((g[:, None] * P).astype(dt))
+        be = np.diag(P).copy()
+        hp.append(dict(n=n, S=S, P=P, ar=ar, ai=ai, be=be))
+        db.append(dict(S=dev(S), P=dev(P), alphar=torch.from_numpy(ar).cuda(), alphai=torch.from_numpy(ai).cuda(),
+                       beta=torch.from_numpy(be).cuda(), VL=dev(np.full((n, n), np.nan, dtype=dt)),
+                       VR=dev(np.full((n, n), np.nan, dtype=dt))))
+    b = X.Batch("B", "A", db)
+    b.run()
+    b.wait()
+    torch.cuda.synchronize()
+    scale = np.finfo(np.float64).eps / np.finfo(np.float32).eps
+    for h, d in zip(hp, db):
+        a_c, b_c = oracle.column_eigenvalues(h["ar"], h["be"], alphai=h["ai"])
+        for side, key in (("R", "VR"), ("L", "VL")):
+            V = d[key].t().cpu().numpy().T
+            assert np.isfinite(V).all(), (h["n"], side)
+            r = oracle.residual_ratio(h["S"], h["P"], oracle.to_complex_real_storage(V, h["ai"]), a_c, b_c,
+                                      left=side == "L") * scale
+            assert r.max() < 100, (h["n"], side, r.max())
+    b.close()

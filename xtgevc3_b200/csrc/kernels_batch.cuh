@@ -398,17 +398,27 @@ __device__ void solve_item(const TileCols<T, NT> &tc, int j, int r0, int r1, con
         }
         Factors<T> F;
         factor_rows(F, sec, nrows, lane, smin, W);
+        // The substitution runs without the per-row cap (in the loop it costs this kernel its
+        // second CTA per SM); a block in which a component passed the cap, or overflowed, is
+        // solved again from its right-hand side with it.  Factors applied to the stored rows
+        // in the first pass (acc) carry over; a non-finite maximum is left to the second.
+        const T cap = limits<T>::big / T(4096);
+        const T r_in[2] = {r[0], r[1]};
+        T acc = T(1);
         auto rescale = [&](T (&rr)[2], T sc) {  // the whole column, by sc
-            rr[0] *= sc; rr[1] *= sc; seed *= sc;
+            rr[0] *= sc; rr[1] *= sc; seed *= sc; acc *= sc;
             if (!diag) { scale_col(colr, XLD, 0, r0, sc, lane); scale_col(colr, XLD, r1, top + 1, sc, lane); }
         };
         auto mid = [&](T (&rr)[2], int jtop) {
             const T mx = warp_max(lane <= jtop ? fabs(rr[0]) : T(0));
-            if (mx > thr_rhs) rescale(rr, thr_rhs / mx);
+            if (mx > thr_rhs && mx <= limits<T>::big) rescale(rr, thr_rhs / mx);
         };
-        // block and mid-block checks, no per-row cap: with it this kernel needs more than
-        // the 128 registers that leave room for a second CTA per SM
-        back_substitute_loop(r, F, sec, nrows, lane, W, 0, make_guard<false>(limits<T>::big / T(4096), thr_rhs, mid, rescale));
+        back_substitute_loop(r, F, sec, nrows, lane, W, 0, make_guard<false>(cap, thr_rhs, mid, rescale));
+        if (__any_sync(0xffffffffu, !(fabs(r[0]) <= cap) || !(fabs(r[1]) <= cap))) {
+            r[0] = acc * r_in[0];
+            r[1] = acc * r_in[1];
+            back_substitute_loop(r, F, sec, nrows, lane, W, 0, make_guard<true>(cap, thr_rhs, mid, rescale));
+        }
         T x[2];
 #pragma unroll
         for (int s = 0; s < 2; s++) {
@@ -473,8 +483,11 @@ __device__ void solve_item(const TileCols<T, NT> &tc, int j, int r0, int r1, con
         }
         Factors<C> F;
         factor_rows(F, sec, nrows, lane, smin, W);
+        const T cap = limits<T>::big / T(4096);  // detect and redo, as for a real column
+        const C r_in[2] = {r[0], r[1]};
+        T acc = T(1);
         auto rescale = [&](C (&rr)[2], T sc) {  // the whole column pair, by sc
-            rr[0] = sc * rr[0]; rr[1] = sc * rr[1]; seed0 = sc * seed0; seed1 = sc * seed1;
+            rr[0] = sc * rr[0]; rr[1] = sc * rr[1]; seed0 = sc * seed0; seed1 = sc * seed1; acc *= sc;
             if (!diag) {
                 scale_col(colr, XLD, 0, r0, sc, lane); scale_col(colr, XLD, r1, top + 1, sc, lane);
                 scale_col(coli, XLD, 0, r0, sc, lane); scale_col(coli, XLD, r1, top + 1, sc, lane);
@@ -482,9 +495,14 @@ __device__ void solve_item(const TileCols<T, NT> &tc, int j, int r0, int r1, con
         };
         auto mid = [&](C (&rr)[2], int jtop) {
             const T mx = warp_max(lane <= jtop ? fmax(fabs(rr[0].x), fabs(rr[0].y)) : T(0));
-            if (mx > thr_rhs) rescale(rr, thr_rhs / mx);
+            if (mx > thr_rhs && mx <= limits<T>::big) rescale(rr, thr_rhs / mx);
         };
-        back_substitute_loop(r, F, sec, nrows, lane, W, 0, make_guard<false>(limits<T>::big / T(4096), thr_rhs, mid, rescale));
+        back_substitute_loop(r, F, sec, nrows, lane, W, 0, make_guard<false>(cap, thr_rhs, mid, rescale));
+        if (__any_sync(0xffffffffu, !(mag(r[0]) <= cap) || !(mag(r[1]) <= cap))) {
+            r[0] = acc * r_in[0];
+            r[1] = acc * r_in[1];
+            back_substitute_loop(r, F, sec, nrows, lane, W, 0, make_guard<true>(cap, thr_rhs, mid, rescale));
+        }
         C x[2];
 #pragma unroll
         for (int s = 0; s < 2; s++) {
@@ -1159,8 +1177,11 @@ __device__ void compute_unit(const Args<T> &a, int p, int side, int t, unsigned 
 }
 
 // ---- the persistent kernel ---------------------------------------------------------------
+// FP32 with 16-column tiles is held to the 128 registers that fit two CTAs per SM (its
+// shared memory allows two; the rarely taken capped re-solve would otherwise set the count).
 template <class T, int NT, int H>
-__global__ void __launch_bounds__(THREADS, 1) batch_kernel(Args<T> a)
+__global__ void __launch_bounds__(THREADS, (std::is_same<T, float>::value && NT == 16) ? 2 : 1)
+    batch_kernel(Args<T> a)
 {
     extern __shared__ __align__(16) unsigned char smem_batch[];
     __shared__ TileCols<T, NT> tc;
