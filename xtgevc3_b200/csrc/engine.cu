@@ -374,6 +374,20 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
     tr.run(kTPrep, 0, 2.0 * n * sizeof(R), st, [&] { colmax_kernel<R><<<1, 1024, 0, st>>>(d_sums, n, d_norms); });
     XTG_CK(cudaGetLastError());
 
+    // diagonal-solve launches: one warp per eigenvector, as many CTAs as stay resident
+    const int diag_threads = CPLX ? kDiagThreadsCplx : 256, diag_warps = diag_threads / 32;
+    int diag_ctas = 2 * 148;
+    {
+        int nsm = 0, occ = 0;
+        const size_t dsm = 2 * kBlock * kSmLd * sizeof(E);
+        cudaError_t e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) {
+            if constexpr (CPLX) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, diag_solve_cplx<R>, diag_threads, dsm);
+            else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, diag_solve_real<R>, diag_threads, dsm);
+        }
+        if (e == cudaSuccess && nsm > 0 && occ > 0) diag_ctas = nsm * occ;
+        XTG_CK(cudaGetLastError());
+    }
     const R safemin = limits<R>::safemin, eps = limits<R>::eps;
     const R bignum = R(1) / (safemin / eps);
     const int ld_n = round_up(n, 32);
@@ -615,7 +629,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             da.left_seed = left ? 1 : 0;
             da.pending = safe_lo >= 0 ? pending : nullptr;
             da.safe_lo = safe_lo;
-            const int grid = std::max(1, std::min((nitems - da.it0 + 7) / 8, 2 * 148));
+            const int grid = std::max(1, std::min((nitems - da.it0 + diag_warps - 1) / diag_warps, diag_ctas));
             // algorithmic work of the shifted solves: ~2 nrows^2 real flops per real column,
             // 4x that per complex column or (Re, Im) pair; bytes: rhs in, solution and
             // update operand out, the S/P block once
@@ -629,8 +643,8 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
                 dby += cols * (double(nr < jnb ? 0 : jnb) + jnb + 2.0 * bpad) * esz;
             }
             tr.run(kTDiag, dfl, dby, st, [&] {
-                if constexpr (CPLX) diag_solve_cplx<R><<<grid, 256, diag_smem, st>>>(da);
-                else diag_solve_real<R><<<grid, 256, diag_smem, st>>>(da);
+                if constexpr (CPLX) diag_solve_cplx<R><<<grid, diag_threads, diag_smem, st>>>(da);
+                else diag_solve_real<R><<<grid, diag_threads, diag_smem, st>>>(da);
             });
         };
         const int nbk = (int)blocks.size();

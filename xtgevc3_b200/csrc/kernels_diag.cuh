@@ -642,8 +642,11 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
 // ------------------------------------------------------------------------------------
 // Complex arithmetic (c/z): S triangular, one complex column per eigenvalue
 // ------------------------------------------------------------------------------------
+// 16 warps per CTA: in double complex the S/P block (133 KB) allows one CTA per SM, so a
+// larger CTA is how more eigenvectors share the block and hide the solves' latency
+constexpr int kDiagThreadsCplx = 512;
 template <class R>
-__global__ void __launch_bounds__(256) diag_solve_cplx(DiagArgs<R> a)
+__global__ void __launch_bounds__(kDiagThreadsCplx, 1) diag_solve_cplx(DiagArgs<R> a)
 {
     using C = cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_diag[];
