@@ -101,3 +101,29 @@ def test_trevc3_large_real_schur_matches_lapack(cuda_ok):
     assert (m, info) == (rm, 0)
     assert _raw_err(VR, rR) < 1e-10
     assert _raw_err(VL, rL) < 1e-10
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 64, 65])
+@pytest.mark.parametrize("dt", [np.float64, np.complex128], ids=["d", "z"])
+def test_trevc3_small_and_block_boundary_orders(cuda_ok, dt, n):
+    """Orders 1-3 (a real 2x2 block can be the whole matrix) and the 64-row block boundary,
+    both sides, back-transformed, against LAPACK without normalisation."""
+    found = None
+    for seed in range(40):  # for n = 2 real, a seed whose Schur form is one 2x2 block
+        T, Q = _schur(dt, n, seed)
+        if dt != np.float64 or n != 2 or T[1, 0] != 0:
+            found = (T, Q)
+            break
+    T, Q = found
+    rL, rR, rm, _ = oracle.lapack_trevc3("B", "B", T, VL=Q, VR=Q)
+    VL, VR, m, info = X.trevc3("B", "B", T, VL=Q.copy(order="F"), VR=Q.copy(order="F"))
+    assert (m, info) == (rm, 0)
+    assert _raw_err(VR, rR) < 1e-11 and _raw_err(VL, rL) < 1e-11
+
+
+def test_trevc3_empty_selection(cuda_ok):
+    """HOWMNY='S' with nothing selected: M = 0, INFO = 0, outputs untouched."""
+    T, Q = _schur(np.float64, 50, 2)
+    VR = np.full((50, 4), 7.0, order="F")
+    _, VR2, m, info = X.trevc3("R", "S", T, VR=VR, select=np.zeros(50, dtype=np.int32), mm=4)
+    assert (m, info) == (0, 0) and (VR2 == 7.0).all()
