@@ -153,6 +153,43 @@ int xtgevc3_ztrevc3_dev(unsigned flags, void *stream, char side, char howmny, co
 int xtgevc3_ctrevc3_dev(unsigned flags, void *stream, char side, char howmny, const int *select, int n,
                         const float *T, int ldt, float *VL, int ldvl, float *VR, int ldvr, int mm, int *m, int *info);
 
+/* ---- eigenvalue condition numbers: xTGSNA, JOB = 'E' (no counterpart upstream) --------
+ * Reciprocal condition numbers S(k) = sqrt(|y^H A x|^2 + |y^H B x|^2) / (||x|| ||y||) of
+ * the selected eigenvalues of a generalized Schur pencil (A, B) (quasi-triangular A,
+ * triangular B) from its left and right eigenvectors VL, VR in Schur coordinates (as
+ * xtgevc3_*tgevc3 return them with HOWMNY 'A' or 'S'), with LAPACK xTGSNA's arguments,
+ * INFO codes and results; a real pair (A(k+1,k) != 0) gets one S for both columns; S = -1
+ * where the numerator is zero (not for a pair, as in LAPACK).  Only JOB = 'E' is
+ * computed: JOB = 'V' or 'B' (DIF) returns INFO = -1 with a message in
+ * xtgevc3_last_error(); DIF and IWORK are not referenced; WORK is not used (the query,
+ * LWORK = -1, answers max(1, n)).  INFO: -1 JOB, -2 HOWMNY, -4 N, -6 LDA, -8 LDB,
+ * -10 LDVL, -12 LDVR, -15 MM < M, -18 LWORK, 1 a CUDA failure.  Complex arrays
+ * interleaved (S real).  Device forms: A, B, VL, VR and S device pointers.              */
+void xtgevc3_dtgsna(char job, char howmny, const int *select, int n, const double *A, int lda, const double *B,
+                    int ldb, const double *VL, int ldvl, const double *VR, int ldvr, double *s, double *dif, int mm,
+                    int *m, double *work, int lwork, int *iwork, int *info);
+void xtgevc3_stgsna(char job, char howmny, const int *select, int n, const float *A, int lda, const float *B, int ldb,
+                    const float *VL, int ldvl, const float *VR, int ldvr, float *s, float *dif, int mm, int *m,
+                    float *work, int lwork, int *iwork, int *info);
+void xtgevc3_ztgsna(char job, char howmny, const int *select, int n, const double *A, int lda, const double *B,
+                    int ldb, const double *VL, int ldvl, const double *VR, int ldvr, double *s, double *dif, int mm,
+                    int *m, double *work, int lwork, int *iwork, int *info);
+void xtgevc3_ctgsna(char job, char howmny, const int *select, int n, const float *A, int lda, const float *B, int ldb,
+                    const float *VL, int ldvl, const float *VR, int ldvr, float *s, float *dif, int mm, int *m,
+                    float *work, int lwork, int *iwork, int *info);
+int xtgevc3_dtgsna_dev(void *stream, char job, char howmny, const int *select, int n, const double *A, int lda,
+                       const double *B, int ldb, const double *VL, int ldvl, const double *VR, int ldvr, double *s,
+                       int mm, int *m, int *info);
+int xtgevc3_stgsna_dev(void *stream, char job, char howmny, const int *select, int n, const float *A, int lda,
+                       const float *B, int ldb, const float *VL, int ldvl, const float *VR, int ldvr, float *s, int mm,
+                       int *m, int *info);
+int xtgevc3_ztgsna_dev(void *stream, char job, char howmny, const int *select, int n, const double *A, int lda,
+                       const double *B, int ldb, const double *VL, int ldvl, const double *VR, int ldvr, double *s,
+                       int mm, int *m, int *info);
+int xtgevc3_ctgsna_dev(void *stream, char job, char howmny, const int *select, int n, const float *A, int lda,
+                       const float *B, int ldb, const float *VL, int ldvl, const float *VR, int ldvr, float *s, int mm,
+                       int *m, int *info);
+
 /* ---- allocation-free device entry point (no counterpart in the upstream library) -----
  * Same computation and arguments as xtgevc3_dtgevc3_dev (without flags), for callers that
  * cannot allocate device memory at this point: e.g. a framework that has reserved the

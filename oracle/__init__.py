@@ -211,6 +211,32 @@ def lapack_trevc3(side, howmny, T, VL=None, VR=None, select=None, mm=None):
     return VL, VR, m.value, info.value
 
 
+def lapack_tgsna(howmny, A, B, VL, VR, select=None):
+    """Oracle of the xTGSNA entry points: LAPACK xTGSNA (JOB = 'E') from SciPy's bundled
+    OpenBLAS.  Returns (S, m, info)."""
+    dt = A.dtype.type
+    pfx = _PREFIX[dt]
+    n = A.shape[0]
+    f = getattr(_openblas(), f"scipy_{pfx}tgsna_")
+    A, B = np.asfortranarray(A), np.asfortranarray(B)
+    VL, VR = np.asfortranarray(VL), np.asfortranarray(VR)
+    rdt = np.float64 if pfx in "dz" else np.float32
+    mm = VR.shape[1]
+    sel = np.zeros(max(n, 1), dtype=np.int32) if select is None else np.ascontiguousarray(select, dtype=np.int32).copy()
+    S = np.zeros(max(mm, 1), dtype=rdt)
+    D = np.zeros(max(mm, 1), dtype=rdt)
+    iv = lambda v: ct.byref(ct.c_int(v))  # noqa: E731
+    m, info = ct.c_int(0), ct.c_int(0)
+    lwork = max(n, 1)
+    work = np.zeros(lwork, dtype=dt)
+    iwork = np.zeros(n + 6, dtype=np.int32)
+    ld = max(n, 1)
+    f(ct.c_char_p(b"E"), ct.c_char_p(howmny.encode()), _ptr(sel), iv(n), _ptr(A), iv(ld), _ptr(B), iv(ld), _ptr(VL),
+      iv(ld), _ptr(VR), iv(ld), _ptr(S), _ptr(D), iv(mm), ct.byref(m), _ptr(work), iv(lwork), _ptr(iwork),
+      ct.byref(info), ct.c_size_t(1), ct.c_size_t(1))
+    return S[:m.value], m.value, info.value
+
+
 def schur_real(n, seed, dtype=np.float64):
     """Real Schur form of an iid N(0,1) matrix (LAPACK xGEES through SciPy: T quasi-upper
     triangular with standardised 2x2 blocks, Q orthogonal)."""

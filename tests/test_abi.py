@@ -235,3 +235,33 @@ def test_trevc3_info_codes_and_query(pfx):
     sel[[1, 4]] = 1
     info, m, _ = call(howmny=b"S", sel=sel.ctypes.data, lwork=-1)
     assert (info, m) == (0, 2)
+
+
+def test_tgsna_info_codes_and_query():
+    """xtgevc3_dtgsna: LAPACK xTGSNA's INFO codes in its order, answered before any CUDA
+    call; JOB = 'V' / 'B' (DIF, not implemented) returns -1 with a message."""
+    n = 5
+    A = np.asfortranarray(np.triu(np.arange(1.0, n * n + 1).reshape(n, n)))
+    V = np.zeros((n, n), order="F")
+    L = X.lib()
+
+    def call(job=b"E", howmny=b"A", nn=n, lda=n, ldb=n, ldvl=n, ldvr=n, mm=n, lwork=n, sel=None):
+        m, info = ct.c_int(-7), ct.c_int(0)
+        s = np.zeros(n)
+        work = np.zeros(n)
+        L.xtgevc3_dtgsna(job, howmny, sel, nn, A.ctypes.data, lda, A.ctypes.data, ldb, V.ctypes.data, ldvl,
+                         V.ctypes.data, ldvr, s.ctypes.data, None, mm, ct.byref(m), work.ctypes.data, lwork, None,
+                         ct.byref(info))
+        return info.value, m.value, work
+    assert call(job=b"X")[0] == -1
+    assert call(job=b"V")[0] == -1 and "JOB='E'" in X.last_error()
+    assert call(howmny=b"B")[0] == -2
+    assert call(nn=-1)[0] == -4
+    assert call(lda=n - 1)[0] == -6
+    assert call(ldb=n - 1)[0] == -8
+    assert call(ldvl=n - 1)[0] == -10
+    assert call(ldvr=n - 1)[0] == -12
+    assert call(mm=n - 1)[:2] == (-15, n)
+    assert call(lwork=0)[0] == -18
+    info, m, work = call(lwork=-1)
+    assert (info, m, int(work[0])) == (0, n, n)

@@ -75,6 +75,13 @@ def lib():
             f = getattr(L, f"xtgevc3_{p}trevc3")
             f.argtypes = [_C, _C, _P, _I, _P, _I, _P, _I, _P, _I, _I, _P, _P, _I, _P, _I, _P]
             f.restype = None
+        for p in "dszc":  # xTGSNA (JOB = 'E')
+            f = getattr(L, f"xtgevc3_{p}tgsna")
+            f.argtypes = [_C, _C, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _P, _I, _P, _P, _I, _P, _P]
+            f.restype = None
+            f = getattr(L, f"xtgevc3_{p}tgsna_dev")
+            f.argtypes = [_P, _C, _C, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _P]
+            f.restype = _I
         for p in "dszc":
             f = getattr(L, f"xtgevc3_{p}trevc3_dev")
             f.argtypes = [_U, _P, _C, _C, _P, _I, _P, _I, _P, _I, _P, _I, _I, _P, _P]
@@ -322,6 +329,31 @@ def trevc3_dev(side, howmny, T, VL=None, VR=None, select=None, flags=0, stream=N
     if rc != 0:
         raise RuntimeError(f"xtgevc3_{pfx}trevc3_dev failed: {last_error()}")
     return m.value, info.value
+
+
+def tgsna(howmny, A, B, VL, VR, select=None, job="E"):
+    """Host-array form of s/d/c/ztgsna with JOB = 'E': reciprocal condition numbers of the
+    selected eigenvalues of the Schur pencil (A, B) from its eigenvectors VL, VR (Schur
+    coordinates, as tgevc3 returns them with HOWMNY 'A' or 'S').  Returns (S, m, info)."""
+    L = lib()
+    dt = A.dtype.type
+    pfx = _PFX[dt]
+    n = A.shape[0]
+    A, B = np.asfortranarray(A), np.asfortranarray(B)
+    VL, VR = np.asfortranarray(VL), np.asfortranarray(VR)
+    rdt = np.float64 if pfx in "dz" else np.float32
+    mm = VR.shape[1]
+    sel = None if select is None else np.ascontiguousarray(select, dtype=np.int32)
+    S = np.zeros(max(mm, 1), dtype=rdt)
+    m, info = ct.c_int(0), ct.c_int(0)
+    work = np.zeros(max(n, 1), dtype=dt)
+    ld = max(n, 1)
+    getattr(L, f"xtgevc3_{pfx}tgsna")(job.encode(), howmny.encode(), _ptr(sel), n, _ptr(A), ld, _ptr(B), ld, _ptr(VL),
+                                      max(VL.shape[0], 1), _ptr(VR), max(VR.shape[0], 1), _ptr(S), None, mm,
+                                      ct.byref(m), _ptr(work), max(n, 1), None, ct.byref(info))
+    if info.value > 0:
+        raise RuntimeError(f"xtgevc3_{pfx}tgsna failed: {last_error()}")
+    return S[:m.value], m.value, info.value
 
 
 # ---- batched form ------------------------------------------------------------------------

@@ -9,7 +9,9 @@
 #include <algorithm>
 #include <atomic>
 #include <cctype>
+#include <climits>
 #include <cmath>
+#include <cstdint>
 #include <complex>
 #include <cstring>
 #include <vector>
@@ -401,6 +403,167 @@ int trevc3_device(unsigned flags, void *stream, char side, char howmny, const in
     return rc;
 }
 
+// ---- eigenvalue condition numbers: xTGSNA, JOB = 'E' ----------------------------------------
+// LAPACK xTGSNA's arguments and INFO order; only JOB = 'E' (S, from the eigenvectors) is
+// computed: JOB = 'V' / 'B' (DIF, which needs eigenvalue reordering and generalized
+// Sylvester solves) returns INFO = -1 with a message.  A real pair is A(k+1, k) != 0.
+// argument checks that need no data, in LAPACK's order
+inline int tgsna_check(char job, char howmny, int n, int lda, int ldb, int ldvl, int ldvr)
+{
+    if (job != 'E' && job != 'V' && job != 'B') return -1;
+    if (job != 'E') {
+        xtg::set_last_error("xTGSNA: only JOB='E' (eigenvalue condition numbers) is implemented");
+        return -1;
+    }
+    if (howmny != 'A' && howmny != 'S') return -2;
+    if (n < 0) return -4;
+    if (lda < std::max(1, n)) return -6;
+    if (ldb < std::max(1, n)) return -8;
+    if (ldvl < n) return -10;
+    if (ldvr < n) return -12;
+    return 0;
+}
+
+// M and the eigenvalue list (sub: A's subdiagonal, n - 1 entries, real pencils); -15 if MM < M
+template <class R, bool CPLX>
+int tgsna_plan(char howmny, const int *select, int n, int mm, const std::vector<R> &sub, int *m,
+               std::vector<int> &items, std::vector<uint8_t> &kinds)
+{
+    int ks = 0;
+    for (int k = 0; k < n;) {
+        const bool pair = !CPLX && k + 1 < n && sub[k] != R(0);
+        const bool sel = howmny == 'A' || (select && (select[k] != 0 || (pair && select[k + 1] != 0)));
+        if (sel) {
+            items.push_back(ks);
+            kinds.push_back(CPLX ? 2 : (pair ? 1 : 0));
+            ks += pair ? 2 : 1;
+        }
+        k += pair ? 2 : 1;
+    }
+    if (m) *m = ks;
+    if (mm < ks) return -15;
+    return 0;
+}
+
+template <class R, bool CPLX>
+int tgsna_subdiag(const void *A, int lda, int n, bool on_device, cudaStream_t st, std::vector<R> &sub)
+{
+    sub.assign(std::max(0, n - 1), R(0));
+    if (CPLX || n < 2) return 0;
+    const R *a = static_cast<const R *>(A);
+    if (!on_device) {
+        for (int k = 0; k + 1 < n; k++) sub[k] = a[(size_t)k * (lda + 1) + 1];
+        return 0;
+    }
+    cudaError_t e = cudaMemcpy2DAsync(sub.data(), sizeof(R), a + 1, (size_t)(lda + 1) * sizeof(R), sizeof(R), n - 1,
+                                      cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        xtg::set_last_error(std::string("xTGSNA subdiagonal of A: ") + cudaGetErrorString(e));
+        return 1;
+    }
+    return 0;
+}
+
+// Device form: A, B, VL, VR and s on the device.
+template <class R, bool CPLX>
+int tgsna_device(void *stream, char job, char howmny, const int *select, int n, const void *A, int lda, const void *B,
+                 int ldb, const void *VL, int ldvl, const void *VR, int ldvr, void *s, int mm, int *m, int *info)
+{
+    int dummy = 0;
+    if (!info) info = &dummy;
+    job = (char)std::toupper((unsigned char)job);
+    howmny = (char)std::toupper((unsigned char)howmny);
+    xtg::set_last_error("");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::vector<R> sub;
+    std::vector<int> items;
+    std::vector<uint8_t> kinds;
+    // the subdiagonal is read only once A's leading dimension is known to be valid
+    *info = tgsna_check(job, howmny, n, lda, ldb, ldvl, ldvr);
+    if (*info) return 0;
+    if (tgsna_subdiag<R, CPLX>(A, lda, n, true, st, sub)) {
+        *info = 1;
+        return 1;
+    }
+    *info = tgsna_plan<R, CPLX>(howmny, select, n, mm, sub, m, items, kinds);
+    if (*info || items.empty()) return 0;
+    const int count = m ? *m : 0;
+    const int rc = xtg::eig_cond_device<R, CPLX>(n, A, lda, B, ldb, VL, ldvl, VR, ldvr, count, items, kinds, s, st);
+    if (rc) *info = 1;
+    return rc;
+}
+
+// Host form: stage A, B, VL, VR on the device, run, copy S back (DIF is not referenced).
+template <class R, bool CPLX>
+void tgsna_host(char job, char howmny, const int *select, int n, const void *A, int lda, const void *B, int ldb,
+                const void *VL, int ldvl, const void *VR, int ldvr, R *s, int mm, int *m, void *work, int lwork,
+                int *info)
+{
+    using E = typename std::conditional<CPLX, std::complex<R>, R>::type;
+    job = (char)std::toupper((unsigned char)job);
+    howmny = (char)std::toupper((unsigned char)howmny);
+    xtg::set_last_error("");
+    const int lwmin = std::max(1, n);
+    const bool lquery = lwork == -1;
+    if (work) static_cast<E *>(work)[0] = E(lwmin);
+    std::vector<R> sub;
+    std::vector<int> items;
+    std::vector<uint8_t> kinds;
+    int count = 0;
+    *info = tgsna_check(job, howmny, n, lda, ldb, ldvl, ldvr);
+    if (*info) return;
+    tgsna_subdiag<R, CPLX>(A, lda, n, false, nullptr, sub);
+    *info = tgsna_plan<R, CPLX>(howmny, select, n, mm, sub, &count, items, kinds);
+    if (m) *m = count;
+    if (*info == 0 && lwork < lwmin && !lquery) *info = -18;
+    if (*info || lquery || items.empty()) return;
+    const int ld = round_up(n, 32);
+    void *dA = nullptr, *dB = nullptr, *dL = nullptr, *dR = nullptr, *dS = nullptr;
+    cudaStream_t st = nullptr;
+    auto cleanup = [&]() {
+        if (st) cudaStreamSynchronize(st);
+        for (void *q : {dA, dB, dL, dR, dS})
+            if (q) cudaFree(q);
+        if (st) cudaStreamDestroy(st);
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    const size_t mat = (size_t)ld * n * sizeof(E), vec = (size_t)ld * count * sizeof(E);
+    for (void **q : {&dA, &dB})
+        if (e == cudaSuccess) e = cudaMallocAsync(q, mat, st);
+    for (void **q : {&dL, &dR})
+        if (e == cudaSuccess) e = cudaMallocAsync(q, vec, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&dS, (size_t)count * sizeof(R), st);
+    if (e == cudaSuccess)
+        e = cudaMemcpy2DAsync(dA, ld * sizeof(E), A, (size_t)lda * sizeof(E), n * sizeof(E), n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpy2DAsync(dB, ld * sizeof(E), B, (size_t)ldb * sizeof(E), n * sizeof(E), n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpy2DAsync(dL, ld * sizeof(E), VL, (size_t)ldvl * sizeof(E), n * sizeof(E), count,
+                              cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpy2DAsync(dR, ld * sizeof(E), VR, (size_t)ldvr * sizeof(E), n * sizeof(E), count,
+                              cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) {
+        xtg::set_last_error(std::string("xTGSNA staging: ") + cudaGetErrorString(e));
+        cleanup();
+        *info = 1;
+        return;
+    }
+    if (xtg::eig_cond_device<R, CPLX>(n, dA, ld, dB, ld, dL, ld, dR, ld, count, items, kinds, dS, st)) {
+        cleanup();
+        *info = 1;
+        return;
+    }
+    e = cudaMemcpyAsync(s, dS, (size_t)count * sizeof(R), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        xtg::set_last_error(std::string("xTGSNA D2H: ") + cudaGetErrorString(e));
+        *info = 1;
+    }
+    cleanup();
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------------------
@@ -545,6 +708,70 @@ int xtgevc3_ctrevc3_dev(unsigned flags, void *stream, char side, char howmny, co
 {
     return trevc3_device<float, true>(flags, stream, side, howmny, select, n, T, ldt, VL, ldvl, VR, ldvr, mm, m,
                                       info);
+}
+
+void xtgevc3_dtgsna(char job, char howmny, const int *select, int n, const double *A, int lda, const double *B,
+                    int ldb, const double *VL, int ldvl, const double *VR, int ldvr, double *s, double *dif, int mm, int *m,
+                    double *work, int lwork, int *iwork, int *info)
+{
+    (void)dif;
+    (void)iwork;
+    tgsna_host<double, false>(job, howmny, select, n, A, lda, B, ldb, VL, ldvl, VR, ldvr, s, mm, m, work, lwork, info);
+}
+
+int xtgevc3_dtgsna_dev(void *stream, char job, char howmny, const int *select, int n, const double *A, int lda,
+                        const double *B, int ldb, const double *VL, int ldvl, const double *VR, int ldvr, double *s, int mm,
+                        int *m, int *info)
+{
+    return tgsna_device<double, false>(stream, job, howmny, select, n, A, lda, B, ldb, VL, ldvl, VR, ldvr, s, mm, m, info);
+}
+
+void xtgevc3_stgsna(char job, char howmny, const int *select, int n, const float *A, int lda, const float *B,
+                    int ldb, const float *VL, int ldvl, const float *VR, int ldvr, float *s, float *dif, int mm, int *m,
+                    float *work, int lwork, int *iwork, int *info)
+{
+    (void)dif;
+    (void)iwork;
+    tgsna_host<float, false>(job, howmny, select, n, A, lda, B, ldb, VL, ldvl, VR, ldvr, s, mm, m, work, lwork, info);
+}
+
+int xtgevc3_stgsna_dev(void *stream, char job, char howmny, const int *select, int n, const float *A, int lda,
+                        const float *B, int ldb, const float *VL, int ldvl, const float *VR, int ldvr, float *s, int mm,
+                        int *m, int *info)
+{
+    return tgsna_device<float, false>(stream, job, howmny, select, n, A, lda, B, ldb, VL, ldvl, VR, ldvr, s, mm, m, info);
+}
+
+void xtgevc3_ztgsna(char job, char howmny, const int *select, int n, const double *A, int lda, const double *B,
+                    int ldb, const double *VL, int ldvl, const double *VR, int ldvr, double *s, double *dif, int mm, int *m,
+                    double *work, int lwork, int *iwork, int *info)
+{
+    (void)dif;
+    (void)iwork;
+    tgsna_host<double, true>(job, howmny, select, n, A, lda, B, ldb, VL, ldvl, VR, ldvr, s, mm, m, work, lwork, info);
+}
+
+int xtgevc3_ztgsna_dev(void *stream, char job, char howmny, const int *select, int n, const double *A, int lda,
+                        const double *B, int ldb, const double *VL, int ldvl, const double *VR, int ldvr, double *s, int mm,
+                        int *m, int *info)
+{
+    return tgsna_device<double, true>(stream, job, howmny, select, n, A, lda, B, ldb, VL, ldvl, VR, ldvr, s, mm, m, info);
+}
+
+void xtgevc3_ctgsna(char job, char howmny, const int *select, int n, const float *A, int lda, const float *B,
+                    int ldb, const float *VL, int ldvl, const float *VR, int ldvr, float *s, float *dif, int mm, int *m,
+                    float *work, int lwork, int *iwork, int *info)
+{
+    (void)dif;
+    (void)iwork;
+    tgsna_host<float, true>(job, howmny, select, n, A, lda, B, ldb, VL, ldvl, VR, ldvr, s, mm, m, work, lwork, info);
+}
+
+int xtgevc3_ctgsna_dev(void *stream, char job, char howmny, const int *select, int n, const float *A, int lda,
+                        const float *B, int ldb, const float *VL, int ldvl, const float *VR, int ldvr, float *s, int mm,
+                        int *m, int *info)
+{
+    return tgsna_device<float, true>(stream, job, howmny, select, n, A, lda, B, ldb, VL, ldvl, VR, ldvr, s, mm, m, info);
 }
 
 }  // extern "C"

@@ -948,4 +948,70 @@ template int solve_device<float, true>(char, char, const int *, int, const void 
                                        const void *, const void *, const void *, void *, int, void *, int, int,
                                        const Options &, cudaStream_t);
 
+
+template <class R, bool CPLX>
+int eig_cond_device(int n, const void *A_, int lda, const void *B_, int ldb, const void *VL_, int ldvl,
+                    const void *VR_, int ldvr, int m, const std::vector<int> &items, const std::vector<uint8_t> &kinds,
+                    void *s_dev, cudaStream_t st)
+{
+    using E = typename std::conditional<CPLX, cplx<R>, R>::type;
+    if (n <= 0 || m <= 0 || items.empty()) return 0;
+    int dev = 0;
+    XTG_CK(cudaGetDevice(&dev));
+    configure_device(dev);
+    Scratch scr(st);
+    const int ldx = round_up(n, 32), ni = (int)items.size();
+    E *AX = scr.get<E>((size_t)ldx * m);
+    E *BX = scr.get<E>((size_t)ldx * m);
+    int *d_items = scr.get<int>(2 * (size_t)ni);
+    uint8_t *d_kinds = scr.get<uint8_t>((size_t)ni);
+    if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
+    std::vector<int> ints(items);
+    ints.insert(ints.end(), items.begin(), items.end());  // S index = first column
+    XTG_CK(cudaMemcpyAsync(d_items, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    XTG_CK(cudaMemcpyAsync(d_kinds, kinds.data(), kinds.size(), cudaMemcpyHostToDevice, st));
+    for (int which = 0; which < 2; which++) {  // AX = A VR, BX = B VR (K = n, padding masked)
+        GemmArgs<E> g;
+        g.M = n;
+        g.N = m;
+        g.mlo = 0;
+        g.nseg = 1;
+        g.seg[0].A = static_cast<const E *>(which ? B_ : A_);
+        g.seg[0].lda = which ? ldb : lda;
+        g.seg[0].acols = n;
+        g.seg[0].K = round_up(n, kKPad);
+        g.seg[0].boff = 0;
+        g.K = g.seg[0].K;
+        g.B = static_cast<const E *>(VR_);
+        g.ldb = ldvr;
+        g.brows = n;
+        g.C = which ? BX : AX;
+        g.ldc = ldx;
+        g.ccol = nullptr;
+        g.kext = nullptr;
+        g.accumulate = 0;
+        launch_gemm<E>(g, false, st);
+        XTG_CK(cudaGetLastError());
+    }
+    eig_cond_kernel<R><<<(ni * 32 + 255) / 256, 256, 0, st>>>(
+        ni, d_items, d_kinds, n, reinterpret_cast<const R *>(AX), reinterpret_cast<const R *>(BX), ldx,
+        static_cast<const R *>(VL_), ldvl, static_cast<const R *>(VR_), ldvr, static_cast<R *>(s_dev), d_items + ni);
+    XTG_CK(cudaGetLastError());
+    XTG_CK(cudaStreamSynchronize(st));
+    return 0;
+}
+
+template int eig_cond_device<double, false>(int, const void *, int, const void *, int, const void *, int, const void *,
+                                             int, int, const std::vector<int> &, const std::vector<uint8_t> &, void *,
+                                             cudaStream_t);
+template int eig_cond_device<float, false>(int, const void *, int, const void *, int, const void *, int, const void *,
+                                            int, int, const std::vector<int> &, const std::vector<uint8_t> &, void *,
+                                            cudaStream_t);
+template int eig_cond_device<double, true>(int, const void *, int, const void *, int, const void *, int, const void *,
+                                            int, int, const std::vector<int> &, const std::vector<uint8_t> &, void *,
+                                            cudaStream_t);
+template int eig_cond_device<float, true>(int, const void *, int, const void *, int, const void *, int, const void *,
+                                           int, int, const std::vector<int> &, const std::vector<uint8_t> &, void *,
+                                           cudaStream_t);
+
 }  // namespace xtg

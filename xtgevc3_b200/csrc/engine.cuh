@@ -1,5 +1,7 @@
 // Host-side driver of the device algorithm (declarations shared by engine.cu and api.cpp).
 #pragma once
+#include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 #include <functional>
 #include <string>
@@ -73,5 +75,15 @@ int trace_get(int cat, long long *launches, double *ms, double *flops, double *b
 long long launch_count();
 // Adds launches made outside solve_device (the batched form's graph launches).
 void count_launches(long long k);
+
+// Eigenvalue condition numbers (LAPACK xTGSNA, JOB = 'E') of the selected eigenvalues of a
+// generalized Schur pencil (A, B) from their eigenvectors VL, VR (m columns, device
+// pointers): AX = A VR, BX = B VR on the tensor cores, then one warp per eigenvalue.
+// items: first column of each eigenvalue; kinds: 0 real, 1 (Re, Im) pair, 2 complex;
+// s_dev: device array of m condition numbers.  Returns 0, or 1 (message in last_error).
+template <class R, bool CPLX>
+int eig_cond_device(int n, const void *A, int lda, const void *B, int ldb, const void *VL, int ldvl, const void *VR,
+                    int ldvr, int m, const std::vector<int> &items, const std::vector<uint8_t> &kinds, void *s_dev,
+                    cudaStream_t st);
 
 }  // namespace xtg

@@ -324,4 +324,113 @@ __global__ void lapack_pair_phase_kernel(R *X, int ldx, int m, const int *colk, 
     }
 }
 
+// Eigenvalue condition numbers (LAPACK xTGSNA, JOB = 'E'):
+//   S(k) = sqrt(|y^H A x|^2 + |y^H B x|^2) / (||x||_2 ||y||_2)
+// for the eigenvector columns x = VR(:, c), y = VL(:, c) of one selected eigenvalue, from
+// AX = A VR and BX = B VR (columns c of the GEMM outputs).  A real pair (Re, Im columns c,
+// c + 1) combines the four real products as LAPACK does (y^H A x = (xr.yr + xi.yi) +
+// i (xi.yr - xr.yi)) and gives both columns the same S.  Norms are scaled by the column
+// maximum (no overflow for any finite input); S = -1 marks a zero numerator (not for a pair,
+// as in LAPACK dtgsna).  One warp per eigenvalue: items[w] is its
+// first column, kind 0 real, 1 pair, 2 complex; s[w] and, for a pair, s[w + 1].
+template <class R>
+__device__ __forceinline__ R warp_sum(R v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <class R>
+__device__ __forceinline__ R warp_maxabs(const R *col, int n, int lane)
+{
+    R mx = R(0);
+    for (int i = lane; i < n; i += 32) mx = fmax(mx, fabs(col[i]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    return mx;
+}
+
+// ||(u, v)||_2 of one or two real vectors of length n (v may be null), scaled
+template <class R>
+__device__ __forceinline__ R warp_norm2(const R *u, const R *v, int n, int lane)
+{
+    R mx = warp_maxabs(u, n, lane);
+    if (v) mx = fmax(mx, warp_maxabs(v, n, lane));
+    if (!(mx > R(0))) return R(0);
+    R acc = R(0);
+    for (int i = lane; i < n; i += 32) {
+        const R a = u[i] / mx;
+        acc += a * a;
+        if (v) {
+            const R b = v[i] / mx;
+            acc += b * b;
+        }
+    }
+    return mx * sqrt(warp_sum(acc));
+}
+
+template <class R>
+__global__ void eig_cond_kernel(int nitems, const int *items, const uint8_t *kinds, int n, const R *AX, const R *BX,
+                                int ldx, const R *VL, int ldvl, const R *VR, int ldvr, R *s, const int *sidx)
+{
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= nitems) return;  // uniform per warp
+    const int c = items[w], kind = kinds[w];
+    R num = R(0), rn = R(0), ln = R(0);
+    if (kind == 0) {  // real
+        const R *x = VR + (size_t)c * ldvr, *y = VL + (size_t)c * ldvl;
+        const R *ax = AX + (size_t)c * ldx, *bx = BX + (size_t)c * ldx;
+        R ta = R(0), tb = R(0);
+        for (int i = lane; i < n; i += 32) {
+            ta += ax[i] * y[i];
+            tb += bx[i] * y[i];
+        }
+        ta = warp_sum(ta);
+        tb = warp_sum(tb);
+        num = hypot(ta, tb);
+        rn = warp_norm2<R>(x, nullptr, n, lane);
+        ln = warp_norm2<R>(y, nullptr, n, lane);
+    } else if (kind == 1) {  // real pair: (Re, Im) columns c, c + 1
+        const R *xr = VR + (size_t)c * ldvr, *xi = xr + ldvr, *yr = VL + (size_t)c * ldvl, *yi = yr + ldvl;
+        const R *ar = AX + (size_t)c * ldx, *ai = ar + ldx, *br = BX + (size_t)c * ldx, *bi = br + ldx;
+        R a_rr = R(0), a_ri = R(0), a_ii = R(0), a_ir = R(0), b_rr = R(0), b_ri = R(0), b_ii = R(0), b_ir = R(0);
+        for (int i = lane; i < n; i += 32) {
+            a_rr += ar[i] * yr[i];
+            a_ri += ar[i] * yi[i];
+            a_ii += ai[i] * yi[i];
+            a_ir += ai[i] * yr[i];
+            b_rr += br[i] * yr[i];
+            b_ri += br[i] * yi[i];
+            b_ii += bi[i] * yi[i];
+            b_ir += bi[i] * yr[i];
+        }
+        a_rr = warp_sum(a_rr); a_ri = warp_sum(a_ri); a_ii = warp_sum(a_ii); a_ir = warp_sum(a_ir);
+        b_rr = warp_sum(b_rr); b_ri = warp_sum(b_ri); b_ii = warp_sum(b_ii); b_ir = warp_sum(b_ir);
+        const R uha = hypot(a_rr + a_ii, a_ir - a_ri), uhb = hypot(b_rr + b_ii, b_ir - b_ri);
+        num = hypot(uha, uhb);
+        rn = warp_norm2<R>(xr, xi, n, lane);
+        ln = warp_norm2<R>(yr, yi, n, lane);
+    } else {  // complex: interleaved columns, y^H A x = sum conj(y_i) (A x)_i
+        const R *x = VR + 2 * (size_t)c * ldvr, *y = VL + 2 * (size_t)c * ldvl;
+        const R *ax = AX + 2 * (size_t)c * ldx, *bx = BX + 2 * (size_t)c * ldx;
+        R ar_ = R(0), ai_ = R(0), br_ = R(0), bi_ = R(0);
+        for (int i = lane; i < n; i += 32) {
+            const R yr = y[2 * i], yi = y[2 * i + 1];
+            ar_ += yr * ax[2 * i] + yi * ax[2 * i + 1];
+            ai_ += yr * ax[2 * i + 1] - yi * ax[2 * i];
+            br_ += yr * bx[2 * i] + yi * bx[2 * i + 1];
+            bi_ += yr * bx[2 * i + 1] - yi * bx[2 * i];
+        }
+        num = hypot(hypot(warp_sum(ar_), warp_sum(ai_)), hypot(warp_sum(br_), warp_sum(bi_)));
+        rn = warp_norm2<R>(x, nullptr, 2 * n, lane);
+        ln = warp_norm2<R>(y, nullptr, 2 * n, lane);
+    }
+    if (lane == 0) {
+        const R v = (num == R(0) && kind != 1) ? R(-1) : num / (rn * ln);  // LAPACK: no -1 for a pair
+        s[sidx[w]] = v;
+        if (kind == 1) s[sidx[w] + 1] = v;
+    }
+}
+
 }  // namespace xtg
