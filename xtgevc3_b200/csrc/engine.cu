@@ -170,8 +170,10 @@ void configure_device(int dev)
                              2 * kBlock * kSmLd * (int)sizeof(cplx<double>));
         cudaFuncSetAttribute(diag_solve_cplx<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              2 * kBlock * kSmLd * (int)sizeof(cplx<float>));
-        cudaFuncSetAttribute(gemm_dmma<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::SMEM_BYTES);
-        cudaFuncSetAttribute(gemm_dmma<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::SMEM_BYTES);
+        cudaFuncSetAttribute(gemm_dmma<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::Tile<128>::SMEM_BYTES);
+        cudaFuncSetAttribute(gemm_dmma<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::Tile<128>::SMEM_BYTES);
+        cudaFuncSetAttribute(gemm_dmma<0, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::Tile<64>::SMEM_BYTES);
+        cudaFuncSetAttribute(gemm_dmma<1, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::Tile<64>::SMEM_BYTES);
         cudaFuncSetAttribute(gemm_dmma_cplx<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, zmma::SMEM_BYTES);
         cudaFuncSetAttribute(gemm_dmma_cplx<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, zmma::SMEM_BYTES);
         cudaFuncSetAttribute(split::gemm_split_kernel<split::kBF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,

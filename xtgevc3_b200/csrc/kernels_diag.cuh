@@ -74,8 +74,18 @@ __device__ __forceinline__ void set_row(T (&r)[2], int row, int lane, T v)
 
 __device__ __forceinline__ double rcp(double v) { return __drcp_rn(v); }
 __device__ __forceinline__ float rcp(float v) { return __frcp_rn(v); }
+// 1 / v by Smith's method (R. L. Smith, Comm. ACM 5(8), 1962), its two real divisions done
+// as reciprocals: with |a| >= |b| the larger and smaller part of v, r = b / a and
+// d = a + r b, 1 / (a + i b) = (1 - i r) / d and 1 / (b + i a) = (r - i) / d.  v != 0.
 template <class R>
-__device__ __forceinline__ cplx<R> rcp(cplx<R> v) { return cdiv(cplx<R>(R(1), R(0)), v); }
+__device__ __forceinline__ cplx<R> rcp(cplx<R> v)
+{
+    const bool re_big = fabs(v.x) >= fabs(v.y);
+    const R a = re_big ? v.x : v.y, b = re_big ? v.y : v.x;
+    const R r = b * rcp(a);
+    const R id = rcp(a + r * b);
+    return re_big ? cplx<R>(id, -r * id) : cplx<R>(r * id, -id);
+}
 
 template <class R>
 __device__ __forceinline__ R mag(R v) { return fabs(v); }
@@ -187,20 +197,42 @@ __device__ __forceinline__ void write_y(const DiagArgs<R> &a, E *ycol, int jnb, 
         }
 }
 
-template <class E>
+template <class E, int kBatch = 8>
 __device__ __forceinline__ void load_block(const E *S, int lds, const E *P, int ldp, int r0, int jnb, int sub,
                                            E *Ss, E *Ps)
 {
-    for (int t = threadIdx.x; t < jnb * jnb; t += blockDim.x) {
-        int i = t % jnb, j = t / jnb;
-        bool keep = i <= j + sub;  // upper triangle (plus the subdiagonal for real S)
-        Ss[i + j * kSmLd] = keep ? S[(size_t)(r0 + i) + (size_t)(r0 + j) * lds] : E(0);
-        Ps[i + j * kSmLd] = keep ? P[(size_t)(r0 + i) + (size_t)(r0 + j) * ldp] : E(0);
+    // kBatch elements of each matrix per thread are loaded before any is stored, so that the
+    // block's loads are in flight together instead of one memory round trip per element
+    // (kBatch x blockDim = 4096 covers a full block in one pass).  The whole square is read
+    // (it lies inside the matrix); the part below the upper triangle (plus the subdiagonal
+    // for real S) is stored as zeros.
+    const int tot = jnb * jnb;
+    for (int t0 = threadIdx.x; t0 < tot; t0 += kBatch * blockDim.x) {
+        E vs[kBatch], vp[kBatch];
+#pragma unroll
+        for (int u = 0; u < kBatch; u++) {
+            const int t = t0 + u * blockDim.x;
+            if (t < tot) {
+                const int i = t % jnb, j = t / jnb;
+                vs[u] = S[(size_t)(r0 + i) + (size_t)(r0 + j) * lds];
+                vp[u] = P[(size_t)(r0 + i) + (size_t)(r0 + j) * ldp];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kBatch; u++) {
+            const int t = t0 + u * blockDim.x;
+            if (t < tot) {
+                const int i = t % jnb, j = t / jnb;
+                const bool keep = i <= j + sub;
+                Ss[i + j * kSmLd] = keep ? vs[u] : E(0);
+                Ps[i + j * kSmLd] = keep ? vp[u] : E(0);
+            }
+        }
     }
 }
 
 // Factors of the diagonal blocks of W for the rows a lane owns: inv1 = 1 / w_ii for every
-// row; for the second row i of a 2x2 block (i-1, i): the LU with partial pivoting on
+// 1x1 row (rows of a 2x2 block keep 0); for the second row i of a 2x2 block (i-1, i): the LU with partial pivoting on
 // column i-1:  swap rows if |w_i,i-1| > |w_i-1,i-1|, then (a b; c d) -> a^-1, b, m = c/a,
 // (d - m b)^-1.
 template <class E>
@@ -219,7 +251,9 @@ __device__ __forceinline__ void factor_rows(Factors<E> &F, uint64_t sec, int nro
         F.fa[s] = F.fb[s] = F.fm[s] = F.fu[s] = E(0);
         F.sw[s] = false;
         if (i < nrows) {
-            F.inv1[s] = rcp(floor_pivot(W(i, i), smin));
+            // rows of a 2x2 block are solved with its LU; inv1 serves 1x1 rows only
+            const bool in2 = ((sec >> i) & 1ull) || (i + 1 < nrows && ((sec >> (i + 1)) & 1ull));
+            if (!in2) F.inv1[s] = rcp(floor_pivot(W(i, i), smin));
             if (i >= 1 && ((sec >> i) & 1ull)) {
                 E w11 = W(i - 1, i - 1), w12 = W(i - 1, i), w21 = W(i, i - 1), w22 = W(i, i);
                 const bool sw = mag(w21) > mag(w11);
@@ -433,18 +467,22 @@ __device__ __forceinline__ void pair_mask(const R *Ss, int jnb, uint64_t *out)
         const bool b0 = l >= 1 && l < jnb && Ss[l + (l - 1) * kSmLd] != R(0);
         const bool b1 = l + 32 < jnb && Ss[(l + 32) + (l + 31) * kSmLd] != R(0);
         const uint64_t sub = (uint64_t)__ballot_sync(0xffffffffu, b0) | ((uint64_t)__ballot_sync(0xffffffffu, b1) << 32);
-        if (l == 0) {
-            uint64_t sec = 0;
-            for (int j = jnb - 1; j >= 1;) {
-                if ((sub >> j) & 1ull) {
-                    sec |= 1ull << j;
-                    j -= 2;
-                } else {
-                    j -= 1;
-                }
+        // Greedy pairing from the bottom takes, in every run of set bits, the top bit and
+        // every second one below it: bit j is taken when the run of set bits directly above
+        // it has even length.  Each lane decides its two bits.
+        uint64_t sec = 0;
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+            const int j = l + 32 * s;
+            bool take = false;
+            if ((sub >> j) & 1ull) {
+                int k = j + 1;
+                while (k < 64 && ((sub >> k) & 1ull)) k++;
+                take = ((k - j - 1) & 1) == 0;
             }
-            *out = sec;
+            sec |= (uint64_t)__ballot_sync(0xffffffffu, take) << (32 * s);
         }
+        if (l == 0) *out = sec;
     }
 }
 
@@ -459,7 +497,7 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
     R *Ss = reinterpret_cast<R *>(smem_diag);
     R *Ps = Ss + kSmLd * kBlock;
     const int jnb = a.r1 - a.r0;
-    load_block(a.S, a.lds, a.P, a.ldp, a.r0, jnb, 1, Ss, Ps);
+    load_block<R, 16>(a.S, a.lds, a.P, a.ldp, a.r0, jnb, 1, Ss, Ps);
     __syncthreads();
     pair_mask(Ss, jnb, &s_sec);
     __syncthreads();

@@ -140,18 +140,23 @@ __global__ void __launch_bounds__(256) gemm_simt(GemmArgs<E> g)
 
 // ------------------------------------------------------------------------------------
 // FP64 tensor-core kernel (DMMA, mma.sync m8n8k4 f64).
-// CTA tile 128 x 64, K step 16, 8 warps as 4 (M) x 2 (N) with 32 x 32 warp tiles,
+// CTA tile BM x 64 (BM = 128, or 64 for launches of at most 64 output rows, such as the
+// update of a group's upper block), K step 16, BM/32 x 2 warps with 32 x 32 warp tiles,
 // 3-stage cp.async pipeline into padded shared memory (conflict-free fragment loads).
 // Requires 16-byte aligned segment bases and B, and even leading dimensions (checked by
 // the launcher, which uses the SIMT kernel otherwise).
 // ------------------------------------------------------------------------------------
 namespace dmma {
-constexpr int BM = 128, BN = 64, BK = 16, STAGES = 3;  // BK divides kKPad (segment K)
-constexpr int ALD = BM + 8;   // A tile stored [k][m]
-constexpr int BLD = BK + 4;   // B tile stored [n][k]
-constexpr int A_STAGE = BK * ALD;
+constexpr int BN = 64, BK = 16, STAGES = 3;  // BK divides kKPad (segment K)
+constexpr int BLD = BK + 4;                  // B tile stored [n][k]
 constexpr int B_STAGE = BN * BLD;
-constexpr int SMEM_BYTES = STAGES * (A_STAGE + B_STAGE) * 8;
+template <int BM>
+struct Tile {
+    static constexpr int NT = 2 * BM;         // threads: BM/32 x 2 warps
+    static constexpr int ALD = BM + 8;        // A tile stored [k][m]
+    static constexpr int A_STAGE = BK * ALD;
+    static constexpr int SMEM_BYTES = STAGES * (A_STAGE + B_STAGE) * 8;
+};
 }  // namespace dmma
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes)
@@ -171,15 +176,18 @@ __device__ __forceinline__ void dmma884(double &d0, double &d1, double a, double
 }
 
 // ACC = 1: trailing update (C += A B); ACC = 0: back-transform (C = A B, triangular B).
-template <int ACC>
-__global__ void __launch_bounds__(256) gemm_dmma(GemmArgs<double> g)
+template <int ACC, int BM = 128>
+__global__ void __launch_bounds__(2 * BM) gemm_dmma(GemmArgs<double> g)
 {
     using namespace dmma;
+    constexpr int NT = Tile<BM>::NT, ALD = Tile<BM>::ALD, A_STAGE = Tile<BM>::A_STAGE;
+    constexpr int WM = BM / 32;  // warps along M
+    static_assert((BK * BM) % (2 * NT) == 0 && (BN * BK) % (2 * NT) == 0, "loader chunks per thread");
     extern __shared__ __align__(16) unsigned char smem_gemm[];
     double *As = reinterpret_cast<double *>(smem_gemm);
     double *Bs = As + STAGES * A_STAGE;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wm = warp & 3, wn = warp >> 2;
+    const int wm = warp % WM, wn = warp / WM;
     const int gq = lane >> 2, tq = lane & 3;
     // with a per-column K extent (back-transform: triangular B, extent growing with the
     // column) the column tiles run last-first, so the longest tiles start first
@@ -204,8 +212,8 @@ __global__ void __launch_bounds__(256) gemm_dmma(GemmArgs<double> g)
         double *as = As + st * A_STAGE;
         double *bs = Bs + st * B_STAGE;
 #pragma unroll
-        for (int q = 0; q < BK * BM / 512; q++) {  // A: BK columns x BM/2 chunks of 16 bytes
-            int e = tid + 256 * q;
+        for (int q = 0; q < BK * BM / (2 * NT); q++) {  // A: BK columns x BM/2 chunks of 16 bytes
+            int e = tid + NT * q;
             int kk = e / (BM / 2), ch = e % (BM / 2);
             int row = m0 + 2 * ch, col = k0 - kb + kk;
             int bytes = 0;
@@ -214,8 +222,8 @@ __global__ void __launch_bounds__(256) gemm_dmma(GemmArgs<double> g)
             cp_async16(as + kk * ALD + 2 * ch, gp, bytes);
         }
 #pragma unroll
-        for (int q = 0; q < BN * BK / 512; q++) {  // B: BN columns x BK/2 chunks
-            int e = tid + 256 * q;
+        for (int q = 0; q < BN * BK / (2 * NT); q++) {  // B: BN columns x BK/2 chunks
+            int e = tid + NT * q;
             int nn = e / (BK / 2), ch = e % (BK / 2);
             int kr = sg.boff + k0 - kb + 2 * ch, col = n0 + nn;
             int lim = min(sg.boff + kmax - kb, g.brows);
