@@ -275,6 +275,38 @@ def test_device_api_matches_host_api(cuda_ok):
     assert n == m
 
 
+@pytest.mark.parametrize("howmny", ["B", "A"])
+@pytest.mark.parametrize("dt", [np.float64, np.float32], ids=["d", "s"])
+def test_host_panels_match_device_api(cuda_ok, dt, howmny):
+    """The host-pointer form of a real pencil uploads S and P in 512-column panels while the
+    solve runs (right to left: the right side waits for each group's panels, the left side
+    for all of them), reads the subdiagonal from the caller's S and takes anorm, bnorm from
+    host threads summing in the device reduction's order.  At n = 1100 (three panels) every
+    column equals the device form's, bit for bit."""
+    import torch
+    n = 1100
+    p = _pencil("schur", n, 7, dt)
+    rng = np.random.default_rng(11)
+    Q = np.asfortranarray(np.linalg.qr(rng.standard_normal((n, n)))[0].astype(dt))
+    Z = np.asfortranarray(np.linalg.qr(rng.standard_normal((n, n)))[0].astype(dt))
+    back = howmny == "B"
+    VLh, VRh, m, info = X.tgevc3("B", howmny, p["S"], p["P"], p["alpha"], p["beta"], alphai=p["alphai"],
+                                 VL=Q.copy(order="F") if back else None, VR=Z.copy(order="F") if back else None)
+    assert (m, info) == (n, 0)
+
+    def dev(a):  # column-major device tensor
+        return torch.from_numpy(np.ascontiguousarray(a.T)).cuda().t()
+
+    VL = dev(Q) if back else dev(np.zeros((n, n), dtype=dt))
+    VR = dev(Z) if back else dev(np.zeros((n, n), dtype=dt))
+    m2, info2 = X.tgevc3_dev("B", howmny, dev(p["S"]), dev(p["P"]), p["alpha"], p["beta"], alphai=p["alphai"],
+                             VL=VL, VR=VR)
+    torch.cuda.synchronize()
+    assert (m2, info2) == (m, info)
+    np.testing.assert_array_equal(VL.t().cpu().numpy().T, VLh[:, :m])
+    np.testing.assert_array_equal(VR.t().cpu().numpy().T, VRh[:, :m])
+
+
 SPLIT_CASES = [
     # (kind, n, seed, side, howmny, slices, elementwise tolerance vs the FP64 oracle, slice kind)
     ("gges", 257, 71, "B", "B", 6, 1e-10, "bf16"),

@@ -14,6 +14,7 @@
 #include <cstdint>
 #include <complex>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 namespace {
@@ -65,12 +66,88 @@ bool check_work(int n, W *work, int lwork, int *info)
 
 inline int round_up(int v, int q) { return (v + q - 1) / q * q; }
 
+// Sum of |a[0..last]| as the device reduction forms it (colsum_kernel): 32 partial sums over
+// rows l, l + 32, ... in increasing row order, then the xor butterfly of its shuffles.  The
+// same additions in the same order give the same value, bit for bit.
+template <class R>
+R col_abs_sum(const R *a, int last)
+{
+    R s[32] = {};
+    int r0 = 0;
+    for (; r0 + 32 <= last + 1; r0 += 32)
+        for (int l = 0; l < 32; l++) s[l] += std::fabs(a[r0 + l]);
+    for (int l = 0; r0 + l <= last; l++) s[l] += std::fabs(a[r0 + l]);
+    for (int o = 16; o > 0; o >>= 1) {
+        R t[32];
+        for (int l = 0; l < 32; l++) t[l] = s[l] + s[l ^ o];
+        std::copy(t, t + 32, s);
+    }
+    return s[0];
+}
+
+// anorm, bnorm of a real pencil (column sums over rows <= col + 1, then their maximum, as
+// colsum_kernel and colmax_kernel compute them), on host threads that run while the call
+// queues its work; P = nullptr is the identity (every column sums to 1).
+template <class R>
+struct HostNorms {
+    const R *S = nullptr, *P = nullptr;
+    int lds = 0, ldp = 0, n = 0;
+    std::vector<R> sums;
+    std::vector<std::thread> th;
+    bool partial = false;  // a thread could not be started: finish() sums every column itself
+    void columns(int t, int nt)
+    {
+        for (int j0 = 64 * t; j0 < n; j0 += 64 * nt)
+            for (int j = j0; j < std::min(n, j0 + 64); j++) {
+                const int last = std::min(j + 1, n - 1);
+                sums[j] = col_abs_sum(S + (size_t)j * lds, last);
+                sums[(size_t)n + j] = P ? col_abs_sum(P + (size_t)j * ldp, last) : R(1);
+            }
+    }
+    void start(const R *S_, int lds_, const R *P_, int ldp_, int n_)
+    {
+        S = S_, P = P_, lds = lds_, ldp = ldp_, n = n_;
+        sums.assign(2 * (size_t)n, R(0));
+        const int hw = (int)std::thread::hardware_concurrency();
+        const int nt = std::max(1, std::min({hw > 0 ? hw : 1, 32, (n + 63) / 64}));
+        try {
+            for (int t = 0; t < nt; t++) th.emplace_back([this, t, nt] { columns(t, nt); });
+        } catch (...) {
+            partial = true;
+        }
+    }
+    void join()
+    {
+        for (auto &x : th)
+            if (x.joinable()) x.join();
+        th.clear();
+    }
+    void finish(double *out)
+    {
+        join();
+        if (partial) columns(0, 1);
+        R a = 0, b = 0;
+        for (int j = 0; j < n; j++) {
+            a = std::fmax(a, sums[j]);
+            b = std::fmax(b, sums[(size_t)n + j]);
+        }
+        out[0] = a;
+        out[1] = b;
+    }
+    ~HostNorms() { join(); }
+};
+
 // Host pointers: stage S, P (and Q/Z for HOWMNY='B') on the device, run, copy back.
 // S and P travel as their upper trapezoid only (every kernel reads rows <= col + 1), in
-// column panels; the device copies are zeroed first so the rest holds no garbage.  Q and Z
-// upload on a second stream while the substitution runs (each side's back-transform waits
-// for its matrix), and each side's result downloads on a third stream as soon as that
-// side's kernels are queued, behind the other side's work.
+// pieces; the device copies are zeroed first so the rest holds no garbage.  Real types: the
+// pieces go up on the input stream while the call runs, after its small copies: column
+// panels from the right (the right side's groups read columns right to left) alternating
+// with row strips from the top (the left side's groups read rows top to bottom), each
+// piece what the ones before left of the trapezoid; every group waits for the pieces it
+// reads, and the norms come from host threads.  Complex types: column panels on the call's
+// stream before the solve.  Q and Z upload on the input stream behind S and P (each side's
+// back-transform waits for its matrix), and each side's result downloads on a third stream
+// as soon as that side's kernels are queued, behind the other side's work.
 template <class R, bool CPLX>
 int run_host(char side, char howmny, const int *select, int n, const void *S, int lds, const void *P, int ldp,
              const void *alpha, const void *alphai, const void *beta, void *VL, int ldvl, void *VR, int ldvr,
@@ -87,6 +164,7 @@ int run_host(char side, char howmny, const int *select, int n, const void *S, in
     struct Res {
         cudaStream_t st = nullptr, sin = nullptr, sout = nullptr;
         cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // Z ready, Q ready, right done, left done
+        std::vector<cudaEvent_t> pev;  // piece k of S and P on the device (real types)
         void *dS = nullptr, *dP = nullptr, *dVL = nullptr, *dVR = nullptr;
         ~Res()
         {
@@ -97,6 +175,8 @@ int run_host(char side, char howmny, const int *select, int n, const void *S, in
                 if (p) cudaFree(p);
             for (cudaEvent_t e : ev)
                 if (e) cudaEventDestroy(e);
+            for (cudaEvent_t e : pev)
+                if (e) cudaEventDestroy(e);
             for (cudaStream_t q : {st, sin, sout})
                 if (q) cudaStreamDestroy(q);
         }
@@ -105,6 +185,9 @@ int run_host(char side, char howmny, const int *select, int n, const void *S, in
         xtg::set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
         return 1;
     };
+    constexpr bool kPanels = !CPLX;  // S, P go up behind the solve, norms from the host
+    HostNorms<R> hn;                 // its threads read only the caller's S and P
+    if constexpr (kPanels) hn.start(static_cast<const R *>(S), lds, static_cast<const R *>(P), ldp, n);
     cudaError_t e;
     for (cudaStream_t *q : {&r.st, &r.sin, &r.sout})
         if ((e = cudaStreamCreateWithFlags(q, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
@@ -118,18 +201,47 @@ int run_host(char side, char howmny, const int *select, int n, const void *S, in
     if (want_r && (e = cudaMallocAsync(&r.dVR, (size_t)ld * vcols * sizeof(E), r.st)) != cudaSuccess)
         return fail(e, "cudaMallocAsync");
     const int panel = 512;
-    for (int which = 0; which < (P ? 2 : 1); which++) {
+    // rows [r0, r1) x columns [c0, c1) of S or P, on stream q
+    auto put = [&](int which, int r0, int r1, int c0, int c1, cudaStream_t q) {
         void *dst = which ? r.dP : r.dS;
         const void *src = which ? P : S;
         const int lsrc = which ? ldp : lds;
-        if ((e = cudaMemsetAsync(dst, 0, mat, r.st)) != cudaSuccess) return fail(e, "cudaMemsetAsync");
-        for (int j0 = 0; j0 < n; j0 += panel) {
-            const int j1 = std::min(n, j0 + panel), rows = std::min(n, j1 + 1);
-            e = cudaMemcpy2DAsync(static_cast<E *>(dst) + (size_t)j0 * ld, ld * sizeof(E),
-                                  static_cast<const E *>(src) + (size_t)j0 * lsrc, (size_t)lsrc * sizeof(E),
-                                  (size_t)rows * sizeof(E), j1 - j0, cudaMemcpyHostToDevice, r.st);
-            if (e != cudaSuccess) return fail(e, which ? "H2D P" : "H2D S");
+        return cudaMemcpy2DAsync(static_cast<E *>(dst) + (size_t)r0 + (size_t)c0 * ld, ld * sizeof(E),
+                                 static_cast<const E *>(src) + (size_t)r0 + (size_t)c0 * lsrc, (size_t)lsrc * sizeof(E),
+                                 (size_t)(r1 - r0) * sizeof(E), c1 - c0, cudaMemcpyHostToDevice, q);
+    };
+    for (int which = 0; which < (P ? 2 : 1); which++) {
+        if ((e = cudaMemsetAsync(which ? r.dP : r.dS, 0, mat, r.st)) != cudaSuccess) return fail(e, "cudaMemsetAsync");
+        if (!kPanels)
+            for (int j0 = 0; j0 < n; j0 += panel) {
+                const int j1 = std::min(n, j0 + panel);
+                if ((e = put(which, 0, std::min(n, j1 + 1), j0, j1, r.st)) != cudaSuccess)
+                    return fail(e, which ? "H2D P" : "H2D S");
+            }
+    }
+    // Upload plan of the trapezoid (rows <= col + 1), real types.  State (cf, rt): columns >= cf
+    // and rows < rt are on the device; what is left is rows >= rt of columns < cf, nonempty
+    // while 1 <= cf and rt <= cf.  A column panel takes columns [cf - panel, cf) from row rt
+    // down; a row strip takes rows [rt, rt + panel) of columns [rt - 1, cf).  Each piece
+    // records the state after it.
+    struct Piece {
+        int r0, r1, c0, c1, cfrom, rto;
+    };
+    std::vector<Piece> plan;
+    if (kPanels) {
+        int cf = n, rt = 0;
+        while (cf >= 1 && rt <= cf) {
+            const int c0 = std::max(cf - panel, 0), rhi = std::min(n, cf + 1);
+            plan.push_back({rt, rhi, c0, cf, c0, rt});
+            cf = c0;
+            if (!(cf >= 1 && rt <= cf)) break;
+            const int r1 = std::min(rt + panel, n), cl = std::max(rt - 1, 0);
+            plan.push_back({rt, r1, cl, cf, cf, r1});
+            rt = r1;
         }
+        r.pev.assign(plan.size(), nullptr);
+        for (cudaEvent_t &ev : r.pev)
+            if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
     }
     xtg::Options opt = make_opts(flags);
     if (!P) {  // xTREVC3 conventions
@@ -144,12 +256,45 @@ int run_host(char side, char howmny, const int *select, int n, const void *S, in
     // link's host-to-device bandwidth with S and P.  The wait also orders the second stream
     // after the allocations of the output buffers it writes.
     cudaError_t in_err = cudaSuccess;
-    if (back) {
-        opt.back_ready[0] = want_r ? r.ev[0] : nullptr;
-        opt.back_ready[1] = want_l ? r.ev[1] : nullptr;
+    // stream q waits for the first piece after which `done` holds (columns [col, n) or rows
+    // [0, rows) all up; the last piece completes everything).  Function scope: opt's hooks
+    // below call it from inside the solve.
+    auto wait_piece = [&](cudaStream_t q, auto done) -> int {
+        if (plan.empty()) return -1;
+        size_t k = 0;
+        while (k + 1 < plan.size() && !done(plan[k])) k++;
+        cudaError_t x = cudaStreamWaitEvent(q, r.pev[k], 0);
+        if (x != cudaSuccess) in_err = x;
+        return (int)k;
+    };
+    if (kPanels) {
+        opt.host_S = S;
+        opt.host_lds = lds;
+        opt.host_norms = [&](double *out) { hn.finish(out); };
+        opt.cols_ready = [&](bool, int col, cudaStream_t q) {
+            wait_piece(q, [&](const Piece &p) { return p.cfrom <= col; });
+        };
+        opt.rows_ready = [&](int rows, cudaStream_t q) {
+            const int k = wait_piece(q, [&](const Piece &p) { return p.rto >= rows; });
+            return (k < 0 || k + 1 == (int)plan.size()) ? n : plan[k].rto;
+        };
+    }
+    if (back || kPanels) {
+        opt.back_ready[0] = back && want_r ? r.ev[0] : nullptr;
+        opt.back_ready[1] = back && want_l ? r.ev[1] : nullptr;
         opt.staged = [&](cudaStream_t sst) {
             cudaError_t x = cudaEventRecord(r.ev[2], sst);
             if (x == cudaSuccess) x = cudaStreamWaitEvent(r.sin, r.ev[2], 0);
+            for (size_t k = 0; k < plan.size() && x == cudaSuccess; k++) {
+                const Piece &p = plan[k];
+                x = put(0, p.r0, p.r1, p.c0, p.c1, r.sin);
+                if (x == cudaSuccess && P) x = put(1, p.r0, p.r1, p.c0, p.c1, r.sin);
+                if (x == cudaSuccess) x = cudaEventRecord(r.pev[k], r.sin);
+            }
+            if (!back) {
+                if (x != cudaSuccess) in_err = x;
+                return;
+            }
             if (x == cudaSuccess && want_r)
                 x = cudaMemcpy2DAsync(r.dVR, ld * sizeof(E), VR, (size_t)ldvr * sizeof(E), (size_t)n * sizeof(E), n,
                                       cudaMemcpyHostToDevice, r.sin);

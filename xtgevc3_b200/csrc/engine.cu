@@ -326,7 +326,10 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
     }
     std::vector<char> sub(n, 0);  // sub[k] = S[k+1, k] != 0
     if constexpr (!CPLX) {
-        if (n > 1) {
+        if (n > 1 && opt.host_S) {  // the caller's copy (the device one may still be in flight)
+            const E *hs = static_cast<const E *>(opt.host_S);
+            for (int k = 0; k + 1 < n; k++) sub[k] = hs[(size_t)(k + 1) + (size_t)k * opt.host_lds] != E(0);
+        } else if (n > 1) {
             std::vector<E> d(n - 1);
             XTG_CK(cudaMemcpy2DAsync(d.data(), sizeof(E), S + 1, (size_t)(lds + 1) * sizeof(E), sizeof(E), n - 1,
                                      cudaMemcpyDeviceToHost, st));
@@ -369,12 +372,15 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         XTG_CK(cudaMemcpyAsync(d_eig + n, alphai_, n * sizeof(R), cudaMemcpyHostToDevice, st));
         XTG_CK(cudaMemcpyAsync(d_eig + 2 * n, beta_, n * sizeof(R), cudaMemcpyHostToDevice, st));
     }
-    // anorm / bnorm (src/dtgevc3.cpp:1254-1270; complex: rows <= col only)
-    tr.run(kTPrep, 0, (double)n * (n + 1) * esz, st, [&] {
-        colsum_kernel<E, R><<<(n + 7) / 8, 256, 0, st>>>(S, lds, P, ldp, n, CPLX ? 0 : 1, d_sums);
-    });
-    tr.run(kTPrep, 0, 2.0 * n * sizeof(R), st, [&] { colmax_kernel<R><<<1, 1024, 0, st>>>(d_sums, n, d_norms); });
-    XTG_CK(cudaGetLastError());
+    // anorm / bnorm (src/dtgevc3.cpp:1254-1270; complex: rows <= col only); with host_norms
+    // they come from the caller after `staged` (below)
+    if (!opt.host_norms) {
+        tr.run(kTPrep, 0, (double)n * (n + 1) * esz, st, [&] {
+            colsum_kernel<E, R><<<(n + 7) / 8, 256, 0, st>>>(S, lds, P, ldp, n, CPLX ? 0 : 1, d_sums);
+        });
+        tr.run(kTPrep, 0, 2.0 * n * sizeof(R), st, [&] { colmax_kernel<R><<<1, 1024, 0, st>>>(d_sums, n, d_norms); });
+        XTG_CK(cudaGetLastError());
+    }
 
     // diagonal-solve launches: one warp per eigenvector, as many CTAs as stay resident
     const int diag_threads = CPLX ? kDiagThreadsCplx : 256, diag_warps = diag_threads / 32;
@@ -449,6 +455,13 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
     if (want_r && build_cols(false, side_cols[0])) return 1;
     if (want_l && build_cols(true, side_cols[1])) return 1;
     if (opt.staged) opt.staged(st);
+    if (opt.host_norms) {
+        // kernel arguments, not a copy: a host-to-device copy could wait behind the panels
+        double hn[2] = {0, 0};
+        opt.host_norms(hn);
+        set_norms_kernel<R><<<1, 1, 0, st>>>(d_norms, R(hn[0]), R(hn[1]));
+        XTG_CK(cudaGetLastError());
+    }
 
     // One side on stream `st` with scratch from `scr` (both shadow the call's own).
     auto run_side = [&](bool left, cudaStream_t st, Scratch &scr) -> int {
@@ -490,16 +503,34 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         const int m = m_total;
         const E *Sp = S, *Pp = P;
         int lsp = lds, lpp = ldp;
+        // Left problem: (F S^H F, F P^H F).  Rows [0, t) of S and P become columns [n - t, n) of
+        // the transposed copies; t_done rows are done.  With opt.rows_ready (S and P still on
+        // their way up) each group transposes the rows it needs once they have arrived,
+        // otherwise all rows are transposed here.
+        E *St = nullptr, *Pt = nullptr;
+        int t_done = 0;
+        auto transpose_rows = [&](int t1) {
+            if (t1 <= t_done) return;
+            const int c0 = n - t1, c1 = n - t_done;
+            dim3 g((n + 31) / 32, (c1 - c0 + 31) / 32), b(32, 8);
+            tr.run(kTPrep, 0, 2.0 * n * (c1 - c0) * esz, st,
+                   [&] { rev_transpose_kernel<E><<<g, b, 0, st>>>(S, lds, St, ld_n, n, 1, c0, c1); });
+            if (Pt)
+                tr.run(kTPrep, 0, 2.0 * n * (c1 - c0) * esz, st,
+                       [&] { rev_transpose_kernel<E><<<g, b, 0, st>>>(P, ldp, Pt, ld_n, n, 1, c0, c1); });
+            t_done = t1;
+        };
+        auto left_rows = [&](int need) {  // rows [0, need) of S, P on the device and transposed
+            if (!left || need <= t_done) return;
+            const int got = opt.rows_ready ? std::min(n, std::max(need, opt.rows_ready(need, st))) : n;
+            transpose_rows(got);
+        };
         if (left) {
-            E *St = scr.get<E>((size_t)ld_n * n);
-            E *Pt = opt.p_identity ? nullptr : scr.get<E>((size_t)ld_n * n);  // F I^H F = I
+            St = scr.get<E>((size_t)ld_n * n);
+            Pt = opt.p_identity ? nullptr : scr.get<E>((size_t)ld_n * n);  // F I^H F = I
             if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
-            dim3 g((n + 31) / 32, (n + 31) / 32), b(32, 8);
-            tr.run(kTPrep, 0, 2.0 * n * n * esz, st,
-                   [&] { rev_transpose_kernel<E><<<g, b, 0, st>>>(S, lds, St, ld_n, n, 1); });
+            if (!opt.rows_ready) transpose_rows(n);
             if (Pt) {
-                tr.run(kTPrep, 0, 2.0 * n * n * esz, st,
-                       [&] { rev_transpose_kernel<E><<<g, b, 0, st>>>(P, ldp, Pt, ld_n, n, 1); });
                 Pp = Pt;
                 lpp = ld_n;
             }
@@ -656,6 +687,10 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             const int ge = std::min(nbk, gi + group);  // blocks [gi, ge); blocks[gi] is the lowest
             const int q0 = blocks[ge - 1].first, q1 = blocks[gi].second;
             const int acols = q1 - q0, kq = round_up(acols, kKPad);
+            // the group reads columns [q0, q1) of S and P (right problem: the caller's columns;
+            // left problem: rows [n - q1, n - q0) of the caller's S and P, transposed)
+            if (opt.cols_ready && !left) opt.cols_ready(false, q0, st);
+            left_rows(n - q0);
             for (int bi = gi; bi < ge; bi++) {
                 const int r0 = blocks[bi].first, r1 = blocks[bi].second, jnb = r1 - r0, ys = r0 - q0;
                 // the lowest block also writes the zero padding of the group's operand rows
@@ -694,6 +729,9 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             }
         } guard{st2, ev_main, ev_tr};
         if (ahead) {
+            // the second stream starts from events of this one: all of S and P first
+            if (opt.cols_ready && !left) opt.cols_ready(false, 0, st);
+            left_rows(n);
             // slice buffers of the trailing updates are sized here, on the main stream: growing
             // them inside a launch on the second stream would not be ordered with its use
             if constexpr (std::is_same<E, double>::value) {

@@ -36,6 +36,21 @@ struct Options {
     // only the back-transform needs start from here (an event recorded on this stream), so
     // the copy engine does not queue the small copies that start the solve behind them.
     std::function<void(cudaStream_t st)> staged;
+    // Host-pointer path, real types: S and P reach the device while the call runs, column
+    // panels from the right alternating with row strips from the top.  host_S (lds
+    // host_lds): the caller's S, from which the subdiagonal is read instead of from the
+    // device copy.  host_norms: fills {anorm, bnorm},
+    // the same column sums in the same order as the device reduction (bit-identical), called
+    // once after `staged`.  cols_ready(left, c, st): makes stream st wait until columns
+    // [c, n) of S and P are on the device (asked by the right side before each group of row
+    // blocks).  rows_ready(r, st): makes st wait until rows [0, r) of S and P are on the
+    // device and returns the number of leading rows that are (>= r); the left side asks
+    // before each group and transposes the rows that arrived.
+    const void *host_S = nullptr;
+    int host_lds = 0;
+    std::function<void(double *anorm_bnorm)> host_norms;
+    std::function<void(bool left, int col, cudaStream_t st)> cols_ready;
+    std::function<int(int rows, cudaStream_t st)> rows_ready;
     std::function<void(bool left, cudaStream_t st)> side_done;
     // HOWMNY='B' without normalisation: the back-transform runs in column chunks and this
     // is called after each with the output columns [o0, o1) it completed.

@@ -2,6 +2,7 @@
 // reversal/transposition that turns the left problem into a right problem, the
 // write-back of untransformed eigenvectors, and the final column normalisation.
 #pragma once
+#include <climits>
 #include "common.cuh"
 
 namespace xtg {
@@ -33,6 +34,14 @@ __global__ void colsum_kernel(const E *S, int lds, const E *P, int ldp, int n, i
         sums[col] = ss;
         sums[n + col] = sp;
     }
+}
+
+// norms = {anorm, bnorm} computed by the caller.
+template <class R>
+__global__ void set_norms_kernel(R *norms, R anorm, R bnorm)
+{
+    norms[0] = anorm;
+    norms[1] = bnorm;
 }
 
 // norms[0] = anorm, norms[1] = bnorm (single block).
@@ -137,22 +146,24 @@ template <class R> __device__ __forceinline__ cplx<R> maybe_conj(cplx<R> v, int 
 
 // out(i, j) = f(in(n-1-j, n-1-i)), f = conj when `cj`: the left problem
 // y^H (b S - a P) = 0 becomes the right problem of (F S^H F, F P^H F), F the reversal.
-// 32 x 32 tiles through shared memory.
+// 32 x 32 tiles through shared memory.  Output columns [c0, c1) only (rows n-c1 .. n-c0-1 of
+// in), grid.y = ceil((c1 - c0) / 32); c0 = 0, c1 = n: the whole matrix.
 template <class E>
-__global__ void rev_transpose_kernel(const E *in, int ldi, E *out, int ldo, int n, int cj)
+__global__ void rev_transpose_kernel(const E *in, int ldi, E *out, int ldo, int n, int cj, int c0 = 0, int c1 = INT_MAX)
 {
     __shared__ E tile[32][33];
-    int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+    if (c1 > n) c1 = n;
+    int i0 = blockIdx.x * 32, j0 = c0 + blockIdx.y * 32;
     // read in(n-1-j, n-1-i) for j in [j0, j0+32) (rows of in), i in [i0, i0+32) (cols of in)
     int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
     for (int q = ty; q < 32; q += 8) {
         int j = j0 + tx, i = i0 + q;
-        if (i < n && j < n) tile[q][tx] = in[(size_t)(n - 1 - j) + (size_t)(n - 1 - i) * ldi];
+        if (i < n && j < c1) tile[q][tx] = in[(size_t)(n - 1 - j) + (size_t)(n - 1 - i) * ldi];
     }
     __syncthreads();
     for (int q = ty; q < 32; q += 8) {
         int i = i0 + tx, j = j0 + q;
-        if (i < n && j < n) out[(size_t)i + (size_t)j * ldo] = maybe_conj(tile[tx][q], cj);
+        if (i < n && j < c1) out[(size_t)i + (size_t)j * ldo] = maybe_conj(tile[tx][q], cj);
     }
 }
 
