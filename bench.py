@@ -872,13 +872,27 @@ def main():
     finally:
         X.set_flags(0)
     e2e_s = max_over_ranks(float(np.mean(e2e_t)), dist, torch)
-    # bytes the host path moves: S and P as their upper trapezoid in 512-column panels (rows
-    # <= last column + 1), Q and Z whole in; VL and VR whole out
-    trap = sum(min(n, j0 + 512 + 1) * (min(n, j0 + 512) - j0) for j0 in range(0, n, 512))
+    # bytes the host path moves: S and P as their upper trapezoid (rows <= col + 1) in the
+    # library's pieces (512-column panels from the right alternating with 512-row strips from
+    # the top, each the rest of the trapezoid), Q and Z whole in; VL and VR whole out
+    def trapezoid_pieces(w=512):
+        tot, cf, rt = 0, n, 0
+        while cf >= 1 and rt <= cf:
+            c0 = max(cf - w, 0)
+            tot += (min(n, cf + 1) - rt) * (cf - c0)
+            cf = c0
+            if not (cf >= 1 and rt <= cf):
+                break
+            r1 = min(rt + w, n)
+            tot += (r1 - rt) * (cf - max(rt - 1, 0))
+            rt = r1
+        return tot
+    trap = trapezoid_pieces()
     e2e = {"value": world * 2 * n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": (2 * trap + 2 * n * n) * 8,
            "d2h_bytes_per_step": 2 * n * n * 8, "ms_per_step": 1e3 * e2e_s,
            "path": f"xtgevc3_dtgevc3 (host pointers, pinned), {head} form, H2D/D2H inside the call (S, P "
-                   f"before the solve; Q, Z and the result columns overlapped with it)"}
+                   f"in pieces while the solve runs, norms from host threads; Q, Z and the result columns "
+                   f"overlapped with it)"}
 
     batched = measure_batched(args, X, torch, dist, world) if args.batch_count > 0 else None
     adjoint = measure_adjoint(args, X, torch) if args.adjoint_n > 0 and rank == 0 else None

@@ -28,6 +28,9 @@
  * upstream algorithm (x_k = 1 on the eigenvalue's own row); when the overflow guards fire,
  * this implementation scales single columns where the upstream code scales a 32-column
  * panel, so those columns differ from the upstream output by a positive factor.
+ *
+ * Host-pointer calls of real pencils upload S and P while the solve runs and compute the
+ * pencil norms on up to 32 host threads of their own, joined before the call returns.
  */
 #ifndef XTGEVC3_H
 #define XTGEVC3_H
@@ -51,8 +54,9 @@ extern "C" {
 #define XTGEVC3_SPLIT_INT8 8u
 /* Look-ahead schedule: the trailing update of each pair of row blocks runs on a second
  * stream while the next pair's diagonal solves run (guard rescaling of the rows that
- * update writes is deferred until it has finished).  Same results bit for bit; on B200
- * it measured no faster (the update fills the GPU), so it is off by default. */
+ * update writes is deferred until it has finished).  Same results to rounding (the default
+ * schedule sums the updates of two row blocks in one GEMM); on B200 it measured no faster
+ * (the update fills the GPU), so it is off by default. */
 #define XTGEVC3_LOOKAHEAD 16u
 
 /* Process-wide flags used by the drop-in entry points below (default 0). */
