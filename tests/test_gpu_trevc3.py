@@ -127,3 +127,24 @@ def test_trevc3_empty_selection(cuda_ok):
     VR = np.full((50, 4), 7.0, order="F")
     _, VR2, m, info = X.trevc3("R", "S", T, VR=VR, select=np.zeros(50, dtype=np.int32), mm=4)
     assert (m, info) == (0, 0) and (VR2 == 7.0).all()
+
+
+def test_trevc3_host_pieces_match_device_form(cuda_ok):
+    """n = 1100: the host-pointer form uploads T in three pieces while the solve runs (P = I is
+    built on the device, bnorm = 1 comes from the host with anorm), and its columns equal the
+    device form's bit for bit."""
+    import torch
+    n = 1100
+    T, Q = _schur(np.float64, n, 1100)
+    VL, VR, m, info = X.trevc3("B", "B", T, VL=Q.copy(order="F"), VR=Q.copy(order="F"))
+    assert (m, info) == (n, 0)
+
+    def dev(a):
+        return torch.from_numpy(np.ascontiguousarray(a.T)).cuda().t()
+
+    dVL, dVR = dev(Q), dev(Q)
+    m2, info2 = X.trevc3_dev("B", "B", dev(T), VL=dVL, VR=dVR)
+    torch.cuda.synchronize()
+    assert (m2, info2) == (m, 0)
+    np.testing.assert_array_equal(dVL.cpu().numpy(), VL)
+    np.testing.assert_array_equal(dVR.cpu().numpy(), VR)

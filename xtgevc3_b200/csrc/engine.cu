@@ -174,6 +174,10 @@ void configure_device(int dev)
         cudaFuncSetAttribute(gemm_dmma<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::Tile<128>::SMEM_BYTES);
         cudaFuncSetAttribute(gemm_dmma<0, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::Tile<64>::SMEM_BYTES);
         cudaFuncSetAttribute(gemm_dmma<1, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::Tile<64>::SMEM_BYTES);
+        cudaFuncSetAttribute(gemm_dmma<0, 128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::Tile<128>::SMEM_BYTES);
+        cudaFuncSetAttribute(gemm_dmma<1, 128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::Tile<128>::SMEM_BYTES);
+        cudaFuncSetAttribute(gemm_dmma<0, 64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::Tile<64>::SMEM_BYTES);
+        cudaFuncSetAttribute(gemm_dmma<1, 64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::Tile<64>::SMEM_BYTES);
         cudaFuncSetAttribute(gemm_dmma_cplx<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, zmma::SMEM_BYTES);
         cudaFuncSetAttribute(gemm_dmma_cplx<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, zmma::SMEM_BYTES);
         cudaFuncSetAttribute(split::gemm_split_kernel<split::kBF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,

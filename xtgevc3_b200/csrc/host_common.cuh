@@ -69,22 +69,35 @@ inline void launch_gemm(const GemmArgs<E> &g, bool simt, cudaStream_t st)
         // the cp.async path copies 16-byte pairs of rows: even leading dimensions and
         // 16-byte aligned bases only (caller-given ld may be odd on the device API)
         auto al = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
-        bool ok = (g.ldb % 2 == 0) && al(g.B) && (g.C != nullptr);
-        for (int s = 0; s < g.nseg; s++) ok = ok && (g.seg[s].lda % 2 == 0) && al(g.seg[s].A) && (g.seg[s].boff % 2 == 0);
+        bool ok = (g.ldb % 2 == 0) && al(g.B) && (g.C != nullptr), odd = false;
+        for (int s = 0; s < g.nseg; s++) {
+            ok = ok && (g.seg[s].lda % 2 == 0) && al(g.seg[s].A);
+            odd = odd || (g.seg[s].boff % 2 != 0);  // B rows at an odd offset: 8-byte loads
+        }
         if (!simt && ok) {
             // up to 128 output rows (the update of a group's upper block: 64 or 65): 64-row
             // tiles, so that no tile computes rows past M and twice as many CTAs share the work
             if (g.M <= 128) {
                 using T = dmma::Tile<64>;
                 dim3 grid((g.M + 63) / 64, (g.N + dmma::BN - 1) / dmma::BN);
-                if (g.accumulate) gemm_dmma<1, 64><<<grid, T::NT, T::SMEM_BYTES, st>>>(g);
-                else gemm_dmma<0, 64><<<grid, T::NT, T::SMEM_BYTES, st>>>(g);
+                if (g.accumulate) {
+                    if (odd) gemm_dmma<1, 64, true><<<grid, T::NT, T::SMEM_BYTES, st>>>(g);
+                    else gemm_dmma<1, 64><<<grid, T::NT, T::SMEM_BYTES, st>>>(g);
+                } else {
+                    if (odd) gemm_dmma<0, 64, true><<<grid, T::NT, T::SMEM_BYTES, st>>>(g);
+                    else gemm_dmma<0, 64><<<grid, T::NT, T::SMEM_BYTES, st>>>(g);
+                }
                 return;
             }
             using T = dmma::Tile<128>;
             dim3 grid((g.M + 127) / 128, (g.N + dmma::BN - 1) / dmma::BN);
-            if (g.accumulate) gemm_dmma<1><<<grid, T::NT, T::SMEM_BYTES, st>>>(g);
-            else gemm_dmma<0><<<grid, T::NT, T::SMEM_BYTES, st>>>(g);
+            if (g.accumulate) {
+                if (odd) gemm_dmma<1, 128, true><<<grid, T::NT, T::SMEM_BYTES, st>>>(g);
+                else gemm_dmma<1><<<grid, T::NT, T::SMEM_BYTES, st>>>(g);
+            } else {
+                if (odd) gemm_dmma<0, 128, true><<<grid, T::NT, T::SMEM_BYTES, st>>>(g);
+                else gemm_dmma<0><<<grid, T::NT, T::SMEM_BYTES, st>>>(g);
+            }
             return;
         }
     }

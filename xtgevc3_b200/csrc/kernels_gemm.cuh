@@ -144,7 +144,8 @@ __global__ void __launch_bounds__(256) gemm_simt(GemmArgs<E> g)
 // update of a group's upper block), K step 16, BM/32 x 2 warps with 32 x 32 warp tiles,
 // 3-stage cp.async pipeline into padded shared memory (conflict-free fragment loads).
 // Requires 16-byte aligned segment bases and B, and even leading dimensions (checked by
-// the launcher, which uses the SIMT kernel otherwise).
+// the launcher, which uses the SIMT kernel otherwise); B rows at an odd offset (a block
+// boundary moved by a 2x2 block) take the BODD loader.
 // ------------------------------------------------------------------------------------
 namespace dmma {
 constexpr int BN = 64, BK = 16, STAGES = 3;  // BK divides kKPad (segment K)
@@ -164,6 +165,12 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src
     unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
 }
+// 8 bytes (8-byte aligned addresses; the 16-byte form needs 16-byte alignment)
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, int src_bytes)
+{
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
@@ -176,7 +183,9 @@ __device__ __forceinline__ void dmma884(double &d0, double &d1, double a, double
 }
 
 // ACC = 1: trailing update (C += A B); ACC = 0: back-transform (C = A B, triangular B).
-template <int ACC, int BM = 128>
+// BODD: some segment's B rows start at an odd offset (boff), so its row pairs are only
+// 8-byte aligned and load as two 8-byte copies.
+template <int ACC, int BM = 128, bool BODD = false>
 __global__ void __launch_bounds__(2 * BM) gemm_dmma(GemmArgs<double> g)
 {
     using namespace dmma;
@@ -230,7 +239,12 @@ __global__ void __launch_bounds__(2 * BM) gemm_dmma(GemmArgs<double> g)
             int bytes = 0;
             if (s >= 0 && col < g.N) bytes = kr + 1 < lim ? 16 : (kr < lim ? 8 : 0);
             const double *gp = bytes ? g.B + (size_t)kr + (size_t)col * g.ldb : g.B;
-            cp_async16(bs + nn * BLD + 2 * ch, gp, bytes);
+            if constexpr (BODD) {
+                cp_async8(bs + nn * BLD + 2 * ch, gp, bytes ? 8 : 0);
+                cp_async8(bs + nn * BLD + 2 * ch + 1, bytes == 16 ? gp + 1 : g.B, bytes == 16 ? 8 : 0);
+            } else {
+                cp_async16(bs + nn * BLD + 2 * ch, gp, bytes);
+            }
         }
     };
 
