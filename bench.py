@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--adjoint-c-n", type=int, default=128)
     ap.add_argument("--z-n", type=int, default=4096, help="order of the ztgevc3 SIDE=R HOWMNY=A leg (0 skips)")
     ap.add_argument("--trevc3-n", type=int, default=8192, help="order of the dtrevc3 SIDE=B HOWMNY=B leg (0 skips)")
+    ap.add_argument("--tgexc-n", type=int, default=4096, help="order of the ztgexc reordering leg (0 skips)")
     ap.add_argument("--profile-case", default=None,
                     help="run one small case for an ncu capture and exit (no JSON line): plain:N (two dtgevc3 "
                          "B/B calls, FP64), split_i8:N (the same, INT8 split form), batch:COUNT (two launches "
@@ -608,6 +609,53 @@ def measure_ztgevc3(args, X, torch):
                     "graded: rows of P scaled by 10^U(-8,8)", **out}
 
 
+def measure_tgexc(args, X, torch):
+    """ztgexc: the last eigenvalue of a complex upper-triangular pencil of order --tgexc-n moves
+    to the top (n - 1 swaps), Q and Z updated (Q = Z = I: the rotations cost the same whatever
+    their values); device-resident inputs restored before each step outside the timed region,
+    CUDA-event timing; LAPACK ZTGEXC (SciPy's OpenBLAS) on the same input and move beside it,
+    with the largest difference between the two results."""
+    from xtgevc3_b200 import pencils as gen
+    n = args.tgexc_n
+    S_h, P_h, _, _ = gen.gen_upper_triangular_complex(n, args.seed + 41)
+    S0, P0 = colmajor_cuda(S_h, torch), colmajor_cuda(P_h, torch)
+    I0 = torch.eye(n, dtype=torch.complex128, device="cuda")
+    A, B, Q, Z = (torch.empty_like(S0) for _ in range(4))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ts, res = [], None
+    warm = max(args.warmup, 1)
+    for it in range(warm + args.steps):
+        A.copy_(S0)
+        B.copy_(P0)
+        Q.copy_(I0)
+        Z.copy_(I0)
+        torch.cuda.synchronize()
+        e0.record()
+        res = X.tgexc_dev(A, B, Q, Z, n, 1)
+        e1.record()
+        torch.cuda.synchronize()
+        if it >= warm:
+            ts.append(e0.elapsed_time(e1))
+    ms = float(np.mean(ts))
+    out = {"n": n, "move": f"{n} -> 1", "swaps": n - 1, "ilst_info": list(res), "ms": ms,
+           "swaps_per_s": (n - 1) / (ms * 1e-3),
+           "data": "complex upper-triangular stand-in pencil (U(-1,1) parts, |P_kk| kept away from 0), Q = Z = I"}
+    if not args.no_cpu:
+        import oracle
+        Ih = np.eye(n, dtype=np.complex128, order="F")
+        t0 = time.perf_counter()
+        ra, rb, rq, rz, rinfo = oracle.lapack_tgexc(S_h, P_h, Ih, Ih.copy(order="F"), n, 1)
+        tc = time.perf_counter() - t0
+        diff = 0.0
+        for D, R in ((A, ra), (B, rb), (Q, rq), (Z, rz)):
+            diff = max(diff, float(np.abs(D.cpu().numpy() - R).max() / np.abs(R).max()))
+        out["cpu_lapack"] = {"seconds": tc, "swaps_per_s": (n - 1) / tc, "cores": host_threads(), "info": int(rinfo),
+                             "kind": "LAPACK ztgexc (SciPy OpenBLAS), one call"}
+        out["max_rel_diff_vs_lapack"] = diff
+    del S0, P0, I0, A, B, Q, Z
+    return out
+
+
 def schur_stand_in(n, seed):
     """Stand-in for the real Schur factor T of an n x n iid N(0,1) matrix (host, Fortran):
     strictly upper part N(0,1); about sqrt(2n/pi) real eigenvalues, uniform on [-sqrt(n),
@@ -898,6 +946,7 @@ def main():
     adjoint = measure_adjoint(args, X, torch) if args.adjoint_n > 0 and rank == 0 else None
     zleg = measure_ztgevc3(args, X, torch) if args.z_n > 0 and rank == 0 else None
     trleg = measure_trevc3(args, X, torch) if args.trevc3_n > 0 and rank == 0 else None
+    txleg = measure_tgexc(args, X, torch) if args.tgexc_n > 0 and rank == 0 else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -929,7 +978,7 @@ def main():
                            "resid_max": h["resid"], "resid_bound": 1e-12},
                 "forms": forms_out, "clocks": h["clocks"], "e2e": e2e, "gpu_launches": h["launches"],
                 "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "batched": batched,
-                "adjoint": adjoint, "ztgevc3": zleg, "dtrevc3": trleg}
+                "adjoint": adjoint, "ztgevc3": zleg, "dtrevc3": trleg, "ztgexc": txleg}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

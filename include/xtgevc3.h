@@ -194,6 +194,26 @@ int xtgevc3_ctgsna_dev(void *stream, char job, char howmny, const int *select, i
                        const float *B, int ldb, const float *VL, int ldvl, const float *VR, int ldvr, float *s, int mm,
                        int *m, int *info);
 
+/* ---- eigenvalue reordering, complex pencils: xTGEXC (no counterpart upstream) ---------
+ * Moves the eigenvalue at row ifst of the complex generalized Schur pencil (A, B) (upper
+ * triangular) to row ilst by swaps of adjacent diagonal entries, each an equivalence
+ * transformation by two rotations, and applies them to Q (wantq != 0) and Z (wantz != 0):
+ * LAPACK ZTGEXC / CTGEXC's arguments (Fortran references become values for inputs), INFO
+ * codes and results.  ifst, *ilst are 1-based.  On return *ilst is the eigenvalue's row;
+ * INFO = 1: a swap failed the stability tests, the pencil is reordered up to it and *ilst
+ * is the first row of that swap (as in LAPACK); INFO = -3 N, -5 LDA, -7 LDB, -9 LDQ,
+ * -11 LDZ, -12 IFST, -13 ILST.  Complex arrays interleaved.  Device forms: A, B, Q, Z
+ * device pointers, the call returns once the reordering is done (0, or 1 when a CUDA call
+ * failed).  Real pencils (2x2 blocks) are not covered. */
+void xtgevc3_ztgexc(int wantq, int wantz, int n, double *A, int lda, double *B, int ldb, double *Q, int ldq, double *Z,
+                    int ldz, int ifst, int *ilst, int *info);
+void xtgevc3_ctgexc(int wantq, int wantz, int n, float *A, int lda, float *B, int ldb, float *Q, int ldq, float *Z,
+                    int ldz, int ifst, int *ilst, int *info);
+int xtgevc3_ztgexc_dev(void *stream, int wantq, int wantz, int n, double *A, int lda, double *B, int ldb, double *Q,
+                       int ldq, double *Z, int ldz, int ifst, int *ilst, int *info);
+int xtgevc3_ctgexc_dev(void *stream, int wantq, int wantz, int n, float *A, int lda, float *B, int ldb, float *Q,
+                       int ldq, float *Z, int ldz, int ifst, int *ilst, int *info);
+
 /* ---- allocation-free device entry point (no counterpart in the upstream library) -----
  * Same computation and arguments as xtgevc3_dtgevc3_dev (without flags), for callers that
  * cannot allocate device memory at this point: e.g. a framework that has reserved the

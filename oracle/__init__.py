@@ -237,6 +237,30 @@ def lapack_tgsna(howmny, A, B, VL, VR, select=None):
     return S[:m.value], m.value, info.value
 
 
+def lapack_tgexc(A, B, Q, Z, ifst, ilst):
+    """Oracle of the complex xTGEXC entry points: LAPACK ZTGEXC / CTGEXC through SciPy
+    (ifst, ilst 1-based; Q, Z may be None: not updated).  Returns (A, B, Q, Z, info)."""
+    import scipy.linalg.lapack as lapack
+    f = getattr(lapack, {np.complex128: "ztgexc", np.complex64: "ctgexc"}[A.dtype.type])
+    n = A.shape[0]
+    wq, wz = Q is not None, Z is not None
+    Qa = Q if wq else np.eye(n, dtype=A.dtype)
+    Za = Z if wz else np.eye(n, dtype=A.dtype)
+    a, b, q, z, info = f(A, B, Qa, Za, ifst, ilst, wantq=int(wq), wantz=int(wz))
+    return a, b, (q if wq else None), (z if wz else None), info
+
+
+def complex_schur_pencil(n, seed, dtype=np.complex128):
+    """Complex generalized Schur form (LAPACK xGGES through SciPy's qz) of a pencil with iid
+    complex N(0,1) entries: returns (A, B, Q, Z) with the original pencil = (Q A Z^H, Q B Z^H)."""
+    import scipy.linalg
+    rng = np.random.default_rng(seed)
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    b = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    AA, BB, Q, Z = scipy.linalg.qz(a.astype(dtype), b.astype(dtype), output="complex")
+    return tuple(np.asfortranarray(M.astype(dtype)) for M in (AA, BB, Q, Z))
+
+
 def schur_real(n, seed, dtype=np.float64):
     """Real Schur form of an iid N(0,1) matrix (LAPACK xGEES through SciPy: T quasi-upper
     triangular with standardised 2x2 blocks, Q orthogonal)."""

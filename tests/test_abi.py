@@ -265,3 +265,32 @@ def test_tgsna_info_codes_and_query():
     assert call(lwork=0)[0] == -18
     info, m, work = call(lwork=-1)
     assert (info, m, int(work[0])) == (0, n, n)
+
+
+def test_tgexc_info_codes_and_quick_returns():
+    """xtgevc3_ztgexc: LAPACK ZTGEXC's INFO codes in its order (-3 N, -5 LDA, -7 LDB, -9 LDQ,
+    -11 LDZ, -12 IFST, -13 ILST), answered before any CUDA call, and its quick returns
+    (N <= 1, IFST = ILST) with the pencil untouched."""
+    n = 5
+    A = np.asfortranarray(np.triu(np.arange(1.0, n * n + 1).reshape(n, n)).astype(np.complex128))
+    A0 = A.copy()
+    L = X.lib()
+
+    def call(wq=1, wz=1, nn=n, lda=n, ldb=n, ldq=n, ldz=n, ifst=1, ilst=3):
+        il, info = ct.c_int(ilst), ct.c_int(7)
+        L.xtgevc3_ztgexc(wq, wz, nn, A.ctypes.data, lda, A.ctypes.data, ldb, A.ctypes.data, ldq, A.ctypes.data, ldz,
+                         ifst, ct.byref(il), ct.byref(info))
+        return info.value, il.value
+    assert call(nn=-1)[0] == -3
+    assert call(lda=n - 1)[0] == -5
+    assert call(ldb=n - 1)[0] == -7
+    assert call(ldq=n - 1)[0] == -9
+    assert call(ldq=0, wq=0)[0] == -9
+    assert call(ldq=1, wq=0, ldz=n - 1)[0] == -11
+    assert call(ldz=0, wz=0)[0] == -11
+    assert call(ifst=0)[0] == -12 and call(ifst=n + 1)[0] == -12
+    assert call(ilst=0)[0] == -13 and call(ilst=n + 1)[0] == -13
+    assert call(nn=0, ifst=1, ilst=1)[0] == -12  # IFST > N
+    assert call(nn=1, ifst=1, ilst=1, lda=1, ldb=1, ldq=1, ldz=1) == (0, 1)
+    assert call(ifst=3, ilst=3) == (0, 3)
+    assert (A == A0).all()

@@ -1,0 +1,81 @@
+"""xtgevc3_{z,c}tgexc (eigenvalue reordering of a complex generalized Schur pencil) against
+LAPACK ZTGEXC / CTGEXC.
+
+The oracle is LAPACK's own xTGEXC from SciPy, given the same pencil (the complex generalized
+Schur form of a pencil with iid complex N(0,1) entries, LAPACK xGGES through SciPy's qz)
+and the same move.  Both apply the same rotations with real cosines >= 0, so A, B, Q and Z
+agree to rounding.  Tolerance: elementwise difference relative to the matrix's largest
+entry, 1e-12 (double) / 2e-4 (single).
+"""
+import numpy as np
+import pytest
+
+import oracle
+import xtgevc3_b200 as X
+
+pytestmark = pytest.mark.gpu
+
+TOL = {np.complex128: 1e-12, np.complex64: 2e-4}
+
+
+def _rel(M, R):
+    return float(np.abs(M - R).max() / max(np.abs(R).max(), 1e-300))
+
+
+MOVES = [(4, 31), (36, 3), (1, 40), (40, 1), (11, 12), (12, 11)]
+
+
+@pytest.mark.parametrize("dt", [np.complex128, np.complex64], ids=["z", "c"])
+@pytest.mark.parametrize("move", MOVES, ids=lambda m: f"{m[0]}to{m[1]}")
+def test_tgexc_matches_lapack(cuda_ok, dt, move):
+    ifst, ilst = move
+    A, B, Q, Z = oracle.complex_schur_pencil(40, 3, dt)
+    ra, rb, rq, rz, rinfo = oracle.lapack_tgexc(A, B, Q, Z, ifst, ilst)
+    a, b, q, z, il, info = X.tgexc(A, B, Q, Z, ifst, ilst)
+    assert (info, il) == (rinfo, ilst) == (0, ilst)
+    tol = TOL[dt]
+    for M, R in ((a, ra), (b, rb), (q, rq), (z, rz)):
+        assert _rel(M, R) < tol
+    # the moved eigenvalue sits at ilst, the pencil is still triangular
+    k = ilst - 1
+    assert abs(a[k, k] / b[k, k] - A[ifst - 1, ifst - 1] / B[ifst - 1, ifst - 1]) < 1e3 * tol * abs(A[ifst - 1, ifst - 1] / B[ifst - 1, ifst - 1])
+    assert (np.tril(a, -1) == 0).all() and (np.tril(b, -1) == 0).all()
+
+
+def test_tgexc_without_q_z(cuda_ok):
+    """wantq = wantz = 0: A and B as LAPACK's, Q and Z not referenced."""
+    A, B, Q, Z = oracle.complex_schur_pencil(60, 8)
+    ra, rb, _, _, rinfo = oracle.lapack_tgexc(A, B, None, None, 50, 2)
+    a, b, q, z, il, info = X.tgexc(A, B, None, None, 50, 2)
+    assert (info, il, q, z) == (0, 2, None, None)
+    assert _rel(a, ra) < 1e-12 and _rel(b, rb) < 1e-12
+
+
+def test_tgexc_long_move_and_invariants(cuda_ok):
+    """n = 400, the last eigenvalue to the top (399 swaps): LAPACK's result to rounding, and
+    Q A Z^H, Q B Z^H unchanged."""
+    A, B, Q, Z = oracle.complex_schur_pencil(400, 5)
+    ra, rb, rq, rz, _ = oracle.lapack_tgexc(A, B, Q, Z, 400, 1)
+    a, b, q, z, il, info = X.tgexc(A, B, Q, Z, 400, 1)
+    assert (info, il) == (0, 1)
+    for M, R in ((a, ra), (b, rb), (q, rq), (z, rz)):
+        assert _rel(M, R) < 1e-11
+    for M, M0 in ((a, A), (b, B)):
+        assert np.abs(q @ M @ z.conj().T - Q @ M0 @ Z.conj().T).max() < 1e-12 * np.abs(M0).max() * 400
+
+
+def test_tgexc_device_form_matches_host_form(cuda_ok):
+    """xtgevc3_ztgexc_dev on column-major CUDA tensors gives the host form's arrays bit for bit."""
+    import torch
+    A, B, Q, Z = oracle.complex_schur_pencil(120, 9)
+    a, b, q, z, il, info = X.tgexc(A, B, Q, Z, 100, 5)
+
+    def dev(M):
+        return torch.from_numpy(np.ascontiguousarray(M.T)).cuda().t()
+
+    dA, dB, dQ, dZ = dev(A), dev(B), dev(Q), dev(Z)
+    il2, info2 = X.tgexc_dev(dA, dB, dQ, dZ, 100, 5)
+    torch.cuda.synchronize()
+    assert (il2, info2) == (il, info) == (5, 0)
+    for D, H in ((dA, a), (dB, b), (dQ, q), (dZ, z)):
+        np.testing.assert_array_equal(D.cpu().numpy(), H)
