@@ -249,12 +249,13 @@ int run_host(char side, char howmny, const int *select, int n, const void *S, in
         opt.lapack_pairs = 1;
         opt.normalize = 1;
     }
-    // Q and Z (second stream) go after every copy that the solve's first kernels need: S and
-    // P, the eigenvalues and the column lists (the solver calls `staged` once those are
-    // queued).  The back-transform needs Q or Z only at the end; queued earlier, their 2n^2
-    // elements would hold the small copies behind them on the copy engine and split the
-    // link's host-to-device bandwidth with S and P.  The wait also orders the second stream
-    // after the allocations of the output buffers it writes.
+    // The input stream's copies (S and P of real pencils, then Q and Z) go after every copy
+    // that the solve's first kernels need: the eigenvalues and the column lists (the solver
+    // calls `staged` once those are queued).  Queued earlier, their elements would hold those
+    // small copies behind them on the copy engine; Q and Z, which only the back-transforms
+    // need, go last so as not to split the link's bandwidth with S and P.  The wait also
+    // orders the input stream after the zeroing of S and P and the allocations of the
+    // buffers it writes.
     cudaError_t in_err = cudaSuccess;
     // stream q waits for the first piece after which `done` holds (columns [col, n) or rows
     // [0, rows) all up; the last piece completes everything).  Function scope: opt's hooks
@@ -334,7 +335,7 @@ int run_host(char side, char howmny, const int *select, int n, const void *S, in
     int rc = xtg::solve_device<R, CPLX>(side, howmny, select, n, r.dS, ld, r.dP, ld, alpha, alphai, beta,
                                         want_l ? r.dVL : nullptr, ld, want_r ? r.dVR : nullptr, ld, count, opt, r.st);
     if (rc) return 1;
-    if (in_err != cudaSuccess) return fail(in_err, "H2D Q/Z");
+    if (in_err != cudaSuccess) return fail(in_err, "H2D of S, P, Q, Z or a wait for it");
     if (out_err != cudaSuccess) return fail(out_err, "D2H");
     if ((e = cudaStreamSynchronize(r.sout)) != cudaSuccess) return fail(e, "cudaStreamSynchronize");
     cudaFreeAsync(r.dS, r.st);
