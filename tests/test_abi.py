@@ -294,3 +294,14 @@ def test_tgexc_info_codes_and_quick_returns():
     assert call(nn=1, ifst=1, ilst=1, lda=1, ldb=1, ldq=1, ldz=1) == (0, 1)
     assert call(ifst=3, ilst=3) == (0, 3)
     assert (A == A0).all()
+
+
+def test_tgexc_python_wrapper_argument_errors():
+    """xtgevc3_b200.tgexc passes 1-based positions through: out-of-range IFST / ILST come back
+    as LAPACK's -12 / -13 (no CUDA call), with the arrays unchanged."""
+    n = 4
+    A = np.triu(np.ones((n, n), dtype=np.complex128))
+    for ifst, ilst, code in ((0, 2, -12), (n + 1, 2, -12), (2, 0, -13), (2, n + 1, -13)):
+        a, b, q, z, il, info = X.tgexc(A, A, A, A, ifst, ilst)
+        assert info == code and il == ilst
+        assert (a == A).all() and (q == A).all()
