@@ -222,9 +222,11 @@ int xtgevc3_ctgexc_dev(void *stream, int wantq, int wantz, int n, float *A, int 
  * is one 8 MiB block of device memory inside the library, held on every GPU that loads
  * the library until exit, so problems are limited to what fits (SIDE='B', HOWMNY='B':
  * n <= 478); larger ones return 2 with a message in xtgevc3_last_error(), without device
- * work.  The first call on a device looks up the block's device address (make it before
- * any stream capture).  All calls share the block: calls whose work overlaps on the GPU
- * race and must be ordered by the caller (e.g. one stream).
+ * work.  The first call on a device looks up the block's device address (a failed lookup
+ * is retried by the next call).  Every call blocks the calling thread until its result is
+ * complete (it synchronises its stream), so it cannot be used inside a stream capture.
+ * All calls share the block: calls whose work overlaps on the GPU race and must be
+ * ordered by the caller (e.g. one stream).
  * Returns 0, 1 (CUDA failure, *info = 1) or 2 (too large).                              */
 int xtgevc3_dtgevc3_dev_noalloc(void *stream, char side, char howmny, const int *select, int n, const double *S,
                                 int lds, const double *P, int ldp, const double *alphar, const double *alphai,

@@ -27,10 +27,14 @@ REF_SO = os.path.join(HERE, "_ref", "libref_tgevc3.so")
 _libs: dict = {}
 
 
-def build(ref: bool = False) -> None:
-    """Compile the C restatement (and, with ``ref``, the upstream sources)."""
+def build(ref: bool | str = False) -> None:
+    """Compile the C restatement; with ``ref=True`` also the upstream sources (an error
+    when they are missing), with ``ref="if-present"`` only where the upstream tree is found
+    (its location: the Makefile's REFDIR, overridable by XTGEVC3_REFERENCE_DIR)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    if ref:
+    if ref == "if-present":
+        subprocess.run(["make", "-s", "-C", HERE, "ref-if-present"], check=True)
+    elif ref:
         subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
 
 
@@ -248,6 +252,26 @@ def lapack_tgexc(A, B, Q, Z, ifst, ilst):
     Za = Z if wz else np.eye(n, dtype=A.dtype)
     a, b, q, z, info = f(A, B, Qa, Za, ifst, ilst, wantq=int(wq), wantz=int(wz))
     return a, b, (q if wq else None), (z if wz else None), info
+
+
+def lapack_tgexc_ilst(A, B, Q, Z, ifst, ilst):
+    """LAPACK ZTGEXC / CTGEXC called through its Fortran interface in SciPy's OpenBLAS, so
+    that ILST on exit is returned as well (SciPy's wrapper drops it): on a rejected swap it
+    is the row the eigenvalue had reached.  Q, Z are updated (WANTQ = WANTZ = true).
+    Returns (A, B, Q, Z, ilst, info)."""
+    dt = A.dtype.type
+    pfx = {np.complex128: "z", np.complex64: "c"}[dt]
+    f = getattr(_openblas(), f"scipy_{pfx}tgexc_")
+    n = A.shape[0]
+    A, B, Q, Z = (np.asfortranarray(M).copy(order="F") for M in (A, B, Q, Z))
+    iv = lambda v: ct.byref(ct.c_int(v))  # noqa: E731
+    f_ = ct.c_int(ifst)
+    l_ = ct.c_int(ilst)
+    info = ct.c_int(0)
+    ld = max(n, 1)
+    f(iv(1), iv(1), iv(n), _ptr(A), iv(ld), _ptr(B), iv(ld), _ptr(Q), iv(ld), _ptr(Z), iv(ld), ct.byref(f_),
+      ct.byref(l_), ct.byref(info))
+    return A, B, Q, Z, l_.value, info.value
 
 
 def complex_schur_pencil(n, seed, dtype=np.complex128):

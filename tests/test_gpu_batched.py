@@ -213,3 +213,31 @@ def test_batched_fp32_graded_pencils_stay_finite(cuda_ok):
                                       left=side == "L") * scale
             assert r.max() < 100, (h["n"], side, r.max())
     b.close()
+
+
+def test_batched_ready_wait_expires_and_reports(cuda_ok, monkeypatch):
+    """The bounded wait of a compute unit for its pencil's ready flag runs out: pencil 1's
+    prep unit is left out of the plan (XTGEVC3_BATCH_WITHHOLD_READY), so its flag is never
+    set, and the poll limit is shortened (XTGEVC3_BATCH_SPIN_LIMIT).  The kernel must end,
+    xtgevc3_batched_wait must return 3 with its message, the other pencils must still be
+    right, and a normal plan in the same process must then run cleanly."""
+    hp = [host_pencil("gges", n, 1100 + n, np.float64) for n in (70, 120, 40)]
+    db = device_batch(hp, "B", "B")
+    monkeypatch.setenv("XTGEVC3_BATCH_SPIN_LIMIT", "2000")
+    monkeypatch.setenv("XTGEVC3_BATCH_WITHHOLD_READY", "1")
+    b = X.Batch("B", "B", db)
+    monkeypatch.delenv("XTGEVC3_BATCH_SPIN_LIMIT")
+    monkeypatch.delenv("XTGEVC3_BATCH_WITHHOLD_READY")
+    b.run()
+    with pytest.raises(RuntimeError, match=r"batched wait \(3\).*bounded wait"):
+        b.wait()
+    b.close()
+    for i in (0, 2):
+        check(hp[i], db[i], "B", "B")
+    db2 = device_batch(hp, "B", "B")
+    b2 = X.Batch("B", "B", db2)
+    b2.run()
+    b2.wait()
+    for h, d in zip(hp, db2):
+        check(h, d, "B", "B")
+    b2.close()

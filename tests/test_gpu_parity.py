@@ -416,3 +416,28 @@ def test_split_form_guards_across_groups(cuda_ok, sk, side):
     assert (np.abs(np.diag(V[:, :n])) < 1).sum() >= 8
     ref = oracle.tgevc3(side, "A", S, P, ar, be, alphai=ai)
     compare(d, VL, VR, m, ref[0], ref[1], TOL_ILL[np.float64], check_resid=False)
+
+
+def test_config_dgges_n1024_both_sides_back_transformed(cuda_ok):
+    """The plain dtgevc3 configuration at its own size: a real pencil of order 1024 made by
+    xGGES (ordering off) from seeded iid N(0,1) A, B, SIDE='B', HOWMNY='B' with Q and Z.
+    Against the upstream library built from its sources (oracle/_ref; the C restatement
+    where that library is absent): INFO and M equal, every column within 1e-11 of the column
+    max after normalisation; and the DGET52-style residual of the back-transformed
+    eigenvectors against the original pencil (A, B) = (Q S Z^T, Q P Z^T) below 100."""
+    n = 1024
+    S, P, ar, ai, be, Q, Z = pencils.gen_gges(n, 1024)
+    impl = "ref" if oracle.ref_available() else "oracle"
+    RL, RR, mr, infor = oracle.tgevc3("B", "B", S, P, ar, be, alphai=ai, VL=Q.copy(order="F"),
+                                      VR=Z.copy(order="F"), impl=impl)
+    VL, VR, m, info = X.tgevc3("B", "B", S, P, ar, be, alphai=ai, VL=Q.copy(order="F"), VR=Z.copy(order="F"))
+    assert (m, info) == (mr, infor) == (n, 0)
+    A, B = Q @ S @ Z.T, Q @ P @ Z.T
+    al, bc = oracle.column_eigenvalues(ar, be, alphai=ai)
+    for side, V, R in (("L", VL, RL), ("R", VR, RR)):
+        a = oracle.to_complex_real_storage(V, ai)
+        b = oracle.to_complex_real_storage(R, ai)
+        err, cols = oracle.max_rel_diff(a, b)
+        assert err <= 1e-11, (side, err, int(np.nanargmax(cols)))
+        r = oracle.residual_ratio(A, B, a, al, bc, left=(side == "L"))
+        assert r.max() < 100, (side, r.max())

@@ -79,3 +79,26 @@ def test_tgexc_device_form_matches_host_form(cuda_ok):
     assert (il2, info2) == (il, info) == (5, 0)
     for D, H in ((dA, a), (dB, b), (dQ, q), (dZ, z)):
         np.testing.assert_array_equal(D.cpu().numpy(), H)
+
+
+def test_tgexc_rejected_swap_matches_lapack(cuda_ok):
+    """Badly scaled 3 x 3 pencils on which LAPACK ZTGEXC rejects a swap (fixture made by
+    tests/golden/make_tgexc_rejections.py): forward and backward moves where swaps were
+    applied before the rejection, and one more.  INFO = 1, the returned ILST (the row the
+    eigenvalue had reached) and A, B, Q, Z (the accepted swaps kept) must equal LAPACK's;
+    entries span hundreds of orders of magnitude, so each matrix is compared column by
+    column relative to that column's largest entry."""
+    import os
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "tgexc", "z_rejections.npz"))
+    for i in range(3):
+        A, B, mv = d[f"A{i}"], d[f"B{i}"], d[f"move{i}"]
+        ifst, ilst = int(mv[0]), int(mv[1])
+        I = np.eye(3, dtype=np.complex128, order="F")
+        ra, rb, rq, rz, ril, rinfo = oracle.lapack_tgexc_ilst(A, B, I, I, ifst, ilst)
+        assert rinfo == 1
+        a, b, q, z, il, info = X.tgexc(A, B, I.copy(order="F"), I.copy(order="F"), ifst, ilst)
+        assert (info, il) == (rinfo, ril), (i, info, il, rinfo, ril)
+        for M, R in ((a, ra), (b, rb), (q, rq), (z, rz)):
+            den = np.abs(R).max(0)
+            den[den == 0] = 1.0
+            assert float((np.abs(M - R).max(0) / den).max()) < 1e-12, i

@@ -5,9 +5,12 @@ Both are called through the C ABI on the same inputs; the allocation-free one ta
 scratch from the 8 MiB block inside the library instead of the CUDA memory pool.  Two
 calls in a row (different sizes, the second smaller, so anything left in the shared block
 by the first call would show), each compared column by column within the tolerance the
-parity tests use for xGGES pencils (1e-11 of the column max).  A problem larger than the
-block must be refused with return code 2 before any device work.
+parity tests use for xGGES pencils (1e-11 of the column max), and the first also against
+the CPU oracle.  The largest accepted order (SIDE='B', HOWMNY='B', n = 478) runs and
+matches; one more (n = 479) and larger problems are refused with return code 2 before any
+device work.
 """
+import oracle
 import ctypes as ct
 
 import numpy as np
@@ -48,33 +51,52 @@ def _max_col_err(A, B):
     return float((np.abs(A - B).max(0) / den).max())
 
 
+def _check_case(torch, n, seed, side, howmny, sel, against_oracle):
+    S, P, ar, ai, be, Q, Z = pencils.gen_gges(n, seed)
+    dS, dP = _colmajor(S, torch), _colmajor(P, torch)
+    VL1, VR1 = _colmajor(Q, torch), _colmajor(Z, torch)
+    m1, info1 = X.tgevc3_dev(side, howmny, dS, dP, ar, be, alphai=ai, VL=VL1, VR=VR1, select=sel)
+    torch.cuda.synchronize()
+    VL2, VR2 = _colmajor(Q, torch), _colmajor(Z, torch)
+    rc, m2, info2 = _noalloc(torch, side, howmny, dS, dP, ar, ai, be, VL2, VR2, select=sel)
+    assert rc == 0, X.last_error()
+    assert (m2, info2) == (m1, info1) and info2 == 0
+    if against_oracle:
+        RL, RR, mr, infor = oracle.tgevc3(side, howmny, S, P, ar, be, alphai=ai, VL=Q.copy(order="F"),
+                                          VR=Z.copy(order="F"), select=sel)
+        assert (mr, infor) == (m2, 0)
+    for k, (A, B) in enumerate(((VL2, VL1), (VR2, VR1))):
+        a = A.t().cpu().numpy().T[:, :m2]
+        b = B.t().cpu().numpy().T[:, :m1]
+        assert np.isfinite(a).all()
+        assert _max_col_err(a, b) <= TOL
+        if against_oracle:
+            R = (RL, RR)[k][:, :m2]
+            err, _ = oracle.max_rel_diff(oracle.to_complex_real_storage(a, ai, howmny, sel),
+                                         oracle.to_complex_real_storage(R, ai, howmny, sel))
+            assert err <= TOL, err
+
+
 def test_noalloc_matches_regular_entry_point_twice(cuda_ok):
     import torch
     rng = np.random.default_rng(5)
-    cases = [(300, 61, "B", "B", None), (170, 62, "B", "S", (rng.random(170) < 0.4).astype(np.int32))]
-    for n, seed, side, howmny, sel in cases:
-        S, P, ar, ai, be, Q, Z = pencils.gen_gges(n, seed)
-        dS, dP = _colmajor(S, torch), _colmajor(P, torch)
-        VL1, VR1 = _colmajor(Q, torch), _colmajor(Z, torch)
-        m1, info1 = X.tgevc3_dev(side, howmny, dS, dP, ar, be, alphai=ai, VL=VL1, VR=VR1, select=sel)
-        torch.cuda.synchronize()
-        VL2, VR2 = _colmajor(Q, torch), _colmajor(Z, torch)
-        rc, m2, info2 = _noalloc(torch, side, howmny, dS, dP, ar, ai, be, VL2, VR2, select=sel)
-        assert rc == 0, X.last_error()
-        assert (m2, info2) == (m1, info1) and info2 == 0
-        for A, B in ((VL2, VL1), (VR2, VR1)):
-            a = A.t().cpu().numpy().T[:, :m2]
-            b = B.t().cpu().numpy().T[:, :m1]
-            assert np.isfinite(a).all()
-            assert _max_col_err(a, b) <= TOL
+    _check_case(torch, 300, 61, "B", "B", None, against_oracle=True)
+    _check_case(torch, 170, 62, "B", "S", (rng.random(170) < 0.4).astype(np.int32), against_oracle=False)
+
+
+def test_noalloc_largest_accepted_order(cuda_ok):
+    import torch
+    # n = 478 is the largest SIDE='B', HOWMNY='B' problem whose scratch fits the block
+    _check_case(torch, 478, 63, "B", "B", None, against_oracle=False)
 
 
 def test_noalloc_refuses_problems_larger_than_its_scratch(cuda_ok):
     import torch
-    n = 600  # SIDE='B', HOWMNY='B' at n = 600 needs more than the 8 MiB block
     dummy = torch.zeros(1, 1, dtype=torch.float64, device="cuda")
-    z = np.zeros(n)
-    rc, m, info = _noalloc(torch, "B", "B", dummy, dummy, z, z, np.ones(n), dummy, dummy, n=n, mm=n)
-    assert rc == 2
-    assert "static scratch" in X.last_error()
-    assert m == n and info == 0
+    # n = 479 is one more than the largest accepted SIDE='B', HOWMNY='B' order; 600 is well past it
+    for n in (479, 600):
+        z = np.zeros(n)
+        rc, m, info = _noalloc(torch, "B", "B", dummy, dummy, z, z, np.ones(n), dummy, dummy, n=n, mm=n)
+        assert rc == 2
+        assert "static scratch" in X.last_error() and "n <= 478" in X.last_error()
+        assert m == n and info == 0

@@ -6,6 +6,7 @@
 """
 from __future__ import annotations
 
+import concurrent.futures
 import glob
 import os
 import subprocess
@@ -41,7 +42,7 @@ def build(force: bool = False, ptxas_v: bool = False, verbose: bool = False) -> 
         return LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
+    jobs = []
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         cmd = [NVCC, *ARCH, *FLAGS, "-I", os.path.join(HERE, "..", "include"), "-c", src, "-o", obj]
@@ -49,7 +50,12 @@ def build(force: bool = False, ptxas_v: bool = False, verbose: bool = False) -> 
             cmd += ["-Xptxas", "-v"]
         if verbose:
             print(" ".join(cmd))
-        r = subprocess.run(cmd, capture_output=True, text=True)
+        jobs.append((src, obj, cmd))
+    # translation units compile independently: one nvcc process each, in parallel
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(lambda j: subprocess.run(j[2], capture_output=True, text=True), jobs))
+    objs = []
+    for (src, obj, _), r in zip(jobs, results):
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError(f"nvcc failed on {src}")

@@ -213,8 +213,19 @@ int create(char side, char howmny, int count, const typename batch::PencilOf<T>:
     std::vector<int> order(count);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return pencils[x].n > pencils[y].n; });
+    // Testing controls, read when a plan is created; neither changes anything when unset.
+    //   XTGEVC3_BATCH_SPIN_LIMIT=k       polls of a pencil's ready flag (128 ns apart) before a
+    //                                    compute unit gives up (default 2^24, ~2 s)
+    //   XTGEVC3_BATCH_WITHHOLD_READY=p   leave out pencil p's prep unit: its ready flag is never
+    //                                    set, every wait for it expires, the kernel records the
+    //                                    timeout and xtgevc3_batched_wait returns 3
+    long long spin_limit = 1ll << 24;
+    int withhold = -1;
+    if (const char *v = std::getenv("XTGEVC3_BATCH_SPIN_LIMIT")) spin_limit = std::max(1ll, std::atoll(v));
+    if (const char *v = std::getenv("XTGEVC3_BATCH_WITHHOLD_READY")) withhold = std::atoi(v);
     std::vector<int4> units;
-    for (int p : order) units.push_back(make_int4(0, p, 0, 0));
+    for (int p : order)
+        if (p != withhold) units.push_back(make_int4(0, p, 0, 0));
     for (int p : order) {
         const int n = pencils[p].n;
         if (n == 0) continue;
@@ -250,7 +261,7 @@ int create(char side, char howmny, int count, const typename batch::PencilOf<T>:
     a.ctrl = b->d_ctrl;
     a.back = back ? 1 : 0;
     a.xrows = xrows;
-    a.spin_limit = 1ll << 24;  // ~2 s of 128 ns sleeps: far beyond any prep unit
+    a.spin_limit = spin_limit;  // default ~2 s of 128 ns sleeps: far beyond any prep unit
 
     cudaStream_t cs = nullptr;
     XTG_BCK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));

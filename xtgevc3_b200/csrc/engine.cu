@@ -187,6 +187,75 @@ void configure_device(int dev)
     });
 }
 
+// ---- reusable per-call resources -------------------------------------------------------
+// A call with both sides runs the left one on a second stream, and a call on a real pencil
+// in device memory copies one status word back to pinned host memory.  Creating and
+// destroying a stream, its events and a pinned word per call costs tens of microseconds
+// (noticeable for small pencils), so they come from a per-device pool: a call leases one
+// set and returns it when it ends; sets are created on demand and kept for the process.
+namespace {
+struct CallRes {
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr, check = nullptr;
+    int *status = nullptr;  // pinned host word written by the structure check's copy
+};
+std::mutex g_res_mu;
+std::vector<CallRes *> g_res_free[64];
+
+class ResLease {
+public:
+    explicit ResLease(int dev) : dev_(dev) {}
+    ~ResLease()
+    {
+        if (r_) {
+            std::lock_guard<std::mutex> lk(g_res_mu);
+            g_res_free[dev_].push_back(r_);
+        }
+    }
+    // The set of this call (created on first use, on the current device); nullptr and a
+    // CUDA error code on failure.
+    CallRes *get(cudaError_t *err)
+    {
+        *err = cudaSuccess;
+        if (r_) return r_;
+        if (dev_ < 0 || dev_ >= 64) {
+            *err = cudaErrorInvalidDevice;
+            return nullptr;
+        }
+        {
+            std::lock_guard<std::mutex> lk(g_res_mu);
+            if (!g_res_free[dev_].empty()) {
+                r_ = g_res_free[dev_].back();
+                g_res_free[dev_].pop_back();
+                return r_;
+            }
+        }
+        CallRes *r = new CallRes;
+        cudaError_t e = cudaStreamCreateWithFlags(&r->side, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->fork, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->join, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->check, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void **>(&r->status), sizeof(int), cudaHostAllocDefault);
+        if (e != cudaSuccess) {
+            if (r->status) cudaFreeHost(r->status);
+            if (r->check) cudaEventDestroy(r->check);
+            if (r->join) cudaEventDestroy(r->join);
+            if (r->fork) cudaEventDestroy(r->fork);
+            if (r->side) cudaStreamDestroy(r->side);
+            delete r;
+            *err = e;
+            return nullptr;
+        }
+        r_ = r;
+        return r_;
+    }
+
+private:
+    int dev_;
+    CallRes *r_ = nullptr;
+};
+}  // namespace
+
 // Selected eigenvalues in ascending order; a complex-conjugate pair (real arithmetic) is
 // one item of two columns.  Selection rule of src/dtgevc3.cpp:1193-1207 / 1295-1324.
 struct Item {
@@ -328,17 +397,22 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             return 1;
         }
     }
+    ResLease res(dev);
     std::vector<char> sub(n, 0);  // sub[k] = S[k+1, k] != 0
+    // device check of a plan made from alphai alone (see Options::read_sub)
+    bool check_sub = false;
     if constexpr (!CPLX) {
         if (n > 1 && opt.host_S) {  // the caller's copy (the device one may still be in flight)
             const E *hs = static_cast<const E *>(opt.host_S);
             for (int k = 0; k + 1 < n; k++) sub[k] = hs[(size_t)(k + 1) + (size_t)k * opt.host_lds] != E(0);
-        } else if (n > 1) {
+        } else if (n > 1 && (opt.read_sub || opt.arena)) {
             std::vector<E> d(n - 1);
             XTG_CK(cudaMemcpy2DAsync(d.data(), sizeof(E), S + 1, (size_t)(lds + 1) * sizeof(E), sizeof(E), n - 1,
                                      cudaMemcpyDeviceToHost, st));
             XTG_CK(cudaStreamSynchronize(st));
             for (int k = 0; k + 1 < n; k++) sub[k] = d[k] != E(0);
+        } else if (n > 1) {
+            check_sub = true;
         }
     }
 
@@ -376,6 +450,35 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         XTG_CK(cudaMemcpyAsync(d_eig + n, alphai_, n * sizeof(R), cudaMemcpyHostToDevice, st));
         XTG_CK(cudaMemcpyAsync(d_eig + 2 * n, beta_, n * sizeof(R), cudaMemcpyHostToDevice, st));
     }
+    // The row blocks below are planned from alphai (pairstart); S's subdiagonal is checked
+    // against that plan on the device, and the result reaches the host through the leased
+    // pinned word.  `gate` (before anything is written to VL / VR) waits for it: a mismatch
+    // abandons the call, which then runs again with the subdiagonal read back.
+    CallRes *cres = nullptr;
+    int gate_state = check_sub ? 0 : 1;  // 0 pending, 1 plan confirmed, 2 plan rejected
+    if (check_sub) {
+        cudaError_t e = cudaSuccess;
+        cres = res.get(&e);
+        XTG_CK(e);
+        uint8_t *d_ps = scr.get<uint8_t>((size_t)n);
+        int *d_flag = scr.get<int>(1);
+        if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
+        std::vector<uint8_t> ps(pairstart.begin(), pairstart.begin() + n);
+        XTG_CK(cudaMemcpyAsync(d_ps, ps.data(), n, cudaMemcpyHostToDevice, st));
+        XTG_CK(cudaMemsetAsync(d_flag, 0, sizeof(int), st));
+        subdiag_check_kernel<R><<<(n + 255) / 256, 256, 0, st>>>(reinterpret_cast<const R *>(S), lds, n, d_ps, d_flag);
+        XTG_CK(cudaGetLastError());
+        XTG_CK(cudaMemcpyAsync(cres->status, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+        XTG_CK(cudaEventRecord(cres->check, st));
+    }
+    auto gate = [&]() -> int {  // 0: go on, 1: CUDA error, 2: plan rejected
+        if (gate_state == 0) {
+            XTG_CK(cudaEventSynchronize(cres->check));
+            gate_state = *cres->status ? 2 : 1;
+        }
+        return gate_state == 1 ? 0 : 2;
+    };
+
     // anorm / bnorm (src/dtgevc3.cpp:1254-1270; complex: rows <= col only); with host_norms
     // they come from the caller after `staged` (below)
     if (!opt.host_norms) {
@@ -833,6 +936,8 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         }
 
         // ---- write-back / back-transform -----------------------------------------------------
+        // nothing has been written to VL / VR so far: a rejected plan stops here
+        if (const int g = gate()) return g;
         E *V = left ? VL : VR;
         const int ldv = left ? ldvl : ldvr;
         if (do_back) {
@@ -930,41 +1035,43 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
     // The two sides are independent problems: with both requested they run concurrently,
     // the left one on a second stream (serially while tracing, so that kernel times are
     // not inflated by overlap).
+    // A side returns 0, 1 (CUDA error) or 2 (plan rejected by the structure check: nothing
+    // was written to VL / VR; the call runs again with the subdiagonal read back).
+    auto rerun = [&]() -> int {
+        XTG_CK(cudaStreamSynchronize(st));
+        Options o2 = opt;
+        o2.read_sub = 1;
+        return solve_device<R, CPLX>(side, howmny, select, n, S_, lds, P_, ldp, alpha_, alphai_, beta_, VL_, ldvl,
+                                     VR_, ldvr, m_total, o2, st);
+    };
     if (want_r && want_l && !tr.on && !opt.arena) {
-        struct Fork {
-            cudaStream_t s = nullptr;
-            cudaEvent_t fork = nullptr, join = nullptr;
-            ~Fork()
-            {
-                if (fork) cudaEventDestroy(fork);
-                if (join) cudaEventDestroy(join);
-                if (s) cudaStreamDestroy(s);
-            }
-        } fk;
-        XTG_CK(cudaStreamCreateWithFlags(&fk.s, cudaStreamNonBlocking));
-        XTG_CK(cudaEventCreateWithFlags(&fk.fork, cudaEventDisableTiming));
-        XTG_CK(cudaEventCreateWithFlags(&fk.join, cudaEventDisableTiming));
-        XTG_CK(cudaEventRecord(fk.fork, st));
-        XTG_CK(cudaStreamWaitEvent(fk.s, fk.fork, 0));
-        int rc = 0;
+        cudaError_t e = cudaSuccess;
+        CallRes *fk = res.get(&e);
+        XTG_CK(e);
+        XTG_CK(cudaEventRecord(fk->fork, st));
+        XTG_CK(cudaStreamWaitEvent(fk->side, fk->fork, 0));
+        int rr = 0, rl = 0;
         {
-            Scratch scr2(fk.s);
-            rc |= run_side(false, st, scr);
-            rc |= run_side(true, fk.s, scr2);
-            XTG_CK(cudaEventRecord(fk.join, fk.s));
-            XTG_CK(cudaStreamWaitEvent(st, fk.join, 0));
+            Scratch scr2(fk->side);
+            rr = run_side(false, st, scr);
+            if (rr == 0) rl = run_side(true, fk->side, scr2);
+            XTG_CK(cudaEventRecord(fk->join, fk->side));
+            XTG_CK(cudaStreamWaitEvent(st, fk->join, 0));
         }
-        if (rc) {
-            cudaStreamSynchronize(fk.s);
+        if (rr == 1 || rl == 1) {
+            cudaStreamSynchronize(fk->side);
             return 1;
         }
+        if (rr == 2 || rl == 2) return rerun();
     } else {
         const size_t mark = scr.used;
-        if (want_r && run_side(false, st, scr)) return 1;
+        int rc = want_r ? run_side(false, st, scr) : 0;
         // arena: the right side's slices are reused; its kernels precede the left side's
         // on the same stream
         if (opt.arena) scr.used = mark;
-        if (want_l && run_side(true, st, scr)) return 1;
+        if (rc == 0 && want_l) rc = run_side(true, st, scr);
+        if (rc == 2) return rerun();
+        if (rc) return 1;
     }
     XTG_CK(cudaStreamSynchronize(st));
     tr.flush();

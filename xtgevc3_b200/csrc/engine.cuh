@@ -27,6 +27,11 @@ struct Options {
     // allocated) and the two sides run one after the other on the caller's stream.
     void *arena = nullptr;
     size_t arena_bytes = 0;
+    // Real pencils on the device: read S's subdiagonal back to the host before planning the
+    // row blocks (a blocking copy).  Otherwise the blocks are planned from alphai and a
+    // kernel checks S against that plan; a call whose check fails is run again with this
+    // set (arena mode always reads it back).
+    int read_sub = 0;
     // Host-pointer path: the back-transform of a side waits for this event (the upload of
     // Z / Q on another stream), and side_done is called once a side's last kernel is
     // queued, with that side's stream (the result can be downloaded behind the other side).

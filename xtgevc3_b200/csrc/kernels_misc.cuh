@@ -279,6 +279,19 @@ __global__ void fill_one_kernel(R *p, int m)
     if (i < m) p[i] = R(1);
 }
 
+// Structure check of a real pencil given on the device (the block partition is planned on
+// the host from alphai, without reading S): *flag becomes 1 when some subdiagonal entry
+// S(k+1, k) is nonzero at a row k that does not start a complex pair, i.e. when the
+// upstream partition rule (snap where S(k+1, k) != 0, src/dtgevc3.cpp:32-47) would
+// differ from the planned one.  *flag is zeroed by the caller.
+template <class R>
+__global__ void subdiag_check_kernel(const R *S, int lds, int n, const uint8_t *pairstart, int *flag)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool bad = k + 1 < n && S[(size_t)(k + 1) + (size_t)k * lds] != R(0) && !pairstart[k];
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicExch(flag, 1);
+}
+
 // Diagonal of the identity (the rest zeroed by the caller): P of the standard problem.
 template <class E>
 __global__ void identity_diag_kernel(E *A, int lda, int n)

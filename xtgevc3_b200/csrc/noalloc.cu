@@ -17,8 +17,10 @@
 //
 // Host code cannot use the symbol's name as a device address (it names a host-side
 // shadow), so the address is looked up with cudaGetSymbolAddress once per device, with
-// that device current, on the first call made on it; make that first call before any
-// stream capture begins.
+// that device current, on the first call made on it.  A lookup that fails is not
+// remembered: the next call on that device tries again.  Every call blocks the calling
+// thread until its result is complete (it synchronises its stream), so the entry point
+// cannot be used inside a stream capture.
 //
 // All calls share the one block, and it keeps whatever the previous call left in it: the
 // computation zeroes what must start at zero itself.  Two calls whose work overlaps on the
@@ -39,9 +41,37 @@ constexpr size_t kNoAllocBytes = size_t(8) << 20;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 constexpr int kMaxDevices = 64;
-std::once_flag g_once[kMaxDevices];
-void *g_addr[kMaxDevices];
-cudaError_t g_addr_err[kMaxDevices];
+std::mutex g_addr_mu;
+void *g_addr[kMaxDevices];  // device address of the block, per device; set once a lookup succeeds
+
+// The largest order n whose SIDE='B', HOWMNY='B' call fits the block (all eigenvectors).
+int max_order_both_sides()
+{
+    static const int nmax = [] {
+        int n = 1;
+        while (xtg::arena_bytes_needed(n + 1, n + 1, true, true, true, false, false, sizeof(double)) <= kNoAllocBytes)
+            n++;
+        return n;
+    }();
+    return nmax;
+}
+
+// Device address of the block on device `dev` (current), looked up on first use.
+cudaError_t scratch_address(int dev, void **addr)
+{
+    std::lock_guard<std::mutex> lk(g_addr_mu);
+    if (!g_addr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();  // the failed lookup is not left pending for later calls
+            return e != cudaSuccess ? e : cudaErrorInvalidSymbol;
+        }
+        g_addr[dev] = p;
+    }
+    *addr = g_addr[dev];
+    return cudaSuccess;
+}
 
 }  // namespace
 
@@ -66,8 +96,8 @@ extern "C" int xtgevc3_dtgevc3_dev_noalloc(void *stream, char side, char howmny,
         char msg[256];
         std::snprintf(msg, sizeof msg,
                       "xtgevc3_dtgevc3_dev_noalloc: n=%d with %d eigenvector columns needs %zu bytes of scratch; "
-                      "the static scratch holds %zu bytes (SIDE='B', HOWMNY='B': n <= 448)",
-                      n, count, need, kNoAllocBytes);
+                      "the static scratch holds %zu bytes (SIDE='B', HOWMNY='B': n <= %d)",
+                      n, count, need, kNoAllocBytes, max_order_both_sides());
         xtg::set_last_error(msg);
         return 2;
     }
@@ -79,18 +109,17 @@ extern "C" int xtgevc3_dtgevc3_dev_noalloc(void *stream, char side, char howmny,
         *info = 1;
         return 1;
     }
-    std::call_once(g_once[dev], [dev]() {
-        g_addr_err[dev] = cudaGetSymbolAddress(&g_addr[dev], g_noalloc_scratch);
-    });
-    if (g_addr_err[dev] != cudaSuccess || !g_addr[dev]) {
+    void *scratch = nullptr;
+    e = scratch_address(dev, &scratch);
+    if (e != cudaSuccess) {
         xtg::set_last_error(std::string("xtgevc3_dtgevc3_dev_noalloc: cudaGetSymbolAddress: ") +
-                            cudaGetErrorString(g_addr_err[dev]));
+                            cudaGetErrorString(e));
         *info = 1;
         return 1;
     }
 
     xtg::Options opt;
-    opt.arena = g_addr[dev];
+    opt.arena = scratch;
     opt.arena_bytes = kNoAllocBytes;
     const int rc = xtg::solve_device<double, false>(side, howmny, select, n, S, lds, P, ldp, alphar, alphai, beta,
                                                     left ? VL : nullptr, ldvl, right ? VR : nullptr, ldvr, count, opt,
