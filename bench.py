@@ -12,9 +12,11 @@ Prints one JSON line (rank 0).  value = eigenvectors/s of the whole job with inp
 resident in HBM; e2e = the same through the host-pointer C ABI (xtgevc3_dtgevc3) from
 pinned host buffers, copies included.  roofline = the dominant kernel class from the
 library's CUDA-event trace against the FP64 GEMM peak measured in this run (cuBLAS
-DGEMM, MEASURED_PEAKS.json has no FP64 figure).  cpu_baseline = the upstream CPU library
-(oracle/_ref, OpenBLAS on all host cores) on a bounded window of the same pencil.
---impl reference times that CPU library alone (rank 0), one window sample per step.
+DGEMM, MEASURED_PEAKS.json has no FP64 figure).  cpu_baseline = one full call of the
+upstream CPU library (oracle/_ref, OpenBLAS on all host cores) on the same pencil, Q and Z;
+its result is also the reference every form is compared with elementwise
+(config.max_rel_diff_vs_reference, config.forms).  --impl reference times that CPU library
+alone (rank 0): one full call of the same workload per step.
 """
 from __future__ import annotations
 
@@ -47,7 +49,8 @@ def parse():
     ap.add_argument("--n", type=int, default=8192)
     ap.add_argument("--seed", type=int, default=8192)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--cpu-window", type=int, default=1024, help="eigenvalues per side in the CPU sample")
+    ap.add_argument("--ref-budget-s", type=float, default=240.0,
+                    help="--impl reference: stop timing further full calls once this many seconds are spent")
     ap.add_argument("--form", default="all", choices=["plain", "split", "split_i8", "all"],
                     help="plain FP64, split precision with BF16 or INT8 slices, or all (the fastest one "
                          "meeting the residual bound is the headline)")
@@ -215,47 +218,33 @@ def residual_max(torch, S, P, ar, ai, be, Q, Z, VL, VR):
 
 
 # ----------------------------------------------------------------------------------------
-# CPU: the upstream library on a bounded window of the same pencil
+# CPU: the upstream library on the whole workload
 # ----------------------------------------------------------------------------------------
-def cpu_windows(n, w):
-    """Right window centred on n/sqrt(3), left on n - n/sqrt(3): the right eigenvector of
-    eigenvalue k costs ~k^2 and the left one ~(n-k)^2, whose means sit at those points.
-    Windows are aligned to the upstream 32-column panels."""
-    c = n / math.sqrt(3.0)
-    a_r = n - 32 * int(round((n - (c - w / 2)) / 32))
-    a_r = max(0, min(a_r, n - w))
-    c_l = n - c
-    a_l = 32 * int(round((c_l - w / 2) / 32))
-    a_l = max(0, min(a_l, n - w))
-    return (a_r, a_r + w), (a_l, a_l + w)
-
-
-def cpu_sample(S, P, ar, ai, be, w, threads):
-    """One sample: upstream dtgevc3 SIDE='R' and SIDE='L', HOWMNY='S' on the two windows.
-    Returns (eigenvectors, seconds, kind)."""
+def cpu_full(S, P, ar, ai, be, Q, Z, threads):
+    """One upstream dtgevc3 call with the bench's arguments (SIDE='B', HOWMNY='B', VL = Q,
+    VR = Z on entry): the library built from the upstream sources (oracle/_ref) with its
+    OpenBLAS on `threads` host threads, or this repository's C restatement where that
+    library is absent.  Returns (VL, VR, seconds, kind)."""
     import oracle
-    n = S.shape[0]
-    (r0, r1), (l0, l1) = cpu_windows(n, w)
     impl = "ref" if oracle.ref_available() else "oracle"
     if impl == "ref":
         oracle.set_ref_threads(threads)
-    tot_m, tot_t = 0, 0.0
-    for side, (a, b) in (("R", (r0, r1)), ("L", (l0, l1))):
-        sel = np.zeros(n, dtype=np.int32)
-        sel[a:b] = 1
-        mm = w + 2
-        V = np.zeros((n, mm), order="F")
-        t0 = time.perf_counter()
-        if side == "R":
-            _, _, m, info = oracle.tgevc3("R", "S", S, P, ar, be, alphai=ai, VR=V, VL=None, select=sel, mm=mm,
-                                          impl=impl)
-        else:
-            _, _, m, info = oracle.tgevc3("L", "S", S, P, ar, be, alphai=ai, VL=V, VR=None, select=sel, mm=mm,
-                                          impl=impl)
-        tot_t += time.perf_counter() - t0
-        assert info == 0
-        tot_m += m
-    return tot_m, tot_t, ("reference" if impl == "ref" else "port")
+    VL = np.array(Q, order="F", dtype=np.float64)
+    VR = np.array(Z, order="F", dtype=np.float64)
+    t0 = time.perf_counter()
+    VL, VR, m, info = oracle.tgevc3("B", "B", S, P, ar, be, alphai=ai, VL=VL, VR=VR, impl=impl)
+    t = time.perf_counter() - t0
+    assert (m, info) == (S.shape[0], 0), (m, info)
+    return VL, VR, t, ("reference" if impl == "ref" else "port")
+
+
+def householder(n, seed):
+    """A dense orthogonal n x n matrix I - 2 v v^T / (v^T v), v ~ N(0,1) seeded (host,
+    Fortran order): Q / Z of the CPU arm, whose run time does not depend on their values."""
+    v = np.random.default_rng(seed).standard_normal(n)
+    H = -(2.0 / (v @ v)) * np.outer(v, v)
+    H[np.diag_indices(n)] += 1.0
+    return np.asfortranarray(H)
 
 
 def host_threads():
@@ -266,30 +255,41 @@ def host_threads():
 
 
 def reference_arm(args):
+    """The upstream library (the reference's CPU implementation of the path) on the bench's
+    own workload: one full dtgevc3 SIDE='B' HOWMNY='B' call on the n = --n pencil per step,
+    on every host thread.  Warm-up steps run the same call at n = 1024 (library, OpenBLAS
+    threads and page-ins warm); timed steps stop early once --ref-budget-s is spent, so that
+    the run ends within minutes (steps reports the calls timed)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     n = args.n
-    S, P, ar, ai, be = host_pencil(n, args.seed)
     thr = host_threads()
-    w = 256
+    S, P, ar, ai, be = host_pencil(n, args.seed)
+    Q, Z = householder(n, args.seed + 1), householder(n, args.seed + 2)
+    nw = min(n, 1024)
+    Sw, Pw, arw, aiw, bew = host_pencil(nw, args.seed + 3)
+    Iw = np.eye(nw, order="F")
     for _ in range(args.warmup):
-        cpu_sample(S, P, ar, ai, be, w, thr)
-    ms_tot, t_tot = 0, 0.0
-    kind = "reference"
+        cpu_full(Sw, Pw, arw, aiw, bew, Iw, Iw, thr)
+    times, kind = [], "reference"
+    t_start = time.perf_counter()
     for _ in range(args.steps):
-        m, t, kind = cpu_sample(S, P, ar, ai, be, w, thr)
-        ms_tot += m
-        t_tot += t
-    v = ms_tot / t_tot
-    sample = (f"upstream dtgevc3 HOWMNY='S' on one window of {w} eigenvalues per side (right window "
-              f"centred at n/sqrt(3), left at n-n/sqrt(3)) of the n={n} pencil per step; excludes the "
-              f"back-transform GEMM, so it overstates the CPU rate of HOWMNY='B'")
+        _, _, t, kind = cpu_full(S, P, ar, ai, be, Q, Z, thr)
+        times.append(t)
+        if time.perf_counter() - t_start + t > args.ref_budget_s:
+            break
+    t_mean = float(np.mean(times))
+    v = 2 * n / t_mean
+    sample = (f"upstream dtgevc3 SIDE=B HOWMNY=B, the whole n={n} job (all {2 * n} eigenvectors, "
+              f"back-transform included) per step, {thr} threads")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_tot / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
+            "steps": len(times), "steps_requested": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_mean, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": DATA,
             "config": {"workload": f"dtgevc3 SIDE=B HOWMNY=B n={n}", "n": n, "side": "B", "howmny": "B",
-                       "form": "upstream CPU (OpenBLAS)"},
+                       "form": "upstream CPU (OpenBLAS)", "same_config": True,
+                       "warmup_calls": f"n={nw} B/B", "budget_s": args.ref_budget_s},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": thr, "kind": kind, "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -329,7 +329,51 @@ def rank_seeds(seed, batch_seed, rank):
             "batch": batch_seed + 7919 * rank}
 
 
-def measure_form(name, flags, args, X, torch, data, dist, local, world):
+def max_rel_diff_vs(torch, V, R, ai):
+    """Elementwise agreement of two real eigenvector matrices in (Re, Im) pair storage (all
+    eigenvalues, ascending), on the device: both are turned into one complex eigenvector per
+    column, scaled by their value at the row where |R| is largest (the comparison
+    normalisation of the oracle package), and the largest |v - r| over the column's largest
+    |r| is returned (max over columns).  Columns go in chunks that never split a pair."""
+    n, m = V.shape
+    starts, k = set(), 0
+    while k < m:
+        if ai[k] != 0 and k + 1 < m:
+            starts.add(k)
+            k += 2
+        else:
+            k += 1
+    worst, c0 = 0.0, 0
+    while c0 < m:
+        c1 = min(m, c0 + 2048)
+        if c1 < m and (c1 - 1) in starts:
+            c1 += 1
+        loc = [c - c0 for c in range(c0, c1) if c in starts]
+        ix = torch.as_tensor(loc, device=V.device, dtype=torch.long)
+
+        def cplx(W):
+            C = torch.complex(W, torch.zeros_like(W))
+            if loc:
+                re, im = W[:, ix], W[:, ix + 1]
+                C[:, ix] = torch.complex(re, im)
+                C[:, ix + 1] = torch.complex(re, -im)
+            return C
+
+        Vc, Rc = cplx(V[:, c0:c1]), cplx(R[:, c0:c1])
+        row = Rc.abs().argmax(0)
+        cols = torch.arange(c1 - c0, device=V.device)
+        a, b = Vc[row, cols], Rc[row, cols]
+        a = torch.where(a == 0, torch.ones_like(a), a)
+        b = torch.where(b == 0, torch.ones_like(b), b)
+        Vn, Rn = Vc / a[None, :], Rc / b[None, :]
+        den = Rn.abs().amax(0).clamp_min(1e-300)
+        worst = max(worst, float(((Vn - Rn).abs().amax(0) / den).max()))
+        del Vc, Rc, Vn, Rn
+        c0 = c1
+    return worst
+
+
+def measure_form(name, flags, args, X, torch, data, dist, local, world, ref=None):
     """Time K steps of one form (device-resident inputs), check the residual of the result,
     then trace K more steps for the per-kernel breakdown."""
     S, P, ar, ai, be, Q, Z, VL, VR = data
@@ -359,6 +403,10 @@ def measure_form(name, flags, args, X, torch, data, dist, local, world):
     clk = clocks.stop()
     ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, torch)
     resid = residual_max(torch, S, P, ar, ai, be, Q, Z, VL, VR)
+    # elementwise error against the upstream library's result on the same inputs
+    err = None
+    if ref is not None:
+        err = max(max_rel_diff_vs(torch, VL, ref[0], ai), max_rel_diff_vs(torch, VR, ref[1], ai))
     X.trace_reset()
     X.trace_enable(True)
     for _ in range(args.steps):
@@ -367,7 +415,7 @@ def measure_form(name, flags, args, X, torch, data, dist, local, world):
     X.trace_enable(False)
     kernels = {k: dict(v, ms_per_step=v["ms"] / args.steps) for k, v in X.trace().items() if v["launches"]}
     return {"name": name, "flags": flags, "ms": ms, "value": world * 2 * n / (ms * 1e-3), "resid": resid,
-            "clocks": clk, "launches": launches, "kernels": kernels}
+            "err_vs_ref": err, "clocks": clk, "launches": launches, "kernels": kernels}
 
 
 def batched_inputs(count, seed, torch):
@@ -843,7 +891,20 @@ def main():
     s8 = max(1, min(7, args.slices_i8))
     forms = {"plain": 0, "split": X.SPLIT | X.slices(s), "split_i8": X.SPLIT | X.SPLIT_INT8 | X.slices(s8)}
     names = ["plain", "split", "split_i8"] if args.form == "all" else [args.form]
-    res = {nm: measure_form(nm, forms[nm], args, X, torch, data, dist, local, world) for nm in names}
+    # the upstream library on the same inputs, once (rank 0 at N = 1): the CPU baseline, and
+    # the reference result every form is compared with elementwise
+    cpu, ref = None, None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        thr = host_threads()
+        Qh, Zh = Q.cpu().numpy(), Z.cpu().numpy()  # column-major tensors -> Fortran arrays
+        RL, RR, t_cpu, kind = cpu_full(S_h, P_h, ar, ai, be, Qh, Zh, thr)
+        cpu = {"value": 2 * n / t_cpu, "unit": UNIT, "cores": thr, "kind": kind, "seconds": t_cpu,
+               "sample": f"one full upstream dtgevc3 SIDE=B HOWMNY=B call on the same n={n} pencil, Q, Z "
+                         f"({thr} threads)"}
+        ref = (colmajor_cuda(RL, torch), colmajor_cuda(RR, torch))
+        del RL, RR, Qh, Zh
+    res = {nm: measure_form(nm, forms[nm], args, X, torch, data, dist, local, world, ref) for nm in names}
+    ref = None
     ok = [nm for nm in names if res[nm]["resid"] <= 1e-12]
     head = min(ok or names, key=lambda nm: res[nm]["ms"])
     h = res[head]
@@ -948,26 +1009,20 @@ def main():
     trleg = measure_trevc3(args, X, torch) if args.trevc3_n > 0 and rank == 0 else None
     txleg = measure_tgexc(args, X, torch) if args.tgexc_n > 0 and rank == 0 else None
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        thr = host_threads()
-        m, t, kind = cpu_sample(S_h, P_h, ar, ai, be, args.cpu_window, thr)
-        cpu = {"value": m / t, "unit": UNIT, "cores": thr, "kind": kind, "seconds": t,
-               "sample": (f"upstream dtgevc3 HOWMNY='S' on one window of {args.cpu_window} eigenvalues per "
-                          f"side (right centred at n/sqrt(3), left at n-n/sqrt(3), where the per-vector cost "
-                          f"equals the mean) of the same n={n} pencil; excludes the back-transform, so it "
-                          f"overstates the CPU rate of HOWMNY='B'")}
-
     if rank == 0:
         form_desc = {"plain": "plain FP64 (DMMA)", "split": f"split precision, {s} BF16 slices (tcgen05)",
                      "split_i8": f"split precision, {s8} INT8 slices (tcgen05 kind::i8)"}
         forms_out = {nm: {"value": r["value"], "ms_per_step": r["ms"], "resid_max": r["resid"],
-                          "meets_resid_bound": r["resid"] <= 1e-12,
+                          "meets_resid_bound": r["resid"] <= 1e-12, "max_rel_diff_vs_reference": r["err_vs_ref"],
                           "kernels_ms_per_step": {k: v["ms_per_step"] for k, v in r["kernels"].items()}}
                      for nm, r in res.items()}
         if "plain" in res:
             for nm in forms_out:
                 forms_out[nm]["speedup_vs_plain"] = res["plain"]["ms"] / res[nm]["ms"]
+        # one compact line per form inside `config` (kept by record parsers that drop extra keys)
+        forms_brief = {nm: {"ms": round(f["ms_per_step"], 3), "resid": f["resid_max"],
+                            "err_vs_ref": f["max_rel_diff_vs_reference"],
+                            "x_plain": round(f.get("speedup_vs_plain", 0.0), 3)} for nm, f in forms_out.items()}
         line = {"metric": METRIC, "value": h["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": h["ms"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": DATA,
@@ -975,7 +1030,15 @@ def main():
                            "form": form_desc[head], "pencils_per_gpu": 1,
                            "l2": "inputs larger than L2 (S,P,Q,Z = 2 GiB); no flush",
                            "parallelism": f"independent pencil per GPU x{world}",
-                           "resid_max": h["resid"], "resid_bound": 1e-12},
+                           "resid_max": h["resid"], "resid_bound": 1e-12,
+                           "max_rel_diff_vs_reference": h["err_vs_ref"],
+                           "reference_for_diff": "upstream dtgevc3 (oracle/_ref) on the same S, P, Q, Z; columns "
+                                                 "compared after normalisation" if h["err_vs_ref"] is not None else None,
+                           "forms": forms_brief,
+                           "batched": None if batched is None else {
+                               "pencils_per_s": batched["value"], "speedup_vs_loop": batched["speedup_vs_loop"],
+                               "d_ms": batched["d"]["ms"], "s_ms": batched["s"]["ms"],
+                               "d_max_rel_diff_vs_loop": batched["d"]["max_rel_diff_vs_loop"]}},
                 "forms": forms_out, "clocks": h["clocks"], "e2e": e2e, "gpu_launches": h["launches"],
                 "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "batched": batched,
                 "adjoint": adjoint, "ztgevc3": zleg, "dtrevc3": trleg, "ztgexc": txleg}

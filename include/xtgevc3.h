@@ -52,12 +52,29 @@ extern "C" {
 /* With XTGEVC3_SPLIT: INT8 slices (7-bit digits, s in [1, 7], default 7, ~49 bits per
  * operand) on the INT8 tensor cores with exact INT32 accumulation over the whole K. */
 #define XTGEVC3_SPLIT_INT8 8u
+/* With XTGEVC3_SPLIT: residue form.  Each row of A / column of B is scaled by a power of two
+ * to an integer of t bits; the product of the integers is recovered exactly from its
+ * residues modulo L pairwise-coprime moduli <= 256 (Chinese remainder theorem), one INT8
+ * tensor-core GEMM with exact INT32 sums per modulus.  XTGEVC3_SLICES(L) picks L in [2, 16]
+ * (default 14: ~47-bit operands at K = 8192; t = floor((log2 P - ceil(log2 K) - 2) / 2)).
+ * L products replace the s(s+1)/2 of the digit slices. */
+#define XTGEVC3_SPLIT_CRT 32u
 /* Look-ahead schedule: the trailing update of each pair of row blocks runs on a second
  * stream while the next pair's diagonal solves run (guard rescaling of the rows that
  * update writes is deferred until it has finished).  Same results to rounding (the default
  * schedule sums the updates of two row blocks in one GEMM); on B200 it measured no faster
  * (the update fills the GPU), so it is off by default. */
 #define XTGEVC3_LOOKAHEAD 16u
+
+/* ---- split-precision GEMM on device operands (no upstream counterpart) ----------------
+ * C (+)= A B with column-major FP64 A (M x K), B (K x N), C (M x N) on the device, through
+ * the tensor-core path of a split form: kind 0 BF16 slices, 1 INT8 digit slices, 2 INT8
+ * residues; slices = the slice / modulus count (0: the form's default).  K < 65536.  The
+ * building block of the split forms, exposed for testing and measurement.  Synchronous on
+ * `stream`; returns 0, 1 (CUDA failure, message in xtgevc3_last_error()) or -1 (bad
+ * argument). */
+int xtgevc3_split_gemm_dev(void *stream, int kind, int slices, int M, int N, int K, const double *A, int lda,
+                           const double *B, int ldb, double *C, int ldc, int accumulate);
 
 /* Process-wide flags used by the drop-in entry points below (default 0). */
 void xtgevc3_set_flags(unsigned flags);

@@ -315,6 +315,10 @@ SPLIT_CASES = [
     ("gges", 257, 71, "B", "B", 7, 1e-10, "int8"),
     ("gges", 300, 72, "B", "A", 7, 1e-10, "int8"),
     ("schur", 700, 73, "B", "B", 7, 1e-6, "int8"),
+    ("gges", 257, 71, "B", "B", 14, 1e-10, "crt"),
+    ("gges", 300, 72, "B", "A", 14, 1e-10, "crt"),
+    ("schur", 700, 73, "B", "B", 14, 1e-6, "crt"),
+    ("gges", 1100, 74, "B", "B", 14, 1e-10, "crt"),
 ]
 
 
@@ -323,7 +327,8 @@ def test_split_precision_form(cuda_ok, case):
     """XTGEVC3_SPLIT: updates and back-transform as slice products on the tensor cores;
     solves stay FP64.  BF16 slices: FP32 accumulation exact per 128-deep chunk, FP64
     summation, 6 slices ~48 bits per operand.  INT8 slices (XTGEVC3_SPLIT_INT8): INT32
-    accumulation exact over the whole K, 7 slices ~49 bits.  The result must match the FP64
+    accumulation exact over the whole K, 7 slices ~49 bits.  Residues (XTGEVC3_SPLIT_CRT):
+    one exact INT8 GEMM per modulus, 14 moduli ~47-bit operands.  The result must match the FP64
     oracle elementwise within the stated tolerance (looser on the ill-conditioned stand-in
     pencil) and its residual must meet the DGET52 bound used for the plain form."""
     kind, n, seed, side, howmny, s, tol, sk = case
@@ -332,7 +337,7 @@ def test_split_precision_form(cuda_ok, case):
              VL_in=p["Q"], VR_in=p["Z"], name=kind)
     ref = oracle.tgevc3(side, howmny, d["S"], d["P"], d["alpha"], d["beta"], alphai=d["alphai"],
                         VL=p["Q"].copy(order="F"), VR=p["Z"].copy(order="F"))
-    X.set_flags(X.SPLIT | X.slices(s) | (X.SPLIT_INT8 if sk == "int8" else 0))
+    X.set_flags(X.SPLIT | X.slices(s) | {"bf16": 0, "int8": X.SPLIT_INT8, "crt": X.SPLIT_CRT}[sk])
     try:
         VL, VR, m, info = run_gpu(d)
     finally:

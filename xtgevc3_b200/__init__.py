@@ -30,11 +30,33 @@ SIMT = 2
 SPLIT = 4
 SPLIT_INT8 = 8
 LOOKAHEAD = 16
+SPLIT_CRT = 32
 
 
 def slices(s: int) -> int:
-    """Flag bits selecting s slices for the SPLIT form (BF16: 1..6, INT8: 1..7)."""
+    """Flag bits selecting s slices for the SPLIT form (BF16: 1..6, INT8: 1..7) or the
+    modulus count of the residue form (SPLIT_CRT: 2..16)."""
     return int(s) << 8
+
+
+def split_gemm(kind, A, B, C=None, accumulate=False, slices=0, stream=None):
+    """C (+)= A B through a split-precision tensor-core path (xtgevc3_split_gemm_dev): kind 0
+    BF16 slices, 1 INT8 digit slices, 2 INT8 residues.  A, B, C: column-major float64 CUDA
+    tensors (C allocated when None).  Returns C."""
+    import torch
+    M, K = A.shape
+    N = B.shape[1]
+    if C is None:
+        C = torch.zeros(N, M, dtype=torch.float64, device=A.device).t()
+    ap, lda = _colmajor(A)
+    bp, ldb = _colmajor(B)
+    cp, ldc = _colmajor(C)
+    st = ct.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+    rc = lib().xtgevc3_split_gemm_dev(st, int(kind), int(slices), M, N, K, ap, lda, bp, ldb, cp, ldc,
+                                      int(bool(accumulate)))
+    if rc != 0:
+        raise RuntimeError(f"xtgevc3_split_gemm_dev failed ({rc}): {last_error()}")
+    return C
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _lib = None

@@ -28,9 +28,9 @@ xtg::Options make_opts(unsigned flags)
     o.simt = (flags & XTGEVC3_SIMT) ? 1 : 0;
     o.lookahead = (flags & XTGEVC3_LOOKAHEAD) ? 1 : 0;
     if (flags & XTGEVC3_SPLIT) {
-        const int s = (int)((flags >> 8) & 15u);
-        o.split_kind = (flags & XTGEVC3_SPLIT_INT8) ? 1 : 0;
-        o.split = s > 0 ? s : (o.split_kind ? 7 : 6);
+        const int s = (int)((flags >> 8) & 31u);
+        o.split_kind = (flags & XTGEVC3_SPLIT_CRT) ? 2 : (flags & XTGEVC3_SPLIT_INT8) ? 1 : 0;
+        o.split = s > 0 ? s : (o.split_kind == 2 ? 14 : o.split_kind ? 7 : 6);
     }
     return o;
 }
@@ -729,6 +729,20 @@ int xtgevc3_trace_get(int cls, long long *launches, double *ms, double *flops, d
 }
 const char *xtgevc3_trace_name(int cls) { return xtg::trace_name(cls); }
 long long xtgevc3_launch_count(void) { return xtg::launch_count(); }
+
+int xtgevc3_split_gemm_dev(void *stream, int kind, int slices, int M, int N, int K, const double *A, int lda,
+                           const double *B, int ldb, double *C, int ldc, int accumulate)
+{
+    xtg::set_last_error("");
+    if (kind < 0 || kind > 2 || M < 0 || N < 0 || K < 0 || (M > 0 && lda < M) || (K > 0 && ldb < K) ||
+        (M > 0 && ldc < M)) {
+        xtg::set_last_error("xtgevc3_split_gemm_dev: bad argument");
+        return -1;
+    }
+    if (slices <= 0) slices = kind == 2 ? 14 : kind == 1 ? 7 : 6;
+    return xtg::split_gemm_device(kind, slices, M, N, K, A, lda, B, ldb, C, ldc, accumulate,
+                                  static_cast<cudaStream_t>(stream));
+}
 
 void xtgevc3_dtgevc3(char side, char howmny, const int *select, int n, const double *S, int lds, const double *P,
                      int ldp, const double *alphar, const double *alphai, const double *beta, double *VL, int ldvl,

@@ -22,12 +22,14 @@
 #include "kernels_gemm.cuh"
 #include "kernels_misc.cuh"
 #include "kernels_split.cuh"
+#include "kernels_crt.cuh"
 #include "host_common.cuh"
 
 #include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -184,6 +186,7 @@ void configure_device(int dev)
                              split::Layout<split::kBF16>::SMEM_BYTES);
         cudaFuncSetAttribute(split::gemm_split_kernel<split::kI8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              split::Layout<split::kI8>::SMEM_BYTES);
+        cudaFuncSetAttribute(crt::gemm_crt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, crt::SMEM_BYTES);
     });
 }
 
@@ -351,6 +354,182 @@ static cudaError_t launch_split(const GemmArgs<double> &g, int s, SplitBufs &sb,
     return cudaGetLastError();
 }
 
+// ---- residue (CRT) split GEMM launcher ------------------------------------------------------
+// Moduli of the residue form: pairwise coprime, largest first (256 = 2^8, 255 = 3 5 17,
+// 253 = 11 23, 247 = 13 19, 217 = 7 31, the rest prime); the first L are used.
+static const int kModuli[crt::MAXL] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 199, 197, 193};
+
+static void build_moduli(crt::Moduli &md, int L)
+{
+    typedef unsigned __int128 u128;
+    md = crt::Moduli{};
+    md.L = L;
+    u128 P = 1;
+    for (int l = 0; l < L; l++) P *= (u128)kModuli[l];
+    int bits = 0;  // bits of the largest M_l = P / p_{L-1}
+    for (u128 v = P / (u128)kModuli[L - 1]; v; v >>= 1) bits++;
+    md.hi = std::max(0, bits - 40);
+    md.lo = std::max(0, md.hi - 40);
+    const u128 mask40 = (((u128)1) << 40) - 1;
+    for (int l = 0; l < L; l++) {
+        const int p = kModuli[l];
+        const u128 Ml = P / (u128)p;
+        const int r = (int)(Ml % (u128)p);
+        int y = 1;
+        while ((r * y) % p != 1) y++;  // the inverse exists: the moduli are pairwise coprime
+        md.p[l] = p;
+        md.y[l] = y;
+        md.invpf[l] = 1.0f / (float)p;
+        md.invp[l] = 1.0 / (double)p;
+        md.m1[l] = (double)(Ml >> md.hi);
+        md.m2[l] = (double)((Ml >> md.lo) & mask40);
+    }
+    md.P1 = (double)(P >> md.hi);
+    md.P2 = (double)((P >> md.lo) & mask40);
+    const double Pd = (double)P;
+    md.c1 = std::ldexp(1.0, md.hi) / Pd;
+    md.c2 = std::ldexp(1.0, md.lo) / Pd;
+    md.log2P = std::log2(Pd);
+}
+
+static const crt::Moduli &crt_moduli(int L)
+{
+    static crt::Moduli tab[crt::MAXL + 1];
+    static std::once_flag once;
+    std::call_once(once, [] {
+        for (int l = 1; l <= crt::MAXL; l++) build_moduli(tab[l], l);
+    });
+    return tab[std::max(1, std::min(L, crt::MAXL))];
+}
+
+// Operand bits t of a residue GEMM with L moduli and K terms: 2t + ceil(log2 K) + 2 <= log2 P,
+// so that |C'| < P / 4 and the rounded quotient of the reconstruction is exact.
+static int crt_bits(int L, int K)
+{
+    int kb = 0;
+    while ((1 << kb) < std::max(K, 2)) kb++;
+    return (int)std::floor((crt_moduli(L).log2P - kb - 2) / 2);
+}
+
+// Reusable residue buffers of one side (grown on demand from the call's scratch).
+struct CrtBufs {
+    int8_t *A = nullptr, *B = nullptr;
+    unsigned char *U = nullptr;
+    int *ea = nullptr, *eb = nullptr;
+    size_t acap = 0, bcap = 0, ucap = 0, eacap = 0, ebcap = 0;
+};
+
+static int sm_count()
+{
+    int dev = 0, nsm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    return std::max(1, nsm);
+}
+
+// C (+)= A B for a GemmArgs<double> launch by L residues on the INT8 tensor cores (see
+// kernels_crt.cuh).  K must stay below 2^16 (exact INT32 sums; the caller checks).
+static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scratch &scr, int *d_err,
+                              cudaStream_t st)
+{
+    using namespace crt;
+    const Moduli &md = crt_moduli(L);
+    const int Kp = round_up(g.K, BK), Mp = round_up(g.M, BM), Np = round_up(g.N, BN);
+    const int t = crt_bits(L, g.K);
+    const size_t an = (size_t)L * Mp * Kp, bn = (size_t)L * Np * Kp, un = (size_t)L * Np * Mp;
+    if (an > cb.acap) { cb.A = scr.get<int8_t>(an); cb.acap = an; }
+    if (bn > cb.bcap) { cb.B = scr.get<int8_t>(bn); cb.bcap = bn; }
+    if (un > cb.ucap) { cb.U = scr.get<unsigned char>(un); cb.ucap = un; }
+    if ((size_t)Mp > cb.eacap) { cb.ea = scr.get<int>(Mp); cb.eacap = Mp; }
+    if ((size_t)Np > cb.ebcap) { cb.eb = scr.get<int>(Np); cb.ebcap = Np; }
+    if (scr.err) return scr.err;
+    residue_rows_kernel<<<Mp / 32, 256, 0, st>>>(g, Kp, Mp, t, md, cb.A, cb.ea);
+    residue_cols_kernel<<<Np / 8, 256, 0, st>>>(g, Kp, Np, t, md, cb.B, cb.eb);
+    CUtensorMap tmA, tmB;
+    if (!slice_tensor_map(&tmA, cb.A, split::kI8, Kp, L * Mp, BM) ||
+        !slice_tensor_map(&tmB, cb.B, split::kI8, Kp, L * Np, BN))
+        return cudaErrorInvalidValue;
+    Params p;
+    p.M = g.M;
+    p.N = g.N;
+    p.Kp = Kp;
+    p.Mp = Mp;
+    p.Np = Np;
+    p.L = L;
+    p.mtiles = Mp / BM;
+    p.ntiles = Np / BN;
+    p.items = L * p.mtiles * p.ntiles;
+    p.kext = g.kext;
+    p.U = cb.U;
+    p.err = d_err;
+    for (int l = 0; l < MAXL; l++) {
+        p.p[l] = md.p[l];
+        p.y[l] = md.y[l];
+        p.invpf[l] = md.invpf[l];
+    }
+    const int grid = std::min(sm_count(), p.items);
+    gemm_crt_kernel<<<grid, THREADS, SMEM_BYTES, st>>>(tmA, tmB, p);
+    crt_kernel<<<dim3((g.M + 255) / 256, g.N), 256, 0, st>>>(cb.U, Mp, Np, md, t, cb.ea, cb.eb, g.M, g.N, g.mlo, g.C,
+                                                            g.ldc, g.ccol, g.accumulate);
+    return cudaGetLastError();
+}
+
+int split_gemm_device(int kind, int slices, int M, int N, int K, const double *A, int lda, const double *B, int ldb,
+                      double *C, int ldc, int accumulate, cudaStream_t st)
+{
+    if (M <= 0 || N <= 0 || K <= 0) return 0;
+    if (K >= (1 << 16)) {
+        set_last_error("split GEMM: K must be below 65536");
+        return -1;
+    }
+    int dev = 0;
+    XTG_CK(cudaGetDevice(&dev));
+    configure_device(dev);
+    Scratch scr(st);
+    int *d_err = scr.get<int>(1);
+    if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
+    XTG_CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    GemmArgs<double> g{};
+    g.M = M;
+    g.N = N;
+    g.mlo = 0;
+    g.nseg = 1;
+    g.seg[0].A = A;
+    g.seg[0].lda = lda;
+    g.seg[0].acols = K;
+    g.seg[0].K = round_up(K, kKPad);
+    g.seg[0].boff = 0;
+    g.K = g.seg[0].K;
+    g.B = B;
+    g.ldb = ldb;
+    g.brows = K;
+    g.C = C;
+    g.ldc = ldc;
+    g.ccol = nullptr;
+    g.kext = nullptr;
+    g.accumulate = accumulate;
+    cudaError_t e;
+    if (kind == 2) {
+        CrtBufs cb;
+        e = launch_crt(g, std::max(2, std::min(slices, crt::MAXL)), cb, scr, d_err, st);
+    } else {
+        SplitBufs sb;
+        e = kind == 1 ? launch_split<split::kI8>(g, std::max(1, std::min(slices, 7)), sb, scr, d_err, st)
+                      : launch_split<split::kBF16>(g, std::max(1, std::min(slices, 6)), sb, scr, d_err, st);
+    }
+    if (e != cudaSuccess) {
+        set_last_error(std::string("split GEMM launch: ") + cudaGetErrorString(e));
+        return 1;
+    }
+    XTG_CK(cudaStreamSynchronize(st));
+    int h_err = 0;
+    XTG_CK(cudaMemcpy(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h_err) {
+        set_last_error("split GEMM: a bounded wait in the tensor-core pipeline expired");
+        return 1;
+    }
+    return 0;
+}
+
 template <class R, bool CPLX>
 int solve_device(char side, char howmny, const int *select, int n, const void *S_, int lds, const void *P_,
                  int ldp, const void *alpha_, const void *alphai_, const void *beta_, void *VL_, int ldvl,
@@ -425,7 +604,9 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
     R *d_sums = scr.get<R>(2 * (size_t)n);
     R *d_norms = scr.get<R>(2);
     // split-precision GEMMs: real double only; their bounded waits report through d_err
-    const int split_max = opt.split_kind == split::kI8 ? split::Cfg<split::kI8>::MAXS : split::Cfg<split::kBF16>::MAXS;
+    const int split_max = opt.split_kind == 2 ? crt::MAXL
+                          : opt.split_kind == split::kI8 ? split::Cfg<split::kI8>::MAXS
+                                                          : split::Cfg<split::kBF16>::MAXS;
     const int nsplit = (!CPLX && std::is_same<R, double>::value && opt.split > 0) ? std::min(opt.split, split_max)
                                                                                  : 0;
     int *d_err = nsplit ? scr.get<int>(1) : nullptr;
@@ -575,6 +756,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         const SideCols &sc = side_cols[left ? 1 : 0];
         const ColList &L = sc.L;
         SplitBufs sbuf;
+        CrtBufs cbuf;
         cudaError_t split_err = cudaSuccess;
         // C (+)= A B of one update or back-transform launch, FP64 DMMA/SIMT or BF16 slices
         auto gemm = [&](const GemmArgs<E> &g, cudaStream_t gs) {
@@ -582,8 +764,9 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
                 // launches with few output rows (the update of the upper block of a pair) do
                 // too little work per tile to amortise slicing and the tensor-core pipeline;
                 // they never use the slice buffers, so the buffers have one user stream
-                if (nsplit && g.M - g.mlo >= 512) {
-                    cudaError_t e = opt.split_kind == split::kI8
+                if (nsplit && g.M - g.mlo >= 512 && (opt.split_kind != 2 || g.K < (1 << 16))) {
+                    cudaError_t e = opt.split_kind == 2 ? launch_crt(g, nsplit, cbuf, scr, d_err, gs)
+                                    : opt.split_kind == split::kI8
                                         ? launch_split<split::kI8>(g, nsplit, sbuf, scr, d_err, gs)
                                         : launch_split<split::kBF16>(g, nsplit, sbuf, scr, d_err, gs);
                     if (e != cudaSuccess) split_err = e;
@@ -650,7 +833,8 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         // look-ahead (XTGEVC3_LOOKAHEAD): the trailing update of a block pair runs on a second
         // stream while the next pair is solved (see the loop below); off while tracing
         // (clean per-kernel times) and in arena mode (fixed scratch)
-        const bool ahead = opt.lookahead && !tr.on && !opt.arena && !opt.p_identity && blocks.size() >= 3;
+        const bool ahead = opt.lookahead && !tr.on && !opt.arena && !opt.p_identity && blocks.size() >= 3 &&
+                           !(nsplit && opt.split_kind == 2);
         // Without look-ahead, row blocks are taken in groups of `group` (one trailing GEMM
         // with K = 2 x the group's rows); arena mode keeps groups of two, so that its fixed
         // scratch holds the update operand.  Look-ahead takes pairs with padded blocks.

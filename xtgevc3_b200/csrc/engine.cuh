@@ -13,7 +13,7 @@ struct Options {
     int normalize = 0;  // scale every eigenvector to max |re| + |im| = 1 (LAPACK convention)
     int simt = 0;       // force the SIMT GEMM kernels instead of the tensor-core kernel
     int split = 0;      // > 0: FP64 GEMMs (real double) as slice products with this many slices
-    int split_kind = 0; // 0: BF16 slices (kind::f16), 1: INT8 slices (kind::i8)
+    int split_kind = 0; // 0: BF16 slices (kind::f16), 1: INT8 slices (kind::i8), 2: INT8 residues (CRT)
     int lookahead = 0;  // trailing updates on a second stream, overlapping the next solves
     // Standard problem (xTREVC3): P is the identity and the caller passes P = nullptr.  The
     // solver builds it from scratch for the diagonal-block solves and the norms; the update
@@ -78,6 +78,13 @@ template <class R, bool CPLX>
 int solve_device(char side, char howmny, const int *select, int n, const void *S, int lds, const void *P,
                  int ldp, const void *alpha, const void *alphai, const void *beta, void *VL, int ldvl, void *VR,
                  int ldvr, int m_total, const Options &opt, cudaStream_t st);
+
+// C (+)= A B (column-major FP64 device operands, M x K times K x N) through one of the
+// split-precision tensor-core paths: kind 0 BF16 slices, 1 INT8 digit slices, 2 INT8 residues
+// (slices = slice / modulus count).  Synchronous.  Returns 0, 1 (CUDA failure or an expired
+// bounded wait; message in last_error()) or -1 (bad argument).
+int split_gemm_device(int kind, int slices, int M, int N, int K, const double *A, int lda, const double *B, int ldb,
+                      double *C, int ldc, int accumulate, cudaStream_t st);
 
 // Once per device: memory-pool release threshold and the kernels' shared-memory limits.
 void configure_device(int dev);

@@ -1,0 +1,373 @@
+// Split-precision FP64 GEMM by residues (Chinese remainder theorem) on the INT8 tensor
+// cores (tcgen05 kind::i8).
+//
+//   C[mlo:M, j] (+)= sum_k A(m, k) B(k, j)        A, B, C in FP64
+//
+// Integers.  Row m of A is scaled by a power of two and rounded to an integer of at most
+// t bits, A'(m, k) = rint(A(m, k) 2^(t - ea_m)) with |A'| <= 2^t (ea_m: the exponent of the
+// row's largest entry); columns of B likewise (eb_j).  Then A B = 2^(ea + eb - 2t) A' B' up to
+// the rounding of the operands (2^-t relative to the row's / column's largest entry).
+//
+// Residues.  With L pairwise-coprime moduli p_l <= 256 (product P), the integer product
+// C' = A' B' is recovered from its residues: c_l = (A' mod p_l)(B' mod p_l) is one INT8 GEMM
+// per modulus (residues in [-128, 127], exact INT32 sums for K < 2^17), and
+//   C' = sum_l u_l M_l - k P,   M_l = P / p_l,   u_l = (c_l y_l) mod p_l,  y_l = M_l^-1 mod p_l,
+// with k = round(sum / P), exact when |C'| < P / 2, i.e. 2t + log2(K) + 1 < log2(P): t is
+// chosen from L and K on the host.  The number of tensor-core products is L (14 for ~47-bit
+// operands), against s(s+1)/2 = 28 digit products of 7-bit slices for 49 bits.
+//
+// Kernels (one GEMM = four launches):
+//   residue_rows_kernel / residue_cols_kernel: A' and B' residues, stored K-major as
+//       out[l][row][k] (INT8, row pitch Kp), with the exponents ea / eb;
+//   gemm_crt_kernel: persistent; work item (l, column tile, row tile), modulus outermost
+//       so that one modulus' operands stay in L2; tile 128 x 256, one CTA per SM.
+//       warp 0: TMA producer (64-byte K rows, 64-byte swizzle, STAGES-deep ring, no
+//               multicast); warp 1: TMEM allocation and MMA issue (one thread; two
+//               128 x 256 x 32 MMAs per stage into one of two TMEM accumulators of 256
+//               columns, so a tile's epilogue overlaps the next tile's MMAs); warps 2-9:
+//               epilogue, one TMEM lane (row) per thread and 128 columns per warp: u_l =
+//               (c_l y_l) mod p_l stored as one byte per element, U[l][col][row];
+//   crt_kernel: per element, the exact sums H = sum u_l M1_l, Mid = sum u_l M2_l (M_l ~
+//       M1_l 2^hi + M2_l 2^lo, each product and partial sum an exact FP64 integer), k, and
+//       C' = (H - k P1) 2^hi + (Mid - k P2) 2^lo, scaled by 2^(ea + eb - 2t) into C.
+// Every mbarrier wait is bounded (abort flag, global error word, in-flight copies and MMAs
+// drained, TMEM released).
+#pragma once
+#include "kernels_split.cuh"
+
+namespace xtg {
+namespace crt {
+
+constexpr int BM = 128;        // rows per tile (one TMEM lane each)
+constexpr int BN = 256;        // columns per tile (one accumulator = 256 TMEM columns)
+constexpr int BK = 64;         // K bytes per stage (one 64-byte swizzle row)
+constexpr int STAGES = 8;
+constexpr int THREADS = 320;   // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
+constexpr int EPI_WARPS = 8;
+constexpr int MAXL = 16;
+constexpr int A_TILE = BM * BK;                 // 8 KB
+constexpr int B_TILE = BN * BK;                 // 16 KB
+constexpr int SMEM_BYTES = STAGES * (A_TILE + B_TILE) + 1024;
+// S8 x S8 -> S32, K-major A and B, M = 128, N = 256
+constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(BM >> 4) << 24);
+// Moduli and reconstruction constants of one modulus count L (built on the host).
+struct Moduli {
+    int L;
+    int p[MAXL];        // moduli, largest first
+    int y[MAXL];        // (P / p_l)^-1 mod p_l
+    float invpf[MAXL];  // 1 / p_l
+    double invp[MAXL];
+    // M_l ~ m1_l 2^hi + m2_l 2^lo with m1_l, m2_l < 2^40 (bits below 2^lo dropped), so that
+    // every u_l m_l and every partial sum of L <= 16 of them is an exact FP64 integer
+    double m1[MAXL], m2[MAXL];
+    double P1, P2;      // the same split of P
+    double c1, c2;      // 2^hi / P, 2^lo / P
+    int hi, lo;
+    double log2P;
+};
+
+struct Params {
+    int M, N, Kp;        // Kp: padded K (multiple of BK)
+    int Mp, Np;          // rows of each modulus' A residues / columns of its B residues
+    int L, mtiles, ntiles, items;
+    const int *kext;     // per output column: K extent (nullptr: Kp)
+    unsigned char *U;    // u_l, [l][col][row], pitch Mp, Np columns per modulus
+    int *err;            // global error word (kErrWaitTimeout on a bounded-wait expiry)
+    int p[MAXL], y[MAXL];
+    float invpf[MAXL];
+};
+
+// ---- operand residues -------------------------------------------------------------------
+// v in (-1, 1): a = rint(v 2^t) (exact integer, |a| <= 2^t), residues a mod p_l in
+// [-128, 127] (symmetric; 128 mod 256 stored as -128).
+__device__ __forceinline__ void residues(double v, int t, const Moduli &md, int8_t *out, size_t stride)
+{
+    const double a = rint(ldexp(v, t));
+    for (int l = 0; l < md.L; l++) {
+        const double q = rint(a * md.invp[l]);
+        int r = (int)fma(-q, (double)md.p[l], a);  // exact: the result is a small integer
+        if (r > 127) r -= md.p[l];
+        if (r < -128) r += md.p[l];
+        out[(size_t)l * stride] = (int8_t)r;
+    }
+}
+
+// Rows of A (through the segment description of a GEMM launch) -> residues
+// out[l][row][k] (row pitch Kp, l-th block of Mp rows), ea[row].  One CTA = 32 rows.
+__global__ void __launch_bounds__(256) residue_rows_kernel(GemmArgs<double> g, int Kp, int Mp, int t, Moduli md,
+                                                           int8_t *out, int *ea)
+{
+    __shared__ double tile[64][33];
+    __shared__ double rmax[8][32];
+    const int r0 = blockIdx.x * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    double mx = 0.0;
+    const int row = r0 + tx;
+    for (int k = ty; k < g.K; k += 8) {
+        int kb = 0;
+        const int sg = find_seg(g, k, kb);
+        const int col = k - kb;
+        if (sg >= 0 && row < g.M && col < g.seg[sg].acols)
+            mx = fmax(mx, fabs(g.seg[sg].A[(size_t)row + (size_t)col * g.seg[sg].lda]));
+    }
+    rmax[ty][tx] = mx;
+    __syncthreads();
+    if (ty == 0) {
+        double m = rmax[0][tx];
+        for (int q = 1; q < 8; q++) m = fmax(m, rmax[q][tx]);
+        rmax[0][tx] = m;
+        if (row < Mp) ea[row] = split::scale_exp(m);
+    }
+    __syncthreads();
+    const int e = split::scale_exp(rmax[0][tx]);
+    for (int k0 = 0; k0 < Kp; k0 += 64) {
+        for (int kk = ty; kk < 64; kk += 8) {
+            const int k = k0 + kk;
+            double v = 0.0;
+            if (k < g.K) {
+                int kb = 0;
+                const int sg = find_seg(g, k, kb);
+                const int col = k - kb;
+                if (sg >= 0 && row < g.M && col < g.seg[sg].acols)
+                    v = g.seg[sg].A[(size_t)row + (size_t)col * g.seg[sg].lda];
+            }
+            tile[kk][tx] = ldexp(v, -e);
+        }
+        __syncthreads();
+        for (int rr = ty * 4; rr < ty * 4 + 4; rr++) {
+            const int gr = r0 + rr;
+            if (gr >= Mp) continue;
+            for (int h = 0; h < 2; h++) {
+                const int kk = tx + 32 * h;
+                if (k0 + kk >= Kp) continue;
+                residues(tile[kk][rr], t, md, out + (size_t)gr * Kp + k0 + kk, (size_t)Mp * Kp);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Columns of B (rows through the segment offsets) -> residues out[l][col][k], eb[col].
+// One warp per column, lanes along K.
+__global__ void __launch_bounds__(256) residue_cols_kernel(GemmArgs<double> g, int Kp, int Np, int t, Moduli md,
+                                                           int8_t *out, int *eb)
+{
+    const int col = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (col >= Np) return;
+    auto bval = [&](int k) -> double {
+        if (col >= g.N || k >= g.K) return 0.0;
+        int kb = 0;
+        const int sg = find_seg(g, k, kb);
+        if (sg < 0) return 0.0;
+        const int r = g.seg[sg].boff + k - kb;
+        if (r >= g.brows || k - kb >= g.seg[sg].acols) return 0.0;
+        return g.B[(size_t)r + (size_t)col * g.ldb];
+    };
+    double mx = 0.0;
+    for (int k = lane; k < g.K; k += 32) mx = fmax(mx, fabs(bval(k)));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const int e = split::scale_exp(mx);
+    if (lane == 0) eb[col] = e;
+    for (int k = lane; k < Kp; k += 32)
+        residues(ldexp(bval(k), -e), t, md, out + (size_t)col * Kp + k, (size_t)Np * Kp);
+}
+
+// ---- the residue GEMM ---------------------------------------------------------------------
+// (c y) mod p in [0, p) for |c| < 2^30, 0 < y < p <= 256.
+__device__ __forceinline__ int mod_mul(int c, int y, int p, float invp)
+{
+    const int q = __float2int_rn((float)c * invp);  // within a few units of c / p
+    const int r = c - q * p;                        // |r| < 4p
+    const int w = r * y;                            // |w| < 2^18: exact in FP32
+    const int q2 = __float2int_rd((float)w * invp);
+    int u = w - q2 * p;                             // in [-p, 2p)
+    u += u < 0 ? p : 0;
+    u -= u >= p ? p : 0;
+    return u;
+}
+
+__device__ __forceinline__ void item_tile(const Params &p, int item, int &l, int &m0, int &n0, int &ksteps)
+{
+    const int per = p.mtiles * p.ntiles;
+    l = item / per;
+    const int r = item - l * per;
+    const int nt = r / p.mtiles;
+    m0 = (r - nt * p.mtiles) * BM;
+    // with a per-column K extent (back-transform) the longest column tiles come first
+    n0 = (p.kext ? p.ntiles - 1 - nt : nt) * BN;
+    int kmax = p.Kp;
+    if (p.kext) kmax = min(kmax, p.kext[min(n0 + BN, p.N) - 1]);
+    ksteps = max(1, (kmax + BK - 1) / BK);
+}
+
+__global__ void __launch_bounds__(THREADS, 1)
+gemm_crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Params p)
+{
+    extern __shared__ __align__(16) unsigned char smem_crt[];
+    unsigned char *base = reinterpret_cast<unsigned char *>(((uintptr_t)smem_crt + 1023) & ~(uintptr_t)1023);
+    unsigned char *sA = base;                      // [STAGES][A_TILE]
+    unsigned char *sB = base + STAGES * A_TILE;    // [STAGES][B_TILE]
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], acc_full[2], acc_empty[2], mma_done;
+    __shared__ uint32_t tmem_base;
+    __shared__ volatile int abort_flag;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+        for (int q = 0; q < STAGES; q++) {
+            split::mbar_init(&full[q], 1);
+            split::mbar_init(&empty[q], 1);
+        }
+        for (int q = 0; q < 2; q++) {
+            split::mbar_init(&acc_full[q], 1);
+            split::mbar_init(&acc_empty[q], EPI_WARPS);
+        }
+        split::mbar_init(&mma_done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {  // TMEM: two accumulators of 256 columns
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         split::smem_u32(&tmem_base)),
+                     "r"(512));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    split::tc_fence_before();
+    __syncthreads();
+    split::tc_fence_after();
+    const uint32_t tmem = tmem_base;
+
+    if (warp == 0) {
+        // ---------------- TMA producer ----------------
+        if (lane == 0) {
+            long long use = 0;  // stage fills issued
+            for (int item = blockIdx.x; item < p.items && !abort_flag; item += gridDim.x) {
+                int l, m0, n0, ks;
+                item_tile(p, item, l, m0, n0, ks);
+                bool ok = true;
+                for (int k = 0; k < ks; k++, use++) {
+                    const int s = (int)(use % STAGES);
+                    if (use >= STAGES &&
+                        !split::mbar_wait(&empty[s], (uint32_t)(((use / STAGES) - 1) & 1), &abort_flag, p.err)) {
+                        ok = false;
+                        break;
+                    }
+                    split::mbar_expect_tx(&full[s], (uint32_t)(A_TILE + B_TILE));
+                    split::tma_load_2d(sA + s * A_TILE, &tmA, k * BK, l * p.Mp + m0, &full[s]);
+                    split::tma_load_2d(sB + s * B_TILE, &tmB, k * BK, l * p.Np + n0, &full[s]);
+                }
+                if (!ok) break;
+            }
+            if (abort_flag) {
+                // let every issued load land before the CTA can exit: the latest fill of
+                // stage s is its n-th with n = fills of s; it completes phase n - 1
+                for (int s = 0; s < STAGES; s++) {
+                    const long long fills = use / STAGES + (s < use % STAGES ? 1 : 0);
+                    if (fills) split::mbar_drain(&full[s], (uint32_t)((fills - 1) & 1));
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issue ----------------
+        if (lane == 0) {
+            long long use = 0;
+            int tcount = 0;
+            bool ok = true;
+            for (int item = blockIdx.x; item < p.items && ok; item += gridDim.x, tcount++) {
+                int l, m0, n0, ks;
+                item_tile(p, item, l, m0, n0, ks);
+                const int buf = tcount & 1;
+                if (tcount >= 2) {
+                    if (!split::mbar_wait(&acc_empty[buf], (uint32_t)(((tcount >> 1) - 1) & 1), &abort_flag, p.err))
+                        break;
+                    split::tc_fence_after();
+                }
+                const uint32_t dcol = tmem + (uint32_t)(buf * BN);
+                for (int k = 0; k < ks; k++, use++) {
+                    const int s = (int)(use % STAGES);
+                    if (!split::mbar_wait(&full[s], (uint32_t)((use / STAGES) & 1), &abort_flag, p.err)) {
+                        ok = false;
+                        break;
+                    }
+                    split::tc_fence_after();
+#pragma unroll
+                    for (int kk = 0; kk < 2; kk++)  // two 32-byte-deep MMAs per 64-byte K step
+                        split::umma_i8(dcol, split::smem_desc(sA + s * A_TILE, kk * 32),
+                                       split::smem_desc(sB + s * B_TILE, kk * 32), IDESC, (k | kk) ? 1u : 0u);
+                    split::umma_commit(&empty[s]);
+                }
+                if (ok) split::umma_commit(&acc_full[buf]);
+            }
+            // every MMA issued so far completes before TMEM can be released
+            split::umma_commit(&mma_done);
+            split::mbar_drain(&mma_done, 0);
+        }
+    } else {
+        // ---------------- epilogue: warps 2..9 ----------------
+        const int quad = warp & 3, half = (warp - 2) >> 2;
+        int tcount = 0;
+        for (int item = blockIdx.x; item < p.items; item += gridDim.x, tcount++) {
+            int l, m0, n0, ks;
+            item_tile(p, item, l, m0, n0, ks);
+            const int buf = tcount & 1;
+            if (!split::mbar_wait(&acc_full[buf], (uint32_t)((tcount >> 1) & 1), &abort_flag, p.err)) break;
+            split::tc_fence_after();
+            const int pl = p.p[l], yl = p.y[l];
+            const float ipl = p.invpf[l];
+            const int row = m0 + quad * 32 + lane;
+            unsigned char *Ul = p.U + (size_t)l * p.Np * p.Mp + row;
+            const uint32_t tb = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(buf * BN + half * 128);
+#pragma unroll 1
+            for (int h = 0; h < 128; h += 32) {
+                uint32_t v[32];
+                split::tmem_ld32(tb + (uint32_t)h, v);
+                split::tmem_wait_ld();
+                const int c0 = n0 + half * 128 + h;
+#pragma unroll
+                for (int q = 0; q < 32; q++)
+                    Ul[(size_t)(c0 + q) * p.Mp] = (unsigned char)mod_mul((int)v[q], yl, pl, ipl);
+            }
+            split::tc_fence_before();
+            __syncwarp();
+            if (lane == 0) split::mbar_arrive(&acc_empty[buf]);
+        }
+    }
+
+    split::tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        split::tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+    }
+}
+
+// ---- reconstruction ---------------------------------------------------------------------
+// One thread per element (rows along threads): C' from its L residues, scaled into C.
+__global__ void __launch_bounds__(256) crt_kernel(const unsigned char *U, int Mp, int Np, Moduli md, int t,
+                                                  const int *ea, const int *eb, int M, int N, int mlo, double *C,
+                                                  int ldc, const int *ccol, int accumulate)
+{
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    const int col = blockIdx.y;
+    if (row < mlo || row >= M || col >= N) return;
+    const unsigned char *u = U + (size_t)col * Mp + row;
+    const size_t plane = (size_t)Np * Mp;
+    double H = 0.0, Mid = 0.0;
+    for (int l = 0; l < md.L; l++) {
+        const double ul = (double)u[(size_t)l * plane];
+        H = fma(ul, md.m1[l], H);
+        Mid = fma(ul, md.m2[l], Mid);
+    }
+    const double k = rint(fma(H, md.c1, Mid * md.c2));
+    const double d1 = fma(-k, md.P1, H);   // exact integers
+    const double d2 = fma(-k, md.P2, Mid);
+    const double cp = ldexp(d1, md.hi) + ldexp(d2, md.lo);
+    const double v = ldexp(cp, ea[row] + eb[col] - 2 * t);
+    double *cptr = C + (size_t)(ccol ? ccol[col] : col) * ldc + row;
+    *cptr = accumulate ? *cptr + v : v;
+}
+
+}  // namespace crt
+}  // namespace xtg

@@ -67,6 +67,28 @@ __device__ __forceinline__ void rot(cplx<R> &x, cplx<R> &y, R c, cplx<R> s)
     y = yn;
 }
 
+// Complex product with every multiply and add rounded on its own (no fused multiply-add):
+// the swap's f and g are formed this way, as LAPACK forms them, so that a product at the
+// edge of the range overflows (and the swap is rejected) exactly when LAPACK's does.
+__device__ __forceinline__ cplx<double> cmul_sep(cplx<double> a, cplx<double> b)
+{
+    return {__dsub_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)), __dadd_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x))};
+}
+__device__ __forceinline__ cplx<float> cmul_sep(cplx<float> a, cplx<float> b)
+{
+    return {__fsub_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fadd_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x))};
+}
+__device__ __forceinline__ cplx<double> csub_sep(cplx<double> a, cplx<double> b)
+{
+    return {__dsub_rn(a.x, b.x), __dsub_rn(a.y, b.y)};
+}
+__device__ __forceinline__ cplx<float> csub_sep(cplx<float> a, cplx<float> b)
+{
+    return {__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y)};
+}
+template <class R>
+__device__ __forceinline__ bool cfinite(cplx<R> v) { return isfinite(v.x) && isfinite(v.y); }
+
 // Frobenius norm of a 2x2 block (scaled: no overflow or underflow of the squares)
 template <class R>
 __device__ __forceinline__ R fnorm2(cplx<R> a, cplx<R> b, cplx<R> c, cplx<R> d)
@@ -102,7 +124,8 @@ __global__ void __launch_bounds__(kReorderThreads) tgexc_cplx_kernel(ReorderArgs
             const C b10 = at(a.B, a.ldb, j + 1, j), b11 = at(a.B, a.ldb, j + 1, j + 1);
             const R tha = fmax(R(20) * eps * fnorm2(a00, a10, a01, a11), smlnum);
             const R thb = fmax(R(20) * eps * fnorm2(b00, b10, b01, b11), smlnum);
-            const C f = a11 * b00 - b11 * a00, g = a11 * b01 - b11 * a01;
+            const C f = csub_sep(cmul_sep(a11, b00), cmul_sep(b11, a00));
+            const C g = csub_sep(cmul_sep(a11, b01), cmul_sep(b11, a01));
             const R sa = cabs_(a11) * cabs_(b00), sb = cabs_(a00) * cabs_(b11);
             R cz;
             C sz;
@@ -121,7 +144,11 @@ __global__ void __launch_bounds__(kReorderThreads) tgexc_cplx_kernel(ReorderArgs
             rot(s01, s11, cq, sq);
             rot(t00, t10, cq, sq);
             rot(t01, t11, cq, sq);
-            bool ok = cabs_(s10) <= tha && cabs_(t10) <= thb;
+            // a swap whose rotations or blocks are not finite is rejected (LAPACK's tests
+            // compare NaN and fail the same way)
+            bool ok = cabs_(s10) <= tha && cabs_(t10) <= thb && isfinite(cz) && isfinite(cq) && cfinite(szc) &&
+                      cfinite(sq) && cfinite(s00) && cfinite(s01) && cfinite(s11) && cfinite(t00) && cfinite(t01) &&
+                      cfinite(t11);
             if (ok) {
                 // undo both rotations on the swapped blocks; the originals must come back
                 const C szu = -szc, squ = -sq;
