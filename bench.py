@@ -51,11 +51,14 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--ref-budget-s", type=float, default=240.0,
                     help="--impl reference: stop timing further full calls once this many seconds are spent")
-    ap.add_argument("--form", default="all", choices=["plain", "split", "split_i8", "all"],
-                    help="plain FP64, split precision with BF16 or INT8 slices, or all (the fastest one "
-                         "meeting the residual bound is the headline)")
+    ap.add_argument("--form", default="all", choices=["plain", "split", "split_i8", "split_crt", "all"],
+                    help="plain FP64, split precision with BF16 slices, INT8 slices or INT8 residues, or all (the "
+                         "fastest one meeting the residual bound is the headline)")
     ap.add_argument("--slices", type=int, default=6, help="BF16 slices of the split form")
     ap.add_argument("--slices-i8", type=int, default=7, help="INT8 slices of the split_i8 form")
+    ap.add_argument("--moduli", type=int, default=14, help="moduli of the split_crt (residue) form")
+    ap.add_argument("--gemm-only", action="store_true",
+                    help="time the split GEMM kinds and cuBLAS DGEMM on one n x n x n product and exit")
     ap.add_argument("--batch-count", type=int, default=2048,
                     help="pencils of the batched workload (0 skips it)")
     ap.add_argument("--batch-seed", type=int, default=2048)
@@ -67,8 +70,9 @@ def parse():
     ap.add_argument("--tgexc-n", type=int, default=4096, help="order of the ztgexc reordering leg (0 skips)")
     ap.add_argument("--profile-case", default=None,
                     help="run one small case for an ncu capture and exit (no JSON line): plain:N (two dtgevc3 "
-                         "B/B calls, FP64), split_i8:N (the same, INT8 split form), batch:COUNT (two launches "
-                         "of the batched dtgevc3 B/B kernel, tiles 32x32)")
+                         "B/B calls, FP64), split_i8:N / split_crt:N (the same, INT8 digit / residue split "
+                         "form), crt_gemm:N (two N^3 residue GEMMs), batch:COUNT (two launches of the batched "
+                         "dtgevc3 B/B kernel, tiles 32x32)")
     return ap.parse_args()
 
 
@@ -819,8 +823,20 @@ def profile_case(args):
     import xtgevc3_b200 as X
     kind, _, size = args.profile_case.partition(":")
     size = int(size)
-    if kind in ("plain", "split_i8"):
-        flags = 0 if kind == "plain" else X.SPLIT | X.SPLIT_INT8 | X.slices(7)
+    if kind == "crt_gemm":  # two residue GEMMs of size^3 (14 moduli)
+        g = torch.Generator(device="cuda")
+        g.manual_seed(1)
+        A = torch.randn(size, size, device="cuda", dtype=torch.float64, generator=g).t()
+        B = torch.randn(size, size, device="cuda", dtype=torch.float64, generator=g).t()
+        for _ in range(2):
+            C = X.split_gemm(2, A, B, slices=14)
+        torch.cuda.synchronize()
+        print(json.dumps({"case": args.profile_case, "fp64_flops": 2.0 * size ** 3,
+                          "max_abs": float(C.abs().max())}))
+        return 0
+    if kind in ("plain", "split_i8", "split_crt"):
+        flags = {"plain": 0, "split_i8": X.SPLIT | X.SPLIT_INT8 | X.slices(7),
+                 "split_crt": X.SPLIT | X.SPLIT_CRT | X.slices(14)}[kind]
         S_h, P_h, ar, ai, be = host_pencil(size, 3)
         S, P = colmajor_cuda(S_h, torch), colmajor_cuda(P_h, torch)
         Q, Z = orthogonal(size, 4, torch), orthogonal(size, 5, torch)
@@ -849,10 +865,44 @@ def profile_case(args):
     return 0
 
 
+def gemm_only(args):
+    """Split GEMM kinds and cuBLAS DGEMM on one n x n x n FP64 product (no JSON line)."""
+    import torch
+    import xtgevc3_b200 as X
+    n = min(args.n, 16384)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1)
+    A = torch.randn(n, n, device="cuda", dtype=torch.float64, generator=g).t()
+    B = torch.randn(n, n, device="cuda", dtype=torch.float64, generator=g).t()
+    C = torch.empty(n, n, device="cuda", dtype=torch.float64).t()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {}
+    ref = A @ B
+    for name, fn in (("dgemm", lambda: torch.matmul(A, B, out=C)),
+                     ("bf16_6", lambda: X.split_gemm(0, A, B, C=C, slices=6)),
+                     ("int8_7", lambda: X.split_gemm(1, A, B, C=C, slices=7)),
+                     ("crt_14", lambda: X.split_gemm(2, A, B, C=C, slices=14))):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(3):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        err = float((C - ref).abs().max() / ref.abs().max())
+        out[name] = {"ms": ms, "fp64_equiv_tflops": 2.0 * n ** 3 / (ms * 1e-3) / 1e12, "max_err_rel": err}
+    print(json.dumps({"n": n, "gemm": out}), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.profile_case:
         return profile_case(args)
+    if args.gemm_only:
+        return gemm_only(args)
     if args.impl == "reference":
         return reference_arm(args)
     import torch
@@ -889,8 +939,10 @@ def main():
 
     s = max(1, min(6, args.slices))
     s8 = max(1, min(7, args.slices_i8))
-    forms = {"plain": 0, "split": X.SPLIT | X.slices(s), "split_i8": X.SPLIT | X.SPLIT_INT8 | X.slices(s8)}
-    names = ["plain", "split", "split_i8"] if args.form == "all" else [args.form]
+    nm_crt = max(2, min(16, args.moduli))
+    forms = {"plain": 0, "split": X.SPLIT | X.slices(s), "split_i8": X.SPLIT | X.SPLIT_INT8 | X.slices(s8),
+             "split_crt": X.SPLIT | X.SPLIT_CRT | X.slices(nm_crt)}
+    names = ["plain", "split", "split_i8", "split_crt"] if args.form == "all" else [args.form]
     # the upstream library on the same inputs, once (rank 0 at N = 1): the CPU baseline, and
     # the reference result every form is compared with elementwise
     cpu, ref = None, None
@@ -931,6 +983,15 @@ def main():
                 "fp64_equivalent_tflops": kd["flops"] / (kd["ms"] * 1e-3) / 1e12,
                 "peak_source": "2 x MEASURED_PEAKS.json bf16_tflops (burst): INT8 dense rate, not measured; "
                                "INT8 slice products counted"}
+    elif kd["flops"] > 0 and head == "split_crt" and dom.startswith("gemm"):
+        # one INT8 product per modulus; the dense INT8 rate is twice the BF16 one on B200
+        achieved = nm_crt * kd["flops"] / (kd["ms"] * 1e-3) / 1e12
+        peak_i8 = 2.0 * peak_bf16
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak_i8, "unit": "TOP/s",
+                "frac": achieved / peak_i8, "kernel": dom,
+                "fp64_equivalent_tflops": kd["flops"] / (kd["ms"] * 1e-3) / 1e12,
+                "peak_source": "2 x MEASURED_PEAKS.json bf16_tflops (burst): INT8 dense rate, not measured; "
+                               "one INT8 product per modulus counted"}
     elif kd["flops"] > 0:
         achieved = kd["flops"] / (kd["ms"] * 1e-3) / 1e12
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak_fp64, "unit": "TFLOP/s",
@@ -1011,7 +1072,8 @@ def main():
 
     if rank == 0:
         form_desc = {"plain": "plain FP64 (DMMA)", "split": f"split precision, {s} BF16 slices (tcgen05)",
-                     "split_i8": f"split precision, {s8} INT8 slices (tcgen05 kind::i8)"}
+                     "split_i8": f"split precision, {s8} INT8 slices (tcgen05 kind::i8)",
+                     "split_crt": f"split precision, {nm_crt} INT8 residues (CRT, tcgen05 kind::i8)"}
         forms_out = {nm: {"value": r["value"], "ms_per_step": r["ms"], "resid_max": r["resid"],
                           "meets_resid_bound": r["resid"] <= 1e-12, "max_rel_diff_vs_reference": r["err_vs_ref"],
                           "kernels_ms_per_step": {k: v["ms_per_step"] for k, v in r["kernels"].items()}}

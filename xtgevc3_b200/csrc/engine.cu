@@ -370,7 +370,7 @@ static void build_moduli(crt::Moduli &md, int L)
     for (u128 v = P / (u128)kModuli[L - 1]; v; v >>= 1) bits++;
     md.hi = std::max(0, bits - 40);
     md.lo = std::max(0, md.hi - 40);
-    const u128 mask40 = (((u128)1) << 40) - 1;
+    const u128 mask_mid = (((u128)1) << (md.hi - md.lo)) - 1;  // bits [lo, hi) of M_l and P
     for (int l = 0; l < L; l++) {
         const int p = kModuli[l];
         const u128 Ml = P / (u128)p;
@@ -382,10 +382,10 @@ static void build_moduli(crt::Moduli &md, int L)
         md.invpf[l] = 1.0f / (float)p;
         md.invp[l] = 1.0 / (double)p;
         md.m1[l] = (double)(Ml >> md.hi);
-        md.m2[l] = (double)((Ml >> md.lo) & mask40);
+        md.m2[l] = (double)((Ml >> md.lo) & mask_mid);
     }
     md.P1 = (double)(P >> md.hi);
-    md.P2 = (double)((P >> md.lo) & mask40);
+    md.P2 = (double)((P >> md.lo) & mask_mid);
     const double Pd = (double)P;
     md.c1 = std::ldexp(1.0, md.hi) / Pd;
     md.c2 = std::ldexp(1.0, md.lo) / Pd;
