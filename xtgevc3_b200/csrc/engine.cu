@@ -416,7 +416,8 @@ struct CrtBufs {
     int8_t *A = nullptr, *B = nullptr;
     unsigned char *U = nullptr;
     int *ea = nullptr, *eb = nullptr;
-    size_t acap = 0, bcap = 0, ucap = 0, eacap = 0, ebcap = 0;
+    unsigned long long *rmax = nullptr;
+    size_t acap = 0, bcap = 0, ucap = 0, eacap = 0, ebcap = 0, rcap = 0;
 };
 
 static int sm_count()
@@ -441,8 +442,12 @@ static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scr
     if (un > cb.ucap) { cb.U = scr.get<unsigned char>(un); cb.ucap = un; }
     if ((size_t)Mp > cb.eacap) { cb.ea = scr.get<int>(Mp); cb.eacap = Mp; }
     if ((size_t)Np > cb.ebcap) { cb.eb = scr.get<int>(Np); cb.ebcap = Np; }
+    if ((size_t)Mp > cb.rcap) { cb.rmax = scr.get<unsigned long long>(Mp); cb.rcap = Mp; }
     if (scr.err) return scr.err;
-    residue_rows_kernel<<<Mp / 32, 256, 0, st>>>(g, Kp, Mp, t, md, cb.A, cb.ea);
+    cudaError_t e = cudaMemsetAsync(cb.rmax, 0, (size_t)Mp * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    row_absmax_kernel<<<dim3(Mp / 32, (g.K + 255) / 256), 256, 0, st>>>(g, cb.rmax);
+    residue_rows_kernel<<<dim3(Mp / 32, Kp / 64), 256, 0, st>>>(g, Kp, Mp, t, md, cb.rmax, cb.A, cb.ea);
     residue_cols_kernel<<<Np / 8, 256, 0, st>>>(g, Kp, Np, t, md, cb.B, cb.eb);
     CUtensorMap tmA, tmB;
     if (!slice_tensor_map(&tmA, cb.A, split::kI8, Kp, L * Mp, BM) ||

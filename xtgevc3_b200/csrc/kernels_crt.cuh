@@ -16,9 +16,9 @@
 // chosen from L and K on the host.  The number of tensor-core products is L (14 for ~47-bit
 // operands), against s(s+1)/2 = 28 digit products of 7-bit slices for 49 bits.
 //
-// Kernels (one GEMM = four launches):
-//   residue_rows_kernel / residue_cols_kernel: A' and B' residues, stored K-major as
-//       out[l][row][k] (INT8, row pitch Kp), with the exponents ea / eb;
+// Kernels (one GEMM = five launches):
+//   row_absmax_kernel, residue_rows_kernel / residue_cols_kernel: A' and B' residues, stored
+//       K-major as out[l][row][k] (INT8, row pitch Kp), with the exponents ea / eb;
 //   gemm_crt_kernel: persistent; work item (l, column tile, row tile), modulus outermost
 //       so that one modulus' operands stay in L2; tile 128 x 256, one CTA per SM.
 //       warp 0: TMA producer (64-byte K rows, 64-byte swizzle, STAGES-deep ring, no
@@ -79,49 +79,54 @@ struct Params {
 };
 
 // ---- operand residues -------------------------------------------------------------------
-// v in (-1, 1): a = rint(v 2^t) (exact integer, |a| <= 2^t), residues a mod p_l in
-// [-128, 127] (symmetric; 128 mod 256 stored as -128).
-__device__ __forceinline__ void residues(double v, int t, const Moduli &md, int8_t *out, size_t stride)
+// v in (-1, 1): a = rint(v 2^t) (exact integer, |a| <= 2^t), residue a mod p_l in [-128, 127]
+// (symmetric; 128 mod 256 stored as -128).
+__device__ __forceinline__ int residue(double a, int l, const Moduli &md)
 {
-    const double a = rint(ldexp(v, t));
-    for (int l = 0; l < md.L; l++) {
-        const double q = rint(a * md.invp[l]);
-        int r = (int)fma(-q, (double)md.p[l], a);  // exact: the result is a small integer
-        if (r > 127) r -= md.p[l];
-        if (r < -128) r += md.p[l];
-        out[(size_t)l * stride] = (int8_t)r;
-    }
+    const double q = rint(a * md.invp[l]);
+    int r = (int)fma(-q, (double)md.p[l], a);  // exact: the result is a small integer
+    if (r > 127) r -= md.p[l];
+    if (r < -128) r += md.p[l];
+    return r;
 }
 
-// Rows of A (through the segment description of a GEMM launch) -> residues
-// out[l][row][k] (row pitch Kp, l-th block of Mp rows), ea[row].  One CTA = 32 rows.
-__global__ void __launch_bounds__(256) residue_rows_kernel(GemmArgs<double> g, int Kp, int Mp, int t, Moduli md,
-                                                           int8_t *out, int *ea)
+// Largest |A(m, k)| of each row (through the segment description of a GEMM launch), as the
+// bit pattern of a non-negative double (ordered like the values), max-reduced into
+// rmax[row] (zeroed by the caller).  Grid: (Mp / 32, K chunks of 256); 256 threads, rows
+// along lanes (coalesced column-major reads).
+__global__ void __launch_bounds__(256) row_absmax_kernel(GemmArgs<double> g, unsigned long long *rmax)
 {
-    __shared__ double tile[64][33];
-    __shared__ double rmax[8][32];
-    const int r0 = blockIdx.x * 32;
+    __shared__ double part[8][32];
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int row = blockIdx.x * 32 + tx;
+    const int k0 = blockIdx.y * 256, k1 = min(g.K, k0 + 256);
     double mx = 0.0;
-    const int row = r0 + tx;
-    for (int k = ty; k < g.K; k += 8) {
+    for (int k = k0 + ty; k < k1; k += 8) {
         int kb = 0;
         const int sg = find_seg(g, k, kb);
         const int col = k - kb;
         if (sg >= 0 && row < g.M && col < g.seg[sg].acols)
             mx = fmax(mx, fabs(g.seg[sg].A[(size_t)row + (size_t)col * g.seg[sg].lda]));
     }
-    rmax[ty][tx] = mx;
+    part[ty][tx] = mx;
     __syncthreads();
     if (ty == 0) {
-        double m = rmax[0][tx];
-        for (int q = 1; q < 8; q++) m = fmax(m, rmax[q][tx]);
-        rmax[0][tx] = m;
-        if (row < Mp) ea[row] = split::scale_exp(m);
+        for (int q = 1; q < 8; q++) mx = fmax(mx, part[q][tx]);
+        if (mx > 0.0) atomicMax(&rmax[blockIdx.x * 32 + tx], (unsigned long long)__double_as_longlong(mx));
     }
-    __syncthreads();
-    const int e = split::scale_exp(rmax[0][tx]);
-    for (int k0 = 0; k0 < Kp; k0 += 64) {
+}
+
+// Rows of A -> residues out[l][row][k] (row pitch Kp, l-th block of Mp rows), ea[row].
+// Grid: (Mp / 32, Kp / 64): one CTA per 32 rows x 64 K; a thread computes 8 consecutive K
+// of one row and stores 8 bytes per modulus.
+__global__ void __launch_bounds__(256) residue_rows_kernel(GemmArgs<double> g, int Kp, int Mp, int t, Moduli md,
+                                                           const unsigned long long *rmax, int8_t *out, int *ea)
+{
+    __shared__ double tile[64][33];
+    const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 64;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    {
+        const int row = r0 + tx;
         for (int kk = ty; kk < 64; kk += 8) {
             const int k = k0 + kk;
             double v = 0.0;
@@ -132,24 +137,31 @@ __global__ void __launch_bounds__(256) residue_rows_kernel(GemmArgs<double> g, i
                 if (sg >= 0 && row < g.M && col < g.seg[sg].acols)
                     v = g.seg[sg].A[(size_t)row + (size_t)col * g.seg[sg].lda];
             }
-            tile[kk][tx] = ldexp(v, -e);
+            tile[kk][tx] = v;
         }
-        __syncthreads();
-        for (int rr = ty * 4; rr < ty * 4 + 4; rr++) {
-            const int gr = r0 + rr;
-            if (gr >= Mp) continue;
-            for (int h = 0; h < 2; h++) {
-                const int kk = tx + 32 * h;
-                if (k0 + kk >= Kp) continue;
-                residues(tile[kk][rr], t, md, out + (size_t)gr * Kp + k0 + kk, (size_t)Mp * Kp);
-            }
+    }
+    __syncthreads();
+    const int rr = threadIdx.x >> 3, kg = (threadIdx.x & 7) * 8;  // row rr, K kg .. kg + 7
+    const int row = r0 + rr;
+    const int e = split::scale_exp(__longlong_as_double((long long)rmax[row]));
+    if (blockIdx.y == 0 && kg == 0) ea[row] = e;
+    double a[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) a[q] = rint(ldexp(tile[kg + q][rr], t - e));
+    int8_t *o = out + (size_t)row * Kp + k0 + kg;
+    for (int l = 0; l < md.L; l++) {
+        uint32_t w0 = 0, w1 = 0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            w0 |= (uint32_t)(residue(a[q], l, md) & 0xff) << (8 * q);
+            w1 |= (uint32_t)(residue(a[q + 4], l, md) & 0xff) << (8 * q);
         }
-        __syncthreads();
+        *reinterpret_cast<uint2 *>(o + (size_t)l * Mp * Kp) = make_uint2(w0, w1);
     }
 }
 
 // Columns of B (rows through the segment offsets) -> residues out[l][col][k], eb[col].
-// One warp per column, lanes along K.
+// One warp per column; a lane handles 4 consecutive K per step and stores 4 bytes per modulus.
 __global__ void __launch_bounds__(256) residue_cols_kernel(GemmArgs<double> g, int Kp, int Np, int t, Moduli md,
                                                            int8_t *out, int *eb)
 {
@@ -171,8 +183,18 @@ __global__ void __launch_bounds__(256) residue_cols_kernel(GemmArgs<double> g, i
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     const int e = split::scale_exp(mx);
     if (lane == 0) eb[col] = e;
-    for (int k = lane; k < Kp; k += 32)
-        residues(ldexp(bval(k), -e), t, md, out + (size_t)col * Kp + k, (size_t)Np * Kp);
+    int8_t *o = out + (size_t)col * Kp;
+    for (int k = 4 * lane; k < Kp; k += 128) {  // Kp is a multiple of 64
+        double a[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) a[q] = rint(ldexp(bval(k + q), t - e));
+        for (int l = 0; l < md.L; l++) {
+            uint32_t w = 0;
+#pragma unroll
+            for (int q = 0; q < 4; q++) w |= (uint32_t)(residue(a[q], l, md) & 0xff) << (8 * q);
+            *reinterpret_cast<uint32_t *>(o + (size_t)l * Np * Kp + k) = w;
+        }
+    }
 }
 
 // ---- the residue GEMM ---------------------------------------------------------------------
@@ -354,11 +376,14 @@ __global__ void __launch_bounds__(256) crt_kernel(const unsigned char *U, int Mp
     if (row < mlo || row >= M || col >= N) return;
     const unsigned char *u = U + (size_t)col * Mp + row;
     const size_t plane = (size_t)Np * Mp;
+    unsigned char ub[MAXL];
+#pragma unroll
+    for (int l = 0; l < MAXL; l++) ub[l] = l < md.L ? u[(size_t)l * plane] : 0;  // all loads in flight at once
     double H = 0.0, Mid = 0.0;
-    for (int l = 0; l < md.L; l++) {
-        const double ul = (double)u[(size_t)l * plane];
-        H = fma(ul, md.m1[l], H);
-        Mid = fma(ul, md.m2[l], Mid);
+#pragma unroll
+    for (int l = 0; l < MAXL; l++) {
+        H = fma((double)ub[l], md.m1[l], H);
+        Mid = fma((double)ub[l], md.m2[l], Mid);
     }
     const double k = rint(fma(H, md.c1, Mid * md.c2));
     const double d1 = fma(-k, md.P1, H);   // exact integers
