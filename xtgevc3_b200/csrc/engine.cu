@@ -442,13 +442,15 @@ static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scr
     if (un > cb.ucap) { cb.U = scr.get<unsigned char>(un); cb.ucap = un; }
     if ((size_t)Mp > cb.eacap) { cb.ea = scr.get<int>(Mp); cb.eacap = Mp; }
     if ((size_t)Np > cb.ebcap) { cb.eb = scr.get<int>(Np); cb.ebcap = Np; }
-    if ((size_t)Mp > cb.rcap) { cb.rmax = scr.get<unsigned long long>(Mp); cb.rcap = Mp; }
+    if ((size_t)(Mp + Np) > cb.rcap) { cb.rmax = scr.get<unsigned long long>(Mp + Np); cb.rcap = Mp + Np; }
     if (scr.err) return scr.err;
-    cudaError_t e = cudaMemsetAsync(cb.rmax, 0, (size_t)Mp * sizeof(unsigned long long), st);
+    unsigned long long *cmax = cb.rmax + Mp;
+    cudaError_t e = cudaMemsetAsync(cb.rmax, 0, (size_t)(Mp + Np) * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
     row_absmax_kernel<<<dim3(Mp / 32, (g.K + 255) / 256), 256, 0, st>>>(g, cb.rmax);
+    col_absmax_kernel<<<dim3(Np / 32, Kp / 64), 256, 0, st>>>(g, cmax);
     residue_rows_kernel<<<dim3(Mp / 32, Kp / 64), 256, 0, st>>>(g, Kp, Mp, t, md, cb.rmax, cb.A, cb.ea);
-    residue_cols_kernel<<<Np / 8, 256, 0, st>>>(g, Kp, Np, t, md, cb.B, cb.eb);
+    residue_cols_kernel<<<dim3(Np / 32, Kp / 64), 256, 0, st>>>(g, Kp, Np, t, md, cmax, cb.B, cb.eb);
     CUtensorMap tmA, tmB;
     if (!slice_tensor_map(&tmA, cb.A, split::kI8, Kp, L * Mp, BM) ||
         !slice_tensor_map(&tmB, cb.B, split::kI8, Kp, L * Np, BN))
@@ -473,7 +475,7 @@ static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scr
     }
     const int grid = std::min(sm_count(), p.items);
     gemm_crt_kernel<<<grid, THREADS, SMEM_BYTES, st>>>(tmA, tmB, p);
-    crt_kernel<<<dim3((g.M + 255) / 256, g.N), 256, 0, st>>>(cb.U, Mp, Np, md, t, cb.ea, cb.eb, g.M, g.N, g.mlo, g.C,
+    crt_kernel<<<dim3((g.M + 1023) / 1024, g.N), 256, 0, st>>>(cb.U, Mp, Np, md, t, cb.ea, cb.eb, g.M, g.N, g.mlo, g.C,
                                                             g.ldc, g.ccol, g.accumulate);
     return cudaGetLastError();
 }

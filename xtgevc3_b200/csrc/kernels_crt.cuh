@@ -16,9 +16,10 @@
 // chosen from L and K on the host.  The number of tensor-core products is L (14 for ~47-bit
 // operands), against s(s+1)/2 = 28 digit products of 7-bit slices for 49 bits.
 //
-// Kernels (one GEMM = five launches):
-//   row_absmax_kernel, residue_rows_kernel / residue_cols_kernel: A' and B' residues, stored
-//       K-major as out[l][row][k] (INT8, row pitch Kp), with the exponents ea / eb;
+// Kernels (one GEMM = six launches):
+//   row_absmax_kernel / col_absmax_kernel, residue_rows_kernel / residue_cols_kernel: the
+//       exponents ea / eb, then A' and B' residues stored K-major as out[l][row][k] (INT8,
+//       row pitch Kp);
 //   gemm_crt_kernel: persistent; work item (l, column tile, row tile), modulus outermost
 //       so that one modulus' operands stay in L2; tile 128 x 256, one CTA per SM.
 //       warp 0: TMA producer (64-byte K rows, 64-byte swizzle, STAGES-deep ring, no
@@ -160,40 +161,64 @@ __global__ void __launch_bounds__(256) residue_rows_kernel(GemmArgs<double> g, i
     }
 }
 
-// Columns of B (rows through the segment offsets) -> residues out[l][col][k], eb[col].
-// One warp per column; a lane handles 4 consecutive K per step and stores 4 bytes per modulus.
-__global__ void __launch_bounds__(256) residue_cols_kernel(GemmArgs<double> g, int Kp, int Np, int t, Moduli md,
-                                                           int8_t *out, int *eb)
+// Eight consecutive K of column `col` of B (rows through the segment offsets; K segments are
+// multiples of 16 long, so k0 % 8 == 0 keeps the eight in one segment); zero outside B.
+__device__ __forceinline__ void b_values8(const GemmArgs<double> &g, int col, int k0, double (&v)[8])
 {
-    const int col = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (col >= Np) return;
-    auto bval = [&](int k) -> double {
-        if (col >= g.N || k >= g.K) return 0.0;
-        int kb = 0;
-        const int sg = find_seg(g, k, kb);
-        if (sg < 0) return 0.0;
-        const int r = g.seg[sg].boff + k - kb;
-        if (r >= g.brows || k - kb >= g.seg[sg].acols) return 0.0;
-        return g.B[(size_t)r + (size_t)col * g.ldb];
-    };
+#pragma unroll
+    for (int q = 0; q < 8; q++) v[q] = 0.0;
+    if (col >= g.N || k0 >= g.K) return;
+    int kb = 0;
+    const int sg = find_seg(g, k0, kb);
+    if (sg < 0) return;
+    const int off = k0 - kb;
+    const double *b = g.B + (size_t)g.seg[sg].boff + off + (size_t)col * g.ldb;
+#pragma unroll
+    for (int q = 0; q < 8; q++)
+        if (off + q < g.seg[sg].acols && g.seg[sg].boff + off + q < g.brows) v[q] = b[q];
+}
+
+// Largest |B(k, j)| of each column, as the bit pattern of a non-negative double, max-reduced
+// into cmax[col] (zeroed by the caller).  Grid: (Np / 32, Kp / 64); thread = (column t / 8,
+// K 8 (t % 8) .. +7 of the block's 64).
+__global__ void __launch_bounds__(256) col_absmax_kernel(GemmArgs<double> g, unsigned long long *cmax)
+{
+    const int col = blockIdx.x * 32 + (threadIdx.x >> 3);
+    const int k0 = blockIdx.y * 64 + (threadIdx.x & 7) * 8;
+    double v[8];
+    b_values8(g, col, k0, v);
     double mx = 0.0;
-    for (int k = lane; k < g.K; k += 32) mx = fmax(mx, fabs(bval(k)));
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    const int e = split::scale_exp(mx);
-    if (lane == 0) eb[col] = e;
-    int8_t *o = out + (size_t)col * Kp;
-    for (int k = 4 * lane; k < Kp; k += 128) {  // Kp is a multiple of 64
-        double a[4];
+    for (int q = 0; q < 8; q++) mx = fmax(mx, fabs(v[q]));
 #pragma unroll
-        for (int q = 0; q < 4; q++) a[q] = rint(ldexp(bval(k + q), t - e));
-        for (int l = 0; l < md.L; l++) {
-            uint32_t w = 0;
+    for (int o = 1; o < 8; o <<= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 7) == 0 && mx > 0.0) atomicMax(&cmax[col], (unsigned long long)__double_as_longlong(mx));
+}
+
+// Columns of B -> residues out[l][col][k] (column pitch Kp, l-th block of Np columns),
+// eb[col].  Grid: (Np / 32, Kp / 64), the thread layout of col_absmax_kernel; a thread
+// stores 8 bytes per modulus.
+__global__ void __launch_bounds__(256) residue_cols_kernel(GemmArgs<double> g, int Kp, int Np, int t, Moduli md,
+                                                           const unsigned long long *cmax, int8_t *out, int *eb)
+{
+    const int col = blockIdx.x * 32 + (threadIdx.x >> 3);
+    const int k0 = blockIdx.y * 64 + (threadIdx.x & 7) * 8;
+    const int e = split::scale_exp(__longlong_as_double((long long)cmax[col]));
+    if (blockIdx.y == 0 && (threadIdx.x & 7) == 0) eb[col] = e;
+    double v[8];
+    b_values8(g, col, k0, v);
+    double a[8];
 #pragma unroll
-            for (int q = 0; q < 4; q++) w |= (uint32_t)(residue(a[q], l, md) & 0xff) << (8 * q);
-            *reinterpret_cast<uint32_t *>(o + (size_t)l * Np * Kp + k) = w;
+    for (int q = 0; q < 8; q++) a[q] = rint(ldexp(v[q], t - e));
+    int8_t *o = out + (size_t)col * Kp + k0;
+    for (int l = 0; l < md.L; l++) {
+        uint32_t w0 = 0, w1 = 0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            w0 |= (uint32_t)(residue(a[q], l, md) & 0xff) << (8 * q);
+            w1 |= (uint32_t)(residue(a[q + 4], l, md) & 0xff) << (8 * q);
         }
+        *reinterpret_cast<uint2 *>(o + (size_t)l * Np * Kp) = make_uint2(w0, w1);
     }
 }
 
@@ -366,32 +391,44 @@ gemm_crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 }
 
 // ---- reconstruction ---------------------------------------------------------------------
-// One thread per element (rows along threads): C' from its L residues, scaled into C.
+// One thread per 4 consecutive rows of one column (grid: (Mp / 1024, N), 256 threads): the
+// 4 residues of each modulus come in one 32-bit load (a warp reads 128 contiguous bytes per
+// modulus), all L loads in flight before the arithmetic; C' of each element from its
+// residues, scaled into C.
 __global__ void __launch_bounds__(256) crt_kernel(const unsigned char *U, int Mp, int Np, Moduli md, int t,
                                                   const int *ea, const int *eb, int M, int N, int mlo, double *C,
                                                   int ldc, const int *ccol, int accumulate)
 {
-    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    const int row0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
     const int col = blockIdx.y;
-    if (row < mlo || row >= M || col >= N) return;
-    const unsigned char *u = U + (size_t)col * Mp + row;
+    if (row0 >= M || col >= N) return;
     const size_t plane = (size_t)Np * Mp;
-    unsigned char ub[MAXL];
+    const uint32_t *u = reinterpret_cast<const uint32_t *>(U + (size_t)col * Mp + row0);  // Mp % 128 == 0
+    uint32_t w[MAXL];
 #pragma unroll
-    for (int l = 0; l < MAXL; l++) ub[l] = l < md.L ? u[(size_t)l * plane] : 0;  // all loads in flight at once
-    double H = 0.0, Mid = 0.0;
+    for (int l = 0; l < MAXL; l++) w[l] = l < md.L ? u[(size_t)l * plane / 4] : 0u;
+    const double two_hi = ldexp(1.0, md.hi), two_lo = ldexp(1.0, md.lo);
+    const int ecol = eb[col] - 2 * t;
+    double *ccolp = C + (size_t)(ccol ? ccol[col] : col) * ldc;
 #pragma unroll
-    for (int l = 0; l < MAXL; l++) {
-        H = fma((double)ub[l], md.m1[l], H);
-        Mid = fma((double)ub[l], md.m2[l], Mid);
+    for (int q = 0; q < 4; q++) {
+        const int row = row0 + q;
+        if (row < mlo || row >= M) continue;
+        double H = 0.0, Mid = 0.0;
+#pragma unroll
+        for (int l = 0; l < MAXL; l++) {
+            const double ul = (double)((w[l] >> (8 * q)) & 0xffu);
+            H = fma(ul, md.m1[l], H);
+            Mid = fma(ul, md.m2[l], Mid);
+        }
+        const double k = rint(fma(H, md.c1, Mid * md.c2));
+        const double d1 = fma(-k, md.P1, H);  // exact integers
+        const double d2 = fma(-k, md.P2, Mid);
+        const double cp = fma(d1, two_hi, d2 * two_lo);  // both products exact (powers of two)
+        const double v = ldexp(cp, ea[row] + ecol);
+        double *cptr = ccolp + row;
+        *cptr = accumulate ? *cptr + v : v;
     }
-    const double k = rint(fma(H, md.c1, Mid * md.c2));
-    const double d1 = fma(-k, md.P1, H);   // exact integers
-    const double d2 = fma(-k, md.P2, Mid);
-    const double cp = ldexp(d1, md.hi) + ldexp(d2, md.lo);
-    const double v = ldexp(cp, ea[row] + eb[col] - 2 * t);
-    double *cptr = C + (size_t)(ccol ? ccol[col] : col) * ldc + row;
-    *cptr = accumulate ? *cptr + v : v;
 }
 
 }  // namespace crt
