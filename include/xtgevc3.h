@@ -59,6 +59,13 @@ extern "C" {
  * (default 14: ~47-bit operands at K = 8192; t = floor((log2 P - ceil(log2 K) - 2) / 2)).
  * L products replace the s(s+1)/2 of the digit slices. */
 #define XTGEVC3_SPLIT_CRT 32u
+/* Split forms: after the split pass, each eigenvector's relative residual in Schur
+ * coordinates, ||(beta S - alpha P) x||_2 / ((|beta| ||S||_1 + |alpha| ||P||_1) ||x||_2) in
+ * the scaling of the solve, is estimated from a 16-row random sketch; eigenvectors whose
+ * estimate exceeds a quarter of the bound (1e-12; the environment variable
+ * XTGEVC3_REFINE_BOUND overrides it) are solved again with FP64 GEMMs (the refinement step)
+ * and overwrite their output columns.  XTGEVC3_SPLIT_NO_REFINE skips the check. */
+#define XTGEVC3_SPLIT_NO_REFINE 64u
 /* Look-ahead schedule: the trailing update of each pair of row blocks runs on a second
  * stream while the next pair's diagonal solves run (guard rescaling of the rows that
  * update writes is deferred until it has finished).  Same results to rounding (the default
@@ -95,6 +102,9 @@ void xtgevc3_trace_reset(void);
 int xtgevc3_trace_get(int cls, long long *launches, double *ms, double *flops, double *bytes);
 const char *xtgevc3_trace_name(int cls);
 long long xtgevc3_launch_count(void);
+/* Eigenvector columns that the calling thread's last split-form call solved again in FP64
+ * (0 after any other call). */
+int xtgevc3_split_refined(void);
 
 /* ---- host-pointer entry points (drop-in) -------------------------------------------
  * C-linkage twins of dtgevc3/stgevc3/ztgevc3/ctgevc3 (include/tgevc3.h).  Inputs are

@@ -31,6 +31,12 @@ SPLIT = 4
 SPLIT_INT8 = 8
 LOOKAHEAD = 16
 SPLIT_CRT = 32
+SPLIT_NO_REFINE = 64
+
+
+def split_refined() -> int:
+    """Eigenvector columns the calling thread's last split-form call solved again in FP64."""
+    return int(lib().xtgevc3_split_refined())
 
 
 def slices(s: int) -> int:

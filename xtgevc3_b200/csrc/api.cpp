@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdint>
 #include <complex>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
 #include <vector>
@@ -31,6 +32,8 @@ xtg::Options make_opts(unsigned flags)
         const int s = (int)((flags >> 8) & 31u);
         o.split_kind = (flags & XTGEVC3_SPLIT_CRT) ? 2 : (flags & XTGEVC3_SPLIT_INT8) ? 1 : 0;
         o.split = s > 0 ? s : (o.split_kind == 2 ? 14 : o.split_kind ? 7 : 6);
+        o.refine = (flags & XTGEVC3_SPLIT_NO_REFINE) ? 0 : 1;
+        if (const char *v = std::getenv("XTGEVC3_REFINE_BOUND")) o.refine_bound = std::atof(v);
     }
     return o;
 }
@@ -729,6 +732,7 @@ int xtgevc3_trace_get(int cls, long long *launches, double *ms, double *flops, d
 }
 const char *xtgevc3_trace_name(int cls) { return xtg::trace_name(cls); }
 long long xtgevc3_launch_count(void) { return xtg::launch_count(); }
+int xtgevc3_split_refined(void) { return xtg::refined_columns(); }
 
 int xtgevc3_split_gemm_dev(void *stream, int kind, int slices, int M, int N, int K, const double *A, int lda,
                            const double *B, int ldb, double *C, int ldc, int accumulate)

@@ -23,6 +23,7 @@
 #include "kernels_misc.cuh"
 #include "kernels_split.cuh"
 #include "kernels_crt.cuh"
+#include "kernels_refine.cuh"
 #include "host_common.cuh"
 
 #include <cudaTypedefs.h>
@@ -40,6 +41,9 @@
 namespace xtg {
 
 static thread_local std::string g_err;
+// eigenvector columns the last split-form call of this thread solved again in FP64
+static thread_local int g_refined = 0;
+int refined_columns() { return g_refined; }
 const char *last_error() { return g_err.c_str(); }
 void set_last_error(const std::string &s) { g_err = s; }
 
@@ -201,6 +205,18 @@ struct CallRes {
     cudaStream_t side = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr, check = nullptr;
     int *status = nullptr;  // pinned host word written by the structure check's copy
+    uint8_t *hflags = nullptr;  // pinned refinement flags of the split form (grown on demand)
+    size_t hflags_cap = 0;
+    cudaError_t reserve_flags(size_t bytes)
+    {
+        if (bytes <= hflags_cap) return cudaSuccess;
+        if (hflags) cudaFreeHost(hflags);
+        hflags = nullptr;
+        hflags_cap = 0;
+        const cudaError_t e = cudaHostAlloc(reinterpret_cast<void **>(&hflags), bytes, cudaHostAllocDefault);
+        if (e == cudaSuccess) hflags_cap = bytes;
+        return e;
+    }
 };
 std::mutex g_res_mu;
 std::vector<CallRes *> g_res_free[64];
@@ -704,9 +720,15 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         const int *d_ints = nullptr;  // colk, src, kext, outcol, starts: m ints each
         const uint8_t *d_kind = nullptr;
     };
-    auto build_cols = [&](bool left, SideCols &sc) -> int {
+    // keep_k (optional): only the eigenvalues k with keep_k[k] set (their output columns kept)
+    auto build_cols = [&](bool left, SideCols &sc, const std::vector<char> *keep_k = nullptr) -> int {
         ColList &L = sc.L;
-        const int m = m_total;
+        int m = m_total;
+        if (keep_k) {
+            m = 0;
+            for (const Item &it : items)
+                if ((*keep_k)[it.k]) m += it.pair ? 2 : 1;
+        }
         L.m = m;
         L.colk.resize(m);
         L.src.resize(m);
@@ -715,6 +737,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         L.kind.resize(m);
         int c = 0;
         auto emit = [&](const Item &it) {
+            if (keep_k && !(*keep_k)[it.k]) return;
             int kk = left ? (it.pair ? n - 2 - it.k : n - 1 - it.k) : it.k;
             int w = it.pair ? 2 : 1;
             for (int q = 0; q < w; q++) {
@@ -759,8 +782,57 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
     }
 
     // One side on stream `st` with scratch from `scr` (both shadow the call's own).
-    auto run_side = [&](bool left, cudaStream_t st, Scratch &scr) -> int {
-        const SideCols &sc = side_cols[left ? 1 : 0];
+    // ---- refinement of the split form (real double) --------------------------------------------
+    // Each side's split pass flags the columns whose sketched residual exceeds the bound
+    // (d_flags, copied to pinned host memory before the call's final synchronisation); the
+    // flagged eigenvectors are then solved again with FP64 GEMMs and written over their
+    // output columns (the back-transform reuses the split pass's copy of Z / Q).
+    const bool refine_on = nsplit > 0 && opt.refine && !CPLX && std::is_same<R, double>::value;
+    uint8_t *d_flags = nullptr, *h_flags = nullptr;
+    if (refine_on) {
+        cudaError_t e = cudaSuccess;
+        CallRes *cr = res.get(&e);
+        XTG_CK(e);
+        XTG_CK(cr->reserve_flags(2 * (size_t)m_total));
+        h_flags = cr->hflags;
+        d_flags = scr.get<uint8_t>(2 * (size_t)m_total);
+        if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
+    }
+    auto refine_side = [&](const E *Sp, int lsp, const E *Pp, int lpp, const E *X, int ldx, const SideCols &sc,
+                           const R *coef, uint8_t *flags, cudaStream_t st, Scratch &scr) -> int {
+        if constexpr (!CPLX && std::is_same<R, double>::value) {
+            using namespace refine;
+            const int m = sc.L.m, nitems = (int)sc.starts.size();
+            double *GS = scr.get<double>((size_t)n * K);
+            double *GP = scr.get<double>((size_t)n * K);
+            double *T = scr.get<double>((size_t)m * (2 * K + 1));
+            int *cnt = scr.get<int>(1);
+            if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
+            XTG_CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
+            tr.run(kTPrep, 0, (double)n * n * esz, st, [&] {
+                sketch_matrix_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(Sp, lsp, n, 1, GS);
+                sketch_matrix_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(Pp, lpp, n, 0, GP);
+            });
+            tr.run(kTPrep, 0, 0.5 * (double)n * m * esz, st, [&] {
+                sketch_columns_kernel<<<(m + 7) / 8, 256, 0, st>>>(GS, GP, X, ldx, m, sc.d_ints + 2 * m, T);
+                refine_flags_kernel<<<(nitems + 255) / 256, 256, 0, st>>>(T, sc.d_ints + 4 * m, nitems, sc.d_kind,
+                                                                          coef, d_norms, opt.refine_bound, flags,
+                                                                          cnt);
+            });
+            XTG_CK(cudaGetLastError());
+            const size_t off = (size_t)(flags - d_flags);
+            XTG_CK(cudaMemcpyAsync(h_flags + off, flags, (size_t)m, cudaMemcpyDeviceToHost, st));
+        }
+        return 0;
+    };
+
+    // `o`: the options of this pass; `sc`: its column list; `plain`: FP64 GEMMs whatever the
+    // call's split form; `zc_in`: the back-transform's copy of Z / reversed Q made by an
+    // earlier pass (else made here), returned through `zc_keep`; `flags`: when set, the split
+    // pass writes one refinement flag per column of sc before anything goes to VL / VR.
+    auto run_side = [&](bool left, cudaStream_t st, Scratch &scr, const Options &o, const SideCols &sc, bool plain,
+                        E *zc_in, E **zc_keep, uint8_t *flags) -> int {
+        const int nsplit_side = plain ? 0 : nsplit;
         const ColList &L = sc.L;
         SplitBufs sbuf;
         CrtBufs cbuf;
@@ -771,16 +843,16 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
                 // launches with few output rows (the update of the upper block of a pair) do
                 // too little work per tile to amortise slicing and the tensor-core pipeline;
                 // they never use the slice buffers, so the buffers have one user stream
-                if (nsplit && g.M - g.mlo >= 512 && (opt.split_kind != 2 || g.K < (1 << 16))) {
-                    cudaError_t e = opt.split_kind == 2 ? launch_crt(g, nsplit, cbuf, scr, d_err, gs)
-                                    : opt.split_kind == split::kI8
-                                        ? launch_split<split::kI8>(g, nsplit, sbuf, scr, d_err, gs)
-                                        : launch_split<split::kBF16>(g, nsplit, sbuf, scr, d_err, gs);
+                if (nsplit_side && g.M - g.mlo >= 512 && (o.split_kind != 2 || g.K < (1 << 16))) {
+                    cudaError_t e = o.split_kind == 2 ? launch_crt(g, nsplit_side, cbuf, scr, d_err, gs)
+                                    : o.split_kind == split::kI8
+                                        ? launch_split<split::kI8>(g, nsplit_side, sbuf, scr, d_err, gs)
+                                        : launch_split<split::kBF16>(g, nsplit_side, sbuf, scr, d_err, gs);
                     if (e != cudaSuccess) split_err = e;
                     return;
                 }
             }
-            launch_gemm<E>(g, opt.simt != 0, gs);
+            launch_gemm<E>(g, o.simt != 0, gs);
         };
         // row blocks (problem orientation), bottom to top; a 2x2 block is never split
         auto split = [&](int j) -> bool {  // rows j-1, j form a 2x2 diagonal block
@@ -797,11 +869,11 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         }
 
         // ---- device buffers -------------------------------------------------------------
-        const int m = m_total;
+        const int m = L.m;
         const E *Sp = S, *Pp = P;
         int lsp = lds, lpp = ldp;
         // Left problem: (F S^H F, F P^H F).  Rows [0, t) of S and P become columns [n - t, n) of
-        // the transposed copies; t_done rows are done.  With opt.rows_ready (S and P still on
+        // the transposed copies; t_done rows are done.  With o.rows_ready (S and P still on
         // their way up) each group transposes the rows it needs once they have arrived,
         // otherwise all rows are transposed here.
         E *St = nullptr, *Pt = nullptr;
@@ -819,14 +891,14 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         };
         auto left_rows = [&](int need) {  // rows [0, need) of S, P on the device and transposed
             if (!left || need <= t_done) return;
-            const int got = opt.rows_ready ? std::min(n, std::max(need, opt.rows_ready(need, st))) : n;
+            const int got = o.rows_ready ? std::min(n, std::max(need, o.rows_ready(need, st))) : n;
             transpose_rows(got);
         };
         if (left) {
             St = scr.get<E>((size_t)ld_n * n);
-            Pt = opt.p_identity ? nullptr : scr.get<E>((size_t)ld_n * n);  // F I^H F = I
+            Pt = o.p_identity ? nullptr : scr.get<E>((size_t)ld_n * n);  // F I^H F = I
             if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
-            if (!opt.rows_ready) transpose_rows(n);
+            if (!o.rows_ready) transpose_rows(n);
             if (Pt) {
                 Pp = Pt;
                 lpp = ld_n;
@@ -840,12 +912,12 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         // look-ahead (XTGEVC3_LOOKAHEAD): the trailing update of a block pair runs on a second
         // stream while the next pair is solved (see the loop below); off while tracing
         // (clean per-kernel times) and in arena mode (fixed scratch)
-        const bool ahead = opt.lookahead && !tr.on && !opt.arena && !opt.p_identity && blocks.size() >= 3 &&
-                           !(nsplit && opt.split_kind == 2);
+        const bool ahead = o.lookahead && !tr.on && !o.arena && !o.p_identity && blocks.size() >= 3 &&
+                           !(nsplit_side && o.split_kind == 2);
         // Without look-ahead, row blocks are taken in groups of `group` (one trailing GEMM
         // with K = 2 x the group's rows); arena mode keeps groups of two, so that its fixed
         // scratch holds the update operand.  Look-ahead takes pairs with padded blocks.
-        const int group = opt.arena ? 2 : (nsplit ? kGroupBlocksSplit : kGroupBlocks);
+        const int group = o.arena ? 2 : (nsplit_side ? kGroupBlocksSplit : kGroupBlocks);
         const int ldx = ld_n;
         const int ldy = ahead ? 4 * kBlock : 2 * round_up(group * kBlock, kKPad);  // both halves
         E *X = scr.get<E>((size_t)ldx * m);
@@ -980,14 +1052,14 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         };
         const int nbk = (int)blocks.size();
         // the P strips of the identity are zero: the standard problem updates with S only
-        const int nstrips = opt.p_identity ? 1 : 2;
+        const int nstrips = o.p_identity ? 1 : 2;
         for (int gi = 0; !ahead && gi < nbk; gi += group) {
             const int ge = std::min(nbk, gi + group);  // blocks [gi, ge); blocks[gi] is the lowest
             const int q0 = blocks[ge - 1].first, q1 = blocks[gi].second;
             const int acols = q1 - q0, kq = round_up(acols, kKPad);
             // the group reads columns [q0, q1) of S and P (right problem: the caller's columns;
             // left problem: rows [n - q1, n - q0) of the caller's S and P, transposed)
-            if (opt.cols_ready && !left) opt.cols_ready(false, q0, st);
+            if (o.cols_ready && !left) o.cols_ready(false, q0, st);
             left_rows(n - q0);
             for (int bi = gi; bi < ge; bi++) {
                 const int r0 = blocks[bi].first, r1 = blocks[bi].second, jnb = r1 - r0, ys = r0 - q0;
@@ -1028,23 +1100,23 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         } guard{st2, ev_main, ev_tr};
         if (ahead) {
             // the second stream starts from events of this one: all of S and P first
-            if (opt.cols_ready && !left) opt.cols_ready(false, 0, st);
+            if (o.cols_ready && !left) o.cols_ready(false, 0, st);
             left_rows(n);
             // slice buffers of the trailing updates are sized here, on the main stream: growing
             // them inside a launch on the second stream would not be ordered with its use
             if constexpr (std::is_same<E, double>::value) {
-                if (nsplit) {
+                if (nsplit_side) {
                     const int kmax = 4 * kBlock;
                     auto reserve = [&](int bk, int bn, size_t esz_) {
-                        const size_t an = (size_t)nsplit * round_up(n, split::BM) * round_up(kmax, bk) * esz_;
-                        const size_t bn_ = (size_t)nsplit * round_up(m, bn) * round_up(kmax, bk) * esz_;
+                        const size_t an = (size_t)nsplit_side * round_up(n, split::BM) * round_up(kmax, bk) * esz_;
+                        const size_t bn_ = (size_t)nsplit_side * round_up(m, bn) * round_up(kmax, bk) * esz_;
                         if (an > sbuf.acap) { sbuf.A = scr.get<unsigned char>(an); sbuf.acap = an; }
                         if (bn_ > sbuf.bcap) { sbuf.B = scr.get<unsigned char>(bn_); sbuf.bcap = bn_; }
                         const size_t mp = round_up(n, split::BM), np = round_up(m, bn);
                         if (mp > sbuf.ecap_a) { sbuf.ea = scr.get<int>(mp); sbuf.ecap_a = mp; }
                         if (np > sbuf.ecap_b) { sbuf.eb = scr.get<int>(np); sbuf.ecap_b = np; }
                     };
-                    if (opt.split_kind == split::kI8)
+                    if (o.split_kind == split::kI8)
                         reserve(split::Cfg<split::kI8>::BK, split::Cfg<split::kI8>::BN, 1);
                     else
                         reserve(split::Cfg<split::kBF16>::BK, split::Cfg<split::kBF16>::BN, 2);
@@ -1118,12 +1190,20 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
 
         // LAPACK xTREVC3's phase for real 2x2 pairs (before the back-transform, which is linear)
         if constexpr (!CPLX) {
-            if (opt.lapack_pairs) {
+            if (o.lapack_pairs) {
                 lapack_pair_phase_kernel<R><<<(m * 32 + 255) / 256, 256, 0, st>>>(
                     reinterpret_cast<R *>(X), ldx, m, d_colk, d_kext, d_kind, reinterpret_cast<const R *>(Sp), lsp,
                     left ? 1 : 0);
                 XTG_CK(cudaGetLastError());
             }
+        }
+
+        // ---- refinement flags (split form) ---------------------------------------------------
+        // Sketched residual of every computed column in problem coordinates: columns whose
+        // residual exceeds the bound are flagged and solved again in FP64 after the call's
+        // split pass (see the end of solve_device).
+        if constexpr (!CPLX && std::is_same<R, double>::value) {
+            if (flags && refine_side(Sp, lsp, Pp, lpp, X, ldx, sc, coef, flags, st, scr)) return 1;
         }
 
         // ---- write-back / back-transform -----------------------------------------------------
@@ -1132,22 +1212,27 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         E *V = left ? VL : VR;
         const int ldv = left ? ldvl : ldvr;
         if (do_back) {
-            if (opt.back_ready[left ? 1 : 0]) XTG_CK(cudaStreamWaitEvent(st, opt.back_ready[left ? 1 : 0], 0));
-            // copy of Z (right) or column-reversed Q (left), so V can be overwritten
-            E *Zc = scr.get<E>((size_t)ld_n * n);
-            if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
-            if (left) {
-                dim3 g((n + 255) / 256, n);
-                tr.run(kTPrep, 0, 2.0 * n * n * esz, st,
-                       [&] { rev_columns_kernel<E><<<g, 256, 0, st>>>(V, ldv, Zc, ld_n, n, n); });
-            } else {
-                XTG_CK(cudaMemcpy2DAsync(Zc, (size_t)ld_n * sizeof(E), V, (size_t)ldv * sizeof(E), n * sizeof(E), n,
-                                         cudaMemcpyDeviceToDevice, st));
+            if (o.back_ready[left ? 1 : 0]) XTG_CK(cudaStreamWaitEvent(st, o.back_ready[left ? 1 : 0], 0));
+            // copy of Z (right) or column-reversed Q (left), so V can be overwritten; a later
+            // pass of the same call (the refinement) reuses it
+            E *Zc = zc_in;
+            if (!Zc) {
+                Zc = scr.get<E>((size_t)ld_n * n);
+                if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
+                if (left) {
+                    dim3 g((n + 255) / 256, n);
+                    tr.run(kTPrep, 0, 2.0 * n * n * esz, st,
+                           [&] { rev_columns_kernel<E><<<g, 256, 0, st>>>(V, ldv, Zc, ld_n, n, n); });
+                } else {
+                    XTG_CK(cudaMemcpy2DAsync(Zc, (size_t)ld_n * sizeof(E), V, (size_t)ldv * sizeof(E), n * sizeof(E),
+                                             n, cudaMemcpyDeviceToDevice, st));
+                }
             }
+            if (zc_keep) *zc_keep = Zc;
             // column chunks of equal work (sum of kext), never splitting a complex pair, so
             // that a caller can download each chunk's output columns while the next runs
             std::vector<int> cuts = {0};
-            if (opt.cols_done && !opt.normalize) {
+            if (o.cols_done && !o.normalize) {
                 double tot = 0;
                 for (int c = 0; c < m; c++) tot += L.kext[c];
                 const int nch = std::min(4, m);
@@ -1182,13 +1267,13 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
                 const double bf = 2.0 * n * bk * cfl;
                 const double bb = ((double)n * L.kext[c1 - 1] + bk + (double)n * (c1 - c0)) * esz;
                 tr.run(kTBack, bf, bb, st, [&] { gemm(g, st); });
-                if (opt.cols_done && !opt.normalize) {
+                if (o.cols_done && !o.normalize) {
                     int o0 = m, o1 = 0;
                     for (int c = c0; c < c1; c++) {
                         o0 = std::min(o0, L.outcol[c]);
                         o1 = std::max(o1, L.outcol[c] + 1);
                     }
-                    if (o1 - o0 == c1 - c0) opt.cols_done(left, st, o0, o1);  // a contiguous block of outputs
+                    if (o1 - o0 == c1 - c0) o.cols_done(left, st, o0, o1);  // a contiguous block of outputs
                 }
             }
         } else {
@@ -1199,19 +1284,14 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         }
         XTG_CK(cudaGetLastError());
 
-        if (opt.normalize) {
+        if (o.normalize) {
             if constexpr (CPLX) {
                 tr.run(kTNormalize, 0, 2.0 * n * m * esz, st, [&] {
-                    normalize_cplx_kernel<R><<<m, 256, 0, st>>>(reinterpret_cast<cplx<R> *>(V), ldv, n, m);
+                    normalize_cplx_kernel<R><<<m, 256, 0, st>>>(reinterpret_cast<cplx<R> *>(V), ldv, n, d_outcol, m);
                 });
             } else {
-                std::vector<uint8_t> ok(m, kReal);
-                for (int c = 0; c < m; c++) ok[L.outcol[c]] = L.kind[c];
-                uint8_t *d_ok = scr.get<uint8_t>(m);
-                if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
-                XTG_CK(cudaMemcpyAsync(d_ok, ok.data(), m, cudaMemcpyHostToDevice, st));
                 tr.run(kTNormalize, 0, 2.0 * n * m * esz, st,
-                       [&] { normalize_real_kernel<R><<<m, 256, 0, st>>>(V, ldv, n, d_ok, m); });
+                       [&] { normalize_real_kernel<R><<<m, 256, 0, st>>>(V, ldv, n, d_outcol, d_kind, m); });
             }
             XTG_CK(cudaGetLastError());
         }
@@ -1219,7 +1299,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             set_last_error(std::string("split-precision GEMM launch: ") + cudaGetErrorString(split_err));
             return 1;
         }
-        if (opt.side_done) opt.side_done(left, st);
+        if (o.side_done) o.side_done(left, st);
         return 0;
     };
 
@@ -1235,20 +1315,21 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         return solve_device<R, CPLX>(side, howmny, select, n, S_, lds, P_, ldp, alpha_, alphai_, beta_, VL_, ldvl,
                                      VR_, ldvr, m_total, o2, st);
     };
+    E *zc_kept[2] = {nullptr, nullptr};  // each side's copy of Z / reversed Q (refinement pass)
+    Scratch scr2(st);                    // the left side's scratch when it runs on its own stream
     if (want_r && want_l && !tr.on && !opt.arena) {
         cudaError_t e = cudaSuccess;
         CallRes *fk = res.get(&e);
+        scr2.st = fk->side;
         XTG_CK(e);
         XTG_CK(cudaEventRecord(fk->fork, st));
         XTG_CK(cudaStreamWaitEvent(fk->side, fk->fork, 0));
         int rr = 0, rl = 0;
-        {
-            Scratch scr2(fk->side);
-            rr = run_side(false, st, scr);
-            if (rr == 0) rl = run_side(true, fk->side, scr2);
-            XTG_CK(cudaEventRecord(fk->join, fk->side));
-            XTG_CK(cudaStreamWaitEvent(st, fk->join, 0));
-        }
+        rr = run_side(false, st, scr, opt, side_cols[0], false, nullptr, &zc_kept[0], d_flags);
+        if (rr == 0) rl = run_side(true, fk->side, scr2, opt, side_cols[1], false, nullptr, &zc_kept[1],
+                                   d_flags ? d_flags + m_total : nullptr);
+        XTG_CK(cudaEventRecord(fk->join, fk->side));
+        XTG_CK(cudaStreamWaitEvent(st, fk->join, 0));
         if (rr == 1 || rl == 1) {
             cudaStreamSynchronize(fk->side);
             return 1;
@@ -1256,15 +1337,61 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         if (rr == 2 || rl == 2) return rerun();
     } else {
         const size_t mark = scr.used;
-        int rc = want_r ? run_side(false, st, scr) : 0;
+        int rc = want_r ? run_side(false, st, scr, opt, side_cols[0], false, nullptr, &zc_kept[0], d_flags) : 0;
         // arena: the right side's slices are reused; its kernels precede the left side's
         // on the same stream
         if (opt.arena) scr.used = mark;
-        if (rc == 0 && want_l) rc = run_side(true, st, scr);
+        if (rc == 0 && want_l)
+            rc = run_side(true, st, scr, opt, side_cols[1], false, nullptr, &zc_kept[1],
+                          d_flags ? d_flags + m_total : nullptr);
         if (rc == 2) return rerun();
         if (rc) return 1;
     }
     XTG_CK(cudaStreamSynchronize(st));
+    int refined = 0;
+    if (refine_on) {
+        // the FP64 pass over the flagged eigenvectors of each side, on the call's stream
+        Options ro = opt;
+        ro.staged = nullptr;
+        ro.host_norms = nullptr;
+        ro.cols_ready = nullptr;
+        ro.rows_ready = nullptr;
+        ro.side_done = nullptr;
+        ro.cols_done = nullptr;
+        ro.back_ready[0] = ro.back_ready[1] = nullptr;
+        for (int sd = 0; sd < 2; sd++) {
+            if (!(sd ? want_l : want_r)) continue;
+            const SideCols &sc = side_cols[sd];
+            const uint8_t *fl = h_flags + (sd ? m_total : 0);
+            std::vector<char> keep(n, 0);
+            int cnt = 0;
+            for (int c = 0; c < sc.L.m; c++)
+                if (fl[c]) {
+                    keep[sc.L.src[c]] = 1;
+                    cnt++;
+                }
+            if (!cnt) continue;
+            refined += cnt;
+            SideCols sub;
+            if (build_cols(sd == 1, sub, &keep)) return 1;
+            const int rc = run_side(sd == 1, st, scr, ro, sub, true, zc_kept[sd], nullptr, nullptr);
+            if (rc) return rc == 2 ? rerun() : 1;
+            if (opt.cols_done || opt.side_done) {
+                // the host-pointer path: download the rewritten output columns again
+                std::vector<int> oc(sub.L.outcol);
+                std::sort(oc.begin(), oc.end());
+                for (size_t a = 0; a < oc.size();) {
+                    size_t b = a + 1;
+                    while (b < oc.size() && oc[b] == oc[b - 1] + 1) b++;
+                    if (opt.cols_done) opt.cols_done(sd == 1, st, oc[a], oc[b - 1] + 1);
+                    a = b;
+                }
+                if (!opt.cols_done) opt.side_done(sd == 1, st);
+            }
+        }
+        XTG_CK(cudaStreamSynchronize(st));
+    }
+    g_refined = refined;
     tr.flush();
     if (d_err) {
         int h_err = 0;

@@ -14,6 +14,10 @@ struct Options {
     int simt = 0;       // force the SIMT GEMM kernels instead of the tensor-core kernel
     int split = 0;      // > 0: FP64 GEMMs (real double) as slice products with this many slices
     int split_kind = 0; // 0: BF16 slices (kind::f16), 1: INT8 slices (kind::i8), 2: INT8 residues (CRT)
+    // Split forms: columns whose sketched relative residual exceeds refine_bound are solved
+    // again with FP64 GEMMs (refine = 0 leaves them as they are).
+    int refine = 1;
+    double refine_bound = 1e-12;
     int lookahead = 0;  // trailing updates on a second stream, overlapping the next solves
     // Standard problem (xTREVC3): P is the identity and the caller passes P = nullptr.  The
     // solver builds it from scratch for the diagonal-block solves and the norms; the update
@@ -90,6 +94,8 @@ int split_gemm_device(int kind, int slices, int M, int N, int K, const double *A
 void configure_device(int dev);
 
 const char *last_error();
+// Columns the last split-form call on this thread solved again in FP64 (0 for other calls).
+int refined_columns();
 void set_last_error(const std::string &s);
 
 // Kernel trace: per kernel class, launches, CUDA-event time on the launching stream and

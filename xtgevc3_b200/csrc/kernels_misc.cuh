@@ -198,13 +198,13 @@ __global__ void writeback_kernel(const E *X, int ldx, E *V, int ldv, int n, int 
 // eigenvector is scaled so that max_i (|re_i| + |im_i|) = 1, a real pair (Re, Im) jointly.
 // One CTA per eigenvector; the column (pair) is read twice, the second time from L2.
 template <class R>
-__global__ void normalize_real_kernel(R *V, int ldv, int n, const uint8_t *outkind, int m)
+__global__ void normalize_real_kernel(R *V, int ldv, int n, const int *outcol, const uint8_t *kind, int m)
 {
     int c = blockIdx.x;
     if (c >= m) return;
-    uint8_t kd = outkind[c];
+    uint8_t kd = kind[c];
     if (kd == kPairIm) return;
-    R *v0 = V + (size_t)c * ldv;
+    R *v0 = V + (size_t)outcol[c] * ldv;  // a pair's (Re, Im) output columns are adjacent
     R *v1 = kd == kPairRe ? v0 + ldv : nullptr;
     R mx = 0;
     for (int r = threadIdx.x; r < n; r += blockDim.x) mx = fmax(mx, fabs(v0[r]) + (v1 ? fabs(v1[r]) : R(0)));
@@ -230,11 +230,11 @@ __global__ void normalize_real_kernel(R *V, int ldv, int n, const uint8_t *outki
 }
 
 template <class R>
-__global__ void normalize_cplx_kernel(cplx<R> *V, int ldv, int n, int m)
+__global__ void normalize_cplx_kernel(cplx<R> *V, int ldv, int n, const int *outcol, int m)
 {
     int c = blockIdx.x;
     if (c >= m) return;
-    cplx<R> *v = V + (size_t)c * ldv;
+    cplx<R> *v = V + (size_t)outcol[c] * ldv;
     R mx = 0;
     for (int r = threadIdx.x; r < n; r += blockDim.x) mx = fmax(mx, l1abs(v[r]));
     __shared__ R red[32];
