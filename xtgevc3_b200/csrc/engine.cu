@@ -382,23 +382,23 @@ static void build_moduli(crt::Moduli &md, int L)
     md.L = L;
     u128 P = 1;
     for (int l = 0; l < L; l++) P *= (u128)kModuli[l];
-    int bits = 0;  // bits of the largest M_l = P / p_{L-1}
-    for (u128 v = P / (u128)kModuli[L - 1]; v; v >>= 1) bits++;
-    md.hi = std::max(0, bits - 40);
-    md.lo = std::max(0, md.hi - 40);
-    const u128 mask_mid = (((u128)1) << (md.hi - md.lo)) - 1;  // bits [lo, hi) of M_l and P
+    int bits = 0;  // bits of P (every weight W_l < P)
+    for (u128 v = P; v; v >>= 1) bits++;
+    md.hi = std::max(0, bits - 41);
+    md.lo = std::max(0, md.hi - 41);
+    const u128 mask_mid = (((u128)1) << (md.hi - md.lo)) - 1;  // bits [lo, hi) of W_l and P
     for (int l = 0; l < L; l++) {
         const int p = kModuli[l];
         const u128 Ml = P / (u128)p;
         const int r = (int)(Ml % (u128)p);
         int y = 1;
         while ((r * y) % p != 1) y++;  // the inverse exists: the moduli are pairwise coprime
+        const u128 W = Ml * (u128)y;  // < Ml p = P (y < p): the weight is already reduced mod P
         md.p[l] = p;
-        md.y[l] = y;
-        md.invpf[l] = 1.0f / (float)p;
+        md.barrett[l] = (unsigned int)((((unsigned long long)1) << 32) / (unsigned long long)p);
         md.invp[l] = 1.0 / (double)p;
-        md.m1[l] = (double)(Ml >> md.hi);
-        md.m2[l] = (double)((Ml >> md.lo) & mask_mid);
+        md.w1[l] = (double)(W >> md.hi);
+        md.w2[l] = (double)((W >> md.lo) & mask_mid);
     }
     md.P1 = (double)(P >> md.hi);
     md.P2 = (double)((P >> md.lo) & mask_mid);
@@ -450,7 +450,7 @@ static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scr
 {
     using namespace crt;
     const Moduli &md = crt_moduli(L);
-    const int Kp = round_up(g.K, BK), Mp = round_up(g.M, BM), Np = round_up(g.N, BN);
+    const int Kp = round_up(g.K, BK), Mp = round_up(g.M, TM), Np = round_up(g.N, TN);
     const int t = crt_bits(L, g.K);
     const size_t an = (size_t)L * Mp * Kp, bn = (size_t)L * Np * Kp, un = (size_t)L * Np * Mp;
     if (an > cb.acap) { cb.A = scr.get<int8_t>(an); cb.acap = an; }
@@ -468,8 +468,8 @@ static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scr
     residue_rows_kernel<<<dim3(Mp / 32, Kp / 64), 256, 0, st>>>(g, Kp, Mp, t, md, cb.rmax, cb.A, cb.ea);
     residue_cols_kernel<<<dim3(Np / 32, Kp / 64), 256, 0, st>>>(g, Kp, Np, t, md, cmax, cb.B, cb.eb);
     CUtensorMap tmA, tmB;
-    if (!slice_tensor_map(&tmA, cb.A, split::kI8, Kp, L * Mp, BM) ||
-        !slice_tensor_map(&tmB, cb.B, split::kI8, Kp, L * Np, BN))
+    if (!slice_tensor_map(&tmA, cb.A, split::kI8, Kp, L * Mp, TM) ||
+        !slice_tensor_map(&tmB, cb.B, split::kI8, Kp, L * Np, TN))
         return cudaErrorInvalidValue;
     Params p;
     p.M = g.M;
@@ -478,16 +478,15 @@ static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scr
     p.Mp = Mp;
     p.Np = Np;
     p.L = L;
-    p.mtiles = Mp / BM;
-    p.ntiles = Np / BN;
+    p.mtiles = Mp / TM;
+    p.ntiles = Np / TN;
     p.items = L * p.mtiles * p.ntiles;
     p.kext = g.kext;
     p.U = cb.U;
     p.err = d_err;
     for (int l = 0; l < MAXL; l++) {
         p.p[l] = md.p[l];
-        p.y[l] = md.y[l];
-        p.invpf[l] = md.invpf[l];
+        p.barrett[l] = md.barrett[l];
     }
     const int grid = std::min(sm_count(), p.items);
     gemm_crt_kernel<<<grid, THREADS, SMEM_BYTES, st>>>(tmA, tmB, p);

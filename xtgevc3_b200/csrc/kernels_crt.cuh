@@ -10,9 +10,9 @@
 //
 // Residues.  With L pairwise-coprime moduli p_l <= 256 (product P), the integer product
 // C' = A' B' is recovered from its residues: c_l = (A' mod p_l)(B' mod p_l) is one INT8 GEMM
-// per modulus (residues in [-128, 127], exact INT32 sums for K < 2^17), and
-//   C' = sum_l u_l M_l - k P,   M_l = P / p_l,   u_l = (c_l y_l) mod p_l,  y_l = M_l^-1 mod p_l,
-// with k = round(sum / P), exact when |C'| < P / 2, i.e. 2t + log2(K) + 1 < log2(P): t is
+// per modulus (residues in [-128, 127], exact INT32 sums), and
+//   C' = sum_l r_l W_l - k P,   r_l = c_l mod p_l,   W_l = M_l (M_l^-1 mod p_l) mod P,  M_l = P / p_l,
+// with k = round(sum / P), exact when |C'| < P / 4, i.e. 2t + log2(K) + 2 <= log2(P): t is
 // chosen from L and K on the host.  The number of tensor-core products is L (14 for ~47-bit
 // operands), against s(s+1)/2 = 28 digit products of 7-bit slices for 49 bits.
 //
@@ -21,15 +21,17 @@
 //       exponents ea / eb, then A' and B' residues stored K-major as out[l][row][k] (INT8,
 //       row pitch Kp);
 //   gemm_crt_kernel: persistent; work item (l, column tile, row tile), modulus outermost
-//       so that one modulus' operands stay in L2; tile 128 x 256, one CTA per SM.
+//       so that one modulus' operands stay in L2; tile 256 rows x 128 columns of C, computed
+//       transposed (MMA M = the tile's columns, N = its rows), one CTA per SM.
 //       warp 0: TMA producer (64-byte K rows, 64-byte swizzle, STAGES-deep ring, no
 //               multicast); warp 1: TMEM allocation and MMA issue (one thread; two
 //               128 x 256 x 32 MMAs per stage into one of two TMEM accumulators of 256
 //               columns, so a tile's epilogue overlaps the next tile's MMAs); warps 2-9:
-//               epilogue, one TMEM lane (row) per thread and 128 columns per warp: u_l =
-//               (c_l y_l) mod p_l stored as one byte per element, U[l][col][row];
-//   crt_kernel: per element, the exact sums H = sum u_l M1_l, Mid = sum u_l M2_l (M_l ~
-//       M1_l 2^hi + M2_l 2^lo, each product and partial sum an exact FP64 integer), k, and
+//               epilogue, one TMEM lane (a column of C) per thread, 128 rows per warp in
+//               chunks of 32: r_l = c_l mod p_l (integer Barrett reduction) stored as 32
+//               contiguous bytes of U[l][col][row];
+//   crt_kernel: per element, the exact sums H = sum r_l W1_l, Mid = sum r_l W2_l (W_l ~
+//       W1_l 2^hi + W2_l 2^lo, each product and partial sum an exact FP64 integer), k, and
 //       C' = (H - k P1) 2^hi + (Mid - k P2) 2^lo, scaled by 2^(ea + eb - 2t) into C.
 // Every mbarrier wait is bounded (abort flag, global error word, in-flight copies and MMAs
 // drained, TMEM released).
@@ -39,44 +41,50 @@
 namespace xtg {
 namespace crt {
 
-constexpr int BM = 128;        // rows per tile (one TMEM lane each)
-constexpr int BN = 256;        // columns per tile (one accumulator = 256 TMEM columns)
+// Tile: TM = 256 rows x TN = 128 columns of C, computed as its transpose on the tensor core:
+// the MMA's M dimension (128, one TMEM lane each) runs over C's columns (B residues) and its
+// N dimension (256) over C's rows (A residues), so that an epilogue thread (one TMEM lane =
+// one column of C) holds 32 consecutive rows per TMEM load and stores them as 32
+// contiguous bytes of U[l][col][row].
+constexpr int TM = 256;        // rows of C per tile  (MMA N)
+constexpr int TN = 128;        // columns of C per tile (MMA M, TMEM lanes)
 constexpr int BK = 64;         // K bytes per stage (one 64-byte swizzle row)
 constexpr int STAGES = 8;
 constexpr int THREADS = 320;   // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
 constexpr int EPI_WARPS = 8;
 constexpr int MAXL = 16;
-constexpr int A_TILE = BM * BK;                 // 8 KB
-constexpr int B_TILE = BN * BK;                 // 16 KB
-constexpr int SMEM_BYTES = STAGES * (A_TILE + B_TILE) + 1024;
-// S8 x S8 -> S32, K-major A and B, M = 128, N = 256
-constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
-                           ((uint32_t)(BM >> 4) << 24);
+constexpr int ROW_TILE = TM * BK;               // 16 KB of A residues per stage
+constexpr int COL_TILE = TN * BK;               // 8 KB of B residues per stage
+constexpr int SMEM_BYTES = STAGES * (ROW_TILE + COL_TILE) + 1024;
+// S8 x S8 -> S32, K-major operands, MMA M = 128, N = 256
+constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TM >> 3) << 17) |
+                           ((uint32_t)(TN >> 4) << 24);
 // Moduli and reconstruction constants of one modulus count L (built on the host).
+//   C' = sum_l r_l W_l - k P,  r_l = c_l mod p_l,  W_l = (P / p_l) ((P / p_l)^-1 mod p_l) mod P,
+// the CRT weights with the inverse folded in (so the epilogue only reduces c_l mod p_l).
 struct Moduli {
     int L;
-    int p[MAXL];        // moduli, largest first
-    int y[MAXL];        // (P / p_l)^-1 mod p_l
-    float invpf[MAXL];  // 1 / p_l
+    int p[MAXL];              // moduli, largest first
+    unsigned int barrett[MAXL];  // floor(2^32 / p_l)
     double invp[MAXL];
-    // M_l ~ m1_l 2^hi + m2_l 2^lo with m1_l, m2_l < 2^40 (bits below 2^lo dropped), so that
-    // every u_l m_l and every partial sum of L <= 16 of them is an exact FP64 integer
-    double m1[MAXL], m2[MAXL];
-    double P1, P2;      // the same split of P
-    double c1, c2;      // 2^hi / P, 2^lo / P
+    // W_l ~ w1_l 2^hi + w2_l 2^lo with w1_l, w2_l < 2^41 (bits below 2^lo dropped), so that
+    // every r_l w_l (r_l < 256) and every partial sum of L <= 16 of them is an exact FP64 integer
+    double w1[MAXL], w2[MAXL];
+    double P1, P2;            // the same split of P
+    double c1, c2;            // 2^hi / P, 2^lo / P
     int hi, lo;
     double log2P;
 };
 
 struct Params {
     int M, N, Kp;        // Kp: padded K (multiple of BK)
-    int Mp, Np;          // rows of each modulus' A residues / columns of its B residues
+    int Mp, Np;          // rows of each modulus' A residues (multiple of TM) / columns of B's (of TN)
     int L, mtiles, ntiles, items;
     const int *kext;     // per output column: K extent (nullptr: Kp)
-    unsigned char *U;    // u_l, [l][col][row], pitch Mp, Np columns per modulus
+    unsigned char *U;    // r_l, [l][col][row], pitch Mp, Np columns per modulus
     int *err;            // global error word (kErrWaitTimeout on a bounded-wait expiry)
-    int p[MAXL], y[MAXL];
-    float invpf[MAXL];
+    int p[MAXL];
+    unsigned int barrett[MAXL];
 };
 
 // ---- operand residues -------------------------------------------------------------------
@@ -223,17 +231,15 @@ __global__ void __launch_bounds__(256) residue_cols_kernel(GemmArgs<double> g, i
 }
 
 // ---- the residue GEMM ---------------------------------------------------------------------
-// (c y) mod p in [0, p) for |c| < 2^30, 0 < y < p <= 256.
-__device__ __forceinline__ int mod_mul(int c, int y, int p, float invp)
+// c mod p in [0, p) for |c| < 2^27 (K <= 2^13 terms of |a b| <= 2^14; the host keeps K below
+// 2^16, |c| < 2^30): c + p 2^23 >= 0 is reduced by Barrett's method with floor(2^32 / p)
+// (a quotient at most one short), integer operations only.
+__device__ __forceinline__ unsigned int mod_p(int c, unsigned int p, unsigned int barrett)
 {
-    const int q = __float2int_rn((float)c * invp);  // within a few units of c / p
-    const int r = c - q * p;                        // |r| < 4p
-    const int w = r * y;                            // |w| < 2^18: exact in FP32
-    const int q2 = __float2int_rd((float)w * invp);
-    int u = w - q2 * p;                             // in [-p, 2p)
-    u += u < 0 ? p : 0;
-    u -= u >= p ? p : 0;
-    return u;
+    const unsigned int x = (unsigned int)c + (p << 23);  // the true sum is in [0, 2^32)
+    const unsigned int q = __umulhi(x, barrett);
+    unsigned int r = x - q * p;                          // in [0, 2p)
+    return r >= p ? r - p : r;
 }
 
 __device__ __forceinline__ void item_tile(const Params &p, int item, int &l, int &m0, int &n0, int &ksteps)
@@ -242,21 +248,22 @@ __device__ __forceinline__ void item_tile(const Params &p, int item, int &l, int
     l = item / per;
     const int r = item - l * per;
     const int nt = r / p.mtiles;
-    m0 = (r - nt * p.mtiles) * BM;
+    m0 = (r - nt * p.mtiles) * TM;
     // with a per-column K extent (back-transform) the longest column tiles come first
-    n0 = (p.kext ? p.ntiles - 1 - nt : nt) * BN;
+    n0 = (p.kext ? p.ntiles - 1 - nt : nt) * TN;
     int kmax = p.Kp;
-    if (p.kext) kmax = min(kmax, p.kext[min(n0 + BN, p.N) - 1]);
+    if (p.kext) kmax = min(kmax, p.kext[min(n0 + TN, p.N) - 1]);
     ksteps = max(1, (kmax + BK - 1) / BK);
 }
 
+// tmR: A residues (rows l Mp + m, K bytes), box TM rows; tmC: B residues (rows l Np + n), box TN.
 __global__ void __launch_bounds__(THREADS, 1)
-gemm_crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Params p)
+gemm_crt_kernel(const __grid_constant__ CUtensorMap tmR, const __grid_constant__ CUtensorMap tmC, Params p)
 {
     extern __shared__ __align__(16) unsigned char smem_crt[];
     unsigned char *base = reinterpret_cast<unsigned char *>(((uintptr_t)smem_crt + 1023) & ~(uintptr_t)1023);
-    unsigned char *sA = base;                      // [STAGES][A_TILE]
-    unsigned char *sB = base + STAGES * A_TILE;    // [STAGES][B_TILE]
+    unsigned char *sR = base;                        // [STAGES][ROW_TILE]
+    unsigned char *sC = base + STAGES * ROW_TILE;    // [STAGES][COL_TILE]
     __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], acc_full[2], acc_empty[2], mma_done;
     __shared__ uint32_t tmem_base;
     __shared__ volatile int abort_flag;
@@ -301,9 +308,9 @@ gemm_crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                         ok = false;
                         break;
                     }
-                    split::mbar_expect_tx(&full[s], (uint32_t)(A_TILE + B_TILE));
-                    split::tma_load_2d(sA + s * A_TILE, &tmA, k * BK, l * p.Mp + m0, &full[s]);
-                    split::tma_load_2d(sB + s * B_TILE, &tmB, k * BK, l * p.Np + n0, &full[s]);
+                    split::mbar_expect_tx(&full[s], (uint32_t)(ROW_TILE + COL_TILE));
+                    split::tma_load_2d(sR + s * ROW_TILE, &tmR, k * BK, l * p.Mp + m0, &full[s]);
+                    split::tma_load_2d(sC + s * COL_TILE, &tmC, k * BK, l * p.Np + n0, &full[s]);
                 }
                 if (!ok) break;
             }
@@ -331,7 +338,7 @@ gemm_crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                         break;
                     split::tc_fence_after();
                 }
-                const uint32_t dcol = tmem + (uint32_t)(buf * BN);
+                const uint32_t dcol = tmem + (uint32_t)(buf * TM);
                 for (int k = 0; k < ks; k++, use++) {
                     const int s = (int)(use % STAGES);
                     if (!split::mbar_wait(&full[s], (uint32_t)((use / STAGES) & 1), &abort_flag, p.err)) {
@@ -341,8 +348,8 @@ gemm_crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
                     split::tc_fence_after();
 #pragma unroll
                     for (int kk = 0; kk < 2; kk++)  // two 32-byte-deep MMAs per 64-byte K step
-                        split::umma_i8(dcol, split::smem_desc(sA + s * A_TILE, kk * 32),
-                                       split::smem_desc(sB + s * B_TILE, kk * 32), IDESC, (k | kk) ? 1u : 0u);
+                        split::umma_i8(dcol, split::smem_desc(sC + s * COL_TILE, kk * 32),
+                                       split::smem_desc(sR + s * ROW_TILE, kk * 32), IDESC, (k | kk) ? 1u : 0u);
                     split::umma_commit(&empty[s]);
                 }
                 if (ok) split::umma_commit(&acc_full[buf]);
@@ -353,6 +360,8 @@ gemm_crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         }
     } else {
         // ---------------- epilogue: warps 2..9 ----------------
+        // TMEM lane = column of C (quadrant of the warp), TMEM column = row of C; the warp
+        // takes 128 of the tile's 256 rows in chunks of 32
         const int quad = warp & 3, half = (warp - 2) >> 2;
         int tcount = 0;
         for (int item = blockIdx.x; item < p.items; item += gridDim.x, tcount++) {
@@ -361,20 +370,23 @@ gemm_crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             const int buf = tcount & 1;
             if (!split::mbar_wait(&acc_full[buf], (uint32_t)((tcount >> 1) & 1), &abort_flag, p.err)) break;
             split::tc_fence_after();
-            const int pl = p.p[l], yl = p.y[l];
-            const float ipl = p.invpf[l];
-            const int row = m0 + quad * 32 + lane;
-            unsigned char *Ul = p.U + (size_t)l * p.Np * p.Mp + row;
-            const uint32_t tb = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(buf * BN + half * 128);
+            const unsigned int pl = (unsigned int)p.p[l], bl = p.barrett[l];
+            const int col = n0 + quad * 32 + lane;
+            unsigned char *Ucol = p.U + ((size_t)l * p.Np + col) * p.Mp + m0 + half * 128;
+            const uint32_t tb = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(buf * TM + half * 128);
 #pragma unroll 1
             for (int h = 0; h < 128; h += 32) {
                 uint32_t v[32];
                 split::tmem_ld32(tb + (uint32_t)h, v);
                 split::tmem_wait_ld();
-                const int c0 = n0 + half * 128 + h;
+                uint32_t w[8];
 #pragma unroll
-                for (int q = 0; q < 32; q++)
-                    Ul[(size_t)(c0 + q) * p.Mp] = (unsigned char)mod_mul((int)v[q], yl, pl, ipl);
+                for (int g = 0; g < 8; g++)
+                    w[g] = mod_p((int)v[4 * g], pl, bl) | (mod_p((int)v[4 * g + 1], pl, bl) << 8) |
+                           (mod_p((int)v[4 * g + 2], pl, bl) << 16) | (mod_p((int)v[4 * g + 3], pl, bl) << 24);
+                uint4 *dst = reinterpret_cast<uint4 *>(Ucol + h);  // 32 rows: 32 contiguous bytes
+                dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+                dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
             }
             split::tc_fence_before();
             __syncwarp();
@@ -418,8 +430,8 @@ __global__ void __launch_bounds__(256) crt_kernel(const unsigned char *U, int Mp
 #pragma unroll
         for (int l = 0; l < MAXL; l++) {
             const double ul = (double)((w[l] >> (8 * q)) & 0xffu);
-            H = fma(ul, md.m1[l], H);
-            Mid = fma(ul, md.m2[l], Mid);
+            H = fma(ul, md.w1[l], H);
+            Mid = fma(ul, md.w2[l], Mid);
         }
         const double k = rint(fma(H, md.c1, Mid * md.c2));
         const double d1 = fma(-k, md.P1, H);  // exact integers
