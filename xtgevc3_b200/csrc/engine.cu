@@ -802,21 +802,42 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         if constexpr (!CPLX && std::is_same<R, double>::value) {
             using namespace refine;
             const int m = sc.L.m, nitems = (int)sc.starts.size();
-            double *GS = scr.get<double>((size_t)n * K);
-            double *GP = scr.get<double>((size_t)n * K);
-            double *T = scr.get<double>((size_t)m * (2 * K + 1));
+            const int *d_kext = sc.d_ints + 2 * m;
+            double *G2 = scr.get<double>((size_t)n * 2 * K);  // [GS; GP], 2K x n column-major
+            double *T = scr.get<double>((size_t)m * 2 * K);   // [GS; GP] X, 2K x m
+            double *x2 = scr.get<double>((size_t)m);
             int *cnt = scr.get<int>(1);
             if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
             XTG_CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
             tr.run(kTPrep, 0, (double)n * n * esz, st, [&] {
-                sketch_matrix_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(Sp, lsp, n, 1, GS);
-                sketch_matrix_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(Pp, lpp, n, 0, GP);
+                sketch_matrix_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(Sp, lsp, n, 1, G2, 2 * K);
+                sketch_matrix_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(Pp, lpp, n, 0, G2 + K, 2 * K);
             });
+            GemmArgs<double> g{};
+            g.M = 2 * K;
+            g.N = m;
+            g.mlo = 0;
+            g.nseg = 1;
+            g.seg[0].A = G2;
+            g.seg[0].lda = 2 * K;
+            g.seg[0].acols = n;
+            g.seg[0].K = round_up(n, kKPad);
+            g.seg[0].boff = 0;
+            g.K = g.seg[0].K;
+            g.B = X;
+            g.ldb = ldx;
+            g.brows = n;
+            g.C = T;
+            g.ldc = 2 * K;
+            g.ccol = nullptr;
+            g.kext = d_kext;
+            g.accumulate = 0;
             tr.run(kTPrep, 0, 0.5 * (double)n * m * esz, st, [&] {
-                sketch_columns_kernel<<<(m + 7) / 8, 256, 0, st>>>(GS, GP, X, ldx, m, sc.d_ints + 2 * m, T);
-                refine_flags_kernel<<<(nitems + 255) / 256, 256, 0, st>>>(T, sc.d_ints + 4 * m, nitems, sc.d_kind,
-                                                                          coef, d_norms, opt.refine_bound, flags,
-                                                                          cnt);
+                launch_gemm<double>(g, false, st);
+                column_sumsq_kernel<<<(m * 32 + 255) / 256, 256, 0, st>>>(X, ldx, m, d_kext, x2);
+                refine_flags_kernel<<<(nitems + 255) / 256, 256, 0, st>>>(T, x2, sc.d_ints + 4 * m, nitems,
+                                                                          sc.d_kind, coef, d_norms, opt.refine_bound,
+                                                                          flags, cnt);
             });
             XTG_CK(cudaGetLastError());
             const size_t off = (size_t)(flags - d_flags);

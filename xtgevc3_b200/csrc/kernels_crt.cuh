@@ -49,7 +49,7 @@ namespace crt {
 constexpr int TM = 256;        // rows of C per tile  (MMA N)
 constexpr int TN = 128;        // columns of C per tile (MMA M, TMEM lanes)
 constexpr int BK = 64;         // K bytes per stage (one 64-byte swizzle row)
-constexpr int STAGES = 8;
+constexpr int STAGES = 6;  // 148 KB of shared memory: a diagonal-solve CTA (66 KB) fits beside it
 constexpr int THREADS = 320;   // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
 constexpr int EPI_WARPS = 8;
 constexpr int MAXL = 16;

@@ -9,7 +9,8 @@
 // complex residual is (ac S - (br + i bi) P)(xr + i xi).  The column's relative residual
 //   est_c = ||G r_c|| / 4 / ((|ac| anorm + |b| bnorm) ||x_c||_2)
 // is flagged when it exceeds bound / 4 (a margin for the spread of the estimate) or is not
-// finite.  Cost: S and P once (16 sums per entry), X once (32 sums per entry).
+// finite.  Cost: S and P once (16 sums per entry); [GS; GP] X as one FP64 tensor-core GEMM
+// (32 x n times the triangular X), and the column norms of X.
 #pragma once
 #include "common.cuh"
 
@@ -30,9 +31,11 @@ __device__ __forceinline__ uint32_t sign_bits(uint32_t i)
     return h;
 }
 
-// GA[j][r] = sum_{i <= min(n-1, j + hess)} G(r, i) A(i, j): one warp per column j (A upper
-// triangular, hess = 0, or upper Hessenberg, hess = 1).
-__global__ void __launch_bounds__(256) sketch_matrix_kernel(const double *A, int lda, int n, int hess, double *GA)
+// GA[j * ldg + r] = sum_{i <= min(n-1, j + hess)} G(r, i) A(i, j): one warp per column j (A
+// upper triangular, hess = 0, or upper Hessenberg, hess = 1); GA is the 16 x n sketch stored
+// column-major with leading dimension ldg.
+__global__ void __launch_bounds__(256) sketch_matrix_kernel(const double *A, int lda, int n, int hess, double *GA,
+                                                            int ldg)
 {
     const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -57,76 +60,38 @@ __global__ void __launch_bounds__(256) sketch_matrix_kernel(const double *A, int
 #pragma unroll
         for (int r = 1; r < K; r++)
             if (lane == r) v = acc[r];
-        GA[(size_t)j * K + lane] = v;
+        GA[(size_t)j * ldg + lane] = v;
     }
 }
 
-// Per column c of X (rows [0, kext_c)): T[c] = {GS x_c (16), GP x_c (16), ||x_c||^2}.  A CTA
-// of 8 warps takes 8 consecutive columns; rows go in chunks of 32 whose GS / GP rows are
-// staged in shared memory (transposed, one row of 32 per sketch row: conflict-free reads).
-__global__ void __launch_bounds__(256) sketch_columns_kernel(const double *GS, const double *GP, const double *X,
-                                                            int ldx, int m, const int *kext, double *T)
+// ||x_c||^2 over rows [0, kext_c) of each column of X: one warp per column.
+__global__ void __launch_bounds__(256) column_sumsq_kernel(const double *X, int ldx, int m, const int *kext,
+                                                           double *x2)
 {
-    __shared__ double gs[K][33], gp[K][33];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int c0 = blockIdx.x * 8, c = c0 + warp;
-    const int kc = c < m ? kext[c] : 0;
-    int kmax = 0;
-    for (int q = 0; q < 8 && c0 + q < m; q++) kmax = max(kmax, kext[c0 + q]);
-    double s[K], p[K], x2 = 0.0;
+    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (c >= m) return;
+    const double *xc = X + (size_t)c * ldx;
+    double s = 0.0;
+    for (int j = lane; j < kext[c]; j += 32) s = fma(xc[j], xc[j], s);
 #pragma unroll
-    for (int r = 0; r < K; r++) s[r] = p[r] = 0.0;
-    const double *xc = X + (size_t)(c < m ? c : 0) * ldx;
-    for (int j0 = 0; j0 < kmax; j0 += 32) {
-        __syncthreads();
-        for (int e = threadIdx.x; e < 32 * K; e += blockDim.x) {
-            const int jj = e / K, r = e % K;
-            const bool in = j0 + jj < kmax;
-            gs[r][jj] = in ? GS[(size_t)(j0 + jj) * K + r] : 0.0;
-            gp[r][jj] = in ? GP[(size_t)(j0 + jj) * K + r] : 0.0;
-        }
-        __syncthreads();
-        const int j = j0 + lane;
-        const double xv = (c < m && j < kc) ? xc[j] : 0.0;
-        x2 = fma(xv, xv, x2);
-#pragma unroll
-        for (int r = 0; r < K; r++) {
-            s[r] = fma(gs[r][lane], xv, s[r]);
-            p[r] = fma(gp[r][lane], xv, p[r]);
-        }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        x2 += __shfl_xor_sync(0xffffffffu, x2, o);
-#pragma unroll
-        for (int r = 0; r < K; r++) {
-            s[r] += __shfl_xor_sync(0xffffffffu, s[r], o);
-            p[r] += __shfl_xor_sync(0xffffffffu, p[r], o);
-        }
-    }
-    if (c < m && lane == 0) {
-        double *t = T + (size_t)c * (2 * K + 1);
-#pragma unroll
-        for (int r = 0; r < K; r++) {
-            t[r] = s[r];
-            t[K + r] = p[r];
-        }
-        t[2 * K] = x2;
-    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) x2[c] = s;
 }
 
 // Flags of the columns of each eigenvector (items: first column of each; a pair's two
-// columns get one flag).  coef: 4 per column (ac, b_re, b_im, smin); norms: {anorm, bnorm}.
-__global__ void refine_flags_kernel(const double *T, const int *items, int nitems, const uint8_t *kind,
-                                    const double *coef, const double *norms, double bound, uint8_t *flags,
-                                    int *count)
+// columns get one flag).  T: 2K x m, column c = {GS x_c, GP x_c}; x2: ||x_c||^2; coef: 4 per
+// column (ac, b_re, b_im, smin); norms: {anorm, bnorm}.
+__global__ void refine_flags_kernel(const double *T, const double *x2s, const int *items, int nitems,
+                                    const uint8_t *kind, const double *coef, const double *norms, double bound,
+                                    uint8_t *flags, int *count)
 {
     const int it = blockIdx.x * blockDim.x + threadIdx.x;
     if (it >= nitems) return;
     const int c = items[it];
     const double ac = coef[4 * c + 0], br = coef[4 * c + 1], bi = coef[4 * c + 2];
-    const double *t = T + (size_t)c * (2 * K + 1);
-    double r2 = 0.0, x2 = t[2 * K];
+    const double *t = T + (size_t)c * (2 * K);
+    double r2 = 0.0, x2 = x2s[c];
     const bool pair = kind[c] == kPairRe;
     if (!pair) {
         for (int r = 0; r < K; r++) {
@@ -134,13 +99,13 @@ __global__ void refine_flags_kernel(const double *T, const int *items, int nitem
             r2 = fma(v, v, r2);
         }
     } else {
-        const double *u = t + (2 * K + 1);  // the Im column
+        const double *u = t + 2 * K;  // the Im column
         for (int r = 0; r < K; r++) {
             const double re = ac * t[r] - br * t[K + r] + bi * u[K + r];
             const double im = ac * u[r] - br * u[K + r] - bi * t[K + r];
             r2 = fma(re, re, fma(im, im, r2));
         }
-        x2 += u[2 * K];
+        x2 += x2s[c + 1];
     }
     const double est = sqrt(r2 / K);
     const double den = (fabs(ac) * norms[0] + hypot(br, bi) * norms[1]) * sqrt(x2);
