@@ -399,7 +399,7 @@ def test_lookahead_matches_serial_path_with_guards(cuda_ok, side):
     compare(d, VL0, VR0, m, ref[0], ref[1], TOL_ILL[np.float64], check_resid=False)
 
 
-@pytest.mark.parametrize("sk,side", [("int8", "R"), ("int8", "L"), ("bf16", "R")])
+@pytest.mark.parametrize("sk,side", [("int8", "R"), ("int8", "L"), ("bf16", "R"), ("crt", "R"), ("crt", "L")])
 def test_split_form_guards_across_groups(cuda_ok, sk, side):
     """Split-precision form on the n = 1536 pencil whose eigenvectors grow by 1e16 per row
     block: its trailing updates (groups of eight row blocks, K = 2 x 512, at least 512 rows)
@@ -411,7 +411,7 @@ def test_split_form_guards_across_groups(cuda_ok, sk, side):
     I = np.eye(n, order="F")
     d = dict(side=side, howmny="A", S=S, P=P, alpha=ar, beta=be, alphai=ai, VL_in=I, VR_in=I.copy(order="F"),
              name="overflow")
-    X.set_flags(X.SPLIT | X.slices(7 if sk == "int8" else 6) | (X.SPLIT_INT8 if sk == "int8" else 0))
+    X.set_flags(X.SPLIT | {"int8": X.SPLIT_INT8 | X.slices(7), "bf16": X.slices(6), "crt": X.SPLIT_CRT}[sk])
     try:
         VL, VR, m, info = run_gpu(d)
     finally:
@@ -419,6 +419,9 @@ def test_split_form_guards_across_groups(cuda_ok, sk, side):
     V = VL if side == "L" else VR
     assert info == 0 and np.isfinite(V).all()
     assert (np.abs(np.diag(V[:, :n])) < 1).sum() >= 8
+    # guards rescale a column's finished rows and its residual sketch together: the check
+    # must not flag the rescaled columns wholesale
+    assert X.split_refined() < n // 8, X.split_refined()
     ref = oracle.tgevc3(side, "A", S, P, ar, be, alphai=ai)
     compare(d, VL, VR, m, ref[0], ref[1], TOL_ILL[np.float64], check_resid=False)
 

@@ -184,7 +184,7 @@ int adjoint_device(int n, const void *S_, int lds, const void *P_, int ldp, cons
         const int r0 = blk.first, r1 = blk.second, jnb = r1 - r0, bpad = round_up(jnb, kKPad);
         const int c0 = int(std::upper_bound(colk.begin(), colk.end(), n - r1) - colk.begin());
         if (c0 >= m) break;  // no column reaches this block, nor any block above it
-        DiagArgs<R> da;
+        DiagArgs<R> da{};
         da.S = reinterpret_cast<const R *>(St);
         da.P = reinterpret_cast<const R *>(Pt);
         da.lds = ld_n;

@@ -797,44 +797,18 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         d_flags = scr.get<uint8_t>(2 * (size_t)m_total);
         if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
     }
-    auto refine_side = [&](const E *Sp, int lsp, const E *Pp, int lpp, const E *X, int ldx, const SideCols &sc,
-                           const R *coef, uint8_t *flags, cudaStream_t st, Scratch &scr) -> int {
+    // Flags of one side's columns from the sketch T = [GS; GP] X (see kernels_refine.cuh).
+    auto refine_side = [&](const E *X, int ldx, const SideCols &sc, const R *coef, const E *T, uint8_t *flags,
+                           cudaStream_t st, Scratch &scr) -> int {
         if constexpr (!CPLX && std::is_same<R, double>::value) {
             using namespace refine;
             const int m = sc.L.m, nitems = (int)sc.starts.size();
-            const int *d_kext = sc.d_ints + 2 * m;
-            double *G2 = scr.get<double>((size_t)n * 2 * K);  // [GS; GP], 2K x n column-major
-            double *T = scr.get<double>((size_t)m * 2 * K);   // [GS; GP] X, 2K x m
             double *x2 = scr.get<double>((size_t)m);
             int *cnt = scr.get<int>(1);
             if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
             XTG_CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
-            tr.run(kTPrep, 0, (double)n * n * esz, st, [&] {
-                sketch_matrix_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(Sp, lsp, n, 1, G2, 2 * K);
-                sketch_matrix_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(Pp, lpp, n, 0, G2 + K, 2 * K);
-            });
-            GemmArgs<double> g{};
-            g.M = 2 * K;
-            g.N = m;
-            g.mlo = 0;
-            g.nseg = 1;
-            g.seg[0].A = G2;
-            g.seg[0].lda = 2 * K;
-            g.seg[0].acols = n;
-            g.seg[0].K = round_up(n, kKPad);
-            g.seg[0].boff = 0;
-            g.K = g.seg[0].K;
-            g.B = X;
-            g.ldb = ldx;
-            g.brows = n;
-            g.C = T;
-            g.ldc = 2 * K;
-            g.ccol = nullptr;
-            g.kext = d_kext;
-            g.accumulate = 0;
             tr.run(kTPrep, 0, 0.5 * (double)n * m * esz, st, [&] {
-                launch_gemm<double>(g, false, st);
-                column_sumsq_kernel<<<(m * 32 + 255) / 256, 256, 0, st>>>(X, ldx, m, d_kext, x2);
+                column_sumsq_kernel<<<(m * 32 + 255) / 256, 256, 0, st>>>(X, ldx, m, sc.d_ints + 2 * m, x2);
                 refine_flags_kernel<<<(nitems + 255) / 256, 256, 0, st>>>(T, x2, sc.d_ints + 4 * m, nitems,
                                                                           sc.d_kind, coef, d_norms, opt.refine_bound,
                                                                           flags, cnt);
@@ -967,6 +941,52 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         });
         XTG_CK(cudaGetLastError());
 
+        // ---- residual sketch of the refinement check (split form) ------------------------------
+        // [GS; GP] = G [S P] column by column and T = [GS; GP] X row group by row group, as the
+        // groups' rows of X become final (a guard that later rescales a column's finished rows
+        // rescales its T column too); without the group loop (look-ahead), after the loop.
+        E *sk_G2 = nullptr, *sk_T = nullptr;
+        const bool sketch_in_loop = flags && !ahead;
+        if (flags) {
+            sk_G2 = scr.get<E>((size_t)n * 2 * refine::K);
+            sk_T = scr.get<E>((size_t)m * 2 * refine::K);
+            if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
+            XTG_CK(cudaMemsetAsync(sk_T, 0, (size_t)m * 2 * refine::K * sizeof(E), st));
+        }
+        // sketch columns [j0, j1) of Sp, Pp into G2, then (accumulate) T[:, c0:] += G2[:, j0:j1] X[j0:j1, c0:]
+        auto sketch_rows = [&](int j0, int j1, int c0, bool accumulate) {
+            if constexpr (!CPLX && std::is_same<R, double>::value) {
+                using namespace refine;
+                const int cnt = j1 - j0;
+                tr.run(kTPrep, 0, 2.0 * cnt * (j0 + j1) / 2 * esz, st, [&] {
+                    sketch_matrix_kernel<<<(cnt * 32 + 255) / 256, 256, 0, st>>>(Sp, lsp, n, 1, sk_G2, 2 * K, j0, j1);
+                    sketch_matrix_kernel<<<(cnt * 32 + 255) / 256, 256, 0, st>>>(Pp, lpp, n, 0, sk_G2 + K, 2 * K, j0,
+                                                                                  j1);
+                });
+                if (c0 >= m) return;
+                GemmArgs<double> g{};
+                g.M = 2 * K;
+                g.N = m - c0;
+                g.mlo = 0;
+                g.nseg = 1;
+                g.seg[0].A = sk_G2 + (size_t)j0 * 2 * K;
+                g.seg[0].lda = 2 * K;
+                g.seg[0].acols = cnt;
+                g.seg[0].K = round_up(cnt, kKPad);
+                g.seg[0].boff = j0;
+                g.K = g.seg[0].K;
+                g.B = X + (size_t)c0 * ldx;
+                g.ldb = ldx;
+                g.brows = n;
+                g.C = sk_T + (size_t)c0 * 2 * K;
+                g.ldc = 2 * K;
+                g.ccol = nullptr;
+                g.kext = accumulate ? nullptr : d_kext + c0;
+                g.accumulate = accumulate ? 1 : 0;
+                tr.run(kTPrep, 2.0 * 2 * K * cnt * (m - c0), 0, st, [&] { launch_gemm<double>(g, false, st); });
+            }
+        };
+
         // ---- blocked substitution ----------------------------------------------------------
         // Row blocks are taken in groups of `group` adjacent blocks, rows [q0, q1), bottom to
         // top: each block is solved, then the rows of the group's blocks above it are updated
@@ -1024,7 +1044,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             const int c0 = first_col(r0);
             if (c0 >= m) return;
             const int bpad = ypad >= 0 ? ypad : round_up(jnb, kKPad);
-            DiagArgs<R> da;
+            DiagArgs<R> da{};
             da.S = reinterpret_cast<const R *>(Sp);
             da.P = reinterpret_cast<const R *>(Pp);
             da.lds = lsp;
@@ -1052,6 +1072,8 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             da.left_seed = left ? 1 : 0;
             da.pending = safe_lo >= 0 ? pending : nullptr;
             da.safe_lo = safe_lo;
+            da.sk = reinterpret_cast<R *>(sk_T);
+            da.sk_rows = 2 * refine::K;
             const int grid = std::max(1, std::min((nitems - da.it0 + diag_warps - 1) / diag_warps, diag_ctas));
             // algorithmic work of the shifted solves: ~2 nrows^2 real flops per real column,
             // 4x that per complex column or (Re, Im) pair; bytes: rhs in, solution and
@@ -1093,12 +1115,14 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
                 }
             }
             const int c0 = first_col(q0);
+            if (sketch_in_loop) sketch_rows(q0, q1, c0, true);  // rows [q0, q1) of X are final
             if (q0 > 0 && c0 < m) {
                 GemmSeg<E> sg[2] = {strip(Sp, lsp, 0, q0, acols, 0), strip(Pp, lpp, 0, q0, acols, kq)};
                 update(0, 0, q0, c0, nstrips, sg, nstrips * double(acols), st);
             }
             XTG_CK(cudaGetLastError());
         }
+        if (flags && !sketch_in_loop) sketch_rows(0, n, 0, false);
         // Look-ahead (ahead == true).  Pair p owns rows [u0_p, l1_p); the next pair's rows are
         // [a0, u0_p).  On the main stream: solve L_p, small update of U_p, solve U_p; wait for
         // the trailing update of pair p-1 (it writes rows [0, u0_p)); apply deferred guard
@@ -1223,7 +1247,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         // residual exceeds the bound are flagged and solved again in FP64 after the call's
         // split pass (see the end of solve_device).
         if constexpr (!CPLX && std::is_same<R, double>::value) {
-            if (flags && refine_side(Sp, lsp, Pp, lpp, X, ldx, sc, coef, flags, st, scr)) return 1;
+            if (flags && refine_side(X, ldx, sc, coef, sk_T, flags, st, scr)) return 1;
         }
 
         // ---- write-back / back-transform -----------------------------------------------------

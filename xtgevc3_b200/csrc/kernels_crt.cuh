@@ -49,7 +49,7 @@ namespace crt {
 constexpr int TM = 256;        // rows of C per tile  (MMA N)
 constexpr int TN = 128;        // columns of C per tile (MMA M, TMEM lanes)
 constexpr int BK = 64;         // K bytes per stage (one 64-byte swizzle row)
-constexpr int STAGES = 6;  // 148 KB of shared memory: a diagonal-solve CTA (66 KB) fits beside it
+constexpr int STAGES = 8;
 constexpr int THREADS = 320;   // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
 constexpr int EPI_WARPS = 8;
 constexpr int MAXL = 16;
@@ -90,13 +90,24 @@ struct Params {
 // ---- operand residues -------------------------------------------------------------------
 // v in (-1, 1): a = rint(v 2^t) (exact integer, |a| <= 2^t), residue a mod p_l in [-128, 127]
 // (symmetric; 128 mod 256 stored as -128).
+// Rounding and conversion through the FP64 adder (x + 1.5 2^52 has unit spacing for
+// |x| < 2^51 and keeps x's integer part, two's complement, in its low word), so the
+// per-modulus work avoids the slower conversion unit: |a / p| < 2^56 / 193 < 2^49.
+constexpr double kRoundMagic = 6755399441055744.0;  // 1.5 * 2^52
 __device__ __forceinline__ int residue(double a, int l, const Moduli &md)
 {
-    const double q = rint(a * md.invp[l]);
-    int r = (int)fma(-q, (double)md.p[l], a);  // exact: the result is a small integer
+    const double q = __dsub_rn(__dadd_rn(__dmul_rn(a, md.invp[l]), kRoundMagic), kRoundMagic);
+    const double rr = fma(-q, (double)md.p[l], a);  // exact: the result is a small integer
+    int r = __double2loint(__dadd_rn(rr, kRoundMagic));
     if (r > 127) r -= md.p[l];
     if (r < -128) r += md.p[l];
     return r;
+}
+
+// v 2^s: one multiplication by the power of two when it is a normal double, else ldexp.
+__device__ __forceinline__ double scale2(double v, int s)
+{
+    return (s > -1000 && s < 1000) ? v * __longlong_as_double((long long)(s + 1023) << 52) : ldexp(v, s);
 }
 
 // Largest |A(m, k)| of each row (through the segment description of a GEMM launch), as the
@@ -156,7 +167,7 @@ __global__ void __launch_bounds__(256) residue_rows_kernel(GemmArgs<double> g, i
     if (blockIdx.y == 0 && kg == 0) ea[row] = e;
     double a[8];
 #pragma unroll
-    for (int q = 0; q < 8; q++) a[q] = rint(ldexp(tile[kg + q][rr], t - e));
+    for (int q = 0; q < 8; q++) a[q] = rint(scale2(tile[kg + q][rr], t - e));
     int8_t *o = out + (size_t)row * Kp + k0 + kg;
     for (int l = 0; l < md.L; l++) {
         uint32_t w0 = 0, w1 = 0;
@@ -217,7 +228,7 @@ __global__ void __launch_bounds__(256) residue_cols_kernel(GemmArgs<double> g, i
     b_values8(g, col, k0, v);
     double a[8];
 #pragma unroll
-    for (int q = 0; q < 8; q++) a[q] = rint(ldexp(v[q], t - e));
+    for (int q = 0; q < 8; q++) a[q] = rint(scale2(v[q], t - e));
     int8_t *o = out + (size_t)col * Kp + k0;
     for (int l = 0; l < md.L; l++) {
         uint32_t w0 = 0, w1 = 0;

@@ -35,11 +35,11 @@ __device__ __forceinline__ uint32_t sign_bits(uint32_t i)
 // upper triangular, hess = 0, or upper Hessenberg, hess = 1); GA is the 16 x n sketch stored
 // column-major with leading dimension ldg.
 __global__ void __launch_bounds__(256) sketch_matrix_kernel(const double *A, int lda, int n, int hess, double *GA,
-                                                            int ldg)
+                                                            int ldg, int j0, int j1)
 {
-    const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int j = j0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);  // columns [j0, j1)
     const int lane = threadIdx.x & 31;
-    if (j >= n) return;
+    if (j >= j1) return;
     double acc[K];
 #pragma unroll
     for (int r = 0; r < K; r++) acc[r] = 0.0;
