@@ -942,27 +942,20 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         XTG_CK(cudaGetLastError());
 
         // ---- residual sketch of the refinement check (split form) ------------------------------
-        // [GS; GP] = G [S P] column by column and T = [GS; GP] X row group by row group, as the
-        // groups' rows of X become final (a guard that later rescales a column's finished rows
-        // rescales its T column too); without the group loop (look-ahead), after the loop.
+        // [GS; GP] = G [S P] and T = [GS; GP] X, after the substitution: X's rows in chunks of
+        // 1024 (short K per launch), each chunk over the columns it can reach.
         E *sk_G2 = nullptr, *sk_T = nullptr;
-        const bool sketch_in_loop = flags && !ahead;
         if (flags) {
             sk_G2 = scr.get<E>((size_t)n * 2 * refine::K);
             sk_T = scr.get<E>((size_t)m * 2 * refine::K);
             if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
             XTG_CK(cudaMemsetAsync(sk_T, 0, (size_t)m * 2 * refine::K * sizeof(E), st));
         }
-        // sketch columns [j0, j1) of Sp, Pp into G2, then (accumulate) T[:, c0:] += G2[:, j0:j1] X[j0:j1, c0:]
-        auto sketch_rows = [&](int j0, int j1, int c0, bool accumulate) {
+        // T[:, c0:] += G2[:, j0:j1] X[j0:j1, c0:] (G2 complete)
+        auto sketch_rows = [&](int j0, int j1, int c0) {
             if constexpr (!CPLX && std::is_same<R, double>::value) {
                 using namespace refine;
                 const int cnt = j1 - j0;
-                tr.run(kTPrep, 0, 2.0 * cnt * (j0 + j1) / 2 * esz, st, [&] {
-                    sketch_matrix_kernel<<<(cnt * 32 + 255) / 256, 256, 0, st>>>(Sp, lsp, n, 1, sk_G2, 2 * K, j0, j1);
-                    sketch_matrix_kernel<<<(cnt * 32 + 255) / 256, 256, 0, st>>>(Pp, lpp, n, 0, sk_G2 + K, 2 * K, j0,
-                                                                                  j1);
-                });
                 if (c0 >= m) return;
                 GemmArgs<double> g{};
                 g.M = 2 * K;
@@ -981,8 +974,8 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
                 g.C = sk_T + (size_t)c0 * 2 * K;
                 g.ldc = 2 * K;
                 g.ccol = nullptr;
-                g.kext = accumulate ? nullptr : d_kext + c0;
-                g.accumulate = accumulate ? 1 : 0;
+                g.kext = nullptr;
+                g.accumulate = 1;
                 tr.run(kTPrep, 2.0 * 2 * K * cnt * (m - c0), 0, st, [&] { launch_gemm<double>(g, false, st); });
             }
         };
@@ -1072,8 +1065,6 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             da.left_seed = left ? 1 : 0;
             da.pending = safe_lo >= 0 ? pending : nullptr;
             da.safe_lo = safe_lo;
-            da.sk = reinterpret_cast<R *>(sk_T);
-            da.sk_rows = 2 * refine::K;
             const int grid = std::max(1, std::min((nitems - da.it0 + diag_warps - 1) / diag_warps, diag_ctas));
             // algorithmic work of the shifted solves: ~2 nrows^2 real flops per real column,
             // 4x that per complex column or (Re, Im) pair; bytes: rhs in, solution and
@@ -1115,14 +1106,24 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
                 }
             }
             const int c0 = first_col(q0);
-            if (sketch_in_loop) sketch_rows(q0, q1, c0, true);  // rows [q0, q1) of X are final
             if (q0 > 0 && c0 < m) {
                 GemmSeg<E> sg[2] = {strip(Sp, lsp, 0, q0, acols, 0), strip(Pp, lpp, 0, q0, acols, kq)};
                 update(0, 0, q0, c0, nstrips, sg, nstrips * double(acols), st);
             }
             XTG_CK(cudaGetLastError());
         }
-        if (flags && !sketch_in_loop) sketch_rows(0, n, 0, false);
+        if constexpr (!CPLX && std::is_same<R, double>::value) {
+            if (flags) {
+                using namespace refine;
+                tr.run(kTPrep, 0, (double)n * n * esz, st, [&] {
+                    sketch_matrix_kernel<<<n, 256, 0, st>>>(Sp, lsp, n, 1, sk_G2, 2 * K);
+                    sketch_matrix_kernel<<<n, 256, 0, st>>>(Pp, lpp, n, 0, sk_G2 + K, 2 * K);
+                });
+                // chunk [j0, j1) reaches the columns whose extent passes j0 (X is zero below it)
+                for (int j0 = 0; j0 < n; j0 += 1024)
+                    sketch_rows(j0, std::min(n, j0 + 1024), first_col(std::max(0, j0 - 1)));
+            }
+        }
         // Look-ahead (ahead == true).  Pair p owns rows [u0_p, l1_p); the next pair's rows are
         // [a0, u0_p).  On the main stream: solve L_p, small update of U_p, solve U_p; wait for
         // the trailing update of pair p-1 (it writes rows [0, u0_p)); apply deferred guard

@@ -134,11 +134,6 @@ struct DiagArgs {
     // caller applies pending to rows [0, safe_lo) once no other kernel writes them.
     R *pending;
     int safe_lo;
-    // Residual sketch accumulated so far (nullable; the split form's refinement check):
-    // sk_rows values per column, computed from rows below this block's group, so a guard
-    // that rescales a column's rows below the block rescales them too.
-    R *sk;
-    int sk_rows;
 };
 
 // Multiply rows [a, b) of one column by s (warp-cooperative).  Used on the rows of a
@@ -147,14 +142,6 @@ template <class E, class R>
 __device__ __forceinline__ void scale_rows(E *col, int a, int b, R s, int lane)
 {
     for (int i = a + lane; i < b; i += 32) col[i] = s * col[i];
-}
-
-// Guard rescaling of column c's rows below the block, [r1, top], and of its sketch values.
-template <class E, class R>
-__device__ __forceinline__ void scale_below(const DiagArgs<R> &a, E *col, int c, int top, R s, int lane)
-{
-    scale_rows(col, a.r1, top + 1, s, lane);
-    if (a.sk) scale_rows(a.sk + (size_t)c * a.sk_rows, 0, a.sk_rows, s, lane);
 }
 
 // Guard rescaling of the rows above the block [0, r0) of column c: all of them at once,
@@ -545,7 +532,7 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
                     R sc = a.thr_rhs / mx;
                     r[0] *= sc; r[1] *= sc; seed *= sc;
                     if (!diag) {
-                        scale_above(a, colr, c, sc, lane); scale_below(a, colr, c, top, sc, lane);
+                        scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane);
                         scale_lower_y(a, a.Y + (size_t)c * a.ldy, sc, lane);
                     }
                 }
@@ -555,7 +542,7 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
             auto rescale = [&](R (&rr)[2], R sc) {  // the whole column, by sc
                 rr[0] *= sc; rr[1] *= sc; seed *= sc;
                 if (!diag) {
-                    scale_above(a, colr, c, sc, lane); scale_below(a, colr, c, top, sc, lane);
+                    scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane);
                     scale_lower_y(a, a.Y + (size_t)c * a.ldy, sc, lane);
                 }
             };
@@ -576,7 +563,7 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
                 R sc = a.thr_upd / mx;
                 x[0] *= sc; x[1] *= sc;
                 if (!diag) {
-                    scale_above(a, colr, c, sc, lane); scale_below(a, colr, c, top, sc, lane);
+                    scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane);
                     scale_lower_y(a, a.Y + (size_t)c * a.ldy, sc, lane);
                 }
             }
@@ -626,8 +613,8 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
                     R sc = a.thr_rhs / mx;
                     r[0] = sc * r[0]; r[1] = sc * r[1]; seed0 = sc * seed0; seed1 = sc * seed1;
                     if (!diag) {
-                        scale_above(a, colr, c, sc, lane); scale_below(a, colr, c, top, sc, lane);
-                        scale_above(a, coli, c + 1, sc, lane); scale_below(a, coli, c + 1, top, sc, lane);
+                        scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane);
+                        scale_above(a, coli, c + 1, sc, lane); scale_rows(coli, a.r1, top + 1, sc, lane);
                         scale_lower_y(a, a.Y + (size_t)c * a.ldy, sc, lane);
                         scale_lower_y(a, a.Y + (size_t)(c + 1) * a.ldy, sc, lane);
                     }
@@ -638,8 +625,8 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
             auto rescale = [&](C (&rr)[2], R sc) {  // the whole column pair, by sc
                 rr[0] = sc * rr[0]; rr[1] = sc * rr[1]; seed0 = sc * seed0; seed1 = sc * seed1;
                 if (!diag) {
-                    scale_above(a, colr, c, sc, lane); scale_below(a, colr, c, top, sc, lane);
-                    scale_above(a, coli, c + 1, sc, lane); scale_below(a, coli, c + 1, top, sc, lane);
+                    scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane);
+                    scale_above(a, coli, c + 1, sc, lane); scale_rows(coli, a.r1, top + 1, sc, lane);
                     scale_lower_y(a, a.Y + (size_t)c * a.ldy, sc, lane);
                     scale_lower_y(a, a.Y + (size_t)(c + 1) * a.ldy, sc, lane);
                 }
@@ -666,8 +653,8 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
                 R sc = a.thr_upd / mx;
                 x[0] = sc * x[0]; x[1] = sc * x[1];
                 if (!diag) {
-                    scale_above(a, colr, c, sc, lane); scale_below(a, colr, c, top, sc, lane);
-                    scale_above(a, coli, c + 1, sc, lane); scale_below(a, coli, c + 1, top, sc, lane);
+                    scale_above(a, colr, c, sc, lane); scale_rows(colr, a.r1, top + 1, sc, lane);
+                    scale_above(a, coli, c + 1, sc, lane); scale_rows(coli, a.r1, top + 1, sc, lane);
                     scale_lower_y(a, a.Y + (size_t)c * a.ldy, sc, lane);
                     scale_lower_y(a, a.Y + (size_t)(c + 1) * a.ldy, sc, lane);
                 }
@@ -739,7 +726,7 @@ __global__ void __launch_bounds__(kDiagThreadsCplx, 1) diag_solve_cplx(DiagArgs<
                 R sc = a.thr_rhs / mx;
                 r[0] = sc * r[0]; r[1] = sc * r[1]; seed = sc * seed;
                 if (!diag) {
-                    scale_above(a, col, c, sc, lane); scale_below(a, col, c, top, sc, lane);
+                    scale_above(a, col, c, sc, lane); scale_rows(col, a.r1, top + 1, sc, lane);
                     scale_lower_y(a, Y + (size_t)c * a.ldy, sc, lane);
                 }
             }
@@ -755,7 +742,7 @@ __global__ void __launch_bounds__(kDiagThreadsCplx, 1) diag_solve_cplx(DiagArgs<
         auto rescale = [&](C (&rr)[2], R sc) {  // the whole column, by sc
             rr[0] = sc * rr[0]; rr[1] = sc * rr[1]; seed = sc * seed; acc *= sc;
             if (!diag) {
-                scale_above(a, col, c, sc, lane); scale_below(a, col, c, top, sc, lane);
+                scale_above(a, col, c, sc, lane); scale_rows(col, a.r1, top + 1, sc, lane);
                 scale_lower_y(a, Y + (size_t)c * a.ldy, sc, lane);
             }
         };
@@ -784,7 +771,7 @@ __global__ void __launch_bounds__(kDiagThreadsCplx, 1) diag_solve_cplx(DiagArgs<
             R sc = a.thr_upd / mx;
             x[0] = sc * x[0]; x[1] = sc * x[1];
             if (!diag) {
-                scale_above(a, col, c, sc, lane); scale_below(a, col, c, top, sc, lane);
+                scale_above(a, col, c, sc, lane); scale_rows(col, a.r1, top + 1, sc, lane);
                 scale_lower_y(a, Y + (size_t)c * a.ldy, sc, lane);
             }
         }

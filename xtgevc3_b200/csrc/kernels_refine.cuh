@@ -31,21 +31,21 @@ __device__ __forceinline__ uint32_t sign_bits(uint32_t i)
     return h;
 }
 
-// GA[j * ldg + r] = sum_{i <= min(n-1, j + hess)} G(r, i) A(i, j): one warp per column j (A
-// upper triangular, hess = 0, or upper Hessenberg, hess = 1); GA is the 16 x n sketch stored
-// column-major with leading dimension ldg.
+// GA[j * ldg + r] = sum_{i <= min(n-1, j + hess)} G(r, i) A(i, j): one CTA of 256 threads
+// per column j (A upper triangular, hess = 0, or upper Hessenberg, hess = 1); GA is the
+// 16 x n sketch stored column-major with leading dimension ldg.
 __global__ void __launch_bounds__(256) sketch_matrix_kernel(const double *A, int lda, int n, int hess, double *GA,
-                                                            int ldg, int j0, int j1)
+                                                            int ldg)
 {
-    const int j = j0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);  // columns [j0, j1)
-    const int lane = threadIdx.x & 31;
-    if (j >= j1) return;
+    __shared__ double part[8][K];
+    const int j = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double acc[K];
 #pragma unroll
     for (int r = 0; r < K; r++) acc[r] = 0.0;
     const int rows = min(n, j + 1 + hess);
     const double *a = A + (size_t)j * lda;
-    for (int i = lane; i < rows; i += 32) {
+    for (int i = threadIdx.x; i < rows; i += blockDim.x) {
         const double v = a[i];
         const uint32_t b = sign_bits((uint32_t)i);
 #pragma unroll
@@ -60,7 +60,13 @@ __global__ void __launch_bounds__(256) sketch_matrix_kernel(const double *A, int
 #pragma unroll
         for (int r = 1; r < K; r++)
             if (lane == r) v = acc[r];
-        GA[(size_t)j * ldg + lane] = v;
+        part[warp][lane] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < K) {
+        double v = 0.0;
+        for (int w = 0; w < 8; w++) v += part[w][threadIdx.x];
+        GA[(size_t)j * ldg + threadIdx.x] = v;
     }
 }
 
