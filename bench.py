@@ -418,8 +418,9 @@ def measure_form(name, flags, args, X, torch, data, dist, local, world, ref=None
     torch.cuda.synchronize()
     X.trace_enable(False)
     kernels = {k: dict(v, ms_per_step=v["ms"] / args.steps) for k, v in X.trace().items() if v["launches"]}
+    refined = X.split_refined() if flags & X.SPLIT else 0  # columns the last (traced) call refined
     return {"name": name, "flags": flags, "ms": ms, "value": world * 2 * n / (ms * 1e-3), "resid": resid,
-            "err_vs_ref": err, "clocks": clk, "launches": launches, "kernels": kernels}
+            "err_vs_ref": err, "refined_columns": refined, "clocks": clk, "launches": launches, "kernels": kernels}
 
 
 def batched_inputs(count, seed, torch):
@@ -1076,6 +1077,7 @@ def main():
                      "split_crt": f"split precision, {nm_crt} INT8 residues (CRT, tcgen05 kind::i8)"}
         forms_out = {nm: {"value": r["value"], "ms_per_step": r["ms"], "resid_max": r["resid"],
                           "meets_resid_bound": r["resid"] <= 1e-12, "max_rel_diff_vs_reference": r["err_vs_ref"],
+                          "refined_columns_per_call": r["refined_columns"],
                           "kernels_ms_per_step": {k: v["ms_per_step"] for k, v in r["kernels"].items()}}
                      for nm, r in res.items()}
         if "plain" in res:
@@ -1083,7 +1085,7 @@ def main():
                 forms_out[nm]["speedup_vs_plain"] = res["plain"]["ms"] / res[nm]["ms"]
         # one compact line per form inside `config` (kept by record parsers that drop extra keys)
         forms_brief = {nm: {"ms": round(f["ms_per_step"], 3), "resid": f["resid_max"],
-                            "err_vs_ref": f["max_rel_diff_vs_reference"],
+                            "err_vs_ref": f["max_rel_diff_vs_reference"], "refined": f["refined_columns_per_call"],
                             "x_plain": round(f.get("speedup_vs_plain", 0.0), 3)} for nm, f in forms_out.items()}
         line = {"metric": METRIC, "value": h["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": h["ms"], "higher_is_better": True, "scaling": "weak",

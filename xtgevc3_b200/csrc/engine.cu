@@ -488,7 +488,7 @@ static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scr
         p.p[l] = md.p[l];
         p.barrett[l] = md.barrett[l];
     }
-    const int grid = std::min(sm_count(), p.items);
+    const int grid = std::min(sm_count(), p.items);  // persistent: one CTA per SM
     gemm_crt_kernel<<<grid, THREADS, SMEM_BYTES, st>>>(tmA, tmB, p);
     crt_kernel<<<dim3((g.M + 1023) / 1024, g.N), 256, 0, st>>>(cb.U, Mp, Np, md, t, cb.ea, cb.eb, g.M, g.N, g.mlo, g.C,
                                                             g.ldc, g.ccol, g.accumulate);
