@@ -170,6 +170,30 @@ def dgemm_peak(torch):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
+def int8_peak(torch):
+    """cuBLASLt INT8 GEMM (torch._int_mm, INT32 accumulation) 8192^3, best of 5: the INT8
+    denominator (MEASURED_PEAKS.json has none).  None if torch lacks the path."""
+    n = 8192
+    try:
+        a = torch.randint(-128, 128, (n, n), device="cuda", dtype=torch.int8)
+        b = torch.randint(-128, 128, (n, n), device="cuda", dtype=torch.int8)
+        for _ in range(2):
+            torch._int_mm(a, b)
+        torch.cuda.synchronize()
+        best = 1e30
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(5):
+            e0.record()
+            torch._int_mm(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        del a, b
+        return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+    except (RuntimeError, AttributeError):
+        return None
+
+
 def residual_max(torch, S, P, ar, ai, be, Q, Z, VL, VR):
     """max over eigenvectors of ||beta S x - alpha P x||_1 / ((|beta| ||S||_1 + |alpha| ||P||_1) ||x||_1)
     in Schur coordinates (x = Z^T v, y = Q^T u; Q, Z orthogonal)."""
@@ -931,6 +955,7 @@ def main():
     VR = torch.empty_like(Z)
     data = (S, P, ar, ai, be, Q, Z, VL, VR)
     peak_fp64 = dgemm_peak(torch)
+    peak_int8 = int8_peak(torch)
     peaks = {}
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pk):
@@ -984,15 +1009,16 @@ def main():
                 "fp64_equivalent_tflops": kd["flops"] / (kd["ms"] * 1e-3) / 1e12,
                 "peak_source": "2 x MEASURED_PEAKS.json bf16_tflops (burst): INT8 dense rate, not measured; "
                                "INT8 slice products counted"}
-    elif kd["flops"] > 0 and head == "split_crt" and dom.startswith("gemm"):
-        # one INT8 product per modulus; the dense INT8 rate is twice the BF16 one on B200
+    elif kd["flops"] > 0 and head == "split_crt" and dom == "split_gemm":
+        # the residue GEMM kernel: one INT8 product per modulus
         achieved = nm_crt * kd["flops"] / (kd["ms"] * 1e-3) / 1e12
-        peak_i8 = 2.0 * peak_bf16
+        peak_i8 = peak_int8 if peak_int8 else 2.0 * peak_bf16
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak_i8, "unit": "TOP/s",
-                "frac": achieved / peak_i8, "kernel": dom,
+                "frac": achieved / peak_i8, "kernel": "gemm_crt_kernel (split_gemm class)",
                 "fp64_equivalent_tflops": kd["flops"] / (kd["ms"] * 1e-3) / 1e12,
-                "peak_source": "2 x MEASURED_PEAKS.json bf16_tflops (burst): INT8 dense rate, not measured; "
-                               "one INT8 product per modulus counted"}
+                "peak_source": ("cuBLASLt INT8 GEMM 8192^3 (torch._int_mm) burst measured in this run"
+                                if peak_int8 else "2 x MEASURED_PEAKS.json bf16_tflops (INT8 not measured)") +
+                               "; one INT8 product per modulus counted"}
     elif kd["flops"] > 0:
         achieved = kd["flops"] / (kd["ms"] * 1e-3) / 1e12
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak_fp64, "unit": "TFLOP/s",
@@ -1099,6 +1125,7 @@ def main():
                            "reference_for_diff": "upstream dtgevc3 (oracle/_ref) on the same S, P, Q, Z; columns "
                                                  "compared after normalisation" if h["err_vs_ref"] is not None else None,
                            "forms": forms_brief,
+                           "peaks_measured_here": {"fp64_dgemm_tflops": peak_fp64, "int8_imma_tops": peak_int8},
                            "batched": None if batched is None else {
                                "pencils_per_s": batched["value"], "speedup_vs_loop": batched["speedup_vs_loop"],
                                "d_ms": batched["d"]["ms"], "s_ms": batched["s"]["ms"],

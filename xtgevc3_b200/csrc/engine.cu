@@ -59,7 +59,7 @@ std::atomic<int> g_trace_on{0};
 std::mutex g_trace_mu;
 TraceTotals g_tot[kTCount];
 const char *g_trace_names[kTCount] = {"prep", "diag_solve", "gemm_update", "gemm_backtransform", "writeback",
-                                      "normalize"};
+                                      "normalize", "split_slices", "split_gemm", "split_reconstruct"};
 
 // Brackets each kernel launch of one call with events when tracing is on; totals are
 // folded in after the call's stream synchronisation.
@@ -446,8 +446,12 @@ static int sm_count()
 // C (+)= A B for a GemmArgs<double> launch by L residues on the INT8 tensor cores (see
 // kernels_crt.cuh).  K must stay below 2^16 (exact INT32 sums; the caller checks).
 static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scratch &scr, int *d_err,
-                              cudaStream_t st)
+                              cudaStream_t st, Tracer *tr = nullptr, double flops = 0)
 {
+    auto run = [&](int cat, double fl, double by, auto &&f) {
+        if (tr) tr->run(cat, fl, by, st, f);
+        else f();
+    };
     using namespace crt;
     const Moduli &md = crt_moduli(L);
     const int Kp = round_up(g.K, BK), Mp = round_up(g.M, TM), Np = round_up(g.N, TN);
@@ -463,10 +467,14 @@ static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scr
     unsigned long long *cmax = cb.rmax + Mp;
     cudaError_t e = cudaMemsetAsync(cb.rmax, 0, (size_t)(Mp + Np) * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
-    row_absmax_kernel<<<dim3(Mp / 32, (g.K + 255) / 256), 256, 0, st>>>(g, cb.rmax);
-    col_absmax_kernel<<<dim3(Np / 32, Kp / 64), 256, 0, st>>>(g, cmax);
-    residue_rows_kernel<<<dim3(Mp / 32, Kp / 64), 256, 0, st>>>(g, Kp, Mp, t, md, cb.rmax, cb.A, cb.ea);
-    residue_cols_kernel<<<dim3(Np / 32, Kp / 64), 256, 0, st>>>(g, Kp, Np, t, md, cmax, cb.B, cb.eb);
+    // operand bytes: A and B read twice (maximum, residues), L residue bytes written per entry
+    const double slice_bytes = ((double)g.M + g.N) * g.K * (2.0 * 8 + L);
+    run(kTSplitPrep, 0, slice_bytes, [&] {
+        row_absmax_kernel<<<dim3(Mp / 32, (g.K + 255) / 256), 256, 0, st>>>(g, cb.rmax);
+        col_absmax_kernel<<<dim3(Np / 32, Kp / 64), 256, 0, st>>>(g, cmax);
+        residue_rows_kernel<<<dim3(Mp / 32, Kp / 64), 256, 0, st>>>(g, Kp, Mp, t, md, cb.rmax, cb.A, cb.ea);
+        residue_cols_kernel<<<dim3(Np / 32, Kp / 64), 256, 0, st>>>(g, Kp, Np, t, md, cmax, cb.B, cb.eb);
+    });
     CUtensorMap tmA, tmB;
     if (!slice_tensor_map(&tmA, cb.A, split::kI8, Kp, L * Mp, TM) ||
         !slice_tensor_map(&tmB, cb.B, split::kI8, Kp, L * Np, TN))
@@ -489,9 +497,13 @@ static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scr
         p.barrett[l] = md.barrett[l];
     }
     const int grid = std::min(sm_count(), p.items);  // persistent: one CTA per SM
-    gemm_crt_kernel<<<grid, THREADS, SMEM_BYTES, st>>>(tmA, tmB, p);
-    crt_kernel<<<dim3((g.M + 1023) / 1024, g.N), 256, 0, st>>>(cb.U, Mp, Np, md, t, cb.ea, cb.eb, g.M, g.N, g.mlo, g.C,
-                                                            g.ldc, g.ccol, g.accumulate);
+    run(kTSplitGemm, flops, 0, [&] { gemm_crt_kernel<<<grid, THREADS, SMEM_BYTES, st>>>(tmA, tmB, p); });
+    // residues in, C (read when accumulating) and out
+    const double crt_bytes = (double)(g.M - g.mlo) * g.N * (L + 8.0 * (1 + g.accumulate));
+    run(kTSplitCrt, 0, crt_bytes, [&] {
+        crt_kernel<<<dim3((g.M + 1023) / 1024, g.N), 256, 0, st>>>(cb.U, Mp, Np, md, t, cb.ea, cb.eb, g.M, g.N, g.mlo,
+                                                                g.C, g.ldc, g.ccol, g.accumulate);
+    });
     return cudaGetLastError();
 }
 
@@ -832,21 +844,29 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         CrtBufs cbuf;
         cudaError_t split_err = cudaSuccess;
         // C (+)= A B of one update or back-transform launch, FP64 DMMA/SIMT or BF16 slices
-        auto gemm = [&](const GemmArgs<E> &g, cudaStream_t gs) {
+        // traced as class `cat` (flops / bytes: the product's algorithmic counts), the residue
+        // form by parts (kTSplitPrep / kTSplitGemm / kTSplitCrt)
+        auto gemm = [&](const GemmArgs<E> &g, cudaStream_t gs, int cat, double flops, double bytes) {
             if constexpr (std::is_same<E, double>::value) {
                 // launches with few output rows (the update of the upper block of a pair) do
                 // too little work per tile to amortise slicing and the tensor-core pipeline;
                 // they never use the slice buffers, so the buffers have one user stream
                 if (nsplit_side && g.M - g.mlo >= 512 && (o.split_kind != 2 || g.K < (1 << 16))) {
-                    cudaError_t e = o.split_kind == 2 ? launch_crt(g, nsplit_side, cbuf, scr, d_err, gs)
-                                    : o.split_kind == split::kI8
-                                        ? launch_split<split::kI8>(g, nsplit_side, sbuf, scr, d_err, gs)
-                                        : launch_split<split::kBF16>(g, nsplit_side, sbuf, scr, d_err, gs);
+                    cudaError_t e = cudaSuccess;
+                    if (o.split_kind == 2) {
+                        e = launch_crt(g, nsplit_side, cbuf, scr, d_err, gs, &tr, flops);
+                    } else {
+                        tr.run(cat, flops, bytes, gs, [&] {
+                            e = o.split_kind == split::kI8
+                                    ? launch_split<split::kI8>(g, nsplit_side, sbuf, scr, d_err, gs)
+                                    : launch_split<split::kBF16>(g, nsplit_side, sbuf, scr, d_err, gs);
+                        });
+                    }
                     if (e != cudaSuccess) split_err = e;
                     return;
                 }
             }
-            launch_gemm<E>(g, o.simt != 0, gs);
+            tr.run(cat, flops, bytes, gs, [&] { launch_gemm<E>(g, o.simt != 0, gs); });
         };
         // row blocks (problem orientation), bottom to top; a 2x2 block is never split
         auto split = [&](int j) -> bool {  // rows j-1, j form a 2x2 diagonal block
@@ -1027,7 +1047,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             const double rows = M - mlo;
             const double uf = 2.0 * rows * g.N * kflops * cfl;
             const double ub = (2.0 * rows * g.N + rows * kflops + kflops * g.N) * esz;
-            tr.run(kTUpdate, uf, ub, us, [&] { gemm(g, us); });
+            gemm(g, us, kTUpdate, uf, ub);
         };
         // safe_lo >= 0: deferred guard scaling of the rows above safe_lo (look-ahead)
         // ypad < 0: the block's rows padded to kKPad
@@ -1311,7 +1331,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
                 for (int c = c0; c < c1; c++) bk += L.kext[c];
                 const double bf = 2.0 * n * bk * cfl;
                 const double bb = ((double)n * L.kext[c1 - 1] + bk + (double)n * (c1 - c0)) * esz;
-                tr.run(kTBack, bf, bb, st, [&] { gemm(g, st); });
+                gemm(g, st, kTBack, bf, bb);
                 if (o.cols_done && !o.normalize) {
                     int o0 = m, o1 = 0;
                     for (int c = c0; c < c1; c++) {

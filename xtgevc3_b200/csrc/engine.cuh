@@ -100,7 +100,12 @@ void set_last_error(const std::string &s);
 
 // Kernel trace: per kernel class, launches, CUDA-event time on the launching stream and
 // algorithmic flops / bytes (the operation counts of the math, not hardware counters).
-enum TraceCat { kTPrep = 0, kTDiag, kTUpdate, kTBack, kTWriteback, kTNormalize, kTCount };
+// The split forms' GEMMs are traced by part: kTSplitPrep (operand exponents and slices /
+// residues), kTSplitGemm (the tensor-core kernel; flops = the FP64 product's 2MNK) and
+// kTSplitCrt (reconstruction of the residue form); the rest of their update / back-transform
+// work stays in kTUpdate / kTBack.
+enum TraceCat { kTPrep = 0, kTDiag, kTUpdate, kTBack, kTWriteback, kTNormalize, kTSplitPrep, kTSplitGemm, kTSplitCrt,
+                kTCount };
 const char *trace_name(int cat);
 void trace_enable(int on);
 void trace_reset();
