@@ -23,6 +23,7 @@
 #include "kernels_misc.cuh"
 #include "kernels_split.cuh"
 #include "kernels_crt.cuh"
+#include "kernels_crt2.cuh"
 #include "kernels_refine.cuh"
 #include "host_common.cuh"
 
@@ -191,6 +192,7 @@ void configure_device(int dev)
         cudaFuncSetAttribute(split::gemm_split_kernel<split::kI8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              split::Layout<split::kI8>::SMEM_BYTES);
         cudaFuncSetAttribute(crt::gemm_crt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, crt::SMEM_BYTES);
+        cudaFuncSetAttribute(crt2::gemm_crt2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, crt2::SMEM_BYTES);
     });
 }
 
@@ -445,6 +447,36 @@ static int sm_count()
 
 // C (+)= A B for a GemmArgs<double> launch by L residues on the INT8 tensor cores (see
 // kernels_crt.cuh).  K must stay below 2^16 (exact INT32 sums; the caller checks).
+// The residue GEMM runs on SM pairs (kernels_crt2.cuh) unless XTGEVC3_CRT_PAIR=0 selects
+// the one-CTA kernel; pairs resident at once, from the occupancy API (cached per device).
+static bool crt_pairs()
+{
+    static const bool on = [] {
+        const char *v = std::getenv("XTGEVC3_CRT_PAIR");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
+static int crt_pair_grid()
+{
+    static int cached[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 2 * (sm_count() / 2);
+    if (!cached[dev]) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(2 * (sm_count() / 2));
+        cfg.blockDim = dim3(crt::THREADS);
+        cfg.dynamicSmemBytes = crt2::SMEM_BYTES;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, crt2::gemm_crt2_kernel, &cfg) != cudaSuccess || clusters <= 0) {
+            cudaGetLastError();
+            clusters = sm_count() / 2;
+        }
+        cached[dev] = 2 * clusters;
+    }
+    return cached[dev];
+}
+
 static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scratch &scr, int *d_err,
                               cudaStream_t st, Tracer *tr = nullptr, double flops = 0)
 {
@@ -454,7 +486,8 @@ static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scr
     };
     using namespace crt;
     const Moduli &md = crt_moduli(L);
-    const int Kp = round_up(g.K, BK), Mp = round_up(g.M, TM), Np = round_up(g.N, TN);
+    const bool pairs = crt_pairs();
+    const int Kp = round_up(g.K, BK), Mp = round_up(g.M, TM), Np = round_up(g.N, pairs ? crt2::TNP : TN);
     const int t = crt_bits(L, g.K);
     const size_t an = (size_t)L * Mp * Kp, bn = (size_t)L * Np * Kp, un = (size_t)L * Np * Mp;
     if (an > cb.acap) { cb.A = scr.get<int8_t>(an); cb.acap = an; }
@@ -476,8 +509,8 @@ static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scr
         residue_cols_kernel<<<dim3(Np / 32, Kp / 64), 256, 0, st>>>(g, Kp, Np, t, md, cmax, cb.B, cb.eb);
     });
     CUtensorMap tmA, tmB;
-    if (!slice_tensor_map(&tmA, cb.A, split::kI8, Kp, L * Mp, TM) ||
-        !slice_tensor_map(&tmB, cb.B, split::kI8, Kp, L * Np, TN))
+    if (!slice_tensor_map(&tmA, cb.A, split::kI8, Kp, L * Mp, pairs ? crt2::HALF : TM) ||
+        !slice_tensor_map(&tmB, cb.B, split::kI8, Kp, L * Np, pairs ? crt2::HALF : TN))
         return cudaErrorInvalidValue;
     Params p;
     p.M = g.M;
@@ -487,7 +520,7 @@ static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scr
     p.Np = Np;
     p.L = L;
     p.mtiles = Mp / TM;
-    p.ntiles = Np / TN;
+    p.ntiles = Np / (pairs ? crt2::TNP : TN);
     p.items = L * p.mtiles * p.ntiles;
     p.kext = g.kext;
     p.U = cb.U;
@@ -496,8 +529,14 @@ static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scr
         p.p[l] = md.p[l];
         p.barrett[l] = md.barrett[l];
     }
-    const int grid = std::min(sm_count(), p.items);  // persistent: one CTA per SM
-    run(kTSplitGemm, flops, 0, [&] { gemm_crt_kernel<<<grid, THREADS, SMEM_BYTES, st>>>(tmA, tmB, p); });
+    if (pairs) {
+        const int grid = std::min(crt_pair_grid(), 2 * p.items);  // persistent pairs of CTAs
+        run(kTSplitGemm, flops, 0,
+            [&] { crt2::gemm_crt2_kernel<<<grid, THREADS, crt2::SMEM_BYTES, st>>>(tmA, tmB, p); });
+    } else {
+        const int grid = std::min(sm_count(), p.items);  // persistent: one CTA per SM
+        run(kTSplitGemm, flops, 0, [&] { gemm_crt_kernel<<<grid, THREADS, SMEM_BYTES, st>>>(tmA, tmB, p); });
+    }
     // residues in, C (read when accumulating) and out
     const double crt_bytes = (double)(g.M - g.mlo) * g.N * (L + 8.0 * (1 + g.accumulate));
     run(kTSplitCrt, 0, crt_bytes, [&] {
