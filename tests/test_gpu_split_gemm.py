@@ -67,3 +67,27 @@ def test_split_gemm_rejects_bad_arguments():
     lib = X.lib()
     rc = lib.xtgevc3_split_gemm_dev(None, 3, 0, 4, 4, 4, None, 4, None, 4, None, 4, 0)
     assert rc == -1 and "bad argument" in X.last_error()
+
+
+def test_split_gemm_crt_pair_kernel(cuda_ok):
+    """The SM-pair form of the residue GEMM (XTGEVC3_CRT_PAIR=1, tcgen05 cta_group::2) against
+    FP64 on ragged and square shapes, in a child process (the kernel choice is read once per
+    process)."""
+    import subprocess
+    import sys
+    import os
+    code = (
+        "import numpy as np, torch, xtgevc3_b200 as X\n"
+        "rng = np.random.default_rng(9)\n"
+        "for M, N, K in ((300, 500, 700), (129, 257, 65), (1024, 1024, 1024), (33, 7, 5)):\n"
+        "    A = torch.from_numpy(np.ascontiguousarray(rng.standard_normal((M, K)).T)).cuda().t()\n"
+        "    B = torch.from_numpy(np.ascontiguousarray(rng.standard_normal((K, N)).T)).cuda().t()\n"
+        "    C = X.split_gemm(2, A, B)\n"
+        "    s = torch.linalg.vector_norm(A, dim=1)[:, None] * torch.linalg.vector_norm(B, dim=0)[None, :]\n"
+        "    e = float(((C - A @ B).abs() / s).max())\n"
+        "    assert e < 1e-13, (M, N, K, e)\n"
+        "print('pair ok')\n")
+    env = dict(os.environ, XTGEVC3_CRT_PAIR="1")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=300,
+                       cwd=os.path.join(os.path.dirname(__file__), ".."))
+    assert r.returncode == 0 and "pair ok" in r.stdout, r.stdout + r.stderr

@@ -447,13 +447,14 @@ static int sm_count()
 
 // C (+)= A B for a GemmArgs<double> launch by L residues on the INT8 tensor cores (see
 // kernels_crt.cuh).  K must stay below 2^16 (exact INT32 sums; the caller checks).
-// The residue GEMM runs on SM pairs (kernels_crt2.cuh) unless XTGEVC3_CRT_PAIR=0 selects
-// the one-CTA kernel; pairs resident at once, from the occupancy API (cached per device).
+// The residue GEMM runs on one CTA per SM (kernels_crt.cuh); XTGEVC3_CRT_PAIR=1 selects the
+// SM-pair kernel (kernels_crt2.cuh: a third less operand traffic per SM, measured slower on
+// this solver's shapes).  Pairs resident at once come from the occupancy API (cached per device).
 static bool crt_pairs()
 {
     static const bool on = [] {
         const char *v = std::getenv("XTGEVC3_CRT_PAIR");
-        return !(v && v[0] == '0');
+        return v && v[0] == '1';
     }();
     return on;
 }
