@@ -447,6 +447,34 @@ def measure_form(name, flags, args, X, torch, data, dist, local, world, ref=None
             "err_vs_ref": err, "refined_columns": refined, "clocks": clk, "launches": launches, "kernels": kernels}
 
 
+def measure_normalize(args, X, torch, data, peak_hbm):
+    """XTGEVC3_NORMALIZE on the plain form: the one-pass normalisation kernel's time per call
+    from the library trace (both sides), and its rate against the HBM peak: each entry of
+    VL and VR read once and written once, 2 x 2 n^2 x 8 bytes per call."""
+    S, P, ar, ai, be, Q, Z, VL, VR = data
+    n = S.shape[0]
+    for _ in range(max(args.warmup, 1)):
+        VL.copy_(Q)
+        VR.copy_(Z)
+        X.tgevc3_dev("B", "B", S, P, ar, be, alphai=ai, VL=VL, VR=VR, flags=X.NORMALIZE)
+    torch.cuda.synchronize()
+    X.trace_reset()
+    X.trace_enable(True)
+    for _ in range(args.steps):
+        VL.copy_(Q)
+        VR.copy_(Z)
+        X.tgevc3_dev("B", "B", S, P, ar, be, alphai=ai, VL=VL, VR=VR, flags=X.NORMALIZE)
+    torch.cuda.synchronize()
+    X.trace_enable(False)
+    t = X.trace()["normalize"]
+    ms = t["ms"] / args.steps
+    byts = t["bytes"] / args.steps
+    mx = max(float(VL.abs().amax(0).max()), float(VR.abs().amax(0).max()))
+    return {"ms_per_call": ms, "bytes_per_call": byts, "gbs": byts / (ms * 1e-3) / 1e9,
+            "frac_of_hbm": byts / (ms * 1e-3) / 1e9 / peak_hbm, "launches_per_call": t["launches"] / args.steps,
+            "largest_entry_after": mx}
+
+
 def batched_inputs(count, seed, torch):
     """The batched workload on the device: `count` pencils of orders n ~ U{16..512}
     (seeded), each in generalized Schur form with the block statistics of the single-pencil
@@ -1091,6 +1119,7 @@ def main():
                    f"in pieces while the solve runs, norms from host threads; Q, Z and the result columns "
                    f"overlapped with it)"}
 
+    norm = measure_normalize(args, X, torch, data, peak_hbm) if rank == 0 else None
     batched = measure_batched(args, X, torch, dist, world) if args.batch_count > 0 else None
     adjoint = measure_adjoint(args, X, torch) if args.adjoint_n > 0 and rank == 0 else None
     zleg = measure_ztgevc3(args, X, torch) if args.z_n > 0 and rank == 0 else None
@@ -1126,12 +1155,14 @@ def main():
                                                  "compared after normalisation" if h["err_vs_ref"] is not None else None,
                            "forms": forms_brief,
                            "peaks_measured_here": {"fp64_dgemm_tflops": peak_fp64, "int8_imma_tops": peak_int8},
+                           "normalize": None if norm is None else {
+                               "ms": norm["ms_per_call"], "gbs": norm["gbs"], "frac_of_hbm": norm["frac_of_hbm"]},
                            "batched": None if batched is None else {
                                "pencils_per_s": batched["value"], "speedup_vs_loop": batched["speedup_vs_loop"],
                                "d_ms": batched["d"]["ms"], "s_ms": batched["s"]["ms"],
                                "d_max_rel_diff_vs_loop": batched["d"]["max_rel_diff_vs_loop"]}},
                 "forms": forms_out, "clocks": h["clocks"], "e2e": e2e, "gpu_launches": h["launches"],
-                "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "batched": batched,
+                "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "normalize": norm, "batched": batched,
                 "adjoint": adjoint, "ztgevc3": zleg, "dtrevc3": trleg, "ztgexc": txleg}
         print(json.dumps(line), flush=True)
     if dist:

@@ -449,3 +449,40 @@ def test_config_dgges_n1024_both_sides_back_transformed(cuda_ok):
         assert err <= 1e-11, (side, err, int(np.nanargmax(cols)))
         r = oracle.residual_ratio(A, B, a, al, bc, left=(side == "L"))
         assert r.max() < 100, (side, r.max())
+
+
+@pytest.mark.parametrize("n", [700, 1500, 3000, 6000, 8300])
+def test_normalize_one_pass_kernel_sizes(cuda_ok, n):
+    """XTGEVC3_NORMALIZE over every register tile of the one-pass kernel (rows per thread 4,
+    8, 16, 32) and the two-pass form past 8192 rows, on the device with a selection: every
+    normalised eigenvector (a real pair jointly) has max |re| + |im| = 1 and is the
+    unnormalised one times a positive scalar (to rounding)."""
+    import torch
+    S, P, ar, ai, be = pencils.gen_schur_like(n, 50 + n)
+    sel = (np.random.default_rng(n).random(n) < 0.3).astype(np.int32)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a.T)).cuda().t()  # noqa: E731
+    dS, dP = dev(S), dev(P)
+    outs = []
+    for flags in (0, X.NORMALIZE):
+        VL = torch.zeros(n, n, dtype=torch.float64, device="cuda").t()
+        VR = torch.zeros(n, n, dtype=torch.float64, device="cuda").t()
+        m, info = X.tgevc3_dev("B", "S", dS, dP, ar, be, alphai=ai, VL=VL, VR=VR, select=sel, flags=flags)
+        assert info == 0
+        outs.append((VL[:, :m], VR[:, :m]))
+    # columns of each eigenvector: a pair's two columns share one scale
+    items, k, c = [], 0, 0
+    while k < n:
+        pair = ai[k] != 0 and k + 1 < n
+        if sel[k] or (pair and sel[k + 1]):
+            items.append((c, pair))
+            c += 2 if pair else 1
+        k += 2 if pair else 1
+    for side in (0, 1):
+        V0, V1 = outs[0][side], outs[1][side]
+        for c, pair in items:
+            a0 = V0[:, c:c + (2 if pair else 1)]
+            a1 = V1[:, c:c + (2 if pair else 1)]
+            mx = float(a1.abs().sum(1).max()) if pair else float(a1.abs().max())
+            assert abs(mx - 1.0) < 1e-14, (side, c, mx)
+            s = float((a0.abs().sum(1).max()) if pair else a0.abs().max())
+            assert float((a0 / s - a1).abs().max()) < 1e-15 * 4, (side, c)

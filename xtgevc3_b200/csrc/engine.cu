@@ -1391,12 +1391,28 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
 
         if (o.normalize) {
             if constexpr (CPLX) {
+                cplx<R> *Vc = reinterpret_cast<cplx<R> *>(V);
                 tr.run(kTNormalize, 0, 2.0 * n * m * esz, st, [&] {
-                    normalize_cplx_kernel<R><<<m, 256, 0, st>>>(reinterpret_cast<cplx<R> *>(V), ldv, n, d_outcol, m);
+                    if (n <= 1024) normalize_cplx_1p_kernel<R, 4><<<m, 256, 0, st>>>(Vc, ldv, n, d_outcol, m);
+                    else if (n <= 2048) normalize_cplx_1p_kernel<R, 8><<<m, 256, 0, st>>>(Vc, ldv, n, d_outcol, m);
+                    else if (n <= 4096) normalize_cplx_1p_kernel<R, 16><<<m, 256, 0, st>>>(Vc, ldv, n, d_outcol, m);
+                    else if (n <= 8192) normalize_cplx_1p_kernel<R, 32><<<m, 256, 0, st>>>(Vc, ldv, n, d_outcol, m);
+                    else normalize_cplx_kernel<R><<<m, 256, 0, st>>>(Vc, ldv, n, d_outcol, m);  // two passes
                 });
             } else {
-                tr.run(kTNormalize, 0, 2.0 * n * m * esz, st,
-                       [&] { normalize_real_kernel<R><<<m, 256, 0, st>>>(V, ldv, n, d_outcol, d_kind, m); });
+                const int ni = nitems;
+                tr.run(kTNormalize, 0, 2.0 * n * m * esz, st, [&] {
+                    if (n <= 1024)
+                        normalize_real_1p_kernel<R, 4><<<ni, 256, 0, st>>>(V, ldv, n, d_items, d_outcol, d_kind, ni);
+                    else if (n <= 2048)
+                        normalize_real_1p_kernel<R, 8><<<ni, 256, 0, st>>>(V, ldv, n, d_items, d_outcol, d_kind, ni);
+                    else if (n <= 4096)
+                        normalize_real_1p_kernel<R, 16><<<ni, 256, 0, st>>>(V, ldv, n, d_items, d_outcol, d_kind, ni);
+                    else if (n <= 8192)
+                        normalize_real_1p_kernel<R, 32><<<ni, 256, 0, st>>>(V, ldv, n, d_items, d_outcol, d_kind, ni);
+                    else
+                        normalize_real_kernel<R><<<m, 256, 0, st>>>(V, ldv, n, d_outcol, d_kind, m);  // two passes
+                });
             }
             XTG_CK(cudaGetLastError());
         }

@@ -229,6 +229,80 @@ __global__ void normalize_real_kernel(R *V, int ldv, int n, const int *outcol, c
     }
 }
 
+// One-pass normalisation (LAPACK convention: max_i |re| + |im| = 1, a real (Re, Im) pair
+// jointly): one CTA of 256 threads per eigenvector (items: its first column), the rows
+// (RPT per thread, coalesced) stay in registers between the maximum and the scaling, so
+// each entry is read once and written once.  n <= 256 RPT.
+template <class R, int RPT>
+__global__ void __launch_bounds__(256) normalize_real_1p_kernel(R *V, int ldv, int n, const int *items,
+                                                               const int *outcol, const uint8_t *kind, int nitems)
+{
+    const int it = blockIdx.x;
+    if (it >= nitems) return;
+    const int c = items[it];
+    const bool pair = kind[c] == kPairRe;
+    R *v0 = V + (size_t)outcol[c] * ldv;  // a pair's (Re, Im) output columns are adjacent
+    R *v1 = v0 + ldv;
+    R a[RPT], b[RPT];
+    R mx = 0;
+#pragma unroll
+    for (int q = 0; q < RPT; q++) {
+        const int r = threadIdx.x + 256 * q;
+        a[q] = r < n ? v0[r] : R(0);
+        b[q] = (pair && r < n) ? v1[r] : R(0);
+        mx = fmax(mx, fabs(a[q]) + fabs(b[q]));
+    }
+    __shared__ R red[8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    mx = red[0];
+#pragma unroll
+    for (int w = 1; w < 8; w++) mx = fmax(mx, red[w]);
+    if (!(mx > R(0))) return;
+    const R s = R(1) / mx;
+#pragma unroll
+    for (int q = 0; q < RPT; q++) {
+        const int r = threadIdx.x + 256 * q;
+        if (r < n) {
+            v0[r] = a[q] * s;
+            if (pair) v1[r] = b[q] * s;
+        }
+    }
+}
+
+template <class R, int RPT>
+__global__ void __launch_bounds__(256) normalize_cplx_1p_kernel(cplx<R> *V, int ldv, int n, const int *outcol, int m)
+{
+    const int c = blockIdx.x;
+    if (c >= m) return;
+    cplx<R> *v = V + (size_t)outcol[c] * ldv;
+    cplx<R> a[RPT];
+    R mx = 0;
+#pragma unroll
+    for (int q = 0; q < RPT; q++) {
+        const int r = threadIdx.x + 256 * q;
+        a[q] = r < n ? v[r] : cplx<R>(R(0), R(0));
+        mx = fmax(mx, l1abs(a[q]));
+    }
+    __shared__ R red[8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    mx = red[0];
+#pragma unroll
+    for (int w = 1; w < 8; w++) mx = fmax(mx, red[w]);
+    if (!(mx > R(0))) return;
+    const R s = R(1) / mx;
+#pragma unroll
+    for (int q = 0; q < RPT; q++) {
+        const int r = threadIdx.x + 256 * q;
+        if (r < n) v[r] = s * a[q];
+    }
+}
+
 template <class R>
 __global__ void normalize_cplx_kernel(cplx<R> *V, int ldv, int n, const int *outcol, int m)
 {
