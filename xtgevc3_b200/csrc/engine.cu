@@ -850,20 +850,20 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
     }
     // Flags of one side's columns from the sketch T = [GS; GP] X (see kernels_refine.cuh).
-    auto refine_side = [&](const E *X, int ldx, const SideCols &sc, const R *coef, const E *T, uint8_t *flags,
+    // Flags of one side's columns from the sketch T = [GS; GP] X and ||x||^2 (see
+    // kernels_refine.cuh), copied to the pinned host flags.
+    auto refine_side = [&](const SideCols &sc, const R *coef, const E *T, const E *x2, uint8_t *flags,
                            cudaStream_t st, Scratch &scr) -> int {
         if constexpr (!CPLX && std::is_same<R, double>::value) {
             using namespace refine;
             const int m = sc.L.m, nitems = (int)sc.starts.size();
-            double *x2 = scr.get<double>((size_t)m);
             int *cnt = scr.get<int>(1);
             if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
             XTG_CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
-            tr.run(kTPrep, 0, 0.5 * (double)n * m * esz, st, [&] {
-                column_sumsq_kernel<<<(m * 32 + 255) / 256, 256, 0, st>>>(X, ldx, m, sc.d_ints + 2 * m, x2);
-                refine_flags_kernel<<<(nitems + 255) / 256, 256, 0, st>>>(T, x2, sc.d_ints + 4 * m, nitems,
-                                                                          sc.d_kind, coef, d_norms, opt.refine_bound,
-                                                                          flags, cnt);
+            tr.run(kTPrep, 0, 0, st, [&] {
+                refine_flags_kernel<<<(nitems + 255) / 256, 256, 0, st>>>(T, x2, sc.d_ints + 4 * m, nitems, sc.d_kind,
+                                                                          coef, d_norms, opt.refine_bound, flags,
+                                                                          cnt);
             });
             XTG_CK(cudaGetLastError());
             const size_t off = (size_t)(flags - d_flags);
@@ -1002,44 +1002,14 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         XTG_CK(cudaGetLastError());
 
         // ---- residual sketch of the refinement check (split form) ------------------------------
-        // [GS; GP] = G [S P] and T = [GS; GP] X, after the substitution: X's rows in chunks of
-        // 1024 (short K per launch), each chunk over the columns it can reach.
-        E *sk_G2 = nullptr, *sk_T = nullptr;
+        // [GS; GP] = G [S P] and T = [GS; GP] X with ||x_c||^2, after the substitution.
+        E *sk_G2 = nullptr, *sk_T = nullptr, *sk_x2 = nullptr;
         if (flags) {
             sk_G2 = scr.get<E>((size_t)n * 2 * refine::K);
             sk_T = scr.get<E>((size_t)m * 2 * refine::K);
+            sk_x2 = scr.get<E>((size_t)m);
             if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
-            XTG_CK(cudaMemsetAsync(sk_T, 0, (size_t)m * 2 * refine::K * sizeof(E), st));
         }
-        // T[:, c0:] += G2[:, j0:j1] X[j0:j1, c0:] (G2 complete)
-        auto sketch_rows = [&](int j0, int j1, int c0) {
-            if constexpr (!CPLX && std::is_same<R, double>::value) {
-                using namespace refine;
-                const int cnt = j1 - j0;
-                if (c0 >= m) return;
-                GemmArgs<double> g{};
-                g.M = 2 * K;
-                g.N = m - c0;
-                g.mlo = 0;
-                g.nseg = 1;
-                g.seg[0].A = sk_G2 + (size_t)j0 * 2 * K;
-                g.seg[0].lda = 2 * K;
-                g.seg[0].acols = cnt;
-                g.seg[0].K = round_up(cnt, kKPad);
-                g.seg[0].boff = j0;
-                g.K = g.seg[0].K;
-                g.B = X + (size_t)c0 * ldx;
-                g.ldb = ldx;
-                g.brows = n;
-                g.C = sk_T + (size_t)c0 * 2 * K;
-                g.ldc = 2 * K;
-                g.ccol = nullptr;
-                g.kext = nullptr;
-                g.accumulate = 1;
-                tr.run(kTPrep, 2.0 * 2 * K * cnt * (m - c0), 0, st, [&] { launch_gemm<double>(g, false, st); });
-            }
-        };
-
         // ---- blocked substitution ----------------------------------------------------------
         // Row blocks are taken in groups of `group` adjacent blocks, rows [q0, q1), bottom to
         // top: each block is solved, then the rows of the group's blocks above it are updated
@@ -1176,12 +1146,11 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             if (flags) {
                 using namespace refine;
                 tr.run(kTPrep, 0, (double)n * n * esz, st, [&] {
-                    sketch_matrix_kernel<<<n, 256, 0, st>>>(Sp, lsp, n, 1, sk_G2, 2 * K);
-                    sketch_matrix_kernel<<<n, 256, 0, st>>>(Pp, lpp, n, 0, sk_G2 + K, 2 * K);
+                    sketch_matrix_kernel<<<n, 256, 0, st>>>(Sp, lsp, Pp, lpp, n, sk_G2);
                 });
-                // chunk [j0, j1) reaches the columns whose extent passes j0 (X is zero below it)
-                for (int j0 = 0; j0 < n; j0 += 1024)
-                    sketch_rows(j0, std::min(n, j0 + 1024), first_col(std::max(0, j0 - 1)));
+                tr.run(kTPrep, 0, 0.5 * (double)n * m * esz, st, [&] {
+                    sketch_columns_kernel<<<(m + 63) / 64, 256, 0, st>>>(sk_G2, X, ldx, m, d_kext, sk_T, sk_x2);
+                });
             }
         }
         // Look-ahead (ahead == true).  Pair p owns rows [u0_p, l1_p); the next pair's rows are
@@ -1308,7 +1277,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         // residual exceeds the bound are flagged and solved again in FP64 after the call's
         // split pass (see the end of solve_device).
         if constexpr (!CPLX && std::is_same<R, double>::value) {
-            if (flags && refine_side(X, ldx, sc, coef, sk_T, flags, st, scr)) return 1;
+            if (flags && refine_side(sc, coef, sk_T, sk_x2, flags, st, scr)) return 1;
         }
 
         // ---- write-back / back-transform -----------------------------------------------------

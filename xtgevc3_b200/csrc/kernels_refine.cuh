@@ -9,8 +9,7 @@
 // complex residual is (ac S - (br + i bi) P)(xr + i xi).  The column's relative residual
 //   est_c = ||G r_c|| / 4 / ((|ac| anorm + |b| bnorm) ||x_c||_2)
 // is flagged when it exceeds bound / 4 (a margin for the spread of the estimate) or is not
-// finite.  Cost: S and P once (16 sums per entry); [GS; GP] X as one FP64 tensor-core GEMM
-// (32 x n times the triangular X), and the column norms of X.
+// finite.  Cost: S and P once (16 sums per entry each), X once (32 sums per entry).
 #pragma once
 #include "common.cuh"
 
@@ -31,58 +30,87 @@ __device__ __forceinline__ uint32_t sign_bits(uint32_t i)
     return h;
 }
 
-// GA[j * ldg + r] = sum_{i <= min(n-1, j + hess)} G(r, i) A(i, j): one CTA of 256 threads
-// per column j (A upper triangular, hess = 0, or upper Hessenberg, hess = 1); GA is the
-// 16 x n sketch stored column-major with leading dimension ldg.
-__global__ void __launch_bounds__(256) sketch_matrix_kernel(const double *A, int lda, int n, int hess, double *GA,
-                                                            int ldg)
+// G2 = [G S; G P], 2K x n column-major (leading dimension 2K): one CTA of 256 threads per
+// column j sums G(r, i) S(i, j) over rows i <= min(n-1, j+1) (S upper Hessenberg) and
+// G(r, i) P(i, j) over i <= j (P upper triangular), one sign word per row.
+__global__ void __launch_bounds__(256) sketch_matrix_kernel(const double *S, int lds, const double *P, int ldp, int n,
+                                                            double *G2)
 {
-    __shared__ double part[8][K];
+    __shared__ double part[8][2 * K];
     const int j = blockIdx.x;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double acc[K];
+    double acc[2 * K];
 #pragma unroll
-    for (int r = 0; r < K; r++) acc[r] = 0.0;
-    const int rows = min(n, j + 1 + hess);
-    const double *a = A + (size_t)j * lda;
+    for (int r = 0; r < 2 * K; r++) acc[r] = 0.0;
+    const int rows = min(n, j + 2);
+    const double *sc = S + (size_t)j * lds, *pc = P + (size_t)j * ldp;
     for (int i = threadIdx.x; i < rows; i += blockDim.x) {
-        const double v = a[i];
+        const double vs = sc[i], vp = i <= j ? pc[i] : 0.0;
         const uint32_t b = sign_bits((uint32_t)i);
 #pragma unroll
-        for (int r = 0; r < K; r++) acc[r] += ((b >> r) & 1u) ? v : -v;
+        for (int r = 0; r < K; r++) {
+            const bool plus = (b >> r) & 1u;
+            acc[r] += plus ? vs : -vs;
+            acc[K + r] += plus ? vp : -vp;
+        }
     }
 #pragma unroll
-    for (int r = 0; r < K; r++)
+    for (int r = 0; r < 2 * K; r++)
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], o);
-    if (lane < K) {
-        double v = acc[0];
+    double v = acc[0];
 #pragma unroll
-        for (int r = 1; r < K; r++)
-            if (lane == r) v = acc[r];
-        part[warp][lane] = v;
-    }
+    for (int r = 1; r < 2 * K; r++)
+        if (lane == r) v = acc[r];
+    part[warp][lane] = v;
     __syncthreads();
-    if (threadIdx.x < K) {
-        double v = 0.0;
-        for (int w = 0; w < 8; w++) v += part[w][threadIdx.x];
-        GA[(size_t)j * ldg + threadIdx.x] = v;
+    if (threadIdx.x < 2 * K) {
+        double t = 0.0;
+        for (int w = 0; w < 8; w++) t += part[w][threadIdx.x];
+        G2[(size_t)j * 2 * K + threadIdx.x] = t;
     }
 }
 
-// ||x_c||^2 over rows [0, kext_c) of each column of X: one warp per column.
-__global__ void __launch_bounds__(256) column_sumsq_kernel(const double *X, int ldx, int m, const int *kext,
-                                                           double *x2)
+// T[:, c] = G2 X[:, c] (2K sums per column over its rows [0, kext_c)) and x2[c] = ||x_c||^2.
+// A CTA of 256 threads takes 64 consecutive columns and walks their rows in chunks of 32,
+// staged in shared memory with the chunk's 32 x 2K sketch entries; thread t computes 8 of
+// the 2K sums (rows 8 (t / 64) .. +7 of T) of column t % 64 and, for t < 64, the norm.
+__global__ void __launch_bounds__(256) sketch_columns_kernel(const double *G2, const double *X, int ldx, int m,
+                                                            const int *kext, double *T, double *x2)
 {
-    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (c >= m) return;
-    const double *xc = X + (size_t)c * ldx;
-    double s = 0.0;
-    for (int j = lane; j < kext[c]; j += 32) s = fma(xc[j], xc[j], s);
+    __shared__ double xs[32][65];
+    __shared__ double gs[32][2 * K + 1];
+    const int c0 = blockIdx.x * 64, tc = threadIdx.x & 63, rg = threadIdx.x >> 6;
+    const int c = c0 + tc;
+    int kmax = 0;
+    for (int q = 0; q < 64 && c0 + q < m; q++) kmax = max(kmax, kext[c0 + q]);
+    double acc[8], nrm = 0.0;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) x2[c] = s;
+    for (int r = 0; r < 8; r++) acc[r] = 0.0;
+    for (int j0 = 0; j0 < kmax; j0 += 32) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < 32 * 64; e += 256) {  // X chunk: 32 rows x 64 columns
+            const int jj = e & 31, cc = e >> 5, col = c0 + cc, j = j0 + jj;
+            xs[jj][cc] = (col < m && j < kext[col]) ? X[(size_t)col * ldx + j] : 0.0;
+        }
+        for (int e = threadIdx.x; e < 32 * 2 * K; e += 256) {  // sketch rows of the chunk
+            const int jj = e / (2 * K), r = e % (2 * K), j = j0 + jj;
+            gs[jj][r] = j < kmax ? G2[(size_t)j * 2 * K + r] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int jj = 0; jj < 32; jj++) {
+            const double xv = xs[jj][tc];
+            if (rg == 0) nrm = fma(xv, xv, nrm);
+#pragma unroll
+            for (int r = 0; r < 8; r++) acc[r] = fma(gs[jj][8 * rg + r], xv, acc[r]);
+        }
+    }
+    if (c < m) {
+#pragma unroll
+        for (int r = 0; r < 8; r++) T[(size_t)c * 2 * K + 8 * rg + r] = acc[r];
+        if (rg == 0) x2[c] = nrm;
+    }
 }
 
 // Flags of the columns of each eigenvector (items: first column of each; a pair's two
