@@ -399,6 +399,7 @@ static void build_moduli(crt::Moduli &md, int L)
         md.p[l] = p;
         md.barrett[l] = (unsigned int)((((unsigned long long)1) << 32) / (unsigned long long)p);
         md.invp[l] = 1.0 / (double)p;
+        md.pd[l] = (double)p;
         md.w1[l] = (double)(W >> md.hi);
         md.w2[l] = (double)((W >> md.lo) & mask_mid);
     }
@@ -426,7 +427,8 @@ static int crt_bits(int L, int K)
 {
     int kb = 0;
     while ((1 << kb) < std::max(K, 2)) kb++;
-    return (int)std::floor((crt_moduli(L).log2P - kb - 2) / 2);
+    // at most 50: the residue kernels round v 2^t against 1.5 2^52, exact for |a| < 2^51
+    return std::min(50, (int)std::floor((crt_moduli(L).log2P - kb - 2) / 2));
 }
 
 // Reusable residue buffers of one side (grown on demand from the call's scratch).
@@ -506,8 +508,15 @@ static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scr
     run(kTSplitPrep, 0, slice_bytes, [&] {
         row_absmax_kernel<<<dim3(Mp / 32, (g.K + 255) / 256), 256, 0, st>>>(g, cb.rmax);
         col_absmax_kernel<<<dim3(Np / 32, Kp / 64), 256, 0, st>>>(g, cmax);
-        residue_rows_kernel<<<dim3(Mp / 32, Kp / 64), 256, 0, st>>>(g, Kp, Mp, t, md, cb.rmax, cb.A, cb.ea);
-        residue_cols_kernel<<<dim3(Np / 32, Kp / 64), 256, 0, st>>>(g, Kp, Np, t, md, cmax, cb.B, cb.eb);
+        const dim3 gr(Mp / 32, Kp / 64), gc(Np / 32, Kp / 64);
+        const int tnw = pairs ? crt2::TNP : TN;
+        if (L == 14) {  // the default modulus count: moduli at fixed offsets
+            residue_rows_kernel<14><<<gr, 256, 0, st>>>(g, Kp, Mp, t, md, cb.rmax, cb.A, cb.ea);
+            residue_cols_kernel<14><<<gc, 256, 0, st>>>(g, Kp, Np, tnw, t, md, cmax, cb.B, cb.eb);
+        } else {
+            residue_rows_kernel<0><<<gr, 256, 0, st>>>(g, Kp, Mp, t, md, cb.rmax, cb.A, cb.ea);
+            residue_cols_kernel<0><<<gc, 256, 0, st>>>(g, Kp, Np, tnw, t, md, cmax, cb.B, cb.eb);
+        }
     });
     CUtensorMap tmA, tmB;
     if (!slice_tensor_map(&tmA, cb.A, split::kI8, Kp, L * Mp, pairs ? crt2::HALF : TM) ||
@@ -849,7 +858,6 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         d_flags = scr.get<uint8_t>(2 * (size_t)m_total);
         if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
     }
-    // Flags of one side's columns from the sketch T = [GS; GP] X (see kernels_refine.cuh).
     // Flags of one side's columns from the sketch T = [GS; GP] X and ||x||^2 (see
     // kernels_refine.cuh), copied to the pinned host flags.
     auto refine_side = [&](const SideCols &sc, const R *coef, const E *T, const E *x2, uint8_t *flags,
@@ -861,9 +869,9 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
             XTG_CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
             tr.run(kTPrep, 0, 0, st, [&] {
-                refine_flags_kernel<<<(nitems + 255) / 256, 256, 0, st>>>(T, x2, sc.d_ints + 4 * m, nitems, sc.d_kind,
-                                                                          coef, d_norms, opt.refine_bound, flags,
-                                                                          cnt);
+                refine_flags_kernel<<<(nitems + 7) / 8, 256, 0, st>>>(
+                    T, x2, sketch_chunks(n), m, sc.d_ints + 4 * m, nitems, sc.d_kind, coef, d_norms,
+                    opt.refine_bound, flags, cnt);
             });
             XTG_CK(cudaGetLastError());
             const size_t off = (size_t)(flags - d_flags);
@@ -1003,12 +1011,56 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
 
         // ---- residual sketch of the refinement check (split form) ------------------------------
         // [GS; GP] = G [S P] and T = [GS; GP] X with ||x_c||^2, after the substitution.
-        E *sk_G2 = nullptr, *sk_T = nullptr, *sk_x2 = nullptr;
+        E *sk_G2 = nullptr, *sk_G2p = nullptr, *sk_T = nullptr, *sk_x2 = nullptr;
+        const int sk_nch = refine::sketch_chunks(n);
         if (flags) {
             sk_G2 = scr.get<E>((size_t)n * 2 * refine::K);
-            sk_T = scr.get<E>((size_t)m * 2 * refine::K);
-            sk_x2 = scr.get<E>((size_t)m);
+            sk_G2p = scr.get<E>((size_t)sk_nch * n * 2 * refine::K);
+            sk_T = scr.get<E>((size_t)sk_nch * m * 2 * refine::K);
+            sk_x2 = scr.get<E>((size_t)sk_nch * m);
             if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
+        }
+        // [GS; GP] depends on S and P only: when all of them are on the device at this point it
+        // is computed on a second stream while the substitution runs (joined before T is
+        // formed), otherwise after the substitution.  An early return joins it before the
+        // stream-ordered scratch is released.
+        cudaStream_t sk_st = nullptr;
+        cudaEvent_t sk_ev[2] = {nullptr, nullptr};
+        bool sk_pending = false;
+        struct SketchGuard {
+            cudaStream_t &s;
+            cudaEvent_t *ev;
+            bool &pending;
+            cudaStream_t main;
+            ~SketchGuard()
+            {
+                if (pending) cudaStreamWaitEvent(main, ev[1], 0);
+                for (int i = 0; i < 2; i++)
+                    if (ev[i]) cudaEventDestroy(ev[i]);
+                if (s) cudaStreamDestroy(s);
+            }
+        } sk_guard{sk_st, sk_ev, sk_pending, st};
+        auto matrix_sketch = [&](cudaStream_t s) -> int {
+            if constexpr (!CPLX && std::is_same<R, double>::value) {
+                using namespace refine;
+                XTG_CK(cudaMemsetAsync(sk_G2p, 0, (size_t)sk_nch * n * 2 * K * sizeof(E), s));
+                tr.run(kTPrep, 0, (double)n * n * esz, s, [&] {
+                    sketch_matrix_kernel<<<dim3((n + SK_COLS - 1) / SK_COLS, sk_nch), 256, 0, s>>>(Sp, lsp, Pp, lpp,
+                                                                                                   n, sk_G2p);
+                    sum_chunks_kernel<<<4 * sm_count(), 256, 0, s>>>(sk_G2p, sk_nch, (size_t)n * 2 * K, sk_G2);
+                });
+                XTG_CK(cudaGetLastError());
+            }
+            return 0;
+        };
+        if (flags && !o.arena && !tr.on && !o.cols_ready && !o.rows_ready) {
+            XTG_CK(cudaStreamCreateWithFlags(&sk_st, cudaStreamNonBlocking));
+            for (int i = 0; i < 2; i++) XTG_CK(cudaEventCreateWithFlags(&sk_ev[i], cudaEventDisableTiming));
+            XTG_CK(cudaEventRecord(sk_ev[0], st));
+            XTG_CK(cudaStreamWaitEvent(sk_st, sk_ev[0], 0));
+            if (matrix_sketch(sk_st)) return 1;
+            XTG_CK(cudaEventRecord(sk_ev[1], sk_st));
+            sk_pending = true;
         }
         // ---- blocked substitution ----------------------------------------------------------
         // Row blocks are taken in groups of `group` adjacent blocks, rows [q0, q1), bottom to
@@ -1142,17 +1194,6 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             }
             XTG_CK(cudaGetLastError());
         }
-        if constexpr (!CPLX && std::is_same<R, double>::value) {
-            if (flags) {
-                using namespace refine;
-                tr.run(kTPrep, 0, (double)n * n * esz, st, [&] {
-                    sketch_matrix_kernel<<<n, 256, 0, st>>>(Sp, lsp, Pp, lpp, n, sk_G2);
-                });
-                tr.run(kTPrep, 0, 0.5 * (double)n * m * esz, st, [&] {
-                    sketch_columns_kernel<<<(m + 63) / 64, 256, 0, st>>>(sk_G2, X, ldx, m, d_kext, sk_T, sk_x2);
-                });
-            }
-        }
         // Look-ahead (ahead == true).  Pair p owns rows [u0_p, l1_p); the next pair's rows are
         // [a0, u0_p).  On the main stream: solve L_p, small update of U_p, solve U_p; wait for
         // the trailing update of pair p-1 (it writes rows [0, u0_p)); apply deferred guard
@@ -1277,7 +1318,23 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         // residual exceeds the bound are flagged and solved again in FP64 after the call's
         // split pass (see the end of solve_device).
         if constexpr (!CPLX && std::is_same<R, double>::value) {
-            if (flags && refine_side(sc, coef, sk_T, sk_x2, flags, st, scr)) return 1;
+            if (flags) {
+                using namespace refine;
+                if (sk_pending) {
+                    XTG_CK(cudaStreamWaitEvent(st, sk_ev[1], 0));
+                    sk_pending = false;
+                } else if (matrix_sketch(st)) {
+                    return 1;
+                }
+                XTG_CK(cudaMemsetAsync(sk_T, 0, (size_t)sk_nch * m * 2 * K * sizeof(E), st));
+                XTG_CK(cudaMemsetAsync(sk_x2, 0, (size_t)sk_nch * m * sizeof(E), st));
+                tr.run(kTPrep, 0, 0.5 * (double)n * m * esz, st, [&] {
+                    sketch_columns_kernel<<<dim3((m + SK_COLS - 1) / SK_COLS, sk_nch), 256, 0, st>>>(
+                        sk_G2, X, ldx, m, d_kext, sk_T, sk_x2);
+                });
+                XTG_CK(cudaGetLastError());
+                if (refine_side(sc, coef, sk_T, sk_x2, flags, st, scr)) return 1;
+            }
         }
 
         // ---- write-back / back-transform -----------------------------------------------------

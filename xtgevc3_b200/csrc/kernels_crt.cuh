@@ -67,6 +67,7 @@ struct Moduli {
     int p[MAXL];              // moduli, largest first
     unsigned int barrett[MAXL];  // floor(2^32 / p_l)
     double invp[MAXL];
+    double pd[MAXL];          // p_l as a double
     // W_l ~ w1_l 2^hi + w2_l 2^lo with w1_l, w2_l < 2^41 (bits below 2^lo dropped), so that
     // every r_l w_l (r_l < 256) and every partial sum of L <= 16 of them is an exact FP64 integer
     double w1[MAXL], w2[MAXL];
@@ -88,26 +89,63 @@ struct Params {
 };
 
 // ---- operand residues -------------------------------------------------------------------
-// v in (-1, 1): a = rint(v 2^t) (exact integer, |a| <= 2^t), residue a mod p_l in [-128, 127]
-// (symmetric; 128 mod 256 stored as -128).
-// Rounding and conversion through the FP64 adder (x + 1.5 2^52 has unit spacing for
-// |x| < 2^51 and keeps x's integer part, two's complement, in its low word), so the
-// per-modulus work avoids the slower conversion unit: |a / p| < 2^56 / 193 < 2^49.
-constexpr double kRoundMagic = 6755399441055744.0;  // 1.5 * 2^52
-__device__ __forceinline__ int residue(double a, int l, const Moduli &md)
+// v in (-1, 1): a = rint(v 2^t) (exact integer, |a| <= 2^t < 2^51), residue a mod p_l in
+// [-128, 127] (symmetric; 128 mod 256 stored as -128).  All rounding goes through the FP64
+// adder against R = 1.5 2^52 (where the spacing of doubles is 1 and the low word of x + R is
+// the two's complement of the integer x), so no conversion-unit instruction is needed:
+//   aR = fma(v, 2^t, R) = a + R  (rint, ties to even: R is even), a = aR - R,
+//   qR = fma(a, 1/p, R) = q + R  (q the integer nearest a / p, |a / p| < 2^43),
+//   fma(-q, p, aR) = a - q p + R (exact), whose low word is r = a - q p, |r| <= p/2 + 1.
+constexpr double kRoundMagic = 6755399441055744.0;  // R = 1.5 * 2^52
+// With q the integer nearest a fl(1/p) (|a| <= 2^50: within 2^-3 / p of a / p), |r| <= p / 2,
+// so for odd p the low byte of r is a residue in [-127, 127], for p = 256 one in [-128, 128]
+// (128 and -128 share the byte 0x80): the byte is taken as it is.
+__device__ __forceinline__ uint32_t residue_word(double a, double aR, double invp, double pd)
 {
-    const double q = __dsub_rn(__dadd_rn(__dmul_rn(a, md.invp[l]), kRoundMagic), kRoundMagic);
-    const double rr = fma(-q, (double)md.p[l], a);  // exact: the result is a small integer
-    int r = __double2loint(__dadd_rn(rr, kRoundMagic));
-    if (r > 127) r -= md.p[l];
-    if (r < -128) r += md.p[l];
-    return r;
+    const double q = __dsub_rn(fma(a, invp, kRoundMagic), kRoundMagic);
+    return (uint32_t)__double2loint(fma(-q, pd, aR));
 }
 
-// v 2^s: one multiplication by the power of two when it is a normal double, else ldexp.
-__device__ __forceinline__ double scale2(double v, int s)
+// The low bytes of four words, packed (w0 in byte 0).
+__device__ __forceinline__ uint32_t pack4(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3)
 {
-    return (s > -1000 && s < 1000) ? v * __longlong_as_double((long long)(s + 1023) << 52) : ldexp(v, s);
+    return __byte_perm(__byte_perm(w0, w1, 0x0040), __byte_perm(w2, w3, 0x0040), 0x5410);
+}
+
+// Residues of eight entries (a, a + R) for every modulus, 8 bytes per modulus at o + l stride.
+// NLC > 0: the modulus count as a compile-time constant (the moduli read at fixed offsets).
+template <int NLC>
+__device__ __forceinline__ void store_residues8(const double (&a)[8], const double (&aR)[8], const Moduli &md,
+                                                int8_t *o, size_t stride)
+{
+    auto one = [&](int l) {
+        const double invp = md.invp[l], pd = md.pd[l];
+        uint32_t w[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) w[q] = residue_word(a[q], aR[q], invp, pd);
+        *reinterpret_cast<uint2 *>(o + (size_t)l * stride) =
+            make_uint2(pack4(w[0], w[1], w[2], w[3]), pack4(w[4], w[5], w[6], w[7]));
+    };
+    if constexpr (NLC > 0) {
+#pragma unroll
+        for (int l = 0; l < NLC; l++) one(l);
+    } else {
+#pragma unroll 1
+        for (int l = 0; l < md.L; l++) one(l);
+    }
+}
+
+// a = rint(v 2^s) and a + R: one fma with the power of two when 2^s is a normal double,
+// else ldexp and rint.
+__device__ __forceinline__ void scaled_int(double v, int s, double &a, double &aR)
+{
+    if (s > -1000 && s < 1000) {
+        aR = fma(v, __longlong_as_double((long long)(s + 1023) << 52), kRoundMagic);
+        a = __dsub_rn(aR, kRoundMagic);
+    } else {
+        a = rint(ldexp(v, s));
+        aR = __dadd_rn(a, kRoundMagic);
+    }
 }
 
 // Largest |A(m, k)| of each row (through the segment description of a GEMM launch), as the
@@ -137,47 +175,36 @@ __global__ void __launch_bounds__(256) row_absmax_kernel(GemmArgs<double> g, uns
 }
 
 // Rows of A -> residues out[l][row][k] (row pitch Kp, l-th block of Mp rows), ea[row].
-// Grid: (Mp / 32, Kp / 64): one CTA per 32 rows x 64 K; a thread computes 8 consecutive K
-// of one row and stores 8 bytes per modulus.
+// Grid: (Mp / 32, Kp / 64): one CTA per 32 rows x 64 K; thread t takes row t / 8 and the 8
+// consecutive K from 8 (t % 8) (K segments are multiples of 16 long: one segment), loaded
+// straight from A (a warp's load covers 4 consecutive rows of 8 columns: whole 32-byte
+// sectors), and stores 8 bytes per modulus.
+template <int NLC>
 __global__ void __launch_bounds__(256) residue_rows_kernel(GemmArgs<double> g, int Kp, int Mp, int t, Moduli md,
                                                            const unsigned long long *rmax, int8_t *out, int *ea)
 {
-    __shared__ double tile[64][33];
-    const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 64;
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    {
-        const int row = r0 + tx;
-        for (int kk = ty; kk < 64; kk += 8) {
-            const int k = k0 + kk;
-            double v = 0.0;
-            if (k < g.K) {
-                int kb = 0;
-                const int sg = find_seg(g, k, kb);
-                const int col = k - kb;
-                if (sg >= 0 && row < g.M && col < g.seg[sg].acols)
-                    v = g.seg[sg].A[(size_t)row + (size_t)col * g.seg[sg].lda];
-            }
-            tile[kk][tx] = v;
+    const int row = blockIdx.x * 32 + (threadIdx.x >> 3);
+    const int k0 = blockIdx.y * 64 + (threadIdx.x & 7) * 8;
+    double v[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) v[q] = 0.0;
+    if (row < g.M && k0 < g.K) {
+        int kb = 0;
+        const int sg = find_seg(g, k0, kb);
+        if (sg >= 0) {
+            const int col = k0 - kb, acols = g.seg[sg].acols;
+            const double *A = g.seg[sg].A + row + (size_t)col * g.seg[sg].lda;
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                if (col + q < acols) v[q] = A[(size_t)q * g.seg[sg].lda];
         }
     }
-    __syncthreads();
-    const int rr = threadIdx.x >> 3, kg = (threadIdx.x & 7) * 8;  // row rr, K kg .. kg + 7
-    const int row = r0 + rr;
     const int e = split::scale_exp(__longlong_as_double((long long)rmax[row]));
-    if (blockIdx.y == 0 && kg == 0) ea[row] = e;
-    double a[8];
+    if (blockIdx.y == 0 && (threadIdx.x & 7) == 0) ea[row] = e;
+    double a[8], aR[8];
 #pragma unroll
-    for (int q = 0; q < 8; q++) a[q] = rint(scale2(tile[kg + q][rr], t - e));
-    int8_t *o = out + (size_t)row * Kp + k0 + kg;
-    for (int l = 0; l < md.L; l++) {
-        uint32_t w0 = 0, w1 = 0;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            w0 |= (uint32_t)(residue(a[q], l, md) & 0xff) << (8 * q);
-            w1 |= (uint32_t)(residue(a[q + 4], l, md) & 0xff) << (8 * q);
-        }
-        *reinterpret_cast<uint2 *>(o + (size_t)l * Mp * Kp) = make_uint2(w0, w1);
-    }
+    for (int q = 0; q < 8; q++) scaled_int(v[q], t - e, a[q], aR[q]);
+    store_residues8<NLC>(a, aR, md, out + (size_t)row * Kp + k0, (size_t)Mp * Kp);
 }
 
 // Eight consecutive K of column `col` of B (rows through the segment offsets; K segments are
@@ -202,6 +229,8 @@ __device__ __forceinline__ void b_values8(const GemmArgs<double> &g, int col, in
 // K 8 (t % 8) .. +7 of the block's 64).
 __global__ void __launch_bounds__(256) col_absmax_kernel(GemmArgs<double> g, unsigned long long *cmax)
 {
+    // with a per-column K extent (nondecreasing), B is zero from kext[col] on
+    if (g.kext && (int)blockIdx.y * 64 >= g.kext[min((int)blockIdx.x * 32 + 31, g.N - 1)]) return;
     const int col = blockIdx.x * 32 + (threadIdx.x >> 3);
     const int k0 = blockIdx.y * 64 + (threadIdx.x & 7) * 8;
     double v[8];
@@ -216,29 +245,27 @@ __global__ void __launch_bounds__(256) col_absmax_kernel(GemmArgs<double> g, uns
 
 // Columns of B -> residues out[l][col][k] (column pitch Kp, l-th block of Np columns),
 // eb[col].  Grid: (Np / 32, Kp / 64), the thread layout of col_absmax_kernel; a thread
-// stores 8 bytes per modulus.
-__global__ void __launch_bounds__(256) residue_cols_kernel(GemmArgs<double> g, int Kp, int Np, int t, Moduli md,
-                                                           const unsigned long long *cmax, int8_t *out, int *eb)
+// stores 8 bytes per modulus.  With a per-column K extent the GEMM reads a tile of `tnw`
+// columns up to the extent of its last column: K blocks beyond it are not written.
+template <int NLC>
+__global__ void __launch_bounds__(256) residue_cols_kernel(GemmArgs<double> g, int Kp, int Np, int tnw, int t,
+                                                           Moduli md, const unsigned long long *cmax, int8_t *out,
+                                                           int *eb)
 {
+    if (g.kext) {
+        const int last = min(((int)blockIdx.x * 32 / tnw + 1) * tnw, g.N) - 1;
+        if ((int)blockIdx.y * 64 >= g.kext[last]) return;
+    }
     const int col = blockIdx.x * 32 + (threadIdx.x >> 3);
     const int k0 = blockIdx.y * 64 + (threadIdx.x & 7) * 8;
     const int e = split::scale_exp(__longlong_as_double((long long)cmax[col]));
     if (blockIdx.y == 0 && (threadIdx.x & 7) == 0) eb[col] = e;
     double v[8];
     b_values8(g, col, k0, v);
-    double a[8];
+    double a[8], aR[8];
 #pragma unroll
-    for (int q = 0; q < 8; q++) a[q] = rint(scale2(v[q], t - e));
-    int8_t *o = out + (size_t)col * Kp + k0;
-    for (int l = 0; l < md.L; l++) {
-        uint32_t w0 = 0, w1 = 0;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            w0 |= (uint32_t)(residue(a[q], l, md) & 0xff) << (8 * q);
-            w1 |= (uint32_t)(residue(a[q + 4], l, md) & 0xff) << (8 * q);
-        }
-        *reinterpret_cast<uint2 *>(o + (size_t)l * Np * Kp) = make_uint2(w0, w1);
-    }
+    for (int q = 0; q < 8; q++) scaled_int(v[q], t - e, a[q], aR[q]);
+    store_residues8<NLC>(a, aR, md, out + (size_t)col * Kp + k0, (size_t)Np * Kp);
 }
 
 // ---- the residue GEMM ---------------------------------------------------------------------
