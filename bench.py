@@ -70,7 +70,7 @@ def parse():
     ap.add_argument("--tgexc-n", type=int, default=4096, help="order of the ztgexc reordering leg (0 skips)")
     ap.add_argument("--profile-case", default=None,
                     help="run one small case for an ncu capture and exit (no JSON line): plain:N (two dtgevc3 "
-                         "B/B calls, FP64), split_i8:N / split_crt:N (the same, INT8 digit / residue split "
+                         "B/B calls, FP64; plain_norm:N with the normalisation), split_i8:N / split_crt:N (the same, INT8 digit / residue split "
                          "form), crt_gemm:N (two N^3 residue GEMMs), batch:COUNT (two launches of the batched "
                          "dtgevc3 B/B kernel, tiles 32x32)")
     return ap.parse_args()
@@ -887,8 +887,8 @@ def profile_case(args):
         print(json.dumps({"case": args.profile_case, "fp64_flops": 2.0 * size ** 3,
                           "max_abs": float(C.abs().max())}))
         return 0
-    if kind in ("plain", "split_i8", "split_crt"):
-        flags = {"plain": 0, "split_i8": X.SPLIT | X.SPLIT_INT8 | X.slices(7),
+    if kind in ("plain", "plain_norm", "split_i8", "split_crt"):
+        flags = {"plain": 0, "plain_norm": X.NORMALIZE, "split_i8": X.SPLIT | X.SPLIT_INT8 | X.slices(7),
                  "split_crt": X.SPLIT | X.SPLIT_CRT | X.slices(14)}[kind]
         S_h, P_h, ar, ai, be = host_pencil(size, 3)
         S, P = colmajor_cuda(S_h, torch), colmajor_cuda(P_h, torch)

@@ -37,6 +37,7 @@
 //   Y[ys_off + i, c] = -ac * x_i,  Y[ys_off + yhalf + i, c] = b * x_i   (zero padded)
 // consumed by the update GEMMs  X[rows above, c] += S[rows above, I] (-ac x) + P[..] (b x).
 #pragma once
+#include <type_traits>
 #include "common.cuh"
 
 namespace xtg {
@@ -458,6 +459,93 @@ __device__ __forceinline__ void back_substitute_loop(E (&r)[2], const Factors<E>
     while (j >= jlo) j = step(j);
 }
 
+// The substitution of back_substitute_loop for the shifted operator W = ac S - b P of the
+// diagonal solves (S, P: the block in shared memory, leading dimension kSmLd; b real for a
+// real column, complex for a (Re, Im) pair), with two differences in form:
+//  * the update of the rows above a solved row j is r -= S(:, j) (ac x) - P(:, j) (b x):
+//    two FMAs per row slot against ac x and b x formed once per step, instead of forming
+//    W(i, j) for every row;
+//  * rows 32..63 (slot 1) and rows 0..31 (slot 0) are solved by separate loops, so every
+//    step reads and writes a slot fixed at compile time; the 2x2 block (31, 32), whose rows
+//    lie in different slots, is a case of its own.
+// Pivots, 2x2 LU steps, the per-row cap and the mid-block check are those of
+// back_substitute_loop (jlo = 0).
+template <class E, class B, class R, class G>
+__device__ __forceinline__ void back_substitute_sp(E (&r)[2], const Factors<E> &F, uint64_t sec, int nrows, int lane,
+                                                   const R *Ss, const R *Ps, R ac, B b, G g)
+{
+    // rows i < j of both slots: r_i -= S(i, j) u - P(i, j) v
+    auto upd1 = [&](int j, E x) {
+        const E u = ac * x, v = b * x;
+        const R *sc = Ss + j * kSmLd, *pc = Ps + j * kSmLd;
+        if (lane < j) r[0] = (r[0] - sc[lane] * u) + pc[lane] * v;
+        if (lane + 32 < j) r[1] = (r[1] - sc[lane + 32] * u) + pc[lane + 32] * v;
+    };
+    auto upd2 = [&](int p, int q, E xp, E xq) {
+        const E up = ac * xp, vp = b * xp, uq = ac * xq, vq = b * xq;
+        const R *sp = Ss + p * kSmLd, *pp = Ps + p * kSmLd, *sq = Ss + q * kSmLd, *pq = Ps + q * kSmLd;
+        if (lane < p) r[0] = ((r[0] - sp[lane] * up) - sq[lane] * uq) + (pp[lane] * vp + pq[lane] * vq);
+        if (lane + 32 < p)
+            r[1] = ((r[1] - sp[lane + 32] * up) - sq[lane + 32] * uq) + (pp[lane + 32] * vp + pq[lane + 32] * vq);
+    };
+    // one 1x1 row j held in slot SL
+    auto step1 = [&](auto slot, int j) {
+        constexpr int SL = decltype(slot)::value;
+        E x = shfl(r[SL] * F.inv1[SL], j & 31);
+        if constexpr (G::on) {
+            if (!(mag(x) <= g.cap)) x = cap_row(r, g, shfl(r[SL], j & 31), shfl(F.inv1[SL], j & 31));
+        }
+        if (lane == (j & 31)) r[SL] = x;
+        upd1(j, x);
+    };
+    // the 2x2 block (p, q = p + 1), rows in slots SP, SQ; the owner of q solves it
+    auto step2 = [&](auto sp_, auto sq_, int p) {
+        constexpr int SP = decltype(sp_)::value, SQ = decltype(sq_)::value;
+        const int q = p + 1;
+        const E rp = shfl(r[SP], p & 31);
+        const E rq = r[SQ];
+        const bool sw = F.sw[SQ];
+        const E ia = F.fa[SQ], bb = F.fb[SQ], m = F.fm[SQ], iu = F.fu[SQ];
+        const E r1 = sw ? rq : rp, r2 = sw ? rp : rq;
+        E xq = (r2 - m * r1) * iu;
+        E xp = (r1 - bb * xq) * ia;
+        xq = shfl(xq, q & 31);
+        xp = shfl(xp, q & 31);
+        if constexpr (G::on) {
+            if (!(mag(xq) <= g.cap && mag(xp) <= g.cap)) {
+                const int o = q & 31;
+                cap_pair(r, g, shfl(r1, o), shfl(r2, o), shfl(m, o), shfl(iu, o), shfl(bb, o), shfl(ia, o), xp, xq);
+            }
+        }
+        if (lane == (p & 31)) r[SP] = xp;
+        if (lane == (q & 31)) r[SQ] = xq;
+        if (p > 0) upd2(p, q, xp, xq);
+    };
+    using S0 = std::integral_constant<int, 0>;
+    using S1 = std::integral_constant<int, 1>;
+    int j = nrows - 1;
+    while (j >= kMidRow) {
+        if ((sec >> j) & 1ull) {
+            if (j == kMidRow) step2(S0(), S1(), j - 1);
+            else step2(S1(), S1(), j - 1);
+            j -= 2;
+        } else {
+            step1(S1(), j);
+            j -= 1;
+        }
+    }
+    if (nrows > kMidRow && j >= 0) g.mid(r, j);
+    while (j >= 0) {
+        if (j >= 1 && ((sec >> j) & 1ull)) {
+            step2(S0(), S0(), j - 1);
+            j -= 2;
+        } else {
+            step1(S0(), j);
+            j -= 1;
+        }
+    }
+}
+
 // bit j set: rows (j-1, j) of the block form a 2x2 block, pairing greedily from the bottom
 template <class R>
 __device__ __forceinline__ void pair_mask(const R *Ss, int jnb, uint64_t *out)
@@ -550,7 +638,8 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
                 const R mx = warp_max(lane <= jtop ? fabs(rr[0]) : R(0));
                 if (mx > a.thr_rhs) rescale(rr, a.thr_rhs / mx);
             };
-            back_substitute_loop(r, F, sec, nrows, lane, W, 0, make_guard<true>(limits<R>::big / R(4096), a.thr_rhs, mid, rescale));
+            back_substitute_sp(r, F, sec, nrows, lane, Ss, Ps, ac, br,
+                               make_guard<true>(limits<R>::big / R(4096), a.thr_rhs, mid, rescale));
             // assemble the block column (solution rows, seed, zeros below the seed)
             R x[2];
 #pragma unroll
@@ -635,7 +724,8 @@ __global__ void __launch_bounds__(256) diag_solve_real(DiagArgs<R> a)
                 const R mx = warp_max(lane <= jtop ? fmax(fabs(rr[0].x), fabs(rr[0].y)) : R(0));
                 if (mx > a.thr_rhs) rescale(rr, a.thr_rhs / mx);
             };
-            back_substitute_loop(r, F, sec, nrows, lane, W, 0, make_guard<true>(limits<R>::big / R(4096), a.thr_rhs, mid, rescale));
+            back_substitute_sp(r, F, sec, nrows, lane, Ss, Ps, ac, b,
+                               make_guard<true>(limits<R>::big / R(4096), a.thr_rhs, mid, rescale));
             C x[2];
 #pragma unroll
             for (int s = 0; s < 2; s++) {
