@@ -550,8 +550,13 @@ static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scr
     // residues in, C (read when accumulating) and out
     const double crt_bytes = (double)(g.M - g.mlo) * g.N * (L + 8.0 * (1 + g.accumulate));
     run(kTSplitCrt, 0, crt_bytes, [&] {
-        crt_kernel<<<dim3((g.M + 1023) / 1024, g.N), 256, 0, st>>>(cb.U, Mp, Np, md, t, cb.ea, cb.eb, g.M, g.N, g.mlo,
-                                                                g.C, g.ldc, g.ccol, g.accumulate);
+        const dim3 grid((g.M + 1023) / 1024, g.N);
+        if (L == 14)
+            crt_kernel<14><<<grid, 256, 0, st>>>(cb.U, Mp, Np, md, t, cb.ea, cb.eb, g.M, g.N, g.mlo, g.C, g.ldc, g.ccol,
+                                                 g.accumulate);
+        else
+            crt_kernel<0><<<grid, 256, 0, st>>>(cb.U, Mp, Np, md, t, cb.ea, cb.eb, g.M, g.N, g.mlo, g.C, g.ldc, g.ccol,
+                                                g.accumulate);
     });
     return cudaGetLastError();
 }

@@ -444,20 +444,26 @@ gemm_crt_kernel(const __grid_constant__ CUtensorMap tmR, const __grid_constant__
 // One thread per 4 consecutive rows of one column (grid: (Mp / 1024, N), 256 threads): the
 // 4 residues of each modulus come in one 32-bit load (a warp reads 128 contiguous bytes per
 // modulus), all L loads in flight before the arithmetic; C' of each element from its
-// residues, scaled into C.
+// residues, scaled into C.  A residue byte u becomes a double as (2^52 + u) - 2^52, the
+// byte placed in the low word of 2^52 (an FP64 add instead of a conversion instruction).
+// NLC > 0: the modulus count as a compile-time constant.
+template <int NLC>
 __global__ void __launch_bounds__(256) crt_kernel(const unsigned char *U, int Mp, int Np, Moduli md, int t,
                                                   const int *ea, const int *eb, int M, int N, int mlo, double *C,
                                                   int ldc, const int *ccol, int accumulate)
 {
+    constexpr int LMAX = NLC > 0 ? NLC : MAXL;
+    const int L = NLC > 0 ? NLC : md.L;
     const int row0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
     const int col = blockIdx.y;
     if (row0 >= M || col >= N) return;
     const size_t plane = (size_t)Np * Mp;
     const uint32_t *u = reinterpret_cast<const uint32_t *>(U + (size_t)col * Mp + row0);  // Mp % 128 == 0
-    uint32_t w[MAXL];
+    uint32_t w[LMAX];
 #pragma unroll
-    for (int l = 0; l < MAXL; l++) w[l] = l < md.L ? u[(size_t)l * plane / 4] : 0u;
+    for (int l = 0; l < LMAX; l++) w[l] = l < L ? u[(size_t)l * plane / 4] : 0u;
     const double two_hi = ldexp(1.0, md.hi), two_lo = ldexp(1.0, md.lo);
+    constexpr double two52 = 4503599627370496.0;
     const int ecol = eb[col] - 2 * t;
     double *ccolp = C + (size_t)(ccol ? ccol[col] : col) * ldc;
 #pragma unroll
@@ -466,8 +472,8 @@ __global__ void __launch_bounds__(256) crt_kernel(const unsigned char *U, int Mp
         if (row < mlo || row >= M) continue;
         double H = 0.0, Mid = 0.0;
 #pragma unroll
-        for (int l = 0; l < MAXL; l++) {
-            const double ul = (double)((w[l] >> (8 * q)) & 0xffu);
+        for (int l = 0; l < LMAX; l++) {
+            const double ul = __dsub_rn(__hiloint2double(0x43300000, (int)__byte_perm(w[l], 0u, 0x4440 + q)), two52);
             H = fma(ul, md.w1[l], H);
             Mid = fma(ul, md.w2[l], Mid);
         }
