@@ -1063,6 +1063,9 @@ def main():
     if tinfo and key in tinfo.get("bytes_per_flop", {}) and kd["flops"] > 0:
         traffic = tinfo["bytes_per_flop"][key] * kd["flops"] / kd["launches"]
         roof["traffic_note"] = tinfo.get("note", "")
+    elif tinfo and key in tinfo.get("bytes_per_algorithmic_byte", {}) and kd["bytes"] > 0:
+        traffic = tinfo["bytes_per_algorithmic_byte"][key] * kd["bytes"] / kd["launches"]
+        roof["traffic_note"] = tinfo.get("note_bytes", "")
     roof["traffic"] = traffic
     roof["algorithmic_per_launch"] = (kd["flops"] if kd["flops"] > 0 else kd["bytes"]) / kd["launches"]
     for k in kernels.values():

@@ -539,13 +539,16 @@ static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scr
         p.p[l] = md.p[l];
         p.barrett[l] = md.barrett[l];
     }
+    // residue bytes: both operands read once, one byte per output entry and modulus written
+    const double gemm_bytes = (double)L * ((double)Mp * Kp + (double)Np * Kp + (double)Mp * Np);
     if (pairs) {
         const int grid = std::min(crt_pair_grid(), 2 * p.items);  // persistent pairs of CTAs
-        run(kTSplitGemm, flops, 0,
+        run(kTSplitGemm, flops, gemm_bytes,
             [&] { crt2::gemm_crt2_kernel<<<grid, THREADS, crt2::SMEM_BYTES, st>>>(tmA, tmB, p); });
     } else {
         const int grid = std::min(sm_count(), p.items);  // persistent: one CTA per SM
-        run(kTSplitGemm, flops, 0, [&] { gemm_crt_kernel<<<grid, THREADS, SMEM_BYTES, st>>>(tmA, tmB, p); });
+        run(kTSplitGemm, flops, gemm_bytes,
+            [&] { gemm_crt_kernel<<<grid, THREADS, SMEM_BYTES, st>>>(tmA, tmB, p); });
     }
     // residues in, C (read when accumulating) and out
     const double crt_bytes = (double)(g.M - g.mlo) * g.N * (L + 8.0 * (1 + g.accumulate));
