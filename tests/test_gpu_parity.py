@@ -486,3 +486,38 @@ def test_normalize_one_pass_kernel_sizes(cuda_ok, n):
             assert abs(mx - 1.0) < 1e-14, (side, c, mx)
             s = float((a0.abs().sum(1).max()) if pair else a0.abs().max())
             assert float((a0 / s - a1).abs().max()) < 1e-15 * 4, (side, c)
+
+
+@pytest.mark.parametrize("case", ["gges_B", "gges_sel_L", "guards_A"])
+def test_tensor_core_solves_match_warp_solves(cuda_ok, monkeypatch, case):
+    """XTGEVC3_DIAG_TC=1 runs the real double diagonal solves with their in-block updates on
+    the FP64 tensor cores (eight columns of a warp share each sub-block's row updates as
+    m8n8k4 MMAs) instead of the default one-eigenvector-per-warp kernel.  Both must give the
+    same eigenvectors to rounding
+    (column max difference 1e-12 after normalisation): an xGGES pencil with Q, Z, both
+    sides; a selection, left side; and a random triangular pencil whose columns the growth
+    guards rescale (n = 2048, HOWMNY 'A')."""
+    if case == "guards_A":
+        n = 2048
+        S, P, al, ai, be = pencils.gen_quasi_triangular(n, 8213)
+        Q = Z = np.eye(n, order="F")
+        side, howmny, sel = "B", "A", None
+    else:
+        n = 700
+        S, P, al, ai, be, Q, Z = pencils.gen_gges(n, 77)
+        side, howmny = ("B", "B") if case == "gges_B" else ("L", "S")
+        sel = (np.random.default_rng(5).random(n) < 0.35).astype(np.int32) if howmny == "S" else None
+    out = {}
+    for simt in ("0", "1"):
+        monkeypatch.setenv("XTGEVC3_DIAG_TC", "0" if simt == "1" else "1")
+        out[simt] = X.tgevc3(side, howmny, S, P, al, be, alphai=ai, VL=Q.copy(order="F"), VR=Z.copy(order="F"),
+                             select=sel)
+    (VL, VR, m, info), (VLs, VRs, ms, infos) = out["0"], out["1"]
+    assert (m, info) == (ms, infos)
+    d = dict(alphai=ai, howmny=howmny, select=sel)
+    for sd, A, B in (("L", VL, VLs), ("R", VR, VRs)):
+        if side not in (sd, "B"):
+            continue
+        assert np.isfinite(A[:, :m]).all()
+        err, _ = oracle.max_rel_diff(as_complex(A[:, :m], d), as_complex(B[:, :m], d))
+        assert err < 1e-12, (sd, err)

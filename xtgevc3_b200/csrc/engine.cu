@@ -19,6 +19,7 @@
 // written back with zeros elsewhere.
 #include "engine.cuh"
 #include "kernels_diag.cuh"
+#include "kernels_diag_tc.cuh"
 #include "kernels_gemm.cuh"
 #include "kernels_misc.cuh"
 #include "kernels_split.cuh"
@@ -175,6 +176,8 @@ void configure_device(int dev)
                              2 * kBlock * kSmLd * (int)sizeof(float));
         cudaFuncSetAttribute(diag_solve_cplx<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              2 * kBlock * kSmLd * (int)sizeof(cplx<double>));
+        cudaFuncSetAttribute(dtc::diag_solve_real_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)dtc::kSmemBytes);
         cudaFuncSetAttribute(diag_solve_cplx<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              2 * kBlock * kSmLd * (int)sizeof(cplx<float>));
         cudaFuncSetAttribute(gemm_dmma<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmma::Tile<128>::SMEM_BYTES);
@@ -779,6 +782,17 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
     const R bignum = R(1) / (safemin / eps);
     const int ld_n = round_up(n, 32);
 
+    // Real double solves with their in-block updates on the FP64 tensor cores
+    // (kernels_diag_tc.cuh) with XTGEVC3_DIAG_TC=1, outside arena mode (fixed scratch).  Off
+    // by default: the solves are bound by each launch's latency (one eigenvector's chain of
+    // 64 dependent row steps), and the eight-column form's per-warp chain is longer (n = 8192
+    // B/B: 14.4 ms per call against 9.5 ms for the one-eigenvector-per-warp kernel).
+    bool diag_tc = false;
+    if constexpr (!CPLX && std::is_same<R, double>::value) {
+        const char *v = std::getenv("XTGEVC3_DIAG_TC");
+        diag_tc = !opt.arena && v && v[0] == '1';
+    }
+
     // ---- column lists of each side (problem orientation) and their device copies ------------
     // Both sides' lists go to the device on the call's stream before either side starts, so
     // that every host-to-device copy of the call's own is queued before `opt.staged` runs.
@@ -787,6 +801,11 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         std::vector<int> starts;  // columns that start an eigenvector (diagonal-solve items)
         const int *d_ints = nullptr;  // colk, src, kext, outcol, starts: m ints each
         const uint8_t *d_kind = nullptr;
+        // slots of the tensor-core diagonal solves: a pair's two columns, or up to two
+        // consecutive real columns; slot_k: eigenvalue index of each slot's last column
+        std::vector<int> slot_k;
+        const int2 *d_slots = nullptr;
+        int nslots = 0;
     };
     // keep_k (optional): only the eigenvalues k with keep_k[k] set (their output columns kept)
     auto build_cols = [&](bool left, SideCols &sc, const std::vector<char> *keep_k = nullptr) -> int {
@@ -822,9 +841,30 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         sc.starts.reserve(m);
         for (int q = 0; q < m; q++)
             if (L.kind[q] != kPairIm) sc.starts.push_back(q);
+        std::vector<int2> slots;
+        for (int q = 0; q < m;) {
+            if (L.kind[q] == kPairRe) {
+                slots.push_back(make_int2(q, q + 1));
+                sc.slot_k.push_back(L.colk[q + 1]);
+                q += 2;
+            } else if (q + 1 < m && L.kind[q + 1] == kReal) {
+                slots.push_back(make_int2(q, q + 1));
+                sc.slot_k.push_back(L.colk[q + 1]);
+                q += 2;
+            } else {
+                slots.push_back(make_int2(q, -1));
+                sc.slot_k.push_back(L.colk[q]);
+                q += 1;
+            }
+        }
+        sc.nslots = (int)slots.size();
         int *d_ints = scr.get<int>(5 * (size_t)m);
         uint8_t *d_kind = scr.get<uint8_t>((size_t)m);
+        int2 *d_slots = diag_tc ? scr.get<int2>(std::max<size_t>(1, slots.size())) : nullptr;
         if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
+        if (d_slots && !slots.empty())
+            XTG_CK(cudaMemcpyAsync(d_slots, slots.data(), slots.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+        sc.d_slots = d_slots;
         std::vector<int> ints(5 * (size_t)m, 0);
         std::copy(L.colk.begin(), L.colk.end(), ints.begin());
         std::copy(L.src.begin(), L.src.end(), ints.begin() + m);
@@ -1169,8 +1209,23 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
                 dby += cols * (double(nr < jnb ? 0 : jnb) + jnb + 2.0 * bpad) * esz;
             }
             tr.run(kTDiag, dfl, dby, st, [&] {
-                if constexpr (CPLX) diag_solve_cplx<R><<<grid, diag_threads, diag_smem, st>>>(da);
-                else diag_solve_real<R><<<grid, diag_threads, diag_smem, st>>>(da);
+                if constexpr (CPLX) {
+                    diag_solve_cplx<R><<<grid, diag_threads, diag_smem, st>>>(da);
+                } else if constexpr (std::is_same<R, double>::value) {
+                    if (diag_tc) {
+                        // first slot with an active column (slots in column order, k ascending)
+                        const int s0 = int(std::lower_bound(sc.slot_k.begin(), sc.slot_k.end(), r0) -
+                                           sc.slot_k.begin());
+                        const int per = dtc::kWarps * dtc::kSlots;
+                        const int tgrid = std::max(1, (sc.nslots - s0 + per - 1) / per);
+                        dtc::diag_solve_real_tc<<<tgrid, dtc::kThreads, dtc::kSmemBytes, st>>>(da, sc.d_slots, s0,
+                                                                                               sc.nslots);
+                    } else {
+                        diag_solve_real<R><<<grid, diag_threads, diag_smem, st>>>(da);
+                    }
+                } else {
+                    diag_solve_real<R><<<grid, diag_threads, diag_smem, st>>>(da);
+                }
             });
         };
         const int nbk = (int)blocks.size();
