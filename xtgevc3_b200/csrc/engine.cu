@@ -455,6 +455,19 @@ static int sm_count()
 // The residue GEMM runs on one CTA per SM (kernels_crt.cuh); XTGEVC3_CRT_PAIR=1 selects the
 // SM-pair kernel (kernels_crt2.cuh: a third less operand traffic per SM, measured slower on
 // this solver's shapes).  Pairs resident at once come from the occupancy API (cached per device).
+// Row blocks per group of the split forms' blocked substitution (one trailing GEMM per
+// group, K = 2 x the group's rows); XTGEVC3_SPLIT_GROUP (1..32) overrides the default for
+// tuning, read once per process.
+static int split_group_blocks()
+{
+    static const int g = [] {
+        const char *v = std::getenv("XTGEVC3_SPLIT_GROUP");
+        const int x = v ? std::atoi(v) : 0;
+        return (x >= 1 && x <= 32) ? x : kGroupBlocksSplit;
+    }();
+    return g;
+}
+
 static bool crt_pairs()
 {
     static const bool on = [] {
@@ -1027,7 +1040,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         // Without look-ahead, row blocks are taken in groups of `group` (one trailing GEMM
         // with K = 2 x the group's rows); arena mode keeps groups of two, so that its fixed
         // scratch holds the update operand.  Look-ahead takes pairs with padded blocks.
-        const int group = o.arena ? 2 : (nsplit_side ? kGroupBlocksSplit : kGroupBlocks);
+        const int group = o.arena ? 2 : (nsplit_side ? split_group_blocks() : kGroupBlocks);
         const int ldx = ld_n;
         const int ldy = ahead ? 4 * kBlock : 2 * round_up(group * kBlock, kKPad);  // both halves
         E *X = scr.get<E>((size_t)ldx * m);
