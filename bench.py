@@ -1119,8 +1119,8 @@ def main():
     e2e = {"value": world * 2 * n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": (2 * trap + 2 * n * n) * 8,
            "d2h_bytes_per_step": 2 * n * n * 8, "ms_per_step": 1e3 * e2e_s,
            "path": f"xtgevc3_dtgevc3 (host pointers, pinned), {head} form, H2D/D2H inside the call (S, P "
-                   f"in pieces while the solve runs, norms from host threads; Q, Z and the result columns "
-                   f"overlapped with it)"}
+                   f"in pieces while the solve runs, norms from host threads; Q, Z in row panels, each "
+                   f"side's back-transform and download following them panel by panel)"}
 
     norm = measure_normalize(args, X, torch, data, peak_hbm) if rank == 0 else None
     batched = measure_batched(args, X, torch, dist, world) if args.batch_count > 0 else None

@@ -521,3 +521,38 @@ def test_tensor_core_solves_match_warp_solves(cuda_ok, monkeypatch, case):
         assert np.isfinite(A[:, :m]).all()
         err, _ = oracle.max_rel_diff(as_complex(A[:, :m], d), as_complex(B[:, :m], d))
         assert err < 1e-12, (sd, err)
+
+
+@pytest.mark.parametrize("form", ["plain", "crt"])
+def test_host_row_panels_match_device_api(cuda_ok, form):
+    """From n = 4096 the host-pointer form uploads Q and Z in row panels (two here) and runs
+    each side's back-transform panel by panel as its rows arrive (V rows = Z rows X),
+    downloading every panel's rows at once; every column must equal the device form's (one
+    back-transform over all rows), bit for bit, in the FP64 form and in the residue form."""
+    import torch
+    n = 4096
+    p = _pencil("schur", n, 9, np.float64)
+    g = torch.Generator(device="cuda").manual_seed(13)
+    Qd = torch.linalg.qr(torch.randn(n, n, device="cuda", dtype=torch.float64, generator=g))[0]
+    Zd = torch.linalg.qr(torch.randn(n, n, device="cuda", dtype=torch.float64, generator=g))[0]
+    Q, Z = np.asfortranarray(Qd.cpu().numpy()), np.asfortranarray(Zd.cpu().numpy())
+    flags = X.SPLIT | X.SPLIT_CRT if form == "crt" else 0
+    X.set_flags(flags)
+    try:
+        VLh, VRh, m, info = X.tgevc3("B", "B", p["S"], p["P"], p["alpha"], p["beta"], alphai=p["alphai"],
+                                     VL=Q.copy(order="F"), VR=Z.copy(order="F"))
+    finally:
+        X.set_flags(0)
+    assert (m, info) == (n, 0)
+
+    def dev(a):  # column-major device tensor
+        return torch.from_numpy(np.ascontiguousarray(a.T)).cuda().t()
+
+    VL, VR = dev(Q), dev(Z)
+    m2, info2 = X.tgevc3_dev("B", "B", dev(p["S"]), dev(p["P"]), p["alpha"], p["beta"], alphai=p["alphai"],
+                             VL=VL, VR=VR, flags=flags)
+    torch.cuda.synchronize()
+    assert (m2, info2) == (m, info)
+    assert np.isfinite(VLh[:, :m]).all() and np.isfinite(VRh[:, :m]).all()
+    np.testing.assert_array_equal(VL.t().cpu().numpy().T, VLh[:, :m])
+    np.testing.assert_array_equal(VR.t().cpu().numpy().T, VRh[:, :m])

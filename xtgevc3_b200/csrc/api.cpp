@@ -168,6 +168,7 @@ int run_host(char side, char howmny, const int *select, int n, const void *S, in
         cudaStream_t st = nullptr, sin = nullptr, sout = nullptr;
         cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // Z ready, Q ready, right done, left done
         std::vector<cudaEvent_t> pev;  // piece k of S and P on the device (real types)
+        std::vector<cudaEvent_t> zev, qev;  // row panel k of Z / Q on the device (HOWMNY='B')
         void *dS = nullptr, *dP = nullptr, *dVL = nullptr, *dVR = nullptr;
         ~Res()
         {
@@ -178,8 +179,9 @@ int run_host(char side, char howmny, const int *select, int n, const void *S, in
                 if (p) cudaFree(p);
             for (cudaEvent_t e : ev)
                 if (e) cudaEventDestroy(e);
-            for (cudaEvent_t e : pev)
-                if (e) cudaEventDestroy(e);
+            for (auto *v : {&pev, &zev, &qev})
+                for (cudaEvent_t e : *v)
+                    if (e) cudaEventDestroy(e);
             for (cudaStream_t q : {st, sin, sout})
                 if (q) cudaStreamDestroy(q);
         }
@@ -246,6 +248,21 @@ int run_host(char side, char howmny, const int *select, int n, const void *S, in
         for (cudaEvent_t &ev : r.pev)
             if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
     }
+    // Row panels of Z and Q (HOWMNY='B'): uploaded alternately behind S and P; the
+    // back-transform of a side follows its panels, and each panel's rows of the result go
+    // down at once (without normalisation, which needs whole columns).
+    std::vector<int> qz_end;  // end row of panel k
+    if (back) {
+        // panel boundaries at multiples of 64 rows (the GEMM operands stay aligned)
+        const int np = std::max(1, std::min(4, n / 2048));
+        for (int k = 1; k < np; k++) qz_end.push_back((int)((long long)n * k / np) / 64 * 64);
+        qz_end.push_back(n);
+        r.zev.assign(np, nullptr);
+        r.qev.assign(np, nullptr);
+        for (auto *v : {&r.zev, &r.qev})
+            for (cudaEvent_t &ev : *v)
+                if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+    }
     xtg::Options opt = make_opts(flags);
     if (!P) {  // xTREVC3 conventions
         opt.p_identity = 1;
@@ -299,13 +316,21 @@ int run_host(char side, char howmny, const int *select, int n, const void *S, in
                 if (x != cudaSuccess) in_err = x;
                 return;
             }
-            if (x == cudaSuccess && want_r)
-                x = cudaMemcpy2DAsync(r.dVR, ld * sizeof(E), VR, (size_t)ldvr * sizeof(E), (size_t)n * sizeof(E), n,
-                                      cudaMemcpyHostToDevice, r.sin);
+            // row panels of Z and Q, alternately; ev[0] / ev[1]: all of Z / Q
+            for (size_t k = 0; k < qz_end.size() && x == cudaSuccess; k++) {
+                const int r0 = k ? qz_end[k - 1] : 0, r1 = qz_end[k];
+                for (int s = 0; s < 2 && x == cudaSuccess; s++) {
+                    const bool lq = s == 1;
+                    if (!(lq ? want_l : want_r)) continue;
+                    E *dv = static_cast<E *>(lq ? r.dVL : r.dVR);
+                    const E *hv = static_cast<const E *>(lq ? VL : VR);
+                    const int ldh = lq ? ldvl : ldvr;
+                    x = cudaMemcpy2DAsync(dv + r0, ld * sizeof(E), hv + r0, (size_t)ldh * sizeof(E),
+                                          (size_t)(r1 - r0) * sizeof(E), n, cudaMemcpyHostToDevice, r.sin);
+                    if (x == cudaSuccess) x = cudaEventRecord((lq ? r.qev : r.zev)[k], r.sin);
+                }
+            }
             if (x == cudaSuccess && want_r) x = cudaEventRecord(r.ev[0], r.sin);
-            if (x == cudaSuccess && want_l)
-                x = cudaMemcpy2DAsync(r.dVL, ld * sizeof(E), VL, (size_t)ldvl * sizeof(E), (size_t)n * sizeof(E), n,
-                                      cudaMemcpyHostToDevice, r.sin);
             if (x == cudaSuccess && want_l) x = cudaEventRecord(r.ev[1], r.sin);
             if (x != cudaSuccess) in_err = x;
         };
@@ -329,7 +354,32 @@ int run_host(char side, char howmny, const int *select, int n, const void *S, in
         download(left, sst, o0, o1);
         chunked.push_back({left, o1 - o0});
     };
+    // rows [r0, r1) of every output column of one side, once its stream reaches this point
+    int rows_down[2] = {0, 0};
+    if (back && !qz_end.empty()) {
+        opt.back_rows_ready = [&](bool left, int rows, cudaStream_t q) -> int {
+            size_t k = 0;
+            while (k + 1 < qz_end.size() && qz_end[k] < rows) k++;
+            cudaError_t x = cudaStreamWaitEvent(q, (left ? r.qev : r.zev)[k], 0);
+            if (x != cudaSuccess) in_err = x;
+            return qz_end[k];
+        };
+        opt.rows_done = [&](bool left, cudaStream_t sst, int r0, int r1) {
+            cudaEvent_t ev = r.ev[left ? 3 : 2];
+            E *hv = static_cast<E *>(left ? VL : VR);
+            const int ldh = left ? ldvl : ldvr;
+            const E *dv = static_cast<const E *>(left ? r.dVL : r.dVR);
+            cudaError_t x = cudaEventRecord(ev, sst);
+            if (x == cudaSuccess) x = cudaStreamWaitEvent(r.sout, ev, 0);
+            if (x == cudaSuccess && r1 > r0 && count > 0)
+                x = cudaMemcpy2DAsync(hv + r0, (size_t)ldh * sizeof(E), dv + r0, ld * sizeof(E),
+                                      (size_t)(r1 - r0) * sizeof(E), count, cudaMemcpyDeviceToHost, r.sout);
+            if (x != cudaSuccess) out_err = x;
+            rows_down[left ? 1 : 0] += r1 - r0;
+        };
+    }
     opt.side_done = [&](bool left, cudaStream_t sst) {
+        if (rows_down[left ? 1 : 0] >= n) return;  // every row went down with its panel
         int done = 0;
         for (auto &c : chunked)
             if (c.first == left) done += c.second;

@@ -1418,7 +1418,49 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         if (const int g = gate()) return g;
         E *V = left ? VL : VR;
         const int ldv = left ? ldvl : ldvr;
-        if (do_back) {
+        // row panels: Z / Q arrive by rows (host-pointer path); each panel's rows of V are
+        // computed as soon as its rows of Z / Q are up (V rows = Z rows X)
+        const bool rpanels = do_back && o.back_rows_ready && o.rows_done && !o.normalize && !zc_in;
+        if (rpanels) {
+            E *Zc = scr.get<E>((size_t)ld_n * n);
+            if (scr.err) { set_last_error(cudaGetErrorString(scr.err)); return 1; }
+            if (zc_keep) *zc_keep = Zc;
+            double bk = 0;
+            for (int c = 0; c < m; c++) bk += L.kext[c];
+            for (int r0 = 0; r0 < n;) {
+                const int r1 = std::min(n, std::max(r0 + 1, o.back_rows_ready(left, r0 + 1, st)));
+                const int rows = r1 - r0;
+                if (left) {  // rows [r0, r1) of the column-reversed Q
+                    dim3 g((rows + 255) / 256, n);
+                    tr.run(kTPrep, 0, 2.0 * rows * n * esz, st, [&] {
+                        rev_columns_kernel<E><<<g, 256, 0, st>>>(V + r0, ldv, Zc + r0, ld_n, rows, n);
+                    });
+                } else {
+                    XTG_CK(cudaMemcpy2DAsync(Zc + r0, (size_t)ld_n * sizeof(E), V + r0, (size_t)ldv * sizeof(E),
+                                             (size_t)rows * sizeof(E), n, cudaMemcpyDeviceToDevice, st));
+                }
+                GemmArgs<E> g;
+                g.M = rows;
+                g.N = m;
+                g.mlo = 0;
+                g.nseg = 1;
+                g.seg[0] = strip(Zc, ld_n, r0, 0, n, 0);
+                g.K = g.seg[0].K;
+                g.B = X;
+                g.ldb = ldx;
+                g.brows = n;
+                g.C = V + r0;
+                g.ldc = ldv;
+                g.ccol = d_outcol;
+                g.kext = d_kext;
+                g.accumulate = 0;
+                const double bf = 2.0 * rows * bk * cfl;
+                const double bb = ((double)rows * n + bk + (double)rows * m) * esz;
+                gemm(g, st, kTBack, bf, bb);
+                o.rows_done(left, st, r0, r1);
+                r0 = r1;
+            }
+        } else if (do_back) {
             if (o.back_ready[left ? 1 : 0]) XTG_CK(cudaStreamWaitEvent(st, o.back_ready[left ? 1 : 0], 0));
             // copy of Z (right) or column-reversed Q (left), so V can be overwritten; a later
             // pass of the same call (the refinement) reuses it
@@ -1582,6 +1624,8 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         ro.side_done = nullptr;
         ro.cols_done = nullptr;
         ro.back_ready[0] = ro.back_ready[1] = nullptr;
+        ro.back_rows_ready = nullptr;
+        ro.rows_done = nullptr;
         for (int sd = 0; sd < 2; sd++) {
             if (!(sd ? want_l : want_r)) continue;
             const SideCols &sc = side_cols[sd];

@@ -64,6 +64,13 @@ struct Options {
     // HOWMNY='B' without normalisation: the back-transform runs in column chunks and this
     // is called after each with the output columns [o0, o1) it completed.
     std::function<void(bool left, cudaStream_t st, int o0, int o1)> cols_done;
+    // Host-pointer path, HOWMNY='B' without normalisation, when set: Z / Q reach the device
+    // in row panels and the back-transform follows them.  back_rows_ready(left, r, st) makes
+    // st wait until rows [0, r) of the side's Z / Q are on the device and returns the number
+    // of leading rows that are (>= r); each panel's rows of every output column are then
+    // computed (V rows = Z rows X) and rows_done(left, st, r0, r1) is called with them.
+    std::function<int(bool left, int rows, cudaStream_t st)> back_rows_ready;
+    std::function<void(bool left, cudaStream_t st, int r0, int r1)> rows_done;
 };
 
 // Device scratch (bytes) a call needs in arena mode: shared eigenvalue data plus the larger
