@@ -194,7 +194,14 @@ int run_host(char side, char howmny, const int *select, int n, const void *S, in
     HostNorms<R> hn;                 // its threads read only the caller's S and P
     if constexpr (kPanels) hn.start(static_cast<const R *>(S), lds, static_cast<const R *>(P), ldp, n);
     cudaError_t e;
-    for (cudaStream_t *q : {&r.st, &r.sin, &r.sout})
+    // The call's stream (the right side's kernels) at the highest priority: with both sides
+    // requested, the right side finishes first and its result goes down while the left side
+    // (on a pooled side stream at the default priority) still computes.
+    int prio_lo = 0, prio_hi = 0;
+    if ((e = cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi)) != cudaSuccess) return fail(e, "stream priorities");
+    if ((e = cudaStreamCreateWithPriority(&r.st, cudaStreamNonBlocking, prio_hi)) != cudaSuccess)
+        return fail(e, "stream");
+    for (cudaStream_t *q : {&r.sin, &r.sout})
         if ((e = cudaStreamCreateWithFlags(q, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
     for (cudaEvent_t &ev : r.ev)
         if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
@@ -316,12 +323,13 @@ int run_host(char side, char howmny, const int *select, int n, const void *S, in
                 if (x != cudaSuccess) in_err = x;
                 return;
             }
-            // row panels of Z and Q, alternately; ev[0] / ev[1]: all of Z / Q
-            for (size_t k = 0; k < qz_end.size() && x == cudaSuccess; k++) {
-                const int r0 = k ? qz_end[k - 1] : 0, r1 = qz_end[k];
-                for (int s = 0; s < 2 && x == cudaSuccess; s++) {
-                    const bool lq = s == 1;
-                    if (!(lq ? want_l : want_r)) continue;
+            // row panels of Z, then of Q (the right side, first to finish, needs Z first);
+            // ev[0] / ev[1]: all of Z / Q
+            for (int s = 0; s < 2 && x == cudaSuccess; s++) {
+                const bool lq = s == 1;
+                if (!(lq ? want_l : want_r)) continue;
+                for (size_t k = 0; k < qz_end.size() && x == cudaSuccess; k++) {
+                    const int r0 = k ? qz_end[k - 1] : 0, r1 = qz_end[k];
                     E *dv = static_cast<E *>(lq ? r.dVL : r.dVR);
                     const E *hv = static_cast<const E *>(lq ? VL : VR);
                     const int ldh = lq ? ldvl : ldvr;
