@@ -441,6 +441,9 @@ struct CrtBufs {
     int *ea = nullptr, *eb = nullptr;
     unsigned long long *rmax = nullptr;
     size_t acap = 0, bcap = 0, ucap = 0, eacap = 0, ebcap = 0, rcap = 0;
+    // what B and eb hold: the operand and shape of the launch that wrote them
+    const void *b_src = nullptr;
+    int b_Kp = 0, b_Np = 0, b_L = 0, b_t = 0;
 };
 
 static int sm_count()
@@ -510,10 +513,10 @@ static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scr
     const int t = crt_bits(L, g.K);
     const size_t an = (size_t)L * Mp * Kp, bn = (size_t)L * Np * Kp, un = (size_t)L * Np * Mp;
     if (an > cb.acap) { cb.A = scr.get<int8_t>(an); cb.acap = an; }
-    if (bn > cb.bcap) { cb.B = scr.get<int8_t>(bn); cb.bcap = bn; }
+    if (bn > cb.bcap) { cb.B = scr.get<int8_t>(bn); cb.bcap = bn; cb.b_src = nullptr; }
     if (un > cb.ucap) { cb.U = scr.get<unsigned char>(un); cb.ucap = un; }
     if ((size_t)Mp > cb.eacap) { cb.ea = scr.get<int>(Mp); cb.eacap = Mp; }
-    if ((size_t)Np > cb.ebcap) { cb.eb = scr.get<int>(Np); cb.ebcap = Np; }
+    if ((size_t)Np > cb.ebcap) { cb.eb = scr.get<int>(Np); cb.ebcap = Np; cb.b_src = nullptr; }
     if ((size_t)(Mp + Np) > cb.rcap) { cb.rmax = scr.get<unsigned long long>(Mp + Np); cb.rcap = Mp + Np; }
     if (scr.err) return scr.err;
     unsigned long long *cmax = cb.rmax + Mp;
@@ -521,19 +524,28 @@ static cudaError_t launch_crt(const GemmArgs<double> &g, int L, CrtBufs &cb, Scr
     if (e != cudaSuccess) return e;
     // operand bytes: A and B read twice (maximum, residues), L residue bytes written per entry
     const double slice_bytes = ((double)g.M + g.N) * g.K * (2.0 * 8 + L);
+    // B's residues stay valid across the row panels of one back-transform (same B, shape and
+    // bits): only the first panel computes them
+    const bool keep_b = g.reuse_b && cb.b_src == (const void *)g.B && cb.b_Kp == Kp && cb.b_Np == Np &&
+                        cb.b_L == L && cb.b_t == t;
     run(kTSplitPrep, 0, slice_bytes, [&] {
         row_absmax_kernel<<<dim3(Mp / 32, (g.K + 255) / 256), 256, 0, st>>>(g, cb.rmax);
-        col_absmax_kernel<<<dim3(Np / 32, Kp / 64), 256, 0, st>>>(g, cmax);
+        if (!keep_b) col_absmax_kernel<<<dim3(Np / 32, Kp / 64), 256, 0, st>>>(g, cmax);
         const dim3 gr(Mp / 32, Kp / 64), gc(Np / 32, Kp / 64);
         const int tnw = pairs ? crt2::TNP : TN;
         if (L == 14) {  // the default modulus count: moduli at fixed offsets
             residue_rows_kernel<14><<<gr, 256, 0, st>>>(g, Kp, Mp, t, md, cb.rmax, cb.A, cb.ea);
-            residue_cols_kernel<14><<<gc, 256, 0, st>>>(g, Kp, Np, tnw, t, md, cmax, cb.B, cb.eb);
+            if (!keep_b) residue_cols_kernel<14><<<gc, 256, 0, st>>>(g, Kp, Np, tnw, t, md, cmax, cb.B, cb.eb);
         } else {
             residue_rows_kernel<0><<<gr, 256, 0, st>>>(g, Kp, Mp, t, md, cb.rmax, cb.A, cb.ea);
-            residue_cols_kernel<0><<<gc, 256, 0, st>>>(g, Kp, Np, tnw, t, md, cmax, cb.B, cb.eb);
+            if (!keep_b) residue_cols_kernel<0><<<gc, 256, 0, st>>>(g, Kp, Np, tnw, t, md, cmax, cb.B, cb.eb);
         }
     });
+    cb.b_src = g.B;
+    cb.b_Kp = Kp;
+    cb.b_Np = Np;
+    cb.b_L = L;
+    cb.b_t = t;
     CUtensorMap tmA, tmB;
     if (!slice_tensor_map(&tmA, cb.A, split::kI8, Kp, L * Mp, pairs ? crt2::HALF : TM) ||
         !slice_tensor_map(&tmB, cb.B, split::kI8, Kp, L * Np, pairs ? crt2::HALF : TN))
@@ -1454,6 +1466,7 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
                 g.ccol = d_outcol;
                 g.kext = d_kext;
                 g.accumulate = 0;
+                g.reuse_b = r0 > 0;  // the same X for every panel
                 const double bf = 2.0 * rows * bk * cfl;
                 const double bb = ((double)rows * n + bk + (double)rows * m) * esz;
                 gemm(g, st, kTBack, bf, bb);

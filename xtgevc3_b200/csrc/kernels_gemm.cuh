@@ -38,6 +38,9 @@ struct GemmArgs {
     const int *ccol;     // output column of result column j (nullptr: j)
     const int *kext;     // nonzero leading rows of B per column (nullptr: K)
     int accumulate;
+    // residue form only: B and its shape are those of the previous launch on the same
+    // buffers (row panels of one back-transform), so its residues are reused
+    int reuse_b = 0;
 };
 
 // Segment holding K row kk (segments are contiguous and cover [0, K)); kb = its first row.
