@@ -212,6 +212,20 @@ struct CallRes {
     int *status = nullptr;  // pinned host word written by the structure check's copy
     uint8_t *hflags = nullptr;  // pinned refinement flags of the split form (grown on demand)
     size_t hflags_cap = 0;
+    // per side: the stream and fork / join events of the refinement sketch of S and P
+    // (created on first use)
+    cudaStream_t sk_stream[2] = {nullptr, nullptr};
+    cudaEvent_t sk_ev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    cudaError_t reserve_sketch()
+    {
+        cudaError_t e = cudaSuccess;
+        for (int s = 0; s < 2 && e == cudaSuccess; s++) {
+            if (!sk_stream[s]) e = cudaStreamCreateWithFlags(&sk_stream[s], cudaStreamNonBlocking);
+            for (int k = 0; k < 2 && e == cudaSuccess; k++)
+                if (!sk_ev[s][k]) e = cudaEventCreateWithFlags(&sk_ev[s][k], cudaEventDisableTiming);
+        }
+        return e;
+    }
     cudaError_t reserve_flags(size_t bytes)
     {
         if (bytes <= hflags_cap) return cudaSuccess;
@@ -1097,22 +1111,19 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
         // is computed on a second stream while the substitution runs (joined before T is
         // formed), otherwise after the substitution.  An early return joins it before the
         // stream-ordered scratch is released.
+        // the stream and events are the call's pooled ones (one set per side)
         cudaStream_t sk_st = nullptr;
         cudaEvent_t sk_ev[2] = {nullptr, nullptr};
         bool sk_pending = false;
         struct SketchGuard {
-            cudaStream_t &s;
             cudaEvent_t *ev;
             bool &pending;
             cudaStream_t main;
             ~SketchGuard()
             {
                 if (pending) cudaStreamWaitEvent(main, ev[1], 0);
-                for (int i = 0; i < 2; i++)
-                    if (ev[i]) cudaEventDestroy(ev[i]);
-                if (s) cudaStreamDestroy(s);
             }
-        } sk_guard{sk_st, sk_ev, sk_pending, st};
+        } sk_guard{sk_ev, sk_pending, st};
         auto matrix_sketch = [&](cudaStream_t s) -> int {
             if constexpr (!CPLX && std::is_same<R, double>::value) {
                 using namespace refine;
@@ -1127,8 +1138,13 @@ int solve_device(char side, char howmny, const int *select, int n, const void *S
             return 0;
         };
         if (flags && !o.arena && !tr.on && !o.cols_ready && !o.rows_ready) {
-            XTG_CK(cudaStreamCreateWithFlags(&sk_st, cudaStreamNonBlocking));
-            for (int i = 0; i < 2; i++) XTG_CK(cudaEventCreateWithFlags(&sk_ev[i], cudaEventDisableTiming));
+            cudaError_t e = cudaSuccess;
+            CallRes *cr = res.get(&e);
+            XTG_CK(e);
+            XTG_CK(cr->reserve_sketch());
+            sk_st = cr->sk_stream[left ? 1 : 0];
+            sk_ev[0] = cr->sk_ev[left ? 1 : 0][0];
+            sk_ev[1] = cr->sk_ev[left ? 1 : 0][1];
             XTG_CK(cudaEventRecord(sk_ev[0], st));
             XTG_CK(cudaStreamWaitEvent(sk_st, sk_ev[0], 0));
             if (matrix_sketch(sk_st)) return 1;
