@@ -231,7 +231,7 @@ int xtgevc3_ctgsna_dev(void *stream, char job, char howmny, const int *select, i
  * is the first row of that swap (as in LAPACK); INFO = -3 N, -5 LDA, -7 LDB, -9 LDQ,
  * -11 LDZ, -12 IFST, -13 ILST.  Complex arrays interleaved.  Device forms: A, B, Q, Z
  * device pointers, the call returns once the reordering is done (0, or 1 when a CUDA call
- * failed).  Real pencils (2x2 blocks) are not covered. */
+ * failed).  Real pencils: the D/STGEXC entry points below (1x1 blocks). */
 void xtgevc3_ztgexc(int wantq, int wantz, int n, double *A, int lda, double *B, int ldb, double *Q, int ldq, double *Z,
                     int ldz, int ifst, int *ilst, int *info);
 void xtgevc3_ctgexc(int wantq, int wantz, int n, float *A, int lda, float *B, int ldb, float *Q, int ldq, float *Z,
@@ -239,6 +239,24 @@ void xtgevc3_ctgexc(int wantq, int wantz, int n, float *A, int lda, float *B, in
 int xtgevc3_ztgexc_dev(void *stream, int wantq, int wantz, int n, double *A, int lda, double *B, int ldb, double *Q,
                        int ldq, double *Z, int ldz, int ifst, int *ilst, int *info);
 int xtgevc3_ctgexc_dev(void *stream, int wantq, int wantz, int n, float *A, int lda, float *B, int ldb, float *Q,
+                       int ldq, float *Z, int ldz, int ifst, int *ilst, int *info);
+
+/* ---- eigenvalue reordering, real pencils with 1x1 blocks: D/STGEXC (no counterpart upstream)
+ * LAPACK DTGEXC / STGEXC's arguments, INFO codes and results for moves whose rows (from the
+ * row above the lower of ifst, ilst to the row below the higher) hold only 1x1 diagonal
+ * blocks of the real generalized Schur pencil (A quasi-upper triangular, B upper
+ * triangular): swaps of adjacent real eigenvalues by two rotations each, as LAPACK's
+ * D/STGEX2 do them.  A move that would cross or start in a 2x2 block (a complex pair)
+ * leaves everything unchanged and sets INFO = 2 (not a LAPACK code) with a message in
+ * xtgevc3_last_error().  Other codes, *ilst and the device forms as for the complex
+ * entry points above. */
+void xtgevc3_dtgexc(int wantq, int wantz, int n, double *A, int lda, double *B, int ldb, double *Q, int ldq, double *Z,
+                    int ldz, int ifst, int *ilst, int *info);
+void xtgevc3_stgexc(int wantq, int wantz, int n, float *A, int lda, float *B, int ldb, float *Q, int ldq, float *Z,
+                    int ldz, int ifst, int *ilst, int *info);
+int xtgevc3_dtgexc_dev(void *stream, int wantq, int wantz, int n, double *A, int lda, double *B, int ldb, double *Q,
+                       int ldq, double *Z, int ldz, int ifst, int *ilst, int *info);
+int xtgevc3_stgexc_dev(void *stream, int wantq, int wantz, int n, float *A, int lda, float *B, int ldb, float *Q,
                        int ldq, float *Z, int ldz, int ifst, int *ilst, int *info);
 
 /* ---- allocation-free device entry point (no counterpart in the upstream library) -----

@@ -242,15 +242,18 @@ def lapack_tgsna(howmny, A, B, VL, VR, select=None):
 
 
 def lapack_tgexc(A, B, Q, Z, ifst, ilst):
-    """Oracle of the complex xTGEXC entry points: LAPACK ZTGEXC / CTGEXC through SciPy
-    (ifst, ilst 1-based; Q, Z may be None: not updated).  Returns (A, B, Q, Z, info)."""
+    """Oracle of the xTGEXC entry points: LAPACK Z/C/D/STGEXC through SciPy (ifst, ilst
+    1-based; Q, Z may be None: not updated).  Returns (A, B, Q, Z, info)."""
     import scipy.linalg.lapack as lapack
-    f = getattr(lapack, {np.complex128: "ztgexc", np.complex64: "ctgexc"}[A.dtype.type])
+    dt = A.dtype.type
+    f = getattr(lapack, {np.complex128: "ztgexc", np.complex64: "ctgexc", np.float64: "dtgexc",
+                         np.float32: "stgexc"}[dt])
     n = A.shape[0]
     wq, wz = Q is not None, Z is not None
     Qa = Q if wq else np.eye(n, dtype=A.dtype)
     Za = Z if wz else np.eye(n, dtype=A.dtype)
-    a, b, q, z, info = f(A, B, Qa, Za, ifst, ilst, wantq=int(wq), wantz=int(wz))
+    out = f(A, B, Qa, Za, ifst, ilst, wantq=int(wq), wantz=int(wz))
+    a, b, q, z, info = out[0], out[1], out[2], out[3], out[-1]  # real forms also return WORK
     return a, b, (q if wq else None), (z if wz else None), info
 
 

@@ -102,3 +102,68 @@ def test_tgexc_rejected_swap_matches_lapack(cuda_ok):
             den = np.abs(R).max(0)
             den[den == 0] = 1.0
             assert float((np.abs(M - R).max(0) / den).max()) < 1e-12, i
+
+
+# ---- real pencils: D/STGEXC over 1x1 blocks --------------------------------------------
+TOL_R = {np.float64: 1e-12, np.float32: 2e-4}
+
+
+def _real_triangular_pencil(n, seed, dt):
+    """A real generalized Schur pencil with only 1x1 blocks: A, B upper triangular (N(0,1)
+    parts, |B_kk| kept away from 0), Q and Z orthogonal."""
+    rng = np.random.default_rng(seed)
+    A = np.triu(rng.standard_normal((n, n)))
+    B = np.triu(rng.standard_normal((n, n)))
+    B[np.diag_indices(n)] = np.abs(B[np.diag_indices(n)]) + 0.5
+    Q = np.linalg.qr(rng.standard_normal((n, n)))[0]
+    Z = np.linalg.qr(rng.standard_normal((n, n)))[0]
+    return tuple(np.asfortranarray(M.astype(dt)) for M in (A, B, Q, Z))
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32], ids=["d", "s"])
+@pytest.mark.parametrize("move", MOVES, ids=lambda m: f"{m[0]}to{m[1]}")
+def test_real_tgexc_matches_lapack(cuda_ok, dt, move):
+    """Moves across real eigenvalues: LAPACK D/STGEXC's swaps (two rotations each, the real
+    routine's sign conventions), so A, B, Q and Z agree with LAPACK's to rounding."""
+    ifst, ilst = move
+    A, B, Q, Z = _real_triangular_pencil(40, 5, dt)
+    ra, rb, rq, rz, rinfo = oracle.lapack_tgexc(A, B, Q, Z, ifst, ilst)
+    a, b, q, z, il, info = X.tgexc(A, B, Q, Z, ifst, ilst)
+    assert (info, il) == (rinfo, ilst) == (0, ilst)
+    for M, R in ((a, ra), (b, rb), (q, rq), (z, rz)):
+        assert _rel(M, R) < TOL_R[dt]
+    k = ilst - 1
+    assert abs(a[k, k] / b[k, k] - A[ifst - 1, ifst - 1] / B[ifst - 1, ifst - 1]) < 1e-6 * max(
+        1.0, abs(A[ifst - 1, ifst - 1] / B[ifst - 1, ifst - 1]))
+    assert np.allclose(np.tril(a, -1), 0) and np.allclose(np.tril(b, -1), 0)
+
+
+def test_real_tgexc_device_form_and_no_qz(cuda_ok):
+    """Device form (column-major CUDA tensors, in place), and WANTQ = WANTZ = 0: the same A
+    and B as LAPACK with Q, Z not referenced."""
+    import torch
+    A, B, Q, Z = _real_triangular_pencil(64, 9, np.float64)
+    ra, rb, _, _, rinfo = oracle.lapack_tgexc(A, B, None, None, 50, 3)
+
+    def dev(M):
+        return torch.from_numpy(np.ascontiguousarray(M.T)).cuda().t()
+
+    da, db = dev(A), dev(B)
+    il, info = X.tgexc_dev(da, db, None, None, 50, 3)
+    torch.cuda.synchronize()
+    assert (info, il) == (rinfo, 3) == (0, 3)
+    assert _rel(da.t().cpu().numpy().T, ra) < 1e-12 and _rel(db.t().cpu().numpy().T, rb) < 1e-12
+
+
+def test_real_tgexc_refuses_moves_across_2x2_blocks(cuda_ok):
+    """A real xGGES pencil has 2x2 blocks (complex pairs): a move across one is not done,
+    INFO = 2 with a message, and A, B, Q, Z are returned unchanged."""
+    from xtgevc3_b200 import pencils
+    S, P, ar, ai, be, Q, Z = pencils.gen_gges(60, 31)
+    k = int(np.flatnonzero(ai > 0)[0])  # first row of a 2x2 block
+    ifst, ilst = (k + 3, 1) if k + 3 <= 60 else (60, 1)
+    a, b, q, z, il, info = X.tgexc(S, P, Q, Z, ifst, ilst)
+    assert info == 2 and "2x2" in X.last_error()
+    assert il == ilst
+    for M, R in ((a, S), (b, P), (q, Q), (z, Z)):
+        np.testing.assert_array_equal(M, R)

@@ -392,12 +392,13 @@ def tgsna(howmny, A, B, VL, VR, select=None, job="E"):
 
 
 def tgexc(A, B, Q=None, Z=None, ifst=1, ilst=1):
-    """Host-array form of z/ctgexc: move the eigenvalue at row ifst of the complex Schur pencil
-    (A, B) to row ilst (1-based, as LAPACK), updating Q and Z when given.  Returns
-    (A, B, Q, Z, ilst, info) with new arrays."""
+    """Host-array form of z/c/d/stgexc: move the eigenvalue at row ifst of the generalized
+    Schur pencil (A, B) to row ilst (1-based, as LAPACK), updating Q and Z when given.  Real
+    pencils: moves across 1x1 blocks only (info = 2 and the pencil unchanged when a 2x2
+    block is in the way).  Returns (A, B, Q, Z, ilst, info) with new arrays."""
     L = lib()
     dt = A.dtype.type
-    pfx = {np.complex128: "z", np.complex64: "c"}[dt]
+    pfx = {np.complex128: "z", np.complex64: "c", np.float64: "d", np.float32: "s"}[dt]
     n = A.shape[0]
     A, B = np.array(A, order="F", dtype=dt), np.array(B, order="F", dtype=dt)
     Qc = None if Q is None else np.array(Q, order="F", dtype=dt)
@@ -406,17 +407,17 @@ def tgexc(A, B, Q=None, Z=None, ifst=1, ilst=1):
     ld = max(n, 1)
     getattr(L, f"xtgevc3_{pfx}tgexc")(int(Qc is not None), int(Zc is not None), n, _ptr(A), ld, _ptr(B), ld, _ptr(Qc),
                                       ld, _ptr(Zc), ld, ifst, ct.byref(il), ct.byref(info))
-    if info.value > 0 and last_error():  # a rejected swap (INFO = 1) leaves no error text
+    if info.value == 1 and last_error():  # a rejected swap (INFO = 1) leaves no error text
         raise RuntimeError(f"xtgevc3_{pfx}tgexc failed: {last_error()}")
     return A, B, Qc, Zc, il.value, info.value
 
 
 def tgexc_dev(A, B, Q=None, Z=None, ifst=1, ilst=1, stream=None):
-    """Device form of z/ctgexc on column-major CUDA tensors (reordered in place).  Returns
+    """Device form of z/c/d/stgexc on column-major CUDA tensors (reordered in place).  Returns
     (ilst, info)."""
     import torch
     L = lib()
-    pfx = {torch.complex128: "z", torch.complex64: "c"}[A.dtype]
+    pfx = {torch.complex128: "z", torch.complex64: "c", torch.float64: "d", torch.float32: "s"}[A.dtype]
     n = A.shape[0]
     st = ct.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
     il, info = ct.c_int(ilst), ct.c_int(0)

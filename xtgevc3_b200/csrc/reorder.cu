@@ -22,6 +22,16 @@
 // B200 form: one CTA walks the swaps in order (each depends on the previous one); thread 0
 // computes a swap's rotations and tests from the 2x2 blocks, then the CTA applies them to the
 // two columns of A, B, Z and the two rows of A, B and columns of Q, O(n) work per swap.
+//
+// Real pencils (D/STGEXC, with their swaps D/STGEX2): moves whose rows hold only 1x1
+// diagonal blocks, by the same method in real arithmetic, following the real routine's own
+// conventions: with (cs, sn) the rotation [cs sn; -sn cs] [F; G] = [r; 0] (cs >= 0, r of
+// F's sign; F = s11 t00 - t11 s00, G = s11 t01 - t11 s01), the columns take (c, s) =
+// (sn, -cs), the rows the rotation that zeroes the new (1, 0) entry of S or T, both applied
+// as (x, y) <- (c x + s y, c y - s x); Z takes the column rotation, Q the row rotation.  A
+// move across or into a 2x2 block (a complex pair; the real routine's general swap through a
+// small generalized Sylvester equation) is not done: the pencil is left unchanged, INFO = 2
+// and xtgevc3_last_error() says so.
 #include "../../include/xtgevc3.h"
 #include "common.cuh"
 #include "engine.cuh"
@@ -207,6 +217,169 @@ __global__ void __launch_bounds__(kReorderThreads) tgexc_cplx_kernel(ReorderArgs
     }
 }
 
+// Real plane rotation [c s; -s c] [f; g] = [r; 0] with c >= 0 and r of f's sign, computed in
+// range (the scaled form near underflow and overflow).
+template <class R>
+__device__ void lartg_real(R f, R g, R &c, R &s)
+{
+    const R safmin = limits<R>::safemin, safmax = R(1) / safmin;
+    const R rtmin = sqrt(safmin), rtmax = sqrt(safmax / R(2));
+    if (g == R(0)) {
+        c = R(1);
+        s = R(0);
+        return;
+    }
+    if (f == R(0)) {
+        c = R(0);
+        s = copysign(R(1), g);
+        return;
+    }
+    const R f1 = fabs(f), g1 = fabs(g);
+    if (f1 > rtmin && f1 < rtmax && g1 > rtmin && g1 < rtmax) {
+        const R d = sqrt(f * f + g * g);
+        c = f1 / d;
+        s = g / copysign(d, f);
+    } else {
+        const R u = fmin(safmax, fmax(safmin, fmax(f1, g1)));
+        const R fs = f / u, gs = g / u, d = sqrt(fs * fs + gs * gs);
+        c = fabs(fs) / d;
+        s = gs / copysign(d, f);
+    }
+}
+
+// (x, y) <- (c x + s y, c y - s x)
+template <class R>
+__device__ __forceinline__ void rot_real(R &x, R &y, R c, R s)
+{
+    const R xn = c * x + s * y, yn = c * y - s * x;
+    x = xn;
+    y = yn;
+}
+
+__device__ __forceinline__ double mul_sep(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_sep(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double sub_sep(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float sub_sep(float a, float b) { return __fsub_rn(a, b); }
+
+template <class R>
+struct ReorderArgsReal {
+    int n, ifst, ilst, wantq, wantz;  // ifst, ilst 0-based
+    R *A, *B, *Q, *Z;
+    int lda, ldb, ldq, ldz;
+    int *status;  // {position reached, or first row of the rejected swap; 0 / 1 / 2}
+};
+
+template <class R>
+__global__ void __launch_bounds__(kReorderThreads) tgexc_real_kernel(ReorderArgsReal<R> a)
+{
+    __shared__ R s_cz, s_sz, s_cq, s_sq;
+    __shared__ int s_ok;
+    const R eps = limits<R>::eps, smlnum = limits<R>::safemin / eps;
+    const int step = a.ifst < a.ilst ? 1 : -1;
+    auto at = [](R *M, int ld, int i, int j) -> R & { return M[(size_t)i + (size_t)j * ld]; };
+    // a 2x2 block in rows [lo - 1, hi + 1] (subdiagonal entries A(k + 1, k)) stops the move
+    if (threadIdx.x == 0) {
+        const int lo = min(a.ifst, a.ilst), hi = max(a.ifst, a.ilst);
+        int pair = 0;
+        for (int k = max(lo - 1, 0); k <= min(hi, a.n - 2); k++)
+            if (at(a.A, a.lda, k + 1, k) != R(0)) pair = 1;
+        s_ok = pair ? 0 : 1;
+    }
+    __syncthreads();
+    if (!s_ok) {
+        if (threadIdx.x == 0) {
+            a.status[0] = a.ifst;
+            a.status[1] = 2;
+        }
+        return;
+    }
+    int here = a.ifst, bad = -1;
+    while (here != a.ilst) {
+        const int j = step > 0 ? here : here - 1;  // swap rows / columns j and j + 1
+        if (threadIdx.x == 0) {
+            const R a00 = at(a.A, a.lda, j, j), a01 = at(a.A, a.lda, j, j + 1);
+            const R a10 = at(a.A, a.lda, j + 1, j), a11 = at(a.A, a.lda, j + 1, j + 1);
+            const R b00 = at(a.B, a.ldb, j, j), b01 = at(a.B, a.ldb, j, j + 1);
+            const R b10 = at(a.B, a.ldb, j + 1, j), b11 = at(a.B, a.ldb, j + 1, j + 1);
+            const R tha = fmax(R(20) * eps * hypot(hypot(a00, a10), hypot(a01, a11)), smlnum);
+            const R thb = fmax(R(20) * eps * hypot(hypot(b00, b10), hypot(b01, b11)), smlnum);
+            const R f = sub_sep(mul_sep(a11, b00), mul_sep(b11, a00));
+            const R g = sub_sep(mul_sep(a11, b01), mul_sep(b11, a01));
+            const R sa = fabs(a11) * fabs(b00), sb = fabs(a00) * fabs(b11);
+            R cs, sn;
+            lartg_real(f, g, cs, sn);
+            const R cz = sn, sz = -cs;  // the column rotation
+            R s00 = a00, s01 = a01, s10 = a10, s11 = a11, t00 = b00, t01 = b01, t10 = b10, t11 = b11;
+            rot_real(s00, s01, cz, sz);
+            rot_real(s10, s11, cz, sz);
+            rot_real(t00, t01, cz, sz);
+            rot_real(t10, t11, cz, sz);
+            R cq, sq;
+            if (sa >= sb) lartg_real(s00, s10, cq, sq);
+            else lartg_real(t00, t10, cq, sq);
+            rot_real(s00, s10, cq, sq);
+            rot_real(s01, s11, cq, sq);
+            rot_real(t00, t10, cq, sq);
+            rot_real(t01, t11, cq, sq);
+            bool ok = fabs(s10) <= tha && fabs(t10) <= thb && isfinite(cz) && isfinite(sz) && isfinite(cq) &&
+                      isfinite(sq) && isfinite(s00) && isfinite(s01) && isfinite(s11) && isfinite(t00) &&
+                      isfinite(t01) && isfinite(t11);
+            if (ok) {  // undo both rotations on the swapped blocks: the originals must come back
+                R w00 = s00, w01 = s01, w10 = s10, w11 = s11, v00 = t00, v01 = t01, v10 = t10, v11 = t11;
+                rot_real(w00, w10, cq, -sq);
+                rot_real(w01, w11, cq, -sq);
+                rot_real(v00, v10, cq, -sq);
+                rot_real(v01, v11, cq, -sq);
+                rot_real(w00, w01, cz, -sz);
+                rot_real(w10, w11, cz, -sz);
+                rot_real(v00, v01, cz, -sz);
+                rot_real(v10, v11, cz, -sz);
+                ok = hypot(hypot(w00 - a00, w10 - a10), hypot(w01 - a01, w11 - a11)) <= tha &&
+                     hypot(hypot(v00 - b00, v10 - b10), hypot(v01 - b01, v11 - b11)) <= thb;
+            }
+            s_ok = ok ? 1 : 0;
+            s_cz = cz;
+            s_sz = sz;
+            s_cq = cq;
+            s_sq = sq;
+        }
+        __syncthreads();
+        if (!s_ok) {
+            bad = j;
+            break;
+        }
+        const R cz = s_cz, sz = s_sz, cq = s_cq, sq = s_sq;
+        // columns j, j+1: rows [0, j + 2) of A and B, all rows of Z
+        for (int i = threadIdx.x; i < j + 2; i += blockDim.x) {
+            rot_real(at(a.A, a.lda, i, j), at(a.A, a.lda, i, j + 1), cz, sz);
+            rot_real(at(a.B, a.ldb, i, j), at(a.B, a.ldb, i, j + 1), cz, sz);
+        }
+        if (a.wantz)
+            for (int i = threadIdx.x; i < a.n; i += blockDim.x)
+                rot_real(at(a.Z, a.ldz, i, j), at(a.Z, a.ldz, i, j + 1), cz, sz);
+        __syncthreads();  // the 2x2 block takes the column rotation before the row rotation
+        // rows j, j+1: columns [j, n) of A and B; Q's columns j, j+1
+        for (int c = j + threadIdx.x; c < a.n; c += blockDim.x) {
+            rot_real(at(a.A, a.lda, j, c), at(a.A, a.lda, j + 1, c), cq, sq);
+            rot_real(at(a.B, a.ldb, j, c), at(a.B, a.ldb, j + 1, c), cq, sq);
+        }
+        if (a.wantq)
+            for (int i = threadIdx.x; i < a.n; i += blockDim.x)
+                rot_real(at(a.Q, a.ldq, i, j), at(a.Q, a.ldq, i, j + 1), cq, sq);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            at(a.A, a.lda, j + 1, j) = R(0);
+            at(a.B, a.ldb, j + 1, j) = R(0);
+        }
+        __syncthreads();
+        here += step;
+    }
+    if (threadIdx.x == 0) {
+        a.status[0] = bad >= 0 ? bad : here;
+        a.status[1] = bad >= 0 ? 1 : 0;
+    }
+}
+
 // LAPACK xTGEXC's argument checks, in its order.
 int tgexc_check(int wantq, int wantz, int n, int lda, int ldb, int ldq, int ldz, int ifst, int ilst)
 {
@@ -304,6 +477,94 @@ void tgexc_host(int wantq, int wantz, int n, cplx<R> *A, int lda, cplx<R> *B, in
     }
 }
 
+// Real pencils, device pointers: as tgexc_device (INFO = 2: a 2x2 block in the move's rows,
+// nothing done).
+template <class R>
+int tgexc_device_real(cudaStream_t st, int wantq, int wantz, int n, R *A, int lda, R *B, int ldb, R *Q, int ldq, R *Z,
+                      int ldz, int ifst, int *ilst, int *info)
+{
+    set_last_error("");
+    *info = tgexc_check(wantq, wantz, n, lda, ldb, ldq, ldz, ifst, *ilst);
+    if (*info) {
+        set_last_error("xTGEXC: argument " + std::to_string(-*info) + " has an illegal value");
+        return 0;
+    }
+    if (n <= 1 || ifst == *ilst) return 0;
+    int *d_status = nullptr;
+    int h_status[2] = {0, 0};
+    cudaError_t e = cudaMallocAsync(&d_status, 2 * sizeof(int), st);
+    if (e == cudaSuccess) {
+        ReorderArgsReal<R> ra{n, ifst - 1, *ilst - 1, wantq ? 1 : 0, wantz ? 1 : 0, A, B, Q, Z, lda, ldb, ldq, ldz,
+                              d_status};
+        tgexc_real_kernel<R><<<1, kReorderThreads, 0, st>>>(ra);
+        count_launches(1);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h_status, d_status, sizeof(h_status), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        cudaFreeAsync(d_status, st);
+    }
+    if (e != cudaSuccess) {
+        set_last_error(std::string("xTGEXC: ") + cudaGetErrorString(e));
+        *info = 1;
+        return 1;
+    }
+    *info = h_status[1];
+    if (*info == 2) {
+        set_last_error("xTGEXC (real): a 2x2 diagonal block (complex pair) lies in the rows of the move; only moves "
+                       "across 1x1 blocks are supported, the pencil is unchanged");
+        return 0;
+    }
+    *ilst = h_status[0] + 1;
+    return 0;
+}
+
+// Real pencils, host pointers: as tgexc_host.
+template <class R>
+void tgexc_host_real(int wantq, int wantz, int n, R *A, int lda, R *B, int ldb, R *Q, int ldq, R *Z, int ldz, int ifst,
+                     int *ilst, int *info)
+{
+    set_last_error("");
+    *info = tgexc_check(wantq, wantz, n, lda, ldb, ldq, ldz, ifst, *ilst);
+    if (*info) {
+        set_last_error("xTGEXC: argument " + std::to_string(-*info) + " has an illegal value");
+        return;
+    }
+    if (n <= 1 || ifst == *ilst) return;
+    cudaStream_t st = nullptr;
+    R *dm[4] = {nullptr, nullptr, nullptr, nullptr};
+    R *hm[4] = {A, B, wantq ? Q : nullptr, wantz ? Z : nullptr};
+    const int hl[4] = {lda, ldb, ldq, ldz};
+    const size_t bytes = (size_t)n * n * sizeof(R);
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    for (int k = 0; k < 4 && e == cudaSuccess; k++) {
+        if (!hm[k]) continue;
+        e = cudaMallocAsync(&dm[k], bytes, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(dm[k], (size_t)n * sizeof(R), hm[k], (size_t)hl[k] * sizeof(R), (size_t)n * sizeof(R),
+                                  n, cudaMemcpyHostToDevice, st);
+    }
+    int rc = 0;
+    if (e == cudaSuccess) {
+        rc = tgexc_device_real<R>(st, wantq, wantz, n, dm[0], n, dm[1], n, dm[2] ? dm[2] : dm[0], n,
+                                  dm[3] ? dm[3] : dm[0], n, ifst, ilst, info);
+        for (int k = 0; k < 4 && rc == 0 && e == cudaSuccess && *info != 2; k++)
+            if (hm[k])
+                e = cudaMemcpy2DAsync(hm[k], (size_t)hl[k] * sizeof(R), dm[k], (size_t)n * sizeof(R),
+                                      (size_t)n * sizeof(R), n, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    for (R *p : dm)
+        if (p) cudaFreeAsync(p, st);
+    if (st) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
+    if (e != cudaSuccess) {
+        set_last_error(std::string("xTGEXC staging: ") + cudaGetErrorString(e));
+        *info = 1;
+    }
+}
+
 }  // namespace
 }  // namespace xtg
 
@@ -343,6 +604,32 @@ int xtgevc3_ctgexc_dev(void *stream, int wantq, int wantz, int n, float *A, int 
                                     reinterpret_cast<cplx<float> *>(A), lda, reinterpret_cast<cplx<float> *>(B), ldb,
                                     reinterpret_cast<cplx<float> *>(Q), ldq, reinterpret_cast<cplx<float> *>(Z), ldz, ifst,
                                     ilst, info);
+}
+
+void xtgevc3_dtgexc(int wantq, int wantz, int n, double *A, int lda, double *B, int ldb, double *Q, int ldq, double *Z,
+                    int ldz, int ifst, int *ilst, int *info)
+{
+    xtg::tgexc_host_real<double>(wantq, wantz, n, A, lda, B, ldb, Q, ldq, Z, ldz, ifst, ilst, info);
+}
+
+void xtgevc3_stgexc(int wantq, int wantz, int n, float *A, int lda, float *B, int ldb, float *Q, int ldq, float *Z,
+                    int ldz, int ifst, int *ilst, int *info)
+{
+    xtg::tgexc_host_real<float>(wantq, wantz, n, A, lda, B, ldb, Q, ldq, Z, ldz, ifst, ilst, info);
+}
+
+int xtgevc3_dtgexc_dev(void *stream, int wantq, int wantz, int n, double *A, int lda, double *B, int ldb, double *Q,
+                       int ldq, double *Z, int ldz, int ifst, int *ilst, int *info)
+{
+    return xtg::tgexc_device_real<double>(static_cast<cudaStream_t>(stream), wantq, wantz, n, A, lda, B, ldb, Q, ldq, Z,
+                                          ldz, ifst, ilst, info);
+}
+
+int xtgevc3_stgexc_dev(void *stream, int wantq, int wantz, int n, float *A, int lda, float *B, int ldb, float *Q,
+                       int ldq, float *Z, int ldz, int ifst, int *ilst, int *info)
+{
+    return xtg::tgexc_device_real<float>(static_cast<cudaStream_t>(stream), wantq, wantz, n, A, lda, B, ldb, Q, ldq, Z,
+                                         ldz, ifst, ilst, info);
 }
 
 }  // extern "C"
