@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--adjoint-c-n", type=int, default=128)
     ap.add_argument("--z-n", type=int, default=4096, help="order of the ztgevc3 SIDE=R HOWMNY=A leg (0 skips)")
     ap.add_argument("--trevc3-n", type=int, default=8192, help="order of the dtrevc3 SIDE=B HOWMNY=B leg (0 skips)")
-    ap.add_argument("--tgexc-n", type=int, default=4096, help="order of the ztgexc reordering leg (0 skips)")
+    ap.add_argument("--tgexc-n", type=int, default=4096, help="order of the ztgexc and dtgexc reordering legs (0 skips)")
     ap.add_argument("--profile-case", default=None,
                     help="run one small case for an ncu capture and exit (no JSON line): plain:N (two dtgevc3 "
                          "B/B calls, FP64; plain_norm:N with the normalisation), split_i8:N / split_crt:N (the same, INT8 digit / residue split "
@@ -714,17 +714,25 @@ def measure_ztgevc3(args, X, torch):
                     "graded: rows of P scaled by 10^U(-8,8)", **out}
 
 
-def measure_tgexc(args, X, torch):
-    """ztgexc: the last eigenvalue of a complex upper-triangular pencil of order --tgexc-n moves
-    to the top (n - 1 swaps), Q and Z updated (Q = Z = I: the rotations cost the same whatever
-    their values); device-resident inputs restored before each step outside the timed region,
-    CUDA-event timing; LAPACK ZTGEXC (SciPy's OpenBLAS) on the same input and move beside it,
-    with the largest difference between the two results."""
+def measure_tgexc(args, X, torch, real=False):
+    """ztgexc (or dtgexc with `real`): the last eigenvalue of an upper-triangular pencil of
+    order --tgexc-n moves to the top (n - 1 swaps), Q and Z updated (Q = Z = I: the rotations
+    cost the same whatever their values); device-resident inputs restored before each step
+    outside the timed region, CUDA-event timing; LAPACK Z/DTGEXC (SciPy's OpenBLAS) on the
+    same input and move beside it, with the largest difference between the two results."""
     from xtgevc3_b200 import pencils as gen
     n = args.tgexc_n
-    S_h, P_h, _, _ = gen.gen_upper_triangular_complex(n, args.seed + 41)
+    if real:  # real eigenvalues only (1x1 blocks): the pencil class the real entry points take
+        rng = np.random.default_rng(args.seed + 43)
+        S_h = np.asfortranarray(np.triu(rng.standard_normal((n, n))))
+        P_h = np.triu(rng.standard_normal((n, n)))
+        P_h[np.diag_indices(n)] = np.abs(P_h[np.diag_indices(n)]) + 0.5
+        P_h = np.asfortranarray(P_h)
+    else:
+        S_h, P_h, _, _ = gen.gen_upper_triangular_complex(n, args.seed + 41)
+    dt_t, dt_n = (torch.float64, np.float64) if real else (torch.complex128, np.complex128)
     S0, P0 = colmajor_cuda(S_h, torch), colmajor_cuda(P_h, torch)
-    I0 = torch.eye(n, dtype=torch.complex128, device="cuda")
+    I0 = torch.eye(n, dtype=dt_t, device="cuda")
     A, B, Q, Z = (torch.empty_like(S0) for _ in range(4))
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ts, res = [], None
@@ -744,10 +752,11 @@ def measure_tgexc(args, X, torch):
     ms = float(np.mean(ts))
     out = {"n": n, "move": f"{n} -> 1", "swaps": n - 1, "ilst_info": list(res), "ms": ms,
            "swaps_per_s": (n - 1) / (ms * 1e-3),
-           "data": "complex upper-triangular stand-in pencil (U(-1,1) parts, |P_kk| kept away from 0), Q = Z = I"}
+           "data": ("real upper-triangular pencil (N(0,1) parts, |P_kk| >= 0.5), Q = Z = I" if real else
+                    "complex upper-triangular stand-in pencil (U(-1,1) parts, |P_kk| kept away from 0), Q = Z = I")}
     if not args.no_cpu:
         import oracle
-        Ih = np.eye(n, dtype=np.complex128, order="F")
+        Ih = np.eye(n, dtype=dt_n, order="F")
         t0 = time.perf_counter()
         ra, rb, rq, rz, rinfo = oracle.lapack_tgexc(S_h, P_h, Ih, Ih.copy(order="F"), n, 1)
         tc = time.perf_counter() - t0
@@ -755,7 +764,7 @@ def measure_tgexc(args, X, torch):
         for D, R in ((A, ra), (B, rb), (Q, rq), (Z, rz)):
             diff = max(diff, float(np.abs(D.cpu().numpy() - R).max() / np.abs(R).max()))
         out["cpu_lapack"] = {"seconds": tc, "swaps_per_s": (n - 1) / tc, "cores": host_threads(), "info": int(rinfo),
-                             "kind": "LAPACK ztgexc (SciPy OpenBLAS), one call"}
+                             "kind": f"LAPACK {'d' if real else 'z'}tgexc (SciPy OpenBLAS), one call"}
         out["max_rel_diff_vs_lapack"] = diff
     del S0, P0, I0, A, B, Q, Z
     return out
@@ -1128,6 +1137,7 @@ def main():
     zleg = measure_ztgevc3(args, X, torch) if args.z_n > 0 and rank == 0 else None
     trleg = measure_trevc3(args, X, torch) if args.trevc3_n > 0 and rank == 0 else None
     txleg = measure_tgexc(args, X, torch) if args.tgexc_n > 0 and rank == 0 else None
+    dxleg = measure_tgexc(args, X, torch, real=True) if args.tgexc_n > 0 and rank == 0 else None
 
     if rank == 0:
         form_desc = {"plain": "plain FP64 (DMMA)", "split": f"split precision, {s} BF16 slices (tcgen05)",
@@ -1166,7 +1176,7 @@ def main():
                                "d_max_rel_diff_vs_loop": batched["d"]["max_rel_diff_vs_loop"]}},
                 "forms": forms_out, "clocks": h["clocks"], "e2e": e2e, "gpu_launches": h["launches"],
                 "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "normalize": norm, "batched": batched,
-                "adjoint": adjoint, "ztgevc3": zleg, "dtrevc3": trleg, "ztgexc": txleg}
+                "adjoint": adjoint, "ztgevc3": zleg, "dtrevc3": trleg, "ztgexc": txleg, "dtgexc": dxleg}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
