@@ -106,6 +106,38 @@ __device__ __forceinline__ R fnorm2(cplx<R> a, cplx<R> b, cplx<R> c, cplx<R> d)
     return hypot(hypot(cabs_(a), cabs_(b)), hypot(cabs_(c), cabs_(d)));
 }
 
+// Rotation passes of a swap, with every thread's pairs loaded before any is stored (one
+// memory round trip per batch instead of one per element): element i of the pass is the
+// pair (x(i), y(i)) of matrix M (one matrix) or of M and N (two, with the same rotation).
+// pairs per thread and batch (double complex: 1, its kernel has no registers to spare)
+template <class E>
+constexpr int kBatchOf = sizeof(E) >= 16 ? 1 : 4;
+
+template <int KB, class E, class AX, class AY, class ROT>
+__device__ __forceinline__ void rot_pass(int cnt, AX ax, AY ay, ROT rot)
+{
+    for (int base = threadIdx.x; base < cnt; base += KB * blockDim.x) {
+        E x[KB], y[KB];
+#pragma unroll
+        for (int u = 0; u < KB; u++) {
+            const int i = base + u * blockDim.x;
+            if (i < cnt) {
+                x[u] = ax(i);
+                y[u] = ay(i);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < KB; u++) {
+            const int i = base + u * blockDim.x;
+            if (i < cnt) {
+                rot(x[u], y[u]);
+                ax(i) = x[u];
+                ay(i) = y[u];
+            }
+        }
+    }
+}
+
 template <class R>
 struct ReorderArgs {
     int n, ifst, ilst, wantq, wantz;  // ifst, ilst 0-based
@@ -115,7 +147,7 @@ struct ReorderArgs {
 };
 
 template <class R>
-__global__ void __launch_bounds__(kReorderThreads) tgexc_cplx_kernel(ReorderArgs<R> a)
+__global__ void __launch_bounds__(kReorderThreads, 1) tgexc_cplx_kernel(ReorderArgs<R> a)
 {
     using C = cplx<R>;
     __shared__ R s_cz, s_cq;
@@ -187,22 +219,38 @@ __global__ void __launch_bounds__(kReorderThreads) tgexc_cplx_kernel(ReorderArgs
         }
         const R cz = s_cz, cq = s_cq;
         const C szc = s_szc, sq = s_sq;
-        // columns j, j+1: rows [0, j + 2) of A and B, all rows of Z
-        for (int i = threadIdx.x; i < j + 2; i += blockDim.x) {
-            rot(at(a.A, a.lda, i, j), at(a.A, a.lda, i, j + 1), cz, szc);
-            rot(at(a.B, a.ldb, i, j), at(a.B, a.ldb, i, j + 1), cz, szc);
+        // columns j, j+1: rows [0, j + 2) of A and B, all rows of Z (A's and B's pairs as one
+        // pass of 2 (j + 2) elements)
+        {
+            const int m2 = j + 2;
+            auto rc = [&](C &x, C &y) { rot(x, y, cz, szc); };
+            rot_pass<kBatchOf<C>, C>(2 * m2,
+                           [&](int i) -> C & { return i < m2 ? at(a.A, a.lda, i, j) : at(a.B, a.ldb, i - m2, j); },
+                           [&](int i) -> C & {
+                               return i < m2 ? at(a.A, a.lda, i, j + 1) : at(a.B, a.ldb, i - m2, j + 1);
+                           },
+                           rc);
+            if (a.wantz)
+                rot_pass<kBatchOf<C>, C>(a.n, [&](int i) -> C & { return at(a.Z, a.ldz, i, j); },
+                               [&](int i) -> C & { return at(a.Z, a.ldz, i, j + 1); }, rc);
         }
-        if (a.wantz)
-            for (int i = threadIdx.x; i < a.n; i += blockDim.x) rot(at(a.Z, a.ldz, i, j), at(a.Z, a.ldz, i, j + 1), cz, szc);
         __syncthreads();  // the 2x2 block takes the column rotation before the row rotation
         // rows j, j+1: columns [j, n) of A and B; Q's columns j, j+1 take the conjugate rotation
-        for (int c = j + threadIdx.x; c < a.n; c += blockDim.x) {
-            rot(at(a.A, a.lda, j, c), at(a.A, a.lda, j + 1, c), cq, sq);
-            rot(at(a.B, a.ldb, j, c), at(a.B, a.ldb, j + 1, c), cq, sq);
+        {
+            const int m2 = a.n - j;
+            rot_pass<kBatchOf<C>, C>(2 * m2,
+                           [&](int i) -> C & { return i < m2 ? at(a.A, a.lda, j, j + i) : at(a.B, a.ldb, j, j + i - m2); },
+                           [&](int i) -> C & {
+                               return i < m2 ? at(a.A, a.lda, j + 1, j + i) : at(a.B, a.ldb, j + 1, j + i - m2);
+                           },
+                           [&](C &x, C &y) { rot(x, y, cq, sq); });
+            if (a.wantq) {
+                const C sqc = conjg(sq);
+                rot_pass<kBatchOf<C>, C>(a.n, [&](int i) -> C & { return at(a.Q, a.ldq, i, j); },
+                               [&](int i) -> C & { return at(a.Q, a.ldq, i, j + 1); },
+                               [&](C &x, C &y) { rot(x, y, cq, sqc); });
+            }
         }
-        if (a.wantq)
-            for (int i = threadIdx.x; i < a.n; i += blockDim.x)
-                rot(at(a.Q, a.ldq, i, j), at(a.Q, a.ldq, i, j + 1), cq, conjg(sq));
         __syncthreads();
         if (threadIdx.x == 0) {
             at(a.A, a.lda, j + 1, j) = C(R(0), R(0));
@@ -270,7 +318,7 @@ struct ReorderArgsReal {
 };
 
 template <class R>
-__global__ void __launch_bounds__(kReorderThreads) tgexc_real_kernel(ReorderArgsReal<R> a)
+__global__ void __launch_bounds__(kReorderThreads, 1) tgexc_real_kernel(ReorderArgsReal<R> a)
 {
     __shared__ R s_cz, s_sz, s_cq, s_sq;
     __shared__ int s_ok;
@@ -350,22 +398,34 @@ __global__ void __launch_bounds__(kReorderThreads) tgexc_real_kernel(ReorderArgs
         }
         const R cz = s_cz, sz = s_sz, cq = s_cq, sq = s_sq;
         // columns j, j+1: rows [0, j + 2) of A and B, all rows of Z
-        for (int i = threadIdx.x; i < j + 2; i += blockDim.x) {
-            rot_real(at(a.A, a.lda, i, j), at(a.A, a.lda, i, j + 1), cz, sz);
-            rot_real(at(a.B, a.ldb, i, j), at(a.B, a.ldb, i, j + 1), cz, sz);
+        {
+            const int m2 = j + 2;
+            auto rc = [&](R &x, R &y) { rot_real(x, y, cz, sz); };
+            rot_pass<kBatchOf<R>, R>(2 * m2,
+                           [&](int i) -> R & { return i < m2 ? at(a.A, a.lda, i, j) : at(a.B, a.ldb, i - m2, j); },
+                           [&](int i) -> R & {
+                               return i < m2 ? at(a.A, a.lda, i, j + 1) : at(a.B, a.ldb, i - m2, j + 1);
+                           },
+                           rc);
+            if (a.wantz)
+                rot_pass<kBatchOf<R>, R>(a.n, [&](int i) -> R & { return at(a.Z, a.ldz, i, j); },
+                               [&](int i) -> R & { return at(a.Z, a.ldz, i, j + 1); }, rc);
         }
-        if (a.wantz)
-            for (int i = threadIdx.x; i < a.n; i += blockDim.x)
-                rot_real(at(a.Z, a.ldz, i, j), at(a.Z, a.ldz, i, j + 1), cz, sz);
         __syncthreads();  // the 2x2 block takes the column rotation before the row rotation
         // rows j, j+1: columns [j, n) of A and B; Q's columns j, j+1
-        for (int c = j + threadIdx.x; c < a.n; c += blockDim.x) {
-            rot_real(at(a.A, a.lda, j, c), at(a.A, a.lda, j + 1, c), cq, sq);
-            rot_real(at(a.B, a.ldb, j, c), at(a.B, a.ldb, j + 1, c), cq, sq);
+        {
+            const int m2 = a.n - j;
+            auto rr = [&](R &x, R &y) { rot_real(x, y, cq, sq); };
+            rot_pass<kBatchOf<R>, R>(2 * m2,
+                           [&](int i) -> R & { return i < m2 ? at(a.A, a.lda, j, j + i) : at(a.B, a.ldb, j, j + i - m2); },
+                           [&](int i) -> R & {
+                               return i < m2 ? at(a.A, a.lda, j + 1, j + i) : at(a.B, a.ldb, j + 1, j + i - m2);
+                           },
+                           rr);
+            if (a.wantq)
+                rot_pass<kBatchOf<R>, R>(a.n, [&](int i) -> R & { return at(a.Q, a.ldq, i, j); },
+                               [&](int i) -> R & { return at(a.Q, a.ldq, i, j + 1); }, rr);
         }
-        if (a.wantq)
-            for (int i = threadIdx.x; i < a.n; i += blockDim.x)
-                rot_real(at(a.Q, a.ldq, i, j), at(a.Q, a.ldq, i, j + 1), cq, sq);
         __syncthreads();
         if (threadIdx.x == 0) {
             at(a.A, a.lda, j + 1, j) = R(0);
