@@ -231,7 +231,7 @@ int xtgevc3_ctgsna_dev(void *stream, char job, char howmny, const int *select, i
  * is the first row of that swap (as in LAPACK); INFO = -3 N, -5 LDA, -7 LDB, -9 LDQ,
  * -11 LDZ, -12 IFST, -13 ILST.  Complex arrays interleaved.  Device forms: A, B, Q, Z
  * device pointers, the call returns once the reordering is done (0, or 1 when a CUDA call
- * failed).  Real pencils: the D/STGEXC entry points below (1x1 blocks). */
+ * failed).  Real pencils: the D/STGEXC entry points below. */
 void xtgevc3_ztgexc(int wantq, int wantz, int n, double *A, int lda, double *B, int ldb, double *Q, int ldq, double *Z,
                     int ldz, int ifst, int *ilst, int *info);
 void xtgevc3_ctgexc(int wantq, int wantz, int n, float *A, int lda, float *B, int ldb, float *Q, int ldq, float *Z,
@@ -241,23 +241,29 @@ int xtgevc3_ztgexc_dev(void *stream, int wantq, int wantz, int n, double *A, int
 int xtgevc3_ctgexc_dev(void *stream, int wantq, int wantz, int n, float *A, int lda, float *B, int ldb, float *Q,
                        int ldq, float *Z, int ldz, int ifst, int *ilst, int *info);
 
-/* ---- eigenvalue reordering, real pencils with 1x1 blocks: D/STGEXC (no counterpart upstream)
- * LAPACK DTGEXC / STGEXC's arguments, INFO codes and results for moves whose rows (from the
- * row above the lower of ifst, ilst to the row below the higher) hold only 1x1 diagonal
- * blocks of the real generalized Schur pencil (A quasi-upper triangular, B upper
- * triangular): swaps of adjacent real eigenvalues by two rotations each, as LAPACK's
- * D/STGEX2 do them.  A move that would cross or start in a 2x2 block (a complex pair)
- * leaves everything unchanged and sets INFO = 2 (not a LAPACK code) with a message in
- * xtgevc3_last_error().  Other codes, *ilst and the device forms as for the complex
- * entry points above. */
+/* ---- eigenvalue reordering, real pencils: D/STGEXC (no counterpart upstream) --------------
+ * LAPACK DTGEXC / STGEXC's arguments, INFO codes and results (Fortran references become
+ * pointers for in/out arguments, values for inputs): the diagonal block (1x1, or 2x2 for a
+ * complex pair) at row *ifst of the real generalized Schur pencil (A quasi-upper
+ * triangular, B upper triangular) moves to row *ilst by swaps of adjacent diagonal blocks
+ * (LAPACK D/STGEX2: two rotations for two 1x1 blocks, otherwise the direct swapping method
+ * through a small generalized Sylvester equation, with each new 2x2 block standardised).
+ * As in LAPACK, *ifst and *ilst move to the first row of their 2x2 blocks, *ilst is
+ * adjusted for the block sizes and returns the block's row; INFO = 1 (a swap failed the
+ * stability tests; the pencil is reordered up to it and *ilst is where the block is).  Q
+ * and Z agree with LAPACK's to rounding for swaps of 1x1 blocks; a swap involving a 2x2
+ * block has a choice between two re-triangularisations that LAPACK decides on rounding
+ * noise, so there the columns of Q and Z (and the rows and columns of A and B) agree with
+ * LAPACK's up to sign.  Other codes and the device forms as for the complex entry points
+ * above. */
 void xtgevc3_dtgexc(int wantq, int wantz, int n, double *A, int lda, double *B, int ldb, double *Q, int ldq, double *Z,
-                    int ldz, int ifst, int *ilst, int *info);
+                    int ldz, int *ifst, int *ilst, int *info);
 void xtgevc3_stgexc(int wantq, int wantz, int n, float *A, int lda, float *B, int ldb, float *Q, int ldq, float *Z,
-                    int ldz, int ifst, int *ilst, int *info);
+                    int ldz, int *ifst, int *ilst, int *info);
 int xtgevc3_dtgexc_dev(void *stream, int wantq, int wantz, int n, double *A, int lda, double *B, int ldb, double *Q,
-                       int ldq, double *Z, int ldz, int ifst, int *ilst, int *info);
+                       int ldq, double *Z, int ldz, int *ifst, int *ilst, int *info);
 int xtgevc3_stgexc_dev(void *stream, int wantq, int wantz, int n, float *A, int lda, float *B, int ldb, float *Q,
-                       int ldq, float *Z, int ldz, int ifst, int *ilst, int *info);
+                       int ldq, float *Z, int ldz, int *ifst, int *ilst, int *info);
 
 /* ---- allocation-free device entry point (no counterpart in the upstream library) -----
  * Same computation and arguments as xtgevc3_dtgevc3_dev (without flags), for callers that

@@ -277,6 +277,50 @@ def lapack_tgexc_ilst(A, B, Q, Z, ifst, ilst):
     return A, B, Q, Z, l_.value, info.value
 
 
+def _real_fortran_args(A, B, Q, Z):
+    n = A.shape[0]
+    wq, wz = Q is not None, Z is not None
+    A, B = (np.asfortranarray(M).copy(order="F") for M in (A, B))
+    Q = np.asfortranarray(Q).copy(order="F") if wq else np.eye(n, dtype=A.dtype, order="F")
+    Z = np.asfortranarray(Z).copy(order="F") if wz else np.eye(n, dtype=A.dtype, order="F")
+    return n, wq, wz, A, B, Q, Z
+
+
+def lapack_tgexc_real(A, B, Q, Z, ifst, ilst):
+    """LAPACK DTGEXC / STGEXC called through its Fortran interface in SciPy's OpenBLAS, so
+    that IFST and ILST on exit are returned too (moved to the first row of their 2x2 blocks;
+    on a rejected swap ILST is the row the block had reached).  Q, Z None: WANTQ / WANTZ
+    false.  Returns (A, B, Q, Z, ifst, ilst, info)."""
+    pfx = {np.float64: "d", np.float32: "s"}[A.dtype.type]
+    f = getattr(_openblas(), f"scipy_{pfx}tgexc_")
+    n, wq, wz, A, B, Q, Z = _real_fortran_args(A, B, Q, Z)
+    iv = lambda v: ct.byref(ct.c_int(v))  # noqa: E731
+    f_, l_, info = ct.c_int(ifst), ct.c_int(ilst), ct.c_int(0)
+    lwork = 4 * n + 16
+    work = np.zeros(lwork, dtype=A.dtype)
+    ld = max(n, 1)
+    f(iv(int(wq)), iv(int(wz)), iv(n), _ptr(A), iv(ld), _ptr(B), iv(ld), _ptr(Q), iv(ld), _ptr(Z), iv(ld),
+      ct.byref(f_), ct.byref(l_), _ptr(work), iv(lwork), ct.byref(info))
+    return A, B, (Q if wq else None), (Z if wz else None), f_.value, l_.value, info.value
+
+
+def lapack_tgex2_real(A, B, Q, Z, j1, n1, n2):
+    """LAPACK DTGEX2 / STGEX2 (one swap of the adjacent diagonal blocks of sizes n1, n2 at
+    row j1, 1-based) through its Fortran interface in SciPy's OpenBLAS.  Returns (A, B, Q, Z,
+    info); info = 1: the swap was rejected and the pencil left as it was."""
+    pfx = {np.float64: "d", np.float32: "s"}[A.dtype.type]
+    f = getattr(_openblas(), f"scipy_{pfx}tgex2_")
+    n, wq, wz, A, B, Q, Z = _real_fortran_args(A, B, Q, Z)
+    iv = lambda v: ct.byref(ct.c_int(v))  # noqa: E731
+    info = ct.c_int(0)
+    lwork = max(1, n * (n1 + n2), 2 * (n1 + n2) ** 2) + 64
+    work = np.zeros(lwork, dtype=A.dtype)
+    ld = max(n, 1)
+    f(iv(int(wq)), iv(int(wz)), iv(n), _ptr(A), iv(ld), _ptr(B), iv(ld), _ptr(Q), iv(ld), _ptr(Z), iv(ld),
+      iv(j1), iv(n1), iv(n2), _ptr(work), iv(lwork), ct.byref(info))
+    return A, B, (Q if wq else None), (Z if wz else None), info.value
+
+
 def complex_schur_pencil(n, seed, dtype=np.complex128):
     """Complex generalized Schur form (LAPACK xGGES through SciPy's qz) of a pencil with iid
     complex N(0,1) entries: returns (A, B, Q, Z) with the original pencil = (Q A Z^H, Q B Z^H)."""

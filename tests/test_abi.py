@@ -296,6 +296,32 @@ def test_tgexc_info_codes_and_quick_returns():
     assert (A == A0).all()
 
 
+@pytest.mark.parametrize("pfx,dt", [("d", np.float64), ("s", np.float32)])
+def test_real_tgexc_info_codes_and_quick_returns(pfx, dt):
+    """xtgevc3_dtgexc / stgexc (IFST by pointer, in and out as in D/STGEXC): LAPACK's INFO
+    codes in its order, answered before any CUDA call with IFST and ILST untouched, and the
+    N <= 1 quick return."""
+    n = 5
+    A = np.asfortranarray(np.triu(np.arange(1.0, n * n + 1).reshape(n, n)).astype(dt))
+    A0 = A.copy()
+    f = getattr(X.lib(), f"xtgevc3_{pfx}tgexc")
+
+    def call(wq=1, wz=1, nn=n, lda=n, ldb=n, ldq=n, ldz=n, ifst=1, ilst=3):
+        fs, il, info = ct.c_int(ifst), ct.c_int(ilst), ct.c_int(7)
+        f(wq, wz, nn, A.ctypes.data, lda, A.ctypes.data, ldb, A.ctypes.data, ldq, A.ctypes.data, ldz, ct.byref(fs),
+          ct.byref(il), ct.byref(info))
+        return info.value, fs.value, il.value
+    assert call(nn=-1)[0] == -3
+    assert call(lda=n - 1)[0] == -5
+    assert call(ldb=n - 1)[0] == -7
+    assert call(ldq=0, wq=0)[0] == -9
+    assert call(ldz=n - 1)[0] == -11
+    assert call(ifst=0) == (-12, 0, 3) and call(ifst=n + 1)[0] == -12
+    assert call(ilst=0) == (-13, 1, 0) and call(ilst=n + 1)[0] == -13
+    assert call(nn=1, ifst=1, ilst=1, lda=1, ldb=1, ldq=1, ldz=1) == (0, 1, 1)
+    assert (A == A0).all()
+
+
 def test_tgexc_python_wrapper_argument_errors():
     """xtgevc3_b200.tgexc passes 1-based positions through: out-of-range IFST / ILST come back
     as LAPACK's -12 / -13 (no CUDA call), with the arrays unchanged."""

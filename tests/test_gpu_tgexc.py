@@ -1,11 +1,14 @@
-"""xtgevc3_{z,c}tgexc (eigenvalue reordering of a complex generalized Schur pencil) against
-LAPACK ZTGEXC / CTGEXC.
+"""xtgevc3_{z,c,d,s}tgexc (eigenvalue reordering of a generalized Schur pencil) against LAPACK
+Z/C/D/STGEXC.
 
-The oracle is LAPACK's own xTGEXC from SciPy, given the same pencil (the complex generalized
-Schur form of a pencil with iid complex N(0,1) entries, LAPACK xGGES through SciPy's qz)
-and the same move.  Both apply the same rotations with real cosines >= 0, so A, B, Q and Z
-agree to rounding.  Tolerance: elementwise difference relative to the matrix's largest
-entry, 1e-12 (double) / 2e-4 (single).
+The oracle is LAPACK's own xTGEXC from SciPy, given the same pencil (complex: the generalized
+Schur form of a pencil with iid complex N(0,1) entries, LAPACK xGGES through SciPy's qz; real:
+LAPACK DGGES of iid N(0,1) pencils, and constructed pencils for rejected and splitting
+swaps) and the same move.  Swaps of 1x1 blocks apply the same rotations as LAPACK, so A, B, Q
+and Z agree to rounding; swaps involving a real 2x2 block agree up to the sign of each
+column of Q and Z (see the block tests below).  Tolerance: elementwise difference relative
+to the matrix's largest entry, 1e-12 (double) / 2e-4 (single) per move, 1e-11 / 1e-10 for
+long block moves.
 """
 import numpy as np
 import pytest
@@ -155,15 +158,102 @@ def test_real_tgexc_device_form_and_no_qz(cuda_ok):
     assert _rel(da.t().cpu().numpy().T, ra) < 1e-12 and _rel(db.t().cpu().numpy().T, rb) < 1e-12
 
 
-def test_real_tgexc_refuses_moves_across_2x2_blocks(cuda_ok):
-    """A real xGGES pencil has 2x2 blocks (complex pairs): a move across one is not done,
-    INFO = 2 with a message, and A, B, Q, Z are returned unchanged."""
+# ---- real pencils with 2x2 blocks: the block kernel ---------------------------------------
+# Parity rules as for the CPU build of the same arithmetic (test_tgexc_blocks_host.py): IFST,
+# ILST and INFO exactly as LAPACK D/STGEXC, the arrays to rounding up to the sign of each
+# column of Q and Z (LAPACK's choice between its RQ and QR re-triangularisation of a swapped
+# 2x2 block is decided by rounding noise), splitting blocks by invariants.
+from test_tgexc_blocks_host import (_near_double_pencil, _twin_blocks_pencil, blocks_of,  # noqa: E402
+                                    sign_aligned)
+
+BLOCK_MOVES = [(1, 40), (40, 1), (7, 33), (33, 7), (20, 21), (21, 20), (2, 39), (39, 2)]
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32], ids=["d", "s"])
+@pytest.mark.parametrize("move", BLOCK_MOVES, ids=lambda m: f"{m[0]}to{m[1]}")
+def test_real_tgexc_blocks_match_lapack(cuda_ok, dt, move):
+    """Moves through a real xGGES pencil (n = 40, most eigenvalues complex pairs)."""
     from xtgevc3_b200 import pencils
-    S, P, ar, ai, be, Q, Z = pencils.gen_gges(60, 31)
-    k = int(np.flatnonzero(ai > 0)[0])  # first row of a 2x2 block
-    ifst, ilst = (k + 3, 1) if k + 3 <= 60 else (60, 1)
-    a, b, q, z, il, info = X.tgexc(S, P, Q, Z, ifst, ilst)
-    assert info == 2 and "2x2" in X.last_error()
-    assert il == ilst
-    for M, R in ((a, S), (b, P), (q, Q), (z, Z)):
-        np.testing.assert_array_equal(M, R)
+    S, P, _, _, _, Q, Z = pencils.gen_gges(40, 31, dtype=dt)
+    assert len(blocks_of(S)) < 40  # 2x2 blocks present
+    r = oracle.lapack_tgexc_real(S, P, Q, Z, *move)
+    a, b, q, z, f, il, info = X.tgexc(S, P, Q, Z, *move, with_ifst=True)
+    assert (f, il, info) == r[4:], (move, (f, il, info), r[4:])
+    a, b, q, z = sign_aligned(a, b, q, z, r[2], r[3])
+    for M, R in ((a, r[0]), (b, r[1]), (q, r[2]), (z, r[3])):
+        assert _rel(M, R) < {np.float64: 1e-11, np.float32: 1e-4}[dt]
+
+
+def test_real_tgexc_blocks_long_move(cuda_ok):
+    """n = 400, the last block to the top and back: LAPACK's IFST / ILST / INFO, its arrays
+    up to column signs, and Q A Z^T, Q B Z^T unchanged."""
+    from xtgevc3_b200 import pencils
+    S, P, _, _, _, Q, Z = pencils.gen_gges(400, 5)
+    for move in ((400, 1), (1, 400)):
+        r = oracle.lapack_tgexc_real(S, P, Q, Z, *move)
+        a, b, q, z, f, il, info = X.tgexc(S, P, Q, Z, *move, with_ifst=True)
+        assert (f, il, info) == r[4:], move
+        for M, M0 in ((a, S), (b, P)):
+            assert np.abs(q @ M @ z.T - Q @ M0 @ Z.T).max() < 1e-12 * np.abs(M0).max() * 400
+        a, b, q, z = sign_aligned(a, b, q, z, r[2], r[3])
+        for M, R in ((a, r[0]), (b, r[1]), (q, r[2]), (z, r[3])):
+            assert _rel(M, R) < 1e-10
+
+
+@pytest.mark.parametrize("move", [(4, 2), (2, 5), (5, 1), (6, 1), (1, 6)], ids=lambda m: f"{m[0]}to{m[1]}")
+def test_real_tgexc_blocks_rejections(cuda_ok, move):
+    """Two identical 2x2 blocks: their swap is rejected (INFO = 1, the pencil as LAPACK
+    leaves it, ILST where the block stopped, IFST moved to its block's first row)."""
+    A, B, Q, Z = _twin_blocks_pencil(1)
+    r = oracle.lapack_tgexc_real(A, B, Q, Z, *move)
+    a, b, q, z, f, il, info = X.tgexc(A, B, Q, Z, *move, with_ifst=True)
+    assert (f, il, info) == r[4:], (move, (f, il, info), r[4:])
+    a, b, q, z = sign_aligned(a, b, q, z, r[2], r[3])
+    for M, R in ((a, r[0]), (b, r[1]), (q, r[2]), (z, r[3])):
+        assert _rel(M, R) < 1e-12
+
+
+def test_real_tgexc_blocks_splitting(cuda_ok):
+    """Near-double 2x2 blocks that LAPACK's walk splits: INFO and ILST as LAPACK, the pencil
+    kept, the two eigenvalues at rows ILST, ILST + 1 (to 1e-6)."""
+    import scipy.linalg
+    done = 0
+    for seed in range(200):
+        A, B, Q, Z = _near_double_pencil(seed)
+        move = (3, 8) if seed % 2 == 0 else (3, 1)
+        r = oracle.lapack_tgexc_real(A, B, Q, Z, *move)
+        if r[6] != 0 or len(blocks_of(r[0])) == len(blocks_of(A)):
+            continue
+        a, b, q, z, f, il, info = X.tgexc(A, B, Q, Z, *move, with_ifst=True)
+        assert (f, il, info) == r[4:], seed
+        for M, M0 in ((a, A), (b, B)):
+            assert np.abs(q @ M @ z.T - Q @ M0 @ Z.T).max() < 1e-13 * np.abs(M0).max() * 8
+        moved = np.sort_complex(scipy.linalg.eigvals(A[2:4, 2:4], B[2:4, 2:4]))
+        here = np.sort_complex(scipy.linalg.eigvals(a[il - 1:il + 1, il - 1:il + 1], b[il - 1:il + 1, il - 1:il + 1]))
+        assert np.abs(moved - here).max() < 1e-6 * max(1.0, np.abs(moved).max()), seed
+        done += 1
+        if done == 6:
+            break
+    assert done >= 4
+
+
+def test_real_tgexc_blocks_device_form(cuda_ok):
+    """xtgevc3_dtgexc_dev on column-major CUDA tensors: the host form's arrays and IFST /
+    ILST bit for bit; without Q and Z the same A and B."""
+    import torch
+    from xtgevc3_b200 import pencils
+    S, P, _, _, _, Q, Z = pencils.gen_gges(96, 12)
+    a, b, q, z, f, il, info = X.tgexc(S, P, Q, Z, 90, 4, with_ifst=True)
+
+    def dev(M):
+        return torch.from_numpy(np.ascontiguousarray(M.T)).cuda().t()
+
+    dA, dB, dQ, dZ = dev(S), dev(P), dev(Q), dev(Z)
+    assert X.tgexc_dev(dA, dB, dQ, dZ, 90, 4, with_ifst=True) == (f, il, info)
+    torch.cuda.synchronize()
+    for D, H in ((dA, a), (dB, b), (dQ, q), (dZ, z)):
+        np.testing.assert_array_equal(D.cpu().numpy(), H)
+    dA, dB = dev(S), dev(P)
+    assert X.tgexc_dev(dA, dB, None, None, 90, 4, with_ifst=True) == (f, il, info)
+    np.testing.assert_array_equal(dA.cpu().numpy(), a)
+    np.testing.assert_array_equal(dB.cpu().numpy(), b)

@@ -117,6 +117,13 @@ def lib():
             f = getattr(L, f"xtgevc3_{p}tgexc_dev")
             f.argtypes = [_P, _I, _I, _I, _P, _I, _P, _I, _P, _I, _P, _I, _I, _P, _P]
             f.restype = _I
+        for p in "ds":  # xTGEXC, real pencils: IFST in and out
+            f = getattr(L, f"xtgevc3_{p}tgexc")
+            f.argtypes = [_I, _I, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _P, _P]
+            f.restype = None
+            f = getattr(L, f"xtgevc3_{p}tgexc_dev")
+            f.argtypes = [_P, _I, _I, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _P, _P]
+            f.restype = _I
         for p in "dszc":
             f = getattr(L, f"xtgevc3_{p}trevc3_dev")
             f.argtypes = [_U, _P, _C, _C, _P, _I, _P, _I, _P, _I, _P, _I, _I, _P, _P]
@@ -391,11 +398,12 @@ def tgsna(howmny, A, B, VL, VR, select=None, job="E"):
     return S[:m.value], m.value, info.value
 
 
-def tgexc(A, B, Q=None, Z=None, ifst=1, ilst=1):
-    """Host-array form of z/c/d/stgexc: move the eigenvalue at row ifst of the generalized
-    Schur pencil (A, B) to row ilst (1-based, as LAPACK), updating Q and Z when given.  Real
-    pencils: moves across 1x1 blocks only (info = 2 and the pencil unchanged when a 2x2
-    block is in the way).  Returns (A, B, Q, Z, ilst, info) with new arrays."""
+def tgexc(A, B, Q=None, Z=None, ifst=1, ilst=1, with_ifst=False):
+    """Host-array form of z/c/d/stgexc: move the eigenvalue (real pencils: the 1x1 or 2x2
+    diagonal block) at row ifst of the generalized Schur pencil (A, B) to row ilst (1-based,
+    as LAPACK), updating Q and Z when given.  Returns (A, B, Q, Z, ilst, info) with new
+    arrays, or (A, B, Q, Z, ifst, ilst, info) with with_ifst (real pencils: IFST moves to the
+    first row of its 2x2 block, as in D/STGEXC)."""
     L = lib()
     dt = A.dtype.type
     pfx = {np.complex128: "z", np.complex64: "c", np.float64: "d", np.float32: "s"}[dt]
@@ -403,24 +411,27 @@ def tgexc(A, B, Q=None, Z=None, ifst=1, ilst=1):
     A, B = np.array(A, order="F", dtype=dt), np.array(B, order="F", dtype=dt)
     Qc = None if Q is None else np.array(Q, order="F", dtype=dt)
     Zc = None if Z is None else np.array(Z, order="F", dtype=dt)
-    il, info = ct.c_int(ilst), ct.c_int(0)
+    fs, il, info = ct.c_int(ifst), ct.c_int(ilst), ct.c_int(0)
     ld = max(n, 1)
     getattr(L, f"xtgevc3_{pfx}tgexc")(int(Qc is not None), int(Zc is not None), n, _ptr(A), ld, _ptr(B), ld, _ptr(Qc),
-                                      ld, _ptr(Zc), ld, ifst, ct.byref(il), ct.byref(info))
+                                      ld, _ptr(Zc), ld, ct.byref(fs) if pfx in "ds" else ifst, ct.byref(il),
+                                      ct.byref(info))
     if info.value == 1 and last_error():  # a rejected swap (INFO = 1) leaves no error text
         raise RuntimeError(f"xtgevc3_{pfx}tgexc failed: {last_error()}")
+    if with_ifst:
+        return A, B, Qc, Zc, fs.value, il.value, info.value
     return A, B, Qc, Zc, il.value, info.value
 
 
-def tgexc_dev(A, B, Q=None, Z=None, ifst=1, ilst=1, stream=None):
+def tgexc_dev(A, B, Q=None, Z=None, ifst=1, ilst=1, stream=None, with_ifst=False):
     """Device form of z/c/d/stgexc on column-major CUDA tensors (reordered in place).  Returns
-    (ilst, info)."""
+    (ilst, info), or (ifst, ilst, info) with with_ifst."""
     import torch
     L = lib()
     pfx = {torch.complex128: "z", torch.complex64: "c", torch.float64: "d", torch.float32: "s"}[A.dtype]
     n = A.shape[0]
     st = ct.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
-    il, info = ct.c_int(ilst), ct.c_int(0)
+    fs, il, info = ct.c_int(ifst), ct.c_int(ilst), ct.c_int(0)
 
     def ld(t):
         return max(t.stride(1), 1) if t is not None else max(n, 1)
@@ -429,10 +440,12 @@ def tgexc_dev(A, B, Q=None, Z=None, ifst=1, ilst=1, stream=None):
         return ct.c_void_p(t.data_ptr()) if t is not None else None
 
     rc = getattr(L, f"xtgevc3_{pfx}tgexc_dev")(st, int(Q is not None), int(Z is not None), n, ptr(A), ld(A), ptr(B),
-                                              ld(B), ptr(Q), ld(Q), ptr(Z), ld(Z), ifst, ct.byref(il),
-                                              ct.byref(info))
+                                              ld(B), ptr(Q), ld(Q), ptr(Z), ld(Z),
+                                              ct.byref(fs) if pfx in "ds" else ifst, ct.byref(il), ct.byref(info))
     if rc:
         raise RuntimeError(f"xtgevc3_{pfx}tgexc_dev failed: {last_error()}")
+    if with_ifst:
+        return fs.value, il.value, info.value
     return il.value, info.value
 
 

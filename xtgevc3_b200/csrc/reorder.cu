@@ -28,13 +28,14 @@
 // conventions: with (cs, sn) the rotation [cs sn; -sn cs] [F; G] = [r; 0] (cs >= 0, r of
 // F's sign; F = s11 t00 - t11 s00, G = s11 t01 - t11 s01), the columns take (c, s) =
 // (sn, -cs), the rows the rotation that zeroes the new (1, 0) entry of S or T, both applied
-// as (x, y) <- (c x + s y, c y - s x); Z takes the column rotation, Q the row rotation.  A
-// move across or into a 2x2 block (a complex pair; the real routine's general swap through a
-// small generalized Sylvester equation) is not done: the pencil is left unchanged, INFO = 2
-// and xtgevc3_last_error() says so.
+// as (x, y) <- (c x + s y, c y - s x); Z takes the column rotation, Q the row rotation.
+// Moves across or of 2x2 blocks (complex pairs) run the general walk and swaps of
+// tgexc_real_blocks.cuh (a small generalized Sylvester equation per swap, LAPACK's block
+// walk with its 2x2 splits); IFST is in and out there, as in D/STGEXC.
 #include "../../include/xtgevc3.h"
 #include "common.cuh"
 #include "engine.cuh"
+#include "tgexc_real_blocks.cuh"
 
 #include <algorithm>
 #include <string>
@@ -440,6 +441,72 @@ __global__ void __launch_bounds__(kReorderThreads, 1) tgexc_real_kernel(ReorderA
     }
 }
 
+// Real pencils with 2x2 blocks in the rows of the move (the general D/STGEXC walk and D/STGEX2
+// swaps of tgexc_real_blocks.cuh).  Thread 0 walks and computes each swap's small-block
+// arithmetic; the CTA applies the swap (O(n) rows and columns) between barriers.  The walk
+// moves the block at least one row every two swaps, so it ends within 4 n + 16 swaps; the
+// loop is bounded by that count all the same (status 3 if it were ever reached).
+// status: {ILST on exit (1-based), INFO (0 / 1 / 3), IFST on exit (1-based)}
+template <class R>
+__global__ void __launch_bounds__(kReorderThreads, 1)
+    tgexc_real_blocks_kernel(rb::Pencil<R> p, int ifst, int ilst, int *status)
+{
+    __shared__ rb::Swap<R> s;
+    __shared__ rb::Walk w;
+    __shared__ int s_go, s_ifst, s_ilst, s_info;
+    if (threadIdx.x == 0) {
+        int f = ifst, l = ilst;
+        s_go = (p.n > 1 && rb::walk_begin(p, w, f, l)) ? 1 : 0;
+        s_ifst = f;
+        s_ilst = l;
+        s_info = 0;
+        s.ok = 0;
+        s.n1 = s.n2 = 1;
+    }
+    const int limit = 4 * p.n + 16;
+    for (int it = 0;; it++) {
+        if (threadIdx.x == 0 && s_go) {
+            int j1, n1, n2;
+            if (it >= limit) {
+                s_go = 0;
+                s_info = 3;
+            } else if (!rb::walk_next(p, w, j1, n1, n2)) {
+                s_go = 0;
+                s_ilst = w.here;
+            } else {
+                s.j1 = j1 - 1;
+                s.n1 = n1;
+                s.n2 = n2;
+                rb::swap_prepare(p, s);
+                if (s.ok == 0) {
+                    s_go = 0;
+                    s_ilst = w.here;
+                    s_info = 1;
+                }
+            }
+        }
+        __syncthreads();  // (1): the decision and the swap are visible to the CTA
+        const int go = s_go, ok = s.ok, m = s.n1 + s.n2;
+        if (!go) break;
+        if (ok == 1) {
+            rb::swap_apply(p, s, 0, threadIdx.x, blockDim.x);
+            if (m == 2) {
+                __syncthreads();  // the 2x2 block takes the column rotation before the row rotation
+                rb::swap_apply(p, s, 1, threadIdx.x, blockDim.x);
+                __syncthreads();
+                rb::swap_apply(p, s, 2, threadIdx.x, blockDim.x);
+            }
+        }
+        __syncthreads();  // (2): the swap is in memory before thread 0 reads A again
+        if (threadIdx.x == 0) rb::walk_after(p, w);
+    }
+    if (threadIdx.x == 0) {
+        status[0] = s_ilst;
+        status[1] = s_info;
+        status[2] = s_ifst;
+    }
+}
+
 // LAPACK xTGEXC's argument checks, in its order.
 int tgexc_check(int wantq, int wantz, int n, int lda, int ldb, int ldq, int ldz, int ifst, int ilst)
 {
@@ -537,30 +604,42 @@ void tgexc_host(int wantq, int wantz, int n, cplx<R> *A, int lda, cplx<R> *B, in
     }
 }
 
-// Real pencils, device pointers: as tgexc_device (INFO = 2: a 2x2 block in the move's rows,
-// nothing done).
+// Real pencils, device pointers: as tgexc_device, with IFST in and out as in D/STGEXC (moved to
+// the first row of its 2x2 block).  A move whose rows hold only 1x1 blocks runs the rotation
+// kernel; when that kernel finds a 2x2 block in the way (status 2, nothing changed) the block
+// kernel does the move.
 template <class R>
 int tgexc_device_real(cudaStream_t st, int wantq, int wantz, int n, R *A, int lda, R *B, int ldb, R *Q, int ldq, R *Z,
-                      int ldz, int ifst, int *ilst, int *info)
+                      int ldz, int *ifst, int *ilst, int *info)
 {
     set_last_error("");
-    *info = tgexc_check(wantq, wantz, n, lda, ldb, ldq, ldz, ifst, *ilst);
+    *info = tgexc_check(wantq, wantz, n, lda, ldb, ldq, ldz, *ifst, *ilst);
     if (*info) {
         set_last_error("xTGEXC: argument " + std::to_string(-*info) + " has an illegal value");
         return 0;
     }
-    if (n <= 1 || ifst == *ilst) return 0;
+    if (n <= 1) return 0;  // IFST = ILST still runs: LAPACK moves both to their blocks' first rows
     int *d_status = nullptr;
-    int h_status[2] = {0, 0};
-    cudaError_t e = cudaMallocAsync(&d_status, 2 * sizeof(int), st);
+    int h_status[3] = {0, 0, 0};
+    cudaError_t e = cudaMallocAsync(&d_status, 3 * sizeof(int), st);
+    bool blocks = false;
     if (e == cudaSuccess) {
-        ReorderArgsReal<R> ra{n, ifst - 1, *ilst - 1, wantq ? 1 : 0, wantz ? 1 : 0, A, B, Q, Z, lda, ldb, ldq, ldz,
+        ReorderArgsReal<R> ra{n, *ifst - 1, *ilst - 1, wantq ? 1 : 0, wantz ? 1 : 0, A, B, Q, Z, lda, ldb, ldq, ldz,
                               d_status};
         tgexc_real_kernel<R><<<1, kReorderThreads, 0, st>>>(ra);
         count_launches(1);
         e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaMemcpyAsync(h_status, d_status, sizeof(h_status), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h_status, d_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e == cudaSuccess && h_status[1] == 2) {
+            blocks = true;
+            rb::Pencil<R> p{n, wantq ? 1 : 0, wantz ? 1 : 0, A, B, Q, Z, lda, ldb, ldq, ldz};
+            tgexc_real_blocks_kernel<R><<<1, kReorderThreads, 0, st>>>(p, *ifst, *ilst, d_status);
+            count_launches(1);
+            e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaMemcpyAsync(h_status, d_status, sizeof(h_status), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        }
         cudaFreeAsync(d_status, st);
     }
     if (e != cudaSuccess) {
@@ -568,28 +647,34 @@ int tgexc_device_real(cudaStream_t st, int wantq, int wantz, int n, R *A, int ld
         *info = 1;
         return 1;
     }
-    *info = h_status[1];
-    if (*info == 2) {
-        set_last_error("xTGEXC (real): a 2x2 diagonal block (complex pair) lies in the rows of the move; only moves "
-                       "across 1x1 blocks are supported, the pencil is unchanged");
+    if (!blocks) {
+        *info = h_status[1];
+        *ilst = h_status[0] + 1;
         return 0;
     }
-    *ilst = h_status[0] + 1;
+    if (h_status[1] == 3) {
+        set_last_error("xTGEXC (real): the block walk did not end within its swap bound");
+        *info = 1;
+        return 1;
+    }
+    *info = h_status[1];
+    *ilst = h_status[0];
+    *ifst = h_status[2];
     return 0;
 }
 
 // Real pencils, host pointers: as tgexc_host.
 template <class R>
-void tgexc_host_real(int wantq, int wantz, int n, R *A, int lda, R *B, int ldb, R *Q, int ldq, R *Z, int ldz, int ifst,
+void tgexc_host_real(int wantq, int wantz, int n, R *A, int lda, R *B, int ldb, R *Q, int ldq, R *Z, int ldz, int *ifst,
                      int *ilst, int *info)
 {
     set_last_error("");
-    *info = tgexc_check(wantq, wantz, n, lda, ldb, ldq, ldz, ifst, *ilst);
+    *info = tgexc_check(wantq, wantz, n, lda, ldb, ldq, ldz, *ifst, *ilst);
     if (*info) {
         set_last_error("xTGEXC: argument " + std::to_string(-*info) + " has an illegal value");
         return;
     }
-    if (n <= 1 || ifst == *ilst) return;
+    if (n <= 1) return;
     cudaStream_t st = nullptr;
     R *dm[4] = {nullptr, nullptr, nullptr, nullptr};
     R *hm[4] = {A, B, wantq ? Q : nullptr, wantz ? Z : nullptr};
@@ -607,7 +692,7 @@ void tgexc_host_real(int wantq, int wantz, int n, R *A, int lda, R *B, int ldb, 
     if (e == cudaSuccess) {
         rc = tgexc_device_real<R>(st, wantq, wantz, n, dm[0], n, dm[1], n, dm[2] ? dm[2] : dm[0], n,
                                   dm[3] ? dm[3] : dm[0], n, ifst, ilst, info);
-        for (int k = 0; k < 4 && rc == 0 && e == cudaSuccess && *info != 2; k++)
+        for (int k = 0; k < 4 && rc == 0 && e == cudaSuccess; k++)
             if (hm[k])
                 e = cudaMemcpy2DAsync(hm[k], (size_t)hl[k] * sizeof(R), dm[k], (size_t)n * sizeof(R),
                                       (size_t)n * sizeof(R), n, cudaMemcpyDeviceToHost, st);
@@ -667,26 +752,26 @@ int xtgevc3_ctgexc_dev(void *stream, int wantq, int wantz, int n, float *A, int 
 }
 
 void xtgevc3_dtgexc(int wantq, int wantz, int n, double *A, int lda, double *B, int ldb, double *Q, int ldq, double *Z,
-                    int ldz, int ifst, int *ilst, int *info)
+                    int ldz, int *ifst, int *ilst, int *info)
 {
     xtg::tgexc_host_real<double>(wantq, wantz, n, A, lda, B, ldb, Q, ldq, Z, ldz, ifst, ilst, info);
 }
 
 void xtgevc3_stgexc(int wantq, int wantz, int n, float *A, int lda, float *B, int ldb, float *Q, int ldq, float *Z,
-                    int ldz, int ifst, int *ilst, int *info)
+                    int ldz, int *ifst, int *ilst, int *info)
 {
     xtg::tgexc_host_real<float>(wantq, wantz, n, A, lda, B, ldb, Q, ldq, Z, ldz, ifst, ilst, info);
 }
 
 int xtgevc3_dtgexc_dev(void *stream, int wantq, int wantz, int n, double *A, int lda, double *B, int ldb, double *Q,
-                       int ldq, double *Z, int ldz, int ifst, int *ilst, int *info)
+                       int ldq, double *Z, int ldz, int *ifst, int *ilst, int *info)
 {
     return xtg::tgexc_device_real<double>(static_cast<cudaStream_t>(stream), wantq, wantz, n, A, lda, B, ldb, Q, ldq, Z,
                                           ldz, ifst, ilst, info);
 }
 
 int xtgevc3_stgexc_dev(void *stream, int wantq, int wantz, int n, float *A, int lda, float *B, int ldb, float *Q,
-                       int ldq, float *Z, int ldz, int ifst, int *ilst, int *info)
+                       int ldq, float *Z, int ldz, int *ifst, int *ilst, int *info)
 {
     return xtg::tgexc_device_real<float>(static_cast<cudaStream_t>(stream), wantq, wantz, n, A, lda, B, ldb, Q, ldq, Z,
                                          ldz, ifst, ilst, info);
