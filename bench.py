@@ -770,6 +770,62 @@ def measure_tgexc(args, X, torch, real=False):
     return out
 
 
+def measure_tgexc_blocks(args, X, torch):
+    """dtgexc across 2x2 blocks: the last diagonal block of a real generalized Schur pencil of
+    order --tgexc-n (the xGGES-statistics stand-in: about n - sqrt(2n/pi) eigenvalues in
+    standardised 2x2 blocks) moves to the top, Q and Z updated (Q = Z = I); one swap of two
+    2x2 blocks solves a 4 x 4 pair of Sylvester equations (an 8 x 8 Kronecker system) on one
+    thread and updates 4 rows and columns.  Device-resident inputs restored before each
+    step outside the timed region, CUDA-event timing; LAPACK DTGEXC (SciPy's OpenBLAS) on the
+    same input and move beside it, results compared up to the sign of each column of Q and Z
+    (LAPACK's choice between two re-triangularisations of a swapped 2x2 block follows its
+    rounding noise)."""
+    from xtgevc3_b200 import pencils as gen
+    n = args.tgexc_n
+    S_h, P_h = gen.gen_schur_like(n, args.seed + 47)[:2]
+    S0, P0 = colmajor_cuda(S_h, torch), colmajor_cuda(P_h, torch)
+    I0 = torch.eye(n, dtype=torch.float64, device="cuda")
+    A, B, Q, Z = (torch.empty_like(S0) for _ in range(4))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ts, res = [], None
+    warm = max(args.warmup, 1)
+    for it in range(warm + args.steps):
+        A.copy_(S0)
+        B.copy_(P0)
+        Q.copy_(I0)
+        Z.copy_(I0)
+        torch.cuda.synchronize()
+        e0.record()
+        res = X.tgexc_dev(A, B, Q, Z, n, 1, with_ifst=True)
+        e1.record()
+        torch.cuda.synchronize()
+        if it >= warm:
+            ts.append(e0.elapsed_time(e1))
+    ms = float(np.mean(ts))
+    pairs = int((np.diag(S_h, -1) != 0).sum())
+    out = {"n": n, "move": f"{n} -> 1", "pairs_in_pencil": pairs, "ifst_ilst_info": list(res), "ms": ms,
+           "data": "real generalized Schur stand-in (xGGES statistics, standardised 2x2 blocks), Q = Z = I"}
+    if not args.no_cpu:
+        import oracle
+        Ih = np.eye(n, order="F")
+        t0 = time.perf_counter()
+        r = oracle.lapack_tgexc_real(S_h, P_h, Ih, Ih.copy(order="F"), n, 1)
+        tc = time.perf_counter() - t0
+        qd, zd = Q.cpu().numpy(), Z.cpu().numpy()
+        dq = np.where(np.einsum("ij,ij->j", qd, r[2]) < 0, -1.0, 1.0)
+        dz = np.where(np.einsum("ij,ij->j", zd, r[3]) < 0, -1.0, 1.0)
+        diff = 0.0
+        for D, R in ((dq[:, None] * A.cpu().numpy() * dz[None, :], r[0]), (dq[:, None] * B.cpu().numpy() * dz[None, :], r[1]),
+                     (qd * dq[None, :], r[2]), (zd * dz[None, :], r[3])):
+            diff = max(diff, float(np.abs(D - R).max() / np.abs(R).max()))
+        out["cpu_lapack"] = {"seconds": tc, "cores": host_threads(), "ifst_ilst_info": [int(v) for v in r[4:]],
+                             "kind": "LAPACK dtgexc (SciPy OpenBLAS), one call"}
+        out["speedup_vs_lapack"] = tc / (ms * 1e-3)
+        out["max_rel_diff_vs_lapack_up_to_column_signs"] = diff
+    del S0, P0, I0, A, B, Q, Z
+    return out
+
+
 def schur_stand_in(n, seed):
     """Stand-in for the real Schur factor T of an n x n iid N(0,1) matrix (host, Fortran):
     strictly upper part N(0,1); about sqrt(2n/pi) real eigenvalues, uniform on [-sqrt(n),
@@ -1138,6 +1194,7 @@ def main():
     trleg = measure_trevc3(args, X, torch) if args.trevc3_n > 0 and rank == 0 else None
     txleg = measure_tgexc(args, X, torch) if args.tgexc_n > 0 and rank == 0 else None
     dxleg = measure_tgexc(args, X, torch, real=True) if args.tgexc_n > 0 and rank == 0 else None
+    bxleg = measure_tgexc_blocks(args, X, torch) if args.tgexc_n > 0 and rank == 0 else None
 
     if rank == 0:
         form_desc = {"plain": "plain FP64 (DMMA)", "split": f"split precision, {s} BF16 slices (tcgen05)",
@@ -1176,7 +1233,8 @@ def main():
                                "d_max_rel_diff_vs_loop": batched["d"]["max_rel_diff_vs_loop"]}},
                 "forms": forms_out, "clocks": h["clocks"], "e2e": e2e, "gpu_launches": h["launches"],
                 "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "normalize": norm, "batched": batched,
-                "adjoint": adjoint, "ztgevc3": zleg, "dtrevc3": trleg, "ztgexc": txleg, "dtgexc": dxleg}
+                "adjoint": adjoint, "ztgevc3": zleg, "dtrevc3": trleg, "ztgexc": txleg, "dtgexc": dxleg,
+                "dtgexc_blocks": bxleg}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
