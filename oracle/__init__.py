@@ -215,14 +215,19 @@ def lapack_trevc3(side, howmny, T, VL=None, VR=None, select=None, mm=None):
     return VL, VR, m.value, info.value
 
 
-def lapack_tgsna(howmny, A, B, VL, VR, select=None):
-    """Oracle of the xTGSNA entry points: LAPACK xTGSNA (JOB = 'E') from SciPy's bundled
-    OpenBLAS.  Returns (S, m, info)."""
+def lapack_tgsna(howmny, A, B, VL, VR, select=None, job="E"):
+    """Oracle of the xTGSNA entry points: LAPACK xTGSNA from SciPy's bundled OpenBLAS.
+    JOB = 'E' returns (S, m, info); JOB = 'V' / 'B' returns (S, DIF, m, info) (VL, VR may
+    then be None for 'V': not referenced)."""
     dt = A.dtype.type
     pfx = _PREFIX[dt]
     n = A.shape[0]
     f = getattr(_openblas(), f"scipy_{pfx}tgsna_")
     A, B = np.asfortranarray(A), np.asfortranarray(B)
+    if VL is None:
+        VL = np.zeros((max(n, 1), max(n, 1)), dtype=dt, order="F")
+    if VR is None:
+        VR = np.zeros((max(n, 1), max(n, 1)), dtype=dt, order="F")
     VL, VR = np.asfortranarray(VL), np.asfortranarray(VR)
     rdt = np.float64 if pfx in "dz" else np.float32
     mm = VR.shape[1]
@@ -231,14 +236,19 @@ def lapack_tgsna(howmny, A, B, VL, VR, select=None):
     D = np.zeros(max(mm, 1), dtype=rdt)
     iv = lambda v: ct.byref(ct.c_int(v))  # noqa: E731
     m, info = ct.c_int(0), ct.c_int(0)
-    lwork = max(n, 1)
+    if job == "E":
+        lwork = max(n, 1)
+    else:
+        lwork = max(1, 2 * n * (n + 2) + 16) if pfx in "ds" else max(1, 2 * n * n)
     work = np.zeros(lwork, dtype=dt)
     iwork = np.zeros(n + 6, dtype=np.int32)
     ld = max(n, 1)
-    f(ct.c_char_p(b"E"), ct.c_char_p(howmny.encode()), _ptr(sel), iv(n), _ptr(A), iv(ld), _ptr(B), iv(ld), _ptr(VL),
-      iv(ld), _ptr(VR), iv(ld), _ptr(S), _ptr(D), iv(mm), ct.byref(m), _ptr(work), iv(lwork), _ptr(iwork),
+    f(ct.c_char_p(job.encode()), ct.c_char_p(howmny.encode()), _ptr(sel), iv(n), _ptr(A), iv(ld), _ptr(B), iv(ld),
+      _ptr(VL), iv(ld), _ptr(VR), iv(ld), _ptr(S), _ptr(D), iv(mm), ct.byref(m), _ptr(work), iv(lwork), _ptr(iwork),
       ct.byref(info), ct.c_size_t(1), ct.c_size_t(1))
-    return S[:m.value], m.value, info.value
+    if job == "E":
+        return S[:m.value], m.value, info.value
+    return S[:m.value], D[:m.value], m.value, info.value
 
 
 def lapack_tgexc(A, B, Q, Z, ifst, ilst):

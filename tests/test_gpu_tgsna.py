@@ -1,4 +1,5 @@
-"""xtgevc3_{d,s,z,c}tgsna (JOB = 'E': eigenvalue condition numbers) against LAPACK xTGSNA.
+"""xtgevc3_{d,s,z,c}tgsna (JOB = 'E': eigenvalue condition numbers; JOB = 'V' / 'B': the
+eigenvector condition estimates DIF of real pencils) against LAPACK xTGSNA.
 
 The oracle is LAPACK's own xTGSNA from SciPy's bundled OpenBLAS, given the same Schur
 pencil and the same eigenvectors (LAPACK xTGEVC's, in Schur coordinates).  S does not
@@ -76,3 +77,69 @@ def test_tgsna_schur_like_700(cuda_ok):
     got, m, info = X.tgsna("A", S, P, VL, VR)
     assert (m, info) == (n, 0)
     assert _rel(got, ref) < 1e-8, _rel(got, ref)
+
+
+# ---- DIF (JOB = 'V' / 'B', real pencils) -------------------------------------------------
+# DTGSNA's estimate, from a copy reordered per eigenvalue and xTGSYL's +-1 look-ahead; the
+# look-ahead follows the reordered copy's signs, which LAPACK leaves to rounding in swaps of
+# 2x2 blocks (test_tgsna_dif_host.py checks the estimate step exactly on LAPACK's own
+# reordered copies).  Here: most DIFs equal LAPACK's to rounding, every one within a factor
+# of two of LAPACK's, JOB = 'B' gives JOB = 'E''s S and JOB = 'V''s DIF, the device form
+# the host form's values.
+from test_tgsna_dif_host import _twin_blocks_pencil, blocks  # noqa: E402
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32], ids=["d", "s"])
+def test_dif_matches_lapack(cuda_ok, dt):
+    tol = {np.float64: 1e-12, np.float32: 1e-4}[dt]
+    same = total = 0
+    for seed, n in ((1, 9), (2, 24), (3, 40)):
+        S, T = pencils.gen_gges(n, 90 + seed, dtype=dt)[:2]
+        _, d, m, info = oracle.lapack_tgsna("A", S, T, None, None, job="V")
+        s_, h, m2, info2 = X.tgsna("A", S, T, None, None, job="V")
+        assert s_ is None and (m2, info2) == (m, info) == (n, 0)
+        for ks in range(n):
+            total += 1
+            if abs(h[ks] - d[ks]) <= tol * abs(d[ks]):
+                same += 1
+            else:
+                assert 0.5 <= h[ks] / d[ks] <= 2.0, (seed, ks, h[ks], d[ks])
+    assert same >= 0.8 * total, (same, total)
+
+
+def test_dif_job_b_and_device_form(cuda_ok):
+    import torch
+    S, P, ar, ai, be = _pencil(np.float64, 30, 17)
+    VL, VR = oracle.lapack_tgevc(S, P)
+    s_e, m_e, _ = X.tgsna("A", S, P, VL, VR, job="E")
+    _, d_v, m_v, _ = X.tgsna("A", S, P, None, None, job="V")
+    s_b, d_b, m_b, info = X.tgsna("A", S, P, VL, VR, job="B")
+    assert info == 0 and m_e == m_v == m_b == 30
+    np.testing.assert_array_equal(s_b, s_e)
+    np.testing.assert_array_equal(d_b, d_v)
+
+    def dev(M):
+        return torch.from_numpy(np.ascontiguousarray(M.T)).cuda().t()
+
+    d_dev, m, info = X.tgsna_dif_dev(dev(S), dev(P))
+    assert (m, info) == (30, 0)
+    np.testing.assert_array_equal(d_dev.cpu().numpy(), d_v)
+
+
+def test_dif_selection_and_rejection(cuda_ok):
+    """HOWMNY = 'S' (a pair selected by its second row), and a rejected reordering (the
+    second of two identical 2x2 blocks: DIF = 0), as LAPACK."""
+    S, T = pencils.gen_gges(14, 77)[:2]
+    sel = np.zeros(14, dtype=np.int32)
+    sel[[k for k, p in blocks(S) if p][0] + 1] = 1
+    sel[[k for k, p in blocks(S) if not p][:1]] = 1
+    _, d, m, _ = oracle.lapack_tgsna("S", S, T, None, None, select=sel, job="V")
+    _, h, m2, info = X.tgsna("S", S, T, None, None, select=sel, job="V")
+    assert (m2, info) == (m, 0) == (3, 0)
+    assert h[1] == h[2]  # the pair's two entries (the real block at row 0 comes first)
+    assert all(abs(x - y) <= 1e-12 * y or 0.5 <= x / y <= 2.0 for x, y in zip(h, d)), (h, d)
+    A, B = _twin_blocks_pencil(2)
+    _, d, m, _ = oracle.lapack_tgsna("A", A, B, None, None, job="V")
+    _, h, m2, _ = X.tgsna("A", A, B, None, None, job="V")
+    assert d[3] == d[4] == 0
+    np.testing.assert_array_equal(h[3:5], d[3:5])

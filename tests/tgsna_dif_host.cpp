@@ -1,0 +1,92 @@
+// The DIF arithmetic of the real xTGSNA kernel compiled for the CPU (test harness, not a
+// product path): xtgevc3_b200/csrc/tgsna_dif.cuh and tgexc_real_blocks.cuh are host and
+// device code, so the estimate the GPU kernel computes per eigenvalue (reorder a copy, then
+// xTGSYL's Frobenius-norm estimate) can be compared with LAPACK D/STGSNA on a machine
+// without a GPU.  Built by tests/test_tgsna_dif_host.py with g++ into a temporary folder.
+#include <vector>
+
+#include "../xtgevc3_b200/csrc/tgsna_dif.cuh"
+
+using namespace xtg::rb;
+
+namespace {
+
+// DTGSNA's DIF for every selected eigenvalue (howmny 'A' or 'S' with select), dif[0 .. m)
+template <class R>
+int dif_all(char howmny, const int *select, int n, const R *A, int lda, const R *B, int ldb, R *dif, int mm, int *m)
+{
+    auto a = [&](int i, int k) { return A[(size_t)i + (size_t)k * lda]; };
+    auto b = [&](int i, int k) { return B[(size_t)i + (size_t)k * ldb]; };
+    std::vector<R> wa((size_t)n * n), wb((size_t)n * n), c(2 * (size_t)n), f(2 * (size_t)n);
+    std::vector<int> starts(n / 2 + 4);
+    int ks = 0;
+    for (int k = 0; k < n;) {
+        const bool pair = k + 1 < n && a(k + 1, k) != R(0);
+        const bool sel = howmny == 'A' || (select[k] != 0 || (pair && select[k + 1] != 0));
+        if (sel) {
+            if (ks + (pair ? 2 : 1) > mm) return -15;
+            R d;
+            if (n == 1) {
+                d = lapy2(a(0, 0), b(0, 0));
+            } else {
+                R cond = R(0);
+                if (pair) cond = pair_cond(a(k, k), a(k + 1, k), a(k, k + 1), a(k + 1, k + 1), b(k, k), b(k + 1, k),
+                                           b(k, k + 1), b(k + 1, k + 1));
+                for (int j = 0; j < n; j++)
+                    for (int i = 0; i < n; i++) {
+                        wa[i + (size_t)j * n] = a(i, j);
+                        wb[i + (size_t)j * n] = b(i, j);
+                    }
+                Pencil<R> p{n, 0, 0, wa.data(), wb.data(), nullptr, nullptr, n, n, 1, 1};
+                int ifst = k + 1, ilst = 1;
+                if (tgexc_serial(p, ifst, ilst) > 0) {
+                    d = R(0);
+                } else {
+                    const int n1 = wa[1] != R(0) ? 2 : 1;
+                    d = (n - n1 == 0) ? cond
+                                      : dif_reordered_serial(n, wa.data(), wb.data(), n, c.data(), f.data(), n,
+                                                             starts.data());
+                    if (pair && n - n1 > 0) d = xmin(d, cond);
+                }
+            }
+            dif[ks] = d;
+            if (pair) dif[ks + 1] = d;
+            ks += pair ? 2 : 1;
+        }
+        k += pair ? 2 : 1;
+    }
+    *m = ks;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int host_ddif(char howmny, const int *select, int n, const double *A, int lda, const double *B, int ldb, double *dif,
+              int mm, int *m)
+{
+    return dif_all(howmny, select, n, A, lda, B, ldb, dif, mm, m);
+}
+
+int host_sdif(char howmny, const int *select, int n, const float *A, int lda, const float *B, int ldb, float *dif,
+              int mm, int *m)
+{
+    return dif_all(howmny, select, n, A, lda, B, ldb, dif, mm, m);
+}
+
+// the estimate alone, on a pencil whose first block is the eigenvalue's (already reordered)
+double host_ddif_reordered(int n, const double *A, const double *B)
+{
+    std::vector<double> c(2 * (size_t)n), f(2 * (size_t)n);
+    std::vector<int> starts(n / 2 + 4);
+    return dif_reordered_serial(n, A, B, n, c.data(), f.data(), n, starts.data());
+}
+
+// a complex pair's own bound from its 2x2 block (column-major a[4], b[4])
+double host_dpair_cond(const double *a, const double *b)
+{
+    return pair_cond(a[0], a[1], a[2], a[3], b[0], b[1], b[2], b[3]);
+}
+
+}  // extern "C"

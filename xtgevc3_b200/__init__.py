@@ -110,6 +110,10 @@ def lib():
             f = getattr(L, f"xtgevc3_{p}tgsna_dev")
             f.argtypes = [_P, _C, _C, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _P]
             f.restype = _I
+        for p in "ds":  # xTGSNA DIF on the device
+            f = getattr(L, f"xtgevc3_{p}tgsna_dif_dev")
+            f.argtypes = [_P, _C, _P, _I, _P, _I, _P, _I, _P, _I, _P, _P]
+            f.restype = _I
         for p in "zc":  # xTGEXC, complex pencils
             f = getattr(L, f"xtgevc3_{p}tgexc")
             f.argtypes = [_I, _I, _I, _P, _I, _P, _I, _P, _I, _P, _I, _I, _P, _P]
@@ -374,28 +378,56 @@ def trevc3_dev(side, howmny, T, VL=None, VR=None, select=None, flags=0, stream=N
 
 
 def tgsna(howmny, A, B, VL, VR, select=None, job="E"):
-    """Host-array form of s/d/c/ztgsna with JOB = 'E': reciprocal condition numbers of the
+    """Host-array form of s/d/c/ztgsna.  JOB = 'E': reciprocal condition numbers S of the
     selected eigenvalues of the Schur pencil (A, B) from its eigenvectors VL, VR (Schur
-    coordinates, as tgevc3 returns them with HOWMNY 'A' or 'S').  Returns (S, m, info)."""
+    coordinates, as tgevc3 returns them with HOWMNY 'A' or 'S'); returns (S, m, info).
+    JOB = 'V' / 'B' (real pencils): also the eigenvector condition estimates DIF; returns
+    (S, DIF, m, info) with S None for 'V' (VL, VR may then be None)."""
     L = lib()
     dt = A.dtype.type
     pfx = _PFX[dt]
     n = A.shape[0]
     A, B = np.asfortranarray(A), np.asfortranarray(B)
+    wants = job != "V"
+    if VL is None or VR is None:
+        VL = VR = np.zeros((max(n, 1), max(n, 1)), dtype=dt, order="F")
     VL, VR = np.asfortranarray(VL), np.asfortranarray(VR)
     rdt = np.float64 if pfx in "dz" else np.float32
     mm = VR.shape[1]
     sel = None if select is None else np.ascontiguousarray(select, dtype=np.int32)
     S = np.zeros(max(mm, 1), dtype=rdt)
+    D = np.zeros(max(mm, 1), dtype=rdt)
     m, info = ct.c_int(0), ct.c_int(0)
-    work = np.zeros(max(n, 1), dtype=dt)
+    lwork = max(n, 1) if job == "E" else max(1, 2 * n * (n + 2) + 16)
+    work = np.zeros(lwork, dtype=dt)
     ld = max(n, 1)
     getattr(L, f"xtgevc3_{pfx}tgsna")(job.encode(), howmny.encode(), _ptr(sel), n, _ptr(A), ld, _ptr(B), ld, _ptr(VL),
-                                      max(VL.shape[0], 1), _ptr(VR), max(VR.shape[0], 1), _ptr(S), None, mm,
-                                      ct.byref(m), _ptr(work), max(n, 1), None, ct.byref(info))
+                                      max(VL.shape[0], 1), _ptr(VR), max(VR.shape[0], 1), _ptr(S), _ptr(D), mm,
+                                      ct.byref(m), _ptr(work), lwork, None, ct.byref(info))
     if info.value > 0:
         raise RuntimeError(f"xtgevc3_{pfx}tgsna failed: {last_error()}")
-    return S[:m.value], m.value, info.value
+    if job == "E":
+        return S[:m.value], m.value, info.value
+    return (S[:m.value] if wants else None), D[:m.value], m.value, info.value
+
+
+def tgsna_dif_dev(A, B, howmny="A", select=None, stream=None):
+    """Device form of the DIF estimates (d/stgsna with JOB = 'V') on column-major CUDA
+    tensors.  Returns (DIF as a CUDA tensor of m entries, m, info)."""
+    import torch
+    L = lib()
+    pfx = {torch.float64: "d", torch.float32: "s"}[A.dtype]
+    n = A.shape[0]
+    st = ct.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+    sel = None if select is None else np.ascontiguousarray(select, dtype=np.int32)
+    dif = torch.zeros(max(n, 1), dtype=A.dtype, device=A.device)
+    m, info = ct.c_int(0), ct.c_int(0)
+    rc = getattr(L, f"xtgevc3_{pfx}tgsna_dif_dev")(st, howmny.encode(), _ptr(sel), n, ct.c_void_p(A.data_ptr()),
+                                                  max(A.stride(1), 1), ct.c_void_p(B.data_ptr()), max(B.stride(1), 1),
+                                                  ct.c_void_p(dif.data_ptr()), max(n, 1), ct.byref(m), ct.byref(info))
+    if rc:
+        raise RuntimeError(f"xtgevc3_{pfx}tgsna_dif_dev failed: {last_error()}")
+    return dif[:m.value], m.value, info.value
 
 
 def tgexc(A, B, Q=None, Z=None, ifst=1, ilst=1, with_ifst=False):

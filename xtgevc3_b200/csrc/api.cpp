@@ -610,31 +610,34 @@ int trevc3_device(unsigned flags, void *stream, char side, char howmny, const in
     return rc;
 }
 
-// ---- eigenvalue condition numbers: xTGSNA, JOB = 'E' ----------------------------------------
-// LAPACK xTGSNA's arguments and INFO order; only JOB = 'E' (S, from the eigenvectors) is
-// computed: JOB = 'V' / 'B' (DIF, which needs eigenvalue reordering and generalized
-// Sylvester solves) returns INFO = -1 with a message.  A real pair is A(k+1, k) != 0.
+// ---- condition numbers: xTGSNA --------------------------------------------------------------
+// LAPACK xTGSNA's arguments and INFO order.  S (JOB = 'E' / 'B') from the eigenvectors; DIF
+// (JOB = 'V' / 'B') for real pencils: a reordered copy per eigenvalue and xTGSYL's estimate
+// (tgsna_dif.cu); complex pencils with JOB = 'V' / 'B' return INFO = -1 with a message.  A real
+// pair is A(k+1, k) != 0.
 // argument checks that need no data, in LAPACK's order
-inline int tgsna_check(char job, char howmny, int n, int lda, int ldb, int ldvl, int ldvr)
+inline int tgsna_check(char job, char howmny, int n, int lda, int ldb, int ldvl, int ldvr, bool cplx)
 {
     if (job != 'E' && job != 'V' && job != 'B') return -1;
-    if (job != 'E') {
-        xtg::set_last_error("xTGSNA: only JOB='E' (eigenvalue condition numbers) is implemented");
+    if (job != 'E' && cplx) {
+        xtg::set_last_error("xTGSNA: DIF (JOB='V' / 'B') is implemented for real pencils (D/STGSNA); complex pencils "
+                            "take JOB='E'");
         return -1;
     }
+    const bool wants = job != 'V';
     if (howmny != 'A' && howmny != 'S') return -2;
     if (n < 0) return -4;
     if (lda < std::max(1, n)) return -6;
     if (ldb < std::max(1, n)) return -8;
-    if (ldvl < n) return -10;
-    if (ldvr < n) return -12;
+    if (wants && ldvl < n) return -10;
+    if (wants && ldvr < n) return -12;
     return 0;
 }
 
 // M and the eigenvalue list (sub: A's subdiagonal, n - 1 entries, real pencils); -15 if MM < M
 template <class R, bool CPLX>
 int tgsna_plan(char howmny, const int *select, int n, int mm, const std::vector<R> &sub, int *m,
-               std::vector<int> &items, std::vector<uint8_t> &kinds)
+               std::vector<int> &items, std::vector<uint8_t> &kinds, std::vector<int> *rows = nullptr)
 {
     int ks = 0;
     for (int k = 0; k < n;) {
@@ -643,6 +646,7 @@ int tgsna_plan(char howmny, const int *select, int n, int mm, const std::vector<
         if (sel) {
             items.push_back(ks);
             kinds.push_back(CPLX ? 2 : (pair ? 1 : 0));
+            if (rows) rows->push_back(k);
             ks += pair ? 2 : 1;
         }
         k += pair ? 2 : 1;
@@ -687,7 +691,11 @@ int tgsna_device(void *stream, char job, char howmny, const int *select, int n, 
     std::vector<int> items;
     std::vector<uint8_t> kinds;
     // the subdiagonal is read only once A's leading dimension is known to be valid
-    *info = tgsna_check(job, howmny, n, lda, ldb, ldvl, ldvr);
+    *info = tgsna_check(job, howmny, n, lda, ldb, ldvl, ldvr, CPLX);
+    if (*info == 0 && job != 'E') {
+        xtg::set_last_error("xTGSNA device form: JOB='E' (S); DIF on the device: xtgevc3_{d,s}tgsna_dif_dev");
+        *info = -1;
+    }
     if (*info) return 0;
     if (tgsna_subdiag<R, CPLX>(A, lda, n, true, st, sub)) {
         *info = 1;
@@ -701,36 +709,38 @@ int tgsna_device(void *stream, char job, char howmny, const int *select, int n, 
     return rc;
 }
 
-// Host form: stage A, B, VL, VR on the device, run, copy S back (DIF is not referenced).
+// Host form: stage A, B (and VL, VR for S) on the device, run, copy S and / or DIF back.
 template <class R, bool CPLX>
 void tgsna_host(char job, char howmny, const int *select, int n, const void *A, int lda, const void *B, int ldb,
-                const void *VL, int ldvl, const void *VR, int ldvr, R *s, int mm, int *m, void *work, int lwork,
-                int *info)
+                const void *VL, int ldvl, const void *VR, int ldvr, R *s, R *dif, int mm, int *m, void *work,
+                int lwork, int *info)
 {
     using E = typename std::conditional<CPLX, std::complex<R>, R>::type;
     job = (char)std::toupper((unsigned char)job);
     howmny = (char)std::toupper((unsigned char)howmny);
     xtg::set_last_error("");
-    const int lwmin = std::max(1, n);
+    const bool wants = job != 'V', wantdf = job != 'E';
+    // LAPACK's LWORK: N for S alone, 2 N (N + 2) + 16 with DIF (real pencils); 1 for N = 0
+    const int lwmin = n == 0 ? 1 : (wantdf ? 2 * n * (n + 2) + 16 : n);
     const bool lquery = lwork == -1;
     if (work) static_cast<E *>(work)[0] = E(lwmin);
     std::vector<R> sub;
-    std::vector<int> items;
+    std::vector<int> items, rows;
     std::vector<uint8_t> kinds;
     int count = 0;
-    *info = tgsna_check(job, howmny, n, lda, ldb, ldvl, ldvr);
+    *info = tgsna_check(job, howmny, n, lda, ldb, ldvl, ldvr, CPLX);
     if (*info) return;
     tgsna_subdiag<R, CPLX>(A, lda, n, false, nullptr, sub);
-    *info = tgsna_plan<R, CPLX>(howmny, select, n, mm, sub, &count, items, kinds);
+    *info = tgsna_plan<R, CPLX>(howmny, select, n, mm, sub, &count, items, kinds, &rows);
     if (m) *m = count;
     if (*info == 0 && lwork < lwmin && !lquery) *info = -18;
     if (*info || lquery || items.empty()) return;
     const int ld = round_up(n, 32);
-    void *dA = nullptr, *dB = nullptr, *dL = nullptr, *dR = nullptr, *dS = nullptr;
+    void *dA = nullptr, *dB = nullptr, *dL = nullptr, *dR = nullptr, *dS = nullptr, *dD = nullptr;
     cudaStream_t st = nullptr;
     auto cleanup = [&]() {
         if (st) cudaStreamSynchronize(st);
-        for (void *q : {dA, dB, dL, dR, dS})
+        for (void *q : {dA, dB, dL, dR, dS, dD})
             if (q) cudaFree(q);
         if (st) cudaStreamDestroy(st);
     };
@@ -738,17 +748,20 @@ void tgsna_host(char job, char howmny, const int *select, int n, const void *A, 
     const size_t mat = (size_t)ld * n * sizeof(E), vec = (size_t)ld * count * sizeof(E);
     for (void **q : {&dA, &dB})
         if (e == cudaSuccess) e = cudaMallocAsync(q, mat, st);
-    for (void **q : {&dL, &dR})
-        if (e == cudaSuccess) e = cudaMallocAsync(q, vec, st);
-    if (e == cudaSuccess) e = cudaMallocAsync(&dS, (size_t)count * sizeof(R), st);
+    if (wants) {
+        for (void **q : {&dL, &dR})
+            if (e == cudaSuccess) e = cudaMallocAsync(q, vec, st);
+        if (e == cudaSuccess) e = cudaMallocAsync(&dS, (size_t)count * sizeof(R), st);
+    }
+    if (wantdf && e == cudaSuccess) e = cudaMallocAsync(&dD, (size_t)count * sizeof(R), st);
     if (e == cudaSuccess)
         e = cudaMemcpy2DAsync(dA, ld * sizeof(E), A, (size_t)lda * sizeof(E), n * sizeof(E), n, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
         e = cudaMemcpy2DAsync(dB, ld * sizeof(E), B, (size_t)ldb * sizeof(E), n * sizeof(E), n, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess)
+    if (wants && e == cudaSuccess)
         e = cudaMemcpy2DAsync(dL, ld * sizeof(E), VL, (size_t)ldvl * sizeof(E), n * sizeof(E), count,
                               cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess)
+    if (wants && e == cudaSuccess)
         e = cudaMemcpy2DAsync(dR, ld * sizeof(E), VR, (size_t)ldvr * sizeof(E), n * sizeof(E), count,
                               cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) {
@@ -757,18 +770,59 @@ void tgsna_host(char job, char howmny, const int *select, int n, const void *A, 
         *info = 1;
         return;
     }
-    if (xtg::eig_cond_device<R, CPLX>(n, dA, ld, dB, ld, dL, ld, dR, ld, count, items, kinds, dS, st)) {
+    if (wants && xtg::eig_cond_device<R, CPLX>(n, dA, ld, dB, ld, dL, ld, dR, ld, count, items, kinds, dS, st)) {
         cleanup();
         *info = 1;
         return;
     }
-    e = cudaMemcpyAsync(s, dS, (size_t)count * sizeof(R), cudaMemcpyDeviceToHost, st);
+    if constexpr (!CPLX) {
+        std::vector<uint8_t> pairs(kinds.size());
+        for (size_t i = 0; i < kinds.size(); i++) pairs[i] = kinds[i] == 1;
+        if (wantdf && xtg::dif_device<R>(n, static_cast<const R *>(dA), ld, static_cast<const R *>(dB), ld, rows, items,
+                                         pairs, static_cast<R *>(dD), st)) {
+            cleanup();
+            *info = 1;
+            return;
+        }
+    }
+    if (wants) e = cudaMemcpyAsync(s, dS, (size_t)count * sizeof(R), cudaMemcpyDeviceToHost, st);
+    if (wantdf && e == cudaSuccess) e = cudaMemcpyAsync(dif, dD, (size_t)count * sizeof(R), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         xtg::set_last_error(std::string("xTGSNA D2H: ") + cudaGetErrorString(e));
         *info = 1;
     }
     cleanup();
+}
+
+// DIF alone, device pointers (real pencils): the checks of xTGSNA with JOB = 'V'.
+template <class R>
+int tgsna_dif_device(void *stream, char howmny, const int *select, int n, const R *A, int lda, const R *B, int ldb,
+                     R *dif, int mm, int *m, int *info)
+{
+    int dummy = 0;
+    if (!info) info = &dummy;
+    howmny = (char)std::toupper((unsigned char)howmny);
+    xtg::set_last_error("");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::vector<R> sub;
+    std::vector<int> items, rows;
+    std::vector<uint8_t> kinds;
+    *info = tgsna_check('V', howmny, n, lda, ldb, 0, 0, false);
+    if (*info) return 0;
+    if (tgsna_subdiag<R, false>(A, lda, n, true, st, sub)) {
+        *info = 1;
+        return 1;
+    }
+    int count = 0;
+    *info = tgsna_plan<R, false>(howmny, select, n, mm, sub, &count, items, kinds, &rows);
+    if (m) *m = count;
+    if (*info || items.empty()) return 0;
+    std::vector<uint8_t> pairs(kinds.size());
+    for (size_t i = 0; i < kinds.size(); i++) pairs[i] = kinds[i] == 1;
+    const int rc = xtg::dif_device<R>(n, A, lda, B, ldb, rows, items, pairs, dif, st);
+    if (rc) *info = 1;
+    return rc;
 }
 
 }  // namespace
@@ -936,9 +990,9 @@ void xtgevc3_dtgsna(char job, char howmny, const int *select, int n, const doubl
                     int ldb, const double *VL, int ldvl, const double *VR, int ldvr, double *s, double *dif, int mm, int *m,
                     double *work, int lwork, int *iwork, int *info)
 {
-    (void)dif;
     (void)iwork;
-    tgsna_host<double, false>(job, howmny, select, n, A, lda, B, ldb, VL, ldvl, VR, ldvr, s, mm, m, work, lwork, info);
+    tgsna_host<double, false>(job, howmny, select, n, A, lda, B, ldb, VL, ldvl, VR, ldvr, s, dif, mm, m, work, lwork,
+                          info);
 }
 
 int xtgevc3_dtgsna_dev(void *stream, char job, char howmny, const int *select, int n, const double *A, int lda,
@@ -952,9 +1006,9 @@ void xtgevc3_stgsna(char job, char howmny, const int *select, int n, const float
                     int ldb, const float *VL, int ldvl, const float *VR, int ldvr, float *s, float *dif, int mm, int *m,
                     float *work, int lwork, int *iwork, int *info)
 {
-    (void)dif;
     (void)iwork;
-    tgsna_host<float, false>(job, howmny, select, n, A, lda, B, ldb, VL, ldvl, VR, ldvr, s, mm, m, work, lwork, info);
+    tgsna_host<float, false>(job, howmny, select, n, A, lda, B, ldb, VL, ldvl, VR, ldvr, s, dif, mm, m, work, lwork,
+                          info);
 }
 
 int xtgevc3_stgsna_dev(void *stream, char job, char howmny, const int *select, int n, const float *A, int lda,
@@ -968,9 +1022,9 @@ void xtgevc3_ztgsna(char job, char howmny, const int *select, int n, const doubl
                     int ldb, const double *VL, int ldvl, const double *VR, int ldvr, double *s, double *dif, int mm, int *m,
                     double *work, int lwork, int *iwork, int *info)
 {
-    (void)dif;
     (void)iwork;
-    tgsna_host<double, true>(job, howmny, select, n, A, lda, B, ldb, VL, ldvl, VR, ldvr, s, mm, m, work, lwork, info);
+    tgsna_host<double, true>(job, howmny, select, n, A, lda, B, ldb, VL, ldvl, VR, ldvr, s, dif, mm, m, work, lwork,
+                          info);
 }
 
 int xtgevc3_ztgsna_dev(void *stream, char job, char howmny, const int *select, int n, const double *A, int lda,
@@ -984,9 +1038,9 @@ void xtgevc3_ctgsna(char job, char howmny, const int *select, int n, const float
                     int ldb, const float *VL, int ldvl, const float *VR, int ldvr, float *s, float *dif, int mm, int *m,
                     float *work, int lwork, int *iwork, int *info)
 {
-    (void)dif;
     (void)iwork;
-    tgsna_host<float, true>(job, howmny, select, n, A, lda, B, ldb, VL, ldvl, VR, ldvr, s, mm, m, work, lwork, info);
+    tgsna_host<float, true>(job, howmny, select, n, A, lda, B, ldb, VL, ldvl, VR, ldvr, s, dif, mm, m, work, lwork,
+                          info);
 }
 
 int xtgevc3_ctgsna_dev(void *stream, char job, char howmny, const int *select, int n, const float *A, int lda,
@@ -994,6 +1048,18 @@ int xtgevc3_ctgsna_dev(void *stream, char job, char howmny, const int *select, i
                         int *m, int *info)
 {
     return tgsna_device<float, true>(stream, job, howmny, select, n, A, lda, B, ldb, VL, ldvl, VR, ldvr, s, mm, m, info);
+}
+
+int xtgevc3_dtgsna_dif_dev(void *stream, char howmny, const int *select, int n, const double *A, int lda,
+                           const double *B, int ldb, double *dif, int mm, int *m, int *info)
+{
+    return tgsna_dif_device<double>(stream, howmny, select, n, A, lda, B, ldb, dif, mm, m, info);
+}
+
+int xtgevc3_stgsna_dif_dev(void *stream, char howmny, const int *select, int n, const float *A, int lda,
+                           const float *B, int ldb, float *dif, int mm, int *m, int *info)
+{
+    return tgsna_dif_device<float>(stream, howmny, select, n, A, lda, B, ldb, dif, mm, m, info);
 }
 
 }  // extern "C"

@@ -131,4 +131,12 @@ int eig_cond_device(int n, const void *A, int lda, const void *B, int ldb, const
                     int ldvr, int m, const std::vector<int> &items, const std::vector<uint8_t> &kinds, void *s_dev,
                     cudaStream_t st);
 
+// Eigenvector condition estimates DIF (LAPACK D/STGSNA, JOB = 'V' / 'B') of the selected
+// blocks of a real generalized Schur pencil (A, B) (device pointers): rows[i] is a block's
+// first row (0-based), outs[i] the index of its DIF in dif_dev (a pair fills two), pairs[i]
+// whether it is a 2x2 block.  Returns 0, or 1 (message in last_error).
+template <class R>
+int dif_device(int n, const R *A, int lda, const R *B, int ldb, const std::vector<int> &rows,
+               const std::vector<int> &outs, const std::vector<uint8_t> &pairs, R *dif_dev, cudaStream_t st);
+
 }  // namespace xtg
