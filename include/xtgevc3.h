@@ -192,22 +192,23 @@ int xtgevc3_ctrevc3_dev(unsigned flags, void *stream, char side, char howmny, co
  * eigenvectors VL, VR in Schur coordinates (as xtgevc3_*tgevc3 return them with HOWMNY 'A'
  * or 'S'); a real pair (A(k+1,k) != 0) gets one S for both columns; S = -1 where the
  * numerator is zero (not for a pair, as in LAPACK).
- * DIF (JOB = 'V' or 'B', real pencils): LAPACK's estimate of the reciprocal condition
- * number of the eigenvectors, as D/STGSNA computes it: a copy of the pencil with the
- * eigenvalue's block reordered to the top (DIF = 0 when a swap is rejected), then xTGSYL's
- * Frobenius-norm estimate for the rest of the pencil (+-1 right-hand sides chosen by
- * look-ahead), a pair's own 2x2 bound taken as well.  The look-ahead choices depend on the
- * signs of the reordered pencil, which LAPACK itself leaves to rounding noise in swaps of
- * 2x2 blocks; where the reordered copy has LAPACK's signs, DIF agrees with LAPACK's to
- * rounding, elsewhere it is an estimate of the same quality (both within a small factor
- * above the true smallest singular value).  Complex pencils: JOB = 'V' / 'B' returns
- * INFO = -1 with a message in xtgevc3_last_error().
+ * DIF (JOB = 'V' or 'B'): LAPACK's estimate of the reciprocal condition number of the
+ * eigenvectors, as xTGSNA computes it: a copy of the pencil with the eigenvalue's block
+ * reordered to the top (DIF = 0 when a swap is rejected), then xTGSYL's Frobenius-norm
+ * estimate for the rest of the pencil (+-1 right-hand sides chosen by look-ahead), a real
+ * pair's own 2x2 bound taken as well.  Complex pencils: the reordering is LAPACK's rotations,
+ * DIF agrees with LAPACK's to rounding.  Real pencils: the look-ahead choices depend on the
+ * signs of the reordered copy, which LAPACK itself leaves to rounding noise in swaps of 2x2
+ * blocks; where the copy has LAPACK's signs, DIF agrees with LAPACK's to rounding,
+ * elsewhere it is an estimate of the same quality (both within a small factor above the
+ * true smallest singular value).
  * VL, VR are not referenced for JOB = 'V'; IWORK is not referenced and WORK is not used
- * (the query, LWORK = -1, answers LAPACK's LWORK: max(1, n) for JOB = 'E', 2 n (n + 2) + 16
- * with DIF).  INFO: -1 JOB, -2 HOWMNY, -4 N, -6 LDA, -8 LDB, -10 LDVL, -12 LDVR (JOB 'E' or
- * 'B'), -15 MM < M, -18 LWORK, 1 a CUDA failure.  Complex arrays interleaved (S real).
- * Device forms: S only (JOB = 'E'; other JOB values return INFO = -1), A, B, VL, VR and S
- * device pointers; DIF on the device: xtgevc3_{d,s}tgsna_dif_dev below.                  */
+ * (the query, LWORK = -1, answers LAPACK's LWORK: max(1, n) for JOB = 'E'; with DIF
+ * 2 n (n + 2) + 16 for real, 2 n^2 for complex pencils).  INFO: -1 JOB, -2 HOWMNY, -4 N,
+ * -6 LDA, -8 LDB, -10 LDVL, -12 LDVR (JOB 'E' or 'B'), -15 MM < M, -18 LWORK, 1 a CUDA
+ * failure.  Complex arrays interleaved (S, DIF real).  Device forms: S only (JOB = 'E'; other
+ * JOB values return INFO = -1), A, B, VL, VR and S device pointers; DIF on the device:
+ * xtgevc3_*tgsna_dif_dev below.                                                            */
 void xtgevc3_dtgsna(char job, char howmny, const int *select, int n, const double *A, int lda, const double *B,
                     int ldb, const double *VL, int ldvl, const double *VR, int ldvr, double *s, double *dif, int mm,
                     int *m, double *work, int lwork, int *iwork, int *info);
@@ -232,12 +233,16 @@ int xtgevc3_ztgsna_dev(void *stream, char job, char howmny, const int *select, i
 int xtgevc3_ctgsna_dev(void *stream, char job, char howmny, const int *select, int n, const float *A, int lda,
                        const float *B, int ldb, const float *VL, int ldvl, const float *VR, int ldvr, float *s, int mm,
                        int *m, int *info);
-/* DIF alone on the device (real pencils): A, B and DIF device pointers, SELECT / M / INFO on
- * the host; the checks of xTGSNA with JOB = 'V' (-2 HOWMNY, -4 N, -6 LDA, -8 LDB, -15 MM).
- * Returns 0, or 1 when a CUDA call failed (INFO = 1).                                    */
+/* DIF alone on the device: A, B and DIF device pointers (complex A, B interleaved, DIF
+ * real), SELECT / M / INFO on the host; the checks of xTGSNA with JOB = 'V' (-2 HOWMNY, -4 N,
+ * -6 LDA, -8 LDB, -15 MM).  Returns 0, or 1 when a CUDA call failed (INFO = 1).           */
 int xtgevc3_dtgsna_dif_dev(void *stream, char howmny, const int *select, int n, const double *A, int lda,
                            const double *B, int ldb, double *dif, int mm, int *m, int *info);
 int xtgevc3_stgsna_dif_dev(void *stream, char howmny, const int *select, int n, const float *A, int lda,
+                           const float *B, int ldb, float *dif, int mm, int *m, int *info);
+int xtgevc3_ztgsna_dif_dev(void *stream, char howmny, const int *select, int n, const double *A, int lda,
+                           const double *B, int ldb, double *dif, int mm, int *m, int *info);
+int xtgevc3_ctgsna_dif_dev(void *stream, char howmny, const int *select, int n, const float *A, int lda,
                            const float *B, int ldb, float *dif, int mm, int *m, int *info);
 
 /* ---- eigenvalue reordering, complex pencils: xTGEXC (no counterpart upstream) ---------

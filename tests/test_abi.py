@@ -240,8 +240,8 @@ def test_trevc3_info_codes_and_query(pfx):
 def test_tgsna_info_codes_and_query():
     """xtgevc3_dtgsna: LAPACK xTGSNA's INFO codes in its order, answered before any CUDA
     call, and its LWORK: N for JOB = 'E', 2 N (N + 2) + 16 with DIF (JOB = 'V' / 'B'); LDVL
-    and LDVR are not checked for JOB = 'V' (VL, VR not referenced).  Complex pencils with
-    JOB = 'V' return -1 with a message."""
+    and LDVR are not checked for JOB = 'V' (VL, VR not referenced); complex pencils' LWORK
+    with DIF is 2 N^2 (Z/CTGSNA)."""
     n = 5
     A = np.asfortranarray(np.triu(np.arange(1.0, n * n + 1).reshape(n, n)))
     V = np.zeros((n, n), order="F")
@@ -262,10 +262,11 @@ def test_tgsna_info_codes_and_query():
     assert call(job=b"V", ldvl=1, ldvr=1, lwork=lw_dif - 1)[0] == -18
     assert call(job=b"B", ldvl=n - 1, lwork=-1)[0] == -10
     zA = A.astype(np.complex128)
+    zwork = np.zeros(2, dtype=np.complex128)
     m, info = ct.c_int(0), ct.c_int(0)
-    L.xtgevc3_ztgsna(b"V", b"A", None, n, zA.ctypes.data, n, zA.ctypes.data, n, zA.ctypes.data, n, zA.ctypes.data, n,
-                     None, None, n, ct.byref(m), None, -1, None, ct.byref(info))
-    assert info.value == -1 and "real pencils" in X.last_error()
+    L.xtgevc3_ztgsna(b"V", b"A", None, n, zA.ctypes.data, n, zA.ctypes.data, n, zA.ctypes.data, 1, zA.ctypes.data, 1,
+                     None, None, n, ct.byref(m), zwork.ctypes.data, -1, None, ct.byref(info))
+    assert (info.value, m.value, int(zwork[0].real)) == (0, n, 2 * n * n)  # ZTGSNA's LWORK with DIF
     assert call(howmny=b"B")[0] == -2
     assert call(nn=-1)[0] == -4
     assert call(lda=n - 1)[0] == -6

@@ -1,5 +1,5 @@
 """xtgevc3_{d,s,z,c}tgsna (JOB = 'E': eigenvalue condition numbers; JOB = 'V' / 'B': the
-eigenvector condition estimates DIF of real pencils) against LAPACK xTGSNA.
+eigenvector condition estimates DIF) against LAPACK xTGSNA.
 
 The oracle is LAPACK's own xTGSNA from SciPy's bundled OpenBLAS, given the same Schur
 pencil and the same eigenvectors (LAPACK xTGEVC's, in Schur coordinates).  S does not
@@ -79,7 +79,7 @@ def test_tgsna_schur_like_700(cuda_ok):
     assert _rel(got, ref) < 1e-8, _rel(got, ref)
 
 
-# ---- DIF (JOB = 'V' / 'B', real pencils) -------------------------------------------------
+# ---- DIF (JOB = 'V' / 'B') ----------------------------------------------------------------
 # DTGSNA's estimate, from a copy reordered per eigenvalue and xTGSYL's +-1 look-ahead; the
 # look-ahead follows the reordered copy's signs, which LAPACK leaves to rounding in swaps of
 # 2x2 blocks (test_tgsna_dif_host.py checks the estimate step exactly on LAPACK's own
@@ -143,3 +143,22 @@ def test_dif_selection_and_rejection(cuda_ok):
     _, h, m2, _ = X.tgsna("A", A, B, None, None, job="V")
     assert d[3] == d[4] == 0
     np.testing.assert_array_equal(h[3:5], d[3:5])
+
+
+@pytest.mark.parametrize("dt", [np.complex128, np.complex64], ids=["z", "c"])
+def test_complex_dif_matches_lapack(cuda_ok, dt):
+    """Z/CTGSNA JOB = 'V': the reordering is LAPACK's rotations, so every DIF equals LAPACK's
+    to rounding (1e-10 double, 1e-3 single); the device form gives the host form's values."""
+    import torch
+    tol = {np.complex128: 1e-10, np.complex64: 1e-3}[dt]
+    for seed, n in ((1, 1), (2, 7), (3, 33)):
+        A, B = oracle.complex_schur_pencil(n, 300 + seed, dt)[:2]
+        _, d, m, info = oracle.lapack_tgsna("A", A, B, None, None, job="V")
+        s_, h, m2, info2 = X.tgsna("A", A, B, None, None, job="V")
+        assert s_ is None and (m2, info2) == (m, info) == (n, 0)
+        np.testing.assert_allclose(h, d, rtol=tol)
+    dA = torch.from_numpy(np.ascontiguousarray(A.T)).cuda().t()
+    dB = torch.from_numpy(np.ascontiguousarray(B.T)).cuda().t()
+    d_dev, m, info = X.tgsna_dif_dev(dA, dB)
+    assert (m, info) == (33, 0)
+    np.testing.assert_array_equal(d_dev.cpu().numpy(), h)

@@ -13,6 +13,8 @@ LAPACK leaves the signs to rounding noise (its RQ-versus-QR choice), so:
     the true value (the smallest singular value of the Kronecker operator, by a dense SVD)
     and ten times it, ours within a factor of two of LAPACK's;
   * a rejected reordering gives DIF = 0, as in LAPACK.
+Complex pencils (ZTGSNA): the reordering is LAPACK's rotations (no sign freedom), so every DIF
+must equal LAPACK's to rounding (1e-12 double, 1e-4 single).
 Runs without a GPU."""
 import ctypes as ct
 import os
@@ -35,7 +37,8 @@ def host():
     os.makedirs(out, exist_ok=True)
     lib = os.path.join(out, "libtgsna_dif_host.so")
     src = os.path.join(ROOT, "tests", "tgsna_dif_host.cpp")
-    hdrs = [os.path.join(ROOT, "xtgevc3_b200", "csrc", h) for h in ("tgsna_dif.cuh", "tgexc_real_blocks.cuh")]
+    hdrs = [os.path.join(ROOT, "xtgevc3_b200", "csrc", h)
+            for h in ("tgsna_dif.cuh", "tgsna_dif_cplx.cuh", "tgexc_real_blocks.cuh")]
     if not os.path.exists(lib) or os.path.getmtime(lib) < max(os.path.getmtime(f) for f in [src] + hdrs):
         r = subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-ffp-contract=off", "-o", lib, src],
                            capture_output=True, text=True)
@@ -162,3 +165,35 @@ def test_dif_selection_rejection_and_n1(host):
     one_a, one_b = np.array([[3.0]], order="F"), np.array([[-4.0]], order="F")
     _, d, m, _ = oracle.lapack_tgsna("A", one_a, one_b, None, None, job="V")
     np.testing.assert_allclose(host_dif(host, one_a, one_b), d, rtol=1e-15)
+
+
+def host_zdif(L, A, B, howmny="A", select=None):
+    n = A.shape[0]
+    pfx = "z" if A.dtype == np.complex128 else "c"
+    rdt = np.float64 if pfx == "z" else np.float32
+    A, B = np.asfortranarray(A), np.asfortranarray(B)
+    dif = np.zeros(max(n, 1), dtype=rdt)
+    sel = np.zeros(max(n, 1), dtype=np.int32) if select is None else np.ascontiguousarray(select, dtype=np.int32)
+    m = ct.c_int()
+    rc = getattr(L, f"host_{pfx}dif")(ct.c_char(howmny.encode()), _p(sel), n, _p(A), _p(B), _p(dif), n, ct.byref(m))
+    assert rc == 0
+    return dif[:m.value]
+
+
+@pytest.mark.parametrize("dt", [np.complex128, np.complex64], ids=["z", "c"])
+def test_complex_dif_matches_lapack(host, dt):
+    """ZTGSNA / CTGSNA JOB = 'V' on complex generalized Schur forms of iid complex N(0,1)
+    pencils, n = 1 .. 30, every eigenvalue; and HOWMNY = 'S'."""
+    tol = {np.complex128: 1e-12, np.complex64: 1e-4}[dt]
+    for seed in range(6):
+        for n in (1, 2, 5, 13, 30):
+            A, B = oracle.complex_schur_pencil(n, 200 + seed, dt)[:2]
+            _, d, m, info = oracle.lapack_tgsna("A", A, B, None, None, job="V")
+            h = host_zdif(host, A, B)
+            assert info == 0 and len(h) == m == n
+            np.testing.assert_allclose(h, d, rtol=tol)
+    A, B = oracle.complex_schur_pencil(20, 9, dt)[:2]
+    sel = np.zeros(20, dtype=np.int32)
+    sel[[2, 11, 19]] = 1
+    _, d, m, _ = oracle.lapack_tgsna("S", A, B, None, None, select=sel, job="V")
+    np.testing.assert_allclose(host_zdif(host, A, B, "S", sel), d, rtol=tol)

@@ -1,4 +1,4 @@
-// The DIF arithmetic of the real xTGSNA kernel compiled for the CPU (test harness, not a
+// The DIF arithmetic of the xTGSNA kernels (real and complex) compiled for the CPU (test harness, not a
 // product path): xtgevc3_b200/csrc/tgsna_dif.cuh and tgexc_real_blocks.cuh are host and
 // device code, so the estimate the GPU kernel computes per eigenvalue (reorder a copy, then
 // xTGSYL's Frobenius-norm estimate) can be compared with LAPACK D/STGSNA on a machine
@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "../xtgevc3_b200/csrc/tgsna_dif.cuh"
+#include "../xtgevc3_b200/csrc/tgsna_dif_cplx.cuh"
 
 using namespace xtg::rb;
 
@@ -59,9 +60,37 @@ int dif_all(char howmny, const int *select, int n, const R *A, int lda, const R 
     return 0;
 }
 
+// ZTGSNA's DIF for every selected eigenvalue (complex A, B interleaved)
+template <class R>
+int zdif_all(char howmny, const int *select, int n, const R *A_, const R *B_, R *dif, int mm, int *m)
+{
+    const zc<R> *A = reinterpret_cast<const zc<R> *>(A_), *B = reinterpret_cast<const zc<R> *>(B_);
+    std::vector<zc<R>> wa((size_t)n * n), wb((size_t)n * n), c(n), f(n);
+    std::vector<int> starts(n / 2 + 4);
+    int ks = 0;
+    for (int k = 0; k < n; k++) {
+        if (howmny != 'A' && !select[k]) continue;
+        if (ks >= mm) return -15;
+        dif[ks++] = zdif_serial(n, A, n, B, n, k, wa.data(), wb.data(), c.data(), f.data(), starts.data());
+    }
+    *m = ks;
+    return 0;
+}
+
 }  // namespace
 
 extern "C" {
+
+int host_zdif(char howmny, const int *select, int n, const double *A, const double *B, double *dif, int mm, int *m)
+{
+    return zdif_all(howmny, select, n, A, B, dif, mm, m);
+}
+
+int host_cdif(char howmny, const int *select, int n, const float *A, const float *B, float *dif, int mm, int *m)
+{
+    return zdif_all(howmny, select, n, A, B, dif, mm, m);
+}
+
 
 int host_ddif(char howmny, const int *select, int n, const double *A, int lda, const double *B, int ldb, double *dif,
               int mm, int *m)

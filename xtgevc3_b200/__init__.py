@@ -110,7 +110,7 @@ def lib():
             f = getattr(L, f"xtgevc3_{p}tgsna_dev")
             f.argtypes = [_P, _C, _C, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _I, _P, _P]
             f.restype = _I
-        for p in "ds":  # xTGSNA DIF on the device
+        for p in "dszc":  # xTGSNA DIF on the device
             f = getattr(L, f"xtgevc3_{p}tgsna_dif_dev")
             f.argtypes = [_P, _C, _P, _I, _P, _I, _P, _I, _P, _I, _P, _P]
             f.restype = _I
@@ -381,8 +381,8 @@ def tgsna(howmny, A, B, VL, VR, select=None, job="E"):
     """Host-array form of s/d/c/ztgsna.  JOB = 'E': reciprocal condition numbers S of the
     selected eigenvalues of the Schur pencil (A, B) from its eigenvectors VL, VR (Schur
     coordinates, as tgevc3 returns them with HOWMNY 'A' or 'S'); returns (S, m, info).
-    JOB = 'V' / 'B' (real pencils): also the eigenvector condition estimates DIF; returns
-    (S, DIF, m, info) with S None for 'V' (VL, VR may then be None)."""
+    JOB = 'V' / 'B': also the eigenvector condition estimates DIF; returns (S, DIF, m, info)
+    with S None for 'V' (VL, VR may then be None)."""
     L = lib()
     dt = A.dtype.type
     pfx = _PFX[dt]
@@ -398,7 +398,7 @@ def tgsna(howmny, A, B, VL, VR, select=None, job="E"):
     S = np.zeros(max(mm, 1), dtype=rdt)
     D = np.zeros(max(mm, 1), dtype=rdt)
     m, info = ct.c_int(0), ct.c_int(0)
-    lwork = max(n, 1) if job == "E" else max(1, 2 * n * (n + 2) + 16)
+    lwork = max(n, 1) if job == "E" else max(1, 2 * n * (n + 2) + 16 if pfx in "ds" else 2 * n * n)
     work = np.zeros(lwork, dtype=dt)
     ld = max(n, 1)
     getattr(L, f"xtgevc3_{pfx}tgsna")(job.encode(), howmny.encode(), _ptr(sel), n, _ptr(A), ld, _ptr(B), ld, _ptr(VL),
@@ -412,15 +412,16 @@ def tgsna(howmny, A, B, VL, VR, select=None, job="E"):
 
 
 def tgsna_dif_dev(A, B, howmny="A", select=None, stream=None):
-    """Device form of the DIF estimates (d/stgsna with JOB = 'V') on column-major CUDA
-    tensors.  Returns (DIF as a CUDA tensor of m entries, m, info)."""
+    """Device form of the DIF estimates (xTGSNA with JOB = 'V') on column-major CUDA
+    tensors.  Returns (DIF as a real CUDA tensor of m entries, m, info)."""
     import torch
     L = lib()
-    pfx = {torch.float64: "d", torch.float32: "s"}[A.dtype]
+    pfx = {torch.float64: "d", torch.float32: "s", torch.complex128: "z", torch.complex64: "c"}[A.dtype]
+    rdt = {"d": torch.float64, "s": torch.float32, "z": torch.float64, "c": torch.float32}[pfx]
     n = A.shape[0]
     st = ct.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
     sel = None if select is None else np.ascontiguousarray(select, dtype=np.int32)
-    dif = torch.zeros(max(n, 1), dtype=A.dtype, device=A.device)
+    dif = torch.zeros(max(n, 1), dtype=rdt, device=A.device)
     m, info = ct.c_int(0), ct.c_int(0)
     rc = getattr(L, f"xtgevc3_{pfx}tgsna_dif_dev")(st, howmny.encode(), _ptr(sel), n, ct.c_void_p(A.data_ptr()),
                                                   max(A.stride(1), 1), ct.c_void_p(B.data_ptr()), max(B.stride(1), 1),

@@ -612,18 +612,13 @@ int trevc3_device(unsigned flags, void *stream, char side, char howmny, const in
 
 // ---- condition numbers: xTGSNA --------------------------------------------------------------
 // LAPACK xTGSNA's arguments and INFO order.  S (JOB = 'E' / 'B') from the eigenvectors; DIF
-// (JOB = 'V' / 'B') for real pencils: a reordered copy per eigenvalue and xTGSYL's estimate
-// (tgsna_dif.cu); complex pencils with JOB = 'V' / 'B' return INFO = -1 with a message.  A real
-// pair is A(k+1, k) != 0.
+// (JOB = 'V' / 'B'): a reordered copy per eigenvalue and xTGSYL's estimate (tgsna_dif.cu).  A
+// real pair is A(k+1, k) != 0.
 // argument checks that need no data, in LAPACK's order
 inline int tgsna_check(char job, char howmny, int n, int lda, int ldb, int ldvl, int ldvr, bool cplx)
 {
+    (void)cplx;
     if (job != 'E' && job != 'V' && job != 'B') return -1;
-    if (job != 'E' && cplx) {
-        xtg::set_last_error("xTGSNA: DIF (JOB='V' / 'B') is implemented for real pencils (D/STGSNA); complex pencils "
-                            "take JOB='E'");
-        return -1;
-    }
     const bool wants = job != 'V';
     if (howmny != 'A' && howmny != 'S') return -2;
     if (n < 0) return -4;
@@ -720,8 +715,9 @@ void tgsna_host(char job, char howmny, const int *select, int n, const void *A, 
     howmny = (char)std::toupper((unsigned char)howmny);
     xtg::set_last_error("");
     const bool wants = job != 'V', wantdf = job != 'E';
-    // LAPACK's LWORK: N for S alone, 2 N (N + 2) + 16 with DIF (real pencils); 1 for N = 0
-    const int lwmin = n == 0 ? 1 : (wantdf ? 2 * n * (n + 2) + 16 : n);
+    // LAPACK's LWORK: N for S alone; with DIF 2 N (N + 2) + 16 (D/STGSNA) or 2 N^2 (Z/CTGSNA);
+    // 1 for N = 0
+    const int lwmin = n == 0 ? 1 : (wantdf ? (CPLX ? 2 * n * n : 2 * n * (n + 2) + 16) : n);
     const bool lquery = lwork == -1;
     if (work) static_cast<E *>(work)[0] = E(lwmin);
     std::vector<R> sub;
@@ -775,11 +771,18 @@ void tgsna_host(char job, char howmny, const int *select, int n, const void *A, 
         *info = 1;
         return;
     }
-    if constexpr (!CPLX) {
-        std::vector<uint8_t> pairs(kinds.size());
-        for (size_t i = 0; i < kinds.size(); i++) pairs[i] = kinds[i] == 1;
-        if (wantdf && xtg::dif_device<R>(n, static_cast<const R *>(dA), ld, static_cast<const R *>(dB), ld, rows, items,
-                                         pairs, static_cast<R *>(dD), st)) {
+    if (wantdf) {
+        int rc;
+        if constexpr (CPLX) {
+            rc = xtg::dif_device_cplx<R>(n, static_cast<const R *>(dA), ld, static_cast<const R *>(dB), ld, rows,
+                                         items, static_cast<R *>(dD), st);
+        } else {
+            std::vector<uint8_t> pairs(kinds.size());
+            for (size_t i = 0; i < kinds.size(); i++) pairs[i] = kinds[i] == 1;
+            rc = xtg::dif_device<R>(n, static_cast<const R *>(dA), ld, static_cast<const R *>(dB), ld, rows, items,
+                                    pairs, static_cast<R *>(dD), st);
+        }
+        if (rc) {
             cleanup();
             *info = 1;
             return;
@@ -795,8 +798,8 @@ void tgsna_host(char job, char howmny, const int *select, int n, const void *A, 
     cleanup();
 }
 
-// DIF alone, device pointers (real pencils): the checks of xTGSNA with JOB = 'V'.
-template <class R>
+// DIF alone, device pointers: the checks of xTGSNA with JOB = 'V'.  Complex A, B interleaved.
+template <class R, bool CPLX>
 int tgsna_dif_device(void *stream, char howmny, const int *select, int n, const R *A, int lda, const R *B, int ldb,
                      R *dif, int mm, int *m, int *info)
 {
@@ -808,19 +811,24 @@ int tgsna_dif_device(void *stream, char howmny, const int *select, int n, const 
     std::vector<R> sub;
     std::vector<int> items, rows;
     std::vector<uint8_t> kinds;
-    *info = tgsna_check('V', howmny, n, lda, ldb, 0, 0, false);
+    *info = tgsna_check('V', howmny, n, lda, ldb, 0, 0, CPLX);
     if (*info) return 0;
-    if (tgsna_subdiag<R, false>(A, lda, n, true, st, sub)) {
+    if (tgsna_subdiag<R, CPLX>(A, lda, n, true, st, sub)) {
         *info = 1;
         return 1;
     }
     int count = 0;
-    *info = tgsna_plan<R, false>(howmny, select, n, mm, sub, &count, items, kinds, &rows);
+    *info = tgsna_plan<R, CPLX>(howmny, select, n, mm, sub, &count, items, kinds, &rows);
     if (m) *m = count;
     if (*info || items.empty()) return 0;
-    std::vector<uint8_t> pairs(kinds.size());
-    for (size_t i = 0; i < kinds.size(); i++) pairs[i] = kinds[i] == 1;
-    const int rc = xtg::dif_device<R>(n, A, lda, B, ldb, rows, items, pairs, dif, st);
+    int rc;
+    if constexpr (CPLX) {
+        rc = xtg::dif_device_cplx<R>(n, A, lda, B, ldb, rows, items, dif, st);
+    } else {
+        std::vector<uint8_t> pairs(kinds.size());
+        for (size_t i = 0; i < kinds.size(); i++) pairs[i] = kinds[i] == 1;
+        rc = xtg::dif_device<R>(n, A, lda, B, ldb, rows, items, pairs, dif, st);
+    }
     if (rc) *info = 1;
     return rc;
 }
@@ -1053,13 +1061,25 @@ int xtgevc3_ctgsna_dev(void *stream, char job, char howmny, const int *select, i
 int xtgevc3_dtgsna_dif_dev(void *stream, char howmny, const int *select, int n, const double *A, int lda,
                            const double *B, int ldb, double *dif, int mm, int *m, int *info)
 {
-    return tgsna_dif_device<double>(stream, howmny, select, n, A, lda, B, ldb, dif, mm, m, info);
+    return tgsna_dif_device<double, false>(stream, howmny, select, n, A, lda, B, ldb, dif, mm, m, info);
 }
 
 int xtgevc3_stgsna_dif_dev(void *stream, char howmny, const int *select, int n, const float *A, int lda,
                            const float *B, int ldb, float *dif, int mm, int *m, int *info)
 {
-    return tgsna_dif_device<float>(stream, howmny, select, n, A, lda, B, ldb, dif, mm, m, info);
+    return tgsna_dif_device<float, false>(stream, howmny, select, n, A, lda, B, ldb, dif, mm, m, info);
+}
+
+int xtgevc3_ztgsna_dif_dev(void *stream, char howmny, const int *select, int n, const double *A, int lda,
+                           const double *B, int ldb, double *dif, int mm, int *m, int *info)
+{
+    return tgsna_dif_device<double, true>(stream, howmny, select, n, A, lda, B, ldb, dif, mm, m, info);
+}
+
+int xtgevc3_ctgsna_dif_dev(void *stream, char howmny, const int *select, int n, const float *A, int lda,
+                           const float *B, int ldb, float *dif, int mm, int *m, int *info)
+{
+    return tgsna_dif_device<float, true>(stream, howmny, select, n, A, lda, B, ldb, dif, mm, m, info);
 }
 
 }  // extern "C"

@@ -138,5 +138,10 @@ int eig_cond_device(int n, const void *A, int lda, const void *B, int ldb, const
 template <class R>
 int dif_device(int n, const R *A, int lda, const R *B, int ldb, const std::vector<int> &rows,
                const std::vector<int> &outs, const std::vector<uint8_t> &pairs, R *dif_dev, cudaStream_t st);
+// The same for a complex generalized Schur pencil (A, B interleaved complex, device pointers;
+// one DIF per selected eigenvalue; rows[i] its row, outs[i] its index in dif_dev).
+template <class R>
+int dif_device_cplx(int n, const R *A, int lda, const R *B, int ldb, const std::vector<int> &rows,
+                    const std::vector<int> &outs, R *dif_dev, cudaStream_t st);
 
 }  // namespace xtg
