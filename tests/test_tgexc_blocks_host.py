@@ -230,3 +230,42 @@ def test_splitting_block_moves(host):
         if done == 12:
             break
     assert done >= 8
+
+
+def _gges_rank_deficient(n, seed):
+    """LAPACK DGGES of a Gaussian pencil whose B repeats (or zeroes) its first columns:
+    infinite eigenvalues among the finite ones."""
+    import scipy.linalg.lapack as la
+    rng = np.random.default_rng(seed)
+    A, B = rng.standard_normal((n, n)), rng.standard_normal((n, n))
+    k = 1 + seed % 3
+    B[:, :k] = B[:, k:2 * k]
+    S, T, _, _, _, _, Q, Z, _, info = la.dgges(lambda *a: 0, np.asfortranarray(A), np.asfortranarray(B), sort_t=0)
+    assert info == 0
+    return [np.asfortranarray(M) for M in (S, T, Q, Z)]
+
+
+@pytest.mark.parametrize("kind", ["graded", "infinite"])
+def test_hard_pencils_keep_lapack_control_flow(host, kind):
+    """Graded pencils (eigenvalues over 16 orders of magnitude) and pencils with infinite
+    eigenvalues: IFST, ILST and INFO exactly as LAPACK DTGEXC on 120 random moves, and every
+    result a valid reordering (Q A Z^T, Q B Z^T kept to 1e-14 relative, Q and Z orthogonal,
+    A quasi-triangular, B triangular).  Elementwise agreement is not asked here: an
+    infinite eigenvalue's B entry becomes rounding noise on the way, differently in LAPACK."""
+    n = 14
+    for seed in range(20):
+        if kind == "graded":
+            S, T, _, _, _, Q, Z = pencils.gen_gges(n, 900 + seed, graded=True)
+        else:
+            S, T, Q, Z = _gges_rank_deficient(n, seed)
+        rng = np.random.default_rng(seed)
+        for _ in range(6):
+            ifst, ilst = (int(x) for x in rng.integers(1, n + 1, 2))
+            r = oracle.lapack_tgexc_real(S, T, Q, Z, ifst, ilst)
+            a, b, q, z, f, l_, info = host_tgexc(host, S, T, Q, Z, ifst, ilst)
+            assert (f, l_, info) == r[4:], (seed, ifst, ilst)
+            for M, M0 in ((a, S), (b, T)):
+                assert np.abs(q @ M @ z.T - Q @ M0 @ Z.T).max() <= 1e-14 * n * np.abs(M0).max()
+            for W in (q, z):
+                assert np.abs(W.T @ W - np.eye(n)).max() < 1e-13
+            assert np.abs(np.tril(b, -1)).max() == 0 and np.abs(np.tril(a, -2)).max() == 0

@@ -197,3 +197,37 @@ def test_complex_dif_matches_lapack(host, dt):
     sel[[2, 11, 19]] = 1
     _, d, m, _ = oracle.lapack_tgsna("S", A, B, None, None, select=sel, job="V")
     np.testing.assert_allclose(host_zdif(host, A, B, "S", sel), d, rtol=tol)
+
+
+def test_estimate_step_every_small_order(host):
+    """The estimate step on LAPACK's reordered copies for every block of 25 pencils of each
+    order n = 2 .. 12 (xTGSYL's block cuts next to 2x2 blocks, n2 = 1 .. 4, the unblocked
+    case): LAPACK's DIF to 1e-12."""
+    for n in range(2, 13):
+        for seed in range(25):
+            S, T = pencils.gen_gges(n, 5000 + 100 * n + seed)[:2]
+            _, d, m, info = oracle.lapack_tgsna("A", S, T, None, None, job="V")
+            ks = 0
+            for k, pair in blocks(S):
+                r = oracle.lapack_tgexc_real(S, T, None, None, k + 1, 1)
+                if r[6] == 0:
+                    a, b = np.asfortranarray(r[0]), np.asfortranarray(r[1])
+                    n1 = 2 if a[1, 0] != 0 else 1
+                    est = host.host_ddif_reordered(n, _p(a), _p(b)) if n > n1 else None
+                    if pair:
+                        cond = host.host_dpair_cond(_p(np.asfortranarray(S[k:k + 2, k:k + 2])),
+                                                    _p(np.asfortranarray(T[k:k + 2, k:k + 2])))
+                        est = cond if est is None else min(est, cond)
+                    assert abs(est - d[ks]) <= 1e-12 * abs(d[ks]), (n, seed, k, est, d[ks])
+                ks += 2 if pair else 1
+
+
+@pytest.mark.parametrize("dt", [np.complex128, np.complex64], ids=["z", "c"])
+def test_complex_dif_every_small_order(host, dt):
+    """Every eigenvalue of 20 complex Schur pencils of each order n = 1 .. 12."""
+    tol = {np.complex128: 1e-12, np.complex64: 1e-4}[dt]
+    for n in range(1, 13):
+        for seed in range(20):
+            A, B = oracle.complex_schur_pencil(n, 7000 + 100 * n + seed, dt)[:2]
+            _, d, m, info = oracle.lapack_tgsna("A", A, B, None, None, job="V")
+            np.testing.assert_allclose(host_zdif(host, A, B), d, rtol=tol, err_msg=f"n={n} seed={seed}")
