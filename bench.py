@@ -826,6 +826,31 @@ def measure_tgexc_blocks(args, X, torch):
     return out
 
 
+def neighbours_brief(legs):
+    """One compact entry per LAPACK-neighbour leg for the `config` block (device ms; LAPACK's
+    seconds on the host and the ratio where the leg timed it).  A leg that is absent, failed
+    or shaped otherwise is left out: this summary must never stop the line from printing."""
+    out = {}
+    for name, leg in legs.items():
+        try:
+            if not isinstance(leg, dict):
+                continue
+            ms = leg.get("ms")
+            if ms is None and isinstance(leg.get("d"), dict):
+                ms = leg["d"].get("ms")
+            if ms is None:
+                continue
+            e = {"ms": round(float(ms), 3)}
+            cpu = leg.get("cpu_lapack")
+            if isinstance(cpu, dict) and cpu.get("seconds"):
+                e["lapack_s"] = round(float(cpu["seconds"]), 3)
+                e["x_lapack"] = round(float(cpu["seconds"]) / (float(ms) * 1e-3), 2)
+            out[name] = e
+        except (TypeError, ValueError, KeyError, ZeroDivisionError):
+            continue
+    return out
+
+
 def schur_stand_in(n, seed):
     """Stand-in for the real Schur factor T of an n x n iid N(0,1) matrix (host, Fortran):
     strictly upper part N(0,1); about sqrt(2n/pi) real eigenvalues, uniform on [-sqrt(n),
@@ -1227,6 +1252,8 @@ def main():
                            "peaks_measured_here": {"fp64_dgemm_tflops": peak_fp64, "int8_imma_tops": peak_int8},
                            "normalize": None if norm is None else {
                                "ms": norm["ms_per_call"], "gbs": norm["gbs"], "frac_of_hbm": norm["frac_of_hbm"]},
+                           "neighbours": neighbours_brief({"ztgexc": txleg, "dtgexc": dxleg, "dtgexc_blocks": bxleg,
+                                                           "dtrevc3": trleg, "adjoint": adjoint}),
                            "batched": None if batched is None else {
                                "pencils_per_s": batched["value"], "speedup_vs_loop": batched["speedup_vs_loop"],
                                "d_ms": batched["d"]["ms"], "s_ms": batched["s"]["ms"],

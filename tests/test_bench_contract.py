@@ -33,3 +33,23 @@ def test_reference_arm_json_line():
     assert cb["value"] == d["value"] and cb["unit"] == d["unit"]
     assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+
+
+def test_neighbours_brief_tolerates_missing_and_odd_legs():
+    """The compact per-leg summary in `config`: ms, LAPACK's seconds and the ratio where a leg
+    has them; absent (None), failed or oddly shaped legs are left out instead of raising."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    legs = {"dtgexc": {"ms": 80.0, "cpu_lapack": {"seconds": 0.46}},
+            "adjoint": {"d": {"ms": 12.5}},
+            "dtrevc3": {"ms": 30.0},
+            "ztgexc": None,
+            "odd": {"ms": "x"},
+            "zero": {"ms": 0.0, "cpu_lapack": {"seconds": 1.0}},
+            "list": [1, 2]}
+    out = bench.neighbours_brief(legs)
+    assert out["dtgexc"] == {"ms": 80.0, "lapack_s": 0.46, "x_lapack": 5.75}
+    assert out["adjoint"] == {"ms": 12.5} and out["dtrevc3"] == {"ms": 30.0}
+    assert "ztgexc" not in out and "odd" not in out and "zero" not in out and "list" not in out
