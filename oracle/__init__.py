@@ -9,6 +9,9 @@ Contents
       - ``oracle`` : this repository's C restatement (oracle/tgevc3_oracle.c),
       - ``ref``    : the upstream sources compiled as they are (oracle/_ref, built by
                      ``make -C oracle ref`` where the upstream tree is present);
+  * LAPACK from SciPy's bundled OpenBLAS (Fortran interface where SciPy's wrapper drops an
+    output) as the oracle of the LAPACK-compatible entry points: xTGEVC, xTREVC3, xTGSNA
+    (JOB 'E', 'V', 'B'), xTGEXC and the single swap xTGEX2;
   * residual checks and the comparison normalisation (the seeded pencil generators live
     in ``xtgevc3_b200.pencils`` and are re-exported here for the tests).
 """
