@@ -15,6 +15,8 @@ LAPACK leaves the signs to rounding noise (its RQ-versus-QR choice), so:
   * a rejected reordering gives DIF = 0, as in LAPACK.
 Complex pencils (ZTGSNA): the reordering is LAPACK's rotations (no sign freedom), so every DIF
 must equal LAPACK's to rounding (1e-12 double, 1e-4 single).
+The GPU kernels' bodies themselves (written against a CTA context) also run here on host
+threads with a barrier and must give the serial build's values bit for bit.
 Runs without a GPU."""
 import ctypes as ct
 import os
@@ -40,8 +42,8 @@ def host():
     hdrs = [os.path.join(ROOT, "xtgevc3_b200", "csrc", h)
             for h in ("tgsna_dif.cuh", "tgsna_dif_cplx.cuh", "tgexc_real_blocks.cuh")]
     if not os.path.exists(lib) or os.path.getmtime(lib) < max(os.path.getmtime(f) for f in [src] + hdrs):
-        r = subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-ffp-contract=off", "-o", lib, src],
-                           capture_output=True, text=True)
+        r = subprocess.run(["g++", "-O2", "-std=c++20", "-pthread", "-shared", "-fPIC", "-ffp-contract=off", "-o", lib,
+                            src], capture_output=True, text=True)
         assert r.returncode == 0, r.stderr
     L = ct.CDLL(lib)
     L.host_ddif_reordered.restype = ct.c_double
@@ -231,3 +233,34 @@ def test_complex_dif_every_small_order(host, dt):
             A, B = oracle.complex_schur_pencil(n, 7000 + 100 * n + seed, dt)[:2]
             _, d, m, info = oracle.lapack_tgsna("A", A, B, None, None, job="V")
             np.testing.assert_allclose(host_zdif(host, A, B), d, rtol=tol, err_msg=f"n={n} seed={seed}")
+
+
+def _threads_dif(L, fn, nth, grid, A, B):
+    n = A.shape[0]
+    dif = np.zeros(max(n, 1))
+    sel = np.zeros(max(n, 1), dtype=np.int32)
+    m = ct.c_int()
+    A, B = np.asfortranarray(A), np.asfortranarray(B)
+    err = getattr(L, fn)(nth, grid, ct.c_char(b"A"), _p(sel), n, _p(A), _p(B), _p(dif), ct.byref(m))
+    return dif[:m.value], err
+
+
+@pytest.mark.timeout(300)
+def test_kernel_bodies_on_host_threads(host):
+    """The DIF kernels' bodies (rb::dif_cta, rb::zdif_cta: the code the GPU kernels run) on host
+    threads, one std::thread per GPU thread and a std::barrier for the CTA barrier, several
+    CTAs: every thread reaches every barrier (a mismatch would hang: the timeout fails it), and
+    the DIFs equal the serial build's bit for bit whatever the thread and CTA counts (each
+    entry is updated by one thread with the same arithmetic)."""
+    for seed, n in ((1, 1), (2, 2), (3, 9), (4, 24), (5, 37)):
+        S, T = pencils.gen_gges(n, 60 + seed)[:2]
+        ref = host_dif(host, S, T)
+        for nth, grid in ((1, 1), (3, 2), (32, 5), (256, 3)):
+            h, err = _threads_dif(host, "threads_ddif", nth, grid, S, T)
+            assert err == 0
+            np.testing.assert_array_equal(h, ref, err_msg=f"real n={n} threads={nth} ctas={grid}")
+        A, B = oracle.complex_schur_pencil(n, 80 + seed)[:2]
+        zref = host_zdif(host, A, B)
+        for nth, grid in ((1, 1), (5, 2), (64, 4)):
+            h, _ = _threads_dif(host, "threads_zdif", nth, grid, A, B)
+            np.testing.assert_array_equal(h, zref, err_msg=f"complex n={n} threads={nth} ctas={grid}")

@@ -3,6 +3,8 @@
 // device code, so the estimate the GPU kernel computes per eigenvalue (reorder a copy, then
 // xTGSYL's Frobenius-norm estimate) can be compared with LAPACK D/STGSNA on a machine
 // without a GPU.  Built by tests/test_tgsna_dif_host.py with g++ into a temporary folder.
+#include <barrier>
+#include <thread>
 #include <vector>
 
 #include "../xtgevc3_b200/csrc/tgsna_dif.cuh"
@@ -77,9 +79,82 @@ int zdif_all(char howmny, const int *select, int n, const R *A_, const R *B_, R 
     return 0;
 }
 
+// The CTA context of the kernel bodies on host threads: one std::thread per GPU thread, the
+// CTA barrier a std::barrier.  Emulated CTAs run one after another.
+struct CtaHost {
+    int t, n, b, nb;
+    std::barrier<> *bar;
+    int tid() const { return t; }
+    int nth() const { return n; }
+    int cta() const { return b; }
+    int ncta() const { return nb; }
+    void sync() const { bar->arrive_and_wait(); }
+};
+
+// the selected blocks as the kernels take them (xTGSNA's selection rule)
+template <class E, class IsPair>
+std::vector<DifItem> dif_items(char howmny, const int *select, int n, IsPair is_pair, int *m)
+{
+    std::vector<DifItem> items;
+    int ks = 0;
+    for (int k = 0; k < n;) {
+        const bool pair = is_pair(k);
+        if (howmny == 'A' || select[k] != 0 || (pair && select[k + 1] != 0)) {
+            items.push_back(DifItem{k, ks, pair ? 1 : 0});
+            ks += pair ? 2 : 1;
+        }
+        k += pair ? 2 : 1;
+    }
+    *m = ks;
+    return items;
+}
+
+template <class Body>
+void run_grid(int nth, int grid, Body body)
+{
+    for (int b = 0; b < grid; b++) {
+        std::barrier<> bar(nth);
+        std::vector<std::thread> th;
+        for (int t = 0; t < nth; t++) th.emplace_back([&, t] { body(CtaHost{t, nth, b, grid, &bar}); });
+        for (auto &x : th) x.join();
+    }
+}
+
 }  // namespace
 
 extern "C" {
+
+// the real DIF kernel's body (rb::dif_cta) on nth host threads per CTA and grid CTAs; returns
+// the kernel's error flag
+int threads_ddif(int nth, int grid, char howmny, const int *select, int n, const double *A, const double *B,
+                 double *dif, int *m)
+{
+    auto items = dif_items<double>(howmny, select, n, [&](int k) { return k + 1 < n && A[k + 1 + (size_t)k * n] != 0.0; }, m);
+    const size_t per = dif_work_elems(n);
+    std::vector<double> work(per * grid);
+    int err = 0;
+    std::vector<DifShared<double>> sh(grid);
+    run_grid(nth, grid, [&](const CtaHost &c) {
+        dif_cta(c, sh[c.b], n, A, n, B, n, items.data(), (int)items.size(), dif, work.data(), per, &err);
+    });
+    return err;
+}
+
+// the complex DIF kernel's body (rb::zdif_cta) likewise
+int threads_zdif(int nth, int grid, char howmny, const int *select, int n, const double *A, const double *B,
+                 double *dif, int *m)
+{
+    auto items = dif_items<zc<double>>(howmny, select, n, [](int) { return false; }, m);
+    const size_t per = zdif_work_elems(n);
+    std::vector<zc<double>> work(per * grid);
+    std::vector<ZDifShared<double>> sh(grid);
+    run_grid(nth, grid, [&](const CtaHost &c) {
+        zdif_cta(c, sh[c.b], n, reinterpret_cast<const zc<double> *>(A), n, reinterpret_cast<const zc<double> *>(B), n,
+                 items.data(), (int)items.size(), dif, work.data(), per);
+    });
+    return 0;
+}
+
 
 int host_zdif(char howmny, const int *select, int n, const double *A, const double *B, double *dif, int mm, int *m)
 {

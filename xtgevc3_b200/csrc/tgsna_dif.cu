@@ -25,231 +25,68 @@ namespace {
 
 constexpr int kDifThreads = 256;
 
-struct DifItem {
-    int k, ks, pair;  // first row of the block (0-based), index of its DIF, complex pair
-};
+using rb::DifItem;
+using rb::dif_work_elems;
+using rb::zdif_work_elems;
 
-// workspace of one CTA, in elements of R: the reordered copy (2 n^2), C and F (n x 2 each),
-// xTGSYL's block starts (n / 2 + 4 ints, n + 8 elements of room)
-inline size_t dif_work_elems(int n) { return 2 * (size_t)n * n + 4 * (size_t)n + (size_t)n + 8; }
+// The CTA context of the kernel bodies (rb::dif_cta, rb::zdif_cta) on the GPU
+struct CtaDev {
+    XTG_HD int tid() const
+    {
+#ifdef __CUDA_ARCH__
+        return (int)threadIdx.x;
+#else
+        return 0;
+#endif
+    }
+    XTG_HD int nth() const
+    {
+#ifdef __CUDA_ARCH__
+        return (int)blockDim.x;
+#else
+        return 1;
+#endif
+    }
+    XTG_HD int cta() const
+    {
+#ifdef __CUDA_ARCH__
+        return (int)blockIdx.x;
+#else
+        return 0;
+#endif
+    }
+    XTG_HD int ncta() const
+    {
+#ifdef __CUDA_ARCH__
+        return (int)gridDim.x;
+#else
+        return 1;
+#endif
+    }
+    XTG_HD void sync() const
+    {
+#ifdef __CUDA_ARCH__
+        __syncthreads();
+#endif
+    }
+};
 
 template <class R>
 __global__ void __launch_bounds__(kDifThreads)
     tgsna_dif_kernel(int n, const R *A, int lda, const R *B, int ldb, const DifItem *items, int count, R *dif,
                      R *work, size_t per_cta, int *err)
 {
-    __shared__ rb::Swap<R> s;
-    __shared__ rb::Walk w;
-    __shared__ rb::Sylv<R> y;
-    __shared__ int s_go, s_info, s_nbk;
-    __shared__ R s_cond, s_d;
-    R *Aw = work + blockIdx.x * per_cta;
-    R *Bw = Aw + (size_t)n * n;
-    R *Cw = Bw + (size_t)n * n;
-    R *Fw = Cw + 2 * (size_t)n;
-    int *starts = reinterpret_cast<int *>(Fw + 2 * (size_t)n);
-    for (int it = blockIdx.x; it < count; it += gridDim.x) {
-        const DifItem item = items[it];
-        if (n == 1) {
-            if (threadIdx.x == 0) dif[item.ks] = rb::lapy2(A[0], B[0]);
-            continue;
-        }
-        for (size_t e = threadIdx.x; e < (size_t)n * n; e += blockDim.x) {
-            const size_t i = e % n, j = e / n;
-            Aw[e] = A[i + j * lda];
-            Bw[e] = B[i + j * ldb];
-        }
-        for (int e = threadIdx.x; e < 2 * n; e += blockDim.x) {
-            Cw[e] = R(0);
-            Fw[e] = R(0);
-        }
-        const rb::Pencil<R> p{n, 0, 0, Aw, Bw, nullptr, nullptr, n, n, 1, 1};
-        if (threadIdx.x == 0) {
-            const int k = item.k;
-            s_cond = R(0);
-            if (item.pair)
-                s_cond = rb::pair_cond(A[k + (size_t)k * lda], A[k + 1 + (size_t)k * lda], A[k + (size_t)(k + 1) * lda],
-                                       A[k + 1 + (size_t)(k + 1) * lda], B[k + (size_t)k * ldb],
-                                       B[k + 1 + (size_t)k * ldb], B[k + (size_t)(k + 1) * ldb],
-                                       B[k + 1 + (size_t)(k + 1) * ldb]);
-        }
-        __syncthreads();  // the copy is complete before thread 0 reads it
-        if (threadIdx.x == 0) {
-            int f = item.k + 1, l = 1;
-            s_go = rb::walk_begin(p, w, f, l) ? 1 : 0;
-            s_info = 0;
-            s.ok = 0;
-            s.n1 = s.n2 = 1;
-        }
-        const int limit = 4 * n + 16;
-        for (int step = 0;; step++) {  // the reordering kernel's walk loop
-            if (threadIdx.x == 0 && s_go) {
-                int j1, n1, n2;
-                if (step >= limit) {
-                    s_go = 0;
-                    s_info = 3;
-                } else if (!rb::walk_next(p, w, j1, n1, n2)) {
-                    s_go = 0;
-                } else {
-                    s.j1 = j1 - 1;
-                    s.n1 = n1;
-                    s.n2 = n2;
-                    rb::swap_prepare(p, s);
-                    if (s.ok == 0) {
-                        s_go = 0;
-                        s_info = 1;
-                    }
-                }
-            }
-            __syncthreads();
-            const int go = s_go, ok = s.ok, m = s.n1 + s.n2;
-            if (!go) break;
-            if (ok == 1) {
-                rb::swap_apply(p, s, 0, threadIdx.x, blockDim.x);
-                if (m == 2) {
-                    __syncthreads();
-                    rb::swap_apply(p, s, 1, threadIdx.x, blockDim.x);
-                    __syncthreads();
-                    rb::swap_apply(p, s, 2, threadIdx.x, blockDim.x);
-                }
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) rb::walk_after(p, w);
-        }
-        __syncthreads();  // every thread has left the walk before its state is reused
-        if (threadIdx.x == 0) {
-            s_nbk = 0;
-            s_d = R(0);  // a rejected swap: DIF = 0
-            if (s_info == 3) atomicExch(err, 1);
-            if (s_info == 0) {
-                const int n1 = Aw[1] != R(0) ? 2 : 1;
-                if (n - n1 == 0) {
-                    s_d = s_cond;
-                } else {
-                    y.n1 = n1;
-                    y.n2 = n - n1;
-                    y.ld = n;
-                    y.ldc = n;
-                    y.A22 = Aw + n1 + (size_t)n1 * n;
-                    y.B22 = Bw + n1 + (size_t)n1 * n;
-                    for (int q = 0; q < 16; q++) {
-                        y.A11s[q] = R(0);
-                        y.B11s[q] = R(0);
-                    }
-                    for (int j = 0; j < n1; j++)
-                        for (int i = 0; i < n1; i++) {
-                            y.A11s[i + rb::LD * j] = Aw[i + (size_t)j * n];
-                            y.B11s[i + rb::LD * j] = Bw[i + (size_t)j * n];
-                        }
-                    y.C = Cw;
-                    y.F = Fw;
-                    y.dsum = R(1);
-                    y.dscale = R(0);
-                    s_nbk = rb::tgsyl_blocks(y, starts);
-                }
-            }
-        }
-        __syncthreads();
-        const int nbk = s_nbk;
-        for (int b = nbk - 1; b >= 0; b--) {
-            if (threadIdx.x == 0) rb::tgsyl_block(y, starts[b], starts[b + 1] - 1);
-            __syncthreads();
-            rb::tgsyl_update_above(y, starts[b], starts[b + 1] - 1, (int)threadIdx.x, (int)blockDim.x);
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) {
-            R d = s_d;
-            if (nbk > 0) {
-                d = rb::xsqrt(R(2 * y.n1 * y.n2)) / (y.dscale * rb::xsqrt(y.dsum));
-                if (item.pair) d = rb::xmin(d, s_cond);
-            }
-            dif[item.ks] = d;
-            if (item.pair) dif[item.ks + 1] = d;
-        }
-        __syncthreads();  // the workspace is reused by the next item
-    }
+    __shared__ rb::DifShared<R> sh;
+    rb::dif_cta(CtaDev{}, sh, n, A, lda, B, ldb, items, count, dif, work, per_cta, err);
 }
-
-// Complex pencils: one CTA per eigenvalue, as above.  status: none needed (the walk is at most
-// k swaps).  Workspace of one CTA in complex elements: the copy (2 n^2), C and F (n each),
-// ZTGSYL's block starts (n / 2 + 4 ints, n + 8 elements of room).
-inline size_t zdif_work_elems(int n) { return 2 * (size_t)n * n + 3 * (size_t)n + 8; }
 
 template <class R>
 __global__ void __launch_bounds__(kDifThreads)
     tgsna_dif_cplx_kernel(int n, const rb::zc<R> *A, int lda, const rb::zc<R> *B, int ldb, const DifItem *items,
                           int count, R *dif, rb::zc<R> *work, size_t per_cta)
 {
-    using C = rb::zc<R>;
-    __shared__ rb::ZSwap<R> s;
-    __shared__ rb::ZSylv<R> y;
-    __shared__ int s_rej, s_nbk;
-    C *Aw = work + blockIdx.x * per_cta;
-    C *Bw = Aw + (size_t)n * n;
-    C *Cw = Bw + (size_t)n * n;
-    C *Fw = Cw + n;
-    int *starts = reinterpret_cast<int *>(Fw + n);
-    for (int it = blockIdx.x; it < count; it += gridDim.x) {
-        const DifItem item = items[it];
-        if (n == 1) {
-            if (threadIdx.x == 0) dif[item.ks] = rb::lapy2(rb::cabs(A[0]), rb::cabs(B[0]));
-            continue;
-        }
-        for (size_t e = threadIdx.x; e < (size_t)n * n; e += blockDim.x) {
-            const size_t i = e % n, j = e / n;
-            Aw[e] = A[i + j * lda];
-            Bw[e] = B[i + j * ldb];
-        }
-        for (int e = threadIdx.x; e < n; e += blockDim.x) {
-            Cw[e] = rb::mk(R(0), R(0));
-            Fw[e] = rb::mk(R(0), R(0));
-        }
-        if (threadIdx.x == 0) s_rej = 0;
-        __syncthreads();  // the copy is complete before thread 0 reads it
-        for (int here = item.k; here > 0; here--) {  // the eigenvalue moves up one row per swap
-            if (threadIdx.x == 0) {
-                s.j = here - 1;
-                rb::zswap_prepare(Aw, Bw, n, s);
-                s_rej = s.ok ? 0 : 1;
-            }
-            __syncthreads();
-            if (s_rej) break;
-            rb::zswap_apply(Aw, Bw, n, n, s, 0, (int)threadIdx.x, (int)blockDim.x);
-            __syncthreads();  // the 2x2 block takes the column rotation before the row rotation
-            rb::zswap_apply(Aw, Bw, n, n, s, 1, (int)threadIdx.x, (int)blockDim.x);
-            __syncthreads();
-            rb::zswap_apply(Aw, Bw, n, n, s, 2, (int)threadIdx.x, (int)blockDim.x);
-            __syncthreads();
-        }
-        __syncthreads();  // every thread has left the walk
-        if (threadIdx.x == 0) {
-            s_nbk = 0;
-            if (!s_rej) {
-                y.n2 = n - 1;
-                y.ld = n;
-                y.A22 = Aw + 1 + (size_t)n;
-                y.B22 = Bw + 1 + (size_t)n;
-                y.a11 = Aw[0];
-                y.b11 = Bw[0];
-                y.C = Cw;
-                y.F = Fw;
-                y.dsum = R(1);
-                y.dscale = R(0);
-                s_nbk = rb::ztgsyl_blocks(n - 1, starts);
-            }
-        }
-        __syncthreads();
-        const int nbk = s_nbk;
-        for (int b = nbk - 1; b >= 0; b--) {
-            if (threadIdx.x == 0) rb::ztgsyl_block(y, starts[b], starts[b + 1] - 1);
-            __syncthreads();
-            rb::ztgsyl_update_above(y, starts[b], starts[b + 1] - 1, (int)threadIdx.x, (int)blockDim.x);
-            __syncthreads();
-        }
-        if (threadIdx.x == 0)  // a rejected swap: DIF = 0
-            dif[item.ks] = nbk > 0 ? rb::xsqrt(R(2 * y.n2)) / (y.dscale * rb::xsqrt(y.dsum)) : R(0);
-        __syncthreads();  // the workspace is reused by the next item
-    }
+    __shared__ rb::ZDifShared<R> sh;
+    rb::zdif_cta(CtaDev{}, sh, n, A, lda, B, ldb, items, count, dif, work, per_cta);
 }
 
 }  // namespace

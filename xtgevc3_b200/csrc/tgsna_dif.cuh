@@ -277,5 +277,166 @@ XTG_HD R dif_reordered_serial(int n, const R *A, const R *B, int ld, R *C, R *F,
     return xsqrt(R(2 * y.n1 * y.n2)) / (y.dscale * xsqrt(y.dsum));
 }
 
+// ---- the GPU kernel's body, one CTA ---------------------------------------------------------
+// Written against a CTA context c (c.tid(), c.nth(): this thread and the CTA's size; c.cta(),
+// c.ncta(): this CTA and the grid's size; c.sync(): the CTA barrier) so that the kernel
+// (tgsna_dif.cu: shared memory, __syncthreads) and the tests (host threads with a barrier)
+// run the same code.
+
+// one selected block: its first row (0-based), the index of its DIF, whether a 2x2 block
+struct DifItem {
+    int k, ks, pair;
+};
+
+// workspace of one CTA in elements of R: the reordered copy (2 n^2), C and F (n x 2 each),
+// xTGSYL's block starts (n / 2 + 4 ints in n + 8 elements of room)
+XTG_HD inline size_t dif_work_elems(int n) { return 2 * (size_t)n * n + 4 * (size_t)n + (size_t)n + 8; }
+
+// the CTA's shared state (shared memory on the GPU)
+template <class R>
+struct DifShared {
+    Swap<R> s;
+    Walk w;
+    Sylv<R> y;
+    int go, info, nbk;
+    R cond, d;
+};
+
+// DIF of the items it = c.cta(), c.cta() + c.ncta(), ... of a real pencil (A, B): copy, walk
+// the block to the top (thread 0 decides and computes each swap, the CTA applies it; bounded
+// by 4 n + 16 swaps, *err = 1 if that bound were reached), xTGSYL's estimate (thread 0 solves
+// each block, the CTA updates the rows above it).
+template <class R, class Cta>
+XTG_HD void dif_cta(const Cta &c, DifShared<R> &sh, int n, const R *A, int lda, const R *B, int ldb,
+                    const DifItem *items, int count, R *dif, R *work, size_t per_cta, int *err)
+{
+    const int tid = c.tid(), nth = c.nth();
+    R *Aw = work + (size_t)c.cta() * per_cta;
+    R *Bw = Aw + (size_t)n * n;
+    R *Cw = Bw + (size_t)n * n;
+    R *Fw = Cw + 2 * (size_t)n;
+    int *starts = reinterpret_cast<int *>(Fw + 2 * (size_t)n);
+    for (int it = c.cta(); it < count; it += c.ncta()) {
+        const DifItem item = items[it];
+        if (n == 1) {
+            if (tid == 0) dif[item.ks] = lapy2(A[0], B[0]);
+            continue;
+        }
+        for (size_t e = tid; e < (size_t)n * n; e += nth) {
+            const size_t i = e % n, j = e / n;
+            Aw[e] = A[i + j * lda];
+            Bw[e] = B[i + j * ldb];
+        }
+        for (int e = tid; e < 2 * n; e += nth) {
+            Cw[e] = R(0);
+            Fw[e] = R(0);
+        }
+        const Pencil<R> p{n, 0, 0, Aw, Bw, nullptr, nullptr, n, n, 1, 1};
+        if (tid == 0) {
+            const int k = item.k;
+            sh.cond = R(0);
+            if (item.pair)
+                sh.cond = pair_cond(A[k + (size_t)k * lda], A[k + 1 + (size_t)k * lda], A[k + (size_t)(k + 1) * lda],
+                                    A[k + 1 + (size_t)(k + 1) * lda], B[k + (size_t)k * ldb], B[k + 1 + (size_t)k * ldb],
+                                    B[k + (size_t)(k + 1) * ldb], B[k + 1 + (size_t)(k + 1) * ldb]);
+        }
+        c.sync();  // the copy is complete before thread 0 reads it
+        if (tid == 0) {
+            int f = item.k + 1, l = 1;
+            sh.go = walk_begin(p, sh.w, f, l) ? 1 : 0;
+            sh.info = 0;
+            sh.s.ok = 0;
+            sh.s.n1 = sh.s.n2 = 1;
+        }
+        const int limit = 4 * n + 16;
+        for (int step = 0;; step++) {  // the reordering kernel's walk loop
+            if (tid == 0 && sh.go) {
+                int j1, n1, n2;
+                if (step >= limit) {
+                    sh.go = 0;
+                    sh.info = 3;
+                } else if (!walk_next(p, sh.w, j1, n1, n2)) {
+                    sh.go = 0;
+                } else {
+                    sh.s.j1 = j1 - 1;
+                    sh.s.n1 = n1;
+                    sh.s.n2 = n2;
+                    swap_prepare(p, sh.s);
+                    if (sh.s.ok == 0) {
+                        sh.go = 0;
+                        sh.info = 1;
+                    }
+                }
+            }
+            c.sync();  // thread 0 writes go / s again only after the barrier at the loop's end
+            const int go = sh.go, ok = sh.s.ok, m = sh.s.n1 + sh.s.n2;
+            if (!go) break;
+            if (ok == 1) {
+                swap_apply(p, sh.s, 0, tid, nth);
+                if (m == 2) {
+                    c.sync();  // the 2x2 block takes the column rotation before the row rotation
+                    swap_apply(p, sh.s, 1, tid, nth);
+                    c.sync();
+                    swap_apply(p, sh.s, 2, tid, nth);
+                }
+            }
+            c.sync();
+            if (tid == 0) walk_after(p, sh.w);
+        }
+        c.sync();  // every thread has left the walk before its state is reused
+        if (tid == 0) {
+            sh.nbk = 0;
+            sh.d = R(0);  // a rejected swap: DIF = 0
+            if (sh.info == 3) *err = 1;
+            if (sh.info == 0) {
+                const int n1 = Aw[1] != R(0) ? 2 : 1;
+                if (n - n1 == 0) {
+                    sh.d = sh.cond;
+                } else {
+                    Sylv<R> &y = sh.y;
+                    y.n1 = n1;
+                    y.n2 = n - n1;
+                    y.ld = n;
+                    y.ldc = n;
+                    y.A22 = Aw + n1 + (size_t)n1 * n;
+                    y.B22 = Bw + n1 + (size_t)n1 * n;
+                    for (int q = 0; q < 16; q++) {
+                        y.A11s[q] = R(0);
+                        y.B11s[q] = R(0);
+                    }
+                    for (int j = 0; j < n1; j++)
+                        for (int i = 0; i < n1; i++) {
+                            y.A11s[i + LD * j] = Aw[i + (size_t)j * n];
+                            y.B11s[i + LD * j] = Bw[i + (size_t)j * n];
+                        }
+                    y.C = Cw;
+                    y.F = Fw;
+                    y.dsum = R(1);
+                    y.dscale = R(0);
+                    sh.nbk = tgsyl_blocks(y, starts);
+                }
+            }
+        }
+        c.sync();
+        const int nbk = sh.nbk;
+        for (int b = nbk - 1; b >= 0; b--) {
+            if (tid == 0) tgsyl_block(sh.y, starts[b], starts[b + 1] - 1);
+            c.sync();
+            tgsyl_update_above(sh.y, starts[b], starts[b + 1] - 1, tid, nth);
+            c.sync();
+        }
+        if (tid == 0) {
+            R d = sh.d;
+            if (nbk > 0) {
+                d = xsqrt(R(2 * sh.y.n1 * sh.y.n2)) / (sh.y.dscale * xsqrt(sh.y.dsum));
+                if (item.pair) d = xmin(d, sh.cond);
+            }
+            dif[item.ks] = d;
+            if (item.pair) dif[item.ks + 1] = d;
+        }
+        c.sync();  // the workspace is reused by the next item
+    }
+}
+
 }  // namespace rb
 }  // namespace xtg

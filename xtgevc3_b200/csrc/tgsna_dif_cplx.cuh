@@ -437,5 +437,95 @@ XTG_HD R zdif_serial(int n, const zc<R> *A, int lda, const zc<R> *B, int ldb, in
     return zdif_reordered_serial(n, Aw, Bw, n, C, F, starts);
 }
 
+// ---- the GPU kernel's body, one CTA (CTA context as for dif_cta in tgsna_dif.cuh) ---------
+
+// workspace of one CTA in complex elements: the copy (2 n^2), C and F (n each), ZTGSYL's block
+// starts (n / 2 + 4 ints in n + 8 elements of room)
+XTG_HD inline size_t zdif_work_elems(int n) { return 2 * (size_t)n * n + 3 * (size_t)n + 8; }
+
+template <class R>
+struct ZDifShared {
+    ZSwap<R> s;
+    ZSylv<R> y;
+    int rej, nbk;
+};
+
+// DIF of the items it = c.cta(), c.cta() + c.ncta(), ... of a complex pencil: copy, move the
+// eigenvalue up one row per swap (thread 0 computes the rotations, the CTA applies them; at
+// most k swaps), ZTGSYL's estimate (thread 0 per block, the CTA updates the rows above).
+template <class R, class Cta>
+XTG_HD void zdif_cta(const Cta &c, ZDifShared<R> &sh, int n, const zc<R> *A, int lda, const zc<R> *B, int ldb,
+                     const DifItem *items, int count, R *dif, zc<R> *work, size_t per_cta)
+{
+    const int tid = c.tid(), nth = c.nth();
+    zc<R> *Aw = work + (size_t)c.cta() * per_cta;
+    zc<R> *Bw = Aw + (size_t)n * n;
+    zc<R> *Cw = Bw + (size_t)n * n;
+    zc<R> *Fw = Cw + n;
+    int *starts = reinterpret_cast<int *>(Fw + n);
+    for (int it = c.cta(); it < count; it += c.ncta()) {
+        const DifItem item = items[it];
+        if (n == 1) {
+            if (tid == 0) dif[item.ks] = lapy2(cabs(A[0]), cabs(B[0]));
+            continue;
+        }
+        for (size_t e = tid; e < (size_t)n * n; e += nth) {
+            const size_t i = e % n, j = e / n;
+            Aw[e] = A[i + j * lda];
+            Bw[e] = B[i + j * ldb];
+        }
+        for (int e = tid; e < n; e += nth) {
+            Cw[e] = mk(R(0), R(0));
+            Fw[e] = mk(R(0), R(0));
+        }
+        if (tid == 0) sh.rej = 0;
+        c.sync();  // the copy is complete before thread 0 reads it
+        for (int here = item.k; here > 0; here--) {
+            if (tid == 0) {
+                sh.s.j = here - 1;
+                zswap_prepare(Aw, Bw, n, sh.s);
+                sh.rej = sh.s.ok ? 0 : 1;
+            }
+            c.sync();  // thread 0 writes rej / s again only after this iteration's last barrier
+            if (sh.rej) break;
+            zswap_apply(Aw, Bw, n, n, sh.s, 0, tid, nth);
+            c.sync();  // the 2x2 block takes the column rotation before the row rotation
+            zswap_apply(Aw, Bw, n, n, sh.s, 1, tid, nth);
+            c.sync();
+            zswap_apply(Aw, Bw, n, n, sh.s, 2, tid, nth);
+            c.sync();
+        }
+        c.sync();  // every thread has left the walk
+        if (tid == 0) {
+            sh.nbk = 0;
+            if (!sh.rej) {
+                ZSylv<R> &y = sh.y;
+                y.n2 = n - 1;
+                y.ld = n;
+                y.A22 = Aw + 1 + (size_t)n;
+                y.B22 = Bw + 1 + (size_t)n;
+                y.a11 = Aw[0];
+                y.b11 = Bw[0];
+                y.C = Cw;
+                y.F = Fw;
+                y.dsum = R(1);
+                y.dscale = R(0);
+                sh.nbk = ztgsyl_blocks(n - 1, starts);
+            }
+        }
+        c.sync();
+        const int nbk = sh.nbk;
+        for (int b = nbk - 1; b >= 0; b--) {
+            if (tid == 0) ztgsyl_block(sh.y, starts[b], starts[b + 1] - 1);
+            c.sync();
+            ztgsyl_update_above(sh.y, starts[b], starts[b + 1] - 1, tid, nth);
+            c.sync();
+        }
+        if (tid == 0)  // a rejected swap: DIF = 0
+            dif[item.ks] = nbk > 0 ? xsqrt(R(2 * sh.y.n2)) / (sh.y.dscale * xsqrt(sh.y.dsum)) : R(0);
+        c.sync();  // the workspace is reused by the next item
+    }
+}
+
 }  // namespace rb
 }  // namespace xtg
