@@ -44,8 +44,8 @@ def host():
     src = os.path.join(ROOT, "tests", "tgexc_blocks_host.cpp")
     hdr = os.path.join(ROOT, "xtgevc3_b200", "csrc", "tgexc_real_blocks.cuh")
     if not os.path.exists(lib) or os.path.getmtime(lib) < max(os.path.getmtime(src), os.path.getmtime(hdr)):
-        r = subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-ffp-contract=off", "-o", lib, src],
-                           capture_output=True, text=True)
+        r = subprocess.run(["g++", "-O2", "-std=c++20", "-pthread", "-shared", "-fPIC", "-ffp-contract=off", "-o", lib,
+                            src], capture_output=True, text=True)
         assert r.returncode == 0, r.stderr
     return ct.CDLL(lib)
 
@@ -269,3 +269,25 @@ def test_hard_pencils_keep_lapack_control_flow(host, kind):
             for W in (q, z):
                 assert np.abs(W.T @ W - np.eye(n)).max() < 1e-13
             assert np.abs(np.tril(b, -1)).max() == 0 and np.abs(np.tril(a, -2)).max() == 0
+
+
+@pytest.mark.timeout(300)
+def test_kernel_body_on_host_threads(host):
+    """The reordering kernel's body (rb::walk_cta, the code the GPU kernel runs) on host
+    threads, one std::thread per GPU thread and a std::barrier for the CTA barrier: every
+    thread reaches every barrier (a mismatch would hang: the timeout fails it), and A, B, Q,
+    Z, IFST, ILST and INFO equal the serial build's bit for bit for 1 to 512 threads."""
+    cases = [(pencils.gen_gges(40, 31)[:2] + pencils.gen_gges(40, 31)[5:7], (40, 1)),
+             (pencils.gen_gges(40, 31)[:2] + pencils.gen_gges(40, 31)[5:7], (2, 39)),
+             (pencils.gen_gges(25, 5)[:2] + pencils.gen_gges(25, 5)[5:7], (13, 14)),
+             (_twin_blocks_pencil(1), (4, 2))]
+    for (S, T, Q, Z), (f0, l0) in cases:
+        ref = host_tgexc(host, S, T, Q, Z, f0, l0)
+        n = S.shape[0]
+        for nth in (1, 5, 64, 512):
+            A, B, Qc, Zc = _copies(S, T, Q, Z)
+            f, l_ = ct.c_int(f0), ct.c_int(l0)
+            info = host.threads_dtgexc(nth, 1, 1, n, _p(A), n, _p(B), n, _p(Qc), n, _p(Zc), n, ct.byref(f), ct.byref(l_))
+            assert (f.value, l_.value, info) == ref[4:], (n, f0, l0, nth)
+            for M, R in zip((A, B, Qc, Zc), ref[:4]):
+                np.testing.assert_array_equal(M, R)

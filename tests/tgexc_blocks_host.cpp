@@ -1,7 +1,12 @@
 // The real reordering kernel's arithmetic compiled for the CPU (test harness, not a product
 // path): xtgevc3_b200/csrc/tgexc_real_blocks.cuh is host and device code, so the swaps and the
 // walk that the GPU kernel runs can be compared with LAPACK D/STGEX2 and D/STGEXC on a machine
-// without a GPU.  Built by tests/test_tgexc_blocks_host.py with g++ into a temporary folder.
+// without a GPU; the kernel's own body (walk_cta) also runs here on host threads.  Built by
+// tests/test_tgexc_blocks_host.py with g++ into tests/_build.
+#include <barrier>
+#include <thread>
+#include <vector>
+
 #include "../xtgevc3_b200/csrc/tgexc_real_blocks.cuh"
 
 using namespace xtg::rb;
@@ -28,9 +33,44 @@ int swap_one(const Pencil<R> &p, int j1, int n1, int n2)
     return s.ok == 0 ? 1 : 0;
 }
 
+// The CTA context of walk_cta on host threads: one std::thread per GPU thread, the CTA
+// barrier a std::barrier.
+struct CtaHost {
+    int t, n;
+    std::barrier<> *bar;
+    int tid() const { return t; }
+    int nth() const { return n; }
+    int cta() const { return 0; }
+    int ncta() const { return 1; }
+    void sync() const { bar->arrive_and_wait(); }
+};
+
+// the reordering kernel's body (walk_cta) on nth host threads: INFO, ifst / ilst as the kernel
+// reports them
+template <class R>
+int walk_threads(int nth, const Pencil<R> &p, int *ifst, int *ilst)
+{
+    WalkShared<R> sh{};
+    std::barrier<> bar(nth);
+    std::vector<std::thread> th;
+    for (int t = 0; t < nth; t++) th.emplace_back([&, t] { walk_cta(CtaHost{t, nth, &bar}, sh, p, *ifst, *ilst); });
+    for (auto &x : th) x.join();
+    if (p.n > 1) {
+        *ifst = sh.ifst;
+        *ilst = sh.ilst;
+    }
+    return sh.info;
+}
+
 }  // namespace
 
 extern "C" {
+
+int threads_dtgexc(int nth, int wantq, int wantz, int n, double *A, int lda, double *B, int ldb, double *Q, int ldq,
+                   double *Z, int ldz, int *ifst, int *ilst)
+{
+    return walk_threads(nth, pencil(wantq, wantz, n, A, lda, B, ldb, Q, ldq, Z, ldz), ifst, ilst);
+}
 
 int host_dtgexc(int wantq, int wantz, int n, double *A, int lda, double *B, int ldb, double *Q, int ldq, double *Z,
                 int ldz, int *ifst, int *ilst)

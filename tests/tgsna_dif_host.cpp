@@ -2,7 +2,7 @@
 // product path): xtgevc3_b200/csrc/tgsna_dif.cuh and tgexc_real_blocks.cuh are host and
 // device code, so the estimate the GPU kernel computes per eigenvalue (reorder a copy, then
 // xTGSYL's Frobenius-norm estimate) can be compared with LAPACK D/STGSNA on a machine
-// without a GPU.  Built by tests/test_tgsna_dif_host.py with g++ into a temporary folder.
+// without a GPU.  Built by tests/test_tgsna_dif_host.py with g++ into tests/_build.
 #include <barrier>
 #include <thread>
 #include <vector>

@@ -442,68 +442,20 @@ __global__ void __launch_bounds__(kReorderThreads, 1) tgexc_real_kernel(ReorderA
 }
 
 // Real pencils with 2x2 blocks in the rows of the move (the general D/STGEXC walk and D/STGEX2
-// swaps of tgexc_real_blocks.cuh).  Thread 0 walks and computes each swap's small-block
-// arithmetic; the CTA applies the swap (O(n) rows and columns) between barriers.  The walk
-// moves the block at least one row every two swaps, so it ends within 4 n + 16 swaps; the
-// loop is bounded by that count all the same (status 3 if it were ever reached).
+// swaps of tgexc_real_blocks.cuh, rb::walk_cta: thread 0 walks and computes each swap's
+// small-block arithmetic, the CTA applies the swap between barriers; bounded by 4 n + 16 swaps,
+// status 3 if that were ever reached).
 // status: {ILST on exit (1-based), INFO (0 / 1 / 3), IFST on exit (1-based)}
 template <class R>
 __global__ void __launch_bounds__(kReorderThreads, 1)
     tgexc_real_blocks_kernel(rb::Pencil<R> p, int ifst, int ilst, int *status)
 {
-    __shared__ rb::Swap<R> s;
-    __shared__ rb::Walk w;
-    __shared__ int s_go, s_ifst, s_ilst, s_info;
+    __shared__ rb::WalkShared<R> sh;
+    rb::walk_cta(rb::CtaDev{}, sh, p, ifst, ilst);
     if (threadIdx.x == 0) {
-        int f = ifst, l = ilst;
-        s_go = (p.n > 1 && rb::walk_begin(p, w, f, l)) ? 1 : 0;
-        s_ifst = f;
-        s_ilst = l;
-        s_info = 0;
-        s.ok = 0;
-        s.n1 = s.n2 = 1;
-    }
-    const int limit = 4 * p.n + 16;
-    for (int it = 0;; it++) {
-        if (threadIdx.x == 0 && s_go) {
-            int j1, n1, n2;
-            if (it >= limit) {
-                s_go = 0;
-                s_info = 3;
-            } else if (!rb::walk_next(p, w, j1, n1, n2)) {
-                s_go = 0;
-                s_ilst = w.here;
-            } else {
-                s.j1 = j1 - 1;
-                s.n1 = n1;
-                s.n2 = n2;
-                rb::swap_prepare(p, s);
-                if (s.ok == 0) {
-                    s_go = 0;
-                    s_ilst = w.here;
-                    s_info = 1;
-                }
-            }
-        }
-        __syncthreads();  // (1): the decision and the swap are visible to the CTA
-        const int go = s_go, ok = s.ok, m = s.n1 + s.n2;
-        if (!go) break;
-        if (ok == 1) {
-            rb::swap_apply(p, s, 0, threadIdx.x, blockDim.x);
-            if (m == 2) {
-                __syncthreads();  // the 2x2 block takes the column rotation before the row rotation
-                rb::swap_apply(p, s, 1, threadIdx.x, blockDim.x);
-                __syncthreads();
-                rb::swap_apply(p, s, 2, threadIdx.x, blockDim.x);
-            }
-        }
-        __syncthreads();  // (2): the swap is in memory before thread 0 reads A again
-        if (threadIdx.x == 0) rb::walk_after(p, w);
-    }
-    if (threadIdx.x == 0) {
-        status[0] = s_ilst;
-        status[1] = s_info;
-        status[2] = s_ifst;
+        status[0] = sh.ilst;
+        status[1] = sh.info;
+        status[2] = sh.ifst;
     }
 }
 

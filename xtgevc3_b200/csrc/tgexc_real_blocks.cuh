@@ -1247,6 +1247,117 @@ XTG_HD void swap_apply(const Pencil<R> &p, const Swap<R> &s, int phase, int tid,
         }
 }
 
+// ---- the reordering on one CTA ----------------------------------------------------------------
+// Written against a CTA context c (c.tid(), c.nth(): this thread and the CTA's size; c.cta(),
+// c.ncta(): this CTA and the grid's size; c.sync(): the CTA barrier): the kernels pass
+// CtaDev (threadIdx, __syncthreads), the tests host threads with a barrier.
+struct CtaDev {
+    XTG_HD int tid() const
+    {
+#ifdef __CUDA_ARCH__
+        return (int)threadIdx.x;
+#else
+        return 0;
+#endif
+    }
+    XTG_HD int nth() const
+    {
+#ifdef __CUDA_ARCH__
+        return (int)blockDim.x;
+#else
+        return 1;
+#endif
+    }
+    XTG_HD int cta() const
+    {
+#ifdef __CUDA_ARCH__
+        return (int)blockIdx.x;
+#else
+        return 0;
+#endif
+    }
+    XTG_HD int ncta() const
+    {
+#ifdef __CUDA_ARCH__
+        return (int)gridDim.x;
+#else
+        return 1;
+#endif
+    }
+    XTG_HD void sync() const
+    {
+#ifdef __CUDA_ARCH__
+        __syncthreads();
+#endif
+    }
+};
+
+// the CTA's shared state of a walk (shared memory on the GPU)
+template <class R>
+struct WalkShared {
+    Swap<R> s;
+    Walk w;
+    int go, info, ifst, ilst;
+};
+
+// The walk of the block at row ifst to row ilst (1-based) on one CTA: thread 0 decides and
+// computes each swap, the CTA applies it.  The walk moves the block at least one row every two
+// swaps, so it ends within 4 n + 16 swaps; the loop is bounded by that count all the same.  On
+// return (every thread, after a barrier): sh.info = 0, 1 (a swap was rejected) or 3 (the
+// bound was reached); sh.ifst, sh.ilst as xTGEXC leaves them.
+template <class R, class Cta>
+XTG_HD void walk_cta(const Cta &c, WalkShared<R> &sh, const Pencil<R> &p, int ifst, int ilst)
+{
+    const int tid = c.tid(), nth = c.nth();
+    if (tid == 0) {
+        int f = ifst, l = ilst;
+        sh.go = (p.n > 1 && walk_begin(p, sh.w, f, l)) ? 1 : 0;
+        sh.ifst = f;
+        sh.ilst = l;
+        sh.info = 0;
+        sh.s.ok = 0;
+        sh.s.n1 = sh.s.n2 = 1;
+    }
+    const int limit = 4 * p.n + 16;
+    for (int step = 0;; step++) {
+        if (tid == 0 && sh.go) {
+            int j1, n1, n2;
+            if (step >= limit) {
+                sh.go = 0;
+                sh.info = 3;
+            } else if (!walk_next(p, sh.w, j1, n1, n2)) {
+                sh.go = 0;
+                sh.ilst = sh.w.here;
+            } else {
+                sh.s.j1 = j1 - 1;
+                sh.s.n1 = n1;
+                sh.s.n2 = n2;
+                swap_prepare(p, sh.s);
+                if (sh.s.ok == 0) {
+                    sh.go = 0;
+                    sh.ilst = sh.w.here;
+                    sh.info = 1;
+                }
+            }
+        }
+        c.sync();  // (1): thread 0 writes go / s again only after barrier (2)
+        const int go = sh.go, ok = sh.s.ok, m = sh.s.n1 + sh.s.n2;
+        if (!go) break;
+        if (ok == 1) {
+            swap_apply(p, sh.s, 0, tid, nth);
+            if (m == 2) {
+                c.sync();  // the 2x2 block takes the column rotation before the row rotation
+                swap_apply(p, sh.s, 1, tid, nth);
+                c.sync();
+                swap_apply(p, sh.s, 2, tid, nth);
+            }
+        }
+        c.sync();  // (2): the swap is in memory before thread 0 reads A again
+        if (tid == 0) walk_after(p, sh.w);
+    }
+    c.sync();  // every thread has left the loop before the state is read or reused
+}
+
 // The whole reordering on one thread (the tests' CPU build of this header): returns INFO
 // (0, or 1 when a swap was rejected), with ifst and ilst as xTGEXC leaves them.
 template <class R>

@@ -29,55 +29,13 @@ using rb::DifItem;
 using rb::dif_work_elems;
 using rb::zdif_work_elems;
 
-// The CTA context of the kernel bodies (rb::dif_cta, rb::zdif_cta) on the GPU
-struct CtaDev {
-    XTG_HD int tid() const
-    {
-#ifdef __CUDA_ARCH__
-        return (int)threadIdx.x;
-#else
-        return 0;
-#endif
-    }
-    XTG_HD int nth() const
-    {
-#ifdef __CUDA_ARCH__
-        return (int)blockDim.x;
-#else
-        return 1;
-#endif
-    }
-    XTG_HD int cta() const
-    {
-#ifdef __CUDA_ARCH__
-        return (int)blockIdx.x;
-#else
-        return 0;
-#endif
-    }
-    XTG_HD int ncta() const
-    {
-#ifdef __CUDA_ARCH__
-        return (int)gridDim.x;
-#else
-        return 1;
-#endif
-    }
-    XTG_HD void sync() const
-    {
-#ifdef __CUDA_ARCH__
-        __syncthreads();
-#endif
-    }
-};
-
 template <class R>
 __global__ void __launch_bounds__(kDifThreads)
     tgsna_dif_kernel(int n, const R *A, int lda, const R *B, int ldb, const DifItem *items, int count, R *dif,
                      R *work, size_t per_cta, int *err)
 {
     __shared__ rb::DifShared<R> sh;
-    rb::dif_cta(CtaDev{}, sh, n, A, lda, B, ldb, items, count, dif, work, per_cta, err);
+    rb::dif_cta(rb::CtaDev{}, sh, n, A, lda, B, ldb, items, count, dif, work, per_cta, err);
 }
 
 template <class R>
@@ -86,7 +44,7 @@ __global__ void __launch_bounds__(kDifThreads)
                           int count, R *dif, rb::zc<R> *work, size_t per_cta)
 {
     __shared__ rb::ZDifShared<R> sh;
-    rb::zdif_cta(CtaDev{}, sh, n, A, lda, B, ldb, items, count, dif, work, per_cta);
+    rb::zdif_cta(rb::CtaDev{}, sh, n, A, lda, B, ldb, items, count, dif, work, per_cta);
 }
 
 }  // namespace

@@ -278,8 +278,7 @@ XTG_HD R dif_reordered_serial(int n, const R *A, const R *B, int ld, R *C, R *F,
 }
 
 // ---- the GPU kernel's body, one CTA ---------------------------------------------------------
-// Written against a CTA context c (c.tid(), c.nth(): this thread and the CTA's size; c.cta(),
-// c.ncta(): this CTA and the grid's size; c.sync(): the CTA barrier) so that the kernel
+// Written against a CTA context (see walk_cta in tgexc_real_blocks.cuh) so that the kernel
 // (tgsna_dif.cu: shared memory, __syncthreads) and the tests (host threads with a barrier)
 // run the same code.
 
@@ -295,17 +294,15 @@ XTG_HD inline size_t dif_work_elems(int n) { return 2 * (size_t)n * n + 4 * (siz
 // the CTA's shared state (shared memory on the GPU)
 template <class R>
 struct DifShared {
-    Swap<R> s;
-    Walk w;
+    WalkShared<R> walk;
     Sylv<R> y;
-    int go, info, nbk;
+    int nbk;
     R cond, d;
 };
 
 // DIF of the items it = c.cta(), c.cta() + c.ncta(), ... of a real pencil (A, B): copy, walk
-// the block to the top (thread 0 decides and computes each swap, the CTA applies it; bounded
-// by 4 n + 16 swaps, *err = 1 if that bound were reached), xTGSYL's estimate (thread 0 solves
-// each block, the CTA updates the rows above it).
+// the block to the top (walk_cta; *err = 1 if its swap bound were reached), xTGSYL's estimate
+// (thread 0 solves each block, the CTA updates the rows above it).
 template <class R, class Cta>
 XTG_HD void dif_cta(const Cta &c, DifShared<R> &sh, int n, const R *A, int lda, const R *B, int ldb,
                     const DifItem *items, int count, R *dif, R *work, size_t per_cta, int *err)
@@ -341,54 +338,12 @@ XTG_HD void dif_cta(const Cta &c, DifShared<R> &sh, int n, const R *A, int lda, 
                                     B[k + (size_t)(k + 1) * ldb], B[k + 1 + (size_t)(k + 1) * ldb]);
         }
         c.sync();  // the copy is complete before thread 0 reads it
-        if (tid == 0) {
-            int f = item.k + 1, l = 1;
-            sh.go = walk_begin(p, sh.w, f, l) ? 1 : 0;
-            sh.info = 0;
-            sh.s.ok = 0;
-            sh.s.n1 = sh.s.n2 = 1;
-        }
-        const int limit = 4 * n + 16;
-        for (int step = 0;; step++) {  // the reordering kernel's walk loop
-            if (tid == 0 && sh.go) {
-                int j1, n1, n2;
-                if (step >= limit) {
-                    sh.go = 0;
-                    sh.info = 3;
-                } else if (!walk_next(p, sh.w, j1, n1, n2)) {
-                    sh.go = 0;
-                } else {
-                    sh.s.j1 = j1 - 1;
-                    sh.s.n1 = n1;
-                    sh.s.n2 = n2;
-                    swap_prepare(p, sh.s);
-                    if (sh.s.ok == 0) {
-                        sh.go = 0;
-                        sh.info = 1;
-                    }
-                }
-            }
-            c.sync();  // thread 0 writes go / s again only after the barrier at the loop's end
-            const int go = sh.go, ok = sh.s.ok, m = sh.s.n1 + sh.s.n2;
-            if (!go) break;
-            if (ok == 1) {
-                swap_apply(p, sh.s, 0, tid, nth);
-                if (m == 2) {
-                    c.sync();  // the 2x2 block takes the column rotation before the row rotation
-                    swap_apply(p, sh.s, 1, tid, nth);
-                    c.sync();
-                    swap_apply(p, sh.s, 2, tid, nth);
-                }
-            }
-            c.sync();
-            if (tid == 0) walk_after(p, sh.w);
-        }
-        c.sync();  // every thread has left the walk before its state is reused
+        walk_cta(c, sh.walk, p, item.k + 1, 1);  // ends with a barrier
         if (tid == 0) {
             sh.nbk = 0;
             sh.d = R(0);  // a rejected swap: DIF = 0
-            if (sh.info == 3) *err = 1;
-            if (sh.info == 0) {
+            if (sh.walk.info == 3) *err = 1;
+            if (sh.walk.info == 0) {
                 const int n1 = Aw[1] != R(0) ? 2 : 1;
                 if (n - n1 == 0) {
                     sh.d = sh.cond;
