@@ -289,6 +289,30 @@ int xtgevc3_dtgexc_dev(void *stream, int wantq, int wantz, int n, double *A, int
 int xtgevc3_stgexc_dev(void *stream, int wantq, int wantz, int n, float *A, int lda, float *B, int ldb, float *Q,
                        int ldq, float *Z, int ldz, int *ifst, int *ilst, int *info);
 
+/* ---- generalized Schur form of a complex pencil: Z/CGGES without ordering (no counterpart
+ * upstream, which assumes this step done) -----------------------------------------------
+ * A = VSL S VSR^H, B = VSL T VSR^H with VSL, VSR unitary, S, T upper triangular (overwriting
+ * A, B) and T's diagonal real and non-negative; alpha = diag(S), beta = diag(T) (the
+ * eigenvalues alpha / beta).  LAPACK ZGGES's arguments without ordering (SORT = 'N': no
+ * SELCTG, SDIM) and without workspace: JOBVSL / JOBVSR 'V' or 'N'; INFO as LAPACK numbers its
+ * arguments (-1 JOBVSL, -2 JOBVSR, -5 N, -7 LDA, -9 LDB, -14 LDVSL, -16 LDVSR), or i > 0 when
+ * the QZ iterations did not deflate eigenvalue i within 30 n iterations (S, T not in Schur
+ * form then).  No balancing of the pencil (LAPACK's ZGGBAL / scaling): the form is computed
+ * for (A, B) as given.  One CTA runs the chain of rotations (B triangular, Hessenberg-
+ * triangular reduction, single-shift QZ), so the call is latency-bound; its value is the
+ * result staying on the device for the eigenvector solve (xtgevc3_ztgevc3_dev).  Complex
+ * arrays interleaved.  Device form: every array a device pointer (alpha, beta n complex
+ * values each), the call returns once the form is computed (0, or 1 when a CUDA call
+ * failed).                                                                                 */
+void xtgevc3_zgges(char jobvsl, char jobvsr, int n, double *A, int lda, double *B, int ldb, double *alpha,
+                   double *beta, double *VSL, int ldvsl, double *VSR, int ldvsr, int *info);
+void xtgevc3_cgges(char jobvsl, char jobvsr, int n, float *A, int lda, float *B, int ldb, float *alpha, float *beta,
+                   float *VSL, int ldvsl, float *VSR, int ldvsr, int *info);
+int xtgevc3_zgges_dev(void *stream, char jobvsl, char jobvsr, int n, double *A, int lda, double *B, int ldb,
+                      double *alpha, double *beta, double *VSL, int ldvsl, double *VSR, int ldvsr, int *info);
+int xtgevc3_cgges_dev(void *stream, char jobvsl, char jobvsr, int n, float *A, int lda, float *B, int ldb, float *alpha,
+                      float *beta, float *VSL, int ldvsl, float *VSR, int ldvsr, int *info);
+
 /* ---- allocation-free device entry point (no counterpart in the upstream library) -----
  * Same computation and arguments as xtgevc3_dtgevc3_dev (without flags), for callers that
  * cannot allocate device memory at this point: e.g. a framework that has reserved the

@@ -1,0 +1,79 @@
+"""xtgevc3_{z,c}gges (the generalized Schur form of a complex pencil, computed on the GPU)
+under the rules of test_qz_host.py (the same kernel body checked on the CPU): A = Q S Z^H,
+B = Q T Z^H, Q and Z unitary, S and T upper triangular with T's diagonal real and
+non-negative, LAPACK's eigenvalues, k zero betas for a B of rank n - k.  And the chain this
+step exists for: the form computed on the device, then the eigenvectors of (A, B) from it
+(xtgevc3_ztgevc3_dev, HOWMNY = 'B' back-transformed by Q and Z), checked by their residuals
+beta A x - alpha B x and y^H (beta A - alpha B) against the original pencil."""
+import numpy as np
+import pytest
+
+import xtgevc3_b200 as X
+from test_qz_host import check_form, eig_match, pencil
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(M):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(M.T)).cuda().t()
+
+
+@pytest.mark.parametrize("dt", [np.complex128, np.complex64], ids=["z", "c"])
+def test_gges_random_pencils(cuda_ok, dt):
+    single = dt == np.complex64
+    for n in (1, 5, 40, 100):
+        A, B = pencil(n, 300 + n, dt)
+        S, T, alpha, beta, Q, Z, info = X.gges(A, B)
+        assert info == 0
+        a2, b2 = check_form(A, B, S, T, Q, Z, single)
+        np.testing.assert_array_equal(alpha, a2)
+        np.testing.assert_array_equal(beta, b2)
+        assert eig_match(alpha, beta, A, B, single) == 0
+
+
+def test_gges_infinite_eigenvalues(cuda_ok):
+    for n, k in ((6, 1), (12, 2), (30, 3)):
+        A, B = pencil(n, 900 + n, rank_drop=k)
+        S, T, alpha, beta, Q, Z, info = X.gges(A, B)
+        assert info == 0
+        check_form(A, B, S, T, Q, Z)
+        assert eig_match(alpha, beta, A, B) == k
+
+
+def test_gges_device_form_matches_host_form(cuda_ok):
+    import torch
+    A, B = pencil(48, 4)
+    S, T, alpha, beta, Q, Z, info = X.gges(A, B)
+    dA, dB = _dev(A), _dev(B)
+    dQ = torch.empty((48, 48), dtype=torch.complex128, device="cuda").t()
+    dZ = torch.empty((48, 48), dtype=torch.complex128, device="cuda").t()
+    da, db, dinfo = X.gges_dev(dA, dB, dQ, dZ)
+    torch.cuda.synchronize()
+    assert dinfo == info == 0
+    for D, H in ((dA, S), (dB, T), (dQ, Q), (dZ, Z), (da, alpha), (db, beta)):
+        np.testing.assert_array_equal(D.cpu().numpy(), H)
+
+
+def test_schur_form_then_eigenvectors_on_the_device(cuda_ok):
+    """The QZ step and the eigenvector solve chained on device memory (only alpha and beta,
+    2 n numbers, cross to the host, as the eigenvector entry point takes them there)."""
+    import torch
+    n = 96
+    A, B = pencil(n, 11)
+    dA, dB = _dev(A), _dev(B)
+    dQ = torch.empty((n, n), dtype=torch.complex128, device="cuda").t()
+    dZ = torch.empty((n, n), dtype=torch.complex128, device="cuda").t()
+    alpha, beta, info = X.gges_dev(dA, dB, dQ, dZ)
+    assert info == 0
+    al, be = alpha.cpu().numpy(), beta.cpu().numpy()
+    m, info = X.tgevc3_dev("B", "B", dA, dB, al, be, VL=dQ, VR=dZ)
+    torch.cuda.synchronize()
+    assert (m, info) == (n, 0)
+    VL, VR = dQ.cpu().numpy(), dZ.cpu().numpy()
+    na, nb = np.abs(A).max(), np.abs(B).max()
+    for k in range(n):
+        x, y = VR[:, k], VL[:, k]
+        scale = (abs(be[k]) * na + abs(al[k]) * nb) * n
+        assert np.abs(be[k] * (A @ x) - al[k] * (B @ x)).max() <= 1e-12 * scale * np.abs(x).max()
+        assert np.abs(be[k] * (y.conj() @ A) - al[k] * (y.conj() @ B)).max() <= 1e-12 * scale * np.abs(y).max()
