@@ -289,8 +289,8 @@ int xtgevc3_dtgexc_dev(void *stream, int wantq, int wantz, int n, double *A, int
 int xtgevc3_stgexc_dev(void *stream, int wantq, int wantz, int n, float *A, int lda, float *B, int ldb, float *Q,
                        int ldq, float *Z, int ldz, int *ifst, int *ilst, int *info);
 
-/* ---- generalized Schur form of a complex pencil: Z/CGGES without ordering (no counterpart
- * upstream, which assumes this step done) -----------------------------------------------
+/* ---- generalized Schur form: Z/C/D/SGGES without ordering (no counterpart upstream, which
+ * assumes this step done) ------------------------------------------------------------------
  * A = VSL S VSR^H, B = VSL T VSR^H with VSL, VSR unitary, S, T upper triangular (overwriting
  * A, B) and T's diagonal real and non-negative; alpha = diag(S), beta = diag(T) (the
  * eigenvalues alpha / beta).  LAPACK ZGGES's arguments without ordering (SORT = 'N': no
@@ -312,6 +312,20 @@ int xtgevc3_zgges_dev(void *stream, char jobvsl, char jobvsr, int n, double *A, 
                       double *alpha, double *beta, double *VSL, int ldvsl, double *VSR, int ldvsr, int *info);
 int xtgevc3_cgges_dev(void *stream, char jobvsl, char jobvsr, int n, float *A, int lda, float *B, int ldb, float *alpha,
                       float *beta, float *VSL, int ldvsl, float *VSR, int ldvsr, int *info);
+/* Real pencils: D/SGGES without ordering, the generalized real Schur form (S upper
+ * quasi-triangular, 2x2 blocks for complex pairs facing diagonal blocks of T with positive
+ * entries, T's diagonal non-negative) and alphar, alphai, beta as LAPACK's DHGEQZ returns them
+ * (a pair: per-row alphar, alphai with alphai(j) > 0 > alphai(j+1), and its own betas).
+ * INFO numbered by DGGES's argument list (-15 LDVSL, -17 LDVSR; the others as above).     */
+void xtgevc3_dgges(char jobvsl, char jobvsr, int n, double *A, int lda, double *B, int ldb, double *alphar,
+                   double *alphai, double *beta, double *VSL, int ldvsl, double *VSR, int ldvsr, int *info);
+void xtgevc3_sgges(char jobvsl, char jobvsr, int n, float *A, int lda, float *B, int ldb, float *alphar, float *alphai,
+                   float *beta, float *VSL, int ldvsl, float *VSR, int ldvsr, int *info);
+int xtgevc3_dgges_dev(void *stream, char jobvsl, char jobvsr, int n, double *A, int lda, double *B, int ldb,
+                      double *alphar, double *alphai, double *beta, double *VSL, int ldvsl, double *VSR, int ldvsr,
+                      int *info);
+int xtgevc3_sgges_dev(void *stream, char jobvsl, char jobvsr, int n, float *A, int lda, float *B, int ldb,
+                      float *alphar, float *alphai, float *beta, float *VSL, int ldvsl, float *VSR, int ldvsr, int *info);
 
 /* ---- allocation-free device entry point (no counterpart in the upstream library) -----
  * Same computation and arguments as xtgevc3_dtgevc3_dev (without flags), for callers that

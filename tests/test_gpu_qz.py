@@ -77,3 +77,55 @@ def test_schur_form_then_eigenvectors_on_the_device(cuda_ok):
         scale = (abs(be[k]) * na + abs(al[k]) * nb) * n
         assert np.abs(be[k] * (A @ x) - al[k] * (B @ x)).max() <= 1e-12 * scale * np.abs(x).max()
         assert np.abs(be[k] * (y.conj() @ A) - al[k] * (y.conj() @ B)).max() <= 1e-12 * scale * np.abs(y).max()
+
+
+# ---- real pencils -------------------------------------------------------------------------
+from test_qz_host import check_real_form, real_eig_match, rpencil  # noqa: E402
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32], ids=["d", "s"])
+def test_real_gges_random_pencils(cuda_ok, dt):
+    single = dt == np.float32
+    for n in (1, 4, 40, 100):
+        A, B = rpencil(n, 600 + n, dt)
+        S, T, ar, ai, be, Q, Z, info = X.gges(A, B)
+        assert info == 0
+        check_real_form(A, B, S, T, Q, Z, ar, ai, be, single)
+        assert real_eig_match(A, B, ar, ai, be, single) == 0
+
+
+def test_real_gges_infinite_eigenvalues(cuda_ok):
+    for n, k in ((6, 1), (12, 2), (30, 3)):
+        A, B = rpencil(n, 800 + n, rank_drop=k)
+        S, T, ar, ai, be, Q, Z, info = X.gges(A, B)
+        assert info == 0
+        check_real_form(A, B, S, T, Q, Z, ar, ai, be)
+        assert real_eig_match(A, B, ar, ai, be) == k
+
+
+def test_real_schur_form_then_eigenvectors_on_the_device(cuda_ok):
+    """DGGES then DTGEVC3 on device memory (alphar, alphai, beta: 3 n numbers to the host)."""
+    import torch
+    n = 96
+    A, B = rpencil(n, 12)
+    dA, dB = _dev(A), _dev(B)
+    dQ = torch.empty((n, n), dtype=torch.float64, device="cuda").t()
+    dZ = torch.empty((n, n), dtype=torch.float64, device="cuda").t()
+    ar, ai, be, info = X.gges_dev(dA, dB, dQ, dZ)
+    assert info == 0
+    ar, ai, be = ar.cpu().numpy(), ai.cpu().numpy(), be.cpu().numpy()
+    m, info = X.tgevc3_dev("B", "B", dA, dB, ar, be, alphai=ai, VL=dQ, VR=dZ)
+    torch.cuda.synchronize()
+    assert (m, info) == (n, 0)
+    VL, VR = dQ.cpu().numpy(), dZ.cpu().numpy()
+    na, nb = np.abs(A).max(), np.abs(B).max()
+    k = 0
+    while k < n:
+        if ai[k] == 0:
+            x, y, a, w = VR[:, k], VL[:, k], ar[k], 1
+        else:
+            x, y, a, w = VR[:, k] + 1j * VR[:, k + 1], VL[:, k] + 1j * VL[:, k + 1], ar[k] + 1j * ai[k], 2
+        scale = (abs(be[k]) * na + abs(a) * nb) * n
+        assert np.abs(be[k] * (A @ x) - a * (B @ x)).max() <= 1e-12 * scale * np.abs(x).max()
+        assert np.abs(be[k] * (y.conj() @ A) - a * (y.conj() @ B)).max() <= 1e-12 * scale * np.abs(y).max()
+        k += w

@@ -158,3 +158,139 @@ def test_gges_argument_checks():
     assert call(ldr=n - 1) == -16
     assert call(nn=0, lda=1, ldb=1, ldl=1, ldr=1) == 0
     assert call(jl=b"N", jr=b"N", nn=0, lda=1, ldb=1, ldl=1, ldr=1) == 0
+
+
+# ---- real pencils (rb::dgges_cta) ------------------------------------------------------------
+def host_rqz(L, A, B, nth=1):
+    dt = A.dtype
+    n = A.shape[0]
+    a, b = np.asfortranarray(A).copy(order="F"), np.asfortranarray(B).copy(order="F")
+    q, z = np.zeros((n, n), dtype=dt, order="F"), np.zeros((n, n), dtype=dt, order="F")
+    ar, ai, be = (np.zeros(max(n, 1), dtype=dt) for _ in range(3))
+    f = L.host_dgges if dt == np.float64 else L.host_sgges
+    info = f(nth, 1, 1, n, *(_p(x) for x in (a, b, q, z, ar, ai, be)))
+    return a, b, q, z, ar[:n], ai[:n], be[:n], info
+
+
+def rpencil(n, seed, dt=np.float64, rank_drop=0):
+    r = np.random.default_rng(seed)
+    A, B = r.standard_normal((n, n)), r.standard_normal((n, n))
+    if rank_drop:
+        k = rank_drop
+        if seed % 2 == 0 or 2 * k > n:
+            B[:, :k] = 0
+        else:
+            B[:, :k] = B[:, k:2 * k]
+    return A.astype(dt), B.astype(dt)
+
+
+def check_real_form(A, B, S, T, Q, Z, ar, ai, be, single=False):
+    """A = Q S Z^T, B = Q T Z^T, Q, Z orthogonal; S quasi-triangular with non-overlapping 2x2
+    blocks, each facing a diagonal block of T with positive entries; T triangular with
+    non-negative diagonal; a 1x1 block's (alphar, alphai, beta) = (S_kk, 0, T_kk), a pair's
+    alphai of opposite signs."""
+    n = A.shape[0]
+    tol = (1e-5 if single else 1e-13) * max(n, 1)
+    for M, M0 in ((S, A), (T, B)):
+        assert np.abs(Q @ M @ Z.T - M0).max() <= tol * max(np.abs(M0).max(), 1e-300)
+    for W in (Q, Z):
+        assert np.abs(W.T @ W - np.eye(n)).max() <= tol
+    if n > 1:
+        assert np.abs(np.tril(S, -2)).max() == 0 and np.abs(np.tril(T, -1)).max() == 0
+    k = 0
+    while k < n:
+        if k + 1 < n and S[k + 1, k] != 0:
+            assert T[k, k + 1] == 0 and T[k, k] > 0 and T[k + 1, k + 1] > 0
+            assert k + 2 >= n or S[k + 2, k + 1] == 0
+            assert ai[k] > 0 > ai[k + 1] and be[k] > 0 and be[k + 1] > 0
+            k += 2
+        else:
+            assert T[k, k] >= 0 and (ar[k], ai[k], be[k]) == (S[k, k], 0, T[k, k])
+            k += 1
+
+
+def real_eig_match(A, B, ar, ai, be, single=False):
+    fin = np.abs(be) > (1e-5 if single else 1e-12) * max(np.abs(B).max(), 1)
+    ev = (ar[fin] + 1j * ai[fin]) / be[fin]
+    ref = scipy.linalg.eigvals(A.astype(np.float64), B.astype(np.float64))
+    ref = ref[np.isfinite(ref)]
+    for e in ev:
+        assert np.min(np.abs(ref - e)) <= (1e-3 if single else 1e-8) * max(1, abs(e)), e
+    return int((~fin).sum())
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32], ids=["d", "s"])
+def test_real_schur_form_of_random_pencils(host, dt):
+    single = dt == np.float32
+    for n in (1, 2, 3, 4, 5, 8, 17, 40, 64):
+        for seed in range(4):
+            A, B = rpencil(n, 3000 * n + seed, dt)
+            S, T, Q, Z, ar, ai, be, info = host_rqz(host, A, B)
+            assert info == 0
+            check_real_form(A, B, S, T, Q, Z, ar, ai, be, single)
+            assert real_eig_match(A, B, ar, ai, be, single) == 0
+
+
+def test_real_infinite_eigenvalues(host):
+    for n in (3, 6, 12, 30):
+        for k in (1, 2, 3):
+            if k >= n:
+                continue
+            for seed in range(4):
+                A, B = rpencil(n, 7000 + 100 * n + 10 * k + seed, rank_drop=k)
+                S, T, Q, Z, ar, ai, be, info = host_rqz(host, A, B)
+                assert info == 0
+                check_real_form(A, B, S, T, Q, Z, ar, ai, be)
+                assert real_eig_match(A, B, ar, ai, be) == k, (n, k, seed)
+
+
+@pytest.mark.timeout(300)
+def test_real_kernel_body_on_host_threads(host):
+    for n, k in ((7, 0), (33, 0), (16, 2)):
+        A, B = rpencil(n, n, rank_drop=k)
+        ref = host_rqz(host, A, B, 1)
+        for nth in (3, 64, 512):
+            got = host_rqz(host, A, B, nth)
+            for x, y in zip(got, ref):
+                np.testing.assert_array_equal(x, y)
+
+
+def test_real_form_feeds_the_eigenvector_solve(host):
+    """The real form and its alphar / alphai / beta taken by xTGEVC3 (the oracle's C
+    restatement, HOWMNY = 'B' with Q, Z): the eigenvectors of the original pencil, by their
+    residuals beta A x - alpha B x and y^H (beta A - alpha B)."""
+    import oracle
+    n = 80
+    A, B = rpencil(n, 5)
+    S, T, Q, Z, ar, ai, be, info = host_rqz(host, A, B)
+    VL, VR, m, info2 = oracle.tgevc3("B", "B", S, T, ar, be, alphai=ai, VL=Q.copy(order="F"), VR=Z.copy(order="F"))
+    assert (info, info2, m) == (0, 0, n)
+    na, nb = np.abs(A).max(), np.abs(B).max()
+    k = 0
+    while k < n:
+        if ai[k] == 0:
+            x, y, a, w = VR[:, k], VL[:, k], ar[k], 1
+        else:
+            x, y, a, w = VR[:, k] + 1j * VR[:, k + 1], VL[:, k] + 1j * VL[:, k + 1], ar[k] + 1j * ai[k], 2
+        b = be[k]
+        scale = (abs(b) * na + abs(a) * nb) * n
+        assert np.abs(b * (A @ x) - a * (B @ x)).max() <= 1e-12 * scale * np.abs(x).max()
+        assert np.abs(b * (y.conj() @ A) - a * (y.conj() @ B)).max() <= 1e-12 * scale * np.abs(y).max()
+        k += w
+
+
+def test_real_gges_argument_checks():
+    """xtgevc3_dgges: DGGES's INFO numbering (ALPHAR, ALPHAI shift LDVSL / LDVSR to -15 / -17)."""
+    n = 4
+    M = np.zeros((n, n), order="F")
+    v = np.zeros(n)
+    L = X.lib()
+
+    def call(jl=b"V", jr=b"V", nn=n, lda=n, ldb=n, ldl=n, ldr=n):
+        info = ct.c_int(99)
+        L.xtgevc3_dgges(jl, jr, nn, _p(M), lda, _p(M), ldb, _p(v), _p(v), _p(v), _p(M), ldl, _p(M), ldr, ct.byref(info))
+        return info.value
+    assert call(jl=b"X") == -1 and call(jr=b"X") == -2 and call(nn=-1) == -5
+    assert call(lda=n - 1) == -7 and call(ldb=n - 1) == -9
+    assert call(ldl=n - 1) == -15 and call(ldr=n - 1) == -17
+    assert call(nn=0, lda=1, ldb=1, ldl=1, ldr=1) == 0

@@ -117,6 +117,13 @@ def lib():
             f = getattr(L, f"xtgevc3_{p}gges_dev")
             f.argtypes = [_P, _C, _C, _I, _P, _I, _P, _I, _P, _P, _P, _I, _P, _I, _P]
             f.restype = _I
+        for p in "ds":  # real pencils: alphar, alphai, beta
+            f = getattr(L, f"xtgevc3_{p}gges")
+            f.argtypes = [_C, _C, _I, _P, _I, _P, _I, _P, _P, _P, _P, _I, _P, _I, _P]
+            f.restype = None
+            f = getattr(L, f"xtgevc3_{p}gges_dev")
+            f.argtypes = [_P, _C, _C, _I, _P, _I, _P, _I, _P, _P, _P, _P, _I, _P, _I, _P]
+            f.restype = _I
         for p in "dszc":  # xTGSNA DIF on the device
             f = getattr(L, f"xtgevc3_{p}tgsna_dif_dev")
             f.argtypes = [_P, _C, _P, _I, _P, _I, _P, _I, _P, _I, _P, _P]
@@ -439,37 +446,40 @@ def tgsna_dif_dev(A, B, howmny="A", select=None, stream=None):
 
 
 def gges(A, B, jobvsl="V", jobvsr="V"):
-    """Host-array form of z/cgges without ordering: the generalized Schur form of the complex
-    pencil (A, B), A = VSL S VSR^H, B = VSL T VSR^H.  Returns (S, T, alpha, beta, VSL, VSR,
-    info) with new arrays (VSL / VSR None for 'N')."""
+    """Host-array form of z/c/d/sgges without ordering: the generalized Schur form of the pencil
+    (A, B), A = VSL S VSR^H, B = VSL T VSR^H.  Complex: returns (S, T, alpha, beta, VSL, VSR,
+    info); real: (S, T, alphar, alphai, beta, VSL, VSR, info).  New arrays; VSL / VSR None for
+    'N'."""
     L = lib()
     dt = A.dtype.type
-    pfx = {np.complex128: "z", np.complex64: "c"}[dt]
+    pfx = {np.complex128: "z", np.complex64: "c", np.float64: "d", np.float32: "s"}[dt]
     n = A.shape[0]
     S, T = np.array(A, order="F", dtype=dt), np.array(B, order="F", dtype=dt)
-    alpha, beta = np.zeros(max(n, 1), dtype=dt), np.zeros(max(n, 1), dtype=dt)
     VL = np.zeros((n, n), dtype=dt, order="F") if jobvsl == "V" else None
     VR = np.zeros((n, n), dtype=dt, order="F") if jobvsr == "V" else None
     info = ct.c_int(0)
     ld = max(n, 1)
-    getattr(L, f"xtgevc3_{pfx}gges")(jobvsl.encode(), jobvsr.encode(), n, _ptr(S), ld, _ptr(T), ld, _ptr(alpha),
-                                     _ptr(beta), _ptr(VL), ld, _ptr(VR), ld, ct.byref(info))
+    if pfx in "zc":
+        eig = [np.zeros(max(n, 1), dtype=dt) for _ in range(2)]
+    else:
+        eig = [np.zeros(max(n, 1), dtype=dt) for _ in range(3)]
+    getattr(L, f"xtgevc3_{pfx}gges")(jobvsl.encode(), jobvsr.encode(), n, _ptr(S), ld, _ptr(T), ld,
+                                     *[_ptr(e) for e in eig], _ptr(VL), ld, _ptr(VR), ld, ct.byref(info))
     if info.value > n:
         raise RuntimeError(f"xtgevc3_{pfx}gges failed: {last_error()}")
-    return S, T, alpha[:n], beta[:n], VL, VR, info.value
+    return (S, T, *[e[:n] for e in eig], VL, VR, info.value)
 
 
 def gges_dev(A, B, VSL=None, VSR=None, stream=None):
-    """Device form of z/cgges on column-major CUDA tensors: A, B become S, T in place, VSL /
-    VSR (when given) the unitary factors.  Returns (alpha, beta, info), alpha / beta CUDA
-    tensors."""
+    """Device form of z/c/d/sgges on column-major CUDA tensors: A, B become S, T in place, VSL /
+    VSR (when given) the orthogonal / unitary factors.  Returns (alpha, beta, info) (complex)
+    or (alphar, alphai, beta, info) (real), the eigenvalue arrays CUDA tensors."""
     import torch
     L = lib()
-    pfx = {torch.complex128: "z", torch.complex64: "c"}[A.dtype]
+    pfx = {torch.complex128: "z", torch.complex64: "c", torch.float64: "d", torch.float32: "s"}[A.dtype]
     n = A.shape[0]
     st = ct.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
-    alpha = torch.zeros(max(n, 1), dtype=A.dtype, device=A.device)
-    beta = torch.zeros(max(n, 1), dtype=A.dtype, device=A.device)
+    eig = [torch.zeros(max(n, 1), dtype=A.dtype, device=A.device) for _ in range(2 if pfx in "zc" else 3)]
     info = ct.c_int(0)
 
     def ld(t):
@@ -479,11 +489,11 @@ def gges_dev(A, B, VSL=None, VSR=None, stream=None):
         return ct.c_void_p(t.data_ptr()) if t is not None else None
 
     rc = getattr(L, f"xtgevc3_{pfx}gges_dev")(st, b"V" if VSL is not None else b"N", b"V" if VSR is not None else b"N",
-                                             n, ptr(A), ld(A), ptr(B), ld(B), ptr(alpha), ptr(beta), ptr(VSL), ld(VSL),
-                                             ptr(VSR), ld(VSR), ct.byref(info))
+                                             n, ptr(A), ld(A), ptr(B), ld(B), *[ptr(e) for e in eig], ptr(VSL),
+                                             ld(VSL), ptr(VSR), ld(VSR), ct.byref(info))
     if rc:
         raise RuntimeError(f"xtgevc3_{pfx}gges_dev failed: {last_error()}")
-    return alpha[:n], beta[:n], info.value
+    return (*[e[:n] for e in eig], info.value)
 
 
 def tgexc(A, B, Q=None, Z=None, ifst=1, ilst=1, with_ifst=False):
