@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--z-n", type=int, default=4096, help="order of the ztgevc3 SIDE=R HOWMNY=A leg (0 skips)")
     ap.add_argument("--trevc3-n", type=int, default=8192, help="order of the dtrevc3 SIDE=B HOWMNY=B leg (0 skips)")
     ap.add_argument("--tgexc-n", type=int, default=4096, help="order of the ztgexc and dtgexc reordering legs (0 skips)")
+    ap.add_argument("--gges-n", type=int, default=0,
+                    help="order of the dgges (QZ step) leg beside LAPACK dgges; 0 (the default) skips it")
     ap.add_argument("--profile-case", default=None,
                     help="run one small case for an ncu capture and exit (no JSON line): plain:N (two dtgevc3 "
                          "B/B calls, FP64; plain_norm:N with the normalisation), split_i8:N / split_crt:N (the same, INT8 digit / residue split "
@@ -825,6 +827,47 @@ def measure_tgexc_blocks(args, X, torch):
     return out
 
 
+def measure_gges(args, X, torch):
+    """dgges without ordering (the QZ step) on an iid N(0,1) real pencil of order --gges-n, Q
+    and Z formed: device-resident inputs restored before each step outside the timed region,
+    CUDA-event timing; LAPACK DGGES (SciPy's OpenBLAS, SORT = 'N') on the same pencil beside it,
+    the eigenvalues compared (each matched to its nearest)."""
+    n = args.gges_n
+    rng = np.random.default_rng(args.seed + 53)
+    A_h, B_h = np.asfortranarray(rng.standard_normal((n, n))), np.asfortranarray(rng.standard_normal((n, n)))
+    A0, B0 = colmajor_cuda(A_h, torch), colmajor_cuda(B_h, torch)
+    A, B, Q, Z = (torch.empty_like(A0) for _ in range(4))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ts, res = [], None
+    for it in range(max(args.warmup, 1) + args.steps):
+        A.copy_(A0)
+        B.copy_(B0)
+        torch.cuda.synchronize()
+        e0.record()
+        res = X.gges_dev(A, B, Q, Z)
+        e1.record()
+        torch.cuda.synchronize()
+        if it >= max(args.warmup, 1):
+            ts.append(e0.elapsed_time(e1))
+    ms = float(np.mean(ts))
+    ar, ai, be = (t.cpu().numpy() for t in res[:3])
+    out = {"n": n, "ms": ms, "info": int(res[3]), "data": "iid N(0,1) real pencil, Q and Z formed"}
+    if not args.no_cpu:
+        import scipy.linalg.lapack as la
+        t0 = time.perf_counter()
+        r = la.dgges(lambda *a: 0, A_h.copy(order="F"), B_h.copy(order="F"), sort_t=0)
+        tc = time.perf_counter() - t0
+        ref = (r[3] + 1j * r[4]) / r[5]
+        fin = be != 0
+        ev = (ar[fin] + 1j * ai[fin]) / be[fin]
+        err = max([float(np.min(np.abs(ref - e)) / max(1.0, abs(e))) for e in ev] + [0.0])
+        out["cpu_lapack"] = {"seconds": tc, "cores": host_threads(), "kind": "LAPACK dgges (SciPy OpenBLAS), SORT='N'"}
+        out["speedup_vs_lapack"] = tc / (ms * 1e-3)
+        out["max_eigenvalue_rel_diff_vs_lapack"] = err
+    del A0, B0, A, B, Q, Z
+    return out
+
+
 def neighbours_brief(legs):
     """One compact entry per LAPACK-neighbour leg for the `config` block (device ms; LAPACK's
     seconds on the host and the ratio where the leg timed it).  A leg that is absent, failed
@@ -1219,6 +1262,7 @@ def main():
     txleg = measure_tgexc(args, X, torch) if args.tgexc_n > 0 and rank == 0 else None
     dxleg = measure_tgexc(args, X, torch, real=True) if args.tgexc_n > 0 and rank == 0 else None
     bxleg = measure_tgexc_blocks(args, X, torch) if args.tgexc_n > 0 and rank == 0 else None
+    qzleg = measure_gges(args, X, torch) if args.gges_n > 0 and rank == 0 else None
 
     if rank == 0:
         form_desc = {"plain": "plain FP64 (DMMA)", "split": f"split precision, {s} BF16 slices (tcgen05)",
@@ -1252,7 +1296,7 @@ def main():
                            "normalize": None if norm is None else {
                                "ms": norm["ms_per_call"], "gbs": norm["gbs"], "frac_of_hbm": norm["frac_of_hbm"]},
                            "neighbours": neighbours_brief({"ztgexc": txleg, "dtgexc": dxleg, "dtgexc_blocks": bxleg,
-                                                           "dtrevc3": trleg, "adjoint": adjoint}),
+                                                           "dtrevc3": trleg, "adjoint": adjoint, "dgges": qzleg}),
                            "batched": None if batched is None else {
                                "pencils_per_s": batched["value"], "speedup_vs_loop": batched["speedup_vs_loop"],
                                "d_ms": batched["d"]["ms"], "s_ms": batched["s"]["ms"],
@@ -1260,7 +1304,7 @@ def main():
                 "forms": forms_out, "clocks": h["clocks"], "e2e": e2e, "gpu_launches": h["launches"],
                 "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "normalize": norm, "batched": batched,
                 "adjoint": adjoint, "ztgevc3": zleg, "dtrevc3": trleg, "ztgexc": txleg, "dtgexc": dxleg,
-                "dtgexc_blocks": bxleg}
+                "dtgexc_blocks": bxleg, "dgges": qzleg}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
