@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--z-n", type=int, default=4096, help="order of the ztgevc3 SIDE=R HOWMNY=A leg (0 skips)")
     ap.add_argument("--trevc3-n", type=int, default=8192, help="order of the dtrevc3 SIDE=B HOWMNY=B leg (0 skips)")
     ap.add_argument("--tgexc-n", type=int, default=4096, help="order of the ztgexc and dtgexc reordering legs (0 skips)")
+    ap.add_argument("--tgsna-n", type=int, default=0,
+                    help="order of the dtgsna DIF leg beside LAPACK dtgsna JOB='V'; 0 (the default) skips it")
     ap.add_argument("--gges-n", type=int, default=0,
                     help="order of the dgges (QZ step) leg beside LAPACK dgges; 0 (the default) skips it")
     ap.add_argument("--profile-case", default=None,
@@ -868,6 +870,44 @@ def measure_gges(args, X, torch):
     return out
 
 
+def measure_tgsna_dif(args, X, torch):
+    """dtgsna JOB='V' (DIF of every eigenvalue) on a real generalized Schur stand-in of order
+    --tgsna-n (xGGES statistics): CUDA-event timing of xtgevc3_dtgsna_dif_dev on device-resident
+    S, P; LAPACK DTGSNA (SciPy's OpenBLAS) on the same pencil beside it, with the share of DIFs
+    equal to LAPACK's (1e-12) and the largest ratio between the two estimates."""
+    from xtgevc3_b200 import pencils as gen
+    import oracle
+    n = args.tgsna_n
+    S_h, P_h = gen.gen_schur_like(n, args.seed + 59)[:2]
+    S0, P0 = colmajor_cuda(S_h, torch), colmajor_cuda(P_h, torch)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ts, dif = [], None
+    for it in range(max(args.warmup, 1) + args.steps):
+        torch.cuda.synchronize()
+        e0.record()
+        dif, m, info = X.tgsna_dif_dev(S0, P0)
+        e1.record()
+        torch.cuda.synchronize()
+        if it >= max(args.warmup, 1):
+            ts.append(e0.elapsed_time(e1))
+    ms = float(np.mean(ts))
+    out = {"n": n, "ms": ms, "eigenvalues": int(m), "info": int(info),
+           "data": "real generalized Schur stand-in (xGGES statistics, standardised 2x2 blocks)"}
+    if not args.no_cpu:
+        t0 = time.perf_counter()
+        _, d, _, _ = oracle.lapack_tgsna("A", S_h, P_h, None, None, job="V")
+        tc = time.perf_counter() - t0
+        h = dif.cpu().numpy()
+        same = np.abs(h - d) <= 1e-12 * np.abs(d)
+        ratio = np.maximum(h / d, d / h)
+        out["cpu_lapack"] = {"seconds": tc, "cores": host_threads(), "kind": "LAPACK dtgsna JOB='V' (SciPy OpenBLAS)"}
+        out["speedup_vs_lapack"] = tc / (ms * 1e-3)
+        out["share_equal_to_lapack"] = float(same.mean())
+        out["max_ratio_to_lapack"] = float(ratio[np.isfinite(ratio)].max()) if np.isfinite(ratio).any() else None
+    del S0, P0
+    return out
+
+
 def neighbours_brief(legs):
     """One compact entry per LAPACK-neighbour leg for the `config` block (device ms; LAPACK's
     seconds on the host and the ratio where the leg timed it).  A leg that is absent, failed
@@ -1263,6 +1303,7 @@ def main():
     dxleg = measure_tgexc(args, X, torch, real=True) if args.tgexc_n > 0 and rank == 0 else None
     bxleg = measure_tgexc_blocks(args, X, torch) if args.tgexc_n > 0 and rank == 0 else None
     qzleg = measure_gges(args, X, torch) if args.gges_n > 0 and rank == 0 else None
+    difleg = measure_tgsna_dif(args, X, torch) if args.tgsna_n > 0 and rank == 0 else None
 
     if rank == 0:
         form_desc = {"plain": "plain FP64 (DMMA)", "split": f"split precision, {s} BF16 slices (tcgen05)",
@@ -1296,7 +1337,8 @@ def main():
                            "normalize": None if norm is None else {
                                "ms": norm["ms_per_call"], "gbs": norm["gbs"], "frac_of_hbm": norm["frac_of_hbm"]},
                            "neighbours": neighbours_brief({"ztgexc": txleg, "dtgexc": dxleg, "dtgexc_blocks": bxleg,
-                                                           "dtrevc3": trleg, "adjoint": adjoint, "dgges": qzleg}),
+                                                           "dtrevc3": trleg, "adjoint": adjoint, "dgges": qzleg,
+                                                           "dtgsna_dif": difleg}),
                            "batched": None if batched is None else {
                                "pencils_per_s": batched["value"], "speedup_vs_loop": batched["speedup_vs_loop"],
                                "d_ms": batched["d"]["ms"], "s_ms": batched["s"]["ms"],
@@ -1304,7 +1346,7 @@ def main():
                 "forms": forms_out, "clocks": h["clocks"], "e2e": e2e, "gpu_launches": h["launches"],
                 "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "normalize": norm, "batched": batched,
                 "adjoint": adjoint, "ztgevc3": zleg, "dtrevc3": trleg, "ztgexc": txleg, "dtgexc": dxleg,
-                "dtgexc_blocks": bxleg, "dgges": qzleg}
+                "dtgexc_blocks": bxleg, "dgges": qzleg, "dtgsna_dif": difleg}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
