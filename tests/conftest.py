@@ -14,6 +14,18 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); run with -m gpu")
+    config.addinivalue_line(
+        "markers",
+        "late(k): runs after every unmarked test, in increasing k; for kernels whose bodies are "
+        "checked on host threads (tests/*_host.py) but have not yet run on a B200, so that a "
+        "failure there under -x cannot hide the results of the kernels already validated")
+
+
+def pytest_collection_modifyitems(config, items):
+    def rank(item):
+        m = item.get_closest_marker("late")
+        return (0, 0) if m is None else (1, m.args[0] if m.args else 0)
+    items[:] = sorted(items, key=rank)  # stable: file order within each rank
 
 
 def golden_files():

@@ -171,6 +171,7 @@ BLOCK_MOVES = [(1, 40), (40, 1), (7, 33), (33, 7), (20, 21), (21, 20), (2, 39), 
 
 @pytest.mark.parametrize("dt", [np.float64, np.float32], ids=["d", "s"])
 @pytest.mark.parametrize("move", BLOCK_MOVES, ids=lambda m: f"{m[0]}to{m[1]}")
+@pytest.mark.late(1)
 def test_real_tgexc_blocks_match_lapack(cuda_ok, dt, move):
     """Moves through a real xGGES pencil (n = 40, most eigenvalues complex pairs)."""
     from xtgevc3_b200 import pencils
@@ -184,6 +185,7 @@ def test_real_tgexc_blocks_match_lapack(cuda_ok, dt, move):
         assert _rel(M, R) < {np.float64: 1e-11, np.float32: 1e-4}[dt]
 
 
+@pytest.mark.late(1)
 def test_real_tgexc_blocks_long_move(cuda_ok):
     """n = 400, the last block to the top and back: LAPACK's IFST / ILST / INFO, its arrays
     up to column signs, and Q A Z^T, Q B Z^T unchanged."""
@@ -201,6 +203,7 @@ def test_real_tgexc_blocks_long_move(cuda_ok):
 
 
 @pytest.mark.parametrize("move", [(4, 2), (2, 5), (5, 1), (6, 1), (1, 6)], ids=lambda m: f"{m[0]}to{m[1]}")
+@pytest.mark.late(1)
 def test_real_tgexc_blocks_rejections(cuda_ok, move):
     """Two identical 2x2 blocks: their swap is rejected (INFO = 1, the pencil as LAPACK
     leaves it, ILST where the block stopped, IFST moved to its block's first row)."""
@@ -213,6 +216,7 @@ def test_real_tgexc_blocks_rejections(cuda_ok, move):
         assert _rel(M, R) < 1e-12
 
 
+@pytest.mark.late(1)
 def test_real_tgexc_blocks_splitting(cuda_ok):
     """Near-double 2x2 blocks that LAPACK's walk splits: INFO and ILST as LAPACK, the pencil
     kept, the two eigenvalues at rows ILST, ILST + 1 (to 1e-6)."""
@@ -237,6 +241,7 @@ def test_real_tgexc_blocks_splitting(cuda_ok):
     assert done >= 4
 
 
+@pytest.mark.late(1)
 def test_real_tgexc_blocks_device_form(cuda_ok):
     """xtgevc3_dtgexc_dev on column-major CUDA tensors: the host form's arrays and IFST /
     ILST bit for bit; without Q and Z the same A and B."""
