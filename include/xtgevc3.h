@@ -327,6 +327,88 @@ int xtgevc3_dgges_dev(void *stream, char jobvsl, char jobvsr, int n, double *A, 
 int xtgevc3_sgges_dev(void *stream, char jobvsl, char jobvsr, int n, float *A, int lda, float *B, int ldb,
                       float *alphar, float *alphai, float *beta, float *VSL, int ldvsl, float *VSR, int ldvsr, int *info);
 
+/* xGGES with ordering: LAPACK Z/C/D/SGGES's SORT, SELCTG and SDIM in its own positions
+ * (replacing the LAPACK call `zgges_(jobvsl, jobvsr, sort, selctg, &n, A, &lda, B, &ldb, &sdim,
+ * alpha, beta, VSL, &ldvsl, VSR, &ldvsr, work, &lwork, rwork, bwork, &info)` and its d/s/c
+ * siblings; no workspace arguments).  SORT = 'N': as the calls above, SDIM = 0.  SORT = 'S':
+ * after the QZ step SELCTG is called on the host for every eigenvalue (real: SELCTG(alphar(j),
+ * alphai(j), beta(j)); complex: SELCTG(alpha(j), beta(j)), each a (re, im) pair; nonzero =
+ * selected, a real complex pair counting as selected when either of its values is), the
+ * pencil is reordered on the device so that the selected eigenvalues lead (xTGSEN with
+ * IJOB = 0: the xTGEXC walks of the reordering entry points below, then the eigenvalues
+ * recomputed from the reordered pencil, xLAG2 for real 2x2 blocks, and the rows normalised
+ * as xTGSEN does), VSL / VSR updated, and SDIM = the number of selected eigenvalues after the
+ * reordering (a pair counts 2).  INFO = n + 3 when a swap was rejected (the pencil partly
+ * reordered), n + 2 when an eigenvalue selected after the reordering follows one that is not
+ * (rounding changed a selection), both as LAPACK's xGGES; SELCTG null with SORT = 'S': INFO =
+ * -4; SORT neither 'N' nor 'S': -3.  The device forms call SELCTG on the host too (reading the
+ * 2-3 n eigenvalue numbers back), so SELCTG is a host function in every form.               */
+typedef int (*xtgevc3_dselect3)(const double *alphar, const double *alphai, const double *beta);
+typedef int (*xtgevc3_sselect3)(const float *alphar, const float *alphai, const float *beta);
+typedef int (*xtgevc3_zselect2)(const double *alpha, const double *beta);
+typedef int (*xtgevc3_cselect2)(const float *alpha, const float *beta);
+void xtgevc3_zgges_sort(char jobvsl, char jobvsr, char sort, xtgevc3_zselect2 selctg, int n, double *A, int lda,
+                        double *B, int ldb, int *sdim, double *alpha, double *beta, double *VSL, int ldvsl, double *VSR,
+                        int ldvsr, int *info);
+void xtgevc3_cgges_sort(char jobvsl, char jobvsr, char sort, xtgevc3_cselect2 selctg, int n, float *A, int lda,
+                        float *B, int ldb, int *sdim, float *alpha, float *beta, float *VSL, int ldvsl, float *VSR,
+                        int ldvsr, int *info);
+int xtgevc3_zgges_sort_dev(void *stream, char jobvsl, char jobvsr, char sort, xtgevc3_zselect2 selctg, int n, double *A,
+                           int lda, double *B, int ldb, int *sdim, double *alpha, double *beta, double *VSL, int ldvsl,
+                           double *VSR, int ldvsr, int *info);
+int xtgevc3_cgges_sort_dev(void *stream, char jobvsl, char jobvsr, char sort, xtgevc3_cselect2 selctg, int n, float *A,
+                           int lda, float *B, int ldb, int *sdim, float *alpha, float *beta, float *VSL, int ldvsl,
+                           float *VSR, int ldvsr, int *info);
+void xtgevc3_dgges_sort(char jobvsl, char jobvsr, char sort, xtgevc3_dselect3 selctg, int n, double *A, int lda,
+                        double *B, int ldb, int *sdim, double *alphar, double *alphai, double *beta, double *VSL,
+                        int ldvsl, double *VSR, int ldvsr, int *info);
+void xtgevc3_sgges_sort(char jobvsl, char jobvsr, char sort, xtgevc3_sselect3 selctg, int n, float *A, int lda,
+                        float *B, int ldb, int *sdim, float *alphar, float *alphai, float *beta, float *VSL, int ldvsl,
+                        float *VSR, int ldvsr, int *info);
+int xtgevc3_dgges_sort_dev(void *stream, char jobvsl, char jobvsr, char sort, xtgevc3_dselect3 selctg, int n,
+                           double *A, int lda, double *B, int ldb, int *sdim, double *alphar, double *alphai,
+                           double *beta, double *VSL, int ldvsl, double *VSR, int ldvsr, int *info);
+int xtgevc3_sgges_sort_dev(void *stream, char jobvsl, char jobvsr, char sort, xtgevc3_sselect3 selctg, int n, float *A,
+                           int lda, float *B, int ldb, int *sdim, float *alphar, float *alphai, float *beta, float *VSL,
+                           int ldvsl, float *VSR, int ldvsr, int *info);
+
+/* LAPACK D/S/Z/CTGSEN with IJOB = 0: the eigenvalues that SELECT flags move to the leading
+ * rows of the generalized Schur pencil (A, B) by the swaps of xTGEXC, Q and Z updated when
+ * WANTQ / WANTZ (replacing `dtgsen_(&ijob, &wantq, &wantz, select, &n, A, &lda, B, &ldb,
+ * alphar, alphai, beta, Q, &ldq, Z, &ldz, &m, &pl, &pr, dif, work, &lwork, iwork, &liwork,
+ * &info)` for IJOB = 0; PL, PR, DIF and the workspaces have no counterpart).  The eigenvalues
+ * of the reordered pencil as xTGSEN returns them (real: xLAG2 on each 2x2 block, 1x1 blocks
+ * with B(k, k) made non-negative by negating row k of A and B and column k of Q; complex: when
+ * 0 < M < n and every swap was done, each row scaled so that B(k, k) is real and
+ * non-negative, Q's columns with it; otherwise the input diagonals).  M = the dimension of the
+ * selected subspace (a real 2x2 block counts 2 when either of its rows is selected).  INFO:
+ * -1 when IJOB is not 0 (the estimates of IJOB 1-5 are not built), -5 N, -7 LDA, -9 LDB, -14 /
+ * -13 LDQ, -16 / -15 LDZ (real / complex); 1 when a swap was rejected (the pencil partly
+ * reordered; real pencils still get the recomputed eigenvalues); n + 1 (not a LAPACK value)
+ * when a CUDA call failed in the host-pointer form.  SELECT is a host array in both forms; the
+ * device form's other arrays are device pointers (returns 0, or 1 when a CUDA call failed).  */
+void xtgevc3_dtgsen(int ijob, int wantq, int wantz, const int *select, int n, double *A, int lda, double *B, int ldb,
+                    double *alphar, double *alphai, double *beta, double *Q, int ldq, double *Z, int ldz, int *m,
+                    int *info);
+void xtgevc3_stgsen(int ijob, int wantq, int wantz, const int *select, int n, float *A, int lda, float *B, int ldb,
+                    float *alphar, float *alphai, float *beta, float *Q, int ldq, float *Z, int ldz, int *m, int *info);
+void xtgevc3_ztgsen(int ijob, int wantq, int wantz, const int *select, int n, double *A, int lda, double *B, int ldb,
+                    double *alpha, double *beta, double *Q, int ldq, double *Z, int ldz, int *m, int *info);
+void xtgevc3_ctgsen(int ijob, int wantq, int wantz, const int *select, int n, float *A, int lda, float *B, int ldb,
+                    float *alpha, float *beta, float *Q, int ldq, float *Z, int ldz, int *m, int *info);
+int xtgevc3_dtgsen_dev(void *stream, int ijob, int wantq, int wantz, const int *select, int n, double *A, int lda,
+                       double *B, int ldb, double *alphar, double *alphai, double *beta, double *Q, int ldq, double *Z,
+                       int ldz, int *m, int *info);
+int xtgevc3_stgsen_dev(void *stream, int ijob, int wantq, int wantz, const int *select, int n, float *A, int lda,
+                       float *B, int ldb, float *alphar, float *alphai, float *beta, float *Q, int ldq, float *Z,
+                       int ldz, int *m, int *info);
+int xtgevc3_ztgsen_dev(void *stream, int ijob, int wantq, int wantz, const int *select, int n, double *A, int lda,
+                       double *B, int ldb, double *alpha, double *beta, double *Q, int ldq, double *Z, int ldz, int *m,
+                       int *info);
+int xtgevc3_ctgsen_dev(void *stream, int ijob, int wantq, int wantz, const int *select, int n, float *A, int lda,
+                       float *B, int ldb, float *alpha, float *beta, float *Q, int ldq, float *Z, int ldz, int *m,
+                       int *info);
+
 /* ---- allocation-free device entry point (no counterpart in the upstream library) -----
  * Same computation and arguments as xtgevc3_dtgevc3_dev (without flags), for callers that
  * cannot allocate device memory at this point: e.g. a framework that has reserved the

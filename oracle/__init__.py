@@ -11,7 +11,8 @@ Contents
                      ``make -C oracle ref`` where the upstream tree is present);
   * LAPACK from SciPy's bundled OpenBLAS (Fortran interface where SciPy's wrapper drops an
     output) as the oracle of the LAPACK-compatible entry points: xTGEVC, xTREVC3, xTGSNA
-    (JOB 'E', 'V', 'B'), xTGEXC and the single swap xTGEX2;
+    (JOB 'E', 'V', 'B'), xTGEXC and the single swap xTGEX2, xTGSEN (IJOB = 0) and xGGES
+    with ordering;
   * residual checks and the comparison normalisation (the seeded pencil generators live
     in ``xtgevc3_b200.pencils`` and are re-exported here for the tests).
 """
@@ -332,6 +333,36 @@ def lapack_tgex2_real(A, B, Q, Z, j1, n1, n2):
     f(iv(int(wq)), iv(int(wz)), iv(n), _ptr(A), iv(ld), _ptr(B), iv(ld), _ptr(Q), iv(ld), _ptr(Z), iv(ld),
       iv(j1), iv(n1), iv(n2), _ptr(work), iv(lwork), ct.byref(info))
     return A, B, (Q if wq else None), (Z if wz else None), info.value
+
+
+def lapack_tgsen0(select, A, B, Q, Z):
+    """LAPACK x TGSEN with IJOB = 0 (SciPy's wrapper of D/S/Z/CTGSEN): the eigenvalues that
+    select flags move to the leading rows of the generalized Schur pencil (A, B), Q and Z
+    updated.  Returns (A, B, eigenvalue arrays..., Q, Z, m, info): real (alphar, alphai, beta),
+    complex (alpha, beta)."""
+    import scipy.linalg.lapack as la
+    pfx = {np.float64: "d", np.float32: "s", np.complex128: "z", np.complex64: "c"}[A.dtype.type]
+    sel = np.asarray(select, dtype=np.int32)
+    r = getattr(la, f"{pfx}tgsen")(sel, A, B, Q, Z, ijob=0)
+    if pfx in "ds":
+        a, b, ar, ai, be, q, z, m, _, _, _, info = r
+        return a, b, ar, ai, be, q, z, int(m), int(info)
+    a, b, al, be, q, z, m, _, _, _, info = r
+    return a, b, al, be, q, z, int(m), int(info)
+
+
+def lapack_gges_sort(A, B, sort):
+    """LAPACK xGGES with SORT = 'S' (SciPy's wrapper), sort a predicate as SELCTG (real:
+    sort(alphar, alphai, beta), complex: sort(alpha, beta)).  Returns (S, T, sdim, eigenvalue
+    arrays..., VSL, VSR, info)."""
+    import scipy.linalg.lapack as la
+    pfx = {np.float64: "d", np.float32: "s", np.complex128: "z", np.complex64: "c"}[A.dtype.type]
+    f = getattr(la, f"{pfx}gges")
+    if pfx in "ds":  # f2py passes as many values as the callback names
+        r = f(lambda ar, ai, b: int(bool(sort(ar, ai, b))), A, B, sort_t=1)
+    else:
+        r = f(lambda a, b: int(bool(sort(a, b))), A, B, sort_t=1)
+    return tuple(x for i, x in enumerate(r) if i != len(r) - 2)  # work dropped
 
 
 def complex_schur_pencil(n, seed, dtype=np.complex128):

@@ -1,5 +1,6 @@
 // The QZ kernels' bodies (xtgevc3_b200/csrc/qz_cplx.cuh: rb::zgges_cta, qz_real.cuh:
-// rb::dgges_cta) compiled for the CPU (test harness, not a product path): on one thread, and
+// rb::dgges_cta) and the reordering kernels' bodies (tgsen.cuh: rb::tgsen_real_cta,
+// rb::tgsen_cplx_cta, with xGGES's SDIM check) compiled for the CPU (test harness, not a product path): on one thread, and
 // on host threads with a std::barrier for the CTA barrier, so that the generalized Schur
 // forms they compute can be checked without a GPU.  Built by tests/test_qz_host.py with g++ into tests/_build.
 #include <barrier>
@@ -7,6 +8,7 @@
 #include <vector>
 
 #include "../xtgevc3_b200/csrc/qz_real.cuh"
+#include "../xtgevc3_b200/csrc/tgsen.cuh"
 
 using namespace xtg::rb;
 
@@ -64,9 +66,95 @@ int run_real(int nth, int wantq, int wantz, int n, R *A, R *B, R *Q, R *Z, R *ar
     return info;
 }
 
+template <class R>
+int run_tgsen_real(int nth, int wantq, int wantz, int n, R *A, R *B, R *Q, R *Z, const int *sel, R *ar, R *ai, R *be)
+{
+    Pencil<R> p{n, wantq, wantz, A, B, wantq ? Q : A, wantz ? Z : A, n, n, n, n};
+    WalkShared<R> sh{};
+    int info = 0;
+    std::barrier<> bar(nth);
+    std::vector<std::thread> th;
+    for (int t = 0; t < nth; t++)
+        th.emplace_back([&, t] {
+            const int i = tgsen_real_cta(CtaHost{t, nth, &bar}, sh, p, sel, ar, ai, be);
+            if (t == 0) info = i;
+        });
+    for (auto &x : th) x.join();
+    return info;
+}
+
+template <class R>
+int run_tgsen_cplx(int nth, int wantq, int wantz, int n, R *A, R *B, R *Q, R *Z, const int *sel, R *al, R *be)
+{
+    using C = zc<R>;
+    C *a = reinterpret_cast<C *>(A), *b = reinterpret_cast<C *>(B);
+    ZPencil<R> p{n, wantq, wantz, a, b, wantq ? reinterpret_cast<C *>(Q) : a, wantz ? reinterpret_cast<C *>(Z) : a,
+                 n, n, n, n};
+    ZSortShared<R> sh{};
+    int info = 0;
+    std::barrier<> bar(nth);
+    std::vector<std::thread> th;
+    for (int t = 0; t < nth; t++)
+        th.emplace_back([&, t] {
+            const int i = tgsen_cplx_cta(CtaHost{t, nth, &bar}, sh, p, sel, reinterpret_cast<C *>(al),
+                                         reinterpret_cast<C *>(be));
+            if (t == 0) info = i;
+        });
+    for (auto &x : th) x.join();
+    return info;
+}
+
+// SELCTG from flags: the test passes the selection that LAPACK's SELCTG made, one flag per
+// eigenvalue in order, and the check reads them back in the same order
+struct FlagSel {
+    const int *flags;
+    mutable int i = 0;
+    template <class T>
+    int operator()(const T *, const T *, const T *) const { return flags[i++]; }
+    template <class T>
+    int operator()(const T *, const T *) const { return flags[i++]; }
+};
+
 }  // namespace
 
 extern "C" {
+
+// xTGSEN (IJOB = 0) bodies: n x n, leading dimension n; returns INFO
+int host_dtgsen0(int nth, int wantq, int wantz, int n, double *A, double *B, double *Q, double *Z, const int *sel,
+                 double *ar, double *ai, double *be)
+{
+    return run_tgsen_real(nth, wantq, wantz, n, A, B, Q, Z, sel, ar, ai, be);
+}
+
+int host_stgsen0(int nth, int wantq, int wantz, int n, float *A, float *B, float *Q, float *Z, const int *sel,
+                 float *ar, float *ai, float *be)
+{
+    return run_tgsen_real(nth, wantq, wantz, n, A, B, Q, Z, sel, ar, ai, be);
+}
+
+int host_ztgsen0(int nth, int wantq, int wantz, int n, double *A, double *B, double *Q, double *Z, const int *sel,
+                 double *al, double *be)
+{
+    return run_tgsen_cplx(nth, wantq, wantz, n, A, B, Q, Z, sel, al, be);
+}
+
+int host_ctgsen0(int nth, int wantq, int wantz, int n, float *A, float *B, float *Q, float *Z, const int *sel,
+                 float *al, float *be)
+{
+    return run_tgsen_cplx(nth, wantq, wantz, n, A, B, Q, Z, sel, al, be);
+}
+
+// xGGES's check: SELCTG's answers as flags in order; returns SDIM, *info as the check leaves it
+int host_dgges_sdim(int n, const int *flags, const double *ar, const double *ai, const double *be, int *info)
+{
+    return gges_sdim_real(n, FlagSel{flags}, ar, ai, be, info);
+}
+
+int host_zgges_sdim(int n, const int *flags, const double *al, const double *be, int *info)
+{
+    return gges_sdim_cplx(n, FlagSel{flags}, reinterpret_cast<const zc<double> *>(al),
+                          reinterpret_cast<const zc<double> *>(be), info);
+}
 
 // real: n x n, leading dimension n; alphar, alphai, beta n each; returns INFO
 int host_dgges(int nth, int wantq, int wantz, int n, double *A, double *B, double *Q, double *Z, double *ar, double *ai,

@@ -70,6 +70,13 @@ _lib = None
 _P = ct.c_void_p
 _I = ct.c_int
 _C = ct.c_char
+# SELCTG of xGGES (include/xtgevc3.h: xtgevc3_dselect3 ... xtgevc3_cselect2)
+_SELECT = {
+    "d": ct.CFUNCTYPE(ct.c_int, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)),
+    "s": ct.CFUNCTYPE(ct.c_int, ct.POINTER(ct.c_float), ct.POINTER(ct.c_float), ct.POINTER(ct.c_float)),
+    "z": ct.CFUNCTYPE(ct.c_int, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)),
+    "c": ct.CFUNCTYPE(ct.c_int, ct.POINTER(ct.c_float), ct.POINTER(ct.c_float)),
+}
 _U = ct.c_uint
 
 
@@ -123,6 +130,23 @@ def lib():
             f.restype = None
             f = getattr(L, f"xtgevc3_{p}gges_dev")
             f.argtypes = [_P, _C, _C, _I, _P, _I, _P, _I, _P, _P, _P, _P, _I, _P, _I, _P]
+            f.restype = _I
+        for p in "zcds":  # xGGES with ordering: SORT, SELCTG, SDIM in LAPACK's positions
+            sel = _SELECT[p]
+            nv = 2 if p in "zc" else 3
+            f = getattr(L, f"xtgevc3_{p}gges_sort")
+            f.argtypes = [_C, _C, _C, sel, _I, _P, _I, _P, _I, _P] + [_P] * nv + [_P, _I, _P, _I, _P]
+            f.restype = None
+            f = getattr(L, f"xtgevc3_{p}gges_sort_dev")
+            f.argtypes = [_P, _C, _C, _C, sel, _I, _P, _I, _P, _I, _P] + [_P] * nv + [_P, _I, _P, _I, _P]
+            f.restype = _I
+        for p in "dszc":  # xTGSEN with IJOB = 0
+            nv = 2 if p in "zc" else 3
+            f = getattr(L, f"xtgevc3_{p}tgsen")
+            f.argtypes = [_I, _I, _I, _P, _I, _P, _I, _P, _I] + [_P] * nv + [_P, _I, _P, _I, _P, _P]
+            f.restype = None
+            f = getattr(L, f"xtgevc3_{p}tgsen_dev")
+            f.argtypes = [_P, _I, _I, _I, _P, _I, _P, _I, _P, _I] + [_P] * nv + [_P, _I, _P, _I, _P, _P]
             f.restype = _I
         for p in "dszc":  # xTGSNA DIF on the device
             f = getattr(L, f"xtgevc3_{p}tgsna_dif_dev")
@@ -445,11 +469,24 @@ def tgsna_dif_dev(A, B, howmny="A", select=None, stream=None):
     return dif[:m.value], m.value, info.value
 
 
-def gges(A, B, jobvsl="V", jobvsr="V"):
-    """Host-array form of z/c/d/sgges without ordering: the generalized Schur form of the pencil
-    (A, B), A = VSL S VSR^H, B = VSL T VSR^H.  Complex: returns (S, T, alpha, beta, VSL, VSR,
-    info); real: (S, T, alphar, alphai, beta, VSL, VSR, info).  New arrays; VSL / VSR None for
-    'N'."""
+def _selctg(pfx, sort):
+    """The C SELCTG for a Python predicate: real sort(alphar, alphai, beta), complex
+    sort(alpha, beta) (Python floats / complex numbers) -> truth value; a NULL pointer for None."""
+    typ = _SELECT[pfx]
+    if sort is None:
+        return typ()
+    if pfx in "zc":
+        return typ(lambda a, b: 1 if sort(complex(a[0], a[1]), complex(b[0], b[1])) else 0)
+    return typ(lambda ar, ai, b: 1 if sort(ar[0], ai[0], b[0]) else 0)
+
+
+def gges(A, B, jobvsl="V", jobvsr="V", sort=None):
+    """Host-array form of z/c/d/sgges: the generalized Schur form of the pencil (A, B),
+    A = VSL S VSR^H, B = VSL T VSR^H.  Complex: returns (S, T, alpha, beta, VSL, VSR, info);
+    real: (S, T, alphar, alphai, beta, VSL, VSR, info).  New arrays; VSL / VSR None for 'N'.
+    With sort (a predicate: real sort(alphar, alphai, beta), complex sort(alpha, beta)) the
+    eigenvalues it selects lead (xGGES with SORT = 'S', xtgevc3_*gges_sort) and SDIM comes
+    before info: (..., VSL, VSR, sdim, info)."""
     L = lib()
     dt = A.dtype.type
     pfx = {np.complex128: "z", np.complex64: "c", np.float64: "d", np.float32: "s"}[dt]
@@ -463,17 +500,25 @@ def gges(A, B, jobvsl="V", jobvsr="V"):
         eig = [np.zeros(max(n, 1), dtype=dt) for _ in range(2)]
     else:
         eig = [np.zeros(max(n, 1), dtype=dt) for _ in range(3)]
-    getattr(L, f"xtgevc3_{pfx}gges")(jobvsl.encode(), jobvsr.encode(), n, _ptr(S), ld, _ptr(T), ld,
-                                     *[_ptr(e) for e in eig], _ptr(VL), ld, _ptr(VR), ld, ct.byref(info))
-    if info.value > n:
+    if sort is None:
+        getattr(L, f"xtgevc3_{pfx}gges")(jobvsl.encode(), jobvsr.encode(), n, _ptr(S), ld, _ptr(T), ld,
+                                         *[_ptr(e) for e in eig], _ptr(VL), ld, _ptr(VR), ld, ct.byref(info))
+    else:
+        sdim, sel = ct.c_int(-1), _selctg(pfx, sort)
+        getattr(L, f"xtgevc3_{pfx}gges_sort")(jobvsl.encode(), jobvsr.encode(), b"S", sel, n, _ptr(S), ld, _ptr(T), ld,
+                                              ct.byref(sdim), *[_ptr(e) for e in eig], _ptr(VL), ld, _ptr(VR), ld,
+                                              ct.byref(info))
+    if info.value == n + 1:  # a CUDA call failed (n + 2, n + 3: xGGES's ordering results)
         raise RuntimeError(f"xtgevc3_{pfx}gges failed: {last_error()}")
-    return (S, T, *[e[:n] for e in eig], VL, VR, info.value)
+    out = (S, T, *[e[:n] for e in eig], VL, VR)
+    return (*out, info.value) if sort is None else (*out, sdim.value, info.value)
 
 
-def gges_dev(A, B, VSL=None, VSR=None, stream=None):
+def gges_dev(A, B, VSL=None, VSR=None, stream=None, sort=None):
     """Device form of z/c/d/sgges on column-major CUDA tensors: A, B become S, T in place, VSL /
     VSR (when given) the orthogonal / unitary factors.  Returns (alpha, beta, info) (complex)
-    or (alphar, alphai, beta, info) (real), the eigenvalue arrays CUDA tensors."""
+    or (alphar, alphai, beta, info) (real), the eigenvalue arrays CUDA tensors.  With sort (as
+    for gges; called on the host) the selected eigenvalues lead and SDIM comes before info."""
     import torch
     L = lib()
     pfx = {torch.complex128: "z", torch.complex64: "c", torch.float64: "d", torch.float32: "s"}[A.dtype]
@@ -488,12 +533,67 @@ def gges_dev(A, B, VSL=None, VSR=None, stream=None):
     def ptr(t):
         return ct.c_void_p(t.data_ptr()) if t is not None else None
 
-    rc = getattr(L, f"xtgevc3_{pfx}gges_dev")(st, b"V" if VSL is not None else b"N", b"V" if VSR is not None else b"N",
-                                             n, ptr(A), ld(A), ptr(B), ld(B), *[ptr(e) for e in eig], ptr(VSL),
-                                             ld(VSL), ptr(VSR), ld(VSR), ct.byref(info))
+    jl, jr = b"V" if VSL is not None else b"N", b"V" if VSR is not None else b"N"
+    if sort is None:
+        rc = getattr(L, f"xtgevc3_{pfx}gges_dev")(st, jl, jr, n, ptr(A), ld(A), ptr(B), ld(B), *[ptr(e) for e in eig],
+                                                 ptr(VSL), ld(VSL), ptr(VSR), ld(VSR), ct.byref(info))
+    else:
+        sdim, sel = ct.c_int(-1), _selctg(pfx, sort)
+        rc = getattr(L, f"xtgevc3_{pfx}gges_sort_dev")(st, jl, jr, b"S", sel, n, ptr(A), ld(A), ptr(B), ld(B),
+                                                      ct.byref(sdim), *[ptr(e) for e in eig], ptr(VSL), ld(VSL),
+                                                      ptr(VSR), ld(VSR), ct.byref(info))
     if rc:
         raise RuntimeError(f"xtgevc3_{pfx}gges_dev failed: {last_error()}")
-    return (*[e[:n] for e in eig], info.value)
+    out = [e[:n] for e in eig]
+    return (*out, info.value) if sort is None else (*out, sdim.value, info.value)
+
+
+def tgsen(select, A, B, Q=None, Z=None):
+    """Host-array form of d/s/z/ctgsen with IJOB = 0: the eigenvalues flagged in select move to
+    the leading rows (Q, Z None: not updated).  Returns (A, B, eigenvalue arrays..., Q, Z, m,
+    info) as new arrays, the eigenvalue arrays (alphar, alphai, beta) or (alpha, beta)."""
+    L = lib()
+    dt = A.dtype.type
+    pfx = {np.complex128: "z", np.complex64: "c", np.float64: "d", np.float32: "s"}[dt]
+    n = A.shape[0]
+    a, b = np.array(A, order="F", dtype=dt), np.array(B, order="F", dtype=dt)
+    q = np.array(Q, order="F", dtype=dt) if Q is not None else None
+    z = np.array(Z, order="F", dtype=dt) if Z is not None else None
+    sel = np.ascontiguousarray(select, dtype=np.int32)
+    ev = [np.zeros(max(n, 1), dtype=dt) for _ in range(2 if pfx in "zc" else 3)]
+    m, info = ct.c_int(0), ct.c_int(0)
+    ld = max(n, 1)
+    getattr(L, f"xtgevc3_{pfx}tgsen")(0, int(q is not None), int(z is not None), _ptr(sel), n, _ptr(a), ld, _ptr(b), ld,
+                                      *[_ptr(e) for e in ev], _ptr(q), ld, _ptr(z), ld, ct.byref(m), ct.byref(info))
+    if info.value == n + 1 and n > 0:
+        raise RuntimeError(f"xtgevc3_{pfx}tgsen failed: {last_error()}")
+    return (a, b, *[e[:n] for e in ev], q, z, m.value, info.value)
+
+
+def tgsen_dev(select, A, B, Q=None, Z=None, stream=None):
+    """Device form of d/s/z/ctgsen with IJOB = 0 on column-major CUDA tensors (in place; select
+    a host array).  Returns (eigenvalue tensors..., m, info)."""
+    import torch
+    L = lib()
+    pfx = {torch.complex128: "z", torch.complex64: "c", torch.float64: "d", torch.float32: "s"}[A.dtype]
+    n = A.shape[0]
+    st = ct.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+    sel = np.ascontiguousarray(select, dtype=np.int32)
+    ev = [torch.zeros(max(n, 1), dtype=A.dtype, device=A.device) for _ in range(2 if pfx in "zc" else 3)]
+    m, info = ct.c_int(0), ct.c_int(0)
+
+    def ld(t):
+        return max(t.stride(1), 1) if t is not None else 1
+
+    def ptr(t):
+        return ct.c_void_p(t.data_ptr()) if t is not None else None
+
+    rc = getattr(L, f"xtgevc3_{pfx}tgsen_dev")(st, 0, int(Q is not None), int(Z is not None), _ptr(sel), n, ptr(A),
+                                              ld(A), ptr(B), ld(B), *[ptr(e) for e in ev], ptr(Q), ld(Q), ptr(Z),
+                                              ld(Z), ct.byref(m), ct.byref(info))
+    if rc:
+        raise RuntimeError(f"xtgevc3_{pfx}tgsen_dev failed: {last_error()}")
+    return (*[e[:n] for e in ev], m.value, info.value)
 
 
 def tgexc(A, B, Q=None, Z=None, ifst=1, ilst=1, with_ifst=False):

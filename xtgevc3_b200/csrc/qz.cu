@@ -1,17 +1,23 @@
-// The generalized Schur form of a pencil on the GPU (LAPACK Z/C/D/SGGES without ordering):
-// rb::zgges_cta (qz_cplx.cuh) or rb::dgges_cta (qz_real.cuh) on one CTA; complex alpha =
-// diag(S), beta = diag(T), real alphar / alphai / beta as DHGEQZ returns them.
-// The three stages are chains of dependent plane rotations, so one CTA runs them (each
+// The generalized Schur form of a pencil on the GPU (LAPACK Z/C/D/SGGES): rb::zgges_cta
+// (qz_cplx.cuh) or rb::dgges_cta (qz_real.cuh) on one CTA; complex alpha = diag(S), beta =
+// diag(T), real alphar / alphai / beta as DHGEQZ returns them.  With SORT = 'S' the
+// eigenvalues that SELCTG selects then move to the leading rows: SELCTG runs on the host over
+// the QZ eigenvalues (2-3 n numbers read back), the reordering kernel (rb::tgsen_real_cta /
+// rb::tgsen_cplx_cta of tgsen.cuh, xTGSEN with IJOB = 0) runs on one CTA, and xGGES's own
+// check of the reordered eigenvalues (SDIM, INFO = n + 2 / n + 3) runs on the host.
+// The stages are chains of dependent plane rotations or swaps, so one CTA runs them (each
 // rotation's O(n) rows or columns spread over its threads); the result stays on the device
 // for the eigenvector solve that follows (xtgevc3_ztgevc3_dev).
 #include "../../include/xtgevc3.h"
 #include "common.cuh"
 #include "engine.cuh"
 #include "qz_real.cuh"
+#include "tgsen.cuh"
 
 #include <algorithm>
 #include <cctype>
 #include <string>
+#include <vector>
 
 namespace xtg {
 namespace {
@@ -37,14 +43,59 @@ __global__ void __launch_bounds__(kQzThreads, 1) dgges_kernel(rb::QzPencilR<R> p
     if (threadIdx.x == 0) *info = i;
 }
 
+// The reordering kernels: rb::tgsen_real_cta / rb::tgsen_cplx_cta on one CTA; info: 0, 1 (a
+// swap was rejected) or 3 (a walk reached its bound)
+// m (optional): DTGSEN's M of the input pencil, the selected eigenvalues counted with a
+// 2x2 block counting 2 when either of its rows is selected (thread 0 reads the subdiagonal
+// before its first barrier, so before any swap writes it)
+template <class R>
+__global__ void __launch_bounds__(kQzThreads, 1)
+    tgsen_real_kernel(rb::Pencil<R> p, const int *select, R *alphar, R *alphai, R *beta, int *info, int *m = nullptr)
+{
+    __shared__ rb::WalkShared<R> sh;
+    if (m && threadIdx.x == 0) {
+        int cnt = 0;
+        for (int k = 0; k < p.n; k++) {
+            if (k + 1 < p.n && p.A[(size_t)(k + 1) + (size_t)k * p.lda] != R(0)) {
+                cnt += (select[k] != 0 || select[k + 1] != 0) ? 2 : 0;
+                k++;
+            } else {
+                cnt += select[k] != 0 ? 1 : 0;
+            }
+        }
+        *m = cnt;
+    }
+    const int i = rb::tgsen_real_cta(rb::CtaDev{}, sh, p, select, alphar, alphai, beta);
+    if (threadIdx.x == 0) *info = i;
+}
+
+template <class R>
+__global__ void __launch_bounds__(kQzThreads, 1)
+    tgsen_cplx_kernel(rb::ZPencil<R> p, const int *select, rb::zc<R> *alpha, rb::zc<R> *beta, int *info)
+{
+    __shared__ rb::ZSortShared<R> sh;
+    const int i = rb::tgsen_cplx_cta(rb::CtaDev{}, sh, p, select, alpha, beta);
+    if (threadIdx.x == 0) *info = i;
+}
+
+// SELCTG of real and complex xGGES (nonzero: selected); complex values as (re, im) pairs
+template <class R>
+using SelReal = int (*)(const R *, const R *, const R *);
+template <class R>
+using SelCplx = int (*)(const R *, const R *);
+
 // LAPACK xGGES's argument checks, numbered by its argument list (JOBVSL, JOBVSR, SORT,
 // SELCTG, N, A, LDA, B, LDB, SDIM, ALPHA, BETA, VSL, LDVSL, VSR, LDVSR, ... complex; real
-// pencils have ALPHAR, ALPHAI in place of ALPHA, one argument more before VSL)
-int gges_check(char jobvsl, char jobvsr, int n, int lda, int ldb, int ldvsl, int ldvsr, bool real = false)
+// pencils have ALPHAR, ALPHAI in place of ALPHA, one argument more before VSL).  A null
+// SELCTG with SORT = 'S' is argument 4.
+int gges_check(char jobvsl, char jobvsr, char sort, bool have_sel, int n, int lda, int ldb, int ldvsl, int ldvsr,
+               bool real = false)
 {
     const bool wl = jobvsl == 'V', wr = jobvsr == 'V';
     if (!wl && jobvsl != 'N') return -1;
     if (!wr && jobvsr != 'N') return -2;
+    if (sort != 'N' && sort != 'S') return -3;
+    if (sort == 'S' && !have_sel) return -4;
     if (n < 0) return -5;
     if (lda < std::max(1, n)) return -7;
     if (ldb < std::max(1, n)) return -9;
@@ -53,20 +104,105 @@ int gges_check(char jobvsl, char jobvsr, int n, int lda, int ldb, int ldvsl, int
     return 0;
 }
 
-// Real pencils, device pointers (alphar, alphai, beta n each).  Returns 0, or 1 when a CUDA
-// call failed.
+// The selection flags to the device, the reordering kernel, the status back (stream st, then
+// synchronised): the common part of the real and complex ordering steps.
+template <class LAUNCH>
+cudaError_t run_tgsen(cudaStream_t st, const std::vector<int> &bw, int *status, LAUNCH launch)
+{
+    const int n = (int)bw.size();
+    int *d_sel = nullptr;  // n flags, then the status word
+    cudaError_t e = cudaMallocAsync(&d_sel, (n + 1) * sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(d_sel, bw.data(), n * sizeof(int), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        launch(d_sel, d_sel + n);
+        count_launches(1);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(status, d_sel + n, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFreeAsync(d_sel, st);
+    return e;
+}
+
+// xGGES's ordering step for real pencils (QZ done, INFO 0): SELCTG over the QZ eigenvalues,
+// DTGSEN (IJOB = 0) on the device, then DGGES's check of the new eigenvalues: SDIM counts the
+// selected ones (a pair counts 2 when either of its values, or the one before, is
+// selected), INFO = n + 3 when a swap was rejected, n + 2 when a selected eigenvalue follows
+// one that is not (rounding in the reordering changed a selection).
 template <class R>
-int gges_device_real(cudaStream_t st, char jobvsl, char jobvsr, int n, R *A, int lda, R *B, int ldb, R *alphar,
-                     R *alphai, R *beta, R *VSL, int ldvsl, R *VSR, int ldvsr, int *info)
+cudaError_t gges_sort_real(cudaStream_t st, SelReal<R> sel, const rb::Pencil<R> &p, R *alphar, R *alphai, R *beta,
+                           int *sdim, int *info)
+{
+    const int n = p.n;
+    std::vector<R> h(3 * (size_t)n);
+    R *dv[3] = {alphar, alphai, beta};
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < 3 && e == cudaSuccess; k++)
+        e = cudaMemcpyAsync(h.data() + (size_t)k * n, dv[k], n * sizeof(R), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+    std::vector<int> bw(n);
+    for (int i = 0; i < n; i++) bw[i] = sel(&h[i], &h[n + i], &h[2 * (size_t)n + i]) != 0 ? 1 : 0;
+    int status = 0;
+    e = run_tgsen(st, bw, &status, [&](int *d_sel, int *d_status) {
+        tgsen_real_kernel<R><<<1, kQzThreads, 0, st>>>(p, d_sel, alphar, alphai, beta, d_status);
+    });
+    for (int k = 0; k < 3 && e == cudaSuccess; k++)
+        e = cudaMemcpyAsync(h.data() + (size_t)k * n, dv[k], n * sizeof(R), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+    if (status != 0) *info = n + 3;
+    if (status == 3) set_last_error("xGGES: the reordering walk did not end within its swap bound");
+    *sdim = rb::gges_sdim_real(n, sel, h.data(), h.data() + n, h.data() + 2 * (size_t)n, info);
+    return cudaSuccess;
+}
+
+// The same for complex pencils: ZTGSEN (IJOB = 0) on the device, then ZGGES's check (SDIM
+// counts the selected eigenvalues, INFO = n + 3 / n + 2 as for real pencils).
+template <class R>
+cudaError_t gges_sort_cplx(cudaStream_t st, SelCplx<R> sel, const rb::ZPencil<R> &p, rb::zc<R> *alpha,
+                           rb::zc<R> *beta, int *sdim, int *info)
+{
+    using C = rb::zc<R>;
+    const int n = p.n;
+    std::vector<C> h(2 * (size_t)n);
+    cudaError_t e = cudaMemcpyAsync(h.data(), alpha, n * sizeof(C), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data() + n, beta, n * sizeof(C), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+    std::vector<int> bw(n);
+    for (int i = 0; i < n; i++) bw[i] = sel(&h[i].re, &h[n + i].re) != 0 ? 1 : 0;
+    int status = 0;
+    e = run_tgsen(st, bw, &status, [&](int *d_sel, int *d_status) {
+        tgsen_cplx_kernel<R><<<1, kQzThreads, 0, st>>>(p, d_sel, alpha, beta, d_status);
+    });
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), alpha, n * sizeof(C), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data() + n, beta, n * sizeof(C), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+    if (status != 0) *info = n + 3;
+    *sdim = rb::gges_sdim_cplx(n, sel, h.data(), h.data() + n, info);
+    return cudaSuccess;
+}
+
+// Real pencils, device pointers (alphar, alphai, beta n each).  Returns 0, or 1 when a CUDA
+// call failed.  sdim may be null when sort is 'N' (it is set to 0 otherwise).
+template <class R>
+int gges_device_real(cudaStream_t st, char jobvsl, char jobvsr, char sort, SelReal<R> sel, int n, R *A, int lda,
+                     R *B, int ldb, int *sdim, R *alphar, R *alphai, R *beta, R *VSL, int ldvsl, R *VSR, int ldvsr,
+                     int *info)
 {
     set_last_error("");
     jobvsl = (char)std::toupper((unsigned char)jobvsl);
     jobvsr = (char)std::toupper((unsigned char)jobvsr);
-    *info = gges_check(jobvsl, jobvsr, n, lda, ldb, ldvsl, ldvsr, true);
+    sort = (char)std::toupper((unsigned char)sort);
+    *info = gges_check(jobvsl, jobvsr, sort, sel != nullptr, n, lda, ldb, ldvsl, ldvsr, true);
     if (*info) {
         set_last_error("xGGES: argument " + std::to_string(-*info) + " has an illegal value");
         return 0;
     }
+    if (sdim) *sdim = 0;
     if (n == 0) return 0;
     const int wl = jobvsl == 'V', wr = jobvsr == 'V';
     int *d_info = nullptr, h_info = 0;
@@ -81,28 +217,36 @@ int gges_device_real(cudaStream_t st, char jobvsl, char jobvsr, int n, R *A, int
         if (e == cudaSuccess) e = cudaMemcpyAsync(&h_info, d_info, sizeof(int), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         cudaFreeAsync(d_info, st);
+        *info = h_info;
+        if (e == cudaSuccess && sort == 'S' && h_info == 0) {
+            const rb::Pencil<R> q{n, wl, wr, A, B, p.Q, p.Z, lda, ldb, p.ldq, p.ldz};
+            int sd = 0;
+            e = gges_sort_real<R>(st, sel, q, alphar, alphai, beta, &sd, info);
+            if (sdim) *sdim = sd;
+        }
     }
     if (e != cudaSuccess) {
         set_last_error(std::string("xGGES: ") + cudaGetErrorString(e));
         *info = n + 1;
         return 1;
     }
-    *info = h_info;
     return 0;
 }
 
 // Real pencils, host pointers
 template <class R>
-void gges_host_real(char jobvsl, char jobvsr, int n, R *A, int lda, R *B, int ldb, R *alphar, R *alphai, R *beta,
-                    R *VSL, int ldvsl, R *VSR, int ldvsr, int *info)
+void gges_host_real(char jobvsl, char jobvsr, char sort, SelReal<R> sel, int n, R *A, int lda, R *B, int ldb, int *sdim,
+                    R *alphar, R *alphai, R *beta, R *VSL, int ldvsl, R *VSR, int ldvsr, int *info)
 {
     set_last_error("");
     const char jl = (char)std::toupper((unsigned char)jobvsl), jr = (char)std::toupper((unsigned char)jobvsr);
-    *info = gges_check(jl, jr, n, lda, ldb, ldvsl, ldvsr, true);
+    const char so = (char)std::toupper((unsigned char)sort);
+    *info = gges_check(jl, jr, so, sel != nullptr, n, lda, ldb, ldvsl, ldvsr, true);
     if (*info) {
         set_last_error("xGGES: argument " + std::to_string(-*info) + " has an illegal value");
         return;
     }
+    if (sdim) *sdim = 0;
     if (n == 0) return;
     const bool wl = jl == 'V', wr = jr == 'V';
     cudaStream_t st = nullptr;
@@ -119,8 +263,8 @@ void gges_host_real(char jobvsl, char jobvsr, int n, R *A, int lda, R *B, int ld
     if (e == cudaSuccess)
         e = cudaMemcpy2DAsync(dB, n * sizeof(R), B, (size_t)ldb * sizeof(R), n * sizeof(R), n, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
-        const int rc = gges_device_real<R>(st, jl, jr, n, dA, n, dB, n, dv, dv + n, dv + 2 * n, dL, wl ? n : 1, dR,
-                                           wr ? n : 1, info);
+        const int rc = gges_device_real<R>(st, jl, jr, so, sel, n, dA, n, dB, n, sdim, dv, dv + n, dv + 2 * n, dL,
+                                           wl ? n : 1, dR, wr ? n : 1, info);
         if (rc == 0) {
             e = cudaMemcpy2DAsync(A, (size_t)lda * sizeof(R), dA, n * sizeof(R), n * sizeof(R), n, cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess)
@@ -153,19 +297,22 @@ void gges_host_real(char jobvsl, char jobvsr, int n, R *A, int lda, R *B, int ld
 }
 
 // Device pointers (alpha, beta interleaved complex, n each).  Returns 0, or 1 when a CUDA call
-// failed (message in last_error()).
+// failed (message in last_error()).  sdim may be null when sort is 'N'.
 template <class R>
-int gges_device(cudaStream_t st, char jobvsl, char jobvsr, int n, rb::zc<R> *A, int lda, rb::zc<R> *B, int ldb,
-                rb::zc<R> *alpha, rb::zc<R> *beta, rb::zc<R> *VSL, int ldvsl, rb::zc<R> *VSR, int ldvsr, int *info)
+int gges_device(cudaStream_t st, char jobvsl, char jobvsr, char sort, SelCplx<R> sel, int n, rb::zc<R> *A, int lda,
+                rb::zc<R> *B, int ldb, int *sdim, rb::zc<R> *alpha, rb::zc<R> *beta, rb::zc<R> *VSL, int ldvsl,
+                rb::zc<R> *VSR, int ldvsr, int *info)
 {
     set_last_error("");
     jobvsl = (char)std::toupper((unsigned char)jobvsl);
     jobvsr = (char)std::toupper((unsigned char)jobvsr);
-    *info = gges_check(jobvsl, jobvsr, n, lda, ldb, ldvsl, ldvsr);
+    sort = (char)std::toupper((unsigned char)sort);
+    *info = gges_check(jobvsl, jobvsr, sort, sel != nullptr, n, lda, ldb, ldvsl, ldvsr);
     if (*info) {
         set_last_error("xGGES: argument " + std::to_string(-*info) + " has an illegal value");
         return 0;
     }
+    if (sdim) *sdim = 0;
     if (n == 0) return 0;
     const int wl = jobvsl == 'V', wr = jobvsr == 'V';
     int *d_info = nullptr, h_info = 0;
@@ -179,29 +326,38 @@ int gges_device(cudaStream_t st, char jobvsl, char jobvsr, int n, rb::zc<R> *A, 
         if (e == cudaSuccess) e = cudaMemcpyAsync(&h_info, d_info, sizeof(int), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         cudaFreeAsync(d_info, st);
+        *info = h_info;
+        if (e == cudaSuccess && sort == 'S' && h_info == 0) {
+            const rb::ZPencil<R> q{n, wl, wr, A, B, p.Q, p.Z, lda, ldb, p.ldq, p.ldz};
+            int sd = 0;
+            e = gges_sort_cplx<R>(st, sel, q, alpha, beta, &sd, info);
+            if (sdim) *sdim = sd;
+        }
     }
     if (e != cudaSuccess) {
         set_last_error(std::string("xGGES: ") + cudaGetErrorString(e));
         *info = n + 1;
         return 1;
     }
-    *info = h_info;
     return 0;
 }
 
 // Host pointers: A, B (and VSL, VSR when wanted) go to the device and come back with alpha, beta.
 template <class R>
-void gges_host(char jobvsl, char jobvsr, int n, rb::zc<R> *A, int lda, rb::zc<R> *B, int ldb, rb::zc<R> *alpha,
-               rb::zc<R> *beta, rb::zc<R> *VSL, int ldvsl, rb::zc<R> *VSR, int ldvsr, int *info)
+void gges_host(char jobvsl, char jobvsr, char sort, SelCplx<R> sel, int n, rb::zc<R> *A, int lda, rb::zc<R> *B, int ldb,
+               int *sdim, rb::zc<R> *alpha, rb::zc<R> *beta, rb::zc<R> *VSL, int ldvsl, rb::zc<R> *VSR, int ldvsr,
+               int *info)
 {
     using C = rb::zc<R>;
     set_last_error("");
     const char jl = (char)std::toupper((unsigned char)jobvsl), jr = (char)std::toupper((unsigned char)jobvsr);
-    *info = gges_check(jl, jr, n, lda, ldb, ldvsl, ldvsr);
+    const char so = (char)std::toupper((unsigned char)sort);
+    *info = gges_check(jl, jr, so, sel != nullptr, n, lda, ldb, ldvsl, ldvsr);
     if (*info) {
         set_last_error("xGGES: argument " + std::to_string(-*info) + " has an illegal value");
         return;
     }
+    if (sdim) *sdim = 0;
     if (n == 0) return;
     const bool wl = jl == 'V', wr = jr == 'V';
     cudaStream_t st = nullptr;
@@ -219,7 +375,8 @@ void gges_host(char jobvsl, char jobvsr, int n, rb::zc<R> *A, int lda, rb::zc<R>
         e = cudaMemcpy2DAsync(dB, n * sizeof(C), B, (size_t)ldb * sizeof(C), n * sizeof(C), n, cudaMemcpyHostToDevice, st);
     int rc = 0;
     if (e == cudaSuccess) {
-        rc = gges_device<R>(st, jl, jr, n, dA, n, dB, n, dab, dab + n, dL, wl ? n : 1, dR, wr ? n : 1, info);
+        rc = gges_device<R>(st, jl, jr, so, sel, n, dA, n, dB, n, sdim, dab, dab + n, dL, wl ? n : 1, dR, wr ? n : 1,
+                            info);
         if (rc == 0) {
             e = cudaMemcpy2DAsync(A, (size_t)lda * sizeof(C), dA, n * sizeof(C), n * sizeof(C), n, cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess)
@@ -248,6 +405,134 @@ void gges_host(char jobvsl, char jobvsr, int n, rb::zc<R> *A, int lda, rb::zc<R>
     }
 }
 
+// LAPACK xTGSEN with IJOB = 0 (reordering only; the condition estimates of IJOB 1-5 are not
+// built and are refused with INFO = -1), device pointers, SELECT on the host.  INFO as LAPACK
+// numbers its arguments (-1 IJOB, -5 N, -7 LDA, -9 LDB, -14 / -13 LDQ, -16 / -15 LDZ for real /
+// complex pencils), 1 when a swap was rejected.  Returns 0, or 1 when a CUDA call failed.
+// xTGSEN's argument checks; sets last_error for a bad one
+int tgsen_check(int ijob, int wantq, int wantz, int n, int lda, int ldb, int ldq, int ldz, bool cplx)
+{
+    int info = 0;
+    if (ijob != 0) info = -1;
+    else if (n < 0) info = -5;
+    else if (lda < std::max(1, n)) info = -7;
+    else if (ldb < std::max(1, n)) info = -9;
+    else if (ldq < 1 || (wantq && ldq < n)) info = cplx ? -13 : -14;
+    else if (ldz < 1 || (wantz && ldz < n)) info = cplx ? -15 : -16;
+    if (info)
+        set_last_error(ijob != 0 ? "xTGSEN: only IJOB = 0 (reordering without condition estimates) is built"
+                                 : "xTGSEN: argument " + std::to_string(-info) + " has an illegal value");
+    return info;
+}
+
+template <class R, bool CPLX>
+int tgsen_device(cudaStream_t st, int ijob, int wantq, int wantz, const int *select, int n, R *A, int lda, R *B,
+                 int ldb, R *ev0, R *ev1, R *ev2, R *Q, int ldq, R *Z, int ldz, int *m, int *info)
+{
+    set_last_error("");
+    *info = tgsen_check(ijob, wantq, wantz, n, lda, ldb, ldq, ldz, CPLX);
+    if (*info) return 0;
+    if (m) *m = 0;
+    if (n == 0) return 0;
+    std::vector<int> bw(n);
+    for (int i = 0; i < n; i++) bw[i] = select[i] != 0 ? 1 : 0;
+    int *d = nullptr;  // n flags, the status, M
+    int h[2] = {0, 0};
+    cudaError_t e = cudaMallocAsync(&d, (n + 2) * sizeof(int), st);
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(d, bw.data(), n * sizeof(int), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) {
+            if constexpr (CPLX) {
+                using C = rb::zc<R>;
+                C *a = reinterpret_cast<C *>(A), *b = reinterpret_cast<C *>(B);
+                const rb::ZPencil<R> p{n, wantq, wantz, a, b, wantq ? reinterpret_cast<C *>(Q) : a,
+                                       wantz ? reinterpret_cast<C *>(Z) : a, lda, ldb, wantq ? ldq : lda,
+                                       wantz ? ldz : lda};
+                tgsen_cplx_kernel<R><<<1, kQzThreads, 0, st>>>(p, d, reinterpret_cast<C *>(ev0),
+                                                                reinterpret_cast<C *>(ev1), d + n);
+                for (int i = 0; i < n; i++) h[1] += bw[i];
+            } else {
+                const rb::Pencil<R> p{n, wantq, wantz, A, B, wantq ? Q : A, wantz ? Z : A, lda, ldb,
+                                      wantq ? ldq : lda, wantz ? ldz : lda};
+                tgsen_real_kernel<R><<<1, kQzThreads, 0, st>>>(p, d, ev0, ev1, ev2, d + n, d + n + 1);
+            }
+            count_launches(1);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h, d + n, (CPLX ? 1 : 2) * sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        cudaFreeAsync(d, st);
+    }
+    if (e != cudaSuccess) {
+        set_last_error(std::string("xTGSEN: ") + cudaGetErrorString(e));
+        return 1;
+    }
+    if (h[0] == 3) {
+        set_last_error("xTGSEN: the reordering walk did not end within its swap bound");
+        return 1;
+    }
+    *info = h[0];
+    if (m) *m = h[1];
+    return 0;
+}
+
+// Host pointers: A, B (and Q, Z when wanted) go to the device and come back with the
+// eigenvalues.  INFO = n + 1 (not a LAPACK value) when a CUDA call failed.
+template <class R, bool CPLX>
+void tgsen_host(int ijob, int wantq, int wantz, const int *select, int n, R *A, int lda, R *B, int ldb, R *ev0,
+                R *ev1, R *ev2, R *Q, int ldq, R *Z, int ldz, int *m, int *info)
+{
+    constexpr int w = CPLX ? 2 : 1;  // reals per element
+    const int nev = CPLX ? 2 : 3;
+    set_last_error("");
+    *info = tgsen_check(ijob, wantq, wantz, n, lda, ldb, ldq, ldz, CPLX);  // before any data moves
+    if (*info) return;
+    if (m) *m = 0;
+    if (n == 0) return;
+    cudaStream_t st = nullptr;
+    R *dA = nullptr, *dB = nullptr, *dQ = nullptr, *dZ = nullptr, *dv = nullptr;
+    const size_t row = (size_t)n * w * sizeof(R), mat = row * n;
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    for (R **q : {&dA, &dB})
+        if (e == cudaSuccess) e = cudaMallocAsync(q, mat, st);
+    if (wantq && e == cudaSuccess) e = cudaMallocAsync(&dQ, mat, st);
+    if (wantz && e == cudaSuccess) e = cudaMallocAsync(&dZ, mat, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&dv, nev * row, st);
+    struct M2 {
+        R *h, *d;
+        int ld;
+    } mats[4] = {{A, dA, lda}, {B, dB, ldb}, {Q, dQ, ldq}, {Z, dZ, ldz}};
+    for (const M2 &x : mats)
+        if (x.d && e == cudaSuccess)
+            e = cudaMemcpy2DAsync(x.d, row, x.h, (size_t)x.ld * w * sizeof(R), row, n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        const int rc = tgsen_device<R, CPLX>(st, 0, wantq, wantz, select, n, dA, n, dB, n, dv, dv + (size_t)n * w,
+                                             dv + 2 * (size_t)n * w, dQ ? dQ : dA, n, dZ ? dZ : dA, n, m, info);
+        if (rc == 0) {
+            for (const M2 &x : mats)
+                if (x.d && e == cudaSuccess)
+                    e = cudaMemcpy2DAsync(x.h, (size_t)x.ld * w * sizeof(R), x.d, row, row, n, cudaMemcpyDeviceToHost,
+                                          st);
+            R *outs[3] = {ev0, ev1, ev2};
+            for (int k = 0; k < nev && e == cudaSuccess; k++)
+                e = cudaMemcpyAsync(outs[k], dv + (size_t)k * n * w, row, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        } else {
+            e = cudaErrorUnknown;
+        }
+    }
+    for (R *q : {dA, dB, dQ, dZ, dv})
+        if (q) cudaFreeAsync(q, st);
+    if (st) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
+    if (e != cudaSuccess) {
+        if (e != cudaErrorUnknown) set_last_error(std::string("xTGSEN staging: ") + cudaGetErrorString(e));
+        *info = n + 1;
+    }
+}
+
 }  // namespace
 }  // namespace xtg
 
@@ -258,64 +543,201 @@ extern "C" {
 void xtgevc3_zgges(char jobvsl, char jobvsr, int n, double *A, int lda, double *B, int ldb, double *alpha,
                    double *beta, double *VSL, int ldvsl, double *VSR, int ldvsr, int *info)
 {
-    xtg::gges_host<double>(jobvsl, jobvsr, n, reinterpret_cast<zc<double> *>(A), lda, reinterpret_cast<zc<double> *>(B),
-                           ldb, reinterpret_cast<zc<double> *>(alpha), reinterpret_cast<zc<double> *>(beta),
-                           reinterpret_cast<zc<double> *>(VSL), ldvsl, reinterpret_cast<zc<double> *>(VSR), ldvsr, info);
+    xtgevc3_zgges_sort(jobvsl, jobvsr, 'N', nullptr, n, A, lda, B, ldb, nullptr, alpha, beta, VSL, ldvsl, VSR, ldvsr,
+                       info);
 }
 
 void xtgevc3_cgges(char jobvsl, char jobvsr, int n, float *A, int lda, float *B, int ldb, float *alpha, float *beta,
                    float *VSL, int ldvsl, float *VSR, int ldvsr, int *info)
 {
-    xtg::gges_host<float>(jobvsl, jobvsr, n, reinterpret_cast<zc<float> *>(A), lda, reinterpret_cast<zc<float> *>(B), ldb,
-                          reinterpret_cast<zc<float> *>(alpha), reinterpret_cast<zc<float> *>(beta),
-                          reinterpret_cast<zc<float> *>(VSL), ldvsl, reinterpret_cast<zc<float> *>(VSR), ldvsr, info);
+    xtgevc3_cgges_sort(jobvsl, jobvsr, 'N', nullptr, n, A, lda, B, ldb, nullptr, alpha, beta, VSL, ldvsl, VSR, ldvsr,
+                       info);
 }
 
 int xtgevc3_zgges_dev(void *stream, char jobvsl, char jobvsr, int n, double *A, int lda, double *B, int ldb,
                       double *alpha, double *beta, double *VSL, int ldvsl, double *VSR, int ldvsr, int *info)
 {
-    return xtg::gges_device<double>(static_cast<cudaStream_t>(stream), jobvsl, jobvsr, n,
-                                    reinterpret_cast<zc<double> *>(A), lda, reinterpret_cast<zc<double> *>(B), ldb,
-                                    reinterpret_cast<zc<double> *>(alpha), reinterpret_cast<zc<double> *>(beta),
-                                    reinterpret_cast<zc<double> *>(VSL), ldvsl, reinterpret_cast<zc<double> *>(VSR),
-                                    ldvsr, info);
+    return xtgevc3_zgges_sort_dev(stream, jobvsl, jobvsr, 'N', nullptr, n, A, lda, B, ldb, nullptr, alpha, beta, VSL,
+                                  ldvsl, VSR, ldvsr, info);
 }
 
 int xtgevc3_cgges_dev(void *stream, char jobvsl, char jobvsr, int n, float *A, int lda, float *B, int ldb, float *alpha,
                       float *beta, float *VSL, int ldvsl, float *VSR, int ldvsr, int *info)
 {
-    return xtg::gges_device<float>(static_cast<cudaStream_t>(stream), jobvsl, jobvsr, n,
-                                   reinterpret_cast<zc<float> *>(A), lda, reinterpret_cast<zc<float> *>(B), ldb,
-                                   reinterpret_cast<zc<float> *>(alpha), reinterpret_cast<zc<float> *>(beta),
-                                   reinterpret_cast<zc<float> *>(VSL), ldvsl, reinterpret_cast<zc<float> *>(VSR), ldvsr,
-                                   info);
+    return xtgevc3_cgges_sort_dev(stream, jobvsl, jobvsr, 'N', nullptr, n, A, lda, B, ldb, nullptr, alpha, beta, VSL,
+                                  ldvsl, VSR, ldvsr, info);
 }
 
 void xtgevc3_dgges(char jobvsl, char jobvsr, int n, double *A, int lda, double *B, int ldb, double *alphar,
                    double *alphai, double *beta, double *VSL, int ldvsl, double *VSR, int ldvsr, int *info)
 {
-    xtg::gges_host_real<double>(jobvsl, jobvsr, n, A, lda, B, ldb, alphar, alphai, beta, VSL, ldvsl, VSR, ldvsr, info);
+    xtg::gges_host_real<double>(jobvsl, jobvsr, 'N', nullptr, n, A, lda, B, ldb, nullptr, alphar, alphai, beta, VSL,
+                                ldvsl, VSR, ldvsr, info);
 }
 
 void xtgevc3_sgges(char jobvsl, char jobvsr, int n, float *A, int lda, float *B, int ldb, float *alphar, float *alphai,
                    float *beta, float *VSL, int ldvsl, float *VSR, int ldvsr, int *info)
 {
-    xtg::gges_host_real<float>(jobvsl, jobvsr, n, A, lda, B, ldb, alphar, alphai, beta, VSL, ldvsl, VSR, ldvsr, info);
+    xtg::gges_host_real<float>(jobvsl, jobvsr, 'N', nullptr, n, A, lda, B, ldb, nullptr, alphar, alphai, beta, VSL,
+                               ldvsl, VSR, ldvsr, info);
 }
 
 int xtgevc3_dgges_dev(void *stream, char jobvsl, char jobvsr, int n, double *A, int lda, double *B, int ldb,
                       double *alphar, double *alphai, double *beta, double *VSL, int ldvsl, double *VSR, int ldvsr,
                       int *info)
 {
-    return xtg::gges_device_real<double>(static_cast<cudaStream_t>(stream), jobvsl, jobvsr, n, A, lda, B, ldb, alphar,
-                                         alphai, beta, VSL, ldvsl, VSR, ldvsr, info);
+    return xtg::gges_device_real<double>(static_cast<cudaStream_t>(stream), jobvsl, jobvsr, 'N', nullptr, n, A, lda, B,
+                                         ldb, nullptr, alphar, alphai, beta, VSL, ldvsl, VSR, ldvsr, info);
 }
 
 int xtgevc3_sgges_dev(void *stream, char jobvsl, char jobvsr, int n, float *A, int lda, float *B, int ldb,
                       float *alphar, float *alphai, float *beta, float *VSL, int ldvsl, float *VSR, int ldvsr, int *info)
 {
-    return xtg::gges_device_real<float>(static_cast<cudaStream_t>(stream), jobvsl, jobvsr, n, A, lda, B, ldb, alphar,
-                                        alphai, beta, VSL, ldvsl, VSR, ldvsr, info);
+    return xtg::gges_device_real<float>(static_cast<cudaStream_t>(stream), jobvsl, jobvsr, 'N', nullptr, n, A, lda, B,
+                                        ldb, nullptr, alphar, alphai, beta, VSL, ldvsl, VSR, ldvsr, info);
+}
+
+// ---- with ordering (SORT, SELCTG, SDIM in LAPACK xGGES's positions) -------------------------
+
+void xtgevc3_zgges_sort(char jobvsl, char jobvsr, char sort, xtgevc3_zselect2 selctg, int n, double *A, int lda,
+                        double *B, int ldb, int *sdim, double *alpha, double *beta, double *VSL, int ldvsl, double *VSR,
+                        int ldvsr, int *info)
+{
+    xtg::gges_host<double>(jobvsl, jobvsr, sort, selctg, n, reinterpret_cast<zc<double> *>(A), lda,
+                           reinterpret_cast<zc<double> *>(B), ldb, sdim, reinterpret_cast<zc<double> *>(alpha),
+                           reinterpret_cast<zc<double> *>(beta), reinterpret_cast<zc<double> *>(VSL), ldvsl,
+                           reinterpret_cast<zc<double> *>(VSR), ldvsr, info);
+}
+
+void xtgevc3_cgges_sort(char jobvsl, char jobvsr, char sort, xtgevc3_cselect2 selctg, int n, float *A, int lda,
+                        float *B, int ldb, int *sdim, float *alpha, float *beta, float *VSL, int ldvsl, float *VSR,
+                        int ldvsr, int *info)
+{
+    xtg::gges_host<float>(jobvsl, jobvsr, sort, selctg, n, reinterpret_cast<zc<float> *>(A), lda,
+                          reinterpret_cast<zc<float> *>(B), ldb, sdim, reinterpret_cast<zc<float> *>(alpha),
+                          reinterpret_cast<zc<float> *>(beta), reinterpret_cast<zc<float> *>(VSL), ldvsl,
+                          reinterpret_cast<zc<float> *>(VSR), ldvsr, info);
+}
+
+int xtgevc3_zgges_sort_dev(void *stream, char jobvsl, char jobvsr, char sort, xtgevc3_zselect2 selctg, int n, double *A,
+                           int lda, double *B, int ldb, int *sdim, double *alpha, double *beta, double *VSL, int ldvsl,
+                           double *VSR, int ldvsr, int *info)
+{
+    return xtg::gges_device<double>(static_cast<cudaStream_t>(stream), jobvsl, jobvsr, sort, selctg, n,
+                                    reinterpret_cast<zc<double> *>(A), lda, reinterpret_cast<zc<double> *>(B), ldb,
+                                    sdim, reinterpret_cast<zc<double> *>(alpha), reinterpret_cast<zc<double> *>(beta),
+                                    reinterpret_cast<zc<double> *>(VSL), ldvsl, reinterpret_cast<zc<double> *>(VSR),
+                                    ldvsr, info);
+}
+
+int xtgevc3_cgges_sort_dev(void *stream, char jobvsl, char jobvsr, char sort, xtgevc3_cselect2 selctg, int n, float *A,
+                           int lda, float *B, int ldb, int *sdim, float *alpha, float *beta, float *VSL, int ldvsl,
+                           float *VSR, int ldvsr, int *info)
+{
+    return xtg::gges_device<float>(static_cast<cudaStream_t>(stream), jobvsl, jobvsr, sort, selctg, n,
+                                   reinterpret_cast<zc<float> *>(A), lda, reinterpret_cast<zc<float> *>(B), ldb, sdim,
+                                   reinterpret_cast<zc<float> *>(alpha), reinterpret_cast<zc<float> *>(beta),
+                                   reinterpret_cast<zc<float> *>(VSL), ldvsl, reinterpret_cast<zc<float> *>(VSR), ldvsr,
+                                   info);
+}
+
+void xtgevc3_dgges_sort(char jobvsl, char jobvsr, char sort, xtgevc3_dselect3 selctg, int n, double *A, int lda,
+                        double *B, int ldb, int *sdim, double *alphar, double *alphai, double *beta, double *VSL,
+                        int ldvsl, double *VSR, int ldvsr, int *info)
+{
+    xtg::gges_host_real<double>(jobvsl, jobvsr, sort, selctg, n, A, lda, B, ldb, sdim, alphar, alphai, beta, VSL, ldvsl,
+                                VSR, ldvsr, info);
+}
+
+void xtgevc3_sgges_sort(char jobvsl, char jobvsr, char sort, xtgevc3_sselect3 selctg, int n, float *A, int lda,
+                        float *B, int ldb, int *sdim, float *alphar, float *alphai, float *beta, float *VSL, int ldvsl,
+                        float *VSR, int ldvsr, int *info)
+{
+    xtg::gges_host_real<float>(jobvsl, jobvsr, sort, selctg, n, A, lda, B, ldb, sdim, alphar, alphai, beta, VSL, ldvsl,
+                               VSR, ldvsr, info);
+}
+
+int xtgevc3_dgges_sort_dev(void *stream, char jobvsl, char jobvsr, char sort, xtgevc3_dselect3 selctg, int n,
+                           double *A, int lda, double *B, int ldb, int *sdim, double *alphar, double *alphai,
+                           double *beta, double *VSL, int ldvsl, double *VSR, int ldvsr, int *info)
+{
+    return xtg::gges_device_real<double>(static_cast<cudaStream_t>(stream), jobvsl, jobvsr, sort, selctg, n, A, lda, B,
+                                         ldb, sdim, alphar, alphai, beta, VSL, ldvsl, VSR, ldvsr, info);
+}
+
+int xtgevc3_sgges_sort_dev(void *stream, char jobvsl, char jobvsr, char sort, xtgevc3_sselect3 selctg, int n, float *A,
+                           int lda, float *B, int ldb, int *sdim, float *alphar, float *alphai, float *beta, float *VSL,
+                           int ldvsl, float *VSR, int ldvsr, int *info)
+{
+    return xtg::gges_device_real<float>(static_cast<cudaStream_t>(stream), jobvsl, jobvsr, sort, selctg, n, A, lda, B,
+                                        ldb, sdim, alphar, alphai, beta, VSL, ldvsl, VSR, ldvsr, info);
+}
+
+}  // extern "C"
+
+// ---- xTGSEN with IJOB = 0 -------------------------------------------------------------------
+
+extern "C" {
+
+void xtgevc3_dtgsen(int ijob, int wantq, int wantz, const int *select, int n, double *A, int lda, double *B, int ldb,
+                    double *alphar, double *alphai, double *beta, double *Q, int ldq, double *Z, int ldz, int *m,
+                    int *info)
+{
+    xtg::tgsen_host<double, false>(ijob, wantq, wantz, select, n, A, lda, B, ldb, alphar, alphai, beta, Q, ldq, Z, ldz,
+                                   m, info);
+}
+
+void xtgevc3_stgsen(int ijob, int wantq, int wantz, const int *select, int n, float *A, int lda, float *B, int ldb,
+                    float *alphar, float *alphai, float *beta, float *Q, int ldq, float *Z, int ldz, int *m, int *info)
+{
+    xtg::tgsen_host<float, false>(ijob, wantq, wantz, select, n, A, lda, B, ldb, alphar, alphai, beta, Q, ldq, Z, ldz,
+                                  m, info);
+}
+
+void xtgevc3_ztgsen(int ijob, int wantq, int wantz, const int *select, int n, double *A, int lda, double *B, int ldb,
+                    double *alpha, double *beta, double *Q, int ldq, double *Z, int ldz, int *m, int *info)
+{
+    xtg::tgsen_host<double, true>(ijob, wantq, wantz, select, n, A, lda, B, ldb, alpha, beta, nullptr, Q, ldq, Z, ldz,
+                                  m, info);
+}
+
+void xtgevc3_ctgsen(int ijob, int wantq, int wantz, const int *select, int n, float *A, int lda, float *B, int ldb,
+                    float *alpha, float *beta, float *Q, int ldq, float *Z, int ldz, int *m, int *info)
+{
+    xtg::tgsen_host<float, true>(ijob, wantq, wantz, select, n, A, lda, B, ldb, alpha, beta, nullptr, Q, ldq, Z, ldz, m,
+                                 info);
+}
+
+int xtgevc3_dtgsen_dev(void *stream, int ijob, int wantq, int wantz, const int *select, int n, double *A, int lda,
+                       double *B, int ldb, double *alphar, double *alphai, double *beta, double *Q, int ldq, double *Z,
+                       int ldz, int *m, int *info)
+{
+    return xtg::tgsen_device<double, false>(static_cast<cudaStream_t>(stream), ijob, wantq, wantz, select, n, A, lda, B,
+                                            ldb, alphar, alphai, beta, Q, ldq, Z, ldz, m, info);
+}
+
+int xtgevc3_stgsen_dev(void *stream, int ijob, int wantq, int wantz, const int *select, int n, float *A, int lda,
+                       float *B, int ldb, float *alphar, float *alphai, float *beta, float *Q, int ldq, float *Z,
+                       int ldz, int *m, int *info)
+{
+    return xtg::tgsen_device<float, false>(static_cast<cudaStream_t>(stream), ijob, wantq, wantz, select, n, A, lda, B,
+                                           ldb, alphar, alphai, beta, Q, ldq, Z, ldz, m, info);
+}
+
+int xtgevc3_ztgsen_dev(void *stream, int ijob, int wantq, int wantz, const int *select, int n, double *A, int lda,
+                       double *B, int ldb, double *alpha, double *beta, double *Q, int ldq, double *Z, int ldz, int *m,
+                       int *info)
+{
+    return xtg::tgsen_device<double, true>(static_cast<cudaStream_t>(stream), ijob, wantq, wantz, select, n, A, lda, B,
+                                           ldb, alpha, beta, nullptr, Q, ldq, Z, ldz, m, info);
+}
+
+int xtgevc3_ctgsen_dev(void *stream, int ijob, int wantq, int wantz, const int *select, int n, float *A, int lda,
+                       float *B, int ldb, float *alpha, float *beta, float *Q, int ldq, float *Z, int ldz, int *m,
+                       int *info)
+{
+    return xtg::tgsen_device<float, true>(static_cast<cudaStream_t>(stream), ijob, wantq, wantz, select, n, A, lda, B,
+                                          ldb, alpha, beta, nullptr, Q, ldq, Z, ldz, m, info);
 }
 
 }  // extern "C"
