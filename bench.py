@@ -69,6 +69,8 @@ def parse():
     ap.add_argument("--tgexc-n", type=int, default=4096, help="order of the ztgexc and dtgexc reordering legs (0 skips)")
     ap.add_argument("--tgsna-n", type=int, default=0,
                     help="order of the dtgsna DIF leg beside LAPACK dtgsna JOB='V'; 0 (the default) skips it")
+    ap.add_argument("--gges-sort", action="store_true",
+                    help="the dgges leg orders the eigenvalues (SORT = 'S', left half-plane first)")
     ap.add_argument("--gges-n", type=int, default=0,
                     help="order of the dgges (QZ step) leg beside LAPACK dgges; 0 (the default) skips it")
     ap.add_argument("--profile-case", default=None,
@@ -830,11 +832,14 @@ def measure_tgexc_blocks(args, X, torch):
 
 
 def measure_gges(args, X, torch):
-    """dgges without ordering (the QZ step) on an iid N(0,1) real pencil of order --gges-n, Q
-    and Z formed: device-resident inputs restored before each step outside the timed region,
-    CUDA-event timing; LAPACK DGGES (SciPy's OpenBLAS, SORT = 'N') on the same pencil beside it,
-    the eigenvalues compared (each matched to its nearest)."""
+    """dgges (the QZ step) on an iid N(0,1) real pencil of order --gges-n, Q and Z formed:
+    device-resident inputs restored before each step outside the timed region, CUDA-event
+    timing; LAPACK DGGES (SciPy's OpenBLAS) on the same pencil beside it, the eigenvalues
+    compared (each matched to its nearest).  With --gges-sort both order the eigenvalues of the
+    left half-plane first (SORT = 'S', SELCTG alphar * beta < 0; xtgevc3_dgges_sort_dev, the
+    reordering kernel inside the timed region) and SDIM is compared too."""
     n = args.gges_n
+    sort = (lambda ar, ai, b: ar * b < 0) if args.gges_sort else None
     rng = np.random.default_rng(args.seed + 53)
     A_h, B_h = np.asfortranarray(rng.standard_normal((n, n))), np.asfortranarray(rng.standard_normal((n, n)))
     A0, B0 = colmajor_cuda(A_h, torch), colmajor_cuda(B_h, torch)
@@ -846,24 +851,33 @@ def measure_gges(args, X, torch):
         B.copy_(B0)
         torch.cuda.synchronize()
         e0.record()
-        res = X.gges_dev(A, B, Q, Z)
+        res = X.gges_dev(A, B, Q, Z, sort=sort)
         e1.record()
         torch.cuda.synchronize()
         if it >= max(args.warmup, 1):
             ts.append(e0.elapsed_time(e1))
     ms = float(np.mean(ts))
     ar, ai, be = (t.cpu().numpy() for t in res[:3])
-    out = {"n": n, "ms": ms, "info": int(res[3]), "data": "iid N(0,1) real pencil, Q and Z formed"}
+    out = {"n": n, "ms": ms, "info": int(res[-1]), "sort": "S (left half-plane first)" if sort else "N",
+           "data": "iid N(0,1) real pencil, Q and Z formed"}
+    if sort:
+        out["sdim"] = int(res[3])
     if not args.no_cpu:
         import scipy.linalg.lapack as la
         t0 = time.perf_counter()
-        r = la.dgges(lambda *a: 0, A_h.copy(order="F"), B_h.copy(order="F"), sort_t=0)
+        if sort:
+            r = la.dgges(lambda x, y, z: int(x * z < 0), A_h.copy(order="F"), B_h.copy(order="F"), sort_t=1)
+        else:
+            r = la.dgges(lambda x, y, z: 0, A_h.copy(order="F"), B_h.copy(order="F"), sort_t=0)
         tc = time.perf_counter() - t0
+        if sort:
+            out["sdim_lapack"] = int(r[2])
         ref = (r[3] + 1j * r[4]) / r[5]
         fin = be != 0
         ev = (ar[fin] + 1j * ai[fin]) / be[fin]
         err = max([float(np.min(np.abs(ref - e)) / max(1.0, abs(e))) for e in ev] + [0.0])
-        out["cpu_lapack"] = {"seconds": tc, "cores": host_threads(), "kind": "LAPACK dgges (SciPy OpenBLAS), SORT='N'"}
+        out["cpu_lapack"] = {"seconds": tc, "cores": host_threads(),
+                             "kind": f"LAPACK dgges (SciPy OpenBLAS), SORT='{'S' if sort else 'N'}'"}
         out["speedup_vs_lapack"] = tc / (ms * 1e-3)
         out["max_eigenvalue_rel_diff_vs_lapack"] = err
     del A0, B0, A, B, Q, Z
