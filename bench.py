@@ -69,6 +69,10 @@ def parse():
     ap.add_argument("--tgexc-n", type=int, default=4096, help="order of the ztgexc and dtgexc reordering legs (0 skips)")
     ap.add_argument("--tgsna-n", type=int, default=0,
                     help="order of the dtgsna DIF leg beside LAPACK dtgsna JOB='V'; 0 (the default) skips it")
+    ap.add_argument("--reference-table", action="store_true",
+                    help="only the upstream benchmark table (BM_xtgevc3 rows: SIDE=B, HOWMNY=A over --table-sizes)")
+    ap.add_argument("--table-sizes", default="", help="comma-separated orders (default: the upstream list)")
+    ap.add_argument("--table-prec", default="dszc", help="types of the table, any of d s z c")
     ap.add_argument("--gges-sort", action="store_true",
                     help="the dgges leg orders the eigenvalues (SORT = 'S', left half-plane first)")
     ap.add_argument("--gges-n", type=int, default=0,
@@ -1136,10 +1140,109 @@ def gemm_only(args):
     return 0
 
 
+# the upstream benchmark's sizes (benchmarks/bench_dtgevc3.cpp:18)
+REF_TABLE_SIZES = (500, 707, 1000, 1414, 2000, 2828, 4000, 5657, 8000)
+_TABLE_TYPES = {"d": np.float64, "s": np.float32, "z": np.complex128, "c": np.complex64}
+
+
+def table_inputs(prec, n, seed):
+    """The pencil of one row of the upstream benchmark table: (S, P, alpha, alphai, beta) on
+    the host (alphai zeros for real types, None for complex)."""
+    from xtgevc3_b200 import pencils as gen
+    dt = _TABLE_TYPES[prec]
+    S, P, al, be = gen.gen_bench_triangular(n, seed=seed, dtype=dt)
+    ai = np.zeros(n, dtype=dt) if prec in "ds" else None
+    return S, P, al, ai, be
+
+
+def table_reference_row(prec, n, seed):
+    """One upstream xtgevc3 call (SIDE='B', HOWMNY='A') on the row's pencil, the library built
+    from the upstream sources (oracle/_ref) on the threads set by oracle.set_ref_threads:
+    returns (seconds, VL, VR)."""
+    import oracle
+    S, P, al, ai, be = table_inputs(prec, n, seed)
+    dt = S.dtype
+    VL, VR = (np.zeros((n, n), dtype=dt, order="F") for _ in range(2))
+    t0 = time.perf_counter()
+    VL, VR, m, info = oracle.tgevc3("B", "A", S, P, al, be, alphai=ai, VL=VL, VR=VR, impl="ref")
+    t = time.perf_counter() - t0
+    assert (m, info) == (n, 0), (prec, n, m, info)
+    return t, VL, VR
+
+
+def reference_table(args):
+    """The upstream benchmark table on this GPU.  benchmarks/bench_{d,s,z,c}tgevc3.cpp time
+    xtgevc3 (BM_xtgevc3) at n = 500, 707, ..., 8000 with SIDE='B', HOWMNY='A' on triangular
+    pencils (pencils.gen_bench_triangular: their distributions, seeded numpy draws).  Per type
+    (--table-prec) and n (--table-sizes): the device form on resident inputs (CUDA events,
+    mean of --steps after --warmup), the host-pointer call as the upstream benchmark makes it
+    (host arrays in and out, every copy inside; wall clock, best of --steps), and beside them
+    the upstream library (oracle/_ref) on every host thread, one call per row until
+    --ref-budget-s is spent (later rows: null), with the largest column difference between its
+    output and the host-pointer call's (both in the upstream scaling).  Prints one JSON line."""
+    import torch
+    import oracle
+    import xtgevc3_b200 as X
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    sizes = [int(v) for v in args.table_sizes.split(",")] if args.table_sizes else list(REF_TABLE_SIZES)
+    thr = host_threads()
+    have_ref = not args.no_cpu and oracle.ref_available()
+    if have_ref:
+        oracle.set_ref_threads(thr)
+        table_reference_row("d", 256, args.seed)  # library, OpenBLAS threads and page-ins warm
+    tdt = {"d": torch.float64, "s": torch.float32, "z": torch.complex128, "c": torch.complex64}
+    rows, spent = [], 0.0
+    for prec in args.table_prec:
+        for n in sizes:
+            S_h, P_h, al, ai, be = table_inputs(prec, n, args.seed)
+            S, P = colmajor_cuda(S_h, torch), colmajor_cuda(P_h, torch)
+            VL, VR = (torch.zeros(n, n, dtype=tdt[prec], device="cuda").t() for _ in range(2))
+            for _ in range(max(args.warmup, 1)):
+                X.tgevc3_dev("B", "A", S, P, al, be, alphai=ai, VL=VL, VR=VR)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(args.steps):
+                X.tgevc3_dev("B", "A", S, P, al, be, alphai=ai, VL=VL, VR=VR)
+            e1.record()
+            torch.cuda.synchronize()
+            dev_ms = e0.elapsed_time(e1) / args.steps
+            del S, P, VL, VR
+            VLh, VRh = (np.zeros((n, n), dtype=S_h.dtype, order="F") for _ in range(2))
+            X.tgevc3("B", "A", S_h, P_h, al, be, alphai=ai, VL=VLh, VR=VRh)
+            host_s = float("inf")
+            for _ in range(args.steps):
+                t0 = time.perf_counter()
+                X.tgevc3("B", "A", S_h, P_h, al, be, alphai=ai, VL=VLh, VR=VRh)
+                host_s = min(host_s, time.perf_counter() - t0)
+            row = {"prec": prec, "n": n, "device_ms": dev_ms, "host_ms": host_s * 1e3, "ref_cpu_ms": None}
+            if have_ref and spent < args.ref_budget_s:
+                t, VLr, VRr = table_reference_row(prec, n, args.seed)
+                spent += t
+                diff = max(float((np.abs(V - R).max(0) / np.maximum(np.abs(R).max(0), 1e-300)).max())
+                           for V, R in ((VLh, VLr), (VRh, VRr)))
+                row.update({"ref_cpu_ms": t * 1e3, "host_speedup_vs_ref": t / host_s,
+                            "max_col_rel_diff_vs_ref": diff})
+            rows.append(row)
+            print(f"[table] {prec} n={n}: device {dev_ms:.2f} ms, host {host_s * 1e3:.2f} ms, "
+                  f"ref {row['ref_cpu_ms']} ms", file=sys.stderr, flush=True)
+    print(json.dumps({"mode": "reference_table", "side": "B", "howmny": "A", "sizes": sizes,
+                      "precisions": args.table_prec, "ref_kind": "reference" if have_ref else None,
+                      "ref_threads": thr, "steps": args.steps, "warmup": args.warmup,
+                      "data": "triangular pencils with the upstream benchmark generators' distributions "
+                              "(U(-1,1) entries, P diagonal p + sign(p)), seeded",
+                      "rows": rows}))
+    return 0
+
+
 def main():
     args = parse()
     if args.profile_case:
         return profile_case(args)
+    if args.reference_table:
+        return reference_table(args)
     if args.gemm_only:
         return gemm_only(args)
     if args.impl == "reference":

@@ -15,6 +15,10 @@ These are inputs, not checkers: the tests and bench.py both use them.
 * ``gen_quasi_triangular`` / ``gen_upper_triangular_complex`` -- random (quasi-)triangular
                         pencils with the structure of the upstream self-tests
                         (tests/test_dtgevc3.cpp:266-316, tests/test_ztgevc3.cpp:126-144).
+* ``gen_bench_triangular`` -- the upstream benchmark's pencils
+                        (benchmarks/bench_dtgevc3.cpp:26-48, bench_ztgevc3.cpp:28-50):
+                        upper-triangular S and P with U(-1,1) entries (complex: U(-1,1) real and
+                        imaginary parts), P's diagonal real, p + sign(p) with p ~ U(-1,1).
 """
 from __future__ import annotations
 
@@ -65,6 +69,26 @@ def gen_upper_triangular_complex(n, seed=0, dtype=np.complex128):
     P = np.triu(rng.uniform(-1, 1, (n, n)) + 1j * rng.uniform(-1, 1, (n, n)))
     d = np.diag(P).copy()
     P[np.diag_indices(n)] = d + d / np.abs(d)
+    S, P = np.asfortranarray(S.astype(dtype)), np.asfortranarray(P.astype(dtype))
+    return S, P, np.diag(S).copy(), np.diag(P).copy()
+
+
+def gen_bench_triangular(n, seed=0, dtype=np.float64):
+    """Upper-triangular pencil with the distributions of the upstream benchmark's generators
+    (seeded numpy draws stand in for their std::mt19937 stream): S and P entries U(-1,1)
+    (complex: both parts), P's diagonal real p + sign(p), p ~ U(-1,1), so |P_kk| in [1, 2).
+    Returns (S, P, alpha, beta) with alpha = diag(S), beta = diag(P); a real pencil has no 2x2
+    blocks (alphai = 0)."""
+    rng = np.random.default_rng(seed)
+    cplx = np.issubdtype(dtype, np.complexfloating)
+
+    def draw():
+        m = rng.uniform(-1, 1, (n, n))
+        return np.triu(m + 1j * rng.uniform(-1, 1, (n, n)) if cplx else m)
+
+    S, P = draw(), draw()
+    p = rng.uniform(-1, 1, n)
+    P[np.diag_indices(n)] = p + np.where(p >= 0, 1.0, -1.0)
     S, P = np.asfortranarray(S.astype(dtype)), np.asfortranarray(P.astype(dtype))
     return S, P, np.diag(S).copy(), np.diag(P).copy()
 
