@@ -11,8 +11,8 @@ Contents
                      ``make -C oracle ref`` where the upstream tree is present);
   * LAPACK from SciPy's bundled OpenBLAS (Fortran interface where SciPy's wrapper drops an
     output) as the oracle of the LAPACK-compatible entry points: xTGEVC, xTREVC3, xTGSNA
-    (JOB 'E', 'V', 'B'), xTGEXC and the single swap xTGEX2, xTGSEN (IJOB = 0) and xGGES
-    with ordering;
+    (JOB 'E', 'V', 'B'), xTGEXC and the single swap xTGEX2, xTGSEN, xTGSYL and xGGES with
+    ordering;
   * residual checks and the comparison normalisation (the seeded pencil generators live
     in ``xtgevc3_b200.pencils`` and are re-exported here for the tests).
 """
@@ -333,6 +333,28 @@ def lapack_tgex2_real(A, B, Q, Z, j1, n1, n2):
     f(iv(int(wq)), iv(int(wz)), iv(n), _ptr(A), iv(ld), _ptr(B), iv(ld), _ptr(Q), iv(ld), _ptr(Z), iv(ld),
       iv(j1), iv(n1), iv(n2), _ptr(work), iv(lwork), ct.byref(info))
     return A, B, (Q if wq else None), (Z if wz else None), info.value
+
+
+def lapack_tgsyl(trans, ijob, A, B, C, D, E, F):
+    """LAPACK D/S/Z/CTGSYL through its Fortran interface in SciPy's OpenBLAS: the generalized
+    Sylvester equation A R - L B = scale C, D R - L E = scale F (TRANS = 'N').  Returns (R, L,
+    scale, dif, info) (R, L new arrays)."""
+    dt = A.dtype.type
+    pfx = {np.float64: "d", np.float32: "s", np.complex128: "z", np.complex64: "c"}[dt]
+    rt = {np.float64: ct.c_double, np.float32: ct.c_float, np.complex128: ct.c_double, np.complex64: ct.c_float}[dt]
+    f = getattr(_openblas(), f"scipy_{pfx}tgsyl_")
+    m, n = C.shape
+    A, B, D, E = (np.asfortranarray(M).copy(order="F") for M in (A, B, D, E))
+    C, F = (np.asfortranarray(M).copy(order="F") for M in (C, F))
+    iv = lambda v: ct.byref(ct.c_int(v))  # noqa: E731
+    scale, dif, info = rt(0), rt(0), ct.c_int(0)
+    lwork = max(1, 2 * m * n)
+    work = np.zeros(lwork, dtype=dt)
+    iwork = np.zeros(m + n + 6, dtype=np.int32)
+    f(ct.c_char_p(trans.encode()), iv(ijob), iv(m), iv(n), _ptr(A), iv(max(m, 1)), _ptr(B), iv(max(n, 1)), _ptr(C),
+      iv(max(m, 1)), _ptr(D), iv(max(m, 1)), _ptr(E), iv(max(n, 1)), _ptr(F), iv(max(m, 1)), ct.byref(scale),
+      ct.byref(dif), _ptr(work), iv(lwork), _ptr(iwork), ct.byref(info), ct.c_size_t(1))
+    return C, F, scale.value, dif.value, info.value
 
 
 def lapack_tgsen0(select, A, B, Q, Z):

@@ -9,6 +9,7 @@
 
 #include "../xtgevc3_b200/csrc/qz_real.cuh"
 #include "../xtgevc3_b200/csrc/tgsen.cuh"
+#include "../xtgevc3_b200/csrc/tgsyl.cuh"
 
 using namespace xtg::rb;
 
@@ -104,6 +105,55 @@ int run_tgsen_cplx(int nth, int wantq, int wantz, int n, R *A, R *B, R *Q, R *Z,
     return info;
 }
 
+template <class R>
+int run_tgsyl(int nth, int ijob, int m, int n, const R *A, const R *B, R *C, const R *D, const R *E, R *F, R *scale,
+              R *dif)
+{
+    SylvShared<R> sh{};
+    SylvG<R> &y = sh.y;
+    y.m = m;
+    y.n = n;
+    y.A = A;
+    y.D = D;
+    y.B = B;
+    y.E = E;
+    y.lda = y.ldd = y.ldc = y.ldf = m;
+    y.ldb = y.lde = n;
+    y.C = C;
+    y.F = F;
+    std::vector<int> cuts(m / 2 + n / 2 + 4);
+    std::vector<R> work(2 * (size_t)m * n);
+    std::barrier<> bar(nth);
+    std::vector<std::thread> th;
+    for (int t = 0; t < nth; t++)
+        th.emplace_back([&, t] { tgsyl_cta(CtaHost{t, nth, &bar}, sh, ijob, cuts.data(), work.data(), dif); });
+    for (auto &x : th) x.join();
+    *scale = sh.scale;
+    return sh.info;
+}
+
+template <class R>
+int run_tgsen_full(int nth, int ijob, int n, R *A, R *B, R *Q, R *Z, const int *sel, R *ar, R *ai, R *be, R *est,
+                   int *m)
+{
+    Pencil<R> p{n, 1, 1, A, B, Q, Z, n, n, n, n};
+    WalkShared<R> shw{};
+    SylvShared<R> shs{};
+    std::vector<R> work((size_t)n * n / 2 + 2);
+    std::vector<int> cuts(n / 2 + 4);
+    int info = 0;
+    std::barrier<> bar(nth);
+    std::vector<std::thread> th;
+    for (int t = 0; t < nth; t++)
+        th.emplace_back([&, t] {
+            const int i = tgsen_real_full_cta(CtaHost{t, nth, &bar}, shw, shs, p, sel, ijob, ar, ai, be, work.data(),
+                                              cuts.data(), est, m);
+            if (t == 0) info = i;
+        });
+    for (auto &x : th) x.join();
+    return info;
+}
+
 // SELCTG from flags: the test passes the selection that LAPACK's SELCTG made, one flag per
 // eigenvalue in order, and the check reads them back in the same order
 struct FlagSel {
@@ -142,6 +192,33 @@ int host_ctgsen0(int nth, int wantq, int wantz, int n, float *A, float *B, float
                  float *al, float *be)
 {
     return run_tgsen_cplx(nth, wantq, wantz, n, A, B, Q, Z, sel, al, be);
+}
+
+// DTGSEN (IJOB 0, 1, 2, 4) body with Q and Z: est = PL, PR, DIF(1), DIF(2); returns INFO
+int host_dtgsen(int nth, int ijob, int n, double *A, double *B, double *Q, double *Z, const int *sel, double *ar,
+                double *ai, double *be, double *est, int *m)
+{
+    return run_tgsen_full(nth, ijob, n, A, B, Q, Z, sel, ar, ai, be, est, m);
+}
+
+int host_stgsen(int nth, int ijob, int n, float *A, float *B, float *Q, float *Z, const int *sel, float *ar, float *ai,
+                float *be, float *est, int *m)
+{
+    return run_tgsen_full(nth, ijob, n, A, B, Q, Z, sel, ar, ai, be, est, m);
+}
+
+// xTGSYL (TRANS = 'N', IJOB 0 / 1 / 3) body: A, D m x m, B, E n x n, C, F m x n (leading
+// dimensions m, n, m); returns INFO
+int host_dtgsyl(int nth, int ijob, int m, int n, const double *A, const double *B, double *C, const double *D,
+                const double *E, double *F, double *scale, double *dif)
+{
+    return run_tgsyl(nth, ijob, m, n, A, B, C, D, E, F, scale, dif);
+}
+
+int host_stgsyl(int nth, int ijob, int m, int n, const float *A, const float *B, float *C, const float *D,
+                const float *E, float *F, float *scale, float *dif)
+{
+    return run_tgsyl(nth, ijob, m, n, A, B, C, D, E, F, scale, dif);
 }
 
 // xGGES's check: SELCTG's answers as flags in order; returns SDIM, *info as the check leaves it

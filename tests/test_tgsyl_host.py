@@ -1,0 +1,190 @@
+"""The generalized Sylvester solver (xtgevc3_b200/csrc/tgsyl.cuh: rb::tgsyl_cta, LAPACK
+D/STGSYL with TRANS = 'N') and xTGSEN's estimates on it (tgsen.cuh: rb::tgsen_real_estimates,
+IJOB 1, 2, 4) compiled for the CPU by tests/qz_host.cpp, against LAPACK.
+
+The oracles are LAPACK's own DTGSYL (its Fortran interface in SciPy's OpenBLAS) and DTGSEN
+(SciPy's wrapper), on generalized Schur pencils from LAPACK DGGES of iid N(0,1) pencils.  The
+solver follows xTGSYL's blocked order, so R, L, SCALE and the DIF estimate agree with LAPACK's
+to rounding (1e-12 double, 2e-4 single).  xTGSEN's PL and PR do not depend on the signs the
+real 2x2 swaps leave on the reordered pencil's columns and agree to rounding too; its DIF
+estimates (xLATDF's look-ahead) do, and the reordering chooses those signs on rounding-level
+quantities as LAPACK does, so DIF is checked exactly on LAPACK's own reordered pencil and
+within a factor of 2 on ours.
+"""
+import ctypes as ct
+
+import numpy as np
+import pytest
+import scipy.linalg.lapack as la
+
+import oracle
+from test_qz_host import _p, host  # noqa: F401  (fixture)
+from test_tgsen_host import REAL_SELECTIONS, _real_schur
+
+
+def _schur(k, seed, dt=np.float64):
+    g = np.random.default_rng(seed)
+    S, T, *_ = la.dgges(lambda x, y, z: 0, g.standard_normal((k, k)), g.standard_normal((k, k)))
+    return np.asfortranarray(S.astype(dt)), np.asfortranarray(T.astype(dt))
+
+
+def host_tgsyl(L, ijob, A, B, C, D, E, F, nth=1):
+    dt = A.dtype.type
+    m, n = C.shape
+    Cw, Fw = np.array(C, order="F"), np.array(F, order="F")
+    rt = ct.c_double if dt == np.float64 else ct.c_float
+    sc, dif = rt(0), rt(0)
+    f = L.host_dtgsyl if dt == np.float64 else L.host_stgsyl
+    info = f(nth, ijob, m, n, _p(A), _p(B), _p(Cw), _p(D), _p(E), _p(Fw), ct.byref(sc), ct.byref(dif))
+    return Cw, Fw, sc.value, dif.value, info
+
+
+SIZES = [(1, 1), (2, 2), (1, 5), (5, 1), (2, 7), (3, 4), (7, 9), (20, 13), (41, 17)]
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32], ids=["d", "s"])
+@pytest.mark.parametrize("mn", SIZES, ids=lambda t: f"{t[0]}x{t[1]}")
+def test_tgsyl_matches_lapack(host, dt, mn):
+    m, n = mn
+    tol = 1e-12 if dt == np.float64 else 2e-4
+    for seed in range(3):
+        A, D = _schur(m, seed, dt)
+        B, E = _schur(n, seed + 100, dt)
+        g = np.random.default_rng(seed + 7)
+        C, F = (np.asfortranarray(g.standard_normal((m, n)).astype(dt)) for _ in range(2))
+        for ijob in (0, 1, 3):
+            rR, rL, rs, rd, ri = oracle.lapack_tgsyl("N", ijob, A, B, C, D, E, F)
+            hR, hL, hs, hd, hi = host_tgsyl(host, ijob, A, B, C, D, E, F)
+            assert (hi, hs) == (ri, rs), (ijob, hi, ri, hs, rs)
+            if ijob != 3:
+                for M, R in ((hR, rR), (hL, rL)):
+                    assert np.abs(M - R).max() <= tol * 10 * max(np.abs(R).max(), 1.0), (ijob, seed)
+            if ijob != 0:
+                assert abs(hd - rd) <= tol * 10 * abs(rd), (ijob, hd, rd)
+
+
+def test_tgsyl_threads_bit_for_bit(host):
+    """The solver's body on 5 and 64 host threads gives the one-thread result bit for bit."""
+    A, D = _schur(23, 1)
+    B, E = _schur(19, 2)
+    g = np.random.default_rng(3)
+    C, F = (np.asfortranarray(g.standard_normal((23, 19))) for _ in range(2))
+    for ijob in (0, 1, 3):
+        one = host_tgsyl(host, ijob, A, B, C, D, E, F, nth=1)
+        for nth in (5, 64):
+            many = host_tgsyl(host, ijob, A, B, C, D, E, F, nth=nth)
+            assert np.array_equal(one[0], many[0]) and np.array_equal(one[1], many[1])
+            assert one[2:] == many[2:]
+
+
+def test_tgsyl_scales_against_overflow(host):
+    """Right-hand sides near the overflow threshold: xGESC2 scales the solution down and SCALE <
+    1 reports it, as LAPACK does (same SCALE, same solution)."""
+    A, D = _schur(6, 4)
+    B, E = _schur(5, 5)
+    A[np.diag_indices(6)] *= 1e-6
+    D[np.diag_indices(6)] *= 1e-6
+    g = np.random.default_rng(6)
+    C, F = (np.asfortranarray(g.standard_normal((6, 5)) * 1e305) for _ in range(2))
+    rR, rL, rs, _, ri = oracle.lapack_tgsyl("N", 0, A, B, C, D, E, F)
+    hR, hL, hs, _, hi = host_tgsyl(host, 0, A, B, C, D, E, F)
+    assert rs < 1 and (hs, hi) == (rs, ri)
+    for M, R in ((hR, rR), (hL, rL)):
+        assert np.all(np.isfinite(M)) and np.abs(M - R).max() <= 1e-11 * np.abs(R).max()
+
+
+def host_tgsen_full(L, ijob, sel, A, B, Q, Z, nth=1):
+    dt = A.dtype.type
+    n = A.shape[0]
+    a, b, q, z = (np.array(M, order="F") for M in (A, B, Q, Z))
+    ev = [np.zeros(max(n, 1), dtype=dt) for _ in range(3)]
+    est = np.zeros(4, dtype=dt)
+    m = ct.c_int(-1)
+    f = L.host_dtgsen if dt == np.float64 else L.host_stgsen
+    s = np.ascontiguousarray(sel, dtype=np.int32)
+    info = f(nth, ijob, n, _p(a), _p(b), _p(q), _p(z), _p(s), *[_p(e) for e in ev], _p(est), ct.byref(m))
+    return a, b, q, z, ev, est, m.value, info
+
+
+@pytest.mark.parametrize("kind", ["neg_real", "pairs", "reals", "first_of_pair", "every_third", "none", "all"],
+                         ids=str)
+@pytest.mark.parametrize("n,seed", [(8, 3), (30, 11), (45, 4)], ids=["8", "30", "45"])
+def test_tgsen_estimates_match_lapack(host, kind, n, seed):
+    S, T, Q, Z, ar, ai, be = _real_schur(n, seed, np.float64)
+    sel = REAL_SELECTIONS[kind](ar, ai, be).astype(np.int32)
+    lw = n * n + 64
+    for ijob in (1, 2, 4):
+        r = la.dtgsen(sel, S, T, Q, Z, ijob=ijob, lwork=lw, liwork=lw)
+        a, b, q, z, ev, est, m, info = host_tgsen_full(host, ijob, sel, S, T, Q, Z)
+        assert (m, info) == (r[7], r[8 + 3]) == (r[7], 0)
+        if ijob in (1, 4):
+            assert abs(est[0] - r[8]) <= 1e-10 * r[8] and abs(est[1] - r[9]) <= 1e-10 * r[9], (est, r[8], r[9])
+        if ijob in (2, 4):
+            d = r[10]
+            if 0 < m < n:
+                assert np.all(est[2:] <= 2 * d) and np.all(est[2:] >= d / 2), (est[2:], d)
+            else:  # ||(A, B)||_F, no swap involved
+                assert np.allclose(est[2:], d, rtol=1e-13)
+    # exact on LAPACK's own reordered pencil: DIF(1), DIF(2) from the solver there
+    if 0 < sel.sum() < n:
+        r0 = la.dtgsen(sel, S, T, Q, Z, ijob=0, lwork=lw, liwork=lw)
+        r2 = la.dtgsen(sel, S, T, Q, Z, ijob=2, lwork=lw, liwork=lw)
+        A, B, m = r0[0], r0[1], r0[7]
+        z0 = np.zeros((m, n - m), order="F")
+        d1 = host_tgsyl(host, 3, np.asfortranarray(A[:m, :m]), np.asfortranarray(A[m:, m:]), z0,
+                        np.asfortranarray(B[:m, :m]), np.asfortranarray(B[m:, m:]), z0)[3]
+        z1 = np.zeros((n - m, m), order="F")
+        d2 = host_tgsyl(host, 3, np.asfortranarray(A[m:, m:]), np.asfortranarray(A[:m, :m]), z1,
+                        np.asfortranarray(B[m:, m:]), np.asfortranarray(B[:m, :m]), z1)[3]
+        assert abs(d1 - r2[10][0]) <= 1e-12 * r2[10][0] and abs(d2 - r2[10][1]) <= 1e-12 * r2[10][1]
+
+
+def test_tgsen_estimates_rejection_and_threads(host):
+    """A rejected swap gives PL = PR = DIF = 0 (INFO = 1), as LAPACK; the estimates' bodies on
+    7 host threads give the one-thread result bit for bit."""
+    from test_tgexc_blocks_host import _twin_blocks_pencil
+    A, B, Q, Z = _twin_blocks_pencil(1)
+    sel = np.array([0, 0, 0, 0, 1, 0], np.int32)
+    r = la.dtgsen(sel, A, B, Q, Z, ijob=4, lwork=200, liwork=200)
+    h = host_tgsen_full(host, 4, sel, A, B, Q, Z)
+    assert h[7] == r[11] == 1 and np.all(h[5] == 0) and r[8] == r[9] == 0 and np.all(r[10] == 0)
+    S, T, Q, Z, ar, ai, be = _real_schur(30, 11, np.float64)
+    sel = REAL_SELECTIONS["neg_real"](ar, ai, be).astype(np.int32)
+    one = host_tgsen_full(host, 4, sel, S, T, Q, Z, nth=1)
+    many = host_tgsen_full(host, 4, sel, S, T, Q, Z, nth=7)
+    for x, y in zip(one[:4] + (one[5],), many[:4] + (many[5],)):
+        assert np.array_equal(x, y)
+
+
+def test_tgsyl_and_tgsen_argument_checks():
+    """xtgevc3_dtgsyl's checks (TRANS -1, IJOB -2, M -3, N -4, LDA -6, LDB -8, LDC -10, LDD -12,
+    LDE -14, LDF -16) and xtgevc3_dtgsen's refusals of IJOB 3, 5 (and complex IJOB != 0), all
+    before any device work."""
+    import xtgevc3_b200 as X
+    L = X.lib()
+    M = np.zeros((4, 4))
+    sc, dif = ct.c_double(0), ct.c_double(0)
+    cases = [(b"T", 0, 4, 4, 4, 4, 4, 4, 4, 4, -1), (b"N", 2, 4, 4, 4, 4, 4, 4, 4, 4, -2),
+             (b"N", 5, 4, 4, 4, 4, 4, 4, 4, 4, -2), (b"N", 0, 0, 4, 4, 4, 4, 4, 4, 4, -3),
+             (b"N", 0, 4, 0, 4, 4, 4, 4, 4, 4, -4), (b"N", 0, 4, 4, 3, 4, 4, 4, 4, 4, -6),
+             (b"N", 0, 4, 4, 4, 3, 4, 4, 4, 4, -8), (b"N", 0, 4, 4, 4, 4, 3, 4, 4, 4, -10),
+             (b"N", 0, 4, 4, 4, 4, 4, 3, 4, 4, -12), (b"N", 0, 4, 4, 4, 4, 4, 4, 3, 4, -14),
+             (b"N", 0, 4, 4, 4, 4, 4, 4, 4, 3, -16)]
+    for tr, ijob, m, n, lda, ldb, ldc, ldd, lde, ldf, want in cases:
+        info = ct.c_int(99)
+        L.xtgevc3_dtgsyl(tr, ijob, m, n, _p(M), lda, _p(M), ldb, _p(M), ldc, _p(M), ldd, _p(M), lde, _p(M), ldf,
+                         ct.byref(sc), ct.byref(dif), ct.byref(info))
+        assert info.value == want, (tr, ijob, want, info.value)
+    sel = np.zeros(4, np.int32)
+    v = np.zeros(8)
+    m = ct.c_int(0)
+    for ijob in (3, 5, -1, 6):
+        info = ct.c_int(99)
+        L.xtgevc3_dtgsen(ijob, 1, 1, _p(sel), 4, _p(M), 4, _p(M), 4, _p(v), _p(v), _p(v), _p(M), 4, _p(M), 4,
+                         ct.byref(m), _p(v), _p(v), _p(v), ct.byref(info))
+        assert info.value == -1
+    Mc, vc = np.zeros((4, 4), complex), np.zeros(8, complex)
+    info = ct.c_int(99)
+    L.xtgevc3_ztgsen(1, 1, 1, _p(sel), 4, _p(Mc), 4, _p(Mc), 4, _p(vc), _p(vc), _p(Mc), 4, _p(Mc), 4, ct.byref(m),
+                     _p(v), _p(v), _p(v), ct.byref(info))
+    assert info.value == -1

@@ -140,13 +140,20 @@ def lib():
             f = getattr(L, f"xtgevc3_{p}gges_sort_dev")
             f.argtypes = [_P, _C, _C, _C, sel, _I, _P, _I, _P, _I, _P] + [_P] * nv + [_P, _I, _P, _I, _P]
             f.restype = _I
-        for p in "dszc":  # xTGSEN with IJOB = 0
+        for p in "dszc":  # xTGSEN: ..., M, PL, PR, DIF, INFO
             nv = 2 if p in "zc" else 3
             f = getattr(L, f"xtgevc3_{p}tgsen")
-            f.argtypes = [_I, _I, _I, _P, _I, _P, _I, _P, _I] + [_P] * nv + [_P, _I, _P, _I, _P, _P]
+            f.argtypes = [_I, _I, _I, _P, _I, _P, _I, _P, _I] + [_P] * nv + [_P, _I, _P, _I, _P, _P, _P, _P, _P]
             f.restype = None
             f = getattr(L, f"xtgevc3_{p}tgsen_dev")
-            f.argtypes = [_P, _I, _I, _I, _P, _I, _P, _I, _P, _I] + [_P] * nv + [_P, _I, _P, _I, _P, _P]
+            f.argtypes = [_P, _I, _I, _I, _P, _I, _P, _I, _P, _I] + [_P] * nv + [_P, _I, _P, _I, _P, _P, _P, _P, _P]
+            f.restype = _I
+        for p in "ds":  # xTGSYL (TRANS = 'N')
+            f = getattr(L, f"xtgevc3_{p}tgsyl")
+            f.argtypes = [_C, _I, _I, _I] + [_P, _I] * 6 + [_P, _P, _P]
+            f.restype = None
+            f = getattr(L, f"xtgevc3_{p}tgsyl_dev")
+            f.argtypes = [_P, _C, _I, _I, _I] + [_P, _I] * 6 + [_P, _P, _P]
             f.restype = _I
         for p in "dszc":  # xTGSNA DIF on the device
             f = getattr(L, f"xtgevc3_{p}tgsna_dif_dev")
@@ -548,10 +555,11 @@ def gges_dev(A, B, VSL=None, VSR=None, stream=None, sort=None):
     return (*out, info.value) if sort is None else (*out, sdim.value, info.value)
 
 
-def tgsen(select, A, B, Q=None, Z=None):
-    """Host-array form of d/s/z/ctgsen with IJOB = 0: the eigenvalues flagged in select move to
-    the leading rows (Q, Z None: not updated).  Returns (A, B, eigenvalue arrays..., Q, Z, m,
-    info) as new arrays, the eigenvalue arrays (alphar, alphai, beta) or (alpha, beta)."""
+def tgsen(select, A, B, Q=None, Z=None, ijob=0):
+    """Host-array form of d/s/z/ctgsen: the eigenvalues flagged in select move to the leading
+    rows (Q, Z None: not updated).  Returns (A, B, eigenvalue arrays..., Q, Z, m, info) as new
+    arrays, the eigenvalue arrays (alphar, alphai, beta) or (alpha, beta); with ijob 1, 2 or 4
+    (real pencils) PL, PR and DIF (2 values) come before info: (..., m, pl, pr, dif, info)."""
     L = lib()
     dt = A.dtype.type
     pfx = {np.complex128: "z", np.complex64: "c", np.float64: "d", np.float32: "s"}[dt]
@@ -562,17 +570,23 @@ def tgsen(select, A, B, Q=None, Z=None):
     sel = np.ascontiguousarray(select, dtype=np.int32)
     ev = [np.zeros(max(n, 1), dtype=dt) for _ in range(2 if pfx in "zc" else 3)]
     m, info = ct.c_int(0), ct.c_int(0)
+    rdt = np.float32 if pfx in "sc" else np.float64
+    est = np.zeros(4, dtype=rdt)  # PL, PR, DIF(1), DIF(2)
     ld = max(n, 1)
-    getattr(L, f"xtgevc3_{pfx}tgsen")(0, int(q is not None), int(z is not None), _ptr(sel), n, _ptr(a), ld, _ptr(b), ld,
-                                      *[_ptr(e) for e in ev], _ptr(q), ld, _ptr(z), ld, ct.byref(m), ct.byref(info))
+    getattr(L, f"xtgevc3_{pfx}tgsen")(ijob, int(q is not None), int(z is not None), _ptr(sel), n, _ptr(a), ld, _ptr(b),
+                                      ld, *[_ptr(e) for e in ev], _ptr(q), ld, _ptr(z), ld, ct.byref(m),
+                                      _ptr(est[0:1]), _ptr(est[1:2]), _ptr(est[2:4]), ct.byref(info))
     if info.value == n + 1 and n > 0:
         raise RuntimeError(f"xtgevc3_{pfx}tgsen failed: {last_error()}")
-    return (a, b, *[e[:n] for e in ev], q, z, m.value, info.value)
+    out = (a, b, *[e[:n] for e in ev], q, z, m.value)
+    if ijob == 0:
+        return (*out, info.value)
+    return (*out, float(est[0]), float(est[1]), est[2:4].copy(), info.value)
 
 
-def tgsen_dev(select, A, B, Q=None, Z=None, stream=None):
-    """Device form of d/s/z/ctgsen with IJOB = 0 on column-major CUDA tensors (in place; select
-    a host array).  Returns (eigenvalue tensors..., m, info)."""
+def tgsen_dev(select, A, B, Q=None, Z=None, stream=None, ijob=0):
+    """Device form of d/s/z/ctgsen on column-major CUDA tensors (in place; select a host array).
+    Returns (eigenvalue tensors..., m, info); with ijob 1, 2 or 4 (..., m, pl, pr, dif, info)."""
     import torch
     L = lib()
     pfx = {torch.complex128: "z", torch.complex64: "c", torch.float64: "d", torch.float32: "s"}[A.dtype]
@@ -588,12 +602,36 @@ def tgsen_dev(select, A, B, Q=None, Z=None, stream=None):
     def ptr(t):
         return ct.c_void_p(t.data_ptr()) if t is not None else None
 
-    rc = getattr(L, f"xtgevc3_{pfx}tgsen_dev")(st, 0, int(Q is not None), int(Z is not None), _ptr(sel), n, ptr(A),
+    est = np.zeros(4, dtype=np.float32 if pfx in "sc" else np.float64)
+    rc = getattr(L, f"xtgevc3_{pfx}tgsen_dev")(st, ijob, int(Q is not None), int(Z is not None), _ptr(sel), n, ptr(A),
                                               ld(A), ptr(B), ld(B), *[ptr(e) for e in ev], ptr(Q), ld(Q), ptr(Z),
-                                              ld(Z), ct.byref(m), ct.byref(info))
+                                              ld(Z), ct.byref(m), _ptr(est[0:1]), _ptr(est[1:2]), _ptr(est[2:4]),
+                                              ct.byref(info))
     if rc:
         raise RuntimeError(f"xtgevc3_{pfx}tgsen_dev failed: {last_error()}")
-    return (*[e[:n] for e in ev], m.value, info.value)
+    out = (*[e[:n] for e in ev], m.value)
+    if ijob == 0:
+        return (*out, info.value)
+    return (*out, float(est[0]), float(est[1]), est[2:4].copy(), info.value)
+
+
+def tgsyl(ijob, A, B, C, D, E, F):
+    """Host-array form of d/stgsyl with TRANS = 'N': A R - L B = scale C, D R - L E = scale F.
+    Returns (R, L, scale, dif, info) (new arrays; dif meaningful for ijob 1 and 3)."""
+    L = lib()
+    dt = A.dtype.type
+    pfx = {np.float64: "d", np.float32: "s"}[dt]
+    m, n = C.shape
+    A, B, D, E = (np.array(M, order="F", dtype=dt) for M in (A, B, D, E))
+    Rm, Lm = np.array(C, order="F", dtype=dt), np.array(F, order="F", dtype=dt)
+    sd = np.zeros(2, dtype=dt)
+    info = ct.c_int(0)
+    lm, ln = max(m, 1), max(n, 1)
+    getattr(L, f"xtgevc3_{pfx}tgsyl")(b"N", ijob, m, n, _ptr(A), lm, _ptr(B), ln, _ptr(Rm), lm, _ptr(D), lm, _ptr(E), ln,
+                                      _ptr(Lm), lm, _ptr(sd[0:1]), _ptr(sd[1:2]), ct.byref(info))
+    if info.value == m + n + 1:
+        raise RuntimeError(f"xtgevc3_{pfx}tgsyl failed: {last_error()}")
+    return Rm, Lm, float(sd[0]), float(sd[1]), info.value
 
 
 def tgexc(A, B, Q=None, Z=None, ifst=1, ilst=1, with_ifst=False):

@@ -45,28 +45,44 @@ __global__ void __launch_bounds__(kQzThreads, 1) dgges_kernel(rb::QzPencilR<R> p
 
 // The reordering kernels: rb::tgsen_real_cta / rb::tgsen_cplx_cta on one CTA; info: 0, 1 (a
 // swap was rejected) or 3 (a walk reached its bound)
-// m (optional): DTGSEN's M of the input pencil, the selected eigenvalues counted with a
-// 2x2 block counting 2 when either of its rows is selected (thread 0 reads the subdiagonal
-// before its first barrier, so before any swap writes it)
 template <class R>
 __global__ void __launch_bounds__(kQzThreads, 1)
-    tgsen_real_kernel(rb::Pencil<R> p, const int *select, R *alphar, R *alphai, R *beta, int *info, int *m = nullptr)
+    tgsen_real_kernel(rb::Pencil<R> p, const int *select, R *alphar, R *alphai, R *beta, int *info)
 {
     __shared__ rb::WalkShared<R> sh;
-    if (m && threadIdx.x == 0) {
-        int cnt = 0;
-        for (int k = 0; k < p.n; k++) {
-            if (k + 1 < p.n && p.A[(size_t)(k + 1) + (size_t)k * p.lda] != R(0)) {
-                cnt += (select[k] != 0 || select[k + 1] != 0) ? 2 : 0;
-                k++;
-            } else {
-                cnt += select[k] != 0 ? 1 : 0;
-            }
-        }
-        *m = cnt;
-    }
     const int i = rb::tgsen_real_cta(rb::CtaDev{}, sh, p, select, alphar, alphai, beta);
     if (threadIdx.x == 0) *info = i;
+}
+
+// DTGSEN with IJOB 0, 1, 2, 4 (rb::tgsen_real_full_cta): status = {INFO, M}; est = PL, PR,
+// DIF(1), DIF(2); work 2 M (n - M) elements, cuts n / 2 + 4 ints
+template <class R>
+__global__ void __launch_bounds__(kQzThreads, 1)
+    tgsen_real_full_kernel(rb::Pencil<R> p, const int *select, int ijob, R *alphar, R *alphai, R *beta, R *work,
+                           int *cuts, R *est, int *status)
+{
+    __shared__ rb::WalkShared<R> shw;
+    __shared__ rb::SylvShared<R> shs;
+    const int i =
+        rb::tgsen_real_full_cta(rb::CtaDev{}, shw, shs, p, select, ijob, alphar, alphai, beta, work, cuts, est, status + 1);
+    if (threadIdx.x == 0) status[0] = i;
+}
+
+// xTGSYL (TRANS = 'N', IJOB 0, 1, 3; rb::tgsyl_cta): status = {INFO}, out = {SCALE, DIF}
+template <class R>
+__global__ void __launch_bounds__(kQzThreads, 1)
+    tgsyl_kernel(rb::SylvG<R> y, int ijob, int *cuts, R *work, R *out, int *status)
+{
+    __shared__ rb::SylvShared<R> sh;
+    if (threadIdx.x == 0) sh.y = y;
+    __syncthreads();
+    R dif = out[1];
+    rb::tgsyl_cta(rb::CtaDev{}, sh, ijob, cuts, work, &dif);
+    if (threadIdx.x == 0) {
+        status[0] = sh.info;
+        out[0] = sh.scale;
+        out[1] = dif;
+    }
 }
 
 template <class R>
@@ -405,29 +421,35 @@ void gges_host(char jobvsl, char jobvsr, char sort, SelCplx<R> sel, int n, rb::z
     }
 }
 
-// LAPACK xTGSEN with IJOB = 0 (reordering only; the condition estimates of IJOB 1-5 are not
-// built and are refused with INFO = -1), device pointers, SELECT on the host.  INFO as LAPACK
-// numbers its arguments (-1 IJOB, -5 N, -7 LDA, -9 LDB, -14 / -13 LDQ, -16 / -15 LDZ for real /
-// complex pencils), 1 when a swap was rejected.  Returns 0, or 1 when a CUDA call failed.
-// xTGSEN's argument checks; sets last_error for a bad one
+// xTGSEN's argument checks (IJOB 0 for complex pencils; 0, 1, 2, 4 for real ones: the 1-norm
+// estimates of IJOB 3 and 5 are not built, INFO = -1); sets last_error for a bad one
 int tgsen_check(int ijob, int wantq, int wantz, int n, int lda, int ldb, int ldq, int ldz, bool cplx)
 {
     int info = 0;
-    if (ijob != 0) info = -1;
+    const bool built = cplx ? ijob == 0 : (ijob == 0 || ijob == 1 || ijob == 2 || ijob == 4);
+    if (!built) info = -1;
     else if (n < 0) info = -5;
     else if (lda < std::max(1, n)) info = -7;
     else if (ldb < std::max(1, n)) info = -9;
     else if (ldq < 1 || (wantq && ldq < n)) info = cplx ? -13 : -14;
     else if (ldz < 1 || (wantz && ldz < n)) info = cplx ? -15 : -16;
-    if (info)
-        set_last_error(ijob != 0 ? "xTGSEN: only IJOB = 0 (reordering without condition estimates) is built"
-                                 : "xTGSEN: argument " + std::to_string(-info) + " has an illegal value");
+    if (info == -1)
+        set_last_error(ijob < 0 || ijob > 5 ? "xTGSEN: argument 1 has an illegal value"
+                       : cplx               ? "xTGSEN: complex pencils: only IJOB = 0 is built"
+                                            : "xTGSEN: IJOB 3 and 5 (1-norm estimates) are not built");
+    else if (info)
+        set_last_error("xTGSEN: argument " + std::to_string(-info) + " has an illegal value");
     return info;
 }
 
+// LAPACK xTGSEN, device pointers, SELECT on the host: the reordering, the eigenvalues, M and
+// (real pencils, IJOB 1, 2, 4) PL, PR, DIF(1:2) (pl, pr, dif may be null).  INFO as LAPACK
+// numbers its arguments (-1 IJOB, -5 N, -7 LDA, -9 LDB, -14 / -13 LDQ, -16 / -15 LDZ for real /
+// complex pencils), 1 when a swap was rejected.  Returns 0, or 1 when a CUDA call failed.
 template <class R, bool CPLX>
 int tgsen_device(cudaStream_t st, int ijob, int wantq, int wantz, const int *select, int n, R *A, int lda, R *B,
-                 int ldb, R *ev0, R *ev1, R *ev2, R *Q, int ldq, R *Z, int ldz, int *m, int *info)
+                 int ldb, R *ev0, R *ev1, R *ev2, R *Q, int ldq, R *Z, int ldz, int *m, R *pl, R *pr, R *dif,
+                 int *info)
 {
     set_last_error("");
     *info = tgsen_check(ijob, wantq, wantz, n, lda, ldb, ldq, ldz, CPLX);
@@ -436,9 +458,32 @@ int tgsen_device(cudaStream_t st, int ijob, int wantq, int wantz, const int *sel
     if (n == 0) return 0;
     std::vector<int> bw(n);
     for (int i = 0; i < n; i++) bw[i] = select[i] != 0 ? 1 : 0;
-    int *d = nullptr;  // n flags, the status, M
     int h[2] = {0, 0};
-    cudaError_t e = cudaMallocAsync(&d, (n + 2) * sizeof(int), st);
+    R est[4] = {R(0), R(0), R(0), R(0)};
+    size_t nwork = 0;  // real IJOB >= 1: 2 M (n - M) for xTGSYL's right-hand sides
+    cudaError_t e = cudaSuccess;
+    if (!CPLX && ijob != 0) {  // M from the subdiagonal (DTGSEN's count), to size the workspace
+        std::vector<R> sub(n > 1 ? n - 1 : 1);
+        if (n > 1)
+            e = cudaMemcpy2DAsync(sub.data(), sizeof(R), A + 1, (size_t)(lda + 1) * sizeof(R), sizeof(R), n - 1,
+                                  cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        int mm = 0;
+        for (int k = 0; k < n; k++) {
+            if (k + 1 < n && sub[k] != R(0)) {
+                mm += (bw[k] || bw[k + 1]) ? 2 : 0;
+                k++;
+            } else {
+                mm += bw[k];
+            }
+        }
+        nwork = 2 * (size_t)mm * (n - mm);
+    }
+    const int ncuts = n / 2 + 4;
+    int *d = nullptr;  // n flags, the status (INFO, M), the cuts
+    R *w = nullptr;    // PL, PR, DIF(1), DIF(2), then the workspace
+    if (e == cudaSuccess) e = cudaMallocAsync(&d, (n + 2 + ncuts) * sizeof(int), st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&w, (4 + nwork) * sizeof(R), st);
     if (e == cudaSuccess) {
         e = cudaMemcpyAsync(d, bw.data(), n * sizeof(int), cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess) {
@@ -454,15 +499,18 @@ int tgsen_device(cudaStream_t st, int ijob, int wantq, int wantz, const int *sel
             } else {
                 const rb::Pencil<R> p{n, wantq, wantz, A, B, wantq ? Q : A, wantz ? Z : A, lda, ldb,
                                       wantq ? ldq : lda, wantz ? ldz : lda};
-                tgsen_real_kernel<R><<<1, kQzThreads, 0, st>>>(p, d, ev0, ev1, ev2, d + n, d + n + 1);
+                tgsen_real_full_kernel<R><<<1, kQzThreads, 0, st>>>(p, d, ijob, ev0, ev1, ev2, w + 4, d + n + 2, w,
+                                                                     d + n);
             }
             count_launches(1);
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) e = cudaMemcpyAsync(h, d + n, (CPLX ? 1 : 2) * sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(est, w, 4 * sizeof(R), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        cudaFreeAsync(d, st);
     }
+    if (d) cudaFreeAsync(d, st);
+    if (w) cudaFreeAsync(w, st);
     if (e != cudaSuccess) {
         set_last_error(std::string("xTGSEN: ") + cudaGetErrorString(e));
         return 1;
@@ -473,6 +521,14 @@ int tgsen_device(cudaStream_t st, int ijob, int wantq, int wantz, const int *sel
     }
     *info = h[0];
     if (m) *m = h[1];
+    if (ijob == 1 || ijob == 4) {
+        if (pl) *pl = est[0];
+        if (pr) *pr = est[1];
+    }
+    if ((ijob == 2 || ijob == 4) && dif) {
+        dif[0] = est[2];
+        dif[1] = est[3];
+    }
     return 0;
 }
 
@@ -480,7 +536,7 @@ int tgsen_device(cudaStream_t st, int ijob, int wantq, int wantz, const int *sel
 // eigenvalues.  INFO = n + 1 (not a LAPACK value) when a CUDA call failed.
 template <class R, bool CPLX>
 void tgsen_host(int ijob, int wantq, int wantz, const int *select, int n, R *A, int lda, R *B, int ldb, R *ev0,
-                R *ev1, R *ev2, R *Q, int ldq, R *Z, int ldz, int *m, int *info)
+                R *ev1, R *ev2, R *Q, int ldq, R *Z, int ldz, int *m, R *pl, R *pr, R *dif, int *info)
 {
     constexpr int w = CPLX ? 2 : 1;  // reals per element
     const int nev = CPLX ? 2 : 3;
@@ -506,8 +562,9 @@ void tgsen_host(int ijob, int wantq, int wantz, const int *select, int n, R *A, 
         if (x.d && e == cudaSuccess)
             e = cudaMemcpy2DAsync(x.d, row, x.h, (size_t)x.ld * w * sizeof(R), row, n, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
-        const int rc = tgsen_device<R, CPLX>(st, 0, wantq, wantz, select, n, dA, n, dB, n, dv, dv + (size_t)n * w,
-                                             dv + 2 * (size_t)n * w, dQ ? dQ : dA, n, dZ ? dZ : dA, n, m, info);
+        const int rc = tgsen_device<R, CPLX>(st, ijob, wantq, wantz, select, n, dA, n, dB, n, dv, dv + (size_t)n * w,
+                                             dv + 2 * (size_t)n * w, dQ ? dQ : dA, n, dZ ? dZ : dA, n, m, pl, pr, dif,
+                                             info);
         if (rc == 0) {
             for (const M2 &x : mats)
                 if (x.d && e == cudaSuccess)
@@ -530,6 +587,132 @@ void tgsen_host(int ijob, int wantq, int wantz, const int *select, int n, R *A, 
     if (e != cudaSuccess) {
         if (e != cudaErrorUnknown) set_last_error(std::string("xTGSEN staging: ") + cudaGetErrorString(e));
         *info = n + 1;
+    }
+}
+
+// LAPACK xTGSYL's argument checks (TRANS = 'N' with IJOB 0, 1, 3 built; TRANS = 'T' and the
+// DGECON-based IJOB 2, 4 are refused with INFO -1 / -2); sets last_error for a bad one
+int tgsyl_check(char trans, int ijob, int m, int n, int lda, int ldb, int ldc, int ldd, int lde, int ldf)
+{
+    int info = 0;
+    if (trans != 'N') info = -1;
+    else if (ijob != 0 && ijob != 1 && ijob != 3) info = -2;
+    else if (m <= 0) info = -3;
+    else if (n <= 0) info = -4;
+    else if (lda < std::max(1, m)) info = -6;
+    else if (ldb < std::max(1, n)) info = -8;
+    else if (ldc < std::max(1, m)) info = -10;
+    else if (ldd < std::max(1, m)) info = -12;
+    else if (lde < std::max(1, n)) info = -14;
+    else if (ldf < std::max(1, m)) info = -16;
+    if (info == -1 && trans == 'T')
+        set_last_error("xTGSYL: TRANS = 'T' is not built");
+    else if (info == -2 && (ijob == 2 || ijob == 4))
+        set_last_error("xTGSYL: IJOB 2 and 4 (DGECON-based estimates) are not built");
+    else if (info)
+        set_last_error("xTGSYL: argument " + std::to_string(-info) + " has an illegal value");
+    return info;
+}
+
+// xTGSYL, device pointers: C, F overwritten by R, L; *scale, *dif (IJOB 1, 3; left as given
+// when the estimate's accumulator stayed 0).  Returns 0, or 1 when a CUDA call failed.
+template <class R>
+int tgsyl_device(cudaStream_t st, char trans, int ijob, int m, int n, const R *A, int lda, const R *B, int ldb, R *C,
+                 int ldc, const R *D, int ldd, const R *E, int lde, R *F, int ldf, R *scale, R *dif, int *info)
+{
+    set_last_error("");
+    trans = (char)std::toupper((unsigned char)trans);
+    *info = tgsyl_check(trans, ijob, m, n, lda, ldb, ldc, ldd, lde, ldf);
+    if (*info) return 0;
+    const int ncuts = m / 2 + n / 2 + 4;
+    const size_t nwork = ijob == 1 ? 2 * (size_t)m * n : 0;
+    int *d = nullptr;  // the status, then the cuts
+    R *w = nullptr;    // SCALE, DIF, then the saved solution (IJOB 1)
+    R out[2] = {R(1), dif ? *dif : R(0)};
+    int h = 0;
+    cudaError_t e = cudaMallocAsync(&d, (1 + ncuts) * sizeof(int), st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&w, (2 + nwork) * sizeof(R), st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(w, out, 2 * sizeof(R), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        rb::SylvG<R> y{};
+        y.m = m;
+        y.n = n;
+        y.A = A;
+        y.D = D;
+        y.B = B;
+        y.E = E;
+        y.lda = lda;
+        y.ldd = ldd;
+        y.ldb = ldb;
+        y.lde = lde;
+        y.C = C;
+        y.F = F;
+        y.ldc = ldc;
+        y.ldf = ldf;
+        tgsyl_kernel<R><<<1, kQzThreads, 0, st>>>(y, ijob, d + 1, w + 2, w, d);
+        count_launches(1);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, w, 2 * sizeof(R), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (d) cudaFreeAsync(d, st);
+    if (w) cudaFreeAsync(w, st);
+    if (e != cudaSuccess) {
+        set_last_error(std::string("xTGSYL: ") + cudaGetErrorString(e));
+        return 1;
+    }
+    *info = h;
+    if (scale) *scale = out[0];
+    if (dif && ijob != 0) *dif = out[1];
+    return 0;
+}
+
+// Host pointers.  INFO = m + n + 1 (not a LAPACK value) when a CUDA call failed.
+template <class R>
+void tgsyl_host(char trans, int ijob, int m, int n, const R *A, int lda, const R *B, int ldb, R *C, int ldc,
+                const R *D, int ldd, const R *E, int lde, R *F, int ldf, R *scale, R *dif, int *info)
+{
+    set_last_error("");
+    *info = tgsyl_check((char)std::toupper((unsigned char)trans), ijob, m, n, lda, ldb, ldc, ldd, lde, ldf);
+    if (*info) return;
+    cudaStream_t st = nullptr;
+    R *buf = nullptr;
+    const size_t mm = (size_t)m * m, nn = (size_t)n * n, mn = (size_t)m * n;
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocAsync(&buf, (2 * mm + 2 * nn + 2 * mn) * sizeof(R), st);
+    R *dA = buf, *dD = buf + mm, *dB = buf + 2 * mm, *dE = dB + nn, *dC = dE + nn, *dF = dC + mn;
+    struct M2 {
+        const R *h;
+        R *d;
+        int ld, rows, cols;
+    } ins[6] = {{A, dA, lda, m, m}, {D, dD, ldd, m, m}, {B, dB, ldb, n, n},
+                {E, dE, lde, n, n}, {C, dC, ldc, m, n}, {F, dF, ldf, m, n}};
+    for (const M2 &x : ins)
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(x.d, x.rows * sizeof(R), x.h, (size_t)x.ld * sizeof(R), x.rows * sizeof(R), x.cols,
+                                  cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        const int rc = tgsyl_device<R>(st, trans, ijob, m, n, dA, m, dB, n, dC, m, dD, m, dE, n, dF, m, scale, dif, info);
+        if (rc == 0) {
+            e = cudaMemcpy2DAsync(C, (size_t)ldc * sizeof(R), dC, m * sizeof(R), m * sizeof(R), n, cudaMemcpyDeviceToHost,
+                                  st);
+            if (e == cudaSuccess)
+                e = cudaMemcpy2DAsync(F, (size_t)ldf * sizeof(R), dF, m * sizeof(R), m * sizeof(R), n,
+                                      cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        } else {
+            e = cudaErrorUnknown;
+        }
+    }
+    if (buf) cudaFreeAsync(buf, st);
+    if (st) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
+    if (e != cudaSuccess) {
+        if (e != cudaErrorUnknown) set_last_error(std::string("xTGSYL staging: ") + cudaGetErrorString(e));
+        *info = m + n + 1;
     }
 }
 
@@ -675,69 +858,102 @@ int xtgevc3_sgges_sort_dev(void *stream, char jobvsl, char jobvsr, char sort, xt
 
 }  // extern "C"
 
-// ---- xTGSEN with IJOB = 0 -------------------------------------------------------------------
+// ---- xTGSEN (IJOB 0; real pencils also 1, 2, 4) and xTGSYL (TRANS = 'N', IJOB 0, 1, 3) ------
 
 extern "C" {
 
 void xtgevc3_dtgsen(int ijob, int wantq, int wantz, const int *select, int n, double *A, int lda, double *B, int ldb,
                     double *alphar, double *alphai, double *beta, double *Q, int ldq, double *Z, int ldz, int *m,
-                    int *info)
+                    double *pl, double *pr, double *dif, int *info)
 {
     xtg::tgsen_host<double, false>(ijob, wantq, wantz, select, n, A, lda, B, ldb, alphar, alphai, beta, Q, ldq, Z, ldz,
-                                   m, info);
+                                   m, pl, pr, dif, info);
 }
 
 void xtgevc3_stgsen(int ijob, int wantq, int wantz, const int *select, int n, float *A, int lda, float *B, int ldb,
-                    float *alphar, float *alphai, float *beta, float *Q, int ldq, float *Z, int ldz, int *m, int *info)
+                    float *alphar, float *alphai, float *beta, float *Q, int ldq, float *Z, int ldz, int *m, float *pl,
+                    float *pr, float *dif, int *info)
 {
     xtg::tgsen_host<float, false>(ijob, wantq, wantz, select, n, A, lda, B, ldb, alphar, alphai, beta, Q, ldq, Z, ldz,
-                                  m, info);
+                                  m, pl, pr, dif, info);
 }
 
 void xtgevc3_ztgsen(int ijob, int wantq, int wantz, const int *select, int n, double *A, int lda, double *B, int ldb,
-                    double *alpha, double *beta, double *Q, int ldq, double *Z, int ldz, int *m, int *info)
+                    double *alpha, double *beta, double *Q, int ldq, double *Z, int ldz, int *m, double *pl,
+                    double *pr, double *dif, int *info)
 {
     xtg::tgsen_host<double, true>(ijob, wantq, wantz, select, n, A, lda, B, ldb, alpha, beta, nullptr, Q, ldq, Z, ldz,
-                                  m, info);
+                                  m, pl, pr, dif, info);
 }
 
 void xtgevc3_ctgsen(int ijob, int wantq, int wantz, const int *select, int n, float *A, int lda, float *B, int ldb,
-                    float *alpha, float *beta, float *Q, int ldq, float *Z, int ldz, int *m, int *info)
+                    float *alpha, float *beta, float *Q, int ldq, float *Z, int ldz, int *m, float *pl, float *pr,
+                    float *dif, int *info)
 {
     xtg::tgsen_host<float, true>(ijob, wantq, wantz, select, n, A, lda, B, ldb, alpha, beta, nullptr, Q, ldq, Z, ldz, m,
-                                 info);
+                                 pl, pr, dif, info);
 }
 
 int xtgevc3_dtgsen_dev(void *stream, int ijob, int wantq, int wantz, const int *select, int n, double *A, int lda,
                        double *B, int ldb, double *alphar, double *alphai, double *beta, double *Q, int ldq, double *Z,
-                       int ldz, int *m, int *info)
+                       int ldz, int *m, double *pl, double *pr, double *dif, int *info)
 {
     return xtg::tgsen_device<double, false>(static_cast<cudaStream_t>(stream), ijob, wantq, wantz, select, n, A, lda, B,
-                                            ldb, alphar, alphai, beta, Q, ldq, Z, ldz, m, info);
+                                            ldb, alphar, alphai, beta, Q, ldq, Z, ldz, m, pl, pr, dif, info);
 }
 
 int xtgevc3_stgsen_dev(void *stream, int ijob, int wantq, int wantz, const int *select, int n, float *A, int lda,
                        float *B, int ldb, float *alphar, float *alphai, float *beta, float *Q, int ldq, float *Z,
-                       int ldz, int *m, int *info)
+                       int ldz, int *m, float *pl, float *pr, float *dif, int *info)
 {
     return xtg::tgsen_device<float, false>(static_cast<cudaStream_t>(stream), ijob, wantq, wantz, select, n, A, lda, B,
-                                           ldb, alphar, alphai, beta, Q, ldq, Z, ldz, m, info);
+                                           ldb, alphar, alphai, beta, Q, ldq, Z, ldz, m, pl, pr, dif, info);
 }
 
 int xtgevc3_ztgsen_dev(void *stream, int ijob, int wantq, int wantz, const int *select, int n, double *A, int lda,
                        double *B, int ldb, double *alpha, double *beta, double *Q, int ldq, double *Z, int ldz, int *m,
-                       int *info)
+                       double *pl, double *pr, double *dif, int *info)
 {
     return xtg::tgsen_device<double, true>(static_cast<cudaStream_t>(stream), ijob, wantq, wantz, select, n, A, lda, B,
-                                           ldb, alpha, beta, nullptr, Q, ldq, Z, ldz, m, info);
+                                           ldb, alpha, beta, nullptr, Q, ldq, Z, ldz, m, pl, pr, dif, info);
 }
 
 int xtgevc3_ctgsen_dev(void *stream, int ijob, int wantq, int wantz, const int *select, int n, float *A, int lda,
                        float *B, int ldb, float *alpha, float *beta, float *Q, int ldq, float *Z, int ldz, int *m,
-                       int *info)
+                       float *pl, float *pr, float *dif, int *info)
 {
     return xtg::tgsen_device<float, true>(static_cast<cudaStream_t>(stream), ijob, wantq, wantz, select, n, A, lda, B,
-                                          ldb, alpha, beta, nullptr, Q, ldq, Z, ldz, m, info);
+                                          ldb, alpha, beta, nullptr, Q, ldq, Z, ldz, m, pl, pr, dif, info);
+}
+
+void xtgevc3_dtgsyl(char trans, int ijob, int m, int n, const double *A, int lda, const double *B, int ldb, double *C,
+                    int ldc, const double *D, int ldd, const double *E, int lde, double *F, int ldf, double *scale,
+                    double *dif, int *info)
+{
+    xtg::tgsyl_host<double>(trans, ijob, m, n, A, lda, B, ldb, C, ldc, D, ldd, E, lde, F, ldf, scale, dif, info);
+}
+
+void xtgevc3_stgsyl(char trans, int ijob, int m, int n, const float *A, int lda, const float *B, int ldb, float *C,
+                    int ldc, const float *D, int ldd, const float *E, int lde, float *F, int ldf, float *scale,
+                    float *dif, int *info)
+{
+    xtg::tgsyl_host<float>(trans, ijob, m, n, A, lda, B, ldb, C, ldc, D, ldd, E, lde, F, ldf, scale, dif, info);
+}
+
+int xtgevc3_dtgsyl_dev(void *stream, char trans, int ijob, int m, int n, const double *A, int lda, const double *B,
+                       int ldb, double *C, int ldc, const double *D, int ldd, const double *E, int lde, double *F,
+                       int ldf, double *scale, double *dif, int *info)
+{
+    return xtg::tgsyl_device<double>(static_cast<cudaStream_t>(stream), trans, ijob, m, n, A, lda, B, ldb, C, ldc, D,
+                                     ldd, E, lde, F, ldf, scale, dif, info);
+}
+
+int xtgevc3_stgsyl_dev(void *stream, char trans, int ijob, int m, int n, const float *A, int lda, const float *B,
+                       int ldb, float *C, int ldc, const float *D, int ldd, const float *E, int lde, float *F, int ldf,
+                       float *scale, float *dif, int *info)
+{
+    return xtg::tgsyl_device<float>(static_cast<cudaStream_t>(stream), trans, ijob, m, n, A, lda, B, ldb, C, ldc, D,
+                                    ldd, E, lde, F, ldf, scale, dif, info);
 }
 
 }  // extern "C"

@@ -30,23 +30,20 @@
 #pragma once
 
 #include "tgsna_dif_cplx.cuh"
+#include "tgsyl.cuh"
 
 namespace xtg {
 namespace rb {
 
 // ---- real pencils: DTGSEN with IJOB = 0 -----------------------------------------------------
 
-// Returns INFO: 0, 1 (a swap was rejected; the eigenvalues are still recomputed) or 3 (a walk
-// reached its bound, which the walk's own argument rules out).  Every thread returns the same
-// value, after a barrier.  alphar, alphai, beta: n each.
+// The moves: returns INFO, 0, 1 (a swap was rejected) or 3 (a walk reached its bound, which
+// the walk's own argument rules out).  Every thread returns the same value, after a barrier.
 template <class R, class Cta>
-XTG_HD int tgsen_real_cta(const Cta &c, WalkShared<R> &sh, const Pencil<R> &p, const int *select, R *alphar,
-                          R *alphai, R *beta)
+XTG_HD int tgsen_real_reorder(const Cta &c, WalkShared<R> &sh, const Pencil<R> &p, const int *select)
 {
-    const int n = p.n, tid = c.tid(), nth = c.nth();
+    const int n = p.n;
     auto A = [&](int i, int j) -> R & { return p.A[(size_t)i + (size_t)j * p.lda]; };
-    auto B = [&](int i, int j) -> R & { return p.B[(size_t)i + (size_t)j * p.ldb]; };
-    auto Q = [&](int i, int j) -> R & { return p.Q[(size_t)i + (size_t)j * p.ldq]; };
     int info = 0, ks = 0;  // ks: the next free leading row (0-based)
     for (int k = 0; k < n; k++) {
         const bool pair = k + 1 < n && A(k + 1, k) != R(0);
@@ -65,6 +62,34 @@ XTG_HD int tgsen_real_cta(const Cta &c, WalkShared<R> &sh, const Pencil<R> &p, c
         if (pair) k++;
     }
     c.sync();  // the last swap is in memory
+    return info;
+}
+
+// DTGSEN's M: the selected eigenvalues, a 2x2 block counting 2 when either of its rows is
+template <class R>
+XTG_HD int tgsen_real_m(const Pencil<R> &p, const int *select)
+{
+    int m = 0;
+    for (int k = 0; k < p.n; k++) {
+        if (k + 1 < p.n && p.A[(size_t)(k + 1) + (size_t)k * p.lda] != R(0)) {
+            m += (select[k] != 0 || select[k + 1] != 0) ? 2 : 0;
+            k++;
+        } else {
+            m += select[k] != 0 ? 1 : 0;
+        }
+    }
+    return m;
+}
+
+// The eigenvalues of the (reordered) pencil, 1x1 blocks made non-negative in B.  Ends with a
+// barrier.
+template <class R, class Cta>
+XTG_HD void tgsen_real_finish(const Cta &c, const Pencil<R> &p, R *alphar, R *alphai, R *beta)
+{
+    const int n = p.n, tid = c.tid(), nth = c.nth();
+    auto A = [&](int i, int j) -> R & { return p.A[(size_t)i + (size_t)j * p.lda]; };
+    auto B = [&](int i, int j) -> R & { return p.B[(size_t)i + (size_t)j * p.ldb]; };
+    auto Q = [&](int i, int j) -> R & { return p.Q[(size_t)i + (size_t)j * p.ldq]; };
     // pass 1: block kind of each row (0: 1x1, 1: first row of a 2x2 block, 2: its second row)
     // into alphai, B(k, k) into beta, by the same top-down scan as the reordering's
     for (int k = 0; k < n; k++) {
@@ -123,6 +148,119 @@ XTG_HD int tgsen_real_cta(const Cta &c, WalkShared<R> &sh, const Pencil<R> &p, c
         }
     }
     c.sync();
+}
+
+// DTGSEN with IJOB = 0: returns INFO as tgsen_real_reorder (the eigenvalues recomputed in
+// every case).  alphar, alphai, beta: n each.
+template <class R, class Cta>
+XTG_HD int tgsen_real_cta(const Cta &c, WalkShared<R> &sh, const Pencil<R> &p, const int *select, R *alphar,
+                          R *alphai, R *beta)
+{
+    const int info = tgsen_real_reorder(c, sh, p, select);
+    tgsen_real_finish(c, p, alphar, alphai, beta);
+    return info;
+}
+
+// DTGSEN's estimates on the reordered pencil (IJOB 1, 2, 4; m = M, info the reordering's):
+// est[0], est[1] = PL, PR (IJOB 1 and 4: 1 / sqrt(1 + ||R||^2 / scale^2) and the same with L,
+// from xTGSYL's solution of A11 R - L A22 = A12, B11 R - L B22 = B12), est[2], est[3] = DIF(1),
+// DIF(2) (IJOB 2 and 4: xTGSYL's Frobenius-norm estimates, IJOB = 3, of Difu on (A11, B11),
+// (A22, B22) and of Difl with the two swapped).  M = 0 or n: PL = PR = 1, DIF = ||(A, B)||_F;
+// a rejected swap: all 0.  work: 2 M (n - M) elements; cuts: n / 2 + 4 ints.  Ends with a
+// barrier.
+template <class R, class Cta>
+XTG_HD void tgsen_real_estimates(const Cta &c, SylvShared<R> &sh, const Pencil<R> &p, int m, int ijob, int info,
+                                 R *work, int *cuts, R *est)
+{
+    const int n = p.n, tid = c.tid(), nth = c.nth();
+    const bool wantp = ijob == 1 || ijob == 4, wantd = ijob == 2 || ijob == 4;
+    if (tid == 0)
+        for (int k = 0; k < 4; k++) est[k] = R(0);
+    if (info != 0 || (!wantp && !wantd)) {
+        c.sync();
+        return;
+    }
+    if (m == 0 || m == n) {
+        if (tid == 0) {
+            if (wantp) est[0] = est[1] = R(1);
+            if (wantd) {
+                R sc = R(0), sq = R(1);
+                for (int j = 0; j < n; j++) {
+                    lassq(n, p.A + (size_t)j * p.lda, sc, sq);
+                    lassq(n, p.B + (size_t)j * p.ldb, sc, sq);
+                }
+                est[2] = est[3] = sc * xsqrt(sq);
+            }
+        }
+        c.sync();
+        return;
+    }
+    const int n1 = m, n2 = n - m;
+    const size_t mn = (size_t)n1 * n2;
+    R *W = work, *V = work + mn;
+    const R *A11 = p.A, *B11 = p.B;
+    const R *A22 = p.A + n1 + (size_t)n1 * p.lda, *B22 = p.B + n1 + (size_t)n1 * p.ldb;
+    // xTGSYL's operands: (a, d) the mm x mm pencil, (b, e) the nn x nn one; a, b in A (lda),
+    // d, e in B (ldb); C, F = W, V with leading dimension mm
+    auto setup = [&](int mm, int nn, const R *a, const R *d, const R *b, const R *e) {
+        if (tid == 0) {
+            SylvG<R> &y = sh.y;
+            y.m = mm;
+            y.n = nn;
+            y.A = a;
+            y.D = d;
+            y.B = b;
+            y.E = e;
+            y.lda = y.ldb = p.lda;
+            y.ldd = y.lde = p.ldb;
+            y.C = W;
+            y.F = V;
+            y.ldc = y.ldf = mm;
+        }
+        c.sync();
+    };
+    if (wantp) {
+        for (size_t t = tid; t < mn; t += nth) {  // C = A12, F = B12
+            const int i = (int)(t % n1), j = n1 + (int)(t / n1);
+            W[t] = p.A[(size_t)i + (size_t)j * p.lda];
+            V[t] = p.B[(size_t)i + (size_t)j * p.ldb];
+        }
+        setup(n1, n2, A11, B11, A22, B22);
+        R unused = R(0);
+        tgsyl_cta(c, sh, 0, cuts, (R *)nullptr, &unused);
+        if (tid == 0) {
+            const R dscale = sh.scale;
+            for (int k = 0; k < 2; k++) {
+                R sc = R(0), sq = R(1);
+                lassq((int)mn, k == 0 ? W : V, sc, sq);
+                R v = sc * xsqrt(sq);
+                v = v == R(0) ? R(1) : dscale / (xsqrt(dscale * dscale / v + v) * xsqrt(v));
+                est[k] = v;
+            }
+        }
+        c.sync();
+    }
+    if (wantd) {
+        setup(n1, n2, A11, B11, A22, B22);
+        tgsyl_cta(c, sh, 3, cuts, (R *)nullptr, est + 2);
+        setup(n2, n1, A22, B22, A11, B11);
+        tgsyl_cta(c, sh, 3, cuts, (R *)nullptr, est + 3);
+    }
+}
+
+// DTGSEN with IJOB 0, 1, 2 or 4 (tgsen_real_estimates): M (into *m_out from thread 0), the
+// moves, the estimates on the reordered pencil, the eigenvalues.  Returns INFO as
+// tgsen_real_reorder.  est: PL, PR, DIF(1), DIF(2).
+template <class R, class Cta>
+XTG_HD int tgsen_real_full_cta(const Cta &c, WalkShared<R> &shw, SylvShared<R> &shs, const Pencil<R> &p,
+                               const int *select, int ijob, R *alphar, R *alphai, R *beta, R *work, int *cuts, R *est,
+                               int *m_out)
+{
+    const int m = tgsen_real_m(p, select);  // reads the subdiagonal before the first swap's barrier
+    if (m_out && c.tid() == 0) *m_out = m;
+    const int info = tgsen_real_reorder(c, shw, p, select);
+    tgsen_real_estimates(c, shs, p, m, ijob, info, work, cuts, est);
+    tgsen_real_finish(c, p, alphar, alphai, beta);
     return info;
 }
 

@@ -1,0 +1,290 @@
+// The generalized Sylvester equation of a pair of real generalized Schur pencils (LAPACK
+// D/STGSYL with TRANS = 'N'):
+//     A R - L B = scale C,   D R - L E = scale F,
+// A, D m x m (A upper quasi-triangular, D upper triangular), B, E n x n (likewise), R and L
+// m x n, overwriting C and F.  IJOB 0 solves; IJOB 3 only estimates DIF (C, F start at zero and
+// every small system is solved by xLATDF's look-ahead, which accumulates a Frobenius-norm
+// estimate of the smallest singular value); IJOB 1 solves, then estimates as IJOB 3 and puts
+// the solution back.  Host and device code: the kernels in qz.cu run tgsyl_cta on one CTA; the
+// tests run it on host threads and on one thread.
+//
+// The solve follows xTGSYL's blocked order, because the estimate's accumulators (and the
+// rounding of the solution) depend on it: A's rows cut into blocks of ILAENV's 2 rows (one row
+// more where a cut would split a 2x2 block), B's columns into 2-column blocks likewise (m <= 2
+// and n <= 2: one block, xTGSYL's unblocked case); column blocks left to right, row blocks
+// bottom to top; each block solved by xTGSY2 (its 1x1 / 2x2 diagonal blocks, each a Kronecker
+// system of order 2, 4 or 8 by xGETC2 with complete pivoting, then xGESC2 with its own scale
+// factor or xLATDF), then the rows above it updated (C -= A R, F -= D R) and the columns right
+// of it (C += L B, F += L E).  A scale factor below 1 scales all of C and F.
+//
+// B200 form: thread 0 solves each block (dependent steps on at most 3 x 3 rows and columns);
+// between barriers the CTA applies the block's two updates (rows above and columns right are
+// disjoint) and any scaling.
+#pragma once
+
+#include "tgsna_dif.cuh"
+
+namespace xtg {
+namespace rb {
+
+template <class R>
+struct SylvG {
+    int m, n;
+    const R *A, *D, *B, *E;
+    int lda, ldd, ldb, lde;
+    R *C, *F;
+    int ldc, ldf;
+    R dsum, dscale;  // xLATDF's accumulators (IJOB 1 and 3)
+};
+
+// xTGSY2 on the block rows [is0, ie0] x columns [js0, je0] of C, F (0-based): the block's own
+// 1x1 / 2x2 diagonal blocks of A (bottom to top) and B (left to right), each solved and
+// substituted into the block's rows above and columns right.  ifunc 0: xGESC2 (scaloc < 1
+// scales the whole block and multiplies into scaloc); 1: xLATDF into y.dsum / y.dscale.
+// Returns xGETC2's INFO (> 0: a pivot was raised).
+template <class R>
+XTG_HD int tgsy2_sub(SylvG<R> &y, int is0, int ie0, int js0, int je0, int ifunc, R &scaloc)
+{
+    auto a = [&](int i, int k) { return y.A[(size_t)i + (size_t)k * y.lda]; };
+    auto d = [&](int i, int k) { return y.D[(size_t)i + (size_t)k * y.ldd]; };
+    auto b = [&](int i, int k) { return y.B[(size_t)i + (size_t)k * y.ldb]; };
+    auto e = [&](int i, int k) { return y.E[(size_t)i + (size_t)k * y.lde]; };
+    auto C = [&](int i, int k) -> R & { return y.C[(size_t)i + (size_t)k * y.ldc]; };
+    auto F = [&](int i, int k) -> R & { return y.F[(size_t)i + (size_t)k * y.ldf]; };
+    int ist[5], jst[5], np = 0, nq = 0;
+    for (int i = is0; i <= ie0;) {
+        ist[np++] = i;
+        i += (i < ie0 && a(i + 1, i) != R(0)) ? 2 : 1;
+    }
+    ist[np] = ie0 + 1;
+    for (int j = js0; j <= je0;) {
+        jst[nq++] = j;
+        j += (j < je0 && b(j + 1, j) != R(0)) ? 2 : 1;
+    }
+    jst[nq] = je0 + 1;
+    int info = 0;
+    for (int jb = 0; jb < nq; jb++) {
+        const int js = jst[jb], nb = jst[jb + 1] - js;
+        for (int ib = np - 1; ib >= 0; ib--) {
+            const int is = ist[ib], mb = ist[ib + 1] - is;
+            const int nn = mb * nb, zdim = 2 * nn;
+            R Z[64], rhs[8];
+            for (int t = 0; t < 64; t++) Z[t] = R(0);
+            for (int j = 0; j < nb; j++)
+                for (int i = 0; i < mb; i++) {
+                    const int k = i + mb * j;
+                    for (int p = 0; p < mb; p++) {
+                        Z[k + 8 * (p + mb * j)] = a(is + i, is + p);
+                        if (p >= i) Z[(nn + k) + 8 * (p + mb * j)] = d(is + i, is + p);
+                    }
+                    for (int q = 0; q < nb; q++) {
+                        Z[k + 8 * (nn + i + mb * q)] = -b(js + q, js + j);
+                        if (q <= j) Z[(nn + k) + 8 * (nn + i + mb * q)] = -e(js + q, js + j);
+                    }
+                    rhs[k] = C(is + i, js + j);
+                    rhs[nn + k] = F(is + i, js + j);
+                }
+            int ipiv[8], jpiv[8];
+            const int ierr = getc2(zdim, Z, ipiv, jpiv);
+            if (ierr > 0) info = ierr;
+            if (ifunc == 0) {
+                R sc = R(1);
+                gesc2(zdim, Z, rhs, ipiv, jpiv, sc);
+                if (sc != R(1)) {
+                    for (int k = js0; k <= je0; k++)
+                        for (int i = is0; i <= ie0; i++) {
+                            C(i, k) *= sc;
+                            F(i, k) *= sc;
+                        }
+                    scaloc *= sc;
+                }
+            } else {
+                latdf(zdim, Z, rhs, y.dsum, y.dscale, ipiv, jpiv);
+            }
+            for (int j = 0; j < nb; j++)
+                for (int i = 0; i < mb; i++) {
+                    C(is + i, js + j) = rhs[i + mb * j];
+                    F(is + i, js + j) = rhs[nn + i + mb * j];
+                }
+            // rows [is0, is) of the block: C -= A R, F -= D R
+            for (int r = is0; r < is; r++)
+                for (int j = 0; j < nb; j++) {
+                    R c = C(r, js + j), f = F(r, js + j);
+                    for (int p = 0; p < mb; p++) {
+                        const R rv = rhs[p + mb * j];
+                        c -= a(r, is + p) * rv;
+                        f -= d(r, is + p) * rv;
+                    }
+                    C(r, js + j) = c;
+                    F(r, js + j) = f;
+                }
+            // columns (js + nb, je0] of the block: C += L B, F += L E
+            for (int col = js + nb; col <= je0; col++)
+                for (int i = 0; i < mb; i++) {
+                    R c = C(is + i, col), f = F(is + i, col);
+                    for (int q = 0; q < nb; q++) {
+                        const R lv = rhs[nn + i + mb * q];
+                        c += lv * b(js + q, col);
+                        f += lv * e(js + q, col);
+                    }
+                    C(is + i, col) = c;
+                    F(is + i, col) = f;
+                }
+        }
+    }
+    return info;
+}
+
+// xTGSYL's block starts of an order-m quasi-triangular matrix T (2-row blocks, one row more
+// where a cut would split a 2x2 block); returns the count, starts[count] = m.  starts has
+// room for m / 2 + 2 entries.  m <= 2 and n <= 2 (the caller's test): one block.
+template <class R>
+XTG_HD int tgsyl_cuts(int m, const R *T, int ldt, int *starts)
+{
+    int p = 0, i = 1;  // 1-based as xTGSYL
+    while (i <= m) {
+        starts[p++] = i - 1;
+        i += 2;
+        if (i >= m) break;
+        if (T[(size_t)(i - 1) + (size_t)(i - 2) * ldt] != R(0)) i++;
+    }
+    starts[p] = m;
+    if (starts[p - 1] == starts[p]) p--;
+    return p;
+}
+
+// the CTA's shared state of tgsyl_cta (shared memory on the GPU)
+template <class R>
+struct SylvShared {
+    SylvG<R> y;
+    R scaloc, scale;
+    int info, np, nq;
+};
+
+// One round of xTGSYL over every block (ifunc 0: solve, 1: estimate) on one CTA.  rows /
+// cols: the block starts of A and B (tgsyl_cuts, or {0, m} / {0, n}).  Ends with a barrier.
+template <class R, class Cta>
+XTG_HD void tgsyl_round(const Cta &c, SylvShared<R> &sh, const int *rows, const int *cols, int ifunc)
+{
+    const int tid = c.tid(), nth = c.nth();
+    SylvG<R> &y = sh.y;
+    const int np = sh.np, nq = sh.nq, m = y.m, n = y.n;
+    for (int jb = 0; jb < nq; jb++) {
+        const int js = cols[jb], je = cols[jb + 1] - 1;
+        for (int ib = np - 1; ib >= 0; ib--) {
+            const int is = rows[ib], ie = rows[ib + 1] - 1;
+            if (tid == 0) {
+                R sl = R(1);
+                const int li = tgsy2_sub(y, is, ie, js, je, ifunc, sl);
+                if (li > 0) sh.info = li;
+                sh.scaloc = sl;
+            }
+            c.sync();  // the block's solution and scaloc are in memory
+            const R sl = sh.scaloc;
+            if (sl != R(1)) {  // every entry outside the block
+                for (size_t t = tid; t < (size_t)m * n; t += nth) {
+                    const int i = (int)(t % m), k = (int)(t / m);
+                    if (k >= js && k <= je && i >= is && i <= ie) continue;
+                    y.C[(size_t)i + (size_t)k * y.ldc] *= sl;
+                    y.F[(size_t)i + (size_t)k * y.ldf] *= sl;
+                }
+                if (tid == 0) sh.scale *= sl;
+                c.sync();  // scaled before the updates read and write the same entries
+            }
+            // rows above the block (C -= A R, F -= D R) and columns right of it (C += L B,
+            // F += L E): disjoint, one pass; R, L read from the block, which nobody writes
+            const int nbk = je - js + 1, mbk = ie - is + 1;
+            const size_t above = (size_t)is * nbk, right = (size_t)mbk * (n - 1 - je);
+            for (size_t t = tid; t < above + right; t += nth) {
+                if (t < above) {
+                    const int r = (int)(t % is), k = js + (int)(t / is);
+                    R cv = y.C[(size_t)r + (size_t)k * y.ldc], fv = y.F[(size_t)r + (size_t)k * y.ldf];
+                    for (int p = is; p <= ie; p++) {
+                        const R rv = y.C[(size_t)p + (size_t)k * y.ldc];
+                        cv -= y.A[(size_t)r + (size_t)p * y.lda] * rv;
+                        fv -= y.D[(size_t)r + (size_t)p * y.ldd] * rv;
+                    }
+                    y.C[(size_t)r + (size_t)k * y.ldc] = cv;
+                    y.F[(size_t)r + (size_t)k * y.ldf] = fv;
+                } else {
+                    const size_t u = t - above;
+                    const int i = is + (int)(u % mbk), k = je + 1 + (int)(u / mbk);
+                    R cv = y.C[(size_t)i + (size_t)k * y.ldc], fv = y.F[(size_t)i + (size_t)k * y.ldf];
+                    for (int q = js; q <= je; q++) {
+                        const R lv = y.F[(size_t)i + (size_t)q * y.ldf];
+                        cv += lv * y.B[(size_t)q + (size_t)k * y.ldb];
+                        fv += lv * y.E[(size_t)q + (size_t)k * y.lde];
+                    }
+                    y.C[(size_t)i + (size_t)k * y.ldc] = cv;
+                    y.F[(size_t)i + (size_t)k * y.ldf] = fv;
+                }
+            }
+            c.sync();  // the updates are in memory before the next block is solved
+        }
+    }
+}
+
+// xTGSYL (TRANS = 'N', IJOB 0, 1 or 3) on one CTA.  sh.y holds the operands on entry (m, n
+// >= 1); cuts: room for m / 2 + n / 2 + 4 ints; work (IJOB 1 only): 2 m n elements for the
+// saved solution.  On return (every thread, after a barrier): sh.scale, sh.info, and *dif for
+// IJOB 1 and 3 (left as it was when the estimate's accumulator stayed 0, as xTGSYL does).
+template <class R, class Cta>
+XTG_HD void tgsyl_cta(const Cta &c, SylvShared<R> &sh, int ijob, int *cuts, R *work, R *dif)
+{
+    const int tid = c.tid(), nth = c.nth();
+    SylvG<R> &y = sh.y;
+    const int m = y.m, n = y.n;
+    int *rows = cuts, *cols = cuts + m / 2 + 2;
+    if (tid == 0) {
+        if (m <= 2 && n <= 2) {
+            rows[0] = 0;
+            rows[1] = m;
+            cols[0] = 0;
+            cols[1] = n;
+            sh.np = sh.nq = 1;
+        } else {
+            sh.np = tgsyl_cuts(m, y.A, y.lda, rows);
+            sh.nq = tgsyl_cuts(n, y.B, y.ldb, cols);
+        }
+        sh.info = 0;
+        sh.scale = R(1);
+        y.dsum = R(1);
+        y.dscale = R(0);
+    }
+    if (ijob == 3)  // only the estimate: C, F start at zero
+        for (size_t t = tid; t < (size_t)m * n; t += nth) {
+            y.C[(t % m) + (t / m) * (size_t)y.ldc] = R(0);
+            y.F[(t % m) + (t / m) * (size_t)y.ldf] = R(0);
+        }
+    c.sync();
+    tgsyl_round(c, sh, rows, cols, ijob == 3 ? 1 : 0);
+    if (ijob == 1) {  // keep the solution, estimate from zero right-hand sides, put it back
+        const R scale1 = sh.scale;
+        for (size_t t = tid; t < (size_t)m * n; t += nth) {
+            R &cv = y.C[(t % m) + (t / m) * (size_t)y.ldc];
+            R &fv = y.F[(t % m) + (t / m) * (size_t)y.ldf];
+            work[t] = cv;
+            work[(size_t)m * n + t] = fv;
+            cv = R(0);
+            fv = R(0);
+        }
+        c.sync();
+        if (tid == 0) {
+            y.dsum = R(1);
+            y.dscale = R(0);
+            sh.scale = R(1);
+        }
+        c.sync();
+        tgsyl_round(c, sh, rows, cols, 1);
+        for (size_t t = tid; t < (size_t)m * n; t += nth) {
+            y.C[(t % m) + (t / m) * (size_t)y.ldc] = work[t];
+            y.F[(t % m) + (t / m) * (size_t)y.ldf] = work[(size_t)m * n + t];
+        }
+        if (tid == 0) sh.scale = scale1;
+    }
+    if (ijob != 0 && tid == 0 && y.dscale != R(0)) *dif = xsqrt(R(2 * m) * R(n)) / (y.dscale * xsqrt(y.dsum));
+    c.sync();
+}
+
+}  // namespace rb
+}  // namespace xtg
