@@ -154,6 +154,57 @@ int run_tgsen_full(int nth, int ijob, int n, R *A, R *B, R *Q, R *Z, const int *
     return info;
 }
 
+template <class R>
+int run_ztgsyl(int nth, int ijob, int m, int n, const R *A, const R *B, R *C, const R *D, const R *E, R *F, R *scale,
+               R *dif)
+{
+    using Cx = zc<R>;
+    ZSylvShared<R> sh{};
+    ZSylvG<R> &y = sh.y;
+    y.m = m;
+    y.n = n;
+    y.A = reinterpret_cast<const Cx *>(A);
+    y.D = reinterpret_cast<const Cx *>(D);
+    y.B = reinterpret_cast<const Cx *>(B);
+    y.E = reinterpret_cast<const Cx *>(E);
+    y.lda = y.ldd = y.ldc = y.ldf = m;
+    y.ldb = y.lde = n;
+    y.C = reinterpret_cast<Cx *>(C);
+    y.F = reinterpret_cast<Cx *>(F);
+    std::vector<int> cuts(m / 2 + n / 2 + 4);
+    std::vector<Cx> work(2 * (size_t)m * n);
+    std::barrier<> bar(nth);
+    std::vector<std::thread> th;
+    for (int t = 0; t < nth; t++)
+        th.emplace_back([&, t] { ztgsyl_cta(CtaHost{t, nth, &bar}, sh, ijob, cuts.data(), work.data(), dif); });
+    for (auto &x : th) x.join();
+    *scale = sh.scale;
+    return sh.info;
+}
+
+template <class R>
+int run_ztgsen_full(int nth, int ijob, int n, R *A, R *B, R *Q, R *Z, const int *sel, R *al, R *be, R *est, int *m)
+{
+    using Cx = zc<R>;
+    Cx *a = reinterpret_cast<Cx *>(A), *b = reinterpret_cast<Cx *>(B);
+    ZPencil<R> p{n, 1, 1, a, b, reinterpret_cast<Cx *>(Q), reinterpret_cast<Cx *>(Z), n, n, n, n};
+    ZSortShared<R> shs{};
+    ZSylvShared<R> shy{};
+    std::vector<Cx> work((size_t)n * n / 2 + 2);
+    std::vector<int> cuts(n / 2 + 4);
+    int info = 0;
+    std::barrier<> bar(nth);
+    std::vector<std::thread> th;
+    for (int t = 0; t < nth; t++)
+        th.emplace_back([&, t] {
+            const int i = tgsen_cplx_full_cta(CtaHost{t, nth, &bar}, shs, shy, p, sel, ijob, reinterpret_cast<Cx *>(al),
+                                              reinterpret_cast<Cx *>(be), work.data(), cuts.data(), est, m);
+            if (t == 0) info = i;
+        });
+    for (auto &x : th) x.join();
+    return info;
+}
+
 // SELCTG from flags: the test passes the selection that LAPACK's SELCTG made, one flag per
 // eigenvalue in order, and the check reads them back in the same order
 struct FlagSel {
@@ -219,6 +270,33 @@ int host_stgsyl(int nth, int ijob, int m, int n, const float *A, const float *B,
                 const float *E, float *F, float *scale, float *dif)
 {
     return run_tgsyl(nth, ijob, m, n, A, B, C, D, E, F, scale, dif);
+}
+
+// ZTGSEN (IJOB 0, 1, 2, 4) body with Q and Z (interleaved complex arrays); est = PL, PR,
+// DIF(1), DIF(2); returns INFO
+int host_ztgsen(int nth, int ijob, int n, double *A, double *B, double *Q, double *Z, const int *sel, double *al,
+                double *be, double *est, int *m)
+{
+    return run_ztgsen_full(nth, ijob, n, A, B, Q, Z, sel, al, be, est, m);
+}
+
+int host_ctgsen(int nth, int ijob, int n, float *A, float *B, float *Q, float *Z, const int *sel, float *al, float *be,
+                float *est, int *m)
+{
+    return run_ztgsen_full(nth, ijob, n, A, B, Q, Z, sel, al, be, est, m);
+}
+
+// Z/CTGSYL body (interleaved complex arrays)
+int host_ztgsyl(int nth, int ijob, int m, int n, const double *A, const double *B, double *C, const double *D,
+                const double *E, double *F, double *scale, double *dif)
+{
+    return run_ztgsyl(nth, ijob, m, n, A, B, C, D, E, F, scale, dif);
+}
+
+int host_ctgsyl(int nth, int ijob, int m, int n, const float *A, const float *B, float *C, const float *D,
+                const float *E, float *F, float *scale, float *dif)
+{
+    return run_ztgsyl(nth, ijob, m, n, A, B, C, D, E, F, scale, dif);
 }
 
 // xGGES's check: SELCTG's answers as flags in order; returns SDIM, *info as the check leaves it

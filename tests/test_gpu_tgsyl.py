@@ -1,10 +1,12 @@
-"""xtgevc3_d/stgsyl (TRANS = 'N', IJOB 0, 1, 3; one CTA) against LAPACK D/STGSYL, and
-xtgevc3_dtgsen's estimates (IJOB 1, 2, 4: PL, PR, DIF) against LAPACK DTGSEN, on the GPU.
+"""xtgevc3_d/s/z/ctgsyl (TRANS = 'N', IJOB 0, 1, 3; one CTA) against LAPACK xTGSYL, and
+xtgevc3_dtgsen / ztgsen's estimates (IJOB 1, 2, 4: PL, PR, DIF) against LAPACK xTGSEN, on the
+GPU.
 
 Inputs and tolerances as in tests/test_tgsyl_host.py, where the same kernel bodies run on host
 threads: R, L, SCALE and the DIF estimate of xTGSYL within 1e-11 (double) / 2e-3 (single) of
 LAPACK's; PL and PR within 1e-9; xTGSEN's DIF within a factor of 2 (it depends on the column
-signs that the real 2x2 swaps choose on rounding-level quantities, as LAPACK's do).
+signs that the real 2x2 swaps choose on rounding-level quantities, as LAPACK's do); complex
+PL, PR, DIF within 1e-10 of LAPACK's.
 """
 import numpy as np
 import pytest
@@ -12,7 +14,7 @@ import pytest
 import oracle
 import xtgevc3_b200 as X
 from test_tgsen_host import REAL_SELECTIONS, _real_schur
-from test_tgsyl_host import _schur
+from test_tgsyl_host import _schur, sylv_operands
 
 pytestmark = [pytest.mark.gpu, pytest.mark.late(5)]
 
@@ -80,3 +82,37 @@ def test_tgsen_estimates_device_form_matches_host_form(cuda_ok):
     for M, R in zip(dev, (h[0], h[1], h[5], h[6])):
         assert np.array_equal(M.cpu().numpy(), R)
     assert (d[3], d[4], d[5], d[7]) == (h[7], h[8], h[9], h[11]) and np.array_equal(d[6], h[10])
+
+
+@pytest.mark.parametrize("dt", [np.complex128, np.complex64], ids=["z", "c"])
+@pytest.mark.parametrize("mn", [(1, 1), (2, 2), (1, 5), (3, 4), (20, 13), (41, 17)], ids=lambda t: f"{t[0]}x{t[1]}")
+def test_complex_tgsyl_matches_lapack(cuda_ok, dt, mn):
+    m, n = mn
+    tol = 1e-11 if dt == np.complex128 else 2e-3
+    A, B, C, D, E, F = sylv_operands(m, n, 0, dt)
+    for ijob in (0, 1, 3):
+        rR, rL, rs, rd, ri = oracle.lapack_tgsyl("N", ijob, A, B, C, D, E, F)
+        hR, hL, hs, hd, hi = X.tgsyl(ijob, A, B, C, D, E, F)
+        assert (hi, hs) == (ri, rs), (ijob, hi, ri, hs, rs)
+        if ijob != 3:
+            for M, R in ((hR, rR), (hL, rL)):
+                assert np.abs(M - R).max() <= tol * max(np.abs(R).max(), 1.0), ijob
+        if ijob != 0:
+            assert abs(hd - rd) <= tol * abs(rd), (ijob, hd, rd)
+
+
+@pytest.mark.parametrize("kind", ["neg_real", "every_third", "none", "last"], ids=str)
+def test_complex_tgsen_estimates_match_lapack(cuda_ok, kind):
+    import scipy.linalg.lapack as la
+    from test_tgsen_host import CPLX_SELECTIONS, _cplx_schur
+    n = 30
+    S, T, Q, Z, al, be = _cplx_schur(n, 12, np.complex128)
+    sel = CPLX_SELECTIONS[kind](al, be).astype(np.int32)
+    r = la.ztgsen(sel, S, T, Q, Z, ijob=4, lwork=2 * n * n + 64, liwork=2 * n * n + 64)
+    h = X.tgsen(sel, S, T, Q, Z, ijob=4)
+    m, pl, pr, dif, info = h[-5:]
+    assert (m, info) == (r[6], r[10]) == (r[6], 0)
+    assert abs(pl - r[7]) <= 1e-10 * r[7] and abs(pr - r[8]) <= 1e-10 * r[8]
+    assert np.all(np.abs(dif - r[9]) <= 1e-10 * r[9]), (dif, r[9])
+    for M, R in ((h[0], r[0]), (h[1], r[1]), (h[4], r[4]), (h[5], r[5])):
+        assert np.abs(M - R).max() <= 1e-11 * max(np.abs(R).max(), 1.0)

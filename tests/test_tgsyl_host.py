@@ -1,6 +1,7 @@
-"""The generalized Sylvester solver (xtgevc3_b200/csrc/tgsyl.cuh: rb::tgsyl_cta, LAPACK
-D/STGSYL with TRANS = 'N') and xTGSEN's estimates on it (tgsen.cuh: rb::tgsen_real_estimates,
-IJOB 1, 2, 4) compiled for the CPU by tests/qz_host.cpp, against LAPACK.
+"""The generalized Sylvester solver (xtgevc3_b200/csrc/tgsyl.cuh: rb::tgsyl_cta and
+rb::ztgsyl_cta, LAPACK D/S/Z/CTGSYL with TRANS = 'N') and xTGSEN's estimates on it (tgsen.cuh:
+rb::tgsen_real_estimates, rb::tgsen_cplx_estimates, IJOB 1, 2, 4) compiled for the CPU by
+tests/qz_host.cpp, against LAPACK.
 
 The oracles are LAPACK's own DTGSYL (its Fortran interface in SciPy's OpenBLAS) and DTGSEN
 (SciPy's wrapper), on generalized Schur pencils from LAPACK DGGES of iid N(0,1) pencils.  The
@@ -9,7 +10,8 @@ to rounding (1e-12 double, 2e-4 single).  xTGSEN's PL and PR do not depend on th
 real 2x2 swaps leave on the reordered pencil's columns and agree to rounding too; its DIF
 estimates (xLATDF's look-ahead) do, and the reordering chooses those signs on rounding-level
 quantities as LAPACK does, so DIF is checked exactly on LAPACK's own reordered pencil and
-within a factor of 2 on ours.
+within a factor of 2 on ours.  Complex swaps have no such choice: ZTGSEN's PL, PR and DIF
+(estimated before the rows are normalised, as ZTGSEN does) agree with LAPACK's to rounding.
 """
 import ctypes as ct
 
@@ -32,9 +34,10 @@ def host_tgsyl(L, ijob, A, B, C, D, E, F, nth=1):
     dt = A.dtype.type
     m, n = C.shape
     Cw, Fw = np.array(C, order="F"), np.array(F, order="F")
-    rt = ct.c_double if dt == np.float64 else ct.c_float
+    rt = ct.c_double if dt in (np.float64, np.complex128) else ct.c_float
     sc, dif = rt(0), rt(0)
-    f = L.host_dtgsyl if dt == np.float64 else L.host_stgsyl
+    f = {np.float64: L.host_dtgsyl, np.float32: L.host_stgsyl, np.complex128: L.host_ztgsyl,
+         np.complex64: L.host_ctgsyl}[dt]
     info = f(nth, ijob, m, n, _p(A), _p(B), _p(Cw), _p(D), _p(E), _p(Fw), ct.byref(sc), ct.byref(dif))
     return Cw, Fw, sc.value, dif.value, info
 
@@ -42,16 +45,29 @@ def host_tgsyl(L, ijob, A, B, C, D, E, F, nth=1):
 SIZES = [(1, 1), (2, 2), (1, 5), (5, 1), (2, 7), (3, 4), (7, 9), (20, 13), (41, 17)]
 
 
-@pytest.mark.parametrize("dt", [np.float64, np.float32], ids=["d", "s"])
+def sylv_operands(m, n, seed, dt):
+    """(A, B, C, D, E, F): (A, D), (B, E) generalized Schur pencils from LAPACK xGGES of iid
+    N(0,1) pencils (complex: complex N(0,1)), C, F iid N(0,1)"""
+    g = np.random.default_rng(seed + 7)
+    if np.dtype(dt).kind == "c":
+        A, D = (M.astype(dt) for M in oracle.complex_schur_pencil(m, seed)[:2])
+        B, E = (M.astype(dt) for M in oracle.complex_schur_pencil(n, seed + 100)[:2])
+        C, F = (np.asfortranarray((g.standard_normal((m, n)) + 1j * g.standard_normal((m, n))).astype(dt))
+                for _ in range(2))
+    else:
+        A, D = _schur(m, seed, dt)
+        B, E = _schur(n, seed + 100, dt)
+        C, F = (np.asfortranarray(g.standard_normal((m, n)).astype(dt)) for _ in range(2))
+    return A, B, C, D, E, F
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32, np.complex128, np.complex64], ids=["d", "s", "z", "c"])
 @pytest.mark.parametrize("mn", SIZES, ids=lambda t: f"{t[0]}x{t[1]}")
 def test_tgsyl_matches_lapack(host, dt, mn):
     m, n = mn
-    tol = 1e-12 if dt == np.float64 else 2e-4
+    tol = 1e-12 if dt in (np.float64, np.complex128) else 2e-4
     for seed in range(3):
-        A, D = _schur(m, seed, dt)
-        B, E = _schur(n, seed + 100, dt)
-        g = np.random.default_rng(seed + 7)
-        C, F = (np.asfortranarray(g.standard_normal((m, n)).astype(dt)) for _ in range(2))
+        A, B, C, D, E, F = sylv_operands(m, n, seed, dt)
         for ijob in (0, 1, 3):
             rR, rL, rs, rd, ri = oracle.lapack_tgsyl("N", ijob, A, B, C, D, E, F)
             hR, hL, hs, hd, hi = host_tgsyl(host, ijob, A, B, C, D, E, F)
@@ -64,17 +80,15 @@ def test_tgsyl_matches_lapack(host, dt, mn):
 
 
 def test_tgsyl_threads_bit_for_bit(host):
-    """The solver's body on 5 and 64 host threads gives the one-thread result bit for bit."""
-    A, D = _schur(23, 1)
-    B, E = _schur(19, 2)
-    g = np.random.default_rng(3)
-    C, F = (np.asfortranarray(g.standard_normal((23, 19))) for _ in range(2))
-    for ijob in (0, 1, 3):
-        one = host_tgsyl(host, ijob, A, B, C, D, E, F, nth=1)
-        for nth in (5, 64):
-            many = host_tgsyl(host, ijob, A, B, C, D, E, F, nth=nth)
-            assert np.array_equal(one[0], many[0]) and np.array_equal(one[1], many[1])
-            assert one[2:] == many[2:]
+    """The solvers' bodies on 5 and 64 host threads give the one-thread result bit for bit."""
+    for dt in (np.float64, np.complex128):
+        A, B, C, D, E, F = sylv_operands(23, 19, 1, dt)
+        for ijob in (0, 1, 3):
+            one = host_tgsyl(host, ijob, A, B, C, D, E, F, nth=1)
+            for nth in (5, 64):
+                many = host_tgsyl(host, ijob, A, B, C, D, E, F, nth=nth)
+                assert np.array_equal(one[0], many[0]) and np.array_equal(one[1], many[1])
+                assert one[2:] == many[2:]
 
 
 def test_tgsyl_scales_against_overflow(host):
@@ -184,7 +198,61 @@ def test_tgsyl_and_tgsen_argument_checks():
                          ct.byref(m), _p(v), _p(v), _p(v), ct.byref(info))
         assert info.value == -1
     Mc, vc = np.zeros((4, 4), complex), np.zeros(8, complex)
-    info = ct.c_int(99)
-    L.xtgevc3_ztgsen(1, 1, 1, _p(sel), 4, _p(Mc), 4, _p(Mc), 4, _p(vc), _p(vc), _p(Mc), 4, _p(Mc), 4, ct.byref(m),
-                     _p(v), _p(v), _p(v), ct.byref(info))
-    assert info.value == -1
+    for ijob in (3, 5):
+        info = ct.c_int(99)
+        L.xtgevc3_ztgsen(ijob, 1, 1, _p(sel), 4, _p(Mc), 4, _p(Mc), 4, _p(vc), _p(vc), _p(Mc), 4, _p(Mc), 4,
+                         ct.byref(m), _p(v), _p(v), _p(v), ct.byref(info))
+        assert info.value == -1
+    for tr, want in ((b"C", -1), (b"N", 0)):
+        info = ct.c_int(99)
+        L.xtgevc3_ztgsyl(tr, 0, 0 if want == 0 else 4, 4, _p(Mc), 4, _p(Mc), 4, _p(Mc), 4, _p(Mc), 4, _p(Mc), 4,
+                         _p(Mc), 4, ct.byref(sc), ct.byref(dif), ct.byref(info))
+        assert info.value == (-3 if want == 0 else -1)
+
+
+def host_ztgsen_full(L, ijob, sel, A, B, Q, Z, nth=1):
+    dt = A.dtype.type
+    n = A.shape[0]
+    a, b, q, z = (np.array(M, order="F") for M in (A, B, Q, Z))
+    ev = [np.zeros(max(n, 1), dtype=dt) for _ in range(2)]
+    est = np.zeros(4, dtype=np.float64 if dt == np.complex128 else np.float32)
+    m = ct.c_int(-1)
+    f = L.host_ztgsen if dt == np.complex128 else L.host_ctgsen
+    s = np.ascontiguousarray(sel, dtype=np.int32)
+    info = f(nth, ijob, n, _p(a), _p(b), _p(q), _p(z), _p(s), *[_p(e) for e in ev], _p(est), ct.byref(m))
+    return a, b, q, z, ev, est, m.value, info
+
+
+@pytest.mark.parametrize("kind", ["neg_real", "every_third", "none", "all", "last", "first"], ids=str)
+@pytest.mark.parametrize("n,seed", [(8, 3), (30, 12), (45, 4)], ids=["8", "30", "45"])
+def test_complex_tgsen_estimates_match_lapack(host, kind, n, seed):
+    """ZTGSEN IJOB 1, 2, 4: PL, PR and DIF(1:2) within 1e-12 of LAPACK's, the pencil, Q and Z
+    within 1e-11, M and INFO equal."""
+    from test_tgsen_host import CPLX_SELECTIONS, _cplx_schur
+    S, T, Q, Z, al, be = _cplx_schur(n, seed, np.complex128)
+    sel = CPLX_SELECTIONS[kind](al, be).astype(np.int32)
+    lw = 2 * n * n + 64
+    for ijob in (1, 2, 4):
+        r = la.ztgsen(sel, S, T, Q, Z, ijob=ijob, lwork=lw, liwork=lw)
+        a, b, q, z, ev, est, m, info = host_ztgsen_full(host, ijob, sel, S, T, Q, Z)
+        assert (m, info) == (r[6], r[10]) == (r[6], 0)
+        want = [r[7], r[8], r[9][0], r[9][1]]
+        got = [est[k] for k in range(4)]
+        if ijob == 1:
+            want[2:] = got[2:] = [0.0, 0.0]
+        if ijob == 2:
+            want[:2] = got[:2] = [0.0, 0.0]
+        for g_, w_ in zip(got, want):
+            assert abs(g_ - w_) <= 1e-12 * abs(w_), (ijob, got, want)
+        for M, R in ((a, r[0]), (b, r[1]), (q, r[4]), (z, r[5])):
+            assert np.abs(M - R).max() <= 1e-11 * max(np.abs(R).max(), 1.0)
+
+
+def test_complex_tgsen_estimates_threads(host):
+    from test_tgsen_host import CPLX_SELECTIONS, _cplx_schur
+    S, T, Q, Z, al, be = _cplx_schur(30, 12, np.complex128)
+    sel = CPLX_SELECTIONS["neg_real"](al, be).astype(np.int32)
+    one = host_ztgsen_full(host, 4, sel, S, T, Q, Z, nth=1)
+    many = host_ztgsen_full(host, 4, sel, S, T, Q, Z, nth=7)
+    for x, y in zip(one[:4] + (one[5],), many[:4] + (many[5],)):
+        assert np.array_equal(x, y)

@@ -148,7 +148,7 @@ def lib():
             f = getattr(L, f"xtgevc3_{p}tgsen_dev")
             f.argtypes = [_P, _I, _I, _I, _P, _I, _P, _I, _P, _I] + [_P] * nv + [_P, _I, _P, _I, _P, _P, _P, _P, _P]
             f.restype = _I
-        for p in "ds":  # xTGSYL (TRANS = 'N')
+        for p in "dszc":  # xTGSYL (TRANS = 'N')
             f = getattr(L, f"xtgevc3_{p}tgsyl")
             f.argtypes = [_C, _I, _I, _I] + [_P, _I] * 6 + [_P, _P, _P]
             f.restype = None
@@ -616,15 +616,15 @@ def tgsen_dev(select, A, B, Q=None, Z=None, stream=None, ijob=0):
 
 
 def tgsyl(ijob, A, B, C, D, E, F):
-    """Host-array form of d/stgsyl with TRANS = 'N': A R - L B = scale C, D R - L E = scale F.
+    """Host-array form of d/s/z/ctgsyl with TRANS = 'N': A R - L B = scale C, D R - L E = scale F.
     Returns (R, L, scale, dif, info) (new arrays; dif meaningful for ijob 1 and 3)."""
     L = lib()
     dt = A.dtype.type
-    pfx = {np.float64: "d", np.float32: "s"}[dt]
+    pfx = {np.float64: "d", np.float32: "s", np.complex128: "z", np.complex64: "c"}[dt]
     m, n = C.shape
     A, B, D, E = (np.array(M, order="F", dtype=dt) for M in (A, B, D, E))
     Rm, Lm = np.array(C, order="F", dtype=dt), np.array(F, order="F", dtype=dt)
-    sd = np.zeros(2, dtype=dt)
+    sd = np.zeros(2, dtype=np.float32 if pfx in "sc" else np.float64)
     info = ct.c_int(0)
     lm, ln = max(m, 1), max(n, 1)
     getattr(L, f"xtgevc3_{pfx}tgsyl")(b"N", ijob, m, n, _ptr(A), lm, _ptr(B), ln, _ptr(Rm), lm, _ptr(D), lm, _ptr(E), ln,

@@ -68,6 +68,36 @@ __global__ void __launch_bounds__(kQzThreads, 1)
     if (threadIdx.x == 0) status[0] = i;
 }
 
+// ZTGSEN with IJOB 0, 1, 2, 4 (rb::tgsen_cplx_full_cta): as tgsen_real_full_kernel
+template <class R>
+__global__ void __launch_bounds__(kQzThreads, 1)
+    tgsen_cplx_full_kernel(rb::ZPencil<R> p, const int *select, int ijob, rb::zc<R> *alpha, rb::zc<R> *beta,
+                           rb::zc<R> *work, int *cuts, R *est, int *status)
+{
+    __shared__ rb::ZSortShared<R> shs;
+    __shared__ rb::ZSylvShared<R> shy;
+    const int i =
+        rb::tgsen_cplx_full_cta(rb::CtaDev{}, shs, shy, p, select, ijob, alpha, beta, work, cuts, est, status + 1);
+    if (threadIdx.x == 0) status[0] = i;
+}
+
+// Z/CTGSYL (TRANS = 'N', IJOB 0, 1, 3; rb::ztgsyl_cta): as tgsyl_kernel
+template <class R>
+__global__ void __launch_bounds__(kQzThreads, 1)
+    ztgsyl_kernel(rb::ZSylvG<R> y, int ijob, int *cuts, rb::zc<R> *work, R *out, int *status)
+{
+    __shared__ rb::ZSylvShared<R> sh;
+    if (threadIdx.x == 0) sh.y = y;
+    __syncthreads();
+    R dif = out[1];
+    rb::ztgsyl_cta(rb::CtaDev{}, sh, ijob, cuts, work, &dif);
+    if (threadIdx.x == 0) {
+        status[0] = sh.info;
+        out[0] = sh.scale;
+        out[1] = dif;
+    }
+}
+
 // xTGSYL (TRANS = 'N', IJOB 0, 1, 3; rb::tgsyl_cta): status = {INFO}, out = {SCALE, DIF}
 template <class R>
 __global__ void __launch_bounds__(kQzThreads, 1)
@@ -421,12 +451,13 @@ void gges_host(char jobvsl, char jobvsr, char sort, SelCplx<R> sel, int n, rb::z
     }
 }
 
-// xTGSEN's argument checks (IJOB 0 for complex pencils; 0, 1, 2, 4 for real ones: the 1-norm
-// estimates of IJOB 3 and 5 are not built, INFO = -1); sets last_error for a bad one
+// xTGSEN's argument checks (IJOB 0, 1, 2, 4: the 1-norm estimates of IJOB 3 and 5 are not
+// built, INFO = -1); sets last_error for a bad one
 int tgsen_check(int ijob, int wantq, int wantz, int n, int lda, int ldb, int ldq, int ldz, bool cplx)
 {
     int info = 0;
-    const bool built = cplx ? ijob == 0 : (ijob == 0 || ijob == 1 || ijob == 2 || ijob == 4);
+    const bool built = ijob == 0 || ijob == 1 || ijob == 2 || ijob == 4;
+    (void)cplx;
     if (!built) info = -1;
     else if (n < 0) info = -5;
     else if (lda < std::max(1, n)) info = -7;
@@ -435,7 +466,6 @@ int tgsen_check(int ijob, int wantq, int wantz, int n, int lda, int ldb, int ldq
     else if (ldz < 1 || (wantz && ldz < n)) info = cplx ? -15 : -16;
     if (info == -1)
         set_last_error(ijob < 0 || ijob > 5 ? "xTGSEN: argument 1 has an illegal value"
-                       : cplx               ? "xTGSEN: complex pencils: only IJOB = 0 is built"
                                             : "xTGSEN: IJOB 3 and 5 (1-norm estimates) are not built");
     else if (info)
         set_last_error("xTGSEN: argument " + std::to_string(-info) + " has an illegal value");
@@ -443,7 +473,7 @@ int tgsen_check(int ijob, int wantq, int wantz, int n, int lda, int ldb, int ldq
 }
 
 // LAPACK xTGSEN, device pointers, SELECT on the host: the reordering, the eigenvalues, M and
-// (real pencils, IJOB 1, 2, 4) PL, PR, DIF(1:2) (pl, pr, dif may be null).  INFO as LAPACK
+// (IJOB 1, 2, 4) PL, PR, DIF(1:2) (pl, pr, dif may be null).  INFO as LAPACK
 // numbers its arguments (-1 IJOB, -5 N, -7 LDA, -9 LDB, -14 / -13 LDQ, -16 / -15 LDZ for real /
 // complex pencils), 1 when a swap was rejected.  Returns 0, or 1 when a CUDA call failed.
 template <class R, bool CPLX>
@@ -460,8 +490,13 @@ int tgsen_device(cudaStream_t st, int ijob, int wantq, int wantz, const int *sel
     for (int i = 0; i < n; i++) bw[i] = select[i] != 0 ? 1 : 0;
     int h[2] = {0, 0};
     R est[4] = {R(0), R(0), R(0), R(0)};
-    size_t nwork = 0;  // real IJOB >= 1: 2 M (n - M) for xTGSYL's right-hand sides
+    size_t nwork = 0;  // IJOB >= 1: 2 M (n - M) elements for xTGSYL's right-hand sides
     cudaError_t e = cudaSuccess;
+    if (CPLX && ijob != 0) {
+        int mm = 0;
+        for (int k = 0; k < n; k++) mm += bw[k];
+        nwork = 2 * (size_t)mm * (n - mm) * 2;  // complex elements as reals
+    }
     if (!CPLX && ijob != 0) {  // M from the subdiagonal (DTGSEN's count), to size the workspace
         std::vector<R> sub(n > 1 ? n - 1 : 1);
         if (n > 1)
@@ -493,9 +528,9 @@ int tgsen_device(cudaStream_t st, int ijob, int wantq, int wantz, const int *sel
                 const rb::ZPencil<R> p{n, wantq, wantz, a, b, wantq ? reinterpret_cast<C *>(Q) : a,
                                        wantz ? reinterpret_cast<C *>(Z) : a, lda, ldb, wantq ? ldq : lda,
                                        wantz ? ldz : lda};
-                tgsen_cplx_kernel<R><<<1, kQzThreads, 0, st>>>(p, d, reinterpret_cast<C *>(ev0),
-                                                                reinterpret_cast<C *>(ev1), d + n);
-                for (int i = 0; i < n; i++) h[1] += bw[i];
+                tgsen_cplx_full_kernel<R><<<1, kQzThreads, 0, st>>>(p, d, ijob, reinterpret_cast<C *>(ev0),
+                                                                     reinterpret_cast<C *>(ev1),
+                                                                     reinterpret_cast<C *>(w + 4), d + n + 2, w, d + n);
             } else {
                 const rb::Pencil<R> p{n, wantq, wantz, A, B, wantq ? Q : A, wantz ? Z : A, lda, ldb,
                                       wantq ? ldq : lda, wantz ? ldz : lda};
@@ -505,7 +540,7 @@ int tgsen_device(cudaStream_t st, int ijob, int wantq, int wantz, const int *sel
             count_launches(1);
             e = cudaGetLastError();
         }
-        if (e == cudaSuccess) e = cudaMemcpyAsync(h, d + n, (CPLX ? 1 : 2) * sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h, d + n, 2 * sizeof(int), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(est, w, 4 * sizeof(R), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     }
@@ -590,8 +625,8 @@ void tgsen_host(int ijob, int wantq, int wantz, const int *select, int n, R *A, 
     }
 }
 
-// LAPACK xTGSYL's argument checks (TRANS = 'N' with IJOB 0, 1, 3 built; TRANS = 'T' and the
-// DGECON-based IJOB 2, 4 are refused with INFO -1 / -2); sets last_error for a bad one
+// LAPACK xTGSYL's argument checks (TRANS = 'N' with IJOB 0, 1, 3 built; TRANS = 'T' / 'C' and
+// the xGECON-based IJOB 2, 4 are refused with INFO -1 / -2); sets last_error for a bad one
 int tgsyl_check(char trans, int ijob, int m, int n, int lda, int ldb, int ldc, int ldd, int lde, int ldf)
 {
     int info = 0;
@@ -605,8 +640,8 @@ int tgsyl_check(char trans, int ijob, int m, int n, int lda, int ldb, int ldc, i
     else if (ldd < std::max(1, m)) info = -12;
     else if (lde < std::max(1, n)) info = -14;
     else if (ldf < std::max(1, m)) info = -16;
-    if (info == -1 && trans == 'T')
-        set_last_error("xTGSYL: TRANS = 'T' is not built");
+    if (info == -1 && (trans == 'T' || trans == 'C'))
+        set_last_error("xTGSYL: TRANS = 'T' / 'C' (the transposed equation) is not built");
     else if (info == -2 && (ijob == 2 || ijob == 4))
         set_last_error("xTGSYL: IJOB 2 and 4 (DGECON-based estimates) are not built");
     else if (info)
@@ -616,7 +651,7 @@ int tgsyl_check(char trans, int ijob, int m, int n, int lda, int ldb, int ldc, i
 
 // xTGSYL, device pointers: C, F overwritten by R, L; *scale, *dif (IJOB 1, 3; left as given
 // when the estimate's accumulator stayed 0).  Returns 0, or 1 when a CUDA call failed.
-template <class R>
+template <class R, bool CPLX = false>
 int tgsyl_device(cudaStream_t st, char trans, int ijob, int m, int n, const R *A, int lda, const R *B, int ldb, R *C,
                  int ldc, const R *D, int ldd, const R *E, int lde, R *F, int ldf, R *scale, R *dif, int *info)
 {
@@ -625,7 +660,7 @@ int tgsyl_device(cudaStream_t st, char trans, int ijob, int m, int n, const R *A
     *info = tgsyl_check(trans, ijob, m, n, lda, ldb, ldc, ldd, lde, ldf);
     if (*info) return 0;
     const int ncuts = m / 2 + n / 2 + 4;
-    const size_t nwork = ijob == 1 ? 2 * (size_t)m * n : 0;
+    const size_t nwork = ijob == 1 ? 2 * (size_t)m * n * (CPLX ? 2 : 1) : 0;
     int *d = nullptr;  // the status, then the cuts
     R *w = nullptr;    // SCALE, DIF, then the saved solution (IJOB 1)
     R out[2] = {R(1), dif ? *dif : R(0)};
@@ -633,7 +668,27 @@ int tgsyl_device(cudaStream_t st, char trans, int ijob, int m, int n, const R *A
     cudaError_t e = cudaMallocAsync(&d, (1 + ncuts) * sizeof(int), st);
     if (e == cudaSuccess) e = cudaMallocAsync(&w, (2 + nwork) * sizeof(R), st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(w, out, 2 * sizeof(R), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) {
+    if (e == cudaSuccess && CPLX) {
+        using Cx = rb::zc<R>;
+        rb::ZSylvG<R> y{};
+        y.m = m;
+        y.n = n;
+        y.A = reinterpret_cast<const Cx *>(A);
+        y.D = reinterpret_cast<const Cx *>(D);
+        y.B = reinterpret_cast<const Cx *>(B);
+        y.E = reinterpret_cast<const Cx *>(E);
+        y.lda = lda;
+        y.ldd = ldd;
+        y.ldb = ldb;
+        y.lde = lde;
+        y.C = reinterpret_cast<Cx *>(C);
+        y.F = reinterpret_cast<Cx *>(F);
+        y.ldc = ldc;
+        y.ldf = ldf;
+        ztgsyl_kernel<R><<<1, kQzThreads, 0, st>>>(y, ijob, d + 1, reinterpret_cast<Cx *>(w + 2), w, d);
+        count_launches(1);
+        e = cudaGetLastError();
+    } else if (e == cudaSuccess) {
         rb::SylvG<R> y{};
         y.m = m;
         y.n = n;
@@ -669,16 +724,17 @@ int tgsyl_device(cudaStream_t st, char trans, int ijob, int m, int n, const R *A
 }
 
 // Host pointers.  INFO = m + n + 1 (not a LAPACK value) when a CUDA call failed.
-template <class R>
+template <class R, bool CPLX = false>
 void tgsyl_host(char trans, int ijob, int m, int n, const R *A, int lda, const R *B, int ldb, R *C, int ldc,
                 const R *D, int ldd, const R *E, int lde, R *F, int ldf, R *scale, R *dif, int *info)
 {
     set_last_error("");
     *info = tgsyl_check((char)std::toupper((unsigned char)trans), ijob, m, n, lda, ldb, ldc, ldd, lde, ldf);
     if (*info) return;
+    constexpr int w = CPLX ? 2 : 1;  // reals per element
     cudaStream_t st = nullptr;
     R *buf = nullptr;
-    const size_t mm = (size_t)m * m, nn = (size_t)n * n, mn = (size_t)m * n;
+    const size_t mm = (size_t)m * m * w, nn = (size_t)n * n * w, mn = (size_t)m * n * w;
     cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMallocAsync(&buf, (2 * mm + 2 * nn + 2 * mn) * sizeof(R), st);
     R *dA = buf, *dD = buf + mm, *dB = buf + 2 * mm, *dE = dB + nn, *dC = dE + nn, *dF = dC + mn;
@@ -690,16 +746,16 @@ void tgsyl_host(char trans, int ijob, int m, int n, const R *A, int lda, const R
                 {E, dE, lde, n, n}, {C, dC, ldc, m, n}, {F, dF, ldf, m, n}};
     for (const M2 &x : ins)
         if (e == cudaSuccess)
-            e = cudaMemcpy2DAsync(x.d, x.rows * sizeof(R), x.h, (size_t)x.ld * sizeof(R), x.rows * sizeof(R), x.cols,
-                                  cudaMemcpyHostToDevice, st);
+            e = cudaMemcpy2DAsync(x.d, x.rows * w * sizeof(R), x.h, (size_t)x.ld * w * sizeof(R), x.rows * w * sizeof(R),
+                                  x.cols, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
-        const int rc = tgsyl_device<R>(st, trans, ijob, m, n, dA, m, dB, n, dC, m, dD, m, dE, n, dF, m, scale, dif, info);
+        const int rc =
+            tgsyl_device<R, CPLX>(st, trans, ijob, m, n, dA, m, dB, n, dC, m, dD, m, dE, n, dF, m, scale, dif, info);
         if (rc == 0) {
-            e = cudaMemcpy2DAsync(C, (size_t)ldc * sizeof(R), dC, m * sizeof(R), m * sizeof(R), n, cudaMemcpyDeviceToHost,
-                                  st);
+            const size_t col = (size_t)m * w * sizeof(R);
+            e = cudaMemcpy2DAsync(C, (size_t)ldc * w * sizeof(R), dC, col, col, n, cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess)
-                e = cudaMemcpy2DAsync(F, (size_t)ldf * sizeof(R), dF, m * sizeof(R), m * sizeof(R), n,
-                                      cudaMemcpyDeviceToHost, st);
+                e = cudaMemcpy2DAsync(F, (size_t)ldf * w * sizeof(R), dF, col, col, n, cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         } else {
             e = cudaErrorUnknown;
@@ -954,6 +1010,42 @@ int xtgevc3_stgsyl_dev(void *stream, char trans, int ijob, int m, int n, const f
 {
     return xtg::tgsyl_device<float>(static_cast<cudaStream_t>(stream), trans, ijob, m, n, A, lda, B, ldb, C, ldc, D,
                                     ldd, E, lde, F, ldf, scale, dif, info);
+}
+
+}  // extern "C"
+
+// ---- Z/CTGSYL (TRANS = 'N', IJOB 0, 1, 3), interleaved complex arrays -------------------------
+
+extern "C" {
+
+void xtgevc3_ztgsyl(char trans, int ijob, int m, int n, const double *A, int lda, const double *B, int ldb, double *C,
+                    int ldc, const double *D, int ldd, const double *E, int lde, double *F, int ldf, double *scale,
+                    double *dif, int *info)
+{
+    xtg::tgsyl_host<double, true>(trans, ijob, m, n, A, lda, B, ldb, C, ldc, D, ldd, E, lde, F, ldf, scale, dif, info);
+}
+
+void xtgevc3_ctgsyl(char trans, int ijob, int m, int n, const float *A, int lda, const float *B, int ldb, float *C,
+                    int ldc, const float *D, int ldd, const float *E, int lde, float *F, int ldf, float *scale,
+                    float *dif, int *info)
+{
+    xtg::tgsyl_host<float, true>(trans, ijob, m, n, A, lda, B, ldb, C, ldc, D, ldd, E, lde, F, ldf, scale, dif, info);
+}
+
+int xtgevc3_ztgsyl_dev(void *stream, char trans, int ijob, int m, int n, const double *A, int lda, const double *B,
+                       int ldb, double *C, int ldc, const double *D, int ldd, const double *E, int lde, double *F,
+                       int ldf, double *scale, double *dif, int *info)
+{
+    return xtg::tgsyl_device<double, true>(static_cast<cudaStream_t>(stream), trans, ijob, m, n, A, lda, B, ldb, C, ldc,
+                                           D, ldd, E, lde, F, ldf, scale, dif, info);
+}
+
+int xtgevc3_ctgsyl_dev(void *stream, char trans, int ijob, int m, int n, const float *A, int lda, const float *B,
+                       int ldb, float *C, int ldc, const float *D, int ldd, const float *E, int lde, float *F, int ldf,
+                       float *scale, float *dif, int *info)
+{
+    return xtg::tgsyl_device<float, true>(static_cast<cudaStream_t>(stream), trans, ijob, m, n, A, lda, B, ldb, C, ldc,
+                                          D, ldd, E, lde, F, ldf, scale, dif, info);
 }
 
 }  // extern "C"

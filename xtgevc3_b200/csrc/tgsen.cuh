@@ -322,16 +322,16 @@ XTG_HD void zsort_apply(const ZPencil<R> &p, const ZSwap<R> &s, int phase, int t
     }
 }
 
-// Returns INFO: 0 or 1 (a swap was rejected).  Every thread returns the same value, after a
-// barrier.  alpha, beta: n each.
+// The moves of ZTGSEN: alpha, beta first the input diagonals; with 0 < M < n each selected
+// eigenvalue walks up to the next free leading row.  Returns INFO, 0 or 1 (a swap was
+// rejected).  Every thread returns the same value, after a barrier.
 template <class R, class Cta>
-XTG_HD int tgsen_cplx_cta(const Cta &c, ZSortShared<R> &sh, const ZPencil<R> &p, const int *select, zc<R> *alpha,
-                          zc<R> *beta)
+XTG_HD int tgsen_cplx_reorder(const Cta &c, ZSortShared<R> &sh, const ZPencil<R> &p, const int *select, zc<R> *alpha,
+                              zc<R> *beta)
 {
     const int n = p.n, tid = c.tid(), nth = c.nth();
     auto A = [&](int i, int j) -> zc<R> & { return p.A[(size_t)i + (size_t)j * p.lda]; };
     auto B = [&](int i, int j) -> zc<R> & { return p.B[(size_t)i + (size_t)j * p.ldb]; };
-    auto Q = [&](int i, int j) -> zc<R> & { return p.Q[(size_t)i + (size_t)j * p.ldq]; };
     for (int k = tid; k < n; k += nth) {
         alpha[k] = A(k, k);
         beta[k] = B(k, k);
@@ -363,6 +363,19 @@ XTG_HD int tgsen_cplx_cta(const Cta &c, ZSortShared<R> &sh, const ZPencil<R> &p,
         }
         ks++;
     }
+    return 0;
+}
+
+// ZTGSEN's normalisation after a complete reordering (0 < M < n): B(k, k) made real and
+// non-negative row by row, Q's columns with it; alpha = diag(A), beta = diag(B).  Ends with a
+// barrier.
+template <class R, class Cta>
+XTG_HD void tgsen_cplx_normalize(const Cta &c, const ZPencil<R> &p, zc<R> *alpha, zc<R> *beta)
+{
+    const int n = p.n, tid = c.tid(), nth = c.nth();
+    auto A = [&](int i, int j) -> zc<R> & { return p.A[(size_t)i + (size_t)j * p.lda]; };
+    auto B = [&](int i, int j) -> zc<R> & { return p.B[(size_t)i + (size_t)j * p.ldb]; };
+    auto Q = [&](int i, int j) -> zc<R> & { return p.Q[(size_t)i + (size_t)j * p.ldq]; };
     // pass 1: each row's factor t into alpha and d into beta (d = -1: no scaling)
     const R safmin = Mach<R>::sfmin;
     for (int k = tid; k < n; k += nth) {
@@ -402,7 +415,115 @@ XTG_HD int tgsen_cplx_cta(const Cta &c, ZSortShared<R> &sh, const ZPencil<R> &p,
         beta[k] = B(k, k);
     }
     c.sync();
-    return 0;
+}
+
+// ZTGSEN with IJOB = 0: returns INFO, 0 or 1 (a swap was rejected).  Every thread returns the
+// same value, after a barrier.  alpha, beta: n each.
+template <class R, class Cta>
+XTG_HD int tgsen_cplx_cta(const Cta &c, ZSortShared<R> &sh, const ZPencil<R> &p, const int *select, zc<R> *alpha,
+                          zc<R> *beta)
+{
+    const int info = tgsen_cplx_reorder(c, sh, p, select, alpha, beta);
+    int m = 0;
+    for (int k = 0; k < p.n; k++) m += select[k] != 0 ? 1 : 0;
+    if (info == 0 && m > 0 && m < p.n) tgsen_cplx_normalize(c, p, alpha, beta);
+    return info;
+}
+
+// ZTGSEN's estimates (IJOB 1, 2, 4) on the reordered pencil before its normalisation, as
+// tgsen_real_estimates with ZTGSYL.  work: 2 M (n - M) complex elements; cuts n / 2 + 4 ints.
+template <class R, class Cta>
+XTG_HD void tgsen_cplx_estimates(const Cta &c, ZSylvShared<R> &sh, const ZPencil<R> &p, int m, int ijob, int info,
+                                 zc<R> *work, int *cuts, R *est)
+{
+    const int n = p.n, tid = c.tid(), nth = c.nth();
+    const bool wantp = ijob == 1 || ijob == 4, wantd = ijob == 2 || ijob == 4;
+    if (tid == 0)
+        for (int k = 0; k < 4; k++) est[k] = R(0);
+    if (info != 0 || (!wantp && !wantd)) {
+        c.sync();
+        return;
+    }
+    if (m == 0 || m == n) {
+        if (tid == 0) {
+            if (wantp) est[0] = est[1] = R(1);
+            if (wantd) {
+                R sc = R(0), sq = R(1);
+                for (int j = 0; j < n; j++) {
+                    zlassq(n, p.A + (size_t)j * p.lda, sc, sq);
+                    zlassq(n, p.B + (size_t)j * p.ldb, sc, sq);
+                }
+                est[2] = est[3] = sc * xsqrt(sq);
+            }
+        }
+        c.sync();
+        return;
+    }
+    const int n1 = m, n2 = n - m;
+    const size_t mn = (size_t)n1 * n2;
+    zc<R> *W = work, *V = work + mn;
+    const zc<R> *A11 = p.A, *B11 = p.B;
+    const zc<R> *A22 = p.A + n1 + (size_t)n1 * p.lda, *B22 = p.B + n1 + (size_t)n1 * p.ldb;
+    auto setup = [&](int mm, int nn, const zc<R> *a, const zc<R> *d, const zc<R> *b, const zc<R> *e) {
+        if (tid == 0) {
+            ZSylvG<R> &y = sh.y;
+            y.m = mm;
+            y.n = nn;
+            y.A = a;
+            y.D = d;
+            y.B = b;
+            y.E = e;
+            y.lda = y.ldb = p.lda;
+            y.ldd = y.lde = p.ldb;
+            y.C = W;
+            y.F = V;
+            y.ldc = y.ldf = mm;
+        }
+        c.sync();
+    };
+    if (wantp) {
+        for (size_t t = tid; t < mn; t += nth) {  // C = A12, F = B12
+            const int i = (int)(t % n1), j = n1 + (int)(t / n1);
+            W[t] = p.A[(size_t)i + (size_t)j * p.lda];
+            V[t] = p.B[(size_t)i + (size_t)j * p.ldb];
+        }
+        setup(n1, n2, A11, B11, A22, B22);
+        R unused = R(0);
+        ztgsyl_cta(c, sh, 0, cuts, (zc<R> *)nullptr, &unused);
+        if (tid == 0) {
+            const R dscale = sh.scale;
+            for (int k = 0; k < 2; k++) {
+                R sc = R(0), sq = R(1);
+                zlassq((int)mn, k == 0 ? W : V, sc, sq);
+                R v = sc * xsqrt(sq);
+                v = v == R(0) ? R(1) : dscale / (xsqrt(dscale * dscale / v + v) * xsqrt(v));
+                est[k] = v;
+            }
+        }
+        c.sync();
+    }
+    if (wantd) {
+        setup(n1, n2, A11, B11, A22, B22);
+        ztgsyl_cta(c, sh, 3, cuts, (zc<R> *)nullptr, est + 2);
+        setup(n2, n1, A22, B22, A11, B11);
+        ztgsyl_cta(c, sh, 3, cuts, (zc<R> *)nullptr, est + 3);
+    }
+}
+
+// ZTGSEN with IJOB 0, 1, 2 or 4: M (into *m_out from thread 0), the moves, the estimates, the
+// normalisation.  Returns INFO.  est: PL, PR, DIF(1), DIF(2).
+template <class R, class Cta>
+XTG_HD int tgsen_cplx_full_cta(const Cta &c, ZSortShared<R> &shs, ZSylvShared<R> &shy, const ZPencil<R> &p,
+                               const int *select, int ijob, zc<R> *alpha, zc<R> *beta, zc<R> *work, int *cuts, R *est,
+                               int *m_out)
+{
+    int m = 0;
+    for (int k = 0; k < p.n; k++) m += select[k] != 0 ? 1 : 0;
+    if (m_out && c.tid() == 0) *m_out = m;
+    const int info = tgsen_cplx_reorder(c, shs, p, select, alpha, beta);
+    tgsen_cplx_estimates(c, shy, p, m, ijob, info, work, cuts, est);
+    if (info == 0 && m > 0 && m < p.n) tgsen_cplx_normalize(c, p, alpha, beta);
+    return info;
 }
 
 // ---- xGGES's check of the reordered eigenvalues (host code) ---------------------------------

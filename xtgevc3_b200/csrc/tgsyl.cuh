@@ -20,9 +20,12 @@
 // B200 form: thread 0 solves each block (dependent steps on at most 3 x 3 rows and columns);
 // between barriers the CTA applies the block's two updates (rows above and columns right are
 // disjoint) and any scaling.
+//
+// Complex pencils (Z/CTGSYL): the same with 1x1 diagonal blocks only (no 2x2 block to keep
+// whole), each small system the 2 x 2 complex one of ZTGSY2, ZGESC2 (below) or ZLATDF.
 #pragma once
 
-#include "tgsna_dif.cuh"
+#include "tgsna_dif_cplx.cuh"
 
 namespace xtg {
 namespace rb {
@@ -276,6 +279,232 @@ XTG_HD void tgsyl_cta(const Cta &c, SylvShared<R> &sh, int ijob, int *cuts, R *w
         }
         c.sync();
         tgsyl_round(c, sh, rows, cols, 1);
+        for (size_t t = tid; t < (size_t)m * n; t += nth) {
+            y.C[(t % m) + (t / m) * (size_t)y.ldc] = work[t];
+            y.F[(t % m) + (t / m) * (size_t)y.ldf] = work[(size_t)m * n + t];
+        }
+        if (tid == 0) sh.scale = scale1;
+    }
+    if (ijob != 0 && tid == 0 && y.dscale != R(0)) *dif = xsqrt(R(2 * m) * R(n)) / (y.dscale * xsqrt(y.dsum));
+    c.sync();
+}
+
+// ---- complex pencils (Z/CTGSYL, TRANS = 'N') -------------------------------------------------
+
+// Solve Z x = scale rhs with zgetc2's 2 x 2 factors, scale <= 1 chosen against overflow
+// (ZGESC2: the largest entry by |re| + |im|, its modulus against the last pivot's)
+template <class R>
+XTG_HD void zgesc2(const zc<R> *Z, zc<R> *rhs, const int *ipiv, const int *jpiv, R &scale)
+{
+    const int n = 2;
+    const R eps = Mach<R>::prec, smlnum = Mach<R>::sfmin / eps;
+    for (int i = 0; i < n - 1; i++)
+        if (ipiv[i] != i) {
+            const zc<R> t = rhs[i];
+            rhs[i] = rhs[ipiv[i]];
+            rhs[ipiv[i]] = t;
+        }
+    for (int i = 0; i < n - 1; i++)
+        for (int j = i + 1; j < n; j++) rhs[j] = rhs[j] - Z[j + 2 * i] * rhs[i];
+    scale = R(1);
+    int imax = 0;
+    for (int i = 1; i < n; i++)
+        if (xabs(rhs[i].re) + xabs(rhs[i].im) > xabs(rhs[imax].re) + xabs(rhs[imax].im)) imax = i;
+    if (R(2) * smlnum * cabs(rhs[imax]) > cabs(Z[(n - 1) + 2 * (n - 1)])) {
+        const R t = R(0.5) / cabs(rhs[imax]);
+        for (int i = 0; i < n; i++) rhs[i] = t * rhs[i];
+        scale *= t;
+    }
+    const zc<R> one = mk(R(1), R(0));
+    for (int i = n - 1; i >= 0; i--) {
+        const zc<R> t = cdiv(one, Z[i + 2 * i]);
+        rhs[i] = rhs[i] * t;
+        for (int j = i + 1; j < n; j++) rhs[i] = rhs[i] - rhs[j] * (Z[i + 2 * j] * t);
+    }
+    for (int i = n - 2; i >= 0; i--)
+        if (jpiv[i] != i) {
+            const zc<R> t = rhs[i];
+            rhs[i] = rhs[jpiv[i]];
+            rhs[jpiv[i]] = t;
+        }
+}
+
+template <class R>
+struct ZSylvG {
+    int m, n;
+    const zc<R> *A, *D, *B, *E;
+    int lda, ldd, ldb, lde;
+    zc<R> *C, *F;
+    int ldc, ldf;
+    R dsum, dscale;
+};
+
+// ZTGSY2 on the block rows [is0, ie0] x columns [js0, je0] (as tgsy2_sub, 1x1 blocks)
+template <class R>
+XTG_HD int ztgsy2_sub(ZSylvG<R> &y, int is0, int ie0, int js0, int je0, int ifunc, R &scaloc)
+{
+    auto a = [&](int i, int k) { return y.A[(size_t)i + (size_t)k * y.lda]; };
+    auto d = [&](int i, int k) { return y.D[(size_t)i + (size_t)k * y.ldd]; };
+    auto b = [&](int i, int k) { return y.B[(size_t)i + (size_t)k * y.ldb]; };
+    auto e = [&](int i, int k) { return y.E[(size_t)i + (size_t)k * y.lde]; };
+    auto C = [&](int i, int k) -> zc<R> & { return y.C[(size_t)i + (size_t)k * y.ldc]; };
+    auto F = [&](int i, int k) -> zc<R> & { return y.F[(size_t)i + (size_t)k * y.ldf]; };
+    int info = 0;
+    for (int j = js0; j <= je0; j++)
+        for (int i = ie0; i >= is0; i--) {
+            zc<R> Z[4] = {a(i, i), d(i, i), -b(j, j), -e(j, j)}, rhs[2] = {C(i, j), F(i, j)};
+            int ipiv[2], jpiv[2];
+            const int ierr = zgetc2(Z, ipiv, jpiv);
+            if (ierr > 0) info = ierr;
+            if (ifunc == 0) {
+                R sc = R(1);
+                zgesc2(Z, rhs, ipiv, jpiv, sc);
+                if (sc != R(1)) {
+                    for (int k = js0; k <= je0; k++)
+                        for (int r = is0; r <= ie0; r++) {
+                            C(r, k) = sc * C(r, k);
+                            F(r, k) = sc * F(r, k);
+                        }
+                    scaloc *= sc;
+                }
+            } else {
+                zlatdf(Z, rhs, y.dsum, y.dscale, ipiv, jpiv);
+            }
+            C(i, j) = rhs[0];
+            F(i, j) = rhs[1];
+            const zc<R> alpha = -rhs[0];
+            for (int r = is0; r < i; r++) {
+                C(r, j) = C(r, j) + alpha * a(r, i);
+                F(r, j) = F(r, j) + alpha * d(r, i);
+            }
+            for (int col = j + 1; col <= je0; col++) {
+                C(i, col) = C(i, col) + rhs[1] * b(j, col);
+                F(i, col) = F(i, col) + rhs[1] * e(j, col);
+            }
+        }
+    return info;
+}
+
+template <class R>
+struct ZSylvShared {
+    ZSylvG<R> y;
+    R scaloc, scale;
+    int info, np, nq;
+};
+
+// One round of ZTGSYL over every block on one CTA (as tgsyl_round).  Ends with a barrier.
+template <class R, class Cta>
+XTG_HD void ztgsyl_round(const Cta &c, ZSylvShared<R> &sh, const int *rows, const int *cols, int ifunc)
+{
+    const int tid = c.tid(), nth = c.nth();
+    ZSylvG<R> &y = sh.y;
+    const int np = sh.np, nq = sh.nq, m = y.m, n = y.n;
+    for (int jb = 0; jb < nq; jb++) {
+        const int js = cols[jb], je = cols[jb + 1] - 1;
+        for (int ib = np - 1; ib >= 0; ib--) {
+            const int is = rows[ib], ie = rows[ib + 1] - 1;
+            if (tid == 0) {
+                R sl = R(1);
+                const int li = ztgsy2_sub(y, is, ie, js, je, ifunc, sl);
+                if (li > 0) sh.info = li;
+                sh.scaloc = sl;
+            }
+            c.sync();
+            const R sl = sh.scaloc;
+            if (sl != R(1)) {
+                for (size_t t = tid; t < (size_t)m * n; t += nth) {
+                    const int i = (int)(t % m), k = (int)(t / m);
+                    if (k >= js && k <= je && i >= is && i <= ie) continue;
+                    zc<R> &cv = y.C[(size_t)i + (size_t)k * y.ldc];
+                    zc<R> &fv = y.F[(size_t)i + (size_t)k * y.ldf];
+                    cv = sl * cv;
+                    fv = sl * fv;
+                }
+                if (tid == 0) sh.scale *= sl;
+                c.sync();
+            }
+            const int nbk = je - js + 1, mbk = ie - is + 1;
+            const size_t above = (size_t)is * nbk, right = (size_t)mbk * (n - 1 - je);
+            for (size_t t = tid; t < above + right; t += nth) {
+                if (t < above) {
+                    const int r = (int)(t % is), k = js + (int)(t / is);
+                    zc<R> cv = y.C[(size_t)r + (size_t)k * y.ldc], fv = y.F[(size_t)r + (size_t)k * y.ldf];
+                    for (int p = is; p <= ie; p++) {
+                        const zc<R> rv = y.C[(size_t)p + (size_t)k * y.ldc];
+                        cv = cv - y.A[(size_t)r + (size_t)p * y.lda] * rv;
+                        fv = fv - y.D[(size_t)r + (size_t)p * y.ldd] * rv;
+                    }
+                    y.C[(size_t)r + (size_t)k * y.ldc] = cv;
+                    y.F[(size_t)r + (size_t)k * y.ldf] = fv;
+                } else {
+                    const size_t u = t - above;
+                    const int i = is + (int)(u % mbk), k = je + 1 + (int)(u / mbk);
+                    zc<R> cv = y.C[(size_t)i + (size_t)k * y.ldc], fv = y.F[(size_t)i + (size_t)k * y.ldf];
+                    for (int q = js; q <= je; q++) {
+                        const zc<R> lv = y.F[(size_t)i + (size_t)q * y.ldf];
+                        cv = cv + lv * y.B[(size_t)q + (size_t)k * y.ldb];
+                        fv = fv + lv * y.E[(size_t)q + (size_t)k * y.lde];
+                    }
+                    y.C[(size_t)i + (size_t)k * y.ldc] = cv;
+                    y.F[(size_t)i + (size_t)k * y.ldf] = fv;
+                }
+            }
+            c.sync();
+        }
+    }
+}
+
+// ZTGSYL (TRANS = 'N', IJOB 0, 1 or 3) on one CTA, as tgsyl_cta (blocks of 2 rows and 2
+// columns, ZTGSYL's unblocked case for m, n <= 2).
+template <class R, class Cta>
+XTG_HD void ztgsyl_cta(const Cta &c, ZSylvShared<R> &sh, int ijob, int *cuts, zc<R> *work, R *dif)
+{
+    const int tid = c.tid(), nth = c.nth();
+    ZSylvG<R> &y = sh.y;
+    const int m = y.m, n = y.n;
+    int *rows = cuts, *cols = cuts + m / 2 + 2;
+    const zc<R> zero = mk(R(0), R(0));
+    if (tid == 0) {
+        if (m <= 2 && n <= 2) {
+            rows[0] = 0;
+            rows[1] = m;
+            cols[0] = 0;
+            cols[1] = n;
+            sh.np = sh.nq = 1;
+        } else {
+            sh.np = ztgsyl_blocks(m, rows);
+            sh.nq = ztgsyl_blocks(n, cols);
+        }
+        sh.info = 0;
+        sh.scale = R(1);
+        y.dsum = R(1);
+        y.dscale = R(0);
+    }
+    if (ijob == 3)
+        for (size_t t = tid; t < (size_t)m * n; t += nth) {
+            y.C[(t % m) + (t / m) * (size_t)y.ldc] = zero;
+            y.F[(t % m) + (t / m) * (size_t)y.ldf] = zero;
+        }
+    c.sync();
+    ztgsyl_round(c, sh, rows, cols, ijob == 3 ? 1 : 0);
+    if (ijob == 1) {
+        const R scale1 = sh.scale;
+        for (size_t t = tid; t < (size_t)m * n; t += nth) {
+            zc<R> &cv = y.C[(t % m) + (t / m) * (size_t)y.ldc];
+            zc<R> &fv = y.F[(t % m) + (t / m) * (size_t)y.ldf];
+            work[t] = cv;
+            work[(size_t)m * n + t] = fv;
+            cv = zero;
+            fv = zero;
+        }
+        c.sync();
+        if (tid == 0) {
+            y.dsum = R(1);
+            y.dscale = R(0);
+            sh.scale = R(1);
+        }
+        c.sync();
+        ztgsyl_round(c, sh, rows, cols, 1);
         for (size_t t = tid; t < (size_t)m * n; t += nth) {
             y.C[(t % m) + (t / m) * (size_t)y.ldc] = work[t];
             y.F[(t % m) + (t / m) * (size_t)y.ldf] = work[(size_t)m * n + t];
