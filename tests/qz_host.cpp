@@ -139,15 +139,15 @@ int run_tgsen_full(int nth, int ijob, int n, R *A, R *B, R *Q, R *Z, const int *
     Pencil<R> p{n, 1, 1, A, B, Q, Z, n, n, n, n};
     WalkShared<R> shw{};
     SylvShared<R> shs{};
-    std::vector<R> work((size_t)n * n / 2 + 2);
-    std::vector<int> cuts(n / 2 + 4);
+    std::vector<R> work((size_t)n * n + 2);
+    std::vector<int> iwork((size_t)n * n / 2 + 2), cuts(n / 2 + 4);
     int info = 0;
     std::barrier<> bar(nth);
     std::vector<std::thread> th;
     for (int t = 0; t < nth; t++)
         th.emplace_back([&, t] {
             const int i = tgsen_real_full_cta(CtaHost{t, nth, &bar}, shw, shs, p, sel, ijob, ar, ai, be, work.data(),
-                                              cuts.data(), est, m);
+                                              iwork.data(), cuts.data(), est, m);
             if (t == 0) info = i;
         });
     for (auto &x : th) x.join();
@@ -203,6 +203,30 @@ int run_ztgsen_full(int nth, int ijob, int n, R *A, R *B, R *Q, R *Z, const int 
         });
     for (auto &x : th) x.join();
     return info;
+}
+
+template <class R>
+int run_tgsyl_t(int nth, int m, int n, const R *A, const R *B, R *C, const R *D, const R *E, R *F, R *scale)
+{
+    SylvShared<R> sh{};
+    SylvG<R> &y = sh.y;
+    y.m = m;
+    y.n = n;
+    y.A = A;
+    y.D = D;
+    y.B = B;
+    y.E = E;
+    y.lda = y.ldd = y.ldc = y.ldf = m;
+    y.ldb = y.lde = n;
+    y.C = C;
+    y.F = F;
+    std::vector<int> cuts(m / 2 + n / 2 + 4);
+    std::barrier<> bar(nth);
+    std::vector<std::thread> th;
+    for (int t = 0; t < nth; t++) th.emplace_back([&, t] { tgsyl_t_cta(CtaHost{t, nth, &bar}, sh, cuts.data()); });
+    for (auto &x : th) x.join();
+    *scale = sh.scale;
+    return sh.info;
 }
 
 // SELCTG from flags: the test passes the selection that LAPACK's SELCTG made, one flag per
@@ -284,6 +308,19 @@ int host_ctgsen(int nth, int ijob, int n, float *A, float *B, float *Q, float *Z
                 float *est, int *m)
 {
     return run_ztgsen_full(nth, ijob, n, A, B, Q, Z, sel, al, be, est, m);
+}
+
+// D/STGSYL with TRANS = 'T' body
+int host_dtgsyl_t(int nth, int m, int n, const double *A, const double *B, double *C, const double *D,
+                  const double *E, double *F, double *scale)
+{
+    return run_tgsyl_t(nth, m, n, A, B, C, D, E, F, scale);
+}
+
+int host_stgsyl_t(int nth, int m, int n, const float *A, const float *B, float *C, const float *D, const float *E,
+                  float *F, float *scale)
+{
+    return run_tgsyl_t(nth, m, n, A, B, C, D, E, F, scale);
 }
 
 // Z/CTGSYL body (interleaved complex arrays)

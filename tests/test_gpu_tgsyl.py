@@ -116,3 +116,41 @@ def test_complex_tgsen_estimates_match_lapack(cuda_ok, kind):
     assert np.all(np.abs(dif - r[9]) <= 1e-10 * r[9]), (dif, r[9])
     for M, R in ((h[0], r[0]), (h[1], r[1]), (h[4], r[4]), (h[5], r[5])):
         assert np.abs(M - R).max() <= 1e-11 * max(np.abs(R).max(), 1.0)
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32], ids=["d", "s"])
+@pytest.mark.parametrize("mn", [(1, 1), (2, 2), (5, 1), (3, 4), (20, 13), (41, 17)], ids=lambda t: f"{t[0]}x{t[1]}")
+def test_tgsyl_transposed_matches_lapack(cuda_ok, dt, mn):
+    m, n = mn
+    tol = 1e-11 if dt == np.float64 else 2e-3
+    A, B, C, D, E, F = sylv_operands(m, n, 0, dt)
+    rR, rL, rs, _, ri = oracle.lapack_tgsyl("T", 0, A, B, C, D, E, F)
+    hR, hL, hs, _, hi = X.tgsyl(0, A, B, C, D, E, F, trans="T")
+    assert (hi, hs) == (ri, rs)
+    for M, R in ((hR, rR), (hL, rL)):
+        assert np.abs(M - R).max() <= tol * max(np.abs(R).max(), 1.0)
+
+
+@pytest.mark.parametrize("ijob", [3, 5])
+def test_tgsen_one_norm_estimates(cuda_ok, ijob):
+    """On LAPACK's reordered pencil with its leading M rows selected (no swaps on either side):
+    PL, PR, DIF(1:2) within 1e-10 of LAPACK's; on the full call DIF within a factor 3."""
+    import scipy.linalg.lapack as la
+    n = 30
+    S, T, Q, Z, ar, ai, be = _real_schur(n, 11, np.float64)
+    lw = 2 * n * n + 64
+    sel = REAL_SELECTIONS["neg_real"](ar, ai, be).astype(np.int32)
+    r = la.dtgsen(sel, S, T, Q, Z, ijob=ijob, lwork=lw, liwork=lw)
+    h = X.tgsen(sel, S, T, Q, Z, ijob=ijob)
+    assert (h[7], h[11]) == (r[7], r[11])
+    assert np.all(h[10] <= 3 * r[10]) and np.all(h[10] >= r[10] / 3)
+    r0 = la.dtgsen(sel, S, T, Q, Z, ijob=0, lwork=lw, liwork=lw)
+    m = r0[7]
+    A, B, Q2, Z2 = (np.asfortranarray(x) for x in (r0[0], r0[1], r0[5], r0[6]))
+    sel2 = np.zeros(n, np.int32)
+    sel2[:m] = 1
+    rr = la.dtgsen(sel2, A, B, Q2, Z2, ijob=ijob, lwork=lw, liwork=lw)
+    h = X.tgsen(sel2, A, B, Q2, Z2, ijob=ijob)
+    assert np.all(np.abs(h[10] - rr[10]) <= 1e-10 * rr[10]), (h[10], rr[10])
+    if ijob == 5:
+        assert abs(h[8] - rr[8]) <= 1e-10 * rr[8] and abs(h[9] - rr[9]) <= 1e-10 * rr[9]

@@ -172,13 +172,13 @@ def test_tgsen_estimates_rejection_and_threads(host):
 
 def test_tgsyl_and_tgsen_argument_checks():
     """xtgevc3_dtgsyl's checks (TRANS -1, IJOB -2, M -3, N -4, LDA -6, LDB -8, LDC -10, LDD -12,
-    LDE -14, LDF -16) and xtgevc3_dtgsen's refusals of IJOB 3, 5 (and complex IJOB != 0), all
-    before any device work."""
+    LDE -14, LDF -16), xtgevc3_dtgsen's of IJOB outside 0..5 and xtgevc3_ztgsen's refusal of the
+    1-norm estimates (IJOB 3, 5), all before any device work."""
     import xtgevc3_b200 as X
     L = X.lib()
     M = np.zeros((4, 4))
     sc, dif = ct.c_double(0), ct.c_double(0)
-    cases = [(b"T", 0, 4, 4, 4, 4, 4, 4, 4, 4, -1), (b"N", 2, 4, 4, 4, 4, 4, 4, 4, 4, -2),
+    cases = [(b"C", 0, 4, 4, 4, 4, 4, 4, 4, 4, -1), (b"N", 2, 4, 4, 4, 4, 4, 4, 4, 4, -2),
              (b"N", 5, 4, 4, 4, 4, 4, 4, 4, 4, -2), (b"N", 0, 0, 4, 4, 4, 4, 4, 4, 4, -3),
              (b"N", 0, 4, 0, 4, 4, 4, 4, 4, 4, -4), (b"N", 0, 4, 4, 3, 4, 4, 4, 4, 4, -6),
              (b"N", 0, 4, 4, 4, 3, 4, 4, 4, 4, -8), (b"N", 0, 4, 4, 4, 4, 3, 4, 4, 4, -10),
@@ -192,7 +192,7 @@ def test_tgsyl_and_tgsen_argument_checks():
     sel = np.zeros(4, np.int32)
     v = np.zeros(8)
     m = ct.c_int(0)
-    for ijob in (3, 5, -1, 6):
+    for ijob in (-1, 6):
         info = ct.c_int(99)
         L.xtgevc3_dtgsen(ijob, 1, 1, _p(sel), 4, _p(M), 4, _p(M), 4, _p(v), _p(v), _p(v), _p(M), 4, _p(M), 4,
                          ct.byref(m), _p(v), _p(v), _p(v), ct.byref(info))
@@ -256,3 +256,60 @@ def test_complex_tgsen_estimates_threads(host):
     many = host_ztgsen_full(host, 4, sel, S, T, Q, Z, nth=7)
     for x, y in zip(one[:4] + (one[5],), many[:4] + (many[5],)):
         assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32], ids=["d", "s"])
+@pytest.mark.parametrize("mn", SIZES, ids=lambda t: f"{t[0]}x{t[1]}")
+def test_tgsyl_transposed_matches_lapack(host, dt, mn):
+    """TRANS = 'T': A^T R + D^T L = scale C, R B^T + L E^T = -scale F, equal to LAPACK DTGSYL's
+    within 1e-12 (double) / 2e-4 (single); 1 and 5 host threads bit for bit."""
+    m, n = mn
+    tol = 1e-12 if dt == np.float64 else 2e-4
+    rt = ct.c_double if dt == np.float64 else ct.c_float
+    f = host.host_dtgsyl_t if dt == np.float64 else host.host_stgsyl_t
+    for seed in range(3):
+        A, B, C, D, E, F = sylv_operands(m, n, seed, dt)
+        rR, rL, rs, _, ri = oracle.lapack_tgsyl("T", 0, A, B, C, D, E, F)
+        outs = []
+        for nth in (1, 5):
+            Cw, Fw = np.array(C, order="F"), np.array(F, order="F")
+            sc = rt(0)
+            info = f(nth, m, n, _p(A), _p(B), _p(Cw), _p(D), _p(E), _p(Fw), ct.byref(sc))
+            assert (info, sc.value) == (ri, rs)
+            for M, R in ((Cw, rR), (Fw, rL)):
+                assert np.abs(M - R).max() <= tol * 10 * max(np.abs(R).max(), 1.0), seed
+            outs.append((Cw, Fw))
+        assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+
+
+@pytest.mark.parametrize("n,seed", [(8, 3), (30, 11), (45, 4)], ids=["8", "30", "45"])
+def test_tgsen_one_norm_estimates(host, n, seed):
+    """IJOB 3, 5 (xLACN2 driving solves with TRANS = 'N' and 'T'): on the same pencil as LAPACK
+    (its reordered output, the leading M rows selected, so that neither side swaps) PL, PR and
+    DIF(1:2) equal LAPACK's within 1e-12 for every IJOB; on the full call DIF within a factor 3
+    (the column signs of the real swaps, as for the Frobenius estimates)."""
+    S, T, Q, Z, ar, ai, be = _real_schur(n, seed, np.float64)
+    lw = 2 * n * n + 64
+    for kind, f in REAL_SELECTIONS.items():
+        sel = f(ar, ai, be).astype(np.int32)
+        for ijob in (3, 5):
+            r = la.dtgsen(sel, S, T, Q, Z, ijob=ijob, lwork=lw, liwork=lw)
+            h = host_tgsen_full(host, ijob, sel, S, T, Q, Z)
+            assert (h[6], h[7]) == (r[7], r[11])
+            if ijob == 5:
+                assert abs(h[5][0] - r[8]) <= 1e-10 * r[8] and abs(h[5][1] - r[9]) <= 1e-10 * r[9]
+            assert np.all(h[5][2:] <= 3 * r[10]) and np.all(h[5][2:] >= r[10] / 3), (kind, h[5], r[10])
+        r0 = la.dtgsen(sel, S, T, Q, Z, ijob=0, lwork=lw, liwork=lw)
+        m = r0[7]
+        A, B, Q2, Z2 = (np.asfortranarray(x) for x in (r0[0], r0[1], r0[5], r0[6]))
+        sel2 = np.zeros(n, np.int32)
+        sel2[:m] = 1
+        for ijob in (1, 2, 3, 4, 5):
+            rr = la.dtgsen(sel2, A, B, Q2, Z2, ijob=ijob, lwork=lw, liwork=lw)
+            est = host_tgsen_full(host, ijob, sel2, A, B, Q2, Z2)[5]
+            ref = np.array([rr[8], rr[9], rr[10][0], rr[10][1]])
+            if ijob in (2, 3):
+                ref[:2] = est[:2] = 0
+            if ijob == 1:
+                ref[2:] = est[2:] = 0
+            assert np.all(np.abs(est - ref) <= 1e-12 * np.abs(ref)), (kind, ijob, est, ref)

@@ -615,9 +615,10 @@ def tgsen_dev(select, A, B, Q=None, Z=None, stream=None, ijob=0):
     return (*out, float(est[0]), float(est[1]), est[2:4].copy(), info.value)
 
 
-def tgsyl(ijob, A, B, C, D, E, F):
-    """Host-array form of d/s/z/ctgsyl with TRANS = 'N': A R - L B = scale C, D R - L E = scale F.
-    Returns (R, L, scale, dif, info) (new arrays; dif meaningful for ijob 1 and 3)."""
+def tgsyl(ijob, A, B, C, D, E, F, trans="N"):
+    """Host-array form of d/s/z/ctgsyl: TRANS = 'N', A R - L B = scale C, D R - L E = scale F;
+    TRANS = 'T' (real types), A^T R + D^T L = scale C, R B^T + L E^T = -scale F.  Returns (R, L,
+    scale, dif, info) (new arrays; dif meaningful for ijob 1 and 3 with TRANS = 'N')."""
     L = lib()
     dt = A.dtype.type
     pfx = {np.float64: "d", np.float32: "s", np.complex128: "z", np.complex64: "c"}[dt]
@@ -627,7 +628,7 @@ def tgsyl(ijob, A, B, C, D, E, F):
     sd = np.zeros(2, dtype=np.float32 if pfx in "sc" else np.float64)
     info = ct.c_int(0)
     lm, ln = max(m, 1), max(n, 1)
-    getattr(L, f"xtgevc3_{pfx}tgsyl")(b"N", ijob, m, n, _ptr(A), lm, _ptr(B), ln, _ptr(Rm), lm, _ptr(D), lm, _ptr(E), ln,
+    getattr(L, f"xtgevc3_{pfx}tgsyl")(trans.encode(), ijob, m, n, _ptr(A), lm, _ptr(B), ln, _ptr(Rm), lm, _ptr(D), lm, _ptr(E), ln,
                                       _ptr(Lm), lm, _ptr(sd[0:1]), _ptr(sd[1:2]), ct.byref(info))
     if info.value == m + n + 1:
         raise RuntimeError(f"xtgevc3_{pfx}tgsyl failed: {last_error()}")

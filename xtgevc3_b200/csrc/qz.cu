@@ -54,17 +54,17 @@ __global__ void __launch_bounds__(kQzThreads, 1)
     if (threadIdx.x == 0) *info = i;
 }
 
-// DTGSEN with IJOB 0, 1, 2, 4 (rb::tgsen_real_full_cta): status = {INFO, M}; est = PL, PR,
-// DIF(1), DIF(2); work 2 M (n - M) elements, cuts n / 2 + 4 ints
+// DTGSEN with IJOB 0 to 5 (rb::tgsen_real_full_cta): status = {INFO, M}; est = PL, PR,
+// DIF(1), DIF(2); work 4 M (n - M) elements, iwork 2 M (n - M) ints, cuts n / 2 + 4 ints
 template <class R>
 __global__ void __launch_bounds__(kQzThreads, 1)
     tgsen_real_full_kernel(rb::Pencil<R> p, const int *select, int ijob, R *alphar, R *alphai, R *beta, R *work,
-                           int *cuts, R *est, int *status)
+                           int *iwork, int *cuts, R *est, int *status)
 {
     __shared__ rb::WalkShared<R> shw;
     __shared__ rb::SylvShared<R> shs;
-    const int i =
-        rb::tgsen_real_full_cta(rb::CtaDev{}, shw, shs, p, select, ijob, alphar, alphai, beta, work, cuts, est, status + 1);
+    const int i = rb::tgsen_real_full_cta(rb::CtaDev{}, shw, shs, p, select, ijob, alphar, alphai, beta, work, iwork,
+                                          cuts, est, status + 1);
     if (threadIdx.x == 0) status[0] = i;
 }
 
@@ -98,16 +98,18 @@ __global__ void __launch_bounds__(kQzThreads, 1)
     }
 }
 
-// xTGSYL (TRANS = 'N', IJOB 0, 1, 3; rb::tgsyl_cta): status = {INFO}, out = {SCALE, DIF}
+// xTGSYL (TRANS = 'N' with IJOB 0, 1, 3: rb::tgsyl_cta; trans: TRANS = 'T', rb::tgsyl_t_cta):
+// status = {INFO}, out = {SCALE, DIF}
 template <class R>
 __global__ void __launch_bounds__(kQzThreads, 1)
-    tgsyl_kernel(rb::SylvG<R> y, int ijob, int *cuts, R *work, R *out, int *status)
+    tgsyl_kernel(rb::SylvG<R> y, int trans, int ijob, int *cuts, R *work, R *out, int *status)
 {
     __shared__ rb::SylvShared<R> sh;
     if (threadIdx.x == 0) sh.y = y;
     __syncthreads();
     R dif = out[1];
-    rb::tgsyl_cta(rb::CtaDev{}, sh, ijob, cuts, work, &dif);
+    if (trans) rb::tgsyl_t_cta(rb::CtaDev{}, sh, cuts);
+    else rb::tgsyl_cta(rb::CtaDev{}, sh, ijob, cuts, work, &dif);
     if (threadIdx.x == 0) {
         status[0] = sh.info;
         out[0] = sh.scale;
@@ -451,13 +453,12 @@ void gges_host(char jobvsl, char jobvsr, char sort, SelCplx<R> sel, int n, rb::z
     }
 }
 
-// xTGSEN's argument checks (IJOB 0, 1, 2, 4: the 1-norm estimates of IJOB 3 and 5 are not
-// built, INFO = -1); sets last_error for a bad one
+// xTGSEN's argument checks (IJOB 0 to 5 for real pencils; complex: 0, 1, 2, 4, the 1-norm
+// estimates of IJOB 3 and 5 not built, INFO = -1); sets last_error for a bad one
 int tgsen_check(int ijob, int wantq, int wantz, int n, int lda, int ldb, int ldq, int ldz, bool cplx)
 {
     int info = 0;
-    const bool built = ijob == 0 || ijob == 1 || ijob == 2 || ijob == 4;
-    (void)cplx;
+    const bool built = ijob >= 0 && ijob <= 5 && (!cplx || (ijob != 3 && ijob != 5));
     if (!built) info = -1;
     else if (n < 0) info = -5;
     else if (lda < std::max(1, n)) info = -7;
@@ -466,14 +467,14 @@ int tgsen_check(int ijob, int wantq, int wantz, int n, int lda, int ldb, int ldq
     else if (ldz < 1 || (wantz && ldz < n)) info = cplx ? -15 : -16;
     if (info == -1)
         set_last_error(ijob < 0 || ijob > 5 ? "xTGSEN: argument 1 has an illegal value"
-                                            : "xTGSEN: IJOB 3 and 5 (1-norm estimates) are not built");
+                                            : "xTGSEN: complex pencils: IJOB 3 and 5 (1-norm estimates) are not built");
     else if (info)
         set_last_error("xTGSEN: argument " + std::to_string(-info) + " has an illegal value");
     return info;
 }
 
 // LAPACK xTGSEN, device pointers, SELECT on the host: the reordering, the eigenvalues, M and
-// (IJOB 1, 2, 4) PL, PR, DIF(1:2) (pl, pr, dif may be null).  INFO as LAPACK
+// (IJOB 1 to 5) PL, PR, DIF(1:2) (pl, pr, dif may be null).  INFO as LAPACK
 // numbers its arguments (-1 IJOB, -5 N, -7 LDA, -9 LDB, -14 / -13 LDQ, -16 / -15 LDZ for real /
 // complex pencils), 1 when a swap was rejected.  Returns 0, or 1 when a CUDA call failed.
 template <class R, bool CPLX>
@@ -512,12 +513,13 @@ int tgsen_device(cudaStream_t st, int ijob, int wantq, int wantz, const int *sel
                 mm += bw[k];
             }
         }
-        nwork = 2 * (size_t)mm * (n - mm);
+        nwork = (ijob == 3 || ijob == 5 ? 4 : 2) * (size_t)mm * (n - mm);
     }
     const int ncuts = n / 2 + 4;
-    int *d = nullptr;  // n flags, the status (INFO, M), the cuts
+    const size_t niwork = (!CPLX && (ijob == 3 || ijob == 5)) ? nwork / 2 : 0;  // xLACN2's signs
+    int *d = nullptr;  // n flags, the status (INFO, M), the cuts, the signs
     R *w = nullptr;    // PL, PR, DIF(1), DIF(2), then the workspace
-    if (e == cudaSuccess) e = cudaMallocAsync(&d, (n + 2 + ncuts) * sizeof(int), st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d, (n + 2 + ncuts + niwork) * sizeof(int), st);
     if (e == cudaSuccess) e = cudaMallocAsync(&w, (4 + nwork) * sizeof(R), st);
     if (e == cudaSuccess) {
         e = cudaMemcpyAsync(d, bw.data(), n * sizeof(int), cudaMemcpyHostToDevice, st);
@@ -534,8 +536,8 @@ int tgsen_device(cudaStream_t st, int ijob, int wantq, int wantz, const int *sel
             } else {
                 const rb::Pencil<R> p{n, wantq, wantz, A, B, wantq ? Q : A, wantz ? Z : A, lda, ldb,
                                       wantq ? ldq : lda, wantz ? ldz : lda};
-                tgsen_real_full_kernel<R><<<1, kQzThreads, 0, st>>>(p, d, ijob, ev0, ev1, ev2, w + 4, d + n + 2, w,
-                                                                     d + n);
+                tgsen_real_full_kernel<R><<<1, kQzThreads, 0, st>>>(p, d, ijob, ev0, ev1, ev2, w + 4,
+                                                                     d + n + 2 + ncuts, d + n + 2, w, d + n);
             }
             count_launches(1);
             e = cudaGetLastError();
@@ -556,11 +558,11 @@ int tgsen_device(cudaStream_t st, int ijob, int wantq, int wantz, const int *sel
     }
     *info = h[0];
     if (m) *m = h[1];
-    if (ijob == 1 || ijob == 4) {
+    if (ijob == 1 || ijob == 4 || ijob == 5) {
         if (pl) *pl = est[0];
         if (pr) *pr = est[1];
     }
-    if ((ijob == 2 || ijob == 4) && dif) {
+    if (ijob >= 2 && dif) {
         dif[0] = est[2];
         dif[1] = est[3];
     }
@@ -625,13 +627,15 @@ void tgsen_host(int ijob, int wantq, int wantz, const int *select, int n, R *A, 
     }
 }
 
-// LAPACK xTGSYL's argument checks (TRANS = 'N' with IJOB 0, 1, 3 built; TRANS = 'T' / 'C' and
-// the xGECON-based IJOB 2, 4 are refused with INFO -1 / -2); sets last_error for a bad one
-int tgsyl_check(char trans, int ijob, int m, int n, int lda, int ldb, int ldc, int ldd, int lde, int ldf)
+// LAPACK xTGSYL's argument checks (TRANS = 'N' with IJOB 0, 1, 3 and, for real pencils,
+// TRANS = 'T' (IJOB not referenced, as LAPACK) built; TRANS = 'C' and the xGECON-based IJOB 2,
+// 4 are refused with INFO -1 / -2); sets last_error for a bad one
+int tgsyl_check(char trans, int ijob, int m, int n, int lda, int ldb, int ldc, int ldd, int lde, int ldf,
+                bool cplx = false)
 {
     int info = 0;
-    if (trans != 'N') info = -1;
-    else if (ijob != 0 && ijob != 1 && ijob != 3) info = -2;
+    if (trans != 'N' && (cplx || trans != 'T')) info = -1;
+    else if (trans == 'N' && ijob != 0 && ijob != 1 && ijob != 3) info = -2;
     else if (m <= 0) info = -3;
     else if (n <= 0) info = -4;
     else if (lda < std::max(1, m)) info = -6;
@@ -641,7 +645,7 @@ int tgsyl_check(char trans, int ijob, int m, int n, int lda, int ldb, int ldc, i
     else if (lde < std::max(1, n)) info = -14;
     else if (ldf < std::max(1, m)) info = -16;
     if (info == -1 && (trans == 'T' || trans == 'C'))
-        set_last_error("xTGSYL: TRANS = 'T' / 'C' (the transposed equation) is not built");
+        set_last_error("xTGSYL: TRANS = 'C' (complex pencils' conjugate-transposed equation) is not built");
     else if (info == -2 && (ijob == 2 || ijob == 4))
         set_last_error("xTGSYL: IJOB 2 and 4 (DGECON-based estimates) are not built");
     else if (info)
@@ -657,8 +661,9 @@ int tgsyl_device(cudaStream_t st, char trans, int ijob, int m, int n, const R *A
 {
     set_last_error("");
     trans = (char)std::toupper((unsigned char)trans);
-    *info = tgsyl_check(trans, ijob, m, n, lda, ldb, ldc, ldd, lde, ldf);
+    *info = tgsyl_check(trans, ijob, m, n, lda, ldb, ldc, ldd, lde, ldf, CPLX);
     if (*info) return 0;
+    if (trans == 'T') ijob = 0;  // not referenced by the transposed solve
     const int ncuts = m / 2 + n / 2 + 4;
     const size_t nwork = ijob == 1 ? 2 * (size_t)m * n * (CPLX ? 2 : 1) : 0;
     int *d = nullptr;  // the status, then the cuts
@@ -704,7 +709,7 @@ int tgsyl_device(cudaStream_t st, char trans, int ijob, int m, int n, const R *A
         y.F = F;
         y.ldc = ldc;
         y.ldf = ldf;
-        tgsyl_kernel<R><<<1, kQzThreads, 0, st>>>(y, ijob, d + 1, w + 2, w, d);
+        tgsyl_kernel<R><<<1, kQzThreads, 0, st>>>(y, trans == 'T' ? 1 : 0, ijob, d + 1, w + 2, w, d);
         count_launches(1);
         e = cudaGetLastError();
     }
@@ -729,7 +734,7 @@ void tgsyl_host(char trans, int ijob, int m, int n, const R *A, int lda, const R
                 const R *D, int ldd, const R *E, int lde, R *F, int ldf, R *scale, R *dif, int *info)
 {
     set_last_error("");
-    *info = tgsyl_check((char)std::toupper((unsigned char)trans), ijob, m, n, lda, ldb, ldc, ldd, lde, ldf);
+    *info = tgsyl_check((char)std::toupper((unsigned char)trans), ijob, m, n, lda, ldb, ldc, ldd, lde, ldf, CPLX);
     if (*info) return;
     constexpr int w = CPLX ? 2 : 1;  // reals per element
     cudaStream_t st = nullptr;

@@ -161,19 +161,22 @@ XTG_HD int tgsen_real_cta(const Cta &c, WalkShared<R> &sh, const Pencil<R> &p, c
     return info;
 }
 
-// DTGSEN's estimates on the reordered pencil (IJOB 1, 2, 4; m = M, info the reordering's):
-// est[0], est[1] = PL, PR (IJOB 1 and 4: 1 / sqrt(1 + ||R||^2 / scale^2) and the same with L,
+// DTGSEN's estimates on the reordered pencil (IJOB 1 to 5; m = M, info the reordering's):
+// est[0], est[1] = PL, PR (IJOB 1, 4, 5: 1 / sqrt(1 + ||R||^2 / scale^2) and the same with L,
 // from xTGSYL's solution of A11 R - L A22 = A12, B11 R - L B22 = B12), est[2], est[3] = DIF(1),
-// DIF(2) (IJOB 2 and 4: xTGSYL's Frobenius-norm estimates, IJOB = 3, of Difu on (A11, B11),
-// (A22, B22) and of Difl with the two swapped).  M = 0 or n: PL = PR = 1, DIF = ||(A, B)||_F;
-// a rejected swap: all 0.  work: 2 M (n - M) elements; cuts: n / 2 + 4 ints.  Ends with a
-// barrier.
+// DIF(2): IJOB 2 and 4 xTGSYL's Frobenius-norm estimates (its IJOB = 3) of Difu on (A11, B11),
+// (A22, B22) and of Difl with the two swapped; IJOB 3 and 5 scale / xLACN2's 1-norm estimate
+// of the inverse of the same operators (xTGSYL solves with TRANS = 'N' and 'T').  M = 0 or n:
+// PL = PR = 1, DIF = ||(A, B)||_F; a rejected swap: all 0.  work: 4 M (n - M) elements (2 M
+// (n - M) for IJOB 1, 2, 4); iwork: 2 M (n - M) ints (IJOB 3, 5); cuts: n / 2 + 4 ints.  Ends
+// with a barrier.
 template <class R, class Cta>
 XTG_HD void tgsen_real_estimates(const Cta &c, SylvShared<R> &sh, const Pencil<R> &p, int m, int ijob, int info,
-                                 R *work, int *cuts, R *est)
+                                 R *work, int *iwork, int *cuts, R *est)
 {
     const int n = p.n, tid = c.tid(), nth = c.nth();
-    const bool wantp = ijob == 1 || ijob == 4, wantd = ijob == 2 || ijob == 4;
+    const bool wantp = ijob == 1 || ijob == 4 || ijob == 5, wantd1 = ijob == 2 || ijob == 4,
+               wantd2 = ijob == 3 || ijob == 5, wantd = wantd1 || wantd2;
     if (tid == 0)
         for (int k = 0; k < 4; k++) est[k] = R(0);
     if (info != 0 || (!wantp && !wantd)) {
@@ -240,26 +243,54 @@ XTG_HD void tgsen_real_estimates(const Cta &c, SylvShared<R> &sh, const Pencil<R
         }
         c.sync();
     }
-    if (wantd) {
+    if (wantd1) {
         setup(n1, n2, A11, B11, A22, B22);
         tgsyl_cta(c, sh, 3, cuts, (R *)nullptr, est + 2);
         setup(n2, n1, A22, B22, A11, B11);
         tgsyl_cta(c, sh, 3, cuts, (R *)nullptr, est + 3);
     }
+    if (wantd2) {  // xLACN2 on [vec C; vec F] = work[0, 2 mn), its v in work[2 mn, 4 mn)
+        const int mn2 = (int)(2 * mn);
+        R *Vl = work + 2 * mn;
+        for (int which = 0; which < 2; which++) {
+            if (tid == 0) {
+                sh.lac.kase = 0;
+                lacn2(mn2, Vl, W, iwork, sh.lac);
+            }
+            c.sync();
+            R dscale = R(1);
+            for (int step = 0; step < 16; step++) {  // xLACN2 asks for at most 11 products
+                const int kase = sh.lac.kase;
+                if (kase == 0) break;
+                if (which == 0) setup(n1, n2, A11, B11, A22, B22);
+                else setup(n2, n1, A22, B22, A11, B11);
+                R unused = R(0);
+                if (kase == 1) tgsyl_cta(c, sh, 0, cuts, (R *)nullptr, &unused);
+                else tgsyl_t_cta(c, sh, cuts);
+                if (tid == 0) {
+                    dscale = sh.scale;
+                    lacn2(mn2, Vl, W, iwork, sh.lac);
+                }
+                c.sync();
+            }
+            if (tid == 0) est[2 + which] = dscale / sh.lac.est;
+            c.sync();
+        }
+    }
 }
 
-// DTGSEN with IJOB 0, 1, 2 or 4 (tgsen_real_estimates): M (into *m_out from thread 0), the
-// moves, the estimates on the reordered pencil, the eigenvalues.  Returns INFO as
-// tgsen_real_reorder.  est: PL, PR, DIF(1), DIF(2).
+// DTGSEN with IJOB 0 to 5 (tgsen_real_estimates): M (into *m_out from thread 0), the moves,
+// the estimates on the reordered pencil, the eigenvalues.  Returns INFO as tgsen_real_reorder.
+// est: PL, PR, DIF(1), DIF(2).
 template <class R, class Cta>
 XTG_HD int tgsen_real_full_cta(const Cta &c, WalkShared<R> &shw, SylvShared<R> &shs, const Pencil<R> &p,
-                               const int *select, int ijob, R *alphar, R *alphai, R *beta, R *work, int *cuts, R *est,
-                               int *m_out)
+                               const int *select, int ijob, R *alphar, R *alphai, R *beta, R *work, int *iwork,
+                               int *cuts, R *est, int *m_out)
 {
     const int m = tgsen_real_m(p, select);  // reads the subdiagonal before the first swap's barrier
     if (m_out && c.tid() == 0) *m_out = m;
     const int info = tgsen_real_reorder(c, shw, p, select);
-    tgsen_real_estimates(c, shs, p, m, ijob, info, work, cuts, est);
+    tgsen_real_estimates(c, shs, p, m, ijob, info, work, iwork, cuts, est);
     tgsen_real_finish(c, p, alphar, alphai, beta);
     return info;
 }

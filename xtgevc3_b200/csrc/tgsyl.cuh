@@ -156,12 +156,20 @@ XTG_HD int tgsyl_cuts(int m, const R *T, int ldt, int *starts)
     return p;
 }
 
-// the CTA's shared state of tgsyl_cta (shared memory on the GPU)
+// the CTA's shared state of tgsyl_cta (shared memory on the GPU); lac: xLACN2's state when the
+// solver is driven by the 1-norm estimator
+template <class R>
+struct Lacn2 {
+    int kase, jump, j, iter;
+    R est, estold;
+};
+
 template <class R>
 struct SylvShared {
     SylvG<R> y;
     R scaloc, scale;
     int info, np, nq;
+    Lacn2<R> lac;
 };
 
 // One round of xTGSYL over every block (ifunc 0: solve, 1: estimate) on one CTA.  rows /
@@ -287,6 +295,287 @@ XTG_HD void tgsyl_cta(const Cta &c, SylvShared<R> &sh, int ijob, int *cuts, R *w
     }
     if (ijob != 0 && tid == 0 && y.dscale != R(0)) *dif = xsqrt(R(2 * m) * R(n)) / (y.dscale * xsqrt(y.dsum));
     c.sync();
+}
+
+// ---- the transposed equation (xTGSYL with TRANS = 'T', IJOB 0) ------------------------------
+//     A^T R + D^T L = scale C,   R B^T + L E^T = -scale F
+// the blocks visited in the other order (row blocks top to bottom, column blocks right to
+// left), each small system the transpose of the one for TRANS = 'N', and the solution
+// substituted into the rows below (C -= A^T R + D^T L) and the columns left (F += R B^T + L E^T).
+
+// xTGSY2 with TRANS = 'T' on the block rows [is0, ie0] x columns [js0, je0]
+template <class R>
+XTG_HD int tgsy2_sub_t(SylvG<R> &y, int is0, int ie0, int js0, int je0, R &scaloc)
+{
+    auto a = [&](int i, int k) { return y.A[(size_t)i + (size_t)k * y.lda]; };
+    auto d = [&](int i, int k) { return y.D[(size_t)i + (size_t)k * y.ldd]; };
+    auto b = [&](int i, int k) { return y.B[(size_t)i + (size_t)k * y.ldb]; };
+    auto e = [&](int i, int k) { return y.E[(size_t)i + (size_t)k * y.lde]; };
+    auto C = [&](int i, int k) -> R & { return y.C[(size_t)i + (size_t)k * y.ldc]; };
+    auto F = [&](int i, int k) -> R & { return y.F[(size_t)i + (size_t)k * y.ldf]; };
+    int ist[5], jst[5], np = 0, nq = 0;
+    for (int i = is0; i <= ie0;) {
+        ist[np++] = i;
+        i += (i < ie0 && a(i + 1, i) != R(0)) ? 2 : 1;
+    }
+    ist[np] = ie0 + 1;
+    for (int j = js0; j <= je0;) {
+        jst[nq++] = j;
+        j += (j < je0 && b(j + 1, j) != R(0)) ? 2 : 1;
+    }
+    jst[nq] = je0 + 1;
+    int info = 0;
+    for (int ib = 0; ib < np; ib++) {
+        const int is = ist[ib], mb = ist[ib + 1] - is, ie = is + mb - 1;
+        for (int jb = nq - 1; jb >= 0; jb--) {
+            const int js = jst[jb], nb = jst[jb + 1] - js;
+            const int nn = mb * nb, zdim = 2 * nn;
+            R Zn[64], Z[64], rhs[8];
+            for (int t = 0; t < 64; t++) Zn[t] = R(0);
+            for (int j = 0; j < nb; j++)
+                for (int i = 0; i < mb; i++) {
+                    const int k = i + mb * j;
+                    for (int p = 0; p < mb; p++) {
+                        Zn[k + 8 * (p + mb * j)] = a(is + i, is + p);
+                        if (p >= i) Zn[(nn + k) + 8 * (p + mb * j)] = d(is + i, is + p);
+                    }
+                    for (int q = 0; q < nb; q++) {
+                        Zn[k + 8 * (nn + i + mb * q)] = -b(js + q, js + j);
+                        if (q <= j) Zn[(nn + k) + 8 * (nn + i + mb * q)] = -e(js + q, js + j);
+                    }
+                    rhs[k] = C(is + i, js + j);
+                    rhs[nn + k] = F(is + i, js + j);
+                }
+            for (int r = 0; r < 8; r++)
+                for (int q = 0; q < 8; q++) Z[r + 8 * q] = Zn[q + 8 * r];
+            int ipiv[8], jpiv[8];
+            const int ierr = getc2(zdim, Z, ipiv, jpiv);
+            if (ierr > 0) info = ierr;
+            R sc = R(1);
+            gesc2(zdim, Z, rhs, ipiv, jpiv, sc);
+            if (sc != R(1)) {
+                for (int k = js0; k <= je0; k++)
+                    for (int i = is0; i <= ie0; i++) {
+                        C(i, k) *= sc;
+                        F(i, k) *= sc;
+                    }
+                scaloc *= sc;
+            }
+            for (int j = 0; j < nb; j++)
+                for (int i = 0; i < mb; i++) {
+                    C(is + i, js + j) = rhs[i + mb * j];
+                    F(is + i, js + j) = rhs[nn + i + mb * j];
+                }
+            // columns [js0, js) of the block: F += R B^T, then F += L E^T
+            for (int col = js0; col < js; col++)
+                for (int i = 0; i < mb; i++) {
+                    R f = F(is + i, col);
+                    for (int q = 0; q < nb; q++) f += rhs[i + mb * q] * b(col, js + q);
+                    for (int q = 0; q < nb; q++) f += rhs[nn + i + mb * q] * e(col, js + q);
+                    F(is + i, col) = f;
+                }
+            // rows (ie, ie0] of the block: C -= A^T R, then C -= D^T L
+            for (int row = ie + 1; row <= ie0; row++)
+                for (int j = 0; j < nb; j++) {
+                    R cv = C(row, js + j);
+                    for (int p = 0; p < mb; p++) cv -= a(is + p, row) * rhs[p + mb * j];
+                    for (int p = 0; p < mb; p++) cv -= d(is + p, row) * rhs[nn + p + mb * j];
+                    C(row, js + j) = cv;
+                }
+        }
+    }
+    return info;
+}
+
+// One pass of xTGSYL with TRANS = 'T' over every block on one CTA.  Ends with a barrier.
+template <class R, class Cta>
+XTG_HD void tgsyl_round_t(const Cta &c, SylvShared<R> &sh, const int *rows, const int *cols)
+{
+    const int tid = c.tid(), nth = c.nth();
+    SylvG<R> &y = sh.y;
+    const int np = sh.np, nq = sh.nq, m = y.m, n = y.n;
+    for (int ib = 0; ib < np; ib++) {
+        const int is = rows[ib], ie = rows[ib + 1] - 1;
+        for (int jb = nq - 1; jb >= 0; jb--) {
+            const int js = cols[jb], je = cols[jb + 1] - 1;
+            if (tid == 0) {
+                R sl = R(1);
+                const int li = tgsy2_sub_t(y, is, ie, js, je, sl);
+                if (li > 0) sh.info = li;
+                sh.scaloc = sl;
+            }
+            c.sync();
+            const R sl = sh.scaloc;
+            if (sl != R(1)) {
+                for (size_t t = tid; t < (size_t)m * n; t += nth) {
+                    const int i = (int)(t % m), k = (int)(t / m);
+                    if (k >= js && k <= je && i >= is && i <= ie) continue;
+                    y.C[(size_t)i + (size_t)k * y.ldc] *= sl;
+                    y.F[(size_t)i + (size_t)k * y.ldf] *= sl;
+                }
+                if (tid == 0) sh.scale *= sl;
+                c.sync();
+            }
+            // columns left of the block in its rows (F += R B^T + L E^T) and rows below it in
+            // its columns (C -= A^T R + D^T L): disjoint, one pass
+            const int nbk = je - js + 1, mbk = ie - is + 1;
+            const size_t left = (size_t)mbk * js, below = (size_t)(m - 1 - ie) * nbk;
+            for (size_t t = tid; t < left + below; t += nth) {
+                if (t < left) {
+                    const int i = is + (int)(t % mbk), col = (int)(t / mbk);
+                    R f = y.F[(size_t)i + (size_t)col * y.ldf];
+                    for (int q = js; q <= je; q++)
+                        f += y.C[(size_t)i + (size_t)q * y.ldc] * y.B[(size_t)col + (size_t)q * y.ldb];
+                    for (int q = js; q <= je; q++)
+                        f += y.F[(size_t)i + (size_t)q * y.ldf] * y.E[(size_t)col + (size_t)q * y.lde];
+                    y.F[(size_t)i + (size_t)col * y.ldf] = f;
+                } else {
+                    const size_t u = t - left;
+                    const int row = ie + 1 + (int)(u % (m - 1 - ie)), k = js + (int)(u / (m - 1 - ie));
+                    R cv = y.C[(size_t)row + (size_t)k * y.ldc];
+                    for (int p = is; p <= ie; p++)
+                        cv -= y.A[(size_t)p + (size_t)row * y.lda] * y.C[(size_t)p + (size_t)k * y.ldc];
+                    for (int p = is; p <= ie; p++)
+                        cv -= y.D[(size_t)p + (size_t)row * y.ldd] * y.F[(size_t)p + (size_t)k * y.ldf];
+                    y.C[(size_t)row + (size_t)k * y.ldc] = cv;
+                }
+            }
+            c.sync();
+        }
+    }
+}
+
+// xTGSYL with TRANS = 'T' (IJOB 0: the solve) on one CTA; sh.y and cuts as for tgsyl_cta.  On
+// return (every thread, after a barrier): sh.scale, sh.info.
+template <class R, class Cta>
+XTG_HD void tgsyl_t_cta(const Cta &c, SylvShared<R> &sh, int *cuts)
+{
+    const int tid = c.tid();
+    SylvG<R> &y = sh.y;
+    const int m = y.m, n = y.n;
+    int *rows = cuts, *cols = cuts + m / 2 + 2;
+    if (tid == 0) {
+        if (m <= 2 && n <= 2) {
+            rows[0] = 0;
+            rows[1] = m;
+            cols[0] = 0;
+            cols[1] = n;
+            sh.np = sh.nq = 1;
+        } else {
+            sh.np = tgsyl_cuts(m, y.A, y.lda, rows);
+            sh.nq = tgsyl_cuts(n, y.B, y.ldb, cols);
+        }
+        sh.info = 0;
+        sh.scale = R(1);
+    }
+    c.sync();
+    tgsyl_round_t(c, sh, rows, cols);
+}
+
+// ---- the 1-norm estimator (xLACN2, N. J. Higham, ACM TOMS 14 (1988) 381-396) --------------
+// Reverse communication: on kase = 0 the caller starts; the estimator sets x and kase = 1
+// (the caller overwrites x by the operator applied to x) or kase = 2 (by its transpose) and is
+// called again, until it returns kase = 0 with est the estimate.  At most 5 iterations.
+template <class R>
+XTG_HD void lacn2(int n, R *v, R *x, int *isgn, Lacn2<R> &s)
+{
+    const int itmax = 5;
+    auto asum = [&](const R *w) {
+        R t = R(0);
+        for (int i = 0; i < n; i++) t += xabs(w[i]);
+        return t;
+    };
+    auto amax = [&]() {
+        int k = 0;
+        for (int i = 1; i < n; i++)
+            if (xabs(x[i]) > xabs(x[k])) k = i;
+        return k;
+    };
+    auto signs = [&]() {
+        for (int i = 0; i < n; i++) {
+            x[i] = x[i] >= R(0) ? R(1) : R(-1);
+            isgn[i] = x[i] > R(0) ? 1 : -1;
+        }
+    };
+    auto unit = [&]() {  // x = e_j, the operator next
+        for (int i = 0; i < n; i++) x[i] = R(0);
+        x[s.j] = R(1);
+        s.kase = 1;
+        s.jump = 3;
+    };
+    auto final_stage = [&]() {
+        R altsgn = R(1);
+        for (int i = 0; i < n; i++) {
+            x[i] = altsgn * (R(1) + R(i) / R(n - 1));
+            altsgn = -altsgn;
+        }
+        s.kase = 1;
+        s.jump = 5;
+    };
+    if (s.kase == 0) {
+        for (int i = 0; i < n; i++) x[i] = R(1) / R(n);
+        s.kase = 1;
+        s.jump = 1;
+        return;
+    }
+    switch (s.jump) {
+    case 1:  // x = A x, first iteration
+        if (n == 1) {
+            v[0] = x[0];
+            s.est = xabs(v[0]);
+            s.kase = 0;
+            return;
+        }
+        s.est = asum(x);
+        signs();
+        s.kase = 2;
+        s.jump = 2;
+        return;
+    case 2:  // x = A^T x, first iteration
+        s.j = amax();
+        s.iter = 2;
+        unit();
+        return;
+    case 3: {  // x = A x
+        for (int i = 0; i < n; i++) v[i] = x[i];
+        s.estold = s.est;
+        s.est = asum(v);
+        bool same = true;
+        for (int i = 0; i < n; i++)
+            if ((x[i] >= R(0) ? 1 : -1) != isgn[i]) {
+                same = false;
+                break;
+            }
+        if (same || s.est <= s.estold) {  // repeated sign vector, or cycling: converged
+            final_stage();
+            return;
+        }
+        signs();
+        s.kase = 2;
+        s.jump = 4;
+        return;
+    }
+    case 4: {  // x = A^T x
+        const int jlast = s.j;
+        s.j = amax();
+        if (x[jlast] != xabs(x[s.j]) && s.iter < itmax) {
+            s.iter++;
+            unit();
+            return;
+        }
+        final_stage();
+        return;
+    }
+    default: {  // case 5: x = A x, final stage
+        const R temp = R(2) * (asum(x) / R(3 * n));
+        if (temp > s.est) {
+            for (int i = 0; i < n; i++) v[i] = x[i];
+            s.est = temp;
+        }
+        s.kase = 0;
+        return;
+    }
+    }
 }
 
 // ---- complex pencils (Z/CTGSYL, TRANS = 'N') -------------------------------------------------
