@@ -190,7 +190,7 @@ int run_ztgsen_full(int nth, int ijob, int n, R *A, R *B, R *Q, R *Z, const int 
     ZPencil<R> p{n, 1, 1, a, b, reinterpret_cast<Cx *>(Q), reinterpret_cast<Cx *>(Z), n, n, n, n};
     ZSortShared<R> shs{};
     ZSylvShared<R> shy{};
-    std::vector<Cx> work((size_t)n * n / 2 + 2);
+    std::vector<Cx> work((size_t)n * n + 2);
     std::vector<int> cuts(n / 2 + 4);
     int info = 0;
     std::barrier<> bar(nth);
@@ -224,6 +224,31 @@ int run_tgsyl_t(int nth, int m, int n, const R *A, const R *B, R *C, const R *D,
     std::barrier<> bar(nth);
     std::vector<std::thread> th;
     for (int t = 0; t < nth; t++) th.emplace_back([&, t] { tgsyl_t_cta(CtaHost{t, nth, &bar}, sh, cuts.data()); });
+    for (auto &x : th) x.join();
+    *scale = sh.scale;
+    return sh.info;
+}
+
+template <class R>
+int run_ztgsyl_c(int nth, int m, int n, const R *A, const R *B, R *C, const R *D, const R *E, R *F, R *scale)
+{
+    using Cx = zc<R>;
+    ZSylvShared<R> sh{};
+    ZSylvG<R> &y = sh.y;
+    y.m = m;
+    y.n = n;
+    y.A = reinterpret_cast<const Cx *>(A);
+    y.D = reinterpret_cast<const Cx *>(D);
+    y.B = reinterpret_cast<const Cx *>(B);
+    y.E = reinterpret_cast<const Cx *>(E);
+    y.lda = y.ldd = y.ldc = y.ldf = m;
+    y.ldb = y.lde = n;
+    y.C = reinterpret_cast<Cx *>(C);
+    y.F = reinterpret_cast<Cx *>(F);
+    std::vector<int> cuts(m / 2 + n / 2 + 4);
+    std::barrier<> bar(nth);
+    std::vector<std::thread> th;
+    for (int t = 0; t < nth; t++) th.emplace_back([&, t] { ztgsyl_c_cta(CtaHost{t, nth, &bar}, sh, cuts.data()); });
     for (auto &x : th) x.join();
     *scale = sh.scale;
     return sh.info;
@@ -321,6 +346,19 @@ int host_stgsyl_t(int nth, int m, int n, const float *A, const float *B, float *
                   float *F, float *scale)
 {
     return run_tgsyl_t(nth, m, n, A, B, C, D, E, F, scale);
+}
+
+// Z/CTGSYL with TRANS = 'C' body
+int host_ztgsyl_c(int nth, int m, int n, const double *A, const double *B, double *C, const double *D,
+                  const double *E, double *F, double *scale)
+{
+    return run_ztgsyl_c(nth, m, n, A, B, C, D, E, F, scale);
+}
+
+int host_ctgsyl_c(int nth, int m, int n, const float *A, const float *B, float *C, const float *D, const float *E,
+                  float *F, float *scale)
+{
+    return run_ztgsyl_c(nth, m, n, A, B, C, D, E, F, scale);
 }
 
 // Z/CTGSYL body (interleaved complex arrays)

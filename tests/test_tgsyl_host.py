@@ -172,8 +172,8 @@ def test_tgsen_estimates_rejection_and_threads(host):
 
 def test_tgsyl_and_tgsen_argument_checks():
     """xtgevc3_dtgsyl's checks (TRANS -1, IJOB -2, M -3, N -4, LDA -6, LDB -8, LDC -10, LDD -12,
-    LDE -14, LDF -16), xtgevc3_dtgsen's of IJOB outside 0..5 and xtgevc3_ztgsen's refusal of the
-    1-norm estimates (IJOB 3, 5), all before any device work."""
+    LDE -14, LDF -16), xtgevc3_d/ztgsen's of IJOB outside 0..5, xtgevc3_ztgsyl's TRANS ('C', not
+    'T'), all before any device work."""
     import xtgevc3_b200 as X
     L = X.lib()
     M = np.zeros((4, 4))
@@ -198,16 +198,16 @@ def test_tgsyl_and_tgsen_argument_checks():
                          ct.byref(m), _p(v), _p(v), _p(v), ct.byref(info))
         assert info.value == -1
     Mc, vc = np.zeros((4, 4), complex), np.zeros(8, complex)
-    for ijob in (3, 5):
+    for ijob in (-1, 6):
         info = ct.c_int(99)
         L.xtgevc3_ztgsen(ijob, 1, 1, _p(sel), 4, _p(Mc), 4, _p(Mc), 4, _p(vc), _p(vc), _p(Mc), 4, _p(Mc), 4,
                          ct.byref(m), _p(v), _p(v), _p(v), ct.byref(info))
         assert info.value == -1
-    for tr, want in ((b"C", -1), (b"N", 0)):
+    for tr, mm, want in ((b"T", 4, -1), (b"C", 0, -3), (b"N", 0, -3)):  # complex: 'C', not 'T'
         info = ct.c_int(99)
-        L.xtgevc3_ztgsyl(tr, 0, 0 if want == 0 else 4, 4, _p(Mc), 4, _p(Mc), 4, _p(Mc), 4, _p(Mc), 4, _p(Mc), 4,
-                         _p(Mc), 4, ct.byref(sc), ct.byref(dif), ct.byref(info))
-        assert info.value == (-3 if want == 0 else -1)
+        L.xtgevc3_ztgsyl(tr, 0, mm, 4, _p(Mc), 4, _p(Mc), 4, _p(Mc), 4, _p(Mc), 4, _p(Mc), 4, _p(Mc), 4,
+                         ct.byref(sc), ct.byref(dif), ct.byref(info))
+        assert info.value == want, (tr, info.value)
 
 
 def host_ztgsen_full(L, ijob, sel, A, B, Q, Z, nth=1):
@@ -313,3 +313,71 @@ def test_tgsen_one_norm_estimates(host, n, seed):
             if ijob == 1:
                 ref[2:] = est[2:] = 0
             assert np.all(np.abs(est - ref) <= 1e-12 * np.abs(ref)), (kind, ijob, est, ref)
+
+
+@pytest.mark.parametrize("dt", [np.complex128, np.complex64], ids=["z", "c"])
+@pytest.mark.parametrize("mn", SIZES, ids=lambda t: f"{t[0]}x{t[1]}")
+def test_complex_tgsyl_conjugate_transposed_matches_lapack(host, dt, mn):
+    """TRANS = 'C': A^H R + D^H L = scale C, R B^H + L E^H = -scale F, equal to LAPACK
+    Z/CTGSYL's within 1e-12 (double) / 2e-4 (single); 1 and 5 host threads bit for bit."""
+    m, n = mn
+    tol = 1e-12 if dt == np.complex128 else 2e-4
+    rt = ct.c_double if dt == np.complex128 else ct.c_float
+    f = host.host_ztgsyl_c if dt == np.complex128 else host.host_ctgsyl_c
+    for seed in range(3):
+        A, B, C, D, E, F = sylv_operands(m, n, seed, dt)
+        rR, rL, rs, _, ri = oracle.lapack_tgsyl("C", 0, A, B, C, D, E, F)
+        outs = []
+        for nth in (1, 5):
+            Cw, Fw = np.array(C, order="F"), np.array(F, order="F")
+            sc = rt(0)
+            info = f(nth, m, n, _p(A), _p(B), _p(Cw), _p(D), _p(E), _p(Fw), ct.byref(sc))
+            assert (info, sc.value) == (ri, rs)
+            for M, R in ((Cw, rR), (Fw, rL)):
+                assert np.abs(M - R).max() <= tol * 10 * max(np.abs(R).max(), 1.0), seed
+            outs.append((Cw, Fw))
+        assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+
+
+def _kron_inv_one_norm(A, D, B, E):
+    """||Z^-1||_1 of the Sylvester operator (R, L) -> (A R - L B, D R - L E), dense"""
+    m, n = A.shape[0], B.shape[0]
+    Im, In = np.eye(m), np.eye(n)
+    Z = np.block([[np.kron(In, A), -np.kron(B.T, Im)], [np.kron(In, D), -np.kron(E.T, Im)]])
+    return np.abs(np.linalg.inv(Z)).sum(0).max()
+
+
+@pytest.mark.parametrize("kind", ["neg_real", "every_third", "none", "all", "last", "first"], ids=str)
+@pytest.mark.parametrize("n,seed", [(8, 3), (12, 5), (30, 12)], ids=["8", "12", "30"])
+def test_complex_tgsen_one_norm_estimates(host, kind, n, seed):
+    """ZTGSEN IJOB 3, 5: PL, PR and DIF(1) (Difu) equal to LAPACK's within 1e-12.  LAPACK's own
+    DIF(2) there is not reproducible (it changes with the contents of the workspace before the
+    call), so DIF(2) is checked against the operator it estimates, (A22, B22 | A11, B11) of the
+    reordered pencil before its normalisation (the operator of DTGSEN's Difl and of ZTGSEN's
+    IJOB 2, 4): a 1-norm estimate never exceeds ||Z^-1||_1, so DIF(2) >= 1 / ||Z^-1||_1, and
+    xLACN2 is exact or close on these orders (within a factor 3)."""
+    from test_tgsen_host import CPLX_SELECTIONS, _cplx_schur
+    S, T, Q, Z, al, be = _cplx_schur(n, seed, np.complex128)
+    sel = CPLX_SELECTIONS[kind](al, be).astype(np.int32)
+    lw = 2 * n * n + 64
+    m = int(sel.sum())
+    for ijob in (3, 5):
+        r = la.ztgsen(sel, S, T, Q, Z, ijob=ijob, lwork=lw, liwork=lw)
+        a, b, q, z, ev, est, mm, info = host_ztgsen_full(host, ijob, sel, S, T, Q, Z)
+        assert (mm, info) == (r[6], r[10]) == (m, 0)
+        if ijob == 5:
+            assert abs(est[0] - r[7]) <= 1e-12 * r[7] and abs(est[1] - r[8]) <= 1e-12 * r[8]
+        if m in (0, n):
+            assert np.allclose(est[2:], r[9], rtol=1e-13)
+            continue
+        assert abs(est[2] - r[9][0]) <= 1e-12 * r[9][0], (est, r[9])
+        if n <= 12:  # the dense operator of Difl on the reordered pencil (LAPACK's moves, before normalisation)
+            A, B = S.copy(order="F"), T.copy(order="F")
+            ks = 0
+            for k in range(1, n + 1):
+                if sel[k - 1]:
+                    ks += 1
+                    if k != ks:
+                        A, B = oracle.lapack_tgexc(A, B, None, None, k, ks)[:2]
+            nrm = _kron_inv_one_norm(A[m:, m:], B[m:, m:], A[:m, :m], B[:m, :m])
+            assert 1 / nrm * (1 - 1e-10) <= est[3] <= 3 / nrm, (est[3], 1 / nrm)

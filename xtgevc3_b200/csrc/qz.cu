@@ -81,16 +81,18 @@ __global__ void __launch_bounds__(kQzThreads, 1)
     if (threadIdx.x == 0) status[0] = i;
 }
 
-// Z/CTGSYL (TRANS = 'N', IJOB 0, 1, 3; rb::ztgsyl_cta): as tgsyl_kernel
+// Z/CTGSYL (TRANS = 'N', IJOB 0, 1, 3: rb::ztgsyl_cta; trans: TRANS = 'C', rb::ztgsyl_c_cta):
+// as tgsyl_kernel
 template <class R>
 __global__ void __launch_bounds__(kQzThreads, 1)
-    ztgsyl_kernel(rb::ZSylvG<R> y, int ijob, int *cuts, rb::zc<R> *work, R *out, int *status)
+    ztgsyl_kernel(rb::ZSylvG<R> y, int trans, int ijob, int *cuts, rb::zc<R> *work, R *out, int *status)
 {
     __shared__ rb::ZSylvShared<R> sh;
     if (threadIdx.x == 0) sh.y = y;
     __syncthreads();
     R dif = out[1];
-    rb::ztgsyl_cta(rb::CtaDev{}, sh, ijob, cuts, work, &dif);
+    if (trans) rb::ztgsyl_c_cta(rb::CtaDev{}, sh, cuts);
+    else rb::ztgsyl_cta(rb::CtaDev{}, sh, ijob, cuts, work, &dif);
     if (threadIdx.x == 0) {
         status[0] = sh.info;
         out[0] = sh.scale;
@@ -453,12 +455,12 @@ void gges_host(char jobvsl, char jobvsr, char sort, SelCplx<R> sel, int n, rb::z
     }
 }
 
-// xTGSEN's argument checks (IJOB 0 to 5 for real pencils; complex: 0, 1, 2, 4, the 1-norm
-// estimates of IJOB 3 and 5 not built, INFO = -1); sets last_error for a bad one
+// xTGSEN's argument checks (IJOB 0 to 5); sets last_error for a bad one
 int tgsen_check(int ijob, int wantq, int wantz, int n, int lda, int ldb, int ldq, int ldz, bool cplx)
 {
     int info = 0;
-    const bool built = ijob >= 0 && ijob <= 5 && (!cplx || (ijob != 3 && ijob != 5));
+    const bool built = ijob >= 0 && ijob <= 5;
+    (void)cplx;
     if (!built) info = -1;
     else if (n < 0) info = -5;
     else if (lda < std::max(1, n)) info = -7;
@@ -466,8 +468,7 @@ int tgsen_check(int ijob, int wantq, int wantz, int n, int lda, int ldb, int ldq
     else if (ldq < 1 || (wantq && ldq < n)) info = cplx ? -13 : -14;
     else if (ldz < 1 || (wantz && ldz < n)) info = cplx ? -15 : -16;
     if (info == -1)
-        set_last_error(ijob < 0 || ijob > 5 ? "xTGSEN: argument 1 has an illegal value"
-                                            : "xTGSEN: complex pencils: IJOB 3 and 5 (1-norm estimates) are not built");
+        set_last_error("xTGSEN: argument 1 has an illegal value");
     else if (info)
         set_last_error("xTGSEN: argument " + std::to_string(-info) + " has an illegal value");
     return info;
@@ -496,7 +497,7 @@ int tgsen_device(cudaStream_t st, int ijob, int wantq, int wantz, const int *sel
     if (CPLX && ijob != 0) {
         int mm = 0;
         for (int k = 0; k < n; k++) mm += bw[k];
-        nwork = 2 * (size_t)mm * (n - mm) * 2;  // complex elements as reals
+        nwork = (ijob == 3 || ijob == 5 ? 4 : 2) * (size_t)mm * (n - mm) * 2;  // complex elements as reals
     }
     if (!CPLX && ijob != 0) {  // M from the subdiagonal (DTGSEN's count), to size the workspace
         std::vector<R> sub(n > 1 ? n - 1 : 1);
@@ -627,14 +628,14 @@ void tgsen_host(int ijob, int wantq, int wantz, const int *select, int n, R *A, 
     }
 }
 
-// LAPACK xTGSYL's argument checks (TRANS = 'N' with IJOB 0, 1, 3 and, for real pencils,
-// TRANS = 'T' (IJOB not referenced, as LAPACK) built; TRANS = 'C' and the xGECON-based IJOB 2,
-// 4 are refused with INFO -1 / -2); sets last_error for a bad one
+// LAPACK xTGSYL's argument checks (TRANS = 'N' with IJOB 0, 1, 3, and TRANS = 'T' (real) /
+// 'C' (complex) with IJOB not referenced, as LAPACK; the xGECON-based IJOB 2, 4 are refused with
+// INFO = -2); sets last_error for a bad one
 int tgsyl_check(char trans, int ijob, int m, int n, int lda, int ldb, int ldc, int ldd, int lde, int ldf,
                 bool cplx = false)
 {
     int info = 0;
-    if (trans != 'N' && (cplx || trans != 'T')) info = -1;
+    if (trans != 'N' && trans != (cplx ? 'C' : 'T')) info = -1;
     else if (trans == 'N' && ijob != 0 && ijob != 1 && ijob != 3) info = -2;
     else if (m <= 0) info = -3;
     else if (n <= 0) info = -4;
@@ -644,9 +645,7 @@ int tgsyl_check(char trans, int ijob, int m, int n, int lda, int ldb, int ldc, i
     else if (ldd < std::max(1, m)) info = -12;
     else if (lde < std::max(1, n)) info = -14;
     else if (ldf < std::max(1, m)) info = -16;
-    if (info == -1 && (trans == 'T' || trans == 'C'))
-        set_last_error("xTGSYL: TRANS = 'C' (complex pencils' conjugate-transposed equation) is not built");
-    else if (info == -2 && (ijob == 2 || ijob == 4))
+    if (info == -2 && (ijob == 2 || ijob == 4))
         set_last_error("xTGSYL: IJOB 2 and 4 (DGECON-based estimates) are not built");
     else if (info)
         set_last_error("xTGSYL: argument " + std::to_string(-info) + " has an illegal value");
@@ -663,7 +662,7 @@ int tgsyl_device(cudaStream_t st, char trans, int ijob, int m, int n, const R *A
     trans = (char)std::toupper((unsigned char)trans);
     *info = tgsyl_check(trans, ijob, m, n, lda, ldb, ldc, ldd, lde, ldf, CPLX);
     if (*info) return 0;
-    if (trans == 'T') ijob = 0;  // not referenced by the transposed solve
+    if (trans != 'N') ijob = 0;  // not referenced by the transposed solve
     const int ncuts = m / 2 + n / 2 + 4;
     const size_t nwork = ijob == 1 ? 2 * (size_t)m * n * (CPLX ? 2 : 1) : 0;
     int *d = nullptr;  // the status, then the cuts
@@ -690,7 +689,8 @@ int tgsyl_device(cudaStream_t st, char trans, int ijob, int m, int n, const R *A
         y.F = reinterpret_cast<Cx *>(F);
         y.ldc = ldc;
         y.ldf = ldf;
-        ztgsyl_kernel<R><<<1, kQzThreads, 0, st>>>(y, ijob, d + 1, reinterpret_cast<Cx *>(w + 2), w, d);
+        ztgsyl_kernel<R><<<1, kQzThreads, 0, st>>>(y, trans == 'C' ? 1 : 0, ijob, d + 1, reinterpret_cast<Cx *>(w + 2),
+                                                    w, d);
         count_launches(1);
         e = cudaGetLastError();
     } else if (e == cudaSuccess) {

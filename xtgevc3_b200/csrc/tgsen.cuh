@@ -461,14 +461,16 @@ XTG_HD int tgsen_cplx_cta(const Cta &c, ZSortShared<R> &sh, const ZPencil<R> &p,
     return info;
 }
 
-// ZTGSEN's estimates (IJOB 1, 2, 4) on the reordered pencil before its normalisation, as
-// tgsen_real_estimates with ZTGSYL.  work: 2 M (n - M) complex elements; cuts n / 2 + 4 ints.
+// ZTGSEN's estimates (IJOB 1 to 5) on the reordered pencil before its normalisation, as
+// tgsen_real_estimates with ZTGSYL (TRANS = 'N' and 'C') and ZLACN2.  work: 4 M (n - M)
+// complex elements (2 M (n - M) for IJOB 1, 2, 4); cuts n / 2 + 4 ints.
 template <class R, class Cta>
 XTG_HD void tgsen_cplx_estimates(const Cta &c, ZSylvShared<R> &sh, const ZPencil<R> &p, int m, int ijob, int info,
                                  zc<R> *work, int *cuts, R *est)
 {
     const int n = p.n, tid = c.tid(), nth = c.nth();
-    const bool wantp = ijob == 1 || ijob == 4, wantd = ijob == 2 || ijob == 4;
+    const bool wantp = ijob == 1 || ijob == 4 || ijob == 5, wantd1 = ijob == 2 || ijob == 4,
+               wantd2 = ijob == 3 || ijob == 5, wantd = wantd1 || wantd2;
     if (tid == 0)
         for (int k = 0; k < 4; k++) est[k] = R(0);
     if (info != 0 || (!wantp && !wantd)) {
@@ -533,11 +535,39 @@ XTG_HD void tgsen_cplx_estimates(const Cta &c, ZSylvShared<R> &sh, const ZPencil
         }
         c.sync();
     }
-    if (wantd) {
+    if (wantd1) {
         setup(n1, n2, A11, B11, A22, B22);
         ztgsyl_cta(c, sh, 3, cuts, (zc<R> *)nullptr, est + 2);
         setup(n2, n1, A22, B22, A11, B11);
         ztgsyl_cta(c, sh, 3, cuts, (zc<R> *)nullptr, est + 3);
+    }
+    if (wantd2) {  // ZLACN2 on [vec C; vec F] = work[0, 2 mn), its v in work[2 mn, 4 mn)
+        const int mn2 = (int)(2 * mn);
+        zc<R> *Vl = work + 2 * mn;
+        for (int which = 0; which < 2; which++) {
+            if (tid == 0) {
+                sh.lac.kase = 0;
+                zlacn2(mn2, Vl, W, sh.lac);
+            }
+            c.sync();
+            R dscale = R(1);
+            for (int step = 0; step < 16; step++) {  // ZLACN2 asks for at most 11 products
+                const int kase = sh.lac.kase;
+                if (kase == 0) break;
+                if (which == 0) setup(n1, n2, A11, B11, A22, B22);
+                else setup(n2, n1, A22, B22, A11, B11);
+                R unused = R(0);
+                if (kase == 1) ztgsyl_cta(c, sh, 0, cuts, (zc<R> *)nullptr, &unused);
+                else ztgsyl_c_cta(c, sh, cuts);
+                if (tid == 0) {
+                    dscale = sh.scale;
+                    zlacn2(mn2, Vl, W, sh.lac);
+                }
+                c.sync();
+            }
+            if (tid == 0) est[2 + which] = dscale / sh.lac.est;
+            c.sync();
+        }
     }
 }
 

@@ -675,10 +675,17 @@ XTG_HD int ztgsy2_sub(ZSylvG<R> &y, int is0, int ie0, int js0, int je0, int ifun
 }
 
 template <class R>
+struct ZLacn2 {
+    int kase, jump, j, iter;
+    R est, estold;
+};
+
+template <class R>
 struct ZSylvShared {
     ZSylvG<R> y;
     R scaloc, scale;
     int info, np, nq;
+    ZLacn2<R> lac;
 };
 
 // One round of ZTGSYL over every block on one CTA (as tgsyl_round).  Ends with a barrier.
@@ -802,6 +809,234 @@ XTG_HD void ztgsyl_cta(const Cta &c, ZSylvShared<R> &sh, int ijob, int *cuts, zc
     }
     if (ijob != 0 && tid == 0 && y.dscale != R(0)) *dif = xsqrt(R(2 * m) * R(n)) / (y.dscale * xsqrt(y.dsum));
     c.sync();
+}
+
+// ---- the conjugate-transposed equation (Z/CTGSYL with TRANS = 'C', IJOB 0) -----------------
+//     A^H R + D^H L = scale C,   R B^H + L E^H = -scale F
+// entries of A top to bottom, of B right to left (within and across the 2 x 2 blocks of
+// rows / columns), each 2 x 2 system Z^H of ZTGSY2, the solution substituted into the rows
+// below (C -= A^H R + D^H L) and the columns left (F += R B^H + L E^H).
+
+template <class R>
+XTG_HD int ztgsy2_sub_c(ZSylvG<R> &y, int is0, int ie0, int js0, int je0, R &scaloc)
+{
+    auto a = [&](int i, int k) { return y.A[(size_t)i + (size_t)k * y.lda]; };
+    auto d = [&](int i, int k) { return y.D[(size_t)i + (size_t)k * y.ldd]; };
+    auto b = [&](int i, int k) { return y.B[(size_t)i + (size_t)k * y.ldb]; };
+    auto e = [&](int i, int k) { return y.E[(size_t)i + (size_t)k * y.lde]; };
+    auto C = [&](int i, int k) -> zc<R> & { return y.C[(size_t)i + (size_t)k * y.ldc]; };
+    auto F = [&](int i, int k) -> zc<R> & { return y.F[(size_t)i + (size_t)k * y.ldf]; };
+    int info = 0;
+    for (int i = is0; i <= ie0; i++)
+        for (int j = je0; j >= js0; j--) {
+            zc<R> Z[4] = {conj(a(i, i)), -conj(b(j, j)), conj(d(i, i)), -conj(e(j, j))}, rhs[2] = {C(i, j), F(i, j)};
+            int ipiv[2], jpiv[2];
+            const int ierr = zgetc2(Z, ipiv, jpiv);
+            if (ierr > 0) info = ierr;
+            R sc = R(1);
+            zgesc2(Z, rhs, ipiv, jpiv, sc);
+            if (sc != R(1)) {
+                for (int k = js0; k <= je0; k++)
+                    for (int r = is0; r <= ie0; r++) {
+                        C(r, k) = sc * C(r, k);
+                        F(r, k) = sc * F(r, k);
+                    }
+                scaloc *= sc;
+            }
+            C(i, j) = rhs[0];
+            F(i, j) = rhs[1];
+            for (int k = js0; k < j; k++) F(i, k) = F(i, k) + rhs[0] * conj(b(k, j)) + rhs[1] * conj(e(k, j));
+            for (int k = i + 1; k <= ie0; k++) C(k, j) = C(k, j) - conj(a(i, k)) * rhs[0] - conj(d(i, k)) * rhs[1];
+        }
+    return info;
+}
+
+template <class R, class Cta>
+XTG_HD void ztgsyl_round_c(const Cta &c, ZSylvShared<R> &sh, const int *rows, const int *cols)
+{
+    const int tid = c.tid(), nth = c.nth();
+    ZSylvG<R> &y = sh.y;
+    const int np = sh.np, nq = sh.nq, m = y.m, n = y.n;
+    for (int ib = 0; ib < np; ib++) {
+        const int is = rows[ib], ie = rows[ib + 1] - 1;
+        for (int jb = nq - 1; jb >= 0; jb--) {
+            const int js = cols[jb], je = cols[jb + 1] - 1;
+            if (tid == 0) {
+                R sl = R(1);
+                const int li = ztgsy2_sub_c(y, is, ie, js, je, sl);
+                if (li > 0) sh.info = li;
+                sh.scaloc = sl;
+            }
+            c.sync();
+            const R sl = sh.scaloc;
+            if (sl != R(1)) {
+                for (size_t t = tid; t < (size_t)m * n; t += nth) {
+                    const int i = (int)(t % m), k = (int)(t / m);
+                    if (k >= js && k <= je && i >= is && i <= ie) continue;
+                    zc<R> &cv = y.C[(size_t)i + (size_t)k * y.ldc];
+                    zc<R> &fv = y.F[(size_t)i + (size_t)k * y.ldf];
+                    cv = sl * cv;
+                    fv = sl * fv;
+                }
+                if (tid == 0) sh.scale *= sl;
+                c.sync();
+            }
+            const int nbk = je - js + 1, mbk = ie - is + 1;
+            const size_t left = (size_t)mbk * js, below = (size_t)(m - 1 - ie) * nbk;
+            for (size_t t = tid; t < left + below; t += nth) {
+                if (t < left) {  // F += R B^H, then F += L E^H
+                    const int i = is + (int)(t % mbk), col = (int)(t / mbk);
+                    zc<R> f = y.F[(size_t)i + (size_t)col * y.ldf];
+                    for (int q = js; q <= je; q++)
+                        f = f + y.C[(size_t)i + (size_t)q * y.ldc] * conj(y.B[(size_t)col + (size_t)q * y.ldb]);
+                    for (int q = js; q <= je; q++)
+                        f = f + y.F[(size_t)i + (size_t)q * y.ldf] * conj(y.E[(size_t)col + (size_t)q * y.lde]);
+                    y.F[(size_t)i + (size_t)col * y.ldf] = f;
+                } else {  // C -= A^H R, then C -= D^H L
+                    const size_t u = t - left;
+                    const int row = ie + 1 + (int)(u % (m - 1 - ie)), k = js + (int)(u / (m - 1 - ie));
+                    zc<R> cv = y.C[(size_t)row + (size_t)k * y.ldc];
+                    for (int p = is; p <= ie; p++)
+                        cv = cv - conj(y.A[(size_t)p + (size_t)row * y.lda]) * y.C[(size_t)p + (size_t)k * y.ldc];
+                    for (int p = is; p <= ie; p++)
+                        cv = cv - conj(y.D[(size_t)p + (size_t)row * y.ldd]) * y.F[(size_t)p + (size_t)k * y.ldf];
+                    y.C[(size_t)row + (size_t)k * y.ldc] = cv;
+                }
+            }
+            c.sync();
+        }
+    }
+}
+
+// Z/CTGSYL with TRANS = 'C' (the solve) on one CTA, as tgsyl_t_cta
+template <class R, class Cta>
+XTG_HD void ztgsyl_c_cta(const Cta &c, ZSylvShared<R> &sh, int *cuts)
+{
+    const int tid = c.tid();
+    ZSylvG<R> &y = sh.y;
+    const int m = y.m, n = y.n;
+    int *rows = cuts, *cols = cuts + m / 2 + 2;
+    if (tid == 0) {
+        if (m <= 2 && n <= 2) {
+            rows[0] = 0;
+            rows[1] = m;
+            cols[0] = 0;
+            cols[1] = n;
+            sh.np = sh.nq = 1;
+        } else {
+            sh.np = ztgsyl_blocks(m, rows);
+            sh.nq = ztgsyl_blocks(n, cols);
+        }
+        sh.info = 0;
+        sh.scale = R(1);
+    }
+    c.sync();
+    ztgsyl_round_c(c, sh, rows, cols);
+}
+
+// ZLACN2 (Higham's estimator for complex operators): as lacn2, with x / |x| (1 where |x| <=
+// safmin) in place of the signs and no repeated-sign test; |.| the modulus throughout.
+template <class R>
+XTG_HD void zlacn2(int n, zc<R> *v, zc<R> *x, ZLacn2<R> &s)
+{
+    const int itmax = 5;
+    const R safmin = Mach<R>::sfmin;
+    const zc<R> one = mk(R(1), R(0)), zero = mk(R(0), R(0));
+    auto asum = [&](const zc<R> *w) {
+        R t = R(0);
+        for (int i = 0; i < n; i++) t += cabs(w[i]);
+        return t;
+    };
+    auto amax = [&]() {
+        int k = 0;
+        R best = cabs(x[0]);
+        for (int i = 1; i < n; i++) {
+            const R v_ = cabs(x[i]);
+            if (v_ > best) {
+                best = v_;
+                k = i;
+            }
+        }
+        return k;
+    };
+    auto phases = [&]() {
+        for (int i = 0; i < n; i++) {
+            const R ax = cabs(x[i]);
+            x[i] = ax > safmin ? mk(x[i].re / ax, x[i].im / ax) : one;
+        }
+    };
+    auto unit = [&]() {
+        for (int i = 0; i < n; i++) x[i] = zero;
+        x[s.j] = one;
+        s.kase = 1;
+        s.jump = 3;
+    };
+    auto final_stage = [&]() {
+        R altsgn = R(1);
+        for (int i = 0; i < n; i++) {
+            x[i] = mk(altsgn * (R(1) + R(i) / R(n - 1)), R(0));
+            altsgn = -altsgn;
+        }
+        s.kase = 1;
+        s.jump = 5;
+    };
+    if (s.kase == 0) {
+        for (int i = 0; i < n; i++) x[i] = mk(R(1) / R(n), R(0));
+        s.kase = 1;
+        s.jump = 1;
+        return;
+    }
+    switch (s.jump) {
+    case 1:
+        if (n == 1) {
+            v[0] = x[0];
+            s.est = cabs(v[0]);
+            s.kase = 0;
+            return;
+        }
+        s.est = asum(x);
+        phases();
+        s.kase = 2;
+        s.jump = 2;
+        return;
+    case 2:
+        s.j = amax();
+        s.iter = 2;
+        unit();
+        return;
+    case 3:
+        for (int i = 0; i < n; i++) v[i] = x[i];
+        s.estold = s.est;
+        s.est = asum(v);
+        if (s.est <= s.estold) {  // cycling: converged
+            final_stage();
+            return;
+        }
+        phases();
+        s.kase = 2;
+        s.jump = 4;
+        return;
+    case 4: {
+        const int jlast = s.j;
+        s.j = amax();
+        if (cabs(x[jlast]) != cabs(x[s.j]) && s.iter < itmax) {
+            s.iter++;
+            unit();
+            return;
+        }
+        final_stage();
+        return;
+    }
+    default: {
+        const R temp = R(2) * (asum(x) / R(3 * n));
+        if (temp > s.est) {
+            for (int i = 0; i < n; i++) v[i] = x[i];
+            s.est = temp;
+        }
+        s.kase = 0;
+        return;
+    }
+    }
 }
 
 }  // namespace rb
