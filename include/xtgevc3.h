@@ -378,13 +378,16 @@ int xtgevc3_sgges_sort_dev(void *stream, char jobvsl, char jobvsr, char sort, xt
  * beta, Q, &ldq, Z, &ldz, &m, &pl, &pr, dif, work, &lwork, iwork, &liwork, &info)`; no
  * workspace arguments).  IJOB 0 (reordering), 1 (PL, PR: the projection norms from xTGSYL's
  * solution of the Sylvester equation of the two diagonal blocks of the reordered pencil), 2
- * (DIF(1:2): xTGSYL's Frobenius-norm estimates of Difu and Difl) and 4 (both); the 1-norm
- * estimates (IJOB 3, 5) are not built (INFO = -1).  pl, pr, dif may be NULL when not wanted.
- * M = 0 or n: PL = PR = 1, DIF = ||(A, B)||_F; a rejected swap: PL = PR = DIF = 0.  Complex
- * pencils: LAPACK's values to rounding (estimated before the rows are normalised, as ZTGSEN
- * does).  Real pencils: DIF depends on the signs of the reordered pencil's columns, which real
- * swaps of 2x2 blocks choose on rounding-level quantities (as LAPACK's), so it can differ from
- * LAPACK's estimate where those signs differ; on the same reordered pencil it is LAPACK's.  The eigenvalues of the reordered pencil as
+ * (DIF(1:2): xTGSYL's Frobenius-norm estimates of Difu and Difl), 3 (DIF(1:2): the 1-norm
+ * estimates, xLACN2 driving solves with TRANS = 'N' and 'T' / 'C'), 4 (1 and 2), 5 (1 and 3).
+ * pl, pr, dif may be NULL when not wanted.  M = 0 or n: PL = PR = 1, DIF = ||(A, B)||_F; a
+ * rejected swap: PL = PR = DIF = 0.  Complex pencils: LAPACK's values to rounding (estimated
+ * before the rows are normalised, as ZTGSEN does), except DIF(2) of IJOB 3, 5, estimated here
+ * on the same operator as DTGSEN's and as IJOB 2, 4 (LAPACK ZTGSEN's value there changes with
+ * the contents of its workspace).  Real pencils: DIF depends on the signs of the reordered
+ * pencil's columns, which real swaps of 2x2 blocks choose on rounding-level quantities (as
+ * LAPACK's), so it can differ from LAPACK's estimate where those signs differ; on the same
+ * reordered pencil it is LAPACK's.  The eigenvalues of the reordered pencil as
  * xTGSEN returns them (real: xLAG2 on each 2x2 block, 1x1 blocks with B(k, k) made
  * non-negative by negating row k of A and B and column k of Q; complex: when 0 < M < n and
  * every swap was done, each row scaled so that B(k, k) is real and non-negative, Q's columns
@@ -419,14 +422,15 @@ int xtgevc3_ctgsen_dev(void *stream, int ijob, int wantq, int wantz, const int *
                        float *B, int ldb, float *alpha, float *beta, float *Q, int ldq, float *Z, int ldz, int *m,
                        float *pl, float *pr, float *dif, int *info);
 
-/* LAPACK D/S/Z/CTGSYL with TRANS = 'N': the generalized Sylvester equation A R - L B = scale C,
- * D R - L E = scale F of two generalized Schur pencils (A, D) m x m, (B, E) n x n; C, F
+/* LAPACK D/S/Z/CTGSYL: the generalized Sylvester equation A R - L B = scale C, D R - L E =
+ * scale F (TRANS = 'N'), or A^T R + D^T L = scale C, R B^T + L E^T = -scale F (TRANS = 'T', real;
+ * 'C' with ^H, complex) of two generalized Schur pencils (A, D) m x m, (B, E) n x n; C, F
  * (m x n) overwritten by R, L (replacing `dtgsyl_(&trans, &ijob, &m, &n, A, &lda, B, &ldb, C,
  * &ldc, D, &ldd, E, &lde, F, &ldf, &scale, &dif, work, &lwork, iwork, &info)`; no workspace).
  * IJOB 0 solves, 1 solves and estimates DIF, 3 only estimates DIF (xLATDF's look-ahead, the
  * Frobenius-norm estimate; C, F zeroed), in xTGSYL's blocked order so that the solution and
- * the estimate are LAPACK's to rounding.  TRANS = 'T' / 'C' (INFO = -1) and the xGECON-based
- * IJOB 2, 4 (INFO = -2) are not built.  Complex arrays interleaved.  INFO: -1 .. -16 as LAPACK numbers its arguments (M, N >= 1), >
+ * the estimate are LAPACK's to rounding; the transposed solves ignore IJOB, as LAPACK's.  The
+ * xGECON-based IJOB 2, 4 (INFO = -2) are not built.  Complex arrays interleaved.  INFO: -1 .. -16 as LAPACK numbers its arguments (M, N >= 1), >
  * 0 when a pivot of a small system was raised (the solution then perturbed, as LAPACK's),
  * m + n + 1 (not a LAPACK value) when a CUDA call failed in the host-pointer form.  One CTA;
  * device form: every array a device pointer, scale and dif host pointers.                    */
