@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--z-n", type=int, default=4096, help="order of the ztgevc3 SIDE=R HOWMNY=A leg (0 skips)")
     ap.add_argument("--trevc3-n", type=int, default=8192, help="order of the dtrevc3 SIDE=B HOWMNY=B leg (0 skips)")
     ap.add_argument("--tgexc-n", type=int, default=4096, help="order of the ztgexc and dtgexc reordering legs (0 skips)")
+    ap.add_argument("--tgsen-n", type=int, default=0,
+                    help="order of the dtgsen IJOB=4 leg beside LAPACK dtgsen; 0 (the default) skips it")
     ap.add_argument("--tgsna-n", type=int, default=0,
                     help="order of the dtgsna DIF leg beside LAPACK dtgsna JOB='V'; 0 (the default) skips it")
     ap.add_argument("--reference-table", action="store_true",
@@ -888,6 +890,54 @@ def measure_gges(args, X, torch):
     return out
 
 
+def measure_tgsen(args, X, torch):
+    """dtgsen IJOB = 4 (reordering with PL, PR and the Frobenius-norm DIF estimates) on a real
+    generalized Schur stand-in of order --tgsen-n (xGGES statistics), the eigenvalues of the left
+    half-plane selected, Q and Z updated: device-resident inputs restored before each step
+    outside the timed region, CUDA-event timing of xtgevc3_dtgsen_dev; LAPACK DTGSEN (SciPy's
+    OpenBLAS) on the same pencil beside it, with M, PL, PR and the DIF ratio compared."""
+    from xtgevc3_b200 import pencils as gen
+    import scipy.linalg.lapack as la
+    n = args.tgsen_n
+    S_h, P_h = gen.gen_schur_like(n, args.seed + 61)[:2]
+    Q_h = Z_h = np.asfortranarray(np.eye(n))
+    ar = np.diag(S_h).copy()
+    for k in range(n - 1):  # the real parts of the pairs, from the 2x2 blocks' trace / 2
+        if S_h[k + 1, k] != 0:
+            ar[k] = ar[k + 1] = 0.5 * (S_h[k, k] / P_h[k, k] + S_h[k + 1, k + 1] / P_h[k + 1, k + 1])
+    sel = (ar * np.sign(np.diag(P_h)) < 0).astype(np.int32)
+    tensors = [colmajor_cuda(M, torch) for M in (S_h, P_h, Q_h, Z_h)]
+    work = [torch.empty_like(t) for t in tensors]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ts, res = [], None
+    for it in range(max(args.warmup, 1) + args.steps):
+        for w, t in zip(work, tensors):
+            w.copy_(t)
+        torch.cuda.synchronize()
+        e0.record()
+        res = X.tgsen_dev(sel, *work, ijob=4)
+        e1.record()
+        torch.cuda.synchronize()
+        if it >= max(args.warmup, 1):
+            ts.append(e0.elapsed_time(e1))
+    ms = float(np.mean(ts))
+    m, pl, pr, dif, info = res[3:]
+    out = {"n": n, "ms": ms, "ijob": 4, "m": int(m), "info": int(info), "pl": pl, "pr": pr, "dif": [float(v) for v in dif],
+           "data": "real generalized Schur stand-in (xGGES statistics), left half-plane selected, Q = Z = I"}
+    if not args.no_cpu:
+        lw = max(4 * n + 16, 2 * int(m) * (n - int(m))) + 64
+        t0 = time.perf_counter()
+        r = la.dtgsen(sel, S_h, P_h, Q_h, Z_h, ijob=4, lwork=lw, liwork=n + 64)
+        tc = time.perf_counter() - t0
+        out["cpu_lapack"] = {"seconds": tc, "cores": host_threads(), "kind": "LAPACK dtgsen IJOB=4 (SciPy OpenBLAS)"}
+        out["speedup_vs_lapack"] = tc / (ms * 1e-3)
+        out["m_equal"] = int(r[7]) == int(m)
+        out["pl_pr_rel_diff"] = float(max(abs(pl - r[8]) / r[8], abs(pr - r[9]) / r[9])) if r[8] > 0 else None
+        out["dif_ratio_to_lapack"] = [float(a / b) for a, b in zip(dif, r[10])]
+    del tensors, work
+    return out
+
+
 def measure_tgsna_dif(args, X, torch):
     """dtgsna JOB='V' (DIF of every eigenvalue) on a real generalized Schur stand-in of order
     --tgsna-n (xGGES statistics): CUDA-event timing of xtgevc3_dtgsna_dif_dev on device-resident
@@ -1421,6 +1471,7 @@ def main():
     bxleg = measure_tgexc_blocks(args, X, torch) if args.tgexc_n > 0 and rank == 0 else None
     qzleg = measure_gges(args, X, torch) if args.gges_n > 0 and rank == 0 else None
     difleg = measure_tgsna_dif(args, X, torch) if args.tgsna_n > 0 and rank == 0 else None
+    senleg = measure_tgsen(args, X, torch) if args.tgsen_n > 0 and rank == 0 else None
 
     if rank == 0:
         form_desc = {"plain": "plain FP64 (DMMA)", "split": f"split precision, {s} BF16 slices (tcgen05)",
@@ -1455,7 +1506,7 @@ def main():
                                "ms": norm["ms_per_call"], "gbs": norm["gbs"], "frac_of_hbm": norm["frac_of_hbm"]},
                            "neighbours": neighbours_brief({"ztgexc": txleg, "dtgexc": dxleg, "dtgexc_blocks": bxleg,
                                                            "dtrevc3": trleg, "adjoint": adjoint, "dgges": qzleg,
-                                                           "dtgsna_dif": difleg}),
+                                                           "dtgsna_dif": difleg, "dtgsen": senleg}),
                            "batched": None if batched is None else {
                                "pencils_per_s": batched["value"], "speedup_vs_loop": batched["speedup_vs_loop"],
                                "d_ms": batched["d"]["ms"], "s_ms": batched["s"]["ms"],
@@ -1463,7 +1514,7 @@ def main():
                 "forms": forms_out, "clocks": h["clocks"], "e2e": e2e, "gpu_launches": h["launches"],
                 "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "normalize": norm, "batched": batched,
                 "adjoint": adjoint, "ztgevc3": zleg, "dtrevc3": trleg, "ztgexc": txleg, "dtgexc": dxleg,
-                "dtgexc_blocks": bxleg, "dgges": qzleg, "dtgsna_dif": difleg}
+                "dtgexc_blocks": bxleg, "dgges": qzleg, "dtgsna_dif": difleg, "dtgsen": senleg}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
