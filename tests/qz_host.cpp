@@ -10,6 +10,7 @@
 #include "../xtgevc3_b200/csrc/qz_real.cuh"
 #include "../xtgevc3_b200/csrc/tgsen.cuh"
 #include "../xtgevc3_b200/csrc/tgsyl.cuh"
+#include "../xtgevc3_b200/csrc/gges_scale.h"
 
 using namespace xtg::rb;
 
@@ -372,6 +373,56 @@ int host_ctgsyl(int nth, int ijob, int m, int n, const float *A, const float *B,
                 const float *E, float *F, float *scale, float *dif)
 {
     return run_ztgsyl(nth, ijob, m, n, A, B, C, D, E, F, scale, dif);
+}
+
+// xLASCL's steps (gges_scale.h) applied to x[0, count): returns the number of factors
+int host_dlascl(double cfrom, double cto, int count, double *x)
+{
+    double mul[8];
+    const int k = xtg::gs::lascl_steps(cfrom, cto, mul);
+    xtg::gs::lascl_apply(k, mul, x, (size_t)count);
+    return k;
+}
+
+// xGGES's scaling decision for a norm (gges_scale.h): 1 and *to when the pencil is scaled
+int host_gges_needs_scaling(double nrm, double *to) { return xtg::gs::needs_scaling(nrm, to) ? 1 : 0; }
+
+// xGGES's scaling back on host arrays (the steps of gges_scale_out without the device):
+// DGGES's pair guard, the eigenvalues, A upper Hessenberg (real) / upper triangular (complex,
+// cplx = 1: interleaved arrays), B upper triangular
+int host_gges_scale_out(int cplx, int n, double *A, double *B, double *ev0, double *ev1, double *ev2, int ilascl,
+                        double anrm, double anrmto, int ilbscl, double bnrm, double bnrmto)
+{
+    const int cw = cplx ? 2 : 1;
+    if (!cplx && (ilascl || ilbscl)) {
+        std::vector<double> aii(n), aii1(n), bii(n);
+        for (int i = 0; i < n; i++) {
+            aii[i] = A[i + (size_t)i * n];
+            aii1[i] = i + 1 < n ? A[i + (size_t)(i + 1) * n] : 0.0;
+            bii[i] = B[i + (size_t)i * n];
+        }
+        xtg::gs::pair_guard(n, ilascl != 0, anrm, anrmto, ilbscl != 0, bnrm, bnrmto, aii.data(), aii1.data(),
+                            bii.data(), ev0, ev1, ev2);
+    }
+    double f[8];
+    for (int w = 0; w < 2; w++) {
+        if (!(w == 0 ? ilascl : ilbscl)) continue;
+        const int k = xtg::gs::lascl_steps(w == 0 ? anrmto : bnrmto, w == 0 ? anrm : bnrm, f);
+        double *M = w == 0 ? A : B;
+        const int kind = (w == 0 && !cplx) ? 2 : 1;
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < n; i++) {
+                if ((kind == 1 && i > j) || (kind == 2 && i > j + 1)) continue;
+                xtg::gs::lascl_apply(k, f, M + ((size_t)i + (size_t)j * n) * cw, cw);
+            }
+        if (w == 0) {
+            xtg::gs::lascl_apply(k, f, ev0, (size_t)n * cw);
+            if (!cplx) xtg::gs::lascl_apply(k, f, ev1, (size_t)n);
+        } else {
+            xtg::gs::lascl_apply(k, f, cplx ? ev1 : ev2, (size_t)n * cw);
+        }
+    }
+    return 0;
 }
 
 // xGGES's check: SELCTG's answers as flags in order; returns SDIM, *info as the check leaves it

@@ -129,3 +129,38 @@ def test_real_schur_form_then_eigenvectors_on_the_device(cuda_ok):
         assert np.abs(be[k] * (A @ x) - a * (B @ x)).max() <= 1e-12 * scale * np.abs(x).max()
         assert np.abs(be[k] * (y.conj() @ A) - a * (y.conj() @ B)).max() <= 1e-12 * scale * np.abs(y).max()
         k += w
+
+
+@pytest.mark.parametrize("sa,sb", [(1e200, 1.0), (1e-200, 1.0), (1.0, 1e200), (1e200, 1e-200)],
+                         ids=["A_huge", "A_tiny", "B_huge", "both"])
+@pytest.mark.parametrize("cplx", [False, True], ids=["d", "z"])
+def test_gges_scales_badly_scaled_pencils(cuda_ok, sa, sb, cplx):
+    """xGGES's scaling on the device (the pencils of tests/test_gges_scale_host.py, where the same
+    flow runs on host arrays): LAPACK's eigenvalues (relative 1e-9, compared as (alpha / sa) /
+    (beta / sb)), A = Q S Z^H and B = Q T Z^H to 1e-12 n, everything finite."""
+    import scipy.linalg.lapack as la
+    n = 24
+    rng = np.random.default_rng(9)
+    A0, B0 = rng.standard_normal((n, n)), rng.standard_normal((n, n))
+    if cplx:
+        A0, B0 = A0 + 1j * rng.standard_normal((n, n)), B0 + 1j * rng.standard_normal((n, n))
+    A, B = A0 * sa, B0 * sb
+    out = X.gges(A, B)
+    if cplx:
+        S, T, al, be, Q, Z, info = out
+        r = la.zgges(lambda a, b: 0, A, B)
+        lam, lam_r = (al / sa) / (be / sb), (r[3] / sa) / (r[4] / sb)
+        ev = (al, be)
+    else:
+        S, T, ar, ai, be, Q, Z, info = out
+        r = la.dgges(lambda x, y, z: 0, A, B)
+        lam, lam_r = ((ar + 1j * ai) / sa) / (be / sb), ((r[3] + 1j * r[4]) / sa) / (r[5] / sb)
+        ev = (ar, ai, be)
+    assert info == 0
+    for M in (S, T, Q, Z, *ev):
+        assert np.all(np.isfinite(M))
+    for x, y in ((lam, lam_r), (lam_r, lam)):
+        d = np.abs(x[:, None] - y[None, :]).min(1) / np.abs(x)
+        assert d.max() <= 1e-9, d.max()
+    for M, M0 in ((S, A), (T, B)):
+        assert np.abs(Q @ M @ Z.conj().T - M0).max() <= 1e-12 * n * np.abs(M0).max()

@@ -11,11 +11,13 @@
 #include "../../include/xtgevc3.h"
 #include "common.cuh"
 #include "engine.cuh"
+#include "gges_scale.h"
 #include "qz_real.cuh"
 #include "tgsen.cuh"
 
 #include <algorithm>
 #include <cctype>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -128,6 +130,178 @@ __global__ void __launch_bounds__(kQzThreads, 1)
     if (threadIdx.x == 0) *info = i;
 }
 
+// ---- xGGES's scaling of the pencil (gges_scale.h) on the device ------------------------------
+
+__device__ __forceinline__ double modulus_(double x) { return fabs(x); }
+__device__ __forceinline__ double modulus_(float x) { return (double)fabsf(x); }
+template <class R>
+__device__ __forceinline__ double modulus_(rb::zc<R> x) { return (double)rb::cabs(x); }
+
+// Largest modulus of the n x n matrix A (xLANGE 'M') as the bits of a non-negative double
+// (integer order of those bits is their numeric order) into *bits; any NaN sets *nan
+template <class E>
+__global__ void __launch_bounds__(256) maxabs_kernel(const E *A, int lda, int n, unsigned long long *bits, int *nan)
+{
+    double mx = 0.0;
+    int bad = 0;
+    const size_t total = (size_t)n * n;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const double v = modulus_(A[(t % n) + (t / n) * (size_t)lda]);
+        if (v != v) bad = 1;
+        else if (v > mx) mx = v;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(bits, (unsigned long long)__double_as_longlong(mx));
+        if (bad) atomicExch(nan, 1);
+    }
+}
+
+template <class R>
+struct Muls {
+    R f[8];
+    int k;
+};
+
+__device__ __forceinline__ void scale_(double &x, double f) { x *= f; }
+__device__ __forceinline__ void scale_(float &x, float f) { x *= f; }
+template <class R>
+__device__ __forceinline__ void scale_(rb::zc<R> &x, R f)
+{
+    x.re *= f;
+    x.im *= f;
+}
+
+// xLASCL's multiplications of the entries of A in region kind (0 all, 1 upper triangle, 2 upper
+// Hessenberg), factor after factor
+template <class E, class R>
+__global__ void __launch_bounds__(256) lascl_kernel(E *A, int lda, int n, int kind, Muls<R> m)
+{
+    const size_t total = (size_t)n * n;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(t % n), j = (int)(t / n);
+        if ((kind == 1 && i > j) || (kind == 2 && i > j + 1)) continue;
+        E v = A[(size_t)i + (size_t)j * lda];
+        for (int s = 0; s < m.k; s++) scale_(v, m.f[s]);
+        A[(size_t)i + (size_t)j * lda] = v;
+    }
+}
+
+// The scaling decisions of xGGES for one run
+template <class R>
+struct GgesScale {
+    bool ilascl = false, ilbscl = false;
+    R anrm = R(0), anrmto = R(0), bnrm = R(0), bnrmto = R(0);
+};
+
+constexpr int kScaleGrid = 4 * 148;
+
+// xGGES's first step: the largest moduli of A and B; A, B scaled into [smlnum, bignum] where
+// they lie outside it (a NaN anywhere leaves the pencil as it is, as xLANGE's NaN does)
+template <class E, class R>
+cudaError_t gges_scale_in(cudaStream_t st, int n, E *A, int lda, E *B, int ldb, GgesScale<R> &g)
+{
+    unsigned long long *d = nullptr;  // bits of |A|max, |B|max, then the two NaN flags
+    cudaError_t e = cudaMallocAsync(&d, 3 * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    unsigned long long h[3] = {0, 0, 0};
+    e = cudaMemsetAsync(d, 0, 3 * sizeof(unsigned long long), st);
+    if (e == cudaSuccess) {
+        int *nan = reinterpret_cast<int *>(d + 2);
+        maxabs_kernel<E><<<kScaleGrid, 256, 0, st>>>(A, lda, n, d, nan);
+        maxabs_kernel<E><<<kScaleGrid, 256, 0, st>>>(B, ldb, n, d + 1, nan + 1);
+        count_launches(2);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFreeAsync(d, st);
+    if (e != cudaSuccess) return e;
+    const int *nan = reinterpret_cast<const int *>(h + 2);
+    double an, bn;
+    memcpy(&an, &h[0], sizeof(double));
+    memcpy(&bn, &h[1], sizeof(double));
+    g.anrm = (R)an;
+    g.bnrm = (R)bn;
+    g.ilascl = !nan[0] && gs::needs_scaling(g.anrm, &g.anrmto);
+    g.ilbscl = !nan[1] && gs::needs_scaling(g.bnrm, &g.bnrmto);
+    for (int w = 0; w < 2 && e == cudaSuccess; w++) {
+        if (!(w == 0 ? g.ilascl : g.ilbscl)) continue;
+        Muls<R> m;
+        m.k = gs::lascl_steps(w == 0 ? g.anrm : g.bnrm, w == 0 ? g.anrmto : g.bnrmto, m.f);
+        lascl_kernel<E, R><<<kScaleGrid, 256, 0, st>>>(w == 0 ? A : B, w == 0 ? lda : ldb, n, 0, m);
+        count_launches(1);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
+// the scaled-back eigenvalue copies SELCTG sees (xGGES undoes the scaling before selecting)
+template <class R>
+void gges_unscale_host(const GgesScale<R> &g, int n, R *a0, R *a1, R *b, int cw)
+{
+    R f[8];
+    if (g.ilascl) {
+        const int k = gs::lascl_steps(g.anrmto, g.anrm, f);
+        gs::lascl_apply(k, f, a0, (size_t)n * cw);
+        if (a1) gs::lascl_apply(k, f, a1, (size_t)n * cw);
+    }
+    if (g.ilbscl) {
+        const int k = gs::lascl_steps(g.bnrmto, g.bnrm, f);
+        gs::lascl_apply(k, f, b, (size_t)n * cw);
+    }
+}
+
+// xGGES's last step: the Schur form and the eigenvalues scaled back (real: A upper Hessenberg,
+// after DGGES's guard of complex pairs; complex: A upper triangular); B upper triangular
+template <class E, class R>
+cudaError_t gges_scale_out(cudaStream_t st, int n, E *A, int lda, E *B, int ldb, E *ev0, E *ev1, E *ev2,
+                           const GgesScale<R> &g)
+{
+    if (!g.ilascl && !g.ilbscl) return cudaSuccess;
+    constexpr bool cplx = sizeof(E) == 2 * sizeof(R);
+    constexpr int cw = cplx ? 2 : 1;
+    const int nev = cplx ? 2 : 3;
+    std::vector<R> h((size_t)3 * n * cw);
+    E *dv[3] = {ev0, ev1, ev2};
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < nev && e == cudaSuccess; k++)
+        e = cudaMemcpyAsync(h.data() + (size_t)k * n * cw, dv[k], n * sizeof(E), cudaMemcpyDeviceToHost, st);
+    std::vector<R> aii(n), aii1(n), bii(n);
+    if (!cplx && e == cudaSuccess) {  // A(i, i), A(i, i + 1), B(i, i) for DGGES's guard
+        e = cudaMemcpy2DAsync(aii.data(), sizeof(R), A, (size_t)(lda + 1) * sizeof(R), sizeof(R), n,
+                              cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && n > 1)
+            e = cudaMemcpy2DAsync(aii1.data(), sizeof(R), reinterpret_cast<const R *>(A) + lda,
+                                  (size_t)(lda + 1) * sizeof(R), sizeof(R), n - 1, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(bii.data(), sizeof(R), B, (size_t)(ldb + 1) * sizeof(R), sizeof(R), n,
+                                  cudaMemcpyDeviceToHost, st);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+    R *a0 = h.data(), *a1 = cplx ? nullptr : h.data() + n, *b = h.data() + (size_t)(cplx ? 1 : 2) * n * cw;
+    if (!cplx) gs::pair_guard(n, g.ilascl, g.anrm, g.anrmto, g.ilbscl, g.bnrm, g.bnrmto, aii.data(), aii1.data(),
+                              bii.data(), a0, a1, b);
+    gges_unscale_host(g, n, a0, a1, b, cw);
+    for (int k = 0; k < nev && e == cudaSuccess; k++)
+        e = cudaMemcpyAsync(dv[k], h.data() + (size_t)k * n * cw, n * sizeof(E), cudaMemcpyHostToDevice, st);
+    for (int w = 0; w < 2 && e == cudaSuccess; w++) {
+        if (!(w == 0 ? g.ilascl : g.ilbscl)) continue;
+        Muls<R> m;
+        m.k = gs::lascl_steps(w == 0 ? g.anrmto : g.bnrmto, w == 0 ? g.anrm : g.bnrm, m.f);
+        lascl_kernel<E, R><<<kScaleGrid, 256, 0, st>>>(w == 0 ? A : B, w == 0 ? lda : ldb, n,
+                                                       (w == 0 && !cplx) ? 2 : 1, m);
+        count_launches(1);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e;
+}
+
 // SELCTG of real and complex xGGES (nonzero: selected); complex values as (re, im) pairs
 template <class R>
 using SelReal = int (*)(const R *, const R *, const R *);
@@ -175,14 +349,13 @@ cudaError_t run_tgsen(cudaStream_t st, const std::vector<int> &bw, int *status, 
     return e;
 }
 
-// xGGES's ordering step for real pencils (QZ done, INFO 0): SELCTG over the QZ eigenvalues,
-// DTGSEN (IJOB = 0) on the device, then DGGES's check of the new eigenvalues: SDIM counts the
-// selected ones (a pair counts 2 when either of its values, or the one before, is
-// selected), INFO = n + 3 when a swap was rejected, n + 2 when a selected eigenvalue follows
-// one that is not (rounding in the reordering changed a selection).
+// xGGES's ordering step for real pencils (QZ done, INFO 0): SELCTG over the QZ eigenvalues
+// (scaled back first, as DGGES does), DTGSEN (IJOB = 0) on the device (INFO = n + 3 when a
+// swap was rejected).  DGGES's check of the new eigenvalues (gges_check_real) follows the
+// scaling back of the Schur form.
 template <class R>
 cudaError_t gges_sort_real(cudaStream_t st, SelReal<R> sel, const rb::Pencil<R> &p, R *alphar, R *alphai, R *beta,
-                           int *sdim, int *info)
+                           const GgesScale<R> &g, int *info)
 {
     const int n = p.n;
     std::vector<R> h(3 * (size_t)n);
@@ -192,27 +365,42 @@ cudaError_t gges_sort_real(cudaStream_t st, SelReal<R> sel, const rb::Pencil<R> 
         e = cudaMemcpyAsync(h.data() + (size_t)k * n, dv[k], n * sizeof(R), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return e;
+    gges_unscale_host(g, n, h.data(), h.data() + n, h.data() + 2 * (size_t)n, 1);
     std::vector<int> bw(n);
     for (int i = 0; i < n; i++) bw[i] = sel(&h[i], &h[n + i], &h[2 * (size_t)n + i]) != 0 ? 1 : 0;
     int status = 0;
     e = run_tgsen(st, bw, &status, [&](int *d_sel, int *d_status) {
         tgsen_real_kernel<R><<<1, kQzThreads, 0, st>>>(p, d_sel, alphar, alphai, beta, d_status);
     });
+    if (e != cudaSuccess) return e;
+    if (status != 0) *info = n + 3;
+    if (status == 3) set_last_error("xGGES: the reordering walk did not end within its swap bound");
+    return cudaSuccess;
+}
+
+// DGGES's check of the final eigenvalues: SDIM counts the selected ones (a pair counts 2 when
+// either of its values is selected), INFO = n + 2 when a selected eigenvalue follows one that
+// is not (rounding in the reordering changed a selection)
+template <class R>
+cudaError_t gges_check_real(cudaStream_t st, SelReal<R> sel, int n, const R *alphar, const R *alphai, const R *beta,
+                            int *sdim, int *info)
+{
+    std::vector<R> h(3 * (size_t)n);
+    const R *dv[3] = {alphar, alphai, beta};
+    cudaError_t e = cudaSuccess;
     for (int k = 0; k < 3 && e == cudaSuccess; k++)
         e = cudaMemcpyAsync(h.data() + (size_t)k * n, dv[k], n * sizeof(R), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return e;
-    if (status != 0) *info = n + 3;
-    if (status == 3) set_last_error("xGGES: the reordering walk did not end within its swap bound");
     *sdim = rb::gges_sdim_real(n, sel, h.data(), h.data() + n, h.data() + 2 * (size_t)n, info);
     return cudaSuccess;
 }
 
-// The same for complex pencils: ZTGSEN (IJOB = 0) on the device, then ZGGES's check (SDIM
-// counts the selected eigenvalues, INFO = n + 3 / n + 2 as for real pencils).
+// The same for complex pencils: ZTGSEN (IJOB = 0) on the device (INFO = n + 3 as for real
+// pencils); ZGGES's check (gges_check_cplx) after the scaling back.
 template <class R>
 cudaError_t gges_sort_cplx(cudaStream_t st, SelCplx<R> sel, const rb::ZPencil<R> &p, rb::zc<R> *alpha,
-                           rb::zc<R> *beta, int *sdim, int *info)
+                           rb::zc<R> *beta, const GgesScale<R> &g, int *info)
 {
     using C = rb::zc<R>;
     const int n = p.n;
@@ -221,17 +409,28 @@ cudaError_t gges_sort_cplx(cudaStream_t st, SelCplx<R> sel, const rb::ZPencil<R>
     if (e == cudaSuccess) e = cudaMemcpyAsync(h.data() + n, beta, n * sizeof(C), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return e;
+    gges_unscale_host(g, n, &h[0].re, (R *)nullptr, &h[n].re, 2);
     std::vector<int> bw(n);
     for (int i = 0; i < n; i++) bw[i] = sel(&h[i].re, &h[n + i].re) != 0 ? 1 : 0;
     int status = 0;
     e = run_tgsen(st, bw, &status, [&](int *d_sel, int *d_status) {
         tgsen_cplx_kernel<R><<<1, kQzThreads, 0, st>>>(p, d_sel, alpha, beta, d_status);
     });
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), alpha, n * sizeof(C), cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return e;
+    if (status != 0) *info = n + 3;
+    return cudaSuccess;
+}
+
+template <class R>
+cudaError_t gges_check_cplx(cudaStream_t st, SelCplx<R> sel, int n, const rb::zc<R> *alpha, const rb::zc<R> *beta,
+                            int *sdim, int *info)
+{
+    using C = rb::zc<R>;
+    std::vector<C> h(2 * (size_t)n);
+    cudaError_t e = cudaMemcpyAsync(h.data(), alpha, n * sizeof(C), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(h.data() + n, beta, n * sizeof(C), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return e;
-    if (status != 0) *info = n + 3;
     *sdim = rb::gges_sdim_cplx(n, sel, h.data(), h.data() + n, info);
     return cudaSuccess;
 }
@@ -256,7 +455,9 @@ int gges_device_real(cudaStream_t st, char jobvsl, char jobvsr, char sort, SelRe
     if (n == 0) return 0;
     const int wl = jobvsl == 'V', wr = jobvsr == 'V';
     int *d_info = nullptr, h_info = 0;
-    cudaError_t e = cudaMallocAsync(&d_info, sizeof(int), st);
+    GgesScale<R> g;
+    cudaError_t e = gges_scale_in<R, R>(st, n, A, lda, B, ldb, g);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d_info, sizeof(int), st);
     if (e == cudaSuccess) {
         // Q and Z are not referenced when not wanted
         rb::QzPencilR<R> p{n,   wl,  wr,  A,      B,      wl ? VSL : A, wr ? VSR : A, lda, ldb, wl ? ldvsl : lda,
@@ -268,11 +469,17 @@ int gges_device_real(cudaStream_t st, char jobvsl, char jobvsr, char sort, SelRe
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         cudaFreeAsync(d_info, st);
         *info = h_info;
-        if (e == cudaSuccess && sort == 'S' && h_info == 0) {
-            const rb::Pencil<R> q{n, wl, wr, A, B, p.Q, p.Z, lda, ldb, p.ldq, p.ldz};
-            int sd = 0;
-            e = gges_sort_real<R>(st, sel, q, alphar, alphai, beta, &sd, info);
-            if (sdim) *sdim = sd;
+        if (e == cudaSuccess && h_info == 0) {  // a QZ failure leaves the pencil scaled, as DGGES
+            if (sort == 'S') {
+                const rb::Pencil<R> q{n, wl, wr, A, B, p.Q, p.Z, lda, ldb, p.ldq, p.ldz};
+                e = gges_sort_real<R>(st, sel, q, alphar, alphai, beta, g, info);
+            }
+            if (e == cudaSuccess) e = gges_scale_out<R, R>(st, n, A, lda, B, ldb, alphar, alphai, beta, g);
+            if (e == cudaSuccess && sort == 'S') {
+                int sd = 0;
+                e = gges_check_real<R>(st, sel, n, alphar, alphai, beta, &sd, info);
+                if (sdim) *sdim = sd;
+            }
         }
     }
     if (e != cudaSuccess) {
@@ -366,7 +573,9 @@ int gges_device(cudaStream_t st, char jobvsl, char jobvsr, char sort, SelCplx<R>
     if (n == 0) return 0;
     const int wl = jobvsl == 'V', wr = jobvsr == 'V';
     int *d_info = nullptr, h_info = 0;
-    cudaError_t e = cudaMallocAsync(&d_info, sizeof(int), st);
+    GgesScale<R> g;
+    cudaError_t e = gges_scale_in<rb::zc<R>, R>(st, n, A, lda, B, ldb, g);
+    if (e == cudaSuccess) e = cudaMallocAsync(&d_info, sizeof(int), st);
     if (e == cudaSuccess) {
         // Q and Z are not referenced when not wanted
         rb::QzPencil<R> p{n, wl, wr, A, B, wl ? VSL : A, wr ? VSR : A, lda, ldb, wl ? ldvsl : lda, wr ? ldvsr : lda};
@@ -377,11 +586,18 @@ int gges_device(cudaStream_t st, char jobvsl, char jobvsr, char sort, SelCplx<R>
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         cudaFreeAsync(d_info, st);
         *info = h_info;
-        if (e == cudaSuccess && sort == 'S' && h_info == 0) {
-            const rb::ZPencil<R> q{n, wl, wr, A, B, p.Q, p.Z, lda, ldb, p.ldq, p.ldz};
-            int sd = 0;
-            e = gges_sort_cplx<R>(st, sel, q, alpha, beta, &sd, info);
-            if (sdim) *sdim = sd;
+        if (e == cudaSuccess && h_info == 0) {  // a QZ failure leaves the pencil scaled, as ZGGES
+            if (sort == 'S') {
+                const rb::ZPencil<R> q{n, wl, wr, A, B, p.Q, p.Z, lda, ldb, p.ldq, p.ldz};
+                e = gges_sort_cplx<R>(st, sel, q, alpha, beta, g, info);
+            }
+            if (e == cudaSuccess)
+                e = gges_scale_out<rb::zc<R>, R>(st, n, A, lda, B, ldb, alpha, beta, (rb::zc<R> *)nullptr, g);
+            if (e == cudaSuccess && sort == 'S') {
+                int sd = 0;
+                e = gges_check_cplx<R>(st, sel, n, alpha, beta, &sd, info);
+                if (sdim) *sdim = sd;
+            }
         }
     }
     if (e != cudaSuccess) {
