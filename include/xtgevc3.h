@@ -297,8 +297,10 @@ int xtgevc3_stgexc_dev(void *stream, int wantq, int wantz, int n, float *A, int 
  * SELCTG, SDIM) and without workspace: JOBVSL / JOBVSR 'V' or 'N'; INFO as LAPACK numbers its
  * arguments (-1 JOBVSL, -2 JOBVSR, -5 N, -7 LDA, -9 LDB, -14 LDVSL, -16 LDVSR), or i > 0 when
  * the QZ iterations did not deflate eigenvalue i within 30 n iterations (S, T not in Schur
- * form then).  No balancing of the pencil (LAPACK's ZGGBAL / scaling): the form is computed
- * for (A, B) as given.  One CTA runs the chain of rotations (B triangular, Hessenberg-
+ * form then).  A (B) whose largest entry in modulus lies outside [sqrt(safmin) / eps, its
+ * inverse] is scaled into that range first and the form and eigenvalues scaled back at the end,
+ * as LAPACK's xGGES does (xLASCL's factors; real pencils with DGGES's guard of complex pairs);
+ * no permutation balancing (xGGBAL with JOB = 'P').  One CTA runs the chain of rotations (B triangular, Hessenberg-
  * triangular reduction, single-shift QZ), so the call is latency-bound; its value is the
  * result staying on the device for the eigenvector solve (xtgevc3_ztgevc3_dev).  Complex
  * arrays interleaved.  Device form: every array a device pointer (alpha, beta n complex
