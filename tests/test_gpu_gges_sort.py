@@ -18,7 +18,7 @@ import xtgevc3_b200 as X
 from test_tgexc_blocks_host import _twin_blocks_pencil, sign_aligned
 from test_tgsen_host import CPLX_SELECTIONS, REAL_SELECTIONS, TOL, _cplx_schur, _pencil, _real_schur, _rel
 
-pytestmark = [pytest.mark.gpu, pytest.mark.late(4)]
+pytestmark = [pytest.mark.gpu, pytest.mark.late(3)]
 
 
 @pytest.mark.parametrize("dt", [np.float64, np.float32], ids=["d", "s"])
@@ -102,6 +102,7 @@ def test_complex_tgsen_rejection(cuda_ok):
 
 
 @pytest.mark.parametrize("dt", [np.float64, np.float32, np.complex128, np.complex64], ids=["d", "s", "z", "c"])
+@pytest.mark.late(6)  # runs the QZ kernels: after their own tests
 def test_gges_sort_matches_lapack(cuda_ok, dt):
     n = 48
     A, B = _pencil(n, 31, dt)
@@ -131,6 +132,7 @@ def test_gges_sort_matches_lapack(cuda_ok, dt):
     assert np.allclose(np.sort_complex(lam[sdim:]), np.sort_complex(lam_r[sdim:]), rtol=rt)
 
 
+@pytest.mark.late(6)  # runs the QZ kernels: after their own tests
 def test_gges_sort_device_form_matches_host_form(cuda_ok):
     import torch
     n = 40

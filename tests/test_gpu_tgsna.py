@@ -90,7 +90,7 @@ from test_tgsna_dif_host import _twin_blocks_pencil, blocks  # noqa: E402
 
 
 @pytest.mark.parametrize("dt", [np.float64, np.float32], ids=["d", "s"])
-@pytest.mark.late(2)
+@pytest.mark.late(4)
 def test_dif_matches_lapack(cuda_ok, dt):
     tol = {np.float64: 1e-12, np.float32: 1e-4}[dt]
     same = total = 0
@@ -108,7 +108,7 @@ def test_dif_matches_lapack(cuda_ok, dt):
     assert same >= 0.8 * total, (same, total)
 
 
-@pytest.mark.late(2)
+@pytest.mark.late(4)
 def test_dif_job_b_and_device_form(cuda_ok):
     import torch
     S, P, ar, ai, be = _pencil(np.float64, 30, 17)
@@ -128,7 +128,7 @@ def test_dif_job_b_and_device_form(cuda_ok):
     np.testing.assert_array_equal(d_dev.cpu().numpy(), d_v)
 
 
-@pytest.mark.late(2)
+@pytest.mark.late(4)
 def test_dif_selection_and_rejection(cuda_ok):
     """HOWMNY = 'S' (a pair selected by its second row), and a rejected reordering (the
     second of two identical 2x2 blocks: DIF = 0), as LAPACK."""
@@ -149,7 +149,7 @@ def test_dif_selection_and_rejection(cuda_ok):
 
 
 @pytest.mark.parametrize("dt", [np.complex128, np.complex64], ids=["z", "c"])
-@pytest.mark.late(2)
+@pytest.mark.late(4)
 def test_complex_dif_matches_lapack(cuda_ok, dt):
     """Z/CTGSNA JOB = 'V': the reordering is LAPACK's rotations, so every DIF equals LAPACK's
     to rounding (1e-10 double, 1e-3 single); the device form gives the host form's values."""

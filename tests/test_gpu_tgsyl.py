@@ -16,7 +16,7 @@ import xtgevc3_b200 as X
 from test_tgsen_host import REAL_SELECTIONS, _real_schur
 from test_tgsyl_host import _schur, sylv_operands
 
-pytestmark = [pytest.mark.gpu, pytest.mark.late(5)]
+pytestmark = [pytest.mark.gpu, pytest.mark.late(2)]
 
 
 @pytest.mark.parametrize("dt", [np.float64, np.float32], ids=["d", "s"])
