@@ -11,6 +11,7 @@
 #include "../xtgevc3_b200/csrc/tgsen.cuh"
 #include "../xtgevc3_b200/csrc/tgsyl.cuh"
 #include "../xtgevc3_b200/csrc/gges_scale.h"
+#include "../xtgevc3_b200/csrc/ggbal.cuh"
 
 using namespace xtg::rb;
 
@@ -255,6 +256,31 @@ int run_ztgsyl_c(int nth, int m, int n, const R *A, const R *B, R *C, const R *D
     return sh.info;
 }
 
+template <class E, class R>
+int run_ggbal(int nth, int n, E *A, E *B, R *ls, R *rs, int *ilo, int *ihi)
+{
+    BalPencil<E> p{n, A, B, n, n};
+    BalShared sh{};
+    std::vector<int> red(2 * (size_t)nth);
+    std::barrier<> bar(nth);
+    std::vector<std::thread> th;
+    for (int t = 0; t < nth; t++)
+        th.emplace_back([&, t] { ggbal_cta(CtaHost{t, nth, &bar}, sh, p, ls, rs, ilo, ihi, red.data()); });
+    for (auto &x : th) x.join();
+    return 0;
+}
+
+template <class E, class R>
+int run_ggbak(int nth, int n, int ilo, int ihi, const R *scale, E *V)
+{
+    std::barrier<> bar(nth);
+    std::vector<std::thread> th;
+    for (int t = 0; t < nth; t++)
+        th.emplace_back([&, t] { ggbak_cta(CtaHost{t, nth, &bar}, n, ilo, ihi, scale, V, n); });
+    for (auto &x : th) x.join();
+    return 0;
+}
+
 // SELCTG from flags: the test passes the selection that LAPACK's SELCTG made, one flag per
 // eigenvalue in order, and the check reads them back in the same order
 struct FlagSel {
@@ -423,6 +449,22 @@ int host_gges_scale_out(int cplx, int n, double *A, double *B, double *ev0, doub
         }
     }
     return 0;
+}
+
+// xGGBAL 'P' / xGGBAK 'P' bodies (d: real double, z: complex double, interleaved)
+int host_dggbal(int nth, int n, double *A, double *B, double *ls, double *rs, int *ilo, int *ihi)
+{
+    return run_ggbal(nth, n, A, B, ls, rs, ilo, ihi);
+}
+
+int host_zggbal(int nth, int n, double *A, double *B, double *ls, double *rs, int *ilo, int *ihi)
+{
+    return run_ggbal(nth, n, reinterpret_cast<zc<double> *>(A), reinterpret_cast<zc<double> *>(B), ls, rs, ilo, ihi);
+}
+
+int host_dggbak(int nth, int n, int ilo, int ihi, const double *scale, double *V)
+{
+    return run_ggbak(nth, n, ilo, ihi, scale, V);
 }
 
 // xGGES's check: SELCTG's answers as flags in order; returns SDIM, *info as the check leaves it

@@ -1,0 +1,104 @@
+"""Permutation balancing (xtgevc3_b200/csrc/ggbal.cuh: rb::ggbal_cta, LAPACK xGGBAL with
+JOB = 'P'; rb::ggbak_cta, xGGBAK with JOB = 'P') compiled for the CPU by tests/qz_host.cpp,
+against LAPACK's own DGGBAL / ZGGBAL / DGGBAK (their Fortran interfaces in SciPy's OpenBLAS),
+bit for bit: the permuted A and B, ILO, IHI and the isolated entries of LSCALE / RSCALE, on
+pencils with isolated eigenvalues of every kind the search meets (rows with no or one
+off-diagonal nonzero, columns likewise, chains of them, a fully triangular pencil, none), on 1
+and several host threads."""
+import ctypes as ct
+
+import numpy as np
+import pytest
+
+import oracle
+from test_qz_host import _p, host  # noqa: F401  (fixture)
+
+
+def lapack_ggbal(A, B):
+    cplx = np.iscomplexobj(A)
+    f = getattr(oracle._openblas(), "scipy_zggbal_" if cplx else "scipy_dggbal_")
+    n = A.shape[0]
+    A, B = np.array(A, order="F"), np.array(B, order="F")
+    ilo, ihi, info = ct.c_int(), ct.c_int(), ct.c_int()
+    ls, rs, work = np.full(n, -7.0), np.full(n, -7.0), np.zeros(6 * n + 6)
+    iv = lambda v: ct.byref(ct.c_int(v))  # noqa: E731
+    f(ct.c_char_p(b"P"), iv(n), _p(A), iv(n), _p(B), iv(n), ct.byref(ilo), ct.byref(ihi), _p(ls), _p(rs), _p(work),
+      ct.byref(info), ct.c_size_t(1))
+    assert info.value == 0
+    return A, B, ilo.value, ihi.value, ls, rs
+
+
+def host_ggbal(L, A, B, nth=1):
+    cplx = np.iscomplexobj(A)
+    n = A.shape[0]
+    A, B = np.array(A, order="F"), np.array(B, order="F")
+    ls, rs = np.full(n, -7.0), np.full(n, -7.0)
+    ilo, ihi = ct.c_int(), ct.c_int()
+    (L.host_zggbal if cplx else L.host_dggbal)(nth, n, _p(A), _p(B), _p(ls), _p(rs), ct.byref(ilo), ct.byref(ihi))
+    return A, B, ilo.value, ihi.value, ls, rs
+
+
+def structured(kind, n, seed, cplx):
+    rng = np.random.default_rng(seed)
+    def draw():
+        M = rng.standard_normal((n, n))
+        return M + 1j * rng.standard_normal((n, n)) if cplx else M
+    A, B = draw(), draw()
+    if kind == "row_offdiag":  # a row with one off-diagonal nonzero
+        A[2, :] = 0
+        B[2, :] = 0
+        A[2, 5] = 1.5
+        B[2, 5] = 0.5
+    elif kind == "row_zero_col":  # a zero row and a column with one nonzero
+        A[4, :] = 0
+        B[4, :] = 0
+        A[:, 1] = 0
+        B[:, 1] = 0
+        A[6, 1] = 2.0
+    elif kind == "chain":  # the first four columns triangular: the column search isolates them in turn
+        for k in range(4):
+            A[k + 1:, k] = 0
+            B[k + 1:, k] = 0
+    elif kind == "triangular":
+        A, B = np.triu(A), np.triu(B)
+    elif kind == "permuted_triangular":
+        p = rng.permutation(n)
+        A, B = np.triu(A)[np.ix_(p, p)], np.triu(B)[np.ix_(p, p)]
+    return np.asfortranarray(A), np.asfortranarray(B)
+
+
+KINDS = ["none", "row_offdiag", "row_zero_col", "chain", "triangular", "permuted_triangular"]
+
+
+@pytest.mark.parametrize("cplx", [False, True], ids=["d", "z"])
+@pytest.mark.parametrize("kind", KINDS, ids=str)
+@pytest.mark.parametrize("n", [1, 2, 9, 17], ids=lambda n: f"n{n}")
+def test_ggbal_matches_lapack(host, cplx, kind, n):
+    if n < 9 and kind not in ("none", "triangular"):
+        pytest.skip("the constructions need n >= 9")
+    A, B = structured(kind, n, 5, cplx)
+    r = lapack_ggbal(A, B)
+    for nth in (1, 4):
+        h = host_ggbal(host, A, B, nth)
+        assert (h[2], h[3]) == (r[2], r[3]), (kind, h[2:4], r[2:4])
+        assert np.array_equal(h[0], r[0]) and np.array_equal(h[1], r[1]), kind
+        iso = [i for i in range(n) if i < r[2] - 1 or i >= r[3]]
+        assert np.array_equal(h[4][iso], r[4][iso]) and np.array_equal(h[5][iso], r[5][iso]), kind
+
+
+@pytest.mark.parametrize("kind", KINDS[1:], ids=str)
+def test_ggbak_matches_lapack(host, kind):
+    n = 17
+    A, B = structured(kind, n, 6, False)
+    r = lapack_ggbal(A, B)
+    V = np.asfortranarray(np.random.default_rng(1).standard_normal((n, n)))
+    for side, scale in ((b"L", r[4]), (b"R", r[5])):
+        Vr = V.copy(order="F")
+        iv = lambda v: ct.byref(ct.c_int(v))  # noqa: E731
+        info = ct.c_int()
+        oracle._openblas().scipy_dggbak_(ct.c_char_p(b"P"), ct.c_char_p(side), iv(n), iv(r[2]), iv(r[3]),
+                                          _p(scale), _p(scale), iv(n), _p(Vr), iv(n), ct.byref(info), ct.c_size_t(1),
+                                          ct.c_size_t(1))
+        Vh = V.copy(order="F")
+        host.host_dggbak(3, n, r[2], r[3], _p(np.ascontiguousarray(scale)), _p(Vh))
+        assert np.array_equal(Vh, Vr), (kind, side)

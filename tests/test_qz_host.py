@@ -34,7 +34,8 @@ def host():
     lib = os.path.join(out, "libqz_host.so")
     src = os.path.join(ROOT, "tests", "qz_host.cpp")
     hdrs = [os.path.join(ROOT, "xtgevc3_b200", "csrc", h)
-            for h in ("qz_cplx.cuh", "qz_real.cuh", "tgsen.cuh", "tgsyl.cuh", "tgsna_dif_cplx.cuh", "tgsna_dif.cuh",
+            for h in ("qz_cplx.cuh", "qz_real.cuh", "tgsen.cuh", "tgsyl.cuh", "ggbal.cuh", "gges_scale.h",
+                      "tgsna_dif_cplx.cuh", "tgsna_dif.cuh",
                       "tgexc_real_blocks.cuh")]
     if not os.path.exists(lib) or os.path.getmtime(lib) < max(os.path.getmtime(f) for f in [src] + hdrs):
         r = subprocess.run(["g++", "-O2", "-std=c++20", "-pthread", "-shared", "-fPIC", "-ffp-contract=off", "-o", lib,
