@@ -467,6 +467,11 @@ int host_dggbak(int nth, int n, int ilo, int ihi, const double *scale, double *V
     return run_ggbak(nth, n, ilo, ihi, scale, V);
 }
 
+int host_zggbak(int nth, int n, int ilo, int ihi, const double *scale, double *V)
+{
+    return run_ggbak(nth, n, ilo, ihi, scale, reinterpret_cast<zc<double> *>(V));
+}
+
 // xGGES's check: SELCTG's answers as flags in order; returns SDIM, *info as the check leaves it
 int host_dgges_sdim(int n, const int *flags, const double *ar, const double *ai, const double *be, int *info)
 {

@@ -102,3 +102,39 @@ def test_ggbak_matches_lapack(host, kind):
         Vh = V.copy(order="F")
         host.host_dggbak(3, n, r[2], r[3], _p(np.ascontiguousarray(scale)), _p(Vh))
         assert np.array_equal(Vh, Vr), (kind, side)
+
+
+@pytest.mark.parametrize("cplx", [False, True], ids=["d", "z"])
+@pytest.mark.parametrize("kind", KINDS, ids=str)
+def test_balanced_qz_flow_matches_lapack_gges(host, cplx, kind):
+    """xGGES's flow with balancing on host threads (the bodies of the device kernels): xGGBAL
+    'P', the QZ step on the whole balanced pencil, xGGBAK 'P' on Q and Z.  A = Q S Z^H and
+    B = Q T Z^H to 1e-12 n, S, T in (quasi-)triangular form, and LAPACK xGGES's eigenvalues
+    (relative 1e-9; the isolated ones exactly the diagonal entries LAPACK reads)."""
+    from test_qz_host import host_qz, host_rqz
+    import scipy.linalg.lapack as la
+    n = 17
+    A, B = structured(kind, n, 5, cplx)
+    Ab, Bb, ilo, ihi, ls, rs = host_ggbal(host, A, B)
+    if cplx:
+        S, T, Q, Z, info = host_qz(host, Ab, Bb)
+        lam = np.diag(S) / np.diag(T)
+        r = la.zgges(lambda a, b: 0, A, B)
+        lam_r = r[3] / r[4]
+        bak = host.host_zggbak
+    else:
+        S, T, Q, Z, ar, ai, be, info = host_rqz(host, Ab, Bb)
+        lam = (ar + 1j * ai) / be
+        r = la.dgges(lambda x, y, z: 0, A, B)
+        lam_r = (r[3] + 1j * r[4]) / r[5]
+        bak = host.host_dggbak
+    assert info == 0
+    bak(2, n, ilo, ihi, _p(np.ascontiguousarray(ls)), _p(Q))
+    bak(2, n, ilo, ihi, _p(np.ascontiguousarray(rs)), _p(Z))
+    for M, M0 in ((S, A), (T, B)):
+        assert np.abs(Q @ M @ Z.conj().T - M0).max() <= 1e-12 * n * np.abs(M0).max()
+    assert np.abs(np.tril(T, -1)).max() == 0 and np.abs(np.tril(S, -2)).max() == 0
+    fin = np.isfinite(lam_r) & np.isfinite(lam)
+    for x, y in ((lam[fin], lam_r[fin]), (lam_r[fin], lam[fin])):
+        d = np.abs(x[:, None] - y[None, :]).min(1) / np.maximum(np.abs(x), 1e-300)
+        assert d.max() <= 1e-9, (kind, d.max())

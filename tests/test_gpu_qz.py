@@ -164,3 +164,34 @@ def test_gges_scales_badly_scaled_pencils(cuda_ok, sa, sb, cplx):
         assert d.max() <= 1e-9, d.max()
     for M, M0 in ((S, A), (T, B)):
         assert np.abs(Q @ M @ Z.conj().T - M0).max() <= 1e-12 * n * np.abs(M0).max()
+
+
+@pytest.mark.parametrize("kind", ["none", "row_offdiag", "row_zero_col", "chain", "triangular", "permuted_triangular"],
+                         ids=str)
+@pytest.mark.parametrize("cplx", [False, True], ids=["d", "z"])
+def test_gges_balances_structured_pencils(cuda_ok, kind, cplx):
+    """xGGES's permutation balancing on the device (the pencils of tests/test_ggbal_host.py, where
+    the same flow runs on host threads and xGGBAL equals LAPACK's bit for bit): A = VSL S VSR^H,
+    B = VSL T VSR^H to 1e-12 n, LAPACK xGGES's eigenvalues (relative 1e-9)."""
+    import scipy.linalg.lapack as la
+    from test_ggbal_host import structured
+    n = 17
+    A, B = structured(kind, n, 5, cplx)
+    out = X.gges(A, B)
+    if cplx:
+        S, T, al, be, Q, Z, info = out
+        lam = al / be
+        r = la.zgges(lambda a, b: 0, A, B)
+        lam_r = r[3] / r[4]
+    else:
+        S, T, ar, ai, be, Q, Z, info = out
+        lam = (ar + 1j * ai) / be
+        r = la.dgges(lambda x, y, z: 0, A, B)
+        lam_r = (r[3] + 1j * r[4]) / r[5]
+    assert info == 0
+    for M, M0 in ((S, A), (T, B)):
+        assert np.abs(Q @ M @ Z.conj().T - M0).max() <= 1e-12 * n * np.abs(M0).max()
+    fin = np.isfinite(lam_r) & np.isfinite(lam)
+    for x, y in ((lam[fin], lam_r[fin]), (lam_r[fin], lam[fin])):
+        d = np.abs(x[:, None] - y[None, :]).min(1) / np.maximum(np.abs(x), 1e-300)
+        assert d.max() <= 1e-9, (kind, d.max())

@@ -11,6 +11,7 @@
 #include "../../include/xtgevc3.h"
 #include "common.cuh"
 #include "engine.cuh"
+#include "ggbal.cuh"
 #include "gges_scale.h"
 #include "qz_real.cuh"
 #include "tgsen.cuh"
@@ -188,6 +189,70 @@ __global__ void __launch_bounds__(256) lascl_kernel(E *A, int lda, int n, int ki
         for (int s = 0; s < m.k; s++) scale_(v, m.f[s]);
         A[(size_t)i + (size_t)j * lda] = v;
     }
+}
+
+// xGGBAL 'P' (rb::ggbal_cta): lscale, rscale n each; ilohi = {ILO, IHI}; red 2 kQzThreads ints
+template <class E, class R>
+__global__ void __launch_bounds__(kQzThreads, 1)
+    ggbal_kernel(rb::BalPencil<E> p, R *lscale, R *rscale, int *ilohi, int *red)
+{
+    __shared__ rb::BalShared sh;
+    rb::ggbal_cta(rb::CtaDev{}, sh, p, lscale, rscale, ilohi, ilohi + 1, red);
+}
+
+// xGGBAK 'P' (rb::ggbak_cta) of the Schur vectors V with xGGBAL's ILO, IHI and scale
+template <class E, class R>
+__global__ void __launch_bounds__(kQzThreads, 1) ggbak_kernel(int n, const int *ilohi, const R *scale, E *V, int ldv)
+{
+    rb::ggbak_cta(rb::CtaDev{}, n, ilohi[0], ilohi[1], scale, V, ldv);
+}
+
+// xGGES's permutation balancing around the QZ step: gges_balance_in permutes A and B (ILO, IHI,
+// LSCALE, RSCALE stay on the device in bal), gges_balance_out permutes the rows of VSL / VSR
+// back (after the ordering, before the scaling back, as xGGES)
+template <class R>
+struct GgesBalance {
+    R *scale = nullptr;  // lscale (n), rscale (n)
+    int *ints = nullptr;  // ILO, IHI, then the reduction scratch
+};
+
+template <class E, class R>
+cudaError_t gges_balance_in(cudaStream_t st, int n, E *A, int lda, E *B, int ldb, GgesBalance<R> &bal)
+{
+    cudaError_t e = cudaMallocAsync(&bal.scale, 2 * (size_t)n * sizeof(R), st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&bal.ints, (2 + 2 * kQzThreads) * sizeof(int), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(bal.scale, 0, 2 * (size_t)n * sizeof(R), st);
+    if (e != cudaSuccess) return e;
+    const rb::BalPencil<E> p{n, A, B, lda, ldb};
+    ggbal_kernel<E, R><<<1, kQzThreads, 0, st>>>(p, bal.scale, bal.scale + n, bal.ints, bal.ints + 2);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+template <class E, class R>
+cudaError_t gges_balance_out(cudaStream_t st, int n, E *VSL, int ldvsl, E *VSR, int ldvsr, const GgesBalance<R> &bal)
+{
+    cudaError_t e = cudaSuccess;
+    if (VSL) {
+        ggbak_kernel<E, R><<<1, kQzThreads, 0, st>>>(n, bal.ints, bal.scale, VSL, ldvsl);
+        count_launches(1);
+        e = cudaGetLastError();
+    }
+    if (VSR && e == cudaSuccess) {
+        ggbak_kernel<E, R><<<1, kQzThreads, 0, st>>>(n, bal.ints, bal.scale + n, VSR, ldvsr);
+        count_launches(1);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
+template <class R>
+void gges_balance_free(cudaStream_t st, GgesBalance<R> &bal)
+{
+    if (bal.scale) cudaFreeAsync(bal.scale, st);
+    if (bal.ints) cudaFreeAsync(bal.ints, st);
+    bal.scale = nullptr;
+    bal.ints = nullptr;
 }
 
 // The scaling decisions of xGGES for one run
@@ -456,7 +521,9 @@ int gges_device_real(cudaStream_t st, char jobvsl, char jobvsr, char sort, SelRe
     const int wl = jobvsl == 'V', wr = jobvsr == 'V';
     int *d_info = nullptr, h_info = 0;
     GgesScale<R> g;
+    GgesBalance<R> bal;
     cudaError_t e = gges_scale_in<R, R>(st, n, A, lda, B, ldb, g);
+    if (e == cudaSuccess) e = gges_balance_in<R, R>(st, n, A, lda, B, ldb, bal);
     if (e == cudaSuccess) e = cudaMallocAsync(&d_info, sizeof(int), st);
     if (e == cudaSuccess) {
         // Q and Z are not referenced when not wanted
@@ -474,6 +541,8 @@ int gges_device_real(cudaStream_t st, char jobvsl, char jobvsr, char sort, SelRe
                 const rb::Pencil<R> q{n, wl, wr, A, B, p.Q, p.Z, lda, ldb, p.ldq, p.ldz};
                 e = gges_sort_real<R>(st, sel, q, alphar, alphai, beta, g, info);
             }
+            if (e == cudaSuccess)
+                e = gges_balance_out<R, R>(st, n, wl ? VSL : nullptr, ldvsl, wr ? VSR : nullptr, ldvsr, bal);
             if (e == cudaSuccess) e = gges_scale_out<R, R>(st, n, A, lda, B, ldb, alphar, alphai, beta, g);
             if (e == cudaSuccess && sort == 'S') {
                 int sd = 0;
@@ -482,6 +551,7 @@ int gges_device_real(cudaStream_t st, char jobvsl, char jobvsr, char sort, SelRe
             }
         }
     }
+    gges_balance_free(st, bal);  // stream-ordered after the kernels that read it
     if (e != cudaSuccess) {
         set_last_error(std::string("xGGES: ") + cudaGetErrorString(e));
         *info = n + 1;
@@ -574,7 +644,9 @@ int gges_device(cudaStream_t st, char jobvsl, char jobvsr, char sort, SelCplx<R>
     const int wl = jobvsl == 'V', wr = jobvsr == 'V';
     int *d_info = nullptr, h_info = 0;
     GgesScale<R> g;
+    GgesBalance<R> bal;
     cudaError_t e = gges_scale_in<rb::zc<R>, R>(st, n, A, lda, B, ldb, g);
+    if (e == cudaSuccess) e = gges_balance_in<rb::zc<R>, R>(st, n, A, lda, B, ldb, bal);
     if (e == cudaSuccess) e = cudaMallocAsync(&d_info, sizeof(int), st);
     if (e == cudaSuccess) {
         // Q and Z are not referenced when not wanted
@@ -592,6 +664,8 @@ int gges_device(cudaStream_t st, char jobvsl, char jobvsr, char sort, SelCplx<R>
                 e = gges_sort_cplx<R>(st, sel, q, alpha, beta, g, info);
             }
             if (e == cudaSuccess)
+                e = gges_balance_out<rb::zc<R>, R>(st, n, wl ? VSL : nullptr, ldvsl, wr ? VSR : nullptr, ldvsr, bal);
+            if (e == cudaSuccess)
                 e = gges_scale_out<rb::zc<R>, R>(st, n, A, lda, B, ldb, alpha, beta, (rb::zc<R> *)nullptr, g);
             if (e == cudaSuccess && sort == 'S') {
                 int sd = 0;
@@ -600,6 +674,7 @@ int gges_device(cudaStream_t st, char jobvsl, char jobvsr, char sort, SelCplx<R>
             }
         }
     }
+    gges_balance_free(st, bal);  // stream-ordered after the kernels that read it
     if (e != cudaSuccess) {
         set_last_error(std::string("xGGES: ") + cudaGetErrorString(e));
         *info = n + 1;
