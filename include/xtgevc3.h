@@ -300,7 +300,8 @@ int xtgevc3_stgexc_dev(void *stream, int wantq, int wantz, int n, float *A, int 
  * form then).  A (B) whose largest entry in modulus lies outside [sqrt(safmin) / eps, its
  * inverse] is scaled into that range first and the form and eigenvalues scaled back at the end,
  * as LAPACK's xGGES does (xLASCL's factors; real pencils with DGGES's guard of complex pairs);
- * no permutation balancing (xGGBAL with JOB = 'P').  One CTA runs the chain of rotations (B triangular, Hessenberg-
+ * then the pencil is balanced by permutations (xGGBAL with JOB = 'P': isolated eigenvalues
+ * moved to the ends) and VSL / VSR permuted back (xGGBAK), as xGGES does.  One CTA runs the chain of rotations (B triangular, Hessenberg-
  * triangular reduction, single-shift QZ), so the call is latency-bound; its value is the
  * result staying on the device for the eigenvector solve (xtgevc3_ztgevc3_dev).  Complex
  * arrays interleaved.  Device form: every array a device pointer (alpha, beta n complex
