@@ -1,13 +1,16 @@
-// The generalized Schur form of a pencil on the GPU (LAPACK Z/C/D/SGGES): rb::zgges_cta
-// (qz_cplx.cuh) or rb::dgges_cta (qz_real.cuh) on one CTA; complex alpha = diag(S), beta =
-// diag(T), real alphar / alphai / beta as DHGEQZ returns them.  With SORT = 'S' the
-// eigenvalues that SELCTG selects then move to the leading rows: SELCTG runs on the host over
-// the QZ eigenvalues (2-3 n numbers read back), the reordering kernel (rb::tgsen_real_cta /
-// rb::tgsen_cplx_cta of tgsen.cuh, xTGSEN with IJOB = 0) runs on one CTA, and xGGES's own
-// check of the reordered eigenvalues (SDIM, INFO = n + 2 / n + 3) runs on the host.
-// The stages are chains of dependent plane rotations or swaps, so one CTA runs them (each
-// rotation's O(n) rows or columns spread over its threads); the result stays on the device
-// for the eigenvector solve that follows (xtgevc3_ztgevc3_dev).
+// The generalized Schur form of a pencil on the GPU (LAPACK Z/C/D/SGGES), in xGGES's order:
+// A and B scaled into range where their largest entries lie outside it (gges_scale.h;
+// maxabs_kernel, lascl_kernel), balanced by permutations (ggbal.cuh: xGGBAL 'P'), the QZ step
+// (rb::zgges_cta of qz_cplx.cuh or rb::dgges_cta of qz_real.cuh on one CTA; complex alpha =
+// diag(S), beta = diag(T), real alphar / alphai / beta as DHGEQZ returns them), with SORT = 'S'
+// the ordering (SELCTG on the host over the 2-3 n eigenvalue numbers read back, the
+// reordering kernel of tgsen.cuh on one CTA), VSL / VSR permuted back (xGGBAK 'P'), the form
+// and eigenvalues scaled back, and xGGES's check of the reordered eigenvalues (SDIM, INFO =
+// n + 2 / n + 3) on the host.  Also here: xTGSEN with IJOB 0-5 (tgsen.cuh) and xTGSYL
+// (tgsyl.cuh) as entry points of their own.  The stages are chains of dependent plane
+// rotations, swaps or small systems, so one CTA runs each (the O(n) rows or columns of a step
+// spread over its threads); the result stays on the device for the eigenvector solve that
+// follows (xtgevc3_ztgevc3_dev).
 #include "../../include/xtgevc3.h"
 #include "common.cuh"
 #include "engine.cuh"

@@ -1,7 +1,9 @@
 // Reordering a generalized Schur pencil by a selection: the selected eigenvalues move to the
 // leading rows (LAPACK D/S/Z/CTGSEN with IJOB = 0, the step xGGES takes when SORT = 'S', its
-// SELECT being SELCTG of the QZ eigenvalues).  Host and device code: the kernels in qz.cu run
-// these bodies on one CTA (rb::CtaDev); the tests run them on host threads and on one thread.
+// SELECT being SELCTG of the QZ eigenvalues), and xTGSEN's estimates for IJOB 1-5 on the
+// reordered pencil (tgsen_real_estimates / tgsen_cplx_estimates, on the solvers of
+// tgsyl.cuh).  Host and device code: the kernels in qz.cu run these bodies on one CTA
+// (rb::CtaDev); the tests run them on host threads and on one thread.
 //
 // Real pencils (DTGSEN): the diagonal blocks are visited from the top, a 2x2 block counting as
 // selected when either of its rows is; each selected block moves up to the next free leading
