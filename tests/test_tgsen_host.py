@@ -329,3 +329,30 @@ def test_gges_sort_argument_checks():
         L.xtgevc3_zgges_sort(b"V", b"V", so, sel, 4, _p(Mc), 4, _p(Mc), 4, ct.byref(sd), _p(vc), _p(vc), _p(Mc), ldl,
                              _p(Mc), 4, ct.byref(info))
         assert info.value == want, (so, want, info.value)
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.complex128], ids=["d", "z"])
+@pytest.mark.parametrize("n", [1, 2, 3, 5], ids=lambda n: f"n{n}")
+def test_qz_then_reordering_small_orders(host, dt, n):
+    """The chain of xtgevc3_*gges_sort on orders 1 to 5 (several seeds): LAPACK's SDIM and INFO,
+    the selected eigenvalues leading, A = Q S Z^H."""
+    for seed in range(4):
+        A, B = _pencil(n, 60 + seed, dt)
+        if np.dtype(dt).kind == "f":
+            S, T, Q, Z, ar, ai, be, info = host_rqz(host, A, B)
+            f = REAL_SELECTIONS["neg_real"]
+            sel = f(ar, ai, be).astype(np.int32)
+            a, b, ar2, ai2, be2, q, z, info2 = host_tgsen(host, sel, S, T, Q, Z)
+            sdim, info3 = _sdim(host, f(ar2, ai2, be2).astype(np.int32), ar2, ai2, be2)
+            r = oracle.lapack_gges_sort(A, B, lambda x, y, w: x * w < 0)
+        else:
+            S, T, Q, Z, info = host_qz(host, A, B)
+            g = CPLX_SELECTIONS["neg_real"]
+            sel = g(np.diag(S), np.diag(T)).astype(np.int32)
+            a, b, al2, be2, q, z, info2 = host_tgsen(host, sel, S, T, Q, Z)
+            sdim, info3 = _sdim(host, g(al2, be2).astype(np.int32), al2, None, be2)
+            r = oracle.lapack_gges_sort(A, B, lambda x, y: (x * np.conj(y)).real < 0)
+        assert (info, info2, info3) == (0, 0, 0) and sdim == r[2], (n, seed, sdim, r[2])
+        scale = max(np.abs(A).max(), np.abs(B).max())
+        assert np.abs(q @ a @ z.conj().T - A).max() < 1e-12 * max(n, 2) * scale
+        assert np.abs(q @ b @ z.conj().T - B).max() < 1e-12 * max(n, 2) * scale

@@ -381,3 +381,38 @@ def test_complex_tgsen_one_norm_estimates(host, kind, n, seed):
                         A, B = oracle.lapack_tgexc(A, B, None, None, k, ks)[:2]
             nrm = _kron_inv_one_norm(A[m:, m:], B[m:, m:], A[:m, :m], B[:m, :m])
             assert 1 / nrm * (1 - 1e-10) <= est[3] <= 3 / nrm, (est[3], 1 / nrm)
+
+
+@pytest.mark.parametrize("cplx", [False, True], ids=["d", "z"])
+@pytest.mark.parametrize("n", [1, 2, 3, 4], ids=lambda n: f"n{n}")
+def test_tgsen_small_orders_every_selection(host, cplx, n):
+    """Orders 1 to 4, every selection pattern, IJOB 0 and 4: M, INFO, the eigenvalues and (complex
+    pencils, no sign choice) PL, PR, DIF equal to LAPACK's; real PL, PR too."""
+    import itertools
+    from test_tgsen_host import _cplx_schur
+    if cplx:
+        S, T, Q, Z, al, be = _cplx_schur(n, 40 + n, np.complex128)
+    else:
+        S, T, Q, Z, ar, ai, be = _real_schur(n, 40 + n, np.float64)
+    lw = 2 * n * n + 64
+    for bits in itertools.product((0, 1), repeat=n):
+        sel = np.array(bits, np.int32)
+        for ijob in (0, 4):
+            if cplx:
+                r = la.ztgsen(sel, S, T, Q, Z, ijob=ijob, lwork=lw, liwork=lw)
+                h = host_ztgsen_full(host, ijob, sel, S, T, Q, Z)
+                assert (h[6], h[7]) == (r[6], r[10]), (bits, ijob)
+                for v, w in zip(h[4], (r[2], r[3])):
+                    assert np.abs(v[:n] - w).max() <= 1e-12 * max(np.abs(w).max(), 1.0)
+                if ijob == 4:
+                    ref = np.array([r[7], r[8], r[9][0], r[9][1]])
+                    assert np.all(np.abs(h[5] - ref) <= 1e-12 * np.abs(ref)), (bits, h[5], ref)
+            else:
+                r = la.dtgsen(sel, S, T, Q, Z, ijob=ijob, lwork=lw, liwork=lw)
+                h = host_tgsen_full(host, ijob, sel, S, T, Q, Z)
+                assert (h[6], h[7]) == (r[7], r[11]), (bits, ijob)
+                lam = (h[4][0][:n] + 1j * h[4][1][:n]) / h[4][2][:n]
+                lam_r = (r[2] + 1j * r[3]) / r[4]
+                assert np.abs(lam - lam_r).max() <= 1e-10 * max(np.abs(lam_r).max(), 1.0), bits
+                if ijob == 4:
+                    assert abs(h[5][0] - r[8]) <= 1e-12 * r[8] and abs(h[5][1] - r[9]) <= 1e-12 * r[9]
