@@ -462,6 +462,49 @@ int xtgevc3_ctgsyl_dev(void *stream, char trans, int ijob, int m, int n, const f
                        int ldb, float *C, int ldc, const float *D, int ldd, const float *E, int lde, float *F, int ldf,
                        float *scale, float *dif, int *info);
 
+/* LAPACK D/S/Z/CGGBAL and xGGBAK with JOB = 'N' or 'P' (permutation balancing, the first and
+ * last steps of xGGES): xGGBAL moves isolated eigenvalues to the ends of the pencil (rows with
+ * at most one nonzero in the active columns to the bottom, then columns with at most one
+ * nonzero in the active rows to the left; LSCALE / RSCALE record the swaps, 1 on [ILO, IHI]),
+ * xGGBAK applies the row swaps back to the vectors V (n x m; SIDE 'L' with LSCALE, 'R' with
+ * RSCALE).  Equal to LAPACK's bit for bit (the search rule of older LAPACK releases, which
+ * also isolates a row whose one nonzero is off the diagonal).  JOB = 'S' / 'B' (the scaling)
+ * are not built: INFO = -1.  INFO as LAPACK numbers its arguments; n + 1 (not a LAPACK value)
+ * when a CUDA call failed in the host-pointer form.  One CTA; device forms: matrices and
+ * scales on the device, ILO / IHI host values (returns 0, or 1 when a CUDA call failed).    */
+void xtgevc3_dggbal(char job, int n, double *A, int lda, double *B, int ldb, int *ilo, int *ihi, double *lscale,
+                    double *rscale, int *info);
+void xtgevc3_sggbal(char job, int n, float *A, int lda, float *B, int ldb, int *ilo, int *ihi, float *lscale,
+                    float *rscale, int *info);
+void xtgevc3_zggbal(char job, int n, double *A, int lda, double *B, int ldb, int *ilo, int *ihi, double *lscale,
+                    double *rscale, int *info);
+void xtgevc3_cggbal(char job, int n, float *A, int lda, float *B, int ldb, int *ilo, int *ihi, float *lscale,
+                    float *rscale, int *info);
+int xtgevc3_dggbal_dev(void *stream, char job, int n, double *A, int lda, double *B, int ldb, int *ilo, int *ihi,
+                       double *lscale, double *rscale, int *info);
+int xtgevc3_sggbal_dev(void *stream, char job, int n, float *A, int lda, float *B, int ldb, int *ilo, int *ihi,
+                       float *lscale, float *rscale, int *info);
+int xtgevc3_zggbal_dev(void *stream, char job, int n, double *A, int lda, double *B, int ldb, int *ilo, int *ihi,
+                       double *lscale, double *rscale, int *info);
+int xtgevc3_cggbal_dev(void *stream, char job, int n, float *A, int lda, float *B, int ldb, int *ilo, int *ihi,
+                       float *lscale, float *rscale, int *info);
+void xtgevc3_dggbak(char job, char side, int n, int ilo, int ihi, const double *lscale, const double *rscale, int m,
+                    double *V, int ldv, int *info);
+void xtgevc3_sggbak(char job, char side, int n, int ilo, int ihi, const float *lscale, const float *rscale, int m,
+                    float *V, int ldv, int *info);
+void xtgevc3_zggbak(char job, char side, int n, int ilo, int ihi, const double *lscale, const double *rscale, int m,
+                    double *V, int ldv, int *info);
+void xtgevc3_cggbak(char job, char side, int n, int ilo, int ihi, const float *lscale, const float *rscale, int m,
+                    float *V, int ldv, int *info);
+int xtgevc3_dggbak_dev(void *stream, char job, char side, int n, int ilo, int ihi, const double *lscale,
+                       const double *rscale, int m, double *V, int ldv, int *info);
+int xtgevc3_sggbak_dev(void *stream, char job, char side, int n, int ilo, int ihi, const float *lscale,
+                       const float *rscale, int m, float *V, int ldv, int *info);
+int xtgevc3_zggbak_dev(void *stream, char job, char side, int n, int ilo, int ihi, const double *lscale,
+                       const double *rscale, int m, double *V, int ldv, int *info);
+int xtgevc3_cggbak_dev(void *stream, char job, char side, int n, int ilo, int ihi, const float *lscale,
+                       const float *rscale, int m, float *V, int ldv, int *info);
+
 /* ---- allocation-free device entry point (no counterpart in the upstream library) -----
  * Same computation and arguments as xtgevc3_dtgevc3_dev (without flags), for callers that
  * cannot allocate device memory at this point: e.g. a framework that has reserved the

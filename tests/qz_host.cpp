@@ -271,12 +271,12 @@ int run_ggbal(int nth, int n, E *A, E *B, R *ls, R *rs, int *ilo, int *ihi)
 }
 
 template <class E, class R>
-int run_ggbak(int nth, int n, int ilo, int ihi, const R *scale, E *V)
+int run_ggbak(int nth, int n, int ilo, int ihi, const R *scale, E *V, int m = -1)
 {
     std::barrier<> bar(nth);
     std::vector<std::thread> th;
     for (int t = 0; t < nth; t++)
-        th.emplace_back([&, t] { ggbak_cta(CtaHost{t, nth, &bar}, n, ilo, ihi, scale, V, n); });
+        th.emplace_back([&, t] { ggbak_cta(CtaHost{t, nth, &bar}, n, ilo, ihi, scale, V, n, m); });
     for (auto &x : th) x.join();
     return 0;
 }
@@ -465,6 +465,12 @@ int host_zggbal(int nth, int n, double *A, double *B, double *ls, double *rs, in
 int host_dggbak(int nth, int n, int ilo, int ihi, const double *scale, double *V)
 {
     return run_ggbak(nth, n, ilo, ihi, scale, V);
+}
+
+// V n x m (leading dimension n)
+int host_dggbak_m(int nth, int n, int m, int ilo, int ihi, const double *scale, double *V)
+{
+    return run_ggbak(nth, n, ilo, ihi, scale, V, m);
 }
 
 int host_zggbak(int nth, int n, int ilo, int ihi, const double *scale, double *V)

@@ -1,7 +1,7 @@
 """Permutation balancing (xtgevc3_b200/csrc/ggbal.cuh: rb::ggbal_cta, LAPACK xGGBAL with
 JOB = 'P'; rb::ggbak_cta, xGGBAK with JOB = 'P') compiled for the CPU by tests/qz_host.cpp,
 against LAPACK's own DGGBAL / ZGGBAL / DGGBAK (their Fortran interfaces in SciPy's OpenBLAS),
-bit for bit: the permuted A and B, ILO, IHI and the isolated entries of LSCALE / RSCALE, on
+bit for bit: the permuted A and B, ILO, IHI, LSCALE and RSCALE, on
 pencils with isolated eigenvalues of every kind the search meets (rows with no or one
 off-diagonal nonzero, columns likewise, chains of them, a fully triangular pencil, none), on 1
 and several host threads."""
@@ -82,8 +82,7 @@ def test_ggbal_matches_lapack(host, cplx, kind, n):
         h = host_ggbal(host, A, B, nth)
         assert (h[2], h[3]) == (r[2], r[3]), (kind, h[2:4], r[2:4])
         assert np.array_equal(h[0], r[0]) and np.array_equal(h[1], r[1]), kind
-        iso = [i for i in range(n) if i < r[2] - 1 or i >= r[3]]
-        assert np.array_equal(h[4][iso], r[4][iso]) and np.array_equal(h[5][iso], r[5][iso]), kind
+        assert np.array_equal(h[4], r[4]) and np.array_equal(h[5], r[5]), (kind, h[4], r[4])
 
 
 @pytest.mark.parametrize("kind", KINDS[1:], ids=str)
@@ -138,3 +137,43 @@ def test_balanced_qz_flow_matches_lapack_gges(host, cplx, kind):
     for x, y in ((lam[fin], lam_r[fin]), (lam_r[fin], lam[fin])):
         d = np.abs(x[:, None] - y[None, :]).min(1) / np.maximum(np.abs(x), 1e-300)
         assert d.max() <= 1e-9, (kind, d.max())
+
+
+def test_ggbal_ggbak_argument_checks():
+    """xtgevc3_dggbal / dggbak: LAPACK's argument numbers, JOB = 'S' / 'B' refused (-1), all
+    before any device work; JOB = 'N' and n = 0 answered on the host (ILO = 1, IHI = n)."""
+    import xtgevc3_b200 as X
+    L = X.lib()
+    M = np.zeros((4, 4))
+    v = np.zeros(4)
+    ilo, ihi, info = ct.c_int(), ct.c_int(), ct.c_int()
+    for job, n, lda, ldb, want in ((b"S", 4, 4, 4, -1), (b"B", 4, 4, 4, -1), (b"X", 4, 4, 4, -1), (b"P", -1, 4, 4, -2),
+                                   (b"P", 4, 3, 4, -4), (b"P", 4, 4, 3, -6), (b"P", 0, 1, 1, 0)):
+        L.xtgevc3_dggbal(job, n, _p(M), lda, _p(M), ldb, ct.byref(ilo), ct.byref(ihi), _p(v), _p(v), ct.byref(info))
+        assert info.value == want, (job, n, info.value)
+    assert (ilo.value, ihi.value) == (1, 0)
+    for job, side, n, lo, hi, m, ldv, want in ((b"S", b"L", 4, 1, 4, 4, 4, -1), (b"P", b"X", 4, 1, 4, 4, 4, -2),
+                                               (b"P", b"L", -1, 1, 4, 4, 4, -3), (b"P", b"L", 4, 0, 4, 4, 4, -4),
+                                               (b"P", b"L", 4, 3, 2, 4, 4, -5), (b"P", b"L", 4, 1, 4, -1, 4, -8),
+                                               (b"P", b"L", 4, 1, 4, 4, 3, -10), (b"N", b"R", 4, 1, 4, 4, 4, 0)):
+        L.xtgevc3_dggbak(job, side, n, lo, hi, _p(v), _p(v), m, _p(M), ldv, ct.byref(info))
+        assert info.value == want, (job, side, info.value)
+
+
+@pytest.mark.parametrize("m", [1, 7, 30], ids=lambda m: f"m{m}")
+def test_ggbak_rectangular_matches_lapack(host, m):
+    """xGGBAK on n x m vectors (m other than n), both sides, against LAPACK DGGBAK."""
+    n = 17
+    A, B = structured("row_zero_col", n, 6, False)
+    r = lapack_ggbal(A, B)
+    V = np.asfortranarray(np.random.default_rng(2).standard_normal((n, m)))
+    for side, scale in ((b"L", r[4]), (b"R", r[5])):
+        Vr = V.copy(order="F")
+        iv = lambda v: ct.byref(ct.c_int(v))  # noqa: E731
+        info = ct.c_int()
+        oracle._openblas().scipy_dggbak_(ct.c_char_p(b"P"), ct.c_char_p(side), iv(n), iv(r[2]), iv(r[3]), _p(scale),
+                                          _p(scale), iv(m), _p(Vr), iv(n), ct.byref(info), ct.c_size_t(1),
+                                          ct.c_size_t(1))
+        Vh = V.copy(order="F")
+        host.host_dggbak_m(4, n, m, r[2], r[3], _p(np.ascontiguousarray(scale)), _p(Vh))
+        assert np.array_equal(Vh, Vr), side

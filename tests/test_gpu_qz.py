@@ -195,3 +195,34 @@ def test_gges_balances_structured_pencils(cuda_ok, kind, cplx):
     for x, y in ((lam[fin], lam_r[fin]), (lam_r[fin], lam[fin])):
         d = np.abs(x[:, None] - y[None, :]).min(1) / np.maximum(np.abs(x), 1e-300)
         assert d.max() <= 1e-9, (kind, d.max())
+
+
+@pytest.mark.late(2)  # the balancing kernels alone, not the QZ step
+@pytest.mark.parametrize("kind", ["none", "row_offdiag", "row_zero_col", "chain", "triangular", "permuted_triangular"],
+                         ids=str)
+@pytest.mark.parametrize("cplx", [False, True], ids=["d", "z"])
+def test_ggbal_ggbak_entry_points_match_lapack(cuda_ok, kind, cplx):
+    """xtgevc3_*ggbal / *ggbak (JOB = 'P') against LAPACK DGGBAL / ZGGBAL / DGGBAK, bit for bit (the
+    pencils and the oracle calls of tests/test_ggbal_host.py)."""
+    from test_ggbal_host import lapack_ggbal, structured
+    import ctypes as ct
+    import oracle
+    n = 17
+    A, B = structured(kind, n, 5, cplx)
+    r = lapack_ggbal(A, B)
+    a, b, ilo, ihi, ls, rs, info = X.ggbal(A, B)
+    assert info == 0 and (ilo, ihi) == (r[2], r[3])
+    assert np.array_equal(a, r[0]) and np.array_equal(b, r[1])
+    assert np.array_equal(ls, r[4]) and np.array_equal(rs, r[5])
+    if not cplx:
+        V = np.asfortranarray(np.random.default_rng(1).standard_normal((n, 7)))
+        for side, scale in (("L", ls), ("R", rs)):
+            Vr = V.copy(order="F")
+            iv = lambda v: ct.byref(ct.c_int(v))  # noqa: E731
+            inf = ct.c_int()
+            oracle._openblas().scipy_dggbak_(ct.c_char_p(b"P"), ct.c_char_p(side.encode()), iv(n), iv(ilo), iv(ihi),
+                                              scale.ctypes.data_as(ct.c_void_p), scale.ctypes.data_as(ct.c_void_p),
+                                              iv(7), Vr.ctypes.data_as(ct.c_void_p), iv(n), ct.byref(inf),
+                                              ct.c_size_t(1), ct.c_size_t(1))
+            Vh, info = X.ggbak(V, ilo, ihi, ls, rs, side=side)
+            assert info == 0 and np.array_equal(Vh, Vr), side

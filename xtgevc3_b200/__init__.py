@@ -155,6 +155,13 @@ def lib():
             f = getattr(L, f"xtgevc3_{p}tgsyl_dev")
             f.argtypes = [_P, _C, _I, _I, _I] + [_P, _I] * 6 + [_P, _P, _P]
             f.restype = _I
+        for p in "dszc":  # xGGBAL / xGGBAK (JOB 'N' or 'P')
+            f = getattr(L, f"xtgevc3_{p}ggbal")
+            f.argtypes = [_C, _I, _P, _I, _P, _I, _P, _P, _P, _P, _P]
+            f.restype = None
+            f = getattr(L, f"xtgevc3_{p}ggbak")
+            f.argtypes = [_C, _C, _I, _I, _I, _P, _P, _I, _P, _I, _P]
+            f.restype = None
         for p in "dszc":  # xTGSNA DIF on the device
             f = getattr(L, f"xtgevc3_{p}tgsna_dif_dev")
             f.argtypes = [_P, _C, _P, _I, _P, _I, _P, _I, _P, _I, _P, _P]
@@ -633,6 +640,41 @@ def tgsyl(ijob, A, B, C, D, E, F, trans="N"):
     if info.value == m + n + 1:
         raise RuntimeError(f"xtgevc3_{pfx}tgsyl failed: {last_error()}")
     return Rm, Lm, float(sd[0]), float(sd[1]), info.value
+
+
+def ggbal(A, B, job="P"):
+    """Host-array form of d/s/z/cggbal (JOB 'N' or 'P'): returns (A, B, ilo, ihi, lscale, rscale,
+    info) with the balanced A, B as new arrays."""
+    L = lib()
+    dt = A.dtype.type
+    pfx = {np.complex128: "z", np.complex64: "c", np.float64: "d", np.float32: "s"}[dt]
+    n = A.shape[0]
+    a, b = np.array(A, order="F", dtype=dt), np.array(B, order="F", dtype=dt)
+    rdt = np.float32 if pfx in "sc" else np.float64
+    ls, rs = np.zeros(max(n, 1), dtype=rdt), np.zeros(max(n, 1), dtype=rdt)
+    ilo, ihi, info = ct.c_int(0), ct.c_int(0), ct.c_int(0)
+    getattr(L, f"xtgevc3_{pfx}ggbal")(job.encode(), n, _ptr(a), max(n, 1), _ptr(b), max(n, 1), ct.byref(ilo),
+                                      ct.byref(ihi), _ptr(ls), _ptr(rs), ct.byref(info))
+    if info.value == n + 1 and n > 0:
+        raise RuntimeError(f"xtgevc3_{pfx}ggbal failed: {last_error()}")
+    return a, b, ilo.value, ihi.value, ls[:n], rs[:n], info.value
+
+
+def ggbak(V, ilo, ihi, lscale, rscale, side="L", job="P"):
+    """Host-array form of d/s/z/cggbak (JOB 'N' or 'P'): returns (V back-permuted, info)."""
+    L = lib()
+    dt = V.dtype.type
+    pfx = {np.complex128: "z", np.complex64: "c", np.float64: "d", np.float32: "s"}[dt]
+    n, m = V.shape
+    v = np.array(V, order="F", dtype=dt)
+    rdt = np.float32 if pfx in "sc" else np.float64
+    ls, rs = (np.ascontiguousarray(x, dtype=rdt) for x in (lscale, rscale))
+    info = ct.c_int(0)
+    getattr(L, f"xtgevc3_{pfx}ggbak")(job.encode(), side.encode(), n, ilo, ihi, _ptr(ls), _ptr(rs), m, _ptr(v),
+                                      max(n, 1), ct.byref(info))
+    if info.value == n + 1 and n > 0:
+        raise RuntimeError(f"xtgevc3_{pfx}ggbak failed: {last_error()}")
+    return v, info.value
 
 
 def tgexc(A, B, Q=None, Z=None, ifst=1, ilst=1, with_ifst=False):

@@ -9,9 +9,8 @@
 // no row qualifies it looks for a column J (from K up to L) whose entries in rows K..L are zero
 // except in at most one row I; it swaps rows I and K and columns J and K, records LSCALE(K) =
 // I, RSCALE(K) = J and repeats with K + 1.  ILO = K, IHI = L: outside [ILO, IHI] the pencil is
-// upper triangular, so those eigenvalues are isolated.  Entries of LSCALE / RSCALE outside the
-// isolated rows are left as given (xGGES does not read them); the permuted rows and columns
-// are exact copies.
+// upper triangular, so those eigenvalues are isolated.  LSCALE = RSCALE = 1 on [ILO, IHI], as
+// xGGBAL with JOB = 'P' leaves them; the permuted rows and columns are exact copies.
 //
 // B200 form: one CTA.  Each search step checks every candidate row (or column) in parallel,
 // a shared reduction picks the one xGGBAL's loop meets first (the largest row, the smallest
@@ -176,17 +175,23 @@ XTG_HD void ggbal_cta(const Cta &c, BalShared &sh, const BalPencil<E> &p, R *lsc
         *ilo = sh.k + 1;
         *ihi = sh.l;
     }
+    for (int i = sh.k + tid; i < sh.l; i += nth) {
+        lscale[i] = R(1);
+        rscale[i] = R(1);
+    }
     c.sync();
 }
 
-// xGGBAK 'P' for the Schur vectors V (n x n, leading dimension ldv): rows ilo-1 .. 1 and
-// ihi+1 .. n (1-based) swapped with the rows scale records, in that order.  Ends with a barrier.
+// xGGBAK 'P' for V (n x m, leading dimension ldv; m = n for the Schur vectors): rows ilo-1 .. 1
+// and ihi+1 .. n (1-based) swapped with the rows scale records, in that order.  Ends with a
+// barrier.
 template <class E, class R, class Cta>
-XTG_HD void ggbak_cta(const Cta &c, int n, int ilo, int ihi, const R *scale, E *V, int ldv)
+XTG_HD void ggbak_cta(const Cta &c, int n, int ilo, int ihi, const R *scale, E *V, int ldv, int m = -1)
 {
     const int tid = c.tid(), nth = c.nth();
+    const int cols = m < 0 ? n : m;
     auto swap_rows = [&](int i, int k) {
-        for (int col = tid; col < n; col += nth) {
+        for (int col = tid; col < cols; col += nth) {
             E t = V[(size_t)i + (size_t)col * ldv];
             V[(size_t)i + (size_t)col * ldv] = V[(size_t)k + (size_t)col * ldv];
             V[(size_t)k + (size_t)col * ldv] = t;

@@ -210,6 +210,14 @@ __global__ void __launch_bounds__(kQzThreads, 1) ggbak_kernel(int n, const int *
     rb::ggbak_cta(rb::CtaDev{}, n, ilohi[0], ilohi[1], scale, V, ldv);
 }
 
+// xGGBAK 'P' of an n x m V with host ILO, IHI (the entry point xtgevc3_*ggbak)
+template <class E, class R>
+__global__ void __launch_bounds__(kQzThreads, 1)
+    ggbak_m_kernel(int n, int ilo, int ihi, const R *scale, E *V, int ldv, int m)
+{
+    rb::ggbak_cta(rb::CtaDev{}, n, ilo, ihi, scale, V, ldv, m);
+}
+
 // xGGES's permutation balancing around the QZ step: gges_balance_in permutes A and B (ILO, IHI,
 // LSCALE, RSCALE stay on the device in bal), gges_balance_out permutes the rows of VSL / VSR
 // back (after the ordering, before the scaling back, as xGGES)
@@ -1071,6 +1079,186 @@ void tgsyl_host(char trans, int ijob, int m, int n, const R *A, int lda, const R
     }
 }
 
+// ---- xGGBAL / xGGBAK as entry points of their own (JOB 'N' or 'P') ---------------------------
+
+// LAPACK xGGBAL's checks: JOB (-1; 'S' and 'B', the scaling, are not built), N (-2), LDA (-4),
+// LDB (-6)
+int ggbal_check(char job, int n, int lda, int ldb)
+{
+    int info = 0;
+    if (job != 'N' && job != 'P') info = -1;
+    else if (n < 0) info = -2;
+    else if (lda < std::max(1, n)) info = -4;
+    else if (ldb < std::max(1, n)) info = -6;
+    if (info == -1 && (job == 'S' || job == 'B'))
+        set_last_error("xGGBAL: JOB = 'S' / 'B' (the scaling) is not built");
+    else if (info)
+        set_last_error("xGGBAL: argument " + std::to_string(-info) + " has an illegal value");
+    return info;
+}
+
+// device pointers (lscale, rscale n each on the device); returns 0, or 1 when a CUDA call failed
+template <class E, class R>
+int ggbal_device(cudaStream_t st, char job, int n, E *A, int lda, E *B, int ldb, int *ilo, int *ihi, R *lscale,
+                 R *rscale, int *info)
+{
+    set_last_error("");
+    job = (char)std::toupper((unsigned char)job);
+    *info = ggbal_check(job, n, lda, ldb);
+    if (*info) return 0;
+    *ilo = 1;
+    *ihi = n;
+    if (n == 0) return 0;
+    cudaError_t e = cudaSuccess;
+    if (job == 'N') {
+        const std::vector<R> ones(n, R(1));
+        e = cudaMemcpyAsync(lscale, ones.data(), n * sizeof(R), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(rscale, ones.data(), n * sizeof(R), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    } else {
+        int *d = nullptr, h[2] = {1, n};
+        e = cudaMallocAsync(&d, (2 + 2 * kQzThreads) * sizeof(int), st);
+        if (e == cudaSuccess) {
+            const rb::BalPencil<E> p{n, A, B, lda, ldb};
+            ggbal_kernel<E, R><<<1, kQzThreads, 0, st>>>(p, lscale, rscale, d, d + 2);
+            count_launches(1);
+            e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, 2 * sizeof(int), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            cudaFreeAsync(d, st);
+        }
+        *ilo = h[0];
+        *ihi = h[1];
+    }
+    if (e != cudaSuccess) {
+        set_last_error(std::string("xGGBAL: ") + cudaGetErrorString(e));
+        return 1;
+    }
+    return 0;
+}
+
+// host pointers; INFO = n + 1 (not a LAPACK value) when a CUDA call failed
+template <class E, class R>
+void ggbal_host(char job, int n, E *A, int lda, E *B, int ldb, int *ilo, int *ihi, R *lscale, R *rscale, int *info)
+{
+    set_last_error("");
+    *info = ggbal_check((char)std::toupper((unsigned char)job), n, lda, ldb);
+    if (*info) return;
+    *ilo = 1;
+    *ihi = n;
+    if (n == 0) return;
+    cudaStream_t st = nullptr;
+    E *dA = nullptr, *dB = nullptr;
+    R *ds = nullptr;
+    const size_t col = (size_t)n * sizeof(E);
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocAsync(&dA, col * n, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&dB, col * n, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&ds, 2 * (size_t)n * sizeof(R), st);
+    if (e == cudaSuccess) e = cudaMemcpy2DAsync(dA, col, A, (size_t)lda * sizeof(E), col, n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpy2DAsync(dB, col, B, (size_t)ldb * sizeof(E), col, n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        if (ggbal_device<E, R>(st, job, n, dA, n, dB, n, ilo, ihi, ds, ds + n, info) != 0) {
+            e = cudaErrorUnknown;
+        } else {
+            e = cudaMemcpy2DAsync(A, (size_t)lda * sizeof(E), dA, col, col, n, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess)
+                e = cudaMemcpy2DAsync(B, (size_t)ldb * sizeof(E), dB, col, col, n, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(lscale, ds, n * sizeof(R), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(rscale, ds + n, n * sizeof(R), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        }
+    }
+    for (void *q : {(void *)dA, (void *)dB, (void *)ds})
+        if (q) cudaFreeAsync(q, st);
+    if (st) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
+    if (e != cudaSuccess) {
+        if (e != cudaErrorUnknown) set_last_error(std::string("xGGBAL staging: ") + cudaGetErrorString(e));
+        *info = n + 1;
+    }
+}
+
+// LAPACK xGGBAK's checks: JOB (-1; 'S', 'B' not built), SIDE (-2), N (-3), ILO (-4), IHI (-5),
+// M (-8), LDV (-10)
+int ggbak_check(char job, char side, int n, int ilo, int ihi, int m, int ldv)
+{
+    int info = 0;
+    if (job != 'N' && job != 'P') info = -1;
+    else if (side != 'L' && side != 'R') info = -2;
+    else if (n < 0) info = -3;
+    else if (ilo < 1 || ilo > std::max(1, n)) info = -4;
+    else if ((n == 0 && ihi != 0 && ilo != 1) || (n > 0 && (ihi < ilo || ihi > std::max(1, n)))) info = -5;
+    else if (m < 0) info = -8;
+    else if (ldv < std::max(1, n)) info = -10;
+    if (info == -1 && (job == 'S' || job == 'B'))
+        set_last_error("xGGBAK: JOB = 'S' / 'B' (the scaling) is not built");
+    else if (info)
+        set_last_error("xGGBAK: argument " + std::to_string(-info) + " has an illegal value");
+    return info;
+}
+
+// device pointers (lscale, rscale and V on the device)
+template <class E, class R>
+int ggbak_device(cudaStream_t st, char job, char side, int n, int ilo, int ihi, const R *lscale, const R *rscale, int m,
+                 E *V, int ldv, int *info)
+{
+    set_last_error("");
+    job = (char)std::toupper((unsigned char)job);
+    side = (char)std::toupper((unsigned char)side);
+    *info = ggbak_check(job, side, n, ilo, ihi, m, ldv);
+    if (*info || n == 0 || m == 0 || job == 'N') return 0;
+    ggbak_m_kernel<E, R><<<1, kQzThreads, 0, st>>>(n, ilo, ihi, side == 'L' ? lscale : rscale, V, ldv, m);
+    count_launches(1);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        set_last_error(std::string("xGGBAK: ") + cudaGetErrorString(e));
+        return 1;
+    }
+    return 0;
+}
+
+template <class E, class R>
+void ggbak_host(char job, char side, int n, int ilo, int ihi, const R *lscale, const R *rscale, int m, E *V, int ldv,
+                int *info)
+{
+    set_last_error("");
+    const char jb = (char)std::toupper((unsigned char)job), sd = (char)std::toupper((unsigned char)side);
+    *info = ggbak_check(jb, sd, n, ilo, ihi, m, ldv);
+    if (*info || n == 0 || m == 0 || jb == 'N') return;
+    cudaStream_t st = nullptr;
+    E *dV = nullptr;
+    R *ds = nullptr;
+    const size_t col = (size_t)n * sizeof(E);
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocAsync(&dV, col * m, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&ds, n * sizeof(R), st);
+    if (e == cudaSuccess) e = cudaMemcpy2DAsync(dV, col, V, (size_t)ldv * sizeof(E), col, m, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ds, sd == 'L' ? lscale : rscale, n * sizeof(R), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        if (ggbak_device<E, R>(st, jb, sd, n, ilo, ihi, ds, ds, m, dV, n, info) != 0) {
+            e = cudaErrorUnknown;
+        } else {
+            e = cudaMemcpy2DAsync(V, (size_t)ldv * sizeof(E), dV, col, col, m, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        }
+    }
+    if (dV) cudaFreeAsync(dV, st);
+    if (ds) cudaFreeAsync(ds, st);
+    if (st) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
+    if (e != cudaSuccess) {
+        if (e != cudaErrorUnknown) set_last_error(std::string("xGGBAK staging: ") + cudaGetErrorString(e));
+        *info = n + 1;
+    }
+}
+
 }  // namespace
 }  // namespace xtg
 
@@ -1346,5 +1534,45 @@ int xtgevc3_ctgsyl_dev(void *stream, char trans, int ijob, int m, int n, const f
     return xtg::tgsyl_device<float, true>(static_cast<cudaStream_t>(stream), trans, ijob, m, n, A, lda, B, ldb, C, ldc,
                                           D, ldd, E, lde, F, ldf, scale, dif, info);
 }
+
+}  // extern "C"
+
+// ---- xGGBAL / xGGBAK (JOB 'N' or 'P') -----------------------------------------------------------
+
+using xtg::rb::zc;
+
+extern "C" {
+
+#define XTG_GGBAL(P, E, R)                                                                                          \
+    void xtgevc3_##P##ggbal(char job, int n, R *A, int lda, R *B, int ldb, int *ilo, int *ihi, R *lscale, R *rscale, \
+                            int *info)                                                                              \
+    {                                                                                                               \
+        xtg::ggbal_host<E, R>(job, n, reinterpret_cast<E *>(A), lda, reinterpret_cast<E *>(B), ldb, ilo, ihi,       \
+                              lscale, rscale, info);                                                                \
+    }                                                                                                               \
+    int xtgevc3_##P##ggbal_dev(void *stream, char job, int n, R *A, int lda, R *B, int ldb, int *ilo, int *ihi,      \
+                               R *lscale, R *rscale, int *info)                                                     \
+    {                                                                                                               \
+        return xtg::ggbal_device<E, R>(static_cast<cudaStream_t>(stream), job, n, reinterpret_cast<E *>(A), lda,    \
+                                       reinterpret_cast<E *>(B), ldb, ilo, ihi, lscale, rscale, info);              \
+    }                                                                                                               \
+    void xtgevc3_##P##ggbak(char job, char side, int n, int ilo, int ihi, const R *lscale, const R *rscale, int m,   \
+                            R *V, int ldv, int *info)                                                               \
+    {                                                                                                               \
+        xtg::ggbak_host<E, R>(job, side, n, ilo, ihi, lscale, rscale, m, reinterpret_cast<E *>(V), ldv, info);      \
+    }                                                                                                               \
+    int xtgevc3_##P##ggbak_dev(void *stream, char job, char side, int n, int ilo, int ihi, const R *lscale,          \
+                               const R *rscale, int m, R *V, int ldv, int *info)                                    \
+    {                                                                                                               \
+        return xtg::ggbak_device<E, R>(static_cast<cudaStream_t>(stream), job, side, n, ilo, ihi, lscale, rscale, m, \
+                                       reinterpret_cast<E *>(V), ldv, info);                                        \
+    }
+
+XTG_GGBAL(d, double, double)
+XTG_GGBAL(s, float, float)
+XTG_GGBAL(z, zc<double>, double)
+XTG_GGBAL(c, zc<float>, float)
+
+#undef XTG_GGBAL
 
 }  // extern "C"
