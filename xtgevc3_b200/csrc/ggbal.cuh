@@ -198,13 +198,14 @@ XTG_HD void ggbak_cta(const Cta &c, int n, int ilo, int ihi, const R *scale, E *
         }
         c.sync();
     };
+    // a recorded row outside 1..n (scales not made by xGGBAL) is skipped: no access outside V
     for (int i = ilo - 1; i >= 1; i--) {
         const int k = (int)scale[i - 1];
-        if (k != i) swap_rows(i - 1, k - 1);
+        if (k != i && k >= 1 && k <= n) swap_rows(i - 1, k - 1);
     }
     for (int i = ihi + 1; i <= n; i++) {
         const int k = (int)scale[i - 1];
-        if (k != i) swap_rows(i - 1, k - 1);
+        if (k != i && k >= 1 && k <= n) swap_rows(i - 1, k - 1);
     }
     c.sync();
 }
